@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the LW-FR time step (TrixiLW hot path) on B200.
+
+Workload (default): isentropic vortex, periodic TreeMesh [-10,10]^2 with 512 x 512 elements, N = 4,
+compressible Euler, FP64, Lax-Wendroff with CFL-based dt (cfl = 0.98 * (N+1) * 0.103) computed on the
+device every step. A step is one perform_step! (dt reduction + rhs + update) over all 6.55 M nodes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+One JSON line on rank 0. `value`: whole-job DOF-updates/s with the state resident in HBM (CUDA events on
+the library's stream around K graph-replayed steps, max over ranks). `e2e`: the same metric through
+the C ABI with host buffers (per step: pinned host -> device upload of u, one step, device -> host
+download of u). `--impl reference` times the CPU oracle port (the reference itself is Julia and cannot
+run on these machines) on the same workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "trixilw.jl_b200"))
+
+METRIC = "LW-FR DOF-updates/s on 1 B200 (% HBM roofline); batched & adjoint vs plain"
+UNIT = "DOF-updates/s"
+
+# name -> (refinement level, N, time discretization, initial condition)
+WORKLOADS = {
+    "vortex_tree512_N4_lw": (9, 4, "lw", "vortex"),
+    "vortex_tree512_N3_lw": (9, 3, "lw", "vortex"),
+    "vortex_tree512_N5_lw": (9, 5, "lw", "vortex"),
+    "vortex_tree256_N4_lw": (8, 4, "lw", "vortex"),
+    "vortex_tree512_N4_mdrk": (9, 4, "mdrk", "vortex"),
+    "riemann_tree512_N4_lw": (9, 4, "lw", "riemann"),
+}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def alg_bytes_per_element_step(N: int, td: str) -> float:
+    """Algorithmic HBM bytes of one rhs/step per element (two-pass model): 8 nv (2n^2 + 28n - 8);
+    an MDRK step is 2 B + 8 nv 6 n^2."""
+    n, nv = N + 1, 4
+    b = 8 * nv * (2 * n * n + 28 * n - 8)
+    return 2 * b + 8 * nv * 6 * n * n if td == "mdrk" else b
+
+
+def volume_kernel_bytes_per_element(N: int, td: str) -> float:
+    """Algorithmic bytes of one LW volume-kernel launch per element: read u (nv n^2), write u_new
+    (nv n^2), write the face traces of U and F.n (2 x 4 faces x n x nv)."""
+    n, nv = N + 1, 4
+    return 8.0 * (2 * nv * n * n + 2 * 4 * n * nv)
+
+
+def volume_flops_per_node(N: int) -> float:
+    """Algorithmic FP64 flops per node of the LW volume kernel (FMA = 2, divides not counted):
+    N >= 4: 20 n nv + 17 * 17 + 300; N = 3: 16 n nv + 11 * 17 + 200."""
+    n, nv = N + 1, 4
+    if N >= 4:
+        return 20 * n * nv + 17 * 17 + 300
+    return 16 * n * nv + 11 * 17 + 200
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(kernel_tag: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if one exists."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_tag}.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch_full_size:\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() in ("active", "1", "0x1"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+
+
+def build_semi(tl, level, N, td, icname, device):
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    tdo = tl.LW() if td == "lw" else tl.MDRK()
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tdo))
+    if icname == "vortex":
+        mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), level)
+        ic = tl.IsentropicVortex(5.0)
+        semi = tl.SemidiscretizationHyperbolic(mesh, tdo, eq, ic, solver, device=device)
+    else:
+        mesh = tl.TreeMesh((0.0, 0.0), (1.0, 1.0), level, periodicity=False)
+        ic = tl.FourQuadrantRiemann()
+        semi = tl.SemidiscretizationHyperbolic(mesh, tdo, eq, ic, solver, device=device,
+                                               boundary_conditions=tl.BoundaryConditionDirichlet(ic))
+        semi._prepare_boundaries(0.0, 0.0, 1.0)
+    return semi
+
+
+def cfl_for(N):
+    """0.98 of the LW stability limit: trixi2lw(0.98) = 0.98 (N+1) lw_fourier_cfl(N) for N <= 4
+    (src/auxiliary/auxiliary.jl:14-23). The reference tabulates no limit for N = 5; 0.98 * 6 * 0.07 is
+    used there (a value below the N = 4 limit, stable on the vortex)."""
+    table = {1: 1.000, 2: 0.333, 3: 0.170, 4: 0.103}
+    return 0.98 * (N + 1) * table.get(N, 0.07)
+
+
+def cpu_oracle_rate(level, N, td, icname, steps_hint, budget_s=20.0):
+    """Oracle port (C++/OpenMP, all host threads) on the same workload: DOF-updates/s over a bounded
+    number of steps (as many as fit in about budget_s seconds, at least one)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle
+    import trixilw as tl
+
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    if icname == "vortex":
+        mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), level)
+        ic = tl.IsentropicVortex(5.0)
+    else:
+        mesh = tl.TreeMesh((0.0, 0.0), (1.0, 1.0), level, periodicity=False)
+        ic = tl.FourQuadrantRiemann()
+    xy = mesh.node_coordinates(N)
+    u = np.ascontiguousarray(np.transpose(ic(xy[0], xy[1], 0.0, eq), (2, 1, 0, 3))).reshape(-1)
+    o = pyoracle.Oracle(mesh, N)
+    if mesh.n_boundaries:
+        bxy = mesh.boundary_node_coordinates(N)
+        now = np.ascontiguousarray(np.transpose(ic(bxy[0], bxy[1], 0.0, eq), (1, 0, 2)))
+        o.set_boundary_data(np.repeat(now[:, :, None, :], N + 1, axis=2), now)
+    threads = os.cpu_count() or 1
+    kind = 0 if td == "lw" else 1
+    cfl = cfl_for(N)
+    t0 = time.perf_counter()
+    o.steps(u, 1, cfl, 0.0, 1e9, kind=kind, nthreads=threads)
+    one = time.perf_counter() - t0
+    nsteps = max(1, min(steps_hint, int(budget_s / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    o.steps(u, nsteps, cfl, 0.0, 1e9, kind=kind, nthreads=threads)
+    el = time.perf_counter() - t0
+    return mesh.ndofs(N) * nsteps / el, threads, nsteps, el
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    level, N, td, icname = WORKLOADS[args.workload]
+    # warm-up: one step; then K steps, each a bounded sample of the same workload (one full step)
+    rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=max(1, args.steps), budget_s=60.0)
+    ndofs = (1 << (2 * level)) * (N + 1) ** 2
+    sample = f"{nsteps} full steps of the {args.workload} workload ({ndofs} DOF) in {el:.2f} s"
+    out = {
+        "metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": nsteps,
+        "warmup": 1, "ms_per_step": 1e3 * el / nsteps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "ndofs": ndofs, "polydeg": N, "time_discretization": td,
+                   "elements": 1 << (2 * level), "implementation": "CPU oracle port (C++/OpenMP) of the TrixiLW "
+                   "LW rhs; the Julia reference cannot run here"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    import trixilw as tl
+    from trixilw import _lib
+
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    level, N, td, icname = WORKLOADS[args.workload]
+    semi = build_semi(tl, level, N, td, icname, local_rank)
+    ndofs = semi.ndofs()
+    cfl = cfl_for(N)
+    u0 = semi.compute_coefficients(0.0)
+    upd = tl.semidiscretize(semi, semi.time_discretization, (0.0, 1e9))
+    integ = tl.LWIntegrator(upd)
+    integ.set_state(u0, 0.0)
+    L = _lib.lib()
+    sp = ctypes.c_void_p()
+    L.tlw_get_stream(semi.handle, ctypes.byref(sp))
+    stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", local_rank))
+
+    # warm-up (also captures the CUDA graphs)
+    integ.step(max(args.warmup, 3) if args.warmup > 0 else 3, cfl)
+    check = L.tlw_synchronize(semi.handle)
+    _lib.check(semi.handle, check)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank]) \
+        if os.environ.get("CUDA_VISIBLE_DEVICES") else local_rank
+    sampler = ClockSampler(gpu_index)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    integ.step(args.steps, cfl)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    _lib.check(semi.handle, L.tlw_synchronize(semi.handle))
+    # per-phase device time of K further steps (events between the kernels of each step)
+    phase = (ctypes.c_double * 5)()
+    _lib.check(semi.handle, L.tlw_step_timed(semi.handle, args.steps, cfl, 0.0, 1e9, phase))
+    clocks = sampler.stop()
+    ms_max = ms
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = ndofs * args.steps * world / (ms_max * 1e-3)
+
+    # end-to-end through the C ABI with host buffers: pinned u in, one step, pinned u out
+    n_e2e = max(1, min(args.steps, 20))
+    uh = torch.empty(u0.size, dtype=torch.float64, pin_memory=True).numpy()
+    uh[:] = u0
+    ub = uh.ctypes.data_as(ctypes.c_void_p)
+    tt = ctypes.c_double()
+    L.tlw_set_state(semi.handle, ub, _lib.TLW_WHERE_HOST, 0.0)
+    L.tlw_step(semi.handle, 1, cfl, 0.0, 1e9, 1)
+    L.tlw_get_state(semi.handle, ub, _lib.TLW_WHERE_HOST, ctypes.byref(tt))
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(n_e2e):
+        _lib.check(semi.handle, L.tlw_set_state(semi.handle, ub, _lib.TLW_WHERE_HOST, tt.value))
+        _lib.check(semi.handle, L.tlw_step(semi.handle, 1, cfl, 0.0, 1e9, 1))
+        _lib.check(semi.handle, L.tlw_get_state(semi.handle, ub, _lib.TLW_WHERE_HOST, ctypes.byref(tt)))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = ndofs * n_e2e * world / (ms_e2e * 1e-3)
+    state_bytes = 8 * 4 * ndofs
+
+    if rank == 0:
+        E = semi.mesh.n_elements
+        peak, peak_kind = measured_peaks()
+        vol_ms = phase[1] / args.steps
+        vol_bytes = volume_kernel_bytes_per_element(N, td) * E
+        achieved = vol_bytes / (vol_ms * 1e-3) / 1e9
+        fp = ctypes.c_double()
+        fp64_peak = fp.value if L.tlw_probe_fp64_tflops(local_rank, ctypes.byref(fp)) == 0 else None
+        vol_flops = volume_flops_per_node(N) * ndofs
+        tag = f"lw_volume_kernel_N{N}_tree{1 << level}"
+        traffic = profile_traffic(tag)
+        step_alg = alg_bytes_per_element_step(N, td) * E
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "polydeg": N, "elements": E, "ndofs": ndofs,
+                       "time_discretization": td, "cfl": cfl, "dt": "device CFL reduction every step",
+                       "l2": "inputs larger than L2 (state %.0f MB per array)" % (state_bytes / 1e6),
+                       "parallelism": f"replicas{world}" if world > 1 else "single"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                    "steps": n_e2e},
+            "roofline": {"kernel": f"lw_volume_kernel<{N}, MODE_STEP>", "bound": "hbm", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                         "alg_bytes_per_launch": vol_bytes, "ms_per_launch": vol_ms,
+                         "fp64": {"achieved_tflops": vol_flops / (vol_ms * 1e-3) / 1e12, "peak_tflops": fp64_peak,
+                                  "frac": (vol_flops / (vol_ms * 1e-3) / 1e12) / fp64_peak if fp64_peak else None,
+                                  "peak_source": "measured live (register FMA loop)"},
+                         "step": {"alg_bytes_per_step": step_alg,
+                                  "achieved_gbs": step_alg * args.steps / (ms_max * 1e-3) / 1e9,
+                                  "frac": step_alg * args.steps / (ms_max * 1e-3) / 1e9 / peak},
+                         "phase_ms_per_step": {"cfl_dt": phase[0] / args.steps, "volume": phase[1] / args.steps,
+                                               "x_faces": phase[2] / args.steps, "y_faces": phase[3] / args.steps,
+                                               "step": phase[4] / args.steps}},
+            "clocks": clocks,
+            "gpu_launches": args.steps * (5 + (2 if semi.mesh.n_boundaries else 0)) * (2 if td == "mdrk" else 1),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=args.steps)
+            out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                   "sample": f"{nsteps} full steps of the same workload ({ndofs} DOF), {el:.1f} s"}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="vortex_tree512_N4_lw", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,138 @@
+/* tlw.h -- C ABI of libtlw, a B200 (sm_100a) implementation of TrixiLW's Lax-Wendroff / MDRK
+ * flux-reconstruction right-hand side for the 2D compressible Euler equations on TreeMesh{2}.
+ *
+ * The entry points are what a Julia shim binds with `ccall` to replace the reference's
+ *   rhs!(du_ode, u_ode, semi, t)         src/semidiscretization/semidiscretization_hyperbolic.jl:4-20
+ *   rhs_mdrk1!/rhs_mdrk2!                src/semidiscretization/semidiscretization_hyperbolic.jl:22-56
+ * and, below them, the mesh-level
+ *   rhs!(du, u, t, dt, mesh::TreeMesh{2}, ..., ::LW, cache, tol)   src/solvers/dgsem_tree/dg_2d.jl:28-83
+ *   rhs_mdrk1!/rhs_mdrk2!(..., mesh::TreeMesh{2}, ...)           src/solvers/dgsem_tree/multi_derivative_2d.jl:1-116
+ * plus the CFL step loop of solve_lwfr (src/solvers/lwfr.jl:176-263, src/solvers/mdrk.jl:1-29) run on the
+ * device. All arrays use the reference's Julia layout (column-major, leftmost index fastest):
+ *   u, du: [v, i, j, element] with v = 1..4 (rho, rho v1, rho v2, rho e), i, j = 1..N+1.
+ * Integer connectivity is accepted exactly as Trixi stores it (Int64, 1-based).
+ *
+ * Every function returns an int status (TLW_OK = 0). A handle is not thread-safe; it owns one CUDA
+ * stream and all device memory it uses. Calls with TLW_WHERE_HOST pointers copy in and out and return
+ * after the result is in host memory; calls with TLW_WHERE_DEVICE pointers are asynchronous on the
+ * handle's stream. Kernels never trap: a square root of a negative number (the reference raises
+ * DomainError there) sets a sticky status that the next synchronising call returns as
+ * TLW_E_NONADMISSIBLE.
+ */
+#ifndef TLW_H
+#define TLW_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TLW_ABI_VERSION 1
+
+enum tlw_status {
+    TLW_OK = 0,
+    TLW_E_ARG = 1,             /* invalid argument / size / option */
+    TLW_E_CUDA = 2,            /* CUDA runtime error (see tlw_last_error) */
+    TLW_E_NONADMISSIBLE = 3,   /* negative pressure or density met in a square root (Julia DomainError) */
+    TLW_E_STATE = 4,           /* call out of order (e.g. no mesh set) */
+    TLW_E_UNSUPPORTED = 5      /* option combination not built */
+};
+
+enum tlw_time_discretization { TLW_LW = 0, TLW_MDRK = 1 };              /* src/basic_types.jl:4-6 */
+enum tlw_surface_flux { TLW_FLUX_RUSANOV = 0, TLW_FLUX_HLL = 1 };        /* flux_lax_friedrichs / FluxHLL */
+enum tlw_max_speed { TLW_SPEED_NAIVE = 0, TLW_SPEED_DAVIS = 1 };         /* Trixi max_abs_speed_naive / max_abs_speed */
+enum tlw_where { TLW_WHERE_HOST = 0, TLW_WHERE_DEVICE = 1 };
+enum tlw_stage { TLW_STAGE_LW = 0, TLW_STAGE_MDRK1 = 1, TLW_STAGE_MDRK2 = 2 };
+enum tlw_cache_item {
+    TLW_CACHE_U_TRACES = 0,    /* time-averaged U on the 4 faces, [v, l, face, element], face = -x,+x,-y,+y */
+    TLW_CACHE_F_TRACES = 1,    /* normal time-averaged flux (F on x faces, G on y faces), same layout */
+    TLW_CACHE_U2 = 2,          /* MDRK stage-1 U2 [v, i, j, element]   (MDRKElementCache.U2) */
+    TLW_CACHE_F2 = 3           /* MDRK stage-1 F2 [v, d, i, j, element] (MDRKElementCache.F2) */
+};
+
+typedef struct tlw_opts {
+    int32_t polydeg;               /* N, 1..7 */
+    int32_t time_discretization;   /* TLW_LW | TLW_MDRK */
+    int32_t surface_flux;          /* TLW_FLUX_RUSANOV | TLW_FLUX_HLL */
+    int32_t max_speed;             /* TLW_SPEED_NAIVE (Trixi default of the reference's era) | TLW_SPEED_DAVIS */
+    double gamma;                  /* CompressibleEulerEquations2D(gamma) */
+    int32_t device;                /* CUDA device ordinal */
+    int32_t reserved[7];           /* zero */
+} tlw_opts;
+
+typedef struct tlw_handle tlw_handle;
+
+int32_t tlw_abi_version(void);
+
+/* Builds the solver state (basis, stream, device scalars). Replaces the cache construction
+ * create_cache(mesh, equations, ::AbstractLWTimeDiscretization, dg, ...)
+ * src/solvers/dgsem_tree/containers.jl:7-71 / src/semidiscretization/semidiscretization_hyperbolic.jl:58-84. */
+int tlw_create(const tlw_opts* opts, tlw_handle** out);
+int tlw_destroy(tlw_handle* h);
+
+/* Uploads TreeMesh{2} connectivity (Trixi containers, 1-based Int64) and the per-element inverse
+ * Jacobian (= 2 / element length). Call again after every AMR resize (src/callbacks/amr.jl:2-20).
+ *   interface_neighbor_ids [2, n_interfaces]  (left, right)  Trixi interfaces.neighbor_ids
+ *   interface_orientations [n_interfaces]     1 = x, 2 = y   Trixi interfaces.orientations
+ *   boundary_* [n_boundaries]                 Trixi boundaries.neighbor_ids / orientations / neighbor_sides
+ *   n_boundaries_per_direction [4]            boundaries grouped by direction 1..4 (dg_2d.jl:1385-1409)
+ * Nonconforming meshes (mortars) are not built: pass none. */
+int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_jacobian, int64_t n_interfaces,
+                      const int64_t* interface_neighbor_ids, const int64_t* interface_orientations,
+                      int64_t n_boundaries, const int64_t* boundary_neighbor_ids,
+                      const int64_t* boundary_orientations, const int64_t* boundary_neighbor_sides,
+                      const int64_t* n_boundaries_per_direction);
+
+/* Exterior states of the time-averaged Dirichlet boundary condition (src/equations/equations.jl:6-37):
+ *   levels [v, q, l, boundary]: boundary_value_function(x_l, t + 0.5*dt_scaled*(x_q + 1)) at the N+1 GLL
+ *                              time levels q (dt_scaled = scaling_factor * dt)
+ *   now    [v, l, boundary]:    boundary_value_function(x_l, t)
+ * Held until replaced; required before any rhs when the mesh has boundaries. */
+int tlw_set_boundary_data(tlw_handle* h, const double* levels, const double* now, int32_t where);
+
+/* One right-hand side evaluation: du = rhs(u) exactly as the reference's rhs!/rhs_mdrk1!/rhs_mdrk2!
+ * (du already multiplied by -J^{-1}, ready for u_new = u + dt*du). For TLW_STAGE_MDRK2, `us` is the
+ * stage state u* = u + dt*du1 (cache.element_cache.mdrk_cache.us); U2/F2 come from the preceding
+ * TLW_STAGE_MDRK1 call on the same handle. */
+int tlw_rhs(tlw_handle* h, int32_t stage, double* du, const double* u, const double* us, double t, double dt,
+            int32_t where);
+
+/* cfl * max_dt(u) (Trixi max_dt for TreeMesh{2}; src/solvers/lwfr.jl:176-190). Synchronous. */
+int tlw_max_dt(tlw_handle* h, const double* u, int32_t where, double cfl, double* dt_out);
+
+/* Device-resident time stepping (the LWIntegrator loop of solve_lwfr, CFLBased). */
+int tlw_set_state(tlw_handle* h, const double* u, int32_t where, double t);
+int tlw_get_state(tlw_handle* h, double* u, int32_t where, double* t_out);
+/* Runs up to nsteps steps of perform_step!(..., ::CFLBased, ::LW|::MDRK): dt = cfl * max_dt(u) (or
+ * fixed_dt when > 0), clamped to t_end, u <- u + dt * rhs(u). dt never leaves the device. The steps are
+ * replayed from a captured CUDA graph when use_graph != 0. Asynchronous. */
+int tlw_step(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double t_end, int32_t use_graph);
+/* As tlw_step without graphs, with CUDA events between the phases of each step. Synchronous. On return
+ * phase_ms[0..4] hold the summed device time of: CFL reduction (max speed + dt), volume kernel(s),
+ * x interfaces + x boundaries, y interfaces + y boundaries, and the whole steps. (Measurement entry: no
+ * counterpart in the reference.) */
+int tlw_step_timed(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double t_end, double* phase_ms);
+/* Measures the device's dense FP64 FMA throughput (TFLOP/s) with a bounded register-resident loop.
+ * Roofline calibration only (no counterpart in the reference). */
+int tlw_probe_fp64_tflops(int32_t device, double* tflops);
+/* Synchronous: current time, last dt and number of accepted steps. */
+int tlw_get_time(tlw_handle* h, double* t, double* dt_last, int64_t* steps);
+
+/* Element/interface caches of the last rhs (layouts in tlw_cache_item). Synchronous. */
+int tlw_get_cache(tlw_handle* h, int32_t item, double* out, int32_t where);
+int64_t tlw_cache_size(tlw_handle* h, int32_t item);
+
+/* Waits for the handle's stream; returns TLW_E_NONADMISSIBLE if a kernel flagged a bad state. */
+int tlw_synchronize(tlw_handle* h);
+/* The handle's cudaStream_t (for event timing / interop). */
+int tlw_get_stream(tlw_handle* h, void** stream);
+/* Device address of the current state (valid until the next tlw_step / tlw_set_tree_mesh). */
+int tlw_state_pointer(tlw_handle* h, double** dptr);
+const char* tlw_last_error(tlw_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TLW_H */

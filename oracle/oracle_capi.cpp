@@ -1,0 +1,158 @@
+// oracle_capi.cpp -- C entry points of the CPU oracle (TEST INFRASTRUCTURE ONLY: called from tests/,
+// the smoke check and the CPU-baseline leg of bench.py; never from the product path).
+// Parity status: unpinned against the reference itself (no Julia here); see tlw_oracle.hpp.
+#include <chrono>
+#include <cstdio>
+#include <memory>
+
+#include "tlw_oracle.hpp"
+
+using namespace tlwo;
+
+struct oracle_handle {
+    Basis basis;
+    Euler eq;
+    Options opt;
+    TreeMesh mesh;
+    Workspace ws;
+    std::vector<double> us;      // MDRK stage state u*
+    std::vector<double> du;
+    std::vector<double> bnd_levels, bnd_now;
+    char err[256] = {0};
+};
+
+extern "C" {
+
+int oracle_basis(int N, double* nodes, double* weights, double* D, double* Dhat) {
+    try {
+        Basis b = make_basis(N);
+        for (int i = 0; i < b.n; ++i) { nodes[i] = b.nodes[i]; weights[i] = b.weights[i]; }
+        for (int k = 0; k < b.n * b.n; ++k) { D[k] = b.D[k]; Dhat[k] = b.Dhat[k]; }
+        return 0;
+    } catch (...) { return 1; }
+}
+
+oracle_handle* oracle_create(int N, double gamma, int flux_kind, int speed_kind, int E, const double* inv_jac,
+                             int I, const int32_t* left, const int32_t* right, const int32_t* orient, int B,
+                             const int32_t* b_elem, const int32_t* b_orient, const int32_t* b_side,
+                             const int32_t* b_dir) {
+    try {
+        auto h = std::make_unique<oracle_handle>();
+        h->basis = make_basis(N);
+        h->eq.gamma = gamma;
+        h->opt.N = N;
+        h->opt.flux_kind = flux_kind;
+        h->opt.speed_kind = speed_kind;
+        h->mesh.n_elements = E;
+        h->mesh.inverse_jacobian.assign(inv_jac, inv_jac + E);
+        h->mesh.n_interfaces = I;
+        h->mesh.interface_left.assign(left, left + I);
+        h->mesh.interface_right.assign(right, right + I);
+        h->mesh.interface_orientation.assign(orient, orient + I);
+        h->mesh.n_boundaries = B;
+        if (B > 0) {
+            h->mesh.boundary_element.assign(b_elem, b_elem + B);
+            h->mesh.boundary_orientation.assign(b_orient, b_orient + B);
+            h->mesh.boundary_side.assign(b_side, b_side + B);
+            h->mesh.boundary_direction.assign(b_dir, b_dir + B);
+        }
+        return h.release();
+    } catch (...) { return nullptr; }
+}
+
+void oracle_destroy(oracle_handle* h) { delete h; }
+
+void oracle_set_temporal_errors(oracle_handle* h, int on, double abstol, double reltol) {
+    h->opt.temporal_errors = on != 0;
+    h->opt.abstol = abstol;
+    h->opt.reltol = reltol;
+}
+
+// Exterior boundary states: levels [v, k, l, B] at t + 0.5 dt_scaled (x_k + 1), now [v, l, B] at t.
+int oracle_set_boundary_data(oracle_handle* h, const double* levels, const double* now) {
+    const size_t n = h->basis.n, B = h->mesh.n_boundaries;
+    h->bnd_levels.assign(levels, levels + NV * n * n * B);
+    h->bnd_now.assign(now, now + NV * n * B);
+    return 0;
+}
+
+// kind: 0 LW rhs!, 1 rhs_mdrk1!, 2 rhs_mdrk2! (u2 = u* for stage 2). Returns 0, or 3 when a square root of
+// a negative number occurred (the reference raises DomainError there).
+int oracle_rhs(oracle_handle* h, int kind, const double* u, const double* u2, double* du, double t, double dt,
+               int nthreads) {
+    try {
+        BoundaryData bd{h->bnd_levels.empty() ? nullptr : h->bnd_levels.data(),
+                        h->bnd_now.empty() ? nullptr : h->bnd_now.data()};
+        rhs(h->basis, h->eq, h->opt, h->mesh, u, u2, du, t, dt, &bd, kind, h->ws, nthreads);
+        return h->ws.bad ? 3 : 0;
+    } catch (const std::exception& ex) {
+        std::snprintf(h->err, sizeof(h->err), "%s", ex.what());
+        return 1;
+    }
+}
+
+// which: 0 U [v,i,j,e], 1 F [v,d,i,j,e], 2 U2, 3 F2, 4 temporal_errors [e], 5 surface_flux_values [v,l,face,e]
+int oracle_get(oracle_handle* h, int which, double* out) {
+    const std::vector<double>* src = nullptr;
+    switch (which) {
+        case 0: src = &h->ws.U; break;
+        case 1: src = &h->ws.F; break;
+        case 2: src = &h->ws.U2; break;
+        case 3: src = &h->ws.F2; break;
+        case 4: src = &h->ws.temporal_errors; break;
+        case 5: src = &h->ws.surface_flux_values; break;
+        default: return 1;
+    }
+    std::copy(src->begin(), src->end(), out);
+    return 0;
+}
+
+double oracle_max_dt(oracle_handle* h, const double* u, double cfl) {
+    bool bad = false;
+    const double dt = max_dt(h->basis, h->eq, h->mesh, u, cfl, bad);
+    return bad ? -1.0 : dt;
+}
+
+// The CFL-based step loop of solve_lwfr / perform_step! (src/solvers/lwfr.jl:212-230, 76-103;
+// src/solvers/mdrk.jl:1-29): dt = cfl * max_dt(u), clamped to t_end, u <- u + dt * du.
+// kind 0 = LW, 1 = MDRK. Runs at most nsteps steps or until t reaches t_end; returns steps taken, or
+// a negative number on error. t_inout is advanced.
+int oracle_steps(oracle_handle* h, int kind, double* u, int nsteps, double cfl, double fixed_dt, double* t_inout,
+                 double t_end, int nthreads) {
+    const size_t ndof = (size_t)NV * h->basis.n * h->basis.n * h->mesh.n_elements;
+    h->du.resize(ndof);
+    h->us.resize(ndof);
+    double t = *t_inout;
+    int s = 0;
+    for (; s < nsteps; ++s) {
+        if (t >= t_end || std::fabs(t - t_end) <= 1e-14 * std::max(1.0, std::fabs(t_end))) break;
+        bool bad = false;
+        double dt = fixed_dt > 0 ? fixed_dt : max_dt(h->basis, h->eq, h->mesh, u, cfl, bad, nthreads);
+        if (bad) return -3;
+        if (t + dt > t_end) dt = t_end - t;
+        BoundaryData bd{h->bnd_levels.empty() ? nullptr : h->bnd_levels.data(),
+                        h->bnd_now.empty() ? nullptr : h->bnd_now.data()};
+        if (kind == 0) {
+            rhs(h->basis, h->eq, h->opt, h->mesh, u, nullptr, h->du.data(), t, dt, &bd, 0, h->ws, nthreads);
+            if (h->ws.bad) return -3;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+            for (long long k = 0; k < (long long)ndof; ++k) u[k] = u[k] + dt * h->du[k];
+        } else {
+            rhs(h->basis, h->eq, h->opt, h->mesh, u, nullptr, h->du.data(), t, dt, &bd, 1, h->ws, nthreads);
+            if (h->ws.bad) return -3;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+            for (long long k = 0; k < (long long)ndof; ++k) h->us[k] = u[k] + dt * h->du[k];
+            rhs(h->basis, h->eq, h->opt, h->mesh, u, h->us.data(), h->du.data(), t, dt, &bd, 2, h->ws, nthreads);
+            if (h->ws.bad) return -3;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+            for (long long k = 0; k < (long long)ndof; ++k) u[k] = u[k] + dt * h->du[k];
+        }
+        t += dt;
+    }
+    *t_inout = t;
+    return s;
+}
+
+const char* oracle_last_error(oracle_handle* h) { return h->err; }
+
+}  // extern "C"

@@ -1,0 +1,144 @@
+"""ctypes wrapper of the CPU oracle (liboracle_tlw.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by the CPU-baseline leg
+of bench.py, as the checker. Parity status of the oracle: unpinned against the reference itself (no
+Julia on this machine); pinned by scheme invariants, see tlw_oracle.hpp.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(_HERE, "liboracle_tlw.so")
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
+            os.path.getmtime(os.path.join(_HERE, f)) for f in ("tlw_oracle.hpp", "oracle_capi.cpp")):
+        subprocess.run(["make", "-C", _HERE, "-B" if force else "liboracle_tlw.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return LIB
+
+
+_L = None
+
+
+def lib():
+    global _L
+    if _L is None:
+        build()
+        L = ctypes.CDLL(LIB)
+        P = ctypes.c_void_p
+        i32, dbl = ctypes.c_int, ctypes.c_double
+        L.oracle_basis.argtypes = [i32, P, P, P, P]
+        L.oracle_create.argtypes = [i32, dbl, i32, i32, i32, P, i32, P, P, P, i32, P, P, P, P]
+        L.oracle_create.restype = P
+        L.oracle_destroy.argtypes = [P]
+        L.oracle_set_temporal_errors.argtypes = [P, i32, dbl, dbl]
+        L.oracle_set_boundary_data.argtypes = [P, P, P]
+        L.oracle_rhs.argtypes = [P, i32, P, P, P, dbl, dbl, i32]
+        L.oracle_get.argtypes = [P, i32, P]
+        L.oracle_max_dt.argtypes = [P, P, dbl]
+        L.oracle_max_dt.restype = dbl
+        L.oracle_steps.argtypes = [P, i32, P, i32, dbl, dbl, P, dbl, i32]
+        L.oracle_last_error.argtypes = [P]
+        L.oracle_last_error.restype = ctypes.c_char_p
+        _L = L
+    return _L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def basis(N: int):
+    n = N + 1
+    nodes, w, D, Dh = np.empty(n), np.empty(n), np.empty(n * n), np.empty(n * n)
+    assert lib().oracle_basis(N, _p(nodes), _p(w), _p(D), _p(Dh)) == 0
+    return nodes, w, D.reshape(n, n), Dh.reshape(n, n)
+
+
+class OracleDomainError(ArithmeticError):
+    pass
+
+
+class Oracle:
+    """One oracle instance for a TreeMesh (the mesh object of trixilw.mesh or any object with the same
+    Trixi-convention arrays)."""
+
+    def __init__(self, mesh, polydeg: int, gamma: float = 1.4, flux_kind: int = 0, speed_kind: int = 0):
+        self.N = polydeg
+        self.n = polydeg + 1
+        self.mesh = mesh
+        self.E = mesh.n_elements
+        ij = np.ascontiguousarray(mesh.inverse_jacobian, dtype=np.float64)
+        ids = np.asarray(mesh.interface_neighbor_ids, dtype=np.int64).reshape(-1, 2)
+        left = np.ascontiguousarray(ids[:, 0] - 1, dtype=np.int32)
+        right = np.ascontiguousarray(ids[:, 1] - 1, dtype=np.int32)
+        orient = np.ascontiguousarray(mesh.interface_orientations, dtype=np.int32)
+        B = mesh.n_boundaries
+        be = np.ascontiguousarray(np.asarray(mesh.boundary_neighbor_ids) - 1, dtype=np.int32)
+        bo = np.ascontiguousarray(mesh.boundary_orientations, dtype=np.int32)
+        bs = np.ascontiguousarray(mesh.boundary_neighbor_sides, dtype=np.int32)
+        bd = np.ascontiguousarray(np.repeat(np.arange(1, 5), np.asarray(mesh.n_boundaries_per_direction)), dtype=np.int32)
+        self._keep = (ij, left, right, orient, be, bo, bs, bd)
+        self.h = lib().oracle_create(polydeg, gamma, flux_kind, speed_kind, self.E, _p(ij), len(orient), _p(left),
+                                     _p(right), _p(orient), B, _p(be) if B else None, _p(bo) if B else None,
+                                     _p(bs) if B else None, _p(bd) if B else None)
+        if not self.h:
+            raise RuntimeError("oracle_create failed")
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().oracle_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def size(self):
+        return 4 * self.n * self.n * self.E
+
+    def set_boundary_data(self, levels: np.ndarray, now: np.ndarray):
+        self._bkeep = (np.ascontiguousarray(levels, dtype=np.float64), np.ascontiguousarray(now, dtype=np.float64))
+        lib().oracle_set_boundary_data(self.h, _p(self._bkeep[0]), _p(self._bkeep[1]))
+
+    def rhs(self, u, t, dt, kind: int = 0, us=None, nthreads: int = 1):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        us = None if us is None else np.ascontiguousarray(us, dtype=np.float64)
+        du = np.empty_like(u)
+        rc = lib().oracle_rhs(self.h, kind, _p(u), _p(us), _p(du), float(t), float(dt), nthreads)
+        if rc == 3:
+            raise OracleDomainError("sqrt of a negative number")
+        if rc != 0:
+            raise RuntimeError(lib().oracle_last_error(self.h).decode())
+        return du
+
+    def get(self, which: int) -> np.ndarray:
+        sizes = {0: self.size(), 1: 2 * self.size(), 2: self.size(), 3: 2 * self.size(), 4: self.E,
+                 5: 4 * self.n * 4 * self.E}
+        out = np.empty(sizes[which])
+        assert lib().oracle_get(self.h, which, _p(out)) == 0
+        return out
+
+    def max_dt(self, u, cfl):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        dt = lib().oracle_max_dt(self.h, _p(u), float(cfl))
+        if dt < 0:
+            raise OracleDomainError("sqrt of a negative number in max_dt")
+        return dt
+
+    def steps(self, u, nsteps: int, cfl: float, t: float, t_end: float, kind: int = 0, fixed_dt: float = 0.0,
+              nthreads: int = 1):
+        """In-place CFL steps; returns (steps_taken, t)."""
+        assert u.dtype == np.float64 and u.flags.c_contiguous
+        tt = ctypes.c_double(t)
+        s = lib().oracle_steps(self.h, kind, _p(u), int(nsteps), float(cfl), float(fixed_dt), ctypes.byref(tt),
+                               float(t_end), nthreads)
+        if s < 0:
+            raise OracleDomainError("oracle step failed")
+        return s, tt.value

@@ -1,0 +1,848 @@
+// tlw_oracle.hpp -- CPU restatement of TrixiLW's Lax-Wendroff / MDRK right-hand side on TreeMesh{2}
+// for the 2D compressible Euler equations.
+//
+// TEST INFRASTRUCTURE ONLY. This header is the oracle against which the CUDA library is checked. Only
+// the test-suite, the smoke check and the CPU-baseline leg of the benchmark may call it; the product
+// path never does.
+//
+// Parity status: UNPINNED against the reference itself. The reference is Julia + Trixi.jl, neither of
+// which exists on this machine, and it ships no tests, golden vectors or rhs fixtures. The restatement is
+// therefore pinned by properties the reference's scheme has by construction (exact free-stream
+// preservation, discrete conservation on periodic meshes, design order of accuracy on the isentropic
+// vortex, symmetry under mirroring) and by hand-checked known answers (GLL nodes/weights, the
+// derivative matrix). Every function cites the reference file:line it restates (paths relative to the
+// TrixiLW.jl repository root). Trixi.jl pieces that are not in the reference (basis, Euler flux,
+// max_abs_speed, surface integral, apply_jacobian, max_dt) are restated from their mathematics.
+//
+// Array layout is the reference's (Julia column-major, leftmost index fastest):
+//   u, du       [v, i, j, e]        -> u[v + NV*(i + n*(j + n*e))]
+//   F (element) [v, d, i, j, e]     -> d = 0 x-flux, d = 1 y-flux
+//   interfaces  [side, v, i, I]     -> side 0 = left, 1 = right
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+#include <vector>
+
+namespace tlwo {
+
+constexpr int NV = 4;
+constexpr int MAXN = 8;   // oracle supports polydeg <= 7
+
+// fixed-size per-element scratch tile [v, i, j]
+struct Tile {
+    double a[NV * MAXN * MAXN];
+    double& operator[](int k) { return a[k]; }
+    const double& operator[](int k) const { return a[k]; }
+    void zero(int m) { for (int k = 0; k < m; ++k) a[k] = 0.0; }
+};
+
+// ------------------------------------------------------------------------------------------------
+// Lobatto-Legendre basis (Trixi.jl LobattoLegendreBasis; restated from Kopriva, "Implementing
+// Spectral Methods for PDEs", Alg. 22/24/25 (Legendre recursion, GLL nodes/weights), Alg. 30
+// (barycentric weights), Alg. 37 (derivative matrix with the negative-sum diagonal)).
+// ------------------------------------------------------------------------------------------------
+struct Basis {
+    int n = 0;                      // nodes per direction, N + 1
+    std::vector<double> nodes, weights, wbary;
+    std::vector<double> D;          // D[a*n + b]    = l_b'(x_a)          (Trixi derivative_matrix[a, b])
+    std::vector<double> Dhat;       // Dhat[a*n + b] = -D[b, a] w_b / w_a (Trixi derivative_dhat[a, b])
+    double inv_w_first = 0, inv_w_last = 0;   // Trixi boundary_interpolation[1,1], [n,2]
+};
+
+inline void legendre_q_and_l(int N, double x, double& q, double& dq, double& LN) {
+    // Kopriva Alg. 24 (qAndLEvaluation)
+    double L_m2 = 1.0, L_m1 = x, dL_m2 = 0.0, dL_m1 = 1.0, L = 0, dL = 0;
+    for (int k = 2; k <= N; ++k) {
+        L = (2.0 * k - 1.0) / k * x * L_m1 - (k - 1.0) / k * L_m2;
+        dL = dL_m2 + (2.0 * k - 1.0) * L_m1;
+        L_m2 = L_m1; L_m1 = L; dL_m2 = dL_m1; dL_m1 = dL;
+    }
+    const int k = N + 1;
+    const double L_p1 = (2.0 * k - 1.0) / k * x * L_m1 - (k - 1.0) / k * L_m2;
+    const double dL_p1 = dL_m2 + (2.0 * k - 1.0) * L_m1;
+    q = L_p1 - L_m2;
+    dq = dL_p1 - dL_m2;
+    LN = L_m1;
+}
+
+inline Basis make_basis(int N) {
+    if (N < 1 || N + 1 > MAXN) throw std::invalid_argument("polydeg out of range");
+    Basis b;
+    b.n = N + 1;
+    const int n = b.n;
+    b.nodes.assign(n, 0.0);
+    b.weights.assign(n, 0.0);
+    // Kopriva Alg. 25 (LegendreGaussLobattoNodesAndWeights)
+    if (N == 1) {
+        b.nodes = {-1.0, 1.0};
+        b.weights = {1.0, 1.0};
+    } else {
+        b.nodes[0] = -1.0; b.nodes[N] = 1.0;
+        b.weights[0] = b.weights[N] = 2.0 / (N * (N + 1.0));
+        const double pi = 3.14159265358979323846;
+        for (int j = 1; j <= (N + 1) / 2 - 1; ++j) {
+            double x = -std::cos((j + 0.25) * pi / N - 3.0 / (8.0 * N * pi * (j + 0.25)));
+            double q, dq, LN;
+            for (int it = 0; it < 100; ++it) {
+                legendre_q_and_l(N, x, q, dq, LN);
+                const double delta = -q / dq;
+                x += delta;
+                if (std::fabs(delta) <= 4.0 * std::numeric_limits<double>::epsilon() * std::fabs(x)) break;
+            }
+            legendre_q_and_l(N, x, q, dq, LN);
+            b.nodes[j] = x;
+            b.nodes[N - j] = -x;
+            b.weights[j] = b.weights[N - j] = 2.0 / (N * (N + 1.0) * LN * LN);
+        }
+        if (N % 2 == 0) {
+            double q, dq, LN;
+            legendre_q_and_l(N, 0.0, q, dq, LN);
+            b.nodes[N / 2] = 0.0;
+            b.weights[N / 2] = 2.0 / (N * (N + 1.0) * LN * LN);
+        }
+    }
+    // Kopriva Alg. 30 (BarycentricWeights)
+    b.wbary.assign(n, 1.0);
+    for (int j = 0; j < n; ++j)
+        for (int k = 0; k < n; ++k)
+            if (k != j) b.wbary[j] *= (b.nodes[j] - b.nodes[k]);
+    for (int j = 0; j < n; ++j) b.wbary[j] = 1.0 / b.wbary[j];
+    // Kopriva Alg. 37 (PolynomialDerivativeMatrix), the form Trixi's polynomial_derivative_matrix uses
+    b.D.assign(n * n, 0.0);
+    for (int a = 0; a < n; ++a)
+        for (int c = 0; c < n; ++c)
+            if (c != a) {
+                b.D[a * n + c] = b.wbary[c] / b.wbary[a] / (b.nodes[a] - b.nodes[c]);
+                b.D[a * n + a] -= b.D[a * n + c];
+            }
+    // Trixi calc_dhat: dhat = D^T, then dhat[j, m] *= -w[m] / w[j]
+    b.Dhat.assign(n * n, 0.0);
+    for (int a = 0; a < n; ++a)
+        for (int c = 0; c < n; ++c) b.Dhat[a * n + c] = -b.D[c * n + a] * b.weights[c] / b.weights[a];
+    b.inv_w_first = 1.0 / b.weights[0];
+    b.inv_w_last = 1.0 / b.weights[n - 1];
+    return b;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Compressible Euler 2D pointwise functions (Trixi.jl CompressibleEulerEquations2D, restated).
+// ------------------------------------------------------------------------------------------------
+struct Euler {
+    double gamma = 1.4;
+
+    // Trixi flux(u, orientation, eq); the pair is TrixiLW `fluxes` (src/solvers/dgsem_tree/dg_2d.jl:368)
+    inline void fluxes(const double* u, double* f, double* g) const {
+        const double rho = u[0], m1 = u[1], m2 = u[2], e = u[3];
+        const double v1 = m1 / rho, v2 = m2 / rho;
+        const double p = (gamma - 1.0) * (e - 0.5 * (m1 * v1 + m2 * v2));
+        f[0] = m1; f[1] = m1 * v1 + p; f[2] = m1 * v2; f[3] = (e + p) * v1;
+        g[0] = m2; g[1] = m2 * v1; g[2] = m2 * v2 + p; g[3] = (e + p) * v2;
+    }
+    inline void flux(const double* u, int orientation, double* f) const {
+        double fx[NV], gy[NV];
+        fluxes(u, fx, gy);
+        for (int v = 0; v < NV; ++v) f[v] = orientation == 1 ? fx[v] : gy[v];
+    }
+    // Trixi cons2prim
+    inline void cons2prim(const double* u, double& rho, double& v1, double& v2, double& p) const {
+        rho = u[0]; v1 = u[1] / rho; v2 = u[2] / rho;
+        p = (gamma - 1.0) * (u[3] - 0.5 * (u[1] * v1 + u[2] * v2));
+    }
+    // Julia's sqrt throws DomainError for a negative argument; the oracle reports it through `bad`.
+    inline double checked_sqrt(double x, bool& bad) const {
+        if (!(x >= 0.0)) { bad = true; return std::numeric_limits<double>::quiet_NaN(); }
+        return std::sqrt(x);
+    }
+    // Trixi max_abs_speed_naive (speed_kind 0) and max_abs_speed (speed_kind 1), orientation 1|2
+    inline double max_abs_speed(const double* ul, const double* ur, int orientation, int speed_kind,
+                                bool& bad) const {
+        double rl, v1l, v2l, pl, rr, v1r, v2r, pr;
+        cons2prim(ul, rl, v1l, v2l, pl);
+        cons2prim(ur, rr, v1r, v2r, pr);
+        const double vl = orientation == 1 ? v1l : v2l;
+        const double vr = orientation == 1 ? v1r : v2r;
+        const double cl = checked_sqrt(gamma * pl / rl, bad);
+        const double cr = checked_sqrt(gamma * pr / rr, bad);
+        if (speed_kind == 0) return std::max(std::fabs(vl), std::fabs(vr)) + std::max(cl, cr);
+        return std::max(std::fabs(vl) + cl, std::fabs(vr) + cr);
+    }
+    // Trixi min_max_speed_naive (the FluxHLL default)
+    inline void min_max_speed(const double* ul, const double* ur, int orientation, double& lmin, double& lmax,
+                              bool& bad) const {
+        double rl, v1l, v2l, pl, rr, v1r, v2r, pr;
+        cons2prim(ul, rl, v1l, v2l, pl);
+        cons2prim(ur, rr, v1r, v2r, pr);
+        const double vl = orientation == 1 ? v1l : v2l;
+        const double vr = orientation == 1 ? v1r : v2r;
+        const double cl = checked_sqrt(gamma * pl / rl, bad);
+        const double cr = checked_sqrt(gamma * pr / rr, bad);
+        lmin = vl - cl;
+        lmax = vr + cr;
+    }
+    // Trixi max_abs_speeds (used by max_dt)
+    inline void max_abs_speeds(const double* u, double& l1, double& l2, bool& bad) const {
+        double rho, v1, v2, p;
+        cons2prim(u, rho, v1, v2, p);
+        const double c = checked_sqrt(gamma * p / rho, bad);
+        l1 = std::fabs(v1) + c;
+        l2 = std::fabs(v2) + c;
+    }
+    // src/equations/compressible_euler_2d.jl:4-7
+    inline bool is_admissible(const double* u) const {
+        double rho, v1, v2, p;
+        cons2prim(u, rho, v1, v2, p);
+        return rho > 0.0 && p > 0.0;
+    }
+};
+
+// 8-argument LW surface flux as called on TreeMesh: surface_flux(f_ll, f_rr, U_ll, U_rr, u_ll, u_rr, ...)
+// (src/solvers/dgsem_tree/dg_2d.jl:1928). For FluxPlusDissipation (src/equations/numerical_fluxes.jl:14-22)
+// the third/fourth arguments feed the speed estimate and the fifth/sixth the jump
+// (DissipationLocalLaxFriedrichs, numerical_fluxes.jl:34-38), so on TreeMesh lambda comes from the
+// time-averaged U and the jump is in the instantaneous u. flux_central is numerical_fluxes.jl:7-12.
+// For FluxHLL (src/equations/compressible_euler_2d.jl:24-40) the argument names are (f, f, U, U, u, u):
+// the speeds come from the fifth/sixth arguments and the jump from the third/fourth.
+enum SurfaceFlux { RUSANOV = 0, HLL = 1 };
+
+inline void lw_surface_flux(const Euler& eq, int flux_kind, int speed_kind, const double* f_ll, const double* f_rr,
+                            const double* a3, const double* a4, const double* a5, const double* a6,
+                            int orientation, double* out, bool& bad) {
+    if (flux_kind == RUSANOV) {
+        // FluxPlusDissipation(f_ll, f_rr, u_ll=a3, u_rr=a4, U_ll=a5, U_rr=a6)
+        const double lambda = eq.max_abs_speed(a3, a4, orientation, speed_kind, bad);
+        for (int v = 0; v < NV; ++v) out[v] = 0.5 * (f_ll[v] + f_rr[v]) + (-0.5 * lambda * (a6[v] - a5[v]));
+    } else {
+        // FluxHLL(f_ll, f_rr, U_ll=a3, U_rr=a4, u_ll=a5, u_rr=a6)
+        double lmin, lmax;
+        eq.min_max_speed(a5, a6, orientation, lmin, lmax, bad);
+        if (lmin >= 0 && lmax >= 0) {
+            for (int v = 0; v < NV; ++v) out[v] = f_ll[v];
+        } else if (lmax <= 0 && lmin <= 0) {
+            for (int v = 0; v < NV; ++v) out[v] = f_rr[v];
+        } else {
+            const double inv = 1.0 / (lmax - lmin);
+            const double fll = lmax * inv, frr = lmin * inv, fd = lmin * lmax * inv;
+            for (int v = 0; v < NV; ++v) out[v] = fll * f_ll[v] - frr * f_rr[v] + fd * (a4[v] - a3[v]);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// TreeMesh connectivity and LW caches (src/solvers/dgsem_tree/containers.jl:73-121, 216-237).
+// ------------------------------------------------------------------------------------------------
+struct TreeMesh {
+    int n_elements = 0;
+    std::vector<double> inverse_jacobian;      // [E]
+    int n_interfaces = 0;
+    std::vector<int32_t> interface_left, interface_right, interface_orientation;   // 0-based ids, 1|2
+    // boundaries (src/solvers/dgsem_tree/dg_2d.jl:1328-1454); neighbor_side 1: element on the -side
+    int n_boundaries = 0;
+    std::vector<int32_t> boundary_element, boundary_orientation, boundary_side, boundary_direction;
+};
+
+struct Options {
+    int N = 4;
+    int flux_kind = RUSANOV;
+    int speed_kind = 0;            // 0 = max_abs_speed_naive
+    bool temporal_errors = false;  // lw_volume_kernel_4! u_np1/u_np1_low tail (dg_2d.jl:1251-1265)
+    double abstol = 0.0, reltol = 0.0;
+};
+
+struct Workspace {
+    // element cache
+    std::vector<double> U, F;            // [v,i,j,e], [v,d,i,j,e]
+    std::vector<double> U2, F2, us;      // MDRK cache (containers.jl:83-98)
+    std::vector<double> temporal_errors; // [E]
+    // interface cache [side, v, i, I]
+    std::vector<double> iu, iU, iF;
+    std::vector<double> surface_flux_values;  // [v, i, face, e], face 0..3 = -x, +x, -y, +y
+    // boundary cache [side, v, i, B] and exterior time-averaged states supplied per call
+    std::vector<double> bu, bU, bF;
+    bool bad = false;                    // a sqrt of a negative number happened (Julia DomainError)
+};
+
+inline size_t idx_u(int n, int v, int i, int j, int e) { return v + NV * (i + (size_t)n * (j + (size_t)n * e)); }
+inline size_t idx_F(int n, int v, int d, int i, int j, int e) {
+    return v + NV * (d + 2 * (i + (size_t)n * (j + (size_t)n * e)));
+}
+
+// ------------------------------------------------------------------------------------------------
+// LW volume kernel for one element: lw_volume_kernel_{1,2,3,4}! (TreeMesh, no source terms).
+//   depth 4: src/solvers/dgsem_tree/dg_2d.jl:918-1267 (every polydeg >= 4, dispatch :179-218)
+//   depth 3: dg_2d.jl:674-916
+//   depth 2: dg_2d.jl:495-672 (as written; the shipped dispatcher cannot call it, see the header)
+//   depth 1: dg_2d.jl:370-493
+// Every time derivative is carried pre-multiplied by dt^k, so the stencils are evaluated at unit step.
+// du receives alpha * (Dhat F + Dhat G) (before surface integral and Jacobian); U/F are stored in ws.
+// ------------------------------------------------------------------------------------------------
+inline void lw_volume_element(const Basis& b, const Euler& eq, const Options& opt, int e, const double* u,
+                              double* du, double dt, double inv_jac, double alpha, Workspace& ws) {
+    const int n = b.n;
+    const int nn = n * n;
+    const int depth = std::min(opt.N, 4);
+    Tile f, g, Fc, Gc, Uc, up, um, upp, umm, ut, utt, uttt, utttt, unp1, unp1_low;
+    ut.zero(NV * nn); utt.zero(NV * nn); uttt.zero(NV * nn); utttt.zero(NV * nn);
+    auto L = [&](int i, int j) { return NV * (i + n * j); };
+    const double* ue = u + idx_u(n, 0, 0, 0, e);
+
+    // contraction target += -dt * D (x: along i, y: along j), scatter form as in the reference loops
+    auto contract = [&](const Tile& fx, const Tile& gy, Tile& tgt) {
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                for (int ii = 0; ii < n; ++ii) {
+                    const double c = -dt * b.D[ii * n + i];
+                    for (int v = 0; v < NV; ++v) tgt[L(ii, j) + v] += c * fx[L(i, j) + v];
+                }
+                for (int jj = 0; jj < n; ++jj) {
+                    const double c = -dt * b.D[jj * n + j];
+                    for (int v = 0; v < NV; ++v) tgt[L(i, jj) + v] += c * gy[L(i, j) + v];
+                }
+            }
+        for (int k = 0; k < NV * nn; ++k) tgt[k] *= inv_jac;
+    };
+    auto fl = [&](const Tile& s, int i, int j, double* fo, double* go) { eq.fluxes(&s[L(i, j)], fo, go); };
+
+    // stage 0: f, g at u; ut (dg_2d.jl:941-978)
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const double* un = ue + L(i, j);
+            eq.fluxes(un, &f[L(i, j)], &g[L(i, j)]);
+            for (int v = 0; v < NV; ++v) {
+                Fc[L(i, j) + v] = f[L(i, j) + v];
+                Gc[L(i, j) + v] = g[L(i, j) + v];
+                up[L(i, j) + v] = um[L(i, j) + v] = upp[L(i, j) + v] = umm[L(i, j) + v] = un[v];
+                Uc[L(i, j) + v] = un[v];
+                unp1[L(i, j) + v] = unp1_low[L(i, j) + v] = un[v];
+            }
+        }
+    if (depth == 2) {
+        // kernel_2 scales after a plain D contraction (dg_2d.jl:526-549); same value as -dt*D then J
+        Tile tmp;
+        tmp.zero(NV * nn);
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                for (int ii = 0; ii < n; ++ii)
+                    for (int v = 0; v < NV; ++v) tmp[L(ii, j) + v] += b.D[ii * n + i] * f[L(i, j) + v];
+                for (int jj = 0; jj < n; ++jj)
+                    for (int v = 0; v < NV; ++v) tmp[L(i, jj) + v] += b.D[jj * n + j] * g[L(i, j) + v];
+            }
+        for (int k = 0; k < NV * nn; ++k) ut[k] = tmp[k] * (-dt * inv_jac);
+    } else {
+        contract(f, g, ut);
+    }
+
+    double fp[NV], gp[NV], fm[NV], gm[NV], fpp[NV], gpp[NV], fmm[NV], gmm[NV];
+    Tile ft, gt;
+
+    // stage 1 (dg_2d.jl:990-1023 for depth 3/4; :435-456 / :561-595 for depth 1/2)
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const int o = L(i, j);
+            for (int v = 0; v < NV; ++v) {
+                const double d = ut[o + v];
+                Uc[o + v] += 0.5 * d;
+                up[o + v] += d;
+                um[o + v] += -d;
+                if (depth >= 3) { umm[o + v] += -2.0 * d; upp[o + v] += 2.0 * d; }
+            }
+            fl(um, i, j, fm, gm);
+            fl(up, i, j, fp, gp);
+            if (depth >= 3) {
+                fl(umm, i, j, fmm, gmm);
+                fl(upp, i, j, fpp, gpp);
+                for (int v = 0; v < NV; ++v) {
+                    ft[o + v] = 1.0 / 12.0 * (-fpp[v] + 8.0 * fp[v] - 8.0 * fm[v] + fmm[v]);
+                    gt[o + v] = 1.0 / 12.0 * (-gpp[v] + 8.0 * gp[v] - 8.0 * gm[v] + gmm[v]);
+                }
+            } else {
+                for (int v = 0; v < NV; ++v) {
+                    ft[o + v] = 0.5 * fp[v] - 0.5 * fm[v];
+                    gt[o + v] = 0.5 * gp[v] - 0.5 * gm[v];
+                }
+            }
+            for (int v = 0; v < NV; ++v) { Fc[o + v] += 0.5 * ft[o + v]; Gc[o + v] += 0.5 * gt[o + v]; }
+        }
+    if (depth >= 2) {
+        contract(ft, gt, utt);
+        // stage 2 (dg_2d.jl:1049-1083 depth 4; :801-831 depth 3; :617-634 depth 2)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const int o = L(i, j);
+                for (int v = 0; v < NV; ++v) {
+                    const double d = utt[o + v];
+                    Uc[o + v] += 1.0 / 6.0 * d;
+                    up[o + v] += 0.5 * d;
+                    um[o + v] += 0.5 * d;
+                    if (depth >= 3) { upp[o + v] += 2.0 * d; umm[o + v] += 2.0 * d; }
+                }
+                if (depth == 4) {
+                    fl(um, i, j, fm, gm);
+                    fl(up, i, j, fp, gp);
+                    fl(umm, i, j, fmm, gmm);
+                    fl(upp, i, j, fpp, gpp);
+                    for (int v = 0; v < NV; ++v) {
+                        ft[o + v] = (1.0 / 12.0) * (-fpp[v] + 16.0 * fp[v] - 30.0 * f[o + v] + 16.0 * fm[v] - fmm[v]);
+                        gt[o + v] = (1.0 / 12.0) * (-gpp[v] + 16.0 * gp[v] - 30.0 * g[o + v] + 16.0 * gm[v] - gmm[v]);
+                    }
+                } else {
+                    fl(um, i, j, fm, gm);
+                    fl(up, i, j, fp, gp);
+                    for (int v = 0; v < NV; ++v) {
+                        ft[o + v] = fp[v] - 2.0 * f[o + v] + fm[v];
+                        gt[o + v] = gp[v] - 2.0 * g[o + v] + gm[v];
+                    }
+                }
+                for (int v = 0; v < NV; ++v) {
+                    Fc[o + v] += 1.0 / 6.0 * ft[o + v];
+                    Gc[o + v] += 1.0 / 6.0 * gt[o + v];
+                }
+            }
+    }
+    if (depth >= 3) {
+        contract(ft, gt, uttt);
+        // stage 3 (dg_2d.jl:1106-1138 depth 4; :854-875 depth 3)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const int o = L(i, j);
+                for (int v = 0; v < NV; ++v) {
+                    const double d = uttt[o + v];
+                    Uc[o + v] += 1.0 / 24.0 * d;
+                    um[o + v] += -1.0 / 6.0 * d;
+                    up[o + v] += 1.0 / 6.0 * d;
+                    umm[o + v] += -4.0 / 3.0 * d;
+                    upp[o + v] += 4.0 / 3.0 * d;
+                }
+                fl(um, i, j, fm, gm);
+                fl(up, i, j, fp, gp);
+                fl(umm, i, j, fmm, gmm);
+                fl(upp, i, j, fpp, gpp);
+                for (int v = 0; v < NV; ++v) {
+                    ft[o + v] = 0.5 * (fpp[v] - 2.0 * fp[v] + 2.0 * fm[v] - fmm[v]);
+                    gt[o + v] = 0.5 * (gpp[v] - 2.0 * gp[v] + 2.0 * gm[v] - gmm[v]);
+                    Fc[o + v] += 1.0 / 24.0 * ft[o + v];
+                    Gc[o + v] += 1.0 / 24.0 * gt[o + v];
+                }
+            }
+    }
+    if (depth >= 4) {
+        contract(ft, gt, utttt);
+        // stage 4 (dg_2d.jl:1164-1226)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const int o = L(i, j);
+                for (int v = 0; v < NV; ++v) {
+                    const double d = utttt[o + v];
+                    Uc[o + v] += 1.0 / 120.0 * d;
+                    um[o + v] += 1.0 / 24.0 * d;
+                    up[o + v] += 1.0 / 24.0 * d;
+                    umm[o + v] += 2.0 / 3.0 * d;
+                    upp[o + v] += 2.0 / 3.0 * d;
+                }
+                fl(um, i, j, fm, gm);
+                fl(up, i, j, fp, gp);
+                fl(umm, i, j, fmm, gmm);
+                fl(upp, i, j, fpp, gpp);
+                if (opt.temporal_errors) {
+                    // u_np1_low uses F, G before the fourth-derivative term (dg_2d.jl:1183-1199)
+                    for (int ii = 0; ii < n; ++ii) {
+                        const double c = -dt * inv_jac * b.D[ii * n + i];
+                        for (int v = 0; v < NV; ++v) unp1_low[L(ii, j) + v] += c * Fc[o + v];
+                    }
+                    for (int jj = 0; jj < n; ++jj) {
+                        const double c = -dt * inv_jac * b.D[jj * n + j];
+                        for (int v = 0; v < NV; ++v) unp1_low[L(i, jj) + v] += c * Gc[o + v];
+                    }
+                }
+                for (int v = 0; v < NV; ++v) {
+                    const double ftttt = 0.5 * (fpp[v] - 4.0 * fp[v] + 6.0 * f[o + v] - 4.0 * fm[v] + fmm[v]);
+                    const double gtttt = 0.5 * (gpp[v] - 4.0 * gp[v] + 6.0 * g[o + v] - 4.0 * gm[v] + gmm[v]);
+                    Fc[o + v] += 1.0 / 120.0 * ftttt;
+                    Gc[o + v] += 1.0 / 120.0 * gtttt;
+                }
+                if (opt.temporal_errors) {
+                    for (int ii = 0; ii < n; ++ii) {
+                        const double c = -dt * inv_jac * b.D[ii * n + i];
+                        for (int v = 0; v < NV; ++v) unp1[L(ii, j) + v] += c * Fc[o + v];
+                    }
+                    for (int jj = 0; jj < n; ++jj) {
+                        const double c = -dt * inv_jac * b.D[jj * n + j];
+                        for (int v = 0; v < NV; ++v) unp1[L(i, jj) + v] += c * Gc[o + v];
+                    }
+                }
+            }
+    }
+    // final: du += alpha * Dhat (F, G); store U and F (dg_2d.jl:1208-1248, :876-912)
+    double* due = du + idx_u(n, 0, 0, 0, e);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const int o = L(i, j);
+            for (int ii = 0; ii < n; ++ii) {
+                const double c = alpha * b.Dhat[ii * n + i];
+                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += c * Fc[o + v];
+            }
+            for (int jj = 0; jj < n; ++jj) {
+                const double c = alpha * b.Dhat[jj * n + j];
+                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += c * Gc[o + v];
+            }
+            for (int v = 0; v < NV; ++v) {
+                ws.F[idx_F(n, v, 0, i, j, e)] = Fc[o + v];
+                ws.F[idx_F(n, v, 1, i, j, e)] = Gc[o + v];
+                ws.U[idx_u(n, v, i, j, e)] = Uc[o + v];
+            }
+        }
+    if (opt.temporal_errors && depth >= 4) {
+        // dg_2d.jl:1251-1265
+        double te = 0.0;
+        for (int k = 0; k < NV * nn; ++k) {
+            const double r = (unp1[k] - unp1_low[k]) /
+                             (opt.abstol + opt.reltol * std::max(std::fabs(unp1[k]), std::fabs(unp1_low[k])));
+            te += r * r;
+        }
+        ws.temporal_errors[e] = te;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// MDRK stage kernels on TreeMesh (src/solvers/dgsem_tree/multi_derivative_2d.jl:263-421, 423-555),
+// no source terms. Stage 1 as shipped unpacks `u_low` from a cache that has no such field (:287); the
+// value is write-only on this path (it never reaches du, U, F, U2 or F2), so it is not computed here.
+// ------------------------------------------------------------------------------------------------
+inline void mdrk1_volume_element(const Basis& b, const Euler& eq, int e, const double* u, double* du, double dt,
+                                 double inv_jac, double alpha, Workspace& ws) {
+    const int n = b.n, nn = n * n;
+    Tile Fh, Gh, F2, G2, Uh, U2, ut, f, g;
+    ut.zero(NV * nn);
+    auto L = [&](int i, int j) { return NV * (i + n * j); };
+    const double* ue = u + idx_u(n, 0, 0, 0, e);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const int o = L(i, j);
+            eq.fluxes(ue + o, &f[o], &g[o]);
+            for (int v = 0; v < NV; ++v) {
+                Fh[o + v] = 0.5 * f[o + v];
+                F2[o + v] = f[o + v];
+                Gh[o + v] = 0.5 * g[o + v];
+                G2[o + v] = g[o + v];
+                Uh[o + v] = 0.5 * ue[o + v];
+                U2[o + v] = ue[o + v];
+            }
+            for (int ii = 0; ii < n; ++ii) {
+                const double c = -dt * b.D[ii * n + i];
+                for (int v = 0; v < NV; ++v) ut[L(ii, j) + v] += c * f[o + v];
+            }
+            for (int jj = 0; jj < n; ++jj) {
+                const double c = -dt * b.D[jj * n + j];
+                for (int v = 0; v < NV; ++v) ut[L(i, jj) + v] += c * g[o + v];
+            }
+        }
+    for (int k = 0; k < NV * nn; ++k) ut[k] *= inv_jac;
+    double* due = du + idx_u(n, 0, 0, 0, e);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const int o = L(i, j);
+            double um[NV], up[NV], umm[NV], upp[NV];
+            for (int v = 0; v < NV; ++v) {
+                um[v] = ue[o + v] - ut[o + v];
+                up[v] = ue[o + v] + ut[o + v];
+                umm[v] = ue[o + v] - 2 * ut[o + v];
+                upp[v] = ue[o + v] + 2 * ut[o + v];
+            }
+            double fm[NV], gm[NV], fp[NV], gp[NV], fmm[NV], gmm[NV], fpp[NV], gpp[NV];
+            eq.fluxes(um, fm, gm);
+            eq.fluxes(up, fp, gp);
+            eq.fluxes(umm, fmm, gmm);
+            eq.fluxes(upp, fpp, gpp);
+            double ft[NV], gt[NV];
+            for (int v = 0; v < NV; ++v) {
+                ft[v] = 1.0 / 12.0 * (-fpp[v] + 8.0 * fp[v] - 8.0 * fm[v] + fmm[v]);
+                gt[v] = 1.0 / 12.0 * (-gpp[v] + 8.0 * gp[v] - 8.0 * gm[v] + gmm[v]);
+                Fh[o + v] += 0.125 * ft[v];
+                Gh[o + v] += 0.125 * gt[v];
+                Uh[o + v] += 0.125 * ut[o + v];
+                F2[o + v] += 1.0 / 6.0 * ft[v];
+                G2[o + v] += 1.0 / 6.0 * gt[v];
+                U2[o + v] += 1.0 / 6.0 * ut[o + v];
+            }
+            for (int ii = 0; ii < n; ++ii) {
+                const double c = alpha * b.Dhat[ii * n + i];
+                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += c * Fh[o + v];
+            }
+            for (int jj = 0; jj < n; ++jj) {
+                const double c = alpha * b.Dhat[jj * n + j];
+                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += c * Gh[o + v];
+            }
+            for (int v = 0; v < NV; ++v) {
+                ws.U[idx_u(n, v, i, j, e)] = Uh[o + v];
+                ws.F[idx_F(n, v, 0, i, j, e)] = Fh[o + v];
+                ws.F[idx_F(n, v, 1, i, j, e)] = Gh[o + v];
+                ws.U2[idx_u(n, v, i, j, e)] = U2[o + v];
+                ws.F2[idx_F(n, v, 0, i, j, e)] = F2[o + v];
+                ws.F2[idx_F(n, v, 1, i, j, e)] = G2[o + v];
+            }
+        }
+}
+
+inline void mdrk2_volume_element(const Basis& b, const Euler& eq, int e, const double* us, double* du, double dt,
+                                 double inv_jac, double alpha, Workspace& ws) {
+    const int n = b.n, nn = n * n;
+    Tile Fc, Gc, Uc, ust;
+    ust.zero(NV * nn);
+    auto L = [&](int i, int j) { return NV * (i + n * j); };
+    const double* ue = us + idx_u(n, 0, 0, 0, e);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+            for (int v = 0; v < NV; ++v) {
+                Fc[L(i, j) + v] = ws.F2[idx_F(n, v, 0, i, j, e)];
+                Gc[L(i, j) + v] = ws.F2[idx_F(n, v, 1, i, j, e)];
+                Uc[L(i, j) + v] = ws.U2[idx_u(n, v, i, j, e)];
+            }
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            double f[NV], g[NV];
+            eq.fluxes(ue + L(i, j), f, g);
+            for (int ii = 0; ii < n; ++ii) {
+                const double c = -dt * b.D[ii * n + i];
+                for (int v = 0; v < NV; ++v) ust[L(ii, j) + v] += c * f[v];
+            }
+            for (int jj = 0; jj < n; ++jj) {
+                const double c = -dt * b.D[jj * n + j];
+                for (int v = 0; v < NV; ++v) ust[L(i, jj) + v] += c * g[v];
+            }
+        }
+    for (int k = 0; k < NV * nn; ++k) ust[k] *= inv_jac;
+    double* due = du + idx_u(n, 0, 0, 0, e);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const int o = L(i, j);
+            double um[NV], up[NV], umm[NV], upp[NV];
+            for (int v = 0; v < NV; ++v) {
+                um[v] = ue[o + v] - ust[o + v];
+                up[v] = ue[o + v] + ust[o + v];
+                umm[v] = ue[o + v] - 2 * ust[o + v];
+                upp[v] = ue[o + v] + 2 * ust[o + v];
+            }
+            double fm[NV], gm[NV], fp[NV], gp[NV], fmm[NV], gmm[NV], fpp[NV], gpp[NV];
+            eq.fluxes(um, fm, gm);
+            eq.fluxes(up, fp, gp);
+            eq.fluxes(umm, fmm, gmm);
+            eq.fluxes(upp, fpp, gpp);
+            for (int v = 0; v < NV; ++v) {
+                const double ft = 1.0 / 12.0 * (-fpp[v] + 8.0 * fp[v] - 8.0 * fm[v] + fmm[v]);
+                const double gt = 1.0 / 12.0 * (-gpp[v] + 8.0 * gp[v] - 8.0 * gm[v] + gmm[v]);
+                Fc[o + v] += 1.0 / 3.0 * ft;
+                Gc[o + v] += 1.0 / 3.0 * gt;
+                Uc[o + v] += 1.0 / 3.0 * ust[o + v];
+            }
+            for (int ii = 0; ii < n; ++ii) {
+                const double c = alpha * b.Dhat[ii * n + i];
+                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += c * Fc[o + v];
+            }
+            for (int jj = 0; jj < n; ++jj) {
+                const double c = alpha * b.Dhat[jj * n + j];
+                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += c * Gc[o + v];
+            }
+            for (int v = 0; v < NV; ++v) {
+                ws.U[idx_u(n, v, i, j, e)] = Uc[o + v];
+                ws.F[idx_F(n, v, 0, i, j, e)] = Fc[o + v];
+                ws.F[idx_F(n, v, 1, i, j, e)] = Gc[o + v];
+            }
+        }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Surface: prolong2interfaces! (dg_2d.jl:1269-1326), calc_interface_flux! (dg_2d.jl:1903-1946, plain FR
+// so compute_alp = 0, :1873-1877), Trixi calc_surface_integral! (weak form, boundary_interpolation =
+// lhat/w) and apply_jacobian! (du *= -inverse_jacobian).
+// ------------------------------------------------------------------------------------------------
+inline void prolong2interfaces(const Basis& b, const TreeMesh& m, const double* u, Workspace& ws, int nthreads = 1) {
+    const int n = b.n;
+    const size_t I = m.n_interfaces;
+    ws.iu.assign(2 * NV * n * I, 0.0);
+    ws.iU.assign(2 * NV * n * I, 0.0);
+    ws.iF.assign(2 * NV * n * I, 0.0);
+    auto ii = [&](int side, int v, int l, size_t k) { return side + 2 * (v + NV * (l + (size_t)n * k)); };
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (size_t k = 0; k < I; ++k) {
+        const int le = m.interface_left[k], re = m.interface_right[k];
+        for (int l = 0; l < n; ++l)
+            for (int v = 0; v < NV; ++v) {
+                if (m.interface_orientation[k] == 1) {
+                    ws.iu[ii(0, v, l, k)] = u[idx_u(n, v, n - 1, l, le)];
+                    ws.iu[ii(1, v, l, k)] = u[idx_u(n, v, 0, l, re)];
+                    ws.iU[ii(0, v, l, k)] = ws.U[idx_u(n, v, n - 1, l, le)];
+                    ws.iU[ii(1, v, l, k)] = ws.U[idx_u(n, v, 0, l, re)];
+                    ws.iF[ii(0, v, l, k)] = ws.F[idx_F(n, v, 0, n - 1, l, le)];
+                    ws.iF[ii(1, v, l, k)] = ws.F[idx_F(n, v, 0, 0, l, re)];
+                } else {
+                    ws.iu[ii(0, v, l, k)] = u[idx_u(n, v, l, n - 1, le)];
+                    ws.iu[ii(1, v, l, k)] = u[idx_u(n, v, l, 0, re)];
+                    ws.iU[ii(0, v, l, k)] = ws.U[idx_u(n, v, l, n - 1, le)];
+                    ws.iU[ii(1, v, l, k)] = ws.U[idx_u(n, v, l, 0, re)];
+                    ws.iF[ii(0, v, l, k)] = ws.F[idx_F(n, v, 1, l, n - 1, le)];
+                    ws.iF[ii(1, v, l, k)] = ws.F[idx_F(n, v, 1, l, 0, re)];
+                }
+            }
+    }
+}
+
+inline void calc_interface_flux(const Basis& b, const Euler& eq, const Options& opt, const TreeMesh& m,
+                                Workspace& ws, int nthreads = 1) {
+    const int n = b.n;
+    auto ii = [&](int side, int v, int l, size_t k) { return side + 2 * (v + NV * (l + (size_t)n * k)); };
+    bool bad = false;
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad)
+    for (int k = 0; k < m.n_interfaces; ++k) {
+        const int le = m.interface_left[k], re = m.interface_right[k];
+        const int o = m.interface_orientation[k];
+        const int left_dir = 2 * o - 1, right_dir = 2 * o - 2;   // 0-based face of Trixi's 2o / 2o-1
+        for (int l = 0; l < n; ++l) {
+            double Ul[NV], Ur[NV], ul[NV], ur[NV], fl[NV], fr[NV], Fn[NV];
+            for (int v = 0; v < NV; ++v) {
+                Ul[v] = ws.iU[ii(0, v, l, k)]; Ur[v] = ws.iU[ii(1, v, l, k)];
+                ul[v] = ws.iu[ii(0, v, l, k)]; ur[v] = ws.iu[ii(1, v, l, k)];
+                fl[v] = ws.iF[ii(0, v, l, k)]; fr[v] = ws.iF[ii(1, v, l, k)];
+            }
+            lw_surface_flux(eq, opt.flux_kind, opt.speed_kind, fl, fr, Ul, Ur, ul, ur, o, Fn, bad);
+            for (int v = 0; v < NV; ++v) {
+                ws.surface_flux_values[v + NV * (l + n * (left_dir + 4 * (size_t)le))] = Fn[v];
+                ws.surface_flux_values[v + NV * (l + n * (right_dir + 4 * (size_t)re))] = Fn[v];
+            }
+        }
+    }
+    if (bad) ws.bad = true;
+}
+
+// Exterior data for time-averaged Dirichlet boundaries (src/equations/equations.jl:6-37): the caller
+// supplies, per boundary node, the exterior state at the n Gauss-Lobatto time levels
+// ts_k = t + 0.5 dt_scaled (x_k + 1) and at t.
+struct BoundaryData {
+    const double* u_levels = nullptr;   // [v, k, l, B]  state at time level k
+    const double* u_now = nullptr;      // [v, l, B]     state at t
+};
+
+inline void calc_boundary_flux(const Basis& b, const Euler& eq, const Options& opt, const TreeMesh& m,
+                               const double* u, const BoundaryData& bd, double scaling_factor, Workspace& ws) {
+    // prolong2boundaries! (dg_2d.jl:1328-1376) + calc_adv_boundary_flux_by_direction! (:1411-1454)
+    const int n = b.n;
+    for (int k = 0; k < m.n_boundaries; ++k) {
+        const int e = m.boundary_element[k];
+        const int o = m.boundary_orientation[k];
+        const int side = m.boundary_side[k];
+        const int dir = m.boundary_direction[k];   // 1..4 (Trixi direction)
+        for (int l = 0; l < n; ++l) {
+            double ui[NV], Ui[NV], Fi[NV];
+            int i, j;
+            if (o == 1) { i = side == 1 ? n - 1 : 0; j = l; } else { i = l; j = side == 1 ? n - 1 : 0; }
+            for (int v = 0; v < NV; ++v) {
+                ui[v] = u[idx_u(n, v, i, j, e)];
+                Ui[v] = ws.U[idx_u(n, v, i, j, e)];
+                Fi[v] = ws.F[idx_F(n, v, o - 1, i, j, e)];
+            }
+            double Uo[NV] = {0, 0, 0, 0}, Fo[NV] = {0, 0, 0, 0}, uo[NV];
+            for (int q = 0; q < n; ++q) {
+                const double* ub = bd.u_levels + NV * (q + (size_t)n * (l + (size_t)n * k));
+                double fb[NV];
+                eq.flux(ub, o, fb);
+                for (int v = 0; v < NV; ++v) {
+                    Uo[v] += 0.5 * scaling_factor * ub[v] * b.weights[q];
+                    Fo[v] += 0.5 * scaling_factor * fb[v] * b.weights[q];
+                }
+            }
+            for (int v = 0; v < NV; ++v) uo[v] = bd.u_now[v + NV * (l + (size_t)n * k)];
+            double Fn[NV];
+            if (dir % 2 == 0)
+                lw_surface_flux(eq, opt.flux_kind, opt.speed_kind, Fi, Fo, Ui, Uo, ui, uo, o, Fn, ws.bad);
+            else
+                lw_surface_flux(eq, opt.flux_kind, opt.speed_kind, Fo, Fi, Uo, Ui, uo, ui, o, Fn, ws.bad);
+            for (int v = 0; v < NV; ++v) ws.surface_flux_values[v + NV * (l + n * ((dir - 1) + 4 * (size_t)e))] = Fn[v];
+        }
+    }
+}
+
+inline void surface_integral_and_jacobian(const Basis& b, const TreeMesh& m, double* du, const Workspace& ws,
+                                          int nthreads = 1) {
+    const int n = b.n;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int e = 0; e < m.n_elements; ++e) {
+        for (int l = 0; l < n; ++l)
+            for (int v = 0; v < NV; ++v) {
+                auto sfv = [&](int face) { return ws.surface_flux_values[v + NV * (l + n * (face + 4 * (size_t)e))]; };
+                du[idx_u(n, v, 0, l, e)] = du[idx_u(n, v, 0, l, e)] - sfv(0) * b.inv_w_first;
+                du[idx_u(n, v, n - 1, l, e)] = du[idx_u(n, v, n - 1, l, e)] + sfv(1) * b.inv_w_last;
+                du[idx_u(n, v, l, 0, e)] = du[idx_u(n, v, l, 0, e)] - sfv(2) * b.inv_w_first;
+                du[idx_u(n, v, l, n - 1, e)] = du[idx_u(n, v, l, n - 1, e)] + sfv(3) * b.inv_w_last;
+            }
+        const double factor = -m.inverse_jacobian[e];
+        for (int k = 0; k < NV * n * n; ++k) du[idx_u(n, 0, 0, 0, e) + k] *= factor;
+    }
+}
+
+inline void ensure_workspace(const Basis& b, const TreeMesh& m, Workspace& ws, bool mdrk) {
+    const size_t nodes = (size_t)b.n * b.n * m.n_elements;
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    if (ws.U.size() != NV * nodes) ws.U.assign(NV * nodes, nan);
+    if (ws.F.size() != 2 * NV * nodes) ws.F.assign(2 * NV * nodes, nan);
+    if (mdrk) {
+        if (ws.U2.size() != NV * nodes) ws.U2.assign(NV * nodes, nan);
+        if (ws.F2.size() != 2 * NV * nodes) ws.F2.assign(2 * NV * nodes, nan);
+    }
+    ws.surface_flux_values.assign((size_t)NV * b.n * 4 * m.n_elements, nan);
+    if (ws.temporal_errors.size() != (size_t)m.n_elements) ws.temporal_errors.assign(m.n_elements, nan);
+}
+
+// rhs!(du, u, t, dt, mesh::TreeMesh{2}, ..., ::LW, ...) (src/solvers/dgsem_tree/dg_2d.jl:28-83)
+// kind 0 = LW, 1 = MDRK stage 1 (multi_derivative_2d.jl:1-57), 2 = MDRK stage 2 (:59-116; `u2` = u*).
+inline void rhs(const Basis& b, const Euler& eq, const Options& opt, const TreeMesh& m, const double* u,
+                const double* u2, double* du, double t, double dt, const BoundaryData* bd, int kind, Workspace& ws,
+                int nthreads = 1) {
+    (void)t;
+    ensure_workspace(b, m, ws, kind != 0);
+    ws.bad = false;
+    const size_t ndof = (size_t)NV * b.n * b.n * m.n_elements;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (long long k = 0; k < (long long)ndof; ++k) du[k] = 0.0;   // reset_du!
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int e = 0; e < m.n_elements; ++e) {
+        if (kind == 0)
+            lw_volume_element(b, eq, opt, e, u, du, dt, m.inverse_jacobian[e], 1.0, ws);
+        else if (kind == 1)
+            mdrk1_volume_element(b, eq, e, u, du, dt, m.inverse_jacobian[e], 1.0, ws);
+        else
+            mdrk2_volume_element(b, eq, e, u2, du, dt, m.inverse_jacobian[e], 1.0, ws);
+    }
+    prolong2interfaces(b, m, u, ws, nthreads);
+    calc_interface_flux(b, eq, opt, m, ws, nthreads);
+    if (m.n_boundaries > 0) {
+        if (!bd || !bd->u_levels || !bd->u_now) throw std::invalid_argument("boundary data missing");
+        calc_boundary_flux(b, eq, opt, m, u, *bd, kind == 1 ? 0.5 : 1.0, ws);
+    }
+    surface_integral_and_jacobian(b, m, du, ws, nthreads);
+}
+
+// Trixi max_dt(u, t, mesh::TreeMesh{2}, constant_speed::False, ...) * cfl (src/solvers/lwfr.jl:176-190)
+inline double max_dt(const Basis& b, const Euler& eq, const TreeMesh& m, const double* u, double cfl, bool& bad,
+                     int nthreads = 1) {
+    const int n = b.n;
+    double max_scaled_speed = std::nextafter(0.0, 1.0);
+    bool bad_any = false;
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(max : max_scaled_speed) reduction(|| : bad_any)
+    for (int e = 0; e < m.n_elements; ++e) {
+        double ml1 = 0.0, ml2 = 0.0;
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                double l1, l2;
+                eq.max_abs_speeds(u + idx_u(n, 0, i, j, e), l1, l2, bad_any);
+                ml1 = std::max(ml1, l1);
+                ml2 = std::max(ml2, l2);
+            }
+        max_scaled_speed = std::max(max_scaled_speed, m.inverse_jacobian[e] * (ml1 + ml2));
+    }
+    if (bad_any) bad = true;
+    return cfl * (2.0 / (n * max_scaled_speed));
+}
+
+}  // namespace tlwo

@@ -1,0 +1,181 @@
+"""CPU tests of the oracle (the checker): known answers for the basis, scheme invariants the reference
+has by construction, agreement with an independent numpy restatement, and regression against the
+committed golden fixtures."""
+import os
+
+import numpy as np
+import pytest
+
+import numpy_lw
+
+
+def test_gll_known_answers(oracle_mod):
+    # N = 4: nodes 0, +-sqrt(3/7), +-1; weights 32/45, 49/90, 1/10
+    x, w, D, Dh = oracle_mod.basis(4)
+    np.testing.assert_allclose(x, [-1, -np.sqrt(3 / 7), 0, np.sqrt(3 / 7), 1], atol=1e-15)
+    np.testing.assert_allclose(w, [1 / 10, 49 / 90, 32 / 45, 49 / 90, 1 / 10], atol=1e-15)
+    # N = 3: +-1, +-sqrt(1/5); weights 1/6, 5/6
+    x, w, _, _ = oracle_mod.basis(3)
+    np.testing.assert_allclose(x, [-1, -np.sqrt(0.2), np.sqrt(0.2), 1], atol=1e-15)
+    np.testing.assert_allclose(w, [1 / 6, 5 / 6, 5 / 6, 1 / 6], atol=1e-15)
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7])
+def test_derivative_matrix_exact_on_polynomials(oracle_mod, N):
+    x, w, D, Dh = oracle_mod.basis(N)
+    for p in range(N + 1):
+        np.testing.assert_allclose(D @ x ** p, p * x ** max(p - 1, 0) * (p > 0), atol=2e-13)
+    # summation-by-parts: M D + D^T M = B
+    M = np.diag(w)
+    B = np.zeros((N + 1, N + 1)); B[0, 0] = -1; B[-1, -1] = 1
+    np.testing.assert_allclose(M @ D + D.T @ M, B, atol=1e-13)
+    # Dhat = -M^-1 D^T M
+    np.testing.assert_allclose(Dh, -np.diag(1 / w) @ D.T @ M, atol=1e-13)
+    assert abs(w.sum() - 2.0) < 1e-14
+
+
+def test_host_basis_matches_oracle(oracle_mod, tl):
+    from trixilw.basis import gauss_lobatto
+    for N in range(1, 8):
+        x, w = gauss_lobatto(N)
+        xo, wo, _, _ = oracle_mod.basis(N)
+        np.testing.assert_allclose(x, xo, atol=1e-15)
+        np.testing.assert_allclose(w, wo, atol=1e-15)
+
+
+def _setup(tl, level, N, ic, lo=-10.0, hi=10.0, periodic=True):
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    mesh = tl.TreeMesh((lo, lo), (hi, hi), level, periodicity=periodic)
+    xy = mesh.node_coordinates(N)
+    u = ic(xy[0], xy[1], 0.0, eq)
+    u = np.ascontiguousarray(np.transpose(u, (2, 1, 0, 3))).reshape(-1)
+    return eq, mesh, u
+
+
+@pytest.mark.parametrize("N", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("kind", [0, 1])
+def test_free_stream_preservation(oracle_mod, tl, N, kind):
+    eq, mesh, u = _setup(tl, 2, N, tl.ConstantState(1.3, 0.4, -0.7, 2.1))
+    o = oracle_mod.Oracle(mesh, N)
+    dt = o.max_dt(u, 0.3)
+    du = o.rhs(u, 0.0, dt, kind=kind)
+    assert np.abs(du).max() < 1e-12
+    if kind == 1:
+        us = u + dt * du
+        du2 = o.rhs(u, 0.0, dt, kind=2, us=us)
+        assert np.abs(du2).max() < 1e-12
+
+
+@pytest.mark.parametrize("N", [2, 3, 4, 5])
+@pytest.mark.parametrize("kind", [0, 1])
+def test_conservation_periodic(oracle_mod, tl, N, kind):
+    eq, mesh, u = _setup(tl, 3, N, tl.IsentropicVortex(5.0, center=(1.0, -2.0)))
+    o = oracle_mod.Oracle(mesh, N)
+    dt = o.max_dt(u, 0.4)
+    du = o.rhs(u, 0.0, dt, kind=kind)
+    _, w, _, _ = oracle_mod.basis(N)
+    n = N + 1
+    d = du.reshape(mesh.n_elements, n, n, 4)
+    total = np.einsum("ejiv,j,i->v", d, w, w) / mesh.inverse_jacobian[0] ** 2
+    scale = np.einsum("ejiv,j,i->v", np.abs(d), w, w) / mesh.inverse_jacobian[0] ** 2
+    assert np.all(np.abs(total) <= 1e-13 * scale)
+
+
+@pytest.mark.parametrize("N", [3, 4, 5])
+def test_mirror_symmetry(oracle_mod, tl, N):
+    """Mirroring x -> -x (with v1 -> -v1) commutes with the rhs."""
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), 3)
+    xy = mesh.node_coordinates(N)
+    ic = tl.IsentropicVortex(4.0, center=(0.7, -1.3), velocity=(0.5, 1.0))
+    u = np.transpose(ic(xy[0], xy[1], 0.0, eq), (2, 1, 0, 3))        # [e, j, i, v]
+    # mirrored field: element at (ix, iy) takes the data of (m-1-ix, iy) with i reversed and v1 negated
+    m = mesh.cells_per_dimension
+    src = mesh.element_at[m - 1 - mesh.ix, mesh.iy]
+    um = u[src][:, :, ::-1, :].copy()
+    um[..., 1] *= -1
+    o = oracle_mod.Oracle(mesh, N)
+    dt = 0.01
+    du = o.rhs(np.ascontiguousarray(u).reshape(-1), 0.0, dt).reshape(u.shape)
+    dum = o.rhs(np.ascontiguousarray(um).reshape(-1), 0.0, dt).reshape(u.shape)
+    expect = du[src][:, :, ::-1, :].copy()
+    expect[..., 1] *= -1
+    np.testing.assert_allclose(dum, expect, atol=1e-12 * np.abs(du).max())
+
+
+@pytest.mark.parametrize("N", [3, 4, 5])
+def test_numpy_restatement_agrees(oracle_mod, tl, N):
+    eq, mesh, u = _setup(tl, 2, N, tl.IsentropicVortex(5.0, center=(0.5, 0.3)))
+    o = oracle_mod.Oracle(mesh, N)
+    dt = o.max_dt(u, 0.9 * (N + 1) * 0.103)
+    du = o.rhs(u, 0.0, dt)
+    x, w, D, Dh = oracle_mod.basis(N)
+    n = N + 1
+    du_np, U, F, G = numpy_lw.rhs(u.reshape(mesh.n_elements, n, n, 4), mesh, D, Dh, w, dt)
+    rel = np.linalg.norm(du - du_np.reshape(-1)) / np.linalg.norm(du)
+    assert rel < 1e-13, rel
+    Uo = o.get(0).reshape(mesh.n_elements, n, n, 4)
+    np.testing.assert_allclose(Uo, U, rtol=0, atol=1e-13)
+    Fo = o.get(1).reshape(mesh.n_elements, n, n, 2, 4)
+    np.testing.assert_allclose(Fo[..., 0, :], F, atol=1e-12)
+    np.testing.assert_allclose(Fo[..., 1, :], G, atol=1e-12)
+
+
+def test_domain_error_on_negative_pressure(oracle_mod, tl):
+    eq, mesh, u = _setup(tl, 2, 3, tl.ConstantState(1.0, 0.1, 0.1, 1.0))
+    u = u.reshape(-1, 4)
+    o = oracle_mod.Oracle(mesh, 3)
+    # interior node: the rhs takes no square root there (as in the reference), max_dt does
+    bad = u.copy()
+    bad[5, 3] = -1.0   # element 1, node (1,1): negative energy -> negative pressure
+    o.rhs(bad.reshape(-1), 0.0, 1e-3)
+    with pytest.raises(oracle_mod.OracleDomainError):
+        o.max_dt(bad.reshape(-1), 0.5)
+    # face node: the interface speed estimate takes sqrt(gamma p / rho) of the time-averaged trace
+    bad = u.copy()
+    bad[0, 3] = -1.0
+    with pytest.raises(oracle_mod.OracleDomainError):
+        o.rhs(bad.reshape(-1), 0.0, 1e-3)
+
+
+def _vortex_error(oracle_mod, tl, level, N, t_end=1.0, kind=0):
+    eq, mesh, u = _setup(tl, level, N, tl.IsentropicVortex(5.0))
+    o = oracle_mod.Oracle(mesh, N)
+    cfl = 0.98 * (N + 1) * tl.lw_fourier_cfl(min(N, 4)) if N <= 4 else 0.3
+    steps, t = o.steps(u, 100000, cfl, 0.0, t_end, kind=kind, nthreads=os.cpu_count() or 1)
+    assert abs(t - t_end) < 1e-12
+    xy = mesh.node_coordinates(N)
+    ue = np.transpose(tl.IsentropicVortex(5.0)(xy[0], xy[1], t_end, eq), (2, 1, 0, 3)).reshape(-1)
+    _, w, _, _ = oracle_mod.basis(N)
+    n = N + 1
+    d = (u - ue).reshape(mesh.n_elements, n, n, 4)
+    return np.sqrt(np.einsum("ejiv,j,i->v", d * d, w, w).sum() / mesh.inverse_jacobian[0] ** 2 / 400.0)
+
+
+@pytest.mark.parametrize("N", [3, 4])
+def test_vortex_convergence_order(oracle_mod, tl, N):
+    # levels 5 -> 6 (32^2 -> 64^2 elements on [-10,10]^2); coarser levels are pre-asymptotic
+    e1 = _vortex_error(oracle_mod, tl, 5, N)
+    e2 = _vortex_error(oracle_mod, tl, 6, N)
+    eoc = np.log2(e1 / e2)
+    assert eoc > N + 0.4, (e1, e2, eoc)
+
+
+def test_mdrk_converges(oracle_mod, tl):
+    e1 = _vortex_error(oracle_mod, tl, 5, 3, kind=1)
+    e2 = _vortex_error(oracle_mod, tl, 6, 3, kind=1)
+    assert np.log2(e1 / e2) > 3.4, (e1, e2)
+
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.mark.parametrize("name", ["lw_vortex_N3_L2", "lw_vortex_N4_L2", "lw_vortex_N5_L2", "mdrk_vortex_N4_L2",
+                                  "lw_riemann_N4_L2"])
+def test_golden_fixtures(oracle_mod, tl, name):
+    import golden_cases
+    path = os.path.join(GOLDEN, name + ".npz")
+    ref = np.load(path)
+    out = golden_cases.run_case(name, oracle_mod, tl)
+    for k in ref.files:
+        np.testing.assert_allclose(out[k], ref[k], rtol=0, atol=1e-13 * max(1.0, np.abs(ref[k]).max()), err_msg=k)

@@ -1,0 +1,774 @@
+// tlw_capi.cu -- host side of libtlw: handle, device memory, kernel launches, the device-resident CFL
+// step loop (captured as CUDA graphs) and the extern "C" entry points declared in include/tlw.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/tlw.h"
+#include "tlw_surface.cuh"
+#include "tlw_volume.cuh"
+
+using namespace tlw;
+
+namespace {
+
+// Gauss-Lobatto-Legendre basis on the host (Kopriva, "Implementing Spectral Methods for PDEs": Legendre
+// recursion Alg. 22/24, nodes/weights Alg. 25, barycentric weights Alg. 30, derivative matrix Alg. 37);
+// Dhat = -M^{-1} D^T M and the weak-form lift factors 1/w_1, 1/w_n as Trixi's LobattoLegendreBasis.
+void legendre_q(int N, double x, double& q, double& dq, double& LN) {
+    double a = 1.0, b = x, da = 0.0, db = 1.0;
+    for (int k = 2; k <= N; ++k) {
+        const double c = ((2.0 * k - 1.0) * x * b - (k - 1.0) * a) / k;
+        const double dc = da + (2.0 * k - 1.0) * b;
+        a = b; b = c; da = db; db = dc;
+    }
+    const int k = N + 1;
+    const double c = ((2.0 * k - 1.0) * x * b - (k - 1.0) * a) / k;
+    const double dc = da + (2.0 * k - 1.0) * b;
+    q = c - a;
+    dq = dc - da;
+    LN = b;
+}
+
+void build_basis(int N, tlw::Basis& B, std::vector<double>& nodes) {
+    const int n = N + 1;
+    std::vector<double> x(n), w(n), wb(n, 1.0);
+    x[0] = -1.0; x[N] = 1.0;
+    w[0] = w[N] = 2.0 / (N * (N + 1.0));
+    const double pi = 3.14159265358979323846;
+    for (int j = 1; j <= (N + 1) / 2 - 1; ++j) {
+        double xj = -std::cos((j + 0.25) * pi / N - 3.0 / (8.0 * N * pi * (j + 0.25)));
+        double q, dq, LN;
+        for (int it = 0; it < 100; ++it) {
+            legendre_q(N, xj, q, dq, LN);
+            const double d = -q / dq;
+            xj += d;
+            if (std::fabs(d) <= 4.0 * 2.220446049250313e-16 * std::fabs(xj)) break;
+        }
+        legendre_q(N, xj, q, dq, LN);
+        x[j] = xj; x[N - j] = -xj;
+        w[j] = w[N - j] = 2.0 / (N * (N + 1.0) * LN * LN);
+    }
+    if (N >= 2 && N % 2 == 0) {
+        double q, dq, LN;
+        legendre_q(N, 0.0, q, dq, LN);
+        x[N / 2] = 0.0;
+        w[N / 2] = 2.0 / (N * (N + 1.0) * LN * LN);
+    }
+    for (int j = 0; j < n; ++j) {
+        for (int k = 0; k < n; ++k)
+            if (k != j) wb[j] *= (x[j] - x[k]);
+        wb[j] = 1.0 / wb[j];
+    }
+    std::memset(&B, 0, sizeof(B));
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c)
+            if (c != r) {
+                B.D[r * n + c] = wb[c] / wb[r] / (x[r] - x[c]);
+                B.D[r * n + r] -= B.D[r * n + c];
+            }
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) B.Dhat[r * n + c] = -B.D[c * n + r] * w[c] / w[r];
+    for (int k = 0; k < n; ++k) B.weights[k] = w[k];
+    B.inv_w_first = 1.0 / w[0];
+    B.inv_w_last = 1.0 / w[n - 1];
+    nodes = x;
+}
+
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+}  // namespace
+
+struct tlw_handle {
+    tlw_opts opts{};
+    int N = 0, n = 0, nn = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    tlw::Basis h_basis{};
+    std::vector<double> nodes;
+    tlw::Basis* d_basis = nullptr;
+    StepState* d_step = nullptr;
+    // mesh
+    bool have_mesh = false;
+    int64_t E = 0;
+    double* d_inv_jac = nullptr;
+    int *d_xl = nullptr, *d_xr = nullptr, *d_yl = nullptr, *d_yr = nullptr;
+    int nx = 0, ny = 0;
+    int64_t nb = 0;
+    int *d_b_elem = nullptr, *d_b_dir = nullptr, *d_bx = nullptr, *d_by = nullptr;
+    int nbx = 0, nby = 0;
+    double *d_levels = nullptr, *d_now = nullptr;
+    bool have_bdata = false;
+    // element-sized buffers
+    double* d_state[2] = {nullptr, nullptr};
+    int cur = 0;
+    double* d_us = nullptr;
+    double *d_in = nullptr, *d_in2 = nullptr, *d_out = nullptr;
+    double *d_tU = nullptr, *d_tF = nullptr, *d_U2 = nullptr, *d_F2 = nullptr;
+    // graphs: [start buffer] one step, two steps
+    cudaGraphExec_t g_one[2] = {nullptr, nullptr};
+    cudaGraphExec_t g_two[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+int fail(tlw_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+#define TLW_CUDA(h, call)                                                                        \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail(h, TLW_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+size_t state_doubles(const tlw_handle* h) { return (size_t)NV * h->nn * h->E; }
+size_t trace_doubles(const tlw_handle* h) { return (size_t)NV * h->n * 4 * h->E; }
+
+void drop_graphs(tlw_handle* h) {
+    for (int k = 0; k < 2; ++k) {
+        if (h->g_one[k]) cudaGraphExecDestroy(h->g_one[k]);
+        if (h->g_two[k]) cudaGraphExecDestroy(h->g_two[k]);
+        h->g_one[k] = h->g_two[k] = nullptr;
+    }
+}
+
+void free_mesh(tlw_handle* h) {
+    drop_graphs(h);
+    dfree(h->d_inv_jac);
+    dfree(h->d_xl); dfree(h->d_xr); dfree(h->d_yl); dfree(h->d_yr);
+    dfree(h->d_b_elem); dfree(h->d_b_dir); dfree(h->d_bx); dfree(h->d_by);
+    dfree(h->d_levels); dfree(h->d_now);
+    dfree(h->d_state[0]); dfree(h->d_state[1]);
+    dfree(h->d_us); dfree(h->d_in); dfree(h->d_in2); dfree(h->d_out);
+    dfree(h->d_tU); dfree(h->d_tF); dfree(h->d_U2); dfree(h->d_F2);
+    h->have_mesh = false;
+    h->have_bdata = false;
+}
+
+// ---- kernel launch helpers (template dispatch over N) -------------------------------------------
+template <int N>
+struct Launch {
+    using C = VolCfg<N>;
+    static void set_attributes() {
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(3));
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(3));
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
+    }
+    static void volume(cudaStream_t s, int stage, int mode, const VolArgs& a) {
+        const int grid = (int)((a.E + C::EB - 1) / C::EB);
+        if (grid == 0) return;
+        if (stage == TLW_STAGE_LW) {
+            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(3), s>>>(a);
+            else lw_volume_kernel<N, MODE_STEP><<<grid, C::THREADS, C::smem_bytes(3), s>>>(a);
+        } else if (stage == TLW_STAGE_MDRK1) {
+            if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(2), s>>>(a);
+            else mdrk1_volume_kernel<N, MODE_STEP><<<grid, C::THREADS, C::smem_bytes(2), s>>>(a);
+        } else {
+            if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(2), s>>>(a);
+            else mdrk2_volume_kernel<N, MODE_STEP><<<grid, C::THREADS, C::smem_bytes(2), s>>>(a);
+        }
+    }
+    static void interfaces(cudaStream_t s, const SurfArgs& a) {
+        const long long threads = (long long)a.count * (N + 1);
+        if (threads == 0) return;
+        interface_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
+    }
+    static void boundaries(cudaStream_t s, const BndArgs& a) {
+        const long long threads = (long long)a.count * (N + 1);
+        if (threads == 0) return;
+        boundary_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
+    }
+    static void max_speed(cudaStream_t s, const double* u, const double* ij, int E, double gamma, StepState* st) {
+        if (E == 0) return;
+        max_speed_kernel<N><<<(E + 255) / 256, 256, 0, s>>>(u, ij, E, gamma, st);
+    }
+};
+
+template <template <int> class F, class... A>
+void dispatch(int N, A&&... args) {
+    switch (N) {
+        case 1: F<1>::run(args...); break;
+        case 2: F<2>::run(args...); break;
+        case 3: F<3>::run(args...); break;
+        case 4: F<4>::run(args...); break;
+        case 5: F<5>::run(args...); break;
+        case 6: F<6>::run(args...); break;
+        case 7: F<7>::run(args...); break;
+        default: break;
+    }
+}
+template <int N> struct SetAttr { static void run() { Launch<N>::set_attributes(); } };
+template <int N> struct Vol { static void run(cudaStream_t s, int st, int m, const VolArgs& a) { Launch<N>::volume(s, st, m, a); } };
+template <int N> struct Ifc { static void run(cudaStream_t s, const SurfArgs& a) { Launch<N>::interfaces(s, a); } };
+template <int N> struct Bnd { static void run(cudaStream_t s, const BndArgs& a) { Launch<N>::boundaries(s, a); } };
+template <int N> struct Spd {
+    static void run(cudaStream_t s, const double* u, const double* ij, int E, double g, StepState* st) {
+        Launch<N>::max_speed(s, u, ij, E, g, st);
+    }
+};
+
+// Events recorded between the phases of a step (tlw_step_timed); null when not timing.
+struct PhaseEvents {
+    cudaEvent_t after_volume, after_x, after_y;
+};
+
+// One rhs (volume + surfaces) launched on h->stream.
+//   u_flux: state the volume fluxes use (u, or u* for MDRK stage 2); u_jump: u^n for the interfaces
+//   out: du (mode RHS) or the stage/updated state (mode STEP, base = u_base)
+void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const double* u_jump, const double* u_base,
+                 double* out, const double* dt_ptr, const PhaseEvents* ev = nullptr) {
+    VolArgs va{};
+    va.u = u_flux;
+    va.u_base = u_base;
+    va.out = out;
+    va.tU = h->d_tU;
+    va.tF = h->d_tF;
+    va.U2 = h->d_U2;
+    va.F2 = h->d_F2;
+    va.inv_jac = h->d_inv_jac;
+    va.dt = dt_ptr;
+    va.basis = h->d_basis;
+    va.E = (int)h->E;
+    va.gamma = h->opts.gamma;
+    dispatch<Vol>(h->N, h->stream, stage, mode, va);
+    if (ev) cudaEventRecord(ev->after_volume, h->stream);
+
+    SurfArgs sa{};
+    sa.u = u_jump;
+    sa.out = out;
+    sa.tU = h->d_tU;
+    sa.tF = h->d_tF;
+    sa.inv_jac = h->d_inv_jac;
+    sa.dt = dt_ptr;
+    sa.step_mode = mode == MODE_STEP;
+    sa.gamma = h->opts.gamma;
+    sa.flux_kind = h->opts.surface_flux;
+    sa.speed_kind = h->opts.max_speed;
+    sa.inv_w_first = h->h_basis.inv_w_first;
+    sa.inv_w_last = h->h_basis.inv_w_last;
+    sa.status = &h->d_step->status;
+
+    BndArgs ba{};
+    ba.u = u_jump;
+    ba.out = out;
+    ba.tU = h->d_tU;
+    ba.tF = h->d_tF;
+    ba.element = h->d_b_elem;
+    ba.direction = h->d_b_dir;
+    ba.levels = h->d_levels;
+    ba.now = h->d_now;
+    ba.inv_jac = h->d_inv_jac;
+    ba.dt = dt_ptr;
+    ba.step_mode = mode == MODE_STEP;
+    ba.scaling_factor = stage == TLW_STAGE_MDRK1 ? 0.5 : 1.0;
+    ba.gamma = h->opts.gamma;
+    ba.flux_kind = h->opts.surface_flux;
+    ba.speed_kind = h->opts.max_speed;
+    ba.inv_w_first = h->h_basis.inv_w_first;
+    ba.inv_w_last = h->h_basis.inv_w_last;
+    ba.weights = h->d_basis->weights;
+    ba.status = &h->d_step->status;
+
+    // x interfaces, x boundaries, y interfaces, y boundaries: corner nodes are shared only between
+    // launches of different orientation, which the stream orders.
+    sa.left = h->d_xl; sa.right = h->d_xr; sa.count = h->nx; sa.orientation = 1;
+    dispatch<Ifc>(h->N, h->stream, sa);
+    ba.bidx = h->d_bx; ba.count = h->nbx; ba.orientation = 1;
+    dispatch<Bnd>(h->N, h->stream, ba);
+    if (ev) cudaEventRecord(ev->after_x, h->stream);
+    sa.left = h->d_yl; sa.right = h->d_yr; sa.count = h->ny; sa.orientation = 2;
+    dispatch<Ifc>(h->N, h->stream, sa);
+    ba.bidx = h->d_by; ba.count = h->nby; ba.orientation = 2;
+    dispatch<Bnd>(h->N, h->stream, ba);
+    if (ev) cudaEventRecord(ev->after_y, h->stream);
+}
+
+// one CFL step from state[from] into state[1 - from]; ev (optional): [after dt, stage 1 phases, stage 2 phases]
+void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const PhaseEvents* ev = nullptr) {
+    const double* u = h->d_state[from];
+    double* unew = h->d_state[1 - from];
+    dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step);
+    finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
+    if (after_dt) cudaEventRecord(after_dt, h->stream);
+    const double* dtp = &h->d_step->dt;
+    if (h->opts.time_discretization == TLW_LW) {
+        enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, dtp, ev);
+    } else {
+        enqueue_rhs(h, TLW_STAGE_MDRK1, MODE_STEP, u, u, u, h->d_us, dtp, ev);
+        enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, dtp, ev ? ev + 1 : nullptr);
+    }
+}
+
+__global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
+    double x[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = 1e-3 * (threadIdx.x + k);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) x[k] = fma(x[k], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += x[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+int check_ready(tlw_handle* h) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
+    if (h->nb > 0 && !h->have_bdata) return fail(h, TLW_E_STATE, "mesh has boundaries: call tlw_set_boundary_data first");
+    return TLW_OK;
+}
+
+int read_status(tlw_handle* h) {
+    unsigned st = 0;
+    TLW_CUDA(h, cudaMemcpyAsync(&st, &h->d_step->status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (st) {
+        const unsigned zero = 0;
+        TLW_CUDA(h, cudaMemcpy(&h->d_step->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+        return fail(h, TLW_E_NONADMISSIBLE, "non-admissible state: square root of a negative number (DomainError)");
+    }
+    return TLW_OK;
+}
+
+int ensure(tlw_handle* h, double*& p, size_t doubles) {
+    if (!p) TLW_CUDA(h, cudaMalloc(&p, doubles * sizeof(double)));
+    return TLW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t tlw_abi_version(void) { return TLW_ABI_VERSION; }
+
+int tlw_create(const tlw_opts* opts, tlw_handle** out) {
+    if (!opts || !out) return TLW_E_ARG;
+    *out = nullptr;
+    if (opts->polydeg < 1 || opts->polydeg > 7) return TLW_E_ARG;
+    if (opts->time_discretization != TLW_LW && opts->time_discretization != TLW_MDRK) return TLW_E_ARG;
+    if (opts->surface_flux != TLW_FLUX_RUSANOV && opts->surface_flux != TLW_FLUX_HLL) return TLW_E_ARG;
+    if (opts->max_speed != TLW_SPEED_NAIVE && opts->max_speed != TLW_SPEED_DAVIS) return TLW_E_ARG;
+    if (!(opts->gamma > 1.0)) return TLW_E_ARG;
+    tlw_handle* h = new (std::nothrow) tlw_handle();
+    if (!h) return TLW_E_ARG;
+    h->opts = *opts;
+    h->N = opts->polydeg;
+    h->n = h->N + 1;
+    h->nn = h->n * h->n;
+    h->device = opts->device;
+    build_basis(h->N, h->h_basis, h->nodes);
+    int rc = TLW_OK;
+    do {
+        if (cudaSetDevice(h->device) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "cudaSetDevice failed"); break; }
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "stream"); break; }
+        if (cudaMalloc(&h->d_basis, sizeof(tlw::Basis)) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "alloc basis"); break; }
+        if (cudaMemcpy(h->d_basis, &h->h_basis, sizeof(tlw::Basis), cudaMemcpyHostToDevice) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "copy basis"); break; }
+        if (cudaMalloc(&h->d_step, sizeof(StepState)) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "alloc step"); break; }
+        StepState st{};
+        st.cfl = 1.0;
+        st.t_end = INFINITY;
+        if (cudaMemcpy(h->d_step, &st, sizeof(st), cudaMemcpyHostToDevice) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "init step"); break; }
+        dispatch<SetAttr>(h->N);
+        if (cudaGetLastError() != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "kernel attributes"); break; }
+    } while (0);
+    if (rc != TLW_OK) {
+        tlw_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return TLW_OK;
+}
+
+int tlw_destroy(tlw_handle* h) {
+    if (!h) return TLW_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_mesh(h);
+    dfree(h->d_basis);
+    dfree(h->d_step);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return TLW_OK;
+}
+
+int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_jacobian, int64_t n_interfaces,
+                      const int64_t* interface_neighbor_ids, const int64_t* interface_orientations,
+                      int64_t n_boundaries, const int64_t* boundary_neighbor_ids,
+                      const int64_t* boundary_orientations, const int64_t* boundary_neighbor_sides,
+                      const int64_t* n_boundaries_per_direction) {
+    if (!h) return TLW_E_ARG;
+    if (n_elements <= 0 || n_elements > (int64_t)0x7fffffff / 64 || !inverse_jacobian) return fail(h, TLW_E_ARG, "n_elements");
+    if (n_interfaces < 0 || (n_interfaces > 0 && (!interface_neighbor_ids || !interface_orientations)))
+        return fail(h, TLW_E_ARG, "interfaces");
+    if (n_boundaries < 0 || (n_boundaries > 0 && (!boundary_neighbor_ids || !boundary_orientations ||
+                                                  !boundary_neighbor_sides || !n_boundaries_per_direction)))
+        return fail(h, TLW_E_ARG, "boundaries");
+    std::vector<int> xl, xr, yl, yr;
+    for (int64_t k = 0; k < n_interfaces; ++k) {
+        const int64_t l = interface_neighbor_ids[2 * k] - 1, r = interface_neighbor_ids[2 * k + 1] - 1;
+        const int64_t o = interface_orientations[k];
+        if (l < 0 || l >= n_elements || r < 0 || r >= n_elements || (o != 1 && o != 2))
+            return fail(h, TLW_E_ARG, "interface " + std::to_string(k + 1) + " out of range");
+        (o == 1 ? xl : yl).push_back((int)l);
+        (o == 1 ? xr : yr).push_back((int)r);
+    }
+    std::vector<int> belem, bdir, bx, by;
+    if (n_boundaries > 0) {
+        int64_t sum = 0;
+        for (int d = 0; d < 4; ++d) sum += n_boundaries_per_direction[d];
+        if (sum != n_boundaries) return fail(h, TLW_E_ARG, "n_boundaries_per_direction does not sum to n_boundaries");
+        int64_t k = 0;
+        for (int d = 1; d <= 4; ++d)
+            for (int64_t c = 0; c < n_boundaries_per_direction[d - 1]; ++c, ++k) {
+                const int64_t e = boundary_neighbor_ids[k] - 1;
+                const int64_t o = boundary_orientations[k];
+                const int64_t side = boundary_neighbor_sides[k];
+                if (e < 0 || e >= n_elements) return fail(h, TLW_E_ARG, "boundary element out of range");
+                // direction d: 1/2 are x faces (orientation 1), 3/4 y faces; odd d -> element on the + side
+                if (o != (d <= 2 ? 1 : 2) || side != (d % 2 == 1 ? 2 : 1))
+                    return fail(h, TLW_E_ARG, "boundary " + std::to_string(k + 1) + " inconsistent with its direction");
+                belem.push_back((int)e);
+                bdir.push_back(d);
+                (o == 1 ? bx : by).push_back((int)k);
+            }
+    }
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    free_mesh(h);
+    h->E = n_elements;
+    auto up_i = [&](int*& d, const std::vector<int>& v) -> int {
+        if (v.empty()) return TLW_OK;
+        TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
+        TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+        return TLW_OK;
+    };
+    int rc;
+    TLW_CUDA(h, cudaMalloc(&h->d_inv_jac, n_elements * sizeof(double)));
+    TLW_CUDA(h, cudaMemcpy(h->d_inv_jac, inverse_jacobian, n_elements * sizeof(double), cudaMemcpyHostToDevice));
+    if ((rc = up_i(h->d_xl, xl)) || (rc = up_i(h->d_xr, xr)) || (rc = up_i(h->d_yl, yl)) || (rc = up_i(h->d_yr, yr)) ||
+        (rc = up_i(h->d_b_elem, belem)) || (rc = up_i(h->d_b_dir, bdir)) || (rc = up_i(h->d_bx, bx)) ||
+        (rc = up_i(h->d_by, by)))
+        return rc;
+    h->nx = (int)xl.size(); h->ny = (int)yl.size();
+    h->nb = n_boundaries; h->nbx = (int)bx.size(); h->nby = (int)by.size();
+    const size_t sd = state_doubles(h), td = trace_doubles(h);
+    if ((rc = ensure(h, h->d_state[0], sd)) || (rc = ensure(h, h->d_state[1], sd)) || (rc = ensure(h, h->d_tU, td)) ||
+        (rc = ensure(h, h->d_tF, td)))
+        return rc;
+    if (h->opts.time_discretization == TLW_MDRK) {
+        if ((rc = ensure(h, h->d_U2, sd)) || (rc = ensure(h, h->d_F2, 2 * sd)) || (rc = ensure(h, h->d_us, sd))) return rc;
+    }
+    h->cur = 0;
+    h->have_mesh = true;
+    return TLW_OK;
+}
+
+int tlw_set_boundary_data(tlw_handle* h, const double* levels, const double* now, int32_t where) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh");
+    if (h->nb == 0) return TLW_OK;
+    if (!levels || !now) return fail(h, TLW_E_ARG, "boundary data pointers");
+    const size_t nl = (size_t)NV * h->n * h->n * h->nb, nw = (size_t)NV * h->n * h->nb;
+    int rc;
+    if ((rc = ensure(h, h->d_levels, nl)) || (rc = ensure(h, h->d_now, nw))) return rc;
+    const cudaMemcpyKind k = where == TLW_WHERE_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    TLW_CUDA(h, cudaMemcpyAsync(h->d_levels, levels, nl * sizeof(double), k, h->stream));
+    TLW_CUDA(h, cudaMemcpyAsync(h->d_now, now, nw * sizeof(double), k, h->stream));
+    if (where != TLW_WHERE_DEVICE) TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->have_bdata = true;
+    return TLW_OK;
+}
+
+int tlw_rhs(tlw_handle* h, int32_t stage, double* du, const double* u, const double* us, double t, double dt,
+            int32_t where) {
+    (void)t;
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!du || !u || (stage == TLW_STAGE_MDRK2 && !us)) return fail(h, TLW_E_ARG, "null pointer");
+    if (stage < TLW_STAGE_LW || stage > TLW_STAGE_MDRK2) return fail(h, TLW_E_ARG, "stage");
+    if (stage != TLW_STAGE_LW && h->opts.time_discretization != TLW_MDRK)
+        return fail(h, TLW_E_STATE, "MDRK stages need a handle created with TLW_MDRK");
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    const size_t bytes = state_doubles(h) * sizeof(double);
+    TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->dt_call, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    const double *du_in = u, *dus = us;
+    double* dout = du;
+    if (where == TLW_WHERE_HOST) {
+        if ((rc = ensure(h, h->d_in, state_doubles(h))) || (rc = ensure(h, h->d_out, state_doubles(h)))) return rc;
+        TLW_CUDA(h, cudaMemcpyAsync(h->d_in, u, bytes, cudaMemcpyHostToDevice, h->stream));
+        du_in = h->d_in;
+        if (stage == TLW_STAGE_MDRK2) {
+            if ((rc = ensure(h, h->d_in2, state_doubles(h)))) return rc;
+            TLW_CUDA(h, cudaMemcpyAsync(h->d_in2, us, bytes, cudaMemcpyHostToDevice, h->stream));
+            dus = h->d_in2;
+        }
+        dout = h->d_out;
+    }
+    const double* u_flux = stage == TLW_STAGE_MDRK2 ? dus : du_in;
+    enqueue_rhs(h, stage, MODE_RHS, u_flux, du_in, du_in, dout, &h->d_step->dt_call);
+    TLW_CUDA(h, cudaGetLastError());
+    if (where == TLW_WHERE_HOST) {
+        TLW_CUDA(h, cudaMemcpyAsync(du, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream));
+        return read_status(h);
+    }
+    return TLW_OK;
+}
+
+int tlw_max_dt(tlw_handle* h, const double* u, int32_t where, double cfl, double* dt_out) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!u || !dt_out) return fail(h, TLW_E_ARG, "null pointer");
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    const double* du_in = u;
+    if (where == TLW_WHERE_HOST) {
+        if ((rc = ensure(h, h->d_in, state_doubles(h)))) return rc;
+        TLW_CUDA(h, cudaMemcpyAsync(h->d_in, u, state_doubles(h) * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        du_in = h->d_in;
+    }
+    const unsigned long long zero = 0;
+    TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->max_bits, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+    dispatch<Spd>(h->N, h->stream, du_in, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step);
+    TLW_CUDA(h, cudaGetLastError());
+    unsigned long long bits = 0;
+    TLW_CUDA(h, cudaMemcpyAsync(&bits, &h->d_step->max_bits, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+    TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->max_bits, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+    if ((rc = read_status(h))) return rc;
+    double m;
+    std::memcpy(&m, &bits, sizeof(m));
+    const double tiny = 4.9406564584124654e-324;
+    if (!(m > tiny)) m = tiny;
+    *dt_out = cfl * (2.0 / (h->n * m));
+    return TLW_OK;
+}
+
+int tlw_set_state(tlw_handle* h, const double* u, int32_t where, double t) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!u) return fail(h, TLW_E_ARG, "null pointer");
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    const cudaMemcpyKind k = where == TLW_WHERE_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    TLW_CUDA(h, cudaMemcpyAsync(h->d_state[h->cur], u, state_doubles(h) * sizeof(double), k, h->stream));
+    StepState* sp = h->d_step;
+    const long long zero = 0;
+    TLW_CUDA(h, cudaMemcpyAsync(&sp->t, &t, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    TLW_CUDA(h, cudaMemcpyAsync(&sp->steps, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+    if (where != TLW_WHERE_DEVICE) TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    return TLW_OK;
+}
+
+int tlw_get_state(tlw_handle* h, double* u, int32_t where, double* t_out) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!u) return fail(h, TLW_E_ARG, "null pointer");
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    const cudaMemcpyKind k = where == TLW_WHERE_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    TLW_CUDA(h, cudaMemcpyAsync(u, h->d_state[h->cur], state_doubles(h) * sizeof(double), k, h->stream));
+    double t = 0;
+    if (t_out) TLW_CUDA(h, cudaMemcpyAsync(&t, &h->d_step->t, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (where != TLW_WHERE_DEVICE || t_out) {
+        if ((rc = read_status(h))) return rc;
+    }
+    if (t_out) *t_out = t;
+    return TLW_OK;
+}
+
+int tlw_step(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double t_end, int32_t use_graph) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (nsteps < 0) return fail(h, TLW_E_ARG, "nsteps");
+    if (nsteps == 0) return TLW_OK;
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    // parameters into the device step state (cfl, fixed_dt, t_end are contiguous after t)
+    double params[3] = {t_end, cfl, fixed_dt};
+    TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->t_end, params, sizeof(params), cudaMemcpyHostToDevice, h->stream));
+    if (!use_graph) {
+        for (int s = 0; s < nsteps; ++s) {
+            enqueue_step(h, h->cur);
+            h->cur ^= 1;
+        }
+        TLW_CUDA(h, cudaGetLastError());
+        return TLW_OK;
+    }
+    auto capture = [&](int from, int count, cudaGraphExec_t& exec) -> int {
+        if (exec) return TLW_OK;
+        cudaGraph_t g = nullptr;
+        TLW_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int b = from;
+        for (int s = 0; s < count; ++s) { enqueue_step(h, b); b ^= 1; }
+        cudaError_t e1 = cudaStreamEndCapture(h->stream, &g);
+        if (e1 != cudaSuccess) return fail(h, TLW_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e1));
+        cudaError_t e2 = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess) { exec = nullptr; return fail(h, TLW_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2)); }
+        return TLW_OK;
+    };
+    int left = nsteps;
+    if (h->cur == 1) {
+        if ((rc = capture(1, 1, h->g_one[1]))) return rc;
+        TLW_CUDA(h, cudaGraphLaunch(h->g_one[1], h->stream));
+        h->cur = 0;
+        --left;
+    }
+    if (left >= 2) {
+        if ((rc = capture(0, 2, h->g_two[0]))) return rc;
+        for (; left >= 2; left -= 2) TLW_CUDA(h, cudaGraphLaunch(h->g_two[0], h->stream));
+    }
+    if (left == 1) {
+        if ((rc = capture(0, 1, h->g_one[0]))) return rc;
+        TLW_CUDA(h, cudaGraphLaunch(h->g_one[0], h->stream));
+        h->cur = 1;
+    }
+    return TLW_OK;
+}
+
+int tlw_step_timed(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double t_end, double* phase_ms) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (nsteps < 0 || !phase_ms) return fail(h, TLW_E_ARG, "nsteps / phase_ms");
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    double params[3] = {t_end, cfl, fixed_dt};
+    TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->t_end, params, sizeof(params), cudaMemcpyHostToDevice, h->stream));
+    const int nstage = h->opts.time_discretization == TLW_LW ? 1 : 2;
+    std::vector<cudaEvent_t> evs((size_t)nsteps * (2 + 3 * nstage));
+    for (auto& e : evs) TLW_CUDA(h, cudaEventCreate(&e));
+    size_t k = 0;
+    std::vector<size_t> starts;
+    for (int s = 0; s < nsteps; ++s) {
+        starts.push_back(k);
+        cudaEvent_t e_start = evs[k++], e_dt = evs[k++];
+        PhaseEvents pe[2];
+        for (int st = 0; st < nstage; ++st) pe[st] = {evs[k++], evs[k++], evs[k++]};
+        cudaEventRecord(e_start, h->stream);
+        enqueue_step(h, h->cur, e_dt, pe);
+        h->cur ^= 1;
+    }
+    TLW_CUDA(h, cudaGetLastError());
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (int p = 0; p < 5; ++p) phase_ms[p] = 0.0;
+    for (int s = 0; s < nsteps; ++s) {
+        size_t b = starts[s];
+        float ms;
+        cudaEventElapsedTime(&ms, evs[b], evs[b + 1]);
+        phase_ms[0] += ms;
+        cudaEvent_t prev = evs[b + 1];
+        for (int st = 0; st < nstage; ++st) {
+            cudaEvent_t* pe = &evs[b + 2 + 3 * st];
+            cudaEventElapsedTime(&ms, prev, pe[0]); phase_ms[1] += ms;
+            cudaEventElapsedTime(&ms, pe[0], pe[1]); phase_ms[2] += ms;
+            cudaEventElapsedTime(&ms, pe[1], pe[2]); phase_ms[3] += ms;
+            prev = pe[2];
+        }
+        cudaEventElapsedTime(&ms, evs[b], prev);
+        phase_ms[4] += ms;
+    }
+    for (auto& e : evs) cudaEventDestroy(e);
+    return read_status(h);
+}
+
+int tlw_probe_fp64_tflops(int32_t device, double* tflops) {
+    if (!tflops) return TLW_E_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return TLW_E_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int threads = 256, blocks = sms * 8, iters = 1 << 14;
+    double* out = nullptr;
+    if (cudaMalloc(&out, (size_t)threads * blocks * sizeof(double)) != cudaSuccess) return TLW_E_CUDA;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    for (int rep = 0; rep < 6; ++rep) {
+        cudaEventRecord(a);
+        fp64_probe_kernel<<<blocks, threads>>>(out, iters, 0.9999999, 1e-7);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float ms;
+        cudaEventElapsedTime(&ms, a, b);
+        if (rep > 0 && ms < best) best = ms;   // first launch is warm-up
+    }
+    const cudaError_t err = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    if (err != cudaSuccess) return TLW_E_CUDA;
+    *tflops = 2.0 * 16.0 * iters * (double)threads * blocks / (best * 1e-3) / 1e12;
+    return TLW_OK;
+}
+
+int tlw_get_time(tlw_handle* h, double* t, double* dt_last, int64_t* steps) {
+    if (!h) return TLW_E_ARG;
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    StepState st{};
+    TLW_CUDA(h, cudaMemcpyAsync(&st, h->d_step, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    int rc = read_status(h);
+    if (t) *t = st.t;
+    if (dt_last) *dt_last = st.dt;
+    if (steps) *steps = st.steps;
+    return rc;
+}
+
+int64_t tlw_cache_size(tlw_handle* h, int32_t item) {
+    if (!h || !h->have_mesh) return -1;
+    switch (item) {
+        case TLW_CACHE_U_TRACES:
+        case TLW_CACHE_F_TRACES: return (int64_t)trace_doubles(h);
+        case TLW_CACHE_U2: return h->d_U2 ? (int64_t)state_doubles(h) : -1;
+        case TLW_CACHE_F2: return h->d_F2 ? (int64_t)(2 * state_doubles(h)) : -1;
+        default: return -1;
+    }
+}
+
+int tlw_get_cache(tlw_handle* h, int32_t item, double* out, int32_t where) {
+    if (!h || !out) return TLW_E_ARG;
+    const int64_t count = tlw_cache_size(h, item);
+    if (count < 0) return fail(h, TLW_E_ARG, "cache item not available");
+    const double* src = item == TLW_CACHE_U_TRACES ? h->d_tU : item == TLW_CACHE_F_TRACES ? h->d_tF
+                        : item == TLW_CACHE_U2 ? h->d_U2 : h->d_F2;
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    const cudaMemcpyKind k = where == TLW_WHERE_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    TLW_CUDA(h, cudaMemcpyAsync(out, src, count * sizeof(double), k, h->stream));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    return TLW_OK;
+}
+
+int tlw_synchronize(tlw_handle* h) {
+    if (!h) return TLW_E_ARG;
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    TLW_CUDA(h, cudaGetLastError());
+    return read_status(h);
+}
+
+int tlw_get_stream(tlw_handle* h, void** stream) {
+    if (!h || !stream) return TLW_E_ARG;
+    *stream = (void*)h->stream;
+    return TLW_OK;
+}
+
+int tlw_state_pointer(tlw_handle* h, double** dptr) {
+    if (!h || !dptr) return TLW_E_ARG;
+    if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh");
+    *dptr = h->d_state[h->cur];
+    return TLW_OK;
+}
+
+const char* tlw_last_error(tlw_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+}  // extern "C"

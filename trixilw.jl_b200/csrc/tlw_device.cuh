@@ -1,0 +1,129 @@
+// tlw_device.cuh -- device-side building blocks shared by the LW / MDRK kernels (FP64, sm_100a).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tlw {
+
+constexpr int NV = 4;   // compressible Euler 2D: rho, rho v1, rho v2, rho e
+
+// status bits written by kernels (never a trap): the host maps them to TLW_E_* codes
+constexpr unsigned STATUS_NONADMISSIBLE = 1u;   // sqrt of a negative number (reference: DomainError)
+
+struct Basis {
+    double D[16 * 16];      // derivative matrix, D[a*n + b] = l_b'(x_a)
+    double Dhat[16 * 16];   // -M^{-1} D^T M
+    double weights[16];
+    double inv_w_first, inv_w_last;
+};
+
+// Euler flux pair (Trixi flux(u, 1|2, eq) for CompressibleEulerEquations2D); 1 divide, ~17 flops.
+__device__ __forceinline__ void euler_fluxes(double gm1, double r, double m1, double m2, double e, double* f,
+                                             double* g) {
+    const double ir = 1.0 / r;
+    const double v1 = m1 * ir, v2 = m2 * ir;
+    const double p = gm1 * (e - 0.5 * (m1 * v1 + m2 * v2));
+    const double ep = e + p;
+    f[0] = m1;
+    f[1] = m1 * v1 + p;
+    f[2] = m1 * v2;
+    f[3] = ep * v1;
+    g[0] = m2;
+    g[1] = f[2];
+    g[2] = m2 * v2 + p;
+    g[3] = ep * v2;
+}
+
+__device__ __forceinline__ void euler_flux_dir(double gm1, const double* u, int orientation, double* fo) {
+    double f[NV], g[NV];
+    euler_fluxes(gm1, u[0], u[1], u[2], u[3], f, g);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) fo[v] = orientation == 1 ? f[v] : g[v];
+}
+
+// sqrt that flags a negative argument instead of trapping
+__device__ __forceinline__ double checked_sqrt(double x, unsigned* status) {
+    if (!(x >= 0.0)) atomicOr(status, STATUS_NONADMISSIBLE);
+    return sqrt(x);
+}
+
+// Trixi max_abs_speed_naive (kind 0) / max_abs_speed (kind 1) for CompressibleEulerEquations2D
+__device__ __forceinline__ double max_abs_speed(double gamma, const double* ul, const double* ur, int orientation,
+                                                int kind, unsigned* status) {
+    const double gm1 = gamma - 1.0;
+    const double irl = 1.0 / ul[0], irr = 1.0 / ur[0];
+    const double v1l = ul[1] * irl, v2l = ul[2] * irl, v1r = ur[1] * irr, v2r = ur[2] * irr;
+    const double pl = gm1 * (ul[3] - 0.5 * (ul[1] * v1l + ul[2] * v2l));
+    const double pr = gm1 * (ur[3] - 0.5 * (ur[1] * v1r + ur[2] * v2r));
+    const double vl = orientation == 1 ? v1l : v2l;
+    const double vr = orientation == 1 ? v1r : v2r;
+    const double cl = checked_sqrt(gamma * pl * irl, status);
+    const double cr = checked_sqrt(gamma * pr * irr, status);
+    if (kind == 0) return fmax(fabs(vl), fabs(vr)) + fmax(cl, cr);
+    return fmax(fabs(vl) + cl, fabs(vr) + cr);
+}
+
+// Trixi min_max_speed_naive (FluxHLL default)
+__device__ __forceinline__ void min_max_speed(double gamma, const double* ul, const double* ur, int orientation,
+                                              double* lmin, double* lmax, unsigned* status) {
+    const double gm1 = gamma - 1.0;
+    const double irl = 1.0 / ul[0], irr = 1.0 / ur[0];
+    const double v1l = ul[1] * irl, v2l = ul[2] * irl, v1r = ur[1] * irr, v2r = ur[2] * irr;
+    const double pl = gm1 * (ul[3] - 0.5 * (ul[1] * v1l + ul[2] * v2l));
+    const double pr = gm1 * (ur[3] - 0.5 * (ur[1] * v1r + ur[2] * v2r));
+    const double vl = orientation == 1 ? v1l : v2l;
+    const double vr = orientation == 1 ? v1r : v2r;
+    *lmin = vl - checked_sqrt(gamma * pl * irl, status);
+    *lmax = vr + checked_sqrt(gamma * pr * irr, status);
+}
+
+// The 8-argument LW surface flux as TreeMesh calls it: surface_flux(f_ll, f_rr, U_ll, U_rr, u_ll, u_rr).
+// Rusanov (FluxPlusDissipation + DissipationLocalLaxFriedrichs): lambda from arguments 3/4, jump in 5/6.
+// HLL (FluxHLL LW method): speeds from arguments 5/6, jump in 3/4.
+__device__ __forceinline__ void lw_surface_flux(double gamma, int flux_kind, int speed_kind, const double* fl,
+                                                const double* fr, const double* a3, const double* a4,
+                                                const double* a5, const double* a6, int orientation, double* out,
+                                                unsigned* status) {
+    if (flux_kind == 0) {
+        const double lambda = max_abs_speed(gamma, a3, a4, orientation, speed_kind, status);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) out[v] = 0.5 * (fl[v] + fr[v]) + (-0.5 * lambda * (a6[v] - a5[v]));
+    } else {
+        double lmin, lmax;
+        min_max_speed(gamma, a5, a6, orientation, &lmin, &lmax, status);
+        if (lmin >= 0 && lmax >= 0) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) out[v] = fl[v];
+        } else if (lmax <= 0 && lmin <= 0) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) out[v] = fr[v];
+        } else {
+            const double inv = 1.0 / (lmax - lmin);
+            const double cll = lmax * inv, crr = lmin * inv, cd = lmin * lmax * inv;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) out[v] = cll * fl[v] - crr * fr[v] + cd * (a4[v] - a3[v]);
+        }
+    }
+}
+
+__device__ __forceinline__ void load4(const double* __restrict__ p, double* x) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+}
+__device__ __forceinline__ void load4_rw(const double* p, double* x) {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *(reinterpret_cast<const double2*>(p) + 1);
+    x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+}
+__device__ __forceinline__ void store4(double* p, const double* x) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(x[0], x[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(x[2], x[3]);
+}
+// streaming store: the output is not re-read by this kernel
+__device__ __forceinline__ void store4_cs(double* p, const double* x) {
+    __stcs(reinterpret_cast<double2*>(p), make_double2(x[0], x[1]));
+    __stcs(reinterpret_cast<double2*>(p) + 1, make_double2(x[2], x[3]));
+}
+
+}  // namespace tlw

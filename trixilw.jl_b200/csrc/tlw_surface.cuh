@@ -1,0 +1,217 @@
+// tlw_surface.cuh -- interface and boundary LW fluxes fused with the weak-form surface lift and the
+// Jacobian (FP64, sm_100a), plus the CFL time-step reduction.
+//
+// Restates (TreeMesh{2}):
+//   prolong2interfaces!   src/solvers/dgsem_tree/dg_2d.jl:1269-1326 (traces read where they lie)
+//   calc_interface_flux!  src/solvers/dgsem_tree/dg_2d.jl:1903-1946 (plain FR: compute_alp = 0)
+//   prolong2boundaries!   src/solvers/dgsem_tree/dg_2d.jl:1328-1376
+//   calc_boundary_flux!   src/solvers/dgsem_tree/dg_2d.jl:1385-1454 + time-averaged Dirichlet
+//                         src/equations/equations.jl:6-37
+//   Trixi calc_surface_integral! (weak form: du[1] -= Fn/w_1, du[n] += Fn/w_n) and apply_jacobian!
+//   (du *= -J^{-1}), folded into a read-modify-write of the face nodes only.
+//   Trixi max_dt (TreeMesh{2}, CompressibleEulerEquations2D) * cfl, src/solvers/lwfr.jl:176-190, with
+//   set_dt! clamping (src/solvers/lwfr.jl:76-90).
+//
+// One thread per (interface, face node). x- and y-oriented interfaces are launched separately: inside
+// one orientation no two threads touch the same node, so the read-modify-writes need no atomics and
+// the result is deterministic.
+#pragma once
+#include "tlw_device.cuh"
+
+namespace tlw {
+
+struct SurfArgs {
+    const double* u;         // instantaneous state u^n (jumps)            [v,i,j,e]
+    double* out;             // du (mode 0) or the updated state (mode 1)  [v,i,j,e]
+    const double* tU;        // [v, l, face, e]
+    const double* tF;        // [v, l, face, e]
+    const int* left;         // interfaces of this orientation
+    const int* right;
+    int count;
+    int orientation;         // 1 = x, 2 = y
+    const double* inv_jac;
+    const double* dt;
+    int step_mode;           // 1: scale the lift by dt (state update)
+    double gamma;
+    int flux_kind, speed_kind;
+    double inv_w_first, inv_w_last;
+    unsigned* status;
+};
+
+template <int N>
+__global__ void __launch_bounds__(128) interface_kernel(SurfArgs a) {
+    constexpr int n = N + 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = t / n;
+    const int l = t - k * n;
+    if (k >= a.count) return;
+    const int le = __ldg(a.left + k), re = __ldg(a.right + k);
+    int nodeL, nodeR, faceL, faceR;
+    if (a.orientation == 1) { nodeL = (n - 1) + n * l; nodeR = n * l; faceL = 1; faceR = 0; }
+    else { nodeL = l + n * (n - 1); nodeR = l; faceL = 3; faceR = 2; }
+    double uL[NV], uR[NV], UL[NV], UR[NV], FL[NV], FR[NV], Fn[NV];
+    load4(a.u + ((size_t)le * n * n + nodeL) * NV, uL);
+    load4(a.u + ((size_t)re * n * n + nodeR) * NV, uR);
+    load4(a.tU + (((size_t)le * 4 + faceL) * n + l) * NV, UL);
+    load4(a.tU + (((size_t)re * 4 + faceR) * n + l) * NV, UR);
+    load4(a.tF + (((size_t)le * 4 + faceL) * n + l) * NV, FL);
+    load4(a.tF + (((size_t)re * 4 + faceR) * n + l) * NV, FR);
+    // TreeMesh argument order: surface_flux(f_ll, f_rr, U_ll, U_rr, u_ll, u_rr) (dg_2d.jl:1928)
+    lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, FL, FR, UL, UR, uL, uR, a.orientation, Fn, a.status);
+    const double dts = a.step_mode ? *a.dt : 1.0;
+    const double sL = -__ldg(a.inv_jac + le) * a.inv_w_last * dts;
+    const double sR = __ldg(a.inv_jac + re) * a.inv_w_first * dts;
+    double* oL = a.out + ((size_t)le * n * n + nodeL) * NV;
+    double* oR = a.out + ((size_t)re * n * n + nodeR) * NV;
+    double x[NV];
+    load4_rw(oL, x);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) x[v] = fma(sL, Fn[v], x[v]);
+    store4(oL, x);
+    load4_rw(oR, x);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) x[v] = fma(sR, Fn[v], x[v]);
+    store4(oR, x);
+}
+
+struct BndArgs {
+    const double* u;
+    double* out;
+    const double* tU;
+    const double* tF;
+    const int* bidx;         // boundaries of this orientation (0-based ids into the arrays below)
+    const int* element;      // [B] element of each boundary
+    const int* direction;    // [B] Trixi direction 1..4 (1: -x face of the element, 2: +x, 3: -y, 4: +y)
+    const double* levels;    // exterior state at the n time levels [v, q, l, B]
+    const double* now;       // exterior state at t                 [v, l, B]
+    int count;
+    int orientation;
+    const double* inv_jac;
+    const double* dt;
+    int step_mode;
+    double scaling_factor;   // 1, or 0.5 for MDRK stage 1 (multi_derivative_2d.jl:34)
+    double gamma;
+    int flux_kind, speed_kind;
+    double inv_w_first, inv_w_last;
+    const double* weights;   // GLL weights (device)
+    unsigned* status;
+};
+
+template <int N>
+__global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
+    constexpr int n = N + 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = t / n;
+    const int l = t - kk * n;
+    if (kk >= a.count) return;
+    const int k = __ldg(a.bidx + kk);
+    const int e = __ldg(a.element + k);
+    const int dir = __ldg(a.direction + k);
+    int node, face;
+    switch (dir) {
+        case 1: node = n * l; face = 0; break;
+        case 2: node = (n - 1) + n * l; face = 1; break;
+        case 3: node = l; face = 2; break;
+        default: node = l + n * (n - 1); face = 3; break;
+    }
+    const double gm1 = a.gamma - 1.0;
+    double ui[NV], Ui[NV], Fi[NV], Uo[NV] = {0, 0, 0, 0}, Fo[NV] = {0, 0, 0, 0}, uo[NV], Fn[NV];
+    load4(a.u + ((size_t)e * n * n + node) * NV, ui);
+    load4(a.tU + (((size_t)e * 4 + face) * n + l) * NV, Ui);
+    load4(a.tF + (((size_t)e * 4 + face) * n + l) * NV, Fi);
+    for (int q = 0; q < n; ++q) {
+        double ub[NV], fb[NV];
+        load4(a.levels + (((size_t)k * n + l) * n + q) * NV, ub);
+        euler_flux_dir(gm1, ub, a.orientation, fb);
+        const double w = 0.5 * a.scaling_factor;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            Uo[v] += w * ub[v] * a.weights[q];
+            Fo[v] += w * fb[v] * a.weights[q];
+        }
+    }
+    load4(a.now + ((size_t)k * n + l) * NV, uo);
+    if (dir % 2 == 0)
+        lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, Fi, Fo, Ui, Uo, ui, uo, a.orientation, Fn, a.status);
+    else
+        lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, Fo, Fi, Uo, Ui, uo, ui, a.orientation, Fn, a.status);
+    const double dts = a.step_mode ? *a.dt : 1.0;
+    const double ij = __ldg(a.inv_jac + e);
+    const double s = (dir % 2 == 0) ? -ij * a.inv_w_last * dts : ij * a.inv_w_first * dts;
+    double* o = a.out + ((size_t)e * n * n + node) * NV;
+    double x[NV];
+    load4_rw(o, x);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) x[v] = fma(s, Fn[v], x[v]);
+    store4(o, x);
+}
+
+// ------------------------------------------------------------------------------------------------
+// CFL time step on the device.
+// ------------------------------------------------------------------------------------------------
+struct StepState {
+    unsigned long long max_bits;   // bits of max_e J^{-1}(lambda1 + lambda2) (non-negative doubles order as ints)
+    double dt;                     // time step used by the current step
+    double t;                      // time at the start of the next step
+    double t_end;
+    double cfl;
+    double fixed_dt;               // > 0: use this dt instead of the CFL estimate
+    long long steps;               // accepted steps
+    unsigned status;               // STATUS_* bits
+    int pad;
+    double dt_call;                // dt for the rhs entry points (set from the host)
+};
+
+// per element: max over nodes of |v1|+c and |v2|+c, times J^{-1}; max over elements (atomic)
+template <int N>
+__global__ void __launch_bounds__(256) max_speed_kernel(const double* __restrict__ u, const double* __restrict__ inv_jac,
+                                                        int E, double gamma, StepState* s) {
+    constexpr int nn = (N + 1) * (N + 1);
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double m = 0.0;
+    if (e < E) {
+        const double gm1 = gamma - 1.0;
+        double ml1 = 0.0, ml2 = 0.0;
+        for (int k = 0; k < nn; ++k) {
+            double x[NV];
+            load4(u + ((size_t)e * nn + k) * NV, x);
+            const double ir = 1.0 / x[0];
+            const double v1 = x[1] * ir, v2 = x[2] * ir;
+            const double p = gm1 * (x[3] - 0.5 * (x[1] * v1 + x[2] * v2));
+            const double c = checked_sqrt(gamma * p * ir, &s->status);
+            ml1 = fmax(ml1, fabs(v1) + c);
+            ml2 = fmax(ml2, fabs(v2) + c);
+        }
+        m = __ldg(inv_jac + e) * (ml1 + ml2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ double wmax[8];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = wmax[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, wmax[w]);
+        if (b > 0.0) atomicMax(&s->max_bits, (unsigned long long)__double_as_longlong(b));
+    }
+}
+
+// dt = cfl * 2 / (n * max_scaled_speed), clamped so that t + dt <= t_end; a finished run gets dt = 0
+// (the remaining launches of a captured step are then exact no-ops on the state).
+__global__ void finalize_dt_kernel(StepState* s, int n) {
+    double maxs = __longlong_as_double((long long)s->max_bits);
+    const double tiny = 4.9406564584124654e-324;   // nextfloat(0.0)
+    if (!(maxs > tiny)) maxs = tiny;
+    double dt = s->fixed_dt > 0.0 ? s->fixed_dt : s->cfl * (2.0 / (n * maxs));
+    const double t = s->t, te = s->t_end;
+    // isapprox(t, t_end) with Julia's default rtol = sqrt(eps(Float64))
+    const bool finished = fabs(t - te) <= 1.4901161193847656e-8 * fmax(fabs(t), fabs(te)) || t >= te;
+    if (finished) dt = 0.0;
+    else if (t + dt > te) dt = te - t;
+    s->dt = dt;
+    s->t = finished ? t : t + dt;
+    if (!finished) s->steps += 1;
+    s->max_bits = 0ull;
+}
+
+}  // namespace tlw

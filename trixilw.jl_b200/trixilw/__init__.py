@@ -1,0 +1,22 @@
+"""trixilw: B200 (sm_100a) drop-in for TrixiLW.jl's Lax-Wendroff / MDRK right-hand side (TreeMesh{2},
+compressible Euler, FP64). The compute runs in libtlw.so (CUDA, C ABI in include/tlw.h); this package is
+the host-side mirror of the reference's Julia interface for that path."""
+from ._lib import DomainError, TlwError, lib
+from .equations import (CompressibleEulerEquations2D, ConstantState, DensityWave, FourQuadrantRiemann,
+                        IsentropicVortex)
+from .lwfr import LWIntegrator, LWSolution, l2_linf_errors, solve_lwfr
+from .mesh import TreeMesh
+from .semidiscretization import (LW, MDRK, DGSEM, Adaptive, BoundaryConditionDirichlet, CFLBased, FluxHLL,
+                                 FluxLaxFriedrichs, SemidiscretizationHyperbolic, VolumeIntegralFR,
+                                 boundary_condition_periodic, flux_hll, flux_lax_friedrichs,
+                                 get_time_discretization, lw_fourier_cfl, rhs, rhs_mdrk1, rhs_mdrk2,
+                                 semidiscretize, trixi2lw)
+
+__all__ = [
+    "DomainError", "TlwError", "lib", "CompressibleEulerEquations2D", "ConstantState", "DensityWave",
+    "FourQuadrantRiemann", "IsentropicVortex", "LWIntegrator", "LWSolution", "l2_linf_errors", "solve_lwfr",
+    "TreeMesh", "LW", "MDRK", "DGSEM", "Adaptive", "BoundaryConditionDirichlet", "CFLBased", "FluxHLL",
+    "FluxLaxFriedrichs", "SemidiscretizationHyperbolic", "VolumeIntegralFR", "boundary_condition_periodic",
+    "flux_hll", "flux_lax_friedrichs", "get_time_discretization", "lw_fourier_cfl", "rhs", "rhs_mdrk1",
+    "rhs_mdrk2", "semidiscretize", "trixi2lw",
+]

@@ -1,0 +1,109 @@
+"""ctypes binding of libtlw.so (the CUDA library; entry points declared in include/tlw.h).
+
+The shared library is built in-tree by ``__graft_entry__.build()`` (or ``python -m trixilw.build``) into
+this directory. There is no CPU fallback: if the library is missing or no CUDA device is usable, every
+call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtlw.so")
+
+TLW_OK = 0
+TLW_E_ARG = 1
+TLW_E_CUDA = 2
+TLW_E_NONADMISSIBLE = 3
+TLW_E_STATE = 4
+TLW_E_UNSUPPORTED = 5
+
+TLW_LW, TLW_MDRK = 0, 1
+TLW_FLUX_RUSANOV, TLW_FLUX_HLL = 0, 1
+TLW_SPEED_NAIVE, TLW_SPEED_DAVIS = 0, 1
+TLW_WHERE_HOST, TLW_WHERE_DEVICE = 0, 1
+TLW_STAGE_LW, TLW_STAGE_MDRK1, TLW_STAGE_MDRK2 = 0, 1, 2
+TLW_CACHE_U_TRACES, TLW_CACHE_F_TRACES, TLW_CACHE_U2, TLW_CACHE_F2 = 0, 1, 2, 3
+
+# every symbol include/tlw.h declares
+EXPORTED = (
+    "tlw_abi_version", "tlw_create", "tlw_destroy", "tlw_set_tree_mesh", "tlw_set_boundary_data", "tlw_rhs",
+    "tlw_max_dt", "tlw_set_state", "tlw_get_state", "tlw_step", "tlw_get_time", "tlw_get_cache",
+    "tlw_cache_size", "tlw_synchronize", "tlw_get_stream", "tlw_state_pointer", "tlw_last_error",
+    "tlw_step_timed", "tlw_probe_fp64_tflops",
+)
+
+
+class TlwOpts(ctypes.Structure):
+    _fields_ = [
+        ("polydeg", ctypes.c_int32),
+        ("time_discretization", ctypes.c_int32),
+        ("surface_flux", ctypes.c_int32),
+        ("max_speed", ctypes.c_int32),
+        ("gamma", ctypes.c_double),
+        ("device", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
+    ]
+
+
+class DomainError(ArithmeticError):
+    """Raised where the reference raises Julia's DomainError (square root of a negative pressure or
+    density), so that adaptive callers can catch it exactly like the reference's ``test_rhs!``."""
+
+
+class TlwError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libtlw error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libtlw.so once; raises if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libtlw.so not built at {LIB_PATH}; run __graft_entry__.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    i32, i64, dbl = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    dp = ctypes.POINTER(ctypes.c_double)
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    L.tlw_abi_version.restype = i32
+    L.tlw_create.argtypes = [ctypes.POINTER(TlwOpts), ctypes.POINTER(P)]
+    L.tlw_destroy.argtypes = [P]
+    L.tlw_set_tree_mesh.argtypes = [P, i64, dp, i64, i64p, i64p, i64, i64p, i64p, i64p, i64p]
+    L.tlw_set_boundary_data.argtypes = [P, P, P, i32]
+    L.tlw_rhs.argtypes = [P, i32, P, P, P, dbl, dbl, i32]
+    L.tlw_max_dt.argtypes = [P, P, i32, dbl, dp]
+    L.tlw_set_state.argtypes = [P, P, i32, dbl]
+    L.tlw_get_state.argtypes = [P, P, i32, dp]
+    L.tlw_step.argtypes = [P, i32, dbl, dbl, dbl, i32]
+    L.tlw_get_time.argtypes = [P, dp, dp, i64p]
+    L.tlw_step_timed.argtypes = [P, i32, dbl, dbl, dbl, dp]
+    L.tlw_probe_fp64_tflops.argtypes = [i32, dp]
+    L.tlw_get_cache.argtypes = [P, i32, P, i32]
+    L.tlw_cache_size.argtypes = [P, i32]
+    L.tlw_cache_size.restype = i64
+    L.tlw_synchronize.argtypes = [P]
+    L.tlw_get_stream.argtypes = [P, ctypes.POINTER(P)]
+    L.tlw_state_pointer.argtypes = [P, ctypes.POINTER(P)]
+    L.tlw_last_error.argtypes = [P]
+    L.tlw_last_error.restype = ctypes.c_char_p
+    for name in EXPORTED:
+        L[name].restype = L[name].restype if name in ("tlw_abi_version", "tlw_cache_size", "tlw_last_error") else ctypes.c_int
+    _lib = L
+    return L
+
+
+def check(handle, rc: int) -> None:
+    if rc == TLW_OK:
+        return
+    msg = lib().tlw_last_error(handle).decode() if handle else ""
+    if rc == TLW_E_NONADMISSIBLE:
+        raise DomainError(msg or "non-admissible state")
+    raise TlwError(rc, msg)

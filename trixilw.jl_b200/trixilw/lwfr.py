@@ -1,0 +1,142 @@
+"""Host-side mirror of the reference's LW time loop, with the step loop itself on the device.
+
+Mirrors solve_lwfr / LWIntegrator / perform_step!(..., ::CFLBased, ::LW|::MDRK)
+(src/solvers/lwfr.jl:31-263, src/solvers/mdrk.jl:1-29): each step computes dt = cfl * max_dt(u)
+(clamped to the final time by set_dt!), evaluates the rhs and updates u = uprev + dt * du. Here that
+whole step - the CFL reduction included - runs in libtlw (``tlw_step``) and dt never leaves the GPU; the
+host only synchronises between callback intervals.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+from .basis import gauss_lobatto
+from .semidiscretization import Adaptive, CFLBased, LWUpdate, SemidiscretizationHyperbolic, _ptr
+
+
+@dataclass
+class Stats:
+    naccept: int = 0
+    nreject: int = 0
+
+
+@dataclass
+class LWSolution:
+    u: list
+    prob: LWUpdate
+    t: list
+    stats: Stats = field(default_factory=Stats)
+
+
+class LWIntegrator:
+    """State of a device-resident LW/MDRK run (LWIntegrator, src/solvers/lwfr.jl:31-56)."""
+
+    def __init__(self, lw_update: LWUpdate, tolerances=None):
+        self.p: SemidiscretizationHyperbolic = lw_update.p
+        self.tspan = lw_update.tspan
+        self.t = self.tspan[0]
+        self.dt = 0.0
+        self.iter = 0
+        self.tolerances = tolerances or {"abstol": 0.0, "reltol": 0.0}
+        self.stats = Stats()
+
+    @property
+    def handle(self):
+        return self.p.handle
+
+    def set_state(self, u: np.ndarray, t: float):
+        check(self.handle, lib().tlw_set_state(self.handle, _ptr(u), _lib.TLW_WHERE_HOST, float(t)))
+        self.t = float(t)
+
+    def get_state(self) -> np.ndarray:
+        u = np.empty(4 * self.p.ndofs())
+        t = ctypes.c_double()
+        check(self.handle, lib().tlw_get_state(self.handle, _ptr(u), _lib.TLW_WHERE_HOST, ctypes.byref(t)))
+        self.t = t.value
+        return u
+
+    def sync_time(self):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        steps = ctypes.c_int64()
+        check(self.handle, lib().tlw_get_time(self.handle, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(steps)))
+        self.t, self.dt, self.iter = t.value, dt.value, int(steps.value)
+        self.stats.naccept = self.iter
+        return self.t
+
+    def step(self, nsteps: int, cfl: float, fixed_dt: float = 0.0, use_graph: bool = True):
+        check(self.handle, lib().tlw_step(self.handle, int(nsteps), float(cfl), float(fixed_dt),
+                                          float(self.tspan[1]), 1 if use_graph else 0))
+
+    def isfinished(self) -> bool:
+        # integrator.t ≈ last(tspan) (src/solvers/lwfr.jl:147-149): Julia isapprox, rtol = sqrt(eps)
+        te = self.tspan[1]
+        return abs(self.t - te) <= math.sqrt(np.finfo(float).eps) * max(abs(self.t), abs(te)) or self.t >= te
+
+
+def solve_lwfr(lw_update: LWUpdate, callbacks=(), dt_initial: float = 0.0, tolerances=None,
+               time_step_computation=None, limiters=(), chunk: int = 64, use_graph: bool = True) -> LWSolution:
+    """solve_lwfr(lw_update, callbacks, dt_initial, tolerances; time_step_computation) (lwfr.jl:233-263).
+
+    callbacks: objects with an ``interval`` (steps) called as ``cb(integrator, u)`` every interval steps
+    and at the end. Limiters are not built on the device path (none of the workloads use one)."""
+    if limiters:
+        raise NotImplementedError("limiters are not built on the device path")
+    if time_step_computation is None or isinstance(time_step_computation, Adaptive):
+        raise NotImplementedError("only CFLBased stepping is built on the device path")
+    assert isinstance(time_step_computation, CFLBased)
+    semi = lw_update.p
+    cfl = time_step_computation.cfl_number
+    integ = LWIntegrator(lw_update, tolerances)
+    u0 = lw_update.u0_ode
+    integ.set_state(u0, lw_update.tspan[0])
+    bc = semi.boundary_conditions
+    time_dependent_bc = semi.mesh.n_boundaries > 0 and not bc.time_independent
+    intervals = [int(cb.interval) for cb in callbacks if getattr(cb, "interval", 0)]
+    stride = min(intervals) if intervals else chunk
+    if not time_dependent_bc:
+        semi._prepare_boundaries(lw_update.tspan[0], 0.0, 1.0)
+    while not integ.isfinished():
+        if time_dependent_bc:
+            # exterior states depend on (t, dt): one step at a time with the dt read back
+            u = integ.get_state()
+            dt = semi.max_dt(u, cfl)
+            dt = min(dt, integ.tspan[1] - integ.t)
+            if semi.solver.volume_integral.time_discretization.code == _lib.TLW_MDRK:
+                raise NotImplementedError("MDRK with time-dependent Dirichlet data is not built")
+            semi._prepare_boundaries(integ.t, dt, 1.0)
+            integ.step(1, cfl, fixed_dt=dt, use_graph=False)
+        else:
+            integ.step(stride, cfl, use_graph=use_graph)
+        integ.sync_time()
+        for cb in callbacks:
+            if getattr(cb, "interval", 0) and integ.iter % int(cb.interval) == 0:
+                cb(integ, integ.get_state())
+    u = integ.get_state()
+    for cb in callbacks:
+        cb(integ, u)
+    return LWSolution([u], lw_update, [integ.t], integ.stats)
+
+
+def l2_linf_errors(semi: SemidiscretizationHyperbolic, u_ode: np.ndarray, t: float, exact=None):
+    """Per-variable L2 and Linf errors against ``exact`` (default: the initial condition at t), L2 by GLL
+    quadrature on the solution nodes: sqrt(sum_e sum_ij w_i w_j |J_e| (u - u_exact)^2 / |domain|)."""
+    exact = exact or semi.initial_condition
+    xy = semi.node_coordinates
+    ue = semi.compute_coefficients(t) if exact is semi.initial_condition else None
+    if ue is None:
+        v = exact(xy[0], xy[1], t, semi.equations)
+        ue = np.ascontiguousarray(np.transpose(v, (2, 1, 0, 3))).reshape(-1)
+    n = semi.nnodes
+    _, w = gauss_lobatto(semi.polydeg)
+    d = (u_ode - ue).reshape(semi.mesh.n_elements, n, n, 4)
+    jac = 1.0 / semi.mesh.inverse_jacobian          # |J| = h/2 per direction -> area factor jac^2
+    ww = (w[None, :, None] * w[None, None, :])      # [1, j, i]
+    l2 = np.sqrt(np.einsum("ejiv,eji->v", d * d, ww * (jac ** 2)[:, None, None]) / semi.mesh.length ** 2)
+    linf = np.abs(d).max(axis=(0, 1, 2))
+    return l2, linf

@@ -1,0 +1,303 @@
+"""Host-side mirror of the reference's semidiscretization API for the LW / MDRK rhs.
+
+Mirrors (names, argument meaning and error behaviour):
+  LW, MDRK                               src/basic_types.jl:4-6
+  CFLBased, Adaptive                     src/basic_types.jl:10-16
+  VolumeIntegralFR                       src/solvers/fr.jl:15-19
+  SemidiscretizationHyperbolic(...)      src/semidiscretization/semidiscretization_hyperbolic.jl:58-84
+  semidiscretize(semi, td, tspan)        src/semidiscretization/semidiscretization.jl:4-15
+  rhs!(du_ode, u_ode, semi, t, tol)      src/semidiscretization/semidiscretization_hyperbolic.jl:4-20
+  rhs_mdrk1!/rhs_mdrk2!                  src/semidiscretization/semidiscretization_hyperbolic.jl:22-56
+  trixi2lw / lw_fourier_cfl              src/auxiliary/auxiliary.jl:14-23
+
+Python cannot spell ``rhs!``; the functions are ``rhs``, ``rhs_mdrk1``, ``rhs_mdrk2``. dt is read from
+``semi.cache["dt"][0]`` exactly as the reference reads ``cache.dt[1]``. Every evaluation runs in libtlw
+on the GPU; a non-admissible state raises :class:`DomainError` as the reference's sqrt does.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import DomainError, check, lib
+from .basis import gauss_lobatto
+from .equations import CompressibleEulerEquations2D
+from .mesh import TreeMesh
+
+
+class LW:
+    """Lax-Wendroff time discretization."""
+    code = _lib.TLW_LW
+
+    def __repr__(self):
+        return "Lax-Wendroff"
+
+
+class MDRK:
+    """Two-stage multi-derivative Runge-Kutta time discretization."""
+    code = _lib.TLW_MDRK
+
+    def __repr__(self):
+        return "Multi-Derivative Runge-Kutta"
+
+
+@dataclass
+class CFLBased:
+    cfl_number: float
+
+
+class Adaptive:
+    """Error-controlled stepping (src/solvers/adaptive.jl). Not built on the device."""
+
+
+@dataclass
+class VolumeIntegralFR:
+    time_discretization: object = field(default_factory=LW)
+
+
+@dataclass
+class FluxLaxFriedrichs:
+    """flux_lax_friedrichs = FluxPlusDissipation(flux_central, DissipationLocalLaxFriedrichs(speed)).
+    max_abs_speed: "naive" (Trixi max_abs_speed_naive, the default of the reference's Trixi era) or
+    "davis" (Trixi max_abs_speed)."""
+    max_abs_speed: str = "naive"
+    code = _lib.TLW_FLUX_RUSANOV
+
+
+@dataclass
+class FluxHLL:
+    """FluxHLL(min_max_speed_naive) with the LW 8-argument method (src/equations/compressible_euler_2d.jl:24-40)."""
+    max_abs_speed: str = "naive"
+    code = _lib.TLW_FLUX_HLL
+
+
+flux_lax_friedrichs = FluxLaxFriedrichs()
+flux_hll = FluxHLL()
+
+
+@dataclass
+class DGSEM:
+    polydeg: int
+    surface_flux: object = field(default_factory=FluxLaxFriedrichs)
+    volume_integral: VolumeIntegralFR = field(default_factory=VolumeIntegralFR)
+
+
+def get_time_discretization(solver: DGSEM):
+    return solver.volume_integral.time_discretization
+
+
+class BoundaryConditionPeriodic:
+    pass
+
+
+boundary_condition_periodic = BoundaryConditionPeriodic()
+
+
+class BoundaryConditionDirichlet:
+    """Time-averaged Dirichlet condition (src/equations/equations.jl:6-37). ``boundary_value_function``
+    is called as f(x, y, t, equations) on arrays and returns conservative states [..., 4]."""
+
+    def __init__(self, boundary_value_function, time_independent=None):
+        self.boundary_value_function = boundary_value_function
+        if time_independent is None:
+            time_independent = bool(getattr(boundary_value_function, "time_independent", False))
+        self.time_independent = time_independent
+
+
+def lw_fourier_cfl(N: int) -> float:
+    """LW Fourier CFL limits for N = 1..4 (src/auxiliary/auxiliary.jl:14). N >= 5 is not tabulated by
+    the reference; callers must supply their own CFL there."""
+    table = (1.000, 0.333, 0.170, 0.103)
+    if not 1 <= N <= 4:
+        raise KeyError(f"lw_fourier_cfl undefined for N={N} (the reference tabulates N = 1..4)")
+    return table[N - 1]
+
+
+def trixi2lw(cfl_number: float, solver: DGSEM) -> float:
+    """src/auxiliary/auxiliary.jl:17-23: cfl * nnodes * lw_fourier_cfl(N)."""
+    N = solver.polydeg
+    return cfl_number * (N + 1) * lw_fourier_cfl(N)
+
+
+class _Handle:
+    def __init__(self, opts):
+        L = lib()
+        self.ptr = ctypes.c_void_p()
+        rc = L.tlw_create(ctypes.byref(opts), ctypes.byref(self.ptr))
+        if rc != 0:
+            raise _lib.TlwError(rc, "tlw_create failed (CUDA device unavailable or invalid options)")
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().tlw_destroy(self.ptr)
+                self.ptr = ctypes.c_void_p()
+        except Exception:
+            pass
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _i64p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+
+
+class SemidiscretizationHyperbolic:
+    """SemidiscretizationHyperbolic(mesh, time_discretization, equations, initial_condition, solver;
+    boundary_conditions=boundary_condition_periodic). Builds the libtlw handle and uploads the mesh."""
+
+    def __init__(self, mesh: TreeMesh, time_discretization, equations: CompressibleEulerEquations2D,
+                 initial_condition, solver: DGSEM, boundary_conditions=boundary_condition_periodic, device: int = 0,
+                 source_terms=None):
+        if source_terms is not None:
+            raise NotImplementedError("source terms are not built on the device path")
+        if not isinstance(mesh, TreeMesh):
+            raise NotImplementedError("only TreeMesh{2} is built")
+        self.mesh = mesh
+        self.equations = equations
+        self.initial_condition = initial_condition
+        self.solver = solver
+        self.time_discretization = time_discretization
+        self.polydeg = solver.polydeg
+        self.nnodes = solver.polydeg + 1
+        self.boundary_conditions = boundary_conditions
+        if mesh.n_boundaries > 0 and not isinstance(boundary_conditions, BoundaryConditionDirichlet):
+            raise ValueError("a non-periodic TreeMesh needs a BoundaryConditionDirichlet")
+        self.cache = {"dt": [math.nan]}
+        sf = solver.surface_flux
+        opts = _lib.TlwOpts()
+        opts.polydeg = solver.polydeg
+        opts.time_discretization = time_discretization.code
+        opts.surface_flux = sf.code
+        opts.max_speed = _lib.TLW_SPEED_DAVIS if getattr(sf, "max_abs_speed", "naive") == "davis" else _lib.TLW_SPEED_NAIVE
+        opts.gamma = equations.gamma
+        opts.device = device
+        self._handle = _Handle(opts)
+        self._upload_mesh()
+        self._bdata_key = None
+        self.node_coordinates = mesh.node_coordinates(self.polydeg)
+        if mesh.n_boundaries:
+            self._bnd_xy = mesh.boundary_node_coordinates(self.polydeg)
+
+    @property
+    def handle(self):
+        return self._handle.ptr
+
+    def _upload_mesh(self):
+        m = self.mesh
+        ij = np.ascontiguousarray(m.inverse_jacobian, dtype=np.float64)
+        nid = np.ascontiguousarray(m.interface_neighbor_ids, dtype=np.int64)
+        nor = np.ascontiguousarray(m.interface_orientations, dtype=np.int64)
+        bid = np.ascontiguousarray(m.boundary_neighbor_ids, dtype=np.int64)
+        bor = np.ascontiguousarray(m.boundary_orientations, dtype=np.int64)
+        bsi = np.ascontiguousarray(m.boundary_neighbor_sides, dtype=np.int64)
+        bpd = np.ascontiguousarray(m.n_boundaries_per_direction, dtype=np.int64)
+        self._keep = (ij, nid, nor, bid, bor, bsi, bpd)
+        rc = lib().tlw_set_tree_mesh(self.handle, m.n_elements, ij.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     m.n_interfaces, _i64p(nid), _i64p(nor), m.n_boundaries, _i64p(bid), _i64p(bor),
+                                     _i64p(bsi), _i64p(bpd))
+        check(self.handle, rc)
+
+    # ---- array helpers -----------------------------------------------------------------------------
+    def ndofs(self) -> int:
+        return self.mesh.ndofs(self.polydeg)
+
+    def wrap_array(self, u_ode: np.ndarray) -> np.ndarray:
+        """View of the flat state as [element, j, i, v] (the reference's u[v, i, j, element])."""
+        n = self.nnodes
+        return u_ode.reshape(self.mesh.n_elements, n, n, 4)
+
+    def compute_coefficients(self, t: float) -> np.ndarray:
+        xy = self.node_coordinates
+        u = self.initial_condition(xy[0], xy[1], t, self.equations)   # [i, j, E, 4]
+        return np.ascontiguousarray(np.transpose(u, (2, 1, 0, 3))).reshape(-1)
+
+    # ---- boundary data ------------------------------------------------------------------------------
+    def _prepare_boundaries(self, t: float, dt: float, scaling_factor: float):
+        if self.mesh.n_boundaries == 0:
+            return
+        bc = self.boundary_conditions
+        key = ("const", scaling_factor) if bc.time_independent else (t, dt, scaling_factor)
+        if key == self._bdata_key or (bc.time_independent and self._bdata_key is not None):
+            return
+        nodes, _ = gauss_lobatto(self.polydeg)
+        n = self.nnodes
+        x, y = self._bnd_xy[0], self._bnd_xy[1]        # [l, B]
+        dts = scaling_factor * dt
+        levels = np.empty((self.mesh.n_boundaries, n, n, 4))  # [B, l, q, v] == [v, q, l, B] column-major
+        for q in range(n):
+            ts = t + 0.5 * dts * (nodes[q] + 1.0) if bc.time_independent is False else t
+            levels[:, :, q, :] = np.transpose(bc.boundary_value_function(x, y, ts, self.equations), (1, 0, 2))
+        now = np.ascontiguousarray(np.transpose(bc.boundary_value_function(x, y, t, self.equations), (1, 0, 2)))
+        levels = np.ascontiguousarray(levels)
+        check(self.handle, lib().tlw_set_boundary_data(self.handle, _ptr(levels), _ptr(now), _lib.TLW_WHERE_HOST))
+        self._bdata_key = key
+
+    # ---- rhs entry points ---------------------------------------------------------------------------
+    def _rhs(self, stage: int, du_ode, u_ode, us_ode, t, dt):
+        where = _lib.TLW_WHERE_HOST
+        for a in (du_ode, u_ode) + ((us_ode,) if us_ode is not None else ()):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and a.size == 4 * self.ndofs()):
+                raise ValueError("state arrays must be contiguous float64 vectors of length 4*ndofs")
+        self._prepare_boundaries(t, dt, 0.5 if stage == _lib.TLW_STAGE_MDRK1 else 1.0)
+        rc = lib().tlw_rhs(self.handle, stage, _ptr(du_ode), _ptr(u_ode),
+                           _ptr(us_ode) if us_ode is not None else None, float(t), float(dt), where)
+        check(self.handle, rc)
+
+    def get_cache(self, item: int) -> np.ndarray:
+        L = lib()
+        size = L.tlw_cache_size(self.handle, item)
+        if size < 0:
+            raise ValueError("cache item not available")
+        out = np.empty(size)
+        check(self.handle, L.tlw_get_cache(self.handle, item, _ptr(out), _lib.TLW_WHERE_HOST))
+        return out
+
+    def max_dt(self, u_ode: np.ndarray, cfl: float) -> float:
+        dt = ctypes.c_double()
+        check(self.handle, lib().tlw_max_dt(self.handle, _ptr(u_ode), _lib.TLW_WHERE_HOST, float(cfl), ctypes.byref(dt)))
+        return dt.value
+
+
+def rhs(du_ode, u_ode, semi: SemidiscretizationHyperbolic, t, tolerances=None):
+    """rhs!(du_ode, u_ode, semi, t, tolerances) with dt = semi.cache["dt"][0]."""
+    semi._rhs(_lib.TLW_STAGE_LW, du_ode, u_ode, None, t, semi.cache["dt"][0])
+
+
+def rhs_mdrk1(du_ode, u_ode, semi: SemidiscretizationHyperbolic, t, tolerances=None):
+    """rhs_mdrk1!(du_ode, u_ode, semi, t): stage 1; keeps U2/F2 in the handle for stage 2."""
+    semi._rhs(_lib.TLW_STAGE_MDRK1, du_ode, u_ode, None, t, semi.cache["dt"][0])
+
+
+def rhs_mdrk2(du_ode, u_ode, semi: SemidiscretizationHyperbolic, t, us_ode, tolerances=None):
+    """rhs_mdrk2!(du_ode, u_ode, semi, t): stage 2 at the stage state ``us_ode`` (the reference reads it
+    from cache.element_cache.mdrk_cache.us, which perform_step! filled with uprev + dt*du)."""
+    semi._rhs(_lib.TLW_STAGE_MDRK2, du_ode, u_ode, us_ode, t, semi.cache["dt"][0])
+
+
+@dataclass
+class LWUpdate:
+    f: object
+    u0_ode: np.ndarray
+    du_ode: np.ndarray
+    tspan: tuple
+    p: SemidiscretizationHyperbolic
+
+
+def semidiscretize(semi: SemidiscretizationHyperbolic, time_discretization, tspan) -> LWUpdate:
+    u0 = semi.compute_coefficients(tspan[0])
+    return LWUpdate(rhs, u0, np.empty_like(u0), (float(tspan[0]), float(tspan[1])), semi)
+
+
+__all__ = [
+    "LW", "MDRK", "CFLBased", "Adaptive", "VolumeIntegralFR", "DGSEM", "FluxLaxFriedrichs", "FluxHLL",
+    "flux_lax_friedrichs", "flux_hll", "BoundaryConditionDirichlet", "boundary_condition_periodic",
+    "SemidiscretizationHyperbolic", "semidiscretize", "rhs", "rhs_mdrk1", "rhs_mdrk2", "lw_fourier_cfl",
+    "trixi2lw", "get_time_discretization", "DomainError", "LWUpdate",
+]
