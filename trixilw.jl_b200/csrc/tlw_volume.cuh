@@ -1,7 +1,7 @@
 // tlw_volume.cuh -- fused per-element LW / MDRK volume kernels for TreeMesh{2} (FP64, sm_100a).
 //
-// One thread per GLL node; EB whole elements per CTA so that every CTA runs full warps (N=3: 8 x 16,
-// N=4: 5 x 25 (+3 idle lanes), N=5: 8 x 36 nodes). The 1-D derivative contractions read the stage fluxes
+// One thread per GLL node; EB whole elements per CTA so that every CTA runs (nearly) full warps (N=3: 8 x 16,
+// N=4: 5 x 25 (+3 idle lanes), N=5: 7 x 36 (+4 idle lanes) nodes). The 1-D derivative contractions read the stage fluxes
 // of the element from shared memory (tiles of double2: (f0,f1) (f2,f3) (g0,g1) (g2,g3) per node, a
 // layout with no bank conflicts for the row and column reads). All other LW stage state (perturbed
 // states u+-ut, u+-2ut, the time averages U, F, G) lives in registers. HBM traffic per element: read u
@@ -23,11 +23,19 @@ template <int N>
 struct VolCfg {
     static constexpr int n = N + 1;
     static constexpr int nn = n * n;
-    static constexpr int EB = N == 1 ? 32 : N == 2 ? 14 : N == 3 ? 8 : N == 4 ? 5 : N == 5 ? 8 : N == 6 ? 5 : 2;
+    // whole elements per CTA, chosen so that the CTA is (nearly) full warps
+    static constexpr int EB = N == 1 ? 32 : N == 2 ? 14 : N == 3 ? 8 : N == 4 ? 5 : N == 5 ? 7 : N == 6 ? 5 : 2;
     static constexpr int THREADS = ((EB * nn + 31) / 32) * 32;
+    // resident CTAs per SM the register allocation must allow (<= 128 registers per thread)
+    static constexpr int MIN_BLOCKS = THREADS <= 128 ? 4 : 2;
+    // the MDRK stage kernels hold fewer values per thread: ask for more resident CTAs
+    static constexpr int MDRK_MIN_BLOCKS = THREADS <= 128 ? 6 : 3;
     static constexpr int TILE = EB * nn;   // double2 entries per tile array
-    // shared memory: Dm, Dhat (2 nn doubles) + NT tiles of 4 double2 arrays
-    static constexpr size_t smem_bytes(int ntiles) { return 2 * nn * sizeof(double) + (size_t)ntiles * 4 * TILE * sizeof(double2); }
+    // shared memory: 4 stage matrices + Dhat (5 nn doubles, padded to 16 B) + NT tiles of 4 double2 arrays
+    static constexpr int MAT_D2 = (5 * nn + 1) / 2;
+    static constexpr size_t smem_bytes(int ntiles) {
+        return (size_t)MAT_D2 * sizeof(double2) + (size_t)ntiles * 4 * TILE * sizeof(double2);
+    }
 };
 
 enum VolMode { MODE_RHS = 0, MODE_STEP = 1 };
@@ -112,22 +120,36 @@ __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, 
 
 // ------------------------------------------------------------------------------------------------
 // Plain LW volume kernel (depth = min(N, 4)).
+// The finite-difference stencils are accumulated unscaled ("raw") and their constant factors are folded
+// into the matrices of the next contraction and into the F/G update coefficients:
+//   depth 4: f_t = raw1/12, f_tt = raw2/12, f_ttt = raw3/2, f_tttt = raw4/2
+//   depth 3: f_t = raw1/12, f_tt = raw2,    f_ttt = raw3/2
+//   depth 2: f_t = raw1/2,  f_tt = raw2;    depth 1: f_t = raw1/2
+// Shared memory holds M_k = -dt c_k D for the contraction of stage k's output (c_0 = 1) and Dhat.
 // ------------------------------------------------------------------------------------------------
 template <int N, int MODE>
-__global__ void __launch_bounds__(VolCfg<N>::THREADS) lw_volume_kernel(VolArgs a) {
+__global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB, TILE = C::TILE;
     constexpr int DEPTH = N >= 4 ? 4 : N;
+    constexpr double C1 = DEPTH >= 3 ? 1.0 / 12.0 : 0.5;
+    constexpr double C2 = DEPTH == 4 ? 1.0 / 12.0 : 1.0;
+    constexpr double C3 = 0.5;
+    constexpr double C4 = 0.5;
     extern __shared__ double2 smem[];
-    double* sDm = reinterpret_cast<double*>(smem);   // -dt * D
-    double* sDh = sDm + nn;                          // Dhat
-    double2* tiles = smem + nn;
+    double* sM = reinterpret_cast<double*>(smem);   // [4][nn]: -dt D, -dt C1 D, -dt C2 D, -dt C3 D
+    double* sDh = sM + 4 * nn;                      // Dhat
+    double2* tiles = smem + C::MAT_D2;
 
     const int tid = threadIdx.x;
     const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
     for (int k = tid; k < nn; k += blockDim.x) {
-        sDm[k] = -dt * a.basis->D[k];
+        const double d = -dt * a.basis->D[k];
+        sM[k] = d;
+        sM[nn + k] = d * C1;
+        sM[2 * nn + k] = d * C2;
+        sM[3 * nn + k] = d * C3;
         sDh[k] = a.basis->Dhat[k];
     }
     const int el = tid / nn;
@@ -157,9 +179,8 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS) lw_volume_kernel(VolArgs a
 
     // stage 1: ut; perturbed states; f_t (dg_2d.jl:972-1023 / :725-775 / :543-582 / :417-454)
     if (active) {
-        double d[NV];
-        contract<n, TILE>(tiles, 0, sDm, base, i, j, d);
-        double ft[NV] = {0, 0, 0, 0}, gt[NV] = {0, 0, 0, 0}, f[NV], g[NV];
+        double d[NV], r[NV], q[NV], f[NV], g[NV];
+        contract<n, TILE>(tiles, 0, sM, base, i, j, d);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             d[v] *= ij;
@@ -169,36 +190,38 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS) lw_volume_kernel(VolArgs a
             if (DEPTH >= 3) { upp[v] = fma(2.0, d[v], upp[v]); umm[v] = fma(-2.0, d[v], umm[v]); }
         }
         if (DEPTH >= 3) {
+            // raw1 = -f(u+2ut) + 8 f(u+ut) - 8 f(u-ut) + f(u-2ut)
             euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { ft[v] = -f[v]; gt[v] = -g[v]; }
+            for (int v = 0; v < NV; ++v) { r[v] = -f[v]; q[v] = -g[v]; }
             euler_fluxes(gm1, up[0], up[1], up[2], up[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { ft[v] = fma(8.0, f[v], ft[v]); gt[v] = fma(8.0, g[v], gt[v]); }
+            for (int v = 0; v < NV; ++v) { r[v] = fma(8.0, f[v], r[v]); q[v] = fma(8.0, g[v], q[v]); }
             euler_fluxes(gm1, um[0], um[1], um[2], um[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { ft[v] = fma(-8.0, f[v], ft[v]); gt[v] = fma(-8.0, g[v], gt[v]); }
+            for (int v = 0; v < NV; ++v) { r[v] = fma(-8.0, f[v], r[v]); q[v] = fma(-8.0, g[v], q[v]); }
             euler_fluxes(gm1, umm[0], umm[1], umm[2], umm[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { ft[v] = (ft[v] + f[v]) * (1.0 / 12.0); gt[v] = (gt[v] + g[v]) * (1.0 / 12.0); }
+            for (int v = 0; v < NV; ++v) { r[v] += f[v]; q[v] += g[v]; }
         } else {
+            // raw1 = f(u+ut) - f(u-ut)
             euler_fluxes(gm1, up[0], up[1], up[2], up[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { ft[v] = 0.5 * f[v]; gt[v] = 0.5 * g[v]; }
+            for (int v = 0; v < NV; ++v) { r[v] = f[v]; q[v] = g[v]; }
             euler_fluxes(gm1, um[0], um[1], um[2], um[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { ft[v] = fma(-0.5, f[v], ft[v]); gt[v] = fma(-0.5, g[v], gt[v]); }
+            for (int v = 0; v < NV; ++v) { r[v] -= f[v]; q[v] -= g[v]; }
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) { F[v] = fma(0.5, ft[v], F[v]); G[v] = fma(0.5, gt[v], G[v]); }
-        if (DEPTH >= 2) tile_put<TILE>(tiles, 1, slot, ft, gt);
+        for (int v = 0; v < NV; ++v) { F[v] = fma(0.5 * C1, r[v], F[v]); G[v] = fma(0.5 * C1, q[v], G[v]); }
+        if (DEPTH >= 2) tile_put<TILE>(tiles, 1, slot, r, q);
     }
     if (DEPTH >= 2) {
         __syncthreads();
         // stage 2: utt; f_tt (dg_2d.jl:1025-1083 / :777-831 / :597-634)
         if (active) {
-            double d[NV], f0[NV], g0[NV], ftt[NV], gtt[NV], f[NV], g[NV];
-            contract<n, TILE>(tiles, 1, sDm, base, i, j, d);
+            double d[NV], f0[NV], g0[NV], r[NV], q[NV], f[NV], g[NV];
+            contract<n, TILE>(tiles, 1, sM + nn, base, i, j, d);
             tile_get<TILE>(tiles, 0, slot, f0, g0);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
@@ -209,40 +232,45 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS) lw_volume_kernel(VolArgs a
                 if (DEPTH >= 3) { upp[v] = fma(2.0, d[v], upp[v]); umm[v] = fma(2.0, d[v], umm[v]); }
             }
             if (DEPTH == 4) {
+                // raw2 = -f(upp) + 16 f(up) - 30 f0 + 16 f(um) - f(umm)
                 euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
 #pragma unroll
-                for (int v = 0; v < NV; ++v) { ftt[v] = -f[v]; gtt[v] = -g[v]; }
+                for (int v = 0; v < NV; ++v) {
+                    r[v] = fma(-30.0, f0[v], -f[v]);
+                    q[v] = fma(-30.0, g0[v], -g[v]);
+                }
                 euler_fluxes(gm1, up[0], up[1], up[2], up[3], f, g);
 #pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    ftt[v] = fma(16.0, f[v], ftt[v]); gtt[v] = fma(16.0, g[v], gtt[v]);
-                    ftt[v] = fma(-30.0, f0[v], ftt[v]); gtt[v] = fma(-30.0, g0[v], gtt[v]);
-                }
+                for (int v = 0; v < NV; ++v) { r[v] = fma(16.0, f[v], r[v]); q[v] = fma(16.0, g[v], q[v]); }
                 euler_fluxes(gm1, um[0], um[1], um[2], um[3], f, g);
 #pragma unroll
-                for (int v = 0; v < NV; ++v) { ftt[v] = fma(16.0, f[v], ftt[v]); gtt[v] = fma(16.0, g[v], gtt[v]); }
+                for (int v = 0; v < NV; ++v) { r[v] = fma(16.0, f[v], r[v]); q[v] = fma(16.0, g[v], q[v]); }
                 euler_fluxes(gm1, umm[0], umm[1], umm[2], umm[3], f, g);
 #pragma unroll
-                for (int v = 0; v < NV; ++v) { ftt[v] = (ftt[v] - f[v]) * (1.0 / 12.0); gtt[v] = (gtt[v] - g[v]) * (1.0 / 12.0); }
+                for (int v = 0; v < NV; ++v) { r[v] -= f[v]; q[v] -= g[v]; }
             } else {
+                // raw2 = f(up) - 2 f0 + f(um)
                 euler_fluxes(gm1, up[0], up[1], up[2], up[3], f, g);
 #pragma unroll
-                for (int v = 0; v < NV; ++v) { ftt[v] = fma(-2.0, f0[v], f[v]); gtt[v] = fma(-2.0, g0[v], g[v]); }
+                for (int v = 0; v < NV; ++v) { r[v] = fma(-2.0, f0[v], f[v]); q[v] = fma(-2.0, g0[v], g[v]); }
                 euler_fluxes(gm1, um[0], um[1], um[2], um[3], f, g);
 #pragma unroll
-                for (int v = 0; v < NV; ++v) { ftt[v] += f[v]; gtt[v] += g[v]; }
+                for (int v = 0; v < NV; ++v) { r[v] += f[v]; q[v] += g[v]; }
             }
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { F[v] = fma(1.0 / 6.0, ftt[v], F[v]); G[v] = fma(1.0 / 6.0, gtt[v], G[v]); }
-            if (DEPTH >= 3) tile_put<TILE>(tiles, 2, slot, ftt, gtt);
+            for (int v = 0; v < NV; ++v) {
+                F[v] = fma(C2 / 6.0, r[v], F[v]);
+                G[v] = fma(C2 / 6.0, q[v], G[v]);
+            }
+            if (DEPTH >= 3) tile_put<TILE>(tiles, 2, slot, r, q);
         }
     }
     if (DEPTH >= 3) {
         __syncthreads();
         // stage 3: uttt; f_ttt (dg_2d.jl:1085-1138 / :833-875)
         if (active) {
-            double d[NV], fttt[NV], gttt[NV], f[NV], g[NV];
-            contract<n, TILE>(tiles, 2, sDm, base, i, j, d);
+            double d[NV], r[NV], q[NV], f[NV], g[NV];
+            contract<n, TILE>(tiles, 2, sM + 2 * nn, base, i, j, d);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 d[v] *= ij;
@@ -252,32 +280,33 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS) lw_volume_kernel(VolArgs a
                 umm[v] = fma(-4.0 / 3.0, d[v], umm[v]);
                 upp[v] = fma(4.0 / 3.0, d[v], upp[v]);
             }
+            // raw3 = f(upp) - 2 f(up) + 2 f(um) - f(umm)
             euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { fttt[v] = f[v]; gttt[v] = g[v]; }
+            for (int v = 0; v < NV; ++v) { r[v] = f[v]; q[v] = g[v]; }
             euler_fluxes(gm1, up[0], up[1], up[2], up[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { fttt[v] = fma(-2.0, f[v], fttt[v]); gttt[v] = fma(-2.0, g[v], gttt[v]); }
+            for (int v = 0; v < NV; ++v) { r[v] = fma(-2.0, f[v], r[v]); q[v] = fma(-2.0, g[v], q[v]); }
             euler_fluxes(gm1, um[0], um[1], um[2], um[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { fttt[v] = fma(2.0, f[v], fttt[v]); gttt[v] = fma(2.0, g[v], gttt[v]); }
+            for (int v = 0; v < NV; ++v) { r[v] = fma(2.0, f[v], r[v]); q[v] = fma(2.0, g[v], q[v]); }
             euler_fluxes(gm1, umm[0], umm[1], umm[2], umm[3], f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                fttt[v] = 0.5 * (fttt[v] - f[v]);
-                gttt[v] = 0.5 * (gttt[v] - g[v]);
-                F[v] = fma(1.0 / 24.0, fttt[v], F[v]);
-                G[v] = fma(1.0 / 24.0, gttt[v], G[v]);
+                r[v] -= f[v];
+                q[v] -= g[v];
+                F[v] = fma(C3 / 24.0, r[v], F[v]);
+                G[v] = fma(C3 / 24.0, q[v], G[v]);
             }
-            if (DEPTH >= 4) tile_put<TILE>(tiles, 1, slot, fttt, gttt);
+            if (DEPTH >= 4) tile_put<TILE>(tiles, 1, slot, r, q);
         }
     }
     if (DEPTH >= 4) {
         __syncthreads();
         // stage 4: utttt; f_tttt (dg_2d.jl:1140-1206)
         if (active) {
-            double d[NV], f0[NV], g0[NV], f4[NV], g4[NV], f[NV], g[NV];
-            contract<n, TILE>(tiles, 1, sDm, base, i, j, d);
+            double d[NV], f0[NV], g0[NV], r[NV], q[NV], f[NV], g[NV];
+            contract<n, TILE>(tiles, 1, sM + 3 * nn, base, i, j, d);
             tile_get<TILE>(tiles, 0, slot, f0, g0);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
@@ -288,29 +317,34 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS) lw_volume_kernel(VolArgs a
                 umm[v] = fma(2.0 / 3.0, d[v], umm[v]);
                 upp[v] = fma(2.0 / 3.0, d[v], upp[v]);
             }
+            // raw4 = f(upp) - 4 f(up) + 6 f0 - 4 f(um) + f(umm)
             euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { f4[v] = fma(6.0, f0[v], f[v]); g4[v] = fma(6.0, g0[v], g[v]); }
+            for (int v = 0; v < NV; ++v) { r[v] = fma(6.0, f0[v], f[v]); q[v] = fma(6.0, g0[v], g[v]); }
             euler_fluxes(gm1, up[0], up[1], up[2], up[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { f4[v] = fma(-4.0, f[v], f4[v]); g4[v] = fma(-4.0, g[v], g4[v]); }
+            for (int v = 0; v < NV; ++v) { r[v] = fma(-4.0, f[v], r[v]); q[v] = fma(-4.0, g[v], q[v]); }
             euler_fluxes(gm1, um[0], um[1], um[2], um[3], f, g);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { f4[v] = fma(-4.0, f[v], f4[v]); g4[v] = fma(-4.0, g[v], g4[v]); }
+            for (int v = 0; v < NV; ++v) { r[v] = fma(-4.0, f[v], r[v]); q[v] = fma(-4.0, g[v], q[v]); }
             euler_fluxes(gm1, umm[0], umm[1], umm[2], umm[3], f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                f4[v] = 0.5 * (f4[v] + f[v]);
-                g4[v] = 0.5 * (g4[v] + g[v]);
-                F[v] = fma(1.0 / 120.0, f4[v], F[v]);
-                G[v] = fma(1.0 / 120.0, g4[v], G[v]);
+                r[v] += f[v];
+                q[v] += g[v];
+                F[v] = fma(C4 / 120.0, r[v], F[v]);
+                G[v] = fma(C4 / 120.0, q[v], G[v]);
             }
+            // tile 2 was last read by the stage-3 contraction, before the barrier above
+            tile_put<TILE>(tiles, 2, slot, F, G);
         }
     }
-    // final: Dhat contraction of the time-averaged fluxes (tile 2 is free for every depth here)
-    constexpr int TF = DEPTH >= 3 ? (DEPTH == 3 ? 1 : 2) : (DEPTH == 2 ? 2 : 1);
-    __syncthreads();
-    if (active) tile_put<TILE>(tiles, TF, slot, F, G);
+    // final: Dhat contraction of the time-averaged fluxes
+    constexpr int TF = DEPTH == 4 ? 2 : DEPTH == 3 ? 1 : DEPTH == 2 ? 2 : 1;
+    if (DEPTH < 4) {
+        __syncthreads();
+        if (active) tile_put<TILE>(tiles, TF, slot, F, G);
+    }
     __syncthreads();
     if (active) {
         double acc[NV];
@@ -324,13 +358,13 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS) lw_volume_kernel(VolArgs a
 // F2 = f + f_t/6, U2 = u + u_t/6 (stored whole for stage 2).
 // ------------------------------------------------------------------------------------------------
 template <int N, int MODE>
-__global__ void __launch_bounds__(VolCfg<N>::THREADS) mdrk1_volume_kernel(VolArgs a) {
+__global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk1_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB, TILE = C::TILE;
     extern __shared__ double2 smem[];
     double* sDm = reinterpret_cast<double*>(smem);
-    double* sDh = sDm + nn;
-    double2* tiles = smem + nn;
+    double* sDh = sDm + 4 * nn;
+    double2* tiles = smem + C::MAT_D2;
     const int tid = threadIdx.x;
     const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
@@ -403,13 +437,13 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS) mdrk1_volume_kernel(VolArg
 // F = F2 + f_t(u*)/3, U = U2 + u*_t/3.
 // ------------------------------------------------------------------------------------------------
 template <int N, int MODE>
-__global__ void __launch_bounds__(VolCfg<N>::THREADS) mdrk2_volume_kernel(VolArgs a) {
+__global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk2_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB, TILE = C::TILE;
     extern __shared__ double2 smem[];
     double* sDm = reinterpret_cast<double*>(smem);
-    double* sDh = sDm + nn;
-    double2* tiles = smem + nn;
+    double* sDh = sDm + 4 * nn;
+    double2* tiles = smem + C::MAT_D2;
     const int tid = threadIdx.x;
     const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
