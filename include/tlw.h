@@ -131,6 +131,23 @@ int tlw_get_stream(tlw_handle* h, void** stream);
 int tlw_state_pointer(tlw_handle* h, double** dptr);
 const char* tlw_last_error(tlw_handle* h);
 
+/* LW rhs for callers that must not allocate device memory (no counterpart in the reference: the
+ * reference's Julia rhs! allocates nothing per call because its caches are built once; this entry point
+ * gives a caller whose device memory is owned by another pool, or who cannot accept cudaMalloc's implicit
+ * synchronisation, the same rhs without a handle). Periodic TreeMesh{2} only (no boundaries, no mortars).
+ * All pointers are device pointers, 16-byte aligned: u, du [v, i, j, element]; inverse_jacobian
+ * [element]; x_left/x_right, y_left/y_right the 0-based element ids of the x- and y-oriented interfaces.
+ * The face-trace scratch is a static device array of TLW_NOALLOC_SCRATCH_BYTES: meshes with
+ * n_elements * 2 * 4 * (N+1) * 4 * 8 bytes of traces beyond it are rejected with TLW_E_ARG. Calls share
+ * that array, so calls that overlap on the GPU race. The first call on a device sets the device up
+ * (make it before any stream capture). Runs on `stream` (a cudaStream_t, 0 = default) and returns
+ * after the result is in du: TLW_OK, TLW_E_NONADMISSIBLE (DomainError), TLW_E_ARG or TLW_E_CUDA. */
+#define TLW_NOALLOC_SCRATCH_BYTES (32u << 20)
+int tlw_rhs_lw_noalloc(int32_t polydeg, double gamma, int32_t surface_flux, int32_t max_speed, int64_t n_elements,
+                       const double* inverse_jacobian, int32_t n_x_interfaces, const int32_t* x_left,
+                       const int32_t* x_right, int32_t n_y_interfaces, const int32_t* y_left,
+                       const int32_t* y_right, const double* u, double* du, double dt, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

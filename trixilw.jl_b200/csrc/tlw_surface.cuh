@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(256) max_speed_kernel(const double* __restrict
 
 // dt = cfl * 2 / (n * max_scaled_speed), clamped so that t + dt <= t_end; a finished run gets dt = 0
 // (the remaining launches of a captured step are then exact no-ops on the state).
-__global__ void finalize_dt_kernel(StepState* s, int n) {
+static __global__ void finalize_dt_kernel(StepState* s, int n) {
     double maxs = __longlong_as_double((long long)s->max_bits);
     const double tiny = 4.9406564584124654e-324;   // nextfloat(0.0)
     if (!(maxs > tiny)) maxs = tiny;
