@@ -10,75 +10,13 @@
 #include <vector>
 
 #include "../../include/tlw.h"
+#include "tlw_basis.h"
 #include "tlw_surface.cuh"
 #include "tlw_volume.cuh"
 
 using namespace tlw;
 
 namespace {
-
-// Gauss-Lobatto-Legendre basis on the host (Kopriva, "Implementing Spectral Methods for PDEs": Legendre
-// recursion Alg. 22/24, nodes/weights Alg. 25, barycentric weights Alg. 30, derivative matrix Alg. 37);
-// Dhat = -M^{-1} D^T M and the weak-form lift factors 1/w_1, 1/w_n as Trixi's LobattoLegendreBasis.
-void legendre_q(int N, double x, double& q, double& dq, double& LN) {
-    double a = 1.0, b = x, da = 0.0, db = 1.0;
-    for (int k = 2; k <= N; ++k) {
-        const double c = ((2.0 * k - 1.0) * x * b - (k - 1.0) * a) / k;
-        const double dc = da + (2.0 * k - 1.0) * b;
-        a = b; b = c; da = db; db = dc;
-    }
-    const int k = N + 1;
-    const double c = ((2.0 * k - 1.0) * x * b - (k - 1.0) * a) / k;
-    const double dc = da + (2.0 * k - 1.0) * b;
-    q = c - a;
-    dq = dc - da;
-    LN = b;
-}
-
-void build_basis(int N, tlw::Basis& B, std::vector<double>& nodes) {
-    const int n = N + 1;
-    std::vector<double> x(n), w(n), wb(n, 1.0);
-    x[0] = -1.0; x[N] = 1.0;
-    w[0] = w[N] = 2.0 / (N * (N + 1.0));
-    const double pi = 3.14159265358979323846;
-    for (int j = 1; j <= (N + 1) / 2 - 1; ++j) {
-        double xj = -std::cos((j + 0.25) * pi / N - 3.0 / (8.0 * N * pi * (j + 0.25)));
-        double q, dq, LN;
-        for (int it = 0; it < 100; ++it) {
-            legendre_q(N, xj, q, dq, LN);
-            const double d = -q / dq;
-            xj += d;
-            if (std::fabs(d) <= 4.0 * 2.220446049250313e-16 * std::fabs(xj)) break;
-        }
-        legendre_q(N, xj, q, dq, LN);
-        x[j] = xj; x[N - j] = -xj;
-        w[j] = w[N - j] = 2.0 / (N * (N + 1.0) * LN * LN);
-    }
-    if (N >= 2 && N % 2 == 0) {
-        double q, dq, LN;
-        legendre_q(N, 0.0, q, dq, LN);
-        x[N / 2] = 0.0;
-        w[N / 2] = 2.0 / (N * (N + 1.0) * LN * LN);
-    }
-    for (int j = 0; j < n; ++j) {
-        for (int k = 0; k < n; ++k)
-            if (k != j) wb[j] *= (x[j] - x[k]);
-        wb[j] = 1.0 / wb[j];
-    }
-    std::memset(&B, 0, sizeof(B));
-    for (int r = 0; r < n; ++r)
-        for (int c = 0; c < n; ++c)
-            if (c != r) {
-                B.D[r * n + c] = wb[c] / wb[r] / (x[r] - x[c]);
-                B.D[r * n + r] -= B.D[r * n + c];
-            }
-    for (int r = 0; r < n; ++r)
-        for (int c = 0; c < n; ++c) B.Dhat[r * n + c] = -B.D[c * n + r] * w[c] / w[r];
-    for (int k = 0; k < n; ++k) B.weights[k] = w[k];
-    B.inv_w_first = 1.0 / w[0];
-    B.inv_w_last = 1.0 / w[n - 1];
-    nodes = x;
-}
 
 template <class T>
 void dfree(T*& p) {
@@ -163,8 +101,8 @@ template <int N>
 struct Launch {
     using C = VolCfg<N>;
     static void set_attributes() {
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(3));
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(3));
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(4));
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(4));
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
@@ -174,8 +112,8 @@ struct Launch {
         const int grid = (int)((a.E + C::EB - 1) / C::EB);
         if (grid == 0) return;
         if (stage == TLW_STAGE_LW) {
-            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(3), s>>>(a);
-            else lw_volume_kernel<N, MODE_STEP><<<grid, C::THREADS, C::smem_bytes(3), s>>>(a);
+            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
+            else lw_volume_kernel<N, MODE_STEP><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
         } else if (stage == TLW_STAGE_MDRK1) {
             if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(2), s>>>(a);
             else mdrk1_volume_kernel<N, MODE_STEP><<<grid, C::THREADS, C::smem_bytes(2), s>>>(a);
@@ -374,7 +312,7 @@ int tlw_create(const tlw_opts* opts, tlw_handle** out) {
     h->n = h->N + 1;
     h->nn = h->n * h->n;
     h->device = opts->device;
-    build_basis(h->N, h->h_basis, h->nodes);
+    host_build_basis(h->N, h->h_basis, &h->nodes);
     int rc = TLW_OK;
     do {
         if (cudaSetDevice(h->device) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "cudaSetDevice failed"); break; }
@@ -386,6 +324,10 @@ int tlw_create(const tlw_opts* opts, tlw_handle** out) {
         st.cfl = 1.0;
         st.t_end = INFINITY;
         if (cudaMemcpy(h->d_step, &st, sizeof(st), cudaMemcpyHostToDevice) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "init step"); break; }
+        tlw::Basis all[8];
+        std::memset(&all[0], 0, sizeof(all[0]));
+        for (int N = 1; N <= 7; ++N) host_build_basis(N, all[N]);
+        if (upload_const_basis(all) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "constant basis"); break; }
         dispatch<SetAttr>(h->N);
         if (cudaGetLastError() != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "kernel attributes"); break; }
     } while (0);
@@ -619,6 +561,9 @@ int tlw_step(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double 
         if (e2 != cudaSuccess) { exec = nullptr; return fail(h, TLW_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2)); }
         return TLW_OK;
     };
+    // capture every variant on first use, so that no capture/instantiation lands inside a later call
+    if ((rc = capture(0, 1, h->g_one[0])) || (rc = capture(1, 1, h->g_one[1])) || (rc = capture(0, 2, h->g_two[0])))
+        return rc;
     int left = nsteps;
     if (h->cur == 1) {
         if ((rc = capture(1, 1, h->g_one[1]))) return rc;

@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "../../include/tlw.h"
+#include "tlw_basis.h"
 #include "tlw_surface.cuh"
 #include "tlw_volume.cuh"
 
@@ -55,66 +56,10 @@ struct DeviceSetup {
 DeviceSetup g_setup[kMaxDevices];
 std::mutex g_setup_mutex;
 
-// GLL basis for degree N on the host (Kopriva, Alg. 24/25/30/37), as in the handle-based path
-void host_basis(int N, tlw::Basis& B) {
-    const int n = N + 1;
-    auto q_and_l = [N](double x, double& q, double& dq, double& LN) {
-        double a = 1.0, b = x, da = 0.0, db = 1.0;
-        for (int k = 2; k <= N; ++k) {
-            const double c = ((2.0 * k - 1.0) * x * b - (k - 1.0) * a) / k;
-            const double dc = da + (2.0 * k - 1.0) * b;
-            a = b; b = c; da = db; db = dc;
-        }
-        const int k = N + 1;
-        const double c = ((2.0 * k - 1.0) * x * b - (k - 1.0) * a) / k;
-        const double dc = da + (2.0 * k - 1.0) * b;
-        q = c - a; dq = dc - da; LN = b;
-    };
-    std::vector<double> x(n), w(n), wb(n, 1.0);
-    x[0] = -1.0; x[N] = 1.0;
-    w[0] = w[N] = 2.0 / (N * (N + 1.0));
-    for (int j = 1; j <= (N + 1) / 2 - 1; ++j) {
-        double xj = -std::cos((j + 0.25) * 3.14159265358979323846 / N - 3.0 / (8.0 * N * 3.14159265358979323846 * (j + 0.25)));
-        double q, dq, LN;
-        for (int it = 0; it < 100; ++it) {
-            q_and_l(xj, q, dq, LN);
-            const double d = -q / dq;
-            xj += d;
-            if (std::fabs(d) <= 4.0 * 2.220446049250313e-16 * std::fabs(xj)) break;
-        }
-        q_and_l(xj, q, dq, LN);
-        x[j] = xj; x[N - j] = -xj;
-        w[j] = w[N - j] = 2.0 / (N * (N + 1.0) * LN * LN);
-    }
-    if (N >= 2 && N % 2 == 0) {
-        double q, dq, LN;
-        q_and_l(0.0, q, dq, LN);
-        x[N / 2] = 0.0;
-        w[N / 2] = 2.0 / (N * (N + 1.0) * LN * LN);
-    }
-    for (int j = 0; j < n; ++j) {
-        for (int k = 0; k < n; ++k)
-            if (k != j) wb[j] *= (x[j] - x[k]);
-        wb[j] = 1.0 / wb[j];
-    }
-    std::memset(&B, 0, sizeof(B));
-    for (int r = 0; r < n; ++r)
-        for (int c = 0; c < n; ++c)
-            if (c != r) {
-                B.D[r * n + c] = wb[c] / wb[r] / (x[r] - x[c]);
-                B.D[r * n + r] -= B.D[r * n + c];
-            }
-    for (int r = 0; r < n; ++r)
-        for (int c = 0; c < n; ++c) B.Dhat[r * n + c] = -B.D[c * n + r] * w[c] / w[r];
-    for (int k = 0; k < n; ++k) B.weights[k] = w[k];
-    B.inv_w_first = 1.0 / w[0];
-    B.inv_w_last = 1.0 / w[n - 1];
-}
-
 template <int N>
 void set_attributes() {
     using C = VolCfg<N>;
-    cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(3));
+    cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(4));
 }
 
 // once per device, with that device current: symbol addresses (checked), bases, kernel attributes
@@ -127,9 +72,10 @@ int setup_device(int dev) {
     if (cudaGetSymbolAddress((void**)&s.dt, g_noalloc_dt) != cudaSuccess) return TLW_E_CUDA;
     if (cudaGetSymbolAddress((void**)&s.status, g_noalloc_status) != cudaSuccess) return TLW_E_CUDA;
     tlw::Basis hb[8];
-    for (int N = 1; N <= 7; ++N) host_basis(N, hb[N]);
+    for (int N = 1; N <= 7; ++N) host_build_basis(N, hb[N]);
     std::memset(&hb[0], 0, sizeof(hb[0]));
     if (cudaMemcpyToSymbol(g_noalloc_basis, hb, sizeof(hb)) != cudaSuccess) return TLW_E_CUDA;
+    if (upload_const_basis(hb) != cudaSuccess) return TLW_E_CUDA;   // this file's constant-memory matrices
     set_attributes<1>(); set_attributes<2>(); set_attributes<3>(); set_attributes<4>();
     set_attributes<5>(); set_attributes<6>(); set_attributes<7>();
     if (cudaGetLastError() != cudaSuccess) return TLW_E_CUDA;
@@ -142,7 +88,7 @@ void launch(cudaStream_t st, const VolArgs& va, SurfArgs sa, int nx, const int* 
             const int* yl, const int* yr) {
     using C = VolCfg<N>;
     const int grid = (int)((va.E + C::EB - 1) / C::EB);
-    lw_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(3), st>>>(va);
+    lw_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(4), st>>>(va);
     sa.left = xl; sa.right = xr; sa.count = nx; sa.orientation = 1;
     if (nx > 0) interface_kernel<N><<<(unsigned)(((long long)nx * (N + 1) + 127) / 128), 128, 0, st>>>(sa);
     sa.left = yl; sa.right = yr; sa.count = ny; sa.orientation = 2;
@@ -198,7 +144,7 @@ extern "C" int tlw_rhs_lw_noalloc(int32_t polydeg, double gamma, int32_t surface
     sa.flux_kind = surface_flux;
     sa.speed_kind = max_speed;
     tlw::Basis hb;
-    host_basis(polydeg, hb);
+    host_build_basis(polydeg, hb);
     sa.inv_w_first = hb.inv_w_first;
     sa.inv_w_last = hb.inv_w_last;
     sa.status = s.status;

@@ -1,11 +1,18 @@
 // tlw_volume.cuh -- fused per-element LW / MDRK volume kernels for TreeMesh{2} (FP64, sm_100a).
 //
-// One thread per GLL node; EB whole elements per CTA so that every CTA runs (nearly) full warps (N=3: 8 x 16,
-// N=4: 5 x 25 (+3 idle lanes), N=5: 7 x 36 (+4 idle lanes) nodes). The 1-D derivative contractions read the stage fluxes
-// of the element from shared memory (tiles of double2: (f0,f1) (f2,f3) (g0,g1) (g2,g3) per node, a
-// layout with no bank conflicts for the row and column reads). All other LW stage state (perturbed
-// states u+-ut, u+-2ut, the time averages U, F, G) lives in registers. HBM traffic per element: read u
-// once, write du (or u^{n+1}) once, write the face traces of U and F.n for the surface kernels.
+// Work split inside a CTA of EB whole elements (N=3: 8 x 16 nodes in 128 threads, N=4: 5 x 25 in 128,
+// N=5: 7 x 36 in 256):
+//  * node phase - one thread per GLL node ("owner") evaluates the Euler fluxes at the perturbed states and
+//    keeps all LW stage state (u +- ut, u +- 2ut, the time averages U, F, G) in registers;
+//  * line phase - each 1-D derivative contraction is done by one thread per (variable, element, line
+//    index) that reads a whole row of f and a whole column of g from shared memory once, multiplies by
+//    the derivative matrix held in constant memory (compile-time indices: the matrix entries are FMA
+//    operands, no loads), and writes the row/column results back in place.
+// Shared memory holds, per variable and element, a row-major plane of the node values with a padded
+// plane stride chosen so that the owner accesses and the row/column accesses of the line phase are
+// (nearly) bank-conflict free. Per stage a node writes 8 doubles and reads 8 back; a line reads and
+// writes 2n. HBM traffic per element: read u once, write du (or u^{n+1}) once, write the face traces of
+// U and F.n for the interface kernels.
 //
 // Restates, per element (TreeMesh, no source terms):
 //   LW depth 4 (N>=4): lw_volume_kernel_4!  src/solvers/dgsem_tree/dg_2d.jl:918-1249
@@ -19,6 +26,23 @@
 
 namespace tlw {
 
+// Derivative matrices per degree (index N), row-major n x n in 64 slots. Static: every translation unit
+// that launches these kernels uploads its copy with upload_const_basis() on each device it uses.
+static __constant__ double c_tlw_D[8][64];
+static __constant__ double c_tlw_Dhat[8][64];
+
+static inline cudaError_t upload_const_basis(const Basis* bases /* [8], index = N */) {
+    static double d[8][64], dh[8][64];
+    for (int N = 0; N < 8; ++N)
+        for (int k = 0; k < 64; ++k) {
+            d[N][k] = bases[N].D[k];
+            dh[N][k] = bases[N].Dhat[k];
+        }
+    cudaError_t e = cudaMemcpyToSymbol(c_tlw_D, d, sizeof(d));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(c_tlw_Dhat, dh, sizeof(dh));
+}
+
 template <int N>
 struct VolCfg {
     static constexpr int n = N + 1;
@@ -28,14 +52,14 @@ struct VolCfg {
     static constexpr int THREADS = ((EB * nn + 31) / 32) * 32;
     // resident CTAs per SM the register allocation must allow (<= 128 registers per thread)
     static constexpr int MIN_BLOCKS = THREADS <= 128 ? 4 : 2;
-    // the MDRK stage kernels hold fewer values per thread: ask for more resident CTAs
-    static constexpr int MDRK_MIN_BLOCKS = THREADS <= 128 ? 6 : 3;
-    static constexpr int TILE = EB * nn;   // double2 entries per tile array
-    // shared memory: 4 stage matrices + Dhat (5 nn doubles, padded to 16 B) + NT tiles of 4 double2 arrays
-    static constexpr int MAT_D2 = (5 * nn + 1) / 2;
-    static constexpr size_t smem_bytes(int ntiles) {
-        return (size_t)MAT_D2 * sizeof(double2) + (size_t)ntiles * 4 * TILE * sizeof(double2);
-    }
+    static constexpr int MDRK_MIN_BLOCKS = THREADS <= 128 ? 5 : 2;
+    // plane layout: node (i, j) of (variable v, element e) at (v*EB + e)*P + i + R*j
+    static constexpr int R = n;
+    static constexpr int P = n == 4 ? 19 : nn;
+    static constexpr int PLANES = 4 * EB * P;          // doubles of one 4-variable field
+    static constexpr int LINES = 4 * n * EB;           // (variable, element, line index)
+    // regions: X (f / x-results), Y (g / y-results), F0X, F0Y (fluxes at u, kept for stages 2 and 4)
+    static constexpr size_t smem_bytes(int regions) { return (size_t)regions * PLANES * sizeof(double); }
 };
 
 enum VolMode { MODE_RHS = 0, MODE_STEP = 1 };
@@ -55,41 +79,71 @@ struct VolArgs {
     double gamma;
 };
 
-// writes the four double values (a,b,c,d) of node slot s into tile t
-template <int TILE>
-__device__ __forceinline__ void tile_put(double2* tiles, int t, int s, const double* f, const double* g) {
-    double2* T = tiles + t * 4 * TILE;
-    T[s] = make_double2(f[0], f[1]);
-    T[TILE + s] = make_double2(f[2], f[3]);
-    T[2 * TILE + s] = make_double2(g[0], g[1]);
-    T[3 * TILE + s] = make_double2(g[2], g[3]);
+// owner: store the node's f (into X) and g (into Y)
+template <int N>
+__device__ __forceinline__ void node_put(double* X, double* Y, int e, int i, int j, const double* f, const double* g) {
+    using C = VolCfg<N>;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const int a = (v * C::EB + e) * C::P + i + C::R * j;
+        X[a] = f[v];
+        Y[a] = g[v];
+    }
 }
-template <int TILE>
-__device__ __forceinline__ void tile_get(const double2* tiles, int t, int s, double* f, double* g) {
-    const double2* T = tiles + t * 4 * TILE;
-    const double2 a = T[s], b = T[TILE + s], c = T[2 * TILE + s], d = T[3 * TILE + s];
-    f[0] = a.x; f[1] = a.y; f[2] = b.x; f[3] = b.y;
-    g[0] = c.x; g[1] = c.y; g[2] = d.x; g[3] = d.y;
+template <int N>
+__device__ __forceinline__ void node_get(const double* X, const double* Y, int e, int i, int j, double* f, double* g) {
+    using C = VolCfg<N>;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const int a = (v * C::EB + e) * C::P + i + C::R * j;
+        f[v] = X[a];
+        g[v] = Y[a];
+    }
+}
+// owner: x-result + y-result at the node
+template <int N>
+__device__ __forceinline__ void node_sum(const double* X, const double* Y, int e, int i, int j, double* d) {
+    using C = VolCfg<N>;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const int a = (v * C::EB + e) * C::P + i + C::R * j;
+        d[v] = X[a] + Y[a];
+    }
 }
 
-// acc = sum_k M[i,k] f(k,j) + sum_k M[j,k] g(i,k) over the element whose first slot is `base`
-template <int n, int TILE>
-__device__ __forceinline__ void contract(const double2* tiles, int t, const double* M, int base, int i, int j,
-                                         double* acc) {
-    const double2* T = tiles + t * 4 * TILE;
-    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+// line phase, in place: X row (v,e,idx) <- M X row, Y column (v,e,idx) <- M Y column, with
+// M = D (HAT = false) or Dhat (HAT = true):  x-result(i, j) = sum_k M[i,k] f(k, j),
+// y-result(i, j) = sum_k M[j,k] g(i, k). Each row and column is read and written by one thread only.
+template <int N, bool HAT>
+__device__ __forceinline__ void line_contract(double* X, double* Y, int tid) {
+    using C = VolCfg<N>;
+    constexpr int n = C::n;
+    const double* M = HAT ? c_tlw_Dhat[N] : c_tlw_D[N];
+#pragma unroll 1
+    for (int t = tid; t < C::LINES; t += C::THREADS) {
+        const int idx = t % n;
+        const int r = t / n;
+        const int e = r % C::EB;
+        const int v = r / C::EB;
+        const int pb = (v * C::EB + e) * C::P;
+        double a[n], b[n];
 #pragma unroll
-    for (int k = 0; k < n; ++k) {
-        const double mx = M[i * n + k];
-        const int sx = base + k + n * j;
-        const double2 p = T[sx], q = T[TILE + sx];
-        a0 = fma(mx, p.x, a0); a1 = fma(mx, p.y, a1); a2 = fma(mx, q.x, a2); a3 = fma(mx, q.y, a3);
-        const double my = M[j * n + k];
-        const int sy = base + i + n * k;
-        const double2 r = T[2 * TILE + sy], s = T[3 * TILE + sy];
-        a0 = fma(my, r.x, a0); a1 = fma(my, r.y, a1); a2 = fma(my, s.x, a2); a3 = fma(my, s.y, a3);
+        for (int k = 0; k < n; ++k) {
+            a[k] = X[pb + k + C::R * idx];
+            b[k] = Y[pb + idx + C::R * k];
+        }
+#pragma unroll
+        for (int o = 0; o < n; ++o) {
+            double sx = 0.0, sy = 0.0;
+#pragma unroll
+            for (int k = 0; k < n; ++k) {
+                sx = fma(M[o * n + k], a[k], sx);
+                sy = fma(M[o * n + k], b[k], sy);
+            }
+            X[pb + o + C::R * idx] = sx;
+            Y[pb + idx + C::R * o] = sy;
+        }
     }
-    acc[0] = a0; acc[1] = a1; acc[2] = a2; acc[3] = a3;
 }
 
 // out/traces epilogue shared by all volume kernels. acc = Dhat-contraction of (F, G).
@@ -120,55 +174,47 @@ __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, 
 
 // ------------------------------------------------------------------------------------------------
 // Plain LW volume kernel (depth = min(N, 4)).
-// The finite-difference stencils are accumulated unscaled ("raw") and their constant factors are folded
-// into the matrices of the next contraction and into the F/G update coefficients:
+// The finite-difference stencils are accumulated unscaled ("raw"); their constant factors and -dt J^{-1}
+// are applied to the contraction result (s below) and folded into the F/G update coefficients:
 //   depth 4: f_t = raw1/12, f_tt = raw2/12, f_ttt = raw3/2, f_tttt = raw4/2
 //   depth 3: f_t = raw1/12, f_tt = raw2,    f_ttt = raw3/2
 //   depth 2: f_t = raw1/2,  f_tt = raw2;    depth 1: f_t = raw1/2
-// Shared memory holds M_k = -dt c_k D for the contraction of stage k's output (c_0 = 1) and Dhat.
 // ------------------------------------------------------------------------------------------------
 template <int N, int MODE>
 __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
-    constexpr int n = C::n, nn = C::nn, EB = C::EB, TILE = C::TILE;
+    constexpr int n = C::n, nn = C::nn, EB = C::EB;
     constexpr int DEPTH = N >= 4 ? 4 : N;
     constexpr double C1 = DEPTH >= 3 ? 1.0 / 12.0 : 0.5;
     constexpr double C2 = DEPTH == 4 ? 1.0 / 12.0 : 1.0;
     constexpr double C3 = 0.5;
     constexpr double C4 = 0.5;
-    extern __shared__ double2 smem[];
-    double* sM = reinterpret_cast<double*>(smem);   // [4][nn]: -dt D, -dt C1 D, -dt C2 D, -dt C3 D
-    double* sDh = sM + 4 * nn;                      // Dhat
-    double2* tiles = smem + C::MAT_D2;
+    extern __shared__ double smem_d[];
+    double* X = smem_d;
+    double* Y = X + C::PLANES;
+    double* F0X = Y + C::PLANES;
+    double* F0Y = F0X + C::PLANES;
 
     const int tid = threadIdx.x;
     const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
-    for (int k = tid; k < nn; k += blockDim.x) {
-        const double d = -dt * a.basis->D[k];
-        sM[k] = d;
-        sM[nn + k] = d * C1;
-        sM[2 * nn + k] = d * C2;
-        sM[3 * nn + k] = d * C3;
-        sDh[k] = a.basis->Dhat[k];
-    }
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
     const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
-    const int base = el * nn;
-    const int slot = base + node;
 
     double U[NV], F[NV], G[NV], up[NV], um[NV], upp[NV], umm[NV];
-    double ij = 0.0;
+    double s0 = 0.0, ij = 0.0;   // s0 = -dt J^{-1}
     // stage 0: f, g at u (dg_2d.jl:941-971)
     if (active) {
         double uu[NV], f[NV], g[NV];
         load4(a.u + ((size_t)e * nn + node) * NV, uu);
         ij = __ldg(a.inv_jac + e);
+        s0 = -dt * ij;
         euler_fluxes(gm1, uu[0], uu[1], uu[2], uu[3], f, g);
-        tile_put<TILE>(tiles, 0, slot, f, g);
+        node_put<N>(X, Y, el, i, j, f, g);
+        if (DEPTH >= 2) node_put<N>(F0X, F0Y, el, i, j, f, g);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             F[v] = f[v]; G[v] = g[v]; U[v] = uu[v];
@@ -176,14 +222,16 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
         }
     }
     __syncthreads();
+    line_contract<N, false>(X, Y, tid);
+    __syncthreads();
 
     // stage 1: ut; perturbed states; f_t (dg_2d.jl:972-1023 / :725-775 / :543-582 / :417-454)
     if (active) {
         double d[NV], r[NV], q[NV], f[NV], g[NV];
-        contract<n, TILE>(tiles, 0, sM, base, i, j, d);
+        node_sum<N>(X, Y, el, i, j, d);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            d[v] *= ij;
+            d[v] *= s0;
             U[v] = fma(0.5, d[v], U[v]);
             up[v] += d[v];
             um[v] -= d[v];
@@ -214,18 +262,21 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
         }
 #pragma unroll
         for (int v = 0; v < NV; ++v) { F[v] = fma(0.5 * C1, r[v], F[v]); G[v] = fma(0.5 * C1, q[v], G[v]); }
-        if (DEPTH >= 2) tile_put<TILE>(tiles, 1, slot, r, q);
+        if (DEPTH >= 2) node_put<N>(X, Y, el, i, j, r, q);
     }
     if (DEPTH >= 2) {
+        __syncthreads();
+        line_contract<N, false>(X, Y, tid);
         __syncthreads();
         // stage 2: utt; f_tt (dg_2d.jl:1025-1083 / :777-831 / :597-634)
         if (active) {
             double d[NV], f0[NV], g0[NV], r[NV], q[NV], f[NV], g[NV];
-            contract<n, TILE>(tiles, 1, sM + nn, base, i, j, d);
-            tile_get<TILE>(tiles, 0, slot, f0, g0);
+            node_sum<N>(X, Y, el, i, j, d);
+            node_get<N>(F0X, F0Y, el, i, j, f0, g0);
+            const double s = s0 * C1;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                d[v] *= ij;
+                d[v] *= s;
                 U[v] = fma(1.0 / 6.0, d[v], U[v]);
                 up[v] = fma(0.5, d[v], up[v]);
                 um[v] = fma(0.5, d[v], um[v]);
@@ -262,18 +313,21 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
                 F[v] = fma(C2 / 6.0, r[v], F[v]);
                 G[v] = fma(C2 / 6.0, q[v], G[v]);
             }
-            if (DEPTH >= 3) tile_put<TILE>(tiles, 2, slot, r, q);
+            if (DEPTH >= 3) node_put<N>(X, Y, el, i, j, r, q);
         }
     }
     if (DEPTH >= 3) {
         __syncthreads();
+        line_contract<N, false>(X, Y, tid);
+        __syncthreads();
         // stage 3: uttt; f_ttt (dg_2d.jl:1085-1138 / :833-875)
         if (active) {
             double d[NV], r[NV], q[NV], f[NV], g[NV];
-            contract<n, TILE>(tiles, 2, sM + 2 * nn, base, i, j, d);
+            node_sum<N>(X, Y, el, i, j, d);
+            const double s = s0 * C2;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                d[v] *= ij;
+                d[v] *= s;
                 U[v] = fma(1.0 / 24.0, d[v], U[v]);
                 um[v] = fma(-1.0 / 6.0, d[v], um[v]);
                 up[v] = fma(1.0 / 6.0, d[v], up[v]);
@@ -298,19 +352,22 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
                 F[v] = fma(C3 / 24.0, r[v], F[v]);
                 G[v] = fma(C3 / 24.0, q[v], G[v]);
             }
-            if (DEPTH >= 4) tile_put<TILE>(tiles, 1, slot, r, q);
+            if (DEPTH >= 4) node_put<N>(X, Y, el, i, j, r, q);
         }
     }
     if (DEPTH >= 4) {
         __syncthreads();
+        line_contract<N, false>(X, Y, tid);
+        __syncthreads();
         // stage 4: utttt; f_tttt (dg_2d.jl:1140-1206)
         if (active) {
             double d[NV], f0[NV], g0[NV], r[NV], q[NV], f[NV], g[NV];
-            contract<n, TILE>(tiles, 1, sM + 3 * nn, base, i, j, d);
-            tile_get<TILE>(tiles, 0, slot, f0, g0);
+            node_sum<N>(X, Y, el, i, j, d);
+            node_get<N>(F0X, F0Y, el, i, j, f0, g0);
+            const double s = s0 * C3;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                d[v] *= ij;
+                d[v] *= s;
                 U[v] = fma(1.0 / 120.0, d[v], U[v]);
                 um[v] = fma(1.0 / 24.0, d[v], um[v]);
                 up[v] = fma(1.0 / 24.0, d[v], up[v]);
@@ -335,20 +392,17 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
                 F[v] = fma(C4 / 120.0, r[v], F[v]);
                 G[v] = fma(C4 / 120.0, q[v], G[v]);
             }
-            // tile 2 was last read by the stage-3 contraction, before the barrier above
-            tile_put<TILE>(tiles, 2, slot, F, G);
         }
     }
-    // final: Dhat contraction of the time-averaged fluxes
-    constexpr int TF = DEPTH == 4 ? 2 : DEPTH == 3 ? 1 : DEPTH == 2 ? 2 : 1;
-    if (DEPTH < 4) {
-        __syncthreads();
-        if (active) tile_put<TILE>(tiles, TF, slot, F, G);
-    }
+    // final: Dhat contraction of the time-averaged fluxes (every owner has read its node's results of
+    // the last contraction before writing F, G over them: same address, same thread)
+    if (active) node_put<N>(X, Y, el, i, j, F, G);
+    __syncthreads();
+    line_contract<N, true>(X, Y, tid);
     __syncthreads();
     if (active) {
         double acc[NV];
-        contract<n, TILE>(tiles, TF, sDh, base, i, j, acc);
+        node_sum<N>(X, Y, el, i, j, acc);
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
     }
 }
@@ -360,39 +414,35 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
 template <int N, int MODE>
 __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk1_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
-    constexpr int n = C::n, nn = C::nn, EB = C::EB, TILE = C::TILE;
-    extern __shared__ double2 smem[];
-    double* sDm = reinterpret_cast<double*>(smem);
-    double* sDh = sDm + 4 * nn;
-    double2* tiles = smem + C::MAT_D2;
+    constexpr int n = C::n, nn = C::nn, EB = C::EB;
+    extern __shared__ double smem_d[];
+    double* X = smem_d;
+    double* Y = X + C::PLANES;
     const int tid = threadIdx.x;
     const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
-    for (int k = tid; k < nn; k += blockDim.x) {
-        sDm[k] = -dt * a.basis->D[k];
-        sDh[k] = a.basis->Dhat[k];
-    }
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
     const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
-    const int base = el * nn;
-    const int slot = base + node;
     double uu[NV], f0[NV], g0[NV], ij = 0.0;
     if (active) {
         load4(a.u + ((size_t)e * nn + node) * NV, uu);
         ij = __ldg(a.inv_jac + e);
         euler_fluxes(gm1, uu[0], uu[1], uu[2], uu[3], f0, g0);
-        tile_put<TILE>(tiles, 0, slot, f0, g0);
+        node_put<N>(X, Y, el, i, j, f0, g0);
     }
+    __syncthreads();
+    line_contract<N, false>(X, Y, tid);
     __syncthreads();
     double U[NV], F[NV], G[NV];
     if (active) {
         double d[NV], ft[NV], gt[NV], f[NV], g[NV], s[NV];
-        contract<n, TILE>(tiles, 0, sDm, base, i, j, d);
+        node_sum<N>(X, Y, el, i, j, d);
+        const double s0 = -dt * ij;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) d[v] *= ij;
+        for (int v = 0; v < NV; ++v) d[v] *= s0;
 #pragma unroll
         for (int v = 0; v < NV; ++v) s[v] = fma(2.0, d[v], uu[v]);
         euler_fluxes(gm1, s[0], s[1], s[2], s[3], f, g);
@@ -421,13 +471,14 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
         store4(a.U2 + off * NV, U2v);
         store4(a.F2 + off * 2 * NV, F2v);
         store4(a.F2 + off * 2 * NV + NV, G2v);
+        node_put<N>(X, Y, el, i, j, F, G);
     }
     __syncthreads();
-    if (active) tile_put<TILE>(tiles, 1, slot, F, G);
+    line_contract<N, true>(X, Y, tid);
     __syncthreads();
     if (active) {
         double acc[NV];
-        contract<n, TILE>(tiles, 1, sDh, base, i, j, acc);
+        node_sum<N>(X, Y, el, i, j, acc);
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
     }
 }
@@ -439,40 +490,36 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
 template <int N, int MODE>
 __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk2_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
-    constexpr int n = C::n, nn = C::nn, EB = C::EB, TILE = C::TILE;
-    extern __shared__ double2 smem[];
-    double* sDm = reinterpret_cast<double*>(smem);
-    double* sDh = sDm + 4 * nn;
-    double2* tiles = smem + C::MAT_D2;
+    constexpr int n = C::n, nn = C::nn, EB = C::EB;
+    extern __shared__ double smem_d[];
+    double* X = smem_d;
+    double* Y = X + C::PLANES;
     const int tid = threadIdx.x;
     const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
-    for (int k = tid; k < nn; k += blockDim.x) {
-        sDm[k] = -dt * a.basis->D[k];
-        sDh[k] = a.basis->Dhat[k];
-    }
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
     const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
-    const int base = el * nn;
-    const int slot = base + node;
     double us[NV], ij = 0.0;
     if (active) {
         double f[NV], g[NV];
         load4(a.u + ((size_t)e * nn + node) * NV, us);
         ij = __ldg(a.inv_jac + e);
         euler_fluxes(gm1, us[0], us[1], us[2], us[3], f, g);
-        tile_put<TILE>(tiles, 0, slot, f, g);
+        node_put<N>(X, Y, el, i, j, f, g);
     }
+    __syncthreads();
+    line_contract<N, false>(X, Y, tid);
     __syncthreads();
     double U[NV], F[NV], G[NV];
     if (active) {
         double d[NV], ft[NV], gt[NV], f[NV], g[NV], s[NV];
-        contract<n, TILE>(tiles, 0, sDm, base, i, j, d);
+        node_sum<N>(X, Y, el, i, j, d);
+        const double s0 = -dt * ij;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) d[v] *= ij;
+        for (int v = 0; v < NV; ++v) d[v] *= s0;
 #pragma unroll
         for (int v = 0; v < NV; ++v) s[v] = fma(2.0, d[v], us[v]);
         euler_fluxes(gm1, s[0], s[1], s[2], s[3], f, g);
@@ -498,13 +545,14 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
             G[v] = fma(1.0 / 3.0, gt[v], G2v[v]);
             U[v] = fma(1.0 / 3.0, d[v], U2v[v]);
         }
+        node_put<N>(X, Y, el, i, j, F, G);
     }
     __syncthreads();
-    if (active) tile_put<TILE>(tiles, 1, slot, F, G);
+    line_contract<N, true>(X, Y, tid);
     __syncthreads();
     if (active) {
         double acc[NV];
-        contract<n, TILE>(tiles, 1, sDh, base, i, j, acc);
+        node_sum<N>(X, Y, el, i, j, acc);
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
     }
 }
