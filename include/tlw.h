@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define TLW_ABI_VERSION 1
+#define TLW_ABI_VERSION 2
 
 enum tlw_status {
     TLW_OK = 0,
@@ -48,7 +48,16 @@ enum tlw_cache_item {
     TLW_CACHE_U_TRACES = 0,    /* time-averaged U on the 4 faces, [v, l, face, element], face = -x,+x,-y,+y */
     TLW_CACHE_F_TRACES = 1,    /* normal time-averaged flux (F on x faces, G on y faces), same layout */
     TLW_CACHE_U2 = 2,          /* MDRK stage-1 U2 [v, i, j, element]   (MDRKElementCache.U2) */
-    TLW_CACHE_F2 = 3           /* MDRK stage-1 F2 [v, d, i, j, element] (MDRKElementCache.F2) */
+    TLW_CACHE_F2 = 3,          /* MDRK stage-1 F2 [v, d, i, j, element] (MDRKElementCache.F2) */
+    TLW_CACHE_ALPHA = 4,       /* shock capturing: blending factor per element (indicator.cache.alpha) */
+    TLW_CACHE_FN_LOW = 5       /* shock capturing: first-order subcell flux next to each face, as the traces
+                                  (element_cache.fn_low) */
+};
+enum tlw_volume_integral {
+    TLW_VOLUME_FR = 0,                  /* VolumeIntegralFR(LW()/MDRK())                                  */
+    TLW_VOLUME_FR_SHOCK_CAPTURING = 1   /* VolumeIntegralFRShockCapturing(IndicatorHennemannGassner(...;
+                                           variable = density_pressure); volume_flux_fv = flux_lax_friedrichs,
+                                           reconstruction = FirstOrderReconstruction()) (src/solvers/fr.jl:59-86) */
 };
 
 typedef struct tlw_opts {
@@ -58,7 +67,11 @@ typedef struct tlw_opts {
     int32_t max_speed;             /* TLW_SPEED_NAIVE (Trixi default of the reference's era) | TLW_SPEED_DAVIS */
     double gamma;                  /* CompressibleEulerEquations2D(gamma) */
     int32_t device;                /* CUDA device ordinal */
-    int32_t reserved[7];           /* zero */
+    int32_t volume_integral;       /* TLW_VOLUME_FR | TLW_VOLUME_FR_SHOCK_CAPTURING */
+    double alpha_max;              /* indicator: alpha_max (Trixi default 0.5) */
+    double alpha_min;              /* indicator: alpha_min (Trixi default 0.001) */
+    int32_t alpha_smooth;          /* indicator: alpha_smooth (Trixi default true) */
+    int32_t reserved[3];           /* zero */
 } tlw_opts;
 
 typedef struct tlw_handle tlw_handle;

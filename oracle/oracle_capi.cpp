@@ -62,6 +62,15 @@ oracle_handle* oracle_create(int N, double gamma, int flux_kind, int speed_kind,
 
 void oracle_destroy(oracle_handle* h) { delete h; }
 
+// VolumeIntegralFRShockCapturing with IndicatorHennemannGassner(alpha_max, alpha_min, alpha_smooth;
+// variable = density_pressure) and first-order subcell reconstruction.
+void oracle_set_shock_capturing(oracle_handle* h, int on, double alpha_max, double alpha_min, int alpha_smooth) {
+    h->opt.shock_capturing = on != 0;
+    h->opt.alpha_max = alpha_max;
+    h->opt.alpha_min = alpha_min;
+    h->opt.alpha_smooth = alpha_smooth != 0;
+}
+
 void oracle_set_temporal_errors(oracle_handle* h, int on, double abstol, double reltol) {
     h->opt.temporal_errors = on != 0;
     h->opt.abstol = abstol;
@@ -91,7 +100,8 @@ int oracle_rhs(oracle_handle* h, int kind, const double* u, const double* u2, do
     }
 }
 
-// which: 0 U [v,i,j,e], 1 F [v,d,i,j,e], 2 U2, 3 F2, 4 temporal_errors [e], 5 surface_flux_values [v,l,face,e]
+// which: 0 U [v,i,j,e], 1 F [v,d,i,j,e], 2 U2, 3 F2, 4 temporal_errors [e], 5 surface_flux_values [v,l,face,e],
+//        6 alpha [e], 7 fn_low [v,l,face,e]
 int oracle_get(oracle_handle* h, int which, double* out) {
     const std::vector<double>* src = nullptr;
     switch (which) {
@@ -101,6 +111,8 @@ int oracle_get(oracle_handle* h, int which, double* out) {
         case 3: src = &h->ws.F2; break;
         case 4: src = &h->ws.temporal_errors; break;
         case 5: src = &h->ws.surface_flux_values; break;
+        case 6: src = &h->ws.alpha; break;
+        case 7: src = &h->ws.fn_low; break;
         default: return 1;
     }
     std::copy(src->begin(), src->end(), out);

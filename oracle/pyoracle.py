@@ -39,6 +39,7 @@ def lib():
         L.oracle_create.restype = P
         L.oracle_destroy.argtypes = [P]
         L.oracle_set_temporal_errors.argtypes = [P, i32, dbl, dbl]
+        L.oracle_set_shock_capturing.argtypes = [P, i32, dbl, dbl, i32]
         L.oracle_set_boundary_data.argtypes = [P, P, P]
         L.oracle_rhs.argtypes = [P, i32, P, P, P, dbl, dbl, i32]
         L.oracle_get.argtypes = [P, i32, P]
@@ -103,6 +104,9 @@ class Oracle:
     def size(self):
         return 4 * self.n * self.n * self.E
 
+    def set_shock_capturing(self, on=True, alpha_max=0.5, alpha_min=0.001, alpha_smooth=True):
+        lib().oracle_set_shock_capturing(self.h, 1 if on else 0, alpha_max, alpha_min, 1 if alpha_smooth else 0)
+
     def set_boundary_data(self, levels: np.ndarray, now: np.ndarray):
         self._bkeep = (np.ascontiguousarray(levels, dtype=np.float64), np.ascontiguousarray(now, dtype=np.float64))
         lib().oracle_set_boundary_data(self.h, _p(self._bkeep[0]), _p(self._bkeep[1]))
@@ -120,7 +124,7 @@ class Oracle:
 
     def get(self, which: int) -> np.ndarray:
         sizes = {0: self.size(), 1: 2 * self.size(), 2: self.size(), 3: 2 * self.size(), 4: self.E,
-                 5: 4 * self.n * 4 * self.E}
+                 5: 4 * self.n * 4 * self.E, 6: self.E, 7: 4 * self.n * 4 * self.E}
         out = np.empty(sizes[which])
         assert lib().oracle_get(self.h, which, _p(out)) == 0
         return out

@@ -250,6 +250,11 @@ struct Options {
     int speed_kind = 0;            // 0 = max_abs_speed_naive
     bool temporal_errors = false;  // lw_volume_kernel_4! u_np1/u_np1_low tail (dg_2d.jl:1251-1265)
     double abstol = 0.0, reltol = 0.0;
+    // VolumeIntegralFRShockCapturing(IndicatorHennemannGassner(...; variable = density_pressure),
+    // volume_flux_fv = flux_lax_friedrichs, reconstruction = FirstOrderReconstruction())
+    bool shock_capturing = false;
+    double alpha_max = 0.5, alpha_min = 0.001;
+    bool alpha_smooth = true;
 };
 
 struct Workspace {
@@ -262,6 +267,8 @@ struct Workspace {
     std::vector<double> surface_flux_values;  // [v, i, face, e], face 0..3 = -x, +x, -y, +y
     // boundary cache [side, v, i, B] and exterior time-averaged states supplied per call
     std::vector<double> bu, bU, bF;
+    std::vector<double> alpha;           // blending factor per element (shock capturing)
+    std::vector<double> fn_low;          // [v, l, face, e] first-order subcell flux next to each face
     bool bad = false;                    // a sqrt of a negative number happened (Julia DomainError)
 };
 
@@ -794,6 +801,194 @@ inline void ensure_workspace(const Basis& b, const TreeMesh& m, Workspace& ws, b
     if (ws.temporal_errors.size() != (size_t)m.n_elements) ws.temporal_errors.assign(m.n_elements, nan);
 }
 
+// ------------------------------------------------------------------------------------------------
+// Shock capturing (VolumeIntegralFRShockCapturing, src/solvers/dgsem_tree/dg_2d.jl:1648-1804).
+// ------------------------------------------------------------------------------------------------
+// Trixi legendre_polynomial_and_derivative, normalised by sqrt(m + 1/2)
+inline double legendre_normalized(int m, double x) {
+    double p;
+    if (m == 0) p = 1.0;
+    else if (m == 1) p = x;
+    else {
+        double a = 1.0, b = x;
+        p = 0.0;
+        for (int k = 2; k <= m; ++k) {
+            p = ((2.0 * k - 1.0) * x * b - (k - 1.0) * a) / k;
+            a = b; b = p;
+        }
+    }
+    return p * std::sqrt(m + 0.5);
+}
+
+// inverse of the Legendre Vandermonde matrix V[i][m] = P~_m(x_i) (Trixi vandermonde_legendre), by
+// Gauss-Jordan elimination with partial pivoting; row-major n x n.
+inline std::vector<double> inverse_vandermonde_legendre(const Basis& b) {
+    const int n = b.n;
+    std::vector<double> A(n * n), I(n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int m = 0; m < n; ++m) A[i * n + m] = legendre_normalized(m, b.nodes[i]);
+    for (int i = 0; i < n; ++i) I[i * n + i] = 1.0;
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(A[r * n + c]) > std::fabs(A[piv * n + c])) piv = r;
+        for (int k = 0; k < n; ++k) { std::swap(A[c * n + k], A[piv * n + k]); std::swap(I[c * n + k], I[piv * n + k]); }
+        const double d = A[c * n + c];
+        for (int k = 0; k < n; ++k) { A[c * n + k] /= d; I[c * n + k] /= d; }
+        for (int r = 0; r < n; ++r)
+            if (r != c) {
+                const double f = A[r * n + c];
+                for (int k = 0; k < n; ++k) { A[r * n + k] -= f * A[c * n + k]; I[r * n + k] -= f * I[c * n + k]; }
+            }
+    }
+    return I;
+}
+
+// Trixi IndicatorHennemannGassner (Hennemann, Rueda-Ramirez, Hindenlang, Gassner, J. Comput. Phys. 426
+// (2021)), indicator variable density_pressure = (gamma-1)(rho rho_e - |rho v|^2 / 2), followed by the
+// interface smoothing alpha_e = max(alpha_e, alpha_nb / 2) (Trixi apply_smoothing!).
+inline void indicator_hennemann_gassner(const Basis& b, const Euler& eq, const Options& opt, const TreeMesh& m,
+                                        const double* u, std::vector<double>& alpha) {
+    const int n = b.n;
+    const std::vector<double> Vinv = inverse_vandermonde_legendre(b);
+    const double threshold = 0.5 * std::pow(10.0, -1.8 * std::pow((double)n, 0.25));
+    const double parameter_s = std::log((1.0 - 0.0001) / 0.0001);
+    alpha.assign(m.n_elements, 0.0);
+    for (int e = 0; e < m.n_elements; ++e) {
+        double ind[MAXN * MAXN], tmp[MAXN * MAXN], modal[MAXN * MAXN];
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const double* x = u + idx_u(n, 0, i, j, e);
+                ind[i + n * j] = (eq.gamma - 1.0) * (x[0] * x[3] - 0.5 * (x[1] * x[1] + x[2] * x[2]));
+            }
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                double r = 0.0;
+                for (int a = 0; a < n; ++a) r += Vinv[i * n + a] * ind[a + n * j];
+                tmp[i + n * j] = r;
+            }
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                double r = 0.0;
+                for (int c = 0; c < n; ++c) r += Vinv[j * n + c] * tmp[i + n * c];
+                modal[i + n * j] = r;
+            }
+        double total = 0.0, clip1 = 0.0, clip2 = 0.0;
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) total += modal[i + n * j] * modal[i + n * j];
+        for (int j = 0; j < n - 1; ++j)
+            for (int i = 0; i < n - 1; ++i) clip1 += modal[i + n * j] * modal[i + n * j];
+        for (int j = 0; j < n - 2; ++j)
+            for (int i = 0; i < n - 2; ++i) clip2 += modal[i + n * j] * modal[i + n * j];
+        const double f1 = total != 0.0 ? (total - clip1) / total : 0.0;
+        const double f2 = clip1 != 0.0 ? (clip1 - clip2) / clip1 : 0.0;
+        const double energy = std::max(f1, f2);
+        double a = 1.0 / (1.0 + std::exp(-parameter_s / threshold * (energy - threshold)));
+        if (a < opt.alpha_min) a = 0.0;
+        if (a > 1.0 - opt.alpha_min) a = 1.0;
+        alpha[e] = std::min(opt.alpha_max, a);
+    }
+    if (opt.alpha_smooth) {
+        const std::vector<double> tmp = alpha;
+        for (int k = 0; k < m.n_interfaces; ++k) {
+            const int l = m.interface_left[k], r = m.interface_right[k];
+            alpha[l] = std::max(std::max(tmp[l], 0.5 * tmp[r]), alpha[l]);
+            alpha[r] = std::max(std::max(tmp[r], 0.5 * tmp[l]), alpha[r]);
+        }
+    }
+}
+
+// Trixi 4-argument flux_lax_friedrichs (FluxPlusDissipation(flux_central, DissipationLocalLaxFriedrichs))
+inline void rusanov(const Euler& eq, int speed_kind, const double* ul, const double* ur, int orientation, double* out,
+                    bool& bad) {
+    double fl[NV], fr[NV];
+    eq.flux(ul, orientation, fl);
+    eq.flux(ur, orientation, fr);
+    const double lambda = eq.max_abs_speed(ul, ur, orientation, speed_kind, bad);
+    for (int v = 0; v < NV; ++v) out[v] = 0.5 * (fl[v] + fr[v]) + (-0.5 * lambda * (ur[v] - ul[v]));
+}
+
+// First-order subcell FV on one element: Trixi calcflux_fv! (TreeMesh{2}) with volume_flux_fv; if
+// `blended`, du += alpha * (w_i^-1 (f*_{i+1} - f*_i) + w_j^-1 (g*_{j+1} - g*_j)) (fv_kernel!,
+// dg_2d.jl:251-282); always the subcell fluxes next to the faces into fn_low (load_fn_low!, :220-234;
+// for pure DG elements calc_fn_low!, :1948-1991, computes exactly these).
+inline void first_order_subcells(const Basis& b, const Euler& eq, const Options& opt, int e, const double* u,
+                                 double* du, double alpha, bool blended, Workspace& ws, bool& bad) {
+    const int n = b.n;
+    double fx[(MAXN + 1) * MAXN * NV], fy[MAXN * (MAXN + 1) * NV];
+    auto FX = [&](int f, int j) { return fx + NV * (f + (n + 1) * j); };   // face f in 0..n along x, row j
+    auto FY = [&](int i, int f) { return fy + NV * (i + n * f); };         // face f in 0..n along y, column i
+    for (int j = 0; j < n; ++j) {
+        for (int v = 0; v < NV; ++v) { FX(0, j)[v] = 0.0; FX(n, j)[v] = 0.0; }
+        for (int f = 1; f < n; ++f) rusanov(eq, opt.speed_kind, u + idx_u(n, 0, f - 1, j, e), u + idx_u(n, 0, f, j, e), 1, FX(f, j), bad);
+    }
+    for (int i = 0; i < n; ++i) {
+        for (int v = 0; v < NV; ++v) { FY(i, 0)[v] = 0.0; FY(i, n)[v] = 0.0; }
+        for (int f = 1; f < n; ++f) rusanov(eq, opt.speed_kind, u + idx_u(n, 0, i, f - 1, e), u + idx_u(n, 0, i, f, e), 2, FY(i, f), bad);
+    }
+    if (blended) {
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i)
+                for (int v = 0; v < NV; ++v)
+                    du[idx_u(n, v, i, j, e)] += alpha * (1.0 / b.weights[i] * (FX(i + 1, j)[v] - FX(i, j)[v]) +
+                                                         1.0 / b.weights[j] * (FY(i, j + 1)[v] - FY(i, j)[v]));
+    }
+    for (int l = 0; l < n; ++l)
+        for (int v = 0; v < NV; ++v) {
+            ws.fn_low[v + NV * (l + n * (0 + 4 * (size_t)e))] = FX(1, l)[v];
+            ws.fn_low[v + NV * (l + n * (1 + 4 * (size_t)e))] = FX(n - 1, l)[v];
+            ws.fn_low[v + NV * (l + n * (2 + 4 * (size_t)e))] = FY(l, 1)[v];
+            ws.fn_low[v + NV * (l + n * (3 + 4 * (size_t)e))] = FY(l, n - 1)[v];
+        }
+}
+
+// calc_interface_flux! with compute_alp for VolumeIntegralFRShockCapturing (dg_2d.jl:1879-1946): the LW
+// flux Fn_ is blended with the first-order flux fn at the instantaneous u by alp = (alpha_L + alpha_R)/2,
+// and alp = 1 where the low-order update of either face subcell (lambda = 1/2 weights) would not be
+// admissible. J^{-1} at TreeMesh interfaces is element 1's (containers_2d.jl:29-31).
+inline void calc_interface_flux_blended(const Basis& b, const Euler& eq, const Options& opt, const TreeMesh& m,
+                                        double dt, Workspace& ws, int nthreads = 1) {
+    const int n = b.n;
+    auto ii = [&](int side, int v, int l, size_t k) { return side + 2 * (v + NV * (l + (size_t)n * k)); };
+    const double J = m.inverse_jacobian[0];
+    bool bad = false;
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad)
+    for (int k = 0; k < m.n_interfaces; ++k) {
+        const int le = m.interface_left[k], re = m.interface_right[k];
+        const int o = m.interface_orientation[k];
+        const int left_dir = 2 * o - 1, right_dir = 2 * o - 2;
+        for (int l = 0; l < n; ++l) {
+            double Ul[NV], Ur[NV], ul[NV], ur[NV], fl[NV], fr[NV], Fn_[NV], fn[NV], fil[NV], fir[NV], Fn[NV];
+            for (int v = 0; v < NV; ++v) {
+                Ul[v] = ws.iU[ii(0, v, l, k)]; Ur[v] = ws.iU[ii(1, v, l, k)];
+                ul[v] = ws.iu[ii(0, v, l, k)]; ur[v] = ws.iu[ii(1, v, l, k)];
+                fl[v] = ws.iF[ii(0, v, l, k)]; fr[v] = ws.iF[ii(1, v, l, k)];
+                fil[v] = ws.fn_low[v + NV * (l + n * (left_dir + 4 * (size_t)le))];
+                fir[v] = ws.fn_low[v + NV * (l + n * (right_dir + 4 * (size_t)re))];
+            }
+            lw_surface_flux(eq, opt.flux_kind, opt.speed_kind, fl, fr, Ul, Ur, ul, ur, o, Fn_, bad);
+            rusanov(eq, opt.speed_kind, ul, ur, o, fn, bad);
+            // compute_alp (dg_2d.jl:1879-1901)
+            double alp = 0.5 * (ws.alpha[le] + ws.alpha[re]);
+            double Fb[NV], low[NV];
+            for (int v = 0; v < NV; ++v) Fb[v] = (1.0 - alp) * Fn_[v] + alp * fn[v];
+            const double lam = 0.5;
+            for (int v = 0; v < NV; ++v) low[v] = ul[v] - dt * J / (b.weights[n - 1] * lam) * (Fb[v] - fil[v]);
+            if (!eq.is_admissible(low)) alp = 1.0;
+            else {
+                for (int v = 0; v < NV; ++v) low[v] = ur[v] - dt * J / (b.weights[0] * lam) * (fir[v] - Fb[v]);
+                if (!eq.is_admissible(low)) alp = 1.0;
+            }
+            for (int v = 0; v < NV; ++v) Fn[v] = alp * fn[v] + (1.0 - alp) * Fn_[v];
+            for (int v = 0; v < NV; ++v) {
+                ws.surface_flux_values[v + NV * (l + n * (left_dir + 4 * (size_t)le))] = Fn[v];
+                ws.surface_flux_values[v + NV * (l + n * (right_dir + 4 * (size_t)re))] = Fn[v];
+            }
+        }
+    }
+    if (bad) ws.bad = true;
+}
+
 // rhs!(du, u, t, dt, mesh::TreeMesh{2}, ..., ::LW, ...) (src/solvers/dgsem_tree/dg_2d.jl:28-83)
 // kind 0 = LW, 1 = MDRK stage 1 (multi_derivative_2d.jl:1-57), 2 = MDRK stage 2 (:59-116; `u2` = u*).
 inline void rhs(const Basis& b, const Euler& eq, const Options& opt, const TreeMesh& m, const double* u,
@@ -805,17 +1000,34 @@ inline void rhs(const Basis& b, const Euler& eq, const Options& opt, const TreeM
     const size_t ndof = (size_t)NV * b.n * b.n * m.n_elements;
 #pragma omp parallel for num_threads(nthreads) schedule(static)
     for (long long k = 0; k < (long long)ndof; ++k) du[k] = 0.0;   // reset_du!
-#pragma omp parallel for num_threads(nthreads) schedule(static)
-    for (int e = 0; e < m.n_elements; ++e) {
-        if (kind == 0)
-            lw_volume_element(b, eq, opt, e, u, du, dt, m.inverse_jacobian[e], 1.0, ws);
-        else if (kind == 1)
-            mdrk1_volume_element(b, eq, e, u, du, dt, m.inverse_jacobian[e], 1.0, ws);
-        else
-            mdrk2_volume_element(b, eq, e, u2, du, dt, m.inverse_jacobian[e], 1.0, ws);
+    if (opt.shock_capturing) {
+        // the indicator and the FV subcells use the instantaneous u in every stage
+        // (dg_2d.jl:1665; multi_derivative_2d.jl:166, 222, 205, 257)
+        indicator_hennemann_gassner(b, eq, opt, m, u, ws.alpha);
+        ws.fn_low.assign((size_t)NV * b.n * 4 * m.n_elements, 0.0);
     }
+    bool bad_fv = false;
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad_fv)
+    for (int e = 0; e < m.n_elements; ++e) {
+        const double a = opt.shock_capturing ? 1.0 - ws.alpha[e] : 1.0;
+        if (kind == 0)
+            lw_volume_element(b, eq, opt, e, u, du, dt, m.inverse_jacobian[e], a, ws);
+        else if (kind == 1)
+            mdrk1_volume_element(b, eq, e, u, du, dt, m.inverse_jacobian[e], a, ws);
+        else
+            mdrk2_volume_element(b, eq, e, u2, du, dt, m.inverse_jacobian[e], a, ws);
+        if (opt.shock_capturing) {
+            // pure_and_blended_element_ids!: DG only where isapprox(alpha, 0, atol = 1e-12)
+            const bool blended = !(std::fabs(ws.alpha[e]) <= 1e-12);
+            first_order_subcells(b, eq, opt, e, u, du, ws.alpha[e], blended, ws, bad_fv);
+        }
+    }
+    if (bad_fv) ws.bad = true;
     prolong2interfaces(b, m, u, ws, nthreads);
-    calc_interface_flux(b, eq, opt, m, ws, nthreads);
+    if (opt.shock_capturing)
+        calc_interface_flux_blended(b, eq, opt, m, dt, ws, nthreads);
+    else
+        calc_interface_flux(b, eq, opt, m, ws, nthreads);
     if (m.n_boundaries > 0) {
         if (!bd || !bd->u_levels || !bd->u_now) throw std::invalid_argument("boundary data missing");
         calc_boundary_flux(b, eq, opt, m, u, *bd, kind == 1 ? 0.5 : 1.0, ws);

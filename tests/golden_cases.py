@@ -9,7 +9,12 @@ CASES = {
     "lw_vortex_N5_L2": ("lw", 5, 2, "vortex", (-10.0, 10.0), True),
     "mdrk_vortex_N4_L2": ("mdrk", 4, 2, "vortex", (-10.0, 10.0), True),
     "lw_riemann_N4_L2": ("lw", 4, 2, "riemann", (0.0, 1.0), False),
+    # shock capturing (HG indicator alpha_max = 0.5, first-order subcells)
+    "sc_lw_riemann_N4_L3": ("lw", 4, 3, "riemann", (0.0, 1.0), False),
+    "sc_mdrk_riemann_N3_L3": ("mdrk", 3, 3, "riemann", (0.0, 1.0), False),
 }
+
+SHOCK_CAPTURING = {"sc_lw_riemann_N4_L3", "sc_mdrk_riemann_N3_L3"}
 
 
 def setup(name, tl):
@@ -37,6 +42,8 @@ def boundary_data(mesh, N, ic, eq, t=0.0):
 def run_case(name, oracle_mod, tl):
     td, N, eq, mesh, ic, u = setup(name, tl)
     o = oracle_mod.Oracle(mesh, N)
+    if name in SHOCK_CAPTURING:
+        o.set_shock_capturing(True, 0.5, 0.001, True)
     levels, now = boundary_data(mesh, N, ic, eq)
     if levels is not None:
         o.set_boundary_data(levels, now)
@@ -47,6 +54,9 @@ def run_case(name, oracle_mod, tl):
         out["du"] = o.rhs(u, 0.0, dt)
         out["U"] = o.get(0)
         out["F"] = o.get(1)
+        if name in SHOCK_CAPTURING:
+            out["alpha"] = o.get(6)
+            out["fn_low"] = o.get(7)
     else:
         du1 = o.rhs(u, 0.0, dt, kind=1)
         out["du1"] = du1
@@ -58,4 +68,7 @@ def run_case(name, oracle_mod, tl):
         out["du2"] = o.rhs(u, 0.0, dt, kind=2, us=us)
         out["U"] = o.get(0)
         out["F"] = o.get(1)
+        if name in SHOCK_CAPTURING:
+            out["alpha"] = o.get(6)
+            out["fn_low"] = o.get(7)
     return out

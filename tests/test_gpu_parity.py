@@ -40,10 +40,13 @@ def faces_from_full(X, n, E, F=None):
     return out
 
 
-def make_semi(tl, mesh, N, ic, td="lw", flux=None, bc=None):
+def make_semi(tl, mesh, N, ic, td="lw", flux=None, bc=None, sc=False):
     eq = tl.CompressibleEulerEquations2D(1.4)
     tdo = tl.LW() if td == "lw" else tl.MDRK()
-    solver = tl.DGSEM(N, flux or tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tdo))
+    vi = tl.VolumeIntegralFR(tdo)
+    if sc:
+        vi = tl.VolumeIntegralFRShockCapturing(tl.IndicatorHennemannGassner(alpha_max=0.5), vi)
+    solver = tl.DGSEM(N, flux or tl.flux_lax_friedrichs, vi)
     kw = {}
     if mesh.n_boundaries:
         kw["boundary_conditions"] = bc or tl.BoundaryConditionDirichlet(ic)
@@ -57,7 +60,8 @@ def test_golden_cases(tl, name):
     td, N, eq, mesh, ic, u = golden_cases.setup(name, tl)
     n = N + 1
     E = mesh.n_elements
-    semi = make_semi(tl, mesh, N, ic, td)
+    sc = name in golden_cases.SHOCK_CAPTURING
+    semi = make_semi(tl, mesh, N, ic, td, sc=sc)
     semi.cache["dt"][0] = float(ref["dt"][0])
     np.testing.assert_array_equal(u, ref["u"])
     du = np.empty_like(u)
@@ -81,6 +85,57 @@ def test_golden_cases(tl, name):
     F = ref["F"].reshape(E, n, n, 2, 4)
     np.testing.assert_allclose(tU, faces_from_full(U, n, E), rtol=0, atol=1e-13 * np.abs(U).max())
     np.testing.assert_allclose(tF, faces_from_full(None, n, E, F), rtol=0, atol=1e-12 * np.abs(F).max())
+    if sc:
+        alpha = semi.get_cache(_lib.TLW_CACHE_ALPHA)
+        np.testing.assert_allclose(alpha, ref["alpha"], rtol=1e-10, atol=1e-14)
+        fnl = semi.get_cache(_lib.TLW_CACHE_FN_LOW)
+        np.testing.assert_allclose(fnl, ref["fn_low"], rtol=0, atol=1e-12 * np.abs(ref["fn_low"]).max())
+
+
+@pytest.mark.parametrize("td,N", [("lw", 4), ("lw", 3), ("mdrk", 4)])
+def test_shock_capturing_riemann_steps(tl, oracle_mod, td, N):
+    """Four-quadrant Riemann problem with HG blending (alpha_max = 0.5) and first-order subcells,
+    Dirichlet boundaries: 20 device steps (indicator fused into the CFL pass, CUDA graphs) vs the oracle."""
+    mesh = tl.TreeMesh((0.0, 0.0), (1.0, 1.0), 4, periodicity=False)
+    ic = tl.FourQuadrantRiemann()
+    semi = make_semi(tl, mesh, N, ic, td, sc=True)
+    u0 = semi.compute_coefficients(0.0)
+    semi._prepare_boundaries(0.0, 0.0, 1.0)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, semi.time_discretization, (0.0, 1e9)))
+    integ.set_state(u0, 0.0)
+    integ.step(20, 0.15)
+    u_gpu = integ.get_state()
+    o = oracle_mod.Oracle(mesh, N)
+    o.set_shock_capturing(True, 0.5, 0.001, True)
+    lv, nw = golden_cases.boundary_data(mesh, N, ic, semi.equations)
+    o.set_boundary_data(lv, nw)
+    u_cpu = u0.copy()
+    o.steps(u_cpu, 20, 0.15, 0.0, 1e9, kind=0 if td == "lw" else 1, nthreads=os.cpu_count() or 1)
+    assert np.all(rel_l2(u_gpu, u_cpu) < 1e-11), rel_l2(u_gpu, u_cpu)
+
+
+def test_shock_capturing_periodic_conservation(tl):
+    """Periodic density square wave with shock capturing: alpha > 0 somewhere, discrete conservation holds."""
+    from trixilw import _lib
+    from trixilw.basis import gauss_lobatto
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    mesh = tl.TreeMesh((-1.0, -1.0), (1.0, 1.0), 5)
+
+    def square(x, y, t, eq):
+        rho = np.where((np.abs(x) < 0.4) & (np.abs(y) < 0.4), 2.0, 1.0)
+        return eq.prim2cons(rho, 0.5, 0.3, 1.0)
+
+    semi = make_semi(tl, mesh, 4, square, sc=True)
+    u = semi.compute_coefficients(0.0)
+    semi.cache["dt"][0] = semi.max_dt(u, 0.15)
+    du = np.empty_like(u)
+    tl.rhs(du, u, semi, 0.0)
+    assert semi.get_cache(_lib.TLW_CACHE_ALPHA).max() > 0.0
+    _, w = gauss_lobatto(4)
+    d = du.reshape(mesh.n_elements, 5, 5, 4)
+    total = np.einsum("ejiv,j,i->v", d, w, w)
+    scale = np.einsum("ejiv,j,i->v", np.abs(d), w, w)
+    assert np.all(np.abs(total) <= 1e-12 * scale)
 
 
 @pytest.mark.parametrize("N", [1, 2, 3, 4, 5, 6, 7])

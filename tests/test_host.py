@@ -68,7 +68,7 @@ def test_library_exports_every_declared_symbol(tl):
     for s in syms:
         assert hasattr(L, s), s
     assert set(syms) == set(_lib.EXPORTED)
-    assert L.tlw_abi_version() == 1
+    assert L.tlw_abi_version() == 2
 
 
 def test_opts_struct_layout(tmp_path):

@@ -171,7 +171,7 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
 @pytest.mark.parametrize("name", ["lw_vortex_N3_L2", "lw_vortex_N4_L2", "lw_vortex_N5_L2", "mdrk_vortex_N4_L2",
-                                  "lw_riemann_N4_L2"])
+                                  "lw_riemann_N4_L2", "sc_lw_riemann_N4_L3", "sc_mdrk_riemann_N3_L3"])
 def test_golden_fixtures(oracle_mod, tl, name):
     import golden_cases
     path = os.path.join(GOLDEN, name + ".npz")
@@ -179,3 +179,85 @@ def test_golden_fixtures(oracle_mod, tl, name):
     out = golden_cases.run_case(name, oracle_mod, tl)
     for k in ref.files:
         np.testing.assert_allclose(out[k], ref[k], rtol=0, atol=1e-13 * max(1.0, np.abs(ref[k]).max()), err_msg=k)
+
+
+def _numpy_indicator(u, n, gamma=1.4, alpha_max=0.5, alpha_min=0.001):
+    """Independent numpy restatement of the Hennemann-Gassner indicator (before smoothing)."""
+    from numpy.polynomial import legendre as Lg
+    x, _ = np.polynomial.legendre.leggauss(2)   # placeholder to import module
+    from trixilw.basis import gauss_lobatto
+    nodes, _ = gauss_lobatto(n - 1)
+    V = np.stack([Lg.legval(nodes, np.eye(n)[m]) * np.sqrt(m + 0.5) for m in range(n)], axis=1)
+    Vi = np.linalg.inv(V)
+    uu = u.reshape(-1, n, n, 4)                                        # [e, j, i, v]
+    ind = (gamma - 1) * (uu[..., 0] * uu[..., 3] - 0.5 * (uu[..., 1] ** 2 + uu[..., 2] ** 2))
+    modal = np.einsum("ia,jb,eba->eji", Vi, Vi, ind)                    # modal[e, j, i]
+    m2 = modal ** 2
+    total = m2.sum(axis=(1, 2))
+    c1 = m2[:, : n - 1, : n - 1].sum(axis=(1, 2))
+    c2 = m2[:, : n - 2, : n - 2].sum(axis=(1, 2))
+    f1 = np.where(total != 0, (total - c1) / np.where(total != 0, total, 1), 0)
+    f2 = np.where(c1 != 0, (c1 - c2) / np.where(c1 != 0, c1, 1), 0)
+    energy = np.maximum(f1, f2)
+    thr = 0.5 * 10 ** (-1.8 * n ** 0.25)
+    s = np.log((1 - 1e-4) / 1e-4)
+    a = 1 / (1 + np.exp(-s / thr * (energy - thr)))
+    a = np.where(a < alpha_min, 0.0, a)
+    a = np.where(a > 1 - alpha_min, 1.0, a)
+    return np.minimum(alpha_max, a)
+
+
+@pytest.mark.parametrize("N", [3, 4, 5])
+def test_indicator_against_numpy(oracle_mod, tl, N):
+    eq, mesh, u = _setup(tl, 3, N, tl.FourQuadrantRiemann(), lo=0.0, hi=1.0, periodic=False)
+    o = oracle_mod.Oracle(mesh, N)
+    o.set_shock_capturing(True, 0.5, 0.001, False)         # no smoothing: compare the raw indicator
+    levels, now = __import__("golden_cases").boundary_data(mesh, N, tl.FourQuadrantRiemann(), eq)
+    o.set_boundary_data(levels, now)
+    o.rhs(u, 0.0, 1e-4)
+    ref = _numpy_indicator(u, N + 1)
+    np.testing.assert_allclose(o.get(6), ref, atol=1e-12)
+    assert ref.max() > 0
+
+
+def test_indicator_zero_on_smooth_vortex(oracle_mod, tl):
+    eq, mesh, u = _setup(tl, 5, 4, tl.IsentropicVortex(5.0))
+    o = oracle_mod.Oracle(mesh, 4)
+    o.set_shock_capturing(True, 0.5)
+    o.rhs(u, 0.0, 1e-3)
+    assert o.get(6).max() == 0.0
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_shock_capturing_free_stream_and_conservation(oracle_mod, tl, kind):
+    eq, mesh, u = _setup(tl, 3, 4, tl.ConstantState(1.1, 0.2, -0.4, 0.9))
+    o = oracle_mod.Oracle(mesh, 4)
+    o.set_shock_capturing(True, 0.5)
+    assert np.abs(o.rhs(u, 0.0, 1e-3, kind=kind)).max() < 1e-12
+
+    def square(x, y, t, eq):
+        rho = np.where((np.abs(x) < 4) & (np.abs(y) < 4), 2.0, 1.0)
+        return eq.prim2cons(rho, 0.5, 0.3, 1.0)
+    eq, mesh, u = _setup(tl, 4, 4, square)
+    o = oracle_mod.Oracle(mesh, 4)
+    o.set_shock_capturing(True, 0.5)
+    du = o.rhs(u, 0.0, 1e-3, kind=kind)
+    assert o.get(6).max() > 0
+    _, w, _, _ = oracle_mod.basis(4)
+    d = du.reshape(mesh.n_elements, 5, 5, 4)
+    total = np.einsum("ejiv,j,i->v", d, w, w)
+    scale = np.einsum("ejiv,j,i->v", np.abs(d), w, w)
+    assert np.all(np.abs(total) <= 1e-13 * scale)
+
+
+def test_riemann_shock_capturing_runs_to_t025(oracle_mod, tl):
+    """Config 2 Riemann problem (32^2, N = 4, alpha_max = 0.5, CFL 0.15) stays admissible to t = 0.25."""
+    import golden_cases
+    eq, mesh, u = _setup(tl, 5, 4, tl.FourQuadrantRiemann(), lo=0.0, hi=1.0, periodic=False)
+    o = oracle_mod.Oracle(mesh, 4)
+    o.set_shock_capturing(True, 0.5)
+    o.set_boundary_data(*golden_cases.boundary_data(mesh, 4, tl.FourQuadrantRiemann(), eq))
+    s, t = o.steps(u, 100000, 0.15, 0.0, 0.25, nthreads=os.cpu_count() or 1)
+    assert abs(t - 0.25) < 1e-12
+    rho = u.reshape(-1, 4)[:, 0]
+    assert rho.min() > 0.05 and rho.max() < 2.5

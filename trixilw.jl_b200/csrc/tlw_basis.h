@@ -5,6 +5,7 @@
 #pragma once
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "tlw_device.cuh"
@@ -68,6 +69,39 @@ inline void host_build_basis(int N, Basis& B, std::vector<double>* nodes_out = n
     for (int k = 0; k < n; ++k) B.weights[k] = w[k];
     B.inv_w_first = 1.0 / w[0];
     B.inv_w_last = 1.0 / w[n - 1];
+    // inverse of V[i][m] = sqrt(m + 1/2) P_m(x_i) (Trixi vandermonde_legendre), Gauss-Jordan with pivoting
+    std::vector<double> A(n * n), I(n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int m = 0; m < n; ++m) {
+            double p = 1.0;
+            if (m >= 1) {
+                double a = 1.0, b = x[i];
+                p = x[i];
+                for (int k = 2; k <= m; ++k) {
+                    p = ((2.0 * k - 1.0) * x[i] * b - (k - 1.0) * a) / k;
+                    a = b; b = p;
+                }
+            }
+            A[i * n + m] = p * std::sqrt(m + 0.5);
+        }
+    for (int i = 0; i < n; ++i) I[i * n + i] = 1.0;
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(A[r * n + c]) > std::fabs(A[piv * n + c])) piv = r;
+        for (int k = 0; k < n; ++k) {
+            std::swap(A[c * n + k], A[piv * n + k]);
+            std::swap(I[c * n + k], I[piv * n + k]);
+        }
+        const double d = A[c * n + c];
+        for (int k = 0; k < n; ++k) { A[c * n + k] /= d; I[c * n + k] /= d; }
+        for (int r = 0; r < n; ++r)
+            if (r != c) {
+                const double f = A[r * n + c];
+                for (int k = 0; k < n; ++k) { A[r * n + k] -= f * A[c * n + k]; I[r * n + k] -= f * I[c * n + k]; }
+            }
+    }
+    for (int k = 0; k < n * n; ++k) B.Vinv[k] = I[k];
     if (nodes_out) *nodes_out = x;
 }
 

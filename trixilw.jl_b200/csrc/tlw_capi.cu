@@ -53,6 +53,12 @@ struct tlw_handle {
     double* d_us = nullptr;
     double *d_in = nullptr, *d_in2 = nullptr, *d_out = nullptr;
     double *d_tU = nullptr, *d_tF = nullptr, *d_U2 = nullptr, *d_F2 = nullptr;
+    // shock capturing
+    bool sc = false;
+    double *d_alpha = nullptr, *d_alpha_raw = nullptr, *d_tFn = nullptr;
+    int *d_il = nullptr, *d_ir = nullptr;   // all interfaces (smoothing)
+    int ni = 0;
+    double jac_first = 0.0;                 // inverse Jacobian of element 1 (TreeMesh interface cache)
     // graphs: [start buffer] one step, two steps
     cudaGraphExec_t g_one[2] = {nullptr, nullptr};
     cudaGraphExec_t g_two[2] = {nullptr, nullptr};
@@ -92,6 +98,7 @@ void free_mesh(tlw_handle* h) {
     dfree(h->d_state[0]); dfree(h->d_state[1]);
     dfree(h->d_us); dfree(h->d_in); dfree(h->d_in2); dfree(h->d_out);
     dfree(h->d_tU); dfree(h->d_tF); dfree(h->d_U2); dfree(h->d_F2);
+    dfree(h->d_alpha); dfree(h->d_alpha_raw); dfree(h->d_tFn); dfree(h->d_il); dfree(h->d_ir);
     h->have_mesh = false;
     h->have_bdata = false;
 }
@@ -100,27 +107,39 @@ void free_mesh(tlw_handle* h) {
 template <int N>
 struct Launch {
     using C = VolCfg<N>;
-    static void set_attributes() {
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(4));
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(4));
-        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
-        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
-        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
-        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(2));
+    template <bool SC>
+    static void set_attr_sc() {
+        const int lw = (int)C::smem_bytes(SC ? 8 : 4), md = (int)C::smem_bytes(SC ? 8 : 2);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
     }
-    static void volume(cudaStream_t s, int stage, int mode, const VolArgs& a) {
+    static void set_attributes() {
+        set_attr_sc<false>();
+        set_attr_sc<true>();
+    }
+    template <bool SC>
+    static void volume_sc(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
+        const size_t lw = C::smem_bytes(SC ? 8 : 4), md = C::smem_bytes(SC ? 8 : 2);
+        if (stage == TLW_STAGE_LW) {
+            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, SC><<<grid, C::THREADS, lw, s>>>(a);
+            else lw_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, lw, s>>>(a);
+        } else if (stage == TLW_STAGE_MDRK1) {
+            if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS, SC><<<grid, C::THREADS, md, s>>>(a);
+            else mdrk1_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, md, s>>>(a);
+        } else {
+            if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS, SC><<<grid, C::THREADS, md, s>>>(a);
+            else mdrk2_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, md, s>>>(a);
+        }
+    }
+    static void volume(cudaStream_t s, int stage, int mode, bool sc, const VolArgs& a) {
         const int grid = (int)((a.E + C::EB - 1) / C::EB);
         if (grid == 0) return;
-        if (stage == TLW_STAGE_LW) {
-            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
-            else lw_volume_kernel<N, MODE_STEP><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
-        } else if (stage == TLW_STAGE_MDRK1) {
-            if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(2), s>>>(a);
-            else mdrk1_volume_kernel<N, MODE_STEP><<<grid, C::THREADS, C::smem_bytes(2), s>>>(a);
-        } else {
-            if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(2), s>>>(a);
-            else mdrk2_volume_kernel<N, MODE_STEP><<<grid, C::THREADS, C::smem_bytes(2), s>>>(a);
-        }
+        if (sc) volume_sc<true>(s, stage, mode, a, grid);
+        else volume_sc<false>(s, stage, mode, a, grid);
     }
     static void interfaces(cudaStream_t s, const SurfArgs& a) {
         const long long threads = (long long)a.count * (N + 1);
@@ -132,9 +151,14 @@ struct Launch {
         if (threads == 0) return;
         boundary_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
     }
-    static void max_speed(cudaStream_t s, const double* u, const double* ij, int E, double gamma, StepState* st) {
+    // speed: CFL reduction; ind: Hennemann-Gassner indicator (both read u once)
+    static void max_speed(cudaStream_t s, const double* u, const double* ij, int E, double gamma, StepState* st,
+                          bool speed, bool ind, const IndicatorArgs& ia) {
         if (E == 0) return;
-        max_speed_kernel<N><<<(E + 255) / 256, 256, 0, s>>>(u, ij, E, gamma, st);
+        const int grid = (E + MS_ELEMS - 1) / MS_ELEMS;
+        if (speed && ind) max_speed_kernel<N, true, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia);
+        else if (speed) max_speed_kernel<N, true, false><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia);
+        else if (ind) max_speed_kernel<N, false, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia);
     }
 };
 
@@ -152,12 +176,15 @@ void dispatch(int N, A&&... args) {
     }
 }
 template <int N> struct SetAttr { static void run() { Launch<N>::set_attributes(); } };
-template <int N> struct Vol { static void run(cudaStream_t s, int st, int m, const VolArgs& a) { Launch<N>::volume(s, st, m, a); } };
+template <int N> struct Vol {
+    static void run(cudaStream_t s, int st, int m, bool sc, const VolArgs& a) { Launch<N>::volume(s, st, m, sc, a); }
+};
 template <int N> struct Ifc { static void run(cudaStream_t s, const SurfArgs& a) { Launch<N>::interfaces(s, a); } };
 template <int N> struct Bnd { static void run(cudaStream_t s, const BndArgs& a) { Launch<N>::boundaries(s, a); } };
 template <int N> struct Spd {
-    static void run(cudaStream_t s, const double* u, const double* ij, int E, double g, StepState* st) {
-        Launch<N>::max_speed(s, u, ij, E, g, st);
+    static void run(cudaStream_t s, const double* u, const double* ij, int E, double g, StepState* st, bool speed,
+                    bool ind, const IndicatorArgs& ia) {
+        Launch<N>::max_speed(s, u, ij, E, g, st, speed, ind, ia);
     }
 };
 
@@ -169,8 +196,31 @@ struct PhaseEvents {
 // One rhs (volume + surfaces) launched on h->stream.
 //   u_flux: state the volume fluxes use (u, or u* for MDRK stage 2); u_jump: u^n for the interfaces
 //   out: du (mode RHS) or the stage/updated state (mode STEP, base = u_base)
+IndicatorArgs indicator_args(tlw_handle* h) {
+    IndicatorArgs ia{};
+    ia.vinv = h->d_basis->Vinv;
+    ia.alpha_raw = h->d_alpha_raw;
+    ia.alpha = h->d_alpha;
+    ia.alpha_max = h->opts.alpha_max;
+    ia.alpha_min = h->opts.alpha_min;
+    // Trixi IndicatorHennemannGassner: threshold = 0.5 * 10^(-1.8 * nnodes^0.25), s = log((1 - 1e-4) / 1e-4)
+    ia.threshold = 0.5 * std::pow(10.0, -1.8 * std::pow((double)h->n, 0.25));
+    ia.parameter_s = std::log((1.0 - 0.0001) / 0.0001);
+    return ia;
+}
+
+// alpha of u (indicator + smoothing); with `speed` the same pass also feeds the CFL reduction
+void enqueue_indicator(tlw_handle* h, const double* u, bool speed) {
+    dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, speed, true,
+                  indicator_args(h));
+    if (h->opts.alpha_smooth && h->ni > 0)
+        alpha_smooth_kernel<<<(h->ni + 255) / 256, 256, 0, h->stream>>>(h->d_il, h->d_ir, h->ni, h->d_alpha_raw,
+                                                                        h->d_alpha);
+}
+
 void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const double* u_jump, const double* u_base,
-                 double* out, const double* dt_ptr, const PhaseEvents* ev = nullptr) {
+                 double* out, const double* dt_ptr, const PhaseEvents* ev = nullptr, bool alpha_ready = false) {
+    if (h->sc && !alpha_ready) enqueue_indicator(h, u_jump, false);   // indicator of the instantaneous u
     VolArgs va{};
     va.u = u_flux;
     va.u_base = u_base;
@@ -184,7 +234,11 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     va.basis = h->d_basis;
     va.E = (int)h->E;
     va.gamma = h->opts.gamma;
-    dispatch<Vol>(h->N, h->stream, stage, mode, va);
+    va.alpha = h->d_alpha;
+    va.tFn = h->d_tFn;
+    va.status = &h->d_step->status;
+    va.speed_kind = h->opts.max_speed;
+    dispatch<Vol>(h->N, h->stream, stage, mode, h->sc, va);
     if (ev) cudaEventRecord(ev->after_volume, h->stream);
 
     SurfArgs sa{};
@@ -201,6 +255,12 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     sa.inv_w_first = h->h_basis.inv_w_first;
     sa.inv_w_last = h->h_basis.inv_w_last;
     sa.status = &h->d_step->status;
+    sa.shock_capturing = h->sc ? 1 : 0;
+    sa.alpha = h->d_alpha;
+    sa.tFn = h->d_tFn;
+    sa.jac_first = h->jac_first;
+    sa.w_first = h->h_basis.weights[0];
+    sa.w_last = h->h_basis.weights[h->n - 1];
 
     BndArgs ba{};
     ba.u = u_jump;
@@ -241,15 +301,17 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
 void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const PhaseEvents* ev = nullptr) {
     const double* u = h->d_state[from];
     double* unew = h->d_state[1 - from];
-    dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step);
+    if (h->sc) enqueue_indicator(h, u, true);   // CFL reduction and indicator in one pass over u
+    else dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, true,
+                       false, indicator_args(h));
     finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
     if (after_dt) cudaEventRecord(after_dt, h->stream);
     const double* dtp = &h->d_step->dt;
     if (h->opts.time_discretization == TLW_LW) {
-        enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, dtp, ev);
+        enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, dtp, ev, true);
     } else {
-        enqueue_rhs(h, TLW_STAGE_MDRK1, MODE_STEP, u, u, u, h->d_us, dtp, ev);
-        enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, dtp, ev ? ev + 1 : nullptr);
+        enqueue_rhs(h, TLW_STAGE_MDRK1, MODE_STEP, u, u, u, h->d_us, dtp, ev, true);
+        enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, dtp, ev ? ev + 1 : nullptr, true);
     }
 }
 
@@ -305,6 +367,10 @@ int tlw_create(const tlw_opts* opts, tlw_handle** out) {
     if (opts->surface_flux != TLW_FLUX_RUSANOV && opts->surface_flux != TLW_FLUX_HLL) return TLW_E_ARG;
     if (opts->max_speed != TLW_SPEED_NAIVE && opts->max_speed != TLW_SPEED_DAVIS) return TLW_E_ARG;
     if (!(opts->gamma > 1.0)) return TLW_E_ARG;
+    if (opts->volume_integral != TLW_VOLUME_FR && opts->volume_integral != TLW_VOLUME_FR_SHOCK_CAPTURING) return TLW_E_ARG;
+    if (opts->volume_integral == TLW_VOLUME_FR_SHOCK_CAPTURING &&
+        !(opts->alpha_max >= 0.0 && opts->alpha_max <= 1.0 && opts->alpha_min >= 0.0 && opts->alpha_min < 0.5))
+        return TLW_E_ARG;
     tlw_handle* h = new (std::nothrow) tlw_handle();
     if (!h) return TLW_E_ARG;
     h->opts = *opts;
@@ -312,6 +378,7 @@ int tlw_create(const tlw_opts* opts, tlw_handle** out) {
     h->n = h->N + 1;
     h->nn = h->n * h->n;
     h->device = opts->device;
+    h->sc = opts->volume_integral == TLW_VOLUME_FR_SHOCK_CAPTURING;
     host_build_basis(h->N, h->h_basis, &h->nodes);
     int rc = TLW_OK;
     do {
@@ -362,7 +429,7 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
     if (n_boundaries < 0 || (n_boundaries > 0 && (!boundary_neighbor_ids || !boundary_orientations ||
                                                   !boundary_neighbor_sides || !n_boundaries_per_direction)))
         return fail(h, TLW_E_ARG, "boundaries");
-    std::vector<int> xl, xr, yl, yr;
+    std::vector<int> xl, xr, yl, yr, al, ar;
     for (int64_t k = 0; k < n_interfaces; ++k) {
         const int64_t l = interface_neighbor_ids[2 * k] - 1, r = interface_neighbor_ids[2 * k + 1] - 1;
         const int64_t o = interface_orientations[k];
@@ -370,6 +437,8 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
             return fail(h, TLW_E_ARG, "interface " + std::to_string(k + 1) + " out of range");
         (o == 1 ? xl : yl).push_back((int)l);
         (o == 1 ? xr : yr).push_back((int)r);
+        al.push_back((int)l);
+        ar.push_back((int)r);
     }
     std::vector<int> belem, bdir, bx, by;
     if (n_boundaries > 0) {
@@ -409,6 +478,11 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
         (rc = up_i(h->d_by, by)))
         return rc;
     h->nx = (int)xl.size(); h->ny = (int)yl.size();
+    h->jac_first = inverse_jacobian[0];
+    if (h->sc) {
+        if ((rc = up_i(h->d_il, al)) || (rc = up_i(h->d_ir, ar))) return rc;
+        h->ni = (int)al.size();
+    }
     h->nb = n_boundaries; h->nbx = (int)bx.size(); h->nby = (int)by.size();
     const size_t sd = state_doubles(h), td = trace_doubles(h);
     if ((rc = ensure(h, h->d_state[0], sd)) || (rc = ensure(h, h->d_state[1], sd)) || (rc = ensure(h, h->d_tU, td)) ||
@@ -416,6 +490,11 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
         return rc;
     if (h->opts.time_discretization == TLW_MDRK) {
         if ((rc = ensure(h, h->d_U2, sd)) || (rc = ensure(h, h->d_F2, 2 * sd)) || (rc = ensure(h, h->d_us, sd))) return rc;
+    }
+    if (h->sc) {
+        if ((rc = ensure(h, h->d_alpha, (size_t)h->E)) || (rc = ensure(h, h->d_alpha_raw, (size_t)h->E)) ||
+            (rc = ensure(h, h->d_tFn, td)))
+            return rc;
     }
     h->cur = 0;
     h->have_mesh = true;
@@ -486,7 +565,8 @@ int tlw_max_dt(tlw_handle* h, const double* u, int32_t where, double cfl, double
     }
     const unsigned long long zero = 0;
     TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->max_bits, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
-    dispatch<Spd>(h->N, h->stream, du_in, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step);
+    dispatch<Spd>(h->N, h->stream, du_in, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, true,
+                  false, indicator_args(h));
     TLW_CUDA(h, cudaGetLastError());
     unsigned long long bits = 0;
     TLW_CUDA(h, cudaMemcpyAsync(&bits, &h->d_step->max_bits, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
@@ -676,6 +756,8 @@ int64_t tlw_cache_size(tlw_handle* h, int32_t item) {
         case TLW_CACHE_F_TRACES: return (int64_t)trace_doubles(h);
         case TLW_CACHE_U2: return h->d_U2 ? (int64_t)state_doubles(h) : -1;
         case TLW_CACHE_F2: return h->d_F2 ? (int64_t)(2 * state_doubles(h)) : -1;
+        case TLW_CACHE_ALPHA: return h->d_alpha ? (int64_t)h->E : -1;
+        case TLW_CACHE_FN_LOW: return h->d_tFn ? (int64_t)trace_doubles(h) : -1;
         default: return -1;
     }
 }
@@ -685,7 +767,8 @@ int tlw_get_cache(tlw_handle* h, int32_t item, double* out, int32_t where) {
     const int64_t count = tlw_cache_size(h, item);
     if (count < 0) return fail(h, TLW_E_ARG, "cache item not available");
     const double* src = item == TLW_CACHE_U_TRACES ? h->d_tU : item == TLW_CACHE_F_TRACES ? h->d_tF
-                        : item == TLW_CACHE_U2 ? h->d_U2 : h->d_F2;
+                        : item == TLW_CACHE_U2 ? h->d_U2 : item == TLW_CACHE_F2 ? h->d_F2
+                        : item == TLW_CACHE_ALPHA ? h->d_alpha : h->d_tFn;
     TLW_CUDA(h, cudaSetDevice(h->device));
     const cudaMemcpyKind k = where == TLW_WHERE_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     TLW_CUDA(h, cudaMemcpyAsync(out, src, count * sizeof(double), k, h->stream));

@@ -13,6 +13,7 @@ constexpr unsigned STATUS_NONADMISSIBLE = 1u;   // sqrt of a negative number (re
 struct Basis {
     double D[16 * 16];      // derivative matrix, D[a*n + b] = l_b'(x_a)
     double Dhat[16 * 16];   // -M^{-1} D^T M
+    double Vinv[16 * 16];   // inverse Legendre Vandermonde (nodal -> normalised modal), row-major
     double weights[16];
     double inv_w_first, inv_w_last;
 };

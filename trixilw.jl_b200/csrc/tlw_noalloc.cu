@@ -59,7 +59,7 @@ std::mutex g_setup_mutex;
 template <int N>
 void set_attributes() {
     using C = VolCfg<N>;
-    cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(4));
+    cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(4));
 }
 
 // once per device, with that device current: symbol addresses (checked), bases, kernel attributes
@@ -88,7 +88,7 @@ void launch(cudaStream_t st, const VolArgs& va, SurfArgs sa, int nx, const int* 
             const int* yl, const int* yr) {
     using C = VolCfg<N>;
     const int grid = (int)((va.E + C::EB - 1) / C::EB);
-    lw_volume_kernel<N, MODE_RHS><<<grid, C::THREADS, C::smem_bytes(4), st>>>(va);
+    lw_volume_kernel<N, MODE_RHS, false><<<grid, C::THREADS, C::smem_bytes(4), st>>>(va);
     sa.left = xl; sa.right = xr; sa.count = nx; sa.orientation = 1;
     if (nx > 0) interface_kernel<N><<<(unsigned)(((long long)nx * (N + 1) + 127) / 128), 128, 0, st>>>(sa);
     sa.left = yl; sa.right = yr; sa.count = ny; sa.orientation = 2;

@@ -36,7 +36,54 @@ struct SurfArgs {
     int flux_kind, speed_kind;
     double inv_w_first, inv_w_last;
     unsigned* status;
+    // shock capturing (compute_alp, src/solvers/dgsem_tree/dg_2d.jl:1879-1901)
+    int shock_capturing;
+    const double* alpha;     // [e]
+    const double* tFn;       // first-order subcell flux next to each face [v, l, face, e]
+    double jac_first;        // J^{-1} used by the admissibility test (element 1's on TreeMesh)
+    double w_first, w_last;  // GLL weights w_1, w_n
 };
+
+__device__ __forceinline__ bool admissible(double gm1, const double* u) {
+    // is_admissible (src/equations/compressible_euler_2d.jl:4-7): rho > 0 and p > 0
+    const double v1 = u[1] / u[0], v2 = u[2] / u[0];
+    const double p = gm1 * (u[3] - 0.5 * (u[1] * v1 + u[2] * v2));
+    return u[0] > 0.0 && p > 0.0;
+}
+
+// Fn <- alp fn + (1 - alp) Fn with compute_alp (dg_2d.jl:1879-1901, 1929-1937): fn is the first-order
+// flux at the instantaneous u, alp = (alpha_L + alpha_R)/2, or 1 when the low-order update of either face
+// subcell (subcell flux next to the face from tFn, lambda = 1/2) is not admissible.
+template <int N>
+__device__ __forceinline__ void blend_interface_flux(const SurfArgs& a, int le, int re, int faceL, int faceR, int l,
+                                                     const double* uL, const double* uR, double dt, double* Fn) {
+    constexpr int n = N + 1;
+    const double gm1 = a.gamma - 1.0;
+    double fl[NV], fr[NV], fn[NV];
+    euler_flux_dir(gm1, uL, a.orientation, fl);
+    euler_flux_dir(gm1, uR, a.orientation, fr);
+    const double lam = max_abs_speed(a.gamma, uL, uR, a.orientation, a.speed_kind, a.status);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) fn[v] = 0.5 * (fl[v] + fr[v]) + (-0.5 * lam * (uR[v] - uL[v]));
+    double alp = 0.5 * (__ldg(a.alpha + le) + __ldg(a.alpha + re));
+    double Fb[NV], fil[NV], fir[NV], low[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Fb[v] = (1.0 - alp) * Fn[v] + alp * fn[v];
+    load4(a.tFn + (((size_t)le * 4 + faceL) * n + l) * NV, fil);
+    load4(a.tFn + (((size_t)re * 4 + faceR) * n + l) * NV, fir);
+    const double lamx = 0.5;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) low[v] = uL[v] - dt * a.jac_first / (a.w_last * lamx) * (Fb[v] - fil[v]);
+    if (!admissible(gm1, low)) {
+        alp = 1.0;
+    } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) low[v] = uR[v] - dt * a.jac_first / (a.w_first * lamx) * (fir[v] - Fb[v]);
+        if (!admissible(gm1, low)) alp = 1.0;
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Fn[v] = alp * fn[v] + (1.0 - alp) * Fn[v];
+}
 
 template <int N>
 __global__ void __launch_bounds__(128) interface_kernel(SurfArgs a) {
@@ -58,6 +105,7 @@ __global__ void __launch_bounds__(128) interface_kernel(SurfArgs a) {
     load4(a.tF + (((size_t)re * 4 + faceR) * n + l) * NV, FR);
     // TreeMesh argument order: surface_flux(f_ll, f_rr, U_ll, U_rr, u_ll, u_rr) (dg_2d.jl:1928)
     lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, FL, FR, UL, UR, uL, uR, a.orientation, Fn, a.status);
+    if (a.shock_capturing) blend_interface_flux<N>(a, le, re, faceL, faceR, l, uL, uR, *a.dt, Fn);
     const double dts = a.step_mode ? *a.dt : 1.0;
     const double sL = -__ldg(a.inv_jac + le) * a.inv_w_last * dts;
     const double sR = __ldg(a.inv_jac + re) * a.inv_w_first * dts;
@@ -162,38 +210,140 @@ struct StepState {
     double dt_call;                // dt for the rhs entry points (set from the host)
 };
 
-// per element: max over nodes of |v1|+c and |v2|+c, times J^{-1}; max over elements (atomic)
-template <int N>
-__global__ void __launch_bounds__(256) max_speed_kernel(const double* __restrict__ u, const double* __restrict__ inv_jac,
-                                                        int E, double gamma, StepState* s) {
-    constexpr int nn = (N + 1) * (N + 1);
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    double m = 0.0;
-    if (e < E) {
-        const double gm1 = gamma - 1.0;
-        double ml1 = 0.0, ml2 = 0.0;
-        for (int k = 0; k < nn; ++k) {
-            double x[NV];
-            load4(u + ((size_t)e * nn + k) * NV, x);
+// per element: max over nodes of |v1|+c and |v2|+c, times J^{-1}; max over elements (atomic).
+// A CTA takes MS_ELEMS consecutive elements; its threads read the nodes in order (coalesced 32-byte node
+// records), park (lambda1, lambda2) per node in shared memory, and one thread per element reduces them.
+constexpr int MS_THREADS = 256;
+constexpr int MS_ELEMS = 32;
+
+struct IndicatorArgs {
+    const double* vinv;      // inverse Legendre Vandermonde of the degree (device), row-major n x n
+    double* alpha_raw;       // [e] indicator before smoothing
+    double* alpha;           // [e] blending factor (smoothed afterwards)
+    double alpha_max, alpha_min, threshold, parameter_s;
+};
+
+template <int N, bool SPEED, bool IND>
+__global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const double* __restrict__ u,
+                                                               const double* __restrict__ inv_jac, int E,
+                                                               double gamma, StepState* s, IndicatorArgs ia) {
+    constexpr int n = N + 1;
+    constexpr int nn = n * n;
+    __shared__ double l1s[MS_ELEMS * nn], l2s[MS_ELEMS * nn];
+    __shared__ double wmax[MS_THREADS / 32];
+    const int e0 = blockIdx.x * MS_ELEMS;
+    const int ne = min(MS_ELEMS, E - e0);
+    const double gm1 = gamma - 1.0;
+    for (int k = threadIdx.x; k < ne * nn; k += MS_THREADS) {
+        double x[NV];
+        load4(u + ((size_t)e0 * nn + k) * NV, x);
+        if (SPEED) {
             const double ir = 1.0 / x[0];
             const double v1 = x[1] * ir, v2 = x[2] * ir;
             const double p = gm1 * (x[3] - 0.5 * (x[1] * v1 + x[2] * v2));
             const double c = checked_sqrt(gamma * p * ir, &s->status);
-            ml1 = fmax(ml1, fabs(v1) + c);
-            ml2 = fmax(ml2, fabs(v2) + c);
+            l1s[k] = fabs(v1) + c;
+            l2s[k] = fabs(v2) + c;
+        } else {
+            // indicator variable density_pressure = (gamma - 1)(rho rho_e - |rho v|^2 / 2)
+            l1s[k] = gm1 * (x[0] * x[3] - 0.5 * (x[1] * x[1] + x[2] * x[2]));
         }
-        m = __ldg(inv_jac + e) * (ml1 + ml2);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    __shared__ double wmax[8];
-    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double b = wmax[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, wmax[w]);
-        if (b > 0.0) atomicMax(&s->max_bits, (unsigned long long)__double_as_longlong(b));
+    double m = 0.0;
+    if (threadIdx.x < ne) {
+        const int e = e0 + threadIdx.x;
+        if (SPEED) {
+            double ml1 = 0.0, ml2 = 0.0;
+            for (int k = 0; k < nn; ++k) {
+                ml1 = fmax(ml1, l1s[threadIdx.x * nn + k]);
+                ml2 = fmax(ml2, l2s[threadIdx.x * nn + k]);
+            }
+            m = __ldg(inv_jac + e) * (ml1 + ml2);
+        }
+        if (IND) {
+            // Hennemann-Gassner indicator (Trixi IndicatorHennemannGassner): modal energy of density_pressure
+            double ind[nn];
+            if (SPEED) {
+                for (int k = 0; k < nn; ++k) {
+                    double x[NV];
+                    load4(u + ((size_t)e * nn + k) * NV, x);
+                    ind[k] = gm1 * (x[0] * x[3] - 0.5 * (x[1] * x[1] + x[2] * x[2]));
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < nn; ++k) ind[k] = l1s[threadIdx.x * nn + k];
+            }
+            const double* Vi = ia.vinv;   // row-major n x n
+            double tmp[nn], md[nn];
+#pragma unroll
+            for (int jj = 0; jj < n; ++jj)
+#pragma unroll
+                for (int ii = 0; ii < n; ++ii) {
+                    double r = 0.0;
+#pragma unroll
+                    for (int q = 0; q < n; ++q) r += Vi[ii * n + q] * ind[q + n * jj];
+                    tmp[ii + n * jj] = r;
+                }
+#pragma unroll
+            for (int jj = 0; jj < n; ++jj)
+#pragma unroll
+                for (int ii = 0; ii < n; ++ii) {
+                    double r = 0.0;
+#pragma unroll
+                    for (int q = 0; q < n; ++q) r += Vi[jj * n + q] * tmp[ii + n * q];
+                    md[ii + n * jj] = r;
+                }
+            double total = 0.0, clip1 = 0.0, clip2 = 0.0;
+#pragma unroll
+            for (int jj = 0; jj < n; ++jj)
+#pragma unroll
+                for (int ii = 0; ii < n; ++ii) {
+                    const double q2 = md[ii + n * jj] * md[ii + n * jj];
+                    total += q2;
+                }
+#pragma unroll
+            for (int jj = 0; jj < n - 1; ++jj)
+#pragma unroll
+                for (int ii = 0; ii < n - 1; ++ii) clip1 += md[ii + n * jj] * md[ii + n * jj];
+#pragma unroll
+            for (int jj = 0; jj < n - 2; ++jj)
+#pragma unroll
+                for (int ii = 0; ii < n - 2; ++ii) clip2 += md[ii + n * jj] * md[ii + n * jj];
+            const double f1 = total != 0.0 ? (total - clip1) / total : 0.0;
+            const double f2 = clip1 != 0.0 ? (clip1 - clip2) / clip1 : 0.0;
+            const double energy = fmax(f1, f2);
+            double al = 1.0 / (1.0 + exp(-ia.parameter_s / ia.threshold * (energy - ia.threshold)));
+            if (al < ia.alpha_min) al = 0.0;
+            if (al > 1.0 - ia.alpha_min) al = 1.0;
+            al = fmin(ia.alpha_max, al);
+            ia.alpha_raw[e] = al;
+            ia.alpha[e] = al;
+        }
     }
+    if (SPEED) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = wmax[0];
+            for (int w = 1; w < MS_THREADS / 32; ++w) b = fmax(b, wmax[w]);
+            if (b > 0.0) atomicMax(&s->max_bits, (unsigned long long)__double_as_longlong(b));
+        }
+    }
+}
+
+// Trixi apply_smoothing! (TreeMesh{2}): alpha_e = max(alpha_e, alpha_raw_nb / 2) over the interfaces,
+// independent of the order (max over non-negative doubles = max over their bit patterns)
+static __global__ void alpha_smooth_kernel(const int* __restrict__ left, const int* __restrict__ right, int count,
+                                    const double* __restrict__ alpha_raw, double* alpha) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int l = __ldg(left + k), r = __ldg(right + k);
+    unsigned long long* ab = reinterpret_cast<unsigned long long*>(alpha);
+    atomicMax(ab + l, (unsigned long long)__double_as_longlong(0.5 * __ldg(alpha_raw + r)));
+    atomicMax(ab + r, (unsigned long long)__double_as_longlong(0.5 * __ldg(alpha_raw + l)));
 }
 
 // dt = cfl * 2 / (n * max_scaled_speed), clamped so that t + dt <= t_end; a finished run gets dt = 0

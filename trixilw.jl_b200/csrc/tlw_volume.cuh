@@ -30,17 +30,24 @@ namespace tlw {
 // that launches these kernels uploads its copy with upload_const_basis() on each device it uses.
 static __constant__ double c_tlw_D[8][64];
 static __constant__ double c_tlw_Dhat[8][64];
+static __constant__ double c_tlw_Vinv[8][64];
+static __constant__ double c_tlw_w[8][8];       // GLL weights
 
 static inline cudaError_t upload_const_basis(const Basis* bases /* [8], index = N */) {
-    static double d[8][64], dh[8][64];
-    for (int N = 0; N < 8; ++N)
+    static double d[8][64], dh[8][64], vi[8][64], w[8][8];
+    for (int N = 0; N < 8; ++N) {
         for (int k = 0; k < 64; ++k) {
             d[N][k] = bases[N].D[k];
             dh[N][k] = bases[N].Dhat[k];
+            vi[N][k] = bases[N].Vinv[k];
         }
+        for (int k = 0; k < 8; ++k) w[N][k] = bases[N].weights[k];
+    }
     cudaError_t e = cudaMemcpyToSymbol(c_tlw_D, d, sizeof(d));
-    if (e != cudaSuccess) return e;
-    return cudaMemcpyToSymbol(c_tlw_Dhat, dh, sizeof(dh));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_Dhat, dh, sizeof(dh));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_Vinv, vi, sizeof(vi));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_w, w, sizeof(w));
+    return e;
 }
 
 template <int N>
@@ -58,7 +65,8 @@ struct VolCfg {
     static constexpr int P = n == 4 ? 19 : nn;
     static constexpr int PLANES = 4 * EB * P;          // doubles of one 4-variable field
     static constexpr int LINES = 4 * n * EB;           // (variable, element, line index)
-    // regions: X (f / x-results), Y (g / y-results), F0X, F0Y (fluxes at u, kept for stages 2 and 4)
+    // regions: X (f / x-results), Y (g / y-results), F0X, F0Y (fluxes at u, kept for stages 2 and 4);
+    // shock capturing adds UU (u), VC (v1, v2, c), FVX, FVY (first-order subcell fluxes)
     static constexpr size_t smem_bytes(int regions) { return (size_t)regions * PLANES * sizeof(double); }
 };
 
@@ -77,6 +85,11 @@ struct VolArgs {
     const Basis* basis;
     int E;
     double gamma;
+    // shock capturing (VolumeIntegralFRShockCapturing, first-order subcells)
+    const double* alpha;    // blending factor per element
+    double* tFn;            // first-order subcell flux next to each face [v, l, face, e] (fn_low)
+    unsigned* status;
+    int speed_kind;
 };
 
 // owner: store the node's f (into X) and g (into Y)
@@ -146,6 +159,100 @@ __device__ __forceinline__ void line_contract(double* X, double* Y, int tid) {
     }
 }
 
+// ---- shock capturing helpers (src/solvers/dgsem_tree/dg_2d.jl:251-282, 1948-1991; Trixi calcflux_fv!) ----
+// stage 0: park u and (v1, v2, c) of the node for the first-order subcell fluxes of its neighbours
+template <int N>
+__device__ __forceinline__ void sc_park(double* UU, double* VC, int el, int i, int j, const double* u, double gamma,
+                                        unsigned* status) {
+    const double ir = 1.0 / u[0];
+    const double v1 = u[1] * ir, v2 = u[2] * ir;
+    const double p = (gamma - 1.0) * (u[3] - 0.5 * (u[1] * v1 + u[2] * v2));
+    const double c = checked_sqrt(gamma * p * ir, status);
+    const double vc[NV] = {v1, v2, c, 0.0};
+    node_put<N>(UU, VC, el, i, j, u, vc);
+}
+
+// Rusanov (Trixi flux_lax_friedrichs, 4 arguments) between node L and node R of one element, from the
+// parked states, fluxes (fx: x-fluxes if orientation 1, else y-fluxes) and speeds
+template <int N>
+__device__ __forceinline__ void sc_face_flux(const double* UU, const double* VC, const double* FL, int el, int iL,
+                                             int jL, int iR, int jR, int orientation, int speed_kind, double* out) {
+    using C = VolCfg<N>;
+    const int aL = el * C::P + iL + C::R * jL, aR = el * C::P + iR + C::R * jR;
+    constexpr int PV = C::EB * C::P;   // stride between variable planes
+    const double vL = VC[(orientation == 1 ? 0 : PV) + aL], vR = VC[(orientation == 1 ? 0 : PV) + aR];
+    const double cL = VC[2 * PV + aL], cR = VC[2 * PV + aR];
+    const double lambda = speed_kind == 0 ? fmax(fabs(vL), fabs(vR)) + fmax(cL, cR)
+                                          : fmax(fabs(vL) + cL, fabs(vR) + cR);
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+        out[v] = 0.5 * (FL[v * PV + aL] + FL[v * PV + aR]) + (-0.5 * lambda * (UU[v * PV + aR] - UU[v * PV + aL]));
+}
+
+// final stage: each node computes the subcell flux on its left (x) and lower (y) subcell face
+template <int N>
+__device__ __forceinline__ void sc_faces(const double* UU, const double* VC, const double* F0X, const double* F0Y,
+                                         double* FVX, double* FVY, int el, int i, int j, int speed_kind) {
+    using C = VolCfg<N>;
+    constexpr int PV = C::EB * C::P;
+    const int a = el * C::P + i + C::R * j;
+    double f[NV];
+    if (i >= 1) {
+        sc_face_flux<N>(UU, VC, F0X, el, i - 1, j, i, j, 1, speed_kind, f);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) FVX[v * PV + a] = f[v];
+    }
+    if (j >= 1) {
+        sc_face_flux<N>(UU, VC, F0Y, el, i, j - 1, i, j, 2, speed_kind, f);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) FVY[v * PV + a] = f[v];
+    }
+}
+
+// epilogue: fv = w_i^-1 (f*_{i+1/2} - f*_{i-1/2}) + w_j^-1 (g*_{j+1/2} - g*_{j-1/2}) (element-boundary
+// subcell fluxes are zero); acc <- (1 - alpha) acc + alpha fv; fn_low traces of the four faces
+template <int N>
+__device__ __forceinline__ void sc_blend(const VolArgs& a, const double* FVX, const double* FVY, int el, int e, int i,
+                                         int j, double alpha, double* acc) {
+    using C = VolCfg<N>;
+    constexpr int n = C::n;
+    constexpr int PV = C::EB * C::P;
+    const int base = el * C::P;
+    const double iwi = 1.0 / c_tlw_w[N][i], iwj = 1.0 / c_tlw_w[N][j];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const double xr = i + 1 < n ? FVX[v * PV + base + (i + 1) + C::R * j] : 0.0;
+        const double xl = i >= 1 ? FVX[v * PV + base + i + C::R * j] : 0.0;
+        const double yt = j + 1 < n ? FVY[v * PV + base + i + C::R * (j + 1)] : 0.0;
+        const double yb = j >= 1 ? FVY[v * PV + base + i + C::R * j] : 0.0;
+        const double fv = iwi * (xr - xl) + iwj * (yt - yb);
+        acc[v] = (1.0 - alpha) * acc[v] + alpha * fv;
+    }
+    // fn_low [v, l, face, e]: faces -x, +x use the subcell faces between nodes 0|1 and n-2|n-1 of row j
+    const size_t tb = (size_t)e * 4 * n * NV;
+    double f[NV];
+    if (i == 1) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = FVX[v * PV + base + 1 + C::R * j];
+        store4(a.tFn + tb + (0 * n + j) * NV, f);
+    }
+    if (i == n - 1) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = FVX[v * PV + base + (n - 1) + C::R * j];
+        store4(a.tFn + tb + (1 * n + j) * NV, f);
+    }
+    if (j == 1) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = FVY[v * PV + base + i + C::R * 1];
+        store4(a.tFn + tb + (2 * n + i) * NV, f);
+    }
+    if (j == n - 1) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = FVY[v * PV + base + i + C::R * (n - 1)];
+        store4(a.tFn + tb + (3 * n + i) * NV, f);
+    }
+}
+
 // out/traces epilogue shared by all volume kernels. acc = Dhat-contraction of (F, G).
 template <int n, int MODE>
 __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, int j, int node, double ij, double dt,
@@ -180,7 +287,7 @@ __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, 
 //   depth 3: f_t = raw1/12, f_tt = raw2,    f_ttt = raw3/2
 //   depth 2: f_t = raw1/2,  f_tt = raw2;    depth 1: f_t = raw1/2
 // ------------------------------------------------------------------------------------------------
-template <int N, int MODE>
+template <int N, int MODE, bool SC>
 __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
@@ -194,6 +301,10 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
     double* Y = X + C::PLANES;
     double* F0X = Y + C::PLANES;
     double* F0Y = F0X + C::PLANES;
+    double* UU = F0Y + C::PLANES;      // shock capturing only
+    double* VC = UU + C::PLANES;
+    double* FVX = VC + C::PLANES;
+    double* FVY = FVX + C::PLANES;
 
     const int tid = threadIdx.x;
     const double dt = *a.dt;
@@ -214,7 +325,8 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
         s0 = -dt * ij;
         euler_fluxes(gm1, uu[0], uu[1], uu[2], uu[3], f, g);
         node_put<N>(X, Y, el, i, j, f, g);
-        if (DEPTH >= 2) node_put<N>(F0X, F0Y, el, i, j, f, g);
+        if (DEPTH >= 2 || SC) node_put<N>(F0X, F0Y, el, i, j, f, g);
+        if (SC) sc_park<N>(UU, VC, el, i, j, uu, a.gamma, a.status);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             F[v] = f[v]; G[v] = g[v]; U[v] = uu[v];
@@ -396,13 +508,17 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
     }
     // final: Dhat contraction of the time-averaged fluxes (every owner has read its node's results of
     // the last contraction before writing F, G over them: same address, same thread)
-    if (active) node_put<N>(X, Y, el, i, j, F, G);
+    if (active) {
+        node_put<N>(X, Y, el, i, j, F, G);
+        if (SC) sc_faces<N>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
+    }
     __syncthreads();
     line_contract<N, true>(X, Y, tid);
     __syncthreads();
     if (active) {
         double acc[NV];
         node_sum<N>(X, Y, el, i, j, acc);
+        if (SC) sc_blend<N>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
     }
 }
@@ -411,13 +527,19 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
 // MDRK stage 1 (mdrk_kernel_1!, multi_derivative_2d.jl:263-421): F = f/2 + f_t/8, U = u/2 + u_t/8,
 // F2 = f + f_t/6, U2 = u + u_t/6 (stored whole for stage 2).
 // ------------------------------------------------------------------------------------------------
-template <int N, int MODE>
+template <int N, int MODE, bool SC>
 __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk1_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
     double* X = smem_d;
     double* Y = X + C::PLANES;
+    double* F0X = Y + C::PLANES;       // shock capturing only: fluxes, u, speeds at u^n, subcell fluxes
+    double* F0Y = F0X + C::PLANES;
+    double* UU = F0Y + C::PLANES;
+    double* VC = UU + C::PLANES;
+    double* FVX = VC + C::PLANES;
+    double* FVY = FVX + C::PLANES;
     const int tid = threadIdx.x;
     const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
@@ -432,6 +554,11 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
         ij = __ldg(a.inv_jac + e);
         euler_fluxes(gm1, uu[0], uu[1], uu[2], uu[3], f0, g0);
         node_put<N>(X, Y, el, i, j, f0, g0);
+        if (SC) {
+            // the subcell FV part uses the instantaneous u^n (multi_derivative_2d.jl:205)
+            node_put<N>(F0X, F0Y, el, i, j, f0, g0);
+            sc_park<N>(UU, VC, el, i, j, uu, a.gamma, a.status);
+        }
     }
     __syncthreads();
     line_contract<N, false>(X, Y, tid);
@@ -472,6 +599,7 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
         store4(a.F2 + off * 2 * NV, F2v);
         store4(a.F2 + off * 2 * NV + NV, G2v);
         node_put<N>(X, Y, el, i, j, F, G);
+        if (SC) sc_faces<N>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
     }
     __syncthreads();
     line_contract<N, true>(X, Y, tid);
@@ -479,6 +607,7 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
     if (active) {
         double acc[NV];
         node_sum<N>(X, Y, el, i, j, acc);
+        if (SC) sc_blend<N>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
     }
 }
@@ -487,13 +616,19 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
 // MDRK stage 2 (mdrk_kernel_2!, multi_derivative_2d.jl:423-555): at u* = a.u,
 // F = F2 + f_t(u*)/3, U = U2 + u*_t/3.
 // ------------------------------------------------------------------------------------------------
-template <int N, int MODE>
+template <int N, int MODE, bool SC>
 __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk2_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
     double* X = smem_d;
     double* Y = X + C::PLANES;
+    double* F0X = Y + C::PLANES;       // shock capturing only: fluxes, u, speeds at u^n, subcell fluxes
+    double* F0Y = F0X + C::PLANES;
+    double* UU = F0Y + C::PLANES;
+    double* VC = UU + C::PLANES;
+    double* FVX = VC + C::PLANES;
+    double* FVY = FVX + C::PLANES;
     const int tid = threadIdx.x;
     const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
@@ -509,6 +644,14 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
         ij = __ldg(a.inv_jac + e);
         euler_fluxes(gm1, us[0], us[1], us[2], us[3], f, g);
         node_put<N>(X, Y, el, i, j, f, g);
+        if (SC) {
+            // the subcell FV part uses the instantaneous u^n, not u* (multi_derivative_2d.jl:257)
+            double un[NV], fn0[NV], gn0[NV];
+            load4(a.u_base + ((size_t)e * nn + node) * NV, un);
+            euler_fluxes(gm1, un[0], un[1], un[2], un[3], fn0, gn0);
+            node_put<N>(F0X, F0Y, el, i, j, fn0, gn0);
+            sc_park<N>(UU, VC, el, i, j, un, a.gamma, a.status);
+        }
     }
     __syncthreads();
     line_contract<N, false>(X, Y, tid);
@@ -546,6 +689,7 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
             U[v] = fma(1.0 / 3.0, d[v], U2v[v]);
         }
         node_put<N>(X, Y, el, i, j, F, G);
+        if (SC) sc_faces<N>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
     }
     __syncthreads();
     line_contract<N, true>(X, Y, tid);
@@ -553,6 +697,7 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
     if (active) {
         double acc[NV];
         node_sum<N>(X, Y, el, i, j, acc);
+        if (SC) sc_blend<N>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
     }
 }

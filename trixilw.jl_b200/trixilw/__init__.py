@@ -7,7 +7,8 @@ from .equations import (CompressibleEulerEquations2D, ConstantState, DensityWave
 from .lwfr import LWIntegrator, LWSolution, l2_linf_errors, solve_lwfr
 from .mesh import TreeMesh
 from .semidiscretization import (LW, MDRK, DGSEM, Adaptive, BoundaryConditionDirichlet, CFLBased, FluxHLL,
-                                 FluxLaxFriedrichs, SemidiscretizationHyperbolic, VolumeIntegralFR,
+                                 FluxLaxFriedrichs, IndicatorHennemannGassner, SemidiscretizationHyperbolic,
+                                 VolumeIntegralFR, VolumeIntegralFRShockCapturing,
                                  boundary_condition_periodic, flux_hll, flux_lax_friedrichs,
                                  get_time_discretization, lw_fourier_cfl, rhs, rhs_mdrk1, rhs_mdrk2,
                                  semidiscretize, trixi2lw)
@@ -16,7 +17,8 @@ __all__ = [
     "DomainError", "TlwError", "lib", "CompressibleEulerEquations2D", "ConstantState", "DensityWave",
     "FourQuadrantRiemann", "IsentropicVortex", "LWIntegrator", "LWSolution", "l2_linf_errors", "solve_lwfr",
     "TreeMesh", "LW", "MDRK", "DGSEM", "Adaptive", "BoundaryConditionDirichlet", "CFLBased", "FluxHLL",
-    "FluxLaxFriedrichs", "SemidiscretizationHyperbolic", "VolumeIntegralFR", "boundary_condition_periodic",
+    "FluxLaxFriedrichs", "IndicatorHennemannGassner", "SemidiscretizationHyperbolic", "VolumeIntegralFR",
+    "VolumeIntegralFRShockCapturing", "boundary_condition_periodic",
     "flux_hll", "flux_lax_friedrichs", "get_time_discretization", "lw_fourier_cfl", "rhs", "rhs_mdrk1",
     "rhs_mdrk2", "semidiscretize", "trixi2lw",
 ]

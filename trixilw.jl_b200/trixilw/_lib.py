@@ -24,7 +24,8 @@ TLW_FLUX_RUSANOV, TLW_FLUX_HLL = 0, 1
 TLW_SPEED_NAIVE, TLW_SPEED_DAVIS = 0, 1
 TLW_WHERE_HOST, TLW_WHERE_DEVICE = 0, 1
 TLW_STAGE_LW, TLW_STAGE_MDRK1, TLW_STAGE_MDRK2 = 0, 1, 2
-TLW_CACHE_U_TRACES, TLW_CACHE_F_TRACES, TLW_CACHE_U2, TLW_CACHE_F2 = 0, 1, 2, 3
+TLW_CACHE_U_TRACES, TLW_CACHE_F_TRACES, TLW_CACHE_U2, TLW_CACHE_F2, TLW_CACHE_ALPHA, TLW_CACHE_FN_LOW = 0, 1, 2, 3, 4, 5
+TLW_VOLUME_FR, TLW_VOLUME_FR_SHOCK_CAPTURING = 0, 1
 
 # every symbol include/tlw.h declares
 EXPORTED = (
@@ -43,7 +44,11 @@ class TlwOpts(ctypes.Structure):
         ("max_speed", ctypes.c_int32),
         ("gamma", ctypes.c_double),
         ("device", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("volume_integral", ctypes.c_int32),
+        ("alpha_max", ctypes.c_double),
+        ("alpha_min", ctypes.c_double),
+        ("alpha_smooth", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 

@@ -80,10 +80,43 @@ flux_hll = FluxHLL()
 
 
 @dataclass
+class IndicatorHennemannGassner:
+    """Trixi IndicatorHennemannGassner(equations, basis; alpha_max, alpha_min, alpha_smooth, variable);
+    only variable = density_pressure is built."""
+    alpha_max: float = 0.5
+    alpha_min: float = 0.001
+    alpha_smooth: bool = True
+    variable: str = "density_pressure"
+
+    def __post_init__(self):
+        if self.variable != "density_pressure":
+            raise NotImplementedError("only the density_pressure indicator variable is built")
+
+
+@dataclass
+class VolumeIntegralFRShockCapturing:
+    """VolumeIntegralFRShockCapturing(indicator; volume_integralFR, volume_flux_fv, reconstruction)
+    (src/solvers/fr.jl:59-86). Built: volume_flux_fv = flux_lax_friedrichs and
+    reconstruction = FirstOrderReconstruction()."""
+    indicator: IndicatorHennemannGassner = field(default_factory=IndicatorHennemannGassner)
+    volume_integralFR: VolumeIntegralFR = field(default_factory=VolumeIntegralFR)
+    volume_flux_fv: object = field(default_factory=FluxLaxFriedrichs)
+    reconstruction: str = "FirstOrderReconstruction"
+
+    def __post_init__(self):
+        if self.reconstruction != "FirstOrderReconstruction":
+            raise NotImplementedError("only FirstOrderReconstruction subcells are built")
+
+    @property
+    def time_discretization(self):
+        return self.volume_integralFR.time_discretization
+
+
+@dataclass
 class DGSEM:
     polydeg: int
     surface_flux: object = field(default_factory=FluxLaxFriedrichs)
-    volume_integral: VolumeIntegralFR = field(default_factory=VolumeIntegralFR)
+    volume_integral: object = field(default_factory=VolumeIntegralFR)
 
 
 def get_time_discretization(solver: DGSEM):
@@ -178,6 +211,14 @@ class SemidiscretizationHyperbolic:
         opts.max_speed = _lib.TLW_SPEED_DAVIS if getattr(sf, "max_abs_speed", "naive") == "davis" else _lib.TLW_SPEED_NAIVE
         opts.gamma = equations.gamma
         opts.device = device
+        vi = solver.volume_integral
+        if isinstance(vi, VolumeIntegralFRShockCapturing):
+            opts.volume_integral = _lib.TLW_VOLUME_FR_SHOCK_CAPTURING
+            opts.alpha_max = vi.indicator.alpha_max
+            opts.alpha_min = vi.indicator.alpha_min
+            opts.alpha_smooth = 1 if vi.indicator.alpha_smooth else 0
+        else:
+            opts.volume_integral = _lib.TLW_VOLUME_FR
         self._handle = _Handle(opts)
         self._upload_mesh()
         self._bdata_key = None
@@ -296,7 +337,8 @@ def semidiscretize(semi: SemidiscretizationHyperbolic, time_discretization, tspa
 
 
 __all__ = [
-    "LW", "MDRK", "CFLBased", "Adaptive", "VolumeIntegralFR", "DGSEM", "FluxLaxFriedrichs", "FluxHLL",
+    "LW", "MDRK", "CFLBased", "Adaptive", "VolumeIntegralFR", "VolumeIntegralFRShockCapturing",
+    "IndicatorHennemannGassner", "DGSEM", "FluxLaxFriedrichs", "FluxHLL",
     "flux_lax_friedrichs", "flux_hll", "BoundaryConditionDirichlet", "boundary_condition_periodic",
     "SemidiscretizationHyperbolic", "semidiscretize", "rhs", "rhs_mdrk1", "rhs_mdrk2", "lw_fourier_cfl",
     "trixi2lw", "get_time_discretization", "DomainError", "LWUpdate",
