@@ -155,7 +155,7 @@ struct Launch {
     static void max_speed(cudaStream_t s, const double* u, const double* ij, int E, double gamma, StepState* st,
                           bool speed, bool ind, const IndicatorArgs& ia) {
         if (E == 0) return;
-        const int grid = (E + MS_ELEMS - 1) / MS_ELEMS;
+        const int grid = (E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS;
         if (speed && ind) max_speed_kernel<N, true, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia);
         else if (speed) max_speed_kernel<N, true, false><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia);
         else if (ind) max_speed_kernel<N, false, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia);
@@ -198,7 +198,6 @@ struct PhaseEvents {
 //   out: du (mode RHS) or the stage/updated state (mode STEP, base = u_base)
 IndicatorArgs indicator_args(tlw_handle* h) {
     IndicatorArgs ia{};
-    ia.vinv = h->d_basis->Vinv;
     ia.alpha_raw = h->d_alpha_raw;
     ia.alpha = h->d_alpha;
     ia.alpha_max = h->opts.alpha_max;

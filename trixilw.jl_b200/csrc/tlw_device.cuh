@@ -18,6 +18,30 @@ struct Basis {
     double inv_w_first, inv_w_last;
 };
 
+// Derivative matrices per degree (index N), row-major n x n in 64 slots. Static: every translation unit
+// that launches these kernels uploads its copy with upload_const_basis() on each device it uses.
+static __constant__ double c_tlw_D[8][64];
+static __constant__ double c_tlw_Dhat[8][64];
+static __constant__ double c_tlw_Vinv[8][64];
+static __constant__ double c_tlw_w[8][8];       // GLL weights
+
+static inline cudaError_t upload_const_basis(const Basis* bases /* [8], index = N */) {
+    static double d[8][64], dh[8][64], vi[8][64], w[8][8];
+    for (int N = 0; N < 8; ++N) {
+        for (int k = 0; k < 64; ++k) {
+            d[N][k] = bases[N].D[k];
+            dh[N][k] = bases[N].Dhat[k];
+            vi[N][k] = bases[N].Vinv[k];
+        }
+        for (int k = 0; k < 8; ++k) w[N][k] = bases[N].weights[k];
+    }
+    cudaError_t e = cudaMemcpyToSymbol(c_tlw_D, d, sizeof(d));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_Dhat, dh, sizeof(dh));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_Vinv, vi, sizeof(vi));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_w, w, sizeof(w));
+    return e;
+}
+
 // Reciprocal by Newton-Raphson refinement of the hardware approximation (rcp.approx.ftz.f64, about 20
 // correct bits): two steps y <- y + y (1 - x y) square the relative error twice, so the result is within
 // one ulp of 1/x for normal x (Newton's method for f(y) = 1/y - x; e.g. P. Markstein, IBM J. Res. Dev. 34

@@ -210,29 +210,37 @@ struct StepState {
     double dt_call;                // dt for the rhs entry points (set from the host)
 };
 
-// per element: max over nodes of |v1|+c and |v2|+c, times J^{-1}; max over elements (atomic).
-// A CTA takes MS_ELEMS consecutive elements; its threads read the nodes in order (coalesced 32-byte node
-// records), park (lambda1, lambda2) per node in shared memory, and one thread per element reduces them.
 constexpr int MS_THREADS = 256;
-constexpr int MS_ELEMS = 32;
+template <int N>
+struct MsCfg {
+    static constexpr int n = N + 1, nn = n * n;
+    static constexpr int ELEMS = N >= 6 ? 16 : 32;   // elements per CTA (shared memory: 4 x ELEMS x nn doubles)
+};
 
 struct IndicatorArgs {
-    const double* vinv;      // inverse Legendre Vandermonde of the degree (device), row-major n x n
     double* alpha_raw;       // [e] indicator before smoothing
     double* alpha;           // [e] blending factor (smoothed afterwards)
     double alpha_max, alpha_min, threshold, parameter_s;
 };
 
+// One pass over u for the CFL reduction (SPEED) and/or the Hennemann-Gassner indicator (IND).
+// The CTA reads its elements' nodes in order (coalesced 32-byte node records) into shared memory.
+//  SPEED: per element max over nodes of |v1|+c and |v2|+c, times J^{-1}; max over elements (atomic).
+//  IND:   Trixi IndicatorHennemannGassner with variable density_pressure: modal = Vinv ind Vinv^T by
+//         eight threads per element (constant-memory Vinv), energy fractions of the highest modes,
+//         logistic map, alpha_min / alpha_max clipping (Hennemann et al., J. Comput. Phys. 426 (2021)).
 template <int N, bool SPEED, bool IND>
 __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const double* __restrict__ u,
                                                                const double* __restrict__ inv_jac, int E,
                                                                double gamma, StepState* s, IndicatorArgs ia) {
     constexpr int n = N + 1;
     constexpr int nn = n * n;
-    __shared__ double l1s[MS_ELEMS * nn], l2s[MS_ELEMS * nn];
+    constexpr int ELEMS = MsCfg<N>::ELEMS;
+    __shared__ double l1s[SPEED ? ELEMS * nn : 1], l2s[SPEED ? ELEMS * nn : 1];
+    __shared__ double inds[IND ? ELEMS * nn : 1], tmps[IND ? ELEMS * nn : 1];
     __shared__ double wmax[MS_THREADS / 32];
-    const int e0 = blockIdx.x * MS_ELEMS;
-    const int ne = min(MS_ELEMS, E - e0);
+    const int e0 = blockIdx.x * ELEMS;
+    const int ne = min(ELEMS, E - e0);
     const double gm1 = gamma - 1.0;
     for (int k = threadIdx.x; k < ne * nn; k += MS_THREADS) {
         double x[NV];
@@ -244,81 +252,64 @@ __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const double* __r
             const double c = checked_sqrt(gamma * p * ir, &s->status);
             l1s[k] = fabs(v1) + c;
             l2s[k] = fabs(v2) + c;
-        } else {
-            // indicator variable density_pressure = (gamma - 1)(rho rho_e - |rho v|^2 / 2)
-            l1s[k] = gm1 * (x[0] * x[3] - 0.5 * (x[1] * x[1] + x[2] * x[2]));
         }
+        // indicator variable density_pressure = (gamma - 1)(rho rho_e - |rho v|^2 / 2)
+        if (IND) inds[k] = gm1 * (x[0] * x[3] - 0.5 * (x[1] * x[1] + x[2] * x[2]));
     }
     __syncthreads();
     double m = 0.0;
-    if (threadIdx.x < ne) {
-        const int e = e0 + threadIdx.x;
-        if (SPEED) {
-            double ml1 = 0.0, ml2 = 0.0;
-            for (int k = 0; k < nn; ++k) {
-                ml1 = fmax(ml1, l1s[threadIdx.x * nn + k]);
-                ml2 = fmax(ml2, l2s[threadIdx.x * nn + k]);
-            }
-            m = __ldg(inv_jac + e) * (ml1 + ml2);
+    if (SPEED && threadIdx.x < ne) {
+        double ml1 = 0.0, ml2 = 0.0;
+        for (int k = 0; k < nn; ++k) {
+            ml1 = fmax(ml1, l1s[threadIdx.x * nn + k]);
+            ml2 = fmax(ml2, l2s[threadIdx.x * nn + k]);
         }
-        if (IND) {
-            // Hennemann-Gassner indicator (Trixi IndicatorHennemannGassner): modal energy of density_pressure
-            double ind[nn];
-            if (SPEED) {
-                for (int k = 0; k < nn; ++k) {
-                    double x[NV];
-                    load4(u + ((size_t)e * nn + k) * NV, x);
-                    ind[k] = gm1 * (x[0] * x[3] - 0.5 * (x[1] * x[1] + x[2] * x[2]));
-                }
-            } else {
+        m = __ldg(inv_jac + e0 + threadIdx.x) * (ml1 + ml2);
+    }
+    if (IND) {
+        const int el = threadIdx.x >> 3, q = threadIdx.x & 7;
+        const double* Vi = c_tlw_Vinv[N];
+        // tmp = Vinv ind (column q of the element)
+        if (el < ne && q < n) {
 #pragma unroll
-                for (int k = 0; k < nn; ++k) ind[k] = l1s[threadIdx.x * nn + k];
+            for (int i = 0; i < n; ++i) {
+                double r = 0.0;
+#pragma unroll
+                for (int a = 0; a < n; ++a) r += Vi[i * n + a] * inds[el * nn + a + n * q];
+                tmps[el * nn + i + n * q] = r;
             }
-            const double* Vi = ia.vinv;   // row-major n x n
-            double tmp[nn], md[nn];
+        }
+        __syncthreads();
+        // modal row q: modal[q][j] = sum_c Vinv[j][c] tmp[q][c]; partial energies of the three sums
+        double tot = 0.0, c1 = 0.0, c2 = 0.0;
+        if (el < ne && q < n) {
 #pragma unroll
-            for (int jj = 0; jj < n; ++jj)
+            for (int j = 0; j < n; ++j) {
+                double r = 0.0;
 #pragma unroll
-                for (int ii = 0; ii < n; ++ii) {
-                    double r = 0.0;
+                for (int c = 0; c < n; ++c) r += Vi[j * n + c] * tmps[el * nn + q + n * c];
+                const double r2 = r * r;
+                tot += r2;
+                if (q < n - 1 && j < n - 1) c1 += r2;
+                if (q < n - 2 && j < n - 2) c2 += r2;
+            }
+        }
 #pragma unroll
-                    for (int q = 0; q < n; ++q) r += Vi[ii * n + q] * ind[q + n * jj];
-                    tmp[ii + n * jj] = r;
-                }
-#pragma unroll
-            for (int jj = 0; jj < n; ++jj)
-#pragma unroll
-                for (int ii = 0; ii < n; ++ii) {
-                    double r = 0.0;
-#pragma unroll
-                    for (int q = 0; q < n; ++q) r += Vi[jj * n + q] * tmp[ii + n * q];
-                    md[ii + n * jj] = r;
-                }
-            double total = 0.0, clip1 = 0.0, clip2 = 0.0;
-#pragma unroll
-            for (int jj = 0; jj < n; ++jj)
-#pragma unroll
-                for (int ii = 0; ii < n; ++ii) {
-                    const double q2 = md[ii + n * jj] * md[ii + n * jj];
-                    total += q2;
-                }
-#pragma unroll
-            for (int jj = 0; jj < n - 1; ++jj)
-#pragma unroll
-                for (int ii = 0; ii < n - 1; ++ii) clip1 += md[ii + n * jj] * md[ii + n * jj];
-#pragma unroll
-            for (int jj = 0; jj < n - 2; ++jj)
-#pragma unroll
-                for (int ii = 0; ii < n - 2; ++ii) clip2 += md[ii + n * jj] * md[ii + n * jj];
-            const double f1 = total != 0.0 ? (total - clip1) / total : 0.0;
-            const double f2 = clip1 != 0.0 ? (clip1 - clip2) / clip1 : 0.0;
+        for (int o = 4; o > 0; o >>= 1) {
+            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+            c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+            c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+        }
+        if (el < ne && q == 0) {
+            const double f1 = tot != 0.0 ? (tot - c1) / tot : 0.0;
+            const double f2 = c1 != 0.0 ? (c1 - c2) / c1 : 0.0;
             const double energy = fmax(f1, f2);
             double al = 1.0 / (1.0 + exp(-ia.parameter_s / ia.threshold * (energy - ia.threshold)));
             if (al < ia.alpha_min) al = 0.0;
             if (al > 1.0 - ia.alpha_min) al = 1.0;
             al = fmin(ia.alpha_max, al);
-            ia.alpha_raw[e] = al;
-            ia.alpha[e] = al;
+            ia.alpha_raw[e0 + el] = al;
+            ia.alpha[e0 + el] = al;
         }
     }
     if (SPEED) {
