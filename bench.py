@@ -40,6 +40,9 @@ WORKLOADS = {
     "vortex_tree512_N4_mdrk": (9, 4, "mdrk", "vortex"),
     "riemann_tree512_N4_lw": (9, 4, "lw", "riemann"),
 }
+# batched form: 512 independent vortex instances (per-instance seed 0..511: side from {8, 16, 32, 64}
+# elements, degree from {3, 4, 5}, strength ~ U[1, 5], centre ~ U[-2, 2]^2), 50 LW steps
+BATCH_WORKLOADS = {"batched512_vortex_lw": 512}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -213,6 +216,8 @@ def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
         return
+    if args.workload in BATCH_WORKLOADS:
+        return run_reference_batched(args, world)
     level, N, td, icname = WORKLOADS[args.workload]
     # warm-up: one step; then K steps, each a bounded sample of the same workload (one full step)
     rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=max(1, args.steps), budget_s=60.0)
@@ -225,6 +230,39 @@ def run_reference(args):
         "config": {"workload": args.workload, "ndofs": ndofs, "polydeg": N, "time_discretization": td,
                    "elements": 1 << (2 * level), "implementation": "CPU oracle port (C++/OpenMP) of the TrixiLW "
                    "LW rhs; the Julia reference cannot run here"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_reference_batched(args, world):
+    """Oracle port over the uneven batch: instances one after another (each with all host threads), as many
+    instances as fit in about a minute, 5 steps each."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    import trixilw as tl
+    _, insts = batch_instances(tl, BATCH_WORKLOADS[args.workload])
+    threads = os.cpu_count() or 1
+    done, el, used = 0, 0.0, 0
+    for inst in insts:
+        o = pyoracle.Oracle(inst["mesh"], inst["polydeg"])
+        u = inst["u0"].copy()
+        t0 = time.perf_counter()
+        o.steps(u, 5, inst["cfl"], 0.0, 1e9, kind=0, nthreads=threads)
+        el += time.perf_counter() - t0
+        done += 5 * inst["mesh"].ndofs(inst["polydeg"])
+        used += 1
+        if el > 60.0:
+            break
+    rate = done / el
+    sample = f"5 steps of each of the first {used} of {len(insts)} instances in {el:.2f} s"
+    out = {
+        "metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": 5,
+        "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "instances": len(insts), "implementation": "CPU oracle port "
+                   "(C++/OpenMP) of the TrixiLW LW rhs, instances in sequence; the Julia reference cannot run here"},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -376,17 +414,220 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def batch_instances(tl, count):
+    """The uneven batch: instance k draws its parameters from numpy's default_rng(k)."""
+    import numpy as np
+    from trixilw.batch import compute_coefficients
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    out = []
+    for k in range(count):
+        rng = np.random.default_rng(k)
+        side = int(rng.choice([8, 16, 32, 64]))
+        N = int(rng.choice([3, 4, 5]))
+        beta = float(rng.uniform(1.0, 5.0))
+        centre = tuple(float(c) for c in rng.uniform(-2.0, 2.0, 2))
+        mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), side.bit_length() - 1)
+        ic = tl.IsentropicVortex(beta, center=centre)
+        out.append({"mesh": mesh, "polydeg": N, "ic": ic, "u0": compute_coefficients(mesh, N, ic, eq),
+                    "cfl": cfl_for(N), "side": side})
+    return eq, out
+
+
+def run_batched(args):
+    """Batched form vs looping the plain (single-instance) path over the same instances."""
+    import numpy as np
+    import torch
+
+    import trixilw as tl
+    from trixilw import _lib
+
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    count = BATCH_WORKLOADS[args.workload]
+    eq, insts = batch_instances(tl, count)
+    ndofs = [i["mesh"].ndofs(i["polydeg"]) for i in insts]
+    total = sum(ndofs)
+    K, W = args.steps, max(args.warmup, 3)
+    L = _lib.lib()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- batched arm
+    b = tl.LWBatch(eq, device=local_rank)
+    for inst in insts:
+        b.add(inst["mesh"], inst["polydeg"])
+    b.finalize()
+    for i, inst in enumerate(insts):
+        b.set_state(i, inst["u0"], 0.0, inst["cfl"])
+    t0 = time.perf_counter()
+    choices = b.autotune(trials=3)
+    tune_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(b.stream(), device=torch.device("cuda", local_rank))
+    b.step(W)
+    b.synchronize()
+    gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[local_rank]) \
+        if os.environ.get("CUDA_VISIBLE_DEVICES") else local_rank
+    sampler = ClockSampler(gpu_index)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    ev0.record(stream)
+    b.step(K)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    wall_batch = time.perf_counter() - w0
+    barrier()
+    ms_batch = max_over_ranks(ev0.elapsed_time(ev1))
+    b.synchronize()
+    res_batch = [b.get_state(i) for i in range(count)]
+
+    # e2e through the public API with host buffers: every step uploads all instances' states from pinned
+    # host memory, runs one batch step and downloads all states
+    n_e2e = 3
+    hosts = []
+    for i, inst in enumerate(insts):
+        h = torch.empty(inst["u0"].size, dtype=torch.float64, pin_memory=True).numpy()
+        h[:] = res_batch[i][0]
+        hosts.append(h)
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    for _ in range(n_e2e):
+        for i, inst in enumerate(insts):
+            _lib.check(b.ptr, L.tlw_batch_set_state(b.ptr, i, hosts[i].ctypes.data_as(ctypes.c_void_p),
+                                                    _lib.TLW_WHERE_HOST, 0.0, inst["cfl"], 1e30), batch=True)
+        b.step(1)
+        for i in range(count):
+            tt, ss = ctypes.c_double(), ctypes.c_int64()
+            _lib.check(b.ptr, L.tlw_batch_get_state(b.ptr, i, hosts[i].ctypes.data_as(ctypes.c_void_p),
+                                                    _lib.TLW_WHERE_HOST, ctypes.byref(tt), ctypes.byref(ss)),
+                       batch=True)
+    ms_e2e = max_over_ranks(1e3 * (time.perf_counter() - e0))
+    b.close()
+
+    # ---- looped plain arm: one single-instance handle per instance, K plain graph steps each, in a loop
+    semis, integs = [], []
+    for inst in insts:
+        solver = tl.DGSEM(inst["polydeg"], tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.LW()))
+        semi = tl.SemidiscretizationHyperbolic(inst["mesh"], tl.LW(), eq, inst["ic"], solver, device=local_rank)
+        integ = tl.LWIntegrator(tl.semidiscretize(semi, tl.LW(), (0.0, 1e30)))
+        integ.set_state(inst["u0"], 0.0)
+        semis.append(semi)
+        integs.append(integ)
+    for inst, integ in zip(insts, integs):
+        integ.step(W, inst["cfl"])
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    for inst, integ in zip(insts, integs):
+        integ.step(K, inst["cfl"])
+    torch.cuda.synchronize()
+    wall_loop = max_over_ranks(time.perf_counter() - w0)
+    barrier()
+    clocks = sampler.stop()
+    # per-instance L2 errors against the exact (advected) vortex, both arms
+    worst_err_diff, bitwise = 0.0, True
+    for i, (semi, integ) in enumerate(zip(semis, integs)):
+        u_loop = integ.get_state()
+        integ.sync_time()
+        u_b, t_b, s_b = res_batch[i]
+        bitwise = bitwise and bool(np.array_equal(u_loop, u_b)) and integ.t == t_b
+        l2_b, _ = tl.l2_linf_errors(semi, u_b, t_b)
+        l2_l, _ = tl.l2_linf_errors(semi, u_loop, integ.t)
+        worst_err_diff = max(worst_err_diff, float(np.max(np.abs(l2_b - l2_l) / np.maximum(np.abs(l2_l), 1e-300))))
+    del integs, semis
+
+    value = total * K * world / (ms_batch * 1e-3)
+    loop_value = total * K * world / wall_loop
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        E_by_N = {}
+        for inst in insts:
+            E_by_N[inst["polydeg"]] = E_by_N.get(inst["polydeg"], 0) + inst["mesh"].n_elements
+        step_alg = sum(alg_bytes_per_element_step(N, "lw") * E for N, E in E_by_N.items())
+        achieved = step_alg * K / (ms_batch * 1e-3) / 1e9
+        state_bytes = 8 * 4 * total
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_batch / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "instances": count, "ndofs_total": total,
+                       "elements_by_degree": {str(k): v for k, v in sorted(E_by_N.items())},
+                       "sides": sorted({i["side"] for i in insts}), "autotune": choices, "autotune_s": tune_s,
+                       "l2": "inputs larger than L2 (state %.0f MB per array)" % (state_bytes / 1e6),
+                       "parallelism": f"replicas{world}" if world > 1 else "single"},
+            "looped_plain": {"value": loop_value, "unit": UNIT, "wall_s": wall_loop,
+                             "how": f"{count} single-instance handles, {K} graph-replayed plain steps each, "
+                                    "enqueued in a host loop; host wall clock to device idle"},
+            "batched_wall_s": wall_batch,
+            "speedup_vs_looped": (total * K / wall_batch) / loop_value if wall_batch > 0 else None,
+            "per_instance_l2_error_max_rel_diff": worst_err_diff,
+            "bitwise_equal_to_looped": bitwise,
+            "e2e": {"value": total * n_e2e * world / (ms_e2e * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes, "steps": n_e2e},
+            "roofline": {"kernel": "batched LW step (all kernels of the graph)", "bound": "hbm", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                         "alg_bytes_per_step": step_alg},
+            "clocks": clocks,
+            "gpu_launches": K * (1 + 4 * len(E_by_N)),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import pyoracle
+            done, el, used = 0, 0.0, 0
+            threads = os.cpu_count() or 1
+            for inst in insts:
+                o = pyoracle.Oracle(inst["mesh"], inst["polydeg"])
+                u = inst["u0"].copy()
+                t0 = time.perf_counter()
+                o.steps(u, 5, inst["cfl"], 0.0, 1e9, kind=0, nthreads=threads)
+                el += time.perf_counter() - t0
+                done += 5 * inst["mesh"].ndofs(inst["polydeg"])
+                used += 1
+                if el > 15.0:
+                    break
+            out["cpu_baseline"] = {"value": done / el, "unit": UNIT, "cores": threads, "kind": "port",
+                                   "sample": f"5 steps of each of the first {used} instances, {el:.1f} s"}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="vortex_tree512_N4_lw", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="vortex_tree512_N4_lw", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload in BATCH_WORKLOADS:
+        run_batched(args)
     else:
         run_ours(args)
 

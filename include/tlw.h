@@ -161,6 +161,44 @@ int tlw_rhs_lw_noalloc(int32_t polydeg, double gamma, int32_t surface_flux, int3
                        const int32_t* x_right, int32_t n_y_interfaces, const int32_t* y_left,
                        const int32_t* y_right, const double* u, double* du, double dt, void* stream);
 
+/* ---- Batched form: many independent periodic TreeMesh{2} LW runs (N = 3, 4, 5, uneven sizes) ----------
+ * No counterpart in the reference, which runs one semidiscretization per `solve_lwfr` call
+ * (src/solvers/lwfr.jl:233-270); each instance here advances exactly as that loop would advance it alone:
+ * its own CFL dt (compute_dt, src/solvers/lwfr.jl:176-190), its own final time (set_dt! clamp and
+ * isfinished, src/solvers/lwfr.jl:76-90 and 146-148), its own step count. A step of the batch is one graph replay.
+ * Order: tlw_batch_create, tlw_batch_add_tree_mesh per instance, tlw_batch_finalize, tlw_batch_set_state per
+ * instance, optionally tlw_batch_autotune, then tlw_batch_step / tlw_batch_get_state. Opts: LW, FR volume
+ * integral, any surface flux / speed; opts->polydeg is ignored (each instance has its own). */
+typedef struct tlw_batch tlw_batch;
+int tlw_batch_create(const tlw_opts* opts, tlw_batch** out);
+int tlw_batch_destroy(tlw_batch* b);
+/* Adds one instance: its degree (3..5), its periodic mesh (arrays as in tlw_set_tree_mesh, without
+ * boundaries). *index_out receives the instance id (0, 1, ... in call order). */
+int tlw_batch_add_tree_mesh(tlw_batch* b, int32_t polydeg, int64_t n_elements, const double* inverse_jacobian,
+                            int64_t n_interfaces, const int64_t* interface_neighbor_ids,
+                            const int64_t* interface_orientations, int32_t* index_out);
+/* Groups the instances by degree and allocates the concatenated device arrays. */
+int tlw_batch_finalize(tlw_batch* b);
+/* State [v, i, j, element] of one instance, its start time, CFL number and final time; resets its step count.
+ * Synchronous. */
+int tlw_batch_set_state(tlw_batch* b, int32_t instance, const double* u, int32_t where, double t, double cfl,
+                        double t_end);
+/* Synchronous: state, time and accepted steps of one instance; TLW_E_NONADMISSIBLE if any kernel flagged a
+ * bad state since the last check. */
+int tlw_batch_get_state(tlw_batch* b, int32_t instance, double* u, int32_t where, double* t_out,
+                        int64_t* steps_out);
+/* Enqueues nsteps batch steps (asynchronous). Instances past their final time take dt = 0 steps. */
+int tlw_batch_step(tlw_batch* b, int32_t nsteps, int32_t use_graph);
+int tlw_batch_synchronize(tlw_batch* b);
+int tlw_batch_get_stream(tlw_batch* b, void** stream);
+/* Times the launch variants on this batch (elements per CTA of the volume kernel per degree group, CTA size of
+ * the interface kernels, degree groups serial or concurrent) and keeps the fastest. choices_out (optional,
+ * 2 * groups + 1 ints): per group (volume variant, interface CTA size), then the concurrency flag. The
+ * current state is not changed. */
+int tlw_batch_autotune(tlw_batch* b, int32_t trials, int32_t* choices_out);
+int32_t tlw_batch_num_groups(tlw_batch* b);
+const char* tlw_batch_last_error(tlw_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

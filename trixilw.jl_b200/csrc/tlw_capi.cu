@@ -153,12 +153,12 @@ struct Launch {
     }
     // speed: CFL reduction; ind: Hennemann-Gassner indicator (both read u once)
     static void max_speed(cudaStream_t s, const double* u, const double* ij, int E, double gamma, StepState* st,
-                          bool speed, bool ind, const IndicatorArgs& ia) {
+                          bool speed, bool ind, const IndicatorArgs& ia, BatchSpeedArgs bs = BatchSpeedArgs{}) {
         if (E == 0) return;
         const int grid = (E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS;
-        if (speed && ind) max_speed_kernel<N, true, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia);
-        else if (speed) max_speed_kernel<N, true, false><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia);
-        else if (ind) max_speed_kernel<N, false, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia);
+        if (speed && ind) max_speed_kernel<N, true, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
+        else if (speed) max_speed_kernel<N, true, false><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
+        else if (ind) max_speed_kernel<N, false, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
     }
 };
 

@@ -42,6 +42,7 @@ struct SurfArgs {
     const double* tFn;       // first-order subcell flux next to each face [v, l, face, e]
     double jac_first;        // J^{-1} used by the admissibility test (element 1's on TreeMesh)
     double w_first, w_last;  // GLL weights w_1, w_n
+    const int* inst;         // batched form: instance of each element (dt indexed by it); null otherwise
 };
 
 __device__ __forceinline__ bool admissible(double gm1, const double* u) {
@@ -105,8 +106,9 @@ __global__ void __launch_bounds__(128) interface_kernel(SurfArgs a) {
     load4(a.tF + (((size_t)re * 4 + faceR) * n + l) * NV, FR);
     // TreeMesh argument order: surface_flux(f_ll, f_rr, U_ll, U_rr, u_ll, u_rr) (dg_2d.jl:1928)
     lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, FL, FR, UL, UR, uL, uR, a.orientation, Fn, a.status);
-    if (a.shock_capturing) blend_interface_flux<N>(a, le, re, faceL, faceR, l, uL, uR, *a.dt, Fn);
-    const double dts = a.step_mode ? *a.dt : 1.0;
+    const double dt = a.inst ? a.dt[__ldg(a.inst + le)] : *a.dt;
+    if (a.shock_capturing) blend_interface_flux<N>(a, le, re, faceL, faceR, l, uL, uR, dt, Fn);
+    const double dts = a.step_mode ? dt : 1.0;
     const double sL = -__ldg(a.inv_jac + le) * a.inv_w_last * dts;
     const double sR = __ldg(a.inv_jac + re) * a.inv_w_first * dts;
     double* oL = a.out + ((size_t)le * n * n + nodeL) * NV;
@@ -229,10 +231,17 @@ struct IndicatorArgs {
 //  IND:   Trixi IndicatorHennemannGassner with variable density_pressure: modal = Vinv ind Vinv^T by
 //         eight threads per element (constant-memory Vinv), energy fractions of the highest modes,
 //         logistic map, alpha_min / alpha_max clipping (Hennemann et al., J. Comput. Phys. 426 (2021)).
+// batched form: per-instance maxima instead of the single StepState one
+struct BatchSpeedArgs {
+    const int* inst;                // instance of each element, or null
+    unsigned long long* inst_max;   // [instance] bits of the max scaled speed
+};
+
 template <int N, bool SPEED, bool IND>
 __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const double* __restrict__ u,
                                                                const double* __restrict__ inv_jac, int E,
-                                                               double gamma, StepState* s, IndicatorArgs ia) {
+                                                               double gamma, StepState* s, IndicatorArgs ia,
+                                                               BatchSpeedArgs bs) {
     constexpr int n = N + 1;
     constexpr int nn = n * n;
     constexpr int ELEMS = MsCfg<N>::ELEMS;
@@ -312,7 +321,23 @@ __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const double* __r
             ia.alpha[e0 + el] = al;
         }
     }
-    if (SPEED) {
+    if (SPEED && bs.inst) {
+        // batched: the (<= 32) element values sit in warp 0; one atomic per instance present
+        if (threadIdx.x < 32) {
+            const int last = min(ne, 32) - 1;
+            const int my = threadIdx.x <= last ? __ldg(bs.inst + e0 + threadIdx.x) : -1;
+            const int first_inst = __shfl_sync(0xffffffffu, my, 0);
+            const int last_inst = __shfl_sync(0xffffffffu, my, last);
+            if (first_inst == last_inst) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+                if (threadIdx.x == 0 && m > 0.0)
+                    atomicMax(bs.inst_max + first_inst, (unsigned long long)__double_as_longlong(m));
+            } else if (threadIdx.x <= last && m > 0.0) {
+                atomicMax(bs.inst_max + my, (unsigned long long)__double_as_longlong(m));
+            }
+        }
+    } else if (SPEED) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
         if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
@@ -323,6 +348,35 @@ __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const double* __r
             if (b > 0.0) atomicMax(&s->max_bits, (unsigned long long)__double_as_longlong(b));
         }
     }
+}
+
+// batched form: dt of every instance from its max scaled speed (finalize_dt_kernel per instance)
+struct BatchTime {
+    unsigned long long* max_bits;
+    double* dt;
+    double* t;
+    const double* t_end;
+    const double* cfl;
+    long long* steps;
+    const int* nnodes;
+    int count;
+};
+
+static __global__ void batch_finalize_dt_kernel(BatchTime b) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= b.count) return;
+    double maxs = __longlong_as_double((long long)b.max_bits[k]);
+    const double tiny = 4.9406564584124654e-324;
+    if (!(maxs > tiny)) maxs = tiny;
+    double dt = b.cfl[k] * (2.0 / (b.nnodes[k] * maxs));
+    const double t = b.t[k], te = b.t_end[k];
+    const bool finished = fabs(t - te) <= 1.4901161193847656e-8 * fmax(fabs(t), fabs(te)) || t >= te;
+    if (finished) dt = 0.0;
+    else if (t + dt > te) dt = te - t;
+    b.dt[k] = dt;
+    b.t[k] = finished ? t : t + dt;
+    if (!finished) b.steps[k] += 1;
+    b.max_bits[k] = 0ull;
 }
 
 // Trixi apply_smoothing! (TreeMesh{2}): alpha_e = max(alpha_e, alpha_raw_nb / 2) over the interfaces,

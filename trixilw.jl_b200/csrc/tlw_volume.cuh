@@ -26,12 +26,13 @@
 
 namespace tlw {
 
-template <int N>
+// EBX = 0: the default number of elements per CTA; another value selects a tuned variant
+template <int N, int EBX = 0>
 struct VolCfg {
     static constexpr int n = N + 1;
     static constexpr int nn = n * n;
     // whole elements per CTA, chosen so that the CTA is (nearly) full warps
-    static constexpr int EB = N == 1 ? 32 : N == 2 ? 14 : N == 3 ? 8 : N == 4 ? 5 : N == 5 ? 7 : N == 6 ? 5 : 2;
+    static constexpr int EB = EBX ? EBX : N == 1 ? 32 : N == 2 ? 14 : N == 3 ? 8 : N == 4 ? 5 : N == 5 ? 7 : N == 6 ? 5 : 2;
     static constexpr int THREADS = ((EB * nn + 31) / 32) * 32;
     // resident CTAs per SM the register allocation must allow (<= 128 registers per thread)
     static constexpr int MIN_BLOCKS = THREADS <= 128 ? 4 : 2;
@@ -66,12 +67,12 @@ struct VolArgs {
     double* tFn;            // first-order subcell flux next to each face [v, l, face, e] (fn_low)
     unsigned* status;
     int speed_kind;
+    const int* inst;        // batched form: instance of each element (dt indexed by it); null otherwise
 };
 
 // owner: store the node's f (into X) and g (into Y)
-template <int N>
+template <int N, class C>
 __device__ __forceinline__ void node_put(double* X, double* Y, int e, int i, int j, const double* f, const double* g) {
-    using C = VolCfg<N>;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         const int a = (v * C::EB + e) * C::P + i + C::R * j;
@@ -79,9 +80,8 @@ __device__ __forceinline__ void node_put(double* X, double* Y, int e, int i, int
         Y[a] = g[v];
     }
 }
-template <int N>
+template <int N, class C>
 __device__ __forceinline__ void node_get(const double* X, const double* Y, int e, int i, int j, double* f, double* g) {
-    using C = VolCfg<N>;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         const int a = (v * C::EB + e) * C::P + i + C::R * j;
@@ -90,9 +90,8 @@ __device__ __forceinline__ void node_get(const double* X, const double* Y, int e
     }
 }
 // owner: x-result + y-result at the node
-template <int N>
+template <int N, class C>
 __device__ __forceinline__ void node_sum(const double* X, const double* Y, int e, int i, int j, double* d) {
-    using C = VolCfg<N>;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         const int a = (v * C::EB + e) * C::P + i + C::R * j;
@@ -103,9 +102,8 @@ __device__ __forceinline__ void node_sum(const double* X, const double* Y, int e
 // line phase, in place: X row (v,e,idx) <- M X row, Y column (v,e,idx) <- M Y column, with
 // M = D (HAT = false) or Dhat (HAT = true):  x-result(i, j) = sum_k M[i,k] f(k, j),
 // y-result(i, j) = sum_k M[j,k] g(i, k). Each row and column is read and written by one thread only.
-template <int N, bool HAT>
+template <int N, class C, bool HAT>
 __device__ __forceinline__ void line_contract(double* X, double* Y, int tid) {
-    using C = VolCfg<N>;
     constexpr int n = C::n;
     const double* M = HAT ? c_tlw_Dhat[N] : c_tlw_D[N];
 #pragma unroll 1
@@ -137,7 +135,7 @@ __device__ __forceinline__ void line_contract(double* X, double* Y, int tid) {
 
 // ---- shock capturing helpers (src/solvers/dgsem_tree/dg_2d.jl:251-282, 1948-1991; Trixi calcflux_fv!) ----
 // stage 0: park u and (v1, v2, c) of the node for the first-order subcell fluxes of its neighbours
-template <int N>
+template <int N, class C>
 __device__ __forceinline__ void sc_park(double* UU, double* VC, int el, int i, int j, const double* u, double gamma,
                                         unsigned* status) {
     const double ir = 1.0 / u[0];
@@ -145,15 +143,14 @@ __device__ __forceinline__ void sc_park(double* UU, double* VC, int el, int i, i
     const double p = (gamma - 1.0) * (u[3] - 0.5 * (u[1] * v1 + u[2] * v2));
     const double c = checked_sqrt(gamma * p * ir, status);
     const double vc[NV] = {v1, v2, c, 0.0};
-    node_put<N>(UU, VC, el, i, j, u, vc);
+    node_put<N, C>(UU, VC, el, i, j, u, vc);
 }
 
 // Rusanov (Trixi flux_lax_friedrichs, 4 arguments) between node L and node R of one element, from the
 // parked states, fluxes (fx: x-fluxes if orientation 1, else y-fluxes) and speeds
-template <int N>
+template <int N, class C>
 __device__ __forceinline__ void sc_face_flux(const double* UU, const double* VC, const double* FL, int el, int iL,
                                              int jL, int iR, int jR, int orientation, int speed_kind, double* out) {
-    using C = VolCfg<N>;
     const int aL = el * C::P + iL + C::R * jL, aR = el * C::P + iR + C::R * jR;
     constexpr int PV = C::EB * C::P;   // stride between variable planes
     const double vL = VC[(orientation == 1 ? 0 : PV) + aL], vR = VC[(orientation == 1 ? 0 : PV) + aR];
@@ -166,20 +163,19 @@ __device__ __forceinline__ void sc_face_flux(const double* UU, const double* VC,
 }
 
 // final stage: each node computes the subcell flux on its left (x) and lower (y) subcell face
-template <int N>
+template <int N, class C>
 __device__ __forceinline__ void sc_faces(const double* UU, const double* VC, const double* F0X, const double* F0Y,
                                          double* FVX, double* FVY, int el, int i, int j, int speed_kind) {
-    using C = VolCfg<N>;
     constexpr int PV = C::EB * C::P;
     const int a = el * C::P + i + C::R * j;
     double f[NV];
     if (i >= 1) {
-        sc_face_flux<N>(UU, VC, F0X, el, i - 1, j, i, j, 1, speed_kind, f);
+        sc_face_flux<N, C>(UU, VC, F0X, el, i - 1, j, i, j, 1, speed_kind, f);
 #pragma unroll
         for (int v = 0; v < NV; ++v) FVX[v * PV + a] = f[v];
     }
     if (j >= 1) {
-        sc_face_flux<N>(UU, VC, F0Y, el, i, j - 1, i, j, 2, speed_kind, f);
+        sc_face_flux<N, C>(UU, VC, F0Y, el, i, j - 1, i, j, 2, speed_kind, f);
 #pragma unroll
         for (int v = 0; v < NV; ++v) FVY[v * PV + a] = f[v];
     }
@@ -187,10 +183,9 @@ __device__ __forceinline__ void sc_faces(const double* UU, const double* VC, con
 
 // epilogue: fv = w_i^-1 (f*_{i+1/2} - f*_{i-1/2}) + w_j^-1 (g*_{j+1/2} - g*_{j-1/2}) (element-boundary
 // subcell fluxes are zero); acc <- (1 - alpha) acc + alpha fv; fn_low traces of the four faces
-template <int N>
+template <int N, class C>
 __device__ __forceinline__ void sc_blend(const VolArgs& a, const double* FVX, const double* FVY, int el, int e, int i,
                                          int j, double alpha, double* acc) {
-    using C = VolCfg<N>;
     constexpr int n = C::n;
     constexpr int PV = C::EB * C::P;
     const int base = el * C::P;
@@ -263,9 +258,9 @@ __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, 
 //   depth 3: f_t = raw1/12, f_tt = raw2,    f_ttt = raw3/2
 //   depth 2: f_t = raw1/2,  f_tt = raw2;    depth 1: f_t = raw1/2
 // ------------------------------------------------------------------------------------------------
-template <int N, int MODE, bool SC>
-__global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
-    using C = VolCfg<N>;
+template <int N, int MODE, bool SC, int EBX = 0>
+__global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
+    using C = VolCfg<N, EBX>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     constexpr int DEPTH = N >= 4 ? 4 : N;
     constexpr double C1 = DEPTH >= 3 ? 1.0 / 12.0 : 0.5;
@@ -283,13 +278,14 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
     double* FVY = FVX + C::PLANES;
 
     const int tid = threadIdx.x;
-    const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
     const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
+    // dt of this element's instance (batched form) or the single dt
+    const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
 
     double U[NV], F[NV], G[NV], up[NV], um[NV], upp[NV], umm[NV];
     double s0 = 0.0, ij = 0.0;   // s0 = -dt J^{-1}
@@ -300,9 +296,9 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
         ij = __ldg(a.inv_jac + e);
         s0 = -dt * ij;
         euler_fluxes(gm1, uu[0], uu[1], uu[2], uu[3], f, g);
-        node_put<N>(X, Y, el, i, j, f, g);
-        if (DEPTH >= 2 || SC) node_put<N>(F0X, F0Y, el, i, j, f, g);
-        if (SC) sc_park<N>(UU, VC, el, i, j, uu, a.gamma, a.status);
+        node_put<N, C>(X, Y, el, i, j, f, g);
+        if (DEPTH >= 2 || SC) node_put<N, C>(F0X, F0Y, el, i, j, f, g);
+        if (SC) sc_park<N, C>(UU, VC, el, i, j, uu, a.gamma, a.status);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             F[v] = f[v]; G[v] = g[v]; U[v] = uu[v];
@@ -310,13 +306,13 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
         }
     }
     __syncthreads();
-    line_contract<N, false>(X, Y, tid);
+    line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
 
     // stage 1: ut; perturbed states; f_t (dg_2d.jl:972-1023 / :725-775 / :543-582 / :417-454)
     if (active) {
         double d[NV], r[NV], q[NV], f[NV], g[NV];
-        node_sum<N>(X, Y, el, i, j, d);
+        node_sum<N, C>(X, Y, el, i, j, d);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             d[v] *= s0;
@@ -350,17 +346,17 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
         }
 #pragma unroll
         for (int v = 0; v < NV; ++v) { F[v] = fma(0.5 * C1, r[v], F[v]); G[v] = fma(0.5 * C1, q[v], G[v]); }
-        if (DEPTH >= 2) node_put<N>(X, Y, el, i, j, r, q);
+        if (DEPTH >= 2) node_put<N, C>(X, Y, el, i, j, r, q);
     }
     if (DEPTH >= 2) {
         __syncthreads();
-        line_contract<N, false>(X, Y, tid);
+        line_contract<N, C, false>(X, Y, tid);
         __syncthreads();
         // stage 2: utt; f_tt (dg_2d.jl:1025-1083 / :777-831 / :597-634)
         if (active) {
             double d[NV], f0[NV], g0[NV], r[NV], q[NV], f[NV], g[NV];
-            node_sum<N>(X, Y, el, i, j, d);
-            node_get<N>(F0X, F0Y, el, i, j, f0, g0);
+            node_sum<N, C>(X, Y, el, i, j, d);
+            node_get<N, C>(F0X, F0Y, el, i, j, f0, g0);
             const double s = s0 * C1;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
@@ -401,17 +397,17 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
                 F[v] = fma(C2 / 6.0, r[v], F[v]);
                 G[v] = fma(C2 / 6.0, q[v], G[v]);
             }
-            if (DEPTH >= 3) node_put<N>(X, Y, el, i, j, r, q);
+            if (DEPTH >= 3) node_put<N, C>(X, Y, el, i, j, r, q);
         }
     }
     if (DEPTH >= 3) {
         __syncthreads();
-        line_contract<N, false>(X, Y, tid);
+        line_contract<N, C, false>(X, Y, tid);
         __syncthreads();
         // stage 3: uttt; f_ttt (dg_2d.jl:1085-1138 / :833-875)
         if (active) {
             double d[NV], r[NV], q[NV], f[NV], g[NV];
-            node_sum<N>(X, Y, el, i, j, d);
+            node_sum<N, C>(X, Y, el, i, j, d);
             const double s = s0 * C2;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
@@ -440,18 +436,18 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
                 F[v] = fma(C3 / 24.0, r[v], F[v]);
                 G[v] = fma(C3 / 24.0, q[v], G[v]);
             }
-            if (DEPTH >= 4) node_put<N>(X, Y, el, i, j, r, q);
+            if (DEPTH >= 4) node_put<N, C>(X, Y, el, i, j, r, q);
         }
     }
     if (DEPTH >= 4) {
         __syncthreads();
-        line_contract<N, false>(X, Y, tid);
+        line_contract<N, C, false>(X, Y, tid);
         __syncthreads();
         // stage 4: utttt; f_tttt (dg_2d.jl:1140-1206)
         if (active) {
             double d[NV], f0[NV], g0[NV], r[NV], q[NV], f[NV], g[NV];
-            node_sum<N>(X, Y, el, i, j, d);
-            node_get<N>(F0X, F0Y, el, i, j, f0, g0);
+            node_sum<N, C>(X, Y, el, i, j, d);
+            node_get<N, C>(F0X, F0Y, el, i, j, f0, g0);
             const double s = s0 * C3;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
@@ -485,16 +481,16 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS) lw_
     // final: Dhat contraction of the time-averaged fluxes (every owner has read its node's results of
     // the last contraction before writing F, G over them: same address, same thread)
     if (active) {
-        node_put<N>(X, Y, el, i, j, F, G);
-        if (SC) sc_faces<N>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
+        node_put<N, C>(X, Y, el, i, j, F, G);
+        if (SC) sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
     }
     __syncthreads();
-    line_contract<N, true>(X, Y, tid);
+    line_contract<N, C, true>(X, Y, tid);
     __syncthreads();
     if (active) {
         double acc[NV];
-        node_sum<N>(X, Y, el, i, j, acc);
-        if (SC) sc_blend<N>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
+        node_sum<N, C>(X, Y, el, i, j, acc);
+        if (SC) sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
     }
 }
@@ -517,32 +513,33 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
     double* FVX = VC + C::PLANES;
     double* FVY = FVX + C::PLANES;
     const int tid = threadIdx.x;
-    const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
     const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
+    // dt of this element's instance (batched form) or the single dt
+    const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
     double uu[NV], f0[NV], g0[NV], ij = 0.0;
     if (active) {
         load4(a.u + ((size_t)e * nn + node) * NV, uu);
         ij = __ldg(a.inv_jac + e);
         euler_fluxes(gm1, uu[0], uu[1], uu[2], uu[3], f0, g0);
-        node_put<N>(X, Y, el, i, j, f0, g0);
+        node_put<N, C>(X, Y, el, i, j, f0, g0);
         if (SC) {
             // the subcell FV part uses the instantaneous u^n (multi_derivative_2d.jl:205)
-            node_put<N>(F0X, F0Y, el, i, j, f0, g0);
-            sc_park<N>(UU, VC, el, i, j, uu, a.gamma, a.status);
+            node_put<N, C>(F0X, F0Y, el, i, j, f0, g0);
+            sc_park<N, C>(UU, VC, el, i, j, uu, a.gamma, a.status);
         }
     }
     __syncthreads();
-    line_contract<N, false>(X, Y, tid);
+    line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
     double U[NV], F[NV], G[NV];
     if (active) {
         double d[NV], ft[NV], gt[NV], f[NV], g[NV], s[NV];
-        node_sum<N>(X, Y, el, i, j, d);
+        node_sum<N, C>(X, Y, el, i, j, d);
         const double s0 = -dt * ij;
 #pragma unroll
         for (int v = 0; v < NV; ++v) d[v] *= s0;
@@ -574,16 +571,16 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
         store4(a.U2 + off * NV, U2v);
         store4(a.F2 + off * 2 * NV, F2v);
         store4(a.F2 + off * 2 * NV + NV, G2v);
-        node_put<N>(X, Y, el, i, j, F, G);
-        if (SC) sc_faces<N>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
+        node_put<N, C>(X, Y, el, i, j, F, G);
+        if (SC) sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
     }
     __syncthreads();
-    line_contract<N, true>(X, Y, tid);
+    line_contract<N, C, true>(X, Y, tid);
     __syncthreads();
     if (active) {
         double acc[NV];
-        node_sum<N>(X, Y, el, i, j, acc);
-        if (SC) sc_blend<N>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
+        node_sum<N, C>(X, Y, el, i, j, acc);
+        if (SC) sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
     }
 }
@@ -606,36 +603,37 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
     double* FVX = VC + C::PLANES;
     double* FVY = FVX + C::PLANES;
     const int tid = threadIdx.x;
-    const double dt = *a.dt;
     const double gm1 = a.gamma - 1.0;
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
     const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
+    // dt of this element's instance (batched form) or the single dt
+    const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
     double us[NV], ij = 0.0;
     if (active) {
         double f[NV], g[NV];
         load4(a.u + ((size_t)e * nn + node) * NV, us);
         ij = __ldg(a.inv_jac + e);
         euler_fluxes(gm1, us[0], us[1], us[2], us[3], f, g);
-        node_put<N>(X, Y, el, i, j, f, g);
+        node_put<N, C>(X, Y, el, i, j, f, g);
         if (SC) {
             // the subcell FV part uses the instantaneous u^n, not u* (multi_derivative_2d.jl:257)
             double un[NV], fn0[NV], gn0[NV];
             load4(a.u_base + ((size_t)e * nn + node) * NV, un);
             euler_fluxes(gm1, un[0], un[1], un[2], un[3], fn0, gn0);
-            node_put<N>(F0X, F0Y, el, i, j, fn0, gn0);
-            sc_park<N>(UU, VC, el, i, j, un, a.gamma, a.status);
+            node_put<N, C>(F0X, F0Y, el, i, j, fn0, gn0);
+            sc_park<N, C>(UU, VC, el, i, j, un, a.gamma, a.status);
         }
     }
     __syncthreads();
-    line_contract<N, false>(X, Y, tid);
+    line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
     double U[NV], F[NV], G[NV];
     if (active) {
         double d[NV], ft[NV], gt[NV], f[NV], g[NV], s[NV];
-        node_sum<N>(X, Y, el, i, j, d);
+        node_sum<N, C>(X, Y, el, i, j, d);
         const double s0 = -dt * ij;
 #pragma unroll
         for (int v = 0; v < NV; ++v) d[v] *= s0;
@@ -664,16 +662,16 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
             G[v] = fma(1.0 / 3.0, gt[v], G2v[v]);
             U[v] = fma(1.0 / 3.0, d[v], U2v[v]);
         }
-        node_put<N>(X, Y, el, i, j, F, G);
-        if (SC) sc_faces<N>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
+        node_put<N, C>(X, Y, el, i, j, F, G);
+        if (SC) sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
     }
     __syncthreads();
-    line_contract<N, true>(X, Y, tid);
+    line_contract<N, C, true>(X, Y, tid);
     __syncthreads();
     if (active) {
         double acc[NV];
-        node_sum<N>(X, Y, el, i, j, acc);
-        if (SC) sc_blend<N>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
+        node_sum<N, C>(X, Y, el, i, j, acc);
+        if (SC) sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
     }
 }

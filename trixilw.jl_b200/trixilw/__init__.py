@@ -2,6 +2,7 @@
 compressible Euler, FP64). The compute runs in libtlw.so (CUDA, C ABI in include/tlw.h); this package is
 the host-side mirror of the reference's Julia interface for that path."""
 from ._lib import DomainError, TlwError, lib
+from .batch import LWBatch, solve_lwfr_batch
 from .equations import (CompressibleEulerEquations2D, ConstantState, DensityWave, FourQuadrantRiemann,
                         IsentropicVortex)
 from .lwfr import LWIntegrator, LWSolution, l2_linf_errors, solve_lwfr
@@ -20,5 +21,5 @@ __all__ = [
     "FluxLaxFriedrichs", "IndicatorHennemannGassner", "SemidiscretizationHyperbolic", "VolumeIntegralFR",
     "VolumeIntegralFRShockCapturing", "boundary_condition_periodic",
     "flux_hll", "flux_lax_friedrichs", "get_time_discretization", "lw_fourier_cfl", "rhs", "rhs_mdrk1",
-    "rhs_mdrk2", "semidiscretize", "trixi2lw",
+    "rhs_mdrk2", "semidiscretize", "trixi2lw", "LWBatch", "solve_lwfr_batch",
 ]

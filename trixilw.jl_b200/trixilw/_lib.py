@@ -33,6 +33,9 @@ EXPORTED = (
     "tlw_max_dt", "tlw_set_state", "tlw_get_state", "tlw_step", "tlw_get_time", "tlw_get_cache",
     "tlw_cache_size", "tlw_synchronize", "tlw_get_stream", "tlw_state_pointer", "tlw_last_error",
     "tlw_step_timed", "tlw_probe_fp64_tflops", "tlw_rhs_lw_noalloc",
+    "tlw_batch_create", "tlw_batch_destroy", "tlw_batch_add_tree_mesh", "tlw_batch_finalize",
+    "tlw_batch_set_state", "tlw_batch_get_state", "tlw_batch_step", "tlw_batch_synchronize",
+    "tlw_batch_get_stream", "tlw_batch_autotune", "tlw_batch_num_groups", "tlw_batch_last_error",
 )
 
 
@@ -100,16 +103,33 @@ def lib() -> ctypes.CDLL:
     L.tlw_state_pointer.argtypes = [P, ctypes.POINTER(P)]
     L.tlw_last_error.argtypes = [P]
     L.tlw_last_error.restype = ctypes.c_char_p
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    L.tlw_batch_create.argtypes = [ctypes.POINTER(TlwOpts), ctypes.POINTER(P)]
+    L.tlw_batch_destroy.argtypes = [P]
+    L.tlw_batch_add_tree_mesh.argtypes = [P, i32, i64, dp, i64, i64p, i64p, i32p]
+    L.tlw_batch_finalize.argtypes = [P]
+    L.tlw_batch_set_state.argtypes = [P, i32, P, i32, dbl, dbl, dbl]
+    L.tlw_batch_get_state.argtypes = [P, i32, P, i32, dp, i64p]
+    L.tlw_batch_step.argtypes = [P, i32, i32]
+    L.tlw_batch_synchronize.argtypes = [P]
+    L.tlw_batch_get_stream.argtypes = [P, ctypes.POINTER(P)]
+    L.tlw_batch_autotune.argtypes = [P, i32, i32p]
+    L.tlw_batch_num_groups.argtypes = [P]
+    L.tlw_batch_num_groups.restype = i32
+    L.tlw_batch_last_error.argtypes = [P]
+    L.tlw_batch_last_error.restype = ctypes.c_char_p
     for name in EXPORTED:
-        L[name].restype = L[name].restype if name in ("tlw_abi_version", "tlw_cache_size", "tlw_last_error") else ctypes.c_int
+        keep = ("tlw_abi_version", "tlw_cache_size", "tlw_last_error", "tlw_batch_num_groups", "tlw_batch_last_error")
+        L[name].restype = L[name].restype if name in keep else ctypes.c_int
     _lib = L
     return L
 
 
-def check(handle, rc: int) -> None:
+def check(handle, rc: int, batch: bool = False) -> None:
     if rc == TLW_OK:
         return
-    msg = lib().tlw_last_error(handle).decode() if handle else ""
+    err = lib().tlw_batch_last_error if batch else lib().tlw_last_error
+    msg = err(handle).decode() if handle else ""
     if rc == TLW_E_NONADMISSIBLE:
         raise DomainError(msg or "non-admissible state")
     raise TlwError(rc, msg)
