@@ -137,7 +137,11 @@ int oracle_steps(oracle_handle* h, int kind, double* u, int nsteps, double cfl, 
     double t = *t_inout;
     int s = 0;
     for (; s < nsteps; ++s) {
-        if (t >= t_end || std::fabs(t - t_end) <= 1e-14 * std::max(1.0, std::fabs(t_end))) break;
+        // isfinished: t ≈ t_end, Julia isapprox with rtol = sqrt(eps(Float64)) (src/solvers/lwfr.jl:146-148)
+        if (t == t_end) break;
+        if (std::isfinite(t_end) &&
+            (t >= t_end || std::fabs(t - t_end) <= 1.4901161193847656e-8 * std::max(std::fabs(t), std::fabs(t_end))))
+            break;
         bool bad = false;
         double dt = fixed_dt > 0 ? fixed_dt : max_dt(h->basis, h->eq, h->mesh, u, cfl, bad, nthreads);
         if (bad) return -3;

@@ -261,3 +261,34 @@ def test_riemann_shock_capturing_runs_to_t025(oracle_mod, tl):
     assert abs(t - 0.25) < 1e-12
     rho = u.reshape(-1, 4)[:, 0]
     assert rho.min() > 0.05 and rho.max() < 2.5
+
+
+def test_step_loop_final_time_semantics(oracle_mod, tl):
+    """isfinished is Julia's t ≈ t_end (rtol sqrt(eps)): an infinite t_end never finishes, a finite one
+    clamps the last dt so that t lands on t_end exactly, and no step is taken from t_end."""
+    mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), 2)
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    xy = mesh.node_coordinates(3)
+    u0 = np.ascontiguousarray(np.transpose(tl.IsentropicVortex(5.0)(xy[0], xy[1], 0.0, eq), (2, 1, 0, 3))).reshape(-1)
+    o = oracle_mod.Oracle(mesh, 3)
+    u = u0.copy()
+    s, t = o.steps(u, 3, 0.5, 0.0, float("inf"))
+    assert s == 3 and 0.0 < t < float("inf")
+    u = u0.copy()
+    s, t = o.steps(u, 1000, 0.5, 0.0, 0.3)
+    assert t == 0.3 and 1 < s < 1000
+    s2, t2 = o.steps(u, 5, 0.5, t, 0.3)
+    assert s2 == 0 and t2 == 0.3
+    # within sqrt(eps) of the final time counts as finished
+    s3, _ = o.steps(u0.copy(), 5, 0.5, 0.3 * (1 - 1e-9), 0.3)
+    assert s3 == 0
+
+
+def test_host_isfinished_semantics(tl):
+    from trixilw.lwfr import LWIntegrator
+
+    integ = LWIntegrator.__new__(LWIntegrator)
+    for t, te, want in [(0.0, float("inf"), False), (1.0, 1.0, True), (1.0 - 1e-10, 1.0, True),
+                        (0.5, 1.0, False), (1e-20, 0.0, True)]:
+        integ.t, integ.tspan = t, (0.0, te)
+        assert integ.isfinished() is want

@@ -87,7 +87,7 @@ __device__ __forceinline__ void blend_interface_flux(const SurfArgs& a, int le, 
 }
 
 template <int N>
-__global__ void __launch_bounds__(128) interface_kernel(SurfArgs a) {
+static __global__ void __launch_bounds__(256) interface_kernel(SurfArgs a) {
     constexpr int n = N + 1;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = t / n;
@@ -148,7 +148,7 @@ struct BndArgs {
 };
 
 template <int N>
-__global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
+static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
     constexpr int n = N + 1;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int kk = t / n;
@@ -238,7 +238,7 @@ struct BatchSpeedArgs {
 };
 
 template <int N, bool SPEED, bool IND>
-__global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const double* __restrict__ u,
+static __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const double* __restrict__ u,
                                                                const double* __restrict__ inv_jac, int E,
                                                                double gamma, StepState* s, IndicatorArgs ia,
                                                                BatchSpeedArgs bs) {
@@ -351,6 +351,15 @@ __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const double* __r
 }
 
 // batched form: dt of every instance from its max scaled speed (finalize_dt_kernel per instance)
+// isfinished: t ≈ t_end (src/solvers/lwfr.jl:146-148) with Julia's isapprox (rtol = sqrt(eps(Float64)),
+// never true against an infinite t_end unless equal); t >= t_end cannot happen after the set_dt! clamp and
+// only guards against an endless run.
+__device__ __forceinline__ bool run_finished(double t, double te) {
+    if (t == te) return true;
+    if (!isfinite(t) || !isfinite(te)) return false;
+    return fabs(t - te) <= 1.4901161193847656e-8 * fmax(fabs(t), fabs(te)) || t >= te;
+}
+
 struct BatchTime {
     unsigned long long* max_bits;
     double* dt;
@@ -370,7 +379,7 @@ static __global__ void batch_finalize_dt_kernel(BatchTime b) {
     if (!(maxs > tiny)) maxs = tiny;
     double dt = b.cfl[k] * (2.0 / (b.nnodes[k] * maxs));
     const double t = b.t[k], te = b.t_end[k];
-    const bool finished = fabs(t - te) <= 1.4901161193847656e-8 * fmax(fabs(t), fabs(te)) || t >= te;
+    const bool finished = run_finished(t, te);
     if (finished) dt = 0.0;
     else if (t + dt > te) dt = te - t;
     b.dt[k] = dt;
@@ -399,8 +408,7 @@ static __global__ void finalize_dt_kernel(StepState* s, int n) {
     if (!(maxs > tiny)) maxs = tiny;
     double dt = s->fixed_dt > 0.0 ? s->fixed_dt : s->cfl * (2.0 / (n * maxs));
     const double t = s->t, te = s->t_end;
-    // isapprox(t, t_end) with Julia's default rtol = sqrt(eps(Float64))
-    const bool finished = fabs(t - te) <= 1.4901161193847656e-8 * fmax(fabs(t), fabs(te)) || t >= te;
+    const bool finished = run_finished(t, te);
     if (finished) dt = 0.0;
     else if (t + dt > te) dt = te - t;
     s->dt = dt;

@@ -259,7 +259,7 @@ __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, 
 //   depth 2: f_t = raw1/2,  f_tt = raw2;    depth 1: f_t = raw1/2
 // ------------------------------------------------------------------------------------------------
 template <int N, int MODE, bool SC, int EBX = 0>
-__global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
+static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
     using C = VolCfg<N, EBX>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     constexpr int DEPTH = N >= 4 ? 4 : N;
@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>::MIN_B
 // F2 = f + f_t/6, U2 = u + u_t/6 (stored whole for stage 2).
 // ------------------------------------------------------------------------------------------------
 template <int N, int MODE, bool SC>
-__global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk1_volume_kernel(VolArgs a) {
+static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk1_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS
 // F = F2 + f_t(u*)/3, U = U2 + u*_t/3.
 // ------------------------------------------------------------------------------------------------
 template <int N, int MODE, bool SC>
-__global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk2_volume_kernel(VolArgs a) {
+static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk2_volume_kernel(VolArgs a) {
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];

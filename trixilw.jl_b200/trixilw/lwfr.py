@@ -76,6 +76,10 @@ class LWIntegrator:
     def isfinished(self) -> bool:
         # integrator.t ≈ last(tspan) (src/solvers/lwfr.jl:147-149): Julia isapprox, rtol = sqrt(eps)
         te = self.tspan[1]
+        if self.t == te:
+            return True
+        if not (math.isfinite(self.t) and math.isfinite(te)):
+            return False
         return abs(self.t - te) <= math.sqrt(np.finfo(float).eps) * max(abs(self.t), abs(te)) or self.t >= te
 
 
