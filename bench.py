@@ -43,6 +43,8 @@ WORKLOADS = {
 # batched form: 512 independent vortex instances (per-instance seed 0..511: side from {8, 16, 32, 64}
 # elements, degree from {3, 4, 5}, strength ~ U[1, 5], centre ~ U[-2, 2]^2), 50 LW steps
 BATCH_WORKLOADS = {"batched512_vortex_lw": 512}
+# differentiable form: 128 x 128 TreeMesh, N = 4, 200 LW steps, checkpoints every 20 steps
+ADJOINT_WORKLOADS = {"adjoint128_vortex_lw": (7, 4, 200, 20)}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -633,19 +635,135 @@ def run_batched(args):
         dist.destroy_process_group()
 
 
+def run_adjoint(args):
+    """Gradient of J = 1/2 ||rho(T) - rho_target||^2 with respect to the discrete initial state by the
+    checkpointed discrete adjoint, against the cost of the plain forward solve; central finite differences
+    on 64 random unit directions check it."""
+    import numpy as np
+    import torch
+
+    import trixilw as tl
+    from trixilw import _lib
+    from trixilw.batch import compute_coefficients
+
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    level, N, nsteps, ck = ADJOINT_WORKLOADS[args.workload]
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), level)
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.LW()))
+    semi = tl.SemidiscretizationHyperbolic(mesh, tl.LW(), eq, tl.IsentropicVortex(5.0), solver, device=local_rank)
+    cfl = cfl_for(N)
+    u0 = compute_coefficients(mesh, N, tl.IsentropicVortex(5.0), eq)
+    u0 = u0 + 1e-3 * np.random.default_rng(0).standard_normal(u0.size)
+    ut0 = compute_coefficients(mesh, N, tl.IsentropicVortex(4.5), eq)
+    target = np.ascontiguousarray(tl.forward_record(semi, ut0, nsteps, cfl, ck)[0::4])
+    ndofs = semi.ndofs()
+    L = _lib.lib()
+    sp = ctypes.c_void_p()
+    L.tlw_get_stream(semi.handle, ctypes.byref(sp))
+    stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", local_rank))
+    # device-resident inputs for the timed calls
+    d_u0 = torch.tensor(u0, dtype=torch.float64, device="cuda")
+    d_target = torch.tensor(target, dtype=torch.float64, device="cuda")
+    d_grad = torch.empty_like(d_u0)
+    d_uT = torch.empty_like(d_u0)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+    J = ctypes.c_double()
+    ph = (ctypes.c_double * 3)()
+
+    def gradient(timing=False):
+        _lib.check(semi.handle, L.tlw_adjoint_solve(semi.handle, vp(d_u0), nsteps, cfl, ck, vp(d_target), vp(d_grad),
+                                                    ctypes.byref(J), vp(d_uT), _lib.TLW_WHERE_DEVICE,
+                                                    ph if timing else None))
+
+    def forward():
+        _lib.check(semi.handle, L.tlw_set_state(semi.handle, vp(d_u0), _lib.TLW_WHERE_DEVICE, 0.0))
+        _lib.check(semi.handle, L.tlw_step(semi.handle, nsteps, cfl, 0.0, 1e30, 1))
+
+    W = max(args.warmup, 3)
+    for _ in range(W):
+        forward()
+        gradient()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    time.sleep(0.3)
+    reps = max(1, min(args.steps, 5))
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for _ in range(reps):
+        forward()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    ev[2].record(stream)
+    for _ in range(reps):
+        gradient()
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = ev[0].elapsed_time(ev[1]) / reps
+    grad_ms = ev[2].elapsed_time(ev[3]) / reps
+    gradient(timing=True)
+    phases = tuple(ph)
+    clocks = sampler.stop()
+    # e2e through the public API with host arrays
+    e0 = time.perf_counter()
+    Jh, g_host, uT_host = tl.adjoint_solve(semi, u0, nsteps, cfl, ck, target)
+    e2e_s = time.perf_counter() - e0
+    # finite-difference check with the recorded dt sequence held fixed
+    dts = tl.adjoint.dt_sequence(semi, nsteps)
+
+    def Jf(x):
+        return 0.5 * np.sum((tl.solve_dts(semi, x, dts)[0::4] - target) ** 2)
+
+    rng = np.random.default_rng(0)
+    worst = 0.0
+    h = 1e-4
+    for _ in range(64):
+        d = rng.standard_normal(u0.size)
+        d /= np.linalg.norm(d)
+        d1 = (Jf(u0 + h * d) - Jf(u0 - h * d)) / (2 * h)
+        d2 = (Jf(u0 + 2 * h * d) - Jf(u0 - 2 * h * d)) / (4 * h)
+        ref = (4 * d1 - d2) / 3
+        worst = max(worst, abs(float(g_host @ d) - ref) / max(abs(ref), 1e-300))
+    value = ndofs * nsteps / (grad_ms * 1e-3)
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT + " (forward steps differentiated per second)",
+            "n_gpus": world, "steps": nsteps, "warmup": W, "ms_per_step": grad_ms / nsteps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "polydeg": N, "elements": mesh.n_elements, "ndofs": ndofs,
+                       "nsteps": nsteps, "checkpoint_every": ck, "cfl": cfl,
+                       "objective": "J = 1/2 sum over nodes (rho(T) - rho_target)^2, rho_target from a strength-4.5 run",
+                       "u0": "strength-5 vortex + N(0, 1e-3^2) noise (seed 0)", "repeats": reps},
+            "forward_solve_ms": fwd_ms, "gradient_ms": grad_ms, "gradient_cost_vs_forward": grad_ms / fwd_ms,
+            "phase_ms": {"forward_record": phases[0], "recompute": phases[1], "adjoint_steps": phases[2]},
+            "backward_cost_vs_forward": (phases[1] + phases[2]) / fwd_ms,
+            "J": Jh, "fd_check": {"directions": 64, "h": h, "max_rel_err": worst, "richardson": True},
+            "e2e": {"value": ndofs * nsteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * 5 * ndofs / nsteps,
+                    "d2h_bytes_per_step": 8 * 8 * ndofs / nsteps, "seconds": e2e_s},
+            "clocks": clocks,
+            "gpu_launches": reps * nsteps * (2 + 4 + 2),
+        }
+        print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="vortex_tree512_N4_lw", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS))
+    ap.add_argument("--workload", default="vortex_tree512_N4_lw", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + sorted(ADJOINT_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload in BATCH_WORKLOADS:
         run_batched(args)
+    elif args.workload in ADJOINT_WORKLOADS:
+        run_adjoint(args)
     else:
         run_ours(args)
 

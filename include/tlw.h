@@ -161,6 +161,34 @@ int tlw_rhs_lw_noalloc(int32_t polydeg, double gamma, int32_t surface_flux, int3
                        const int32_t* x_right, int32_t n_y_interfaces, const int32_t* y_left,
                        const int32_t* y_right, const double* u, double* du, double dt, void* stream);
 
+/* ---- Differentiable form: discrete adjoint of the LW step (periodic TreeMesh{2}, N = 3..5, LW, FR volume
+ * integral, Rusanov surface flux with either speed estimate) -----------------------------------------------
+ * No counterpart in the reference. What is differentiated is the reference's forward map of one step at a
+ * fixed dt, u_new = u + dt * rhs(u) (src/solvers/dgsem_tree/dg_2d.jl:28-83, src/solvers/lwfr.jl:212-230);
+ * the dt sequence of a run is recorded on the forward sweep and held fixed on the reverse sweep. */
+/* lam_out = (d u_new / d u)^T lam_in for one step from u at the given dt. Synchronous. */
+int tlw_adjoint_step(tlw_handle* h, double* lam_out, const double* lam_in, const double* u, double dt, int32_t where);
+/* Forward sweep of nsteps CFL steps from u0 (dt = cfl * max_dt(u) each step) that records the dt sequence
+ * and checkpoints the state every checkpoint_every steps; u(T) into uT_out (optional). Uses the handle's
+ * state buffers (the state set by tlw_set_state is overwritten). Synchronous. */
+int tlw_forward_record(tlw_handle* h, const double* u0, int32_t nsteps, double cfl, int32_t checkpoint_every,
+                       double* uT_out, int32_t where);
+/* Reverse sweep of the recorded run: grad_out = (d u(T) / d u0)^T lam_T, the states between checkpoints
+ * recomputed segment by segment. phase_ms (optional, 2 doubles): device time of the recomputation and of
+ * the adjoint steps (adds synchronisations). Synchronous. */
+int tlw_adjoint_sweep(tlw_handle* h, const double* lam_T, double* grad_out, int32_t where, double* phase_ms);
+/* Both sweeps for the objective
+ * J = 1/2 sum_nodes (rho(T) - rho_target)^2 (rho_target [i, j, element], one value per node), and the
+ * gradient dJ/du0 [v, i, j, element]. uT_out (optional) receives u(T). phase_ms (optional, 3 doubles): device
+ * time of the forward sweep (with the objective), of the recomputation and of the adjoint steps. */
+int tlw_adjoint_solve(tlw_handle* h, const double* u0, int32_t nsteps, double cfl, int32_t checkpoint_every,
+                      const double* rho_target, double* grad_out, double* J_out, double* uT_out, int32_t where,
+                      double* phase_ms);
+/* The dt of the first n steps of the recorded forward sweep (host array). */
+int tlw_adjoint_dt_sequence(tlw_handle* h, double* dts, int32_t n);
+/* Forward solve of nsteps LW steps from u0 at the given dt sequence (host array), u(T) into uT_out. Synchronous. */
+int tlw_solve_dts(tlw_handle* h, const double* u0, int32_t nsteps, const double* dts, double* uT_out, int32_t where);
+
 /* ---- Batched form: many independent periodic TreeMesh{2} LW runs (N = 3, 4, 5, uneven sizes) ----------
  * No counterpart in the reference, which runs one semidiscretization per `solve_lwfr` call
  * (src/solvers/lwfr.jl:233-270); each instance here advances exactly as that loop would advance it alone:

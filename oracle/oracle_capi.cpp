@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <memory>
 
+#include "tlw_adjoint.hpp"
 #include "tlw_oracle.hpp"
 
 using namespace tlwo;
@@ -93,6 +94,21 @@ int oracle_rhs(oracle_handle* h, int kind, const double* u, const double* u2, do
         BoundaryData bd{h->bnd_levels.empty() ? nullptr : h->bnd_levels.data(),
                         h->bnd_now.empty() ? nullptr : h->bnd_now.data()};
         rhs(h->basis, h->eq, h->opt, h->mesh, u, u2, du, t, dt, &bd, kind, h->ws, nthreads);
+        return h->ws.bad ? 3 : 0;
+    } catch (const std::exception& ex) {
+        std::snprintf(h->err, sizeof(h->err), "%s", ex.what());
+        return 1;
+    }
+}
+
+// lam_out = (d u_new / d u)^T lam_in for one LW step u_new = u + dt rhs(u) at fixed dt (periodic mesh,
+// FR volume integral, Rusanov flux). Returns 0, 3 (non-admissible state), 4 (unsupported options).
+int oracle_adjoint_step(oracle_handle* h, const double* u, double dt, const double* lam_in, double* lam_out,
+                        int nthreads) {
+    try {
+        if (h->opt.flux_kind != RUSANOV || h->opt.shock_capturing || h->mesh.n_boundaries || h->opt.N < 3) return 4;
+        h->ws.bad = false;
+        adjoint_step(h->basis, h->eq, h->opt, h->mesh, u, dt, lam_in, lam_out, h->ws, nthreads);
         return h->ws.bad ? 3 : 0;
     } catch (const std::exception& ex) {
         std::snprintf(h->err, sizeof(h->err), "%s", ex.what());

@@ -46,6 +46,7 @@ def lib():
         L.oracle_max_dt.argtypes = [P, P, dbl]
         L.oracle_max_dt.restype = dbl
         L.oracle_steps.argtypes = [P, i32, P, i32, dbl, dbl, P, dbl, i32]
+        L.oracle_adjoint_step.argtypes = [P, P, dbl, P, P, i32]
         L.oracle_last_error.argtypes = [P]
         L.oracle_last_error.restype = ctypes.c_char_p
         _L = L
@@ -121,6 +122,24 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(lib().oracle_last_error(self.h).decode())
         return du
+
+    def adjoint_step(self, u, dt, lam, nthreads: int = 1):
+        """(d u_new / d u)^T lam for one LW step u_new = u + dt rhs(u) at fixed dt."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        out = np.empty_like(u)
+        rc = lib().oracle_adjoint_step(self.h, _p(u), float(dt), _p(lam), _p(out), nthreads)
+        if rc == 3:
+            raise OracleDomainError("sqrt of a negative number")
+        if rc == 4:
+            raise ValueError("adjoint: periodic mesh, FR volume integral, Rusanov flux and N >= 3 only")
+        if rc != 0:
+            raise RuntimeError(lib().oracle_last_error(self.h).decode())
+        return out
+
+    def step_fixed(self, u, dt, nthreads: int = 1):
+        """One LW step u + dt rhs(u) at the given dt (returns a new array)."""
+        return u + dt * self.rhs(u, 0.0, dt, nthreads=nthreads)
 
     def get(self, which: int) -> np.ndarray:
         sizes = {0: self.size(), 1: 2 * self.size(), 2: self.size(), 3: 2 * self.size(), 4: self.E,

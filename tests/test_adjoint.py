@@ -1,0 +1,188 @@
+"""Discrete adjoint of the LW step: the oracle's restatement against finite differences (CPU), and the CUDA
+adjoint kernels, the checkpointed reverse sweep and the torch.autograd wrapper against the oracle (GPU).
+
+Tolerances: finite differences are central with Richardson extrapolation; the Rusanov speed and |v| are
+piecewise smooth, so a perturbation that crosses a kink limits FD accuracy to O(h): 1e-5 relative there.
+GPU against oracle: 1e-12 relative L2 per variable for one step, 1e-10 over a multi-step sweep."""
+import os
+
+import numpy as np
+import pytest
+
+NTH = os.cpu_count() or 1
+
+
+def rel_l2(a, b):
+    a = a.reshape(-1, 4)
+    b = b.reshape(-1, 4)
+    return np.linalg.norm(a - b, axis=0) / np.maximum(np.linalg.norm(b, axis=0), 1e-300)
+
+
+def vortex(tl, level, N, beta=5.0, center=(0.7, -0.4), noise=0.0, seed=0):
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), level)
+    from trixilw.batch import compute_coefficients
+    u = compute_coefficients(mesh, N, tl.IsentropicVortex(beta, center=center), eq)
+    if noise:
+        u = u + noise * np.random.default_rng(seed).standard_normal(u.size)
+    return eq, mesh, u
+
+
+def fd(J, u, d, h):
+    d1 = (J(u + h * d) - J(u - h * d)) / (2 * h)
+    d2 = (J(u + 2 * h * d) - J(u - 2 * h * d)) / (4 * h)
+    return (4 * d1 - d2) / 3
+
+
+def oracle_gradient(o, u0, dts, lam_T):
+    states = [u0]
+    for dt in dts[:-1]:
+        states.append(o.step_fixed(states[-1], dt, nthreads=NTH))
+    lam = lam_T
+    for u, dt in zip(reversed(states), reversed(dts)):
+        lam = o.adjoint_step(u, dt, lam, nthreads=NTH)
+    return lam
+
+
+# ---------------------------------------------------------------------------------------------- CPU
+@pytest.mark.parametrize("N,speed", [(3, 0), (4, 0), (4, 1), (5, 0)])
+def test_oracle_adjoint_step_matches_finite_differences(oracle_mod, tl, N, speed):
+    eq, mesh, u = vortex(tl, 2, N)
+    o = oracle_mod.Oracle(mesh, N, speed_kind=speed)
+    dt = o.max_dt(u, 0.4)
+    rng = np.random.default_rng(N)
+    lam = rng.standard_normal(u.size)
+    g = o.adjoint_step(u, dt, lam)
+    for _ in range(2):
+        d = rng.standard_normal(u.size)
+        ref = fd(lambda x: lam @ o.step_fixed(x, dt), u, d, 1e-6)
+        assert abs(g @ d - ref) <= 1e-5 * abs(ref)
+
+
+def test_oracle_multistep_gradient_matches_finite_differences(oracle_mod, tl):
+    """Stands in for forward-mode differentiation through the reference at 8x8 (no Julia here): the
+    oracle's reverse sweep over 10 fixed-dt steps against central differences of the oracle's forward."""
+    eq, mesh, u0 = vortex(tl, 3, 4, noise=1e-3)
+    o = oracle_mod.Oracle(mesh, 4)
+    dts = []
+    u = u0.copy()
+    for _ in range(10):
+        dt = o.max_dt(u, 0.5)
+        dts.append(dt)
+        u = o.step_fixed(u, dt, nthreads=NTH)
+    target = np.random.default_rng(1).uniform(0.9, 1.1, u.size // 4)
+
+    def J(x):
+        for dt in dts:
+            x = o.step_fixed(x, dt, nthreads=NTH)
+        return 0.5 * np.sum((x[0::4] - target) ** 2)
+
+    lam_T = np.zeros_like(u)
+    lam_T[0::4] = u[0::4] - target
+    g = oracle_gradient(o, u0, dts, lam_T)
+    rng = np.random.default_rng(2)
+    for _ in range(3):
+        d = rng.standard_normal(u0.size)
+        d /= np.linalg.norm(d)
+        ref = fd(J, u0, d, 1e-5)
+        assert abs(g @ d - ref) <= 1e-5 * abs(ref)
+
+
+def test_oracle_adjoint_rejects_unsupported(oracle_mod, tl):
+    eq, mesh, u = vortex(tl, 2, 4)
+    o = oracle_mod.Oracle(mesh, 4, flux_kind=1)
+    with pytest.raises(ValueError):
+        o.adjoint_step(u, 0.01, u)
+
+
+# ---------------------------------------------------------------------------------------------- GPU
+def make_semi(tl, mesh, N, speed="naive"):
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    flux = tl.FluxLaxFriedrichs(max_abs_speed=speed) if speed != "naive" else tl.flux_lax_friedrichs
+    solver = tl.DGSEM(N, flux, tl.VolumeIntegralFR(tl.LW()))
+    return tl.SemidiscretizationHyperbolic(mesh, tl.LW(), eq, tl.IsentropicVortex(5.0), solver)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,speed", [(3, 0), (4, 0), (4, 1), (5, 0), (5, 1)])
+def test_gpu_adjoint_step_matches_oracle(oracle_mod, tl, N, speed):
+    eq, mesh, u = vortex(tl, 3, N, noise=1e-3)
+    semi = make_semi(tl, mesh, N, "davis" if speed else "naive")
+    o = oracle_mod.Oracle(mesh, N, speed_kind=speed)
+    dt = o.max_dt(u, 0.4)
+    lam = np.random.default_rng(N).standard_normal(u.size)
+    g_cpu = o.adjoint_step(u, dt, lam, nthreads=NTH)
+    g_gpu = tl.adjoint_step(semi, lam, u, dt)
+    assert np.all(rel_l2(g_gpu, g_cpu) < 1e-12)
+
+
+@pytest.mark.gpu
+def test_gpu_fixed_dt_solve_matches_oracle(oracle_mod, tl):
+    eq, mesh, u0 = vortex(tl, 3, 4)
+    semi = make_semi(tl, mesh, 4)
+    o = oracle_mod.Oracle(mesh, 4)
+    dts = [0.05, 0.04, 0.045, 0.03]
+    u = u0.copy()
+    for dt in dts:
+        u = o.step_fixed(u, dt, nthreads=NTH)
+    assert np.all(rel_l2(tl.solve_dts(semi, u0, dts), u) < 1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ck", [1, 7, 25])
+def test_gpu_sweep_matches_oracle_and_checkpoint_interval(oracle_mod, tl, ck):
+    eq, mesh, u0 = vortex(tl, 3, 4, noise=1e-3)
+    semi = make_semi(tl, mesh, 4)
+    nsteps, cfl = 25, 0.4
+    uT = tl.forward_record(semi, u0, nsteps, cfl, ck)
+    dts = tl.adjoint.dt_sequence(semi, nsteps)
+    o = oracle_mod.Oracle(mesh, 4)
+    u = u0.copy()
+    for dt in dts:
+        u = o.step_fixed(u, dt, nthreads=NTH)
+    assert np.all(rel_l2(uT, u) < 1e-11)
+    lam_T = np.random.default_rng(3).standard_normal(u0.size)
+    g = tl.adjoint_sweep(semi, lam_T)
+    g_ref = oracle_gradient(o, u0, dts, lam_T)
+    assert np.all(rel_l2(g, g_ref) < 1e-10)
+    if ck != 1:
+        tl.forward_record(semi, u0, nsteps, cfl, 1)
+        np.testing.assert_array_equal(tl.adjoint_sweep(semi, lam_T), g)
+
+
+@pytest.mark.gpu
+def test_gpu_objective_gradient_finite_differences(tl):
+    """The differentiable-form check at a small size: J = 1/2 ||rho(T) - rho_target||^2 after 40 steps on
+    16x16, N = 4, checkpoints every 10 steps, 8 random unit directions, 1e-6 relative."""
+    eq, mesh, u0 = vortex(tl, 4, 4, beta=5.0, center=(0.0, 0.0), noise=1e-3)
+    semi = make_semi(tl, mesh, 4)
+    _, _, ut0 = vortex(tl, 4, 4, beta=4.5, center=(0.0, 0.0))
+    nsteps, cfl = 40, tl.trixi2lw(0.98, semi.solver)
+    target = tl.forward_record(semi, ut0, nsteps, cfl, 10)[0::4].copy()
+    J, g, uT = tl.adjoint_solve(semi, u0, nsteps, cfl, 10, target)
+    assert J == pytest.approx(0.5 * np.sum((uT[0::4] - target) ** 2), rel=1e-12)
+    dts = tl.adjoint.dt_sequence(semi, nsteps)
+
+    def Jf(x):
+        return 0.5 * np.sum((tl.solve_dts(semi, x, dts)[0::4] - target) ** 2)
+
+    rng = np.random.default_rng(0)
+    for _ in range(8):
+        d = rng.standard_normal(u0.size)
+        d /= np.linalg.norm(d)
+        ref = fd(Jf, u0, d, 1e-4)
+        assert abs(g @ d - ref) <= 1e-6 * abs(ref) + 1e-14
+
+
+@pytest.mark.gpu
+def test_torch_autograd_function(tl):
+    import torch
+    eq, mesh, u0 = vortex(tl, 3, 4, noise=1e-3)
+    semi = make_semi(tl, mesh, 4)
+    for dev in ("cpu", "cuda"):
+        x = torch.tensor(u0, dtype=torch.float64, device=dev, requires_grad=True)
+        y = tl.lw_solve(x, semi, 12, 0.4, 5)
+        w = torch.linspace(-1.0, 1.0, y.numel(), dtype=torch.float64, device=dev)
+        (y * w).sum().backward()
+        ref = tl.adjoint_sweep(semi, w.cpu().numpy())
+        np.testing.assert_array_equal(x.grad.cpu().numpy(), ref)

@@ -1,0 +1,892 @@
+// tlw_adjoint.cu -- the differentiable form: a hand-written discrete adjoint (vector-Jacobian product) of
+// the full Lax-Wendroff step on a periodic TreeMesh{2}, and a checkpointed reverse sweep over a whole run.
+//
+// What is differentiated is the forward map of one step at a fixed dt,
+//   u_new = u + dt * rhs(u)    (src/solvers/dgsem_tree/dg_2d.jl:28-83, perform_step! src/solvers/lwfr.jl:212-230)
+// with the LW volume procedure of depth 3 (N = 3, dg_2d.jl:674-916) or 4 (N >= 4, dg_2d.jl:918-1267), the
+// Rusanov interface flux in the TreeMesh argument order (dg_2d.jl:1903-1946: speed from the time-averaged
+// U, jump in the instantaneous u), the weak-form surface lift and apply_jacobian. The reference has no
+// adjoint; the step sizes of the forward run are recorded and held fixed in the reverse sweep, so the
+// gradient is that of the discrete solution map at the recorded dt sequence.
+//
+// Notation: d_1 = ut, d_2 = utt, ... are the dt-scaled time derivatives; C(x, y) = -dt J^{-1} (D x + D y)
+// produces the next one from the stage fluxes; the perturbed states of stage s are P_q = u + sum_{m<=s}
+// a[q][m] d_m, q in {-, +, --, ++}; ft_s = w_s[0] f(u) + sum_q w_s[q] f(P_q); the time averages are
+// F = f(u) + sum_s tw_s ft_s and U = u + sum_s tw_s d_s.
+//
+// Kernels (one adjoint step = two launches after a forward recompute that leaves the U traces):
+//   adj_interface_kernel<N>: per interface node, the adjoint of Fn = (F_L + F_R)/2 - lambda(U_L, U_R) (u_R - u_L)/2
+//     with the lift weights and -dt J^{-1}: adjoint face traces of F, U and u for both elements.
+//   adj_volume_kernel<N>: per element (one thread per node), recomputes d_1..d_depth, then runs the LW
+//     procedure backwards with the Euler flux Jacobians transposed at every perturbed state, the transposed
+//     contractions through shared memory, and writes lam_out = lam_in + (du_new/du)^T lam_in.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/tlw.h"
+#include "tlw_basis.h"
+#include "tlw_handle.h"
+#include "tlw_surface.cuh"
+#include "tlw_volume.cuh"
+
+using namespace tlw;
+
+namespace {
+
+int afail(tlw_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+#define TLW_ACUDA(h, call)                                                                       \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return afail(h, TLW_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+// ---- LW stencil constants (compile-time after unrolling) ------------------------------------------
+template <int DEPTH>
+struct LWC {
+    // Taylor weight of stage s = 1..4
+    static __device__ __forceinline__ constexpr double tw(int s) {
+        return s == 1 ? 0.5 : s == 2 ? 1.0 / 6.0 : s == 3 ? 1.0 / 24.0 : 1.0 / 120.0;
+    }
+    // perturbation coefficient of d_m in state q (0: -, 1: +, 2: --, 3: ++)
+    static __device__ __forceinline__ constexpr double a(int q, int m) {
+        return q == 0 ? (m == 1 ? -1.0 : m == 2 ? 0.5 : m == 3 ? -1.0 / 6.0 : 1.0 / 24.0)
+             : q == 1 ? (m == 1 ? 1.0 : m == 2 ? 0.5 : m == 3 ? 1.0 / 6.0 : 1.0 / 24.0)
+             : q == 2 ? (m == 1 ? -2.0 : m == 2 ? 2.0 : m == 3 ? -4.0 / 3.0 : 2.0 / 3.0)
+                      : (m == 1 ? 2.0 : m == 2 ? 2.0 : m == 3 ? 4.0 / 3.0 : 2.0 / 3.0);
+    }
+    // stencil weight of stage s: k = 0 -> f(u), k = 1 + q -> f(P_q)
+    static __device__ __forceinline__ constexpr double w(int s, int k) {
+        // stage 1: (-fpp + 8 fp - 8 fm + fmm) / 12
+        return s == 1 ? (k == 0 ? 0.0 : k == 1 ? -8.0 / 12.0 : k == 2 ? 8.0 / 12.0 : k == 3 ? 1.0 / 12.0 : -1.0 / 12.0)
+             // stage 2: depth 4 (-fpp + 16 fp - 30 f + 16 fm - fmm) / 12; depth 3 fp - 2 f + fm
+             : s == 2 ? (DEPTH == 4 ? (k == 0 ? -30.0 / 12.0 : k <= 2 ? 16.0 / 12.0 : -1.0 / 12.0)
+                                    : (k == 0 ? -2.0 : k <= 2 ? 1.0 : 0.0))
+             // stage 3: (fpp - 2 fp + 2 fm - fmm) / 2
+             : s == 3 ? (k == 0 ? 0.0 : k == 1 ? 1.0 : k == 2 ? -1.0 : k == 3 ? -0.5 : 0.5)
+             // stage 4: (fpp - 4 fp + 6 f - 4 fm + fmm) / 2
+                      : (k == 0 ? 3.0 : k <= 2 ? -2.0 : 0.5);
+    }
+};
+
+// out += Jf(u)^T wf + Jg(u)^T wg for the Euler fluxes (conservative variables)
+__device__ __forceinline__ void euler_flux_vjp(double gamma, const double* u, const double* wf, const double* wg,
+                                               double* out) {
+    const double gm1 = gamma - 1.0;
+    const double ir = nr_reciprocal(u[0]);
+    const double v1 = u[1] * ir, v2 = u[2] * ir;
+    const double q = 0.5 * (v1 * v1 + v2 * v2);
+    const double p = gm1 * (u[3] - u[0] * q);
+    const double H = (u[3] + p) * ir;
+    const double gq = gm1 * q, v12 = v1 * v2;
+    out[0] += wf[1] * (gq - v1 * v1) - (wf[2] + wg[1]) * v12 + wf[3] * v1 * (gq - H) + wg[2] * (gq - v2 * v2) +
+              wg[3] * v2 * (gq - H);
+    out[1] += wf[0] + wf[1] * (2.0 - gm1) * v1 + wf[2] * v2 + wf[3] * (H - gm1 * v1 * v1) + wg[1] * v2 -
+              wg[2] * gm1 * v1 - wg[3] * gm1 * v12;
+    out[2] += -wf[1] * gm1 * v2 + wf[2] * v1 - wf[3] * gm1 * v12 + wg[0] + wg[1] * v1 + wg[2] * (2.0 - gm1) * v2 +
+              wg[3] * (H - gm1 * v2 * v2);
+    out[3] += (wf[1] + wg[2]) * gm1 + gamma * (wf[3] * v1 + wg[3] * v2);
+}
+
+// gradients of |v_d| and c = sqrt(gamma p / rho) with respect to the conservative state; returns |v_d|, c
+__device__ __forceinline__ void speed_partials(double gamma, const double* u, int orientation, double* dv,
+                                               double* dc, double* absv, double* c, unsigned* status) {
+    const double gm1 = gamma - 1.0;
+    const double ir = 1.0 / u[0];
+    const double v1 = u[1] * ir, v2 = u[2] * ir;
+    const double q = 0.5 * (v1 * v1 + v2 * v2);
+    const double p = gm1 * (u[3] - 0.5 * (u[1] * v1 + u[2] * v2));
+    const double cc = checked_sqrt(gamma * p * ir, status);
+    const double vd = orientation == 1 ? v1 : v2;
+    const double sg = (vd > 0.0) - (vd < 0.0);
+    dv[0] = -sg * vd * ir;
+    dv[1] = orientation == 1 ? sg * ir : 0.0;
+    dv[2] = orientation == 2 ? sg * ir : 0.0;
+    dv[3] = 0.0;
+    const double k = gamma / (2.0 * cc * u[0]);
+    dc[0] = k * (gm1 * q - p * ir);
+    dc[1] = -k * gm1 * v1;
+    dc[2] = -k * gm1 * v2;
+    dc[3] = k * gm1;
+    *absv = fabs(vd);
+    *c = cc;
+}
+
+struct AdjSurfArgs {
+    const double* u;        // state of the step [v, i, j, e]
+    const double* tU;       // forward time-averaged U traces of the step [v, l, face, e]
+    const double* lam;      // adjoint of u_new [v, i, j, e]
+    double* bF;             // out: adjoint of the normal flux trace   [v, l, face, e]
+    double* bU;             // out: adjoint of the U trace             [v, l, face, e]
+    double* bu;             // out: direct adjoint of the u face value [v, l, face, e]
+    const int *xl, *xr, *yl, *yr;
+    int nx, ny;
+    const double* inv_jac;
+    const double* dt;
+    double gamma;
+    int speed_kind;
+    double inv_w_first, inv_w_last;
+    unsigned* status;
+};
+
+template <int N>
+static __global__ void __launch_bounds__(128) adj_interface_kernel(AdjSurfArgs a) {
+    constexpr int n = N + 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int k = t / n;
+    const int l = t - k * n;
+    int orientation = 1;
+    if (k >= a.nx) {
+        k -= a.nx;
+        orientation = 2;
+        if (k >= a.ny) return;
+    }
+    const int le = orientation == 1 ? __ldg(a.xl + k) : __ldg(a.yl + k);
+    const int re = orientation == 1 ? __ldg(a.xr + k) : __ldg(a.yr + k);
+    int nodeL, nodeR, faceL, faceR;
+    if (orientation == 1) { nodeL = (n - 1) + n * l; nodeR = n * l; faceL = 1; faceR = 0; }
+    else { nodeL = l + n * (n - 1); nodeR = l; faceL = 3; faceR = 2; }
+    double uL[NV], uR[NV], UL[NV], UR[NV], lL[NV], lR[NV];
+    load4(a.u + ((size_t)le * n * n + nodeL) * NV, uL);
+    load4(a.u + ((size_t)re * n * n + nodeR) * NV, uR);
+    load4(a.tU + (((size_t)le * 4 + faceL) * n + l) * NV, UL);
+    load4(a.tU + (((size_t)re * 4 + faceR) * n + l) * NV, UR);
+    load4(a.lam + ((size_t)le * n * n + nodeL) * NV, lL);
+    load4(a.lam + ((size_t)re * n * n + nodeR) * NV, lR);
+    const double dt = *a.dt;
+    const double sL = -dt * __ldg(a.inv_jac + le) * a.inv_w_last;
+    const double sR = dt * __ldg(a.inv_jac + re) * a.inv_w_first;
+    double bFn[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) bFn[v] = sL * lL[v] + sR * lR[v];
+    double dvL[NV], dcL[NV], dvR[NV], dcR[NV], vl, cl, vr, cr;
+    speed_partials(a.gamma, UL, orientation, dvL, dcL, &vl, &cl, a.status);
+    speed_partials(a.gamma, UR, orientation, dvR, dcR, &vr, &cr, a.status);
+    const double lambda = a.speed_kind == 0 ? fmax(vl, vr) + fmax(cl, cr) : fmax(vl + cl, vr + cr);
+    double blam = 0.0;
+    double o[NV];
+    const size_t tl = (((size_t)le * 4 + faceL) * n + l) * NV, tr = (((size_t)re * 4 + faceR) * n + l) * NV;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        blam -= 0.5 * bFn[v] * (uR[v] - uL[v]);
+        o[v] = 0.5 * bFn[v];
+    }
+    store4(a.bF + tl, o);
+    store4(a.bF + tr, o);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) o[v] = 0.5 * lambda * bFn[v];
+    store4(a.bu + tl, o);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) o[v] = -o[v];
+    store4(a.bu + tr, o);
+    double gL[NV] = {0.0, 0.0, 0.0, 0.0}, gR[NV] = {0.0, 0.0, 0.0, 0.0};
+    if (a.speed_kind == 0) {
+        // max(|v_L|, |v_R|) + max(c_L, c_R): the left argument wins ties
+        double* gv = vl >= vr ? gL : gR;
+        const double* dv = vl >= vr ? dvL : dvR;
+        double* gc = cl >= cr ? gL : gR;
+        const double* dc = cl >= cr ? dcL : dcR;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { gv[v] += blam * dv[v]; gc[v] += blam * dc[v]; }
+    } else {
+        const bool left = vl + cl >= vr + cr;
+        double* gs = left ? gL : gR;
+        const double* dv = left ? dvL : dvR;
+        const double* dc = left ? dcL : dcR;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) gs[v] += blam * (dv[v] + dc[v]);
+    }
+    store4(a.bU + tl, gL);
+    store4(a.bU + tr, gR);
+}
+
+template <int N>
+struct AdjCfg {
+    static constexpr int n = N + 1;
+    static constexpr int nn = n * n;
+    static constexpr int EB = VolCfg<N>::EB;
+    static constexpr int THREADS = VolCfg<N>::THREADS;
+    static constexpr int DEPTH = N >= 4 ? 4 : 3;
+    static constexpr size_t smem_bytes() { return (size_t)(2 * nn + 2 * NV * EB * nn) * sizeof(double); }
+};
+
+struct AdjVolArgs {
+    const double* u;        // state of the step
+    const double* lam;      // adjoint of u_new
+    double* lam_out;        // adjoint of u
+    const double* bF;       // adjoint face traces from adj_interface_kernel
+    const double* bU;
+    const double* bu;
+    const double* inv_jac;
+    const double* dt;
+    int E;
+    double gamma;
+};
+
+template <int N>
+static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, 1) adj_volume_kernel(AdjVolArgs a) {
+    using C = AdjCfg<N>;
+    using K = LWC<C::DEPTH>;
+    constexpr int n = C::n, nn = C::nn, EB = C::EB, DEPTH = C::DEPTH;
+    extern __shared__ double sm[];
+    double* sD = sm;
+    double* sDh = sm + nn;
+    double* X = sm + 2 * nn;
+    double* Y = X + NV * EB * nn;
+    for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+        sD[k] = c_tlw_D[N][k];
+        sDh[k] = c_tlw_Dhat[N][k];
+    }
+    const int el = threadIdx.x / nn;
+    const int node = threadIdx.x - el * nn;
+    const int i = node % n, j = node / n;
+    const long long e = (long long)blockIdx.x * EB + el;
+    const bool active = el < EB && e < a.E;
+    // threads past the last element slot of the CTA take part in the barriers only: they read slot 0 and
+    // write nothing to shared memory
+    const bool in_tile = el < EB;
+    const int slot = in_tile ? el : 0;
+    double sink = 0.0;
+    auto XS = [&](int v) -> double& { return in_tile ? X[(v * EB + slot) * nn + node] : sink; };
+    auto YS = [&](int v) -> double& { return in_tile ? Y[(v * EB + slot) * nn + node] : sink; };
+    double u[NV] = {1.0, 0.0, 0.0, 2.5};
+    double ij = 1.0;
+    if (active) {
+        load4(a.u + ((size_t)e * nn + node) * NV, u);
+        ij = __ldg(a.inv_jac + e);
+    }
+    const double dt = *a.dt;
+    const double sc = -dt * ij;
+    const double gm1 = a.gamma - 1.0;
+    // x contraction at this node of a shared field: sum_k M[i][k] F[k, j] (M row-major)
+    auto cx = [&](const double* M, const double* F, int v) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) s = fma(M[i * n + k], F[(v * EB + slot) * nn + k + n * j], s);
+        return s;
+    };
+    auto cy = [&](const double* M, const double* F, int v) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) s = fma(M[j * n + k], F[(v * EB + slot) * nn + i + n * k], s);
+        return s;
+    };
+    // transposed: sum_k M[k][i] W[k, j] and sum_k M[k][j] W[i, k]
+    auto cxt = [&](const double* M, const double* W, int v) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) s = fma(M[k * n + i], W[(v * EB + slot) * nn + k + n * j], s);
+        return s;
+    };
+    auto cyt = [&](const double* M, const double* W, int v) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) s = fma(M[k * n + j], W[(v * EB + slot) * nn + i + n * k], s);
+        return s;
+    };
+
+    // ---- forward recompute of d_1 .. d_DEPTH
+    double d[DEPTH][NV];
+    {
+        double f[NV], g[NV];
+        euler_fluxes(gm1, u[0], u[1], u[2], u[3], f, g);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { XS(v) = f[v]; YS(v) = g[v]; }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < NV; ++v) d[0][v] = sc * (cx(sD, X, v) + cy(sD, Y, v));
+    __syncthreads();
+#pragma unroll
+    for (int s = 1; s < DEPTH; ++s) {
+        double ft[NV] = {0.0, 0.0, 0.0, 0.0}, gt[NV] = {0.0, 0.0, 0.0, 0.0};
+        if (K::w(s, 0) != 0.0) {
+            double f[NV], g[NV];
+            euler_fluxes(gm1, u[0], u[1], u[2], u[3], f, g);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { ft[v] = K::w(s, 0) * f[v]; gt[v] = K::w(s, 0) * g[v]; }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (K::w(s, 1 + q) == 0.0) continue;
+            double P[NV], f[NV], g[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                double x = u[v];
+#pragma unroll
+                for (int m = 1; m <= s; ++m) x = fma(K::a(q, m), d[m - 1][v], x);
+                P[v] = x;
+            }
+            euler_fluxes(gm1, P[0], P[1], P[2], P[3], f, g);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { ft[v] = fma(K::w(s, 1 + q), f[v], ft[v]); gt[v] = fma(K::w(s, 1 + q), g[v], gt[v]); }
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { XS(v) = ft[v]; YS(v) = gt[v]; }
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < NV; ++v) d[s][v] = sc * (cx(sD, X, v) + cy(sD, Y, v));
+        __syncthreads();
+    }
+
+    // ---- adjoint inputs: volume term u_new += sc (Dhat F + Dhat G), then the face traces
+    double bF[NV], bG[NV], bU[NV] = {0.0, 0.0, 0.0, 0.0}, bud[NV] = {0.0, 0.0, 0.0, 0.0};
+    {
+        double lam[NV] = {0.0, 0.0, 0.0, 0.0};
+        if (active) load4(a.lam + ((size_t)e * nn + node) * NV, lam);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) XS(v) = sc * lam[v];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { bF[v] = cxt(sDh, X, v); bG[v] = cyt(sDh, X, v); }
+    __syncthreads();
+    if (active) {
+        auto face = [&](int f, int l, double* tgt) {
+            const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
+            double x[NV];
+            load4(a.bF + t, x);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) tgt[v] += x[v];
+            load4(a.bU + t, x);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) bU[v] += x[v];
+            load4(a.bu + t, x);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) bud[v] += x[v];
+        };
+        if (i == 0) face(0, j, bF);
+        if (i == n - 1) face(1, j, bF);
+        if (j == 0) face(2, i, bG);
+        if (j == n - 1) face(3, i, bG);
+    }
+
+    // ---- reverse sweep
+    double bd[DEPTH][NV], bu[NV], bf0[NV], bg0[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+#pragma unroll
+        for (int m = 0; m < DEPTH; ++m) bd[m][v] = K::tw(m + 1) * bU[v];
+        bu[v] = bU[v];
+        bf0[v] = bF[v];
+        bg0[v] = bG[v];
+    }
+#pragma unroll
+    for (int s = DEPTH; s >= 1; --s) {
+        double bfx[NV], bgy[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { bfx[v] = K::tw(s) * bF[v]; bgy[v] = K::tw(s) * bG[v]; }
+        if (s < DEPTH) {
+            // d_{s+1} = C(ft_s, gt_s)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) XS(v) = bd[s][v];
+            __syncthreads();
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { bfx[v] = fma(sc, cxt(sD, X, v), bfx[v]); bgy[v] = fma(sc, cyt(sD, X, v), bgy[v]); }
+            __syncthreads();
+        }
+        if (K::w(s, 0) != 0.0) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { bf0[v] = fma(K::w(s, 0), bfx[v], bf0[v]); bg0[v] = fma(K::w(s, 0), bgy[v], bg0[v]); }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (K::w(s, 1 + q) == 0.0) continue;
+            double P[NV], wf[NV], wg[NV], bP[NV] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                double x = u[v];
+#pragma unroll
+                for (int m = 1; m <= s; ++m) x = fma(K::a(q, m), d[m - 1][v], x);
+                P[v] = x;
+                wf[v] = K::w(s, 1 + q) * bfx[v];
+                wg[v] = K::w(s, 1 + q) * bgy[v];
+            }
+            euler_flux_vjp(a.gamma, P, wf, wg, bP);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                bu[v] += bP[v];
+#pragma unroll
+                for (int m = 1; m <= s; ++m) bd[m - 1][v] = fma(K::a(q, m), bP[v], bd[m - 1][v]);
+            }
+        }
+    }
+    // d_1 = C(f(u), g(u))
+#pragma unroll
+    for (int v = 0; v < NV; ++v) XS(v) = bd[0][v];
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { bf0[v] = fma(sc, cxt(sD, X, v), bf0[v]); bg0[v] = fma(sc, cyt(sD, X, v), bg0[v]); }
+    euler_flux_vjp(a.gamma, u, bf0, bg0, bu);
+    if (active) {
+        double lam[NV], o[NV];
+        load4(a.lam + ((size_t)e * nn + node) * NV, lam);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) o[v] = lam[v] + bu[v] + bud[v];
+        store4(a.lam_out + ((size_t)e * nn + node) * NV, o);
+    }
+}
+
+// J = 1/2 sum_nodes (rho - rho_target)^2: per-block partial sums (fixed order) and the seed lam = (rho - rho_t, 0, 0, 0)
+constexpr int OBJ_THREADS = 256;
+static __global__ void __launch_bounds__(OBJ_THREADS) objective_kernel(const double* u, const double* target,
+                                                                       long long nodes, double* partial, double* lam) {
+    __shared__ double red[OBJ_THREADS];
+    const long long k = (long long)blockIdx.x * OBJ_THREADS + threadIdx.x;
+    double r = 0.0;
+    if (k < nodes) {
+        r = u[k * NV] - target[k];
+        double o[NV] = {r, 0.0, 0.0, 0.0};
+        store4(lam + k * NV, o);
+    }
+    red[threadIdx.x] = 0.5 * r * r;
+    __syncthreads();
+    for (int w = OBJ_THREADS / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+static __global__ void __launch_bounds__(OBJ_THREADS) sum_kernel(const double* partial, int count, double* out) {
+    __shared__ double red[OBJ_THREADS];
+    double s = 0.0;
+    for (int k = threadIdx.x; k < count; k += OBJ_THREADS) s += partial[k];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = OBJ_THREADS / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+// ---- launches ---------------------------------------------------------------------------------------
+template <int N>
+struct AL {
+    static void set_attributes() {
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)VolCfg<N>::smem_bytes(4));
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)VolCfg<N>::smem_bytes(4));
+        cudaFuncSetAttribute(adj_volume_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)AdjCfg<N>::smem_bytes());
+    }
+    static void forward_volume(cudaStream_t s, int mode, const VolArgs& va) {
+        using C = VolCfg<N>;
+        const int grid = (int)((va.E + C::EB - 1) / C::EB);
+        if (mode == MODE_STEP) lw_volume_kernel<N, MODE_STEP, false><<<grid, C::THREADS, C::smem_bytes(4), s>>>(va);
+        else lw_volume_kernel<N, MODE_RHS, false><<<grid, C::THREADS, C::smem_bytes(4), s>>>(va);
+    }
+    static void forward_interfaces(cudaStream_t s, SurfArgs sa, const tlw_handle* h) {
+        sa.left = h->d_xl; sa.right = h->d_xr; sa.count = h->nx; sa.orientation = 1;
+        long long th = (long long)sa.count * (N + 1);
+        if (th) interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(sa);
+        sa.left = h->d_yl; sa.right = h->d_yr; sa.count = h->ny; sa.orientation = 2;
+        th = (long long)sa.count * (N + 1);
+        if (th) interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(sa);
+    }
+    static void speed(cudaStream_t s, const tlw_handle* h, const double* u) {
+        const int E = (int)h->E;
+        const int grid = (E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS;
+        max_speed_kernel<N, true, false><<<grid, MS_THREADS, 0, s>>>(u, h->d_inv_jac, E, h->opts.gamma, h->d_step,
+                                                                     IndicatorArgs{}, BatchSpeedArgs{});
+    }
+    static void adjoint(cudaStream_t s, const AdjSurfArgs& sa, const AdjVolArgs& va) {
+        const long long th = (long long)(sa.nx + sa.ny) * (N + 1);
+        if (th) adj_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(sa);
+        using C = AdjCfg<N>;
+        const int grid = (va.E + C::EB - 1) / C::EB;
+        adj_volume_kernel<N><<<grid, C::THREADS, C::smem_bytes(), s>>>(va);
+    }
+};
+
+template <class F>
+bool adj_degree(int N, F&& f) {
+    switch (N) {
+        case 3: f(std::integral_constant<int, 3>{}); return true;
+        case 4: f(std::integral_constant<int, 4>{}); return true;
+        case 5: f(std::integral_constant<int, 5>{}); return true;
+        default: return false;
+    }
+}
+
+size_t nstate(const tlw_handle* h) { return (size_t)NV * h->nn * h->E; }
+size_t ntrace(const tlw_handle* h) { return (size_t)NV * h->n * 4 * h->E; }
+
+int adj_ready(tlw_handle* h) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh) return afail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
+    if (h->opts.time_discretization != TLW_LW || h->sc || h->opts.surface_flux != TLW_FLUX_RUSANOV || h->nb > 0 ||
+        h->N < 3 || h->N > 5)
+        return afail(h, TLW_E_UNSUPPORTED,
+                     "adjoint: LW, FR volume integral, Rusanov flux, periodic TreeMesh, N = 3..5");
+    TLW_ACUDA(h, cudaSetDevice(h->device));
+    AdjointBuffers& A = h->adj;
+    if (!A.const_uploaded) {
+        Basis all[8];
+        std::memset(&all[0], 0, sizeof(all[0]));
+        for (int N = 1; N <= 7; ++N) host_build_basis(N, all[N]);
+        TLW_ACUDA(h, upload_const_basis(all));
+        adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::set_attributes(); });
+        A.const_uploaded = true;
+    }
+    if (A.E != h->E) {
+        const bool keep = A.const_uploaded;
+        free_adjoint(A);
+        A.const_uploaded = keep;
+        A.E = h->E;
+    }
+    if (!A.d_lam[0]) {
+        TLW_ACUDA(h, cudaMalloc(&A.d_lam[0], nstate(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_lam[1], nstate(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_bF, ntrace(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_bU, ntrace(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_bu, ntrace(h) * sizeof(double)));
+        const size_t blocks = ((size_t)h->nn * h->E + OBJ_THREADS - 1) / OBJ_THREADS;
+        TLW_ACUDA(h, cudaMalloc(&A.d_work, (blocks + 8) * sizeof(double)));
+    }
+    return TLW_OK;
+}
+
+int ensure_steps(tlw_handle* h, int nsteps, int ck) {
+    AdjointBuffers& A = h->adj;
+    if (A.capacity_steps < nsteps) {
+        dfree(A.d_dts);
+        TLW_ACUDA(h, cudaMalloc(&A.d_dts, (size_t)std::max(nsteps, 1) * sizeof(double)));
+        A.capacity_steps = std::max(nsteps, 1);
+    }
+    const int nck = (nsteps + ck - 1) / ck;
+    if (A.capacity_ckpt < nck) {
+        dfree(A.d_ckpt);
+        TLW_ACUDA(h, cudaMalloc(&A.d_ckpt, (size_t)std::max(nck, 1) * nstate(h) * sizeof(double)));
+        A.capacity_ckpt = std::max(nck, 1);
+    }
+    if (A.capacity_states < ck) {
+        dfree(A.d_seg);
+        dfree(A.d_segU);
+        TLW_ACUDA(h, cudaMalloc(&A.d_seg, (size_t)ck * nstate(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_segU, (size_t)ck * ntrace(h) * sizeof(double)));
+        A.capacity_states = ck;
+    }
+    return TLW_OK;
+}
+
+VolArgs fwd_vol_args(tlw_handle* h, const double* u, double* out, double* tU, const double* dtp) {
+    VolArgs va{};
+    va.u = u;
+    va.u_base = u;
+    va.out = out;
+    va.tU = tU;
+    va.tF = h->d_tF;
+    va.inv_jac = h->d_inv_jac;
+    va.dt = dtp;
+    va.basis = h->d_basis;
+    va.E = (int)h->E;
+    va.gamma = h->opts.gamma;
+    va.status = &h->d_step->status;
+    va.speed_kind = h->opts.max_speed;
+    return va;
+}
+
+SurfArgs fwd_surf_args(tlw_handle* h, const double* u, double* out, const double* tU, const double* dtp, int step) {
+    SurfArgs sa{};
+    sa.u = u;
+    sa.out = out;
+    sa.tU = tU;
+    sa.tF = h->d_tF;
+    sa.inv_jac = h->d_inv_jac;
+    sa.dt = dtp;
+    sa.step_mode = step;
+    sa.gamma = h->opts.gamma;
+    sa.flux_kind = h->opts.surface_flux;
+    sa.speed_kind = h->opts.max_speed;
+    sa.inv_w_first = h->h_basis.inv_w_first;
+    sa.inv_w_last = h->h_basis.inv_w_last;
+    sa.status = &h->d_step->status;
+    return sa;
+}
+
+// one forward LW step at the dt stored at dtp; U traces into tU
+void enqueue_fixed_step(tlw_handle* h, const double* u, double* unew, double* tU, const double* dtp) {
+    const VolArgs va = fwd_vol_args(h, u, unew, tU, dtp);
+    const SurfArgs sa = fwd_surf_args(h, u, unew, tU, dtp, 1);
+    adj_degree(h->N, [&](auto Nc) {
+        constexpr int N = decltype(Nc)::value;
+        AL<N>::forward_volume(h->stream, MODE_STEP, va);
+        AL<N>::forward_interfaces(h->stream, sa, h);
+    });
+}
+
+// lam_out = (du_new/du)^T lam_in for the step from u at dt (*dtp); tU = that step's forward U traces
+void enqueue_adjoint_step(tlw_handle* h, const double* u, const double* tU, const double* dtp, const double* lam_in,
+                          double* lam_out) {
+    AdjointBuffers& A = h->adj;
+    AdjSurfArgs sa{};
+    sa.u = u;
+    sa.tU = tU;
+    sa.lam = lam_in;
+    sa.bF = A.d_bF;
+    sa.bU = A.d_bU;
+    sa.bu = A.d_bu;
+    sa.xl = h->d_xl; sa.xr = h->d_xr; sa.yl = h->d_yl; sa.yr = h->d_yr;
+    sa.nx = h->nx; sa.ny = h->ny;
+    sa.inv_jac = h->d_inv_jac;
+    sa.dt = dtp;
+    sa.gamma = h->opts.gamma;
+    sa.speed_kind = h->opts.max_speed;
+    sa.inv_w_first = h->h_basis.inv_w_first;
+    sa.inv_w_last = h->h_basis.inv_w_last;
+    sa.status = &h->d_step->status;
+    AdjVolArgs va{};
+    va.u = u;
+    va.lam = lam_in;
+    va.lam_out = lam_out;
+    va.bF = A.d_bF;
+    va.bU = A.d_bU;
+    va.bu = A.d_bu;
+    va.inv_jac = h->d_inv_jac;
+    va.dt = dtp;
+    va.E = (int)h->E;
+    va.gamma = h->opts.gamma;
+    adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::adjoint(h->stream, sa, va); });
+}
+
+int adj_status(tlw_handle* h) {
+    TLW_ACUDA(h, cudaGetLastError());
+    unsigned st = 0;
+    TLW_ACUDA(h, cudaMemcpyAsync(&st, &h->d_step->status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    TLW_ACUDA(h, cudaStreamSynchronize(h->stream));
+    if (st) {
+        const unsigned zero = 0;
+        TLW_ACUDA(h, cudaMemcpy(&h->d_step->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+        return afail(h, TLW_E_NONADMISSIBLE, "non-admissible state: square root of a negative number (DomainError)");
+    }
+    return TLW_OK;
+}
+
+// copies n doubles from a caller pointer (host or device) into device memory on the handle's stream
+int copy_in(tlw_handle* h, double* dst, const double* src, size_t n, int where) {
+    TLW_ACUDA(h, cudaMemcpyAsync(dst, src, n * sizeof(double),
+                                 where == TLW_WHERE_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 h->stream));
+    return TLW_OK;
+}
+int copy_out(tlw_handle* h, double* dst, const double* src, size_t n, int where) {
+    TLW_ACUDA(h, cudaMemcpyAsync(dst, src, n * sizeof(double),
+                                 where == TLW_WHERE_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                 h->stream));
+    return TLW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tlw_adjoint_step(tlw_handle* h, double* lam_out, const double* lam_in, const double* u, double dt,
+                     int32_t where) {
+    int rc = adj_ready(h);
+    if (rc) return rc;
+    if (!lam_out || !lam_in || !u) return afail(h, TLW_E_ARG, "null array");
+    AdjointBuffers& A = h->adj;
+    if ((rc = ensure_steps(h, 1, 1))) return rc;
+    const size_t ns = nstate(h);
+    // u -> seg[0], lam_in -> lam[0], dt -> dts[0]
+    if ((rc = copy_in(h, A.d_seg, u, ns, where)) || (rc = copy_in(h, A.d_lam[0], lam_in, ns, where))) return rc;
+    TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    // forward rhs for the U traces (du into lam[1] as scratch), then the adjoint
+    const VolArgs va = fwd_vol_args(h, A.d_seg, A.d_lam[1], A.d_segU, A.d_dts);
+    adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::forward_volume(h->stream, MODE_RHS, va); });
+    enqueue_adjoint_step(h, A.d_seg, A.d_segU, A.d_dts, A.d_lam[0], A.d_lam[1]);
+    if ((rc = copy_out(h, lam_out, A.d_lam[1], ns, where))) return rc;
+    return adj_status(h);
+}
+
+int tlw_solve_dts(tlw_handle* h, const double* u0, int32_t nsteps, const double* dts, double* uT_out,
+                  int32_t where) {
+    int rc = adj_ready(h);
+    if (rc) return rc;
+    if (!u0 || !uT_out || (nsteps > 0 && !dts) || nsteps < 0) return afail(h, TLW_E_ARG, "arguments");
+    if ((rc = ensure_steps(h, nsteps, 1))) return rc;
+    AdjointBuffers& A = h->adj;
+    const size_t ns = nstate(h);
+    if ((rc = copy_in(h, A.d_lam[0], u0, ns, where))) return rc;
+    if (nsteps) TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts, dts, nsteps * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    int cur = 0;
+    for (int k = 0; k < nsteps; ++k) {
+        enqueue_fixed_step(h, A.d_lam[cur], A.d_lam[1 - cur], A.d_segU, A.d_dts + k);
+        cur ^= 1;
+    }
+    if ((rc = copy_out(h, uT_out, A.d_lam[cur], ns, where))) return rc;
+    return adj_status(h);
+}
+
+int tlw_forward_record(tlw_handle* h, const double* u0, int32_t nsteps, double cfl, int32_t checkpoint_every,
+                       double* uT_out, int32_t where) {
+    int rc = adj_ready(h);
+    if (rc) return rc;
+    if (!u0 || nsteps < 1 || checkpoint_every < 1 || !(cfl > 0.0)) return afail(h, TLW_E_ARG, "arguments");
+    const int ck = std::min<int>(checkpoint_every, nsteps);
+    if ((rc = ensure_steps(h, nsteps, ck))) return rc;
+    AdjointBuffers& A = h->adj;
+    A.rec_steps = 0;
+    const size_t ns = nstate(h);
+    // CFL dt recorded per step, checkpoints every ck steps; runs in the handle's two state buffers
+    StepState st{};
+    st.t = 0.0;
+    st.t_end = INFINITY;
+    st.cfl = cfl;
+    TLW_ACUDA(h, cudaMemcpyAsync(h->d_step, &st, sizeof(st), cudaMemcpyHostToDevice, h->stream));
+    double* s0 = h->d_state[0];
+    double* s1 = h->d_state[1];
+    if ((rc = copy_in(h, s0, u0, ns, where))) return rc;
+    for (int k = 0; k < nsteps; ++k) {
+        if (k % ck == 0)
+            TLW_ACUDA(h, cudaMemcpyAsync(A.d_ckpt + (size_t)(k / ck) * ns, s0, ns * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, h->stream));
+        adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::speed(h->stream, h, s0); });
+        finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
+        TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts + k, &h->d_step->dt, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        enqueue_fixed_step(h, s0, s1, h->d_tU, A.d_dts + k);
+        std::swap(s0, s1);
+    }
+    A.d_final = s0;
+    if (uT_out && (rc = copy_out(h, uT_out, s0, ns, where))) return rc;
+    if ((rc = adj_status(h))) return rc;
+    A.rec_steps = nsteps;
+    A.rec_ck = ck;
+    return TLW_OK;
+}
+
+namespace {
+
+// reverse sweep of the recorded run, starting from the adjoint in A.d_lam[cur]; cur ends at the buffer
+// that holds the gradient
+int reverse_sweep(tlw_handle* h, int& cur, double* phase_ms) {
+    AdjointBuffers& A = h->adj;
+    const size_t ns = nstate(h), nt = ntrace(h);
+    const int nsteps = A.rec_steps, ck = A.rec_ck;
+    const int nseg = (nsteps + ck - 1) / ck;
+    cudaEvent_t ev[2] = {};
+    if (phase_ms)
+        for (auto& x : ev) TLW_ACUDA(h, cudaEventCreate(&x));
+    float rec_ms = 0.0f, adj_ms = 0.0f;
+    for (int sgi = nseg - 1; sgi >= 0; --sgi) {
+        const int start = sgi * ck;
+        const int len = std::min(ck, nsteps - start);
+        if (phase_ms) cudaEventRecord(ev[0], h->stream);
+        // recompute the segment's states and U traces from its checkpoint
+        TLW_ACUDA(h, cudaMemcpyAsync(A.d_seg, A.d_ckpt + (size_t)sgi * ns, ns * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, h->stream));
+        for (int j = 0; j < len; ++j) {
+            if (j + 1 < len) {
+                enqueue_fixed_step(h, A.d_seg + (size_t)j * ns, A.d_seg + (size_t)(j + 1) * ns,
+                                   A.d_segU + (size_t)j * nt, A.d_dts + start + j);
+            } else {
+                // the segment's last output state is not needed, only the U traces of its step (volume
+                // kernel alone, its du into the free adjoint buffer)
+                const VolArgs va = fwd_vol_args(h, A.d_seg + (size_t)j * ns, A.d_lam[1 - cur],
+                                                A.d_segU + (size_t)j * nt, A.d_dts + start + j);
+                adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::forward_volume(h->stream, MODE_RHS, va); });
+            }
+        }
+        if (phase_ms) {
+            cudaEventRecord(ev[1], h->stream);
+            TLW_ACUDA(h, cudaEventSynchronize(ev[1]));
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev[0], ev[1]);
+            rec_ms += ms;
+        }
+        for (int j = len - 1; j >= 0; --j) {
+            enqueue_adjoint_step(h, A.d_seg + (size_t)j * ns, A.d_segU + (size_t)j * nt, A.d_dts + start + j,
+                                 A.d_lam[cur], A.d_lam[1 - cur]);
+            cur ^= 1;
+        }
+        if (phase_ms) {
+            cudaEventRecord(ev[0], h->stream);
+            TLW_ACUDA(h, cudaEventSynchronize(ev[0]));
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev[1], ev[0]);
+            adj_ms += ms;
+        }
+    }
+    if (phase_ms) {
+        phase_ms[0] = rec_ms;
+        phase_ms[1] = adj_ms;
+        for (auto& x : ev) cudaEventDestroy(x);
+    }
+    return TLW_OK;
+}
+
+}  // namespace
+
+int tlw_adjoint_sweep(tlw_handle* h, const double* lam_T, double* grad_out, int32_t where, double* phase_ms) {
+    int rc = adj_ready(h);
+    if (rc) return rc;
+    if (!lam_T || !grad_out) return afail(h, TLW_E_ARG, "null array");
+    if (h->adj.rec_steps < 1) return afail(h, TLW_E_STATE, "no recorded forward run: call tlw_forward_record first");
+    const size_t ns = nstate(h);
+    if ((rc = copy_in(h, h->adj.d_lam[0], lam_T, ns, where))) return rc;
+    int cur = 0;
+    if ((rc = reverse_sweep(h, cur, phase_ms))) return rc;
+    if ((rc = copy_out(h, grad_out, h->adj.d_lam[cur], ns, where))) return rc;
+    return adj_status(h);
+}
+
+int tlw_adjoint_solve(tlw_handle* h, const double* u0, int32_t nsteps, double cfl, int32_t checkpoint_every,
+                      const double* rho_target, double* grad_out, double* J_out, double* uT_out, int32_t where,
+                      double* phase_ms) {
+    if (!h || !rho_target || !grad_out) return TLW_E_ARG;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (phase_ms) {
+        TLW_ACUDA(h, cudaEventCreate(&e0));
+        TLW_ACUDA(h, cudaEventCreate(&e1));
+        TLW_ACUDA(h, cudaSetDevice(h->device));
+        cudaEventRecord(e0, h->stream);
+    }
+    int rc = tlw_forward_record(h, u0, nsteps, cfl, checkpoint_every, uT_out, where);
+    if (rc) return rc;
+    AdjointBuffers& A = h->adj;
+    const long long nodes = (long long)h->nn * h->E;
+    const int blocks = (int)((nodes + OBJ_THREADS - 1) / OBJ_THREADS);
+    double* d_target = A.d_bF;   // staged in the trace-adjoint buffer, which the sweep overwrites later
+    if ((size_t)nodes > ntrace(h)) return afail(h, TLW_E_ARG, "internal: target staging");
+    if ((rc = copy_in(h, d_target, rho_target, (size_t)nodes, where))) return rc;
+    objective_kernel<<<blocks, OBJ_THREADS, 0, h->stream>>>(A.d_final, d_target, nodes, A.d_work, A.d_lam[0]);
+    sum_kernel<<<1, OBJ_THREADS, 0, h->stream>>>(A.d_work, blocks, A.d_work + blocks);
+    double J = 0.0;
+    TLW_ACUDA(h, cudaMemcpyAsync(&J, A.d_work + blocks, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (phase_ms) cudaEventRecord(e1, h->stream);
+    int cur = 0;
+    if ((rc = reverse_sweep(h, cur, phase_ms ? phase_ms + 1 : nullptr))) return rc;
+    if ((rc = copy_out(h, grad_out, A.d_lam[cur], nodes * NV, where))) return rc;
+    rc = adj_status(h);
+    if (J_out) *J_out = J;
+    if (phase_ms) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        phase_ms[0] = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    return rc;
+}
+
+int tlw_adjoint_dt_sequence(tlw_handle* h, double* dts, int32_t n) {
+    if (!h || !dts || n < 0) return TLW_E_ARG;
+    if (n > h->adj.capacity_steps || !h->adj.d_dts) return afail(h, TLW_E_STATE, "no recorded dt sequence of that length");
+    TLW_ACUDA(h, cudaMemcpyAsync(dts, h->adj.d_dts, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TLW_ACUDA(h, cudaStreamSynchronize(h->stream));
+    return TLW_OK;
+}
+
+}  // extern "C"

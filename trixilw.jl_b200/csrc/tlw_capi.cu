@@ -16,53 +16,7 @@
 
 using namespace tlw;
 
-namespace {
-
-template <class T>
-void dfree(T*& p) {
-    if (p) cudaFree(p);
-    p = nullptr;
-}
-
-}  // namespace
-
-struct tlw_handle {
-    tlw_opts opts{};
-    int N = 0, n = 0, nn = 0;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    tlw::Basis h_basis{};
-    std::vector<double> nodes;
-    tlw::Basis* d_basis = nullptr;
-    StepState* d_step = nullptr;
-    // mesh
-    bool have_mesh = false;
-    int64_t E = 0;
-    double* d_inv_jac = nullptr;
-    int *d_xl = nullptr, *d_xr = nullptr, *d_yl = nullptr, *d_yr = nullptr;
-    int nx = 0, ny = 0;
-    int64_t nb = 0;
-    int *d_b_elem = nullptr, *d_b_dir = nullptr, *d_bx = nullptr, *d_by = nullptr;
-    int nbx = 0, nby = 0;
-    double *d_levels = nullptr, *d_now = nullptr;
-    bool have_bdata = false;
-    // element-sized buffers
-    double* d_state[2] = {nullptr, nullptr};
-    int cur = 0;
-    double* d_us = nullptr;
-    double *d_in = nullptr, *d_in2 = nullptr, *d_out = nullptr;
-    double *d_tU = nullptr, *d_tF = nullptr, *d_U2 = nullptr, *d_F2 = nullptr;
-    // shock capturing
-    bool sc = false;
-    double *d_alpha = nullptr, *d_alpha_raw = nullptr, *d_tFn = nullptr;
-    int *d_il = nullptr, *d_ir = nullptr;   // all interfaces (smoothing)
-    int ni = 0;
-    double jac_first = 0.0;                 // inverse Jacobian of element 1 (TreeMesh interface cache)
-    // graphs: [start buffer] one step, two steps
-    cudaGraphExec_t g_one[2] = {nullptr, nullptr};
-    cudaGraphExec_t g_two[2] = {nullptr, nullptr};
-};
+#include "tlw_handle.h"
 
 namespace {
 
@@ -99,6 +53,7 @@ void free_mesh(tlw_handle* h) {
     dfree(h->d_us); dfree(h->d_in); dfree(h->d_in2); dfree(h->d_out);
     dfree(h->d_tU); dfree(h->d_tF); dfree(h->d_U2); dfree(h->d_F2);
     dfree(h->d_alpha); dfree(h->d_alpha_raw); dfree(h->d_tFn); dfree(h->d_il); dfree(h->d_ir);
+    free_adjoint(h->adj);
     h->have_mesh = false;
     h->have_bdata = false;
 }

@@ -1,0 +1,85 @@
+// tlw_handle.h -- internal: the handle behind tlw_handle* (shared by the translation units of libtlw that
+// launch on a handle's mesh and buffers). Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/tlw.h"
+#include "tlw_device.cuh"
+#include "tlw_surface.cuh"
+
+namespace tlw {
+
+template <class T>
+inline void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+// device buffers of the discrete adjoint (allocated on first use by the adjoint entry points)
+struct AdjointBuffers {
+    int64_t E = 0;                          // element count the buffers were sized for
+    int capacity_steps = 0;                 // dt sequence capacity
+    int capacity_states = 0;                // states of one checkpoint segment
+    double* d_lam[2] = {nullptr, nullptr};  // adjoint state ping-pong
+    double *d_bF = nullptr, *d_bU = nullptr, *d_bu = nullptr;   // face-trace adjoints [v, l, face, e]
+    double* d_dts = nullptr;                // dt of every forward step
+    double* d_ckpt = nullptr;               // checkpoint states
+    int capacity_ckpt = 0;
+    double* d_seg = nullptr;                // recomputed states of one segment
+    double* d_segU = nullptr;               // time-averaged U traces of one segment
+    double* d_work = nullptr;               // scratch (objective partial sums)
+    double* d_final = nullptr;              // u(T) of the recorded run (one of the handle's state buffers)
+    int rec_steps = 0, rec_ck = 0;          // recorded forward run: steps, checkpoint interval
+    bool const_uploaded = false;            // the adjoint translation unit's constant bank is set
+};
+
+inline void free_adjoint(AdjointBuffers& a) {
+    dfree(a.d_lam[0]); dfree(a.d_lam[1]); dfree(a.d_bF); dfree(a.d_bU); dfree(a.d_bu); dfree(a.d_dts);
+    dfree(a.d_ckpt); dfree(a.d_seg); dfree(a.d_segU); dfree(a.d_work);
+    a = AdjointBuffers{};
+}
+
+}  // namespace tlw
+
+struct tlw_handle {
+    tlw_opts opts{};
+    int N = 0, n = 0, nn = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    tlw::Basis h_basis{};
+    std::vector<double> nodes;
+    tlw::Basis* d_basis = nullptr;
+    tlw::StepState* d_step = nullptr;
+    // mesh
+    bool have_mesh = false;
+    int64_t E = 0;
+    double* d_inv_jac = nullptr;
+    int *d_xl = nullptr, *d_xr = nullptr, *d_yl = nullptr, *d_yr = nullptr;
+    int nx = 0, ny = 0;
+    int64_t nb = 0;
+    int *d_b_elem = nullptr, *d_b_dir = nullptr, *d_bx = nullptr, *d_by = nullptr;
+    int nbx = 0, nby = 0;
+    double *d_levels = nullptr, *d_now = nullptr;
+    bool have_bdata = false;
+    // element-sized buffers
+    double* d_state[2] = {nullptr, nullptr};
+    int cur = 0;
+    double* d_us = nullptr;
+    double *d_in = nullptr, *d_in2 = nullptr, *d_out = nullptr;
+    double *d_tU = nullptr, *d_tF = nullptr, *d_U2 = nullptr, *d_F2 = nullptr;
+    // shock capturing
+    bool sc = false;
+    double *d_alpha = nullptr, *d_alpha_raw = nullptr, *d_tFn = nullptr;
+    int *d_il = nullptr, *d_ir = nullptr;   // all interfaces (smoothing)
+    int ni = 0;
+    double jac_first = 0.0;                 // inverse Jacobian of element 1 (TreeMesh interface cache)
+    // graphs: [start buffer] one step, two steps
+    cudaGraphExec_t g_one[2] = {nullptr, nullptr};
+    cudaGraphExec_t g_two[2] = {nullptr, nullptr};
+    // discrete adjoint
+    tlw::AdjointBuffers adj;
+};

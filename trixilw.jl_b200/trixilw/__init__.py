@@ -2,6 +2,7 @@
 compressible Euler, FP64). The compute runs in libtlw.so (CUDA, C ABI in include/tlw.h); this package is
 the host-side mirror of the reference's Julia interface for that path."""
 from ._lib import DomainError, TlwError, lib
+from .adjoint import adjoint_solve, adjoint_step, adjoint_sweep, forward_record, lw_solve, solve_dts
 from .batch import LWBatch, solve_lwfr_batch
 from .equations import (CompressibleEulerEquations2D, ConstantState, DensityWave, FourQuadrantRiemann,
                         IsentropicVortex)
@@ -22,4 +23,5 @@ __all__ = [
     "VolumeIntegralFRShockCapturing", "boundary_condition_periodic",
     "flux_hll", "flux_lax_friedrichs", "get_time_discretization", "lw_fourier_cfl", "rhs", "rhs_mdrk1",
     "rhs_mdrk2", "semidiscretize", "trixi2lw", "LWBatch", "solve_lwfr_batch",
+    "adjoint_solve", "adjoint_step", "adjoint_sweep", "forward_record", "lw_solve", "solve_dts",
 ]

@@ -36,6 +36,8 @@ EXPORTED = (
     "tlw_batch_create", "tlw_batch_destroy", "tlw_batch_add_tree_mesh", "tlw_batch_finalize",
     "tlw_batch_set_state", "tlw_batch_get_state", "tlw_batch_step", "tlw_batch_synchronize",
     "tlw_batch_get_stream", "tlw_batch_autotune", "tlw_batch_num_groups", "tlw_batch_last_error",
+    "tlw_adjoint_step", "tlw_forward_record", "tlw_adjoint_sweep", "tlw_adjoint_solve", "tlw_adjoint_dt_sequence",
+    "tlw_solve_dts",
 )
 
 
@@ -104,6 +106,12 @@ def lib() -> ctypes.CDLL:
     L.tlw_last_error.argtypes = [P]
     L.tlw_last_error.restype = ctypes.c_char_p
     i32p = ctypes.POINTER(ctypes.c_int32)
+    L.tlw_adjoint_step.argtypes = [P, P, P, P, dbl, i32]
+    L.tlw_forward_record.argtypes = [P, P, i32, dbl, i32, P, i32]
+    L.tlw_adjoint_sweep.argtypes = [P, P, P, i32, dp]
+    L.tlw_adjoint_solve.argtypes = [P, P, i32, dbl, i32, P, P, dp, P, i32, dp]
+    L.tlw_adjoint_dt_sequence.argtypes = [P, dp, i32]
+    L.tlw_solve_dts.argtypes = [P, P, i32, dp, P, i32]
     L.tlw_batch_create.argtypes = [ctypes.POINTER(TlwOpts), ctypes.POINTER(P)]
     L.tlw_batch_destroy.argtypes = [P]
     L.tlw_batch_add_tree_mesh.argtypes = [P, i32, i64, dp, i64, i64p, i64p, i32p]
