@@ -220,6 +220,8 @@ def run_reference(args):
         return
     if args.workload in BATCH_WORKLOADS:
         return run_reference_batched(args, world)
+    if args.workload in ADJOINT_WORKLOADS:
+        return run_reference_adjoint(args, world)
     level, N, td, icname = WORKLOADS[args.workload]
     # warm-up: one step; then K steps, each a bounded sample of the same workload (one full step)
     rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=max(1, args.steps), budget_s=60.0)
@@ -232,6 +234,54 @@ def run_reference(args):
         "config": {"workload": args.workload, "ndofs": ndofs, "polydeg": N, "time_discretization": td,
                    "elements": 1 << (2 * level), "implementation": "CPU oracle port (C++/OpenMP) of the TrixiLW "
                    "LW rhs; the Julia reference cannot run here"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_reference_adjoint(args, world):
+    """Oracle port: forward sweep with stored states, then the reverse sweep of oracle adjoint steps (all host
+    threads), on the same 128 x 128, N = 4 problem; as many steps as fit in about a minute."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle
+    import trixilw as tl
+    from trixilw.batch import compute_coefficients
+    level, N, nsteps, ck = ADJOINT_WORKLOADS[args.workload]
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), level)
+    u0 = compute_coefficients(mesh, N, tl.IsentropicVortex(5.0), eq)
+    u0 = u0 + 1e-3 * np.random.default_rng(0).standard_normal(u0.size)
+    threads = os.cpu_count() or 1
+    o = pyoracle.Oracle(mesh, N)
+    cfl = cfl_for(N)
+    t0 = time.perf_counter()
+    states, dts, u = [], [], u0
+    while len(dts) < nsteps and time.perf_counter() - t0 < 20.0:
+        dt = o.max_dt(u, cfl)
+        states.append(u)
+        dts.append(dt)
+        u = o.step_fixed(u, dt, nthreads=threads)
+    t_fwd = time.perf_counter() - t0
+    lam = np.zeros_like(u)
+    lam[0::4] = u[0::4] - 1.0
+    t1 = time.perf_counter()
+    for x, dt in zip(reversed(states), reversed(dts)):
+        lam = o.adjoint_step(x, dt, lam, nthreads=threads)
+    t_adj = time.perf_counter() - t1
+    k = len(dts)
+    ndofs = mesh.ndofs(N)
+    rate = ndofs * k / (t_fwd + t_adj)
+    sample = (f"{k} of {nsteps} steps of the {args.workload} problem: forward {t_fwd:.2f} s, reverse {t_adj:.2f} s "
+              "(states stored, no recomputation)")
+    out = {
+        "metric": METRIC, "value": rate, "unit": UNIT + " (forward steps differentiated per second)",
+        "impl": "reference", "n_gpus": world, "steps": k, "warmup": 0, "ms_per_step": 1e3 * (t_fwd + t_adj) / k,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "implementation": "CPU oracle port (C++/OpenMP) of the LW step and "
+                   "of its discrete adjoint; the reference has no adjoint and its Julia code cannot run here",
+                   "gradient_cost_vs_forward": (t_fwd + t_adj) / t_fwd},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

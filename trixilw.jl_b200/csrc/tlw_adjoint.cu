@@ -188,22 +188,25 @@ static __global__ void __launch_bounds__(128) adj_interface_kernel(AdjSurfArgs a
 #pragma unroll
     for (int v = 0; v < NV; ++v) o[v] = -o[v];
     store4(a.bu + tr, o);
-    double gL[NV] = {0.0, 0.0, 0.0, 0.0}, gR[NV] = {0.0, 0.0, 0.0, 0.0};
+    // speed adjoint goes to the side whose |v| (and c) the max selected; the left argument wins ties
+    double gL[NV], gR[NV];
     if (a.speed_kind == 0) {
-        // max(|v_L|, |v_R|) + max(c_L, c_R): the left argument wins ties
-        double* gv = vl >= vr ? gL : gR;
-        const double* dv = vl >= vr ? dvL : dvR;
-        double* gc = cl >= cr ? gL : gR;
-        const double* dc = cl >= cr ? dcL : dcR;
+        // max(|v_L|, |v_R|) + max(c_L, c_R)
+        const double wvL = vl >= vr ? blam : 0.0, wvR = blam - wvL;
+        const double wcL = cl >= cr ? blam : 0.0, wcR = blam - wcL;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) { gv[v] += blam * dv[v]; gc[v] += blam * dc[v]; }
+        for (int v = 0; v < NV; ++v) {
+            gL[v] = wvL * dvL[v] + wcL * dcL[v];
+            gR[v] = wvR * dvR[v] + wcR * dcR[v];
+        }
     } else {
-        const bool left = vl + cl >= vr + cr;
-        double* gs = left ? gL : gR;
-        const double* dv = left ? dvL : dvR;
-        const double* dc = left ? dcL : dcR;
+        // max(|v_L| + c_L, |v_R| + c_R)
+        const double wL = vl + cl >= vr + cr ? blam : 0.0, wR = blam - wL;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) gs[v] += blam * (dv[v] + dc[v]);
+        for (int v = 0; v < NV; ++v) {
+            gL[v] = wL * (dvL[v] + dcL[v]);
+            gR[v] = wR * (dvR[v] + dcR[v]);
+        }
     }
     store4(a.bU + tl, gL);
     store4(a.bU + tr, gR);
@@ -216,7 +219,12 @@ struct AdjCfg {
     static constexpr int EB = VolCfg<N>::EB;
     static constexpr int THREADS = VolCfg<N>::THREADS;
     static constexpr int DEPTH = N >= 4 ? 4 : 3;
-    static constexpr size_t smem_bytes() { return (size_t)(2 * nn + 2 * NV * EB * nn) * sizeof(double); }
+    // resident CTAs per SM the register budget must allow (stage derivatives and their adjoints live in
+    // shared memory, so the per-thread state is small)
+    static constexpr int MIN_BLOCKS = THREADS <= 128 ? 3 : 1;
+    // shared memory: D, Dhat, the two contraction tiles X, Y, the stage derivatives d_m and their adjoints
+    static constexpr int TILE = NV * EB * nn;
+    static constexpr size_t smem_bytes() { return (size_t)(2 * nn + (2 + 2 * DEPTH) * TILE) * sizeof(double); }
 };
 
 struct AdjVolArgs {
@@ -233,15 +241,17 @@ struct AdjVolArgs {
 };
 
 template <int N>
-static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, 1) adj_volume_kernel(AdjVolArgs a) {
+static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOCKS) adj_volume_kernel(AdjVolArgs a) {
     using C = AdjCfg<N>;
     using K = LWC<C::DEPTH>;
-    constexpr int n = C::n, nn = C::nn, EB = C::EB, DEPTH = C::DEPTH;
+    constexpr int n = C::n, nn = C::nn, EB = C::EB, DEPTH = C::DEPTH, TILE = C::TILE;
     extern __shared__ double sm[];
     double* sD = sm;
     double* sDh = sm + nn;
     double* X = sm + 2 * nn;
-    double* Y = X + NV * EB * nn;
+    double* Y = X + TILE;
+    double* Dm = Y + TILE;             // d_m,     m = 1..DEPTH at Dm + (m - 1) * TILE
+    double* Bm = Dm + DEPTH * TILE;    // bar d_m, same layout
     for (int k = threadIdx.x; k < nn; k += blockDim.x) {
         sD[k] = c_tlw_D[N][k];
         sDh[k] = c_tlw_Dhat[N][k];
@@ -255,9 +265,11 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, 1) adj_volume_kerne
     // write nothing to shared memory
     const bool in_tile = el < EB;
     const int slot = in_tile ? el : 0;
-    double sink = 0.0;
-    auto XS = [&](int v) -> double& { return in_tile ? X[(v * EB + slot) * nn + node] : sink; };
-    auto YS = [&](int v) -> double& { return in_tile ? Y[(v * EB + slot) * nn + node] : sink; };
+    const int me = slot * nn + node;   // this node's offset inside a variable plane of a tile
+    auto at = [&](double* T, int v) -> double* { return T + v * EB * nn + me; };
+    auto put = [&](double* T, int v, double x) {
+        if (in_tile) *at(T, v) = x;
+    };
     double u[NV] = {1.0, 0.0, 0.0, 2.5};
     double ij = 1.0;
     if (active) {
@@ -267,45 +279,63 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, 1) adj_volume_kerne
     const double dt = *a.dt;
     const double sc = -dt * ij;
     const double gm1 = a.gamma - 1.0;
-    // x contraction at this node of a shared field: sum_k M[i][k] F[k, j] (M row-major)
+    // x / y contraction of a shared tile at this node: sum_k M[i][k] F[k, j] and sum_k M[j][k] F[i, k]
     auto cx = [&](const double* M, const double* F, int v) {
+        const double* p = F + v * EB * nn + slot * nn + n * j;
         double s = 0.0;
 #pragma unroll
-        for (int k = 0; k < n; ++k) s = fma(M[i * n + k], F[(v * EB + slot) * nn + k + n * j], s);
+        for (int k = 0; k < n; ++k) s = fma(M[i * n + k], p[k], s);
         return s;
     };
     auto cy = [&](const double* M, const double* F, int v) {
+        const double* p = F + v * EB * nn + slot * nn + i;
         double s = 0.0;
 #pragma unroll
-        for (int k = 0; k < n; ++k) s = fma(M[j * n + k], F[(v * EB + slot) * nn + i + n * k], s);
+        for (int k = 0; k < n; ++k) s = fma(M[j * n + k], p[n * k], s);
         return s;
     };
     // transposed: sum_k M[k][i] W[k, j] and sum_k M[k][j] W[i, k]
     auto cxt = [&](const double* M, const double* W, int v) {
+        const double* p = W + v * EB * nn + slot * nn + n * j;
         double s = 0.0;
 #pragma unroll
-        for (int k = 0; k < n; ++k) s = fma(M[k * n + i], W[(v * EB + slot) * nn + k + n * j], s);
+        for (int k = 0; k < n; ++k) s = fma(M[k * n + i], p[k], s);
         return s;
     };
     auto cyt = [&](const double* M, const double* W, int v) {
+        const double* p = W + v * EB * nn + slot * nn + i;
         double s = 0.0;
 #pragma unroll
-        for (int k = 0; k < n; ++k) s = fma(M[k * n + j], W[(v * EB + slot) * nn + i + n * k], s);
+        for (int k = 0; k < n; ++k) s = fma(M[k * n + j], p[n * k], s);
         return s;
     };
+    // perturbed state q of stage s at this node
+    auto state = [&](int s, int q, double* P) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            double x = u[v];
+#pragma unroll
+            for (int m = 1; m <= s; ++m) x = fma(K::a(q, m), *at(Dm + (m - 1) * TILE, v), x);
+            P[v] = x;
+        }
+    };
 
-    // ---- forward recompute of d_1 .. d_DEPTH
-    double d[DEPTH][NV];
+    // ---- forward recompute of d_1 .. d_DEPTH (into shared memory)
     {
         double f[NV], g[NV];
         euler_fluxes(gm1, u[0], u[1], u[2], u[3], f, g);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) { XS(v) = f[v]; YS(v) = g[v]; }
+        for (int v = 0; v < NV; ++v) { put(X, v, f[v]); put(Y, v, g[v]); }
     }
     __syncthreads();
+    {
+        double d1[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) d[0][v] = sc * (cx(sD, X, v) + cy(sD, Y, v));
-    __syncthreads();
+        for (int v = 0; v < NV; ++v) d1[v] = sc * (cx(sD, X, v) + cy(sD, Y, v));
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < NV; ++v) put(Dm, v, d1[v]);
+    }
 #pragma unroll
     for (int s = 1; s < DEPTH; ++s) {
         double ft[NV] = {0.0, 0.0, 0.0, 0.0}, gt[NV] = {0.0, 0.0, 0.0, 0.0};
@@ -319,23 +349,20 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, 1) adj_volume_kerne
         for (int q = 0; q < 4; ++q) {
             if (K::w(s, 1 + q) == 0.0) continue;
             double P[NV], f[NV], g[NV];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                double x = u[v];
-#pragma unroll
-                for (int m = 1; m <= s; ++m) x = fma(K::a(q, m), d[m - 1][v], x);
-                P[v] = x;
-            }
+            state(s, q, P);
             euler_fluxes(gm1, P[0], P[1], P[2], P[3], f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { ft[v] = fma(K::w(s, 1 + q), f[v], ft[v]); gt[v] = fma(K::w(s, 1 + q), g[v], gt[v]); }
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) { XS(v) = ft[v]; YS(v) = gt[v]; }
+        for (int v = 0; v < NV; ++v) { put(X, v, ft[v]); put(Y, v, gt[v]); }
+        __syncthreads();
+        double dn[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) dn[v] = sc * (cx(sD, X, v) + cy(sD, Y, v));
         __syncthreads();
 #pragma unroll
-        for (int v = 0; v < NV; ++v) d[s][v] = sc * (cx(sD, X, v) + cy(sD, Y, v));
-        __syncthreads();
+        for (int v = 0; v < NV; ++v) put(Dm + s * TILE, v, dn[v]);
     }
 
     // ---- adjoint inputs: volume term u_new += sc (Dhat F + Dhat G), then the face traces
@@ -344,12 +371,11 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, 1) adj_volume_kerne
         double lam[NV] = {0.0, 0.0, 0.0, 0.0};
         if (active) load4(a.lam + ((size_t)e * nn + node) * NV, lam);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) XS(v) = sc * lam[v];
+        for (int v = 0; v < NV; ++v) put(X, v, sc * lam[v]);
     }
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < NV; ++v) { bF[v] = cxt(sDh, X, v); bG[v] = cyt(sDh, X, v); }
-    __syncthreads();
     if (active) {
         auto face = [&](int f, int l, double* tgt) {
             const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
@@ -370,12 +396,12 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, 1) adj_volume_kerne
         if (j == n - 1) face(3, i, bG);
     }
 
-    // ---- reverse sweep
-    double bd[DEPTH][NV], bu[NV], bf0[NV], bg0[NV];
+    // ---- reverse sweep (bar d_m accumulate in shared memory, each thread on its own node)
+    double bu[NV], bf0[NV], bg0[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
 #pragma unroll
-        for (int m = 0; m < DEPTH; ++m) bd[m][v] = K::tw(m + 1) * bU[v];
+        for (int m = 0; m < DEPTH; ++m) put(Bm + m * TILE, v, K::tw(m + 1) * bU[v]);
         bu[v] = bU[v];
         bf0[v] = bF[v];
         bg0[v] = bG[v];
@@ -386,13 +412,13 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, 1) adj_volume_kerne
 #pragma unroll
         for (int v = 0; v < NV; ++v) { bfx[v] = K::tw(s) * bF[v]; bgy[v] = K::tw(s) * bG[v]; }
         if (s < DEPTH) {
-            // d_{s+1} = C(ft_s, gt_s)
-#pragma unroll
-            for (int v = 0; v < NV; ++v) XS(v) = bd[s][v];
+            // d_{s+1} = C(ft_s, gt_s): its adjoint is complete (stages > s are done)
             __syncthreads();
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { bfx[v] = fma(sc, cxt(sD, X, v), bfx[v]); bgy[v] = fma(sc, cyt(sD, X, v), bgy[v]); }
-            __syncthreads();
+            for (int v = 0; v < NV; ++v) {
+                bfx[v] = fma(sc, cxt(sD, Bm + s * TILE, v), bfx[v]);
+                bgy[v] = fma(sc, cyt(sD, Bm + s * TILE, v), bgy[v]);
+            }
         }
         if (K::w(s, 0) != 0.0) {
 #pragma unroll
@@ -402,12 +428,9 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, 1) adj_volume_kerne
         for (int q = 0; q < 4; ++q) {
             if (K::w(s, 1 + q) == 0.0) continue;
             double P[NV], wf[NV], wg[NV], bP[NV] = {0.0, 0.0, 0.0, 0.0};
+            state(s, q, P);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-                double x = u[v];
-#pragma unroll
-                for (int m = 1; m <= s; ++m) x = fma(K::a(q, m), d[m - 1][v], x);
-                P[v] = x;
                 wf[v] = K::w(s, 1 + q) * bfx[v];
                 wg[v] = K::w(s, 1 + q) * bgy[v];
             }
@@ -415,17 +438,17 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, 1) adj_volume_kerne
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 bu[v] += bP[v];
+                if (in_tile) {
 #pragma unroll
-                for (int m = 1; m <= s; ++m) bd[m - 1][v] = fma(K::a(q, m), bP[v], bd[m - 1][v]);
+                    for (int m = 1; m <= s; ++m) *at(Bm + (m - 1) * TILE, v) = fma(K::a(q, m), bP[v], *at(Bm + (m - 1) * TILE, v));
+                }
             }
         }
     }
     // d_1 = C(f(u), g(u))
-#pragma unroll
-    for (int v = 0; v < NV; ++v) XS(v) = bd[0][v];
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < NV; ++v) { bf0[v] = fma(sc, cxt(sD, X, v), bf0[v]); bg0[v] = fma(sc, cyt(sD, X, v), bg0[v]); }
+    for (int v = 0; v < NV; ++v) { bf0[v] = fma(sc, cxt(sD, Bm, v), bf0[v]); bg0[v] = fma(sc, cyt(sD, Bm, v), bg0[v]); }
     euler_flux_vjp(a.gamma, u, bf0, bg0, bu);
     if (active) {
         double lam[NV], o[NV];
@@ -560,6 +583,13 @@ int adj_ready(tlw_handle* h) {
 
 int ensure_steps(tlw_handle* h, int nsteps, int ck) {
     AdjointBuffers& A = h->adj;
+    // captured sweeps hold the buffer addresses: drop them when a buffer is replaced
+    auto drop = [&]() {
+        if (A.g_fwd) cudaGraphExecDestroy(A.g_fwd);
+        if (A.g_rev) cudaGraphExecDestroy(A.g_rev);
+        A.g_fwd = A.g_rev = nullptr;
+    };
+    if (A.capacity_steps < nsteps || A.capacity_ckpt < (nsteps + ck - 1) / ck || A.capacity_states < ck) drop();
     if (A.capacity_steps < nsteps) {
         dfree(A.d_dts);
         TLW_ACUDA(h, cudaMalloc(&A.d_dts, (size_t)std::max(nsteps, 1) * sizeof(double)));
@@ -577,6 +607,17 @@ int ensure_steps(tlw_handle* h, int nsteps, int ck) {
         TLW_ACUDA(h, cudaMalloc(&A.d_seg, (size_t)ck * nstate(h) * sizeof(double)));
         TLW_ACUDA(h, cudaMalloc(&A.d_segU, (size_t)ck * ntrace(h) * sizeof(double)));
         A.capacity_states = ck;
+    }
+    return TLW_OK;
+}
+
+// caller-given dt sequences (tlw_solve_dts, tlw_adjoint_step) live apart from the recorded one
+int ensure_given_dts(tlw_handle* h, int nsteps) {
+    AdjointBuffers& A = h->adj;
+    if (A.capacity_given < nsteps) {
+        dfree(A.d_dts_given);
+        TLW_ACUDA(h, cudaMalloc(&A.d_dts_given, (size_t)nsteps * sizeof(double)));
+        A.capacity_given = nsteps;
     }
     return TLW_OK;
 }
@@ -688,6 +729,31 @@ int copy_out(tlw_handle* h, double* dst, const double* src, size_t n, int where)
     return TLW_OK;
 }
 
+// captures what body() enqueues on the handle's stream into exec (replaced if present)
+template <class F>
+int capture_graph(tlw_handle* h, cudaGraphExec_t& exec, F&& body) {
+    if (exec) {
+        cudaGraphExecDestroy(exec);
+        exec = nullptr;
+    }
+    TLW_ACUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return afail(h, TLW_E_CUDA, std::string("adjoint graph capture: ") + cudaGetErrorString(e));
+    const cudaError_t e2 = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) {
+        exec = nullptr;
+        return afail(h, TLW_E_CUDA, std::string("adjoint graph instantiate: ") + cudaGetErrorString(e2));
+    }
+    return TLW_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -701,12 +767,13 @@ int tlw_adjoint_step(tlw_handle* h, double* lam_out, const double* lam_in, const
     if ((rc = ensure_steps(h, 1, 1))) return rc;
     const size_t ns = nstate(h);
     // u -> seg[0], lam_in -> lam[0], dt -> dts[0]
+    if ((rc = ensure_given_dts(h, 1))) return rc;
     if ((rc = copy_in(h, A.d_seg, u, ns, where)) || (rc = copy_in(h, A.d_lam[0], lam_in, ns, where))) return rc;
-    TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts_given, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
     // forward rhs for the U traces (du into lam[1] as scratch), then the adjoint
-    const VolArgs va = fwd_vol_args(h, A.d_seg, A.d_lam[1], A.d_segU, A.d_dts);
+    const VolArgs va = fwd_vol_args(h, A.d_seg, A.d_lam[1], A.d_segU, A.d_dts_given);
     adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::forward_volume(h->stream, MODE_RHS, va); });
-    enqueue_adjoint_step(h, A.d_seg, A.d_segU, A.d_dts, A.d_lam[0], A.d_lam[1]);
+    enqueue_adjoint_step(h, A.d_seg, A.d_segU, A.d_dts_given, A.d_lam[0], A.d_lam[1]);
     if ((rc = copy_out(h, lam_out, A.d_lam[1], ns, where))) return rc;
     return adj_status(h);
 }
@@ -716,14 +783,16 @@ int tlw_solve_dts(tlw_handle* h, const double* u0, int32_t nsteps, const double*
     int rc = adj_ready(h);
     if (rc) return rc;
     if (!u0 || !uT_out || (nsteps > 0 && !dts) || nsteps < 0) return afail(h, TLW_E_ARG, "arguments");
-    if ((rc = ensure_steps(h, nsteps, 1))) return rc;
+    // dt array of nsteps, one trace buffer; no checkpoints
+    if ((rc = ensure_steps(h, 1, 1))) return rc;
     AdjointBuffers& A = h->adj;
+    if ((rc = ensure_given_dts(h, nsteps))) return rc;
     const size_t ns = nstate(h);
     if ((rc = copy_in(h, A.d_lam[0], u0, ns, where))) return rc;
-    if (nsteps) TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts, dts, nsteps * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (nsteps) TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts_given, dts, nsteps * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     int cur = 0;
     for (int k = 0; k < nsteps; ++k) {
-        enqueue_fixed_step(h, A.d_lam[cur], A.d_lam[1 - cur], A.d_segU, A.d_dts + k);
+        enqueue_fixed_step(h, A.d_lam[cur], A.d_lam[1 - cur], A.d_segU, A.d_dts_given + k);
         cur ^= 1;
     }
     if ((rc = copy_out(h, uT_out, A.d_lam[cur], ns, where))) return rc;
@@ -746,20 +815,32 @@ int tlw_forward_record(tlw_handle* h, const double* u0, int32_t nsteps, double c
     st.t_end = INFINITY;
     st.cfl = cfl;
     TLW_ACUDA(h, cudaMemcpyAsync(h->d_step, &st, sizeof(st), cudaMemcpyHostToDevice, h->stream));
-    double* s0 = h->d_state[0];
-    double* s1 = h->d_state[1];
-    if ((rc = copy_in(h, s0, u0, ns, where))) return rc;
-    for (int k = 0; k < nsteps; ++k) {
-        if (k % ck == 0)
-            TLW_ACUDA(h, cudaMemcpyAsync(A.d_ckpt + (size_t)(k / ck) * ns, s0, ns * sizeof(double),
-                                         cudaMemcpyDeviceToDevice, h->stream));
-        adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::speed(h->stream, h, s0); });
-        finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
-        TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts + k, &h->d_step->dt, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-        enqueue_fixed_step(h, s0, s1, h->d_tU, A.d_dts + k);
-        std::swap(s0, s1);
+    if ((rc = copy_in(h, h->d_state[0], u0, ns, where))) return rc;
+    // the whole sweep is one CUDA graph, captured once per (nsteps, checkpoint interval, buffers)
+    auto body = [&]() -> int {
+        double* s0 = h->d_state[0];
+        double* s1 = h->d_state[1];
+        for (int k = 0; k < nsteps; ++k) {
+            if (k % ck == 0)
+                TLW_ACUDA(h, cudaMemcpyAsync(A.d_ckpt + (size_t)(k / ck) * ns, s0, ns * sizeof(double),
+                                             cudaMemcpyDeviceToDevice, h->stream));
+            adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::speed(h->stream, h, s0); });
+            finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
+            TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts + k, &h->d_step->dt, sizeof(double), cudaMemcpyDeviceToDevice,
+                                         h->stream));
+            enqueue_fixed_step(h, s0, s1, h->d_tU, A.d_dts + k);
+            std::swap(s0, s1);
+        }
+        return TLW_OK;
+    };
+    const long long key = (long long)nsteps * 100003 + ck;
+    if (!A.g_fwd || A.g_fwd_key != key) {
+        if ((rc = capture_graph(h, A.g_fwd, body))) return rc;
+        A.g_fwd_key = key;
     }
-    A.d_final = s0;
+    TLW_ACUDA(h, cudaGraphLaunch(A.g_fwd, h->stream));
+    A.d_final = h->d_state[nsteps % 2];
+    double* s0 = A.d_final;
     if (uT_out && (rc = copy_out(h, uT_out, s0, ns, where))) return rc;
     if ((rc = adj_status(h))) return rc;
     A.rec_steps = nsteps;
@@ -771,7 +852,25 @@ namespace {
 
 // reverse sweep of the recorded run, starting from the adjoint in A.d_lam[cur]; cur ends at the buffer
 // that holds the gradient
+int reverse_sweep_enqueue(tlw_handle* h, int& cur, double* phase_ms);
+
 int reverse_sweep(tlw_handle* h, int& cur, double* phase_ms) {
+    if (phase_ms) return reverse_sweep_enqueue(h, cur, phase_ms);
+    AdjointBuffers& A = h->adj;
+    const long long key = (long long)A.rec_steps * 100003 + A.rec_ck;
+    if (cur != 0) return afail(h, TLW_E_ARG, "internal: sweep start buffer");
+    if (!A.g_rev || A.g_rev_key != key) {
+        int c = 0;
+        int rc = capture_graph(h, A.g_rev, [&]() { return reverse_sweep_enqueue(h, c, nullptr); });
+        if (rc) return rc;
+        A.g_rev_key = key;
+    }
+    TLW_ACUDA(h, cudaGraphLaunch(A.g_rev, h->stream));
+    cur = A.rec_steps % 2;
+    return TLW_OK;
+}
+
+int reverse_sweep_enqueue(tlw_handle* h, int& cur, double* phase_ms) {
     AdjointBuffers& A = h->adj;
     const size_t ns = nstate(h), nt = ntrace(h);
     const int nsteps = A.rec_steps, ck = A.rec_ck;

@@ -25,7 +25,9 @@ struct AdjointBuffers {
     int capacity_states = 0;                // states of one checkpoint segment
     double* d_lam[2] = {nullptr, nullptr};  // adjoint state ping-pong
     double *d_bF = nullptr, *d_bU = nullptr, *d_bu = nullptr;   // face-trace adjoints [v, l, face, e]
-    double* d_dts = nullptr;                // dt of every forward step
+    double* d_dts = nullptr;                // dt of every recorded forward step
+    double* d_dts_given = nullptr;          // dt sequence given by the caller (fixed-dt solves)
+    int capacity_given = 0;
     double* d_ckpt = nullptr;               // checkpoint states
     int capacity_ckpt = 0;
     double* d_seg = nullptr;                // recomputed states of one segment
@@ -33,12 +35,18 @@ struct AdjointBuffers {
     double* d_work = nullptr;               // scratch (objective partial sums)
     double* d_final = nullptr;              // u(T) of the recorded run (one of the handle's state buffers)
     int rec_steps = 0, rec_ck = 0;          // recorded forward run: steps, checkpoint interval
+    // the forward and reverse sweeps as CUDA graphs, keyed by (steps, interval); dropped whenever a buffer
+    // they address is replaced
+    cudaGraphExec_t g_fwd = nullptr, g_rev = nullptr;
+    long long g_fwd_key = -1, g_rev_key = -1;
     bool const_uploaded = false;            // the adjoint translation unit's constant bank is set
 };
 
 inline void free_adjoint(AdjointBuffers& a) {
+    if (a.g_fwd) cudaGraphExecDestroy(a.g_fwd);
+    if (a.g_rev) cudaGraphExecDestroy(a.g_rev);
     dfree(a.d_lam[0]); dfree(a.d_lam[1]); dfree(a.d_bF); dfree(a.d_bU); dfree(a.d_bu); dfree(a.d_dts);
-    dfree(a.d_ckpt); dfree(a.d_seg); dfree(a.d_segU); dfree(a.d_work);
+    dfree(a.d_dts_given); dfree(a.d_ckpt); dfree(a.d_seg); dfree(a.d_segU); dfree(a.d_work);
     a = AdjointBuffers{};
 }
 
