@@ -97,6 +97,25 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
                       const int64_t* boundary_orientations, const int64_t* boundary_neighbor_sides,
                       const int64_t* n_boundaries_per_direction);
 
+/* Conforming curvilinear mesh (StructuredMesh{2}, or P4estMesh{2} / UnstructuredMesh2D without mortars), in
+ * place of a TreeMesh; LW with the FR volume integral, periodic or fully connected (no boundaries).
+ * Replaces the volume and surface kernels of src/solvers/dgsem_structured/dg_2d.jl:1379-2105, 2107-2391
+ * and src/solvers/dgsem_p4est/dg_2d.jl:8-191.
+ *   contravariant_vectors [2, 2, n, n, element]  Trixi elements.contravariant_vectors (Ja^a_d at [d, a, ...])
+ *   inverse_jacobian      [n, n, element]         Trixi elements.inverse_jacobian (positive)
+ *   interface k: primary element / face, secondary element / face (1-based elements; faces 0: -xi (i = 1),
+ *   1: +xi (i = n), 2: -eta (j = 1), 3: +eta (j = n)) and whether the secondary's face index runs backwards
+ *   (P4est node_indices :i_backward). The normal is the primary's outward contravariant vector; a
+ *   StructuredMesh interface takes the right / upper element as primary (its -xi / -eta face), which is the
+ *   normal the StructuredMesh code uses (dgsem_structured/dg_2d.jl:2233-2267). Every element face must
+ *   belong to exactly one interface. */
+int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contravariant_vectors,
+                        const double* inverse_jacobian, int64_t n_interfaces, const int64_t* primary_elements,
+                        const int32_t* primary_faces, const int64_t* secondary_elements,
+                        const int32_t* secondary_faces, const int32_t* secondary_reversed);
+/* Number of interface colours (launches per interface pass) of the curvilinear mesh; 0 for a TreeMesh. */
+int32_t tlw_curved_colors(tlw_handle* h);
+
 /* Exterior states of the time-averaged Dirichlet boundary condition (src/equations/equations.jl:6-37):
  *   levels [v, q, l, boundary]: boundary_value_function(x_l, t + 0.5*dt_scaled*(x_q + 1)) at the N+1 GLL
  *                              time levels q (dt_scaled = scaling_factor * dt)

@@ -6,6 +6,7 @@
 #include <memory>
 
 #include "tlw_adjoint.hpp"
+#include "tlw_curved.hpp"
 #include "tlw_oracle.hpp"
 
 using namespace tlwo;
@@ -19,8 +20,25 @@ struct oracle_handle {
     std::vector<double> us;      // MDRK stage state u*
     std::vector<double> du;
     std::vector<double> bnd_levels, bnd_now;
+    bool curved = false;         // conforming curvilinear mesh (cmesh) instead of the TreeMesh
+    CurvedMesh cmesh;
     char err[256] = {0};
 };
+
+namespace {
+
+// LW / MDRK rhs on whichever mesh the handle holds (curvilinear: LW, FR volume integral only)
+void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, double t, double dt,
+             const BoundaryData* bd, int kind, int nthreads) {
+    if (!h->curved) {
+        rhs(h->basis, h->eq, h->opt, h->mesh, u, u2, du, t, dt, bd, kind, h->ws, nthreads);
+        return;
+    }
+    if (kind != 0 || h->opt.shock_capturing) throw std::runtime_error("curvilinear oracle: LW, FR volume integral only");
+    rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads);
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -61,6 +79,35 @@ oracle_handle* oracle_create(int N, double gamma, int flux_kind, int speed_kind,
     } catch (...) { return nullptr; }
 }
 
+// Conforming curvilinear mesh: Ja [4, i, j, e] (Trixi contravariant_vectors order Ja^1_1, Ja^1_2, Ja^2_1,
+// Ja^2_2), inv_jac [i, j, e]; interfaces (primary element, face; secondary element, face; reversed), 0-based,
+// faces 0: -xi, 1: +xi, 2: -eta, 3: +eta.
+oracle_handle* oracle_create_curved(int N, double gamma, int flux_kind, int speed_kind, int E, const double* Ja,
+                                    const double* inv_jac, int I, const int32_t* pe, const int32_t* pf,
+                                    const int32_t* se, const int32_t* sf, const int32_t* rev) {
+    try {
+        auto h = std::make_unique<oracle_handle>();
+        h->basis = make_basis(N);
+        h->eq.gamma = gamma;
+        h->opt.N = N;
+        h->opt.flux_kind = flux_kind;
+        h->opt.speed_kind = speed_kind;
+        const size_t nn = (size_t)h->basis.n * h->basis.n;
+        h->curved = true;
+        h->mesh.n_elements = E;   // element count for the shared step loop
+        h->cmesh.n_elements = E;
+        h->cmesh.Ja.assign(Ja, Ja + 4 * nn * E);
+        h->cmesh.inv_jac.assign(inv_jac, inv_jac + nn * E);
+        h->cmesh.n_interfaces = I;
+        h->cmesh.p_elem.assign(pe, pe + I);
+        h->cmesh.p_face.assign(pf, pf + I);
+        h->cmesh.s_elem.assign(se, se + I);
+        h->cmesh.s_face.assign(sf, sf + I);
+        h->cmesh.s_rev.assign(rev, rev + I);
+        return h.release();
+    } catch (...) { return nullptr; }
+}
+
 void oracle_destroy(oracle_handle* h) { delete h; }
 
 // VolumeIntegralFRShockCapturing with IndicatorHennemannGassner(alpha_max, alpha_min, alpha_smooth;
@@ -93,7 +140,7 @@ int oracle_rhs(oracle_handle* h, int kind, const double* u, const double* u2, do
     try {
         BoundaryData bd{h->bnd_levels.empty() ? nullptr : h->bnd_levels.data(),
                         h->bnd_now.empty() ? nullptr : h->bnd_now.data()};
-        rhs(h->basis, h->eq, h->opt, h->mesh, u, u2, du, t, dt, &bd, kind, h->ws, nthreads);
+        any_rhs(h, u, u2, du, t, dt, &bd, kind, nthreads);
         return h->ws.bad ? 3 : 0;
     } catch (const std::exception& ex) {
         std::snprintf(h->err, sizeof(h->err), "%s", ex.what());
@@ -137,7 +184,8 @@ int oracle_get(oracle_handle* h, int which, double* out) {
 
 double oracle_max_dt(oracle_handle* h, const double* u, double cfl) {
     bool bad = false;
-    const double dt = max_dt(h->basis, h->eq, h->mesh, u, cfl, bad);
+    const double dt = h->curved ? max_dt_curved(h->basis, h->eq, h->cmesh, u, cfl, bad)
+                                : max_dt(h->basis, h->eq, h->mesh, u, cfl, bad);
     return bad ? -1.0 : dt;
 }
 
@@ -148,6 +196,7 @@ double oracle_max_dt(oracle_handle* h, const double* u, double cfl) {
 int oracle_steps(oracle_handle* h, int kind, double* u, int nsteps, double cfl, double fixed_dt, double* t_inout,
                  double t_end, int nthreads) {
     const size_t ndof = (size_t)NV * h->basis.n * h->basis.n * h->mesh.n_elements;
+    try {
     h->du.resize(ndof);
     h->us.resize(ndof);
     double t = *t_inout;
@@ -159,22 +208,24 @@ int oracle_steps(oracle_handle* h, int kind, double* u, int nsteps, double cfl, 
             (t >= t_end || std::fabs(t - t_end) <= 1.4901161193847656e-8 * std::max(std::fabs(t), std::fabs(t_end))))
             break;
         bool bad = false;
-        double dt = fixed_dt > 0 ? fixed_dt : max_dt(h->basis, h->eq, h->mesh, u, cfl, bad, nthreads);
+        double dt = fixed_dt > 0 ? fixed_dt
+                    : h->curved ? max_dt_curved(h->basis, h->eq, h->cmesh, u, cfl, bad, nthreads)
+                                : max_dt(h->basis, h->eq, h->mesh, u, cfl, bad, nthreads);
         if (bad) return -3;
         if (t + dt > t_end) dt = t_end - t;
         BoundaryData bd{h->bnd_levels.empty() ? nullptr : h->bnd_levels.data(),
                         h->bnd_now.empty() ? nullptr : h->bnd_now.data()};
         if (kind == 0) {
-            rhs(h->basis, h->eq, h->opt, h->mesh, u, nullptr, h->du.data(), t, dt, &bd, 0, h->ws, nthreads);
+            any_rhs(h, u, nullptr, h->du.data(), t, dt, &bd, 0, nthreads);
             if (h->ws.bad) return -3;
 #pragma omp parallel for num_threads(nthreads) schedule(static)
             for (long long k = 0; k < (long long)ndof; ++k) u[k] = u[k] + dt * h->du[k];
         } else {
-            rhs(h->basis, h->eq, h->opt, h->mesh, u, nullptr, h->du.data(), t, dt, &bd, 1, h->ws, nthreads);
+            any_rhs(h, u, nullptr, h->du.data(), t, dt, &bd, 1, nthreads);
             if (h->ws.bad) return -3;
 #pragma omp parallel for num_threads(nthreads) schedule(static)
             for (long long k = 0; k < (long long)ndof; ++k) h->us[k] = u[k] + dt * h->du[k];
-            rhs(h->basis, h->eq, h->opt, h->mesh, u, h->us.data(), h->du.data(), t, dt, &bd, 2, h->ws, nthreads);
+            any_rhs(h, u, h->us.data(), h->du.data(), t, dt, &bd, 2, nthreads);
             if (h->ws.bad) return -3;
 #pragma omp parallel for num_threads(nthreads) schedule(static)
             for (long long k = 0; k < (long long)ndof; ++k) u[k] = u[k] + dt * h->du[k];
@@ -183,6 +234,10 @@ int oracle_steps(oracle_handle* h, int kind, double* u, int nsteps, double cfl, 
     }
     *t_inout = t;
     return s;
+    } catch (const std::exception& ex) {
+        std::snprintf(h->err, sizeof(h->err), "%s", ex.what());
+        return -1;
+    }
 }
 
 const char* oracle_last_error(oracle_handle* h) { return h->err; }

@@ -47,6 +47,8 @@ def lib():
         L.oracle_max_dt.restype = dbl
         L.oracle_steps.argtypes = [P, i32, P, i32, dbl, dbl, P, dbl, i32]
         L.oracle_adjoint_step.argtypes = [P, P, dbl, P, P, i32]
+        L.oracle_create_curved.argtypes = [i32, dbl, i32, i32, i32, P, P, i32, P, P, P, P, P]
+        L.oracle_create_curved.restype = P
         L.oracle_last_error.argtypes = [P]
         L.oracle_last_error.restype = ctypes.c_char_p
         _L = L
@@ -77,6 +79,10 @@ class Oracle:
         self.n = polydeg + 1
         self.mesh = mesh
         self.E = mesh.n_elements
+        if hasattr(mesh, "curved") or hasattr(mesh, "Ja"):
+            self._init_curved(mesh.curved(polydeg) if hasattr(mesh, "curved") else mesh, polydeg, gamma, flux_kind,
+                              speed_kind)
+            return
         ij = np.ascontiguousarray(mesh.inverse_jacobian, dtype=np.float64)
         ids = np.asarray(mesh.interface_neighbor_ids, dtype=np.int64).reshape(-1, 2)
         left = np.ascontiguousarray(ids[:, 0] - 1, dtype=np.int32)
@@ -93,6 +99,21 @@ class Oracle:
                                      _p(bs) if B else None, _p(bd) if B else None)
         if not self.h:
             raise RuntimeError("oracle_create failed")
+
+    def _init_curved(self, cm, polydeg, gamma, flux_kind, speed_kind):
+        """Conforming curvilinear mesh (trixilw.curved_mesh.CurvedMesh or StructuredMesh)."""
+        Ja = np.ascontiguousarray(cm.Ja, dtype=np.float64)
+        ij = np.ascontiguousarray(cm.inverse_jacobian_nodes, dtype=np.float64)
+        pe = np.ascontiguousarray(cm.primary_elements - 1, dtype=np.int32)
+        se = np.ascontiguousarray(cm.secondary_elements - 1, dtype=np.int32)
+        pf = np.ascontiguousarray(cm.primary_faces, dtype=np.int32)
+        sf = np.ascontiguousarray(cm.secondary_faces, dtype=np.int32)
+        rv = np.ascontiguousarray(cm.secondary_reversed, dtype=np.int32)
+        self._keep = (Ja, ij, pe, se, pf, sf, rv)
+        self.h = lib().oracle_create_curved(polydeg, gamma, flux_kind, speed_kind, self.E, _p(Ja), _p(ij), len(pe),
+                                            _p(pe), _p(pf), _p(se), _p(sf), _p(rv))
+        if not self.h:
+            raise RuntimeError("oracle_create_curved failed")
 
     def __del__(self):
         try:

@@ -1,0 +1,286 @@
+// tlw_curved.hpp -- test infrastructure only: CPU restatement of the LW right-hand side on curvilinear
+// conforming meshes (StructuredMesh{2}, and P4estMesh{2} / UnstructuredMesh2D without mortars), used to
+// check the CUDA curvilinear kernels.
+//
+// Volume: lw_volume_kernel_3! / lw_volume_kernel_4! for Union{StructuredMesh{2}, UnstructuredMesh2D,
+// P4estMesh{2}} (src/solvers/dgsem_structured/dg_2d.jl:1379-1685, 1687-2105): the LW procedure of the
+// TreeMesh kernels applied to the contravariant fluxes f~ = Ja^1 . (f, g), g~ = Ja^2 . (f, g)
+// (contravariant_flux, :541-556) with the per-node inverse Jacobian; the element cache keeps the
+// physical time averages F, G for the surface; du = Dhat F~ + Dhat G~.
+// Surface: every conforming interface is (primary element, face; secondary element, face; whether the
+// secondary's face index runs backwards). The normal is the primary's outward contravariant vector at the
+// face node (get_normal_direction); each side's normal flux uses its own outward normal, the secondary's
+// negated (prolong2interfaces!, src/solvers/dgsem_p4est/dg_2d.jl:8-84), and the 8-argument surface flux is
+// called in the curvilinear order (f_ll, f_rr, u_ll, u_rr, U_ll, U_rr, normal) (dgsem_p4est/dg_2d.jl:165,
+// dgsem_structured/dg_2d.jl:2271): for Rusanov the speed comes from the instantaneous u and the jump is
+// in the time-averaged U. The primary receives Fn and the secondary -Fn as outward fluxes
+// (dgsem_p4est/dg_2d.jl:176-189). A StructuredMesh interface is given with the right element as primary
+// (its -x / -y face), which is the normal the StructuredMesh code takes (dgsem_structured/dg_2d.jl:2233-2267).
+// Surface integral and apply_jacobian (Trixi): du(face node) += outward flux / w_face, then du *= -J^{-1}
+// per node. max_dt (Trixi, curved meshes): 2 / (n max_e max_nodes(|Ja^1 . lambda| J^{-1}) + ...).
+// Faces are numbered 0: -xi (i = 1), 1: +xi (i = n), 2: -eta (j = 1), 3: +eta (j = n).
+#pragma once
+#include "tlw_adjoint.hpp"
+#include "tlw_oracle.hpp"
+
+namespace tlwo {
+
+struct CurvedMesh {
+    int n_elements = 0;
+    std::vector<double> Ja;         // [4, i, j, e]: Ja^1_1, Ja^1_2, Ja^2_1, Ja^2_2 (Trixi contravariant_vectors)
+    std::vector<double> inv_jac;    // [i, j, e]
+    int n_interfaces = 0;
+    std::vector<int32_t> p_elem, p_face, s_elem, s_face, s_rev;   // 0-based elements
+};
+
+// node (i, j) of face f at face index l
+inline void face_node(int n, int f, int l, int& i, int& j) {
+    switch (f) {
+        case 0: i = 0; j = l; break;
+        case 1: i = n - 1; j = l; break;
+        case 2: i = l; j = 0; break;
+        default: i = l; j = n - 1; break;
+    }
+}
+
+// outward normal of face f at node (i, j): -+Ja^1 on xi faces, -+Ja^2 on eta faces (get_normal_direction)
+inline void outward_normal(const CurvedMesh& m, int n, int f, int i, int j, int e, double* nrm) {
+    const double* J = &m.Ja[4 * (i + (size_t)n * (j + (size_t)n * e))];
+    const double s = (f == 1 || f == 3) ? 1.0 : -1.0;
+    nrm[0] = s * (f < 2 ? J[0] : J[2]);
+    nrm[1] = s * (f < 2 ? J[1] : J[3]);
+}
+
+// Trixi max_abs_speed_naive / max_abs_speed / min_max_speed_naive with a normal direction
+inline double max_abs_speed_normal(const Euler& eq, const double* ul, const double* ur, const double* nrm, int kind,
+                                   bool& bad) {
+    double rl, v1l, v2l, pl, rr, v1r, v2r, pr;
+    eq.cons2prim(ul, rl, v1l, v2l, pl);
+    eq.cons2prim(ur, rr, v1r, v2r, pr);
+    const double vl = v1l * nrm[0] + v2l * nrm[1], vr = v1r * nrm[0] + v2r * nrm[1];
+    const double cl = eq.checked_sqrt(eq.gamma * pl / rl, bad), cr = eq.checked_sqrt(eq.gamma * pr / rr, bad);
+    const double nn = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1]);
+    if (kind == 0) return std::max(std::fabs(vl), std::fabs(vr)) + std::max(cl, cr) * nn;
+    return std::max(std::fabs(vl) + cl * nn, std::fabs(vr) + cr * nn);
+}
+inline void min_max_speed_normal(const Euler& eq, const double* ul, const double* ur, const double* nrm, double& lmin,
+                                 double& lmax, bool& bad) {
+    double rl, v1l, v2l, pl, rr, v1r, v2r, pr;
+    eq.cons2prim(ul, rl, v1l, v2l, pl);
+    eq.cons2prim(ur, rr, v1r, v2r, pr);
+    const double nn = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1]);
+    lmin = (v1l * nrm[0] + v2l * nrm[1]) - eq.checked_sqrt(eq.gamma * pl / rl, bad) * nn;
+    lmax = (v1r * nrm[0] + v2r * nrm[1]) + eq.checked_sqrt(eq.gamma * pr / rr, bad) * nn;
+}
+
+// the 8-argument LW surface flux (numerical_fluxes.jl:14-38, compressible_euler_2d.jl:24-40) with a normal
+inline void lw_surface_flux_normal(const Euler& eq, int flux_kind, int speed_kind, const double* f_ll,
+                                   const double* f_rr, const double* a3, const double* a4, const double* a5,
+                                   const double* a6, const double* nrm, double* out, bool& bad) {
+    if (flux_kind == RUSANOV) {
+        const double lambda = max_abs_speed_normal(eq, a3, a4, nrm, speed_kind, bad);
+        for (int v = 0; v < NV; ++v) out[v] = 0.5 * (f_ll[v] + f_rr[v]) + (-0.5 * lambda * (a6[v] - a5[v]));
+    } else {
+        double lmin, lmax;
+        min_max_speed_normal(eq, a5, a6, nrm, lmin, lmax, bad);
+        if (lmin >= 0 && lmax >= 0) {
+            for (int v = 0; v < NV; ++v) out[v] = f_ll[v];
+        } else if (lmax <= 0 && lmin <= 0) {
+            for (int v = 0; v < NV; ++v) out[v] = f_rr[v];
+        } else {
+            const double inv = 1.0 / (lmax - lmin);
+            const double fll = lmax * inv, frr = lmin * inv, fd = lmin * lmax * inv;
+            for (int v = 0; v < NV; ++v) out[v] = fll * f_ll[v] - frr * f_rr[v] + fd * (a4[v] - a3[v]);
+        }
+    }
+}
+
+// One element of the curvilinear LW volume kernel. du receives Dhat F~ + Dhat G~ (before the surface
+// integral and the Jacobian); ws.U / ws.F receive the time-averaged U and the physical F, G.
+inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, const CurvedMesh& m, int e,
+                                     const double* u, double* du, double dt, Workspace& ws) {
+    const int n = b.n, nn = n * n;
+    const LWStencils S = lw_stencils(N);
+    const int depth = S.depth;
+    auto L = [&](int i, int j) { return NV * (i + n * j); };
+    const double* ue = u + idx_u(n, 0, 0, 0, e);
+    const double* Jae = &m.Ja[4 * (size_t)nn * e];
+    const double* ije = &m.inv_jac[(size_t)nn * e];
+    std::vector<double> d(5 * NV * nn, 0.0), ft(NV * nn), gt(NV * nn), Fp(NV * nn), Gp(NV * nn), Ft(NV * nn),
+        Gt(NV * nn), Uc(NV * nn);
+    auto Dm = [&](int k) { return d.data() + (size_t)k * NV * nn; };
+    // physical and contravariant fluxes of a state at node (i, j) (contravariant_flux)
+    auto cflux = [&](const double* s, int i, int j, double* f, double* g, double* cf, double* cg) {
+        eq.fluxes(s, f, g);
+        const double* J = Jae + 4 * (i + n * j);
+        for (int v = 0; v < NV; ++v) {
+            cf[v] = J[0] * f[v] + J[1] * g[v];
+            cg[v] = J[2] * f[v] + J[3] * g[v];
+        }
+    };
+    // t = -dt J^{-1}(node) (D x + D y) (the per-node Jacobian scaling follows the contraction)
+    auto contract = [&](const std::vector<double>& x, const std::vector<double>& y, double* t) {
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i)
+                for (int v = 0; v < NV; ++v) {
+                    double s = 0.0;
+                    for (int k = 0; k < n; ++k) s += -dt * b.D[i * n + k] * x[L(k, j) + v] - dt * b.D[j * n + k] * y[L(i, k) + v];
+                    t[L(i, j) + v] = s * ije[i + n * j];
+                }
+    };
+    auto state = [&](int s, int q, int i, int j, double* P) {
+        for (int v = 0; v < NV; ++v) {
+            double x = ue[L(i, j) + v];
+            for (int mm = 1; mm <= s; ++mm) x += S.a[q][mm] * Dm(mm)[L(i, j) + v];
+            P[v] = x;
+        }
+    };
+    // stage 0
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const int o = L(i, j);
+            cflux(ue + o, i, j, &Fp[o], &Gp[o], &ft[o], &gt[o]);
+            for (int v = 0; v < NV; ++v) { Ft[o + v] = ft[o + v]; Gt[o + v] = gt[o + v]; Uc[o + v] = ue[o + v]; }
+        }
+    contract(ft, gt, Dm(1));
+    // stages 1 .. depth: stencils of physical and contravariant fluxes, time averages, next derivative
+    for (int s = 1; s <= depth; ++s) {
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const int o = L(i, j);
+                double f[NV], g[NV], cf[NV], cg[NV], pf[NV] = {0, 0, 0, 0}, pg[NV] = {0, 0, 0, 0};
+                double tf[NV] = {0, 0, 0, 0}, tg[NV] = {0, 0, 0, 0};
+                if (S.w[s][0] != 0.0) {
+                    cflux(ue + o, i, j, f, g, cf, cg);
+                    for (int v = 0; v < NV; ++v) {
+                        pf[v] = S.w[s][0] * f[v]; pg[v] = S.w[s][0] * g[v];
+                        tf[v] = S.w[s][0] * cf[v]; tg[v] = S.w[s][0] * cg[v];
+                    }
+                }
+                for (int q = 0; q < 4; ++q) {
+                    if (S.w[s][1 + q] == 0.0) continue;
+                    double P[NV];
+                    state(s, q, i, j, P);
+                    cflux(P, i, j, f, g, cf, cg);
+                    for (int v = 0; v < NV; ++v) {
+                        pf[v] += S.w[s][1 + q] * f[v]; pg[v] += S.w[s][1 + q] * g[v];
+                        tf[v] += S.w[s][1 + q] * cf[v]; tg[v] += S.w[s][1 + q] * cg[v];
+                    }
+                }
+                for (int v = 0; v < NV; ++v) {
+                    Fp[o + v] += S.tw[s] * pf[v]; Gp[o + v] += S.tw[s] * pg[v];
+                    Ft[o + v] += S.tw[s] * tf[v]; Gt[o + v] += S.tw[s] * tg[v];
+                    Uc[o + v] += S.tw[s] * Dm(s)[o + v];
+                    ft[o + v] = tf[v]; gt[o + v] = tg[v];
+                }
+            }
+        if (s < depth) contract(ft, gt, Dm(s + 1));
+    }
+    // du += Dhat F~ + Dhat G~; element cache
+    double* due = du + idx_u(n, 0, 0, 0, e);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const int o = L(i, j);
+            for (int ii = 0; ii < n; ++ii)
+                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += b.Dhat[ii * n + i] * Ft[o + v];
+            for (int jj = 0; jj < n; ++jj)
+                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += b.Dhat[jj * n + j] * Gt[o + v];
+            for (int v = 0; v < NV; ++v) {
+                ws.F[idx_F(n, v, 0, i, j, e)] = Fp[o + v];
+                ws.F[idx_F(n, v, 1, i, j, e)] = Gp[o + v];
+                ws.U[idx_u(n, v, i, j, e)] = Uc[o + v];
+            }
+        }
+}
+
+// du = rhs(u) on a conforming curvilinear mesh (LW, FR volume integral, no boundaries)
+inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m, const double* u,
+                       double* du, double dt, Workspace& ws, int nthreads = 1) {
+    const int n = b.n, nn = n * n;
+    const size_t ndof = (size_t)NV * nn * m.n_elements;
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    ws.U.assign(ndof, nan);
+    ws.F.assign(2 * ndof, nan);
+    ws.surface_flux_values.assign((size_t)NV * n * 4 * m.n_elements, nan);
+    ws.bad = false;
+    for (size_t k = 0; k < ndof; ++k) du[k] = 0.0;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int e = 0; e < m.n_elements; ++e) lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws);
+    bool bad = false;
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad)
+    for (int k = 0; k < m.n_interfaces; ++k) {
+        const int pe = m.p_elem[k], pf = m.p_face[k], se = m.s_elem[k], sf = m.s_face[k];
+        for (int l = 0; l < n; ++l) {
+            const int ls = m.s_rev[k] ? n - 1 - l : l;
+            int ip, jp, is, js;
+            face_node(n, pf, l, ip, jp);
+            face_node(n, sf, ls, is, js);
+            double nP[2], nS[2], f_ll[NV], f_rr[NV], u_ll[NV], u_rr[NV], U_ll[NV], U_rr[NV], Fn[NV];
+            outward_normal(m, n, pf, ip, jp, pe, nP);
+            outward_normal(m, n, sf, is, js, se, nS);
+            for (int v = 0; v < NV; ++v) {
+                f_ll[v] = ws.F[idx_F(n, v, 0, ip, jp, pe)] * nP[0] + ws.F[idx_F(n, v, 1, ip, jp, pe)] * nP[1];
+                f_rr[v] = ws.F[idx_F(n, v, 0, is, js, se)] * (-nS[0]) + ws.F[idx_F(n, v, 1, is, js, se)] * (-nS[1]);
+                u_ll[v] = u[idx_u(n, v, ip, jp, pe)];
+                u_rr[v] = u[idx_u(n, v, is, js, se)];
+                U_ll[v] = ws.U[idx_u(n, v, ip, jp, pe)];
+                U_rr[v] = ws.U[idx_u(n, v, is, js, se)];
+            }
+            bool b_ = false;
+            lw_surface_flux_normal(eq, opt.flux_kind, opt.speed_kind, f_ll, f_rr, u_ll, u_rr, U_ll, U_rr, nP, Fn, b_);
+            bad = bad || b_;
+            for (int v = 0; v < NV; ++v) {
+                ws.surface_flux_values[v + NV * (l + n * (pf + 4 * (size_t)pe))] = Fn[v];
+                ws.surface_flux_values[v + NV * (ls + n * (sf + 4 * (size_t)se))] = -Fn[v];
+            }
+        }
+    }
+    ws.bad = ws.bad || bad;
+    // surface integral (outward fluxes) and apply_jacobian (per node)
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int e = 0; e < m.n_elements; ++e) {
+        for (int f = 0; f < 4; ++f) {
+            const double iw = (f == 1 || f == 3) ? b.inv_w_last : b.inv_w_first;
+            for (int l = 0; l < n; ++l) {
+                int i, j;
+                face_node(n, f, l, i, j);
+                for (int v = 0; v < NV; ++v)
+                    du[idx_u(n, v, i, j, e)] += ws.surface_flux_values[v + NV * (l + n * (f + 4 * (size_t)e))] * iw;
+            }
+        }
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const double s = -m.inv_jac[i + n * (j + (size_t)n * e)];
+                for (int v = 0; v < NV; ++v) du[idx_u(n, v, i, j, e)] *= s;
+            }
+    }
+}
+
+// Trixi max_dt for curved meshes: per node lambda~_d = |Ja^d . (|v1| + c, |v2| + c)| |J^{-1}|
+inline double max_dt_curved(const Basis& b, const Euler& eq, const CurvedMesh& m, const double* u, double cfl,
+                            bool& bad, int nthreads = 1) {
+    const int n = b.n;
+    double max_scaled = std::nextafter(0.0, 1.0);
+    bool bad_any = false;
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(max : max_scaled) reduction(|| : bad_any)
+    for (int e = 0; e < m.n_elements; ++e) {
+        double m1 = 0.0, m2 = 0.0;
+        bool b_ = false;
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                double l1, l2;
+                eq.max_abs_speeds(u + idx_u(n, 0, i, j, e), l1, l2, b_);
+                const size_t node = i + n * (j + (size_t)n * e);
+                const double* J = &m.Ja[4 * node];
+                const double ij = std::fabs(m.inv_jac[node]);
+                m1 = std::max(m1, std::fabs(J[0] * l1 + J[1] * l2) * ij);
+                m2 = std::max(m2, std::fabs(J[2] * l1 + J[3] * l2) * ij);
+            }
+        max_scaled = std::max(max_scaled, m1 + m2);
+        bad_any = bad_any || b_;
+    }
+    bad = bad_any;
+    return cfl * 2.0 / (n * max_scaled);
+}
+
+}  // namespace tlwo

@@ -549,7 +549,7 @@ size_t ntrace(const tlw_handle* h) { return (size_t)NV * h->n * 4 * h->E; }
 int adj_ready(tlw_handle* h) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh) return afail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
-    if (h->opts.time_discretization != TLW_LW || h->sc || h->opts.surface_flux != TLW_FLUX_RUSANOV || h->nb > 0 ||
+    if (h->opts.time_discretization != TLW_LW || h->sc || h->opts.surface_flux != TLW_FLUX_RUSANOV || h->nb > 0 || h->curved ||
         h->N < 3 || h->N > 5)
         return afail(h, TLW_E_UNSUPPORTED,
                      "adjoint: LW, FR volume integral, Rusanov flux, periodic TreeMesh, N = 3..5");

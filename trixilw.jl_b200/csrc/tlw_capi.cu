@@ -2,6 +2,7 @@
 // step loop (captured as CUDA graphs) and the extern "C" entry points declared in include/tlw.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -11,12 +12,12 @@
 
 #include "../../include/tlw.h"
 #include "tlw_basis.h"
+#include "tlw_curved.cuh"
+#include "tlw_handle.h"
 #include "tlw_surface.cuh"
 #include "tlw_volume.cuh"
 
 using namespace tlw;
-
-#include "tlw_handle.h"
 
 namespace {
 
@@ -54,6 +55,9 @@ void free_mesh(tlw_handle* h) {
     dfree(h->d_tU); dfree(h->d_tF); dfree(h->d_U2); dfree(h->d_F2);
     dfree(h->d_alpha); dfree(h->d_alpha_raw); dfree(h->d_tFn); dfree(h->d_il); dfree(h->d_ir);
     free_adjoint(h->adj);
+    dfree(h->d_Ja); dfree(h->d_ijn); dfree(h->d_cp); dfree(h->d_cs); dfree(h->d_cf);
+    h->color_off.clear();
+    h->curved = false;
     h->have_mesh = false;
     h->have_bdata = false;
 }
@@ -75,6 +79,9 @@ struct Launch {
     static void set_attributes() {
         set_attr_sc<false>();
         set_attr_sc<true>();
+        const int lw = (int)C::smem_bytes(4);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
     }
     template <bool SC>
     static void volume_sc(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
@@ -93,6 +100,11 @@ struct Launch {
     static void volume(cudaStream_t s, int stage, int mode, bool sc, const VolArgs& a) {
         const int grid = (int)((a.E + C::EB - 1) / C::EB);
         if (grid == 0) return;
+        if (a.metrics) {   // curvilinear mesh (LW, FR volume integral)
+            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, false, 0, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
+            else lw_volume_kernel<N, MODE_STEP, false, 0, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
+            return;
+        }
         if (sc) volume_sc<true>(s, stage, mode, a, grid);
         else volume_sc<false>(s, stage, mode, a, grid);
     }
@@ -100,6 +112,16 @@ struct Launch {
         const long long threads = (long long)a.count * (N + 1);
         if (threads == 0) return;
         interface_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
+    }
+    static void curved_interfaces(cudaStream_t s, const CurvedSurfArgs& a) {
+        const long long threads = (long long)a.count * (N + 1);
+        if (threads == 0) return;
+        curved_interface_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
+    }
+    static void curved_speed(cudaStream_t s, const double* u, const double* Ja, const double* ij, int E, double g,
+                             StepState* st) {
+        if (E == 0) return;
+        curved_max_speed_kernel<N><<<(E + 127) / 128, 128, 0, s>>>(u, Ja, ij, E, g, st);
     }
     static void boundaries(cudaStream_t s, const BndArgs& a) {
         const long long threads = (long long)a.count * (N + 1);
@@ -136,6 +158,12 @@ template <int N> struct Vol {
 };
 template <int N> struct Ifc { static void run(cudaStream_t s, const SurfArgs& a) { Launch<N>::interfaces(s, a); } };
 template <int N> struct Bnd { static void run(cudaStream_t s, const BndArgs& a) { Launch<N>::boundaries(s, a); } };
+template <int N> struct CIfc { static void run(cudaStream_t s, const CurvedSurfArgs& a) { Launch<N>::curved_interfaces(s, a); } };
+template <int N> struct CSpd {
+    static void run(cudaStream_t s, const double* u, const double* Ja, const double* ij, int E, double g, StepState* st) {
+        Launch<N>::curved_speed(s, u, Ja, ij, E, g, st);
+    }
+};
 template <int N> struct Spd {
     static void run(cudaStream_t s, const double* u, const double* ij, int E, double g, StepState* st, bool speed,
                     bool ind, const IndicatorArgs& ia) {
@@ -192,8 +220,42 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     va.tFn = h->d_tFn;
     va.status = &h->d_step->status;
     va.speed_kind = h->opts.max_speed;
+    if (h->curved) {
+        va.metrics = h->d_Ja;
+        va.inv_jac_node = h->d_ijn;
+    }
     dispatch<Vol>(h->N, h->stream, stage, mode, h->sc, va);
     if (ev) cudaEventRecord(ev->after_volume, h->stream);
+    if (h->curved) {
+        // interfaces colour by colour (no two launches' threads share a node within a colour)
+        CurvedSurfArgs ca{};
+        ca.u = u_jump;
+        ca.out = out;
+        ca.tU = h->d_tU;
+        ca.tF = h->d_tF;
+        ca.metrics = h->d_Ja;
+        ca.inv_jac = h->d_ijn;
+        ca.dt = dt_ptr;
+        ca.step_mode = mode == MODE_STEP;
+        ca.gamma = h->opts.gamma;
+        ca.flux_kind = h->opts.surface_flux;
+        ca.speed_kind = h->opts.max_speed;
+        ca.inv_w_first = h->h_basis.inv_w_first;
+        ca.inv_w_last = h->h_basis.inv_w_last;
+        ca.status = &h->d_step->status;
+        for (size_t c = 0; c + 1 < h->color_off.size(); ++c) {
+            const int b = h->color_off[c];
+            ca.p_elem = h->d_cp + b;
+            ca.s_elem = h->d_cs + b;
+            ca.faces = h->d_cf + b;
+            ca.count = h->color_off[c + 1] - b;
+            dispatch<CIfc>(h->N, h->stream, ca);
+            if (ev && c == 0) cudaEventRecord(ev->after_x, h->stream);
+        }
+        if (ev && h->color_off.size() <= 2) cudaEventRecord(ev->after_x, h->stream);
+        if (ev) cudaEventRecord(ev->after_y, h->stream);
+        return;
+    }
 
     SurfArgs sa{};
     sa.u = u_jump;
@@ -256,6 +318,8 @@ void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const
     const double* u = h->d_state[from];
     double* unew = h->d_state[1 - from];
     if (h->sc) enqueue_indicator(h, u, true);   // CFL reduction and indicator in one pass over u
+    else if (h->curved) dispatch<CSpd>(h->N, h->stream, u, (const double*)h->d_Ja, (const double*)h->d_ijn, (int)h->E,
+                                       h->opts.gamma, h->d_step);
     else dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, true,
                        false, indicator_args(h));
     finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
@@ -455,6 +519,99 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
     return TLW_OK;
 }
 
+int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contravariant_vectors,
+                        const double* inverse_jacobian, int64_t n_interfaces, const int64_t* primary_elements,
+                        const int32_t* primary_faces, const int64_t* secondary_elements,
+                        const int32_t* secondary_faces, const int32_t* secondary_reversed) {
+    if (!h) return TLW_E_ARG;
+    if (h->opts.time_discretization != TLW_LW || h->sc || h->N < 3)
+        return fail(h, TLW_E_UNSUPPORTED, "curvilinear meshes: LW with the FR volume integral, N >= 3");
+    if (n_elements <= 0 || n_elements > (int64_t)0x7fffffff / 64 || !contravariant_vectors || !inverse_jacobian)
+        return fail(h, TLW_E_ARG, "n_elements / metrics");
+    if (n_interfaces < 0 || (n_interfaces > 0 && (!primary_elements || !primary_faces || !secondary_elements ||
+                                                  !secondary_faces || !secondary_reversed)))
+        return fail(h, TLW_E_ARG, "interfaces");
+    // greedy colouring: within a colour, every element has interfaces on faces of one class only (xi or
+    // eta), so no two threads of a launch update the same corner node
+    struct Ifc { int p, s, code, cp, cs; };
+    std::vector<Ifc> all((size_t)n_interfaces);
+    std::vector<int64_t> seen((size_t)n_elements * 4, -1);
+    for (int64_t k = 0; k < n_interfaces; ++k) {
+        const int64_t p = primary_elements[k] - 1, q = secondary_elements[k] - 1;
+        const int pf = primary_faces[k], sf = secondary_faces[k], rv = secondary_reversed[k];
+        if (p < 0 || p >= n_elements || q < 0 || q >= n_elements || pf < 0 || pf > 3 || sf < 0 || sf > 3 ||
+            (rv != 0 && rv != 1))
+            return fail(h, TLW_E_ARG, "interface " + std::to_string(k + 1) + " out of range");
+        if (seen[(size_t)p * 4 + pf] >= 0 || seen[(size_t)q * 4 + sf] >= 0 || (p == q && pf == sf))
+            return fail(h, TLW_E_ARG, "interface " + std::to_string(k + 1) + ": element face used twice");
+        seen[(size_t)p * 4 + pf] = k;
+        seen[(size_t)q * 4 + sf] = k;
+        if (p == q && (pf >> 1) != (sf >> 1))
+            return fail(h, TLW_E_ARG, "interface " + std::to_string(k + 1) + " joins two face classes of one element");
+        all[(size_t)k] = Ifc{(int)p, (int)q, pf | (sf << 2) | (rv << 4), pf >> 1, sf >> 1};
+    }
+    std::stable_sort(all.begin(), all.end(), [](const Ifc& a, const Ifc& b) {
+        return (a.cp != a.cs) < (b.cp != b.cs) || ((a.cp != a.cs) == (b.cp != b.cs) && a.cp < b.cp);
+    });
+    std::vector<std::vector<signed char>> cls;   // [colour][element] face class used, -1 none
+    std::vector<std::vector<int>> bucket;
+    for (const Ifc& f : all) {
+        size_t c = 0;
+        for (; c < cls.size(); ++c) {
+            const signed char a = cls[c][f.p], b = cls[c][f.s];
+            if ((a < 0 || a == f.cp) && (b < 0 || b == f.cs)) break;
+        }
+        if (c == cls.size()) {
+            cls.emplace_back((size_t)n_elements, (signed char)-1);
+            bucket.emplace_back();
+        }
+        cls[c][f.p] = (signed char)f.cp;
+        cls[c][f.s] = (signed char)f.cs;
+        bucket[c].push_back((int)(&f - all.data()));
+    }
+    std::vector<int> cp, cs, cf, off{0};
+    for (const auto& bk : bucket) {
+        for (int k : bk) {
+            cp.push_back(all[k].p);
+            cs.push_back(all[k].s);
+            cf.push_back(all[k].code);
+        }
+        off.push_back((int)cp.size());
+    }
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    free_mesh(h);
+    h->E = n_elements;
+    const size_t nodes = (size_t)h->nn * n_elements;
+    auto up_i = [&](int*& d, const std::vector<int>& v) -> int {
+        if (v.empty()) return TLW_OK;
+        TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
+        TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+        return TLW_OK;
+    };
+    int rc;
+    TLW_CUDA(h, cudaMalloc(&h->d_Ja, nodes * 4 * sizeof(double)));
+    TLW_CUDA(h, cudaMemcpy(h->d_Ja, contravariant_vectors, nodes * 4 * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, cudaMalloc(&h->d_ijn, nodes * sizeof(double)));
+    TLW_CUDA(h, cudaMemcpy(h->d_ijn, inverse_jacobian, nodes * sizeof(double), cudaMemcpyHostToDevice));
+    if ((rc = up_i(h->d_cp, cp)) || (rc = up_i(h->d_cs, cs)) || (rc = up_i(h->d_cf, cf))) return rc;
+    h->color_off = off;
+    h->nx = h->ny = 0;
+    h->nb = 0; h->nbx = h->nby = 0;
+    const size_t sd = state_doubles(h), td = trace_doubles(h);
+    if ((rc = ensure(h, h->d_state[0], sd)) || (rc = ensure(h, h->d_state[1], sd)) || (rc = ensure(h, h->d_tU, td)) ||
+        (rc = ensure(h, h->d_tF, td)))
+        return rc;
+    h->curved = true;
+    h->cur = 0;
+    h->have_mesh = true;
+    return TLW_OK;
+}
+
+int32_t tlw_curved_colors(tlw_handle* h) {
+    return (h && h->curved) ? (int32_t)h->color_off.size() - 1 : 0;
+}
+
 int tlw_set_boundary_data(tlw_handle* h, const double* levels, const double* now, int32_t where) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh");
@@ -519,8 +676,12 @@ int tlw_max_dt(tlw_handle* h, const double* u, int32_t where, double cfl, double
     }
     const unsigned long long zero = 0;
     TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->max_bits, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
-    dispatch<Spd>(h->N, h->stream, du_in, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, true,
-                  false, indicator_args(h));
+    if (h->curved)
+        dispatch<CSpd>(h->N, h->stream, du_in, (const double*)h->d_Ja, (const double*)h->d_ijn, (int)h->E,
+                       h->opts.gamma, h->d_step);
+    else
+        dispatch<Spd>(h->N, h->stream, du_in, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step,
+                      true, false, indicator_args(h));
     TLW_CUDA(h, cudaGetLastError());
     unsigned long long bits = 0;
     TLW_CUDA(h, cudaMemcpyAsync(&bits, &h->d_step->max_bits, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));

@@ -1,0 +1,186 @@
+// tlw_curved.cuh -- surface and CFL kernels for conforming curvilinear meshes (StructuredMesh{2}, and
+// P4estMesh{2} / UnstructuredMesh2D without mortars). The volume kernel is lw_volume_kernel<..., CURVED>.
+//
+// An interface is (primary element, face; secondary element, face; whether the secondary's face index runs
+// backwards), faces 0: -xi, 1: +xi, 2: -eta, 3: +eta. The volume kernel leaves, per face node, the time
+// averaged U and the contravariant flux along the face's coordinate direction (F~ on xi faces, G~ on eta
+// faces), i.e. the physical flux dotted with +Ja^1 / +Ja^2 of that node. With sigma = +1 on faces 1, 3 and -1
+// on faces 0, 2 the outward normal flux of a side is sigma * trace. As prolong2interfaces! and
+// calc_interface_flux! for P4estMesh{2} (src/solvers/dgsem_p4est/dg_2d.jl:8-191):
+//   n     = outward normal of the primary at the node (get_normal_direction: sigma_P Ja^d_P)
+//   f_ll  = F_P . n_P (its own outward normal), f_rr = F_S . (-n_S) (the secondary's own normal, negated)
+//   Fn    = surface_flux(f_ll, f_rr, u_P, u_S, U_P, U_S, n)   (curvilinear argument order: Rusanov speed from
+//           the instantaneous u, jump in the time-averaged U; HLL speeds from U, jump in u)
+//   outward flux Fn on the primary, -Fn on the secondary; surface integral + apply_jacobian:
+//   du(face node) += -J^{-1}(node) / w_face * outward flux.
+// Corner nodes are shared by an element's xi and eta faces, so the host colours the interfaces such that no
+// launch touches both classes of faces of one element (two colours on a StructuredMesh); the launches of
+// one step run in colour order on one stream.
+#pragma once
+#include "tlw_device.cuh"
+#include "tlw_surface.cuh"
+
+namespace tlw {
+
+// Trixi max_abs_speed_naive (kind 0) / max_abs_speed (kind 1) with a normal direction
+__device__ __forceinline__ double max_abs_speed_normal(double gamma, const double* ul, const double* ur,
+                                                       const double* nrm, int kind, unsigned* status) {
+    const double gm1 = gamma - 1.0;
+    const double irl = 1.0 / ul[0], irr = 1.0 / ur[0];
+    const double v1l = ul[1] * irl, v2l = ul[2] * irl, v1r = ur[1] * irr, v2r = ur[2] * irr;
+    const double pl = gm1 * (ul[3] - 0.5 * (ul[1] * v1l + ul[2] * v2l));
+    const double pr = gm1 * (ur[3] - 0.5 * (ur[1] * v1r + ur[2] * v2r));
+    const double vl = v1l * nrm[0] + v2l * nrm[1];
+    const double vr = v1r * nrm[0] + v2r * nrm[1];
+    const double cl = checked_sqrt(gamma * pl * irl, status);
+    const double cr = checked_sqrt(gamma * pr * irr, status);
+    const double nn = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1]);
+    if (kind == 0) return fmax(fabs(vl), fabs(vr)) + fmax(cl, cr) * nn;
+    return fmax(fabs(vl) + cl * nn, fabs(vr) + cr * nn);
+}
+
+// Trixi min_max_speed_naive with a normal direction
+__device__ __forceinline__ void min_max_speed_normal(double gamma, const double* ul, const double* ur,
+                                                     const double* nrm, double* lmin, double* lmax,
+                                                     unsigned* status) {
+    const double gm1 = gamma - 1.0;
+    const double irl = 1.0 / ul[0], irr = 1.0 / ur[0];
+    const double v1l = ul[1] * irl, v2l = ul[2] * irl, v1r = ur[1] * irr, v2r = ur[2] * irr;
+    const double pl = gm1 * (ul[3] - 0.5 * (ul[1] * v1l + ul[2] * v2l));
+    const double pr = gm1 * (ur[3] - 0.5 * (ur[1] * v1r + ur[2] * v2r));
+    const double nn = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1]);
+    *lmin = (v1l * nrm[0] + v2l * nrm[1]) - checked_sqrt(gamma * pl * irl, status) * nn;
+    *lmax = (v1r * nrm[0] + v2r * nrm[1]) + checked_sqrt(gamma * pr * irr, status) * nn;
+}
+
+// the 8-argument LW surface flux with a normal direction, arguments (f_ll, f_rr, a3, a4, a5, a6)
+__device__ __forceinline__ void lw_surface_flux_normal(double gamma, int flux_kind, int speed_kind,
+                                                       const double* fl, const double* fr, const double* a3,
+                                                       const double* a4, const double* a5, const double* a6,
+                                                       const double* nrm, double* out, unsigned* status) {
+    if (flux_kind == 0) {
+        const double lambda = max_abs_speed_normal(gamma, a3, a4, nrm, speed_kind, status);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) out[v] = 0.5 * (fl[v] + fr[v]) + (-0.5 * lambda * (a6[v] - a5[v]));
+    } else {
+        double lmin, lmax;
+        min_max_speed_normal(gamma, a5, a6, nrm, &lmin, &lmax, status);
+        if (lmin >= 0.0 && lmax >= 0.0) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) out[v] = fl[v];
+        } else if (lmax <= 0.0 && lmin <= 0.0) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) out[v] = fr[v];
+        } else {
+            const double inv = 1.0 / (lmax - lmin);
+            const double fll = lmax * inv, frr = lmin * inv, fd = lmin * lmax * inv;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) out[v] = fll * fl[v] - frr * fr[v] + fd * (a4[v] - a3[v]);
+        }
+    }
+}
+
+// node (i, j) of face f at face index l
+__device__ __forceinline__ int face_node_index(int n, int f, int l) {
+    return f == 0 ? n * l : f == 1 ? (n - 1) + n * l : f == 2 ? l : l + n * (n - 1);
+}
+
+struct CurvedSurfArgs {
+    const double* u;          // [v, i, j, e]
+    double* out;              // du (rhs) or the updated state (step)
+    const double* tU;         // [v, l, face, e]
+    const double* tF;         // contravariant flux traces [v, l, face, e]
+    const double* metrics;    // [4, i, j, e]
+    const double* inv_jac;    // [i, j, e]
+    const int* p_elem;        // interfaces of this colour
+    const int* s_elem;
+    const int* faces;         // p_face | s_face << 2 | reversed << 4
+    int count;
+    const double* dt;
+    int step_mode;
+    double gamma;
+    int flux_kind, speed_kind;
+    double inv_w_first, inv_w_last;
+    unsigned* status;
+};
+
+template <int N>
+static __global__ void __launch_bounds__(128) curved_interface_kernel(CurvedSurfArgs a) {
+    constexpr int n = N + 1;
+    constexpr int nn = n * n;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = t / n;
+    const int l = t - k * n;
+    if (k >= a.count) return;
+    const int pe = __ldg(a.p_elem + k), se = __ldg(a.s_elem + k), code = __ldg(a.faces + k);
+    const int pf = code & 3, sf = (code >> 2) & 3;
+    const int ls = (code >> 4) & 1 ? n - 1 - l : l;
+    const int np = face_node_index(n, pf, l), ns = face_node_index(n, sf, ls);
+    const double sgP = (pf & 1) ? 1.0 : -1.0, sgS = (sf & 1) ? 1.0 : -1.0;
+    double uP[NV], uS[NV], UP[NV], US[NV], FP[NV], FS[NV], Fn[NV], J[4];
+    load4(a.u + ((size_t)pe * nn + np) * NV, uP);
+    load4(a.u + ((size_t)se * nn + ns) * NV, uS);
+    const size_t tp = (((size_t)pe * 4 + pf) * n + l) * NV, ts = (((size_t)se * 4 + sf) * n + ls) * NV;
+    load4(a.tU + tp, UP);
+    load4(a.tU + ts, US);
+    load4(a.tF + tp, FP);
+    load4(a.tF + ts, FS);
+    load4(a.metrics + ((size_t)pe * nn + np) * 4, J);
+    const double nrm[2] = {sgP * (pf < 2 ? J[0] : J[2]), sgP * (pf < 2 ? J[1] : J[3])};
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        FP[v] *= sgP;     // F_P . n_P
+        FS[v] *= -sgS;    // F_S . (-n_S)
+    }
+    lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, FP, FS, uP, uS, UP, US, nrm, Fn, a.status);
+    const double dts = a.step_mode ? *a.dt : 1.0;
+    const double cP = -dts * __ldg(a.inv_jac + (size_t)pe * nn + np) * ((pf & 1) ? a.inv_w_last : a.inv_w_first);
+    const double cS = dts * __ldg(a.inv_jac + (size_t)se * nn + ns) * ((sf & 1) ? a.inv_w_last : a.inv_w_first);
+    double* oP = a.out + ((size_t)pe * nn + np) * NV;
+    double* oS = a.out + ((size_t)se * nn + ns) * NV;
+    double x[NV];
+    load4_rw(oP, x);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) x[v] = fma(cP, Fn[v], x[v]);
+    store4(oP, x);
+    load4_rw(oS, x);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) x[v] = fma(cS, Fn[v], x[v]);
+    store4(oS, x);
+}
+
+// CFL reduction on curvilinear meshes (Trixi max_dt): per element max_nodes |Ja^1 . (l1, l2)| |J^{-1}| +
+// max_nodes |Ja^2 . (l1, l2)| |J^{-1}|, l_d = |v_d| + c; one thread per element
+template <int N>
+static __global__ void __launch_bounds__(128) curved_max_speed_kernel(const double* __restrict__ u,
+                                                                      const double* __restrict__ metrics,
+                                                                      const double* __restrict__ inv_jac, int E,
+                                                                      double gamma, StepState* s) {
+    constexpr int n = N + 1;
+    constexpr int nn = n * n;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double m = 0.0;
+    if (e < E) {
+        const double gm1 = gamma - 1.0;
+        double m1 = 0.0, m2 = 0.0;
+        for (int k = 0; k < nn; ++k) {
+            double x[NV], J[4];
+            load4(u + ((size_t)e * nn + k) * NV, x);
+            load4(metrics + ((size_t)e * nn + k) * 4, J);
+            const double ir = 1.0 / x[0];
+            const double v1 = x[1] * ir, v2 = x[2] * ir;
+            const double p = gm1 * (x[3] - 0.5 * (x[1] * v1 + x[2] * v2));
+            const double c = checked_sqrt(gamma * p * ir, &s->status);
+            const double l1 = fabs(v1) + c, l2 = fabs(v2) + c;
+            const double ij = fabs(__ldg(inv_jac + (size_t)e * nn + k));
+            m1 = fmax(m1, fabs(J[0] * l1 + J[1] * l2) * ij);
+            m2 = fmax(m2, fabs(J[2] * l1 + J[3] * l2) * ij);
+        }
+        m = m1 + m2;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(&s->max_bits, (unsigned long long)__double_as_longlong(m));
+}
+
+}  // namespace tlw

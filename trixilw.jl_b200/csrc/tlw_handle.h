@@ -85,6 +85,12 @@ struct tlw_handle {
     int *d_il = nullptr, *d_ir = nullptr;   // all interfaces (smoothing)
     int ni = 0;
     double jac_first = 0.0;                 // inverse Jacobian of element 1 (TreeMesh interface cache)
+    // conforming curvilinear mesh (instead of the TreeMesh arrays above; d_state etc. shared)
+    bool curved = false;
+    double* d_Ja = nullptr;                 // contravariant vectors [4, i, j, e]
+    double* d_ijn = nullptr;                // inverse Jacobian per node [i, j, e]
+    int *d_cp = nullptr, *d_cs = nullptr, *d_cf = nullptr;   // interfaces sorted by colour
+    std::vector<int> color_off;             // colour c covers [color_off[c], color_off[c + 1])
     // graphs: [start buffer] one step, two steps
     cudaGraphExec_t g_one[2] = {nullptr, nullptr};
     cudaGraphExec_t g_two[2] = {nullptr, nullptr};

@@ -68,7 +68,22 @@ struct VolArgs {
     unsigned* status;
     int speed_kind;
     const int* inst;        // batched form: instance of each element (dt indexed by it); null otherwise
+    // curvilinear meshes: contravariant vectors per node [4, i, j, e] (Ja^1_1, Ja^1_2, Ja^2_1, Ja^2_2) and the
+    // inverse Jacobian per node [i, j, e] (inv_jac is then unused)
+    const double* metrics;
+    const double* inv_jac_node;
 };
+
+// curvilinear: contravariant fluxes f~ = Ja^1_1 f + Ja^1_2 g, g~ = Ja^2_1 f + Ja^2_2 g of a node
+// (contravariant_flux, src/solvers/dgsem_structured/dg_2d.jl:541-556)
+__device__ __forceinline__ void contravariant(const double* Ja, const double* f, const double* g, double* ft,
+                                              double* gt) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        ft[v] = fma(Ja[0], f[v], Ja[1] * g[v]);
+        gt[v] = fma(Ja[2], f[v], Ja[3] * g[v]);
+    }
+}
 
 // owner: store the node's f (into X) and g (into Y)
 template <int N, class C>
@@ -258,8 +273,9 @@ __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, 
 //   depth 3: f_t = raw1/12, f_tt = raw2,    f_ttt = raw3/2
 //   depth 2: f_t = raw1/2,  f_tt = raw2;    depth 1: f_t = raw1/2
 // ------------------------------------------------------------------------------------------------
-template <int N, int MODE, bool SC, int EBX = 0>
+template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false>
 static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
+    static_assert(!(SC && CURVED), "shock capturing is built for TreeMesh only");
     using C = VolCfg<N, EBX>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     constexpr int DEPTH = N >= 4 ? 4 : N;
@@ -288,15 +304,31 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
 
     double U[NV], F[NV], G[NV], up[NV], um[NV], upp[NV], umm[NV];
-    double s0 = 0.0, ij = 0.0;   // s0 = -dt J^{-1}
-    // stage 0: f, g at u (dg_2d.jl:941-971)
+    double s0 = 0.0, ij = 0.0;   // s0 = -dt J^{-1} (of the element, or of the node on curvilinear meshes)
+    double Ja[4] = {0.0, 0.0, 0.0, 0.0};
+    // stage fluxes into the contraction planes (contravariant on curvilinear meshes)
+    auto put = [&](const double* f, const double* g) {
+        if (CURVED) {
+            double ft[NV], gt[NV];
+            contravariant(Ja, f, g, ft, gt);
+            node_put<N, C>(X, Y, el, i, j, ft, gt);
+        } else {
+            node_put<N, C>(X, Y, el, i, j, f, g);
+        }
+    };
+    // stage 0: f, g at u (dg_2d.jl:941-971; dgsem_structured/dg_2d.jl:1709-1740)
     if (active) {
         double uu[NV], f[NV], g[NV];
         load4(a.u + ((size_t)e * nn + node) * NV, uu);
-        ij = __ldg(a.inv_jac + e);
+        if (CURVED) {
+            load4(a.metrics + ((size_t)e * nn + node) * 4, Ja);
+            ij = __ldg(a.inv_jac_node + (size_t)e * nn + node);
+        } else {
+            ij = __ldg(a.inv_jac + e);
+        }
         s0 = -dt * ij;
         euler_fluxes(gm1, uu[0], uu[1], uu[2], uu[3], f, g);
-        node_put<N, C>(X, Y, el, i, j, f, g);
+        put(f, g);
         if (DEPTH >= 2 || SC) node_put<N, C>(F0X, F0Y, el, i, j, f, g);
         if (SC) sc_park<N, C>(UU, VC, el, i, j, uu, a.gamma, a.status);
 #pragma unroll
@@ -346,7 +378,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
         }
 #pragma unroll
         for (int v = 0; v < NV; ++v) { F[v] = fma(0.5 * C1, r[v], F[v]); G[v] = fma(0.5 * C1, q[v], G[v]); }
-        if (DEPTH >= 2) node_put<N, C>(X, Y, el, i, j, r, q);
+        if (DEPTH >= 2) put(r, q);
     }
     if (DEPTH >= 2) {
         __syncthreads();
@@ -397,7 +429,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
                 F[v] = fma(C2 / 6.0, r[v], F[v]);
                 G[v] = fma(C2 / 6.0, q[v], G[v]);
             }
-            if (DEPTH >= 3) node_put<N, C>(X, Y, el, i, j, r, q);
+            if (DEPTH >= 3) put(r, q);
         }
     }
     if (DEPTH >= 3) {
@@ -436,7 +468,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
                 F[v] = fma(C3 / 24.0, r[v], F[v]);
                 G[v] = fma(C3 / 24.0, q[v], G[v]);
             }
-            if (DEPTH >= 4) node_put<N, C>(X, Y, el, i, j, r, q);
+            if (DEPTH >= 4) put(r, q);
         }
     }
     if (DEPTH >= 4) {
@@ -481,6 +513,14 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     // final: Dhat contraction of the time-averaged fluxes (every owner has read its node's results of
     // the last contraction before writing F, G over them: same address, same thread)
     if (active) {
+        if (CURVED) {
+            // the surface needs the normal fluxes: keep the contravariant time averages F~, G~ (their face
+            // values are F . Ja^1 and F . Ja^2)
+            double ft[NV], gt[NV];
+            contravariant(Ja, F, G, ft, gt);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { F[v] = ft[v]; G[v] = gt[v]; }
+        }
         node_put<N, C>(X, Y, el, i, j, F, G);
         if (SC) sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
     }

@@ -37,7 +37,7 @@ EXPORTED = (
     "tlw_batch_set_state", "tlw_batch_get_state", "tlw_batch_step", "tlw_batch_synchronize",
     "tlw_batch_get_stream", "tlw_batch_autotune", "tlw_batch_num_groups", "tlw_batch_last_error",
     "tlw_adjoint_step", "tlw_forward_record", "tlw_adjoint_sweep", "tlw_adjoint_solve", "tlw_adjoint_dt_sequence",
-    "tlw_solve_dts",
+    "tlw_solve_dts", "tlw_set_curved_mesh", "tlw_curved_colors",
 )
 
 
@@ -106,6 +106,9 @@ def lib() -> ctypes.CDLL:
     L.tlw_last_error.argtypes = [P]
     L.tlw_last_error.restype = ctypes.c_char_p
     i32p = ctypes.POINTER(ctypes.c_int32)
+    L.tlw_set_curved_mesh.argtypes = [P, i64, dp, dp, i64, i64p, i32p, i64p, i32p, i32p]
+    L.tlw_curved_colors.argtypes = [P]
+    L.tlw_curved_colors.restype = i32
     L.tlw_adjoint_step.argtypes = [P, P, P, P, dbl, i32]
     L.tlw_forward_record.argtypes = [P, P, i32, dbl, i32, P, i32]
     L.tlw_adjoint_sweep.argtypes = [P, P, P, i32, dp]
@@ -127,7 +130,8 @@ def lib() -> ctypes.CDLL:
     L.tlw_batch_last_error.argtypes = [P]
     L.tlw_batch_last_error.restype = ctypes.c_char_p
     for name in EXPORTED:
-        keep = ("tlw_abi_version", "tlw_cache_size", "tlw_last_error", "tlw_batch_num_groups", "tlw_batch_last_error")
+        keep = ("tlw_abi_version", "tlw_cache_size", "tlw_last_error", "tlw_batch_num_groups", "tlw_batch_last_error",
+                "tlw_curved_colors")
         L[name].restype = L[name].restype if name in keep else ctypes.c_int
     _lib = L
     return L

@@ -52,3 +52,23 @@ def gauss_lobatto(N: int):
     """(nodes, weights) of the N+1 point Gauss-Lobatto-Legendre rule on [-1, 1]."""
     x, w = _gll(int(N))
     return x.copy(), w.copy()
+
+
+@functools.lru_cache(maxsize=None)
+def _dmat(N: int):
+    # Kopriva Algs. 30 and 37: barycentric weights, then the polynomial derivative matrix
+    x, _ = _gll(N)
+    n = N + 1
+    wb = np.array([1.0 / np.prod([x[c] - x[k] for k in range(n) if k != c]) for c in range(n)])
+    D = np.zeros((n, n))
+    for r in range(n):
+        for c in range(n):
+            if c != r:
+                D[r, c] = wb[c] / wb[r] / (x[r] - x[c])
+                D[r, r] -= D[r, c]
+    return D
+
+
+def derivative_matrix(N: int) -> np.ndarray:
+    """D[r, c] = l_c'(x_r) on the N+1 GLL nodes (Trixi derivative_matrix)."""
+    return _dmat(int(N)).copy()

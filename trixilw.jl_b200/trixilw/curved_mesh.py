@@ -1,0 +1,185 @@
+"""Curvilinear conforming meshes built on the host: StructuredMesh{2} from a mapping, and the generic
+form (primary / secondary element faces) that P4estMesh{2} and UnstructuredMesh2D reduce to.
+
+Metric terms as Trixi computes them for 2D curved meshes (from the mathematics: the derivative matrix
+applied to the nodal coordinates of each element):
+    x_xi = D x (along i), x_eta = D x (along j), same for y
+    Ja^1 = (y_eta, -x_eta),  Ja^2 = (-y_xi, x_xi),  J = x_xi y_eta - x_eta y_xi,  inverse_jacobian = 1 / J
+stored as contravariant_vectors[d, a, i, j, element] = Ja^a_d (Trixi's layout) and inverse_jacobian[i, j, e].
+
+StructuredMesh{2}(cells_per_dimension, mapping): elements in column-major cell order (x fastest), node
+coordinates mapping(xi_g, eta_g) at the global reference coordinates of the GLL nodes, computed as
+(cell + (xi + 1) / 2) * 2 / cells - 1 so that the two elements of a face see bitwise identical face nodes
+(Trixi writes the same points as -1 + (cell - 1) dx + dx / 2 (1 + xi)). Interfaces take the right / upper
+element as primary (its -xi / -eta face), which is the normal StructuredMesh's calc_interface_flux! uses
+(src/solvers/dgsem_structured/dg_2d.jl:2233-2267). Periodic in both directions (boundaries are not built
+on the curvilinear device path).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .basis import derivative_matrix, gauss_lobatto
+
+
+def metric_terms(xy: np.ndarray, polydeg: int):
+    """(Ja [E, j, i, 4] = Ja^1_1, Ja^1_2, Ja^2_1, Ja^2_2 per node, inverse_jacobian [E, j, i]) of node
+    coordinates xy [2, n(i), n(j), E]."""
+    D = derivative_matrix(polydeg)
+    x = np.transpose(xy[0], (2, 1, 0))   # [E, j, i]
+    y = np.transpose(xy[1], (2, 1, 0))
+    x_xi = np.einsum("ik,ejk->eji", D, x)
+    y_xi = np.einsum("ik,ejk->eji", D, y)
+    x_eta = np.einsum("jk,eki->eji", D, x)
+    y_eta = np.einsum("jk,eki->eji", D, y)
+    Ja = np.stack([y_eta, -x_eta, -y_xi, x_xi], axis=-1)
+    J = x_xi * y_eta - x_eta * y_xi
+    return np.ascontiguousarray(Ja), np.ascontiguousarray(1.0 / J)
+
+
+class CurvedMesh:
+    """A conforming curvilinear mesh in the form the library takes: per node metric terms and per
+    interface (primary element, face; secondary element, face; secondary index reversed). Faces 0: -xi
+    (i = 1), 1: +xi (i = n), 2: -eta (j = 1), 3: +eta (j = n); elements 1-based as Trixi stores them."""
+
+    n_boundaries = 0
+
+    def __init__(self, xy: np.ndarray, polydeg: int, primary_elements, primary_faces, secondary_elements,
+                 secondary_faces, secondary_reversed, area: float):
+        self.polydeg = polydeg
+        self.xy = np.ascontiguousarray(xy)                   # [2, n, n, E]
+        self.n_elements = xy.shape[-1]
+        self.Ja, self.inverse_jacobian_nodes = metric_terms(xy, polydeg)
+        if np.any(self.inverse_jacobian_nodes <= 0):
+            raise ValueError("the mapping must preserve orientation (positive Jacobian)")
+        self.primary_elements = np.ascontiguousarray(primary_elements, dtype=np.int64)
+        self.primary_faces = np.ascontiguousarray(primary_faces, dtype=np.int32)
+        self.secondary_elements = np.ascontiguousarray(secondary_elements, dtype=np.int64)
+        self.secondary_faces = np.ascontiguousarray(secondary_faces, dtype=np.int32)
+        self.secondary_reversed = np.ascontiguousarray(secondary_reversed, dtype=np.int32)
+        self.n_interfaces = len(self.primary_elements)
+        self.area = float(area)
+
+    def node_coordinates(self, polydeg: int) -> np.ndarray:
+        if polydeg != self.polydeg:
+            raise ValueError("this curved mesh was built for polydeg %d" % self.polydeg)
+        return self.xy
+
+    def ndofs(self, polydeg: int) -> int:
+        return self.n_elements * (polydeg + 1) ** 2
+
+    def jacobian_nodes(self) -> np.ndarray:
+        """|J| per node [E, j, i] (quadrature weight factor)."""
+        return 1.0 / self.inverse_jacobian_nodes
+
+
+class StructuredMesh:
+    """StructuredMesh{2}(cells_per_dimension, mapping; periodicity = true). ``mapping(xi, eta)`` maps the
+    reference square [-1, 1]^2 onto the domain (vectorised over numpy arrays) and must be periodic-compatible:
+    opposite sides of the square map to sides that differ by a translation."""
+
+    n_boundaries = 0
+
+    def __init__(self, cells_per_dimension, mapping, periodicity=True):
+        if isinstance(periodicity, bool):
+            periodicity = (periodicity, periodicity)
+        if not all(periodicity):
+            raise NotImplementedError("boundaries are not built on the curvilinear device path: use a periodic mesh")
+        self.cells = tuple(int(c) for c in cells_per_dimension)
+        self.mapping = mapping
+        nx, ny = self.cells
+        self.n_elements = nx * ny
+        self._curved = {}
+
+    def element(self, cx, cy):
+        return cx + self.cells[0] * cy
+
+    def node_coordinates(self, polydeg: int) -> np.ndarray:
+        nodes, _ = gauss_lobatto(polydeg)
+        nx, ny = self.cells
+        cx = np.arange(nx)
+        cy = np.arange(ny)
+        xi_g = (cx[:, None] + 0.5 * (nodes[None, :] + 1.0)) * (2.0 / nx) - 1.0    # [cx, i]
+        eta_g = (cy[:, None] + 0.5 * (nodes[None, :] + 1.0)) * (2.0 / ny) - 1.0   # [cy, j]
+        n = len(nodes)
+        e = np.arange(self.n_elements)
+        XI = np.ascontiguousarray(np.broadcast_to(xi_g[e % nx].T[:, None, :], (n, n, self.n_elements)))
+        ETA = np.ascontiguousarray(np.broadcast_to(eta_g[e // nx].T[None, :, :], (n, n, self.n_elements)))
+        x, y = self.mapping(XI, ETA)
+        return np.stack([np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64)])
+
+    def curved(self, polydeg: int) -> CurvedMesh:
+        if polydeg not in self._curved:
+            nx, ny = self.cells
+            pe, pf, se, sf = [], [], [], []
+            for cy in range(ny):
+                for cx in range(nx):
+                    e = self.element(cx, cy)
+                    pe.append(e); pf.append(0); se.append(self.element((cx - 1) % nx, cy)); sf.append(1)
+            for cy in range(ny):
+                for cx in range(nx):
+                    e = self.element(cx, cy)
+                    pe.append(e); pf.append(2); se.append(self.element(cx, (cy - 1) % ny)); sf.append(3)
+            xy = self.node_coordinates(polydeg)
+            area = float(np.einsum("eji,j,i->", 1.0 / metric_terms(xy, polydeg)[1], *(2 * [gauss_lobatto(polydeg)[1]])))
+            self._curved[polydeg] = CurvedMesh(xy, polydeg, np.array(pe) + 1, pf, np.array(se) + 1, sf,
+                                               np.zeros(len(pe), dtype=np.int32), area)
+        return self._curved[polydeg]
+
+    def ndofs(self, polydeg: int) -> int:
+        return self.n_elements * (polydeg + 1) ** 2
+
+
+# rotation of an element's local frame by a quarter turn: new node (a, b) holds old node (n-1-b, a);
+# old face f becomes new face _FACE_ROT[f], and the index along it runs backwards when _FLIP_ROT[f]
+_FACE_ROT = (3, 2, 0, 1)
+_FLIP_ROT = (0, 0, 1, 1)
+
+
+def rotate_elements(mesh: CurvedMesh, turns) -> CurvedMesh:
+    """The same mesh with element e's local frame turned by turns[e] quarter turns (P4est-like element
+    orientations: faces and face directions no longer line up). Metrics are recomputed from the rotated
+    node coordinates. Use rotate_state to carry states along."""
+    turns = np.asarray(turns, dtype=np.int64) % 4
+    xy = mesh.xy.copy()
+    for r in range(1, 4):
+        sel = turns == r
+        for _ in range(r):
+            xy[:, :, :, sel] = rot_nodes(xy[:, :, :, sel])
+    def face_map(f, r):
+        flip = 0
+        for _ in range(r):
+            flip ^= _FLIP_ROT[f]
+            f = _FACE_ROT[f]
+        return f, flip
+    pe = mesh.primary_elements - 1
+    se = mesh.secondary_elements - 1
+    pf, sf, rev = [], [], []
+    for k in range(mesh.n_interfaces):
+        fp, flp = face_map(int(mesh.primary_faces[k]), int(turns[pe[k]]))
+        fs, fls = face_map(int(mesh.secondary_faces[k]), int(turns[se[k]]))
+        pf.append(fp); sf.append(fs); rev.append(int(mesh.secondary_reversed[k]) ^ flp ^ fls)
+    return CurvedMesh(xy, mesh.polydeg, mesh.primary_elements, pf, mesh.secondary_elements, sf, rev, mesh.area)
+
+
+def rot_nodes(a: np.ndarray) -> np.ndarray:
+    """One quarter turn of node arrays [..., n(i), n(j), E]: new[a, b] = old[n-1-b, a]."""
+    n = a.shape[-3]
+    out = np.empty_like(a)
+    for ia in range(n):
+        for ib in range(n):
+            out[..., ia, ib, :] = a[..., n - 1 - ib, ia, :]
+    return out
+
+
+def rotate_state(u: np.ndarray, polydeg: int, turns) -> np.ndarray:
+    """Carry a flat state [v, i, j, e] into the rotated frames of rotate_elements."""
+    n = polydeg + 1
+    turns = np.asarray(turns, dtype=np.int64) % 4
+    E = len(turns)
+    x = np.transpose(u.reshape(E, n, n, 4), (3, 2, 1, 0)).copy()    # [v, i, j, e]
+    for r in range(1, 4):
+        sel = turns == r
+        for _ in range(r):
+            x[:, :, :, sel] = rot_nodes(x[:, :, :, sel])
+    return np.ascontiguousarray(np.transpose(x, (3, 2, 1, 0))).reshape(-1)

@@ -138,9 +138,13 @@ def l2_linf_errors(semi: SemidiscretizationHyperbolic, u_ode: np.ndarray, t: flo
         ue = np.ascontiguousarray(np.transpose(v, (2, 1, 0, 3))).reshape(-1)
     n = semi.nnodes
     _, w = gauss_lobatto(semi.polydeg)
-    d = (u_ode - ue).reshape(semi.mesh.n_elements, n, n, 4)
-    jac = 1.0 / semi.mesh.inverse_jacobian          # |J| = h/2 per direction -> area factor jac^2
+    d = (u_ode - ue).reshape(-1, n, n, 4)
     ww = (w[None, :, None] * w[None, None, :])      # [1, j, i]
-    l2 = np.sqrt(np.einsum("ejiv,eji->v", d * d, ww * (jac ** 2)[:, None, None]) / semi.mesh.length ** 2)
+    if getattr(semi, "curved", None) is not None:
+        # curvilinear: |J| per node, domain area from the same quadrature
+        l2 = np.sqrt(np.einsum("ejiv,eji->v", d * d, ww * semi.curved.jacobian_nodes()) / semi.curved.area)
+    else:
+        jac = 1.0 / semi.mesh.inverse_jacobian          # |J| = h/2 per direction -> area factor jac^2
+        l2 = np.sqrt(np.einsum("ejiv,eji->v", d * d, ww * (jac ** 2)[:, None, None]) / semi.mesh.length ** 2)
     linf = np.abs(d).max(axis=(0, 1, 2))
     return l2, linf

@@ -190,8 +190,15 @@ class SemidiscretizationHyperbolic:
                  source_terms=None):
         if source_terms is not None:
             raise NotImplementedError("source terms are not built on the device path")
-        if not isinstance(mesh, TreeMesh):
-            raise NotImplementedError("only TreeMesh{2} is built")
+        from .curved_mesh import CurvedMesh, StructuredMesh
+        if isinstance(mesh, StructuredMesh):
+            self.curved = mesh.curved(solver.polydeg)
+        elif isinstance(mesh, CurvedMesh):
+            self.curved = mesh
+        elif isinstance(mesh, TreeMesh):
+            self.curved = None
+        else:
+            raise NotImplementedError("TreeMesh{2}, StructuredMesh{2} and conforming curvilinear meshes are built")
         self.mesh = mesh
         self.equations = equations
         self.initial_condition = initial_condition
@@ -222,7 +229,8 @@ class SemidiscretizationHyperbolic:
         self._handle = _Handle(opts)
         self._upload_mesh()
         self._bdata_key = None
-        self.node_coordinates = mesh.node_coordinates(self.polydeg)
+        self.node_coordinates = (self.curved.xy if self.curved is not None
+                                 else mesh.node_coordinates(self.polydeg))
         if mesh.n_boundaries:
             self._bnd_xy = mesh.boundary_node_coordinates(self.polydeg)
 
@@ -231,6 +239,23 @@ class SemidiscretizationHyperbolic:
         return self._handle.ptr
 
     def _upload_mesh(self):
+        if self.curved is not None:
+            c = self.curved
+            Ja = np.ascontiguousarray(c.Ja, dtype=np.float64)                     # [E, j, i, 4] = [4, i, j, E]
+            ij = np.ascontiguousarray(c.inverse_jacobian_nodes, dtype=np.float64)  # [E, j, i] = [i, j, E]
+            arrs = (np.ascontiguousarray(c.primary_elements, dtype=np.int64),
+                    np.ascontiguousarray(c.primary_faces, dtype=np.int32),
+                    np.ascontiguousarray(c.secondary_elements, dtype=np.int64),
+                    np.ascontiguousarray(c.secondary_faces, dtype=np.int32),
+                    np.ascontiguousarray(c.secondary_reversed, dtype=np.int32))
+            self._keep = (Ja, ij) + arrs
+            i32p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+            dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            rc = lib().tlw_set_curved_mesh(self.handle, c.n_elements, dp(Ja), dp(ij), c.n_interfaces,
+                                           _i64p(arrs[0]), i32p(arrs[1]), _i64p(arrs[2]), i32p(arrs[3]),
+                                           i32p(arrs[4]))
+            check(self.handle, rc)
+            return
         m = self.mesh
         ij = np.ascontiguousarray(m.inverse_jacobian, dtype=np.float64)
         nid = np.ascontiguousarray(m.interface_neighbor_ids, dtype=np.int64)
