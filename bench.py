@@ -39,6 +39,8 @@ WORKLOADS = {
     "vortex_tree256_N4_lw": (8, 4, "lw", "vortex"),
     "vortex_tree512_N4_mdrk": (9, 4, "mdrk", "vortex"),
     "riemann_tree512_N4_lw": (9, 4, "lw", "riemann"),
+    # StructuredMesh{2} 512 x 512 on [-10, 10]^2 warped by x += sin(pi (x+10)/10) sin(pi (y+10)/10) (same for y)
+    "vortex_warped512_N4_lw": (9, 4, "lw", "warped"),
 }
 # batched form: 512 independent vortex instances (per-instance seed 0..511: side from {8, 16, 32, 64}
 # elements, degree from {3, 4, 5}, strength ~ U[1, 5], centre ~ U[-2, 2]^2), 50 LW steps
@@ -48,19 +50,24 @@ ADJOINT_WORKLOADS = {"adjoint128_vortex_lw": (7, 4, 200, 20)}
 FALLBACK_HBM_GBS = 6650.0
 
 
-def alg_bytes_per_element_step(N: int, td: str) -> float:
+def alg_bytes_per_element_step(N: int, td: str, curved: bool = False) -> float:
     """Algorithmic HBM bytes of one rhs/step per element (two-pass model): 8 nv (2n^2 + 28n - 8);
-    an MDRK step is 2 B + 8 nv 6 n^2."""
+    an MDRK step is 2 B + 8 nv 6 n^2. Curvilinear meshes add the metric terms (Ja, 4 doubles, and J^-1 per
+    node) read by the volume and CFL passes and, per interface node, Ja of the primary and J^-1 of both
+    sides: 8 (2 * 5 n^2 + 2 n * 6)."""
     n, nv = N + 1, 4
     b = 8 * nv * (2 * n * n + 28 * n - 8)
+    if curved:
+        b += 8 * (2 * 5 * n * n + 2 * n * 6)
     return 2 * b + 8 * nv * 6 * n * n if td == "mdrk" else b
 
 
-def volume_kernel_bytes_per_element(N: int, td: str) -> float:
+def volume_kernel_bytes_per_element(N: int, td: str, curved: bool = False) -> float:
     """Algorithmic bytes of one LW volume-kernel launch per element: read u (nv n^2), write u_new
-    (nv n^2), write the face traces of U and F.n (2 x 4 faces x n x nv)."""
+    (nv n^2), write the face traces of U and F.n (2 x 4 faces x n x nv); curvilinear: read Ja and J^-1
+    (5 n^2)."""
     n, nv = N + 1, 4
-    return 8.0 * (2 * nv * n * n + 2 * 4 * n * nv)
+    return 8.0 * (2 * nv * n * n + 2 * 4 * n * nv + (5 * n * n if curved else 0))
 
 
 def volume_flops_per_node(N: int) -> float:
@@ -143,10 +150,31 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
 
 
+def warp_mapping(xi, eta):
+    """[-1, 1]^2 -> [-10, 10]^2 with a periodic sinusoidal warp of 5 % of the side."""
+    import numpy as np
+    X = 10.0 * xi
+    Y = 10.0 * eta
+    s = np.sin(np.pi * (X + 10.0) / 10.0) * np.sin(np.pi * (Y + 10.0) / 10.0)
+    return X + s, Y + s
+
+
+def make_mesh(tl, level, icname):
+    if icname == "warped":
+        m = 1 << level
+        return tl.StructuredMesh((m, m), warp_mapping)
+    if icname == "vortex":
+        return tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), level)
+    return tl.TreeMesh((0.0, 0.0), (1.0, 1.0), level, periodicity=False)
+
+
 def build_semi(tl, level, N, td, icname, device):
     eq = tl.CompressibleEulerEquations2D(1.4)
     tdo = tl.LW() if td == "lw" else tl.MDRK()
     solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tdo))
+    if icname == "warped":
+        return tl.SemidiscretizationHyperbolic(make_mesh(tl, level, icname), tdo, eq, tl.IsentropicVortex(5.0),
+                                               solver, device=device)
     if icname == "vortex":
         mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), level)
         ic = tl.IsentropicVortex(5.0)
@@ -186,13 +214,9 @@ def cpu_oracle_rate(level, N, td, icname, steps_hint, budget_s=20.0):
     import trixilw as tl
 
     eq = tl.CompressibleEulerEquations2D(1.4)
-    if icname == "vortex":
-        mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), level)
-        ic = tl.IsentropicVortex(5.0)
-    else:
-        mesh = tl.TreeMesh((0.0, 0.0), (1.0, 1.0), level, periodicity=False)
-        ic = tl.FourQuadrantRiemann()
-    xy = mesh.node_coordinates(N)
+    mesh = make_mesh(tl, level, icname)
+    ic = tl.FourQuadrantRiemann() if icname == "riemann" else tl.IsentropicVortex(5.0)
+    xy = mesh.curved(N).xy if icname == "warped" else mesh.node_coordinates(N)
     u = np.ascontiguousarray(np.transpose(ic(xy[0], xy[1], 0.0, eq), (2, 1, 0, 3))).reshape(-1)
     o = pyoracle.Oracle(mesh, N)
     if mesh.n_boundaries:
@@ -201,8 +225,8 @@ def cpu_oracle_rate(level, N, td, icname, steps_hint, budget_s=20.0):
         o.set_boundary_data(np.repeat(now[:, :, None, :], N + 1, axis=2), now)
     threads = os.cpu_count() or 1
     kind = 0 if td == "lw" else 1
-    cfl = cfl_for(N) if icname == "vortex" else RIEMANN_CFL
-    if icname != "vortex":
+    cfl = RIEMANN_CFL if icname == "riemann" else cfl_for(N)
+    if icname == "riemann":
         o.set_shock_capturing(True, 0.5, 0.001, True)
     t0 = time.perf_counter()
     o.steps(u, 1, cfl, 0.0, 1e9, kind=kind, nthreads=threads)
@@ -338,7 +362,7 @@ def run_ours(args):
     level, N, td, icname = WORKLOADS[args.workload]
     semi = build_semi(tl, level, N, td, icname, local_rank)
     ndofs = semi.ndofs()
-    cfl = cfl_for(N) if icname == "vortex" else RIEMANN_CFL
+    cfl = RIEMANN_CFL if icname == "riemann" else cfl_for(N)
     u0 = semi.compute_coefficients(0.0)
     upd = tl.semidiscretize(semi, semi.time_discretization, (0.0, 1e9))
     integ = tl.LWIntegrator(upd)
@@ -418,16 +442,17 @@ def run_ours(args):
 
     if rank == 0:
         E = semi.mesh.n_elements
+        curved = icname == "warped"
         peak, peak_kind = measured_peaks()
         vol_ms = phase[1] / args.steps
-        vol_bytes = volume_kernel_bytes_per_element(N, td) * E
+        vol_bytes = volume_kernel_bytes_per_element(N, td, curved) * E
         achieved = vol_bytes / (vol_ms * 1e-3) / 1e9
         fp = ctypes.c_double()
         fp64_peak = fp.value if L.tlw_probe_fp64_tflops(local_rank, ctypes.byref(fp)) == 0 else None
         vol_flops = volume_flops_per_node(N) * ndofs
-        tag = f"lw_volume_kernel_N{N}_tree{1 << level}"
+        tag = f"lw_volume_kernel_N{N}_{'warped' if curved else 'tree'}{1 << level}"
         traffic = profile_traffic(tag)
-        step_alg = alg_bytes_per_element_step(N, td) * E
+        step_alg = alg_bytes_per_element_step(N, td, curved) * E
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -438,7 +463,8 @@ def run_ours(args):
                        "parallelism": f"replicas{world}" if world > 1 else "single"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                     "steps": n_e2e},
-            "roofline": {"kernel": f"lw_volume_kernel<{N}, MODE_STEP>", "bound": "hbm", "achieved": achieved,
+            "roofline": {"kernel": f"lw_volume_kernel<{N}, MODE_STEP{', CURVED' if curved else ''}>", "bound": "hbm",
+                         "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                          "alg_bytes_per_launch": vol_bytes, "ms_per_launch": vol_ms,
@@ -453,7 +479,7 @@ def run_ours(args):
                                                "step": phase[4] / args.steps}},
             "clocks": clocks,
             "gpu_launches": args.steps * (2 + (3 + (2 if semi.mesh.n_boundaries else 0)) * (2 if td == "mdrk" else 1)
-                                          + (1 if icname != "vortex" else 0)),
+                                          + (1 if icname == "riemann" else 0)),
         }
         if world == 1 and not args.no_cpu_baseline:
             rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=args.steps)
