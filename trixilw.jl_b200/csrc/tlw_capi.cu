@@ -121,7 +121,7 @@ struct Launch {
     static void curved_speed(cudaStream_t s, const double* u, const double* Ja, const double* ij, int E, double g,
                              StepState* st) {
         if (E == 0) return;
-        curved_max_speed_kernel<N><<<(E + 127) / 128, 128, 0, s>>>(u, Ja, ij, E, g, st);
+        curved_max_speed_kernel<N><<<(E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS, MS_THREADS, 0, s>>>(u, Ja, ij, E, g, st);
     }
     static void boundaries(cudaStream_t s, const BndArgs& a) {
         const long long threads = (long long)a.count * (N + 1);

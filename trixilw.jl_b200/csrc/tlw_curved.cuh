@@ -150,37 +150,54 @@ static __global__ void __launch_bounds__(128) curved_interface_kernel(CurvedSurf
 }
 
 // CFL reduction on curvilinear meshes (Trixi max_dt): per element max_nodes |Ja^1 . (l1, l2)| |J^{-1}| +
-// max_nodes |Ja^2 . (l1, l2)| |J^{-1}|, l_d = |v_d| + c; one thread per element
+// max_nodes |Ja^2 . (l1, l2)| |J^{-1}|, l_d = |v_d| + c. A CTA takes MsCfg<N>::ELEMS elements: a coalesced pass
+// over their nodes into shared memory, then one thread per element reduces its nodes.
 template <int N>
-static __global__ void __launch_bounds__(128) curved_max_speed_kernel(const double* __restrict__ u,
-                                                                      const double* __restrict__ metrics,
-                                                                      const double* __restrict__ inv_jac, int E,
-                                                                      double gamma, StepState* s) {
+static __global__ void __launch_bounds__(MS_THREADS) curved_max_speed_kernel(const double* __restrict__ u,
+                                                                             const double* __restrict__ metrics,
+                                                                             const double* __restrict__ inv_jac,
+                                                                             int E, double gamma, StepState* s) {
     constexpr int n = N + 1;
     constexpr int nn = n * n;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int ELEMS = MsCfg<N>::ELEMS;
+    __shared__ double l1s[ELEMS * nn], l2s[ELEMS * nn];
+    __shared__ double wmax[MS_THREADS / 32];
+    const int e0 = blockIdx.x * ELEMS;
+    const int ne = min(ELEMS, E - e0);
+    const double gm1 = gamma - 1.0;
+    for (int k = threadIdx.x; k < ne * nn; k += MS_THREADS) {
+        const size_t node = (size_t)e0 * nn + k;
+        double x[NV], J[4];
+        load4(u + node * NV, x);
+        load4(metrics + node * 4, J);
+        const double ir = 1.0 / x[0];
+        const double v1 = x[1] * ir, v2 = x[2] * ir;
+        const double p = gm1 * (x[3] - 0.5 * (x[1] * v1 + x[2] * v2));
+        const double c = checked_sqrt(gamma * p * ir, &s->status);
+        const double l1 = fabs(v1) + c, l2 = fabs(v2) + c;
+        const double ij = fabs(__ldg(inv_jac + node));
+        l1s[k] = fabs(J[0] * l1 + J[1] * l2) * ij;
+        l2s[k] = fabs(J[2] * l1 + J[3] * l2) * ij;
+    }
+    __syncthreads();
     double m = 0.0;
-    if (e < E) {
-        const double gm1 = gamma - 1.0;
+    if (threadIdx.x < ne) {
         double m1 = 0.0, m2 = 0.0;
         for (int k = 0; k < nn; ++k) {
-            double x[NV], J[4];
-            load4(u + ((size_t)e * nn + k) * NV, x);
-            load4(metrics + ((size_t)e * nn + k) * 4, J);
-            const double ir = 1.0 / x[0];
-            const double v1 = x[1] * ir, v2 = x[2] * ir;
-            const double p = gm1 * (x[3] - 0.5 * (x[1] * v1 + x[2] * v2));
-            const double c = checked_sqrt(gamma * p * ir, &s->status);
-            const double l1 = fabs(v1) + c, l2 = fabs(v2) + c;
-            const double ij = fabs(__ldg(inv_jac + (size_t)e * nn + k));
-            m1 = fmax(m1, fabs(J[0] * l1 + J[1] * l2) * ij);
-            m2 = fmax(m2, fabs(J[2] * l1 + J[3] * l2) * ij);
+            m1 = fmax(m1, l1s[threadIdx.x * nn + k]);
+            m2 = fmax(m2, l2s[threadIdx.x * nn + k]);
         }
         m = m1 + m2;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(&s->max_bits, (unsigned long long)__double_as_longlong(m));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = wmax[0];
+        for (int w = 1; w < MS_THREADS / 32; ++w) b = fmax(b, wmax[w]);
+        if (b > 0.0) atomicMax(&s->max_bits, (unsigned long long)__double_as_longlong(b));
+    }
 }
 
 }  // namespace tlw
