@@ -90,12 +90,21 @@ int tlw_destroy(tlw_handle* h);
  *   interface_orientations [n_interfaces]     1 = x, 2 = y   Trixi interfaces.orientations
  *   boundary_* [n_boundaries]                 Trixi boundaries.neighbor_ids / orientations / neighbor_sides
  *   n_boundaries_per_direction [4]            boundaries grouped by direction 1..4 (dg_2d.jl:1385-1409)
- * Nonconforming meshes (mortars) are not built: pass none. */
+ * Non-conforming meshes: add their mortars with tlw_set_tree_mortars. */
 int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_jacobian, int64_t n_interfaces,
                       const int64_t* interface_neighbor_ids, const int64_t* interface_orientations,
                       int64_t n_boundaries, const int64_t* boundary_neighbor_ids,
                       const int64_t* boundary_orientations, const int64_t* boundary_neighbor_sides,
                       const int64_t* n_boundaries_per_direction);
+
+/* L2 mortars of a non-conforming TreeMesh{2} (after AMR), set after tlw_set_tree_mesh (which clears them):
+ *   mortar_neighbor_ids [3, n_mortars]  (lower small, upper small, large element), 1-based  Trixi mortars.neighbor_ids
+ *   mortar_large_sides  [n_mortars]     1: large element on the -side, 2: on the +side   Trixi mortars.large_sides
+ *   mortar_orientations [n_mortars]     1 = x, 2 = y                                     Trixi mortars.orientations
+ * The LW traces are carried over the mortar as prolong2mortars! / calc_mortar_flux! do
+ * (src/solvers/dgsem_tree/dg_2d.jl:1456-1646), with Trixi's L2 mortar operators. Not with shock capturing. */
+int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar_neighbor_ids,
+                         const int64_t* mortar_large_sides, const int64_t* mortar_orientations);
 
 /* Conforming curvilinear mesh (StructuredMesh{2}, or P4estMesh{2} / UnstructuredMesh2D without mortars), in
  * place of a TreeMesh; LW with the FR volume integral, periodic or fully connected (no boundaries).

@@ -108,6 +108,34 @@ oracle_handle* oracle_create_curved(int N, double gamma, int flux_kind, int spee
     } catch (...) { return nullptr; }
 }
 
+// L2 mortars of a TreeMesh: lower, upper, large element (0-based), large side (1: large on the -side), orientation
+int oracle_set_mortars(oracle_handle* h, int M, const int32_t* lower, const int32_t* upper, const int32_t* large,
+                       const int32_t* large_side, const int32_t* orientation) {
+    if (h->curved) return 1;
+    h->mesh.n_mortars = M;
+    h->mesh.mortar_lower.assign(lower, lower + M);
+    h->mesh.mortar_upper.assign(upper, upper + M);
+    h->mesh.mortar_large.assign(large, large + M);
+    h->mesh.mortar_large_side.assign(large_side, large_side + M);
+    h->mesh.mortar_orientation.assign(orientation, orientation + M);
+    return 0;
+}
+
+// the mortar operators of degree N: [4][n][n] = forward_upper, forward_lower, reverse_upper, reverse_lower
+int oracle_mortar_operators(int N, double* out) {
+    try {
+        const Basis b = make_basis(N);
+        const int nn = b.n * b.n;
+        for (int k = 0; k < nn; ++k) {
+            out[k] = b.fwd_upper[k];
+            out[nn + k] = b.fwd_lower[k];
+            out[2 * nn + k] = b.rev_upper[k];
+            out[3 * nn + k] = b.rev_lower[k];
+        }
+        return 0;
+    } catch (...) { return 1; }
+}
+
 void oracle_destroy(oracle_handle* h) { delete h; }
 
 // VolumeIntegralFRShockCapturing with IndicatorHennemannGassner(alpha_max, alpha_min, alpha_smooth;

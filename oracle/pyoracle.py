@@ -47,6 +47,8 @@ def lib():
         L.oracle_max_dt.restype = dbl
         L.oracle_steps.argtypes = [P, i32, P, i32, dbl, dbl, P, dbl, i32]
         L.oracle_adjoint_step.argtypes = [P, P, dbl, P, P, i32]
+        L.oracle_set_mortars.argtypes = [P, i32, P, P, P, P, P]
+        L.oracle_mortar_operators.argtypes = [i32, P]
         L.oracle_create_curved.argtypes = [i32, dbl, i32, i32, i32, P, P, i32, P, P, P, P, P]
         L.oracle_create_curved.restype = P
         L.oracle_last_error.argtypes = [P]
@@ -57,6 +59,14 @@ def lib():
 
 def _p(a):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def mortar_operators(N: int):
+    """(forward_upper, forward_lower, reverse_upper, reverse_lower), each [n, n]."""
+    n = N + 1
+    out = np.empty(4 * n * n)
+    assert lib().oracle_mortar_operators(N, _p(out)) == 0
+    return tuple(out.reshape(4, n, n))
 
 
 def basis(N: int):
@@ -99,6 +109,13 @@ class Oracle:
                                      _p(bs) if B else None, _p(bd) if B else None)
         if not self.h:
             raise RuntimeError("oracle_create failed")
+        if getattr(mesh, "n_mortars", 0):
+            ids = np.asarray(mesh.mortar_neighbor_ids, dtype=np.int64).reshape(-1, 3) - 1
+            arrs = [np.ascontiguousarray(ids[:, k], dtype=np.int32) for k in range(3)]
+            arrs += [np.ascontiguousarray(mesh.mortar_large_sides, dtype=np.int32),
+                     np.ascontiguousarray(mesh.mortar_orientations, dtype=np.int32)]
+            self._mkeep = arrs
+            assert lib().oracle_set_mortars(self.h, len(arrs[0]), *[_p(a) for a in arrs]) == 0
 
     def _init_curved(self, cm, polydeg, gamma, flux_kind, speed_kind):
         """Conforming curvilinear mesh (trixilw.curved_mesh.CurvedMesh or StructuredMesh)."""

@@ -51,7 +51,102 @@ struct Basis {
     std::vector<double> D;          // D[a*n + b]    = l_b'(x_a)          (Trixi derivative_matrix[a, b])
     std::vector<double> Dhat;       // Dhat[a*n + b] = -D[b, a] w_b / w_a (Trixi derivative_dhat[a, b])
     double inv_w_first = 0, inv_w_last = 0;   // Trixi boundary_interpolation[1,1], [n,2]
+    // LobattoLegendreMortarL2 (Trixi): forward_{upper,lower}[i*n + j] = l_j((x_i +- 1) / 2), reverse_* the L2
+    // projections back onto the large face (computed in make_basis from their mathematics)
+    std::vector<double> fwd_upper, fwd_lower, rev_upper, rev_lower;
 };
+
+// Lagrange basis polynomials of `nodes` at x (barycentric form, exact at the nodes)
+inline std::vector<double> lagrange_at(const std::vector<double>& nodes, double x) {
+    const int n = (int)nodes.size();
+    std::vector<double> wb(n, 1.0), l(n, 0.0);
+    for (int j = 0; j < n; ++j)
+        for (int k = 0; k < n; ++k)
+            if (k != j) wb[j] *= nodes[j] - nodes[k];
+    for (int j = 0; j < n; ++j) {
+        if (x == nodes[j]) { l[j] = 1.0; return l; }
+        wb[j] = 1.0 / wb[j];
+    }
+    double den = 0.0;
+    for (int j = 0; j < n; ++j) {
+        l[j] = wb[j] / (x - nodes[j]);
+        den += l[j];
+    }
+    for (int j = 0; j < n; ++j) l[j] /= den;
+    return l;
+}
+
+// Gauss-Legendre nodes and weights with n points (Newton on P_n, Kopriva Alg. 23)
+inline void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    const double pi = 3.14159265358979323846;
+    for (int j = 0; j < n; ++j) {
+        double xj = -std::cos((2.0 * j + 1.0) * pi / (2.0 * n)), dp = 0.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = xj;
+            dp = 1.0;
+            double d0 = 0.0;
+            for (int k = 2; k <= n; ++k) {
+                const double p2 = ((2.0 * k - 1.0) * xj * p1 - (k - 1.0) * p0) / k;
+                const double d2 = d0 + (2.0 * k - 1.0) * p1;
+                p0 = p1; p1 = p2; d0 = dp; dp = d2;
+            }
+            if (n == 1) { p1 = xj; dp = 1.0; }
+            const double delta = -p1 / dp;
+            xj += delta;
+            if (std::fabs(delta) <= 4.0 * std::numeric_limits<double>::epsilon() * std::fabs(xj)) break;
+        }
+        // derivative at the converged root
+        double p0 = 1.0, p1 = xj, d0 = 0.0;
+        dp = 1.0;
+        for (int k = 2; k <= n; ++k) {
+            const double p2 = ((2.0 * k - 1.0) * xj * p1 - (k - 1.0) * p0) / k;
+            const double d2 = d0 + (2.0 * k - 1.0) * p1;
+            p0 = p1; p1 = p2; d0 = dp; dp = d2;
+        }
+        x[j] = xj;
+        w[j] = 2.0 / ((1.0 - xj * xj) * dp * dp);
+    }
+}
+
+// The L2 mortar operators: forward = interpolation of the large face onto the small halves; reverse = the
+// L2 projection of the two halves back onto the large face, exact (done in the Gauss basis, whose mass
+// matrix is diagonal and exact for these degree-2N products, then mapped to and from the Lobatto nodes).
+inline void mortar_operators(Basis& b) {
+    const int n = b.n;
+    b.fwd_upper.assign(n * n, 0.0);
+    b.fwd_lower.assign(n * n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        const auto lu = lagrange_at(b.nodes, 0.5 * (b.nodes[i] + 1.0));
+        const auto ll = lagrange_at(b.nodes, 0.5 * (b.nodes[i] - 1.0));
+        for (int j = 0; j < n; ++j) { b.fwd_upper[i * n + j] = lu[j]; b.fwd_lower[i * n + j] = ll[j]; }
+    }
+    std::vector<double> g, wg;
+    gauss_legendre(n, g, wg);
+    std::vector<double> g2l(n * n), l2g(n * n);   // g2l[i][j] = lg_j(x_i); l2g[i][j] = l_j(g_i)
+    for (int i = 0; i < n; ++i) {
+        const auto a = lagrange_at(g, b.nodes[i]);
+        const auto c = lagrange_at(b.nodes, g[i]);
+        for (int j = 0; j < n; ++j) { g2l[i * n + j] = a[j]; l2g[i * n + j] = c[j]; }
+    }
+    auto reverse = [&](double shift, std::vector<double>& out) {
+        std::vector<double> op(n * n), tmp(n * n, 0.0);
+        for (int j = 0; j < n; ++j) {
+            const auto lg = lagrange_at(g, 0.5 * (g[j] + shift));
+            for (int i = 0; i < n; ++i) op[i * n + j] = 0.5 * lg[i] * wg[j] / wg[i];
+        }
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+                for (int k = 0; k < n; ++k) tmp[i * n + j] += op[i * n + k] * l2g[k * n + j];
+        out.assign(n * n, 0.0);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+                for (int k = 0; k < n; ++k) out[i * n + j] += g2l[i * n + k] * tmp[k * n + j];
+    };
+    reverse(1.0, b.rev_upper);
+    reverse(-1.0, b.rev_lower);
+}
 
 inline void legendre_q_and_l(int N, double x, double& q, double& dq, double& LN) {
     // Kopriva Alg. 24 (qAndLEvaluation)
@@ -125,6 +220,7 @@ inline Basis make_basis(int N) {
         for (int c = 0; c < n; ++c) b.Dhat[a * n + c] = -b.D[c * n + a] * b.weights[c] / b.weights[a];
     b.inv_w_first = 1.0 / b.weights[0];
     b.inv_w_last = 1.0 / b.weights[n - 1];
+    mortar_operators(b);
     return b;
 }
 
@@ -242,6 +338,10 @@ struct TreeMesh {
     // boundaries (src/solvers/dgsem_tree/dg_2d.jl:1328-1454); neighbor_side 1: element on the -side
     int n_boundaries = 0;
     std::vector<int32_t> boundary_element, boundary_orientation, boundary_side, boundary_direction;
+    // L2 mortars (Trixi mortars container): lower / upper small element, large element (0-based),
+    // large_sides 1: large element on the -side, 2: on the +side; orientation 1 (x) / 2 (y)
+    int n_mortars = 0;
+    std::vector<int32_t> mortar_lower, mortar_upper, mortar_large, mortar_large_side, mortar_orientation;
 };
 
 struct Options {
@@ -788,6 +888,70 @@ inline void surface_integral_and_jacobian(const Basis& b, const TreeMesh& m, dou
     }
 }
 
+// L2 mortars on TreeMesh{2} with the LW traces (src/solvers/dgsem_tree/dg_2d.jl:1456-1646):
+// prolong2mortars! copies the small elements' u, U, F face traces and interpolates the large element's
+// (element_solutions_to_mortars!), calc_fstar! evaluates the surface flux in the TreeMesh argument order on
+// both halves, and mortar_fluxes_to_elements! (Trixi) hands fstar to the small faces and its L2 projection
+// to the large face.
+inline void calc_mortar_flux(const Basis& b, const Euler& eq, const Options& opt, const TreeMesh& m,
+                             const double* u, Workspace& ws, int nthreads = 1) {
+    const int n = b.n;
+    bool bad = false;
+    auto face_node = [&](int f, int l, int& i, int& j) {
+        i = f == 0 ? 0 : f == 1 ? n - 1 : l;
+        j = f == 2 ? 0 : f == 3 ? n - 1 : l;
+    };
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad)
+    for (int k = 0; k < m.n_mortars; ++k) {
+        const int o = m.mortar_orientation[k];
+        const bool large_left = m.mortar_large_side[k] == 1;
+        const int small_face = large_left ? (o == 1 ? 0 : 2) : (o == 1 ? 1 : 3);
+        const int large_face = large_left ? (o == 1 ? 1 : 3) : (o == 1 ? 0 : 2);
+        const int d = o - 1;   // normal flux component
+        const int le = m.mortar_large[k];
+        std::vector<double> fstar(2 * n * NV);
+        for (int h = 0; h < 2; ++h) {
+            const int se = h ? m.mortar_upper[k] : m.mortar_lower[k];
+            const std::vector<double>& fwd = h ? b.fwd_upper : b.fwd_lower;
+            for (int l = 0; l < n; ++l) {
+                int is, js;
+                face_node(small_face, l, is, js);
+                double us[NV], Us[NV], Fs[NV], ul[NV] = {0, 0, 0, 0}, Ul[NV] = {0, 0, 0, 0}, Fl[NV] = {0, 0, 0, 0};
+                for (int v = 0; v < NV; ++v) {
+                    us[v] = u[idx_u(n, v, is, js, se)];
+                    Us[v] = ws.U[idx_u(n, v, is, js, se)];
+                    Fs[v] = ws.F[idx_F(n, v, d, is, js, se)];
+                }
+                for (int jj = 0; jj < n; ++jj) {
+                    int il, jl;
+                    face_node(large_face, jj, il, jl);
+                    const double c = fwd[l * n + jj];
+                    for (int v = 0; v < NV; ++v) {
+                        ul[v] += c * u[idx_u(n, v, il, jl, le)];
+                        Ul[v] += c * ws.U[idx_u(n, v, il, jl, le)];
+                        Fl[v] += c * ws.F[idx_F(n, v, d, il, jl, le)];
+                    }
+                }
+                bool b_ = false;
+                double* out = &fstar[(h * n + l) * NV];
+                if (large_left) lw_surface_flux(eq, opt.flux_kind, opt.speed_kind, Fl, Fs, Ul, Us, ul, us, o, out, b_);
+                else lw_surface_flux(eq, opt.flux_kind, opt.speed_kind, Fs, Fl, Us, Ul, us, ul, o, out, b_);
+                bad = bad || b_;
+                for (int v = 0; v < NV; ++v)
+                    ws.surface_flux_values[v + NV * (l + n * (small_face + 4 * (size_t)se))] = out[v];
+            }
+        }
+        for (int mm = 0; mm < n; ++mm)
+            for (int v = 0; v < NV; ++v) {
+                double acc = 0.0;
+                for (int l = 0; l < n; ++l)
+                    acc += b.rev_upper[mm * n + l] * fstar[(n + l) * NV + v] + b.rev_lower[mm * n + l] * fstar[l * NV + v];
+                ws.surface_flux_values[v + NV * (mm + n * (large_face + 4 * (size_t)le))] = acc;
+            }
+    }
+    if (bad) ws.bad = true;
+}
+
 inline void ensure_workspace(const Basis& b, const TreeMesh& m, Workspace& ws, bool mdrk) {
     const size_t nodes = (size_t)b.n * b.n * m.n_elements;
     const double nan = std::numeric_limits<double>::quiet_NaN();
@@ -1031,6 +1195,10 @@ inline void rhs(const Basis& b, const Euler& eq, const Options& opt, const TreeM
     if (m.n_boundaries > 0) {
         if (!bd || !bd->u_levels || !bd->u_now) throw std::invalid_argument("boundary data missing");
         calc_boundary_flux(b, eq, opt, m, u, *bd, kind == 1 ? 0.5 : 1.0, ws);
+    }
+    if (m.n_mortars > 0) {
+        if (opt.shock_capturing) throw std::invalid_argument("mortars with shock capturing are not restated");
+        calc_mortar_flux(b, eq, opt, m, u, ws, nthreads);
     }
     surface_integral_and_jacobian(b, m, du, ws, nthreads);
 }

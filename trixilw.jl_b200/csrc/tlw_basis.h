@@ -105,4 +105,87 @@ inline void host_build_basis(int N, Basis& B, std::vector<double>* nodes_out = n
     if (nodes_out) *nodes_out = x;
 }
 
+// Lagrange polynomials of `nodes` evaluated at t (barycentric; exact at a node)
+inline std::vector<double> host_lagrange(const std::vector<double>& nodes, double t) {
+    const int n = (int)nodes.size();
+    std::vector<double> wb(n, 1.0), l(n, 0.0);
+    for (int j = 0; j < n; ++j) {
+        for (int k = 0; k < n; ++k)
+            if (k != j) wb[j] *= nodes[j] - nodes[k];
+        wb[j] = 1.0 / wb[j];
+    }
+    for (int j = 0; j < n; ++j)
+        if (t == nodes[j]) { l[j] = 1.0; return l; }
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) { l[j] = wb[j] / (t - nodes[j]); s += l[j]; }
+    for (int j = 0; j < n; ++j) l[j] /= s;
+    return l;
+}
+
+// Operators of the L2 mortar between one large face and its two halves (Trixi LobattoLegendreMortarL2,
+// restated from the mathematics): out[0] forward_upper, [1] forward_lower (interpolation of the large face
+// polynomial at the half's GLL nodes, t = (x +- 1) / 2), [2] reverse_upper, [3] reverse_lower (exact L2
+// projection of the halves back onto the large face, computed through the N+1 point Gauss basis whose
+// mass matrix is diagonal and exact for the degree-2N products). Row-major n x n in 64 slots.
+inline void host_mortar_operators(int N, double out[4][64]) {
+    const int n = N + 1;
+    std::vector<double> x;
+    Basis B;
+    host_build_basis(N, B, &x);
+    std::memset(out, 0, 4 * 64 * sizeof(double));
+    for (int i = 0; i < n; ++i) {
+        const auto lu = host_lagrange(x, 0.5 * (x[i] + 1.0));
+        const auto ll = host_lagrange(x, 0.5 * (x[i] - 1.0));
+        for (int j = 0; j < n; ++j) { out[0][i * n + j] = lu[j]; out[1][i * n + j] = ll[j]; }
+    }
+    // Gauss-Legendre nodes / weights (Newton on P_n from -cos((2j+1) pi / 2n))
+    std::vector<double> g(n), wg(n);
+    const double pi = 3.14159265358979323846;
+    auto legendre = [&](double t, double& p, double& dp) {
+        double p0 = 1.0, p1 = t, d0 = 0.0, d1 = 1.0;
+        for (int k = 2; k <= n; ++k) {
+            const double p2 = ((2.0 * k - 1.0) * t * p1 - (k - 1.0) * p0) / k;
+            const double d2 = d0 + (2.0 * k - 1.0) * p1;
+            p0 = p1; p1 = p2; d0 = d1; d1 = d2;
+        }
+        p = p1;
+        dp = d1;
+    };
+    for (int j = 0; j < n; ++j) {
+        double t = -std::cos((2.0 * j + 1.0) * pi / (2.0 * n)), p, dp;
+        for (int it = 0; it < 100; ++it) {
+            legendre(t, p, dp);
+            const double d = -p / dp;
+            t += d;
+            if (std::fabs(d) <= 4.0 * 2.220446049250313e-16 * std::fabs(t)) break;
+        }
+        legendre(t, p, dp);
+        g[j] = t;
+        wg[j] = 2.0 / ((1.0 - t * t) * dp * dp);
+    }
+    std::vector<double> g2l(n * n), l2g(n * n);
+    for (int i = 0; i < n; ++i) {
+        const auto a = host_lagrange(g, x[i]);
+        const auto c = host_lagrange(x, g[i]);
+        for (int j = 0; j < n; ++j) { g2l[i * n + j] = a[j]; l2g[i * n + j] = c[j]; }
+    }
+    for (int half = 0; half < 2; ++half) {
+        const double shift = half == 0 ? 1.0 : -1.0;
+        std::vector<double> op(n * n), tmp(n * n, 0.0);
+        for (int j = 0; j < n; ++j) {
+            const auto lg = host_lagrange(g, 0.5 * (g[j] + shift));
+            for (int i = 0; i < n; ++i) op[i * n + j] = 0.5 * lg[i] * wg[j] / wg[i];
+        }
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j)
+                for (int k = 0; k < n; ++k) tmp[i * n + j] += op[i * n + k] * l2g[k * n + j];
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                double acc = 0.0;
+                for (int k = 0; k < n; ++k) acc += g2l[i * n + k] * tmp[k * n + j];
+                out[2 + half][i * n + j] = acc;
+            }
+    }
+}
+
 }  // namespace tlw

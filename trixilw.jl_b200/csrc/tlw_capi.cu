@@ -14,6 +14,7 @@
 #include "tlw_basis.h"
 #include "tlw_curved.cuh"
 #include "tlw_handle.h"
+#include "tlw_mortar.cuh"
 #include "tlw_surface.cuh"
 #include "tlw_volume.cuh"
 
@@ -56,6 +57,8 @@ void free_mesh(tlw_handle* h) {
     dfree(h->d_alpha); dfree(h->d_alpha_raw); dfree(h->d_tFn); dfree(h->d_il); dfree(h->d_ir);
     free_adjoint(h->adj);
     dfree(h->d_Ja); dfree(h->d_ijn); dfree(h->d_cp); dfree(h->d_cs); dfree(h->d_cf);
+    dfree(h->d_ml); dfree(h->d_mu); dfree(h->d_mg); dfree(h->d_ms);
+    h->nmx = h->nmy = 0;
     h->color_off.clear();
     h->curved = false;
     h->have_mesh = false;
@@ -113,6 +116,11 @@ struct Launch {
         if (threads == 0) return;
         interface_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
     }
+    static void mortars(cudaStream_t s, const MortarArgs& a) {
+        if (a.count == 0) return;
+        using M = MortarCfg<N>;
+        mortar_kernel<N><<<(a.count + M::PER_CTA - 1) / M::PER_CTA, M::THREADS, 0, s>>>(a);
+    }
     static void curved_interfaces(cudaStream_t s, const CurvedSurfArgs& a) {
         const long long threads = (long long)a.count * (N + 1);
         if (threads == 0) return;
@@ -158,6 +166,7 @@ template <int N> struct Vol {
 };
 template <int N> struct Ifc { static void run(cudaStream_t s, const SurfArgs& a) { Launch<N>::interfaces(s, a); } };
 template <int N> struct Bnd { static void run(cudaStream_t s, const BndArgs& a) { Launch<N>::boundaries(s, a); } };
+template <int N> struct Mrt { static void run(cudaStream_t s, const MortarArgs& a) { Launch<N>::mortars(s, a); } };
 template <int N> struct CIfc { static void run(cudaStream_t s, const CurvedSurfArgs& a) { Launch<N>::curved_interfaces(s, a); } };
 template <int N> struct CSpd {
     static void run(cudaStream_t s, const double* u, const double* Ja, const double* ij, int E, double g, StepState* st) {
@@ -301,15 +310,40 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
 
     // x interfaces, x boundaries, y interfaces, y boundaries: corner nodes are shared only between
     // launches of different orientation, which the stream orders.
+    MortarArgs ma{};
+    ma.u = u_jump;
+    ma.out = out;
+    ma.tU = h->d_tU;
+    ma.tF = h->d_tF;
+    ma.inv_jac = h->d_inv_jac;
+    ma.dt = dt_ptr;
+    ma.step_mode = mode == MODE_STEP;
+    ma.gamma = h->opts.gamma;
+    ma.flux_kind = h->opts.surface_flux;
+    ma.speed_kind = h->opts.max_speed;
+    ma.inv_w_first = h->h_basis.inv_w_first;
+    ma.inv_w_last = h->h_basis.inv_w_last;
+    ma.status = &h->d_step->status;
     sa.left = h->d_xl; sa.right = h->d_xr; sa.count = h->nx; sa.orientation = 1;
     dispatch<Ifc>(h->N, h->stream, sa);
     ba.bidx = h->d_bx; ba.count = h->nbx; ba.orientation = 1;
     dispatch<Bnd>(h->N, h->stream, ba);
+    if (h->nmx) {
+        ma.lower = h->d_ml; ma.upper = h->d_mu; ma.large = h->d_mg; ma.large_side = h->d_ms;
+        ma.count = h->nmx; ma.orientation = 1;
+        dispatch<Mrt>(h->N, h->stream, ma);
+    }
     if (ev) cudaEventRecord(ev->after_x, h->stream);
     sa.left = h->d_yl; sa.right = h->d_yr; sa.count = h->ny; sa.orientation = 2;
     dispatch<Ifc>(h->N, h->stream, sa);
     ba.bidx = h->d_by; ba.count = h->nby; ba.orientation = 2;
     dispatch<Bnd>(h->N, h->stream, ba);
+    if (h->nmy) {
+        ma.lower = h->d_ml + h->nmx; ma.upper = h->d_mu + h->nmx; ma.large = h->d_mg + h->nmx;
+        ma.large_side = h->d_ms + h->nmx;
+        ma.count = h->nmy; ma.orientation = 2;
+        dispatch<Mrt>(h->N, h->stream, ma);
+    }
     if (ev) cudaEventRecord(ev->after_y, h->stream);
 }
 
@@ -412,7 +446,10 @@ int tlw_create(const tlw_opts* opts, tlw_handle** out) {
         tlw::Basis all[8];
         std::memset(&all[0], 0, sizeof(all[0]));
         for (int N = 1; N <= 7; ++N) host_build_basis(N, all[N]);
-        if (upload_const_basis(all) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "constant basis"); break; }
+        if (upload_const_basis(all) != cudaSuccess || upload_const_mortar() != cudaSuccess) {
+            rc = fail(h, TLW_E_CUDA, "constant basis");
+            break;
+        }
         dispatch<SetAttr>(h->N);
         if (cudaGetLastError() != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "kernel attributes"); break; }
     } while (0);
@@ -605,6 +642,46 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
     h->curved = true;
     h->cur = 0;
     h->have_mesh = true;
+    return TLW_OK;
+}
+
+int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar_neighbor_ids,
+                         const int64_t* mortar_large_sides, const int64_t* mortar_orientations) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh || h->curved) return fail(h, TLW_E_STATE, "mortars follow tlw_set_tree_mesh");
+    if (h->sc && n_mortars > 0) return fail(h, TLW_E_UNSUPPORTED, "mortars with shock capturing are not built");
+    if (n_mortars < 0 || (n_mortars > 0 && (!mortar_neighbor_ids || !mortar_large_sides || !mortar_orientations)))
+        return fail(h, TLW_E_ARG, "mortars");
+    std::vector<int> ml[2], mu[2], mg[2], ms[2];
+    for (int64_t k = 0; k < n_mortars; ++k) {
+        const int64_t lo = mortar_neighbor_ids[3 * k] - 1, up = mortar_neighbor_ids[3 * k + 1] - 1;
+        const int64_t lg = mortar_neighbor_ids[3 * k + 2] - 1;
+        const int64_t side = mortar_large_sides[k], o = mortar_orientations[k];
+        if (lo < 0 || lo >= h->E || up < 0 || up >= h->E || lg < 0 || lg >= h->E || (side != 1 && side != 2) ||
+            (o != 1 && o != 2) || lo == up || lo == lg || up == lg)
+            return fail(h, TLW_E_ARG, "mortar " + std::to_string(k + 1) + " out of range");
+        const int d = (int)o - 1;
+        ml[d].push_back((int)lo); mu[d].push_back((int)up); mg[d].push_back((int)lg); ms[d].push_back((int)side);
+    }
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    dfree(h->d_ml); dfree(h->d_mu); dfree(h->d_mg); dfree(h->d_ms);
+    h->nmx = (int)ml[0].size();
+    h->nmy = (int)ml[1].size();
+    if (n_mortars > 0) {
+        auto up_cat = [&](int*& d, const std::vector<int>& a, const std::vector<int>& b) -> int {
+            std::vector<int> v(a);
+            v.insert(v.end(), b.begin(), b.end());
+            TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
+            TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+            return TLW_OK;
+        };
+        int rc;
+        if ((rc = up_cat(h->d_ml, ml[0], ml[1])) || (rc = up_cat(h->d_mu, mu[0], mu[1])) ||
+            (rc = up_cat(h->d_mg, mg[0], mg[1])) || (rc = up_cat(h->d_ms, ms[0], ms[1])))
+            return rc;
+    }
     return TLW_OK;
 }
 

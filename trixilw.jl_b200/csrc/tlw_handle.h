@@ -85,6 +85,9 @@ struct tlw_handle {
     int *d_il = nullptr, *d_ir = nullptr;   // all interfaces (smoothing)
     int ni = 0;
     double jac_first = 0.0;                 // inverse Jacobian of element 1 (TreeMesh interface cache)
+    // L2 mortars of a non-conforming TreeMesh: x-mortars [0, nmx), then y-mortars [nmx, nmx + nmy)
+    int *d_ml = nullptr, *d_mu = nullptr, *d_mg = nullptr, *d_ms = nullptr;
+    int nmx = 0, nmy = 0;
     // conforming curvilinear mesh (instead of the TreeMesh arrays above; d_state etc. shared)
     bool curved = false;
     double* d_Ja = nullptr;                 // contravariant vectors [4, i, j, e]

@@ -8,7 +8,7 @@ from .curved_mesh import CurvedMesh, StructuredMesh, rotate_elements, rotate_sta
 from .equations import (CompressibleEulerEquations2D, ConstantState, DensityWave, FourQuadrantRiemann,
                         IsentropicVortex)
 from .lwfr import LWIntegrator, LWSolution, l2_linf_errors, solve_lwfr
-from .mesh import TreeMesh
+from .mesh import RefinedTreeMesh, TreeMesh
 from .semidiscretization import (LW, MDRK, DGSEM, Adaptive, BoundaryConditionDirichlet, CFLBased, FluxHLL,
                                  FluxLaxFriedrichs, IndicatorHennemannGassner, SemidiscretizationHyperbolic,
                                  VolumeIntegralFR, VolumeIntegralFRShockCapturing,
@@ -25,5 +25,5 @@ __all__ = [
     "flux_hll", "flux_lax_friedrichs", "get_time_discretization", "lw_fourier_cfl", "rhs", "rhs_mdrk1",
     "rhs_mdrk2", "semidiscretize", "trixi2lw", "LWBatch", "solve_lwfr_batch",
     "adjoint_solve", "adjoint_step", "adjoint_sweep", "forward_record", "lw_solve", "solve_dts",
-    "CurvedMesh", "StructuredMesh", "rotate_elements", "rotate_state",
+    "CurvedMesh", "StructuredMesh", "rotate_elements", "rotate_state", "RefinedTreeMesh",
 ]

@@ -138,3 +138,96 @@ class TreeMesh:
 
     def ndofs(self, polydeg: int) -> int:
         return self.n_elements * (polydeg + 1) ** 2
+
+
+class RefinedTreeMesh:
+    """A non-conforming TreeMesh{2}: the uniform mesh of ``initial_refinement_level`` with the cells whose
+    centres lie in ``refine_box`` ((xmin, ymin), (xmax, ymax)) refined once more, as an AMR step leaves it.
+    Same-size neighbours share an interface; a coarse cell next to refined ones shares an L2 mortar with the
+    two small cells (Trixi mortars container: neighbor_ids [lower, upper, large] per mortar, 1-based;
+    large_sides 1 when the large element is on the -side, 2 on the +side; orientations 1 = x, 2 = y; for an
+    x-mortar the lower small cell has the smaller y, for a y-mortar the smaller x). Periodic.
+
+    Elements: the coarse leaves in Morton order, then the fine leaves (four children per refined cell in the
+    order (-x,-y), (+x,-y), (-x,+y), (+x,+y))."""
+
+    n_boundaries = 0
+
+    def __init__(self, coordinates_min, coordinates_max, initial_refinement_level: int, refine_box):
+        base = TreeMesh(coordinates_min, coordinates_max, initial_refinement_level, periodicity=True)
+        self.length = base.length
+        self.center = base.center
+        m = base.cells_per_dimension
+        lo = self.center - 0.5 * self.length
+        h = base.element_length
+        (bx0, by0), (bx1, by1) = refine_box
+        cx = lo[0] + (base.ix + 0.5) * h
+        cy = lo[1] + (base.iy + 0.5) * h
+        refined = (cx >= bx0) & (cx <= bx1) & (cy >= by0) & (cy <= by1)
+        if not refined.any() or refined.all():
+            raise ValueError("the refine box must select some but not all cells")
+        leaves = {}   # (level 0 coarse / 1 fine, ix, iy) -> element
+        centers, lengths = [], []
+        for k in range(base.n_elements):
+            if not refined[k]:
+                leaves[(0, int(base.ix[k]), int(base.iy[k]))] = len(centers)
+                centers.append((cx[k], cy[k]))
+                lengths.append(h)
+        for k in range(base.n_elements):
+            if refined[k]:
+                for dy in (0, 1):
+                    for dx in (0, 1):
+                        fx, fy = 2 * int(base.ix[k]) + dx, 2 * int(base.iy[k]) + dy
+                        leaves[(1, fx, fy)] = len(centers)
+                        centers.append((lo[0] + (fx + 0.5) * h / 2, lo[1] + (fy + 0.5) * h / 2))
+                        lengths.append(h / 2)
+        self.n_elements = len(centers)
+        self.element_centers = np.array(centers)
+        self.element_lengths = np.array(lengths)
+        self.inverse_jacobian = 2.0 / self.element_lengths
+        il, ir, io, ml, mu, mg, ms, mo = [], [], [], [], [], [], [], []
+        for (lev, ix, iy), e in leaves.items():
+            mm = m << lev
+            for o, (dx, dy) in ((1, (1, 0)), (2, (0, 1))):
+                nb = leaves.get((lev, (ix + dx) % mm, (iy + dy) % mm))
+                if nb is not None:
+                    il.append(e); ir.append(nb); io.append(o)
+            if lev == 0:
+                # mortars: a refined same-level neighbour on either side in either direction
+                for o, sgn in ((1, 1), (1, -1), (2, 1), (2, -1)):
+                    nx, ny = (ix + sgn) % m if o == 1 else ix, (iy + sgn) % m if o == 2 else iy
+                    if (0, nx, ny) in leaves:
+                        continue
+                    # the two children of (nx, ny) next to the shared face
+                    if o == 1:
+                        c = 2 * nx + (0 if sgn == 1 else 1)
+                        lower, upper = leaves[(1, c, 2 * ny)], leaves[(1, c, 2 * ny + 1)]
+                    else:
+                        c = 2 * ny + (0 if sgn == 1 else 1)
+                        lower, upper = leaves[(1, 2 * nx, c)], leaves[(1, 2 * nx + 1, c)]
+                    ml.append(lower); mu.append(upper); mg.append(e); ms.append(1 if sgn == 1 else 2); mo.append(o)
+        self.interface_neighbor_ids = (np.array([il, ir], dtype=np.int64) + 1).T.reshape(-1)
+        self.interface_orientations = np.array(io, dtype=np.int64)
+        self.n_interfaces = len(io)
+        self.mortar_neighbor_ids = (np.array([ml, mu, mg], dtype=np.int64) + 1).T.reshape(-1)
+        self.mortar_large_sides = np.array(ms, dtype=np.int64)
+        self.mortar_orientations = np.array(mo, dtype=np.int64)
+        self.n_mortars = len(mo)
+        empty = np.zeros(0, dtype=np.int64)
+        self.boundary_neighbor_ids = self.boundary_orientations = self.boundary_neighbor_sides = empty
+        self.boundary_directions = empty
+        self.n_boundaries_per_direction = np.zeros(4, dtype=np.int64)
+
+    def node_coordinates(self, polydeg: int) -> np.ndarray:
+        nodes, _ = gauss_lobatto(polydeg)
+        hl = 0.5 * self.element_lengths
+        x = self.element_centers[:, 0][None, None, :] + hl[None, None, :] * nodes[:, None, None]
+        y = self.element_centers[:, 1][None, None, :] + hl[None, None, :] * nodes[None, :, None]
+        n = len(nodes)
+        out = np.empty((2, n, n, self.n_elements))
+        out[0] = np.broadcast_to(x, (n, n, self.n_elements))
+        out[1] = np.broadcast_to(y, (n, n, self.n_elements))
+        return out
+
+    def ndofs(self, polydeg: int) -> int:
+        return self.n_elements * (polydeg + 1) ** 2

@@ -26,7 +26,7 @@ from . import _lib
 from ._lib import DomainError, check, lib
 from .basis import gauss_lobatto
 from .equations import CompressibleEulerEquations2D
-from .mesh import TreeMesh
+from .mesh import RefinedTreeMesh, TreeMesh
 
 
 class LW:
@@ -195,7 +195,7 @@ class SemidiscretizationHyperbolic:
             self.curved = mesh.curved(solver.polydeg)
         elif isinstance(mesh, CurvedMesh):
             self.curved = mesh
-        elif isinstance(mesh, TreeMesh):
+        elif isinstance(mesh, (TreeMesh, RefinedTreeMesh)):
             self.curved = None
         else:
             raise NotImplementedError("TreeMesh{2}, StructuredMesh{2} and conforming curvilinear meshes are built")
@@ -269,6 +269,12 @@ class SemidiscretizationHyperbolic:
                                      m.n_interfaces, _i64p(nid), _i64p(nor), m.n_boundaries, _i64p(bid), _i64p(bor),
                                      _i64p(bsi), _i64p(bpd))
         check(self.handle, rc)
+        if getattr(m, "n_mortars", 0):
+            mids = np.ascontiguousarray(m.mortar_neighbor_ids, dtype=np.int64)
+            msd = np.ascontiguousarray(m.mortar_large_sides, dtype=np.int64)
+            mor = np.ascontiguousarray(m.mortar_orientations, dtype=np.int64)
+            self._mkeep = (mids, msd, mor)
+            check(self.handle, lib().tlw_set_tree_mortars(self.handle, m.n_mortars, _i64p(mids), _i64p(msd), _i64p(mor)))
 
     # ---- array helpers -----------------------------------------------------------------------------
     def ndofs(self) -> int:
