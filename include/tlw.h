@@ -97,6 +97,13 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
                       const int64_t* boundary_orientations, const int64_t* boundary_neighbor_sides,
                       const int64_t* n_boundaries_per_direction);
 
+/* Compressible Navier-Stokes (SemidiscretizationHyperbolicParabolic with CompressibleNavierStokesDiffusion2D,
+ * conservative gradient variables, BR1) on the handle's periodic conforming TreeMesh, set after
+ * tlw_set_tree_mesh (which clears it): LW with the FR volume integral, N >= 3. mu = dynamic viscosity,
+ * prandtl = Prandtl number; the handle's gamma. Replaces rhs! of src/solvers/dgsem_tree/dg_2d_parabolic.jl:15-99
+ * (kernels :725-1860, interface flux :1911-1949) and compute_dt (src/solvers/lwfr.jl:192-210). */
+int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl);
+
 /* L2 mortars of a non-conforming TreeMesh{2} (after AMR), set after tlw_set_tree_mesh (which clears them):
  *   mortar_neighbor_ids [3, n_mortars]  (lower small, upper small, large element), 1-based  Trixi mortars.neighbor_ids
  *   mortar_large_sides  [n_mortars]     1: large element on the -side, 2: on the +side   Trixi mortars.large_sides

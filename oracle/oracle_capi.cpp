@@ -7,6 +7,7 @@
 
 #include "tlw_adjoint.hpp"
 #include "tlw_curved.hpp"
+#include "tlw_parabolic.hpp"
 #include "tlw_oracle.hpp"
 
 using namespace tlwo;
@@ -22,6 +23,8 @@ struct oracle_handle {
     std::vector<double> bnd_levels, bnd_now;
     bool curved = false;         // conforming curvilinear mesh (cmesh) instead of the TreeMesh
     CurvedMesh cmesh;
+    bool parabolic = false;      // compressible Navier-Stokes (TreeMesh, periodic, LW)
+    NavierStokes ns;
     char err[256] = {0};
 };
 
@@ -30,12 +33,23 @@ namespace {
 // LW / MDRK rhs on whichever mesh the handle holds (curvilinear: LW, FR volume integral only)
 void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, double t, double dt,
              const BoundaryData* bd, int kind, int nthreads) {
+    if (h->parabolic) {
+        if (kind != 0) throw std::runtime_error("parabolic oracle: LW only");
+        rhs_parabolic(h->basis, h->eq, h->ns, h->opt, h->mesh, u, du, dt, h->ws, nthreads);
+        return;
+    }
     if (!h->curved) {
         rhs(h->basis, h->eq, h->opt, h->mesh, u, u2, du, t, dt, bd, kind, h->ws, nthreads);
         return;
     }
     if (kind != 0 || h->opt.shock_capturing) throw std::runtime_error("curvilinear oracle: LW, FR volume integral only");
     rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads);
+}
+
+double any_max_dt(oracle_handle* h, const double* u, double cfl, bool& bad, int nthreads) {
+    if (h->parabolic) return max_dt_parabolic(h->basis, h->eq, h->ns, h->mesh, u, cfl, bad, nthreads);
+    if (h->curved) return max_dt_curved(h->basis, h->eq, h->cmesh, u, cfl, bad, nthreads);
+    return max_dt(h->basis, h->eq, h->mesh, u, cfl, bad, nthreads);
 }
 
 }  // namespace
@@ -136,6 +150,16 @@ int oracle_mortar_operators(int N, double* out) {
     } catch (...) { return 1; }
 }
 
+// compressible Navier-Stokes: dynamic viscosity mu and Prandtl number (the handle's gamma)
+int oracle_set_parabolic(oracle_handle* h, double mu, double Pr) {
+    if (h->curved || h->mesh.n_boundaries > 0) return 1;
+    h->parabolic = true;
+    h->ns.gamma = h->eq.gamma;
+    h->ns.mu = mu;
+    h->ns.Pr = Pr;
+    return 0;
+}
+
 void oracle_destroy(oracle_handle* h) { delete h; }
 
 // VolumeIntegralFRShockCapturing with IndicatorHennemannGassner(alpha_max, alpha_min, alpha_smooth;
@@ -212,8 +236,7 @@ int oracle_get(oracle_handle* h, int which, double* out) {
 
 double oracle_max_dt(oracle_handle* h, const double* u, double cfl) {
     bool bad = false;
-    const double dt = h->curved ? max_dt_curved(h->basis, h->eq, h->cmesh, u, cfl, bad)
-                                : max_dt(h->basis, h->eq, h->mesh, u, cfl, bad);
+    const double dt = any_max_dt(h, u, cfl, bad, 1);
     return bad ? -1.0 : dt;
 }
 
@@ -236,9 +259,7 @@ int oracle_steps(oracle_handle* h, int kind, double* u, int nsteps, double cfl, 
             (t >= t_end || std::fabs(t - t_end) <= 1.4901161193847656e-8 * std::max(std::fabs(t), std::fabs(t_end))))
             break;
         bool bad = false;
-        double dt = fixed_dt > 0 ? fixed_dt
-                    : h->curved ? max_dt_curved(h->basis, h->eq, h->cmesh, u, cfl, bad, nthreads)
-                                : max_dt(h->basis, h->eq, h->mesh, u, cfl, bad, nthreads);
+        double dt = fixed_dt > 0 ? fixed_dt : any_max_dt(h, u, cfl, bad, nthreads);
         if (bad) return -3;
         if (t + dt > t_end) dt = t_end - t;
         BoundaryData bd{h->bnd_levels.empty() ? nullptr : h->bnd_levels.data(),

@@ -48,6 +48,7 @@ def lib():
         L.oracle_steps.argtypes = [P, i32, P, i32, dbl, dbl, P, dbl, i32]
         L.oracle_adjoint_step.argtypes = [P, P, dbl, P, P, i32]
         L.oracle_set_mortars.argtypes = [P, i32, P, P, P, P, P]
+        L.oracle_set_parabolic.argtypes = [P, dbl, dbl]
         L.oracle_mortar_operators.argtypes = [i32, P]
         L.oracle_create_curved.argtypes = [i32, dbl, i32, i32, i32, P, P, i32, P, P, P, P, P]
         L.oracle_create_curved.restype = P
@@ -142,6 +143,10 @@ class Oracle:
 
     def size(self):
         return 4 * self.n * self.n * self.E
+
+    def set_parabolic(self, mu: float, Pr: float = 0.72):
+        """Compressible Navier-Stokes with dynamic viscosity mu and Prandtl number Pr (periodic TreeMesh)."""
+        assert lib().oracle_set_parabolic(self.h, float(mu), float(Pr)) == 0
 
     def set_shock_capturing(self, on=True, alpha_max=0.5, alpha_min=0.001, alpha_smooth=True):
         lib().oracle_set_shock_capturing(self.h, 1 if on else 0, alpha_max, alpha_min, 1 if alpha_smooth else 0)

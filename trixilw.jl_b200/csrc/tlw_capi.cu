@@ -15,6 +15,7 @@
 #include "tlw_curved.cuh"
 #include "tlw_handle.h"
 #include "tlw_mortar.cuh"
+#include "tlw_parabolic.cuh"
 #include "tlw_surface.cuh"
 #include "tlw_volume.cuh"
 
@@ -59,10 +60,21 @@ void free_mesh(tlw_handle* h) {
     dfree(h->d_Ja); dfree(h->d_ijn); dfree(h->d_cp); dfree(h->d_cs); dfree(h->d_cf);
     dfree(h->d_ml); dfree(h->d_mu); dfree(h->d_mg); dfree(h->d_ms);
     h->nmx = h->nmy = 0;
+    dfree(h->d_gx); dfree(h->d_gy); dfree(h->d_tFv); dfree(h->d_visc);
+    h->parabolic = false;
     h->color_off.clear();
     h->curved = false;
     h->have_mesh = false;
     h->have_bdata = false;
+}
+
+NSParams ns_params(const tlw_handle* h) {
+    NSParams p{};
+    p.gamma = h->opts.gamma;
+    p.mu = h->ns_mu;
+    p.Pr = h->ns_Pr;
+    p.kappa = h->opts.gamma / ((h->opts.gamma - 1.0) * h->ns_Pr);
+    return p;
 }
 
 // ---- kernel launch helpers (template dispatch over N) -------------------------------------------
@@ -116,6 +128,49 @@ struct Launch {
         if (threads == 0) return;
         interface_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
     }
+    static void parabolic(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out,
+                          const double* dtp) {
+        if constexpr (N >= 3) {
+            const int E = (int)h->E;
+            using P = ParCfg<N>;
+            const int grid = (E + P::EB - 1) / P::EB;
+            grad_volume_kernel<N><<<grid, P::THREADS, 0, s>>>(u, h->d_inv_jac, E, h->d_gx, h->d_gy);
+            const long long th = (long long)(h->nx + h->ny) * (N + 1);
+            if (th)
+                grad_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(
+                    u, h->d_xl, h->d_xr, h->nx, h->d_yl, h->d_yr, h->ny, h->d_inv_jac, h->h_basis.inv_w_first,
+                    h->h_basis.inv_w_last, h->d_gx, h->d_gy);
+            ParArgs pa{};
+            pa.u = u;
+            pa.gx = h->d_gx;
+            pa.gy = h->d_gy;
+            pa.out = out;
+            pa.tU = h->d_tU;
+            pa.tF = h->d_tF;
+            pa.tFv = h->d_tFv;
+            pa.inv_jac = h->d_inv_jac;
+            pa.dt = dtp;
+            pa.E = E;
+            pa.ns = ns_params(h);
+            if (mode == MODE_RHS) par_volume_kernel<N, MODE_RHS><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
+            else par_volume_kernel<N, MODE_STEP><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
+        }
+    }
+    static void par_speed(cudaStream_t s, const tlw_handle* h, const double* u) {
+        if constexpr (N >= 3) {
+            const int E = (int)h->E;
+            par_speed_kernel<N><<<(E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS, MS_THREADS, 0, s>>>(
+                u, h->d_inv_jac, E, ns_params(h), h->d_step, h->d_visc);
+        }
+    }
+    static void par_attributes() {
+        if constexpr (N >= 3) {
+            cudaFuncSetAttribute(par_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ParCfg<N>::smem_bytes());
+            cudaFuncSetAttribute(par_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ParCfg<N>::smem_bytes());
+        }
+    }
     static void mortars(cudaStream_t s, const MortarArgs& a) {
         if (a.count == 0) return;
         using M = MortarCfg<N>;
@@ -166,6 +221,13 @@ template <int N> struct Vol {
 };
 template <int N> struct Ifc { static void run(cudaStream_t s, const SurfArgs& a) { Launch<N>::interfaces(s, a); } };
 template <int N> struct Bnd { static void run(cudaStream_t s, const BndArgs& a) { Launch<N>::boundaries(s, a); } };
+template <int N> struct Par {
+    static void run(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out, const double* dtp) {
+        Launch<N>::parabolic(s, h, mode, u, out, dtp);
+    }
+};
+template <int N> struct ParSpd { static void run(cudaStream_t s, const tlw_handle* h, const double* u) { Launch<N>::par_speed(s, h, u); } };
+template <int N> struct ParAttr { static void run() { Launch<N>::par_attributes(); } };
 template <int N> struct Mrt { static void run(cudaStream_t s, const MortarArgs& a) { Launch<N>::mortars(s, a); } };
 template <int N> struct CIfc { static void run(cudaStream_t s, const CurvedSurfArgs& a) { Launch<N>::curved_interfaces(s, a); } };
 template <int N> struct CSpd {
@@ -212,6 +274,33 @@ void enqueue_indicator(tlw_handle* h, const double* u, bool speed) {
 void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const double* u_jump, const double* u_base,
                  double* out, const double* dt_ptr, const PhaseEvents* ev = nullptr, bool alpha_ready = false) {
     if (h->sc && !alpha_ready) enqueue_indicator(h, u_jump, false);   // indicator of the instantaneous u
+    if (h->parabolic) {
+        // BR1 gradients, parabolic LW volume kernel, then the interfaces with the viscous traces
+        dispatch<Par>(h->N, h->stream, (const tlw_handle*)h, mode, u_flux, out, dt_ptr);
+        if (ev) cudaEventRecord(ev->after_volume, h->stream);
+        SurfArgs sp{};
+        sp.u = u_jump;
+        sp.out = out;
+        sp.tU = h->d_tU;
+        sp.tF = h->d_tF;
+        sp.tFv = h->d_tFv;
+        sp.inv_jac = h->d_inv_jac;
+        sp.dt = dt_ptr;
+        sp.step_mode = mode == MODE_STEP;
+        sp.gamma = h->opts.gamma;
+        sp.flux_kind = h->opts.surface_flux;
+        sp.speed_kind = h->opts.max_speed;
+        sp.inv_w_first = h->h_basis.inv_w_first;
+        sp.inv_w_last = h->h_basis.inv_w_last;
+        sp.status = &h->d_step->status;
+        sp.left = h->d_xl; sp.right = h->d_xr; sp.count = h->nx; sp.orientation = 1;
+        dispatch<Ifc>(h->N, h->stream, sp);
+        if (ev) cudaEventRecord(ev->after_x, h->stream);
+        sp.left = h->d_yl; sp.right = h->d_yr; sp.count = h->ny; sp.orientation = 2;
+        dispatch<Ifc>(h->N, h->stream, sp);
+        if (ev) cudaEventRecord(ev->after_y, h->stream);
+        return;
+    }
     VolArgs va{};
     va.u = u_flux;
     va.u_base = u_base;
@@ -354,9 +443,11 @@ void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const
     if (h->sc) enqueue_indicator(h, u, true);   // CFL reduction and indicator in one pass over u
     else if (h->curved) dispatch<CSpd>(h->N, h->stream, u, (const double*)h->d_Ja, (const double*)h->d_ijn, (int)h->E,
                                        h->opts.gamma, h->d_step);
+    else if (h->parabolic) dispatch<ParSpd>(h->N, h->stream, (const tlw_handle*)h, u);
     else dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, true,
                        false, indicator_args(h));
-    finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
+    if (h->parabolic) par_finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->d_visc, h->N);
+    else finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
     if (after_dt) cudaEventRecord(after_dt, h->stream);
     const double* dtp = &h->d_step->dt;
     if (h->opts.time_discretization == TLW_LW) {
@@ -685,6 +776,31 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
     return TLW_OK;
 }
 
+int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh || h->curved) return fail(h, TLW_E_STATE, "the parabolic terms follow tlw_set_tree_mesh");
+    if (h->opts.time_discretization != TLW_LW || h->sc || h->N < 3 || h->nb > 0 || h->nmx + h->nmy > 0)
+        return fail(h, TLW_E_UNSUPPORTED, "Navier-Stokes: LW, FR volume integral, N >= 3, periodic conforming TreeMesh");
+    if (!(mu >= 0.0) || !(prandtl > 0.0)) return fail(h, TLW_E_ARG, "mu / Prandtl");
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    int rc;
+    if ((rc = ensure(h, h->d_gx, state_doubles(h))) || (rc = ensure(h, h->d_gy, state_doubles(h))) ||
+        (rc = ensure(h, h->d_tFv, trace_doubles(h))))
+        return rc;
+    if (!h->d_visc) {
+        TLW_CUDA(h, cudaMalloc(&h->d_visc, sizeof(unsigned long long)));
+        TLW_CUDA(h, cudaMemset(h->d_visc, 0, sizeof(unsigned long long)));
+    }
+    dispatch<ParAttr>(h->N);
+    TLW_CUDA(h, cudaGetLastError());
+    h->ns_mu = mu;
+    h->ns_Pr = prandtl;
+    h->parabolic = true;
+    return TLW_OK;
+}
+
 int32_t tlw_curved_colors(tlw_handle* h) {
     return (h && h->curved) ? (int32_t)h->color_off.size() - 1 : 0;
 }
@@ -753,6 +869,27 @@ int tlw_max_dt(tlw_handle* h, const double* u, int32_t where, double cfl, double
     }
     const unsigned long long zero = 0;
     TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->max_bits, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+    if (h->parabolic) {
+        // both maxima, combined on the host exactly as par_finalize_dt_kernel does
+        TLW_CUDA(h, cudaMemcpyAsync(h->d_visc, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+        dispatch<ParSpd>(h->N, h->stream, (const tlw_handle*)h, du_in);
+        TLW_CUDA(h, cudaGetLastError());
+        unsigned long long ba = 0, bv = 0;
+        TLW_CUDA(h, cudaMemcpyAsync(&ba, &h->d_step->max_bits, sizeof(ba), cudaMemcpyDeviceToHost, h->stream));
+        TLW_CUDA(h, cudaMemcpyAsync(&bv, h->d_visc, sizeof(bv), cudaMemcpyDeviceToHost, h->stream));
+        TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->max_bits, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+        TLW_CUDA(h, cudaMemcpyAsync(h->d_visc, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+        if ((rc = read_status(h))) return rc;
+        double la, lv;
+        std::memcpy(&la, &ba, sizeof(la));
+        std::memcpy(&lv, &bv, sizeof(lv));
+        const double tiny = 4.9406564584124654e-324;
+        if (!(la > tiny)) la = tiny;
+        if (!(lv > tiny)) lv = tiny;
+        const double k = 2.0 * (2.0 * h->N + 1.0);
+        *dt_out = std::fmin(cfl * (2.0 / (h->n * la)), cfl / ((la + lv * k) * k));
+        return TLW_OK;
+    }
     if (h->curved)
         dispatch<CSpd>(h->N, h->stream, du_in, (const double*)h->d_Ja, (const double*)h->d_ijn, (int)h->E,
                        h->opts.gamma, h->d_step);

@@ -85,6 +85,11 @@ struct tlw_handle {
     int *d_il = nullptr, *d_ir = nullptr;   // all interfaces (smoothing)
     int ni = 0;
     double jac_first = 0.0;                 // inverse Jacobian of element 1 (TreeMesh interface cache)
+    // compressible Navier-Stokes (TreeMesh, periodic, LW): BR1 gradients, viscous traces, viscous dt bound
+    bool parabolic = false;
+    double ns_mu = 0.0, ns_Pr = 0.72;
+    double *d_gx = nullptr, *d_gy = nullptr, *d_tFv = nullptr;
+    unsigned long long* d_visc = nullptr;
     // L2 mortars of a non-conforming TreeMesh: x-mortars [0, nmx), then y-mortars [nmx, nmx + nmy)
     int *d_ml = nullptr, *d_mu = nullptr, *d_mg = nullptr, *d_ms = nullptr;
     int nmx = 0, nmy = 0;

@@ -43,6 +43,7 @@ struct SurfArgs {
     double jac_first;        // J^{-1} used by the admissibility test (element 1's on TreeMesh)
     double w_first, w_last;  // GLL weights w_1, w_n
     const int* inst;         // batched form: instance of each element (dt indexed by it); null otherwise
+    const double* tFv;      // compressible Navier-Stokes: viscous normal flux traces (null otherwise)
 };
 
 __device__ __forceinline__ bool admissible(double gm1, const double* u) {
@@ -108,6 +109,14 @@ static __global__ void __launch_bounds__(256) interface_kernel(SurfArgs a) {
     lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, FL, FR, UL, UR, uL, uR, a.orientation, Fn, a.status);
     const double dt = a.inst ? a.dt[__ldg(a.inst + le)] : *a.dt;
     if (a.shock_capturing) blend_interface_flux<N>(a, le, re, faceL, faceR, l, uL, uR, dt, Fn);
+    if (a.tFv) {
+        // compressible Navier-Stokes: minus the central viscous flux (Fv_L + Fv_R) / 2
+        double vL[NV], vR[NV];
+        load4(a.tFv + (((size_t)le * 4 + faceL) * n + l) * NV, vL);
+        load4(a.tFv + (((size_t)re * 4 + faceR) * n + l) * NV, vR);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fn[v] -= 0.5 * (vL[v] + vR[v]);
+    }
     const double dts = a.step_mode ? dt : 1.0;
     const double sL = -__ldg(a.inv_jac + le) * a.inv_w_last * dts;
     const double sR = __ldg(a.inv_jac + re) * a.inv_w_first * dts;

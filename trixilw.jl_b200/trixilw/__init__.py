@@ -5,12 +5,13 @@ from ._lib import DomainError, TlwError, lib
 from .adjoint import adjoint_solve, adjoint_step, adjoint_sweep, forward_record, lw_solve, solve_dts
 from .batch import LWBatch, solve_lwfr_batch
 from .curved_mesh import CurvedMesh, StructuredMesh, rotate_elements, rotate_state
-from .equations import (CompressibleEulerEquations2D, ConstantState, DensityWave, FourQuadrantRiemann,
-                        IsentropicVortex)
+from .equations import (CompressibleEulerEquations2D, CompressibleNavierStokesDiffusion2D, ConstantState,
+                        DensityWave, FourQuadrantRiemann, GradientVariablesConservative, IsentropicVortex)
 from .lwfr import LWIntegrator, LWSolution, l2_linf_errors, solve_lwfr
 from .mesh import RefinedTreeMesh, TreeMesh
 from .semidiscretization import (LW, MDRK, DGSEM, Adaptive, BoundaryConditionDirichlet, CFLBased, FluxHLL,
                                  FluxLaxFriedrichs, IndicatorHennemannGassner, SemidiscretizationHyperbolic,
+                                 SemidiscretizationHyperbolicParabolic,
                                  VolumeIntegralFR, VolumeIntegralFRShockCapturing,
                                  boundary_condition_periodic, flux_hll, flux_lax_friedrichs,
                                  get_time_discretization, lw_fourier_cfl, rhs, rhs_mdrk1, rhs_mdrk2,
@@ -26,4 +27,5 @@ __all__ = [
     "rhs_mdrk2", "semidiscretize", "trixi2lw", "LWBatch", "solve_lwfr_batch",
     "adjoint_solve", "adjoint_step", "adjoint_sweep", "forward_record", "lw_solve", "solve_dts",
     "CurvedMesh", "StructuredMesh", "rotate_elements", "rotate_state", "RefinedTreeMesh",
+    "CompressibleNavierStokesDiffusion2D", "GradientVariablesConservative", "SemidiscretizationHyperbolicParabolic",
 ]

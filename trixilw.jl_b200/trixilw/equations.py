@@ -5,6 +5,25 @@ from __future__ import annotations
 import numpy as np
 
 
+class GradientVariablesConservative:
+    """Gradients of the conservative variables (the reference's GradientVariablesConservative,
+    src/equations/compressible_navier_stokes_2d.jl:14)."""
+
+
+class CompressibleNavierStokesDiffusion2D:
+    """Trixi's CompressibleNavierStokesDiffusion2D(equations; mu, Prandtl, gradient_variables): constant dynamic
+    viscosity mu, Prandtl number, T = p / rho, kappa = gamma / ((gamma - 1) Pr). The device path takes the
+    conservative gradient variables, as the reference's Navier-Stokes setups do."""
+
+    def __init__(self, equations, mu: float, Prandtl: float = 0.72, gradient_variables=None):
+        self.equations_hyperbolic = equations
+        self.gamma = equations.gamma
+        self.mu = float(mu)
+        self.Pr = float(Prandtl)
+        if gradient_variables is not None and not isinstance(gradient_variables, GradientVariablesConservative):
+            raise NotImplementedError("the device path takes GradientVariablesConservative")
+
+
 class CompressibleEulerEquations2D:
     """Trixi's CompressibleEulerEquations2D(gamma): variables (rho, rho v1, rho v2, rho e)."""
 

@@ -362,6 +362,23 @@ class LWUpdate:
     p: SemidiscretizationHyperbolic
 
 
+class SemidiscretizationHyperbolicParabolic(SemidiscretizationHyperbolic):
+    """SemidiscretizationHyperbolicParabolic(mesh, (equations, equations_parabolic), initial_condition, solver):
+    compressible Navier-Stokes on a periodic TreeMesh{2} (BR1 gradients of the conservative variables), LW."""
+
+    def __init__(self, mesh, equations, initial_condition, solver, device: int = 0, **kw):
+        eq, eq_par = equations
+        super().__init__(mesh, get_time_discretization(solver), eq, initial_condition, solver, device=device, **kw)
+        self.equations_parabolic = eq_par
+        check(self.handle, lib().tlw_set_parabolic(self.handle, eq_par.mu, eq_par.Pr))
+
+    def _upload_mesh(self):
+        super()._upload_mesh()
+        if hasattr(self, "equations_parabolic"):
+            check(self.handle, lib().tlw_set_parabolic(self.handle, self.equations_parabolic.mu,
+                                                       self.equations_parabolic.Pr))
+
+
 def semidiscretize(semi: SemidiscretizationHyperbolic, time_discretization, tspan) -> LWUpdate:
     u0 = semi.compute_coefficients(tspan[0])
     return LWUpdate(rhs, u0, np.empty_like(u0), (float(tspan[0]), float(tspan[1])), semi)
@@ -371,6 +388,6 @@ __all__ = [
     "LW", "MDRK", "CFLBased", "Adaptive", "VolumeIntegralFR", "VolumeIntegralFRShockCapturing",
     "IndicatorHennemannGassner", "DGSEM", "FluxLaxFriedrichs", "FluxHLL",
     "flux_lax_friedrichs", "flux_hll", "BoundaryConditionDirichlet", "boundary_condition_periodic",
-    "SemidiscretizationHyperbolic", "semidiscretize", "rhs", "rhs_mdrk1", "rhs_mdrk2", "lw_fourier_cfl",
+    "SemidiscretizationHyperbolic", "SemidiscretizationHyperbolicParabolic", "semidiscretize", "rhs", "rhs_mdrk1", "rhs_mdrk2", "lw_fourier_cfl",
     "trixi2lw", "get_time_discretization", "DomainError", "LWUpdate",
 ]
