@@ -816,6 +816,7 @@ int tlw_forward_record(tlw_handle* h, const double* u0, int32_t nsteps, double c
     st.cfl = cfl;
     TLW_ACUDA(h, cudaMemcpyAsync(h->d_step, &st, sizeof(st), cudaMemcpyHostToDevice, h->stream));
     if ((rc = copy_in(h, h->d_state[0], u0, ns, where))) return rc;
+    h->slots_valid = false;   // the handle's state buffers are reused here
     // the whole sweep is one CUDA graph, captured once per (nsteps, checkpoint interval, buffers)
     auto body = [&]() -> int {
         double* s0 = h->d_state[0];

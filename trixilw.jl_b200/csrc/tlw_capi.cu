@@ -62,6 +62,8 @@ void free_mesh(tlw_handle* h) {
     h->nmx = h->nmy = 0;
     dfree(h->d_gx); dfree(h->d_gy); dfree(h->d_tFv); dfree(h->d_visc);
     h->parabolic = false;
+    dfree(h->d_slots);
+    h->slots_valid = false;
     h->color_off.clear();
     h->curved = false;
     h->have_mesh = false;
@@ -271,6 +273,13 @@ void enqueue_indicator(tlw_handle* h, const double* u, bool speed) {
                                                                         h->d_alpha);
 }
 
+// the step's final values all come from the volume and interface kernels: the plain LW step on a periodic
+// conforming TreeMesh (no boundaries, mortars, shock capturing, curvilinear or parabolic terms)
+bool use_slots(const tlw_handle* h) {
+    return h->d_slots && h->opts.time_discretization == TLW_LW && !h->sc && !h->curved && !h->parabolic &&
+           h->nb == 0 && h->nmx + h->nmy == 0;
+}
+
 void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const double* u_jump, const double* u_base,
                  double* out, const double* dt_ptr, const PhaseEvents* ev = nullptr, bool alpha_ready = false) {
     if (h->sc && !alpha_ready) enqueue_indicator(h, u_jump, false);   // indicator of the instantaneous u
@@ -318,6 +327,7 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     va.tFn = h->d_tFn;
     va.status = &h->d_step->status;
     va.speed_kind = h->opts.max_speed;
+    if (mode == MODE_STEP && stage == TLW_STAGE_LW && use_slots(h)) va.cfl_slots = h->d_slots;
     if (h->curved) {
         va.metrics = h->d_Ja;
         va.inv_jac_node = h->d_ijn;
@@ -375,6 +385,7 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     sa.jac_first = h->jac_first;
     sa.w_first = h->h_basis.weights[0];
     sa.w_last = h->h_basis.weights[h->n - 1];
+    sa.cfl_slots = va.cfl_slots;
 
     BndArgs ba{};
     ba.u = u_jump;
@@ -440,7 +451,11 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
 void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const PhaseEvents* ev = nullptr) {
     const double* u = h->d_state[from];
     double* unew = h->d_state[1 - from];
-    if (h->sc) enqueue_indicator(h, u, true);   // CFL reduction and indicator in one pass over u
+    if (use_slots(h) && h->slots_valid) {
+        // the previous step left the per-element maxima of this state
+        const int grid = std::min<int>((int)((h->E + 255) / 256), 4 * 148);
+        cfl_slots_reduce_kernel<<<grid, 256, 0, h->stream>>>(h->d_slots, h->d_inv_jac, (int)h->E, h->d_step);
+    } else if (h->sc) enqueue_indicator(h, u, true);   // CFL reduction and indicator in one pass over u
     else if (h->curved) dispatch<CSpd>(h->N, h->stream, u, (const double*)h->d_Ja, (const double*)h->d_ijn, (int)h->E,
                                        h->opts.gamma, h->d_step);
     else if (h->parabolic) dispatch<ParSpd>(h->N, h->stream, (const tlw_handle*)h, u);
@@ -630,6 +645,8 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
         h->ni = (int)al.size();
     }
     h->nb = n_boundaries; h->nbx = (int)bx.size(); h->nby = (int)by.size();
+    TLW_CUDA(h, cudaMalloc(&h->d_slots, (size_t)n_elements * CFL_SLOTS * sizeof(unsigned long long)));
+    h->slots_valid = false;
     const size_t sd = state_doubles(h), td = trace_doubles(h);
     if ((rc = ensure(h, h->d_state[0], sd)) || (rc = ensure(h, h->d_state[1], sd)) || (rc = ensure(h, h->d_tU, td)) ||
         (rc = ensure(h, h->d_tF, td)))
@@ -910,6 +927,7 @@ int tlw_max_dt(tlw_handle* h, const double* u, int32_t where, double cfl, double
 }
 
 int tlw_set_state(tlw_handle* h, const double* u, int32_t where, double t) {
+    if (h) h->slots_valid = false;
     int rc = check_ready(h);
     if (rc) return rc;
     if (!u) return fail(h, TLW_E_ARG, "null pointer");
@@ -949,6 +967,16 @@ int tlw_step(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double 
     // parameters into the device step state (cfl, fixed_dt, t_end are contiguous after t)
     double params[3] = {t_end, cfl, fixed_dt};
     TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->t_end, params, sizeof(params), cudaMemcpyHostToDevice, h->stream));
+    if (use_slots(h) && !h->slots_valid) {
+        // one step with the full CFL pass; it leaves the per-element slots that later steps reduce
+        enqueue_step(h, h->cur);
+        h->cur ^= 1;
+        h->slots_valid = true;
+        if (--nsteps == 0) {
+            TLW_CUDA(h, cudaGetLastError());
+            return TLW_OK;
+        }
+    }
     if (!use_graph) {
         for (int s = 0; s < nsteps; ++s) {
             enqueue_step(h, h->cur);
@@ -1012,6 +1040,7 @@ int tlw_step_timed(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, d
         cudaEventRecord(e_start, h->stream);
         enqueue_step(h, h->cur, e_dt, pe);
         h->cur ^= 1;
+        if (use_slots(h)) h->slots_valid = true;
     }
     TLW_CUDA(h, cudaGetLastError());
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1120,6 +1149,7 @@ int tlw_get_stream(tlw_handle* h, void** stream) {
 }
 
 int tlw_state_pointer(tlw_handle* h, double** dptr) {
+    if (h) h->slots_valid = false;   // the caller may write the state through the pointer
     if (!h || !dptr) return TLW_E_ARG;
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh");
     *dptr = h->d_state[h->cur];

@@ -85,6 +85,23 @@ __device__ __forceinline__ double checked_sqrt(double x, unsigned* status) {
     return sqrt(x);
 }
 
+// Trixi max_abs_speeds: |v1| + c and |v2| + c of a state, computed the same way by every CFL pass
+__device__ __forceinline__ void node_speeds(double gamma, const double* x, unsigned* status, double& l1, double& l2) {
+    const double ir = 1.0 / x[0];
+    const double v1 = x[1] * ir, v2 = x[2] * ir;
+    const double p = (gamma - 1.0) * (x[3] - 0.5 * (x[1] * v1 + x[2] * v2));
+    const double c = checked_sqrt(gamma * p * ir, status);
+    l1 = fabs(v1) + c;
+    l2 = fabs(v2) + c;
+}
+
+// Per-element CFL slots written by the kernels that produce the final values of a step (plain LW on a
+// periodic conforming TreeMesh): slot s of element e holds the bits of max(|v1| + c) and max(|v2| + c) over
+// the nodes finalised there: 0 interior (volume kernel), 1 / 2 the -x / +x face without corners
+// (x interfaces), 3 / 4 the -y / +y face with corners (y interfaces). The next step reduces them instead of
+// reading the whole state again.
+constexpr int CFL_SLOTS = 10;
+
 // Trixi max_abs_speed_naive (kind 0) / max_abs_speed (kind 1) for CompressibleEulerEquations2D
 __device__ __forceinline__ double max_abs_speed(double gamma, const double* ul, const double* ur, int orientation,
                                                 int kind, unsigned* status) {

@@ -85,6 +85,9 @@ struct tlw_handle {
     int *d_il = nullptr, *d_ir = nullptr;   // all interfaces (smoothing)
     int ni = 0;
     double jac_first = 0.0;                 // inverse Jacobian of element 1 (TreeMesh interface cache)
+    // per-element CFL slots of the state in d_state[cur] (plain LW step on a periodic conforming TreeMesh)
+    unsigned long long* d_slots = nullptr;
+    bool slots_valid = false;
     // compressible Navier-Stokes (TreeMesh, periodic, LW): BR1 gradients, viscous traces, viscous dt bound
     bool parabolic = false;
     double ns_mu = 0.0, ns_Pr = 0.72;

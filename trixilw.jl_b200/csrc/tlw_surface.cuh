@@ -44,6 +44,7 @@ struct SurfArgs {
     double w_first, w_last;  // GLL weights w_1, w_n
     const int* inst;         // batched form: instance of each element (dt indexed by it); null otherwise
     const double* tFv;      // compressible Navier-Stokes: viscous normal flux traces (null otherwise)
+    unsigned long long* cfl_slots;   // plain LW step: per-element CFL slots of the nodes finalised here
 };
 
 __device__ __forceinline__ bool admissible(double gm1, const double* u) {
@@ -122,16 +123,30 @@ static __global__ void __launch_bounds__(256) interface_kernel(SurfArgs a) {
     const double sR = __ldg(a.inv_jac + re) * a.inv_w_first * dts;
     double* oL = a.out + ((size_t)le * n * n + nodeL) * NV;
     double* oR = a.out + ((size_t)re * n * n + nodeR) * NV;
-    double x[NV];
+    // x faces finalise their non-corner nodes, y faces all of theirs (the y launch runs after the x launch)
+    const bool slots = a.cfl_slots && (a.orientation == 2 || (l > 0 && l < n - 1));
+    const int sL_slot = a.orientation == 1 ? 2 : 4, sR_slot = a.orientation == 1 ? 1 : 3;
+    double x[NV], l1, l2;
     load4_rw(oL, x);
 #pragma unroll
     for (int v = 0; v < NV; ++v) x[v] = fma(sL, Fn[v], x[v]);
     store4(oL, x);
+    if (slots) {
+        node_speeds(a.gamma, x, a.status, l1, l2);
+        atomicMax(a.cfl_slots + (size_t)le * CFL_SLOTS + 2 * sL_slot, (unsigned long long)__double_as_longlong(l1));
+        atomicMax(a.cfl_slots + (size_t)le * CFL_SLOTS + 2 * sL_slot + 1, (unsigned long long)__double_as_longlong(l2));
+    }
     load4_rw(oR, x);
 #pragma unroll
     for (int v = 0; v < NV; ++v) x[v] = fma(sR, Fn[v], x[v]);
     store4(oR, x);
+    if (slots) {
+        node_speeds(a.gamma, x, a.status, l1, l2);
+        atomicMax(a.cfl_slots + (size_t)re * CFL_SLOTS + 2 * sR_slot, (unsigned long long)__double_as_longlong(l1));
+        atomicMax(a.cfl_slots + (size_t)re * CFL_SLOTS + 2 * sR_slot + 1, (unsigned long long)__double_as_longlong(l2));
+    }
 }
+
 
 struct BndArgs {
     const double* u;
@@ -263,14 +278,7 @@ static __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const doub
     for (int k = threadIdx.x; k < ne * nn; k += MS_THREADS) {
         double x[NV];
         load4(u + ((size_t)e0 * nn + k) * NV, x);
-        if (SPEED) {
-            const double ir = 1.0 / x[0];
-            const double v1 = x[1] * ir, v2 = x[2] * ir;
-            const double p = gm1 * (x[3] - 0.5 * (x[1] * v1 + x[2] * v2));
-            const double c = checked_sqrt(gamma * p * ir, &s->status);
-            l1s[k] = fabs(v1) + c;
-            l2s[k] = fabs(v2) + c;
-        }
+        if (SPEED) node_speeds(gamma, x, &s->status, l1s[k], l2s[k]);
         // indicator variable density_pressure = (gamma - 1)(rho rho_e - |rho v|^2 / 2)
         if (IND) inds[k] = gm1 * (x[0] * x[3] - 0.5 * (x[1] * x[1] + x[2] * x[2]));
     }
@@ -424,6 +432,33 @@ static __global__ void finalize_dt_kernel(StepState* s, int n) {
     s->t = finished ? t : t + dt;
     if (!finished) s->steps += 1;
     s->max_bits = 0ull;
+}
+
+// the next step's CFL maximum from the per-element slots: max_e J^{-1} (max_s l1 + max_s l2)
+static __global__ void __launch_bounds__(256) cfl_slots_reduce_kernel(const unsigned long long* __restrict__ slots,
+                                                                      const double* __restrict__ inv_jac, int E,
+                                                                      StepState* s) {
+    __shared__ double wmax[8];
+    double m = 0.0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        const unsigned long long* sl = slots + (size_t)e * CFL_SLOTS;
+        unsigned long long b1 = 0ull, b2 = 0ull;
+#pragma unroll
+        for (int k = 0; k < CFL_SLOTS / 2; ++k) {
+            b1 = max(b1, __ldg(sl + 2 * k));
+            b2 = max(b2, __ldg(sl + 2 * k + 1));
+        }
+        m = fmax(m, __ldg(inv_jac + e) * (__longlong_as_double((long long)b1) + __longlong_as_double((long long)b2)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = wmax[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, wmax[w]);
+        if (b > 0.0) atomicMax(&s->max_bits, (unsigned long long)__double_as_longlong(b));
+    }
 }
 
 }  // namespace tlw

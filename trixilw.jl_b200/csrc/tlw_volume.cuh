@@ -27,6 +27,10 @@
 namespace tlw {
 
 // EBX = 0: the default number of elements per CTA; another value selects a tuned variant
+#ifndef TLW_VOLUME_MIN_BLOCKS
+#define TLW_VOLUME_MIN_BLOCKS 5
+#endif
+
 template <int N, int EBX = 0>
 struct VolCfg {
     static constexpr int n = N + 1;
@@ -34,8 +38,9 @@ struct VolCfg {
     // whole elements per CTA, chosen so that the CTA is (nearly) full warps
     static constexpr int EB = EBX ? EBX : N == 1 ? 32 : N == 2 ? 14 : N == 3 ? 8 : N == 4 ? 5 : N == 5 ? 7 : N == 6 ? 5 : 2;
     static constexpr int THREADS = ((EB * nn + 31) / 32) * 32;
-    // resident CTAs per SM the register allocation must allow (<= 128 registers per thread)
-    static constexpr int MIN_BLOCKS = THREADS <= 128 ? 4 : 2;
+    // resident CTAs per SM the register allocation must allow (5 CTAs of 128 threads: <= 96 registers, measured
+    // 4 % faster than 4 CTAs at 128 registers on the N = 4 workload; 6 CTAs spill)
+    static constexpr int MIN_BLOCKS = THREADS <= 128 ? TLW_VOLUME_MIN_BLOCKS : 2;
     static constexpr int MDRK_MIN_BLOCKS = THREADS <= 128 ? 5 : 2;
     // plane layout: node (i, j) of (variable v, element e) at (v*EB + e)*P + i + R*j
     static constexpr int R = n;
@@ -72,6 +77,7 @@ struct VolArgs {
     // inverse Jacobian per node [i, j, e] (inv_jac is then unused)
     const double* metrics;
     const double* inv_jac_node;
+    unsigned long long* cfl_slots;   // plain LW step on a periodic TreeMesh: per-element CFL slots (or null)
 };
 
 // curvilinear: contravariant fluxes f~ = Ja^1_1 f + Ja^1_2 g, g~ = Ja^2_1 f + Ja^2_2 g of a node
@@ -243,9 +249,8 @@ __device__ __forceinline__ void sc_blend(const VolArgs& a, const double* FVX, co
 template <int n, int MODE>
 __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, int j, int node, double ij, double dt,
                                                 const double* acc, const double* U, const double* F,
-                                                const double* G) {
+                                                const double* G, double* o) {
     const size_t off = ((size_t)e * n * n + node) * NV;
-    double o[NV];
     if (MODE == MODE_RHS) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) o[v] = -ij * acc[v];
@@ -302,6 +307,10 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     const bool active = el < EB && e < a.E;
     // dt of this element's instance (batched form) or the single dt
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
+    // per-element maxima of the interior nodes' speeds for the next step's CFL (plain LW step only)
+    constexpr bool SLOTS = MODE == MODE_STEP && !SC && !CURVED;
+    __shared__ unsigned long long emax[SLOTS ? EB : 1][2];
+    if (SLOTS && tid < 2 * EB) emax[tid >> 1][tid & 1] = 0ull;
 
     double U[NV], F[NV], G[NV], up[NV], um[NV], upp[NV], umm[NV];
     double s0 = 0.0, ij = 0.0;   // s0 = -dt J^{-1} (of the element, or of the node on curvilinear meshes)
@@ -528,10 +537,27 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     line_contract<N, C, true>(X, Y, tid);
     __syncthreads();
     if (active) {
-        double acc[NV];
+        double acc[NV], o[NV];
         node_sum<N, C>(X, Y, el, i, j, acc);
         if (SC) sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
-        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
+        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o);
+        if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) {
+            double l1, l2;
+            node_speeds(a.gamma, o, a.status, l1, l2);
+            atomicMax(&emax[el][0], (unsigned long long)__double_as_longlong(l1));
+            atomicMax(&emax[el][1], (unsigned long long)__double_as_longlong(l2));
+        }
+    }
+    if (SLOTS && a.cfl_slots) {
+        __syncthreads();
+        const int ee = blockIdx.x * EB + tid;
+        if (tid < EB && ee < a.E) {
+            unsigned long long* sl = a.cfl_slots + (size_t)ee * CFL_SLOTS;
+            sl[0] = emax[tid][0];
+            sl[1] = emax[tid][1];
+#pragma unroll
+            for (int k = 2; k < CFL_SLOTS; ++k) sl[k] = 0ull;
+        }
     }
 }
 
@@ -621,7 +647,8 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
         double acc[NV];
         node_sum<N, C>(X, Y, el, i, j, acc);
         if (SC) sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
-        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
+        double o[NV];
+        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o);
     }
 }
 
@@ -712,7 +739,8 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
         double acc[NV];
         node_sum<N, C>(X, Y, el, i, j, acc);
         if (SC) sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
-        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G);
+        double o[NV];
+        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o);
     }
 }
 
