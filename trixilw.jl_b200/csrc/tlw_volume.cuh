@@ -309,8 +309,6 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
     // per-element maxima of the interior nodes' speeds for the next step's CFL (plain LW step only)
     constexpr bool SLOTS = MODE == MODE_STEP && !SC && !CURVED;
-    __shared__ unsigned long long emax[SLOTS ? EB : 1][2];
-    if (SLOTS && tid < 2 * EB) emax[tid >> 1][tid & 1] = 0ull;
 
     double U[NV], F[NV], G[NV], up[NV], um[NV], upp[NV], umm[NV];
     double s0 = 0.0, ij = 0.0;   // s0 = -dt J^{-1} (of the element, or of the node on curvilinear meshes)
@@ -536,27 +534,34 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     __syncthreads();
     line_contract<N, C, true>(X, Y, tid);
     __syncthreads();
+    double l1 = 0.0, l2 = 0.0;
     if (active) {
         double acc[NV], o[NV];
         node_sum<N, C>(X, Y, el, i, j, acc);
         if (SC) sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o);
-        if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) {
-            double l1, l2;
-            node_speeds(a.gamma, o, a.status, l1, l2);
-            atomicMax(&emax[el][0], (unsigned long long)__double_as_longlong(l1));
-            atomicMax(&emax[el][1], (unsigned long long)__double_as_longlong(l2));
-        }
+        if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) node_speeds(a.gamma, o, a.status, l1, l2);
     }
     if (SLOTS && a.cfl_slots) {
+        // the interior nodes' speeds through the (now free) X plane, one thread per (element, component)
         __syncthreads();
-        const int ee = blockIdx.x * EB + tid;
-        if (tid < EB && ee < a.E) {
-            unsigned long long* sl = a.cfl_slots + (size_t)ee * CFL_SLOTS;
-            sl[0] = emax[tid][0];
-            sl[1] = emax[tid][1];
+        if (active) {
+            X[el * C::P + i + C::R * j] = l1;
+            X[(EB + el) * C::P + i + C::R * j] = l2;
+        }
+        __syncthreads();
+        const int ee = blockIdx.x * EB + (tid >> 1);
+        if (tid < 2 * EB && ee < a.E) {
+            const double* p = X + ((tid & 1) * EB + (tid >> 1)) * C::P;
+            double m = 0.0;
 #pragma unroll
-            for (int k = 2; k < CFL_SLOTS; ++k) sl[k] = 0ull;
+            for (int jj = 1; jj < n - 1; ++jj)
+#pragma unroll
+                for (int ii = 1; ii < n - 1; ++ii) m = fmax(m, p[ii + C::R * jj]);
+            unsigned long long* sl = a.cfl_slots + (size_t)ee * CFL_SLOTS;
+            sl[tid & 1] = (unsigned long long)__double_as_longlong(m);
+#pragma unroll
+            for (int k = 1; k < CFL_SLOTS / 2; ++k) sl[2 * k + (tid & 1)] = 0ull;
         }
     }
 }
