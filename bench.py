@@ -796,7 +796,7 @@ def run_adjoint(args):
     rng = np.random.default_rng(0)
     worst = 0.0
     h = 1e-4
-    for _ in range(64):
+    for _ in range(args.fd_directions):
         d = rng.standard_normal(u0.size)
         d /= np.linalg.norm(d)
         d1 = (Jf(u0 + h * d) - Jf(u0 - h * d)) / (2 * h)
@@ -816,7 +816,7 @@ def run_adjoint(args):
             "forward_solve_ms": fwd_ms, "gradient_ms": grad_ms, "gradient_cost_vs_forward": grad_ms / fwd_ms,
             "phase_ms": {"forward_record": phases[0], "recompute": phases[1], "adjoint_steps": phases[2]},
             "backward_cost_vs_forward": (phases[1] + phases[2]) / fwd_ms,
-            "J": Jh, "fd_check": {"directions": 64, "h": h, "max_rel_err": worst, "richardson": True},
+            "J": Jh, "fd_check": {"directions": args.fd_directions, "h": h, "max_rel_err": worst, "richardson": True},
             "e2e": {"value": ndofs * nsteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * 5 * ndofs / nsteps,
                     "d2h_bytes_per_step": 8 * 8 * ndofs / nsteps, "seconds": e2e_s},
             "clocks": clocks,
@@ -833,6 +833,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="vortex_tree512_N4_lw", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + sorted(ADJOINT_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fd-directions", type=int, default=64,
+                    help="adjoint workload: random directions of the finite-difference gradient check")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
