@@ -94,11 +94,11 @@ int bfail(tlw_batch* b, int code, const std::string& msg) {
             return bfail(b, TLW_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
     } while (0)
 
-// alternative elements-per-CTA choices the autotuner compares with the defaults (N = 3: 8, 4: 5, 5: 7)
+// alternative elements-per-CTA choices the autotuner compares with the defaults (N = 3: 8, 4: 5, 5: 3)
 template <int N> struct AltEB;
 template <> struct AltEB<3> { static constexpr int v = 16; };
 template <> struct AltEB<4> { static constexpr int v = 10; };
-template <> struct AltEB<5> { static constexpr int v = 3; };
+template <> struct AltEB<5> { static constexpr int v = 7; };
 
 template <int N>
 struct BLaunch {

@@ -27,6 +27,11 @@
 namespace tlw {
 
 // EBX = 0: the default number of elements per CTA; another value selects a tuned variant
+// elements per CTA at N = 5: 3 (108 of 128 threads busy, 5 CTAs per SM) measured 4 % faster than 7 (252 of
+// 256 threads, 2 CTAs per SM) and 10 % faster than 10 on the 512^2 step
+#ifndef TLW_EB_N5
+#define TLW_EB_N5 3
+#endif
 #ifndef TLW_VOLUME_MIN_BLOCKS
 #define TLW_VOLUME_MIN_BLOCKS 5
 #endif
@@ -36,7 +41,7 @@ struct VolCfg {
     static constexpr int n = N + 1;
     static constexpr int nn = n * n;
     // whole elements per CTA, chosen so that the CTA is (nearly) full warps
-    static constexpr int EB = EBX ? EBX : N == 1 ? 32 : N == 2 ? 14 : N == 3 ? 8 : N == 4 ? 5 : N == 5 ? 7 : N == 6 ? 5 : 2;
+    static constexpr int EB = EBX ? EBX : N == 1 ? 32 : N == 2 ? 14 : N == 3 ? 8 : N == 4 ? 5 : N == 5 ? TLW_EB_N5 : N == 6 ? 5 : 2;
     static constexpr int THREADS = ((EB * nn + 31) / 32) * 32;
     // resident CTAs per SM the register allocation must allow (5 CTAs of 128 threads: <= 96 registers, measured
     // 4 % faster than 4 CTAs at 128 registers on the N = 4 workload; 6 CTAs spill)
