@@ -144,6 +144,10 @@ class Oracle:
     def size(self):
         return 4 * self.n * self.n * self.E
 
+    def set_temporal_errors(self, on=True, abstol: float = 1e-6, reltol: float = 1e-6):
+        """Compute lw_volume_kernel_4!'s temporal error estimate (get(4) after rhs)."""
+        lib().oracle_set_temporal_errors(self.h, 1 if on else 0, float(abstol), float(reltol))
+
     def set_parabolic(self, mu: float, Pr: float = 0.72):
         """Compressible Navier-Stokes with dynamic viscosity mu and Prandtl number Pr (periodic TreeMesh)."""
         assert lib().oracle_set_parabolic(self.h, float(mu), float(Pr)) == 0

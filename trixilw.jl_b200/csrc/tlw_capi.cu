@@ -64,6 +64,8 @@ void free_mesh(tlw_handle* h) {
     h->parabolic = false;
     dfree(h->d_slots);
     h->slots_valid = false;
+    dfree(h->d_te); dfree(h->d_check);
+    if (h->d_bad) { cudaFree(h->d_bad); h->d_bad = nullptr; }
     h->color_off.clear();
     h->curved = false;
     h->have_mesh = false;
@@ -98,6 +100,9 @@ struct Launch {
         set_attr_sc<true>();
         const int lw = (int)C::smem_bytes(4);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        if constexpr (N >= 4)
+            cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
     }
     template <bool SC>
@@ -117,6 +122,10 @@ struct Launch {
     static void volume(cudaStream_t s, int stage, int mode, bool sc, const VolArgs& a) {
         const int grid = (int)((a.E + C::EB - 1) / C::EB);
         if (grid == 0) return;
+        if (a.temporal_errors) {   // Adaptive trial step: the depth-4 kernel with the error estimate
+            if constexpr (N >= 4) lw_volume_kernel<N, MODE_STEP, false, 0, false, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
+            return;
+        }
         if (a.metrics) {   // curvilinear mesh (LW, FR volume integral)
             if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, false, 0, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
             else lw_volume_kernel<N, MODE_STEP, false, 0, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
@@ -327,7 +336,12 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     va.tFn = h->d_tFn;
     va.status = &h->d_step->status;
     va.speed_kind = h->opts.max_speed;
-    if (mode == MODE_STEP && stage == TLW_STAGE_LW && use_slots(h)) va.cfl_slots = h->d_slots;
+    if (mode == MODE_STEP && stage == TLW_STAGE_LW && use_slots(h) && !h->te_request) va.cfl_slots = h->d_slots;
+    if (h->te_request) {
+        va.temporal_errors = h->d_te;
+        va.abstol = h->te_abstol;
+        va.reltol = h->te_reltol;
+    }
     if (h->curved) {
         va.metrics = h->d_Ja;
         va.inv_jac_node = h->d_ijn;
@@ -815,6 +829,59 @@ int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl) {
     h->ns_mu = mu;
     h->ns_Pr = prandtl;
     h->parabolic = true;
+    return TLW_OK;
+}
+
+int tlw_adaptive_trial(tlw_handle* h, double dt, double abstol, double reltol, double* total_temporal_error,
+                       int32_t* admissible) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!total_temporal_error || !admissible || !(dt > 0.0)) return fail(h, TLW_E_ARG, "arguments");
+    if (h->opts.time_discretization != TLW_LW || h->sc || h->curved || h->parabolic || h->N < 4)
+        return fail(h, TLW_E_UNSUPPORTED, "Adaptive: LW on a TreeMesh with N >= 4 (the depth-4 kernel's estimate)");
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    const int blocks = (int)std::min<int64_t>(((int64_t)h->nn * h->E + 255) / 256, 4 * 148);
+    if (!h->d_te) {
+        TLW_CUDA(h, cudaMalloc(&h->d_te, (size_t)h->E * sizeof(double)));
+        TLW_CUDA(h, cudaMalloc(&h->d_check, (size_t)(4 * 148 + 1) * sizeof(double)));
+        TLW_CUDA(h, cudaMalloc(&h->d_bad, sizeof(unsigned)));
+    }
+    TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->dt_call, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    TLW_CUDA(h, cudaMemsetAsync(h->d_bad, 0, sizeof(unsigned), h->stream));
+    const double* u = h->d_state[h->cur];
+    double* trial = h->d_state[1 - h->cur];
+    h->te_request = true;
+    h->te_abstol = abstol;
+    h->te_reltol = reltol;
+    enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, trial, &h->d_step->dt_call);
+    h->te_request = false;
+    adaptive_check_kernel<<<blocks, 256, 0, h->stream>>>(h->d_te, (int)h->E, trial, (long long)h->nn * h->E,
+                                                          h->opts.gamma, h->d_check, h->d_bad);
+    adaptive_sum_kernel<<<1, 32, 0, h->stream>>>(h->d_check, blocks, h->d_check + 4 * 148);
+    TLW_CUDA(h, cudaGetLastError());
+    double sum = 0.0;
+    unsigned bad = 0, st = 0;
+    TLW_CUDA(h, cudaMemcpyAsync(&sum, h->d_check + 4 * 148, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TLW_CUDA(h, cudaMemcpyAsync(&bad, h->d_bad, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    TLW_CUDA(h, cudaMemcpyAsync(&st, &h->d_step->status, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (st) {   // a square root of a negative number: the reference's test_rhs! catches the DomainError
+        const unsigned zero = 0;
+        TLW_CUDA(h, cudaMemcpy(&h->d_step->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+    }
+    *admissible = (bad == 0 && st == 0) ? 1 : 0;
+    *total_temporal_error = std::sqrt(sum / ((double)h->nn * (double)h->E));
+    return TLW_OK;
+}
+
+int tlw_adaptive_accept(tlw_handle* h, double dt) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    adaptive_accept_kernel<<<1, 1, 0, h->stream>>>(h->d_step, dt);
+    TLW_CUDA(h, cudaGetLastError());
+    h->cur ^= 1;
+    h->slots_valid = false;
     return TLW_OK;
 }
 

@@ -85,6 +85,12 @@ struct tlw_handle {
     int *d_il = nullptr, *d_ir = nullptr;   // all interfaces (smoothing)
     int ni = 0;
     double jac_first = 0.0;                 // inverse Jacobian of element 1 (TreeMesh interface cache)
+    // Adaptive step control: per-element temporal errors, check scratch, tolerances of the trial in flight
+    double* d_te = nullptr;
+    double* d_check = nullptr;   // [blocks] partial sums, then the total
+    unsigned* d_bad = nullptr;
+    bool te_request = false;
+    double te_abstol = 0.0, te_reltol = 0.0;
     // per-element CFL slots of the state in d_state[cur] (plain LW step on a periodic conforming TreeMesh)
     unsigned long long* d_slots = nullptr;
     bool slots_valid = false;

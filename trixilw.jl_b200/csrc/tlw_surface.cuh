@@ -461,4 +461,46 @@ static __global__ void __launch_bounds__(256) cfl_slots_reduce_kernel(const unsi
     }
 }
 
+
+// Adaptive step control: partial sums of the per-element temporal errors (fixed order within a block) and
+// admissibility (is_admissible, src/equations/compressible_euler_2d.jl:4-7) of every node of the trial state
+static __global__ void __launch_bounds__(256) adaptive_check_kernel(const double* __restrict__ te, int E,
+                                                                    const double* __restrict__ u, long long nodes,
+                                                                    double gamma, double* partial, unsigned* bad) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int e = blockIdx.x * 256 + threadIdx.x; e < E; e += gridDim.x * 256) s += te[e];
+    red[threadIdx.x] = s;
+    bool ok = true;
+    for (long long k = (long long)blockIdx.x * 256 + threadIdx.x; k < nodes; k += (long long)gridDim.x * 256) {
+        double x[NV];
+        load4(u + k * NV, x);
+        const double v1 = x[1] / x[0], v2 = x[2] / x[0];
+        const double p = (gamma - 1.0) * (x[3] - 0.5 * (x[1] * v1 + x[2] * v2));
+        ok = ok && x[0] > 0.0 && p > 0.0;
+    }
+    if (!ok) atomicOr(bad, 1u);
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+static __global__ void adaptive_sum_kernel(const double* partial, int count, double* out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < count; ++k) s += partial[k];
+        *out = s;
+    }
+}
+
+// accept the trial step: t += dt, one more accepted step
+static __global__ void adaptive_accept_kernel(StepState* s, double dt) {
+    s->dt = dt;
+    s->t += dt;
+    s->steps += 1;
+}
+
 }  // namespace tlw

@@ -83,6 +83,9 @@ struct VolArgs {
     const double* metrics;
     const double* inv_jac_node;
     unsigned long long* cfl_slots;   // plain LW step on a periodic TreeMesh: per-element CFL slots (or null)
+    // temporal error estimate of the Adaptive step control (lw_volume_kernel_4!'s u_np1 / u_np1_low tail)
+    double* temporal_errors;          // [e]
+    double abstol, reltol;
 };
 
 // curvilinear: contravariant fluxes f~ = Ja^1_1 f + Ja^1_2 g, g~ = Ja^2_1 f + Ja^2_2 g of a node
@@ -283,9 +286,10 @@ __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, 
 //   depth 3: f_t = raw1/12, f_tt = raw2,    f_ttt = raw3/2
 //   depth 2: f_t = raw1/2,  f_tt = raw2;    depth 1: f_t = raw1/2
 // ------------------------------------------------------------------------------------------------
-template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false>
+template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false>
 static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
     static_assert(!(SC && CURVED), "shock capturing is built for TreeMesh only");
+    static_assert(!TE || (N >= 4 && !SC && !CURVED), "temporal errors: depth-4 TreeMesh kernel");
     using C = VolCfg<N, EBX>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     constexpr int DEPTH = N >= 4 ? 4 : N;
@@ -318,6 +322,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     double U[NV], F[NV], G[NV], up[NV], um[NV], upp[NV], umm[NV];
     double s0 = 0.0, ij = 0.0;   // s0 = -dt J^{-1} (of the element, or of the node on curvilinear meshes)
     double Ja[4] = {0.0, 0.0, 0.0, 0.0};
+    double dF[NV], dG[NV], u0[NV];   // TE: the fourth-derivative term of F, G, and u
     // stage fluxes into the contraction planes (contravariant on curvilinear meshes)
     auto put = [&](const double* f, const double* g) {
         if (CURVED) {
@@ -332,6 +337,10 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     if (active) {
         double uu[NV], f[NV], g[NV];
         load4(a.u + ((size_t)e * nn + node) * NV, uu);
+        if (TE) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u0[v] = uu[v];
+        }
         if (CURVED) {
             load4(a.metrics + ((size_t)e * nn + node) * 4, Ja);
             ij = __ldg(a.inv_jac_node + (size_t)e * nn + node);
@@ -518,6 +527,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
                 r[v] += f[v];
                 q[v] += g[v];
                 F[v] = fma(C4 / 120.0, r[v], F[v]);
+                if (TE) { dF[v] = (C4 / 120.0) * r[v]; dG[v] = (C4 / 120.0) * q[v]; }
                 G[v] = fma(C4 / 120.0, q[v], G[v]);
             }
         }
@@ -567,6 +577,48 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
             sl[tid & 1] = (unsigned long long)__double_as_longlong(m);
 #pragma unroll
             for (int k = 1; k < CFL_SLOTS / 2; ++k) sl[2 * k + (tid & 1)] = 0ull;
+        }
+    }
+    if (TE) {
+        // lw_volume_kernel_4!'s error estimate (dg_2d.jl:1183-1265): the strong-form volume updates
+        // u_np1 = u - dt J^{-1} (D F + D G) and u_np1_low with F, G before the fourth-derivative term;
+        // temporal_errors[e] = sum over nodes and variables of ((u_np1 - u_np1_low) / (abstol + reltol max))^2
+        double un[NV], err = 0.0;
+        __syncthreads();
+        if (active) node_put<N, C>(X, Y, el, i, j, F, G);
+        __syncthreads();
+        line_contract<N, C, false>(X, Y, tid);
+        __syncthreads();
+        if (active) {
+            double dd[NV];
+            node_sum<N, C>(X, Y, el, i, j, dd);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) un[v] = fma(s0, dd[v], u0[v]);
+        }
+        __syncthreads();
+        if (active) node_put<N, C>(X, Y, el, i, j, dF, dG);
+        __syncthreads();
+        line_contract<N, C, false>(X, Y, tid);
+        __syncthreads();
+        if (active) {
+            double dd[NV];
+            node_sum<N, C>(X, Y, el, i, j, dd);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const double lo = un[v] - s0 * dd[v];
+                const double r = (un[v] - lo) / (a.abstol + a.reltol * fmax(fabs(un[v]), fabs(lo)));
+                err = fma(r, r, err);
+            }
+        }
+        __syncthreads();
+        if (active) X[el * C::P + i + C::R * j] = err;
+        __syncthreads();
+        const int ee = blockIdx.x * EB + tid;
+        if (tid < EB && ee < a.E) {
+            double sum = 0.0;
+            for (int jj = 0; jj < n; ++jj)
+                for (int ii = 0; ii < n; ++ii) sum += X[tid * C::P + ii + C::R * jj];
+            a.temporal_errors[ee] = sum;
         }
     }
 }

@@ -38,7 +38,7 @@ EXPORTED = (
     "tlw_batch_get_stream", "tlw_batch_autotune", "tlw_batch_num_groups", "tlw_batch_last_error",
     "tlw_adjoint_step", "tlw_forward_record", "tlw_adjoint_sweep", "tlw_adjoint_solve", "tlw_adjoint_dt_sequence",
     "tlw_solve_dts", "tlw_set_curved_mesh", "tlw_curved_colors", "tlw_set_tree_mortars",
-    "tlw_set_parabolic",
+    "tlw_set_parabolic", "tlw_adaptive_trial", "tlw_adaptive_accept",
 )
 
 
@@ -110,6 +110,8 @@ def lib() -> ctypes.CDLL:
     L.tlw_set_curved_mesh.argtypes = [P, i64, dp, dp, i64, i64p, i32p, i64p, i32p, i32p]
     L.tlw_set_tree_mortars.argtypes = [P, i64, i64p, i64p, i64p]
     L.tlw_set_parabolic.argtypes = [P, dbl, dbl]
+    L.tlw_adaptive_trial.argtypes = [P, dbl, dbl, dbl, dp, ctypes.POINTER(ctypes.c_int32)]
+    L.tlw_adaptive_accept.argtypes = [P, dbl]
     L.tlw_curved_colors.argtypes = [P]
     L.tlw_curved_colors.restype = i32
     L.tlw_adjoint_step.argtypes = [P, P, P, P, dbl, i32]

@@ -91,8 +91,10 @@ def solve_lwfr(lw_update: LWUpdate, callbacks=(), dt_initial: float = 0.0, toler
     and at the end. Limiters are not built on the device path (none of the workloads use one)."""
     if limiters:
         raise NotImplementedError("limiters are not built on the device path")
-    if time_step_computation is None or isinstance(time_step_computation, Adaptive):
-        raise NotImplementedError("only CFLBased stepping is built on the device path")
+    if isinstance(time_step_computation, Adaptive):
+        return _solve_adaptive(lw_update, callbacks, dt_initial, tolerances)
+    if time_step_computation is None:
+        raise NotImplementedError("give CFLBased(cfl) or Adaptive()")
     assert isinstance(time_step_computation, CFLBased)
     semi = lw_update.p
     cfl = time_step_computation.cfl_number
@@ -121,6 +123,85 @@ def solve_lwfr(lw_update: LWUpdate, callbacks=(), dt_initial: float = 0.0, toler
         for cb in callbacks:
             if getattr(cb, "interval", 0) and integ.iter % int(cb.interval) == 0:
                 cb(integ, integ.get_state())
+    u = integ.get_state()
+    for cb in callbacks:
+        cb(integ, u)
+    return LWSolution([u], lw_update, [integ.t], integ.stats)
+
+
+CONTROLLER = (0.6, -0.2, 0.0)   # (beta1, beta2, beta3), src/solvers/lwfr.jl:162
+
+
+def dt_factor(epsilon: dict, k: int, controller=CONTROLLER) -> float:
+    """dt_factor (src/solvers/adaptive.jl:94-99): 1 + atan(eps_1^(b1/k) eps_0^(b2/k) eps_-1^(b3/k) - 1)."""
+    b1, b2, b3 = controller
+    f = epsilon[1] ** (b1 / k) * epsilon[0] ** (b2 / k) * epsilon[-1] ** (b3 / k)
+    return 1.0 + math.atan(f - 1.0)
+
+
+class AdaptiveController:
+    """The step-size logic of perform_step!(..., ::Adaptive, ::LW) (src/solvers/adaptive.jl:101-172), apart
+    from the trial step itself: ``propose`` gives the dt to try, ``judge`` takes the trial's total temporal
+    error and admissibility and says whether to accept; the epsilon history is updated as
+    load_temporal_errors! does (shifted only on the first try of a step)."""
+
+    def __init__(self, nnodes: int, t0: float, t_end: float, dt_initial: float):
+        self.k = nnodes
+        self.t_end = t_end
+        self.t = t0
+        self.epsilon = {-1: 1.0, 0: 1.0, 1: 1.0}
+        self.n_fail = 0
+        self.nreject = 0
+        self.iter = 0
+        self.dt = self._clamp(dt_initial)
+        self.factor = 1.0
+
+    def _clamp(self, dt):   # set_dt!
+        return self.t_end - self.t if self.t + dt > self.t_end else dt
+
+    def judge(self, total_error: float, admissible: bool) -> bool:
+        if self.n_fail == 0:
+            self.epsilon[-1], self.epsilon[0] = self.epsilon[0], self.epsilon[1]
+        if math.isfinite(total_error):   # a trial with non-finite values keeps the previous estimate
+            self.epsilon[1] = 1.0 / (total_error + 1e-12)
+        self.factor = dt_factor(self.epsilon, self.k)
+        if admissible and not self.factor <= 0.81:
+            self.nreject += self.n_fail
+            self.n_fail = 0
+            dt = self.dt
+            self.t += dt
+            self.iter += 1
+            self.dt = self._clamp(min(self.factor, 1.5) * dt)
+            return True
+        self.n_fail += 1
+        self.dt = self._clamp(min(self.factor, 0.95) * self.dt)
+        return False
+
+    def finished(self) -> bool:
+        te = self.t_end
+        return self.t == te or abs(self.t - te) <= math.sqrt(np.finfo(float).eps) * max(abs(self.t), abs(te))
+
+
+def _solve_adaptive(lw_update: LWUpdate, callbacks, dt_initial: float, tolerances) -> LWSolution:
+    semi = lw_update.p
+    tol = tolerances or {"abstol": 1e-6, "reltol": 1e-6}
+    integ = LWIntegrator(lw_update, tol)
+    integ.set_state(lw_update.u0_ode, lw_update.tspan[0])
+    semi._prepare_boundaries(lw_update.tspan[0], 0.0, 1.0)
+    ctl = AdaptiveController(semi.nnodes, lw_update.tspan[0], lw_update.tspan[1], dt_initial)
+    err = ctypes.c_double()
+    ok = ctypes.c_int32()
+    while not ctl.finished():
+        dt = ctl.dt
+        check(integ.handle, lib().tlw_adaptive_trial(integ.handle, float(dt), float(tol["abstol"]),
+                                                     float(tol["reltol"]), ctypes.byref(err), ctypes.byref(ok)))
+        if ctl.judge(err.value, bool(ok.value)):
+            check(integ.handle, lib().tlw_adaptive_accept(integ.handle, float(dt)))
+            for cb in callbacks:
+                if getattr(cb, "interval", 0) and ctl.iter % int(cb.interval) == 0:
+                    cb(integ, integ.get_state())
+    integ.sync_time()
+    integ.stats.nreject = ctl.nreject
     u = integ.get_state()
     for cb in callbacks:
         cb(integ, u)

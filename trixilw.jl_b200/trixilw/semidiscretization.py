@@ -51,7 +51,9 @@ class CFLBased:
 
 
 class Adaptive:
-    """Error-controlled stepping (src/solvers/adaptive.jl). Not built on the device."""
+    """Error-controlled stepping (src/solvers/adaptive.jl:47-172): the LW step's temporal error estimate,
+    the PI controller with (beta1, beta2, beta3) = (0.6, -0.2, 0.0) (src/solvers/lwfr.jl:162) and rejection
+    below a factor of 0.81. LW on a TreeMesh with N >= 4."""
 
 
 @dataclass
