@@ -108,6 +108,22 @@ int tlw_adaptive_trial(tlw_handle* h, double dt, double abstol, double reltol, d
                        int32_t* admissible);
 int tlw_adaptive_accept(tlw_handle* h, double dt);
 
+/* Zhang-Shu positivity-preserving limiter, PositivityPreservingLimiterZhangShu(thresholds, variables) as a
+ * stage limiter (src/callbacks/callbacks_stage/positivity_zhang_shu.jl:10-42, positivity_zhang_shu_dg2d.jl:8-176):
+ * count (threshold, variable) pairs, applied in order; per pair the element pass and, on a TreeMesh with
+ * mortars, the large-element mortar pass. count = 0 switches it off; at most TLW_LIMITER_MAX_PAIRS pairs.
+ * Once set, tlw_step applies it after every step where solve_lwfr does (LW: twice, perform_step! and the
+ * step loop, src/solvers/lwfr.jl:226,257; MDRK: once, the loop), tlw_adaptive_trial applies it to the trial
+ * state before the admissibility check (adaptive.jl:131-132) and tlw_adaptive_accept once more (the loop).
+ * Not with the adjoint entry points. tlw_apply_positivity_limiter applies it once to the current state
+ * (solve_lwfr before its loop, lwfr.jl:251); asynchronous on the handle's stream. */
+#define TLW_LIMIT_DENSITY 0           /* Trixi density(u, equations) */
+#define TLW_LIMIT_PRESSURE 1          /* Trixi pressure(u, equations) */
+#define TLW_LIMIT_DENSITY_PRESSURE 2  /* Trixi density_pressure(u, equations) */
+#define TLW_LIMITER_MAX_PAIRS 4
+int tlw_set_positivity_limiter(tlw_handle* h, int32_t count, const double* thresholds, const int32_t* variables);
+int tlw_apply_positivity_limiter(tlw_handle* h);
+
 /* Compressible Navier-Stokes (SemidiscretizationHyperbolicParabolic with CompressibleNavierStokesDiffusion2D,
  * conservative gradient variables, BR1) on the handle's periodic conforming TreeMesh, set after
  * tlw_set_tree_mesh (which clears it): LW with the FR volume integral, N >= 3. mu = dynamic viscosity,

@@ -7,6 +7,7 @@
 
 #include "tlw_adjoint.hpp"
 #include "tlw_curved.hpp"
+#include "tlw_limiter.hpp"
 #include "tlw_parabolic.hpp"
 #include "tlw_oracle.hpp"
 
@@ -25,7 +26,10 @@ struct oracle_handle {
     CurvedMesh cmesh;
     bool parabolic = false;      // compressible Navier-Stokes (TreeMesh, periodic, LW)
     NavierStokes ns;
+    PositivityLimiter lim;       // applied after every step of oracle_steps when not empty
     char err[256] = {0};
+
+    int n_elements() const { return curved ? cmesh.n_elements : mesh.n_elements; }
 };
 
 namespace {
@@ -279,6 +283,12 @@ int oracle_steps(oracle_handle* h, int kind, double* u, int nsteps, double cfl, 
 #pragma omp parallel for num_threads(nthreads) schedule(static)
             for (long long k = 0; k < (long long)ndof; ++k) u[k] = u[k] + dt * h->du[k];
         }
+        // the positivity limiter as solve_lwfr applies it: LW twice (perform_step!, src/solvers/lwfr.jl:226,
+        // and the loop, :257), MDRK once (the loop; the mid-step call at src/solvers/mdrk.jl:19 acts on u^n,
+        // which the previous step's application has limited already)
+        if (!h->lim.thresholds.empty())
+            for (int a = 0; a < (kind == 0 ? 2 : 1); ++a)
+                apply_positivity_limiter(h->basis, h->eq, h->mesh, h->n_elements(), h->lim, u);
         t += dt;
     }
     *t_inout = t;
@@ -287,6 +297,23 @@ int oracle_steps(oracle_handle* h, int kind, double* u, int nsteps, double cfl, 
         std::snprintf(h->err, sizeof(h->err), "%s", ex.what());
         return -1;
     }
+}
+
+// Zhang-Shu positivity limiter pairs (PositivityPreservingLimiterZhangShu(thresholds, variables));
+// variables: 0 density, 1 pressure, 2 density_pressure. count 0 switches it off.
+int oracle_set_limiter(oracle_handle* h, int count, const double* thresholds, const int32_t* variables) {
+    if (count < 0) return 1;
+    h->lim.thresholds.assign(thresholds, thresholds + count);
+    h->lim.variables.assign(variables, variables + count);
+    for (int v : h->lim.variables)
+        if (v < 0 || v > 2) return 1;
+    return 0;
+}
+
+// one application of the limiter to u in place
+int oracle_apply_limiter(oracle_handle* h, double* u) {
+    apply_positivity_limiter(h->basis, h->eq, h->mesh, h->n_elements(), h->lim, u);
+    return 0;
 }
 
 const char* oracle_last_error(oracle_handle* h) { return h->err; }

@@ -18,7 +18,7 @@ LIB = os.path.join(_HERE, "liboracle_tlw.so")
 
 def build(force: bool = False) -> str:
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(
-            os.path.getmtime(os.path.join(_HERE, f)) for f in ("tlw_oracle.hpp", "oracle_capi.cpp")):
+            os.path.getmtime(os.path.join(_HERE, f)) for f in os.listdir(_HERE) if f.endswith((".hpp", ".cpp"))):
         subprocess.run(["make", "-C", _HERE, "-B" if force else "liboracle_tlw.so"], check=True,
                        stdout=subprocess.DEVNULL)
     return LIB
@@ -52,6 +52,8 @@ def lib():
         L.oracle_mortar_operators.argtypes = [i32, P]
         L.oracle_create_curved.argtypes = [i32, dbl, i32, i32, i32, P, P, i32, P, P, P, P, P]
         L.oracle_create_curved.restype = P
+        L.oracle_set_limiter.argtypes = [P, i32, P, P]
+        L.oracle_apply_limiter.argtypes = [P, P]
         L.oracle_last_error.argtypes = [P]
         L.oracle_last_error.restype = ctypes.c_char_p
         _L = L
@@ -151,6 +153,19 @@ class Oracle:
     def set_parabolic(self, mu: float, Pr: float = 0.72):
         """Compressible Navier-Stokes with dynamic viscosity mu and Prandtl number Pr (periodic TreeMesh)."""
         assert lib().oracle_set_parabolic(self.h, float(mu), float(Pr)) == 0
+
+    def set_positivity_limiter(self, thresholds=(5.0e-6, 5.0e-6), variables=(0, 1)):
+        """Zhang-Shu limiter pairs applied after every step of ``steps`` (variables: 0 density, 1 pressure,
+        2 density_pressure); an empty tuple switches it off."""
+        self._lkeep = (np.ascontiguousarray(thresholds, dtype=np.float64),
+                       np.ascontiguousarray(variables, dtype=np.int32))
+        assert lib().oracle_set_limiter(self.h, len(thresholds), _p(self._lkeep[0]), _p(self._lkeep[1])) == 0
+
+    def apply_positivity_limiter(self, u):
+        """One application of the limiter to a copy of u."""
+        u = np.array(u, dtype=np.float64, copy=True)
+        assert lib().oracle_apply_limiter(self.h, _p(u)) == 0
+        return u
 
     def set_shock_capturing(self, on=True, alpha_max=0.5, alpha_min=0.001, alpha_smooth=True):
         lib().oracle_set_shock_capturing(self.h, 1 if on else 0, alpha_max, alpha_min, 1 if alpha_smooth else 0)

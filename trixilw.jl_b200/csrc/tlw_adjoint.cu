@@ -550,9 +550,10 @@ int adj_ready(tlw_handle* h) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh) return afail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
     if (h->opts.time_discretization != TLW_LW || h->sc || h->opts.surface_flux != TLW_FLUX_RUSANOV || h->nb > 0 || h->curved ||
-        h->N < 3 || h->N > 5)
+        h->N < 3 || h->N > 5 || h->nmx + h->nmy > 0 || h->parabolic || h->lim_count > 0)
         return afail(h, TLW_E_UNSUPPORTED,
-                     "adjoint: LW, FR volume integral, Rusanov flux, periodic TreeMesh, N = 3..5");
+                     "adjoint: LW, FR volume integral, Rusanov flux, periodic conforming TreeMesh, Euler, N = 3..5, "
+                     "no positivity limiter");
     TLW_ACUDA(h, cudaSetDevice(h->device));
     AdjointBuffers& A = h->adj;
     if (!A.const_uploaded) {

@@ -15,6 +15,7 @@
 #include "tlw_curved.cuh"
 #include "tlw_handle.h"
 #include "tlw_mortar.cuh"
+#include "tlw_limiter.cuh"
 #include "tlw_parabolic.cuh"
 #include "tlw_surface.cuh"
 #include "tlw_volume.cuh"
@@ -60,6 +61,7 @@ void free_mesh(tlw_handle* h) {
     dfree(h->d_Ja); dfree(h->d_ijn); dfree(h->d_cp); dfree(h->d_cs); dfree(h->d_cf);
     dfree(h->d_ml); dfree(h->d_mu); dfree(h->d_mg); dfree(h->d_ms);
     h->nmx = h->nmy = 0;
+    if (h->d_mface) { cudaFree(h->d_mface); h->d_mface = nullptr; }
     dfree(h->d_gx); dfree(h->d_gy); dfree(h->d_tFv); dfree(h->d_visc);
     h->parabolic = false;
     dfree(h->d_slots);
@@ -213,6 +215,13 @@ struct Launch {
     }
 };
 
+template <int N> struct Lim {
+    static void run(cudaStream_t s, const LimiterArgs& a) {
+        if (a.E == 0) return;
+        positivity_limiter_kernel<N><<<(a.E + LIMITER_WARPS - 1) / LIMITER_WARPS, 32 * LIMITER_WARPS, 0, s>>>(a);
+    }
+};
+
 template <template <int> class F, class... A>
 void dispatch(int N, A&&... args) {
     switch (N) {
@@ -287,6 +296,22 @@ void enqueue_indicator(tlw_handle* h, const double* u, bool speed) {
 bool use_slots(const tlw_handle* h) {
     return h->d_slots && h->opts.time_discretization == TLW_LW && !h->sc && !h->curved && !h->parabolic &&
            h->nb == 0 && h->nmx + h->nmy == 0;
+}
+
+// `reps` applications of the positivity limiter to u (in place); slots: the CFL slots of u to keep current
+void enqueue_limiter(tlw_handle* h, double* u, int reps, unsigned long long* slots) {
+    if (h->lim_count == 0) return;
+    LimiterArgs a{};
+    a.u = u;
+    a.E = (int)h->E;
+    a.gamma = h->opts.gamma;
+    a.npairs = h->lim_count;
+    a.reps = reps;
+    for (int p = 0; p < h->lim_count; ++p) { a.threshold[p] = h->lim_thr[p]; a.variable[p] = h->lim_var[p]; }
+    a.mortar_faces = h->d_mface;
+    a.cfl_slots = slots;
+    a.status = &h->d_step->status;
+    dispatch<Lim>(h->N, h->stream, a);
 }
 
 void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const double* u_jump, const double* u_base,
@@ -481,9 +506,14 @@ void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const
     const double* dtp = &h->d_step->dt;
     if (h->opts.time_discretization == TLW_LW) {
         enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, dtp, ev, true);
+        // solve_lwfr limits twice per LW step: in perform_step! (src/solvers/lwfr.jl:226) and in its loop (:257)
+        enqueue_limiter(h, unew, 2, use_slots(h) ? h->d_slots : nullptr);
     } else {
         enqueue_rhs(h, TLW_STAGE_MDRK1, MODE_STEP, u, u, u, h->d_us, dtp, ev, true);
         enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, dtp, ev ? ev + 1 : nullptr, true);
+        // once per MDRK step (the loop); perform_step!'s mid-step call (src/solvers/mdrk.jl:19) acts on u^n,
+        // which the previous step's application has limited already
+        enqueue_limiter(h, unew, 1, nullptr);
     }
 }
 
@@ -775,6 +805,7 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
     if (n_mortars < 0 || (n_mortars > 0 && (!mortar_neighbor_ids || !mortar_large_sides || !mortar_orientations)))
         return fail(h, TLW_E_ARG, "mortars");
     std::vector<int> ml[2], mu[2], mg[2], ms[2];
+    std::vector<int> mface(n_mortars > 0 ? (size_t)h->E : 0, 0);
     for (int64_t k = 0; k < n_mortars; ++k) {
         const int64_t lo = mortar_neighbor_ids[3 * k] - 1, up = mortar_neighbor_ids[3 * k + 1] - 1;
         const int64_t lg = mortar_neighbor_ids[3 * k + 2] - 1;
@@ -783,12 +814,17 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
             (o != 1 && o != 2) || lo == up || lo == lg || up == lg)
             return fail(h, TLW_E_ARG, "mortar " + std::to_string(k + 1) + " out of range");
         const int d = (int)o - 1;
+        int& desc = mface[(size_t)lg];
+        if ((desc & 7) >= 4) return fail(h, TLW_E_ARG, "element " + std::to_string(lg + 1) + " is the large side of more than 4 mortars");
+        const int face = side == 1 ? (o == 1 ? 1 : 3) : (o == 1 ? 0 : 2);
+        desc = ((desc & ~7) | ((desc & 7) + 1)) | (face << (3 + 2 * (desc & 7)));
         ml[d].push_back((int)lo); mu[d].push_back((int)up); mg[d].push_back((int)lg); ms[d].push_back((int)side);
     }
     TLW_CUDA(h, cudaSetDevice(h->device));
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));
     drop_graphs(h);
     dfree(h->d_ml); dfree(h->d_mu); dfree(h->d_mg); dfree(h->d_ms);
+    if (h->d_mface) { cudaFree(h->d_mface); h->d_mface = nullptr; }
     h->nmx = (int)ml[0].size();
     h->nmy = (int)ml[1].size();
     if (n_mortars > 0) {
@@ -801,9 +837,36 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
         };
         int rc;
         if ((rc = up_cat(h->d_ml, ml[0], ml[1])) || (rc = up_cat(h->d_mu, mu[0], mu[1])) ||
-            (rc = up_cat(h->d_mg, mg[0], mg[1])) || (rc = up_cat(h->d_ms, ms[0], ms[1])))
+            (rc = up_cat(h->d_mg, mg[0], mg[1])) || (rc = up_cat(h->d_ms, ms[0], ms[1])) ||
+            (rc = up_cat(h->d_mface, mface, std::vector<int>())))
             return rc;
     }
+    return TLW_OK;
+}
+
+int tlw_set_positivity_limiter(tlw_handle* h, int32_t count, const double* thresholds, const int32_t* variables) {
+    if (!h) return TLW_E_ARG;
+    if (count < 0 || count > TLW_LIMITER_MAX_PAIRS || (count > 0 && (!thresholds || !variables)))
+        return fail(h, TLW_E_ARG, "limiter: 0..4 (threshold, variable) pairs");
+    for (int p = 0; p < count; ++p)
+        if (variables[p] < TLW_LIMIT_DENSITY || variables[p] > TLW_LIMIT_DENSITY_PRESSURE || !std::isfinite(thresholds[p]))
+            return fail(h, TLW_E_ARG, "limiter: variable " + std::to_string(p + 1));
+    if (h->stream) {
+        TLW_CUDA(h, cudaSetDevice(h->device));
+        TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    drop_graphs(h);
+    h->lim_count = count;
+    for (int p = 0; p < count; ++p) { h->lim_thr[p] = thresholds[p]; h->lim_var[p] = variables[p]; }
+    return TLW_OK;
+}
+
+int tlw_apply_positivity_limiter(tlw_handle* h) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    enqueue_limiter(h, h->d_state[h->cur], 1, (use_slots(h) && h->slots_valid) ? h->d_slots : nullptr);
+    TLW_CUDA(h, cudaGetLastError());
     return TLW_OK;
 }
 
@@ -855,6 +918,7 @@ int tlw_adaptive_trial(tlw_handle* h, double dt, double abstol, double reltol, d
     h->te_reltol = reltol;
     enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, trial, &h->d_step->dt_call);
     h->te_request = false;
+    enqueue_limiter(h, trial, 1, nullptr);   // perform_step!(..., ::Adaptive, ::LW) (adaptive.jl:131-132)
     adaptive_check_kernel<<<blocks, 256, 0, h->stream>>>(h->d_te, (int)h->E, trial, (long long)h->nn * h->E,
                                                           h->opts.gamma, h->d_check, h->d_bad);
     adaptive_sum_kernel<<<1, 32, 0, h->stream>>>(h->d_check, blocks, h->d_check + 4 * 148);
@@ -879,6 +943,7 @@ int tlw_adaptive_accept(tlw_handle* h, double dt) {
     if (rc) return rc;
     TLW_CUDA(h, cudaSetDevice(h->device));
     adaptive_accept_kernel<<<1, 1, 0, h->stream>>>(h->d_step, dt);
+    enqueue_limiter(h, h->d_state[1 - h->cur], 1, nullptr);   // solve_lwfr's loop (lwfr.jl:257)
     TLW_CUDA(h, cudaGetLastError());
     h->cur ^= 1;
     h->slots_valid = false;

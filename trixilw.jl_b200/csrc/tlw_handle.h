@@ -102,6 +102,13 @@ struct tlw_handle {
     // L2 mortars of a non-conforming TreeMesh: x-mortars [0, nmx), then y-mortars [nmx, nmx + nmy)
     int *d_ml = nullptr, *d_mu = nullptr, *d_mg = nullptr, *d_ms = nullptr;
     int nmx = 0, nmy = 0;
+    // per element: the faces (0..3) through which it is the large element of a mortar, in mortar order
+    // (bits 0-2 count, then 2 bits per mortar); for the positivity limiter's mortar pass
+    int* d_mface = nullptr;
+    // Zhang-Shu positivity limiter after each step (lim_count = 0: off)
+    int lim_count = 0;
+    double lim_thr[4] = {0.0, 0.0, 0.0, 0.0};
+    int lim_var[4] = {0, 0, 0, 0};
     // conforming curvilinear mesh (instead of the TreeMesh arrays above; d_state etc. shared)
     bool curved = false;
     double* d_Ja = nullptr;                 // contravariant vectors [4, i, j, e]

@@ -7,6 +7,7 @@ from .batch import LWBatch, solve_lwfr_batch
 from .curved_mesh import CurvedMesh, StructuredMesh, rotate_elements, rotate_state
 from .equations import (CompressibleEulerEquations2D, CompressibleNavierStokesDiffusion2D, ConstantState,
                         DensityWave, FourQuadrantRiemann, GradientVariablesConservative, IsentropicVortex)
+from .limiters import PositivityPreservingLimiterZhangShu, density, density_pressure, pressure
 from .lwfr import LWIntegrator, LWSolution, l2_linf_errors, solve_lwfr
 from .mesh import RefinedTreeMesh, TreeMesh
 from .semidiscretization import (LW, MDRK, DGSEM, Adaptive, BoundaryConditionDirichlet, CFLBased, FluxHLL,
@@ -28,4 +29,5 @@ __all__ = [
     "adjoint_solve", "adjoint_step", "adjoint_sweep", "forward_record", "lw_solve", "solve_dts",
     "CurvedMesh", "StructuredMesh", "rotate_elements", "rotate_state", "RefinedTreeMesh",
     "CompressibleNavierStokesDiffusion2D", "GradientVariablesConservative", "SemidiscretizationHyperbolicParabolic",
+    "PositivityPreservingLimiterZhangShu", "density", "pressure", "density_pressure",
 ]

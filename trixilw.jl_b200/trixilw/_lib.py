@@ -26,6 +26,7 @@ TLW_WHERE_HOST, TLW_WHERE_DEVICE = 0, 1
 TLW_STAGE_LW, TLW_STAGE_MDRK1, TLW_STAGE_MDRK2 = 0, 1, 2
 TLW_CACHE_U_TRACES, TLW_CACHE_F_TRACES, TLW_CACHE_U2, TLW_CACHE_F2, TLW_CACHE_ALPHA, TLW_CACHE_FN_LOW = 0, 1, 2, 3, 4, 5
 TLW_VOLUME_FR, TLW_VOLUME_FR_SHOCK_CAPTURING = 0, 1
+TLW_LIMIT_DENSITY, TLW_LIMIT_PRESSURE, TLW_LIMIT_DENSITY_PRESSURE = 0, 1, 2
 
 # every symbol include/tlw.h declares
 EXPORTED = (
@@ -39,6 +40,7 @@ EXPORTED = (
     "tlw_adjoint_step", "tlw_forward_record", "tlw_adjoint_sweep", "tlw_adjoint_solve", "tlw_adjoint_dt_sequence",
     "tlw_solve_dts", "tlw_set_curved_mesh", "tlw_curved_colors", "tlw_set_tree_mortars",
     "tlw_set_parabolic", "tlw_adaptive_trial", "tlw_adaptive_accept",
+    "tlw_set_positivity_limiter", "tlw_apply_positivity_limiter",
 )
 
 
@@ -110,6 +112,8 @@ def lib() -> ctypes.CDLL:
     L.tlw_set_curved_mesh.argtypes = [P, i64, dp, dp, i64, i64p, i32p, i64p, i32p, i32p]
     L.tlw_set_tree_mortars.argtypes = [P, i64, i64p, i64p, i64p]
     L.tlw_set_parabolic.argtypes = [P, dbl, dbl]
+    L.tlw_set_positivity_limiter.argtypes = [P, i32, P, P]
+    L.tlw_apply_positivity_limiter.argtypes = [P]
     L.tlw_adaptive_trial.argtypes = [P, dbl, dbl, dbl, dp, ctypes.POINTER(ctypes.c_int32)]
     L.tlw_adaptive_accept.argtypes = [P, dbl]
     L.tlw_curved_colors.argtypes = [P]

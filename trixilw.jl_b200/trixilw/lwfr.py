@@ -17,6 +17,7 @@ import numpy as np
 from . import _lib
 from ._lib import check, lib
 from .basis import gauss_lobatto
+from .limiters import install as install_limiters
 from .semidiscretization import Adaptive, CFLBased, LWUpdate, SemidiscretizationHyperbolic, _ptr
 
 
@@ -88,19 +89,21 @@ def solve_lwfr(lw_update: LWUpdate, callbacks=(), dt_initial: float = 0.0, toler
     """solve_lwfr(lw_update, callbacks, dt_initial, tolerances; time_step_computation) (lwfr.jl:233-263).
 
     callbacks: objects with an ``interval`` (steps) called as ``cb(integrator, u)`` every interval steps
-    and at the end. Limiters are not built on the device path (none of the workloads use one)."""
-    if limiters:
-        raise NotImplementedError("limiters are not built on the device path")
-    if isinstance(time_step_computation, Adaptive):
-        return _solve_adaptive(lw_update, callbacks, dt_initial, tolerances)
+    and at the end. limiters: PositivityPreservingLimiterZhangShu instances; applied on the device once
+    before the loop and after every step as solve_lwfr does (lwfr.jl:226, 251, 257)."""
     if time_step_computation is None:
         raise NotImplementedError("give CFLBased(cfl) or Adaptive()")
-    assert isinstance(time_step_computation, CFLBased)
     semi = lw_update.p
+    n_pairs = install_limiters(semi, limiters)
+    if isinstance(time_step_computation, Adaptive):
+        return _solve_adaptive(lw_update, callbacks, dt_initial, tolerances, n_pairs > 0)
+    assert isinstance(time_step_computation, CFLBased)
     cfl = time_step_computation.cfl_number
     integ = LWIntegrator(lw_update, tolerances)
     u0 = lw_update.u0_ode
     integ.set_state(u0, lw_update.tspan[0])
+    if n_pairs:
+        check(integ.handle, lib().tlw_apply_positivity_limiter(integ.handle))
     bc = semi.boundary_conditions
     time_dependent_bc = semi.mesh.n_boundaries > 0 and not bc.time_independent
     intervals = [int(cb.interval) for cb in callbacks if getattr(cb, "interval", 0)]
@@ -182,11 +185,13 @@ class AdaptiveController:
         return self.t == te or abs(self.t - te) <= math.sqrt(np.finfo(float).eps) * max(abs(self.t), abs(te))
 
 
-def _solve_adaptive(lw_update: LWUpdate, callbacks, dt_initial: float, tolerances) -> LWSolution:
+def _solve_adaptive(lw_update: LWUpdate, callbacks, dt_initial: float, tolerances, limit: bool = False) -> LWSolution:
     semi = lw_update.p
     tol = tolerances or {"abstol": 1e-6, "reltol": 1e-6}
     integ = LWIntegrator(lw_update, tol)
     integ.set_state(lw_update.u0_ode, lw_update.tspan[0])
+    if limit:   # the trial and the accept apply it after that (tlw_adaptive_trial / tlw_adaptive_accept)
+        check(integ.handle, lib().tlw_apply_positivity_limiter(integ.handle))
     semi._prepare_boundaries(lw_update.tspan[0], 0.0, 1.0)
     ctl = AdaptiveController(semi.nnodes, lw_update.tspan[0], lw_update.tspan[1], dt_initial)
     err = ctypes.c_double()
