@@ -125,11 +125,22 @@ int tlw_set_positivity_limiter(tlw_handle* h, int32_t count, const double* thres
 int tlw_apply_positivity_limiter(tlw_handle* h);
 
 /* Compressible Navier-Stokes (SemidiscretizationHyperbolicParabolic with CompressibleNavierStokesDiffusion2D,
- * conservative gradient variables, BR1) on the handle's periodic conforming TreeMesh, set after
- * tlw_set_tree_mesh (which clears it): LW with the FR volume integral, N >= 3. mu = dynamic viscosity,
- * prandtl = Prandtl number; the handle's gamma. Replaces rhs! of src/solvers/dgsem_tree/dg_2d_parabolic.jl:15-99
- * (kernels :725-1860, interface flux :1911-1949) and compute_dt (src/solvers/lwfr.jl:192-210). */
+ * conservative gradient variables, BR1) on the handle's conforming TreeMesh, set after tlw_set_tree_mesh
+ * (which clears it): LW with the FR volume integral, N >= 3. mu = dynamic viscosity, prandtl = Prandtl number;
+ * the handle's gamma. Replaces rhs! of src/solvers/dgsem_tree/dg_2d_parabolic.jl:15-99 (kernels :725-1860,
+ * interface flux :1911-1949, boundaries :1951-2084) and compute_dt (src/solvers/lwfr.jl:192-210). A mesh with
+ * boundaries also needs tlw_set_parabolic_walls. */
 int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl);
+
+/* Walls of the parabolic part, one per boundary (Trixi boundaries order), after tlw_set_parabolic:
+ * BoundaryConditionNavierStokesWall(NoSlip(v), Adiabatic(q)) or (NoSlip(v), Isothermal(T))
+ * (src/equations/compressible_navier_stokes_2d.jl:81-124). wall_data [3, l, boundary] = (v1, v2, q) or
+ * (v1, v2, T) at the boundary's nodes, held until replaced (the reference evaluates the wall functions at the
+ * step's t; re-send for walls that change in time). The gradient sees prim2cons(rho_inner, v, p_inner or
+ * rho_inner T); the viscous boundary flux is the inner one with, for Adiabatic, the energy flux v . tau_n + q. */
+#define TLW_WALL_NOSLIP_ADIABATIC 1
+#define TLW_WALL_NOSLIP_ISOTHERMAL 2
+int tlw_set_parabolic_walls(tlw_handle* h, const int32_t* kinds, const double* wall_data);
 
 /* L2 mortars of a non-conforming TreeMesh{2} (after AMR), set after tlw_set_tree_mesh (which clears them):
  *   mortar_neighbor_ids [3, n_mortars]  (lower small, upper small, large element), 1-based  Trixi mortars.neighbor_ids
@@ -159,11 +170,20 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
 /* Number of interface colours (launches per interface pass) of the curvilinear mesh; 0 for a TreeMesh. */
 int32_t tlw_curved_colors(tlw_handle* h);
 
+/* Boundary condition of each boundary (Trixi boundaries order) of a TreeMesh, after tlw_set_tree_mesh (which
+ * resets all to Dirichlet): TLW_BC_DIRICHLET, the time-averaged Dirichlet condition below, or the LW slip walls
+ * boundary_condition_slip_wall_vertical / _horizontal (src/equations/equations.jl:95-135), which mirror the
+ * normal momentum of u, U and the normal flux trace and need no exterior data. */
+#define TLW_BC_DIRICHLET 0
+#define TLW_BC_SLIP_WALL_VERTICAL 1
+#define TLW_BC_SLIP_WALL_HORIZONTAL 2
+int tlw_set_boundary_kinds(tlw_handle* h, const int32_t* kinds);
+
 /* Exterior states of the time-averaged Dirichlet boundary condition (src/equations/equations.jl:6-37):
  *   levels [v, q, l, boundary]: boundary_value_function(x_l, t + 0.5*dt_scaled*(x_q + 1)) at the N+1 GLL
  *                              time levels q (dt_scaled = scaling_factor * dt)
  *   now    [v, l, boundary]:    boundary_value_function(x_l, t)
- * Held until replaced; required before any rhs when the mesh has boundaries. */
+ * Held until replaced; required before any rhs when the mesh has Dirichlet boundaries. */
 int tlw_set_boundary_data(tlw_handle* h, const double* levels, const double* now, int32_t where);
 
 /* One right-hand side evaluation: du = rhs(u) exactly as the reference's rhs!/rhs_mdrk1!/rhs_mdrk2!

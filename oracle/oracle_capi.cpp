@@ -39,7 +39,7 @@ void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, do
              const BoundaryData* bd, int kind, int nthreads) {
     if (h->parabolic) {
         if (kind != 0) throw std::runtime_error("parabolic oracle: LW only");
-        rhs_parabolic(h->basis, h->eq, h->ns, h->opt, h->mesh, u, du, dt, h->ws, nthreads);
+        rhs_parabolic(h->basis, h->eq, h->ns, h->opt, h->mesh, u, du, dt, h->ws, nthreads, bd);
         return;
     }
     if (!h->curved) {
@@ -156,11 +156,27 @@ int oracle_mortar_operators(int N, double* out) {
 
 // compressible Navier-Stokes: dynamic viscosity mu and Prandtl number (the handle's gamma)
 int oracle_set_parabolic(oracle_handle* h, double mu, double Pr) {
-    if (h->curved || h->mesh.n_boundaries > 0) return 1;
+    if (h->curved) return 1;
     h->parabolic = true;
     h->ns.gamma = h->eq.gamma;
     h->ns.mu = mu;
     h->ns.Pr = Pr;
+    return 0;
+}
+
+// per boundary: 0 time-averaged Dirichlet, 1 slip wall vertical, 2 slip wall horizontal
+int oracle_set_boundary_kinds(oracle_handle* h, const int32_t* kinds) {
+    if (h->curved) return 1;
+    h->mesh.boundary_kind.assign(kinds, kinds + h->mesh.n_boundaries);
+    return 0;
+}
+
+// Navier-Stokes walls per boundary (1 no-slip adiabatic, 2 no-slip isothermal) and their data [3, l, B]
+int oracle_set_walls(oracle_handle* h, const int32_t* kinds, const double* data) {
+    if (h->curved) return 1;
+    const size_t B = h->mesh.n_boundaries, n = h->basis.n;
+    h->ns.wall_kind.assign(kinds, kinds + B);
+    h->ns.wall.assign(data, data + 3 * n * B);
     return 0;
 }
 

@@ -53,6 +53,8 @@ def lib():
         L.oracle_create_curved.argtypes = [i32, dbl, i32, i32, i32, P, P, i32, P, P, P, P, P]
         L.oracle_create_curved.restype = P
         L.oracle_set_limiter.argtypes = [P, i32, P, P]
+        L.oracle_set_boundary_kinds.argtypes = [P, P]
+        L.oracle_set_walls.argtypes = [P, P, P]
         L.oracle_apply_limiter.argtypes = [P, P]
         L.oracle_last_error.argtypes = [P]
         L.oracle_last_error.restype = ctypes.c_char_p
@@ -153,6 +155,17 @@ class Oracle:
     def set_parabolic(self, mu: float, Pr: float = 0.72):
         """Compressible Navier-Stokes with dynamic viscosity mu and Prandtl number Pr (periodic TreeMesh)."""
         assert lib().oracle_set_parabolic(self.h, float(mu), float(Pr)) == 0
+
+    def set_boundary_kinds(self, kinds):
+        """Per boundary (the mesh's boundary order): 0 Dirichlet, 1 slip wall vertical, 2 slip wall horizontal."""
+        self._kkeep = np.ascontiguousarray(kinds, dtype=np.int32)
+        assert lib().oracle_set_boundary_kinds(self.h, _p(self._kkeep)) == 0
+
+    def set_walls(self, kinds, data):
+        """Navier-Stokes walls per boundary (1 no-slip adiabatic, 2 no-slip isothermal), data [B, l, 3] =
+        (v1, v2, q or T) per boundary node."""
+        self._wkeep = (np.ascontiguousarray(kinds, dtype=np.int32), np.ascontiguousarray(data, dtype=np.float64))
+        assert lib().oracle_set_walls(self.h, _p(self._wkeep[0]), _p(self._wkeep[1])) == 0
 
     def set_positivity_limiter(self, thresholds=(5.0e-6, 5.0e-6), variables=(0, 1)):
         """Zhang-Shu limiter pairs applied after every step of ``steps`` (variables: 0 density, 1 pressure,

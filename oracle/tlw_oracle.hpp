@@ -338,6 +338,8 @@ struct TreeMesh {
     // boundaries (src/solvers/dgsem_tree/dg_2d.jl:1328-1454); neighbor_side 1: element on the -side
     int n_boundaries = 0;
     std::vector<int32_t> boundary_element, boundary_orientation, boundary_side, boundary_direction;
+    // condition per boundary (empty: all Dirichlet): BC_DIRICHLET, BC_SLIP_WALL_VERTICAL, BC_SLIP_WALL_HORIZONTAL
+    std::vector<int32_t> boundary_kind;
     // L2 mortars (Trixi mortars container): lower / upper small element, large element (0-based),
     // large_sides 1: large element on the -side, 2: on the +side; orientation 1 (x) / 2 (y)
     int n_mortars = 0;
@@ -831,6 +833,31 @@ struct BoundaryData {
     const double* u_now = nullptr;      // [v, l, B]     state at t
 };
 
+enum BoundaryKind { BC_DIRICHLET = 0, BC_SLIP_WALL_VERTICAL = 1, BC_SLIP_WALL_HORIZONTAL = 2 };
+
+inline int boundary_kind(const TreeMesh& m, int k) { return m.boundary_kind.empty() ? BC_DIRICHLET : m.boundary_kind[k]; }
+
+inline bool has_dirichlet_boundaries(const TreeMesh& m) {
+    for (int k = 0; k < m.n_boundaries; ++k)
+        if (boundary_kind(m, k) == BC_DIRICHLET) return true;
+    return false;
+}
+
+// Slip walls (boundary_condition_slip_wall_vertical / _horizontal, src/equations/equations.jl:95-135): the
+// exterior normal flux, U and u are the inner ones mirrored in the wall's normal momentum.
+inline void slip_wall_exterior(int kind, const double* Fi, const double* Ui, const double* ui, double* Fo, double* Uo,
+                               double* uo) {
+    if (kind == BC_SLIP_WALL_VERTICAL) {
+        Fo[0] = -Fi[0]; Fo[1] = Fi[1]; Fo[2] = -Fi[2]; Fo[3] = -Fi[3];
+        Uo[0] = Ui[0]; Uo[1] = -Ui[1]; Uo[2] = Ui[2]; Uo[3] = Ui[3];
+        uo[0] = ui[0]; uo[1] = -ui[1]; uo[2] = ui[2]; uo[3] = ui[3];
+    } else {
+        Fo[0] = -Fi[0]; Fo[1] = -Fi[1]; Fo[2] = Fi[2]; Fo[3] = -Fi[3];
+        Uo[0] = Ui[0]; Uo[1] = Ui[1]; Uo[2] = -Ui[2]; Uo[3] = Ui[3];
+        uo[0] = ui[0]; uo[1] = ui[1]; uo[2] = -ui[2]; uo[3] = ui[3];
+    }
+}
+
 inline void calc_boundary_flux(const Basis& b, const Euler& eq, const Options& opt, const TreeMesh& m,
                                const double* u, const BoundaryData& bd, double scaling_factor, Workspace& ws) {
     // prolong2boundaries! (dg_2d.jl:1328-1376) + calc_adv_boundary_flux_by_direction! (:1411-1454)
@@ -840,6 +867,7 @@ inline void calc_boundary_flux(const Basis& b, const Euler& eq, const Options& o
         const int o = m.boundary_orientation[k];
         const int side = m.boundary_side[k];
         const int dir = m.boundary_direction[k];   // 1..4 (Trixi direction)
+        const int kind = boundary_kind(m, k);
         for (int l = 0; l < n; ++l) {
             double ui[NV], Ui[NV], Fi[NV];
             int i, j;
@@ -850,6 +878,16 @@ inline void calc_boundary_flux(const Basis& b, const Euler& eq, const Options& o
                 Fi[v] = ws.F[idx_F(n, v, o - 1, i, j, e)];
             }
             double Uo[NV] = {0, 0, 0, 0}, Fo[NV] = {0, 0, 0, 0}, uo[NV];
+            if (kind != BC_DIRICHLET) {
+                slip_wall_exterior(kind, Fi, Ui, ui, Fo, Uo, uo);
+                double Fn[NV];
+                if (dir % 2 == 0)
+                    lw_surface_flux(eq, opt.flux_kind, opt.speed_kind, Fi, Fo, Ui, Uo, ui, uo, o, Fn, ws.bad);
+                else
+                    lw_surface_flux(eq, opt.flux_kind, opt.speed_kind, Fo, Fi, Uo, Ui, uo, ui, o, Fn, ws.bad);
+                for (int v = 0; v < NV; ++v) ws.surface_flux_values[v + NV * (l + n * ((dir - 1) + 4 * (size_t)e))] = Fn[v];
+                continue;
+            }
             for (int q = 0; q < n; ++q) {
                 const double* ub = bd.u_levels + NV * (q + (size_t)n * (l + (size_t)n * k));
                 double fb[NV];
@@ -1193,8 +1231,9 @@ inline void rhs(const Basis& b, const Euler& eq, const Options& opt, const TreeM
     else
         calc_interface_flux(b, eq, opt, m, ws, nthreads);
     if (m.n_boundaries > 0) {
-        if (!bd || !bd->u_levels || !bd->u_now) throw std::invalid_argument("boundary data missing");
-        calc_boundary_flux(b, eq, opt, m, u, *bd, kind == 1 ? 0.5 : 1.0, ws);
+        if (has_dirichlet_boundaries(m) && (!bd || !bd->u_levels || !bd->u_now))
+            throw std::invalid_argument("boundary data missing");
+        calc_boundary_flux(b, eq, opt, m, u, bd ? *bd : BoundaryData{}, kind == 1 ? 0.5 : 1.0, ws);
     }
     if (m.n_mortars > 0) {
         if (opt.shock_capturing) throw std::invalid_argument("mortars with shock capturing are not restated");

@@ -24,10 +24,43 @@
 
 namespace tlwo {
 
+// Wall conditions of the parabolic part per boundary: BoundaryConditionNavierStokesWall(NoSlip(v), Adiabatic(q))
+// or (NoSlip(v), Isothermal(T)), src/equations/compressible_navier_stokes_2d.jl:81-124; wall data per
+// boundary node [3, l, B] = (v1, v2, q or T) at the boundary's node coordinates.
+enum WallKind { WALL_NONE = 0, WALL_ADIABATIC = 1, WALL_ISOTHERMAL = 2 };
+
 struct NavierStokes {
     double gamma = 1.4, mu = 0.0, Pr = 0.72;
+    std::vector<int32_t> wall_kind;   // [B]
+    std::vector<double> wall;         // [3, l, B]
     double kappa() const { return gamma / ((gamma - 1.0) * Pr); }
 };
+
+// the face node (i, j) of boundary k's element, face index l
+inline void boundary_node(const TreeMesh& m, int n, int k, int l, int& i, int& j) {
+    const int o = m.boundary_orientation[k], side = m.boundary_side[k];
+    if (o == 1) { i = side == 1 ? n - 1 : 0; j = l; } else { i = l; j = side == 1 ? n - 1 : 0; }
+}
+
+// the gradient's boundary value (operator Gradient): prim2cons(rho_inner, v_wall, p) with p the inner
+// pressure (Adiabatic, :113-124) or rho_inner T_wall (Isothermal, :92-100)
+inline void wall_gradient_value(const NavierStokes& ns, int kind, const double* w, const double* ui, double* uo) {
+    const double rho = ui[0];
+    const double p = kind == WALL_ADIABATIC
+                         ? (ns.gamma - 1.0) * (ui[3] - 0.5 * (ui[1] * ui[1] + ui[2] * ui[2]) / rho)
+                         : rho * w[2];
+    uo[0] = rho;
+    uo[1] = rho * w[0];
+    uo[2] = rho * w[1];
+    uo[3] = p / (ns.gamma - 1.0) + 0.5 * rho * (w[0] * w[0] + w[1] * w[1]);
+}
+
+// the viscous boundary flux (operator Divergence) from the inner normal viscous flux trace: Adiabatic keeps
+// its momentum components and sets the energy flux to v_wall . tau_n + q (:81-90); Isothermal keeps it (:102-108)
+inline void wall_viscous_flux(int kind, const double* w, const double* fi, double* fo) {
+    for (int v = 0; v < NV; ++v) fo[v] = fi[v];
+    if (kind == WALL_ADIABATIC) fo[3] = w[0] * fi[1] + w[1] * fi[2] + w[2];
+}
 
 // viscous flux pair of state u with conservative gradients gx, gy
 inline void viscous_fluxes(const NavierStokes& ns, const double* u, const double* gx, const double* gy, double* fv,
@@ -54,8 +87,8 @@ inline void viscous_fluxes(const NavierStokes& ns, const double* u, const double
 }
 
 // BR1 gradients of the conservative variables: g_d = J^{-1} (Dhat u + lifted interface averages)
-inline void gradients_br1(const Basis& b, const TreeMesh& m, const double* u, std::vector<double>& gx,
-                          std::vector<double>& gy, int nthreads = 1) {
+inline void gradients_br1(const Basis& b, const TreeMesh& m, const NavierStokes& ns, const double* u,
+                          std::vector<double>& gx, std::vector<double>& gy, int nthreads = 1) {
     const int n = b.n, nn = n * n;
     const size_t ndof = (size_t)NV * nn * m.n_elements;
     gx.assign(ndof, 0.0);
@@ -84,6 +117,22 @@ inline void gradients_br1(const Basis& b, const TreeMesh& m, const double* u, st
                 const double us = 0.5 * (u[idx_u(n, v, iL, jL, le)] + u[idx_u(n, v, iR, jR, re)]);
                 g[idx_u(n, v, iL, jL, le)] += us * b.inv_w_last;
                 g[idx_u(n, v, iR, jR, re)] -= us * b.inv_w_first;
+            }
+        }
+    }
+    // boundaries (Trixi calc_boundary_flux_by_direction_gradient!): the wall value itself is the flux
+    for (int k = 0; k < m.n_boundaries; ++k) {
+        const int e = m.boundary_element[k], o = m.boundary_orientation[k], side = m.boundary_side[k];
+        std::vector<double>& g = o == 1 ? gx : gy;
+        for (int l = 0; l < n; ++l) {
+            int i, j;
+            boundary_node(m, n, k, l, i, j);
+            double ui[NV], uo[NV];
+            for (int v = 0; v < NV; ++v) ui[v] = u[idx_u(n, v, i, j, e)];
+            wall_gradient_value(ns, ns.wall_kind[k], &ns.wall[3 * (l + (size_t)n * k)], ui, uo);
+            for (int v = 0; v < NV; ++v) {
+                if (side == 1) g[idx_u(n, v, i, j, e)] += uo[v] * b.inv_w_last;    // the boundary at the +face
+                else g[idx_u(n, v, i, j, e)] -= uo[v] * b.inv_w_first;             // at the -face
             }
         }
     }
@@ -215,12 +264,15 @@ inline void lw_volume_element_parabolic(const Basis& b, const Euler& eq, const N
 
 // du = rhs(u) for compressible Navier-Stokes on a periodic TreeMesh{2} (LW)
 inline void rhs_parabolic(const Basis& b, const Euler& eq, const NavierStokes& ns, const Options& opt,
-                          const TreeMesh& m, const double* u, double* du, double dt, Workspace& ws, int nthreads = 1) {
+                          const TreeMesh& m, const double* u, double* du, double dt, Workspace& ws, int nthreads = 1,
+                          const BoundaryData* bd = nullptr) {
     const int n = b.n, nn = n * n;
     const size_t ndof = (size_t)NV * nn * m.n_elements;
-    if (m.n_boundaries > 0 || m.n_mortars > 0) throw std::invalid_argument("parabolic oracle: periodic conforming mesh");
+    if (m.n_mortars > 0) throw std::invalid_argument("parabolic oracle: conforming mesh");
+    if (m.n_boundaries > 0 && ns.wall_kind.size() != (size_t)m.n_boundaries)
+        throw std::invalid_argument("parabolic oracle: boundaries need wall conditions");
     std::vector<double> gx, gy, Fv(2 * ndof);
-    gradients_br1(b, m, u, gx, gy, nthreads);
+    gradients_br1(b, m, ns, u, gx, gy, nthreads);
     ws.U.assign(ndof, 0.0);
     ws.F.assign(2 * ndof, 0.0);
     ws.surface_flux_values.assign((size_t)NV * n * 4 * m.n_elements, 0.0);
@@ -255,6 +307,24 @@ inline void rhs_parabolic(const Basis& b, const Euler& eq, const NavierStokes& n
         }
     }
     ws.bad = bad;
+    if (m.n_boundaries > 0) {
+        // the advective boundary flux (calc_boundary_flux!), then minus the wall's viscous flux
+        // (prolong2boundaries_visc_lw! + calc_boundary_flux_divergence_lw!, dg_2d_parabolic.jl:1951-2084)
+        if (has_dirichlet_boundaries(m) && (!bd || !bd->u_levels || !bd->u_now))
+            throw std::invalid_argument("boundary data missing");
+        calc_boundary_flux(b, eq, opt, m, u, bd ? *bd : BoundaryData{}, 1.0, ws);
+        for (int k = 0; k < m.n_boundaries; ++k) {
+            const int e = m.boundary_element[k], o = m.boundary_orientation[k], dir = m.boundary_direction[k];
+            for (int l = 0; l < n; ++l) {
+                int i, j;
+                boundary_node(m, n, k, l, i, j);
+                double fi[NV], fo[NV];
+                for (int v = 0; v < NV; ++v) fi[v] = Fv[idx_F(n, v, o - 1, i, j, e)];
+                wall_viscous_flux(ns.wall_kind[k], &ns.wall[3 * (l + (size_t)n * k)], fi, fo);
+                for (int v = 0; v < NV; ++v) ws.surface_flux_values[v + NV * (l + n * ((dir - 1) + 4 * (size_t)e))] -= fo[v];
+            }
+        }
+    }
     surface_integral_and_jacobian(b, m, du, ws, nthreads);
 }
 

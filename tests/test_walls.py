@@ -1,0 +1,260 @@
+"""Walls on a non-periodic TreeMesh{2}: the LW slip walls of the advective part
+(boundary_condition_slip_wall_vertical / _horizontal, src/equations/equations.jl:95-135) and the Navier-Stokes
+no-slip walls of the parabolic part (BoundaryConditionNavierStokesWall(NoSlip, Adiabatic | Isothermal),
+src/equations/compressible_navier_stokes_2d.jl:81-124; src/solvers/dgsem_tree/dg_2d_parabolic.jl:1951-2084),
+as the reference's TreeMesh lid-driven cavity (examples/tree_2d_dgsem/elixir_navierstokes_lid_driven_cavity.jl)
+uses them. CPU: the oracle's rest-state preservation and conservation; GPU: libtlw against the oracle (1e-12
+relative L2 per variable) and a cavity run through solve_lwfr."""
+import os
+
+import numpy as np
+import pytest
+
+NTH = os.cpu_count() or 1
+GAMMA = 1.4
+MA = 0.1
+
+
+def rel_l2(a, b):
+    a = a.reshape(-1, 4)
+    b = b.reshape(-1, 4)
+    return np.linalg.norm(a - b, axis=0) / np.maximum(np.linalg.norm(b, axis=0), 1e-300)
+
+
+def box(tl, level=3):
+    return tl.TreeMesh((-1.0, -1.0), (1.0, 1.0), level, periodicity=False)
+
+
+def state(tl, mesh, N, amp=0.1, p0=None):
+    """rho = 1 + smooth bump, v = amp (sin(pi x) cos(pi y / 2), -cos(pi x / 2) sin(pi y)), p = p0 (default
+    the cavity's 1 / (Ma^2 gamma)) + bump."""
+    eq = tl.CompressibleEulerEquations2D(GAMMA)
+    x, y = mesh.node_coordinates(N)
+    p0 = 1.0 / (MA ** 2 * GAMMA) if p0 is None else p0
+    rho = 1.0 + 0.2 * np.exp(-4 * ((x - 0.2) ** 2 + (y + 0.1) ** 2))
+    v1 = amp * np.sin(np.pi * x) * np.cos(0.5 * np.pi * y)
+    v2 = -amp * np.cos(0.5 * np.pi * x) * np.sin(np.pi * y) + 0.3 * amp
+    p = p0 * (1.0 + 0.05 * np.exp(-3 * ((x + 0.3) ** 2 + (y - 0.2) ** 2)))
+    U = eq.prim2cons(rho, v1, v2, p)
+    return np.ascontiguousarray(np.transpose(U, (2, 1, 0, 3))).reshape(-1)
+
+
+def rest(tl, mesh, N):
+    n = mesh.n_elements * (N + 1) ** 2
+    p0 = 1.0 / (MA ** 2 * GAMMA)
+    return np.tile(np.array([1.0, 0.0, 0.0, p0 / (GAMMA - 1.0)]), n)
+
+
+def kinds_by_direction(mesh, per_dir):
+    return np.repeat(np.asarray(per_dir, dtype=np.int32), np.asarray(mesh.n_boundaries_per_direction))
+
+
+SLIP = (1, 1, 2, 2)        # x_neg, x_pos vertical; y_neg, y_pos horizontal
+
+
+def cavity_walls(mesh, N, lid=1.0, kind=1, T=None):
+    """Wall kinds and data [B, l, 3]: no-slip everywhere, the lid (y_pos) moving with v1 = lid."""
+    B = mesh.n_boundaries
+    per = np.asarray(mesh.n_boundaries_per_direction)
+    data = np.zeros((B, N + 1, 3))
+    data[per[:3].sum():, :, 0] = lid
+    if kind == 2:
+        data[:, :, 2] = T
+    return np.full(B, kind, dtype=np.int32), data
+
+
+def masses(u, mesh, N):
+    from trixilw.basis import gauss_lobatto
+    _, w = gauss_lobatto(N)
+    return np.einsum("ejiv,e,j,i->v", u.reshape(-1, N + 1, N + 1, 4), (1.0 / mesh.inverse_jacobian) ** 2, w, w)
+
+
+# ---------------------------------------------------------------------------------------------- CPU
+@pytest.mark.parametrize("N", [2, 3, 4])
+def test_oracle_slip_walls_rest_and_conservation(oracle_mod, tl, N):
+    m = box(tl)
+    o = oracle_mod.Oracle(m, N)
+    o.set_boundary_kinds(kinds_by_direction(m, SLIP))
+    u0 = rest(tl, m, N)
+    assert np.abs(o.rhs(u0, 0.0, 1e-3)).max() < 1e-10 * u0.max()
+    u = state(tl, m, N, p0=1.0)
+    du = o.rhs(u, 0.0, o.max_dt(u, 0.3))
+    tot = masses(du, m, N)
+    # no mass or energy crosses a slip wall; the walls' pressure changes the momenta
+    assert abs(tot[0]) < 1e-12 and abs(tot[3]) < 1e-11
+    assert abs(tot[1]) > 1e-6
+
+
+@pytest.mark.parametrize("N", [3, 4])
+def test_oracle_navier_stokes_walls(oracle_mod, tl, N):
+    m = box(tl)
+    o = oracle_mod.Oracle(m, N)
+    o.set_parabolic(0.01)
+    o.set_boundary_kinds(kinds_by_direction(m, SLIP))
+    o.set_walls(*cavity_walls(m, N, lid=0.0))
+    u0 = rest(tl, m, N)
+    assert np.abs(o.rhs(u0, 0.0, 1e-3)).max() < 1e-9 * u0.max()
+    # the moving lid shears the fluid at rest; mass stays, the lid does work (energy changes)
+    o.set_walls(*cavity_walls(m, N, lid=1.0))
+    du = o.rhs(u0, 0.0, 1e-3)
+    tot = masses(du, m, N)
+    assert abs(tot[0]) < 1e-12 and tot[1] > 0.0
+    nn = (N + 1) ** 2
+    top = np.unique(m.boundary_neighbor_ids[np.asarray(m.n_boundaries_per_direction)[:3].sum():] - 1)
+    assert du.reshape(-1, nn, 4)[top, :, 1].sum() > 0.0
+    # isothermal walls at the fluid's temperature behave like the adiabatic ones at rest
+    T = (1.0 / (MA ** 2 * GAMMA)) / 1.0
+    o.set_walls(*cavity_walls(m, N, lid=0.0, kind=2, T=T))
+    assert np.abs(o.rhs(u0, 0.0, 1e-3)).max() < 1e-9 * u0.max()
+
+
+def test_python_boundary_condition_mapping(tl):
+    from trixilw.semidiscretization import digest_boundary_conditions
+    bcs = {"x_neg": tl.boundary_condition_slip_wall_vertical, "x_pos": tl.boundary_condition_slip_wall_vertical,
+           "y_neg": tl.boundary_condition_slip_wall_horizontal, "y_pos": tl.boundary_condition_slip_wall_horizontal}
+    d = digest_boundary_conditions(bcs)
+    assert [b.code for b in d] == [1, 1, 2, 2]
+    with pytest.raises(ValueError):
+        digest_boundary_conditions({"x_neg": tl.boundary_condition_slip_wall_vertical})
+    wall = tl.BoundaryConditionNavierStokesWall(tl.NoSlip(lambda x, y, t, e: (1.0, 0.0)),
+                                                tl.Adiabatic(lambda x, y, t, e: 0.0))
+    x = np.linspace(0, 1, 5)
+    dat = wall.data(x, 0 * x, 0.0, None)
+    assert dat.shape == (5, 3) and np.all(dat[:, 0] == 1.0) and wall.code == 1
+
+
+# ---------------------------------------------------------------------------------------------- GPU
+def make_semi(tl, mesh, N, td="lw", flux=None, mu=None, lid=1.0, hyperbolic=None):
+    eq = tl.CompressibleEulerEquations2D(GAMMA)
+    tdo = tl.LW() if td == "lw" else tl.MDRK()
+    solver = tl.DGSEM(N, flux or tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tdo))
+    bc = hyperbolic or {"x_neg": tl.boundary_condition_slip_wall_vertical,
+                        "x_pos": tl.boundary_condition_slip_wall_vertical,
+                        "y_neg": tl.boundary_condition_slip_wall_horizontal,
+                        "y_pos": tl.boundary_condition_slip_wall_horizontal}
+    if mu is None:
+        return tl.SemidiscretizationHyperbolic(mesh, tdo, eq, tl.ConstantState(), solver, boundary_conditions=bc)
+    eq_par = tl.CompressibleNavierStokesDiffusion2D(eq, mu=mu, Prandtl=0.72,
+                                                    gradient_variables=tl.GradientVariablesConservative())
+    heat = tl.Adiabatic(lambda x, y, t, e: 0.0)
+    cavity = tl.BoundaryConditionNavierStokesWall(tl.NoSlip(lambda x, y, t, e: (0.0, 0.0)), heat)
+    lidbc = tl.BoundaryConditionNavierStokesWall(tl.NoSlip(lambda x, y, t, e: (lid, 0.0)), heat)
+    par = {"x_neg": cavity, "y_neg": cavity, "y_pos": lidbc, "x_pos": cavity}
+    return tl.SemidiscretizationHyperbolicParabolic(mesh, tdo, (eq, eq_par), tl.ConstantState(), solver,
+                                                    boundary_conditions=(bc, par))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,td,flux", [(3, "lw", "rusanov"), (4, "lw", "rusanov"), (4, "lw", "hll"),
+                                       (5, "lw", "rusanov"), (4, "mdrk", "rusanov"), (2, "lw", "rusanov")])
+def test_gpu_slip_walls_match_oracle(oracle_mod, tl, N, td, flux):
+    m = box(tl)
+    semi = make_semi(tl, m, N, td, tl.flux_hll if flux == "hll" else None)
+    u0 = state(tl, m, N, p0=1.0)
+    o = oracle_mod.Oracle(m, N, flux_kind=0 if flux == "rusanov" else 1)
+    o.set_boundary_kinds(kinds_by_direction(m, SLIP))
+    dt = o.max_dt(u0, 0.3)
+    semi.cache["dt"][0] = dt
+    if td == "lw":
+        du_gpu = np.empty_like(u0)
+        tl.rhs(du_gpu, u0, semi, 0.0)
+        assert np.all(rel_l2(u0 + dt * du_gpu, u0 + dt * o.rhs(u0, 0.0, dt)) < 1e-12)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, semi.time_discretization, (0.0, 1e9)))
+    integ.set_state(u0, 0.0)
+    integ.step(8, 0.3, use_graph=True)
+    integ.sync_time()
+    u_cpu = u0.copy()
+    s, t = o.steps(u_cpu, 8, 0.3, 0.0, 1e9, kind=0 if td == "lw" else 1, nthreads=NTH)
+    assert s == integ.iter == 8 and integ.t == pytest.approx(t, rel=1e-12)
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-12)
+
+
+@pytest.mark.gpu
+def test_gpu_mixed_dirichlet_and_slip_walls(oracle_mod, tl):
+    """Dirichlet data on x_neg / x_pos (the state itself), slip walls on y_neg / y_pos."""
+    N = 4
+    m = box(tl)
+    eq = tl.CompressibleEulerEquations2D(GAMMA)
+    ic = tl.ConstantState(rho=1.0, v1=0.3, v2=0.0, p=1.0)
+    bc = {"x_neg": tl.BoundaryConditionDirichlet(ic), "x_pos": tl.BoundaryConditionDirichlet(ic),
+          "y_neg": tl.boundary_condition_slip_wall_horizontal, "y_pos": tl.boundary_condition_slip_wall_horizontal}
+    semi = make_semi(tl, m, N, hyperbolic=bc)
+    u0 = state(tl, m, N, p0=1.0)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, semi.time_discretization, (0.0, 1e9)))
+    semi._prepare_boundaries(0.0, 0.0, 1.0)
+    integ.set_state(u0, 0.0)
+    integ.step(6, 0.3, use_graph=True)
+    integ.sync_time()
+    o = oracle_mod.Oracle(m, N)
+    o.set_boundary_kinds(kinds_by_direction(m, (0, 0, 2, 2)))
+    n = N + 1
+    xy = m.boundary_node_coordinates(N)
+    now = np.transpose(ic(xy[0], xy[1], 0.0, eq), (1, 0, 2))           # [B, l, v]
+    levels = np.repeat(now[:, :, None, :], n, axis=2)                   # [B, l, q, v]
+    o.set_boundary_data(levels, now)
+    u_cpu = u0.copy()
+    o.steps(u_cpu, 6, 0.3, 0.0, 1e9, nthreads=NTH)
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,kind", [(3, 1), (4, 1), (5, 1), (4, 2)])
+def test_gpu_navier_stokes_walls_match_oracle(oracle_mod, tl, N, kind):
+    m = box(tl)
+    mu = 0.01
+    semi = make_semi(tl, m, N, mu=mu)
+    T = 1.0 / (MA ** 2 * GAMMA)
+    if kind == 2:   # isothermal walls through the C ABI directly
+        k, d = cavity_walls(m, N, lid=1.0, kind=2, T=T)
+        tl._lib.check(semi.handle, tl._lib.lib().tlw_set_parabolic_walls(
+            semi.handle, k.ctypes.data, np.ascontiguousarray(d).ctypes.data))
+    u0 = state(tl, m, N)
+    o = oracle_mod.Oracle(m, N)
+    o.set_parabolic(mu)
+    o.set_boundary_kinds(kinds_by_direction(m, SLIP))
+    o.set_walls(*cavity_walls(m, N, lid=1.0, kind=kind, T=T))
+    dt = o.max_dt(u0, 0.3)
+    semi.cache["dt"][0] = dt
+    du_gpu = np.empty_like(u0)
+    tl.rhs(du_gpu, u0, semi, 0.0)
+    du_cpu = o.rhs(u0, 0.0, dt)
+    assert np.all(rel_l2(u0 + dt * du_gpu, u0 + dt * du_cpu) < 1e-12)
+    assert np.all(rel_l2(du_gpu, du_cpu) < 1e-10)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, semi.time_discretization, (0.0, 1e9)))
+    integ.set_state(u0, 0.0)
+    integ.step(10, 0.3, use_graph=True)
+    integ.sync_time()
+    u_cpu = u0.copy()
+    s, t = o.steps(u_cpu, 10, 0.3, 0.0, 1e9, nthreads=NTH)
+    assert s == integ.iter == 10 and integ.t == pytest.approx(t, rel=1e-12)
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-12)
+
+
+@pytest.mark.gpu
+def test_gpu_tree_lid_driven_cavity_runs(tl):
+    """The reference's TreeMesh lid-driven cavity (level 4, N = 4, mu = 0.001, Pr = 0.72, slip walls for the
+    advective part, no-slip adiabatic walls with the lid at v1 = 1) for 2000 steps at CFL 0.98: it stays
+    admissible, conserves mass, and the lid drags the fluid below it along (u > 0 under the lid, total
+    x-momentum gained from the lid)."""
+    N = 4
+    m = box(tl, 4)
+    semi = make_semi(tl, m, N, mu=0.001)
+    u0 = rest(tl, m, N)
+    ode = tl.semidiscretize(semi, tl.LW(), (0.0, 1e9))
+    ode.u0_ode[:] = u0
+    integ = tl.LWIntegrator(ode)
+    integ.set_state(u0, 0.0)
+    integ.step(2000, 0.98 * 5 * 0.103, use_graph=True)
+    integ.sync_time()
+    assert integ.iter == 2000
+    u = integ.get_state()
+    assert np.all(np.isfinite(u))
+    np.testing.assert_allclose(masses(u, m, N)[0], masses(u0, m, N)[0], rtol=1e-12)
+    x, y = m.node_coordinates(N)
+    xs = np.transpose(x, (2, 1, 0)).reshape(-1)
+    ys = np.transpose(y, (2, 1, 0)).reshape(-1)
+    uu = u.reshape(-1, 4)
+    v1 = uu[:, 1] / uu[:, 0]
+    near_axis = np.abs(xs) < 0.07
+    assert v1[near_axis & (ys > 0.9)].mean() > 0.05
+    assert masses(u, m, N)[1] > 0.0

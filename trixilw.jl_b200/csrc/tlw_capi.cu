@@ -53,6 +53,10 @@ void free_mesh(tlw_handle* h) {
     dfree(h->d_xl); dfree(h->d_xr); dfree(h->d_yl); dfree(h->d_yr);
     dfree(h->d_b_elem); dfree(h->d_b_dir); dfree(h->d_bx); dfree(h->d_by);
     dfree(h->d_levels); dfree(h->d_now);
+    if (h->d_bkind) { cudaFree(h->d_bkind); h->d_bkind = nullptr; }
+    if (h->d_wkind) { cudaFree(h->d_wkind); h->d_wkind = nullptr; }
+    dfree(h->d_wall);
+    h->bnd_dirichlet = true;
     dfree(h->d_state[0]); dfree(h->d_state[1]);
     dfree(h->d_us); dfree(h->d_in); dfree(h->d_in2); dfree(h->d_out);
     dfree(h->d_tU); dfree(h->d_tF); dfree(h->d_U2); dfree(h->d_F2);
@@ -153,6 +157,11 @@ struct Launch {
                 grad_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(
                     u, h->d_xl, h->d_xr, h->nx, h->d_yl, h->d_yr, h->ny, h->d_inv_jac, h->h_basis.inv_w_first,
                     h->h_basis.inv_w_last, h->d_gx, h->d_gy);
+            const long long tb = (long long)h->nb * (N + 1);
+            if (tb)
+                grad_boundary_kernel<N><<<(unsigned)((tb + 127) / 128), 128, 0, s>>>(
+                    u, h->d_b_elem, h->d_b_dir, h->d_wkind, h->d_wall, (int)h->nb, h->d_inv_jac, h->opts.gamma,
+                    h->h_basis.inv_w_first, h->h_basis.inv_w_last, h->d_gx, h->d_gy);
             ParArgs pa{};
             pa.u = u;
             pa.gx = h->d_gx;
@@ -314,6 +323,36 @@ void enqueue_limiter(tlw_handle* h, double* u, int reps, unsigned long long* slo
     dispatch<Lim>(h->N, h->stream, a);
 }
 
+BndArgs boundary_args(tlw_handle* h, int stage, int mode, const double* u_jump, double* out, const double* dt_ptr) {
+    BndArgs ba{};
+    ba.u = u_jump;
+    ba.out = out;
+    ba.tU = h->d_tU;
+    ba.tF = h->d_tF;
+    ba.element = h->d_b_elem;
+    ba.direction = h->d_b_dir;
+    ba.levels = h->d_levels;
+    ba.now = h->d_now;
+    ba.inv_jac = h->d_inv_jac;
+    ba.dt = dt_ptr;
+    ba.step_mode = mode == MODE_STEP;
+    ba.scaling_factor = stage == TLW_STAGE_MDRK1 ? 0.5 : 1.0;
+    ba.gamma = h->opts.gamma;
+    ba.flux_kind = h->opts.surface_flux;
+    ba.speed_kind = h->opts.max_speed;
+    ba.inv_w_first = h->h_basis.inv_w_first;
+    ba.inv_w_last = h->h_basis.inv_w_last;
+    ba.weights = h->d_basis->weights;
+    ba.status = &h->d_step->status;
+    ba.kind = h->d_bkind;
+    if (h->parabolic && h->nb > 0) {
+        ba.tFv = h->d_tFv;
+        ba.wall_kind = h->d_wkind;
+        ba.wall = h->d_wall;
+    }
+    return ba;
+}
+
 void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const double* u_jump, const double* u_base,
                  double* out, const double* dt_ptr, const PhaseEvents* ev = nullptr, bool alpha_ready = false) {
     if (h->sc && !alpha_ready) enqueue_indicator(h, u_jump, false);   // indicator of the instantaneous u
@@ -336,11 +375,16 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
         sp.inv_w_first = h->h_basis.inv_w_first;
         sp.inv_w_last = h->h_basis.inv_w_last;
         sp.status = &h->d_step->status;
+        BndArgs bp = boundary_args(h, stage, mode, u_jump, out, dt_ptr);
         sp.left = h->d_xl; sp.right = h->d_xr; sp.count = h->nx; sp.orientation = 1;
         dispatch<Ifc>(h->N, h->stream, sp);
+        bp.bidx = h->d_bx; bp.count = h->nbx; bp.orientation = 1;
+        dispatch<Bnd>(h->N, h->stream, bp);
         if (ev) cudaEventRecord(ev->after_x, h->stream);
         sp.left = h->d_yl; sp.right = h->d_yr; sp.count = h->ny; sp.orientation = 2;
         dispatch<Ifc>(h->N, h->stream, sp);
+        bp.bidx = h->d_by; bp.count = h->nby; bp.orientation = 2;
+        dispatch<Bnd>(h->N, h->stream, bp);
         if (ev) cudaEventRecord(ev->after_y, h->stream);
         return;
     }
@@ -426,26 +470,7 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     sa.w_last = h->h_basis.weights[h->n - 1];
     sa.cfl_slots = va.cfl_slots;
 
-    BndArgs ba{};
-    ba.u = u_jump;
-    ba.out = out;
-    ba.tU = h->d_tU;
-    ba.tF = h->d_tF;
-    ba.element = h->d_b_elem;
-    ba.direction = h->d_b_dir;
-    ba.levels = h->d_levels;
-    ba.now = h->d_now;
-    ba.inv_jac = h->d_inv_jac;
-    ba.dt = dt_ptr;
-    ba.step_mode = mode == MODE_STEP;
-    ba.scaling_factor = stage == TLW_STAGE_MDRK1 ? 0.5 : 1.0;
-    ba.gamma = h->opts.gamma;
-    ba.flux_kind = h->opts.surface_flux;
-    ba.speed_kind = h->opts.max_speed;
-    ba.inv_w_first = h->h_basis.inv_w_first;
-    ba.inv_w_last = h->h_basis.inv_w_last;
-    ba.weights = h->d_basis->weights;
-    ba.status = &h->d_step->status;
+    BndArgs ba = boundary_args(h, stage, mode, u_jump, out, dt_ptr);
 
     // x interfaces, x boundaries, y interfaces, y boundaries: corner nodes are shared only between
     // launches of different orientation, which the stream orders.
@@ -534,7 +559,10 @@ __global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
 int check_ready(tlw_handle* h) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
-    if (h->nb > 0 && !h->have_bdata) return fail(h, TLW_E_STATE, "mesh has boundaries: call tlw_set_boundary_data first");
+    if (h->nb > 0 && h->bnd_dirichlet && !h->have_bdata)
+        return fail(h, TLW_E_STATE, "mesh has Dirichlet boundaries: call tlw_set_boundary_data first");
+    if (h->parabolic && h->nb > 0 && !h->d_wkind)
+        return fail(h, TLW_E_STATE, "Navier-Stokes with boundaries: call tlw_set_parabolic_walls first");
     return TLW_OK;
 }
 
@@ -844,6 +872,47 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
     return TLW_OK;
 }
 
+int tlw_set_boundary_kinds(tlw_handle* h, const int32_t* kinds) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh || h->curved) return fail(h, TLW_E_STATE, "boundary kinds follow tlw_set_tree_mesh");
+    if (h->nb == 0) return TLW_OK;
+    if (!kinds) return fail(h, TLW_E_ARG, "kinds");
+    bool dirichlet = false;
+    for (int64_t k = 0; k < h->nb; ++k) {
+        if (kinds[k] < TLW_BC_DIRICHLET || kinds[k] > TLW_BC_SLIP_WALL_HORIZONTAL)
+            return fail(h, TLW_E_ARG, "boundary " + std::to_string(k + 1) + ": unknown kind");
+        dirichlet = dirichlet || kinds[k] == TLW_BC_DIRICHLET;
+    }
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    if (!h->d_bkind) TLW_CUDA(h, cudaMalloc(&h->d_bkind, (size_t)h->nb * sizeof(int)));
+    TLW_CUDA(h, cudaMemcpy(h->d_bkind, kinds, (size_t)h->nb * sizeof(int), cudaMemcpyHostToDevice));
+    h->bnd_dirichlet = dirichlet;
+    return TLW_OK;
+}
+
+int tlw_set_parabolic_walls(tlw_handle* h, const int32_t* kinds, const double* wall_data) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh || !h->parabolic) return fail(h, TLW_E_STATE, "walls follow tlw_set_parabolic");
+    if (h->nb == 0) return TLW_OK;
+    if (!kinds || !wall_data) return fail(h, TLW_E_ARG, "kinds / wall data");
+    for (int64_t k = 0; k < h->nb; ++k)
+        if (kinds[k] != TLW_WALL_NOSLIP_ADIABATIC && kinds[k] != TLW_WALL_NOSLIP_ISOTHERMAL)
+            return fail(h, TLW_E_ARG, "boundary " + std::to_string(k + 1) + ": unknown wall kind");
+    const size_t nd = (size_t)3 * h->n * h->nb;
+    for (size_t k = 0; k < nd; ++k)
+        if (!std::isfinite(wall_data[k])) return fail(h, TLW_E_ARG, "wall data must be finite");
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    if (!h->d_wkind) TLW_CUDA(h, cudaMalloc(&h->d_wkind, (size_t)h->nb * sizeof(int)));
+    if (!h->d_wall) TLW_CUDA(h, cudaMalloc(&h->d_wall, nd * sizeof(double)));
+    TLW_CUDA(h, cudaMemcpy(h->d_wkind, kinds, (size_t)h->nb * sizeof(int), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, cudaMemcpy(h->d_wall, wall_data, nd * sizeof(double), cudaMemcpyHostToDevice));
+    return TLW_OK;
+}
+
 int tlw_set_positivity_limiter(tlw_handle* h, int32_t count, const double* thresholds, const int32_t* variables) {
     if (!h) return TLW_E_ARG;
     if (count < 0 || count > TLW_LIMITER_MAX_PAIRS || (count > 0 && (!thresholds || !variables)))
@@ -873,8 +942,8 @@ int tlw_apply_positivity_limiter(tlw_handle* h) {
 int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh || h->curved) return fail(h, TLW_E_STATE, "the parabolic terms follow tlw_set_tree_mesh");
-    if (h->opts.time_discretization != TLW_LW || h->sc || h->N < 3 || h->nb > 0 || h->nmx + h->nmy > 0)
-        return fail(h, TLW_E_UNSUPPORTED, "Navier-Stokes: LW, FR volume integral, N >= 3, periodic conforming TreeMesh");
+    if (h->opts.time_discretization != TLW_LW || h->sc || h->N < 3 || h->nmx + h->nmy > 0)
+        return fail(h, TLW_E_UNSUPPORTED, "Navier-Stokes: LW, FR volume integral, N >= 3, conforming TreeMesh");
     if (!(mu >= 0.0) || !(prandtl > 0.0)) return fail(h, TLW_E_ARG, "mu / Prandtl");
     TLW_CUDA(h, cudaSetDevice(h->device));
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));

@@ -102,6 +102,12 @@ struct tlw_handle {
     // L2 mortars of a non-conforming TreeMesh: x-mortars [0, nmx), then y-mortars [nmx, nmx + nmy)
     int *d_ml = nullptr, *d_mu = nullptr, *d_mg = nullptr, *d_ms = nullptr;
     int nmx = 0, nmy = 0;
+    // boundary condition per boundary (BC_*; null: all Dirichlet) and whether any is Dirichlet
+    int* d_bkind = nullptr;
+    bool bnd_dirichlet = true;
+    // Navier-Stokes walls per boundary (WALL_*) and their data [3, l, B] (v1, v2, q or T)
+    int* d_wkind = nullptr;
+    double* d_wall = nullptr;
     // per element: the faces (0..3) through which it is the large element of a mortar, in mortar order
     // (bits 0-2 count, then 2 bits per mortar); for the positivity limiter's mortar pass
     int* d_mface = nullptr;

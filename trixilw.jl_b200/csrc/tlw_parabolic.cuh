@@ -146,6 +146,41 @@ static __global__ void __launch_bounds__(128) grad_interface_kernel(const double
     store4(pR, x);
 }
 
+// gradient boundary term (Trixi calc_boundary_flux_by_direction_gradient!): the wall value of
+// BoundaryConditionNavierStokesWall(NoSlip(v), Adiabatic | Isothermal) (compressible_navier_stokes_2d.jl:92-124),
+// prim2cons(rho_inner, v_wall, p) with p the inner pressure (adiabatic) or rho_inner T_wall (isothermal), is the
+// flux itself; x-boundaries lift into gx, y-boundaries into gy
+template <int N>
+static __global__ void __launch_bounds__(128) grad_boundary_kernel(const double* __restrict__ u, const int* element,
+                                                                   const int* direction, const int* wall_kind,
+                                                                   const double* __restrict__ wall, int B,
+                                                                   const double* __restrict__ inv_jac, double gamma,
+                                                                   double inv_w_first, double inv_w_last, double* gx,
+                                                                   double* gy) {
+    constexpr int n = N + 1, nn = n * n;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = t / n;
+    const int l = t - k * n;
+    if (k >= B) return;
+    const int e = __ldg(element + k), dir = __ldg(direction + k);
+    const int node = dir == 1 ? n * l : dir == 2 ? (n - 1) + n * l : dir == 3 ? l : l + n * (n - 1);
+    double ui[NV], x[NV];
+    load4(u + ((size_t)e * nn + node) * NV, ui);
+    const double* w = wall + 3 * ((size_t)k * n + l);
+    const double v1 = __ldg(w), v2 = __ldg(w + 1);
+    const double rho = ui[0];
+    const double p = __ldg(wall_kind + k) == WALL_ADIABATIC
+                         ? (gamma - 1.0) * (ui[3] - 0.5 * (ui[1] * ui[1] + ui[2] * ui[2]) / rho)
+                         : rho * __ldg(w + 2);
+    const double uo[NV] = {rho, rho * v1, rho * v2, p / (gamma - 1.0) + 0.5 * rho * (v1 * v1 + v2 * v2)};
+    double* g = (dir <= 2 ? gx : gy) + ((size_t)e * nn + node) * NV;
+    const double c = (dir % 2 == 0 ? inv_w_last : -inv_w_first) * __ldg(inv_jac + e);
+    load4_rw(g, x);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) x[v] = fma(c, uo[v], x[v]);
+    store4(g, x);
+}
+
 struct ParArgs {
     const double* u;
     const double* gx;

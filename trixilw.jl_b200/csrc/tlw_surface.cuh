@@ -169,7 +169,26 @@ struct BndArgs {
     double inv_w_first, inv_w_last;
     const double* weights;   // GLL weights (device)
     unsigned* status;
+    const int* kind;         // [B] BC_* per boundary, or null (all Dirichlet)
+    // compressible Navier-Stokes walls: the viscous normal flux traces, the wall kind and data [3, l, B]
+    const double* tFv;       // or null
+    const int* wall_kind;
+    const double* wall;
 };
+
+// boundary conditions of the advective part (the parabolic walls are WALL_*)
+constexpr int BC_DIRICHLET = 0, BC_SLIP_WALL_VERTICAL = 1, BC_SLIP_WALL_HORIZONTAL = 2;
+constexpr int WALL_NONE = 0, WALL_ADIABATIC = 1, WALL_ISOTHERMAL = 2;
+
+// boundary_condition_slip_wall_vertical / _horizontal (src/equations/equations.jl:95-135): the exterior
+// normal flux, U and u are the inner ones mirrored in the wall's normal momentum
+__device__ __forceinline__ void slip_wall_exterior(int kind, const double* Fi, const double* Ui, const double* ui,
+                                                   double* Fo, double* Uo, double* uo) {
+    const bool vert = kind == BC_SLIP_WALL_VERTICAL;
+    Fo[0] = -Fi[0]; Fo[1] = vert ? Fi[1] : -Fi[1]; Fo[2] = vert ? -Fi[2] : Fi[2]; Fo[3] = -Fi[3];
+    Uo[0] = Ui[0]; Uo[1] = vert ? -Ui[1] : Ui[1]; Uo[2] = vert ? Ui[2] : -Ui[2]; Uo[3] = Ui[3];
+    uo[0] = ui[0]; uo[1] = vert ? -ui[1] : ui[1]; uo[2] = vert ? ui[2] : -ui[2]; uo[3] = ui[3];
+}
 
 template <int N>
 static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
@@ -193,22 +212,39 @@ static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
     load4(a.u + ((size_t)e * n * n + node) * NV, ui);
     load4(a.tU + (((size_t)e * 4 + face) * n + l) * NV, Ui);
     load4(a.tF + (((size_t)e * 4 + face) * n + l) * NV, Fi);
-    for (int q = 0; q < n; ++q) {
-        double ub[NV], fb[NV];
-        load4(a.levels + (((size_t)k * n + l) * n + q) * NV, ub);
-        euler_flux_dir(gm1, ub, a.orientation, fb);
-        const double w = 0.5 * a.scaling_factor;
+    const int kind = a.kind ? __ldg(a.kind + k) : BC_DIRICHLET;
+    if (kind == BC_DIRICHLET) {
+        for (int q = 0; q < n; ++q) {
+            double ub[NV], fb[NV];
+            load4(a.levels + (((size_t)k * n + l) * n + q) * NV, ub);
+            euler_flux_dir(gm1, ub, a.orientation, fb);
+            const double w = 0.5 * a.scaling_factor;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            Uo[v] += w * ub[v] * a.weights[q];
-            Fo[v] += w * fb[v] * a.weights[q];
+            for (int v = 0; v < NV; ++v) {
+                Uo[v] += w * ub[v] * a.weights[q];
+                Fo[v] += w * fb[v] * a.weights[q];
+            }
         }
+        load4(a.now + ((size_t)k * n + l) * NV, uo);
+    } else {
+        slip_wall_exterior(kind, Fi, Ui, ui, Fo, Uo, uo);
     }
-    load4(a.now + ((size_t)k * n + l) * NV, uo);
     if (dir % 2 == 0)
         lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, Fi, Fo, Ui, Uo, ui, uo, a.orientation, Fn, a.status);
     else
         lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, Fo, Fi, Uo, Ui, uo, ui, a.orientation, Fn, a.status);
+    if (a.tFv) {
+        // minus the wall's viscous flux (calc_boundary_flux_divergence_lw!, dg_2d_parabolic.jl:2005-2084;
+        // BoundaryConditionNavierStokesWall, compressible_navier_stokes_2d.jl:81-108)
+        double fv[NV];
+        load4(a.tFv + (((size_t)e * 4 + face) * n + l) * NV, fv);
+        if (__ldg(a.wall_kind + k) == WALL_ADIABATIC) {
+            const double* w = a.wall + 3 * ((size_t)k * n + l);
+            fv[3] = fma(__ldg(w), fv[1], fma(__ldg(w + 1), fv[2], __ldg(w + 2)));
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fn[v] -= fv[v];
+    }
     const double dts = a.step_mode ? *a.dt : 1.0;
     const double ij = __ldg(a.inv_jac + e);
     const double s = (dir % 2 == 0) ? -ij * a.inv_w_last * dts : ij * a.inv_w_first * dts;

@@ -10,7 +10,9 @@ from .equations import (CompressibleEulerEquations2D, CompressibleNavierStokesDi
 from .limiters import PositivityPreservingLimiterZhangShu, density, density_pressure, pressure
 from .lwfr import LWIntegrator, LWSolution, l2_linf_errors, solve_lwfr
 from .mesh import RefinedTreeMesh, TreeMesh
-from .semidiscretization import (LW, MDRK, DGSEM, Adaptive, BoundaryConditionDirichlet, CFLBased, FluxHLL,
+from .semidiscretization import (LW, MDRK, DGSEM, Adaptive, Adiabatic, BoundaryConditionDirichlet,
+                                 BoundaryConditionNavierStokesWall, CFLBased, FluxHLL, Isothermal, NoSlip,
+                                 boundary_condition_slip_wall_horizontal, boundary_condition_slip_wall_vertical,
                                  FluxLaxFriedrichs, IndicatorHennemannGassner, SemidiscretizationHyperbolic,
                                  SemidiscretizationHyperbolicParabolic,
                                  VolumeIntegralFR, VolumeIntegralFRShockCapturing,
@@ -30,4 +32,6 @@ __all__ = [
     "CurvedMesh", "StructuredMesh", "rotate_elements", "rotate_state", "RefinedTreeMesh",
     "CompressibleNavierStokesDiffusion2D", "GradientVariablesConservative", "SemidiscretizationHyperbolicParabolic",
     "PositivityPreservingLimiterZhangShu", "density", "pressure", "density_pressure",
+    "boundary_condition_slip_wall_vertical", "boundary_condition_slip_wall_horizontal", "NoSlip", "Adiabatic",
+    "Isothermal", "BoundaryConditionNavierStokesWall",
 ]

@@ -27,6 +27,8 @@ TLW_STAGE_LW, TLW_STAGE_MDRK1, TLW_STAGE_MDRK2 = 0, 1, 2
 TLW_CACHE_U_TRACES, TLW_CACHE_F_TRACES, TLW_CACHE_U2, TLW_CACHE_F2, TLW_CACHE_ALPHA, TLW_CACHE_FN_LOW = 0, 1, 2, 3, 4, 5
 TLW_VOLUME_FR, TLW_VOLUME_FR_SHOCK_CAPTURING = 0, 1
 TLW_LIMIT_DENSITY, TLW_LIMIT_PRESSURE, TLW_LIMIT_DENSITY_PRESSURE = 0, 1, 2
+TLW_BC_DIRICHLET, TLW_BC_SLIP_WALL_VERTICAL, TLW_BC_SLIP_WALL_HORIZONTAL = 0, 1, 2
+TLW_WALL_NOSLIP_ADIABATIC, TLW_WALL_NOSLIP_ISOTHERMAL = 1, 2
 
 # every symbol include/tlw.h declares
 EXPORTED = (
@@ -40,7 +42,7 @@ EXPORTED = (
     "tlw_adjoint_step", "tlw_forward_record", "tlw_adjoint_sweep", "tlw_adjoint_solve", "tlw_adjoint_dt_sequence",
     "tlw_solve_dts", "tlw_set_curved_mesh", "tlw_curved_colors", "tlw_set_tree_mortars",
     "tlw_set_parabolic", "tlw_adaptive_trial", "tlw_adaptive_accept",
-    "tlw_set_positivity_limiter", "tlw_apply_positivity_limiter",
+    "tlw_set_positivity_limiter", "tlw_apply_positivity_limiter", "tlw_set_boundary_kinds", "tlw_set_parabolic_walls",
 )
 
 
@@ -114,6 +116,8 @@ def lib() -> ctypes.CDLL:
     L.tlw_set_parabolic.argtypes = [P, dbl, dbl]
     L.tlw_set_positivity_limiter.argtypes = [P, i32, P, P]
     L.tlw_apply_positivity_limiter.argtypes = [P]
+    L.tlw_set_boundary_kinds.argtypes = [P, P]
+    L.tlw_set_parabolic_walls.argtypes = [P, P, P]
     L.tlw_adaptive_trial.argtypes = [P, dbl, dbl, dbl, dp, ctypes.POINTER(ctypes.c_int32)]
     L.tlw_adaptive_accept.argtypes = [P, dbl]
     L.tlw_curved_colors.argtypes = [P]

@@ -104,8 +104,7 @@ def solve_lwfr(lw_update: LWUpdate, callbacks=(), dt_initial: float = 0.0, toler
     integ.set_state(u0, lw_update.tspan[0])
     if n_pairs:
         check(integ.handle, lib().tlw_apply_positivity_limiter(integ.handle))
-    bc = semi.boundary_conditions
-    time_dependent_bc = semi.mesh.n_boundaries > 0 and not bc.time_independent
+    time_dependent_bc = semi.mesh.n_boundaries > 0 and semi.time_dependent_boundaries()
     intervals = [int(cb.interval) for cb in callbacks if getattr(cb, "interval", 0)]
     stride = min(intervals) if intervals else chunk
     if not time_dependent_bc:

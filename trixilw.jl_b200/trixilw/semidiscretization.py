@@ -143,6 +143,89 @@ class BoundaryConditionDirichlet:
         self.time_independent = time_independent
 
 
+class BoundaryConditionSlipWall:
+    """TrixiLW's LW slip walls (src/equations/equations.jl:95-135): the exterior u, U and normal flux are
+    the inner ones with the wall-normal momentum mirrored; no exterior data."""
+
+    time_independent = True
+
+    def __init__(self, code: int, name: str):
+        self.code = code
+        self.name = name
+
+    def __repr__(self):
+        return self.name
+
+
+boundary_condition_slip_wall_vertical = BoundaryConditionSlipWall(_lib.TLW_BC_SLIP_WALL_VERTICAL,
+                                                                  "boundary_condition_slip_wall_vertical")
+boundary_condition_slip_wall_horizontal = BoundaryConditionSlipWall(_lib.TLW_BC_SLIP_WALL_HORIZONTAL,
+                                                                    "boundary_condition_slip_wall_horizontal")
+
+DIRECTIONS = ("x_neg", "x_pos", "y_neg", "y_pos")   # Trixi directions 1..4
+
+
+def digest_boundary_conditions(bc):
+    """One condition per direction (x_neg, x_pos, y_neg, y_pos), as Trixi's digest_boundary_conditions: a
+    single condition for all, or a mapping / named tuple with those four keys."""
+    if isinstance(bc, dict):
+        missing = [d for d in DIRECTIONS if d not in bc]
+        if missing:
+            raise ValueError(f"boundary conditions missing for {missing}")
+        return tuple(bc[d] for d in DIRECTIONS)
+    if hasattr(bc, "_fields"):
+        return digest_boundary_conditions(bc._asdict())
+    return (bc,) * 4
+
+
+# ---- walls of the parabolic part (Trixi BoundaryConditionNavierStokesWall) ------------------------------
+class NoSlip:
+    """NoSlip(boundary_value_function): f(x, y, t, equations) -> (v1, v2) of the wall."""
+
+    def __init__(self, boundary_value_function):
+        self.boundary_value_function = boundary_value_function
+
+
+class Adiabatic:
+    """Adiabatic(boundary_value_normal_flux_function): f(x, y, t, equations) -> normal heat flux q."""
+
+    def __init__(self, boundary_value_normal_flux_function):
+        self.boundary_value_normal_flux_function = boundary_value_normal_flux_function
+
+
+class Isothermal:
+    """Isothermal(boundary_value_function): f(x, y, t, equations) -> wall temperature T (= p / rho)."""
+
+    def __init__(self, boundary_value_function):
+        self.boundary_value_function = boundary_value_function
+
+
+class BoundaryConditionNavierStokesWall:
+    """BoundaryConditionNavierStokesWall(boundary_condition_velocity, boundary_condition_heat_flux) as TrixiLW
+    imposes it with conservative gradient variables (src/equations/compressible_navier_stokes_2d.jl:81-124)."""
+
+    def __init__(self, boundary_condition_velocity: NoSlip, boundary_condition_heat_flux):
+        if not isinstance(boundary_condition_velocity, NoSlip):
+            raise NotImplementedError("NoSlip velocity walls are built")
+        if not isinstance(boundary_condition_heat_flux, (Adiabatic, Isothermal)):
+            raise NotImplementedError("Adiabatic or Isothermal heat conditions are built")
+        self.boundary_condition_velocity = boundary_condition_velocity
+        self.boundary_condition_heat_flux = boundary_condition_heat_flux
+
+    @property
+    def code(self) -> int:
+        return (_lib.TLW_WALL_NOSLIP_ADIABATIC if isinstance(self.boundary_condition_heat_flux, Adiabatic)
+                else _lib.TLW_WALL_NOSLIP_ISOTHERMAL)
+
+    def data(self, x, y, t, equations) -> np.ndarray:
+        """[..., 3] = (v1, v2, q or T) at the points (x, y)."""
+        v1, v2 = self.boundary_condition_velocity.boundary_value_function(x, y, t, equations)
+        h = self.boundary_condition_heat_flux
+        third = (h.boundary_value_normal_flux_function(x, y, t, equations) if isinstance(h, Adiabatic)
+                 else h.boundary_value_function(x, y, t, equations))
+        return np.stack(np.broadcast_arrays(v1, v2, third, x), axis=-1)[..., :3].astype(np.float64)
+
+
 def lw_fourier_cfl(N: int) -> float:
     """LW Fourier CFL limits for N = 1..4 (src/auxiliary/auxiliary.jl:14). N >= 5 is not tabulated by
     the reference; callers must supply their own CFL there."""
@@ -209,8 +292,10 @@ class SemidiscretizationHyperbolic:
         self.polydeg = solver.polydeg
         self.nnodes = solver.polydeg + 1
         self.boundary_conditions = boundary_conditions
-        if mesh.n_boundaries > 0 and not isinstance(boundary_conditions, BoundaryConditionDirichlet):
-            raise ValueError("a non-periodic TreeMesh needs a BoundaryConditionDirichlet")
+        self._bcs = digest_boundary_conditions(boundary_conditions) if mesh.n_boundaries > 0 else ()
+        for d, bc in zip(DIRECTIONS, self._bcs):
+            if not isinstance(bc, (BoundaryConditionDirichlet, BoundaryConditionSlipWall)):
+                raise ValueError(f"{d}: a non-periodic TreeMesh needs BoundaryConditionDirichlet or a slip wall")
         self.cache = {"dt": [math.nan]}
         sf = solver.surface_flux
         opts = _lib.TlwOpts()
@@ -235,6 +320,7 @@ class SemidiscretizationHyperbolic:
                                  else mesh.node_coordinates(self.polydeg))
         if mesh.n_boundaries:
             self._bnd_xy = mesh.boundary_node_coordinates(self.polydeg)
+            self._upload_boundary_kinds()
 
     @property
     def handle(self):
@@ -293,23 +379,44 @@ class SemidiscretizationHyperbolic:
         return np.ascontiguousarray(np.transpose(u, (2, 1, 0, 3))).reshape(-1)
 
     # ---- boundary data ------------------------------------------------------------------------------
+    def _direction_ranges(self):
+        last = np.cumsum(self.mesh.n_boundaries_per_direction)
+        return [(int(b - c), int(b)) for b, c in zip(last, self.mesh.n_boundaries_per_direction)]
+
+    def _upload_boundary_kinds(self):
+        kinds = np.zeros(self.mesh.n_boundaries, dtype=np.int32)
+        for (a, b), bc in zip(self._direction_ranges(), self._bcs):
+            kinds[a:b] = bc.code if isinstance(bc, BoundaryConditionSlipWall) else _lib.TLW_BC_DIRICHLET
+        self._kinds = kinds
+        check(self.handle, lib().tlw_set_boundary_kinds(self.handle, _ptr(kinds)))
+
+    def time_dependent_boundaries(self) -> bool:
+        return any(isinstance(bc, BoundaryConditionDirichlet) and not bc.time_independent for bc in self._bcs)
+
     def _prepare_boundaries(self, t: float, dt: float, scaling_factor: float):
         if self.mesh.n_boundaries == 0:
             return
-        bc = self.boundary_conditions
-        key = ("const", scaling_factor) if bc.time_independent else (t, dt, scaling_factor)
-        if key == self._bdata_key or (bc.time_independent and self._bdata_key is not None):
+        dirichlet = [(r, bc) for r, bc in zip(self._direction_ranges(), self._bcs)
+                     if isinstance(bc, BoundaryConditionDirichlet) and r[1] > r[0]]
+        if not dirichlet:
+            return
+        const = not self.time_dependent_boundaries()
+        key = ("const", scaling_factor) if const else (t, dt, scaling_factor)
+        if key == self._bdata_key or (const and self._bdata_key is not None):
             return
         nodes, _ = gauss_lobatto(self.polydeg)
         n = self.nnodes
-        x, y = self._bnd_xy[0], self._bnd_xy[1]        # [l, B]
         dts = scaling_factor * dt
-        levels = np.empty((self.mesh.n_boundaries, n, n, 4))  # [B, l, q, v] == [v, q, l, B] column-major
-        for q in range(n):
-            ts = t + 0.5 * dts * (nodes[q] + 1.0) if bc.time_independent is False else t
-            levels[:, :, q, :] = np.transpose(bc.boundary_value_function(x, y, ts, self.equations), (1, 0, 2))
-        now = np.ascontiguousarray(np.transpose(bc.boundary_value_function(x, y, t, self.equations), (1, 0, 2)))
+        levels = np.zeros((self.mesh.n_boundaries, n, n, 4))  # [B, l, q, v] == [v, q, l, B] column-major
+        now = np.zeros((self.mesh.n_boundaries, n, 4))
+        for (a, b), bc in dirichlet:
+            x, y = self._bnd_xy[0][:, a:b], self._bnd_xy[1][:, a:b]        # [l, B_d]
+            for q in range(n):
+                ts = t + 0.5 * dts * (nodes[q] + 1.0) if bc.time_independent is False else t
+                levels[a:b, :, q, :] = np.transpose(bc.boundary_value_function(x, y, ts, self.equations), (1, 0, 2))
+            now[a:b] = np.transpose(bc.boundary_value_function(x, y, t, self.equations), (1, 0, 2))
         levels = np.ascontiguousarray(levels)
+        now = np.ascontiguousarray(now)
         check(self.handle, lib().tlw_set_boundary_data(self.handle, _ptr(levels), _ptr(now), _lib.TLW_WHERE_HOST))
         self._bdata_key = key
 
@@ -365,20 +472,46 @@ class LWUpdate:
 
 
 class SemidiscretizationHyperbolicParabolic(SemidiscretizationHyperbolic):
-    """SemidiscretizationHyperbolicParabolic(mesh, (equations, equations_parabolic), initial_condition, solver):
-    compressible Navier-Stokes on a periodic TreeMesh{2} (BR1 gradients of the conservative variables), LW."""
+    """SemidiscretizationHyperbolicParabolic(mesh, [time_discretization,] (equations, equations_parabolic),
+    initial_condition, solver; boundary_conditions=(hyperbolic, parabolic)): compressible Navier-Stokes on a
+    conforming TreeMesh{2} (BR1 gradients of the conservative variables), LW. On a non-periodic mesh the
+    parabolic conditions are BoundaryConditionNavierStokesWall, one per direction (x_neg, x_pos, y_neg, y_pos);
+    their wall data are taken at t = 0 (the lid-driven cavity's walls do not change in time)."""
 
-    def __init__(self, mesh, equations, initial_condition, solver, device: int = 0, **kw):
+    def __init__(self, mesh, *args, device: int = 0, boundary_conditions=None, **kw):
+        if len(args) == 4:   # the reference's form with the time discretization second
+            _, equations, initial_condition, solver = args
+        else:
+            equations, initial_condition, solver = args
         eq, eq_par = equations
-        super().__init__(mesh, get_time_discretization(solver), eq, initial_condition, solver, device=device, **kw)
+        bc_hyp, bc_par = boundary_conditions if boundary_conditions is not None else (
+            boundary_condition_periodic, boundary_condition_periodic)
         self.equations_parabolic = eq_par
-        check(self.handle, lib().tlw_set_parabolic(self.handle, eq_par.mu, eq_par.Pr))
+        self._bcs_par = digest_boundary_conditions(bc_par) if mesh.n_boundaries > 0 else ()
+        for d, bc in zip(DIRECTIONS, self._bcs_par):
+            if not isinstance(bc, BoundaryConditionNavierStokesWall):
+                raise ValueError(f"{d}: the parabolic part needs a BoundaryConditionNavierStokesWall")
+        super().__init__(mesh, get_time_discretization(solver), eq, initial_condition, solver, device=device,
+                         boundary_conditions=bc_hyp, **kw)
+        self.boundary_conditions_parabolic = bc_par
+        self._upload_parabolic()
 
-    def _upload_mesh(self):
-        super()._upload_mesh()
-        if hasattr(self, "equations_parabolic"):
-            check(self.handle, lib().tlw_set_parabolic(self.handle, self.equations_parabolic.mu,
-                                                       self.equations_parabolic.Pr))
+    def _upload_parabolic(self):
+        eq_par = self.equations_parabolic
+        check(self.handle, lib().tlw_set_parabolic(self.handle, eq_par.mu, eq_par.Pr))
+        if self.mesh.n_boundaries == 0:
+            return
+        n = self.nnodes
+        kinds = np.zeros(self.mesh.n_boundaries, dtype=np.int32)
+        data = np.zeros((self.mesh.n_boundaries, n, 3))     # [B, l, 3] == [3, l, B] column-major
+        xy = self.mesh.boundary_node_coordinates(self.polydeg)
+        for (a, b), bc in zip(self._direction_ranges(), self._bcs_par):
+            kinds[a:b] = bc.code
+            if b > a:
+                data[a:b] = np.transpose(bc.data(xy[0][:, a:b], xy[1][:, a:b], 0.0, self.equations), (1, 0, 2))
+        self._wkeep = (kinds, np.ascontiguousarray(data))
+        check(self.handle, lib().tlw_set_parabolic_walls(self.handle, _ptr(kinds), _ptr(self._wkeep[1])))
+
 
 
 def semidiscretize(semi: SemidiscretizationHyperbolic, time_discretization, tspan) -> LWUpdate:
@@ -390,6 +523,8 @@ __all__ = [
     "LW", "MDRK", "CFLBased", "Adaptive", "VolumeIntegralFR", "VolumeIntegralFRShockCapturing",
     "IndicatorHennemannGassner", "DGSEM", "FluxLaxFriedrichs", "FluxHLL",
     "flux_lax_friedrichs", "flux_hll", "BoundaryConditionDirichlet", "boundary_condition_periodic",
+    "boundary_condition_slip_wall_vertical", "boundary_condition_slip_wall_horizontal", "NoSlip", "Adiabatic",
+    "Isothermal", "BoundaryConditionNavierStokesWall",
     "SemidiscretizationHyperbolic", "SemidiscretizationHyperbolicParabolic", "semidiscretize", "rhs", "rhs_mdrk1", "rhs_mdrk2", "lw_fourier_cfl",
     "trixi2lw", "get_time_discretization", "DomainError", "LWUpdate",
 ]
