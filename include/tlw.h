@@ -125,11 +125,12 @@ int tlw_set_positivity_limiter(tlw_handle* h, int32_t count, const double* thres
 int tlw_apply_positivity_limiter(tlw_handle* h);
 
 /* Compressible Navier-Stokes (SemidiscretizationHyperbolicParabolic with CompressibleNavierStokesDiffusion2D,
- * conservative gradient variables, BR1) on the handle's conforming TreeMesh, set after tlw_set_tree_mesh
- * (which clears it): LW with the FR volume integral, N >= 3. mu = dynamic viscosity, prandtl = Prandtl number;
- * the handle's gamma. Replaces rhs! of src/solvers/dgsem_tree/dg_2d_parabolic.jl:15-99 (kernels :725-1860,
- * interface flux :1911-1949, boundaries :1951-2084) and compute_dt (src/solvers/lwfr.jl:192-210). A mesh with
- * boundaries also needs tlw_set_parabolic_walls. */
+ * conservative gradient variables, BR1) on the handle's conforming TreeMesh or curvilinear mesh, set after
+ * tlw_set_tree_mesh / tlw_set_curved_mesh (which clear it): LW with the FR volume integral, N >= 3.
+ * mu = dynamic viscosity, prandtl = Prandtl number; the handle's gamma. Replaces rhs! of
+ * src/solvers/dgsem_tree/dg_2d_parabolic.jl:15-99 (TreeMesh kernels :725-1860, interface flux :1911-1949,
+ * boundaries :1951-2084; P4estMesh kernels and surfaces of src/solvers/dgsem_p4est/dg_2d_parabolic.jl) and
+ * compute_dt (src/solvers/lwfr.jl:192-210). A mesh with boundaries also needs tlw_set_parabolic_walls. */
 int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl);
 
 /* Walls of the parabolic part, one per boundary (Trixi boundaries order), after tlw_set_parabolic:
@@ -167,6 +168,13 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
                         const double* inverse_jacobian, int64_t n_interfaces, const int64_t* primary_elements,
                         const int32_t* primary_faces, const int64_t* secondary_elements,
                         const int32_t* secondary_faces, const int32_t* secondary_reversed);
+/* Boundary faces of the curvilinear mesh (P4estMesh boundaries: element, face), after tlw_set_curved_mesh
+ * (which clears them): elements 1-based, faces 0: -xi, 1: +xi, 2: -eta, 3: +eta (a face no interface covers),
+ * kinds TLW_BC_SLIP_WALL_VERTICAL / _HORIZONTAL (the normal-direction slip walls of src/equations/equations.jl:
+ * 137-169, called as calc_boundary_flux! of src/solvers/dgsem_p4est/dg_2d.jl:285-393 does). The boundaries keep
+ * the caller's order for tlw_set_parabolic_walls. */
+int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t* elements, const int32_t* faces,
+                              const int32_t* kinds);
 /* Number of interface colours (launches per interface pass) of the curvilinear mesh; 0 for a TreeMesh. */
 int32_t tlw_curved_colors(tlw_handle* h);
 

@@ -7,6 +7,7 @@
 
 #include "tlw_adjoint.hpp"
 #include "tlw_curved.hpp"
+#include "tlw_curved_parabolic.hpp"
 #include "tlw_limiter.hpp"
 #include "tlw_parabolic.hpp"
 #include "tlw_oracle.hpp"
@@ -39,7 +40,8 @@ void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, do
              const BoundaryData* bd, int kind, int nthreads) {
     if (h->parabolic) {
         if (kind != 0) throw std::runtime_error("parabolic oracle: LW only");
-        rhs_parabolic(h->basis, h->eq, h->ns, h->opt, h->mesh, u, du, dt, h->ws, nthreads, bd);
+        if (h->curved) rhs_parabolic_curved(h->basis, h->eq, h->ns, h->opt, h->cmesh, u, du, dt, h->ws, nthreads);
+        else rhs_parabolic(h->basis, h->eq, h->ns, h->opt, h->mesh, u, du, dt, h->ws, nthreads, bd);
         return;
     }
     if (!h->curved) {
@@ -51,6 +53,7 @@ void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, do
 }
 
 double any_max_dt(oracle_handle* h, const double* u, double cfl, bool& bad, int nthreads) {
+    if (h->parabolic && h->curved) return max_dt_parabolic_curved(h->basis, h->eq, h->ns, h->cmesh, u, cfl, bad, nthreads);
     if (h->parabolic) return max_dt_parabolic(h->basis, h->eq, h->ns, h->mesh, u, cfl, bad, nthreads);
     if (h->curved) return max_dt_curved(h->basis, h->eq, h->cmesh, u, cfl, bad, nthreads);
     return max_dt(h->basis, h->eq, h->mesh, u, cfl, bad, nthreads);
@@ -156,11 +159,22 @@ int oracle_mortar_operators(int N, double* out) {
 
 // compressible Navier-Stokes: dynamic viscosity mu and Prandtl number (the handle's gamma)
 int oracle_set_parabolic(oracle_handle* h, double mu, double Pr) {
-    if (h->curved) return 1;
     h->parabolic = true;
     h->ns.gamma = h->eq.gamma;
     h->ns.mu = mu;
     h->ns.Pr = Pr;
+    return 0;
+}
+
+// boundary faces of a curvilinear mesh: element (0-based), face 0..3, slip wall kind 1 (vertical) / 2 (horizontal)
+int oracle_set_curved_boundaries(oracle_handle* h, int B, const int32_t* elem, const int32_t* face, const int32_t* kind) {
+    if (!h->curved) return 1;
+    h->cmesh.n_boundaries = B;
+    h->cmesh.b_elem.assign(elem, elem + B);
+    h->cmesh.b_face.assign(face, face + B);
+    h->cmesh.b_kind.assign(kind, kind + B);
+    for (int k = 0; k < B; ++k)
+        if (kind[k] != BC_SLIP_WALL_VERTICAL && kind[k] != BC_SLIP_WALL_HORIZONTAL) return 1;
     return 0;
 }
 
@@ -173,8 +187,7 @@ int oracle_set_boundary_kinds(oracle_handle* h, const int32_t* kinds) {
 
 // Navier-Stokes walls per boundary (1 no-slip adiabatic, 2 no-slip isothermal) and their data [3, l, B]
 int oracle_set_walls(oracle_handle* h, const int32_t* kinds, const double* data) {
-    if (h->curved) return 1;
-    const size_t B = h->mesh.n_boundaries, n = h->basis.n;
+    const size_t B = h->curved ? h->cmesh.n_boundaries : h->mesh.n_boundaries, n = h->basis.n;
     h->ns.wall_kind.assign(kinds, kinds + B);
     h->ns.wall.assign(data, data + 3 * n * B);
     return 0;

@@ -55,6 +55,7 @@ def lib():
         L.oracle_set_limiter.argtypes = [P, i32, P, P]
         L.oracle_set_boundary_kinds.argtypes = [P, P]
         L.oracle_set_walls.argtypes = [P, P, P]
+        L.oracle_set_curved_boundaries.argtypes = [P, i32, P, P, P]
         L.oracle_apply_limiter.argtypes = [P, P]
         L.oracle_last_error.argtypes = [P]
         L.oracle_last_error.restype = ctypes.c_char_p
@@ -160,6 +161,13 @@ class Oracle:
         """Per boundary (the mesh's boundary order): 0 Dirichlet, 1 slip wall vertical, 2 slip wall horizontal."""
         self._kkeep = np.ascontiguousarray(kinds, dtype=np.int32)
         assert lib().oracle_set_boundary_kinds(self.h, _p(self._kkeep)) == 0
+
+    def set_curved_boundaries(self, elements, faces, kinds):
+        """Boundary faces of a curvilinear mesh: elements 1-based, faces 0..3, kinds 1 (slip wall vertical) or
+        2 (slip wall horizontal)."""
+        self._cbkeep = (np.ascontiguousarray(np.asarray(elements) - 1, dtype=np.int32),
+                        np.ascontiguousarray(faces, dtype=np.int32), np.ascontiguousarray(kinds, dtype=np.int32))
+        assert lib().oracle_set_curved_boundaries(self.h, len(self._cbkeep[0]), *[_p(a) for a in self._cbkeep]) == 0
 
     def set_walls(self, kinds, data):
         """Navier-Stokes walls per boundary (1 no-slip adiabatic, 2 no-slip isothermal), data [B, l, 3] =

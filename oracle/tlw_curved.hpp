@@ -31,6 +31,9 @@ struct CurvedMesh {
     std::vector<double> inv_jac;    // [i, j, e]
     int n_interfaces = 0;
     std::vector<int32_t> p_elem, p_face, s_elem, s_face, s_rev;   // 0-based elements
+    // boundary faces (P4estMesh boundaries: element, face) with their condition (BC_SLIP_WALL_*)
+    int n_boundaries = 0;
+    std::vector<int32_t> b_elem, b_face, b_kind;
 };
 
 // node (i, j) of face f at face index l
@@ -193,7 +196,56 @@ inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, con
         }
 }
 
-// du = rhs(u) on a conforming curvilinear mesh (LW, FR volume integral, no boundaries)
+// Boundary faces with the LW slip walls in their normal-direction form (src/equations/equations.jl:137-169;
+// prolong2boundaries! and calc_boundary_flux!, src/solvers/dgsem_p4est/dg_2d.jl:285-393): the inner normal flux
+// uses the outward normal, the exterior state mirrors it, and the surface flux takes the inner side as _ll in
+// the curvilinear order (f_in, f_out, u_in, u_out, U_in, U_out, normal); the result is the outward flux.
+inline void calc_boundary_flux_curved(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m,
+                                      const double* u, Workspace& ws) {
+    const int n = b.n;
+    for (int k = 0; k < m.n_boundaries; ++k) {
+        const int e = m.b_elem[k], f = m.b_face[k], kind = m.b_kind[k];
+        for (int l = 0; l < n; ++l) {
+            int i, j;
+            face_node(n, f, l, i, j);
+            double nrm[2], Fi[NV], Ui[NV], ui[NV], Fo[NV], Uo[NV], uo[NV], Fn[NV];
+            outward_normal(m, n, f, i, j, e, nrm);
+            for (int v = 0; v < NV; ++v) {
+                Fi[v] = ws.F[idx_F(n, v, 0, i, j, e)] * nrm[0] + ws.F[idx_F(n, v, 1, i, j, e)] * nrm[1];
+                Ui[v] = ws.U[idx_u(n, v, i, j, e)];
+                ui[v] = u[idx_u(n, v, i, j, e)];
+            }
+            slip_wall_exterior(kind, Fi, Ui, ui, Fo, Uo, uo);
+            lw_surface_flux_normal(eq, opt.flux_kind, opt.speed_kind, Fi, Fo, ui, uo, Ui, Uo, nrm, Fn, ws.bad);
+            for (int v = 0; v < NV; ++v) ws.surface_flux_values[v + NV * (l + n * (f + 4 * (size_t)e))] = Fn[v];
+        }
+    }
+}
+
+// surface integral (outward fluxes) and apply_jacobian (per node) on a curvilinear mesh
+inline void surface_integral_and_jacobian_curved(const Basis& b, const CurvedMesh& m, double* du, const Workspace& ws,
+                                                 int nthreads = 1) {
+    const int n = b.n;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int e = 0; e < m.n_elements; ++e) {
+        for (int f = 0; f < 4; ++f) {
+            const double iw = (f == 1 || f == 3) ? b.inv_w_last : b.inv_w_first;
+            for (int l = 0; l < n; ++l) {
+                int i, j;
+                face_node(n, f, l, i, j);
+                for (int v = 0; v < NV; ++v)
+                    du[idx_u(n, v, i, j, e)] += ws.surface_flux_values[v + NV * (l + n * (f + 4 * (size_t)e))] * iw;
+            }
+        }
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const double s = -m.inv_jac[i + n * (j + (size_t)n * e)];
+                for (int v = 0; v < NV; ++v) du[idx_u(n, v, i, j, e)] *= s;
+            }
+    }
+}
+
+// du = rhs(u) on a conforming curvilinear mesh (LW, FR volume integral; boundaries: slip walls)
 inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m, const double* u,
                        double* du, double dt, Workspace& ws, int nthreads = 1) {
     const int n = b.n, nn = n * n;
@@ -236,24 +288,8 @@ inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, cons
         }
     }
     ws.bad = ws.bad || bad;
-    // surface integral (outward fluxes) and apply_jacobian (per node)
-#pragma omp parallel for num_threads(nthreads) schedule(static)
-    for (int e = 0; e < m.n_elements; ++e) {
-        for (int f = 0; f < 4; ++f) {
-            const double iw = (f == 1 || f == 3) ? b.inv_w_last : b.inv_w_first;
-            for (int l = 0; l < n; ++l) {
-                int i, j;
-                face_node(n, f, l, i, j);
-                for (int v = 0; v < NV; ++v)
-                    du[idx_u(n, v, i, j, e)] += ws.surface_flux_values[v + NV * (l + n * (f + 4 * (size_t)e))] * iw;
-            }
-        }
-        for (int j = 0; j < n; ++j)
-            for (int i = 0; i < n; ++i) {
-                const double s = -m.inv_jac[i + n * (j + (size_t)n * e)];
-                for (int v = 0; v < NV; ++v) du[idx_u(n, v, i, j, e)] *= s;
-            }
-    }
+    calc_boundary_flux_curved(b, eq, opt, m, u, ws);
+    surface_integral_and_jacobian_curved(b, m, du, ws, nthreads);
 }
 
 // Trixi max_dt for curved meshes: per node lambda~_d = |Ja^d . (|v1| + c, |v2| + c)| |J^{-1}|

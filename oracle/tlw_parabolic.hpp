@@ -146,9 +146,14 @@ inline void gradients_br1(const Basis& b, const TreeMesh& m, const NavierStokes&
 
 // one element of the parabolic LW volume kernel (depth 3 for N = 3, 4 for N >= 4); du += Dhat (F, G);
 // Ua = time-averaged U, Fa = advective [v, d, i, j], Fv = viscous time averages
+// On a curvilinear mesh (Jae = the element's contravariant vectors [4, i, j], ije = its inverse Jacobian per
+// node; src/solvers/dgsem_p4est/dg_2d_parabolic.jl:1190-1787): the stage fluxes are the contravariant ones
+// Ja^1 . (f_a - f_v, g_a - g_v), Ja^2 . (...), d_m carries the per-node J^{-1}, and its gradient is
+// J^{-1} (Ja^1_d D_xi d_m + Ja^2_d D_eta d_m) (compute_local_grad_u!, :51-104); Fao / Fvo stay physical.
 inline void lw_volume_element_parabolic(const Basis& b, const Euler& eq, const NavierStokes& ns, int N, int e,
                                         const double* u, const double* gx, const double* gy, double* du, double dt,
-                                        double ij, double* Uo, double* Fao, double* Fvo) {
+                                        double ij, double* Uo, double* Fao, double* Fvo,
+                                        const double* Jae = nullptr, const double* ije = nullptr) {
     const int n = b.n, nn = n * n;
     const LWStencils S = lw_stencils(N);
     const int depth = S.depth;
@@ -166,15 +171,23 @@ inline void lw_volume_element_parabolic(const Basis& b, const Euler& eq, const N
         eq.fluxes(s, fa, ga);
         viscous_fluxes(ns, s, sx, sy, fv, gv);
     };
+    auto ijn = [&](int i, int j) { return Jae ? ije[i + n * j] : ij; };
+    // the stage flux pair along the reference coordinates: contravariant on a curvilinear mesh
+    auto contra = [&](int i, int j, double f, double g, double& cf, double& cg) {
+        if (!Jae) { cf = f; cg = g; return; }
+        const double* J = Jae + 4 * (i + n * j);
+        cf = J[0] * f + J[1] * g;
+        cg = J[2] * f + J[3] * g;
+    };
     auto next = [&](int m) {
-        // d_m = -dt J^{-1} (D ft + D gt); grad d_m = J^{-1} (D d_m along i, along j)
+        // d_m = -dt J^{-1} (D ft + D gt); grad d_m = J^{-1} (D d_m along i, along j), mixed by the metrics
         double* dm = at(d, m);
         for (int j = 0; j < n; ++j)
             for (int i = 0; i < n; ++i)
                 for (int v = 0; v < NV; ++v) {
                     double s = 0.0;
                     for (int k = 0; k < n; ++k) s += b.D[i * n + k] * ft[L(k, j) + v] + b.D[j * n + k] * gt[L(i, k) + v];
-                    dm[L(i, j) + v] = -dt * ij * s;
+                    dm[L(i, j) + v] = -dt * ijn(i, j) * s;
                 }
         for (int j = 0; j < n; ++j)
             for (int i = 0; i < n; ++i)
@@ -184,8 +197,14 @@ inline void lw_volume_element_parabolic(const Basis& b, const Euler& eq, const N
                         sx += b.D[i * n + k] * dm[L(k, j) + v];
                         sy += b.D[j * n + k] * dm[L(i, k) + v];
                     }
-                    at(dx, m)[L(i, j) + v] = ij * sx;
-                    at(dy, m)[L(i, j) + v] = ij * sy;
+                    if (Jae) {
+                        const double* J = Jae + 4 * (i + n * j);
+                        at(dx, m)[L(i, j) + v] = ijn(i, j) * (J[0] * sx + J[2] * sy);
+                        at(dy, m)[L(i, j) + v] = ijn(i, j) * (J[1] * sx + J[3] * sy);
+                    } else {
+                        at(dx, m)[L(i, j) + v] = ij * sx;
+                        at(dy, m)[L(i, j) + v] = ij * sy;
+                    }
                 }
     };
     auto state = [&](int s, int q, int o, double* P, double* Px, double* Py) {
@@ -207,7 +226,7 @@ inline void lw_volume_element_parabolic(const Basis& b, const Euler& eq, const N
             all_fluxes(ue + o, gxe + o, gye + o, fa, ga, fv, gv);
             for (int v = 0; v < NV; ++v) {
                 Fa[o + v] = fa[v]; Ga[o + v] = ga[v]; Fv[o + v] = fv[v]; Gv[o + v] = gv[v];
-                ft[o + v] = fa[v] - fv[v]; gt[o + v] = ga[v] - gv[v];
+                contra(i, j, fa[v] - fv[v], ga[v] - gv[v], ft[o + v], gt[o + v]);
                 U[o + v] = ue[o + v];
             }
         }
@@ -239,7 +258,7 @@ inline void lw_volume_element_parabolic(const Basis& b, const Euler& eq, const N
                     Fa[o + v] += S.tw[s] * sfa[v]; Ga[o + v] += S.tw[s] * sga[v];
                     Fv[o + v] += S.tw[s] * sfv[v]; Gv[o + v] += S.tw[s] * sgv[v];
                     U[o + v] += S.tw[s] * at(d, s)[o + v];
-                    ft[o + v] = sfa[v] - sfv[v]; gt[o + v] = sga[v] - sgv[v];
+                    contra(i, j, sfa[v] - sfv[v], sga[v] - sgv[v], ft[o + v], gt[o + v]);
                 }
             }
         if (s < depth) next(s + 1);
@@ -248,10 +267,12 @@ inline void lw_volume_element_parabolic(const Basis& b, const Euler& eq, const N
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
             const int o = L(i, j);
+            double cf[NV], cg[NV];
+            for (int v = 0; v < NV; ++v) contra(i, j, Fa[o + v] - Fv[o + v], Ga[o + v] - Gv[o + v], cf[v], cg[v]);
             for (int ii = 0; ii < n; ++ii)
-                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += b.Dhat[ii * n + i] * (Fa[o + v] - Fv[o + v]);
+                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += b.Dhat[ii * n + i] * cf[v];
             for (int jj = 0; jj < n; ++jj)
-                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += b.Dhat[jj * n + j] * (Ga[o + v] - Gv[o + v]);
+                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += b.Dhat[jj * n + j] * cg[v];
             for (int v = 0; v < NV; ++v) {
                 Uo[idx_u(n, v, i, j, e)] = U[o + v];
                 Fao[idx_F(n, v, 0, i, j, e)] = Fa[o + v];

@@ -73,6 +73,12 @@ void free_mesh(tlw_handle* h) {
     dfree(h->d_te); dfree(h->d_check);
     if (h->d_bad) { cudaFree(h->d_bad); h->d_bad = nullptr; }
     h->color_off.clear();
+    h->face_used.clear();
+    if (h->d_cbe) { cudaFree(h->d_cbe); h->d_cbe = nullptr; }
+    if (h->d_cbf) { cudaFree(h->d_cbf); h->d_cbf = nullptr; }
+    if (h->d_cbk) { cudaFree(h->d_cbk); h->d_cbk = nullptr; }
+    if (h->d_cbi) { cudaFree(h->d_cbi); h->d_cbi = nullptr; }
+    h->ncb = h->ncbx = 0;
     h->curved = false;
     h->have_mesh = false;
     h->have_bdata = false;
@@ -151,17 +157,39 @@ struct Launch {
             const int E = (int)h->E;
             using P = ParCfg<N>;
             const int grid = (E + P::EB - 1) / P::EB;
-            grad_volume_kernel<N><<<grid, P::THREADS, 0, s>>>(u, h->d_inv_jac, E, h->d_gx, h->d_gy);
-            const long long th = (long long)(h->nx + h->ny) * (N + 1);
-            if (th)
-                grad_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(
-                    u, h->d_xl, h->d_xr, h->nx, h->d_yl, h->d_yr, h->ny, h->d_inv_jac, h->h_basis.inv_w_first,
-                    h->h_basis.inv_w_last, h->d_gx, h->d_gy);
-            const long long tb = (long long)h->nb * (N + 1);
-            if (tb)
-                grad_boundary_kernel<N><<<(unsigned)((tb + 127) / 128), 128, 0, s>>>(
-                    u, h->d_b_elem, h->d_b_dir, h->d_wkind, h->d_wall, (int)h->nb, h->d_inv_jac, h->opts.gamma,
-                    h->h_basis.inv_w_first, h->h_basis.inv_w_last, h->d_gx, h->d_gy);
+            const double iwf = h->h_basis.inv_w_first, iwl = h->h_basis.inv_w_last;
+            if (h->curved) {
+                grad_volume_kernel<N, true><<<grid, P::THREADS, 0, s>>>(u, h->d_ijn, E, h->d_gx, h->d_gy, h->d_Ja);
+                for (size_t c = 0; c + 1 < h->color_off.size(); ++c) {
+                    const int b = h->color_off[c], cnt = h->color_off[c + 1] - b;
+                    const long long th = (long long)cnt * (N + 1);
+                    if (th)
+                        curved_grad_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(
+                            u, h->d_cp + b, h->d_cs + b, h->d_cf + b, cnt, h->d_Ja, h->d_ijn, iwf, iwl, h->d_gx,
+                            h->d_gy);
+                }
+                // xi-face boundaries, then eta-face ones (they share corner nodes)
+                const int first[2] = {0, h->ncbx}, count[2] = {h->ncbx, h->ncb - h->ncbx};
+                for (int cls = 0; cls < 2; ++cls) {
+                    const long long tb = (long long)count[cls] * (N + 1);
+                    if (tb)
+                        curved_grad_boundary_kernel<N><<<(unsigned)((tb + 127) / 128), 128, 0, s>>>(
+                            u, h->d_cbe + first[cls], h->d_cbf + first[cls], h->d_cbi + first[cls], count[cls],
+                            h->d_wkind, h->d_wall, h->d_Ja, h->d_ijn, h->opts.gamma, iwf, iwl, h->d_gx, h->d_gy);
+                }
+            } else {
+                grad_volume_kernel<N><<<grid, P::THREADS, 0, s>>>(u, h->d_inv_jac, E, h->d_gx, h->d_gy);
+                const long long th = (long long)(h->nx + h->ny) * (N + 1);
+                if (th)
+                    grad_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(
+                        u, h->d_xl, h->d_xr, h->nx, h->d_yl, h->d_yr, h->ny, h->d_inv_jac, iwf, iwl, h->d_gx,
+                        h->d_gy);
+                const long long tb = (long long)h->nb * (N + 1);
+                if (tb)
+                    grad_boundary_kernel<N><<<(unsigned)((tb + 127) / 128), 128, 0, s>>>(
+                        u, h->d_b_elem, h->d_b_dir, h->d_wkind, h->d_wall, (int)h->nb, h->d_inv_jac, h->opts.gamma,
+                        iwf, iwl, h->d_gx, h->d_gy);
+            }
             ParArgs pa{};
             pa.u = u;
             pa.gx = h->d_gx;
@@ -174,15 +202,31 @@ struct Launch {
             pa.dt = dtp;
             pa.E = E;
             pa.ns = ns_params(h);
-            if (mode == MODE_RHS) par_volume_kernel<N, MODE_RHS><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
-            else par_volume_kernel<N, MODE_STEP><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
+            if (h->curved) {
+                pa.inv_jac = h->d_ijn;
+                pa.metrics = h->d_Ja;
+                if (mode == MODE_RHS) par_volume_kernel<N, MODE_RHS, true><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
+                else par_volume_kernel<N, MODE_STEP, true><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
+            } else {
+                if (mode == MODE_RHS) par_volume_kernel<N, MODE_RHS><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
+                else par_volume_kernel<N, MODE_STEP><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
+            }
         }
     }
     static void par_speed(cudaStream_t s, const tlw_handle* h, const double* u) {
         if constexpr (N >= 3) {
             const int E = (int)h->E;
-            par_speed_kernel<N><<<(E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS, MS_THREADS, 0, s>>>(
-                u, h->d_inv_jac, E, ns_params(h), h->d_step, h->d_visc);
+            const int grid = (E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS;
+            if (h->curved) {
+                // the CFL maximum of the curvilinear max_dt, then the parabolic max_dt's own maxima
+                curved_max_speed_kernel<N><<<grid, MS_THREADS, 0, s>>>(u, h->d_Ja, h->d_ijn, E, h->opts.gamma,
+                                                                        h->d_step);
+                par_speed_kernel<N><<<grid, MS_THREADS, 0, s>>>(u, h->d_ijn, E, ns_params(h), h->d_step, h->d_visc,
+                                                                 h->d_visc + 1);
+            } else {
+                par_speed_kernel<N><<<grid, MS_THREADS, 0, s>>>(u, h->d_inv_jac, E, ns_params(h), h->d_step,
+                                                                 h->d_visc, &h->d_step->max_bits);
+            }
         }
     }
     static void par_attributes() {
@@ -190,6 +234,10 @@ struct Launch {
             cudaFuncSetAttribute(par_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)ParCfg<N>::smem_bytes());
             cudaFuncSetAttribute(par_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ParCfg<N>::smem_bytes());
+            cudaFuncSetAttribute(par_volume_kernel<N, MODE_RHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ParCfg<N>::smem_bytes());
+            cudaFuncSetAttribute(par_volume_kernel<N, MODE_STEP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)ParCfg<N>::smem_bytes());
         }
     }
@@ -259,6 +307,13 @@ template <int N> struct ParSpd { static void run(cudaStream_t s, const tlw_handl
 template <int N> struct ParAttr { static void run() { Launch<N>::par_attributes(); } };
 template <int N> struct Mrt { static void run(cudaStream_t s, const MortarArgs& a) { Launch<N>::mortars(s, a); } };
 template <int N> struct CIfc { static void run(cudaStream_t s, const CurvedSurfArgs& a) { Launch<N>::curved_interfaces(s, a); } };
+template <int N> struct CBnd {
+    static void run(cudaStream_t s, const CurvedBndArgs& a) {
+        const long long threads = (long long)a.count * (N + 1);
+        if (threads == 0) return;
+        curved_boundary_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
+    }
+};
 template <int N> struct CSpd {
     static void run(cudaStream_t s, const double* u, const double* Ja, const double* ij, int E, double g, StepState* st) {
         Launch<N>::curved_speed(s, u, Ja, ij, E, g, st);
@@ -323,6 +378,68 @@ void enqueue_limiter(tlw_handle* h, double* u, int reps, unsigned long long* slo
     dispatch<Lim>(h->N, h->stream, a);
 }
 
+// the surfaces of a curvilinear mesh: interfaces colour by colour (no two threads of a launch share a node),
+// then the xi-face and the eta-face boundaries; with the viscous traces for Navier-Stokes
+void enqueue_curved_surfaces(tlw_handle* h, int mode, const double* u_jump, double* out, const double* dt_ptr,
+                             const PhaseEvents* ev) {
+    CurvedSurfArgs ca{};
+    ca.u = u_jump;
+    ca.out = out;
+    ca.tU = h->d_tU;
+    ca.tF = h->d_tF;
+    ca.tFv = h->parabolic ? h->d_tFv : nullptr;
+    ca.metrics = h->d_Ja;
+    ca.inv_jac = h->d_ijn;
+    ca.dt = dt_ptr;
+    ca.step_mode = mode == MODE_STEP;
+    ca.gamma = h->opts.gamma;
+    ca.flux_kind = h->opts.surface_flux;
+    ca.speed_kind = h->opts.max_speed;
+    ca.inv_w_first = h->h_basis.inv_w_first;
+    ca.inv_w_last = h->h_basis.inv_w_last;
+    ca.status = &h->d_step->status;
+    for (size_t c = 0; c + 1 < h->color_off.size(); ++c) {
+        const int b = h->color_off[c];
+        ca.p_elem = h->d_cp + b;
+        ca.s_elem = h->d_cs + b;
+        ca.faces = h->d_cf + b;
+        ca.count = h->color_off[c + 1] - b;
+        dispatch<CIfc>(h->N, h->stream, ca);
+        if (ev && c == 0) cudaEventRecord(ev->after_x, h->stream);
+    }
+    if (ev && h->color_off.size() <= 2) cudaEventRecord(ev->after_x, h->stream);
+    if (h->ncb > 0) {
+        CurvedBndArgs cb{};
+        cb.u = u_jump;
+        cb.out = out;
+        cb.tU = h->d_tU;
+        cb.tF = h->d_tF;
+        cb.tFv = h->parabolic ? h->d_tFv : nullptr;
+        cb.metrics = h->d_Ja;
+        cb.inv_jac = h->d_ijn;
+        cb.wall_kind = h->d_wkind;
+        cb.wall = h->d_wall;
+        cb.dt = dt_ptr;
+        cb.step_mode = mode == MODE_STEP;
+        cb.gamma = h->opts.gamma;
+        cb.flux_kind = h->opts.surface_flux;
+        cb.speed_kind = h->opts.max_speed;
+        cb.inv_w_first = h->h_basis.inv_w_first;
+        cb.inv_w_last = h->h_basis.inv_w_last;
+        cb.status = &h->d_step->status;
+        const int first[2] = {0, h->ncbx}, count[2] = {h->ncbx, h->ncb - h->ncbx};
+        for (int cls = 0; cls < 2; ++cls) {
+            cb.elem = h->d_cbe + first[cls];
+            cb.face = h->d_cbf + first[cls];
+            cb.kind = h->d_cbk + first[cls];
+            cb.index = h->d_cbi + first[cls];
+            cb.count = count[cls];
+            dispatch<CBnd>(h->N, h->stream, cb);
+        }
+    }
+    if (ev) cudaEventRecord(ev->after_y, h->stream);
+}
+
 BndArgs boundary_args(tlw_handle* h, int stage, int mode, const double* u_jump, double* out, const double* dt_ptr) {
     BndArgs ba{};
     ba.u = u_jump;
@@ -360,6 +477,10 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
         // BR1 gradients, parabolic LW volume kernel, then the interfaces with the viscous traces
         dispatch<Par>(h->N, h->stream, (const tlw_handle*)h, mode, u_flux, out, dt_ptr);
         if (ev) cudaEventRecord(ev->after_volume, h->stream);
+        if (h->curved) {
+            enqueue_curved_surfaces(h, mode, u_jump, out, dt_ptr, ev);
+            return;
+        }
         SurfArgs sp{};
         sp.u = u_jump;
         sp.out = out;
@@ -418,33 +539,7 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     dispatch<Vol>(h->N, h->stream, stage, mode, h->sc, va);
     if (ev) cudaEventRecord(ev->after_volume, h->stream);
     if (h->curved) {
-        // interfaces colour by colour (no two launches' threads share a node within a colour)
-        CurvedSurfArgs ca{};
-        ca.u = u_jump;
-        ca.out = out;
-        ca.tU = h->d_tU;
-        ca.tF = h->d_tF;
-        ca.metrics = h->d_Ja;
-        ca.inv_jac = h->d_ijn;
-        ca.dt = dt_ptr;
-        ca.step_mode = mode == MODE_STEP;
-        ca.gamma = h->opts.gamma;
-        ca.flux_kind = h->opts.surface_flux;
-        ca.speed_kind = h->opts.max_speed;
-        ca.inv_w_first = h->h_basis.inv_w_first;
-        ca.inv_w_last = h->h_basis.inv_w_last;
-        ca.status = &h->d_step->status;
-        for (size_t c = 0; c + 1 < h->color_off.size(); ++c) {
-            const int b = h->color_off[c];
-            ca.p_elem = h->d_cp + b;
-            ca.s_elem = h->d_cs + b;
-            ca.faces = h->d_cf + b;
-            ca.count = h->color_off[c + 1] - b;
-            dispatch<CIfc>(h->N, h->stream, ca);
-            if (ev && c == 0) cudaEventRecord(ev->after_x, h->stream);
-        }
-        if (ev && h->color_off.size() <= 2) cudaEventRecord(ev->after_x, h->stream);
-        if (ev) cudaEventRecord(ev->after_y, h->stream);
+        enqueue_curved_surfaces(h, mode, u_jump, out, dt_ptr, ev);
         return;
     }
 
@@ -520,12 +615,12 @@ void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const
         const int grid = std::min<int>((int)((h->E + 255) / 256), 4 * 148);
         cfl_slots_reduce_kernel<<<grid, 256, 0, h->stream>>>(h->d_slots, h->d_inv_jac, (int)h->E, h->d_step);
     } else if (h->sc) enqueue_indicator(h, u, true);   // CFL reduction and indicator in one pass over u
+    else if (h->parabolic) dispatch<ParSpd>(h->N, h->stream, (const tlw_handle*)h, u);   // (curvilinear too)
     else if (h->curved) dispatch<CSpd>(h->N, h->stream, u, (const double*)h->d_Ja, (const double*)h->d_ijn, (int)h->E,
                                        h->opts.gamma, h->d_step);
-    else if (h->parabolic) dispatch<ParSpd>(h->N, h->stream, (const tlw_handle*)h, u);
     else dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, true,
                        false, indicator_args(h));
-    if (h->parabolic) par_finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->d_visc, h->N);
+    if (h->parabolic) par_finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->d_visc, h->N, h->curved ? 1 : 0);
     else finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
     if (after_dt) cudaEventRecord(after_dt, h->stream);
     const double* dtp = &h->d_step->dt;
@@ -561,7 +656,7 @@ int check_ready(tlw_handle* h) {
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
     if (h->nb > 0 && h->bnd_dirichlet && !h->have_bdata)
         return fail(h, TLW_E_STATE, "mesh has Dirichlet boundaries: call tlw_set_boundary_data first");
-    if (h->parabolic && h->nb > 0 && !h->d_wkind)
+    if (h->parabolic && (h->nb > 0 || h->ncb > 0) && !h->d_wkind)
         return fail(h, TLW_E_STATE, "Navier-Stokes with boundaries: call tlw_set_parabolic_walls first");
     return TLW_OK;
 }
@@ -813,6 +908,11 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
     TLW_CUDA(h, cudaMemcpy(h->d_ijn, inverse_jacobian, nodes * sizeof(double), cudaMemcpyHostToDevice));
     if ((rc = up_i(h->d_cp, cp)) || (rc = up_i(h->d_cs, cs)) || (rc = up_i(h->d_cf, cf))) return rc;
     h->color_off = off;
+    h->face_used.assign((size_t)n_elements * 4, 0);
+    for (const Ifc& f : all) {
+        h->face_used[(size_t)f.p * 4 + (f.code & 3)] = 1;
+        h->face_used[(size_t)f.s * 4 + ((f.code >> 2) & 3)] = 1;
+    }
     h->nx = h->ny = 0;
     h->nb = 0; h->nbx = h->nby = 0;
     const size_t sd = state_doubles(h), td = trace_doubles(h);
@@ -872,6 +972,51 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
     return TLW_OK;
 }
 
+int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t* elements, const int32_t* faces,
+                              const int32_t* kinds) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh || !h->curved) return fail(h, TLW_E_STATE, "curved boundaries follow tlw_set_curved_mesh");
+    if (n_boundaries < 0 || (n_boundaries > 0 && (!elements || !faces || !kinds))) return fail(h, TLW_E_ARG, "boundaries");
+    std::vector<int> be[2], bf[2], bk[2], bi[2];
+    std::vector<signed char> used = h->face_used;
+    for (int64_t k = 0; k < n_boundaries; ++k) {
+        const int64_t e = elements[k] - 1;
+        const int f = faces[k];
+        if (e < 0 || e >= h->E || f < 0 || f > 3)
+            return fail(h, TLW_E_ARG, "boundary " + std::to_string(k + 1) + " out of range");
+        if (kinds[k] != TLW_BC_SLIP_WALL_VERTICAL && kinds[k] != TLW_BC_SLIP_WALL_HORIZONTAL)
+            return fail(h, TLW_E_UNSUPPORTED, "curvilinear boundaries: slip walls are built");
+        if (used[(size_t)e * 4 + f])
+            return fail(h, TLW_E_ARG, "boundary " + std::to_string(k + 1) + ": the face already has a neighbour");
+        used[(size_t)e * 4 + f] = 1;
+        const int c = f >> 1;
+        be[c].push_back((int)e); bf[c].push_back(f); bk[c].push_back(kinds[k]); bi[c].push_back((int)k);
+    }
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    for (int** d : {&h->d_cbe, &h->d_cbf, &h->d_cbk, &h->d_cbi})
+        if (*d) { cudaFree(*d); *d = nullptr; }
+    if (h->d_wkind) { cudaFree(h->d_wkind); h->d_wkind = nullptr; }
+    dfree(h->d_wall);
+    h->ncb = (int)n_boundaries;
+    h->ncbx = (int)be[0].size();
+    if (n_boundaries > 0) {
+        auto up = [&](int*& d, const std::vector<int>& a, const std::vector<int>& b) -> int {
+            std::vector<int> v(a);
+            v.insert(v.end(), b.begin(), b.end());
+            TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
+            TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+            return TLW_OK;
+        };
+        int rc;
+        if ((rc = up(h->d_cbe, be[0], be[1])) || (rc = up(h->d_cbf, bf[0], bf[1])) || (rc = up(h->d_cbk, bk[0], bk[1])) ||
+            (rc = up(h->d_cbi, bi[0], bi[1])))
+            return rc;
+    }
+    return TLW_OK;
+}
+
 int tlw_set_boundary_kinds(tlw_handle* h, const int32_t* kinds) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh || h->curved) return fail(h, TLW_E_STATE, "boundary kinds follow tlw_set_tree_mesh");
@@ -895,20 +1040,21 @@ int tlw_set_boundary_kinds(tlw_handle* h, const int32_t* kinds) {
 int tlw_set_parabolic_walls(tlw_handle* h, const int32_t* kinds, const double* wall_data) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh || !h->parabolic) return fail(h, TLW_E_STATE, "walls follow tlw_set_parabolic");
-    if (h->nb == 0) return TLW_OK;
+    const int64_t nbnd = h->curved ? h->ncb : h->nb;
+    if (nbnd == 0) return TLW_OK;
     if (!kinds || !wall_data) return fail(h, TLW_E_ARG, "kinds / wall data");
-    for (int64_t k = 0; k < h->nb; ++k)
+    for (int64_t k = 0; k < nbnd; ++k)
         if (kinds[k] != TLW_WALL_NOSLIP_ADIABATIC && kinds[k] != TLW_WALL_NOSLIP_ISOTHERMAL)
             return fail(h, TLW_E_ARG, "boundary " + std::to_string(k + 1) + ": unknown wall kind");
-    const size_t nd = (size_t)3 * h->n * h->nb;
+    const size_t nd = (size_t)3 * h->n * nbnd;
     for (size_t k = 0; k < nd; ++k)
         if (!std::isfinite(wall_data[k])) return fail(h, TLW_E_ARG, "wall data must be finite");
     TLW_CUDA(h, cudaSetDevice(h->device));
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));
     drop_graphs(h);
-    if (!h->d_wkind) TLW_CUDA(h, cudaMalloc(&h->d_wkind, (size_t)h->nb * sizeof(int)));
+    if (!h->d_wkind) TLW_CUDA(h, cudaMalloc(&h->d_wkind, (size_t)nbnd * sizeof(int)));
     if (!h->d_wall) TLW_CUDA(h, cudaMalloc(&h->d_wall, nd * sizeof(double)));
-    TLW_CUDA(h, cudaMemcpy(h->d_wkind, kinds, (size_t)h->nb * sizeof(int), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, cudaMemcpy(h->d_wkind, kinds, (size_t)nbnd * sizeof(int), cudaMemcpyHostToDevice));
     TLW_CUDA(h, cudaMemcpy(h->d_wall, wall_data, nd * sizeof(double), cudaMemcpyHostToDevice));
     return TLW_OK;
 }
@@ -941,7 +1087,7 @@ int tlw_apply_positivity_limiter(tlw_handle* h) {
 
 int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl) {
     if (!h) return TLW_E_ARG;
-    if (!h->have_mesh || h->curved) return fail(h, TLW_E_STATE, "the parabolic terms follow tlw_set_tree_mesh");
+    if (!h->have_mesh) return fail(h, TLW_E_STATE, "the parabolic terms follow tlw_set_tree_mesh / tlw_set_curved_mesh");
     if (h->opts.time_discretization != TLW_LW || h->sc || h->N < 3 || h->nmx + h->nmy > 0)
         return fail(h, TLW_E_UNSUPPORTED, "Navier-Stokes: LW, FR volume integral, N >= 3, conforming TreeMesh");
     if (!(mu >= 0.0) || !(prandtl > 0.0)) return fail(h, TLW_E_ARG, "mu / Prandtl");
@@ -953,8 +1099,8 @@ int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl) {
         (rc = ensure(h, h->d_tFv, trace_doubles(h))))
         return rc;
     if (!h->d_visc) {
-        TLW_CUDA(h, cudaMalloc(&h->d_visc, sizeof(unsigned long long)));
-        TLW_CUDA(h, cudaMemset(h->d_visc, 0, sizeof(unsigned long long)));
+        TLW_CUDA(h, cudaMalloc(&h->d_visc, 2 * sizeof(unsigned long long)));
+        TLW_CUDA(h, cudaMemset(h->d_visc, 0, 2 * sizeof(unsigned long long)));
     }
     dispatch<ParAttr>(h->N);
     TLW_CUDA(h, cudaGetLastError());
@@ -1088,24 +1234,28 @@ int tlw_max_dt(tlw_handle* h, const double* u, int32_t where, double cfl, double
     const unsigned long long zero = 0;
     TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->max_bits, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
     if (h->parabolic) {
-        // both maxima, combined on the host exactly as par_finalize_dt_kernel does
-        TLW_CUDA(h, cudaMemcpyAsync(h->d_visc, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+        // the maxima, combined on the host exactly as par_finalize_dt_kernel does
+        const unsigned long long zeros[2] = {0, 0};
+        TLW_CUDA(h, cudaMemcpyAsync(h->d_visc, zeros, sizeof(zeros), cudaMemcpyHostToDevice, h->stream));
         dispatch<ParSpd>(h->N, h->stream, (const tlw_handle*)h, du_in);
         TLW_CUDA(h, cudaGetLastError());
-        unsigned long long ba = 0, bv = 0;
+        unsigned long long ba = 0, bv[2] = {0, 0};
         TLW_CUDA(h, cudaMemcpyAsync(&ba, &h->d_step->max_bits, sizeof(ba), cudaMemcpyDeviceToHost, h->stream));
-        TLW_CUDA(h, cudaMemcpyAsync(&bv, h->d_visc, sizeof(bv), cudaMemcpyDeviceToHost, h->stream));
+        TLW_CUDA(h, cudaMemcpyAsync(bv, h->d_visc, sizeof(bv), cudaMemcpyDeviceToHost, h->stream));
         TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->max_bits, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
-        TLW_CUDA(h, cudaMemcpyAsync(h->d_visc, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+        TLW_CUDA(h, cudaMemcpyAsync(h->d_visc, zeros, sizeof(zeros), cudaMemcpyHostToDevice, h->stream));
         if ((rc = read_status(h))) return rc;
-        double la, lv;
+        double la, lv, lq;
         std::memcpy(&la, &ba, sizeof(la));
-        std::memcpy(&lv, &bv, sizeof(lv));
+        std::memcpy(&lv, &bv[0], sizeof(lv));
+        std::memcpy(&lq, &bv[1], sizeof(lq));
+        if (!h->curved) lq = la;
         const double tiny = 4.9406564584124654e-324;
         if (!(la > tiny)) la = tiny;
         if (!(lv > tiny)) lv = tiny;
+        if (!(lq > tiny)) lq = tiny;
         const double k = 2.0 * (2.0 * h->N + 1.0);
-        *dt_out = std::fmin(cfl * (2.0 / (h->n * la)), cfl / ((la + lv * k) * k));
+        *dt_out = std::fmin(cfl * (2.0 / (h->n * la)), cfl / ((lq + lv * k) * k));
         return TLW_OK;
     }
     if (h->curved)

@@ -102,6 +102,7 @@ struct CurvedSurfArgs {
     int flux_kind, speed_kind;
     double inv_w_first, inv_w_last;
     unsigned* status;
+    const double* tFv;        // Navier-Stokes: contravariant viscous flux traces (or null)
 };
 
 template <int N>
@@ -133,6 +134,15 @@ static __global__ void __launch_bounds__(128) curved_interface_kernel(CurvedSurf
         FS[v] *= -sgS;    // F_S . (-n_S)
     }
     lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, FP, FS, uP, uS, UP, US, nrm, Fn, a.status);
+    if (a.tFv) {
+        // minus the mean of both sides' viscous normal fluxes (calc_interface_flux_hyperbolic_parabolic!,
+        // src/solvers/dgsem_p4est/dg_2d_parabolic.jl:1878-1958)
+        double vP[NV], vS[NV];
+        load4(a.tFv + tp, vP);
+        load4(a.tFv + ts, vS);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fn[v] -= 0.5 * (sgP * vP[v] + (-sgS) * vS[v]);
+    }
     const double dts = a.step_mode ? *a.dt : 1.0;
     const double cP = -dts * __ldg(a.inv_jac + (size_t)pe * nn + np) * ((pf & 1) ? a.inv_w_last : a.inv_w_first);
     const double cS = dts * __ldg(a.inv_jac + (size_t)se * nn + ns) * ((sf & 1) ? a.inv_w_last : a.inv_w_first);
@@ -147,6 +157,80 @@ static __global__ void __launch_bounds__(128) curved_interface_kernel(CurvedSurf
 #pragma unroll
     for (int v = 0; v < NV; ++v) x[v] = fma(cS, Fn[v], x[v]);
     store4(oS, x);
+}
+
+// Boundary faces of a curvilinear mesh: the LW slip walls in their normal-direction form
+// (src/equations/equations.jl:137-169; prolong2boundaries! / calc_boundary_flux!, src/solvers/dgsem_p4est/
+// dg_2d.jl:285-393): inner normal flux with the outward normal, the mirrored exterior, the surface flux with the
+// inner side as _ll in the curvilinear order; for Navier-Stokes minus the wall's viscous flux
+// (calc_boundary_flux_lw!, src/solvers/dgsem_p4est/dg_2d_parabolic.jl:2057-2127). One launch per class of faces
+// (xi, eta): a corner node is shared only between the classes.
+struct CurvedBndArgs {
+    const double* u;
+    double* out;
+    const double* tU;
+    const double* tF;         // contravariant flux traces [v, l, face, e]
+    const double* tFv;        // viscous ones (Navier-Stokes) or null
+    const double* metrics;
+    const double* inv_jac;    // [i, j, e]
+    const int* elem;          // boundaries of this class
+    const int* face;
+    const int* kind;          // BC_SLIP_WALL_*
+    const int* index;         // original boundary index (wall data)
+    int count;
+    const int* wall_kind;
+    const double* wall;       // [3, l, B]
+    const double* dt;
+    int step_mode;
+    double gamma;
+    int flux_kind, speed_kind;
+    double inv_w_first, inv_w_last;
+    unsigned* status;
+};
+
+template <int N>
+static __global__ void __launch_bounds__(128) curved_boundary_kernel(CurvedBndArgs a) {
+    constexpr int n = N + 1;
+    constexpr int nn = n * n;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = t / n;
+    const int l = t - k * n;
+    if (k >= a.count) return;
+    const int e = __ldg(a.elem + k), f = __ldg(a.face + k), kind = __ldg(a.kind + k);
+    const int node = face_node_index(n, f, l);
+    const double sg = (f & 1) ? 1.0 : -1.0;
+    double ui[NV], Ui[NV], Fi[NV], uo[NV], Uo[NV], Fo[NV], Fn[NV], J[4];
+    load4(a.u + ((size_t)e * nn + node) * NV, ui);
+    const size_t tb = (((size_t)e * 4 + f) * n + l) * NV;
+    load4(a.tU + tb, Ui);
+    load4(a.tF + tb, Fi);
+    load4(a.metrics + ((size_t)e * nn + node) * 4, J);
+    const double nrm[2] = {sg * (f < 2 ? J[0] : J[2]), sg * (f < 2 ? J[1] : J[3])};
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Fi[v] *= sg;
+    slip_wall_exterior(kind, Fi, Ui, ui, Fo, Uo, uo);
+    lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, Fi, Fo, ui, uo, Ui, Uo, nrm, Fn, a.status);
+    if (a.tFv) {
+        double fv[NV];
+        load4(a.tFv + tb, fv);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fv[v] *= sg;
+        const int b = __ldg(a.index + k);
+        if (__ldg(a.wall_kind + b) == WALL_ADIABATIC) {
+            const double* w = a.wall + 3 * ((size_t)b * n + l);
+            fv[3] = fma(__ldg(w), fv[1], fma(__ldg(w + 1), fv[2], __ldg(w + 2)));
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fn[v] -= fv[v];
+    }
+    const double dts = a.step_mode ? *a.dt : 1.0;
+    const double c = -dts * __ldg(a.inv_jac + (size_t)e * nn + node) * ((f & 1) ? a.inv_w_last : a.inv_w_first);
+    double* o = a.out + ((size_t)e * nn + node) * NV;
+    double x[NV];
+    load4_rw(o, x);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) x[v] = fma(c, Fn[v], x[v]);
+    store4(o, x);
 }
 
 // CFL reduction on curvilinear meshes (Trixi max_dt): per element max_nodes |Ja^1 . (l1, l2)| |J^{-1}| +

@@ -121,6 +121,11 @@ struct tlw_handle {
     double* d_ijn = nullptr;                // inverse Jacobian per node [i, j, e]
     int *d_cp = nullptr, *d_cs = nullptr, *d_cf = nullptr;   // interfaces sorted by colour
     std::vector<int> color_off;             // colour c covers [color_off[c], color_off[c + 1])
+    std::vector<signed char> face_used;     // [e * 4 + face]: 1 when an interface covers the face
+    // boundary faces of the curvilinear mesh: xi faces [0, ncbx), then eta faces [ncbx, ncb); element, face,
+    // slip-wall kind and the boundary's index in the caller's order (wall data)
+    int ncb = 0, ncbx = 0;
+    int *d_cbe = nullptr, *d_cbf = nullptr, *d_cbk = nullptr, *d_cbi = nullptr;
     // graphs: [start buffer] one step, two steps
     cudaGraphExec_t g_one[2] = {nullptr, nullptr};
     cudaGraphExec_t g_two[2] = {nullptr, nullptr};

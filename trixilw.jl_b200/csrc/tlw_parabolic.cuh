@@ -17,6 +17,7 @@
 #include "tlw_device.cuh"
 #include "tlw_surface.cuh"
 #include "tlw_volume.cuh"
+#include "tlw_curved.cuh"
 
 namespace tlw {
 
@@ -67,11 +68,15 @@ struct ParCfg {
     static constexpr size_t smem_bytes() { return (size_t)(2 * nn + 15 * TILE) * sizeof(double); }
 };
 
-// gradient volume term: gx = J^{-1} Dhat u (along i), gy = J^{-1} Dhat u (along j)
-template <int N>
+// gradient volume term: gx = J^{-1} Dhat u (along i), gy = J^{-1} Dhat u (along j); on a curvilinear mesh
+// (metrics [4, i, j, e], inv_jac per node) the two reference derivatives r_xi, r_eta mix as
+// gx = J^{-1} (Ja^1_1 r_xi + Ja^2_1 r_eta), gy = J^{-1} (Ja^1_2 r_xi + Ja^2_2 r_eta) (Trixi calc_gradient! for
+// P4estMesh{2})
+template <int N, bool CURVED = false>
 static __global__ void __launch_bounds__(VolCfg<N>::THREADS) grad_volume_kernel(const double* __restrict__ u,
                                                                               const double* __restrict__ inv_jac,
-                                                                              int E, double* gx, double* gy) {
+                                                                              int E, double* gx, double* gy,
+                                                                              const double* __restrict__ metrics = nullptr) {
     using C = ParCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     __shared__ double sU[NV * EB * nn];
@@ -89,7 +94,9 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS) grad_volume_kernel(
     }
     __syncthreads();
     if (!active) return;
-    const double ij = __ldg(inv_jac + e);
+    const double ij = CURVED ? __ldg(inv_jac + (size_t)e * nn + node) : __ldg(inv_jac + e);
+    double J[4] = {1.0, 0.0, 0.0, 1.0};
+    if (CURVED) load4(metrics + ((size_t)e * nn + node) * 4, J);
     double ox[NV], oy[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
@@ -100,8 +107,13 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS) grad_volume_kernel(
             sx = fma(sDh[i * n + k], p[k + n * j], sx);
             sy = fma(sDh[j * n + k], p[i + n * k], sy);
         }
-        ox[v] = ij * sx;
-        oy[v] = ij * sy;
+        if (CURVED) {
+            ox[v] = ij * fma(J[0], sx, J[2] * sy);
+            oy[v] = ij * fma(J[1], sx, J[3] * sy);
+        } else {
+            ox[v] = ij * sx;
+            oy[v] = ij * sy;
+        }
     }
     store4(gx + ((size_t)e * nn + node) * NV, ox);
     store4(gy + ((size_t)e * nn + node) * NV, oy);
@@ -181,6 +193,78 @@ static __global__ void __launch_bounds__(128) grad_boundary_kernel(const double*
     store4(g, x);
 }
 
+// gradient surface terms on a curvilinear mesh: the face value u* times the element's own outward normal and
+// 1 / w, scaled by J^{-1} of the node, into both gx and gy (interfaces of one colour per launch, so that no
+// launch touches a corner node twice)
+__device__ __forceinline__ void curved_grad_lift(const double* __restrict__ metrics, const double* __restrict__ inv_jac,
+                                                 int n, int e, int f, int node, const double* us, double iw,
+                                                 double* gx, double* gy) {
+    const int nn = n * n;
+    double J[4], x[NV], y[NV];
+    load4(metrics + ((size_t)e * nn + node) * 4, J);
+    const double sg = (f & 1) ? 1.0 : -1.0;
+    const double c = iw * __ldg(inv_jac + (size_t)e * nn + node);
+    const double n0 = sg * (f < 2 ? J[0] : J[2]) * c, n1 = sg * (f < 2 ? J[1] : J[3]) * c;
+    double* px = gx + ((size_t)e * nn + node) * NV;
+    double* py = gy + ((size_t)e * nn + node) * NV;
+    load4_rw(px, x);
+    load4_rw(py, y);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        x[v] = fma(n0, us[v], x[v]);
+        y[v] = fma(n1, us[v], y[v]);
+    }
+    store4(px, x);
+    store4(py, y);
+}
+
+template <int N>
+static __global__ void __launch_bounds__(128) curved_grad_interface_kernel(
+    const double* __restrict__ u, const int* p_elem, const int* s_elem, const int* faces, int count,
+    const double* __restrict__ metrics, const double* __restrict__ inv_jac, double inv_w_first, double inv_w_last,
+    double* gx, double* gy) {
+    constexpr int n = N + 1, nn = n * n;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = t / n;
+    const int l = t - k * n;
+    if (k >= count) return;
+    const int pe = __ldg(p_elem + k), se = __ldg(s_elem + k), code = __ldg(faces + k);
+    const int pf = code & 3, sf = (code >> 2) & 3;
+    const int ls = (code >> 4) & 1 ? n - 1 - l : l;
+    const int np = face_node_index(n, pf, l), ns = face_node_index(n, sf, ls);
+    double uP[NV], uS[NV], us[NV];
+    load4(u + ((size_t)pe * nn + np) * NV, uP);
+    load4(u + ((size_t)se * nn + ns) * NV, uS);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) us[v] = 0.5 * (uP[v] + uS[v]);
+    curved_grad_lift(metrics, inv_jac, n, pe, pf, np, us, (pf & 1) ? inv_w_last : inv_w_first, gx, gy);
+    curved_grad_lift(metrics, inv_jac, n, se, sf, ns, us, (sf & 1) ? inv_w_last : inv_w_first, gx, gy);
+}
+
+template <int N>
+static __global__ void __launch_bounds__(128) curved_grad_boundary_kernel(
+    const double* __restrict__ u, const int* elem, const int* face, const int* index, int count, const int* wall_kind,
+    const double* __restrict__ wall, const double* __restrict__ metrics, const double* __restrict__ inv_jac,
+    double gamma, double inv_w_first, double inv_w_last, double* gx, double* gy) {
+    constexpr int n = N + 1, nn = n * n;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = t / n;
+    const int l = t - k * n;
+    if (k >= count) return;
+    const int e = __ldg(elem + k), f = __ldg(face + k), b = __ldg(index + k);
+    const int node = face_node_index(n, f, l);
+    double ui[NV];
+    load4(u + ((size_t)e * nn + node) * NV, ui);
+    const double* w = wall + 3 * ((size_t)b * n + l);
+    const double v1 = __ldg(w), v2 = __ldg(w + 1);
+    const double rho = ui[0];
+    const double p = __ldg(wall_kind + b) == WALL_ADIABATIC
+                         ? (gamma - 1.0) * (ui[3] - 0.5 * (ui[1] * ui[1] + ui[2] * ui[2]) / rho)
+                         : rho * __ldg(w + 2);
+    const double uo[NV] = {rho, rho * v1, rho * v2, p / (gamma - 1.0) + 0.5 * rho * (v1 * v1 + v2 * v2)};
+    curved_grad_lift(metrics, inv_jac, n, e, f, node, uo, (f & 1) ? inv_w_last : inv_w_first, gx, gy);
+}
+
 struct ParArgs {
     const double* u;
     const double* gx;
@@ -193,6 +277,7 @@ struct ParArgs {
     const double* dt;
     int E;
     NSParams ns;
+    const double* metrics;   // curvilinear: [4, i, j, e] (inv_jac is then per node)
 };
 
 template <int DEPTH>
@@ -215,7 +300,10 @@ struct ParLW {
     }
 };
 
-template <int N, int MODE>
+// CURVED: the stage fluxes are the contravariant ones (Ja^1 . (f_a - f_v, g_a - g_v), Ja^2 . (...)), d_m carries
+// the node's J^{-1} and its gradient J^{-1} (Ja^1_d D_xi d_m + Ja^2_d D_eta d_m) (src/solvers/dgsem_p4est/
+// dg_2d_parabolic.jl:51-104, 641-1787); the face traces are the contravariant fluxes along the face direction.
+template <int N, int MODE, bool CURVED = false>
 static __global__ void __launch_bounds__(ParCfg<N>::THREADS, 1) par_volume_kernel(ParArgs a) {
     using C = ParCfg<N>;
     using K = ParLW<C::DEPTH>;
@@ -259,13 +347,34 @@ static __global__ void __launch_bounds__(ParCfg<N>::THREADS, 1) par_volume_kerne
         return s;
     };
     double u[NV] = {1.0, 0.0, 0.0, 2.5}, gx[NV] = {0, 0, 0, 0}, gy[NV] = {0, 0, 0, 0};
-    double ij = 1.0;
+    double ij = 1.0, J[4] = {1.0, 0.0, 0.0, 1.0};
     if (active) {
         load4(a.u + ((size_t)e * nn + node) * NV, u);
         load4(a.gx + ((size_t)e * nn + node) * NV, gx);
         load4(a.gy + ((size_t)e * nn + node) * NV, gy);
-        ij = __ldg(a.inv_jac + e);
+        if (CURVED) {
+            ij = __ldg(a.inv_jac + (size_t)e * nn + node);
+            load4(a.metrics + ((size_t)e * nn + node) * 4, J);
+        } else {
+            ij = __ldg(a.inv_jac + e);
+        }
     }
+    // the flux pair along the reference coordinates
+    auto contra = [&](double f, double g, double& cf, double& cg) {
+        if (CURVED) {
+            cf = fma(J[0], f, J[1] * g);
+            cg = fma(J[2], f, J[3] * g);
+        } else {
+            cf = f;
+            cg = g;
+        }
+    };
+    auto put_pair = [&](int v, double f, double g) {
+        double cf, cg;
+        contra(f, g, cf, cg);
+        put(X, v, cf);
+        put(Y, v, cg);
+    };
     const double dt = *a.dt;
     const double sc = -dt * ij;
     const double gm1 = a.ns.gamma - 1.0;
@@ -285,8 +394,7 @@ static __global__ void __launch_bounds__(ParCfg<N>::THREADS, 1) par_volume_kerne
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             Fv[v] = fv[v]; Gv[v] = gv[v]; U[v] = u[v];
-            put(X, v, Fa[v] - fv[v]);
-            put(Y, v, Ga[v] - gv[v]);
+            put_pair(v, Fa[v] - fv[v], Ga[v] - gv[v]);
         }
     }
     // d and its gradient from the stage fluxes in X, Y
@@ -301,8 +409,14 @@ static __global__ void __launch_bounds__(ParCfg<N>::THREADS, 1) par_volume_kerne
         __syncthreads();
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            dx[v] = ij * cx(sD, W, v);
-            dy[v] = ij * cy(sD, W, v);
+            const double r1 = cx(sD, W, v), r2 = cy(sD, W, v);
+            if (CURVED) {
+                dx[v] = ij * fma(J[0], r1, J[2] * r2);
+                dy[v] = ij * fma(J[1], r1, J[3] * r2);
+            } else {
+                dx[v] = ij * r1;
+                dy[v] = ij * r2;
+            }
         }
         __syncthreads();
     };
@@ -352,19 +466,13 @@ static __global__ void __launch_bounds__(ParCfg<N>::THREADS, 1) par_volume_kerne
         }
         if (s < DEPTH) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                put(X, v, sfa[v] - sfv[v]);
-                put(Y, v, sga[v] - sgv[v]);
-            }
+            for (int v = 0; v < NV; ++v) put_pair(v, sfa[v] - sfv[v], sga[v] - sgv[v]);
             derive();
         }
     }
-    // du = Dhat (Fa - Fv) + Dhat (Ga - Gv)
+    // du = Dhat (Fa - Fv) + Dhat (Ga - Gv) (contravariant on a curvilinear mesh)
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-        put(X, v, Fa[v] - Fv[v]);
-        put(Y, v, Ga[v] - Gv[v]);
-    }
+    for (int v = 0; v < NV; ++v) put_pair(v, Fa[v] - Fv[v], Ga[v] - Gv[v]);
     __syncthreads();
     if (!active) return;
     double acc[NV], o[NV];
@@ -379,6 +487,19 @@ static __global__ void __launch_bounds__(ParCfg<N>::THREADS, 1) par_volume_kerne
         for (int v = 0; v < NV; ++v) o[v] = fma(sc, acc[v], u[v]);
     }
     store4(a.out + off, o);
+    if (CURVED) {
+        // traces: the fluxes along the face's reference direction
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            double cf, cg;
+            contra(Fa[v], Ga[v], cf, cg);
+            Fa[v] = cf;
+            Ga[v] = cg;
+            contra(Fv[v], Gv[v], cf, cg);
+            Fv[v] = cf;
+            Gv[v] = cg;
+        }
+    }
     const size_t tb = (size_t)e * 4 * n * NV;
     if (i == 0) { store4(a.tU + tb + (0 * n + j) * NV, U); store4(a.tF + tb + (0 * n + j) * NV, Fa); store4(a.tFv + tb + (0 * n + j) * NV, Fv); }
     if (i == n - 1) { store4(a.tU + tb + (1 * n + j) * NV, U); store4(a.tF + tb + (1 * n + j) * NV, Fa); store4(a.tFv + tb + (1 * n + j) * NV, Fv); }
@@ -388,11 +509,15 @@ static __global__ void __launch_bounds__(ParCfg<N>::THREADS, 1) par_volume_kerne
 
 // advective and viscous maxima for the parabolic dt: max_bits <- max_e J^{-1} (l1 + l2),
 // visc_bits <- max_nodes J^{-2} max(4 mu / (3 rho), mu kappa / (rho Pr))
+// (on a curvilinear mesh inv_jac is the per-node array and element e reads its e-th entry, which is how the
+// reference's parabolic max_dt indexes cache.elements.inverse_jacobian[element] on a P4estMesh; adv_bits then
+// receives this TreeMesh-style advective maximum, the CFL one comes from curved_max_speed_kernel)
 template <int N>
 static __global__ void __launch_bounds__(MS_THREADS) par_speed_kernel(const double* __restrict__ u,
                                                                       const double* __restrict__ inv_jac, int E,
                                                                       NSParams ns, StepState* s,
-                                                                      unsigned long long* visc_bits) {
+                                                                      unsigned long long* visc_bits,
+                                                                      unsigned long long* adv_bits) {
     constexpr int n = N + 1, nn = n * n;
     constexpr int ELEMS = MsCfg<N>::ELEMS;
     __shared__ double l1s[ELEMS * nn], l2s[ELEMS * nn];
@@ -439,21 +564,24 @@ static __global__ void __launch_bounds__(MS_THREADS) par_speed_kernel(const doub
             b = fmax(b, wmax[w]);
             bv = fmax(bv, wvis[w]);
         }
-        if (b > 0.0) atomicMax(&s->max_bits, (unsigned long long)__double_as_longlong(b));
+        if (b > 0.0) atomicMax(adv_bits, (unsigned long long)__double_as_longlong(b));
         if (bv > 0.0) atomicMax(visc_bits, (unsigned long long)__double_as_longlong(bv));
     }
 }
 
-// dt = min(cfl 2 / (n lam_a), cfl / ((lam_a + 2 (2N + 1) lam_v) 2 (2N + 1))), then the set_dt! clamp
-static __global__ void par_finalize_dt_kernel(StepState* s, unsigned long long* visc_bits, int N) {
+// dt = min(cfl 2 / (n lam_a), cfl / ((lam_a' + 2 (2N + 1) lam_v) 2 (2N + 1))), then the set_dt! clamp;
+// lam_a' = lam_a on a TreeMesh, visc_bits[1] (the parabolic max_dt's own advective maximum) when curved
+static __global__ void par_finalize_dt_kernel(StepState* s, unsigned long long* visc_bits, int N, int curved = 0) {
     const double tiny = 4.9406564584124654e-324;
     double la = __longlong_as_double((long long)s->max_bits);
-    double lv = __longlong_as_double((long long)*visc_bits);
+    double lv = __longlong_as_double((long long)visc_bits[0]);
+    double lq = curved ? __longlong_as_double((long long)visc_bits[1]) : la;
     if (!(la > tiny)) la = tiny;
     if (!(lv > tiny)) lv = tiny;
+    if (!(lq > tiny)) lq = tiny;
     const double k = 2.0 * (2.0 * N + 1.0);
     const double dt_adv = s->cfl * (2.0 / ((N + 1) * la));
-    const double dt_visc = s->cfl / ((la + lv * k) * k);
+    const double dt_visc = s->cfl / ((lq + lv * k) * k);
     double dt = s->fixed_dt > 0.0 ? s->fixed_dt : fmin(dt_adv, dt_visc);
     const double t = s->t, te = s->t_end;
     const bool finished = run_finished(t, te);
@@ -463,7 +591,8 @@ static __global__ void par_finalize_dt_kernel(StepState* s, unsigned long long* 
     s->t = finished ? t : t + dt;
     if (!finished) s->steps += 1;
     s->max_bits = 0ull;
-    *visc_bits = 0ull;
+    visc_bits[0] = 0ull;
+    if (curved) visc_bits[1] = 0ull;
 }
 
 }  // namespace tlw

@@ -43,6 +43,7 @@ EXPORTED = (
     "tlw_solve_dts", "tlw_set_curved_mesh", "tlw_curved_colors", "tlw_set_tree_mortars",
     "tlw_set_parabolic", "tlw_adaptive_trial", "tlw_adaptive_accept",
     "tlw_set_positivity_limiter", "tlw_apply_positivity_limiter", "tlw_set_boundary_kinds", "tlw_set_parabolic_walls",
+    "tlw_set_curved_boundaries",
 )
 
 
@@ -118,6 +119,7 @@ def lib() -> ctypes.CDLL:
     L.tlw_apply_positivity_limiter.argtypes = [P]
     L.tlw_set_boundary_kinds.argtypes = [P, P]
     L.tlw_set_parabolic_walls.argtypes = [P, P, P]
+    L.tlw_set_curved_boundaries.argtypes = [P, i64, P, P, P]
     L.tlw_adaptive_trial.argtypes = [P, dbl, dbl, dbl, dp, ctypes.POINTER(ctypes.c_int32)]
     L.tlw_adaptive_accept.argtypes = [P, dbl]
     L.tlw_curved_colors.argtypes = [P]

@@ -12,8 +12,9 @@ coordinates mapping(xi_g, eta_g) at the global reference coordinates of the GLL 
 (cell + (xi + 1) / 2) * 2 / cells - 1 so that the two elements of a face see bitwise identical face nodes
 (Trixi writes the same points as -1 + (cell - 1) dx + dx / 2 (1 + xi)). Interfaces take the right / upper
 element as primary (its -xi / -eta face), which is the normal StructuredMesh's calc_interface_flux! uses
-(src/solvers/dgsem_structured/dg_2d.jl:2233-2267). Periodic in both directions (boundaries are not built
-on the curvilinear device path).
+(src/solvers/dgsem_structured/dg_2d.jl:2233-2267). A non-periodic direction has boundary faces instead of the
+wrap-around interfaces, listed by direction (x_neg: the -xi faces of the first column, x_pos, y_neg, y_pos),
+as a P4estMesh's named boundaries :x_neg, :x_pos, :y_neg, :y_pos.
 """
 from __future__ import annotations
 
@@ -45,7 +46,8 @@ class CurvedMesh:
     n_boundaries = 0
 
     def __init__(self, xy: np.ndarray, polydeg: int, primary_elements, primary_faces, secondary_elements,
-                 secondary_faces, secondary_reversed, area: float):
+                 secondary_faces, secondary_reversed, area: float, boundary_elements=(), boundary_faces=(),
+                 n_boundaries_per_direction=(0, 0, 0, 0)):
         self.polydeg = polydeg
         self.xy = np.ascontiguousarray(xy)                   # [2, n, n, E]
         self.n_elements = xy.shape[-1]
@@ -59,11 +61,26 @@ class CurvedMesh:
         self.secondary_reversed = np.ascontiguousarray(secondary_reversed, dtype=np.int32)
         self.n_interfaces = len(self.primary_elements)
         self.area = float(area)
+        # boundary faces, grouped by direction (x_neg, x_pos, y_neg, y_pos); elements 1-based
+        self.boundary_elements = np.ascontiguousarray(boundary_elements, dtype=np.int64)
+        self.boundary_faces = np.ascontiguousarray(boundary_faces, dtype=np.int32)
+        self.n_boundaries = len(self.boundary_elements)
+        self.n_boundaries_per_direction = np.asarray(n_boundaries_per_direction, dtype=np.int64)
 
     def node_coordinates(self, polydeg: int) -> np.ndarray:
         if polydeg != self.polydeg:
             raise ValueError("this curved mesh was built for polydeg %d" % self.polydeg)
         return self.xy
+
+    def boundary_node_coordinates(self, polydeg: int) -> np.ndarray:
+        """[2, n, B] coordinates of each boundary face's nodes in the element's own index order."""
+        xy = self.node_coordinates(polydeg)
+        n = polydeg + 1
+        out = np.empty((2, n, self.n_boundaries))
+        for b, (e, f) in enumerate(zip(self.boundary_elements - 1, self.boundary_faces)):
+            out[:, :, b] = (xy[:, 0, :, e] if f == 0 else xy[:, n - 1, :, e] if f == 1 else
+                            xy[:, :, 0, e] if f == 2 else xy[:, :, n - 1, e])
+        return out
 
     def ndofs(self, polydeg: int) -> int:
         return self.n_elements * (polydeg + 1) ** 2
@@ -83,12 +100,15 @@ class StructuredMesh:
     def __init__(self, cells_per_dimension, mapping, periodicity=True):
         if isinstance(periodicity, bool):
             periodicity = (periodicity, periodicity)
-        if not all(periodicity):
-            raise NotImplementedError("boundaries are not built on the curvilinear device path: use a periodic mesh")
+        self.periodicity = tuple(bool(p) for p in periodicity)
         self.cells = tuple(int(c) for c in cells_per_dimension)
         self.mapping = mapping
         nx, ny = self.cells
         self.n_elements = nx * ny
+        px, py = self.periodicity
+        self.n_boundaries_per_direction = np.array([0 if px else ny, 0 if px else ny, 0 if py else nx, 0 if py else nx],
+                                                   dtype=np.int64)
+        self.n_boundaries = int(self.n_boundaries_per_direction.sum())
         self._curved = {}
 
     def element(self, cx, cy):
@@ -111,23 +131,41 @@ class StructuredMesh:
     def curved(self, polydeg: int) -> CurvedMesh:
         if polydeg not in self._curved:
             nx, ny = self.cells
+            px, py = self.periodicity
             pe, pf, se, sf = [], [], [], []
             for cy in range(ny):
                 for cx in range(nx):
+                    if cx == 0 and not px:
+                        continue
                     e = self.element(cx, cy)
                     pe.append(e); pf.append(0); se.append(self.element((cx - 1) % nx, cy)); sf.append(1)
             for cy in range(ny):
                 for cx in range(nx):
+                    if cy == 0 and not py:
+                        continue
                     e = self.element(cx, cy)
                     pe.append(e); pf.append(2); se.append(self.element(cx, (cy - 1) % ny)); sf.append(3)
+            be, bf = [], []
+            if not px:
+                for face, cx in ((0, 0), (1, nx - 1)):
+                    for cy in range(ny):
+                        be.append(self.element(cx, cy)); bf.append(face)
+            if not py:
+                for face, cy in ((2, 0), (3, ny - 1)):
+                    for cx in range(nx):
+                        be.append(self.element(cx, cy)); bf.append(face)
             xy = self.node_coordinates(polydeg)
             area = float(np.einsum("eji,j,i->", 1.0 / metric_terms(xy, polydeg)[1], *(2 * [gauss_lobatto(polydeg)[1]])))
             self._curved[polydeg] = CurvedMesh(xy, polydeg, np.array(pe) + 1, pf, np.array(se) + 1, sf,
-                                               np.zeros(len(pe), dtype=np.int32), area)
+                                               np.zeros(len(pe), dtype=np.int32), area, np.array(be, dtype=np.int64) + 1,
+                                               bf, self.n_boundaries_per_direction)
         return self._curved[polydeg]
 
     def ndofs(self, polydeg: int) -> int:
         return self.n_elements * (polydeg + 1) ** 2
+
+    def boundary_node_coordinates(self, polydeg: int) -> np.ndarray:
+        return self.curved(polydeg).boundary_node_coordinates(polydeg)
 
 
 # rotation of an element's local frame by a quarter turn: new node (a, b) holds old node (n-1-b, a);
@@ -159,7 +197,9 @@ def rotate_elements(mesh: CurvedMesh, turns) -> CurvedMesh:
         fp, flp = face_map(int(mesh.primary_faces[k]), int(turns[pe[k]]))
         fs, fls = face_map(int(mesh.secondary_faces[k]), int(turns[se[k]]))
         pf.append(fp); sf.append(fs); rev.append(int(mesh.secondary_reversed[k]) ^ flp ^ fls)
-    return CurvedMesh(xy, mesh.polydeg, mesh.primary_elements, pf, mesh.secondary_elements, sf, rev, mesh.area)
+    bf = [face_map(int(f), int(turns[e - 1]))[0] for e, f in zip(mesh.boundary_elements, mesh.boundary_faces)]
+    return CurvedMesh(xy, mesh.polydeg, mesh.primary_elements, pf, mesh.secondary_elements, sf, rev, mesh.area,
+                      mesh.boundary_elements, bf, mesh.n_boundaries_per_direction)
 
 
 def rot_nodes(a: np.ndarray) -> np.ndarray:

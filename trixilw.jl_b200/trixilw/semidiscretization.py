@@ -296,6 +296,8 @@ class SemidiscretizationHyperbolic:
         for d, bc in zip(DIRECTIONS, self._bcs):
             if not isinstance(bc, (BoundaryConditionDirichlet, BoundaryConditionSlipWall)):
                 raise ValueError(f"{d}: a non-periodic TreeMesh needs BoundaryConditionDirichlet or a slip wall")
+            if self.curved is not None and not isinstance(bc, BoundaryConditionSlipWall):
+                raise NotImplementedError(f"{d}: curvilinear boundaries are built for the slip walls")
         self.cache = {"dt": [math.nan]}
         sf = solver.surface_flux
         opts = _lib.TlwOpts()
@@ -388,6 +390,13 @@ class SemidiscretizationHyperbolic:
         for (a, b), bc in zip(self._direction_ranges(), self._bcs):
             kinds[a:b] = bc.code if isinstance(bc, BoundaryConditionSlipWall) else _lib.TLW_BC_DIRICHLET
         self._kinds = kinds
+        if self.curved is not None:
+            c = self.curved
+            self._cbkeep = (np.ascontiguousarray(c.boundary_elements, dtype=np.int64),
+                            np.ascontiguousarray(c.boundary_faces, dtype=np.int32), kinds)
+            check(self.handle, lib().tlw_set_curved_boundaries(self.handle, c.n_boundaries, _ptr(self._cbkeep[0]),
+                                                               _ptr(self._cbkeep[1]), _ptr(kinds)))
+            return
         check(self.handle, lib().tlw_set_boundary_kinds(self.handle, _ptr(kinds)))
 
     def time_dependent_boundaries(self) -> bool:
