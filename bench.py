@@ -41,7 +41,11 @@ WORKLOADS = {
     "riemann_tree512_N4_lw": (9, 4, "lw", "riemann"),
     # StructuredMesh{2} 512 x 512 on [-10, 10]^2 warped by x += sin(pi (x+10)/10) sin(pi (y+10)/10) (same for y)
     "vortex_warped512_N4_lw": (9, 4, "lw", "warped"),
+    # compressible Navier-Stokes lid-driven cavity (Re 1000, Ma 0.1, Pr 0.72): [0, 1]^2 with 64 x 64 elements
+    # warped by x += 0.05 sin(pi x) sin(pi y) (same for y), slip walls + no-slip adiabatic walls, lid v1 = 1
+    "cavity_warped64_N4_ns": (6, 4, "lw", "cavity"),
 }
+CAVITY_MU, CAVITY_PR, CAVITY_P0 = 0.001, 0.72, 1.0 / (0.1 ** 2 * 1.4)
 # batched form: 512 independent vortex instances (per-instance seed 0..511: side from {8, 16, 32, 64}
 # elements, degree from {3, 4, 5}, strength ~ U[1, 5], centre ~ U[-2, 2]^2), 50 LW steps
 BATCH_WORKLOADS = {"batched512_vortex_lw": 512}
@@ -68,6 +72,16 @@ def volume_kernel_bytes_per_element(N: int, td: str, curved: bool = False) -> fl
     (5 n^2)."""
     n, nv = N + 1, 4
     return 8.0 * (2 * nv * n * n + 2 * 4 * n * nv + (5 * n * n if curved else 0))
+
+
+def ns_volume_bytes_per_element(N: int) -> float:
+    """Algorithmic bytes of the Navier-Stokes launches before the surfaces, per element on a curvilinear mesh:
+    the BR1 gradient (read u, Ja, J^-1; write both gradients) and the parabolic LW volume kernel (read u, both
+    gradients, Ja, J^-1; write u_new and the U, F.n, Fv.n face traces)."""
+    n, nv = N + 1, 4
+    grad = nv * n * n + 5 * n * n + 2 * nv * n * n
+    vol = 3 * nv * n * n + 5 * n * n + nv * n * n + 3 * 4 * n * nv
+    return 8.0 * (grad + vol)
 
 
 def volume_flops_per_node(N: int) -> float:
@@ -159,7 +173,23 @@ def warp_mapping(xi, eta):
     return X + s, Y + s
 
 
+def cavity_mapping(xi, eta):
+    """[-1, 1]^2 -> [0, 1]^2, then x += 0.05 sin(pi x) sin(pi y) and y likewise (the sides stay straight)."""
+    import numpy as np
+    X = 0.5 * (xi + 1.0)
+    Y = 0.5 * (eta + 1.0)
+    s = 0.05 * np.sin(np.pi * X) * np.sin(np.pi * Y)
+    return X + s, Y + s
+
+
+def cavity_ic(tl):
+    return tl.ConstantState(rho=1.0, v1=0.0, v2=0.0, p=CAVITY_P0)
+
+
 def make_mesh(tl, level, icname):
+    if icname == "cavity":
+        m = 1 << level
+        return tl.StructuredMesh((m, m), cavity_mapping, periodicity=False)
     if icname == "warped":
         m = 1 << level
         return tl.StructuredMesh((m, m), warp_mapping)
@@ -175,6 +205,18 @@ def build_semi(tl, level, N, td, icname, device):
     if icname == "warped":
         return tl.SemidiscretizationHyperbolic(make_mesh(tl, level, icname), tdo, eq, tl.IsentropicVortex(5.0),
                                                solver, device=device)
+    if icname == "cavity":
+        eq_par = tl.CompressibleNavierStokesDiffusion2D(eq, mu=CAVITY_MU, Prandtl=CAVITY_PR,
+                                                        gradient_variables=tl.GradientVariablesConservative())
+        slip = {"x_neg": tl.boundary_condition_slip_wall_vertical, "x_pos": tl.boundary_condition_slip_wall_vertical,
+                "y_neg": tl.boundary_condition_slip_wall_horizontal, "y_pos": tl.boundary_condition_slip_wall_horizontal}
+        heat = tl.Adiabatic(lambda x, y, t, e: 0.0)
+        wall = tl.BoundaryConditionNavierStokesWall(tl.NoSlip(lambda x, y, t, e: (0.0, 0.0)), heat)
+        lid = tl.BoundaryConditionNavierStokesWall(tl.NoSlip(lambda x, y, t, e: (1.0, 0.0)), heat)
+        walls = {"x_neg": wall, "x_pos": wall, "y_neg": wall, "y_pos": lid}
+        return tl.SemidiscretizationHyperbolicParabolic(make_mesh(tl, level, icname), tdo, (eq, eq_par),
+                                                        cavity_ic(tl), solver, device=device,
+                                                        boundary_conditions=(slip, walls))
     if icname == "vortex":
         mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), level)
         ic = tl.IsentropicVortex(5.0)
@@ -215,11 +257,21 @@ def cpu_oracle_rate(level, N, td, icname, steps_hint, budget_s=20.0):
 
     eq = tl.CompressibleEulerEquations2D(1.4)
     mesh = make_mesh(tl, level, icname)
-    ic = tl.FourQuadrantRiemann() if icname == "riemann" else tl.IsentropicVortex(5.0)
-    xy = mesh.curved(N).xy if icname == "warped" else mesh.node_coordinates(N)
+    ic = (tl.FourQuadrantRiemann() if icname == "riemann" else cavity_ic(tl) if icname == "cavity"
+          else tl.IsentropicVortex(5.0))
+    xy = mesh.curved(N).xy if icname in ("warped", "cavity") else mesh.node_coordinates(N)
     u = np.ascontiguousarray(np.transpose(ic(xy[0], xy[1], 0.0, eq), (2, 1, 0, 3))).reshape(-1)
     o = pyoracle.Oracle(mesh, N)
-    if mesh.n_boundaries:
+    if icname == "cavity":
+        cm = mesh.curved(N)
+        per = cm.n_boundaries_per_direction
+        o.set_curved_boundaries(cm.boundary_elements, cm.boundary_faces,
+                                np.repeat(np.array([1, 1, 2, 2], dtype=np.int32), per))
+        o.set_parabolic(CAVITY_MU, CAVITY_PR)
+        data = np.zeros((cm.n_boundaries, N + 1, 3))
+        data[per[:3].sum():, :, 0] = 1.0
+        o.set_walls(np.ones(cm.n_boundaries, dtype=np.int32), data)
+    elif mesh.n_boundaries:
         bxy = mesh.boundary_node_coordinates(N)
         now = np.ascontiguousarray(np.transpose(ic(bxy[0], bxy[1], 0.0, eq), (1, 0, 2)))
         o.set_boundary_data(np.repeat(now[:, :, None, :], N + 1, axis=2), now)
@@ -442,15 +494,17 @@ def run_ours(args):
 
     if rank == 0:
         E = semi.mesh.n_elements
-        curved = icname == "warped"
+        curved = icname in ("warped", "cavity")
+        ns = icname == "cavity"
         peak, peak_kind = measured_peaks()
         vol_ms = phase[1] / args.steps
-        vol_bytes = volume_kernel_bytes_per_element(N, td, curved) * E
+        vol_bytes = (ns_volume_bytes_per_element(N) if ns else volume_kernel_bytes_per_element(N, td, curved)) * E
         achieved = vol_bytes / (vol_ms * 1e-3) / 1e9
         fp = ctypes.c_double()
         fp64_peak = fp.value if L.tlw_probe_fp64_tflops(local_rank, ctypes.byref(fp)) == 0 else None
-        vol_flops = volume_flops_per_node(N) * ndofs
-        tag = f"lw_volume_kernel_N{N}_{'warped' if curved else 'tree'}{1 << level}"
+        vol_flops = None if ns else volume_flops_per_node(N) * ndofs
+        tag = (f"par_volume_kernel_N{N}_cavity{1 << level}" if ns
+               else f"lw_volume_kernel_N{N}_{'warped' if curved else 'tree'}{1 << level}")
         traffic = profile_traffic(tag)
         step_alg = alg_bytes_per_element_step(N, td, curved) * E
         out = {
@@ -463,14 +517,18 @@ def run_ours(args):
                        "parallelism": f"replicas{world}" if world > 1 else "single"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                     "steps": n_e2e},
-            "roofline": {"kernel": f"lw_volume_kernel<{N}, MODE_STEP{', CURVED' if curved else ''}>", "bound": "hbm",
+            "roofline": {"kernel": (f"grad_volume_kernel + curved_grad_*_kernel + par_volume_kernel<{N}, MODE_STEP, CURVED>"
+                                    if ns else f"lw_volume_kernel<{N}, MODE_STEP{', CURVED' if curved else ''}>"),
+                         "bound": "hbm",
                          "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                          "alg_bytes_per_launch": vol_bytes, "ms_per_launch": vol_ms,
-                         "fp64": {"achieved_tflops": vol_flops / (vol_ms * 1e-3) / 1e12, "peak_tflops": fp64_peak,
-                                  "frac": (vol_flops / (vol_ms * 1e-3) / 1e12) / fp64_peak if fp64_peak else None,
-                                  "peak_source": "measured live (register FMA loop)"},
+                         "fp64": ({"achieved_tflops": vol_flops / (vol_ms * 1e-3) / 1e12, "peak_tflops": fp64_peak,
+                                   "frac": (vol_flops / (vol_ms * 1e-3) / 1e12) / fp64_peak if fp64_peak else None,
+                                   "peak_source": "measured live (register FMA loop)"} if vol_flops else
+                                  {"achieved_tflops": None, "peak_tflops": fp64_peak,
+                                   "note": "no algorithmic flop model for the Navier-Stokes kernels"}),
                          "step": {"alg_bytes_per_step": step_alg,
                                   "achieved_gbs": step_alg * args.steps / (ms_max * 1e-3) / 1e9,
                                   "frac": step_alg * args.steps / (ms_max * 1e-3) / 1e9 / peak},
@@ -478,8 +536,9 @@ def run_ours(args):
                                                "x_faces": phase[2] / args.steps, "y_faces": phase[3] / args.steps,
                                                "step": phase[4] / args.steps}},
             "clocks": clocks,
-            "gpu_launches": args.steps * (2 + (3 + (2 if semi.mesh.n_boundaries else 0)) * (2 if td == "mdrk" else 1)
-                                          + (1 if icname == "riemann" else 0)),
+            "gpu_launches": args.steps * ((9 + 2 * int(L.tlw_curved_colors(semi.handle))) if ns else
+                                          (2 + (3 + (2 if semi.mesh.n_boundaries else 0)) * (2 if td == "mdrk" else 1)
+                                           + (1 if icname == "riemann" else 0))),
         }
         if world == 1 and not args.no_cpu_baseline:
             rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=args.steps)
