@@ -48,8 +48,8 @@ void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, do
         rhs(h->basis, h->eq, h->opt, h->mesh, u, u2, du, t, dt, bd, kind, h->ws, nthreads);
         return;
     }
-    if (kind != 0 || h->opt.shock_capturing) throw std::runtime_error("curvilinear oracle: LW, FR volume integral only");
-    rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads);
+    if (h->opt.shock_capturing) throw std::runtime_error("curvilinear oracle: FR volume integral only");
+    rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, kind, u2);
 }
 
 double any_max_dt(oracle_handle* h, const double* u, double cfl, bool& bad, int nthreads) {

@@ -246,8 +246,11 @@ inline void surface_integral_and_jacobian_curved(const Basis& b, const CurvedMes
 }
 
 // du = rhs(u) on a conforming curvilinear mesh (LW, FR volume integral; boundaries: slip walls)
+// kind 0: LW rhs!; 1: rhs_mdrk1! (keeps U2, F2); 2: rhs_mdrk2! with the stage state u2 in the volume terms and
+// u (u^n) at the interfaces (src/solvers/dgsem_structured/multi_derivative_2d.jl:1-80)
 inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m, const double* u,
-                       double* du, double dt, Workspace& ws, int nthreads = 1) {
+                       double* du, double dt, Workspace& ws, int nthreads = 1, int kind = 0,
+                       const double* u2 = nullptr) {
     const int n = b.n, nn = n * n;
     const size_t ndof = (size_t)NV * nn * m.n_elements;
     const double nan = std::numeric_limits<double>::quiet_NaN();
@@ -255,9 +258,20 @@ inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, cons
     ws.F.assign(2 * ndof, nan);
     ws.surface_flux_values.assign((size_t)NV * n * 4 * m.n_elements, nan);
     ws.bad = false;
+    if (kind == 1) {
+        ws.U2.assign(ndof, nan);
+        ws.F2.assign(2 * ndof, nan);
+    }
+    if (kind == 2 && (ws.U2.size() != ndof || !u2)) throw std::invalid_argument("rhs_mdrk2 before rhs_mdrk1");
     for (size_t k = 0; k < ndof; ++k) du[k] = 0.0;
 #pragma omp parallel for num_threads(nthreads) schedule(static)
-    for (int e = 0; e < m.n_elements; ++e) lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws);
+    for (int e = 0; e < m.n_elements; ++e) {
+        const double* Jae = &m.Ja[4 * (size_t)nn * e];
+        const double* ije = &m.inv_jac[(size_t)nn * e];
+        if (kind == 0) lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws);
+        else if (kind == 1) mdrk1_volume_element(b, eq, e, u, du, dt, 0.0, 1.0, ws, Jae, ije);
+        else mdrk2_volume_element(b, eq, e, u2, du, dt, 0.0, 1.0, ws, Jae, ije);
+    }
     bool bad = false;
 #pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad)
     for (int k = 0; k < m.n_interfaces; ++k) {

@@ -620,8 +620,24 @@ inline void lw_volume_element(const Basis& b, const Euler& eq, const Options& op
 // no source terms. Stage 1 as shipped unpacks `u_low` from a cache that has no such field (:287); the
 // value is write-only on this path (it never reaches du, U, F, U2 or F2), so it is not computed here.
 // ------------------------------------------------------------------------------------------------
+// On a curvilinear mesh (Jae = the element's contravariant vectors [4, i, j], ije = its inverse Jacobian per
+// node; mdrk_kernel_1! / _2! of src/solvers/dgsem_structured/multi_derivative_2d.jl:82-445) the contractions
+// take the contravariant fluxes and ut carries the node's J^{-1}; F, F2 stay physical.
+inline void mdrk_contra(const double* Jae, int n, int i, int j, const double* f, const double* g, double* cf, double* cg) {
+    if (!Jae) {
+        for (int v = 0; v < NV; ++v) { cf[v] = f[v]; cg[v] = g[v]; }
+        return;
+    }
+    const double* J = Jae + 4 * (i + n * j);
+    for (int v = 0; v < NV; ++v) {
+        cf[v] = J[0] * f[v] + J[1] * g[v];
+        cg[v] = J[2] * f[v] + J[3] * g[v];
+    }
+}
+
 inline void mdrk1_volume_element(const Basis& b, const Euler& eq, int e, const double* u, double* du, double dt,
-                                 double inv_jac, double alpha, Workspace& ws) {
+                                 double inv_jac, double alpha, Workspace& ws, const double* Jae = nullptr,
+                                 const double* ije = nullptr) {
     const int n = b.n, nn = n * n;
     Tile Fh, Gh, F2, G2, Uh, U2, ut, f, g;
     ut.zero(NV * nn);
@@ -639,16 +655,18 @@ inline void mdrk1_volume_element(const Basis& b, const Euler& eq, int e, const d
                 Uh[o + v] = 0.5 * ue[o + v];
                 U2[o + v] = ue[o + v];
             }
+            double cf[NV], cg[NV];
+            mdrk_contra(Jae, n, i, j, &f[o], &g[o], cf, cg);
             for (int ii = 0; ii < n; ++ii) {
                 const double c = -dt * b.D[ii * n + i];
-                for (int v = 0; v < NV; ++v) ut[L(ii, j) + v] += c * f[o + v];
+                for (int v = 0; v < NV; ++v) ut[L(ii, j) + v] += c * cf[v];
             }
             for (int jj = 0; jj < n; ++jj) {
                 const double c = -dt * b.D[jj * n + j];
-                for (int v = 0; v < NV; ++v) ut[L(i, jj) + v] += c * g[o + v];
+                for (int v = 0; v < NV; ++v) ut[L(i, jj) + v] += c * cg[v];
             }
         }
-    for (int k = 0; k < NV * nn; ++k) ut[k] *= inv_jac;
+    for (int k = 0; k < NV * nn; ++k) ut[k] *= Jae ? ije[k / NV] : inv_jac;
     double* due = du + idx_u(n, 0, 0, 0, e);
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
@@ -676,13 +694,15 @@ inline void mdrk1_volume_element(const Basis& b, const Euler& eq, int e, const d
                 G2[o + v] += 1.0 / 6.0 * gt[v];
                 U2[o + v] += 1.0 / 6.0 * ut[o + v];
             }
+            double cF[NV], cG[NV];
+            mdrk_contra(Jae, n, i, j, &Fh[o], &Gh[o], cF, cG);
             for (int ii = 0; ii < n; ++ii) {
                 const double c = alpha * b.Dhat[ii * n + i];
-                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += c * Fh[o + v];
+                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += c * cF[v];
             }
             for (int jj = 0; jj < n; ++jj) {
                 const double c = alpha * b.Dhat[jj * n + j];
-                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += c * Gh[o + v];
+                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += c * cG[v];
             }
             for (int v = 0; v < NV; ++v) {
                 ws.U[idx_u(n, v, i, j, e)] = Uh[o + v];
@@ -696,7 +716,8 @@ inline void mdrk1_volume_element(const Basis& b, const Euler& eq, int e, const d
 }
 
 inline void mdrk2_volume_element(const Basis& b, const Euler& eq, int e, const double* us, double* du, double dt,
-                                 double inv_jac, double alpha, Workspace& ws) {
+                                 double inv_jac, double alpha, Workspace& ws, const double* Jae = nullptr,
+                                 const double* ije = nullptr) {
     const int n = b.n, nn = n * n;
     Tile Fc, Gc, Uc, ust;
     ust.zero(NV * nn);
@@ -711,18 +732,19 @@ inline void mdrk2_volume_element(const Basis& b, const Euler& eq, int e, const d
             }
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
-            double f[NV], g[NV];
+            double f[NV], g[NV], cf[NV], cg[NV];
             eq.fluxes(ue + L(i, j), f, g);
+            mdrk_contra(Jae, n, i, j, f, g, cf, cg);
             for (int ii = 0; ii < n; ++ii) {
                 const double c = -dt * b.D[ii * n + i];
-                for (int v = 0; v < NV; ++v) ust[L(ii, j) + v] += c * f[v];
+                for (int v = 0; v < NV; ++v) ust[L(ii, j) + v] += c * cf[v];
             }
             for (int jj = 0; jj < n; ++jj) {
                 const double c = -dt * b.D[jj * n + j];
-                for (int v = 0; v < NV; ++v) ust[L(i, jj) + v] += c * g[v];
+                for (int v = 0; v < NV; ++v) ust[L(i, jj) + v] += c * cg[v];
             }
         }
-    for (int k = 0; k < NV * nn; ++k) ust[k] *= inv_jac;
+    for (int k = 0; k < NV * nn; ++k) ust[k] *= Jae ? ije[k / NV] : inv_jac;
     double* due = du + idx_u(n, 0, 0, 0, e);
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
@@ -746,13 +768,15 @@ inline void mdrk2_volume_element(const Basis& b, const Euler& eq, int e, const d
                 Gc[o + v] += 1.0 / 3.0 * gt;
                 Uc[o + v] += 1.0 / 3.0 * ust[o + v];
             }
+            double cF[NV], cG[NV];
+            mdrk_contra(Jae, n, i, j, &Fc[o], &Gc[o], cF, cG);
             for (int ii = 0; ii < n; ++ii) {
                 const double c = alpha * b.Dhat[ii * n + i];
-                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += c * Fc[o + v];
+                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += c * cF[v];
             }
             for (int jj = 0; jj < n; ++jj) {
                 const double c = alpha * b.Dhat[jj * n + j];
-                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += c * Gc[o + v];
+                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += c * cG[v];
             }
             for (int v = 0; v < NV; ++v) {
                 ws.U[idx_u(n, v, i, j, e)] = Uc[o + v];

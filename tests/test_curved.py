@@ -149,3 +149,97 @@ def test_gpu_curved_steps_match_oracle(oracle_mod, tl):
     s, t = o.steps(u_cpu, 9, 0.4, 0.0, 1e9, nthreads=NTH)
     assert s == integ.iter == 9 and integ.t == pytest.approx(t, rel=1e-13)
     assert np.all(rel_l2(u_gpu, u_cpu) < 1e-12)
+
+
+# ------------------------------------------------------------------ MDRK on curvilinear meshes (CPU and GPU)
+# mdrk_kernel_1! / _2! of src/solvers/dgsem_structured/multi_derivative_2d.jl:82-445: the TreeMesh procedure
+# on contravariant fluxes; stage 2 takes the stage state in the volume terms and u^n at the interfaces.
+@pytest.mark.parametrize("N", [3, 4])
+def test_oracle_curved_mdrk_free_stream_conservation_rotations(oracle_mod, tl, N):
+    m = tl.StructuredMesh((5, 4), warp)
+    cm = m.curved(N)
+    o = oracle_mod.Oracle(cm, N)
+    u = np.tile(np.array([1.0, 0.3, -0.2, 2.5]), cm.n_elements * (N + 1) ** 2)
+    s_, _ = o.steps(u, 3, 0.3, 0.0, 1e9, kind=1)
+    assert s_ == 3 and np.abs(u - np.tile(np.array([1.0, 0.3, -0.2, 2.5]), cm.n_elements * (N + 1) ** 2)).max() < 1e-12
+    u0 = vortex_state(tl, cm)
+    mass0 = quad(cm, N, u0)
+    u1 = u0.copy()
+    o.steps(u1, 4, 0.3, 0.0, 1e9, kind=1)
+    np.testing.assert_allclose(quad(cm, N, u1), mass0, rtol=1e-12)
+    turns = np.random.default_rng(N).integers(0, 4, cm.n_elements)
+    o2 = oracle_mod.Oracle(tl.rotate_elements(cm, turns), N)
+    ur = tl.rotate_state(u0, N, turns)
+    o2.steps(ur, 4, 0.3, 0.0, 1e9, kind=1)
+    assert np.all(rel_l2(ur, tl.rotate_state(u1, N, turns)) < 1e-12)
+
+
+def make_mdrk_semi(tl, mesh, N, bc=None):
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.MDRK()))
+    kw = {} if bc is None else {"boundary_conditions": bc}
+    return tl.SemidiscretizationHyperbolic(mesh, tl.MDRK(), eq, tl.IsentropicVortex(5.0), solver, **kw)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,rotated", [(3, False), (4, False), (4, True), (5, True)])
+def test_gpu_curved_mdrk_matches_oracle(oracle_mod, tl, N, rotated):
+    m = tl.StructuredMesh((6, 5), warp)
+    cm = m.curved(N)
+    if rotated:
+        cm = tl.rotate_elements(cm, np.random.default_rng(N + 20).integers(0, 4, cm.n_elements))
+    semi = make_mdrk_semi(tl, cm, N)
+    u = vortex_state(tl, cm)
+    o = oracle_mod.Oracle(cm, N)
+    dt = o.max_dt(u, 0.3)
+    semi.cache["dt"][0] = dt
+    # the two stages through the rhs entry points
+    d1_gpu = np.empty_like(u)
+    tl.rhs_mdrk1(d1_gpu, u, semi, 0.0)
+    d1_cpu = o.rhs(u, 0.0, dt, kind=1)
+    assert np.all(rel_l2(u + dt * d1_gpu, u + dt * d1_cpu) < 1e-12)
+    us = u + dt * d1_cpu
+    d2_gpu = np.empty_like(u)
+    tl.rhs_mdrk2(d2_gpu, u, semi, 0.0, us)
+    d2_cpu = o.rhs(u, 0.0, dt, kind=2, us=us)
+    assert np.all(rel_l2(u + dt * d2_gpu, u + dt * d2_cpu) < 1e-12)
+    # whole MDRK steps on the device
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, tl.MDRK(), (0.0, 1e9)))
+    integ.set_state(u, 0.0)
+    integ.step(7, 0.3, use_graph=True)
+    integ.sync_time()
+    u_cpu = u.copy()
+    s, t = o.steps(u_cpu, 7, 0.3, 0.0, 1e9, kind=1, nthreads=NTH)
+    assert s == integ.iter == 7 and integ.t == pytest.approx(t, rel=1e-13)
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-12)
+
+
+@pytest.mark.gpu
+def test_gpu_curved_mdrk_with_slip_walls(oracle_mod, tl):
+    """MDRK on the warped box with slip walls on all sides (the walls take the stage-1 traces as they are)."""
+    def box_warp(xi, eta):
+        X, Y = 0.5 * (xi + 1.0), 0.5 * (eta + 1.0)
+        s = 0.05 * np.sin(np.pi * X) * np.sin(np.pi * Y)
+        return X + s, Y + s
+    N = 4
+    cm = tl.StructuredMesh((6, 6), box_warp, periodicity=False).curved(N)
+    bc = {"x_neg": tl.boundary_condition_slip_wall_vertical, "x_pos": tl.boundary_condition_slip_wall_vertical,
+          "y_neg": tl.boundary_condition_slip_wall_horizontal, "y_pos": tl.boundary_condition_slip_wall_horizontal}
+    semi = make_mdrk_semi(tl, cm, N, bc)
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    x, y = cm.xy
+    rho = 1.0 + 0.2 * np.exp(-20 * ((x - 0.6) ** 2 + (y - 0.45) ** 2))
+    U = eq.prim2cons(rho, 0.1 * np.sin(np.pi * x), -0.1 * np.sin(np.pi * y), 1.0 + 0 * x)
+    u = np.ascontiguousarray(np.transpose(U, (2, 1, 0, 3))).reshape(-1)
+    o = oracle_mod.Oracle(cm, N)
+    o.set_curved_boundaries(cm.boundary_elements, cm.boundary_faces,
+                            np.repeat(np.array([1, 1, 2, 2], dtype=np.int32), cm.n_boundaries_per_direction))
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, tl.MDRK(), (0.0, 1e9)))
+    integ.set_state(u, 0.0)
+    integ.step(6, 0.3, use_graph=True)
+    integ.sync_time()
+    u_cpu = u.copy()
+    s, t = o.steps(u_cpu, 6, 0.3, 0.0, 1e9, kind=1, nthreads=NTH)
+    assert s == integ.iter == 6 and integ.t == pytest.approx(t, rel=1e-13)
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-12)
+    np.testing.assert_allclose(quad(cm, N, u_cpu)[0], quad(cm, N, u)[0], rtol=1e-12)

@@ -116,6 +116,11 @@ struct Launch {
             cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        const int md = (int)C::smem_bytes(2);
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
     }
     template <bool SC>
     static void volume_sc(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
@@ -138,9 +143,19 @@ struct Launch {
             if constexpr (N >= 4) lw_volume_kernel<N, MODE_STEP, false, 0, false, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
             return;
         }
-        if (a.metrics) {   // curvilinear mesh (LW, FR volume integral)
-            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, false, 0, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
-            else lw_volume_kernel<N, MODE_STEP, false, 0, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
+        if (a.metrics) {   // curvilinear mesh (LW or MDRK, FR volume integral)
+            const size_t md = C::smem_bytes(2);
+            if (stage == TLW_STAGE_MDRK1) {
+                if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS, false, true><<<grid, C::THREADS, md, s>>>(a);
+                else mdrk1_volume_kernel<N, MODE_STEP, false, true><<<grid, C::THREADS, md, s>>>(a);
+            } else if (stage == TLW_STAGE_MDRK2) {
+                if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS, false, true><<<grid, C::THREADS, md, s>>>(a);
+                else mdrk2_volume_kernel<N, MODE_STEP, false, true><<<grid, C::THREADS, md, s>>>(a);
+            } else if (mode == MODE_RHS) {
+                lw_volume_kernel<N, MODE_RHS, false, 0, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
+            } else {
+                lw_volume_kernel<N, MODE_STEP, false, 0, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
+            }
             return;
         }
         if (sc) volume_sc<true>(s, stage, mode, a, grid);
@@ -836,8 +851,8 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
                         const int32_t* primary_faces, const int64_t* secondary_elements,
                         const int32_t* secondary_faces, const int32_t* secondary_reversed) {
     if (!h) return TLW_E_ARG;
-    if (h->opts.time_discretization != TLW_LW || h->sc || h->N < 3)
-        return fail(h, TLW_E_UNSUPPORTED, "curvilinear meshes: LW with the FR volume integral, N >= 3");
+    if (h->sc || h->N < 3)
+        return fail(h, TLW_E_UNSUPPORTED, "curvilinear meshes: LW or MDRK with the FR volume integral, N >= 3");
     if (n_elements <= 0 || n_elements > (int64_t)0x7fffffff / 64 || !contravariant_vectors || !inverse_jacobian)
         return fail(h, TLW_E_ARG, "n_elements / metrics");
     if (n_interfaces < 0 || (n_interfaces > 0 && (!primary_elements || !primary_faces || !secondary_elements ||
@@ -919,6 +934,9 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
     if ((rc = ensure(h, h->d_state[0], sd)) || (rc = ensure(h, h->d_state[1], sd)) || (rc = ensure(h, h->d_tU, td)) ||
         (rc = ensure(h, h->d_tF, td)))
         return rc;
+    if (h->opts.time_discretization == TLW_MDRK) {
+        if ((rc = ensure(h, h->d_U2, sd)) || (rc = ensure(h, h->d_F2, 2 * sd)) || (rc = ensure(h, h->d_us, sd))) return rc;
+    }
     h->curved = true;
     h->cur = 0;
     h->have_mesh = true;

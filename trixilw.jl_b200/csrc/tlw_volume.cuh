@@ -627,8 +627,11 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
 // MDRK stage 1 (mdrk_kernel_1!, multi_derivative_2d.jl:263-421): F = f/2 + f_t/8, U = u/2 + u_t/8,
 // F2 = f + f_t/6, U2 = u + u_t/6 (stored whole for stage 2).
 // ------------------------------------------------------------------------------------------------
-template <int N, int MODE, bool SC>
+// CURVED (mdrk_kernel_1!, src/solvers/dgsem_structured/multi_derivative_2d.jl:82-243): the contractions take the
+// contravariant fluxes, d carries the node's J^{-1}; F2, G2 stay physical, the traces are contravariant.
+template <int N, int MODE, bool SC, bool CURVED = false>
 static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk1_volume_kernel(VolArgs a) {
+    static_assert(!(SC && CURVED), "shock capturing is built for TreeMesh only");
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
@@ -649,12 +652,27 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
     const bool active = el < EB && e < a.E;
     // dt of this element's instance (batched form) or the single dt
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
-    double uu[NV], f0[NV], g0[NV], ij = 0.0;
+    double uu[NV], f0[NV], g0[NV], ij = 0.0, Ja[4] = {0.0, 0.0, 0.0, 0.0};
+    // a flux pair into the contraction planes (contravariant on curvilinear meshes)
+    auto put = [&](const double* f, const double* g) {
+        if (CURVED) {
+            double ft[NV], gt[NV];
+            contravariant(Ja, f, g, ft, gt);
+            node_put<N, C>(X, Y, el, i, j, ft, gt);
+        } else {
+            node_put<N, C>(X, Y, el, i, j, f, g);
+        }
+    };
     if (active) {
         load4(a.u + ((size_t)e * nn + node) * NV, uu);
-        ij = __ldg(a.inv_jac + e);
+        if (CURVED) {
+            load4(a.metrics + ((size_t)e * nn + node) * 4, Ja);
+            ij = __ldg(a.inv_jac_node + (size_t)e * nn + node);
+        } else {
+            ij = __ldg(a.inv_jac + e);
+        }
         euler_fluxes(gm1, uu[0], uu[1], uu[2], uu[3], f0, g0);
-        node_put<N, C>(X, Y, el, i, j, f0, g0);
+        put(f0, g0);
         if (SC) {
             // the subcell FV part uses the instantaneous u^n (multi_derivative_2d.jl:205)
             node_put<N, C>(F0X, F0Y, el, i, j, f0, g0);
@@ -699,6 +717,12 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
         store4(a.U2 + off * NV, U2v);
         store4(a.F2 + off * 2 * NV, F2v);
         store4(a.F2 + off * 2 * NV + NV, G2v);
+        if (CURVED) {
+            double ft2[NV], gt2[NV];
+            contravariant(Ja, F, G, ft2, gt2);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { F[v] = ft2[v]; G[v] = gt2[v]; }
+        }
         node_put<N, C>(X, Y, el, i, j, F, G);
         if (SC) sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
     }
@@ -718,8 +742,10 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
 // MDRK stage 2 (mdrk_kernel_2!, multi_derivative_2d.jl:423-555): at u* = a.u,
 // F = F2 + f_t(u*)/3, U = U2 + u*_t/3.
 // ------------------------------------------------------------------------------------------------
-template <int N, int MODE, bool SC>
+// CURVED (mdrk_kernel_2!, src/solvers/dgsem_structured/multi_derivative_2d.jl:245-445): as in stage 1.
+template <int N, int MODE, bool SC, bool CURVED = false>
 static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk2_volume_kernel(VolArgs a) {
+    static_assert(!(SC && CURVED), "shock capturing is built for TreeMesh only");
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
@@ -740,13 +766,24 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
     const bool active = el < EB && e < a.E;
     // dt of this element's instance (batched form) or the single dt
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
-    double us[NV], ij = 0.0;
+    double us[NV], ij = 0.0, Ja[4] = {0.0, 0.0, 0.0, 0.0};
     if (active) {
         double f[NV], g[NV];
         load4(a.u + ((size_t)e * nn + node) * NV, us);
-        ij = __ldg(a.inv_jac + e);
+        if (CURVED) {
+            load4(a.metrics + ((size_t)e * nn + node) * 4, Ja);
+            ij = __ldg(a.inv_jac_node + (size_t)e * nn + node);
+        } else {
+            ij = __ldg(a.inv_jac + e);
+        }
         euler_fluxes(gm1, us[0], us[1], us[2], us[3], f, g);
-        node_put<N, C>(X, Y, el, i, j, f, g);
+        if (CURVED) {
+            double ft[NV], gt[NV];
+            contravariant(Ja, f, g, ft, gt);
+            node_put<N, C>(X, Y, el, i, j, ft, gt);
+        } else {
+            node_put<N, C>(X, Y, el, i, j, f, g);
+        }
         if (SC) {
             // the subcell FV part uses the instantaneous u^n, not u* (multi_derivative_2d.jl:257)
             double un[NV], fn0[NV], gn0[NV];
@@ -790,6 +827,12 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
             F[v] = fma(1.0 / 3.0, ft[v], F2v[v]);
             G[v] = fma(1.0 / 3.0, gt[v], G2v[v]);
             U[v] = fma(1.0 / 3.0, d[v], U2v[v]);
+        }
+        if (CURVED) {
+            double ft2[NV], gt2[NV];
+            contravariant(Ja, F, G, ft2, gt2);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { F[v] = ft2[v]; G[v] = gt2[v]; }
         }
         node_put<N, C>(X, Y, el, i, j, F, G);
         if (SC) sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
