@@ -171,8 +171,10 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
 /* Boundary faces of the curvilinear mesh (P4estMesh boundaries: element, face), after tlw_set_curved_mesh
  * (which clears them): elements 1-based, faces 0: -xi, 1: +xi, 2: -eta, 3: +eta (a face no interface covers),
  * kinds TLW_BC_SLIP_WALL_VERTICAL / _HORIZONTAL (the normal-direction slip walls of src/equations/equations.jl:
- * 137-169, called as calc_boundary_flux! of src/solvers/dgsem_p4est/dg_2d.jl:285-393 does). The boundaries keep
- * the caller's order for tlw_set_parabolic_walls. */
+ * 137-169) or TLW_BC_DIRICHLET (the normal-direction time-averaged Dirichlet condition, :64-93, with exterior
+ * data from tlw_set_boundary_data in this order; the MDRK stage 1 halves its time averages as the P4estMesh path
+ * does), called as calc_boundary_flux! of src/solvers/dgsem_p4est/dg_2d.jl:285-393 does. The boundaries keep the
+ * caller's order for tlw_set_boundary_data and tlw_set_parabolic_walls (Navier-Stokes: slip walls only). */
 int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t* elements, const int32_t* faces,
                               const int32_t* kinds);
 /* Number of interface colours (launches per interface pass) of the curvilinear mesh; 0 for a TreeMesh. */

@@ -49,7 +49,7 @@ void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, do
         return;
     }
     if (h->opt.shock_capturing) throw std::runtime_error("curvilinear oracle: FR volume integral only");
-    rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, kind, u2);
+    rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, kind, u2, bd);
 }
 
 double any_max_dt(oracle_handle* h, const double* u, double cfl, bool& bad, int nthreads) {
@@ -174,7 +174,7 @@ int oracle_set_curved_boundaries(oracle_handle* h, int B, const int32_t* elem, c
     h->cmesh.b_face.assign(face, face + B);
     h->cmesh.b_kind.assign(kind, kind + B);
     for (int k = 0; k < B; ++k)
-        if (kind[k] != BC_SLIP_WALL_VERTICAL && kind[k] != BC_SLIP_WALL_HORIZONTAL) return 1;
+        if (kind[k] != BC_DIRICHLET && kind[k] != BC_SLIP_WALL_VERTICAL && kind[k] != BC_SLIP_WALL_HORIZONTAL) return 1;
     return 0;
 }
 
@@ -212,7 +212,7 @@ void oracle_set_temporal_errors(oracle_handle* h, int on, double abstol, double 
 
 // Exterior boundary states: levels [v, k, l, B] at t + 0.5 dt_scaled (x_k + 1), now [v, l, B] at t.
 int oracle_set_boundary_data(oracle_handle* h, const double* levels, const double* now) {
-    const size_t n = h->basis.n, B = h->mesh.n_boundaries;
+    const size_t n = h->basis.n, B = h->curved ? h->cmesh.n_boundaries : h->mesh.n_boundaries;
     h->bnd_levels.assign(levels, levels + NV * n * n * B);
     h->bnd_now.assign(now, now + NV * n * B);
     return 0;

@@ -200,20 +200,40 @@ inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, con
 // prolong2boundaries! and calc_boundary_flux!, src/solvers/dgsem_p4est/dg_2d.jl:285-393): the inner normal flux
 // uses the outward normal, the exterior state mirrors it, and the surface flux takes the inner side as _ll in
 // the curvilinear order (f_in, f_out, u_in, u_out, U_in, U_out, normal); the result is the outward flux.
+// Time-averaged Dirichlet boundaries in the normal-direction form (src/equations/equations.jl:64-93): U_outer,
+// F_outer are GLL time averages of the exterior state and of its flux along the outward normal (levels as for
+// the TreeMesh), and the surface flux is called with U_outer in the place of the exterior u:
+// (f_in, f_out, u_in, U_out, U_in, U_out, normal).
 inline void calc_boundary_flux_curved(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m,
-                                      const double* u, Workspace& ws) {
+                                      const double* u, Workspace& ws, const BoundaryData* bd = nullptr,
+                                      double scaling_factor = 1.0) {
     const int n = b.n;
     for (int k = 0; k < m.n_boundaries; ++k) {
         const int e = m.b_elem[k], f = m.b_face[k], kind = m.b_kind[k];
+        if (kind == BC_DIRICHLET && (!bd || !bd->u_levels)) throw std::invalid_argument("boundary data missing");
         for (int l = 0; l < n; ++l) {
             int i, j;
             face_node(n, f, l, i, j);
-            double nrm[2], Fi[NV], Ui[NV], ui[NV], Fo[NV], Uo[NV], uo[NV], Fn[NV];
+            double nrm[2], Fi[NV], Ui[NV], ui[NV], Fo[NV] = {0, 0, 0, 0}, Uo[NV] = {0, 0, 0, 0}, uo[NV], Fn[NV];
             outward_normal(m, n, f, i, j, e, nrm);
             for (int v = 0; v < NV; ++v) {
                 Fi[v] = ws.F[idx_F(n, v, 0, i, j, e)] * nrm[0] + ws.F[idx_F(n, v, 1, i, j, e)] * nrm[1];
                 Ui[v] = ws.U[idx_u(n, v, i, j, e)];
                 ui[v] = u[idx_u(n, v, i, j, e)];
+            }
+            if (kind == BC_DIRICHLET) {
+                for (int q = 0; q < n; ++q) {
+                    const double* ub = bd->u_levels + NV * (q + (size_t)n * (l + (size_t)n * k));
+                    double fx[NV], gy[NV];
+                    eq.fluxes(ub, fx, gy);
+                    for (int v = 0; v < NV; ++v) {
+                        Uo[v] += ub[v] * scaling_factor * b.weights[q] / 2.0;
+                        Fo[v] += (fx[v] * nrm[0] + gy[v] * nrm[1]) * scaling_factor * b.weights[q] / 2.0;
+                    }
+                }
+                lw_surface_flux_normal(eq, opt.flux_kind, opt.speed_kind, Fi, Fo, ui, Uo, Ui, Uo, nrm, Fn, ws.bad);
+                for (int v = 0; v < NV; ++v) ws.surface_flux_values[v + NV * (l + n * (f + 4 * (size_t)e))] = Fn[v];
+                continue;
             }
             slip_wall_exterior(kind, Fi, Ui, ui, Fo, Uo, uo);
             lw_surface_flux_normal(eq, opt.flux_kind, opt.speed_kind, Fi, Fo, ui, uo, Ui, Uo, nrm, Fn, ws.bad);
@@ -250,7 +270,7 @@ inline void surface_integral_and_jacobian_curved(const Basis& b, const CurvedMes
 // u (u^n) at the interfaces (src/solvers/dgsem_structured/multi_derivative_2d.jl:1-80)
 inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m, const double* u,
                        double* du, double dt, Workspace& ws, int nthreads = 1, int kind = 0,
-                       const double* u2 = nullptr) {
+                       const double* u2 = nullptr, const BoundaryData* bd = nullptr) {
     const int n = b.n, nn = n * n;
     const size_t ndof = (size_t)NV * nn * m.n_elements;
     const double nan = std::numeric_limits<double>::quiet_NaN();
@@ -302,7 +322,8 @@ inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, cons
         }
     }
     ws.bad = ws.bad || bad;
-    calc_boundary_flux_curved(b, eq, opt, m, u, ws);
+    // MDRK stage 1 scales the time averages by 1/2 (as the P4estMesh path does, multi_derivative_2d.jl:34)
+    calc_boundary_flux_curved(b, eq, opt, m, u, ws, bd, kind == 1 ? 0.5 : 1.0);
     surface_integral_and_jacobian_curved(b, m, du, ws, nthreads);
 }
 

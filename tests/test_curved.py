@@ -243,3 +243,83 @@ def test_gpu_curved_mdrk_with_slip_walls(oracle_mod, tl):
     assert s == integ.iter == 6 and integ.t == pytest.approx(t, rel=1e-13)
     assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-12)
     np.testing.assert_allclose(quad(cm, N, u_cpu)[0], quad(cm, N, u)[0], rtol=1e-12)
+
+
+# ------------------------------------------------- time-averaged Dirichlet boundaries on curvilinear meshes
+def _box_warp(xi, eta):
+    X, Y = 0.5 * (xi + 1.0), 0.5 * (eta + 1.0)
+    s = 0.05 * np.sin(np.pi * X) * np.sin(np.pi * Y)
+    return X + s, Y + s
+
+
+def _dirichlet_setup(tl, oracle_mod, N, td):
+    """The warped unit box: Dirichlet data (a moving density wave, time-dependent) on x_neg / x_pos, slip walls
+    on y_neg / y_pos."""
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    mesh = tl.StructuredMesh((6, 6), _box_warp, periodicity=False)
+    cm = mesh.curved(N)
+    ic = tl.DensityWave(amplitude=0.3, v=(0.4, 0.0), p=1.0, k=1.0)
+    bc = {"x_neg": tl.BoundaryConditionDirichlet(ic), "x_pos": tl.BoundaryConditionDirichlet(ic),
+          "y_neg": tl.boundary_condition_slip_wall_horizontal, "y_pos": tl.boundary_condition_slip_wall_horizontal}
+    tdo = tl.LW() if td == "lw" else tl.MDRK()
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tdo))
+    semi = tl.SemidiscretizationHyperbolic(cm, tdo, eq, ic, solver, boundary_conditions=bc)
+    o = oracle_mod.Oracle(cm, N)
+    o.set_curved_boundaries(cm.boundary_elements, cm.boundary_faces,
+                            np.repeat(np.array([0, 0, 2, 2], dtype=np.int32), cm.n_boundaries_per_direction))
+    u = np.ascontiguousarray(np.transpose(ic(cm.xy[0], cm.xy[1], 0.0, eq), (2, 1, 0, 3))).reshape(-1)
+    return eq, cm, ic, semi, o, u
+
+
+def _oracle_boundary_data(cm, N, ic, eq, t, dt, scaling):
+    from trixilw.basis import gauss_lobatto
+    nodes, _ = gauss_lobatto(N)
+    xy = cm.boundary_node_coordinates(N)
+    levels = np.empty((cm.n_boundaries, N + 1, N + 1, 4))
+    for q in range(N + 1):
+        levels[:, :, q, :] = np.transpose(ic(xy[0], xy[1], t + 0.5 * scaling * dt * (nodes[q] + 1.0), eq), (1, 0, 2))
+    now = np.transpose(ic(xy[0], xy[1], t, eq), (1, 0, 2))
+    return np.ascontiguousarray(levels), np.ascontiguousarray(now)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,td", [(3, "lw"), (4, "lw"), (4, "mdrk")])
+def test_gpu_curved_dirichlet_matches_oracle(oracle_mod, tl, N, td):
+    eq, cm, ic, semi, o, u = _dirichlet_setup(tl, oracle_mod, N, td)
+    t, dt = 0.13, 0.4 * o.max_dt(u, 0.3) / 0.3
+    semi.cache["dt"][0] = dt
+    if td == "lw":
+        o.set_boundary_data(*_oracle_boundary_data(cm, N, ic, eq, t, dt, 1.0))
+        du = np.empty_like(u)
+        tl.rhs(du, u, semi, t)
+        assert np.all(rel_l2(u + dt * du, u + dt * o.rhs(u, t, dt)) < 1e-12)
+    else:
+        o.set_boundary_data(*_oracle_boundary_data(cm, N, ic, eq, t, dt, 0.5))
+        d1 = np.empty_like(u)
+        tl.rhs_mdrk1(d1, u, semi, t)
+        d1_cpu = o.rhs(u, t, dt, kind=1)
+        assert np.all(rel_l2(u + dt * d1, u + dt * d1_cpu) < 1e-12)
+        o.set_boundary_data(*_oracle_boundary_data(cm, N, ic, eq, t, dt, 1.0))
+        us = u + dt * d1_cpu
+        d2 = np.empty_like(u)
+        tl.rhs_mdrk2(d2, u, semi, t, us)
+        assert np.all(rel_l2(u + dt * d2, u + dt * o.rhs(u, t, dt, kind=2, us=us)) < 1e-12)
+
+
+@pytest.mark.gpu
+def test_gpu_curved_dirichlet_solve_converges_to_the_wave(tl):
+    """solve_lwfr on the warped box with the moving density wave as Dirichlet data at x and slip walls at y
+    (the wave moves along x, so the walls are exact): the error against the exact wave stays at the level of
+    the discretisation."""
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    mesh = tl.StructuredMesh((8, 8), _box_warp, periodicity=False)
+    ic = tl.DensityWave(amplitude=0.3, v=(0.4, 0.0), p=1.0, k=1.0)
+    ic_x = lambda x, y, t, e: ic(x, 0 * y, t, e)   # a wave in x only: rho(x - 0.4 t)
+    bc = {"x_neg": tl.BoundaryConditionDirichlet(ic_x), "x_pos": tl.BoundaryConditionDirichlet(ic_x),
+          "y_neg": tl.boundary_condition_slip_wall_horizontal, "y_pos": tl.boundary_condition_slip_wall_horizontal}
+    solver = tl.DGSEM(4, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.LW()))
+    semi = tl.SemidiscretizationHyperbolic(mesh, tl.LW(), eq, ic_x, solver, boundary_conditions=bc)
+    sol = tl.solve_lwfr(tl.semidiscretize(semi, tl.LW(), (0.0, 0.5)), (), 0.0, None,
+                        time_step_computation=tl.CFLBased(0.98 * 5 * 0.103))
+    l2, linf = tl.l2_linf_errors(semi, sol.u[-1], 0.5)
+    assert sol.t[-1] == pytest.approx(0.5) and l2[0] < 2e-4

@@ -396,7 +396,7 @@ void enqueue_limiter(tlw_handle* h, double* u, int reps, unsigned long long* slo
 // the surfaces of a curvilinear mesh: interfaces colour by colour (no two threads of a launch share a node),
 // then the xi-face and the eta-face boundaries; with the viscous traces for Navier-Stokes
 void enqueue_curved_surfaces(tlw_handle* h, int mode, const double* u_jump, double* out, const double* dt_ptr,
-                             const PhaseEvents* ev) {
+                             const PhaseEvents* ev, double scaling_factor = 1.0) {
     CurvedSurfArgs ca{};
     ca.u = u_jump;
     ca.out = out;
@@ -442,6 +442,9 @@ void enqueue_curved_surfaces(tlw_handle* h, int mode, const double* u_jump, doub
         cb.inv_w_first = h->h_basis.inv_w_first;
         cb.inv_w_last = h->h_basis.inv_w_last;
         cb.status = &h->d_step->status;
+        cb.levels = h->d_levels;
+        cb.weights = h->d_basis->weights;
+        cb.scaling_factor = scaling_factor;
         const int first[2] = {0, h->ncbx}, count[2] = {h->ncbx, h->ncb - h->ncbx};
         for (int cls = 0; cls < 2; ++cls) {
             cb.elem = h->d_cbe + first[cls];
@@ -554,7 +557,9 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     dispatch<Vol>(h->N, h->stream, stage, mode, h->sc, va);
     if (ev) cudaEventRecord(ev->after_volume, h->stream);
     if (h->curved) {
-        enqueue_curved_surfaces(h, mode, u_jump, out, dt_ptr, ev);
+        // MDRK stage 1 scales the Dirichlet time averages by 1/2, as the P4estMesh path does
+        // (src/solvers/dgsem_tree/multi_derivative_2d.jl:34)
+        enqueue_curved_surfaces(h, mode, u_jump, out, dt_ptr, ev, stage == TLW_STAGE_MDRK1 ? 0.5 : 1.0);
         return;
     }
 
@@ -669,7 +674,7 @@ __global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
 int check_ready(tlw_handle* h) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
-    if (h->nb > 0 && h->bnd_dirichlet && !h->have_bdata)
+    if ((h->nb > 0 || h->ncb > 0) && h->bnd_dirichlet && !h->have_bdata)
         return fail(h, TLW_E_STATE, "mesh has Dirichlet boundaries: call tlw_set_boundary_data first");
     if (h->parabolic && (h->nb > 0 || h->ncb > 0) && !h->d_wkind)
         return fail(h, TLW_E_STATE, "Navier-Stokes with boundaries: call tlw_set_parabolic_walls first");
@@ -997,13 +1002,17 @@ int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t
     if (n_boundaries < 0 || (n_boundaries > 0 && (!elements || !faces || !kinds))) return fail(h, TLW_E_ARG, "boundaries");
     std::vector<int> be[2], bf[2], bk[2], bi[2];
     std::vector<signed char> used = h->face_used;
+    bool dirichlet = false;
     for (int64_t k = 0; k < n_boundaries; ++k) {
         const int64_t e = elements[k] - 1;
         const int f = faces[k];
         if (e < 0 || e >= h->E || f < 0 || f > 3)
             return fail(h, TLW_E_ARG, "boundary " + std::to_string(k + 1) + " out of range");
-        if (kinds[k] != TLW_BC_SLIP_WALL_VERTICAL && kinds[k] != TLW_BC_SLIP_WALL_HORIZONTAL)
-            return fail(h, TLW_E_UNSUPPORTED, "curvilinear boundaries: slip walls are built");
+        if (kinds[k] != TLW_BC_DIRICHLET && kinds[k] != TLW_BC_SLIP_WALL_VERTICAL && kinds[k] != TLW_BC_SLIP_WALL_HORIZONTAL)
+            return fail(h, TLW_E_ARG, "boundary " + std::to_string(k + 1) + ": unknown kind");
+        if (kinds[k] == TLW_BC_DIRICHLET && h->parabolic)
+            return fail(h, TLW_E_UNSUPPORTED, "curvilinear Navier-Stokes: slip walls are built");
+        dirichlet = dirichlet || kinds[k] == TLW_BC_DIRICHLET;
         if (used[(size_t)e * 4 + f])
             return fail(h, TLW_E_ARG, "boundary " + std::to_string(k + 1) + ": the face already has a neighbour");
         used[(size_t)e * 4 + f] = 1;
@@ -1019,6 +1028,9 @@ int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t
     dfree(h->d_wall);
     h->ncb = (int)n_boundaries;
     h->ncbx = (int)be[0].size();
+    h->bnd_dirichlet = dirichlet;
+    h->have_bdata = false;
+    dfree(h->d_levels); dfree(h->d_now);
     if (n_boundaries > 0) {
         auto up = [&](int*& d, const std::vector<int>& a, const std::vector<int>& b) -> int {
             std::vector<int> v(a);
@@ -1109,6 +1121,8 @@ int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl) {
     if (h->opts.time_discretization != TLW_LW || h->sc || h->N < 3 || h->nmx + h->nmy > 0)
         return fail(h, TLW_E_UNSUPPORTED, "Navier-Stokes: LW, FR volume integral, N >= 3, conforming TreeMesh");
     if (!(mu >= 0.0) || !(prandtl > 0.0)) return fail(h, TLW_E_ARG, "mu / Prandtl");
+    if (h->curved && h->ncb > 0 && h->bnd_dirichlet)
+        return fail(h, TLW_E_UNSUPPORTED, "curvilinear Navier-Stokes: slip walls are built");
     TLW_CUDA(h, cudaSetDevice(h->device));
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));
     drop_graphs(h);
@@ -1190,9 +1204,10 @@ int32_t tlw_curved_colors(tlw_handle* h) {
 int tlw_set_boundary_data(tlw_handle* h, const double* levels, const double* now, int32_t where) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh");
-    if (h->nb == 0) return TLW_OK;
+    const int64_t nbnd = h->curved ? h->ncb : h->nb;
+    if (nbnd == 0) return TLW_OK;
     if (!levels || !now) return fail(h, TLW_E_ARG, "boundary data pointers");
-    const size_t nl = (size_t)NV * h->n * h->n * h->nb, nw = (size_t)NV * h->n * h->nb;
+    const size_t nl = (size_t)NV * h->n * h->n * nbnd, nw = (size_t)NV * h->n * nbnd;
     int rc;
     if ((rc = ensure(h, h->d_levels, nl)) || (rc = ensure(h, h->d_now, nw))) return rc;
     const cudaMemcpyKind k = where == TLW_WHERE_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;

@@ -186,6 +186,11 @@ struct CurvedBndArgs {
     int flux_kind, speed_kind;
     double inv_w_first, inv_w_last;
     unsigned* status;
+    // time-averaged Dirichlet: exterior states at the GLL time levels [v, q, l, B], GLL weights, the MDRK
+    // stage-1 scaling
+    const double* levels;
+    const double* weights;
+    double scaling_factor;
 };
 
 template <int N>
@@ -208,8 +213,29 @@ static __global__ void __launch_bounds__(128) curved_boundary_kernel(CurvedBndAr
     const double nrm[2] = {sg * (f < 2 ? J[0] : J[2]), sg * (f < 2 ? J[1] : J[3])};
 #pragma unroll
     for (int v = 0; v < NV; ++v) Fi[v] *= sg;
-    slip_wall_exterior(kind, Fi, Ui, ui, Fo, Uo, uo);
-    lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, Fi, Fo, ui, uo, Ui, Uo, nrm, Fn, a.status);
+    if (kind == BC_DIRICHLET) {
+        // (src/equations/equations.jl:64-93): GLL time averages of the exterior state and of its flux along the
+        // normal; the surface flux gets U_outer in the place of the exterior u
+        const int b = __ldg(a.index + k);
+        const double gm1 = a.gamma - 1.0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Uo[v] = Fo[v] = 0.0;
+        for (int q = 0; q < n; ++q) {
+            double ub[NV], fx[NV], gy[NV];
+            load4(a.levels + (((size_t)b * n + l) * n + q) * NV, ub);
+            euler_fluxes(gm1, ub[0], ub[1], ub[2], ub[3], fx, gy);
+            const double w = a.scaling_factor * a.weights[q] / 2.0;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                Uo[v] += ub[v] * w;
+                Fo[v] += (fx[v] * nrm[0] + gy[v] * nrm[1]) * w;
+            }
+        }
+        lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, Fi, Fo, ui, Uo, Ui, Uo, nrm, Fn, a.status);
+    } else {
+        slip_wall_exterior(kind, Fi, Ui, ui, Fo, Uo, uo);
+        lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, Fi, Fo, ui, uo, Ui, Uo, nrm, Fn, a.status);
+    }
     if (a.tFv) {
         double fv[NV];
         load4(a.tFv + tb, fv);

@@ -296,8 +296,7 @@ class SemidiscretizationHyperbolic:
         for d, bc in zip(DIRECTIONS, self._bcs):
             if not isinstance(bc, (BoundaryConditionDirichlet, BoundaryConditionSlipWall)):
                 raise ValueError(f"{d}: a non-periodic TreeMesh needs BoundaryConditionDirichlet or a slip wall")
-            if self.curved is not None and not isinstance(bc, BoundaryConditionSlipWall):
-                raise NotImplementedError(f"{d}: curvilinear boundaries are built for the slip walls")
+
         self.cache = {"dt": [math.nan]}
         sf = solver.surface_flux
         opts = _lib.TlwOpts()
