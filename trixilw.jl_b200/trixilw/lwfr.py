@@ -101,14 +101,14 @@ def solve_lwfr(lw_update: LWUpdate, callbacks=(), dt_initial: float = 0.0, toler
     cfl = time_step_computation.cfl_number
     integ = LWIntegrator(lw_update, tolerances)
     u0 = lw_update.u0_ode
+    # exterior data first (time-dependent data is set again before every step)
+    semi._prepare_boundaries(lw_update.tspan[0], 0.0, 1.0)
     integ.set_state(u0, lw_update.tspan[0])
     if n_pairs:
         check(integ.handle, lib().tlw_apply_positivity_limiter(integ.handle))
     time_dependent_bc = semi.mesh.n_boundaries > 0 and semi.time_dependent_boundaries()
     intervals = [int(cb.interval) for cb in callbacks if getattr(cb, "interval", 0)]
     stride = min(intervals) if intervals else chunk
-    if not time_dependent_bc:
-        semi._prepare_boundaries(lw_update.tspan[0], 0.0, 1.0)
     while not integ.isfinished():
         if time_dependent_bc:
             # exterior states depend on (t, dt): one step at a time with the dt read back
@@ -188,10 +188,10 @@ def _solve_adaptive(lw_update: LWUpdate, callbacks, dt_initial: float, tolerance
     semi = lw_update.p
     tol = tolerances or {"abstol": 1e-6, "reltol": 1e-6}
     integ = LWIntegrator(lw_update, tol)
+    semi._prepare_boundaries(lw_update.tspan[0], 0.0, 1.0)
     integ.set_state(lw_update.u0_ode, lw_update.tspan[0])
     if limit:   # the trial and the accept apply it after that (tlw_adaptive_trial / tlw_adaptive_accept)
         check(integ.handle, lib().tlw_apply_positivity_limiter(integ.handle))
-    semi._prepare_boundaries(lw_update.tspan[0], 0.0, 1.0)
     ctl = AdaptiveController(semi.nnodes, lw_update.tspan[0], lw_update.tspan[1], dt_initial)
     err = ctypes.c_double()
     ok = ctypes.c_int32()
