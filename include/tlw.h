@@ -168,6 +168,26 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
                         const double* inverse_jacobian, int64_t n_interfaces, const int64_t* primary_elements,
                         const int32_t* primary_faces, const int64_t* secondary_elements,
                         const int32_t* secondary_faces, const int32_t* secondary_reversed);
+/* Domain decomposition (the reference's MPI path, src/solvers/dgsem_tree/dg_2d_parallel.jl:23-200, with the same
+ * message per cut face node: the u face value, U trace and F.n trace, 3 nv doubles, dg_parallel.jl:12-13). A rank
+ * uploads its part of the TreeMesh with tlw_set_tree_mesh (local elements, the interfaces between them, its
+ * boundaries) and lists its cut faces here: elements 1-based local, faces 0: -x, 1: +x, 2: -y, 3: +y, in the
+ * order of its send / receive buffers ([halo][l][12] doubles, tlw_dd_buffers; a neighbour's send buffer
+ * segment lands in this rank's receive buffer at the same positions). LW, FR volume integral, conforming
+ * TreeMesh, Euler. A step is then
+ *   tlw_dd_begin(h, cfl, fixed_dt, t_end)  this part's CFL maximum into *max_bits (a non-negative double's bits)
+ *   caller: allreduce(MAX) of *max_bits over the ranks (uint64)
+ *   tlw_dd_volume(h)                       dt, the volume kernel, this part's cut-face traces into send
+ *   caller: send / receive the halo buffers
+ *   tlw_dd_finish(h)                       interfaces, boundaries, cut faces; the new state becomes current
+ * all asynchronous on the handle's stream (tlw_get_stream): the caller orders its collectives on that stream.
+ * tlw_step / tlw_step_timed / tlw_rhs refuse a handle with cut faces. */
+int tlw_set_halo(tlw_handle* h, int64_t n_halo, const int64_t* elements, const int32_t* faces);
+int tlw_dd_buffers(tlw_handle* h, double** send, double** recv, unsigned long long** max_bits);
+int tlw_dd_begin(tlw_handle* h, double cfl, double fixed_dt, double t_end);
+int tlw_dd_volume(tlw_handle* h);
+int tlw_dd_finish(tlw_handle* h);
+
 /* Boundary faces of the curvilinear mesh (P4estMesh boundaries: element, face), after tlw_set_curved_mesh
  * (which clears them): elements 1-based, faces 0: -xi, 1: +xi, 2: -eta, 3: +eta (a face no interface covers),
  * kinds TLW_BC_SLIP_WALL_VERTICAL / _HORIZONTAL (the normal-direction slip walls of src/equations/equations.jl:

@@ -16,6 +16,7 @@
 #include "tlw_handle.h"
 #include "tlw_mortar.cuh"
 #include "tlw_limiter.cuh"
+#include "tlw_halo.cuh"
 #include "tlw_parabolic.cuh"
 #include "tlw_surface.cuh"
 #include "tlw_volume.cuh"
@@ -74,6 +75,10 @@ void free_mesh(tlw_handle* h) {
     if (h->d_bad) { cudaFree(h->d_bad); h->d_bad = nullptr; }
     h->color_off.clear();
     h->face_used.clear();
+    for (int** d : {&h->d_he, &h->d_hf, &h->d_hs})
+        if (*d) { cudaFree(*d); *d = nullptr; }
+    dfree(h->d_send); dfree(h->d_recv);
+    h->nh = h->nhx = 0;
     if (h->d_cbe) { cudaFree(h->d_cbe); h->d_cbe = nullptr; }
     if (h->d_cbf) { cudaFree(h->d_cbf); h->d_cbf = nullptr; }
     if (h->d_cbk) { cudaFree(h->d_cbk); h->d_cbk = nullptr; }
@@ -322,6 +327,14 @@ template <int N> struct ParSpd { static void run(cudaStream_t s, const tlw_handl
 template <int N> struct ParAttr { static void run() { Launch<N>::par_attributes(); } };
 template <int N> struct Mrt { static void run(cudaStream_t s, const MortarArgs& a) { Launch<N>::mortars(s, a); } };
 template <int N> struct CIfc { static void run(cudaStream_t s, const CurvedSurfArgs& a) { Launch<N>::curved_interfaces(s, a); } };
+template <int N> struct Halo {
+    static void run(cudaStream_t s, const HaloArgs& a, bool pack) {
+        const long long threads = (long long)a.count * (N + 1);
+        if (threads == 0) return;
+        if (pack) halo_pack_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
+        else halo_face_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
+    }
+};
 template <int N> struct CBnd {
     static void run(cudaStream_t s, const CurvedBndArgs& a) {
         const long long threads = (long long)a.count * (N + 1);
@@ -374,7 +387,34 @@ void enqueue_indicator(tlw_handle* h, const double* u, bool speed) {
 // conforming TreeMesh (no boundaries, mortars, shock capturing, curvilinear or parabolic terms)
 bool use_slots(const tlw_handle* h) {
     return h->d_slots && h->opts.time_discretization == TLW_LW && !h->sc && !h->curved && !h->parabolic &&
-           h->nb == 0 && h->nmx + h->nmy == 0;
+           h->nb == 0 && h->nmx + h->nmy == 0 && h->nh == 0;
+}
+
+// the halo faces of one class (cls 0: x, 1: y) as kernel arguments
+HaloArgs halo_args(tlw_handle* h, int cls, int mode, const double* u_jump, double* out, const double* dt_ptr) {
+    HaloArgs a{};
+    const int first = cls == 0 ? 0 : h->nhx;
+    a.u = u_jump;
+    a.out = out;
+    a.tU = h->d_tU;
+    a.tF = h->d_tF;
+    a.send = h->d_send;
+    a.recv = h->d_recv;
+    a.elem = h->d_he + first;
+    a.face = h->d_hf + first;
+    a.slot = h->d_hs + first;
+    a.count = cls == 0 ? h->nhx : h->nh - h->nhx;
+    a.orientation = cls + 1;
+    a.inv_jac = h->d_inv_jac;
+    a.dt = dt_ptr;
+    a.step_mode = mode == MODE_STEP;
+    a.gamma = h->opts.gamma;
+    a.flux_kind = h->opts.surface_flux;
+    a.speed_kind = h->opts.max_speed;
+    a.inv_w_first = h->h_basis.inv_w_first;
+    a.inv_w_last = h->h_basis.inv_w_last;
+    a.status = &h->d_step->status;
+    return a;
 }
 
 // `reps` applications of the positivity limiter to u (in place); slots: the CFL slots of u to keep current
@@ -488,8 +528,10 @@ BndArgs boundary_args(tlw_handle* h, int stage, int mode, const double* u_jump, 
     return ba;
 }
 
+// phases: 1 the volume kernel (and the halo packing), 2 the surfaces (and the halo faces), 3 both
 void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const double* u_jump, const double* u_base,
-                 double* out, const double* dt_ptr, const PhaseEvents* ev = nullptr, bool alpha_ready = false) {
+                 double* out, const double* dt_ptr, const PhaseEvents* ev = nullptr, bool alpha_ready = false,
+                 int phases = 3) {
     if (h->sc && !alpha_ready) enqueue_indicator(h, u_jump, false);   // indicator of the instantaneous u
     if (h->parabolic) {
         // BR1 gradients, parabolic LW volume kernel, then the interfaces with the viscous traces
@@ -554,8 +596,13 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
         va.metrics = h->d_Ja;
         va.inv_jac_node = h->d_ijn;
     }
-    dispatch<Vol>(h->N, h->stream, stage, mode, h->sc, va);
-    if (ev) cudaEventRecord(ev->after_volume, h->stream);
+    if (phases & 1) {
+        dispatch<Vol>(h->N, h->stream, stage, mode, h->sc, va);
+        if (ev) cudaEventRecord(ev->after_volume, h->stream);
+        for (int cls = 0; cls < 2 && h->nh > 0; ++cls)
+            dispatch<Halo>(h->N, h->stream, halo_args(h, cls, mode, u_jump, out, dt_ptr), true);
+    }
+    if (!(phases & 2)) return;
     if (h->curved) {
         // MDRK stage 1 scales the Dirichlet time averages by 1/2, as the P4estMesh path does
         // (src/solvers/dgsem_tree/multi_derivative_2d.jl:34)
@@ -612,6 +659,7 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
         ma.count = h->nmx; ma.orientation = 1;
         dispatch<Mrt>(h->N, h->stream, ma);
     }
+    if (h->nh > 0) dispatch<Halo>(h->N, h->stream, halo_args(h, 0, mode, u_jump, out, dt_ptr), false);
     if (ev) cudaEventRecord(ev->after_x, h->stream);
     sa.left = h->d_yl; sa.right = h->d_yr; sa.count = h->ny; sa.orientation = 2;
     dispatch<Ifc>(h->N, h->stream, sa);
@@ -623,6 +671,7 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
         ma.count = h->nmy; ma.orientation = 2;
         dispatch<Mrt>(h->N, h->stream, ma);
     }
+    if (h->nh > 0) dispatch<Halo>(h->N, h->stream, halo_args(h, 1, mode, u_jump, out, dt_ptr), false);
     if (ev) cudaEventRecord(ev->after_y, h->stream);
 }
 
@@ -995,6 +1044,98 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
     return TLW_OK;
 }
 
+int tlw_set_halo(tlw_handle* h, int64_t n_halo, const int64_t* elements, const int32_t* faces) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh || h->curved) return fail(h, TLW_E_STATE, "halo faces follow tlw_set_tree_mesh");
+    if (n_halo > 0 && (h->opts.time_discretization != TLW_LW || h->sc || h->parabolic || h->nmx + h->nmy > 0))
+        return fail(h, TLW_E_UNSUPPORTED, "domain decomposition: LW, FR volume integral, conforming TreeMesh, Euler");
+    if (n_halo < 0 || (n_halo > 0 && (!elements || !faces))) return fail(h, TLW_E_ARG, "halo faces");
+    std::vector<int> he[2], hf[2], hs[2];
+    std::vector<signed char> seen((size_t)h->E * 4, 0);
+    for (int64_t k = 0; k < n_halo; ++k) {
+        const int64_t e = elements[k] - 1;
+        const int f = faces[k];
+        if (e < 0 || e >= h->E || f < 0 || f > 3 || seen[(size_t)e * 4 + f])
+            return fail(h, TLW_E_ARG, "halo face " + std::to_string(k + 1) + " out of range or repeated");
+        seen[(size_t)e * 4 + f] = 1;
+        const int c = f >> 1;
+        he[c].push_back((int)e); hf[c].push_back(f); hs[c].push_back((int)k);
+    }
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    for (int** d : {&h->d_he, &h->d_hf, &h->d_hs})
+        if (*d) { cudaFree(*d); *d = nullptr; }
+    dfree(h->d_send); dfree(h->d_recv);
+    h->nh = (int)n_halo;
+    h->nhx = (int)he[0].size();
+    h->slots_valid = false;
+    if (n_halo > 0) {
+        auto up = [&](int*& d, const std::vector<int>& a, const std::vector<int>& b) -> int {
+            std::vector<int> v(a);
+            v.insert(v.end(), b.begin(), b.end());
+            TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
+            TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+            return TLW_OK;
+        };
+        int rc;
+        if ((rc = up(h->d_he, he[0], he[1])) || (rc = up(h->d_hf, hf[0], hf[1])) || (rc = up(h->d_hs, hs[0], hs[1])))
+            return rc;
+        const size_t nd = (size_t)n_halo * h->n * HALO_VALUES;
+        TLW_CUDA(h, cudaMalloc(&h->d_send, nd * sizeof(double)));
+        TLW_CUDA(h, cudaMalloc(&h->d_recv, nd * sizeof(double)));
+        TLW_CUDA(h, cudaMemset(h->d_send, 0, nd * sizeof(double)));
+        TLW_CUDA(h, cudaMemset(h->d_recv, 0, nd * sizeof(double)));
+    }
+    return TLW_OK;
+}
+
+int tlw_dd_buffers(tlw_handle* h, double** send, double** recv, unsigned long long** max_bits) {
+    if (!h) return TLW_E_ARG;
+    if (send) *send = h->d_send;
+    if (recv) *recv = h->d_recv;
+    if (max_bits) *max_bits = h->d_step ? &h->d_step->max_bits : nullptr;
+    return TLW_OK;
+}
+
+int tlw_dd_begin(tlw_handle* h, double cfl, double fixed_dt, double t_end) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    double params[3] = {t_end, cfl, fixed_dt};
+    TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->t_end, params, sizeof(params), cudaMemcpyHostToDevice, h->stream));
+    // this part's maximum; the caller reduces it over the ranks (MAX) before tlw_dd_volume
+    const double* u = h->d_state[h->cur];
+    dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, true, false,
+                  indicator_args(h));
+    TLW_CUDA(h, cudaGetLastError());
+    return TLW_OK;
+}
+
+int tlw_dd_volume(tlw_handle* h) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
+    const double* u = h->d_state[h->cur];
+    enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, h->d_state[1 - h->cur], &h->d_step->dt, nullptr, true, 1);
+    TLW_CUDA(h, cudaGetLastError());
+    return TLW_OK;
+}
+
+int tlw_dd_finish(tlw_handle* h) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    const double* u = h->d_state[h->cur];
+    double* unew = h->d_state[1 - h->cur];
+    enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, &h->d_step->dt, nullptr, true, 2);
+    enqueue_limiter(h, unew, 2, nullptr);
+    TLW_CUDA(h, cudaGetLastError());
+    h->cur ^= 1;
+    return TLW_OK;
+}
+
 int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t* elements, const int32_t* faces,
                               const int32_t* kinds) {
     if (!h) return TLW_E_ARG;
@@ -1223,6 +1364,7 @@ int tlw_rhs(tlw_handle* h, int32_t stage, double* du, const double* u, const dou
     (void)t;
     int rc = check_ready(h);
     if (rc) return rc;
+    if (h->nh > 0) return fail(h, TLW_E_STATE, "a partitioned mesh steps with tlw_dd_begin / _volume / _finish");
     if (!du || !u || (stage == TLW_STAGE_MDRK2 && !us)) return fail(h, TLW_E_ARG, "null pointer");
     if (stage < TLW_STAGE_LW || stage > TLW_STAGE_MDRK2) return fail(h, TLW_E_ARG, "stage");
     if (stage != TLW_STAGE_LW && h->opts.time_discretization != TLW_MDRK)
@@ -1345,6 +1487,7 @@ int tlw_get_state(tlw_handle* h, double* u, int32_t where, double* t_out) {
 int tlw_step(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double t_end, int32_t use_graph) {
     int rc = check_ready(h);
     if (rc) return rc;
+    if (h->nh > 0) return fail(h, TLW_E_STATE, "a partitioned mesh steps with tlw_dd_begin / _volume / _finish");
     if (nsteps < 0) return fail(h, TLW_E_ARG, "nsteps");
     if (nsteps == 0) return TLW_OK;
     TLW_CUDA(h, cudaSetDevice(h->device));
@@ -1407,6 +1550,7 @@ int tlw_step(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double 
 int tlw_step_timed(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double t_end, double* phase_ms) {
     int rc = check_ready(h);
     if (rc) return rc;
+    if (h->nh > 0) return fail(h, TLW_E_STATE, "a partitioned mesh steps with tlw_dd_begin / _volume / _finish");
     if (nsteps < 0 || !phase_ms) return fail(h, TLW_E_ARG, "nsteps / phase_ms");
     TLW_CUDA(h, cudaSetDevice(h->device));
     double params[3] = {t_end, cfl, fixed_dt};

@@ -108,6 +108,11 @@ struct tlw_handle {
     // Navier-Stokes walls per boundary (WALL_*) and their data [3, l, B] (v1, v2, q or T)
     int* d_wkind = nullptr;
     double* d_wall = nullptr;
+    // faces shared with other ranks' parts (domain decomposition): x-faces [0, nhx), y-faces [nhx, nh); local
+    // element, face, position in the caller's order; send / receive buffers [halo][l][12]
+    int nh = 0, nhx = 0;
+    int *d_he = nullptr, *d_hf = nullptr, *d_hs = nullptr;
+    double *d_send = nullptr, *d_recv = nullptr;
     // per element: the faces (0..3) through which it is the large element of a mortar, in mortar order
     // (bits 0-2 count, then 2 bits per mortar); for the positivity limiter's mortar pass
     int* d_mface = nullptr;

@@ -44,6 +44,7 @@ EXPORTED = (
     "tlw_set_parabolic", "tlw_adaptive_trial", "tlw_adaptive_accept",
     "tlw_set_positivity_limiter", "tlw_apply_positivity_limiter", "tlw_set_boundary_kinds", "tlw_set_parabolic_walls",
     "tlw_set_curved_boundaries",
+    "tlw_set_halo", "tlw_dd_buffers", "tlw_dd_begin", "tlw_dd_volume", "tlw_dd_finish",
 )
 
 
@@ -120,6 +121,11 @@ def lib() -> ctypes.CDLL:
     L.tlw_set_boundary_kinds.argtypes = [P, P]
     L.tlw_set_parabolic_walls.argtypes = [P, P, P]
     L.tlw_set_curved_boundaries.argtypes = [P, i64, P, P, P]
+    L.tlw_set_halo.argtypes = [P, i64, P, P]
+    L.tlw_dd_buffers.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P)]
+    L.tlw_dd_begin.argtypes = [P, dbl, dbl, dbl]
+    L.tlw_dd_volume.argtypes = [P]
+    L.tlw_dd_finish.argtypes = [P]
     L.tlw_adaptive_trial.argtypes = [P, dbl, dbl, dbl, dp, ctypes.POINTER(ctypes.c_int32)]
     L.tlw_adaptive_accept.argtypes = [P, dbl]
     L.tlw_curved_colors.argtypes = [P]

@@ -306,6 +306,7 @@ class SemidiscretizationHyperbolic:
         opts.max_speed = _lib.TLW_SPEED_DAVIS if getattr(sf, "max_abs_speed", "naive") == "davis" else _lib.TLW_SPEED_NAIVE
         opts.gamma = equations.gamma
         opts.device = device
+        self.device = int(device)
         vi = solver.volume_integral
         if isinstance(vi, VolumeIntegralFRShockCapturing):
             opts.volume_integral = _lib.TLW_VOLUME_FR_SHOCK_CAPTURING
