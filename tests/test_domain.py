@@ -102,8 +102,10 @@ def _semi(tl, mesh, N, bc=None):
     eq = tl.CompressibleEulerEquations2D(1.4)
     solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.LW()))
     kw = {} if bc is None else {"boundary_conditions": bc}
-    return tl.SemidiscretizationHyperbolic(mesh, tl.LW(), eq, tl.IsentropicVortex(5.0, center=(0.3, -0.2)), solver,
-                                           **kw)
+    # with walls: a vortex at rest (no background flow into the walls)
+    ic = (tl.IsentropicVortex(5.0, center=(0.3, -0.2)) if bc is None else
+          tl.IsentropicVortex(3.0, center=(0.3, -0.2), domain=(-5.0, 5.0), velocity=(0.0, 0.0)))
+    return tl.SemidiscretizationHyperbolic(mesh, tl.LW(), eq, ic, solver, **kw)
 
 
 def _lockstep(tl, parts, semis, steps, cfl):
