@@ -551,6 +551,99 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_decomposed(args):
+    """Strong scaling of one TreeMesh over the ranks: each rank owns a contiguous range of the elements'
+    space-filling-curve order and steps with the library's split step (tlw_dd_begin / _volume / _finish);
+    the CFL maximum is all-reduced (MAX) and the cut-face traces exchanged with the neighbouring ranks over
+    NCCL, both ordered on the library's stream. value = the whole mesh's DOF-updates over the max-over-ranks
+    device time."""
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import trixilw as tl
+    from trixilw import _lib
+    from trixilw.domain import DomainDecomposedLW, partition, torch_collectives
+
+    rank, local_rank, world = dist_env()
+    torch.cuda.set_device(local_rank)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local_rank))
+    level, N, td, icname = WORKLOADS[args.workload]
+    if td != "lw" or icname not in ("vortex",):
+        raise SystemExit("--decompose: the periodic vortex LW workloads")
+    mesh = make_mesh(tl, level, icname)
+    part = partition(mesh, world)[rank]
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.LW()))
+    semi = tl.SemidiscretizationHyperbolic(part.mesh, tl.LW(), eq, tl.IsentropicVortex(5.0), solver, device=local_rank)
+    cfl = cfl_for(N)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, tl.LW(), (0.0, 1e9)))
+    u0 = semi.compute_coefficients(0.0)
+    integ.set_state(u0, 0.0)
+    allreduce_max, exchange = torch_collectives()
+    dd = DomainDecomposedLW(semi, part, allreduce_max, exchange)
+    dd.step(max(args.warmup, 3), cfl)
+    torch.cuda.synchronize()
+    gpu_index = int(os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local_rank]) \
+        if os.environ.get("CUDA_VISIBLE_DEVICES") else local_rank
+    sampler = ClockSampler(gpu_index)
+    sampler.start()
+    time.sleep(0.3)
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(dd.stream)
+    dd.step(args.steps, cfl)
+    ev1.record(dd.stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = sampler.stop()
+    t = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    # end to end: this rank's part from pinned host memory, one split step, back to host
+    n_e2e = max(1, min(args.steps, 10))
+    uh = torch.empty(u0.size, dtype=torch.float64, pin_memory=True).numpy()
+    uh[:] = u0
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(dd.stream)
+    for _ in range(n_e2e):
+        integ.set_state(uh, 0.0)
+        dd.step(1, cfl)
+        uh[:] = integ.get_state()
+    e1.record(dd.stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_e2e = float(t.item())
+    ndofs = mesh.ndofs(N)
+    if rank == 0:
+        part_bytes = 8 * 4 * part.mesh.ndofs(N)
+        out = {
+            "metric": METRIC, "value": ndofs * args.steps / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "polydeg": N, "elements": mesh.n_elements, "ndofs": ndofs,
+                       "cfl": cfl, "parallelism": f"domain decomposition over {world} ranks (space-filling-curve "
+                       "ranges; MAX all-reduce of the CFL maximum and cut-face trace exchange over NCCL)",
+                       "halo_faces_rank0": int(len(part.halo_keys)),
+                       "l2": "inputs larger than L2" if part_bytes > 126e6 else "state of a part may fit in L2"},
+            "e2e": {"value": ndofs * n_e2e / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": part_bytes,
+                    "d2h_bytes_per_step": part_bytes, "steps": n_e2e, "note": "per rank: its part"},
+            "clocks": clocks,
+            # speed, dt, volume, x / y interfaces, and per class of cut faces one pack and one halo launch
+            "gpu_launches": args.steps * (5 + 2 * len({int(f) >> 1 for f in part.halo_faces})),
+        }
+        print(json.dumps(out), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def batch_instances(tl, count):
     """The uneven batch: instance k draws its parameters from numpy's default_rng(k)."""
     import numpy as np
@@ -894,8 +987,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fd-directions", type=int, default=64,
                     help="adjoint workload: random directions of the finite-difference gradient check")
+    ap.add_argument("--decompose", action="store_true",
+                    help="under torchrun: split one mesh over the ranks (halo exchange over NCCL) instead of "
+                         "running independent replicas")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.impl == "ours" and args.decompose:
+        run_decomposed(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload in BATCH_WORKLOADS:
         run_batched(args)
