@@ -238,9 +238,12 @@ struct AdjVolArgs {
     const double* dt;
     int E;
     double gamma;
+    const double* dstore;   // the step's stage derivatives d_1..d_depth [m][e][node][v] (LOADD), from the recompute
 };
 
-template <int N>
+// LOADD: read the stage derivatives the segment recompute stored (lw_volume_kernel<..., DSTORE>) instead of
+// recomputing them here
+template <int N, bool LOADD = false>
 static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOCKS) adj_volume_kernel(AdjVolArgs a) {
     using C = AdjCfg<N>;
     using K = LWC<C::DEPTH>;
@@ -320,7 +323,16 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
         }
     };
 
-    // ---- forward recompute of d_1 .. d_DEPTH (into shared memory)
+    // ---- d_1 .. d_DEPTH into shared memory: stored by the recompute, or recomputed here
+    if (LOADD) {
+#pragma unroll
+        for (int m = 0; m < DEPTH; ++m) {
+            double d[NV] = {0.0, 0.0, 0.0, 0.0};
+            if (active) load4(a.dstore + ((size_t)m * a.E * nn + (size_t)e * nn + node) * NV, d);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) put(Dm + m * TILE, v, d[v]);
+        }
+    } else {
     {
         double f[NV], g[NV];
         euler_fluxes(gm1, u[0], u[1], u[2], u[3], f, g);
@@ -363,6 +375,7 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
         __syncthreads();
 #pragma unroll
         for (int v = 0; v < NV; ++v) put(Dm + s * TILE, v, dn[v]);
+    }
     }
 
     // ---- adjoint inputs: volume term u_new += sc (Dhat F + Dhat G), then the face traces
@@ -503,12 +516,25 @@ struct AL {
                              (int)VolCfg<N>::smem_bytes(4));
         cudaFuncSetAttribute(adj_volume_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)AdjCfg<N>::smem_bytes());
+        cudaFuncSetAttribute(adj_volume_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)AdjCfg<N>::smem_bytes());
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, false, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VolCfg<N>::smem_bytes(4));
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, false, false, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VolCfg<N>::smem_bytes(4));
     }
+    // with va.dstore: also store the stage derivatives for the adjoint
     static void forward_volume(cudaStream_t s, int mode, const VolArgs& va) {
         using C = VolCfg<N>;
         const int grid = (int)((va.E + C::EB - 1) / C::EB);
-        if (mode == MODE_STEP) lw_volume_kernel<N, MODE_STEP, false><<<grid, C::THREADS, C::smem_bytes(4), s>>>(va);
-        else lw_volume_kernel<N, MODE_RHS, false><<<grid, C::THREADS, C::smem_bytes(4), s>>>(va);
+        const size_t sm = C::smem_bytes(4);
+        if (va.dstore) {
+            if (mode == MODE_STEP) lw_volume_kernel<N, MODE_STEP, false, 0, false, false, true><<<grid, C::THREADS, sm, s>>>(va);
+            else lw_volume_kernel<N, MODE_RHS, false, 0, false, false, true><<<grid, C::THREADS, sm, s>>>(va);
+        } else {
+            if (mode == MODE_STEP) lw_volume_kernel<N, MODE_STEP, false><<<grid, C::THREADS, sm, s>>>(va);
+            else lw_volume_kernel<N, MODE_RHS, false><<<grid, C::THREADS, sm, s>>>(va);
+        }
     }
     static void forward_interfaces(cudaStream_t s, SurfArgs sa, const tlw_handle* h) {
         sa.left = h->d_xl; sa.right = h->d_xr; sa.count = h->nx; sa.orientation = 1;
@@ -529,7 +555,8 @@ struct AL {
         if (th) adj_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(sa);
         using C = AdjCfg<N>;
         const int grid = (va.E + C::EB - 1) / C::EB;
-        adj_volume_kernel<N><<<grid, C::THREADS, C::smem_bytes(), s>>>(va);
+        if (va.dstore) adj_volume_kernel<N, true><<<grid, C::THREADS, C::smem_bytes(), s>>>(va);
+        else adj_volume_kernel<N><<<grid, C::THREADS, C::smem_bytes(), s>>>(va);
     }
 };
 
@@ -545,6 +572,8 @@ bool adj_degree(int N, F&& f) {
 
 size_t nstate(const tlw_handle* h) { return (size_t)NV * h->nn * h->E; }
 size_t ntrace(const tlw_handle* h) { return (size_t)NV * h->n * 4 * h->E; }
+// stages of the volume procedure: 3 for N = 3, 4 for N >= 4
+int depth(const tlw_handle* h) { return h->N >= 4 ? 4 : 3; }
 
 int adj_ready(tlw_handle* h) {
     if (!h) return TLW_E_ARG;
@@ -605,8 +634,10 @@ int ensure_steps(tlw_handle* h, int nsteps, int ck) {
     if (A.capacity_states < ck) {
         dfree(A.d_seg);
         dfree(A.d_segU);
+        dfree(A.d_segD);
         TLW_ACUDA(h, cudaMalloc(&A.d_seg, (size_t)ck * nstate(h) * sizeof(double)));
         TLW_ACUDA(h, cudaMalloc(&A.d_segU, (size_t)ck * ntrace(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_segD, (size_t)ck * depth(h) * nstate(h) * sizeof(double)));
         A.capacity_states = ck;
     }
     return TLW_OK;
@@ -659,8 +690,10 @@ SurfArgs fwd_surf_args(tlw_handle* h, const double* u, double* out, const double
 }
 
 // one forward LW step at the dt stored at dtp; U traces into tU
-void enqueue_fixed_step(tlw_handle* h, const double* u, double* unew, double* tU, const double* dtp) {
-    const VolArgs va = fwd_vol_args(h, u, unew, tU, dtp);
+void enqueue_fixed_step(tlw_handle* h, const double* u, double* unew, double* tU, const double* dtp,
+                        double* dstore = nullptr) {
+    VolArgs va = fwd_vol_args(h, u, unew, tU, dtp);
+    va.dstore = dstore;
     const SurfArgs sa = fwd_surf_args(h, u, unew, tU, dtp, 1);
     adj_degree(h->N, [&](auto Nc) {
         constexpr int N = decltype(Nc)::value;
@@ -671,7 +704,7 @@ void enqueue_fixed_step(tlw_handle* h, const double* u, double* unew, double* tU
 
 // lam_out = (du_new/du)^T lam_in for the step from u at dt (*dtp); tU = that step's forward U traces
 void enqueue_adjoint_step(tlw_handle* h, const double* u, const double* tU, const double* dtp, const double* lam_in,
-                          double* lam_out) {
+                          double* lam_out, const double* dstore = nullptr) {
     AdjointBuffers& A = h->adj;
     AdjSurfArgs sa{};
     sa.u = u;
@@ -700,6 +733,7 @@ void enqueue_adjoint_step(tlw_handle* h, const double* u, const double* tU, cons
     va.dt = dtp;
     va.E = (int)h->E;
     va.gamma = h->opts.gamma;
+    va.dstore = dstore;
     adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::adjoint(h->stream, sa, va); });
 }
 
@@ -888,15 +922,18 @@ int reverse_sweep_enqueue(tlw_handle* h, int& cur, double* phase_ms) {
         // recompute the segment's states and U traces from its checkpoint
         TLW_ACUDA(h, cudaMemcpyAsync(A.d_seg, A.d_ckpt + (size_t)sgi * ns, ns * sizeof(double),
                                      cudaMemcpyDeviceToDevice, h->stream));
+        // each recomputed step also stores its stage derivatives, which its adjoint step reads back
+        const size_t nd = (size_t)depth(h) * ns;
         for (int j = 0; j < len; ++j) {
             if (j + 1 < len) {
                 enqueue_fixed_step(h, A.d_seg + (size_t)j * ns, A.d_seg + (size_t)(j + 1) * ns,
-                                   A.d_segU + (size_t)j * nt, A.d_dts + start + j);
+                                   A.d_segU + (size_t)j * nt, A.d_dts + start + j, A.d_segD + (size_t)j * nd);
             } else {
                 // the segment's last output state is not needed, only the U traces of its step (volume
                 // kernel alone, its du into the free adjoint buffer)
-                const VolArgs va = fwd_vol_args(h, A.d_seg + (size_t)j * ns, A.d_lam[1 - cur],
-                                                A.d_segU + (size_t)j * nt, A.d_dts + start + j);
+                VolArgs va = fwd_vol_args(h, A.d_seg + (size_t)j * ns, A.d_lam[1 - cur], A.d_segU + (size_t)j * nt,
+                                          A.d_dts + start + j);
+                va.dstore = A.d_segD + (size_t)j * nd;
                 adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::forward_volume(h->stream, MODE_RHS, va); });
             }
         }
@@ -909,7 +946,7 @@ int reverse_sweep_enqueue(tlw_handle* h, int& cur, double* phase_ms) {
         }
         for (int j = len - 1; j >= 0; --j) {
             enqueue_adjoint_step(h, A.d_seg + (size_t)j * ns, A.d_segU + (size_t)j * nt, A.d_dts + start + j,
-                                 A.d_lam[cur], A.d_lam[1 - cur]);
+                                 A.d_lam[cur], A.d_lam[1 - cur], A.d_segD + (size_t)j * nd);
             cur ^= 1;
         }
         if (phase_ms) {

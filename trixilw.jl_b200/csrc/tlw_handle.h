@@ -32,6 +32,7 @@ struct AdjointBuffers {
     int capacity_ckpt = 0;
     double* d_seg = nullptr;                // recomputed states of one segment
     double* d_segU = nullptr;               // time-averaged U traces of one segment
+    double* d_segD = nullptr;               // stage derivatives d_1..d_depth of every step of one segment
     double* d_work = nullptr;               // scratch (objective partial sums)
     double* d_final = nullptr;              // u(T) of the recorded run (one of the handle's state buffers)
     int rec_steps = 0, rec_ck = 0;          // recorded forward run: steps, checkpoint interval
@@ -46,7 +47,7 @@ inline void free_adjoint(AdjointBuffers& a) {
     if (a.g_fwd) cudaGraphExecDestroy(a.g_fwd);
     if (a.g_rev) cudaGraphExecDestroy(a.g_rev);
     dfree(a.d_lam[0]); dfree(a.d_lam[1]); dfree(a.d_bF); dfree(a.d_bU); dfree(a.d_bu); dfree(a.d_dts);
-    dfree(a.d_dts_given); dfree(a.d_ckpt); dfree(a.d_seg); dfree(a.d_segU); dfree(a.d_work);
+    dfree(a.d_dts_given); dfree(a.d_ckpt); dfree(a.d_seg); dfree(a.d_segU); dfree(a.d_segD); dfree(a.d_work);
     a = AdjointBuffers{};
 }
 
