@@ -225,6 +225,8 @@ struct AdjCfg {
     // shared memory: D, Dhat, the two contraction tiles X, Y, the stage derivatives d_m and their adjoints
     static constexpr int TILE = NV * EB * nn;
     static constexpr size_t smem_bytes() { return (size_t)(2 * nn + (2 + 2 * DEPTH) * TILE) * sizeof(double); }
+    // adj_volume_reg_kernel: D, Dhat, X, Y and the d_m (their adjoints are in registers)
+    static constexpr size_t reg_smem_bytes() { return (size_t)(2 * nn + (2 + DEPTH) * TILE) * sizeof(double); }
 };
 
 struct AdjVolArgs {
@@ -472,6 +474,184 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
     }
 }
 
+// adj_volume_kernel with the stage derivatives stored by the segment recompute, held in registers with their
+// adjoints: each thread reads and accumulates only its own node's d_m and bar d_m, so only the transposed
+// contractions go through shared memory (one tile per stage, alternating between X and Y so that one barrier a
+// stage separates a tile's reads from its next writes). Same operations in the same order as the LOADD kernel.
+// DREG: the d_m in registers too; otherwise in shared memory, where each thread reads back only what it wrote.
+template <int N, int MINB, bool DREG>
+static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_reg_kernel(AdjVolArgs a) {
+    using C = AdjCfg<N>;
+    using K = LWC<C::DEPTH>;
+    constexpr int n = C::n, nn = C::nn, EB = C::EB, DEPTH = C::DEPTH, TILE = C::TILE;
+    extern __shared__ double sm[];
+    double* sD = sm;
+    double* sDh = sm + nn;
+    double* X = sm + 2 * nn;
+    double* Y = X + TILE;
+    double* Dt = Y + TILE;   // d_m at Dt + (m - 1) * TILE (!DREG)
+    for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+        sD[k] = c_tlw_D[N][k];
+        sDh[k] = c_tlw_Dhat[N][k];
+    }
+    const int el = threadIdx.x / nn;
+    const int node = threadIdx.x - el * nn;
+    const int i = node % n, j = node / n;
+    const long long e = (long long)blockIdx.x * EB + el;
+    const bool active = el < EB && e < a.E;
+    const bool in_tile = el < EB;
+    const int slot = in_tile ? el : 0;
+    const int me = slot * nn + node;
+    auto put = [&](double* T, int v, double x) {
+        if (in_tile) T[v * EB * nn + me] = x;
+    };
+    double u[NV] = {1.0, 0.0, 0.0, 2.5};
+    double ij = 1.0;
+    double dm[DREG ? DEPTH : 1][NV];
+#pragma unroll
+    for (int m = 0; m < (DREG ? DEPTH : 1); ++m)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) dm[m][v] = 0.0;
+    double lam[NV] = {0.0, 0.0, 0.0, 0.0};
+    if (active) {
+        load4(a.u + ((size_t)e * nn + node) * NV, u);
+        ij = __ldg(a.inv_jac + e);
+        if (DREG) {
+#pragma unroll
+            for (int m = 0; m < DEPTH; ++m)
+                load4(a.dstore + ((size_t)m * a.E * nn + (size_t)e * nn + node) * NV, dm[DREG ? m : 0]);
+        }
+        load4(a.lam + ((size_t)e * nn + node) * NV, lam);
+    }
+    if (!DREG) {
+#pragma unroll
+        for (int m = 0; m < DEPTH; ++m) {
+            double d[NV] = {0.0, 0.0, 0.0, 0.0};
+            if (active) load4(a.dstore + ((size_t)m * a.E * nn + (size_t)e * nn + node) * NV, d);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) put(Dt + m * TILE, v, d[v]);
+        }
+    }
+    // d_m of this node, m = 1..DEPTH (a thread outside the tile reads zeros)
+    auto dget = [&](int m, int v) -> double {
+        if (DREG) return dm[DREG ? m - 1 : 0][v];
+        return in_tile ? Dt[(m - 1) * TILE + v * EB * nn + me] : 0.0;
+    };
+    const double dt = *a.dt;
+    const double sc = -dt * ij;
+    auto cxt = [&](const double* M, const double* W, int v) {
+        const double* p = W + v * EB * nn + slot * nn + n * j;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) s = fma(M[k * n + i], p[k], s);
+        return s;
+    };
+    auto cyt = [&](const double* M, const double* W, int v) {
+        const double* p = W + v * EB * nn + slot * nn + i;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) s = fma(M[k * n + j], p[n * k], s);
+        return s;
+    };
+
+    // ---- adjoint inputs: volume term u_new += sc (Dhat F + Dhat G), then the face traces
+    double bF[NV], bG[NV], bU[NV] = {0.0, 0.0, 0.0, 0.0}, bud[NV] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int v = 0; v < NV; ++v) put(X, v, sc * lam[v]);
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { bF[v] = cxt(sDh, X, v); bG[v] = cyt(sDh, X, v); }
+    if (active) {
+        auto face = [&](int f, int l, double* tgt) {
+            const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
+            double x[NV];
+            load4(a.bF + t, x);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) tgt[v] += x[v];
+            load4(a.bU + t, x);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) bU[v] += x[v];
+            load4(a.bu + t, x);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) bud[v] += x[v];
+        };
+        if (i == 0) face(0, j, bF);
+        if (i == n - 1) face(1, j, bF);
+        if (j == 0) face(2, i, bG);
+        if (j == n - 1) face(3, i, bG);
+    }
+
+    // ---- reverse sweep
+    double bd[DEPTH][NV], bu[NV], bf0[NV], bg0[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+#pragma unroll
+        for (int m = 0; m < DEPTH; ++m) bd[m][v] = K::tw(m + 1) * bU[v];
+        bu[v] = bU[v];
+        bf0[v] = bF[v];
+        bg0[v] = bG[v];
+    }
+#pragma unroll
+    for (int s = DEPTH; s >= 1; --s) {
+        double bfx[NV], bgy[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { bfx[v] = K::tw(s) * bF[v]; bgy[v] = K::tw(s) * bG[v]; }
+        if (s < DEPTH) {
+            // d_{s+1} = C(ft_s, gt_s): its adjoint is complete (stages > s are done)
+            double* T = ((DEPTH - s) & 1) ? Y : X;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) put(T, v, bd[s][v]);
+            __syncthreads();
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                bfx[v] = fma(sc, cxt(sD, T, v), bfx[v]);
+                bgy[v] = fma(sc, cyt(sD, T, v), bgy[v]);
+            }
+        }
+        if (K::w(s, 0) != 0.0) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { bf0[v] = fma(K::w(s, 0), bfx[v], bf0[v]); bg0[v] = fma(K::w(s, 0), bgy[v], bg0[v]); }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (K::w(s, 1 + q) == 0.0) continue;
+            double P[NV], wf[NV], wg[NV], bP[NV] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                double x = u[v];
+#pragma unroll
+                for (int m = 1; m <= s; ++m) x = fma(K::a(q, m), dget(m, v), x);
+                P[v] = x;
+                wf[v] = K::w(s, 1 + q) * bfx[v];
+                wg[v] = K::w(s, 1 + q) * bgy[v];
+            }
+            euler_flux_vjp(a.gamma, P, wf, wg, bP);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                bu[v] += bP[v];
+#pragma unroll
+                for (int m = 1; m <= s; ++m) bd[m - 1][v] = fma(K::a(q, m), bP[v], bd[m - 1][v]);
+            }
+        }
+    }
+    // d_1 = C(f(u), g(u))
+    {
+        double* T = (DEPTH & 1) ? Y : X;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) put(T, v, bd[0][v]);
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { bf0[v] = fma(sc, cxt(sD, T, v), bf0[v]); bg0[v] = fma(sc, cyt(sD, T, v), bg0[v]); }
+    }
+    euler_flux_vjp(a.gamma, u, bf0, bg0, bu);
+    if (active) {
+        double o[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) o[v] = lam[v] + bu[v] + bud[v];
+        store4(a.lam_out + ((size_t)e * nn + node) * NV, o);
+    }
+}
+
 // J = 1/2 sum_nodes (rho - rho_target)^2: per-block partial sums (fixed order) and the seed lam = (rho - rho_t, 0, 0, 0)
 constexpr int OBJ_THREADS = 256;
 static __global__ void __launch_bounds__(OBJ_THREADS) objective_kernel(const double* u, const double* target,
@@ -516,8 +696,8 @@ struct AL {
                              (int)VolCfg<N>::smem_bytes(4));
         cudaFuncSetAttribute(adj_volume_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)AdjCfg<N>::smem_bytes());
-        cudaFuncSetAttribute(adj_volume_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)AdjCfg<N>::smem_bytes());
+        cudaFuncSetAttribute(adj_volume_reg_kernel<N, AdjCfg<N>::MIN_BLOCKS, false>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AdjCfg<N>::reg_smem_bytes());
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, false, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VolCfg<N>::smem_bytes(4));
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, false, false, true>,
@@ -555,7 +735,7 @@ struct AL {
         if (th) adj_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(sa);
         using C = AdjCfg<N>;
         const int grid = (va.E + C::EB - 1) / C::EB;
-        if (va.dstore) adj_volume_kernel<N, true><<<grid, C::THREADS, C::smem_bytes(), s>>>(va);
+        if (va.dstore) adj_volume_reg_kernel<N, C::MIN_BLOCKS, false><<<grid, C::THREADS, C::reg_smem_bytes(), s>>>(va);
         else adj_volume_kernel<N><<<grid, C::THREADS, C::smem_bytes(), s>>>(va);
     }
 };
