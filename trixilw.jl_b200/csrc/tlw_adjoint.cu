@@ -225,8 +225,11 @@ struct AdjCfg {
     // shared memory: D, Dhat, the two contraction tiles X, Y, the stage derivatives d_m and their adjoints
     static constexpr int TILE = NV * EB * nn;
     static constexpr size_t smem_bytes() { return (size_t)(2 * nn + (2 + 2 * DEPTH) * TILE) * sizeof(double); }
-    // adj_volume_reg_kernel: D, Dhat, X, Y and the d_m (their adjoints are in registers)
-    static constexpr size_t reg_smem_bytes() { return (size_t)(2 * nn + (2 + DEPTH) * TILE) * sizeof(double); }
+    // adj_volume_stored_kernel: D, Dhat, X, Y, two stage buffers (u, lam, d_1..d_DEPTH) and their two mbarriers
+    static constexpr int STAGE = (2 + DEPTH) * TILE;
+    static constexpr size_t stored_smem_bytes() {
+        return (size_t)(2 * nn + 2 * TILE + 2 * STAGE) * sizeof(double) + 2 * sizeof(uint64_t);
+    }
 };
 
 struct AdjVolArgs {
@@ -240,12 +243,11 @@ struct AdjVolArgs {
     const double* dt;
     int E;
     double gamma;
-    const double* dstore;   // the step's stage derivatives d_1..d_depth [m][e][node][v] (LOADD), from the recompute
+    const double* dstore;   // the step's stage derivatives d_1..d_depth [m][e][v][node], from the recompute
+    unsigned* status;       // STATUS_WAIT_TIMEOUT
 };
 
-// LOADD: read the stage derivatives the segment recompute stored (lw_volume_kernel<..., DSTORE>) instead of
-// recomputing them here
-template <int N, bool LOADD = false>
+template <int N>
 static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOCKS) adj_volume_kernel(AdjVolArgs a) {
     using C = AdjCfg<N>;
     using K = LWC<C::DEPTH>;
@@ -325,16 +327,7 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
         }
     };
 
-    // ---- d_1 .. d_DEPTH into shared memory: stored by the recompute, or recomputed here
-    if (LOADD) {
-#pragma unroll
-        for (int m = 0; m < DEPTH; ++m) {
-            double d[NV] = {0.0, 0.0, 0.0, 0.0};
-            if (active) load4(a.dstore + ((size_t)m * a.E * nn + (size_t)e * nn + node) * NV, d);
-#pragma unroll
-            for (int v = 0; v < NV; ++v) put(Dm + m * TILE, v, d[v]);
-        }
-    } else {
+    // ---- d_1 .. d_DEPTH into shared memory
     {
         double f[NV], g[NV];
         euler_fluxes(gm1, u[0], u[1], u[2], u[3], f, g);
@@ -377,7 +370,6 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
         __syncthreads();
 #pragma unroll
         for (int v = 0; v < NV; ++v) put(Dm + s * TILE, v, dn[v]);
-    }
     }
 
     // ---- adjoint inputs: volume term u_new += sc (Dhat F + Dhat G), then the face traces
@@ -474,71 +466,59 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
     }
 }
 
-// adj_volume_kernel with the stage derivatives stored by the segment recompute, held in registers with their
-// adjoints: each thread reads and accumulates only its own node's d_m and bar d_m, so only the transposed
-// contractions go through shared memory (one tile per stage, alternating between X and Y so that one barrier a
-// stage separates a tile's reads from its next writes). Same operations in the same order as the LOADD kernel.
-// DREG: the d_m in registers too; otherwise in shared memory, where each thread reads back only what it wrote.
-template <int N, int MINB, bool DREG>
-static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_reg_kernel(AdjVolArgs a) {
+// The adjoint volume step with the stage derivatives the segment recompute stored (lw_volume_kernel<...,
+// DSTORE>): a persistent kernel over tiles of EB elements whose state u, adjoint lam and d_1..d_DEPTH arrive by
+// bulk asynchronous copies into one of two shared-memory stage buffers, the next tile's copies in flight while
+// the current tile is processed. The bar d_m accumulate in registers (each thread owns its node's), so only
+// the transposed contractions go through shared memory: one tile per stage, alternating between X and Y so that
+// one barrier a stage separates a tile's reads from its next writes. Each wait on a copy is bounded: on
+// timeout the kernel flags STATUS_WAIT_TIMEOUT, waits (bounded) for its copies in flight and returns.
+template <int N, int MINB>
+static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_stored_kernel(AdjVolArgs a) {
     using C = AdjCfg<N>;
     using K = LWC<C::DEPTH>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB, DEPTH = C::DEPTH, TILE = C::TILE;
-    extern __shared__ double sm[];
+    constexpr int STAGE = C::STAGE;   // one stage buffer: u, lam ([slot][node][v]), d_1..d_DEPTH ([m][slot][v][node])
+    extern __shared__ __align__(16) double sm[];
     double* sD = sm;
     double* sDh = sm + nn;
     double* X = sm + 2 * nn;
     double* Y = X + TILE;
-    double* Dt = Y + TILE;   // d_m at Dt + (m - 1) * TILE (!DREG)
+    double* buf = Y + TILE;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(buf + 2 * STAGE);
     for (int k = threadIdx.x; k < nn; k += blockDim.x) {
         sD[k] = c_tlw_D[N][k];
         sDh[k] = c_tlw_Dhat[N][k];
     }
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const int ntiles = (a.E + EB - 1) / EB;
+    // thread 0: the copies of one tile into stage buffer b
+    auto issue = [&](int tile, int b) {
+        const long long e0 = (long long)tile * EB;
+        const int ne = (int)min((long long)EB, (long long)a.E - e0);
+        const unsigned bytes = (unsigned)(ne * nn * NV * sizeof(double));
+        double* B = buf + b * STAGE;
+        mbar_arrive_expect_tx(&bar[b], (2 + DEPTH) * bytes);
+        bulk_copy_g2s(B, a.u + e0 * nn * NV, bytes, &bar[b]);
+        bulk_copy_g2s(B + TILE, a.lam + e0 * nn * NV, bytes, &bar[b]);
+#pragma unroll
+        for (int m = 0; m < DEPTH; ++m)
+            bulk_copy_g2s(B + (2 + m) * TILE, a.dstore + ((size_t)m * a.E + e0) * nn * NV, bytes, &bar[b]);
+    };
     const int el = threadIdx.x / nn;
     const int node = threadIdx.x - el * nn;
     const int i = node % n, j = node / n;
-    const long long e = (long long)blockIdx.x * EB + el;
-    const bool active = el < EB && e < a.E;
     const bool in_tile = el < EB;
     const int slot = in_tile ? el : 0;
     const int me = slot * nn + node;
     auto put = [&](double* T, int v, double x) {
         if (in_tile) T[v * EB * nn + me] = x;
     };
-    double u[NV] = {1.0, 0.0, 0.0, 2.5};
-    double ij = 1.0;
-    double dm[DREG ? DEPTH : 1][NV];
-#pragma unroll
-    for (int m = 0; m < (DREG ? DEPTH : 1); ++m)
-#pragma unroll
-        for (int v = 0; v < NV; ++v) dm[m][v] = 0.0;
-    double lam[NV] = {0.0, 0.0, 0.0, 0.0};
-    if (active) {
-        load4(a.u + ((size_t)e * nn + node) * NV, u);
-        ij = __ldg(a.inv_jac + e);
-        if (DREG) {
-#pragma unroll
-            for (int m = 0; m < DEPTH; ++m)
-                load4(a.dstore + ((size_t)m * a.E * nn + (size_t)e * nn + node) * NV, dm[DREG ? m : 0]);
-        }
-        load4(a.lam + ((size_t)e * nn + node) * NV, lam);
-    }
-    if (!DREG) {
-#pragma unroll
-        for (int m = 0; m < DEPTH; ++m) {
-            double d[NV] = {0.0, 0.0, 0.0, 0.0};
-            if (active) load4(a.dstore + ((size_t)m * a.E * nn + (size_t)e * nn + node) * NV, d);
-#pragma unroll
-            for (int v = 0; v < NV; ++v) put(Dt + m * TILE, v, d[v]);
-        }
-    }
-    // d_m of this node, m = 1..DEPTH (a thread outside the tile reads zeros)
-    auto dget = [&](int m, int v) -> double {
-        if (DREG) return dm[DREG ? m - 1 : 0][v];
-        return in_tile ? Dt[(m - 1) * TILE + v * EB * nn + me] : 0.0;
-    };
-    const double dt = *a.dt;
-    const double sc = -dt * ij;
     auto cxt = [&](const double* M, const double* W, int v) {
         const double* p = W + v * EB * nn + slot * nn + n * j;
         double s = 0.0;
@@ -553,102 +533,146 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_re
         for (int k = 0; k < n; ++k) s = fma(M[k * n + j], p[n * k], s);
         return s;
     };
-
-    // ---- adjoint inputs: volume term u_new += sc (Dhat F + Dhat G), then the face traces
-    double bF[NV], bG[NV], bU[NV] = {0.0, 0.0, 0.0, 0.0}, bud[NV] = {0.0, 0.0, 0.0, 0.0};
+    const double dt = *a.dt;
+    // the it-th tile of this CTA is in buffer it & 1, that buffer's (it >> 1)-th phase
+    if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    bool failed = false;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int b = it & 1;
+        const int next = tile + (int)gridDim.x;
+        // buffer b ^ 1 was last read before the previous tile's final barrier
+        if (threadIdx.x == 0 && next < ntiles) issue(next, b ^ 1);
+        const long long e = (long long)tile * EB + el;
+        const bool active = in_tile && e < a.E;
+        // face-trace adjoints (plain loads, issued before the wait)
+        double bF[NV] = {0.0, 0.0, 0.0, 0.0}, bG[NV] = {0.0, 0.0, 0.0, 0.0}, bU[NV] = {0.0, 0.0, 0.0, 0.0};
+        double bud[NV] = {0.0, 0.0, 0.0, 0.0};
+        if (active) {
+            auto face = [&](int f, int l, double* tgt) {
+                const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
+                double x[NV];
+                load4(a.bF + t, x);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) put(X, v, sc * lam[v]);
-    __syncthreads();
+                for (int v = 0; v < NV; ++v) tgt[v] += x[v];
+                load4(a.bU + t, x);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) { bF[v] = cxt(sDh, X, v); bG[v] = cyt(sDh, X, v); }
-    if (active) {
-        auto face = [&](int f, int l, double* tgt) {
-            const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
-            double x[NV];
-            load4(a.bF + t, x);
+                for (int v = 0; v < NV; ++v) bU[v] += x[v];
+                load4(a.bu + t, x);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) tgt[v] += x[v];
-            load4(a.bU + t, x);
+                for (int v = 0; v < NV; ++v) bud[v] += x[v];
+            };
+            if (i == 0) face(0, j, bF);
+            if (i == n - 1) face(1, j, bF);
+            if (j == 0) face(2, i, bG);
+            if (j == n - 1) face(3, i, bG);
+        }
+        const double ij = active ? __ldg(a.inv_jac + e) : 1.0;
+        // (the barrier also orders the previous tile's last reads of X / Y before this tile's first writes)
+        const bool ok = mbar_wait_bounded(&bar[b], (unsigned)((it >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        const double* B = buf + b * STAGE;
+        double u[NV] = {1.0, 0.0, 0.0, 2.5}, lam[NV] = {0.0, 0.0, 0.0, 0.0};
+        if (active) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) bU[v] += x[v];
-            load4(a.bu + t, x);
-#pragma unroll
-            for (int v = 0; v < NV; ++v) bud[v] += x[v];
+            for (int v = 0; v < NV; ++v) {
+                u[v] = B[me * NV + v];
+                lam[v] = B[TILE + me * NV + v];
+            }
+        }
+        // d_m of this node, m = 1..DEPTH (zeros outside the mesh)
+        auto dget = [&](int m, int v) -> double {
+            return active ? B[(1 + m) * TILE + (slot * NV + v) * nn + node] : 0.0;
         };
-        if (i == 0) face(0, j, bF);
-        if (i == n - 1) face(1, j, bF);
-        if (j == 0) face(2, i, bG);
-        if (j == n - 1) face(3, i, bG);
-    }
+        const double sc = -dt * ij;
 
-    // ---- reverse sweep
-    double bd[DEPTH][NV], bu[NV], bf0[NV], bg0[NV];
+        // ---- adjoint inputs: volume term u_new += sc (Dhat F + Dhat G), then the face traces
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-#pragma unroll
-        for (int m = 0; m < DEPTH; ++m) bd[m][v] = K::tw(m + 1) * bU[v];
-        bu[v] = bU[v];
-        bf0[v] = bF[v];
-        bg0[v] = bG[v];
-    }
-#pragma unroll
-    for (int s = DEPTH; s >= 1; --s) {
-        double bfx[NV], bgy[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) { bfx[v] = K::tw(s) * bF[v]; bgy[v] = K::tw(s) * bG[v]; }
-        if (s < DEPTH) {
-            // d_{s+1} = C(ft_s, gt_s): its adjoint is complete (stages > s are done)
-            double* T = ((DEPTH - s) & 1) ? Y : X;
-#pragma unroll
-            for (int v = 0; v < NV; ++v) put(T, v, bd[s][v]);
-            __syncthreads();
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                bfx[v] = fma(sc, cxt(sD, T, v), bfx[v]);
-                bgy[v] = fma(sc, cyt(sD, T, v), bgy[v]);
-            }
-        }
-        if (K::w(s, 0) != 0.0) {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) { bf0[v] = fma(K::w(s, 0), bfx[v], bf0[v]); bg0[v] = fma(K::w(s, 0), bgy[v], bg0[v]); }
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (K::w(s, 1 + q) == 0.0) continue;
-            double P[NV], wf[NV], wg[NV], bP[NV] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                double x = u[v];
-#pragma unroll
-                for (int m = 1; m <= s; ++m) x = fma(K::a(q, m), dget(m, v), x);
-                P[v] = x;
-                wf[v] = K::w(s, 1 + q) * bfx[v];
-                wg[v] = K::w(s, 1 + q) * bgy[v];
-            }
-            euler_flux_vjp(a.gamma, P, wf, wg, bP);
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                bu[v] += bP[v];
-#pragma unroll
-                for (int m = 1; m <= s; ++m) bd[m - 1][v] = fma(K::a(q, m), bP[v], bd[m - 1][v]);
-            }
-        }
-    }
-    // d_1 = C(f(u), g(u))
-    {
-        double* T = (DEPTH & 1) ? Y : X;
-#pragma unroll
-        for (int v = 0; v < NV; ++v) put(T, v, bd[0][v]);
+        for (int v = 0; v < NV; ++v) put(X, v, sc * lam[v]);
         __syncthreads();
 #pragma unroll
-        for (int v = 0; v < NV; ++v) { bf0[v] = fma(sc, cxt(sD, T, v), bf0[v]); bg0[v] = fma(sc, cyt(sD, T, v), bg0[v]); }
-    }
-    euler_flux_vjp(a.gamma, u, bf0, bg0, bu);
-    if (active) {
-        double o[NV];
+        for (int v = 0; v < NV; ++v) { bF[v] += cxt(sDh, X, v); bG[v] += cyt(sDh, X, v); }
+
+        // ---- reverse sweep
+        double bd[DEPTH][NV], bu[NV], bf0[NV], bg0[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) o[v] = lam[v] + bu[v] + bud[v];
-        store4(a.lam_out + ((size_t)e * nn + node) * NV, o);
+        for (int v = 0; v < NV; ++v) {
+#pragma unroll
+            for (int m = 0; m < DEPTH; ++m) bd[m][v] = K::tw(m + 1) * bU[v];
+            bu[v] = bU[v];
+            bf0[v] = bF[v];
+            bg0[v] = bG[v];
+        }
+#pragma unroll
+        for (int s = DEPTH; s >= 1; --s) {
+            double bfx[NV], bgy[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { bfx[v] = K::tw(s) * bF[v]; bgy[v] = K::tw(s) * bG[v]; }
+            if (s < DEPTH) {
+                // d_{s+1} = C(ft_s, gt_s): its adjoint is complete (stages > s are done)
+                double* T = ((DEPTH - s) & 1) ? Y : X;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) put(T, v, bd[s][v]);
+                __syncthreads();
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    bfx[v] = fma(sc, cxt(sD, T, v), bfx[v]);
+                    bgy[v] = fma(sc, cyt(sD, T, v), bgy[v]);
+                }
+            }
+            if (K::w(s, 0) != 0.0) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) { bf0[v] = fma(K::w(s, 0), bfx[v], bf0[v]); bg0[v] = fma(K::w(s, 0), bgy[v], bg0[v]); }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                if (K::w(s, 1 + q) == 0.0) continue;
+                double P[NV], wf[NV], wg[NV], bP[NV] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    double x = u[v];
+#pragma unroll
+                    for (int m = 1; m <= s; ++m) x = fma(K::a(q, m), dget(m, v), x);
+                    P[v] = x;
+                    wf[v] = K::w(s, 1 + q) * bfx[v];
+                    wg[v] = K::w(s, 1 + q) * bgy[v];
+                }
+                euler_flux_vjp(a.gamma, P, wf, wg, bP);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    bu[v] += bP[v];
+#pragma unroll
+                    for (int m = 1; m <= s; ++m) bd[m - 1][v] = fma(K::a(q, m), bP[v], bd[m - 1][v]);
+                }
+            }
+        }
+        // d_1 = C(f(u), g(u)); after this barrier the stage buffer is no longer read
+        {
+            double* T = (DEPTH & 1) ? Y : X;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) put(T, v, bd[0][v]);
+            __syncthreads();
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { bf0[v] = fma(sc, cxt(sD, T, v), bf0[v]); bg0[v] = fma(sc, cyt(sD, T, v), bg0[v]); }
+        }
+        euler_flux_vjp(a.gamma, u, bf0, bg0, bu);
+        if (active) {
+            double o[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) o[v] = lam[v] + bu[v] + bud[v];
+            store4(a.lam_out + ((size_t)e * nn + node) * NV, o);
+        }
+    }
+    if (failed && threadIdx.x == 0) {
+        atomicOr(a.status, STATUS_WAIT_TIMEOUT);
+        // the copies still in flight (this tile's, and the next tile's if issued) land before the CTA's shared
+        // memory is released
+        mbar_wait_bounded(&bar[it & 1], (unsigned)((it >> 1) & 1));
+        if ((int)blockIdx.x + (it + 1) * (int)gridDim.x < ntiles)
+            mbar_wait_bounded(&bar[(it + 1) & 1], (unsigned)(((it + 1) >> 1) & 1));
     }
 }
 
@@ -687,6 +711,14 @@ static __global__ void __launch_bounds__(OBJ_THREADS) sum_kernel(const double* p
 }
 
 // ---- launches ---------------------------------------------------------------------------------------
+// SMs of the current device (persistent grids)
+int sm_count() {
+    int d = 0, c = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, d);
+    return c > 0 ? c : 1;
+}
+
 template <int N>
 struct AL {
     static void set_attributes() {
@@ -696,8 +728,8 @@ struct AL {
                              (int)VolCfg<N>::smem_bytes(4));
         cudaFuncSetAttribute(adj_volume_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)AdjCfg<N>::smem_bytes());
-        cudaFuncSetAttribute(adj_volume_reg_kernel<N, AdjCfg<N>::MIN_BLOCKS, false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AdjCfg<N>::reg_smem_bytes());
+        cudaFuncSetAttribute(adj_volume_stored_kernel<N, AdjCfg<N>::MIN_BLOCKS>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AdjCfg<N>::stored_smem_bytes());
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, false, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VolCfg<N>::smem_bytes(4));
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, false, false, true>,
@@ -735,8 +767,13 @@ struct AL {
         if (th) adj_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(sa);
         using C = AdjCfg<N>;
         const int grid = (va.E + C::EB - 1) / C::EB;
-        if (va.dstore) adj_volume_reg_kernel<N, C::MIN_BLOCKS, false><<<grid, C::THREADS, C::reg_smem_bytes(), s>>>(va);
-        else adj_volume_kernel<N><<<grid, C::THREADS, C::smem_bytes(), s>>>(va);
+        if (va.dstore) {
+            // persistent: MIN_BLOCKS CTAs per SM, each over every gridDim-th tile
+            const int persistent = std::min(grid, sm_count() * C::MIN_BLOCKS);
+            adj_volume_stored_kernel<N, C::MIN_BLOCKS><<<persistent, C::THREADS, C::stored_smem_bytes(), s>>>(va);
+        } else {
+            adj_volume_kernel<N><<<grid, C::THREADS, C::smem_bytes(), s>>>(va);
+        }
     }
 };
 
@@ -754,6 +791,18 @@ size_t nstate(const tlw_handle* h) { return (size_t)NV * h->nn * h->E; }
 size_t ntrace(const tlw_handle* h) { return (size_t)NV * h->n * 4 * h->E; }
 // stages of the volume procedure: 3 for N = 3, 4 for N >= 4
 int depth(const tlw_handle* h) { return h->N >= 4 ? 4 : 3; }
+
+// segment buffer b (0 or 1): step j's input state (j = len: the segment's output, or scratch), U traces and
+// stage derivatives
+double* seg_state(tlw_handle* h, int b, int j) {
+    return h->adj.d_seg + ((size_t)b * (h->adj.capacity_states + 1) + j) * nstate(h);
+}
+double* seg_trace(tlw_handle* h, int b, int j) {
+    return h->adj.d_segU + ((size_t)b * h->adj.capacity_states + j) * ntrace(h);
+}
+double* seg_D(tlw_handle* h, int b, int j) {
+    return h->adj.d_segD + ((size_t)b * h->adj.capacity_states + j) * depth(h) * nstate(h);
+}
 
 int adj_ready(tlw_handle* h) {
     if (!h) return TLW_E_ARG;
@@ -788,6 +837,17 @@ int adj_ready(tlw_handle* h) {
         const size_t blocks = ((size_t)h->nn * h->E + OBJ_THREADS - 1) / OBJ_THREADS;
         TLW_ACUDA(h, cudaMalloc(&A.d_work, (blocks + 8) * sizeof(double)));
     }
+    if (!A.s_rec) {
+        // the reverse sweep's two streams: the adjoint chain (the critical path) above the recomputation in
+        // priority
+        int least = 0, greatest = 0;
+        TLW_ACUDA(h, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        TLW_ACUDA(h, cudaStreamCreateWithPriority(&A.s_rec, cudaStreamNonBlocking, least));
+        TLW_ACUDA(h, cudaStreamCreateWithPriority(&A.s_adj, cudaStreamNonBlocking, greatest));
+        for (cudaEvent_t* ev : {&A.ev_fork, &A.ev_join, &A.ev_join2, &A.ev_ready[0], &A.ev_ready[1], &A.ev_free[0],
+                                &A.ev_free[1]})
+            TLW_ACUDA(h, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    }
     return TLW_OK;
 }
 
@@ -815,9 +875,11 @@ int ensure_steps(tlw_handle* h, int nsteps, int ck) {
         dfree(A.d_seg);
         dfree(A.d_segU);
         dfree(A.d_segD);
-        TLW_ACUDA(h, cudaMalloc(&A.d_seg, (size_t)ck * nstate(h) * sizeof(double)));
-        TLW_ACUDA(h, cudaMalloc(&A.d_segU, (size_t)ck * ntrace(h) * sizeof(double)));
-        TLW_ACUDA(h, cudaMalloc(&A.d_segD, (size_t)ck * depth(h) * nstate(h) * sizeof(double)));
+        A.capacity_states = 0;
+        A.last_resident = false;
+        TLW_ACUDA(h, cudaMalloc(&A.d_seg, 2 * (size_t)(ck + 1) * nstate(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_segU, 2 * (size_t)ck * ntrace(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_segD, 2 * (size_t)ck * depth(h) * nstate(h) * sizeof(double)));
         A.capacity_states = ck;
     }
     return TLW_OK;
@@ -869,22 +931,22 @@ SurfArgs fwd_surf_args(tlw_handle* h, const double* u, double* out, const double
     return sa;
 }
 
-// one forward LW step at the dt stored at dtp; U traces into tU
-void enqueue_fixed_step(tlw_handle* h, const double* u, double* unew, double* tU, const double* dtp,
+// one forward LW step on stream s at the dt stored at dtp; U traces into tU, stage derivatives into dstore
+void enqueue_fixed_step(tlw_handle* h, cudaStream_t s, const double* u, double* unew, double* tU, const double* dtp,
                         double* dstore = nullptr) {
     VolArgs va = fwd_vol_args(h, u, unew, tU, dtp);
     va.dstore = dstore;
     const SurfArgs sa = fwd_surf_args(h, u, unew, tU, dtp, 1);
     adj_degree(h->N, [&](auto Nc) {
         constexpr int N = decltype(Nc)::value;
-        AL<N>::forward_volume(h->stream, MODE_STEP, va);
-        AL<N>::forward_interfaces(h->stream, sa, h);
+        AL<N>::forward_volume(s, MODE_STEP, va);
+        AL<N>::forward_interfaces(s, sa, h);
     });
 }
 
 // lam_out = (du_new/du)^T lam_in for the step from u at dt (*dtp); tU = that step's forward U traces
 void enqueue_adjoint_step(tlw_handle* h, const double* u, const double* tU, const double* dtp, const double* lam_in,
-                          double* lam_out, const double* dstore = nullptr) {
+                          double* lam_out, const double* dstore = nullptr, cudaStream_t s = nullptr) {
     AdjointBuffers& A = h->adj;
     AdjSurfArgs sa{};
     sa.u = u;
@@ -914,7 +976,8 @@ void enqueue_adjoint_step(tlw_handle* h, const double* u, const double* tU, cons
     va.E = (int)h->E;
     va.gamma = h->opts.gamma;
     va.dstore = dstore;
-    adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::adjoint(h->stream, sa, va); });
+    va.status = &h->d_step->status;
+    adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::adjoint(s ? s : h->stream, sa, va); });
 }
 
 int adj_status(tlw_handle* h) {
@@ -925,6 +988,8 @@ int adj_status(tlw_handle* h) {
     if (st) {
         const unsigned zero = 0;
         TLW_ACUDA(h, cudaMemcpy(&h->d_step->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+        if (st & STATUS_WAIT_TIMEOUT)
+            return afail(h, TLW_E_CUDA, "adjoint volume kernel: a bounded wait on a bulk copy timed out");
         return afail(h, TLW_E_NONADMISSIBLE, "non-admissible state: square root of a negative number (DomainError)");
     }
     return TLW_OK;
@@ -946,7 +1011,7 @@ int copy_out(tlw_handle* h, double* dst, const double* src, size_t n, int where)
 
 // captures what body() enqueues on the handle's stream into exec (replaced if present)
 template <class F>
-int capture_graph(tlw_handle* h, cudaGraphExec_t& exec, F&& body) {
+int capture_graph(tlw_handle* h, cudaGraphExec_t& exec, F&& body, unsigned long long flags = 0) {
     if (exec) {
         cudaGraphExecDestroy(exec);
         exec = nullptr;
@@ -960,7 +1025,7 @@ int capture_graph(tlw_handle* h, cudaGraphExec_t& exec, F&& body) {
         return rc;
     }
     if (e != cudaSuccess) return afail(h, TLW_E_CUDA, std::string("adjoint graph capture: ") + cudaGetErrorString(e));
-    const cudaError_t e2 = cudaGraphInstantiate(&exec, g, 0);
+    const cudaError_t e2 = cudaGraphInstantiate(&exec, g, flags);
     cudaGraphDestroy(g);
     if (e2 != cudaSuccess) {
         exec = nullptr;
@@ -980,6 +1045,7 @@ int tlw_adjoint_step(tlw_handle* h, double* lam_out, const double* lam_in, const
     if (!lam_out || !lam_in || !u) return afail(h, TLW_E_ARG, "null array");
     AdjointBuffers& A = h->adj;
     if ((rc = ensure_steps(h, 1, 1))) return rc;
+    A.last_resident = false;   // segment buffer 0 is reused here
     const size_t ns = nstate(h);
     // u -> seg[0], lam_in -> lam[0], dt -> dts[0]
     if ((rc = ensure_given_dts(h, 1))) return rc;
@@ -1001,13 +1067,14 @@ int tlw_solve_dts(tlw_handle* h, const double* u0, int32_t nsteps, const double*
     // dt array of nsteps, one trace buffer; no checkpoints
     if ((rc = ensure_steps(h, 1, 1))) return rc;
     AdjointBuffers& A = h->adj;
+    A.last_resident = false;   // segment buffer 0's first trace is reused here
     if ((rc = ensure_given_dts(h, nsteps))) return rc;
     const size_t ns = nstate(h);
     if ((rc = copy_in(h, A.d_lam[0], u0, ns, where))) return rc;
     if (nsteps) TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts_given, dts, nsteps * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     int cur = 0;
     for (int k = 0; k < nsteps; ++k) {
-        enqueue_fixed_step(h, A.d_lam[cur], A.d_lam[1 - cur], A.d_segU, A.d_dts_given + k);
+        enqueue_fixed_step(h, h->stream, A.d_lam[cur], A.d_lam[1 - cur], A.d_segU, A.d_dts_given + k);
         cur ^= 1;
     }
     if ((rc = copy_out(h, uT_out, A.d_lam[cur], ns, where))) return rc;
@@ -1023,29 +1090,42 @@ int tlw_forward_record(tlw_handle* h, const double* u0, int32_t nsteps, double c
     if ((rc = ensure_steps(h, nsteps, ck))) return rc;
     AdjointBuffers& A = h->adj;
     A.rec_steps = 0;
+    A.last_resident = false;
     const size_t ns = nstate(h);
-    // CFL dt recorded per step, checkpoints every ck steps; runs in the handle's two state buffers
+    const int nseg = (nsteps + ck - 1) / ck;
+    const int last = (nseg - 1) * ck, bl = (nseg - 1) & 1;
+    // CFL dt recorded per step, checkpoints every ck steps; runs in the handle's two state buffers, except the
+    // last segment, whose states, U traces and stage derivatives go straight into its segment buffer (the
+    // reverse sweep starts there without recomputing it)
     StepState st{};
     st.t = 0.0;
     st.t_end = INFINITY;
     st.cfl = cfl;
     TLW_ACUDA(h, cudaMemcpyAsync(h->d_step, &st, sizeof(st), cudaMemcpyHostToDevice, h->stream));
-    if ((rc = copy_in(h, h->d_state[0], u0, ns, where))) return rc;
+    if ((rc = copy_in(h, last == 0 ? seg_state(h, bl, 0) : h->d_state[0], u0, ns, where))) return rc;
     h->slots_valid = false;   // the handle's state buffers are reused here
     // the whole sweep is one CUDA graph, captured once per (nsteps, checkpoint interval, buffers)
     auto body = [&]() -> int {
         double* s0 = h->d_state[0];
         double* s1 = h->d_state[1];
         for (int k = 0; k < nsteps; ++k) {
+            const bool in_last = k >= last;
+            const int j = k - last;
+            double* u = in_last ? seg_state(h, bl, j) : s0;
             if (k % ck == 0)
-                TLW_ACUDA(h, cudaMemcpyAsync(A.d_ckpt + (size_t)(k / ck) * ns, s0, ns * sizeof(double),
+                TLW_ACUDA(h, cudaMemcpyAsync(A.d_ckpt + (size_t)(k / ck) * ns, u, ns * sizeof(double),
                                              cudaMemcpyDeviceToDevice, h->stream));
-            adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::speed(h->stream, h, s0); });
+            adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::speed(h->stream, h, u); });
             finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
             TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts + k, &h->d_step->dt, sizeof(double), cudaMemcpyDeviceToDevice,
                                          h->stream));
-            enqueue_fixed_step(h, s0, s1, h->d_tU, A.d_dts + k);
-            std::swap(s0, s1);
+            if (in_last) {
+                enqueue_fixed_step(h, h->stream, u, seg_state(h, bl, j + 1), seg_trace(h, bl, j), A.d_dts + k,
+                                   seg_D(h, bl, j));
+            } else {
+                enqueue_fixed_step(h, h->stream, s0, k + 1 == last ? seg_state(h, bl, 0) : s1, h->d_tU, A.d_dts + k);
+                std::swap(s0, s1);
+            }
         }
         return TLW_OK;
     };
@@ -1055,12 +1135,12 @@ int tlw_forward_record(tlw_handle* h, const double* u0, int32_t nsteps, double c
         A.g_fwd_key = key;
     }
     TLW_ACUDA(h, cudaGraphLaunch(A.g_fwd, h->stream));
-    A.d_final = h->d_state[nsteps % 2];
-    double* s0 = A.d_final;
-    if (uT_out && (rc = copy_out(h, uT_out, s0, ns, where))) return rc;
+    A.d_final = seg_state(h, bl, nsteps - last);
+    if (uT_out && (rc = copy_out(h, uT_out, A.d_final, ns, where))) return rc;
     if ((rc = adj_status(h))) return rc;
     A.rec_steps = nsteps;
     A.rec_ck = ck;
+    A.last_resident = true;
     return TLW_OK;
 }
 
@@ -1071,78 +1151,121 @@ namespace {
 int reverse_sweep_enqueue(tlw_handle* h, int& cur, double* phase_ms);
 
 int reverse_sweep(tlw_handle* h, int& cur, double* phase_ms) {
-    if (phase_ms) return reverse_sweep_enqueue(h, cur, phase_ms);
     AdjointBuffers& A = h->adj;
-    const long long key = (long long)A.rec_steps * 100003 + A.rec_ck;
-    if (cur != 0) return afail(h, TLW_E_ARG, "internal: sweep start buffer");
-    if (!A.g_rev || A.g_rev_key != key) {
-        int c = 0;
-        int rc = capture_graph(h, A.g_rev, [&]() { return reverse_sweep_enqueue(h, c, nullptr); });
-        if (rc) return rc;
-        A.g_rev_key = key;
+    const int nseg = (A.rec_steps + A.rec_ck - 1) / A.rec_ck;
+    int rc = TLW_OK;
+    if (phase_ms) {
+        rc = reverse_sweep_enqueue(h, cur, phase_ms);
+    } else {
+        const long long key = ((long long)A.rec_steps * 100003 + A.rec_ck) * 2 + (A.last_resident ? 1 : 0);
+        if (cur != 0) return afail(h, TLW_E_ARG, "internal: sweep start buffer");
+        if (!A.g_rev || A.g_rev_key != key) {
+            int c = 0;
+            // the kernels keep the priorities of the streams they were captured from
+            rc = capture_graph(h, A.g_rev, [&]() { return reverse_sweep_enqueue(h, c, nullptr); },
+                               cudaGraphInstantiateFlagUseNodePriority);
+            if (rc) return rc;
+            A.g_rev_key = key;
+        }
+        TLW_ACUDA(h, cudaGraphLaunch(A.g_rev, h->stream));
+        cur = A.rec_steps % 2;
     }
-    TLW_ACUDA(h, cudaGraphLaunch(A.g_rev, h->stream));
-    cur = A.rec_steps % 2;
-    return TLW_OK;
+    // with three or more segments the sweep has reused the last segment's buffer
+    if (nseg > 2) A.last_resident = false;
+    return rc;
 }
 
+// The segments from last to first: segment k's states, U traces and stage derivatives are recomputed from
+// its checkpoint into buffer k & 1, then its adjoint steps run backwards over them. Without phase timing the
+// recomputations run on their own stream (s_rec), one segment ahead of the adjoint chain (s_adj, highest
+// priority), both forked from and joined back into the handle's stream: "ready" events order each segment's
+// adjoint after its recompute and "free" events each buffer's reuse after the adjoint that read it. With phase
+// timing everything runs in the same order on the handle's stream.
 int reverse_sweep_enqueue(tlw_handle* h, int& cur, double* phase_ms) {
     AdjointBuffers& A = h->adj;
-    const size_t ns = nstate(h), nt = ntrace(h);
     const int nsteps = A.rec_steps, ck = A.rec_ck;
     const int nseg = (nsteps + ck - 1) / ck;
+    const bool overlap = phase_ms == nullptr;
+    const bool resident = A.last_resident;
+    cudaStream_t sa = overlap ? A.s_adj : h->stream, sr = overlap ? A.s_rec : h->stream;
     cudaEvent_t ev[2] = {};
-    if (phase_ms)
+    if (!overlap)
         for (auto& x : ev) TLW_ACUDA(h, cudaEventCreate(&x));
     float rec_ms = 0.0f, adj_ms = 0.0f;
-    for (int sgi = nseg - 1; sgi >= 0; --sgi) {
-        const int start = sgi * ck;
-        const int len = std::min(ck, nsteps - start);
-        if (phase_ms) cudaEventRecord(ev[0], h->stream);
-        // recompute the segment's states and U traces from its checkpoint
-        TLW_ACUDA(h, cudaMemcpyAsync(A.d_seg, A.d_ckpt + (size_t)sgi * ns, ns * sizeof(double),
-                                     cudaMemcpyDeviceToDevice, h->stream));
-        // each recomputed step also stores its stage derivatives, which its adjoint step reads back
-        const size_t nd = (size_t)depth(h) * ns;
-        for (int j = 0; j < len; ++j) {
-            if (j + 1 < len) {
-                enqueue_fixed_step(h, A.d_seg + (size_t)j * ns, A.d_seg + (size_t)(j + 1) * ns,
-                                   A.d_segU + (size_t)j * nt, A.d_dts + start + j, A.d_segD + (size_t)j * nd);
-            } else {
-                // the segment's last output state is not needed, only the U traces of its step (volume
-                // kernel alone, its du into the free adjoint buffer)
-                VolArgs va = fwd_vol_args(h, A.d_seg + (size_t)j * ns, A.d_lam[1 - cur], A.d_segU + (size_t)j * nt,
-                                          A.d_dts + start + j);
-                va.dstore = A.d_segD + (size_t)j * nd;
-                adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::forward_volume(h->stream, MODE_RHS, va); });
+    auto timed = [&](float& acc, auto&& enqueue) -> int {
+        if (overlap) return enqueue();
+        cudaEventRecord(ev[0], sa);
+        const int rc = enqueue();
+        cudaEventRecord(ev[1], sa);
+        TLW_ACUDA(h, cudaEventSynchronize(ev[1]));
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev[0], ev[1]);
+        acc += ms;
+        return rc;
+    };
+    bool used[2] = {false, false};
+    auto recompute = [&](int sgi) -> int {
+        if (resident && sgi == nseg - 1) return TLW_OK;
+        const int b = sgi & 1, start = sgi * ck, len = std::min(ck, nsteps - start);
+        return timed(rec_ms, [&]() -> int {
+            if (overlap && used[b]) TLW_ACUDA(h, cudaStreamWaitEvent(sr, A.ev_free[b], 0));
+            TLW_ACUDA(h, cudaMemcpyAsync(seg_state(h, b, 0), A.d_ckpt + (size_t)sgi * nstate(h),
+                                         nstate(h) * sizeof(double), cudaMemcpyDeviceToDevice, sr));
+            for (int j = 0; j < len; ++j) {
+                if (j + 1 < len) {
+                    enqueue_fixed_step(h, sr, seg_state(h, b, j), seg_state(h, b, j + 1), seg_trace(h, b, j),
+                                       A.d_dts + start + j, seg_D(h, b, j));
+                } else {
+                    // the segment's output state is not needed, only the U traces and stage derivatives of its
+                    // last step (volume kernel alone, its du into the free state slot)
+                    VolArgs va = fwd_vol_args(h, seg_state(h, b, j), seg_state(h, b, len), seg_trace(h, b, j),
+                                              A.d_dts + start + j);
+                    va.dstore = seg_D(h, b, j);
+                    adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::forward_volume(sr, MODE_RHS, va); });
+                }
             }
-        }
-        if (phase_ms) {
-            cudaEventRecord(ev[1], h->stream);
-            TLW_ACUDA(h, cudaEventSynchronize(ev[1]));
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, ev[0], ev[1]);
-            rec_ms += ms;
-        }
-        for (int j = len - 1; j >= 0; --j) {
-            enqueue_adjoint_step(h, A.d_seg + (size_t)j * ns, A.d_segU + (size_t)j * nt, A.d_dts + start + j,
-                                 A.d_lam[cur], A.d_lam[1 - cur], A.d_segD + (size_t)j * nd);
-            cur ^= 1;
-        }
-        if (phase_ms) {
-            cudaEventRecord(ev[0], h->stream);
-            TLW_ACUDA(h, cudaEventSynchronize(ev[0]));
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, ev[1], ev[0]);
-            adj_ms += ms;
-        }
+            if (overlap) TLW_ACUDA(h, cudaEventRecord(A.ev_ready[b], sr));
+            return TLW_OK;
+        });
+    };
+    auto adjoint = [&](int sgi) -> int {
+        const int b = sgi & 1, start = sgi * ck, len = std::min(ck, nsteps - start);
+        return timed(adj_ms, [&]() -> int {
+            if (overlap && !(resident && sgi == nseg - 1)) TLW_ACUDA(h, cudaStreamWaitEvent(sa, A.ev_ready[b], 0));
+            for (int j = len - 1; j >= 0; --j) {
+                enqueue_adjoint_step(h, seg_state(h, b, j), seg_trace(h, b, j), A.d_dts + start + j, A.d_lam[cur],
+                                     A.d_lam[1 - cur], seg_D(h, b, j), sa);
+                cur ^= 1;
+            }
+            if (overlap) TLW_ACUDA(h, cudaEventRecord(A.ev_free[b], sa));
+            used[b] = true;
+            return TLW_OK;
+        });
+    };
+    int rc = TLW_OK;
+    if (overlap) {
+        TLW_ACUDA(h, cudaEventRecord(A.ev_fork, h->stream));
+        TLW_ACUDA(h, cudaStreamWaitEvent(sr, A.ev_fork, 0));
+        TLW_ACUDA(h, cudaStreamWaitEvent(sa, A.ev_fork, 0));
     }
-    if (phase_ms) {
+    rc = recompute(nseg - 1);
+    for (int k = nseg - 1; k >= 0 && !rc; --k) {
+        if (k >= 1) rc = recompute(k - 1);
+        if (!rc) rc = adjoint(k);
+    }
+    if (overlap) {
+        // both streams rejoin the handle's stream
+        TLW_ACUDA(h, cudaEventRecord(A.ev_join, sr));
+        TLW_ACUDA(h, cudaEventRecord(A.ev_join2, sa));
+        TLW_ACUDA(h, cudaStreamWaitEvent(h->stream, A.ev_join, 0));
+        TLW_ACUDA(h, cudaStreamWaitEvent(h->stream, A.ev_join2, 0));
+    }
+    if (!overlap) {
         phase_ms[0] = rec_ms;
         phase_ms[1] = adj_ms;
         for (auto& x : ev) cudaEventDestroy(x);
     }
-    return TLW_OK;
+    return rc;
 }
 
 }  // namespace

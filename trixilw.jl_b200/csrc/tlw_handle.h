@@ -30,9 +30,16 @@ struct AdjointBuffers {
     int capacity_given = 0;
     double* d_ckpt = nullptr;               // checkpoint states
     int capacity_ckpt = 0;
-    double* d_seg = nullptr;                // recomputed states of one segment
-    double* d_segU = nullptr;               // time-averaged U traces of one segment
-    double* d_segD = nullptr;               // stage derivatives d_1..d_depth of every step of one segment
+    // two segment buffers (one is recomputed while the reverse sweep reads the other), each of
+    // capacity_states steps: the step input states (+1 slot: u(T), or scratch), U traces, stage derivatives
+    double* d_seg = nullptr;                // [2][capacity_states + 1] states
+    double* d_segU = nullptr;               // [2][capacity_states] time-averaged U traces
+    double* d_segD = nullptr;               // [2][capacity_states][depth] stage derivatives d_1..d_depth
+    bool last_resident = false;             // the recorded run's last segment is in its buffer (no recompute)
+    cudaStream_t s_rec = nullptr;           // reverse sweep: recompute stream (lowest priority)
+    cudaStream_t s_adj = nullptr;           // reverse sweep: adjoint chain (highest priority)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
+    cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
     double* d_work = nullptr;               // scratch (objective partial sums)
     double* d_final = nullptr;              // u(T) of the recorded run (one of the handle's state buffers)
     int rec_steps = 0, rec_ck = 0;          // recorded forward run: steps, checkpoint interval
@@ -48,6 +55,10 @@ inline void free_adjoint(AdjointBuffers& a) {
     if (a.g_rev) cudaGraphExecDestroy(a.g_rev);
     dfree(a.d_lam[0]); dfree(a.d_lam[1]); dfree(a.d_bF); dfree(a.d_bU); dfree(a.d_bu); dfree(a.d_dts);
     dfree(a.d_dts_given); dfree(a.d_ckpt); dfree(a.d_seg); dfree(a.d_segU); dfree(a.d_segD); dfree(a.d_work);
+    for (cudaEvent_t ev : {a.ev_fork, a.ev_join, a.ev_join2, a.ev_ready[0], a.ev_ready[1], a.ev_free[0], a.ev_free[1]})
+        if (ev) cudaEventDestroy(ev);
+    if (a.s_rec) cudaStreamDestroy(a.s_rec);
+    if (a.s_adj) cudaStreamDestroy(a.s_adj);
     a = AdjointBuffers{};
 }
 

@@ -86,7 +86,7 @@ struct VolArgs {
     // temporal error estimate of the Adaptive step control (lw_volume_kernel_4!'s u_np1 / u_np1_low tail)
     double* temporal_errors;          // [e]
     double abstol, reltol;
-    double* dstore;                   // [m][e][node][v]: the stage derivatives d_1..d_depth (DSTORE kernels)
+    double* dstore;                   // [m][e][v][node]: the stage derivatives d_1..d_depth (DSTORE kernels)
 };
 
 // curvilinear: contravariant fluxes f~ = Ja^1_1 f + Ja^1_2 g, g~ = Ja^2_1 f + Ja^2_2 g of a node
@@ -288,7 +288,16 @@ __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, 
 //   depth 2: f_t = raw1/2,  f_tt = raw2;    depth 1: f_t = raw1/2
 // ------------------------------------------------------------------------------------------------
 // DSTORE: also write each stage derivative d_m (dt-scaled time derivative of u) to a.dstore, for the discrete
-// adjoint's reverse sweep, which then reads them instead of recomputing them
+// adjoint's reverse sweep, which then reads them instead of recomputing them. Layout [m][e][v][node]: one
+// element's d_m is contiguous (a bulk copy per tile of elements) with the nodes innermost (conflict-free
+// shared-memory reads, one thread per node).
+template <int nn>
+__device__ __forceinline__ void store_stage_derivative(const VolArgs& a, int m, long long e, int node, const double* d) {
+    double* p = a.dstore + ((size_t)(m - 1) * a.E + e) * NV * nn + node;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) p[v * nn] = d[v];
+}
+
 template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false>
 static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
     static_assert(!(SC && CURVED), "shock capturing is built for TreeMesh only");
@@ -378,7 +387,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
             um[v] -= d[v];
             if (DEPTH >= 3) { upp[v] = fma(2.0, d[v], upp[v]); umm[v] = fma(-2.0, d[v], umm[v]); }
         }
-        if (DSTORE) store4(a.dstore + ((size_t)(1 - 1) * a.E * nn + (size_t)e * nn + node) * NV, d);
+        if (DSTORE) store_stage_derivative<nn>(a, 1, e, node, d);
         if (DEPTH >= 3) {
             // raw1 = -f(u+2ut) + 8 f(u+ut) - 8 f(u-ut) + f(u-2ut)
             euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
@@ -424,7 +433,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
                 um[v] = fma(0.5, d[v], um[v]);
                 if (DEPTH >= 3) { upp[v] = fma(2.0, d[v], upp[v]); umm[v] = fma(2.0, d[v], umm[v]); }
             }
-            if (DSTORE) store4(a.dstore + ((size_t)(2 - 1) * a.E * nn + (size_t)e * nn + node) * NV, d);
+            if (DSTORE) store_stage_derivative<nn>(a, 2, e, node, d);
             if (DEPTH == 4) {
                 // raw2 = -f(upp) + 16 f(up) - 30 f0 + 16 f(um) - f(umm)
                 euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
@@ -477,7 +486,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
                 umm[v] = fma(-4.0 / 3.0, d[v], umm[v]);
                 upp[v] = fma(4.0 / 3.0, d[v], upp[v]);
             }
-            if (DSTORE) store4(a.dstore + ((size_t)(3 - 1) * a.E * nn + (size_t)e * nn + node) * NV, d);
+            if (DSTORE) store_stage_derivative<nn>(a, 3, e, node, d);
             // raw3 = f(upp) - 2 f(up) + 2 f(um) - f(umm)
             euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
 #pragma unroll
@@ -518,7 +527,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
                 umm[v] = fma(2.0 / 3.0, d[v], umm[v]);
                 upp[v] = fma(2.0 / 3.0, d[v], upp[v]);
             }
-            if (DSTORE) store4(a.dstore + ((size_t)(4 - 1) * a.E * nn + (size_t)e * nn + node) * NV, d);
+            if (DSTORE) store_stage_derivative<nn>(a, 4, e, node, d);
             // raw4 = f(upp) - 4 f(up) + 6 f0 - 4 f(um) + f(umm)
             euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
 #pragma unroll
