@@ -900,9 +900,9 @@ def run_adjoint(args):
     J = ctypes.c_double()
     ph = (ctypes.c_double * 3)()
 
-    def gradient(timing=False):
-        _lib.check(semi.handle, L.tlw_adjoint_solve(semi.handle, vp(d_u0), nsteps, cfl, ck, vp(d_target), vp(d_grad),
-                                                    ctypes.byref(J), vp(d_uT), _lib.TLW_WHERE_DEVICE,
+    def gradient(timing=False, every=ck):
+        _lib.check(semi.handle, L.tlw_adjoint_solve(semi.handle, vp(d_u0), nsteps, cfl, every, vp(d_target),
+                                                    vp(d_grad), ctypes.byref(J), vp(d_uT), _lib.TLW_WHERE_DEVICE,
                                                     ph if timing else None))
 
     def forward():
@@ -934,6 +934,18 @@ def run_adjoint(args):
     grad_ms = ev[2].elapsed_time(ev[3]) / reps
     gradient(timing=True)
     phases = tuple(ph)
+    g_ck = d_grad.clone()
+    # the same gradient with every step's data kept from the record pass (one segment: no recomputation)
+    for _ in range(2):
+        gradient(every=nsteps)
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for _ in range(reps):
+        gradient(every=nsteps)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    all_ms = ev[0].elapsed_time(ev[1]) / reps
+    all_equal = bool(torch.equal(d_grad, g_ck))
     clocks = sampler.stop()
     # e2e through the public API with host arrays
     e0 = time.perf_counter()
@@ -966,13 +978,24 @@ def run_adjoint(args):
                        "objective": "J = 1/2 sum over nodes (rho(T) - rho_target)^2, rho_target from a strength-4.5 run",
                        "u0": "strength-5 vortex + N(0, 1e-3^2) noise (seed 0)", "repeats": reps},
             "forward_solve_ms": fwd_ms, "gradient_ms": grad_ms, "gradient_cost_vs_forward": grad_ms / fwd_ms,
-            "phase_ms": {"forward_record": phases[0], "recompute": phases[1], "adjoint_steps": phases[2]},
-            "backward_cost_vs_forward": (phases[1] + phases[2]) / fwd_ms,
+            # phases timed one after another on one stream; the timed gradient overlaps the recomputation
+            # with the adjoint steps
+            "phase_ms": {"forward_record": phases[0], "recompute": phases[1], "adjoint_steps": phases[2],
+                         "serial": True},
+            "backward_cost_vs_forward": (grad_ms - phases[0]) / fwd_ms,
+            "store_all": {"checkpoint_every": nsteps, "gradient_ms": all_ms, "gradient_cost_vs_forward": all_ms / fwd_ms,
+                          # per step: the input state (4 values a node), U traces (16 / (N + 1) a node) and
+                          # stage derivatives (4 * depth a node), plus u(T)
+                          "device_bytes": int(8 * ndofs * (nsteps * (4 + 16 / (N + 1) + 4 * (4 if N >= 4 else 3)) + 4)),
+                          "gradient_bit_equal": all_equal},
             "J": Jh, "fd_check": {"directions": args.fd_directions, "h": h, "max_rel_err": worst, "richardson": True},
             "e2e": {"value": ndofs * nsteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * 5 * ndofs / nsteps,
                     "d2h_bytes_per_step": 8 * 8 * ndofs / nsteps, "seconds": e2e_s},
             "clocks": clocks,
-            "gpu_launches": reps * nsteps * (2 + 4 + 2),
+            # per gradient: record 5 a step (speed, dt, volume, 2 interface sweeps), objective 2, recompute 3 a
+            # step (the last segment comes from the record, each segment's last step is a volume launch only),
+            # adjoint 2 a step
+            "gpu_launches": reps * (5 * nsteps + 2 + 3 * (nsteps - ck) - 2 * ((nsteps - 1) // ck) + 2 * nsteps),
         }
         print(json.dumps(out), flush=True)
 

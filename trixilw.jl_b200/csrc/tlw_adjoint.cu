@@ -225,11 +225,8 @@ struct AdjCfg {
     // shared memory: D, Dhat, the two contraction tiles X, Y, the stage derivatives d_m and their adjoints
     static constexpr int TILE = NV * EB * nn;
     static constexpr size_t smem_bytes() { return (size_t)(2 * nn + (2 + 2 * DEPTH) * TILE) * sizeof(double); }
-    // adj_volume_stored_kernel: D, Dhat, X, Y, two stage buffers (u, lam, d_1..d_DEPTH) and their two mbarriers
-    static constexpr int STAGE = (2 + DEPTH) * TILE;
-    static constexpr size_t stored_smem_bytes() {
-        return (size_t)(2 * nn + 2 * TILE + 2 * STAGE) * sizeof(double) + 2 * sizeof(uint64_t);
-    }
+    // adj_volume_reg_kernel: D, Dhat, X, Y and the d_m (their adjoints are in registers)
+    static constexpr size_t reg_smem_bytes() { return (size_t)(2 * nn + (2 + DEPTH) * TILE) * sizeof(double); }
 };
 
 struct AdjVolArgs {
@@ -244,7 +241,6 @@ struct AdjVolArgs {
     int E;
     double gamma;
     const double* dstore;   // the step's stage derivatives d_1..d_depth [m][e][v][node], from the recompute
-    unsigned* status;       // STATUS_WAIT_TIMEOUT
 };
 
 template <int N>
@@ -466,59 +462,74 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
     }
 }
 
-// The adjoint volume step with the stage derivatives the segment recompute stored (lw_volume_kernel<...,
-// DSTORE>): a persistent kernel over tiles of EB elements whose state u, adjoint lam and d_1..d_DEPTH arrive by
-// bulk asynchronous copies into one of two shared-memory stage buffers, the next tile's copies in flight while
-// the current tile is processed. The bar d_m accumulate in registers (each thread owns its node's), so only
-// the transposed contractions go through shared memory: one tile per stage, alternating between X and Y so that
-// one barrier a stage separates a tile's reads from its next writes. Each wait on a copy is bounded: on
-// timeout the kernel flags STATUS_WAIT_TIMEOUT, waits (bounded) for its copies in flight and returns.
-template <int N, int MINB>
-static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_stored_kernel(AdjVolArgs a) {
+// adj_volume_kernel with the stage derivatives stored by the segment recompute, held in registers with their
+// adjoints: each thread reads and accumulates only its own node's d_m and bar d_m, so only the transposed
+// contractions go through shared memory (one tile per stage, alternating between X and Y so that one barrier a
+// stage separates a tile's reads from its next writes). Same operations in the same order as the LOADD kernel.
+// DREG: the d_m in registers too; otherwise in shared memory, where each thread reads back only what it wrote.
+template <int N, int MINB, bool DREG = false>
+static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_reg_kernel(AdjVolArgs a) {
     using C = AdjCfg<N>;
     using K = LWC<C::DEPTH>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB, DEPTH = C::DEPTH, TILE = C::TILE;
-    constexpr int STAGE = C::STAGE;   // one stage buffer: u, lam ([slot][node][v]), d_1..d_DEPTH ([m][slot][v][node])
-    extern __shared__ __align__(16) double sm[];
+    extern __shared__ double sm[];
     double* sD = sm;
     double* sDh = sm + nn;
     double* X = sm + 2 * nn;
     double* Y = X + TILE;
-    double* buf = Y + TILE;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(buf + 2 * STAGE);
+    double* Dt = Y + TILE;   // d_m at Dt + (m - 1) * TILE (!DREG)
     for (int k = threadIdx.x; k < nn; k += blockDim.x) {
         sD[k] = c_tlw_D[N][k];
         sDh[k] = c_tlw_Dhat[N][k];
     }
-    if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    const int ntiles = (a.E + EB - 1) / EB;
-    // thread 0: the copies of one tile into stage buffer b
-    auto issue = [&](int tile, int b) {
-        const long long e0 = (long long)tile * EB;
-        const int ne = (int)min((long long)EB, (long long)a.E - e0);
-        const unsigned bytes = (unsigned)(ne * nn * NV * sizeof(double));
-        double* B = buf + b * STAGE;
-        mbar_arrive_expect_tx(&bar[b], (2 + DEPTH) * bytes);
-        bulk_copy_g2s(B, a.u + e0 * nn * NV, bytes, &bar[b]);
-        bulk_copy_g2s(B + TILE, a.lam + e0 * nn * NV, bytes, &bar[b]);
-#pragma unroll
-        for (int m = 0; m < DEPTH; ++m)
-            bulk_copy_g2s(B + (2 + m) * TILE, a.dstore + ((size_t)m * a.E + e0) * nn * NV, bytes, &bar[b]);
-    };
     const int el = threadIdx.x / nn;
     const int node = threadIdx.x - el * nn;
     const int i = node % n, j = node / n;
+    const long long e = (long long)blockIdx.x * EB + el;
+    const bool active = el < EB && e < a.E;
     const bool in_tile = el < EB;
     const int slot = in_tile ? el : 0;
     const int me = slot * nn + node;
     auto put = [&](double* T, int v, double x) {
         if (in_tile) T[v * EB * nn + me] = x;
     };
+    double u[NV] = {1.0, 0.0, 0.0, 2.5};
+    double ij = 1.0;
+    double dm[DREG ? DEPTH : 1][NV];
+#pragma unroll
+    for (int m = 0; m < (DREG ? DEPTH : 1); ++m)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) dm[m][v] = 0.0;
+    double lam[NV] = {0.0, 0.0, 0.0, 0.0};
+    if (active) {
+        load4(a.u + ((size_t)e * nn + node) * NV, u);
+        ij = __ldg(a.inv_jac + e);
+        if (DREG) {
+#pragma unroll
+            for (int m = 0; m < DEPTH; ++m)
+                for (int v = 0; v < NV; ++v) dm[DREG ? m : 0][v] = a.dstore[((size_t)m * a.E + e) * NV * nn + v * nn + node];
+        }
+        load4(a.lam + ((size_t)e * nn + node) * NV, lam);
+    }
+    if (!DREG) {
+#pragma unroll
+        for (int m = 0; m < DEPTH; ++m) {
+            double d[NV] = {0.0, 0.0, 0.0, 0.0};
+            if (active) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) d[v] = a.dstore[((size_t)m * a.E + e) * NV * nn + v * nn + node];
+            }
+#pragma unroll
+            for (int v = 0; v < NV; ++v) put(Dt + m * TILE, v, d[v]);
+        }
+    }
+    // d_m of this node, m = 1..DEPTH (a thread outside the tile reads zeros)
+    auto dget = [&](int m, int v) -> double {
+        if (DREG) return dm[DREG ? m - 1 : 0][v];
+        return in_tile ? Dt[(m - 1) * TILE + v * EB * nn + me] : 0.0;
+    };
+    const double dt = *a.dt;
+    const double sc = -dt * ij;
     auto cxt = [&](const double* M, const double* W, int v) {
         const double* p = W + v * EB * nn + slot * nn + n * j;
         double s = 0.0;
@@ -533,146 +544,102 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_st
         for (int k = 0; k < n; ++k) s = fma(M[k * n + j], p[n * k], s);
         return s;
     };
-    const double dt = *a.dt;
-    // the it-th tile of this CTA is in buffer it & 1, that buffer's (it >> 1)-th phase
-    if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
-    bool failed = false;
-    int it = 0;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-        const int b = it & 1;
-        const int next = tile + (int)gridDim.x;
-        // buffer b ^ 1 was last read before the previous tile's final barrier
-        if (threadIdx.x == 0 && next < ntiles) issue(next, b ^ 1);
-        const long long e = (long long)tile * EB + el;
-        const bool active = in_tile && e < a.E;
-        // face-trace adjoints (plain loads, issued before the wait)
-        double bF[NV] = {0.0, 0.0, 0.0, 0.0}, bG[NV] = {0.0, 0.0, 0.0, 0.0}, bU[NV] = {0.0, 0.0, 0.0, 0.0};
-        double bud[NV] = {0.0, 0.0, 0.0, 0.0};
-        if (active) {
-            auto face = [&](int f, int l, double* tgt) {
-                const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
-                double x[NV];
-                load4(a.bF + t, x);
+
+    // ---- adjoint inputs: volume term u_new += sc (Dhat F + Dhat G), then the face traces
+    double bF[NV], bG[NV], bU[NV] = {0.0, 0.0, 0.0, 0.0}, bud[NV] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-                for (int v = 0; v < NV; ++v) tgt[v] += x[v];
-                load4(a.bU + t, x);
+    for (int v = 0; v < NV; ++v) put(X, v, sc * lam[v]);
+    __syncthreads();
 #pragma unroll
-                for (int v = 0; v < NV; ++v) bU[v] += x[v];
-                load4(a.bu + t, x);
+    for (int v = 0; v < NV; ++v) { bF[v] = cxt(sDh, X, v); bG[v] = cyt(sDh, X, v); }
+    if (active) {
+        auto face = [&](int f, int l, double* tgt) {
+            const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
+            double x[NV];
+            load4(a.bF + t, x);
 #pragma unroll
-                for (int v = 0; v < NV; ++v) bud[v] += x[v];
-            };
-            if (i == 0) face(0, j, bF);
-            if (i == n - 1) face(1, j, bF);
-            if (j == 0) face(2, i, bG);
-            if (j == n - 1) face(3, i, bG);
-        }
-        const double ij = active ? __ldg(a.inv_jac + e) : 1.0;
-        // (the barrier also orders the previous tile's last reads of X / Y before this tile's first writes)
-        const bool ok = mbar_wait_bounded(&bar[b], (unsigned)((it >> 1) & 1));
-        if (__syncthreads_or(!ok)) {
-            failed = true;
-            break;
-        }
-        const double* B = buf + b * STAGE;
-        double u[NV] = {1.0, 0.0, 0.0, 2.5}, lam[NV] = {0.0, 0.0, 0.0, 0.0};
-        if (active) {
+            for (int v = 0; v < NV; ++v) tgt[v] += x[v];
+            load4(a.bU + t, x);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                u[v] = B[me * NV + v];
-                lam[v] = B[TILE + me * NV + v];
-            }
-        }
-        // d_m of this node, m = 1..DEPTH (zeros outside the mesh)
-        auto dget = [&](int m, int v) -> double {
-            return active ? B[(1 + m) * TILE + (slot * NV + v) * nn + node] : 0.0;
+            for (int v = 0; v < NV; ++v) bU[v] += x[v];
+            load4(a.bu + t, x);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) bud[v] += x[v];
         };
-        const double sc = -dt * ij;
+        if (i == 0) face(0, j, bF);
+        if (i == n - 1) face(1, j, bF);
+        if (j == 0) face(2, i, bG);
+        if (j == n - 1) face(3, i, bG);
+    }
 
-        // ---- adjoint inputs: volume term u_new += sc (Dhat F + Dhat G), then the face traces
+    // ---- reverse sweep
+    double bd[DEPTH][NV], bu[NV], bf0[NV], bg0[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) put(X, v, sc * lam[v]);
-        __syncthreads();
+    for (int v = 0; v < NV; ++v) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) { bF[v] += cxt(sDh, X, v); bG[v] += cyt(sDh, X, v); }
-
-        // ---- reverse sweep
-        double bd[DEPTH][NV], bu[NV], bf0[NV], bg0[NV];
+        for (int m = 0; m < DEPTH; ++m) bd[m][v] = K::tw(m + 1) * bU[v];
+        bu[v] = bU[v];
+        bf0[v] = bF[v];
+        bg0[v] = bG[v];
+    }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
+    for (int s = DEPTH; s >= 1; --s) {
+        double bfx[NV], bgy[NV];
 #pragma unroll
-            for (int m = 0; m < DEPTH; ++m) bd[m][v] = K::tw(m + 1) * bU[v];
-            bu[v] = bU[v];
-            bf0[v] = bF[v];
-            bg0[v] = bG[v];
-        }
+        for (int v = 0; v < NV; ++v) { bfx[v] = K::tw(s) * bF[v]; bgy[v] = K::tw(s) * bG[v]; }
+        if (s < DEPTH) {
+            // d_{s+1} = C(ft_s, gt_s): its adjoint is complete (stages > s are done)
+            double* T = ((DEPTH - s) & 1) ? Y : X;
 #pragma unroll
-        for (int s = DEPTH; s >= 1; --s) {
-            double bfx[NV], bgy[NV];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) { bfx[v] = K::tw(s) * bF[v]; bgy[v] = K::tw(s) * bG[v]; }
-            if (s < DEPTH) {
-                // d_{s+1} = C(ft_s, gt_s): its adjoint is complete (stages > s are done)
-                double* T = ((DEPTH - s) & 1) ? Y : X;
-#pragma unroll
-                for (int v = 0; v < NV; ++v) put(T, v, bd[s][v]);
-                __syncthreads();
-#pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    bfx[v] = fma(sc, cxt(sD, T, v), bfx[v]);
-                    bgy[v] = fma(sc, cyt(sD, T, v), bgy[v]);
-                }
-            }
-            if (K::w(s, 0) != 0.0) {
-#pragma unroll
-                for (int v = 0; v < NV; ++v) { bf0[v] = fma(K::w(s, 0), bfx[v], bf0[v]); bg0[v] = fma(K::w(s, 0), bgy[v], bg0[v]); }
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (K::w(s, 1 + q) == 0.0) continue;
-                double P[NV], wf[NV], wg[NV], bP[NV] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    double x = u[v];
-#pragma unroll
-                    for (int m = 1; m <= s; ++m) x = fma(K::a(q, m), dget(m, v), x);
-                    P[v] = x;
-                    wf[v] = K::w(s, 1 + q) * bfx[v];
-                    wg[v] = K::w(s, 1 + q) * bgy[v];
-                }
-                euler_flux_vjp(a.gamma, P, wf, wg, bP);
-#pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    bu[v] += bP[v];
-#pragma unroll
-                    for (int m = 1; m <= s; ++m) bd[m - 1][v] = fma(K::a(q, m), bP[v], bd[m - 1][v]);
-                }
-            }
-        }
-        // d_1 = C(f(u), g(u)); after this barrier the stage buffer is no longer read
-        {
-            double* T = (DEPTH & 1) ? Y : X;
-#pragma unroll
-            for (int v = 0; v < NV; ++v) put(T, v, bd[0][v]);
+            for (int v = 0; v < NV; ++v) put(T, v, bd[s][v]);
             __syncthreads();
 #pragma unroll
-            for (int v = 0; v < NV; ++v) { bf0[v] = fma(sc, cxt(sD, T, v), bf0[v]); bg0[v] = fma(sc, cyt(sD, T, v), bg0[v]); }
+            for (int v = 0; v < NV; ++v) {
+                bfx[v] = fma(sc, cxt(sD, T, v), bfx[v]);
+                bgy[v] = fma(sc, cyt(sD, T, v), bgy[v]);
+            }
         }
-        euler_flux_vjp(a.gamma, u, bf0, bg0, bu);
-        if (active) {
-            double o[NV];
+        if (K::w(s, 0) != 0.0) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) o[v] = lam[v] + bu[v] + bud[v];
-            store4(a.lam_out + ((size_t)e * nn + node) * NV, o);
+            for (int v = 0; v < NV; ++v) { bf0[v] = fma(K::w(s, 0), bfx[v], bf0[v]); bg0[v] = fma(K::w(s, 0), bgy[v], bg0[v]); }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (K::w(s, 1 + q) == 0.0) continue;
+            double P[NV], wf[NV], wg[NV], bP[NV] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                double x = u[v];
+#pragma unroll
+                for (int m = 1; m <= s; ++m) x = fma(K::a(q, m), dget(m, v), x);
+                P[v] = x;
+                wf[v] = K::w(s, 1 + q) * bfx[v];
+                wg[v] = K::w(s, 1 + q) * bgy[v];
+            }
+            euler_flux_vjp(a.gamma, P, wf, wg, bP);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                bu[v] += bP[v];
+#pragma unroll
+                for (int m = 1; m <= s; ++m) bd[m - 1][v] = fma(K::a(q, m), bP[v], bd[m - 1][v]);
+            }
         }
     }
-    if (failed && threadIdx.x == 0) {
-        atomicOr(a.status, STATUS_WAIT_TIMEOUT);
-        // the copies still in flight (this tile's, and the next tile's if issued) land before the CTA's shared
-        // memory is released
-        mbar_wait_bounded(&bar[it & 1], (unsigned)((it >> 1) & 1));
-        if ((int)blockIdx.x + (it + 1) * (int)gridDim.x < ntiles)
-            mbar_wait_bounded(&bar[(it + 1) & 1], (unsigned)(((it + 1) >> 1) & 1));
+    // d_1 = C(f(u), g(u))
+    {
+        double* T = (DEPTH & 1) ? Y : X;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) put(T, v, bd[0][v]);
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { bf0[v] = fma(sc, cxt(sD, T, v), bf0[v]); bg0[v] = fma(sc, cyt(sD, T, v), bg0[v]); }
+    }
+    euler_flux_vjp(a.gamma, u, bf0, bg0, bu);
+    if (active) {
+        double o[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) o[v] = lam[v] + bu[v] + bud[v];
+        store4(a.lam_out + ((size_t)e * nn + node) * NV, o);
     }
 }
 
@@ -711,14 +678,6 @@ static __global__ void __launch_bounds__(OBJ_THREADS) sum_kernel(const double* p
 }
 
 // ---- launches ---------------------------------------------------------------------------------------
-// SMs of the current device (persistent grids)
-int sm_count() {
-    int d = 0, c = 0;
-    cudaGetDevice(&d);
-    cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, d);
-    return c > 0 ? c : 1;
-}
-
 template <int N>
 struct AL {
     static void set_attributes() {
@@ -728,8 +687,8 @@ struct AL {
                              (int)VolCfg<N>::smem_bytes(4));
         cudaFuncSetAttribute(adj_volume_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)AdjCfg<N>::smem_bytes());
-        cudaFuncSetAttribute(adj_volume_stored_kernel<N, AdjCfg<N>::MIN_BLOCKS>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AdjCfg<N>::stored_smem_bytes());
+        cudaFuncSetAttribute(adj_volume_reg_kernel<N, AdjCfg<N>::MIN_BLOCKS>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AdjCfg<N>::reg_smem_bytes());
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, false, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VolCfg<N>::smem_bytes(4));
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, false, false, true>,
@@ -768,9 +727,7 @@ struct AL {
         using C = AdjCfg<N>;
         const int grid = (va.E + C::EB - 1) / C::EB;
         if (va.dstore) {
-            // persistent: MIN_BLOCKS CTAs per SM, each over every gridDim-th tile
-            const int persistent = std::min(grid, sm_count() * C::MIN_BLOCKS);
-            adj_volume_stored_kernel<N, C::MIN_BLOCKS><<<persistent, C::THREADS, C::stored_smem_bytes(), s>>>(va);
+            adj_volume_reg_kernel<N, C::MIN_BLOCKS><<<grid, C::THREADS, C::reg_smem_bytes(), s>>>(va);
         } else {
             adj_volume_kernel<N><<<grid, C::THREADS, C::smem_bytes(), s>>>(va);
         }
@@ -859,7 +816,11 @@ int ensure_steps(tlw_handle* h, int nsteps, int ck) {
         if (A.g_rev) cudaGraphExecDestroy(A.g_rev);
         A.g_fwd = A.g_rev = nullptr;
     };
-    if (A.capacity_steps < nsteps || A.capacity_ckpt < (nsteps + ck - 1) / ck || A.capacity_states < ck) drop();
+    // a run of one segment needs one segment buffer, otherwise two (recompute and adjoint alternate)
+    const int nbuf = nsteps > ck ? 2 : 1;
+    if (A.capacity_steps < nsteps || A.capacity_ckpt < (nsteps + ck - 1) / ck || A.capacity_states < ck ||
+        A.capacity_buffers < nbuf)
+        drop();
     if (A.capacity_steps < nsteps) {
         dfree(A.d_dts);
         TLW_ACUDA(h, cudaMalloc(&A.d_dts, (size_t)std::max(nsteps, 1) * sizeof(double)));
@@ -871,16 +832,17 @@ int ensure_steps(tlw_handle* h, int nsteps, int ck) {
         TLW_ACUDA(h, cudaMalloc(&A.d_ckpt, (size_t)std::max(nck, 1) * nstate(h) * sizeof(double)));
         A.capacity_ckpt = std::max(nck, 1);
     }
-    if (A.capacity_states < ck) {
+    if (A.capacity_states < ck || A.capacity_buffers < nbuf) {
         dfree(A.d_seg);
         dfree(A.d_segU);
         dfree(A.d_segD);
-        A.capacity_states = 0;
+        A.capacity_states = A.capacity_buffers = 0;
         A.last_resident = false;
-        TLW_ACUDA(h, cudaMalloc(&A.d_seg, 2 * (size_t)(ck + 1) * nstate(h) * sizeof(double)));
-        TLW_ACUDA(h, cudaMalloc(&A.d_segU, 2 * (size_t)ck * ntrace(h) * sizeof(double)));
-        TLW_ACUDA(h, cudaMalloc(&A.d_segD, 2 * (size_t)ck * depth(h) * nstate(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_seg, nbuf * (size_t)(ck + 1) * nstate(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_segU, nbuf * (size_t)ck * ntrace(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_segD, nbuf * (size_t)ck * depth(h) * nstate(h) * sizeof(double)));
         A.capacity_states = ck;
+        A.capacity_buffers = nbuf;
     }
     return TLW_OK;
 }
@@ -976,7 +938,6 @@ void enqueue_adjoint_step(tlw_handle* h, const double* u, const double* tU, cons
     va.E = (int)h->E;
     va.gamma = h->opts.gamma;
     va.dstore = dstore;
-    va.status = &h->d_step->status;
     adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::adjoint(s ? s : h->stream, sa, va); });
 }
 
@@ -988,8 +949,6 @@ int adj_status(tlw_handle* h) {
     if (st) {
         const unsigned zero = 0;
         TLW_ACUDA(h, cudaMemcpy(&h->d_step->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
-        if (st & STATUS_WAIT_TIMEOUT)
-            return afail(h, TLW_E_CUDA, "adjoint volume kernel: a bounded wait on a bulk copy timed out");
         return afail(h, TLW_E_NONADMISSIBLE, "non-admissible state: square root of a negative number (DomainError)");
     }
     return TLW_OK;

@@ -9,43 +9,6 @@ constexpr int NV = 4;   // compressible Euler 2D: rho, rho v1, rho v2, rho e
 
 // status bits written by kernels (never a trap): the host maps them to TLW_E_* codes
 constexpr unsigned STATUS_NONADMISSIBLE = 1u;   // sqrt of a negative number (reference: DomainError)
-constexpr unsigned STATUS_WAIT_TIMEOUT = 2u;    // a bounded wait on a bulk copy gave up (the kernel returned early)
-
-// ---- bulk asynchronous copies global -> shared (cp.async.bulk), completed on a CTA mbarrier -------------
-// Both addresses 16-byte aligned, the size a multiple of 16 bytes. No multicast.
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-// makes initialised mbarriers visible to the asynchronous proxy (followed by a CTA barrier)
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-// the calling thread's arrival, expecting `bytes` of transactions in the current phase
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// waits for the phase with the given parity to complete; false after `limit` unsuccessful tries (each try may
-// suspend the thread for a hardware-defined interval, so the bound is on the order of a second)
-constexpr long long MBAR_WAIT_LIMIT = 1ll << 20;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, long long limit = MBAR_WAIT_LIMIT) {
-    for (long long k = 0; k < limit; ++k)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
 
 struct Basis {
     double D[16 * 16];      // derivative matrix, D[a*n + b] = l_b'(x_a)

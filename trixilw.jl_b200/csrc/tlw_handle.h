@@ -23,6 +23,7 @@ struct AdjointBuffers {
     int64_t E = 0;                          // element count the buffers were sized for
     int capacity_steps = 0;                 // dt sequence capacity
     int capacity_states = 0;                // states of one checkpoint segment
+    int capacity_buffers = 0;               // segment buffers allocated (1 or 2)
     double* d_lam[2] = {nullptr, nullptr};  // adjoint state ping-pong
     double *d_bF = nullptr, *d_bU = nullptr, *d_bu = nullptr;   // face-trace adjoints [v, l, face, e]
     double* d_dts = nullptr;                // dt of every recorded forward step
@@ -30,11 +31,12 @@ struct AdjointBuffers {
     int capacity_given = 0;
     double* d_ckpt = nullptr;               // checkpoint states
     int capacity_ckpt = 0;
-    // two segment buffers (one is recomputed while the reverse sweep reads the other), each of
-    // capacity_states steps: the step input states (+1 slot: u(T), or scratch), U traces, stage derivatives
-    double* d_seg = nullptr;                // [2][capacity_states + 1] states
-    double* d_segU = nullptr;               // [2][capacity_states] time-averaged U traces
-    double* d_segD = nullptr;               // [2][capacity_states][depth] stage derivatives d_1..d_depth
+    // segment buffers (two when a run has several segments: one is recomputed while the reverse sweep reads
+    // the other), each of capacity_states steps: the step input states (+1 slot: u(T), or scratch), U traces,
+    // stage derivatives
+    double* d_seg = nullptr;                // [buffers][capacity_states + 1] states
+    double* d_segU = nullptr;               // [buffers][capacity_states] time-averaged U traces
+    double* d_segD = nullptr;               // [buffers][capacity_states][depth] stage derivatives d_1..d_depth
     bool last_resident = false;             // the recorded run's last segment is in its buffer (no recompute)
     cudaStream_t s_rec = nullptr;           // reverse sweep: recompute stream (lowest priority)
     cudaStream_t s_adj = nullptr;           // reverse sweep: adjoint chain (highest priority)
