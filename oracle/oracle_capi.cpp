@@ -8,6 +8,7 @@
 #include "tlw_adjoint.hpp"
 #include "tlw_curved.hpp"
 #include "tlw_curved_parabolic.hpp"
+#include "tlw_curved_sc.hpp"
 #include "tlw_limiter.hpp"
 #include "tlw_parabolic.hpp"
 #include "tlw_oracle.hpp"
@@ -48,7 +49,11 @@ void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, do
         rhs(h->basis, h->eq, h->opt, h->mesh, u, u2, du, t, dt, bd, kind, h->ws, nthreads);
         return;
     }
-    if (h->opt.shock_capturing) throw std::runtime_error("curvilinear oracle: FR volume integral only");
+    if (h->opt.shock_capturing) {
+        if (kind != 0) throw std::runtime_error("curvilinear shock capturing: LW only");
+        rhs_curved_sc(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, bd);
+        return;
+    }
     rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, kind, u2, bd);
 }
 
@@ -203,6 +208,9 @@ void oracle_set_shock_capturing(oracle_handle* h, int on, double alpha_max, doub
     h->opt.alpha_min = alpha_min;
     h->opt.alpha_smooth = alpha_smooth != 0;
 }
+
+// the subcell reconstruction of blended elements on curvilinear meshes: 0 first order, 1 MUSCL
+void oracle_set_reconstruction(oracle_handle* h, int reconstruction) { h->opt.reconstruction = reconstruction; }
 
 void oracle_set_temporal_errors(oracle_handle* h, int on, double abstol, double reltol) {
     h->opt.temporal_errors = on != 0;

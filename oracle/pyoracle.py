@@ -40,6 +40,7 @@ def lib():
         L.oracle_destroy.argtypes = [P]
         L.oracle_set_temporal_errors.argtypes = [P, i32, dbl, dbl]
         L.oracle_set_shock_capturing.argtypes = [P, i32, dbl, dbl, i32]
+        L.oracle_set_reconstruction.argtypes = [P, i32]
         L.oracle_set_boundary_data.argtypes = [P, P, P]
         L.oracle_rhs.argtypes = [P, i32, P, P, P, dbl, dbl, i32]
         L.oracle_get.argtypes = [P, i32, P]
@@ -188,8 +189,9 @@ class Oracle:
         assert lib().oracle_apply_limiter(self.h, _p(u)) == 0
         return u
 
-    def set_shock_capturing(self, on=True, alpha_max=0.5, alpha_min=0.001, alpha_smooth=True):
+    def set_shock_capturing(self, on=True, alpha_max=0.5, alpha_min=0.001, alpha_smooth=True, reconstruction=0):
         lib().oracle_set_shock_capturing(self.h, 1 if on else 0, alpha_max, alpha_min, 1 if alpha_smooth else 0)
+        lib().oracle_set_reconstruction(self.h, int(reconstruction))
 
     def set_boundary_data(self, levels: np.ndarray, now: np.ndarray):
         self._bkeep = (np.ascontiguousarray(levels, dtype=np.float64), np.ascontiguousarray(now, dtype=np.float64))

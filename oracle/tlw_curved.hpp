@@ -100,8 +100,9 @@ inline void lw_surface_flux_normal(const Euler& eq, int flux_kind, int speed_kin
 
 // One element of the curvilinear LW volume kernel. du receives Dhat F~ + Dhat G~ (before the surface
 // integral and the Jacobian); ws.U / ws.F receive the time-averaged U and the physical F, G.
+// alpha: the factor of the Dhat terms (1 - the element's blending factor under shock capturing).
 inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, const CurvedMesh& m, int e,
-                                     const double* u, double* du, double dt, Workspace& ws) {
+                                     const double* u, double* du, double dt, Workspace& ws, double alpha = 1.0) {
     const int n = b.n, nn = n * n;
     const LWStencils S = lw_stencils(N);
     const int depth = S.depth;
@@ -185,9 +186,9 @@ inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, con
         for (int i = 0; i < n; ++i) {
             const int o = L(i, j);
             for (int ii = 0; ii < n; ++ii)
-                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += b.Dhat[ii * n + i] * Ft[o + v];
+                for (int v = 0; v < NV; ++v) due[L(ii, j) + v] += alpha * b.Dhat[ii * n + i] * Ft[o + v];
             for (int jj = 0; jj < n; ++jj)
-                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += b.Dhat[jj * n + j] * Gt[o + v];
+                for (int v = 0; v < NV; ++v) due[L(i, jj) + v] += alpha * b.Dhat[jj * n + j] * Gt[o + v];
             for (int v = 0; v < NV; ++v) {
                 ws.F[idx_F(n, v, 0, i, j, e)] = Fp[o + v];
                 ws.F[idx_F(n, v, 1, i, j, e)] = Gp[o + v];

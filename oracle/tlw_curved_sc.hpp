@@ -1,0 +1,376 @@
+// tlw_curved_sc.hpp -- test infrastructure only: CPU restatement of shock capturing on conforming curvilinear
+// meshes as the P4estMesh{2} path of the reference computes it, used to check the CUDA kernels.
+//
+// Volume (calc_volume_integral!(..., ::VolumeIntegralFRShockCapturing, ...), src/solvers/dgsem_tree/
+// dg_2d.jl:1648-1804, whose mesh Union covers P4estMesh{2}): the Hennemann-Gassner factor alpha_e of every
+// element (density_pressure, smoothed over the interfaces), the LW volume terms scaled by (1 - alpha_e), and
+//  * on blended elements (alpha_e not within 1e-12 of 0) fv_kernel! (dg_2d.jl:251-282, 326-365): du +=
+//    alpha_e (w_i^-1 (f*_{i+1} - f*_i) + w_j^-1 (g*_{j+1} - g*_j)) with the subcell fluxes of Trixi's
+//    curvilinear calcflux_fv! (FirstOrderReconstruction) or calcflux_muscl! (MUSCLReconstruction,
+//    src/solvers/dgsem_structured/dg_2d.jl:176-311, first order on elements with a boundary face);
+//  * on pure DG elements calc_fn_low! (dgsem_structured/dg_2d.jl:111-174), which evaluates only the subcell
+//    faces next to the element faces and, looping over the tuple (2, nnodes), accumulates the subcell normal
+//    of the last inner face from the first and the last metric increments only;
+//  * load_fn_low! for P4estMesh (dgsem_tree/dg_2d.jl:236-249) stores those face-adjacent fluxes in the order
+//    (bottom, right, top, left).
+// Subcell normals: along xi, face f (between nodes f-1 and f) has Ja^1(0, j) + sum_{k < f} w_k sum_m
+// D[k][m] Ja^1(m, j); along eta likewise with Ja^2. The subcell flux is volume_flux_fv (flux_lax_friedrichs)
+// in its normal-direction form.
+// Interfaces (calc_interface_flux!, src/solvers/dgsem_p4est/dg_2d.jl:149-191; prolong2interfaces!, :8-84):
+// the LW flux Fn_ and the first-order flux fn at u along the primary's normal are blended by get_blended_flux
+// (:227-250): alp = (alpha_P + alpha_S) / 2, Fn = (1 - alp) Fn_ + alp fn, and where the subcell update
+// u - c (Fn - fn_inner) (c = dt J^{-1} / (w / 2), J^{-1} of the primary's face node for both sides) is not
+// admissible, zhang_shu_flux_fix (:199-225) pulls Fn towards fn, first for density, then for pressure.
+// fn_inner of a side is fn_low[:, l, direction, element] with the primary's node index l on both sides and
+// the direction numbering (-xi, +xi, -eta, +eta), while load_fn_low! filled the slots as (bottom, right, top,
+// left): both are kept as the reference has them. Boundary faces are not blended (dgsem_p4est/dg_2d.jl:366-393).
+#pragma once
+#include <cmath>
+#include <vector>
+
+#include "tlw_curved.hpp"
+#include "tlw_limiter.hpp"
+
+namespace tlwo {
+
+enum Reconstruction { REC_FIRST_ORDER = 0, REC_MUSCL = 1 };
+
+// Trixi flux_lax_friedrichs(u_ll, u_rr, normal_direction, equations)
+inline void rusanov_normal(const Euler& eq, int speed_kind, const double* ul, const double* ur, const double* nrm,
+                           double* out, bool& bad) {
+    double fl[NV], gl[NV], fr[NV], gr[NV];
+    eq.fluxes(ul, fl, gl);
+    eq.fluxes(ur, fr, gr);
+    const double lambda = max_abs_speed_normal(eq, ul, ur, nrm, speed_kind, bad);
+    for (int v = 0; v < NV; ++v) {
+        const double fnl = fl[v] * nrm[0] + gl[v] * nrm[1], fnr = fr[v] * nrm[0] + gr[v] * nrm[1];
+        out[v] = 0.5 * (fnl + fnr) + (-0.5 * lambda * (ur[v] - ul[v]));
+    }
+}
+
+// metric increment w_k sum_m D[k][m] Ja^d(m along the line) of contravariant direction d (0: xi, 1: eta) on
+// the line `line` (j for xi, i for eta) at line position k
+inline void metric_increment(const Basis& b, const double* Jae, int d, int line, int k, double* inc) {
+    const int n = b.n;
+    inc[0] = inc[1] = 0.0;
+    for (int m = 0; m < n; ++m) {
+        const double* J = Jae + 4 * (d == 0 ? m + n * line : line + n * m);
+        const double c = b.weights[k] * b.D[k * n + m];
+        inc[0] += c * J[2 * d];
+        inc[1] += c * J[2 * d + 1];
+    }
+}
+
+// Subcell fluxes of one element: X(f, j) on xi faces f = 0..n (0 and n zero), Y(i, f) on eta faces.
+struct SubcellFluxes {
+    int n = 0;
+    std::vector<double> fx, fy;
+    void init(int nn) {
+        n = nn;
+        fx.assign((size_t)NV * (n + 1) * n, 0.0);
+        fy.assign((size_t)NV * n * (n + 1), 0.0);
+    }
+    double* X(int f, int j) { return fx.data() + NV * (f + (n + 1) * j); }
+    double* Y(int i, int f) { return fy.data() + NV * (i + n * f); }
+};
+
+// subcell fluxes from the face states: uL(d, f, line) / uR(d, f, line) give the states left / right of inner
+// face f; fn_low_only: only faces 1 and n-1, with the normal accumulated over the faces visited (calc_fn_low!)
+template <class GetL, class GetR>
+inline void subcell_fluxes_curved(const Basis& b, const Euler& eq, int speed_kind, const double* Jae, bool fn_low_only,
+                                  GetL uL, GetR uR, SubcellFluxes& S, bool& bad) {
+    const int n = b.n;
+    for (int d = 0; d < 2; ++d)
+        for (int line = 0; line < n; ++line) {
+            // normal_direction = Ja^d at the line's first node, then the increments of the faces visited
+            const double* J0 = Jae + 4 * (d == 0 ? 0 + n * line : line + 0);
+            double nrm[2] = {J0[2 * d], J0[2 * d + 1]};
+            for (int f = 1; f < n; ++f) {
+                if (fn_low_only && f != 1 && f != n - 1) continue;
+                double inc[2];
+                metric_increment(b, Jae, d, line, f - 1, inc);
+                nrm[0] += inc[0];
+                nrm[1] += inc[1];
+                double out[NV];
+                rusanov_normal(eq, speed_kind, uL(d, f, line), uR(d, f, line), nrm, out, bad);
+                double* dst = d == 0 ? S.X(f, line) : S.Y(line, f);
+                for (int v = 0; v < NV; ++v) dst[v] = out[v];
+            }
+        }
+}
+
+// Julia sign
+inline double julia_sign(double x) { return x == 0.0 || std::isnan(x) ? x : (x > 0.0 ? 1.0 : -1.0); }
+
+// minmod(a, b, Mdx2) of dgsem_structured/dg_2d.jl:97-109 (Julia min propagates NaN; NaN signs differ)
+inline double minmod2(double a, double b, double Mdx2) {
+    if (std::fabs(b) < Mdx2 && std::fabs(a) < Mdx2) return b;
+    const double slope = julia_min(std::fabs(a), std::fabs(b));
+    const double s1 = julia_sign(a), s2 = julia_sign(b);
+    if (s1 != s2) return 0.0;
+    return s1 * slope;
+}
+
+// limit_variable_slope (src/equations/equations.jl:262-287) for `variable` (LIMIT_DENSITY / LIMIT_PRESSURE)
+inline void limit_variable_slope(const Euler& eq, int variable, double* slope, double* usl, double* usr,
+                                 const double* ue, double xl, double xr) {
+    const double vsl = limiter_value(eq, variable, usl), vsr = limiter_value(eq, variable, usr);
+    const double vlow = limiter_value(eq, variable, ue);
+    const double eps = 1e-10;
+    const double threshold = 0.1 * vlow;
+    if (vsl < eps || vsr < eps) {
+        const double rl = std::fabs(threshold - vlow) / (std::fabs(vsl - vlow) + 1e-13);
+        const double rr = std::fabs(threshold - vlow) / (std::fabs(vsr - vlow) + 1e-13);
+        const double theta = julia_min(julia_min(rl, rr), 1.0);
+        for (int v = 0; v < NV; ++v) {
+            slope[v] *= theta;
+            usl[v] = ue[v] + (2.0 * theta) * (xl * slope[v]);
+            usr[v] = ue[v] + (2.0 * theta) * (xr * slope[v]);
+        }
+    }
+}
+
+// limit_slope (src/equations/compressible_euler_2d.jl:9-21): density, then pressure; face values from the slope
+inline void limit_slope(const Euler& eq, double* slope, double* usl, double* usr, const double* ue, double xl,
+                        double xr, double* ufl, double* ufr) {
+    limit_variable_slope(eq, LIMIT_DENSITY, slope, usl, usr, ue, xl, xr);
+    limit_variable_slope(eq, LIMIT_PRESSURE, slope, usl, usr, ue, xl, xr);
+    for (int v = 0; v < NV; ++v) {
+        ufl[v] = ue[v] + slope[v] * xl;
+        ufr[v] = ue[v] + slope[v] * xr;
+    }
+}
+
+// compute_subcells (dgsem_tree/dg_2d.jl:1806-1824): subcell faces and the extended node positions
+struct Subcells {
+    std::vector<double> faces;   // [0..n]: -1, -1 + w_0, ..., 1
+    std::vector<double> xi_ext;  // [0..n+1]: -1, nodes, 1
+};
+inline Subcells compute_subcells(const Basis& b) {
+    const int n = b.n;
+    Subcells s;
+    s.faces.assign(n + 1, -1.0);
+    for (int i = 1; i <= n; ++i) {
+        double acc = 0.0;
+        for (int k = 0; k < i; ++k) acc += b.weights[k];
+        s.faces[i] = -1.0 + acc;
+    }
+    s.xi_ext.assign(n + 2, -1.0);
+    for (int i = 0; i < n; ++i) s.xi_ext[i + 1] = b.nodes[i];
+    s.xi_ext[n + 1] = 1.0;
+    return s;
+}
+
+// The face values of the MUSCL reconstruction of one element (calcflux_muscl!, dgsem_structured/dg_2d.jl:
+// 196-253): uf[node][k][v], k = 0 left, 1 right, 2 down, 3 up; element-local (the extended state copies the
+// edge nodes, so the one-sided difference into the copy is 0 / 0 and the edge subcells get a zero slope)
+inline void muscl_face_values(const Basis& b, const Euler& eq, const Subcells& sc, const double* u, int e,
+                              std::vector<double>& uf) {
+    const int n = b.n;
+    uf.assign((size_t)4 * NV * n * n, 0.0);
+    auto ue = [&](int i, int j) {   // extended indices 0..n+1
+        i = std::min(std::max(i, 1), n);
+        j = std::min(std::max(j, 1), n);
+        return u + idx_u(n, 0, i - 1, j - 1, e);
+    };
+    for (int j = 1; j <= n; ++j)
+        for (int i = 1; i <= n; ++i) {
+            const double *u_ = ue(i, j), *ul = ue(i - 1, j), *ur = ue(i + 1, j), *ud = ue(i, j - 1),
+                         *uu = ue(i, j + 1);
+            const double dx1 = sc.xi_ext[i] - sc.xi_ext[i - 1], dx2 = sc.xi_ext[i + 1] - sc.xi_ext[i];
+            const double dy1 = sc.xi_ext[j] - sc.xi_ext[j - 1], dy2 = sc.xi_ext[j + 1] - sc.xi_ext[j];
+            double sx[NV], sy[NV];
+            for (int v = 0; v < NV; ++v) {
+                const double bx = (u_[v] - ul[v]) / dx1, fx = (ur[v] - u_[v]) / dx2;
+                const double by = (u_[v] - ud[v]) / dy1, fy = (uu[v] - u_[v]) / dy2;
+                sx[v] = minmod2(bx, fx, 0.0);
+                sy[v] = minmod2(by, fy, 0.0);
+            }
+            const double xl = sc.faces[i - 1] - sc.xi_ext[i], xr = sc.faces[i] - sc.xi_ext[i];
+            const double yl = sc.faces[j - 1] - sc.xi_ext[j], yr = sc.faces[j] - sc.xi_ext[j];
+            double usl[NV], usr[NV], usd[NV], usu[NV];
+            for (int v = 0; v < NV; ++v) {
+                usl[v] = u_[v] + 2.0 * sx[v] * xl;
+                usr[v] = u_[v] + 2.0 * sx[v] * xr;
+                usd[v] = u_[v] + 2.0 * sy[v] * yl;
+                usu[v] = u_[v] + 2.0 * sy[v] * yr;
+            }
+            double* o = uf.data() + (size_t)4 * NV * ((i - 1) + n * (j - 1));
+            limit_slope(eq, sx, usl, usr, u_, xl, xr, o + 0 * NV, o + 1 * NV);
+            limit_slope(eq, sy, usd, usu, u_, yl, yr, o + 2 * NV, o + 3 * NV);
+        }
+}
+
+// One element's subcell pass: blended elements add alpha_e times the FV divergence to du; every element fills
+// its fn_low slots (P4est order: bottom, right, top, left).
+inline void curved_subcells(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m,
+                            const Subcells& sc, const std::vector<char>& at_boundary, int e, const double* u,
+                            double* du, double alpha, bool blended, Workspace& ws, bool& bad) {
+    const int n = b.n, nn = n * n;
+    const double* Jae = &m.Ja[4 * (size_t)nn * e];
+    SubcellFluxes S;
+    S.init(n);
+    auto node = [&](int i, int j) { return u + idx_u(n, 0, i, j, e); };
+    // the states left / right of inner face f on line `line` of direction d from the nodes
+    auto nodeL = [&](int d, int f, int line) { return d == 0 ? node(f - 1, line) : node(line, f - 1); };
+    auto nodeR = [&](int d, int f, int line) { return d == 0 ? node(f, line) : node(line, f); };
+    if (!blended) {
+        subcell_fluxes_curved(b, eq, opt.speed_kind, Jae, true, nodeL, nodeR, S, bad);
+    } else if (opt.reconstruction == REC_MUSCL && !at_boundary[e]) {
+        std::vector<double> uf;
+        muscl_face_values(b, eq, sc, u, e, uf);
+        auto F = [&](int i, int j, int k) { return uf.data() + (size_t)4 * NV * (i + n * j) + NV * k; };
+        // u_ll: the right (up) face value of the node before the face, u_rr: the left (down) value after it
+        auto fL = [&](int d, int f, int line) { return d == 0 ? F(f - 1, line, 1) : F(line, f - 1, 3); };
+        auto fR = [&](int d, int f, int line) { return d == 0 ? F(f, line, 0) : F(line, f, 2); };
+        subcell_fluxes_curved(b, eq, opt.speed_kind, Jae, false, fL, fR, S, bad);
+    } else {
+        subcell_fluxes_curved(b, eq, opt.speed_kind, Jae, false, nodeL, nodeR, S, bad);
+    }
+    if (blended) {
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i)
+                for (int v = 0; v < NV; ++v)
+                    du[idx_u(n, v, i, j, e)] += alpha * (1.0 / b.weights[i] * (S.X(i + 1, j)[v] - S.X(i, j)[v]) +
+                                                         1.0 / b.weights[j] * (S.Y(i, j + 1)[v] - S.Y(i, j)[v]));
+    }
+    for (int l = 0; l < n; ++l)
+        for (int v = 0; v < NV; ++v) {
+            ws.fn_low[v + NV * (l + n * (0 + 4 * (size_t)e))] = S.Y(l, 1)[v];       // bottom
+            ws.fn_low[v + NV * (l + n * (1 + 4 * (size_t)e))] = S.X(n - 1, l)[v];   // right
+            ws.fn_low[v + NV * (l + n * (2 + 4 * (size_t)e))] = S.Y(l, n - 1)[v];   // top
+            ws.fn_low[v + NV * (l + n * (3 + 4 * (size_t)e))] = S.X(1, l)[v];       // left
+        }
+}
+
+// Hennemann-Gassner factors on a curvilinear mesh, smoothed over its interfaces (Trixi apply_smoothing!)
+inline void indicator_curved(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m, const double* u,
+                             std::vector<double>& alpha) {
+    TreeMesh none;
+    none.n_elements = m.n_elements;
+    none.n_interfaces = 0;
+    Options o = opt;
+    o.alpha_smooth = false;
+    indicator_hennemann_gassner(b, eq, o, none, u, alpha);
+    if (opt.alpha_smooth) {
+        const std::vector<double> tmp = alpha;
+        for (int k = 0; k < m.n_interfaces; ++k) {
+            const int l = m.p_elem[k], r = m.s_elem[k];
+            alpha[l] = std::max(std::max(tmp[l], 0.5 * tmp[r]), alpha[l]);
+            alpha[r] = std::max(std::max(tmp[r], 0.5 * tmp[l]), alpha[r]);
+        }
+    }
+}
+
+// zhang_shu_flux_fix (src/solvers/dgsem_p4est/dg_2d.jl:199-225)
+inline void zhang_shu_flux_fix(const Euler& eq, const double* uprev, const double* ulow, double* Fn,
+                               const double* fn_inner, const double* fn, double c) {
+    double uhigh[NV];
+    for (int v = 0; v < NV; ++v) uhigh[v] = uprev[v] - c * (Fn[v] - fn_inner[v]);
+    double lo = ulow[0], hi = uhigh[0];
+    double eps = 0.1 * lo;
+    double theta = julia_min(std::fabs(eps - lo) / (std::fabs(hi - lo) + 1e-13), 1.0);
+    if (theta < 1.0)
+        for (int v = 0; v < NV; ++v) Fn[v] = theta * Fn[v] + (1.0 - theta) * fn[v];
+    for (int v = 0; v < NV; ++v) uhigh[v] = uprev[v] - c * (Fn[v] - fn_inner[v]);
+    lo = limiter_value(eq, LIMIT_PRESSURE, ulow);
+    hi = limiter_value(eq, LIMIT_PRESSURE, uhigh);
+    eps = 0.1 * lo;
+    theta = julia_min(std::fabs(eps - lo) / (std::fabs(hi - lo) + 1e-13), 1.0);
+    if (theta < 1.0)
+        for (int v = 0; v < NV; ++v) Fn[v] = theta * Fn[v] + (1.0 - theta) * fn[v];
+}
+
+// get_blended_flux (src/solvers/dgsem_p4est/dg_2d.jl:227-250); J = the primary face node's J^{-1}
+inline void get_blended_flux(const Basis& b, const Euler& eq, const double* u_ll, const double* u_rr, double alpha_p,
+                             double alpha_s, double J, double dt, const double* fn, const double* Fn_,
+                             const double* fil, const double* fir, double* Fn) {
+    const int n = b.n;
+    const double alp = 0.5 * (alpha_p + alpha_s);
+    for (int v = 0; v < NV; ++v) Fn[v] = (1.0 - alp) * Fn_[v] + alp * fn[v];
+    const double lam = 0.5;
+    const double c_ll = dt * J / (b.weights[n - 1] * lam);
+    double test[NV], low[NV];
+    for (int v = 0; v < NV; ++v) {
+        test[v] = u_ll[v] - c_ll * (Fn[v] - fil[v]);
+        low[v] = u_ll[v] - c_ll * (fn[v] - fil[v]);
+    }
+    if (!eq.is_admissible(test)) zhang_shu_flux_fix(eq, u_ll, low, Fn, fil, fn, c_ll);
+    const double c_rr = -dt * J / (b.weights[0] * lam);
+    for (int v = 0; v < NV; ++v) {
+        test[v] = u_rr[v] - c_rr * (Fn[v] - fir[v]);
+        low[v] = u_rr[v] - c_rr * (fn[v] - fir[v]);
+    }
+    if (!eq.is_admissible(test)) zhang_shu_flux_fix(eq, u_rr, low, Fn, fir, fn, c_rr);
+}
+
+// du = rhs(u) of the LW step with VolumeIntegralFRShockCapturing on a conforming curvilinear mesh (Rusanov
+// surface flux); the factors of the call are left in ws.alpha.
+inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m, const double* u,
+                          double* du, double dt, Workspace& ws, int nthreads = 1, const BoundaryData* bd = nullptr) {
+    if (opt.flux_kind != RUSANOV) throw std::invalid_argument("curvilinear shock capturing: Rusanov surface flux");
+    const int n = b.n, nn = n * n;
+    const size_t ndof = (size_t)NV * nn * m.n_elements;
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    ws.U.assign(ndof, nan);
+    ws.F.assign(2 * ndof, nan);
+    ws.surface_flux_values.assign((size_t)NV * n * 4 * m.n_elements, nan);
+    ws.fn_low.assign((size_t)NV * n * 4 * m.n_elements, 0.0);
+    ws.bad = false;
+    for (size_t k = 0; k < ndof; ++k) du[k] = 0.0;
+    indicator_curved(b, eq, opt, m, u, ws.alpha);
+    const Subcells sc = compute_subcells(b);
+    std::vector<char> at_boundary(m.n_elements, 0);
+    for (int k = 0; k < m.n_boundaries; ++k) at_boundary[m.b_elem[k]] = 1;
+    bool bad = false;
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad)
+    for (int e = 0; e < m.n_elements; ++e) {
+        const double a = ws.alpha[e];
+        lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws, 1.0 - a);
+        // pure_and_blended_element_ids!: DG only where isapprox(alpha, 0, atol = 1e-12)
+        const bool blended = !(std::fabs(a) <= 1e-12);
+        bool b_ = false;
+        curved_subcells(b, eq, opt, m, sc, at_boundary, e, u, du, a, blended, ws, b_);
+        bad = bad || b_;
+    }
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad)
+    for (int k = 0; k < m.n_interfaces; ++k) {
+        const int pe = m.p_elem[k], pf = m.p_face[k], se = m.s_elem[k], sf = m.s_face[k];
+        for (int l = 0; l < n; ++l) {
+            const int ls = m.s_rev[k] ? n - 1 - l : l;
+            int ip, jp, is, js;
+            face_node(n, pf, l, ip, jp);
+            face_node(n, sf, ls, is, js);
+            double nP[2], nS[2], f_ll[NV], f_rr[NV], u_ll[NV], u_rr[NV], U_ll[NV], U_rr[NV], Fn_[NV], fn[NV];
+            double fil[NV], fir[NV], Fn[NV];
+            outward_normal(m, n, pf, ip, jp, pe, nP);
+            outward_normal(m, n, sf, is, js, se, nS);
+            for (int v = 0; v < NV; ++v) {
+                f_ll[v] = ws.F[idx_F(n, v, 0, ip, jp, pe)] * nP[0] + ws.F[idx_F(n, v, 1, ip, jp, pe)] * nP[1];
+                f_rr[v] = ws.F[idx_F(n, v, 0, is, js, se)] * (-nS[0]) + ws.F[idx_F(n, v, 1, is, js, se)] * (-nS[1]);
+                u_ll[v] = u[idx_u(n, v, ip, jp, pe)];
+                u_rr[v] = u[idx_u(n, v, is, js, se)];
+                U_ll[v] = ws.U[idx_u(n, v, ip, jp, pe)];
+                U_rr[v] = ws.U[idx_u(n, v, is, js, se)];
+                // the primary's node index on both sides, slots as load_fn_low! filled them
+                fil[v] = ws.fn_low[v + NV * (l + n * (pf + 4 * (size_t)pe))];
+                fir[v] = ws.fn_low[v + NV * (l + n * (sf + 4 * (size_t)se))];
+            }
+            bool b_ = false;
+            lw_surface_flux_normal(eq, opt.flux_kind, opt.speed_kind, f_ll, f_rr, u_ll, u_rr, U_ll, U_rr, nP, Fn_, b_);
+            rusanov_normal(eq, opt.speed_kind, u_ll, u_rr, nP, fn, b_);
+            const double J = m.inv_jac[ip + n * (jp + (size_t)n * pe)];
+            get_blended_flux(b, eq, u_ll, u_rr, ws.alpha[pe], ws.alpha[se], J, dt, fn, Fn_, fil, fir, Fn);
+            bad = bad || b_;
+            for (int v = 0; v < NV; ++v) {
+                ws.surface_flux_values[v + NV * (l + n * (pf + 4 * (size_t)pe))] = Fn[v];
+                ws.surface_flux_values[v + NV * (ls + n * (sf + 4 * (size_t)se))] = -Fn[v];
+            }
+        }
+    }
+    ws.bad = ws.bad || bad;
+    calc_boundary_flux_curved(b, eq, opt, m, u, ws, bd, 1.0);
+    surface_integral_and_jacobian_curved(b, m, du, ws, nthreads);
+}
+
+}  // namespace tlwo

@@ -357,6 +357,7 @@ struct Options {
     bool shock_capturing = false;
     double alpha_max = 0.5, alpha_min = 0.001;
     bool alpha_smooth = true;
+    int reconstruction = 0;        // curvilinear meshes: 0 FirstOrderReconstruction, 1 MUSCLReconstruction
 };
 
 struct Workspace {

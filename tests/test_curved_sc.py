@@ -1,0 +1,86 @@
+"""Shock capturing on curvilinear conforming meshes (the reference's P4estMesh{2} path: Hennemann-Gassner
+blending with first-order or MUSCL subcells, the blended interface flux with the Zhang-Shu flux fix): the
+oracle's properties on the CPU, and libtlw's kernels against the oracle on the GPU."""
+import os
+
+import numpy as np
+import pytest
+
+from test_curved import quad, rel_l2, warp
+
+NTH = os.cpu_count() or 1
+GAMMA = 1.4
+
+
+def blast_state(cm, rho_in=1.0, p_in=10.0, rho_out=0.125, p_out=1.0, r0=3.0, center=(0.5, -0.7)):
+    """A circular blast at rest: (rho_in, p_in) inside radius r0, (rho_out, p_out) outside."""
+    x, y = cm.xy
+    inside = (x - center[0]) ** 2 + (y - center[1]) ** 2 < r0 ** 2
+    rho = np.where(inside, rho_in, rho_out)
+    p = np.where(inside, p_in, p_out)
+    v = np.stack([rho, 0.0 * rho, 0.0 * rho, p / (GAMMA - 1.0)], axis=-1)   # [i, j, e, v]
+    return np.ascontiguousarray(np.transpose(v, (2, 1, 0, 3))).reshape(-1)
+
+
+def make(oracle_mod, tl, N, cells=(6, 6), rec=0, alpha_max=0.5, rotate=False):
+    m = tl.StructuredMesh(cells, warp)
+    cm = m.curved(N)
+    if rotate:
+        turns = np.random.default_rng(N + 7).integers(0, 4, cm.n_elements)
+        cm = tl.rotate_elements(cm, turns)
+    o = oracle_mod.Oracle(cm if rotate else m, N)
+    o.set_shock_capturing(True, alpha_max=alpha_max, alpha_min=0.001, alpha_smooth=True, reconstruction=rec)
+    return m, cm, o
+
+
+# ---------------------------------------------------------------------------------------------- CPU
+@pytest.mark.parametrize("N", [3, 4])
+def test_oracle_curved_sc_without_blending_is_the_fr_rhs(oracle_mod, tl, N):
+    """alpha_max = 0: every element is pure DG and the blended interface flux is the LW flux, so the rhs is
+    the FR one bit for bit (a smooth state keeps every subcell update admissible)."""
+    m = tl.StructuredMesh((6, 6), warp)
+    cm = m.curved(N)
+    from test_curved import vortex_state
+    u = vortex_state(tl, cm)
+    plain = oracle_mod.Oracle(m, N)
+    dt = plain.max_dt(u, 0.4)
+    _, _, o = make(oracle_mod, tl, N, alpha_max=0.0)
+    np.testing.assert_array_equal(o.rhs(u, 0.0, dt), plain.rhs(u, 0.0, dt))
+    assert np.all(o.get(6) == 0.0)
+
+
+@pytest.mark.parametrize("N,rec", [(3, 0), (4, 0), (4, 1), (5, 1)])
+def test_oracle_curved_sc_blast_conservation(oracle_mod, tl, N, rec):
+    """The blast: blending is active near the discontinuity, the rhs conserves every variable on the
+    periodic mesh, and a few steps stay admissible."""
+    _, cm, o = make(oracle_mod, tl, N, cells=(8, 8), rec=rec)
+    u = blast_state(cm)
+    dt = o.max_dt(u, 0.2)
+    du = o.rhs(u, 0.0, dt)
+    alpha = o.get(6)
+    assert alpha.max() > 0.1 and (alpha == 0.0).sum() > 0
+    assert np.all(np.abs(quad(cm, N, du)) < 1e-11 * np.abs(quad(cm, N, u)).max())
+    mass0 = quad(cm, N, u)
+    s, _ = o.steps(u, 20, 0.2, 0.0, 1e9, nthreads=NTH)
+    assert s == 20 and np.all(np.isfinite(u))
+    np.testing.assert_allclose(quad(cm, N, u), mass0, rtol=1e-12, atol=1e-12)
+    uu = u.reshape(-1, 4)
+    p = (GAMMA - 1.0) * (uu[:, 3] - 0.5 * (uu[:, 1] ** 2 + uu[:, 2] ** 2) / uu[:, 0])
+    assert uu[:, 0].min() > 0.0 and p.min() > 0.0
+
+
+def test_oracle_curved_muscl_differs_from_first_order(oracle_mod, tl):
+    """MUSCL subcells change the blended elements' rhs once the state is no longer piecewise constant (on the
+    initial blast every minmod slope is zero)."""
+    N = 4
+    _, cm, o1 = make(oracle_mod, tl, N, cells=(8, 8), rec=0)
+    _, _, o2 = make(oracle_mod, tl, N, cells=(8, 8), rec=1)
+    u = blast_state(cm)
+    dt = o1.max_dt(u, 0.2)
+    np.testing.assert_array_equal(o1.rhs(u, 0.0, dt), o2.rhs(u, 0.0, dt))
+    o1.steps(u, 10, 0.2, 0.0, 1e9, nthreads=NTH)
+    dt = o1.max_dt(u, 0.2)
+    d1, d2 = o1.rhs(u, 0.0, dt).reshape(cm.n_elements, -1), o2.rhs(u, 0.0, dt).reshape(cm.n_elements, -1)
+    alpha = o1.get(6)
+    diff = np.abs(d1 - d2).max(axis=1)
+    assert diff[alpha > 0].max() > 1e-3
