@@ -188,6 +188,17 @@ int tlw_dd_begin(tlw_handle* h, double cfl, double fixed_dt, double t_end);
 int tlw_dd_volume(tlw_handle* h);
 int tlw_dd_finish(tlw_handle* h);
 
+/* Subcell reconstruction of the blended elements under shock capturing on a curvilinear mesh (the reference's
+ * VolumeIntegralFRShockCapturing(...; reconstruction), src/solvers/dgsem_tree/dg_2d.jl:251-365):
+ * TLW_RECONSTRUCTION_FIRST_ORDER (FirstOrderReconstruction, the default) or TLW_RECONSTRUCTION_MUSCL
+ * (MUSCLReconstruction: calcflux_muscl!, src/solvers/dgsem_structured/dg_2d.jl:176-311, first order on elements
+ * with a boundary face). Shock capturing on a curvilinear mesh follows the P4estMesh{2} path: LW, Rusanov surface
+ * flux, the blended interface flux of get_blended_flux / zhang_shu_flux_fix (src/solvers/dgsem_p4est/
+ * dg_2d.jl:199-250). TreeMesh shock capturing takes first-order subcells only. */
+#define TLW_RECONSTRUCTION_FIRST_ORDER 0
+#define TLW_RECONSTRUCTION_MUSCL 1
+int tlw_set_reconstruction(tlw_handle* h, int32_t reconstruction);
+
 /* Boundary faces of the curvilinear mesh (P4estMesh boundaries: element, face), after tlw_set_curved_mesh
  * (which clears them): elements 1-based, faces 0: -xi, 1: +xi, 2: -eta, 3: +eta (a face no interface covers),
  * kinds TLW_BC_SLIP_WALL_VERTICAL / _HORIZONTAL (the normal-direction slip walls of src/equations/equations.jl:

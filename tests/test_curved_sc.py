@@ -84,3 +84,89 @@ def test_oracle_curved_muscl_differs_from_first_order(oracle_mod, tl):
     alpha = o1.get(6)
     diff = np.abs(d1 - d2).max(axis=1)
     assert diff[alpha > 0].max() > 1e-3
+
+
+# ---------------------------------------------------------------------------------------------- GPU
+def sc_semi(tl, mesh, N, rec, bc=None):
+    eq = tl.CompressibleEulerEquations2D(GAMMA)
+    vi = tl.VolumeIntegralFRShockCapturing(tl.IndicatorHennemannGassner(alpha_max=0.5, alpha_min=0.001),
+                                           tl.VolumeIntegralFR(tl.LW()),
+                                           reconstruction=tl.MUSCLReconstruction() if rec else
+                                           tl.FirstOrderReconstruction())
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, vi)
+    kw = {} if bc is None else {"boundary_conditions": bc}
+    return tl.SemidiscretizationHyperbolic(mesh, tl.LW(), eq, tl.ConstantState(), solver, **kw)
+
+
+def gpu_rhs(tl, semi, u, dt):
+    semi.cache["dt"][0] = dt
+    du = np.empty_like(u)
+    tl.rhs(du, u, semi, 0.0)
+    return du
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,rec,rotated", [(3, 0, False), (4, 0, True), (5, 0, False), (3, 1, True), (4, 1, False),
+                                           (5, 1, True)])
+def test_gpu_curved_sc_rhs_matches_oracle(oracle_mod, tl, N, rec, rotated):
+    """One rhs of a blast that has run a few oracle steps (nonzero MUSCL slopes): blending factors, the
+    face-adjacent subcell fluxes and du against the oracle."""
+    from trixilw import _lib
+    m, cm, o = make(oracle_mod, tl, N, cells=(8, 8), rec=rec, rotate=rotated)
+    u = blast_state(cm)
+    o.steps(u, 6, 0.2, 0.0, 1e9, nthreads=NTH)
+    semi = sc_semi(tl, cm, N, rec)
+    dt = o.max_dt(u, 0.2)
+    assert semi.max_dt(u, 0.2) == pytest.approx(dt, rel=1e-13)
+    du_cpu = o.rhs(u, 0.0, dt)
+    du_gpu = gpu_rhs(tl, semi, u, dt)
+    alpha = o.get(6)
+    assert alpha.max() > 0.1
+    np.testing.assert_allclose(semi.get_cache(_lib.TLW_CACHE_ALPHA), alpha, rtol=1e-12, atol=1e-15)
+    fl_cpu, fl_gpu = o.get(7), semi.get_cache(_lib.TLW_CACHE_FN_LOW)
+    assert np.all(rel_l2(fl_gpu, fl_cpu) < 1e-12)
+    assert np.all(rel_l2(u + dt * du_gpu, u + dt * du_cpu) < 1e-12)
+    assert np.all(rel_l2(du_gpu, du_cpu) < 1e-10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rec", [0, 1])
+def test_gpu_curved_sc_steps_match_oracle(oracle_mod, tl, rec):
+    """20 CFL steps of the blast (N = 4, rotated element frames) on the device against the oracle."""
+    _, cm, o = make(oracle_mod, tl, 4, cells=(8, 8), rec=rec, rotate=True)
+    semi = sc_semi(tl, cm, 4, rec)
+    u0 = blast_state(cm)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, tl.LW(), (0.0, 1e9)))
+    integ.set_state(u0, 0.0)
+    integ.step(20, 0.2, use_graph=True)
+    integ.sync_time()
+    u_cpu = u0.copy()
+    s, t = o.steps(u_cpu, 20, 0.2, 0.0, 1e9, nthreads=NTH)
+    assert s == integ.iter == 20 and integ.t == pytest.approx(t, rel=1e-12)
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-11)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rec", [0, 1])
+def test_gpu_curved_sc_walls_match_oracle(oracle_mod, tl, rec):
+    """The blast in a warped box with slip walls: MUSCL falls back to first-order subcells on the elements
+    next to the walls; 10 steps against the oracle."""
+    N = 4
+    m = tl.StructuredMesh((8, 8), warp, periodicity=False)
+    cm = m.curved(N)
+    bc = {"x_neg": tl.boundary_condition_slip_wall_vertical, "x_pos": tl.boundary_condition_slip_wall_vertical,
+          "y_neg": tl.boundary_condition_slip_wall_horizontal, "y_pos": tl.boundary_condition_slip_wall_horizontal}
+    semi = sc_semi(tl, cm, N, rec, bc)
+    o = oracle_mod.Oracle(cm, N)
+    o.set_curved_boundaries(cm.boundary_elements, cm.boundary_faces,
+                            np.repeat(np.array([1, 1, 2, 2], dtype=np.int32), cm.n_boundaries_per_direction))
+    o.set_shock_capturing(True, alpha_max=0.5, alpha_min=0.001, alpha_smooth=True, reconstruction=rec)
+    u0 = blast_state(cm, center=(-5.0, 4.0))
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, tl.LW(), (0.0, 1e9)))
+    integ.set_state(u0, 0.0)
+    integ.step(10, 0.2, use_graph=False)
+    integ.sync_time()
+    u_cpu = u0.copy()
+    s, _ = o.steps(u_cpu, 10, 0.2, 0.0, 1e9, nthreads=NTH)
+    assert s == integ.iter == 10
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-11)

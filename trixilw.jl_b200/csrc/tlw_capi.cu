@@ -62,6 +62,8 @@ void free_mesh(tlw_handle* h) {
     dfree(h->d_us); dfree(h->d_in); dfree(h->d_in2); dfree(h->d_out);
     dfree(h->d_tU); dfree(h->d_tF); dfree(h->d_U2); dfree(h->d_F2);
     dfree(h->d_alpha); dfree(h->d_alpha_raw); dfree(h->d_tFn); dfree(h->d_il); dfree(h->d_ir);
+    dfree(h->d_subn); dfree(h->d_subq); dfree(h->d_mgeom);
+    if (h->d_atb) { cudaFree(h->d_atb); h->d_atb = nullptr; }
     free_adjoint(h->adj);
     dfree(h->d_Ja); dfree(h->d_ijn); dfree(h->d_cp); dfree(h->d_cs); dfree(h->d_cf);
     dfree(h->d_ml); dfree(h->d_mu); dfree(h->d_mg); dfree(h->d_ms);
@@ -121,6 +123,11 @@ struct Launch {
             cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        const int sc0 = (int)C::smem_bytes(8), sc1 = (int)C::smem_bytes(12);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc0);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc0);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc1);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc1);
         const int md = (int)C::smem_bytes(2);
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
@@ -146,6 +153,16 @@ struct Launch {
         if (grid == 0) return;
         if (a.temporal_errors) {   // Adaptive trial step: the depth-4 kernel with the error estimate
             if constexpr (N >= 4) lw_volume_kernel<N, MODE_STEP, false, 0, false, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
+            return;
+        }
+        if (a.metrics && sc) {   // curvilinear mesh, LW with shock capturing (MUSCL when the geometry is given)
+            if (a.muscl_geom) {
+                if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, 1><<<grid, C::THREADS, C::smem_bytes(12), s>>>(a);
+                else lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, 1><<<grid, C::THREADS, C::smem_bytes(12), s>>>(a);
+            } else {
+                if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, 0><<<grid, C::THREADS, C::smem_bytes(8), s>>>(a);
+                else lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, 0><<<grid, C::THREADS, C::smem_bytes(8), s>>>(a);
+            }
             return;
         }
         if (a.metrics) {   // curvilinear mesh (LW or MDRK, FR volume integral)
@@ -378,9 +395,12 @@ IndicatorArgs indicator_args(tlw_handle* h) {
 void enqueue_indicator(tlw_handle* h, const double* u, bool speed) {
     dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, speed, true,
                   indicator_args(h));
-    if (h->opts.alpha_smooth && h->ni > 0)
-        alpha_smooth_kernel<<<(h->ni + 255) / 256, 256, 0, h->stream>>>(h->d_il, h->d_ir, h->ni, h->d_alpha_raw,
-                                                                        h->d_alpha);
+    // interfaces for the smoothing: the TreeMesh list, or the curvilinear mesh's (primary, secondary) pairs
+    const int ni = h->curved ? (h->color_off.empty() ? 0 : h->color_off.back()) : h->ni;
+    if (h->opts.alpha_smooth && ni > 0)
+        alpha_smooth_kernel<<<(ni + 255) / 256, 256, 0, h->stream>>>(h->curved ? h->d_cp : h->d_il,
+                                                                    h->curved ? h->d_cs : h->d_ir, ni,
+                                                                    h->d_alpha_raw, h->d_alpha);
 }
 
 // the step's final values all come from the volume and interface kernels: the plain LW step on a periodic
@@ -453,6 +473,12 @@ void enqueue_curved_surfaces(tlw_handle* h, int mode, const double* u_jump, doub
     ca.inv_w_first = h->h_basis.inv_w_first;
     ca.inv_w_last = h->h_basis.inv_w_last;
     ca.status = &h->d_step->status;
+    if (h->sc) {
+        ca.alpha = h->d_alpha;
+        ca.tFn = h->d_tFn;
+        ca.w_first = h->h_basis.weights[0];
+        ca.w_last = h->h_basis.weights[h->n - 1];
+    }
     for (size_t c = 0; c + 1 < h->color_off.size(); ++c) {
         const int b = h->color_off[c];
         ca.p_elem = h->d_cp + b;
@@ -595,6 +621,12 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     if (h->curved) {
         va.metrics = h->d_Ja;
         va.inv_jac_node = h->d_ijn;
+        if (h->sc) {
+            va.subn = h->d_subn;
+            va.subq = h->d_subq;
+            va.atb = h->d_atb;
+            va.muscl_geom = h->reconstruction == 1 ? h->d_mgeom : nullptr;
+        }
     }
     if (phases & 1) {
         dispatch<Vol>(h->N, h->stream, stage, mode, h->sc, va);
@@ -683,6 +715,10 @@ void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const
         // the previous step left the per-element maxima of this state
         const int grid = std::min<int>((int)((h->E + 255) / 256), 4 * 148);
         cfl_slots_reduce_kernel<<<grid, 256, 0, h->stream>>>(h->d_slots, h->d_inv_jac, (int)h->E, h->d_step);
+    } else if (h->sc && h->curved) {
+        dispatch<CSpd>(h->N, h->stream, u, (const double*)h->d_Ja, (const double*)h->d_ijn, (int)h->E, h->opts.gamma,
+                       h->d_step);
+        enqueue_indicator(h, u, false);
     } else if (h->sc) enqueue_indicator(h, u, true);   // CFL reduction and indicator in one pass over u
     else if (h->parabolic) dispatch<ParSpd>(h->N, h->stream, (const tlw_handle*)h, u);   // (curvilinear too)
     else if (h->curved) dispatch<CSpd>(h->N, h->stream, u, (const double*)h->d_Ja, (const double*)h->d_ijn, (int)h->E,
@@ -900,13 +936,92 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
     return TLW_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Shock capturing on a curvilinear mesh: the subcell-face normals of every element (Trixi calcflux_fv! for
+// curved meshes: along xi, face f between nodes f-1 and f of row j has Ja^1(0, j) + sum_{k < f} w_k
+// sum_m D[k][m] Ja^1(m, j); along eta likewise), the normal the reference's calc_fn_low! takes for face n-1
+// (src/solvers/dgsem_structured/dg_2d.jl:111-174: the increments of faces 1 and n-1 only), the MUSCL geometry
+// (compute_subcells, src/solvers/dgsem_tree/dg_2d.jl:1806-1824) and the buffers of the blending.
+int upload_curved_subcells(tlw_handle* h, const double* Ja) {
+    const int n = h->n, nn = h->nn;
+    const int64_t E = h->E;
+    const tlw::Basis& b = h->h_basis;
+    std::vector<double> subn((size_t)E * 2 * n * (n - 1) * 2), subq((size_t)E * 2 * n * 2);
+    for (int64_t e = 0; e < E; ++e)
+        for (int d = 0; d < 2; ++d)
+            for (int line = 0; line < n; ++line) {
+                auto J = [&](int m, int c) {
+                    const int node = d == 0 ? m + n * line : line + n * m;
+                    return Ja[4 * ((size_t)e * nn + node) + 2 * d + c];
+                };
+                auto inc = [&](int k, double* o) {
+                    o[0] = o[1] = 0.0;
+                    for (int m = 0; m < n; ++m) {
+                        const double c = b.weights[k] * b.D[k * n + m];
+                        o[0] += c * J(m, 0);
+                        o[1] += c * J(m, 1);
+                    }
+                };
+                const size_t row = ((size_t)e * 2 + d) * n + line;
+                double nrm[2] = {J(0, 0), J(0, 1)}, q[2] = {J(0, 0), J(0, 1)}, o[2];
+                for (int f = 1; f < n; ++f) {
+                    inc(f - 1, o);
+                    nrm[0] += o[0];
+                    nrm[1] += o[1];
+                    subn[(row * (n - 1) + (f - 1)) * 2] = nrm[0];
+                    subn[(row * (n - 1) + (f - 1)) * 2 + 1] = nrm[1];
+                    if (f == 1 || f == n - 1) { q[0] += o[0]; q[1] += o[1]; }
+                }
+                subq[row * 2] = q[0];
+                subq[row * 2 + 1] = q[1];
+            }
+    std::vector<double> geom(2 * n + 3, -1.0);
+    double acc = 0.0;
+    for (int i = 1; i <= n; ++i) {
+        acc += b.weights[i - 1];
+        geom[i] = -1.0 + acc;
+    }
+    for (int i = 0; i < n; ++i) geom[n + 2 + i] = h->nodes[i];
+    geom[2 * n + 2] = 1.0;
+    int rc;
+    if ((rc = ensure(h, h->d_subn, subn.size())) || (rc = ensure(h, h->d_subq, subq.size())) ||
+        (rc = ensure(h, h->d_mgeom, geom.size())) || (rc = ensure(h, h->d_alpha, (size_t)E)) ||
+        (rc = ensure(h, h->d_alpha_raw, (size_t)E)) || (rc = ensure(h, h->d_tFn, trace_doubles(h))))
+        return rc;
+    TLW_CUDA(h, cudaMemcpy(h->d_subn, subn.data(), subn.size() * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, cudaMemcpy(h->d_subq, subq.data(), subq.size() * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, cudaMemcpy(h->d_mgeom, geom.data(), geom.size() * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, cudaMalloc(&h->d_atb, (size_t)E));
+    TLW_CUDA(h, cudaMemset(h->d_atb, 0, (size_t)E));
+    return TLW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tlw_set_reconstruction(tlw_handle* h, int32_t reconstruction) {
+    if (!h) return TLW_E_ARG;
+    if (reconstruction != TLW_RECONSTRUCTION_FIRST_ORDER && reconstruction != TLW_RECONSTRUCTION_MUSCL)
+        return fail(h, TLW_E_ARG, "reconstruction");
+    if (reconstruction == TLW_RECONSTRUCTION_MUSCL && (!h->sc || (h->have_mesh && !h->curved)))
+        return fail(h, TLW_E_UNSUPPORTED, "MUSCL subcells: shock capturing on a curvilinear mesh");
+    drop_graphs(h);
+    h->reconstruction = reconstruction;
+    return TLW_OK;
+}
+
 int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contravariant_vectors,
                         const double* inverse_jacobian, int64_t n_interfaces, const int64_t* primary_elements,
                         const int32_t* primary_faces, const int64_t* secondary_elements,
                         const int32_t* secondary_faces, const int32_t* secondary_reversed) {
     if (!h) return TLW_E_ARG;
-    if (h->sc || h->N < 3)
-        return fail(h, TLW_E_UNSUPPORTED, "curvilinear meshes: LW or MDRK with the FR volume integral, N >= 3");
+    if (h->N < 3) return fail(h, TLW_E_UNSUPPORTED, "curvilinear meshes: N >= 3");
+    if (h->sc && (h->opts.time_discretization != TLW_LW || h->opts.surface_flux != TLW_FLUX_RUSANOV))
+        return fail(h, TLW_E_UNSUPPORTED, "curvilinear shock capturing: LW with the Rusanov surface flux");
     if (n_elements <= 0 || n_elements > (int64_t)0x7fffffff / 64 || !contravariant_vectors || !inverse_jacobian)
         return fail(h, TLW_E_ARG, "n_elements / metrics");
     if (n_interfaces < 0 || (n_interfaces > 0 && (!primary_elements || !primary_faces || !secondary_elements ||
@@ -991,6 +1106,7 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
     if (h->opts.time_discretization == TLW_MDRK) {
         if ((rc = ensure(h, h->d_U2, sd)) || (rc = ensure(h, h->d_F2, 2 * sd)) || (rc = ensure(h, h->d_us, sd))) return rc;
     }
+    if (h->sc && (rc = upload_curved_subcells(h, contravariant_vectors))) return rc;
     h->curved = true;
     h->cur = 0;
     h->have_mesh = true;
@@ -1184,6 +1300,12 @@ int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t
         if ((rc = up(h->d_cbe, be[0], be[1])) || (rc = up(h->d_cbf, bf[0], bf[1])) || (rc = up(h->d_cbk, bk[0], bk[1])) ||
             (rc = up(h->d_cbi, bi[0], bi[1])))
             return rc;
+    }
+    if (h->d_atb) {
+        // shock capturing: calcflux_muscl! falls back to first-order subcells on elements with a boundary face
+        std::vector<unsigned char> atb((size_t)h->E, 0);
+        for (int64_t k = 0; k < n_boundaries; ++k) atb[(size_t)(elements[k] - 1)] = 1;
+        TLW_CUDA(h, cudaMemcpy(h->d_atb, atb.data(), atb.size(), cudaMemcpyHostToDevice));
     }
     return TLW_OK;
 }

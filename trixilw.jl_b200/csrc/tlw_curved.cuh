@@ -103,7 +103,76 @@ struct CurvedSurfArgs {
     double inv_w_first, inv_w_last;
     unsigned* status;
     const double* tFv;        // Navier-Stokes: contravariant viscous flux traces (or null)
+    // shock capturing (or null): blending factors [e] and the face-adjacent subcell fluxes fn_low [v, l, slot, e]
+    const double* alpha;
+    const double* tFn;
+    double w_first, w_last;
 };
+
+// zhang_shu_flux_fix (src/solvers/dgsem_p4est/dg_2d.jl:199-225): Fn is pulled towards the first-order fn until
+// the density, then the pressure, of the subcell update uprev - c (Fn - fn_inner) is no further from the
+// first-order update's than 9/10 of that value
+__device__ __forceinline__ void zhang_shu_flux_fix(double gm1, const double* uprev, const double* ulow, double* Fn,
+                                                   const double* fin, const double* fn, double c) {
+    double uh[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) uh[v] = uprev[v] - c * (Fn[v] - fin[v]);
+#pragma unroll
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) uh[v] = uprev[v] - c * (Fn[v] - fin[v]);
+        }
+        const double lo = pass == 0 ? ulow[0] : gm1 * (ulow[3] - 0.5 * (ulow[1] * ulow[1] + ulow[2] * ulow[2]) / ulow[0]);
+        const double hi = pass == 0 ? uh[0] : gm1 * (uh[3] - 0.5 * (uh[1] * uh[1] + uh[2] * uh[2]) / uh[0]);
+        const double eps = 0.1 * lo;
+        const double theta = julia_min(fabs(eps - lo) / (fabs(hi - lo) + 1e-13), 1.0);
+        if (theta < 1.0) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) Fn[v] = theta * Fn[v] + (1.0 - theta) * fn[v];
+        }
+    }
+}
+
+// get_blended_flux (src/solvers/dgsem_p4est/dg_2d.jl:227-250) at an interface node: Fn <- (1 - alp) Fn + alp fn
+// with fn = flux_lax_friedrichs(u_P, u_S, n) and alp = (alpha_P + alpha_S) / 2, then the Zhang-Shu fix on each
+// side whose subcell update is not admissible. As in prolong2interfaces! (:8-84), both sides' fn_inner come from
+// fn_low at the primary's node index l, and J^{-1} is the primary face node's for both.
+template <int N>
+__device__ __forceinline__ void blend_curved_flux(const CurvedSurfArgs& a, int pe, int se, int pf, int sf, int l, int np,
+                                                  const double* uP, const double* uS, const double* nrm, double* Fn) {
+    constexpr int n = N + 1, nn = n * n;
+    const double gm1 = a.gamma - 1.0;
+    double fP[NV], gP[NV], fS[NV], gS[NV], fn[NV], fil[NV], fir[NV];
+    euler_fluxes(gm1, uP[0], uP[1], uP[2], uP[3], fP, gP);
+    euler_fluxes(gm1, uS[0], uS[1], uS[2], uS[3], fS, gS);
+    const double lam = max_abs_speed_normal(a.gamma, uP, uS, nrm, a.speed_kind, a.status);
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+        fn[v] = 0.5 * ((fP[v] * nrm[0] + gP[v] * nrm[1]) + (fS[v] * nrm[0] + gS[v] * nrm[1])) + (-0.5 * lam * (uS[v] - uP[v]));
+    load4(a.tFn + (((size_t)pe * 4 + pf) * n + l) * NV, fil);
+    load4(a.tFn + (((size_t)se * 4 + sf) * n + l) * NV, fir);
+    const double alp = 0.5 * (__ldg(a.alpha + pe) + __ldg(a.alpha + se));
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Fn[v] = (1.0 - alp) * Fn[v] + alp * fn[v];
+    const double dt = *a.dt;
+    const double J = __ldg(a.inv_jac + (size_t)pe * nn + np);
+    double test[NV], low[NV];
+    const double cl = dt * J / (a.w_last * 0.5);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        test[v] = uP[v] - cl * (Fn[v] - fil[v]);
+        low[v] = uP[v] - cl * (fn[v] - fil[v]);
+    }
+    if (!admissible(gm1, test)) zhang_shu_flux_fix(gm1, uP, low, Fn, fil, fn, cl);
+    const double cr = -dt * J / (a.w_first * 0.5);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        test[v] = uS[v] - cr * (Fn[v] - fir[v]);
+        low[v] = uS[v] - cr * (fn[v] - fir[v]);
+    }
+    if (!admissible(gm1, test)) zhang_shu_flux_fix(gm1, uS, low, Fn, fir, fn, cr);
+}
 
 template <int N>
 static __global__ void __launch_bounds__(128) curved_interface_kernel(CurvedSurfArgs a) {
@@ -134,6 +203,7 @@ static __global__ void __launch_bounds__(128) curved_interface_kernel(CurvedSurf
         FS[v] *= -sgS;    // F_S . (-n_S)
     }
     lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, FP, FS, uP, uS, UP, US, nrm, Fn, a.status);
+    if (a.alpha) blend_curved_flux<N>(a, pe, se, pf, sf, l, np, uP, uS, nrm, Fn);
     if (a.tFv) {
         // minus the mean of both sides' viscous normal fluxes (calc_interface_flux_hyperbolic_parabolic!,
         // src/solvers/dgsem_p4est/dg_2d_parabolic.jl:1878-1958)

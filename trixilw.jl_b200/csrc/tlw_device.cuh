@@ -80,6 +80,11 @@ __device__ __forceinline__ void euler_flux_dir(double gm1, const double* u, int 
 }
 
 // sqrt that flags a negative argument instead of trapping
+// Julia min: a NaN argument propagates (fmin would drop it)
+__device__ __forceinline__ double julia_min(double a, double b) {
+    return a != a ? a : (b != b ? b : fmin(a, b));
+}
+
 __device__ __forceinline__ double checked_sqrt(double x, unsigned* status) {
     if (!(x >= 0.0)) atomicOr(status, STATUS_NONADMISSIBLE);
     return sqrt(x);

@@ -98,6 +98,10 @@ struct tlw_handle {
     double *d_alpha = nullptr, *d_alpha_raw = nullptr, *d_tFn = nullptr;
     int *d_il = nullptr, *d_ir = nullptr;   // all interfaces (smoothing)
     int ni = 0;
+    // curvilinear shock capturing: subcell normals, calc_fn_low! normals, boundary-element flags, MUSCL geometry
+    double *d_subn = nullptr, *d_subq = nullptr, *d_mgeom = nullptr;
+    unsigned char* d_atb = nullptr;
+    int reconstruction = 0;                 // 0 first-order subcells, 1 MUSCL (curvilinear meshes)
     double jac_first = 0.0;                 // inverse Jacobian of element 1 (TreeMesh interface cache)
     // Adaptive step control: per-element temporal errors, check scratch, tolerances of the trial in flight
     double* d_te = nullptr;

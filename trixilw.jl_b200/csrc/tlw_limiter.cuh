@@ -37,10 +37,6 @@ struct LimiterArgs {
     unsigned* status;
 };
 
-__device__ __forceinline__ double julia_min(double a, double b) {
-    return a != a ? a : (b != b ? b : fmin(a, b));
-}
-
 __device__ __forceinline__ double limiter_value(double gamma, int variable, const double* x) {
     if (variable == 0) return x[0];
     if (variable == 1) return (gamma - 1.0) * (x[3] - 0.5 * (x[1] * x[1] + x[2] * x[2]) / x[0]);

@@ -87,6 +87,14 @@ struct VolArgs {
     double* temporal_errors;          // [e]
     double abstol, reltol;
     double* dstore;                   // [m][e][v][node]: the stage derivatives d_1..d_depth (DSTORE kernels)
+    // shock capturing on curvilinear meshes: subcell-face normals [e][d][line][f - 1][2] (d 0: xi faces on row
+    // j, 1: eta faces on column i; f = 1..n-1), the normals the reference's calc_fn_low! takes for face n-1 of
+    // pure DG elements [e][d][line][2], elements with a boundary face [e] (MUSCL: first order there), and the
+    // MUSCL geometry: subcell faces [0..n] then the extended nodes [0..n+1] of the reference element
+    const double* subn;
+    const double* subq;
+    const unsigned char* atb;
+    const double* muscl_geom;
 };
 
 // curvilinear: contravariant fluxes f~ = Ja^1_1 f + Ja^1_2 g, g~ = Ja^2_1 f + Ja^2_2 g of a node
@@ -254,6 +262,196 @@ __device__ __forceinline__ void sc_blend(const VolArgs& a, const double* FVX, co
     }
 }
 
+// ---- shock capturing on curvilinear meshes, the reference's P4estMesh{2} path (src/solvers/dgsem_tree/
+// dg_2d.jl:236-365, src/solvers/dgsem_structured/dg_2d.jl:75-311; Trixi calcflux_fv! for curved meshes) ----
+// flux_lax_friedrichs(uL, uR, nrm) from the states, their physical fluxes, normal velocities and sound speeds
+__device__ __forceinline__ void sc_normal_flux(int speed_kind, const double* uL, const double* fL, const double* gL,
+                                               double vnL, double cL, const double* uR, const double* fR,
+                                               const double* gR, double vnR, double cR, const double* nrm,
+                                               double* out) {
+    const double nn = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1]);
+    const double lambda = speed_kind == 0 ? fmax(fabs(vnL), fabs(vnR)) + fmax(cL, cR) * nn
+                                          : fmax(fabs(vnL) + cL * nn, fabs(vnR) + cR * nn);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const double fnL = fL[v] * nrm[0] + gL[v] * nrm[1], fnR = fR[v] * nrm[0] + gR[v] * nrm[1];
+        out[v] = 0.5 * (fnL + fnR) + (-0.5 * lambda * (uR[v] - uL[v]));
+    }
+}
+
+// Julia sign
+__device__ __forceinline__ double julia_sign(double x) { return (x == 0.0 || isnan(x)) ? x : (x > 0.0 ? 1.0 : -1.0); }
+
+// minmod(a, b, 0) (src/solvers/dgsem_structured/dg_2d.jl:97-109): a NaN difference (0 / 0 at the element
+// edges, where the extended state copies the edge node) has no sign equal to the other's and gives 0
+__device__ __forceinline__ double minmod2(double a, double b) {
+    const double slope = julia_min(fabs(a), fabs(b));
+    const double s1 = julia_sign(a), s2 = julia_sign(b);
+    if (s1 != s2) return 0.0;
+    return s1 * slope;
+}
+
+// limit_variable_slope (src/equations/equations.jl:262-287), variable 0 density, 1 pressure
+__device__ __forceinline__ double sc_limit_value(double gm1, int variable, const double* u) {
+    return variable == 0 ? u[0] : gm1 * (u[3] - 0.5 * (u[1] * u[1] + u[2] * u[2]) / u[0]);
+}
+__device__ __forceinline__ void limit_variable_slope(double gm1, int variable, double* slope, double* usl, double* usr,
+                                                     const double* ue, double xl, double xr) {
+    const double vsl = sc_limit_value(gm1, variable, usl), vsr = sc_limit_value(gm1, variable, usr);
+    const double vlow = sc_limit_value(gm1, variable, ue);
+    const double threshold = 0.1 * vlow;
+    if (vsl < 1e-10 || vsr < 1e-10) {
+        const double rl = fabs(threshold - vlow) / (fabs(vsl - vlow) + 1e-13);
+        const double rr = fabs(threshold - vlow) / (fabs(vsr - vlow) + 1e-13);
+        const double theta = julia_min(julia_min(rl, rr), 1.0);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            slope[v] *= theta;
+            usl[v] = ue[v] + (2.0 * theta) * (xl * slope[v]);
+            usr[v] = ue[v] + (2.0 * theta) * (xr * slope[v]);
+        }
+    }
+}
+
+// MUSCL face values of node (i, j) (calcflux_muscl!, dgsem_structured/dg_2d.jl:196-253 with limit_slope,
+// src/equations/compressible_euler_2d.jl:9-21): minmod slopes of the element-local extended state, limited for
+// density then pressure; into the UF regions k = 0 left, 1 right, 2 down, 3 up
+template <int N, class C>
+__device__ __forceinline__ void sc_muscl_faces(const double* UU, double* UF, const double* geom, int el, int i, int j,
+                                               double gm1) {
+    constexpr int n = C::n;
+    constexpr int PV = C::EB * C::P;
+    const double* sf = geom;           // subcell faces [0..n]
+    const double* xe = geom + n + 1;   // extended nodes [0..n+1]
+    auto at = [&](int ii, int jj, int v) {
+        ii = ii < 0 ? 0 : (ii > n - 1 ? n - 1 : ii);
+        jj = jj < 0 ? 0 : (jj > n - 1 ? n - 1 : jj);
+        return UU[v * PV + el * C::P + ii + C::R * jj];
+    };
+    const int I = i + 1, J = j + 1;
+    const double dx1 = __ldg(xe + I) - __ldg(xe + I - 1), dx2 = __ldg(xe + I + 1) - __ldg(xe + I);
+    const double dy1 = __ldg(xe + J) - __ldg(xe + J - 1), dy2 = __ldg(xe + J + 1) - __ldg(xe + J);
+    double u_[NV], sx[NV], sy[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        u_[v] = at(i, j, v);
+        sx[v] = minmod2((u_[v] - at(i - 1, j, v)) / dx1, (at(i + 1, j, v) - u_[v]) / dx2);
+        sy[v] = minmod2((u_[v] - at(i, j - 1, v)) / dy1, (at(i, j + 1, v) - u_[v]) / dy2);
+    }
+    const double xl = __ldg(sf + I - 1) - __ldg(xe + I), xr = __ldg(sf + I) - __ldg(xe + I);
+    const double yl = __ldg(sf + J - 1) - __ldg(xe + J), yr = __ldg(sf + J) - __ldg(xe + J);
+    double a[NV], b[NV];
+    const int o = el * C::P + i + C::R * j;
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+        double* s = d == 0 ? sx : sy;
+        const double lo = d == 0 ? xl : yl, hi = d == 0 ? xr : yr;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            a[v] = u_[v] + 2.0 * s[v] * lo;
+            b[v] = u_[v] + 2.0 * s[v] * hi;
+        }
+        limit_variable_slope(gm1, 0, s, a, b, u_, lo, hi);
+        limit_variable_slope(gm1, 1, s, a, b, u_, lo, hi);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            UF[(2 * d) * C::PLANES + v * PV + o] = u_[v] + s[v] * lo;
+            UF[(2 * d + 1) * C::PLANES + v * PV + o] = u_[v] + s[v] * hi;
+        }
+    }
+}
+
+// final stage on a curvilinear mesh: the subcell flux on the node's left (xi) and lower (eta) face along the
+// subcell normal; pure DG elements only need faces 1 and n-1, the latter with the reference's calc_fn_low!
+// normal; MUSCL elements take the reconstructed face values (their fluxes and speeds computed here)
+template <int N, class C, int REC>
+__device__ __forceinline__ void sc_faces_curved(const VolArgs& a, const double* UU, const double* VC, const double* F0X,
+                                                const double* F0Y, const double* UF, double* FVX, double* FVY, int el,
+                                                int e, int i, int j, bool blended, bool muscl) {
+    constexpr int n = C::n;
+    constexpr int PV = C::EB * C::P;
+    const double gm1 = a.gamma - 1.0;
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+        const int f = d == 0 ? i : j, line = d == 0 ? j : i;
+        if (f < 1 || (!blended && f != 1 && f != n - 1)) continue;
+        const double* np = (!blended && f == n - 1)
+                               ? a.subq + (((size_t)e * 2 + d) * n + line) * 2
+                               : a.subn + ((((size_t)e * 2 + d) * n + line) * (n - 1) + (f - 1)) * 2;
+        const double nrm[2] = {__ldg(np), __ldg(np + 1)};
+        const int aL = el * C::P + (d == 0 ? i - 1 : i) + C::R * (d == 0 ? j : j - 1);
+        const int aR = el * C::P + i + C::R * j;
+        double uL[NV], uR[NV], fL[NV], gL[NV], fR[NV], gR[NV], vnL, vnR, cL, cR, out[NV];
+        if (REC == 1 && muscl) {
+            // the right (up) face value of the node before the face, the left (down) one of the node after it
+            const double* PL = UF + (d == 0 ? 1 : 3) * C::PLANES;
+            const double* PR = UF + (d == 0 ? 0 : 2) * C::PLANES;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) { uL[v] = PL[v * PV + aL]; uR[v] = PR[v * PV + aR]; }
+            euler_fluxes(gm1, uL[0], uL[1], uL[2], uL[3], fL, gL);
+            euler_fluxes(gm1, uR[0], uR[1], uR[2], uR[3], fR, gR);
+            const double irL = 1.0 / uL[0], irR = 1.0 / uR[0];
+            const double v1L = uL[1] * irL, v2L = uL[2] * irL, v1R = uR[1] * irR, v2R = uR[2] * irR;
+            cL = checked_sqrt(a.gamma * (gm1 * (uL[3] - 0.5 * (uL[1] * v1L + uL[2] * v2L))) * irL, a.status);
+            cR = checked_sqrt(a.gamma * (gm1 * (uR[3] - 0.5 * (uR[1] * v1R + uR[2] * v2R))) * irR, a.status);
+            vnL = v1L * nrm[0] + v2L * nrm[1];
+            vnR = v1R * nrm[0] + v2R * nrm[1];
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                uL[v] = UU[v * PV + aL]; uR[v] = UU[v * PV + aR];
+                fL[v] = F0X[v * PV + aL]; gL[v] = F0Y[v * PV + aL];
+                fR[v] = F0X[v * PV + aR]; gR[v] = F0Y[v * PV + aR];
+            }
+            vnL = VC[aL] * nrm[0] + VC[PV + aL] * nrm[1];
+            vnR = VC[aR] * nrm[0] + VC[PV + aR] * nrm[1];
+            cL = VC[2 * PV + aL];
+            cR = VC[2 * PV + aR];
+        }
+        sc_normal_flux(a.speed_kind, uL, fL, gL, vnL, cL, uR, fR, gR, vnR, cR, nrm, out);
+        double* dst = d == 0 ? FVX : FVY;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) dst[v * PV + aR] = out[v];
+    }
+}
+
+// epilogue on a curvilinear mesh: acc <- (1 - alpha) acc (+ alpha fv on blended elements); fn_low of the four
+// faces in load_fn_low!'s P4estMesh order (slot 0 bottom, 1 right, 2 top, 3 left)
+template <int N, class C>
+__device__ __forceinline__ void sc_blend_curved(const VolArgs& a, const double* FVX, const double* FVY, int el, int e,
+                                                int i, int j, double alpha, bool blended, double* acc) {
+    constexpr int n = C::n;
+    constexpr int PV = C::EB * C::P;
+    const int base = el * C::P;
+    if (blended) {
+        const double iwi = 1.0 / c_tlw_w[N][i], iwj = 1.0 / c_tlw_w[N][j];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const double xr = i + 1 < n ? FVX[v * PV + base + (i + 1) + C::R * j] : 0.0;
+            const double xl = i >= 1 ? FVX[v * PV + base + i + C::R * j] : 0.0;
+            const double yt = j + 1 < n ? FVY[v * PV + base + i + C::R * (j + 1)] : 0.0;
+            const double yb = j >= 1 ? FVY[v * PV + base + i + C::R * j] : 0.0;
+            const double fv = iwi * (xr - xl) + iwj * (yt - yb);
+            acc[v] = (1.0 - alpha) * acc[v] + alpha * fv;
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[v] = (1.0 - alpha) * acc[v];
+    }
+    const size_t tb = (size_t)e * 4 * n * NV;
+    double f[NV];
+    if (i == 1 || i == n - 1) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = FVX[v * PV + base + i + C::R * j];
+        store4(a.tFn + tb + ((i == 1 ? 3 : 1) * n + j) * NV, f);
+    }
+    if (j == 1 || j == n - 1) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) f[v] = FVY[v * PV + base + i + C::R * j];
+        store4(a.tFn + tb + ((j == 1 ? 0 : 2) * n + i) * NV, f);
+    }
+}
+
 // out/traces epilogue shared by all volume kernels. acc = Dhat-contraction of (F, G).
 template <int n, int MODE>
 __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, int j, int node, double ij, double dt,
@@ -298,9 +496,10 @@ __device__ __forceinline__ void store_stage_derivative(const VolArgs& a, int m, 
     for (int v = 0; v < NV; ++v) p[v * nn] = d[v];
 }
 
-template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false>
+// REC (curvilinear shock capturing): 0 first-order subcells, 1 MUSCL subcells
+template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false, int REC = 0>
 static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
-    static_assert(!(SC && CURVED), "shock capturing is built for TreeMesh only");
+    static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     static_assert(!TE || (N >= 4 && !SC && !CURVED), "temporal errors: depth-4 TreeMesh kernel");
     static_assert(!DSTORE || (!SC && !CURVED && !TE), "stored stage derivatives: the plain TreeMesh kernel");
     using C = VolCfg<N, EBX>;
@@ -319,6 +518,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     double* VC = UU + C::PLANES;
     double* FVX = VC + C::PLANES;
     double* FVY = FVX + C::PLANES;
+    double* UF = FVY + C::PLANES;      // curvilinear MUSCL: face values, 4 regions (left, right, down, up)
 
     const int tid = threadIdx.x;
     const double gm1 = a.gamma - 1.0;
@@ -327,6 +527,15 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     const int i = node % n, j = node / n;
     const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
+    // curvilinear shock capturing: pure_and_blended_element_ids! (DG only where alpha is within 1e-12 of 0);
+    // MUSCL subcells on blended elements without a boundary face
+    double alpha_e = 0.0;
+    bool blended = false, muscl = false;
+    if (SC && CURVED && active) {
+        alpha_e = __ldg(a.alpha + e);
+        blended = !(fabs(alpha_e) <= 1e-12);
+        muscl = REC == 1 && blended && !__ldg(a.atb + e);
+    }
     // dt of this element's instance (batched form) or the single dt
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
     // per-element maxima of the interior nodes' speeds for the next step's CFL (plain LW step only)
@@ -374,6 +583,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     __syncthreads();
     line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
+    if (SC && CURVED && REC == 1 && muscl) sc_muscl_faces<N, C>(UU, UF, a.muscl_geom, el, i, j, gm1);
 
     // stage 1: ut; perturbed states; f_t (dg_2d.jl:972-1023 / :725-775 / :543-582 / :417-454)
     if (active) {
@@ -561,7 +771,10 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
             for (int v = 0; v < NV; ++v) { F[v] = ft[v]; G[v] = gt[v]; }
         }
         node_put<N, C>(X, Y, el, i, j, F, G);
-        if (SC) sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
+        if (SC) {
+            if constexpr (CURVED) sc_faces_curved<N, C, REC>(a, UU, VC, F0X, F0Y, UF, FVX, FVY, el, e, i, j, blended, muscl);
+            else sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
+        }
     }
     __syncthreads();
     line_contract<N, C, true>(X, Y, tid);
@@ -570,7 +783,10 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>
     if (active) {
         double acc[NV], o[NV];
         node_sum<N, C>(X, Y, el, i, j, acc);
-        if (SC) sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
+        if (SC) {
+            if constexpr (CURVED) sc_blend_curved<N, C>(a, FVX, FVY, el, e, i, j, alpha_e, blended, acc);
+            else sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
+        }
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o);
         if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) node_speeds(a.gamma, o, a.status, l1, l2);
     }

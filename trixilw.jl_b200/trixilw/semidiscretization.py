@@ -95,19 +95,32 @@ class IndicatorHennemannGassner:
             raise NotImplementedError("only the density_pressure indicator variable is built")
 
 
+class FirstOrderReconstruction:
+    """FirstOrderReconstruction(): first-order subcells of the blended elements."""
+
+
+class MUSCLReconstruction:
+    """MUSCLReconstruction(): minmod-limited MUSCL subcells (curvilinear meshes)."""
+
+
 @dataclass
 class VolumeIntegralFRShockCapturing:
     """VolumeIntegralFRShockCapturing(indicator; volume_integralFR, volume_flux_fv, reconstruction)
-    (src/solvers/fr.jl:59-86). Built: volume_flux_fv = flux_lax_friedrichs and
-    reconstruction = FirstOrderReconstruction()."""
+    (src/solvers/fr.jl:59-86). Built: volume_flux_fv = flux_lax_friedrichs; reconstruction =
+    FirstOrderReconstruction() (every mesh) or MUSCLReconstruction() (curvilinear meshes), given as an instance
+    or by name."""
     indicator: IndicatorHennemannGassner = field(default_factory=IndicatorHennemannGassner)
     volume_integralFR: VolumeIntegralFR = field(default_factory=VolumeIntegralFR)
     volume_flux_fv: object = field(default_factory=FluxLaxFriedrichs)
-    reconstruction: str = "FirstOrderReconstruction"
+    reconstruction: object = "FirstOrderReconstruction"
 
     def __post_init__(self):
-        if self.reconstruction != "FirstOrderReconstruction":
-            raise NotImplementedError("only FirstOrderReconstruction subcells are built")
+        name = self.reconstruction if isinstance(self.reconstruction, str) else type(self.reconstruction).__name__
+        codes = {"FirstOrderReconstruction": _lib.TLW_RECONSTRUCTION_FIRST_ORDER,
+                 "MUSCLReconstruction": _lib.TLW_RECONSTRUCTION_MUSCL}
+        if name not in codes:
+            raise NotImplementedError(f"{name} subcells are not built")
+        self.reconstruction_code = codes[name]
 
     @property
     def time_discretization(self):
@@ -317,6 +330,8 @@ class SemidiscretizationHyperbolic:
             opts.volume_integral = _lib.TLW_VOLUME_FR
         self._handle = _Handle(opts)
         self._upload_mesh()
+        if isinstance(vi, VolumeIntegralFRShockCapturing):
+            check(self.handle, lib().tlw_set_reconstruction(self.handle, vi.reconstruction_code))
         self._bdata_key = None
         self.node_coordinates = (self.curved.xy if self.curved is not None
                                  else mesh.node_coordinates(self.polydeg))
