@@ -170,3 +170,27 @@ def test_gpu_curved_sc_walls_match_oracle(oracle_mod, tl, rec):
     s, _ = o.steps(u_cpu, 10, 0.2, 0.0, 1e9, nthreads=NTH)
     assert s == integ.iter == 10
     assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-11)
+
+
+@pytest.mark.gpu
+def test_gpu_curved_sc_with_positivity_limiter_matches_oracle(oracle_mod, tl):
+    """MUSCL shock capturing with the Zhang-Shu limiter after every step (twice per LW step, as solve_lwfr), as
+    the reference's curvilinear shock elixirs run; thresholds high enough that it acts. 8 steps."""
+    from trixilw import limiters
+    N = 4
+    _, cm, o = make(oracle_mod, tl, N, cells=(8, 8), rec=1, rotate=True)
+    semi = sc_semi(tl, cm, N, 1)
+    u0 = blast_state(cm, p_in=100.0)
+    thr = (0.13, 1.05)
+    o.set_positivity_limiter(thr, (0, 1))
+    u_cpu = o.apply_positivity_limiter(u0)
+    assert not np.array_equal(u_cpu, u0)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, tl.LW(), (0.0, 1e9)))
+    integ.set_state(u0, 0.0)
+    limiters.install(semi, (tl.PositivityPreservingLimiterZhangShu(thr, (tl.density, tl.pressure)),))
+    tl._lib.check(semi.handle, tl._lib.lib().tlw_apply_positivity_limiter(semi.handle))
+    integ.step(8, 0.2, use_graph=True)
+    integ.sync_time()
+    s, t = o.steps(u_cpu, 8, 0.2, 0.0, 1e9, nthreads=NTH)
+    assert s == integ.iter == 8 and integ.t == pytest.approx(t, rel=1e-12)
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-11)
