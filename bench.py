@@ -44,7 +44,24 @@ WORKLOADS = {
     # compressible Navier-Stokes lid-driven cavity (Re 1000, Ma 0.1, Pr 0.72): [0, 1]^2 with 64 x 64 elements
     # warped by x += 0.05 sin(pi x) sin(pi y) (same for y), slip walls + no-slip adiabatic walls, lid v1 = 1
     "cavity_warped64_N4_ns": (6, 4, "lw", "cavity"),
+    # shock capturing on the warped 512 x 512 StructuredMesh (the reference's P4estMesh path): a circular blast
+    # (rho 1 / 0.125, p 10 / 1 at radius 3 around (0.5, -0.7)), Hennemann-Gassner blending (alpha_max 0.5) with
+    # MUSCL subcells
+    "blast_warped512_N4_muscl": (9, 4, "lw", "blast"),
 }
+
+
+class Blast:
+    """Circular blast at rest: (rho, p) = (1, 10) inside radius 3 around (0.5, -0.7), (0.125, 1) outside."""
+
+    time_independent = True
+
+    def __call__(self, x, y, t, eq):
+        import numpy as np
+        x, y = np.broadcast_arrays(np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64))
+        inside = (x - 0.5) ** 2 + (y + 0.7) ** 2 < 9.0
+        z = np.zeros(x.shape)
+        return eq.prim2cons(np.where(inside, 1.0, 0.125), z, z, np.where(inside, 10.0, 1.0))
 CAVITY_MU, CAVITY_PR, CAVITY_P0 = 0.001, 0.72, 1.0 / (0.1 ** 2 * 1.4)
 # batched form: 512 independent vortex instances (per-instance seed 0..511: side from {8, 16, 32, 64}
 # elements, degree from {3, 4, 5}, strength ~ U[1, 5], centre ~ U[-2, 2]^2), 50 LW steps
@@ -66,12 +83,16 @@ def alg_bytes_per_element_step(N: int, td: str, curved: bool = False) -> float:
     return 2 * b + 8 * nv * 6 * n * n if td == "mdrk" else b
 
 
-def volume_kernel_bytes_per_element(N: int, td: str, curved: bool = False) -> float:
+def volume_kernel_bytes_per_element(N: int, td: str, curved: bool = False, sc: bool = False) -> float:
     """Algorithmic bytes of one LW volume-kernel launch per element: read u (nv n^2), write u_new
     (nv n^2), write the face traces of U and F.n (2 x 4 faces x n x nv); curvilinear: read Ja and J^-1
-    (5 n^2)."""
+    (5 n^2); shock capturing: write the fn_low traces (4 faces x n x nv), and on curvilinear meshes read the
+    subcell normals (2 directions x n lines x (n - 1) faces x 2, and 2 x n x 2 for the calc_fn_low! normal)."""
     n, nv = N + 1, 4
-    return 8.0 * (2 * nv * n * n + 2 * 4 * n * nv + (5 * n * n if curved else 0))
+    b = 2 * nv * n * n + 2 * 4 * n * nv + (5 * n * n if curved else 0)
+    if sc:
+        b += 4 * n * nv + (4 * n * (n - 1) + 4 * n if curved else 0)
+    return 8.0 * b
 
 
 def ns_volume_bytes_per_element(N: int) -> float:
@@ -190,7 +211,7 @@ def make_mesh(tl, level, icname):
     if icname == "cavity":
         m = 1 << level
         return tl.StructuredMesh((m, m), cavity_mapping, periodicity=False)
-    if icname == "warped":
+    if icname in ("warped", "blast"):
         m = 1 << level
         return tl.StructuredMesh((m, m), warp_mapping)
     if icname == "vortex":
@@ -205,6 +226,11 @@ def build_semi(tl, level, N, td, icname, device):
     if icname == "warped":
         return tl.SemidiscretizationHyperbolic(make_mesh(tl, level, icname), tdo, eq, tl.IsentropicVortex(5.0),
                                                solver, device=device)
+    if icname == "blast":
+        vi = tl.VolumeIntegralFRShockCapturing(tl.IndicatorHennemannGassner(alpha_max=0.5), tl.VolumeIntegralFR(tdo),
+                                               reconstruction=tl.MUSCLReconstruction())
+        return tl.SemidiscretizationHyperbolic(make_mesh(tl, level, icname), tdo, eq, Blast(),
+                                               tl.DGSEM(N, tl.flux_lax_friedrichs, vi), device=device)
     if icname == "cavity":
         eq_par = tl.CompressibleNavierStokesDiffusion2D(eq, mu=CAVITY_MU, Prandtl=CAVITY_PR,
                                                         gradient_variables=tl.GradientVariablesConservative())
@@ -258,8 +284,8 @@ def cpu_oracle_rate(level, N, td, icname, steps_hint, budget_s=20.0):
     eq = tl.CompressibleEulerEquations2D(1.4)
     mesh = make_mesh(tl, level, icname)
     ic = (tl.FourQuadrantRiemann() if icname == "riemann" else cavity_ic(tl) if icname == "cavity"
-          else tl.IsentropicVortex(5.0))
-    xy = mesh.curved(N).xy if icname in ("warped", "cavity") else mesh.node_coordinates(N)
+          else Blast() if icname == "blast" else tl.IsentropicVortex(5.0))
+    xy = mesh.curved(N).xy if icname in ("warped", "cavity", "blast") else mesh.node_coordinates(N)
     u = np.ascontiguousarray(np.transpose(ic(xy[0], xy[1], 0.0, eq), (2, 1, 0, 3))).reshape(-1)
     o = pyoracle.Oracle(mesh, N)
     if icname == "cavity":
@@ -277,9 +303,11 @@ def cpu_oracle_rate(level, N, td, icname, steps_hint, budget_s=20.0):
         o.set_boundary_data(np.repeat(now[:, :, None, :], N + 1, axis=2), now)
     threads = os.cpu_count() or 1
     kind = 0 if td == "lw" else 1
-    cfl = RIEMANN_CFL if icname == "riemann" else cfl_for(N)
+    cfl = RIEMANN_CFL if icname in ("riemann", "blast") else cfl_for(N)
     if icname == "riemann":
         o.set_shock_capturing(True, 0.5, 0.001, True)
+    if icname == "blast":
+        o.set_shock_capturing(True, 0.5, 0.001, True, reconstruction=1)
     t0 = time.perf_counter()
     o.steps(u, 1, cfl, 0.0, 1e9, kind=kind, nthreads=threads)
     one = time.perf_counter() - t0
@@ -414,7 +442,7 @@ def run_ours(args):
     level, N, td, icname = WORKLOADS[args.workload]
     semi = build_semi(tl, level, N, td, icname, local_rank)
     ndofs = semi.ndofs()
-    cfl = RIEMANN_CFL if icname == "riemann" else cfl_for(N)
+    cfl = RIEMANN_CFL if icname in ("riemann", "blast") else cfl_for(N)
     u0 = semi.compute_coefficients(0.0)
     upd = tl.semidiscretize(semi, semi.time_discretization, (0.0, 1e9))
     integ = tl.LWIntegrator(upd)
@@ -494,16 +522,18 @@ def run_ours(args):
 
     if rank == 0:
         E = semi.mesh.n_elements
-        curved = icname in ("warped", "cavity")
+        curved = icname in ("warped", "cavity", "blast")
         ns = icname == "cavity"
+        sc = icname in ("riemann", "blast")
         peak, peak_kind = measured_peaks()
         vol_ms = phase[1] / args.steps
-        vol_bytes = (ns_volume_bytes_per_element(N) if ns else volume_kernel_bytes_per_element(N, td, curved)) * E
+        vol_bytes = (ns_volume_bytes_per_element(N) if ns else volume_kernel_bytes_per_element(N, td, curved, sc)) * E
         achieved = vol_bytes / (vol_ms * 1e-3) / 1e9
         fp = ctypes.c_double()
         fp64_peak = fp.value if L.tlw_probe_fp64_tflops(local_rank, ctypes.byref(fp)) == 0 else None
-        vol_flops = None if ns else volume_flops_per_node(N) * ndofs
+        vol_flops = None if (ns or sc) else volume_flops_per_node(N) * ndofs
         tag = (f"par_volume_kernel_N{N}_cavity{1 << level}" if ns
+               else f"lw_volume_kernel_N{N}_blast_muscl{1 << level}" if icname == "blast"
                else f"lw_volume_kernel_N{N}_{'warped' if curved else 'tree'}{1 << level}")
         traffic = profile_traffic(tag)
         step_alg = alg_bytes_per_element_step(N, td, curved) * E
@@ -518,7 +548,8 @@ def run_ours(args):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                     "steps": n_e2e},
             "roofline": {"kernel": (f"grad_volume_kernel + curved_grad_*_kernel + par_volume_kernel<{N}, MODE_STEP, CURVED>"
-                                    if ns else f"lw_volume_kernel<{N}, MODE_STEP{', CURVED' if curved else ''}>"),
+                                    if ns else f"lw_volume_kernel<{N}, MODE_STEP, SC, CURVED, MUSCL>" if icname == "blast"
+                                    else f"lw_volume_kernel<{N}, MODE_STEP{', SC' if sc else ''}{', CURVED' if curved else ''}>"),
                          "bound": "hbm",
                          "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
@@ -528,7 +559,7 @@ def run_ours(args):
                                    "frac": (vol_flops / (vol_ms * 1e-3) / 1e12) / fp64_peak if fp64_peak else None,
                                    "peak_source": "measured live (register FMA loop)"} if vol_flops else
                                   {"achieved_tflops": None, "peak_tflops": fp64_peak,
-                                   "note": "no algorithmic flop model for the Navier-Stokes kernels"}),
+                                   "note": "no algorithmic flop model for the Navier-Stokes or the shock-capturing kernels"}),
                          "step": {"alg_bytes_per_step": step_alg,
                                   "achieved_gbs": step_alg * args.steps / (ms_max * 1e-3) / 1e9,
                                   "frac": step_alg * args.steps / (ms_max * 1e-3) / 1e9 / peak},
@@ -537,6 +568,7 @@ def run_ours(args):
                                                "step": phase[4] / args.steps}},
             "clocks": clocks,
             "gpu_launches": args.steps * ((9 + 2 * int(L.tlw_curved_colors(semi.handle))) if ns else
+                                          (5 + int(L.tlw_curved_colors(semi.handle))) if icname == "blast" else
                                           (2 + (3 + (2 if semi.mesh.n_boundaries else 0)) * (2 if td == "mdrk" else 1)
                                            + (1 if icname == "riemann" else 0))),
         }

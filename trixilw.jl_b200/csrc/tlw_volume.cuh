@@ -47,6 +47,8 @@ struct VolCfg {
     // 4 % faster than 4 CTAs at 128 registers on the N = 4 workload; 6 CTAs spill)
     static constexpr int MIN_BLOCKS = THREADS <= 128 ? TLW_VOLUME_MIN_BLOCKS : 2;
     static constexpr int MDRK_MIN_BLOCKS = THREADS <= 128 ? 5 : 2;
+    // curvilinear shock capturing (subcell normals, MUSCL face values): 4 CTAs of 128 threads, 128 registers
+    static constexpr int SC_CURVED_MIN_BLOCKS = THREADS <= 128 ? 4 : 2;
     // plane layout: node (i, j) of (variable v, element e) at (v*EB + e)*P + i + R*j
     static constexpr int R = n;
     static constexpr int P = n == 4 ? 19 : nn;
@@ -498,7 +500,9 @@ __device__ __forceinline__ void store_stage_derivative(const VolArgs& a, int m, 
 
 // REC (curvilinear shock capturing): 0 first-order subcells, 1 MUSCL subcells
 template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false, int REC = 0>
-static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, VolCfg<N, EBX>::MIN_BLOCKS) lw_volume_kernel(VolArgs a) {
+static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED) ? VolCfg<N, EBX>::SC_CURVED_MIN_BLOCKS
+                                                                                 : VolCfg<N, EBX>::MIN_BLOCKS)
+    lw_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     static_assert(!TE || (N >= 4 && !SC && !CURVED), "temporal errors: depth-4 TreeMesh kernel");
     static_assert(!DSTORE || (!SC && !CURVED && !TE), "stored stage derivatives: the plain TreeMesh kernel");
