@@ -50,8 +50,7 @@ void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, do
         return;
     }
     if (h->opt.shock_capturing) {
-        if (kind != 0) throw std::runtime_error("curvilinear shock capturing: LW only");
-        rhs_curved_sc(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, bd);
+        rhs_curved_sc(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, bd, kind, u2);
         return;
     }
     rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, kind, u2, bd);

@@ -304,10 +304,14 @@ inline void get_blended_flux(const Basis& b, const Euler& eq, const double* u_ll
     if (!eq.is_admissible(test)) zhang_shu_flux_fix(eq, u_rr, low, Fn, fir, fn, c_rr);
 }
 
-// du = rhs(u) of the LW step with VolumeIntegralFRShockCapturing on a conforming curvilinear mesh (Rusanov
-// surface flux); the factors of the call are left in ws.alpha.
+// du = rhs(u) with VolumeIntegralFRShockCapturing on a conforming curvilinear mesh (Rusanov surface flux); the
+// factors of the call are left in ws.alpha. kind 0: LW; 1: rhs_mdrk1!; 2: rhs_mdrk2! with the stage state u2 in
+// the DG volume terms (calc_volume_integral_mdrk1! / _mdrk2!, src/solvers/dgsem_tree/multi_derivative_2d.jl:
+// 150-262: the indicator and the subcells take u in both stages; the interfaces blend with the full dt and the
+// instantaneous u, the boundaries of stage 1 halve their time averages).
 inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m, const double* u,
-                          double* du, double dt, Workspace& ws, int nthreads = 1, const BoundaryData* bd = nullptr) {
+                          double* du, double dt, Workspace& ws, int nthreads = 1, const BoundaryData* bd = nullptr,
+                          int kind = 0, const double* u2 = nullptr) {
     if (opt.flux_kind != RUSANOV) throw std::invalid_argument("curvilinear shock capturing: Rusanov surface flux");
     const int n = b.n, nn = n * n;
     const size_t ndof = (size_t)NV * nn * m.n_elements;
@@ -317,6 +321,11 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
     ws.surface_flux_values.assign((size_t)NV * n * 4 * m.n_elements, nan);
     ws.fn_low.assign((size_t)NV * n * 4 * m.n_elements, 0.0);
     ws.bad = false;
+    if (kind == 1) {
+        ws.U2.assign(ndof, nan);
+        ws.F2.assign(2 * ndof, nan);
+    }
+    if (kind == 2 && (ws.U2.size() != ndof || !u2)) throw std::invalid_argument("rhs_mdrk2 before rhs_mdrk1");
     for (size_t k = 0; k < ndof; ++k) du[k] = 0.0;
     indicator_curved(b, eq, opt, m, u, ws.alpha);
     const Subcells sc = compute_subcells(b);
@@ -326,7 +335,11 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
 #pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad)
     for (int e = 0; e < m.n_elements; ++e) {
         const double a = ws.alpha[e];
-        lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws, 1.0 - a);
+        const double* Jae = &m.Ja[4 * (size_t)nn * e];
+        const double* ije = &m.inv_jac[(size_t)nn * e];
+        if (kind == 0) lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws, 1.0 - a);
+        else if (kind == 1) mdrk1_volume_element(b, eq, e, u, du, dt, 0.0, 1.0 - a, ws, Jae, ije);
+        else mdrk2_volume_element(b, eq, e, u2, du, dt, 0.0, 1.0 - a, ws, Jae, ije);
         // pure_and_blended_element_ids!: DG only where isapprox(alpha, 0, atol = 1e-12)
         const bool blended = !(std::fabs(a) <= 1e-12);
         bool b_ = false;
@@ -369,7 +382,7 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
         }
     }
     ws.bad = ws.bad || bad;
-    calc_boundary_flux_curved(b, eq, opt, m, u, ws, bd, 1.0);
+    calc_boundary_flux_curved(b, eq, opt, m, u, ws, bd, kind == 1 ? 0.5 : 1.0);
     surface_integral_and_jacobian_curved(b, m, du, ws, nthreads);
 }
 

@@ -202,3 +202,70 @@ def test_gpu_curved_sc_with_positivity_limiter_matches_oracle(oracle_mod, tl):
     s, t = o.steps(u_cpu, 8, 0.2, 0.0, 1e9, nthreads=NTH)
     assert s == integ.iter == 8 and integ.t == pytest.approx(t, rel=1e-12)
     assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-11)
+
+
+# ---------------------------------------------------------------------------------------------- MDRK
+@pytest.mark.parametrize("rec", [0, 1])
+def test_oracle_curved_sc_mdrk_conservation(oracle_mod, tl, rec):
+    """MDRK with shock capturing on the curvilinear mesh (the reference's double Mach elixirs): both stages
+    conserve on the periodic mesh and a few two-stage steps stay admissible."""
+    N = 4
+    _, cm, o = make(oracle_mod, tl, N, cells=(8, 8), rec=rec, rotate=True)
+    u = blast_state(cm)
+    dt = o.max_dt(u, 0.15)
+    scale = np.abs(quad(cm, N, u)).max()
+    d1 = o.rhs(u, 0.0, dt, kind=1)
+    assert np.all(np.abs(quad(cm, N, d1)) < 1e-11 * scale)
+    d2 = o.rhs(u, 0.0, dt, kind=2, us=u + dt * d1)
+    assert np.all(np.abs(quad(cm, N, d2)) < 1e-11 * scale)
+    mass0 = quad(cm, N, u)
+    s, _ = o.steps(u, 10, 0.15, 0.0, 1e9, kind=1, nthreads=NTH)
+    assert s == 10 and np.all(np.isfinite(u))
+    np.testing.assert_allclose(quad(cm, N, u), mass0, rtol=1e-12, atol=1e-12)
+
+
+def sc_semi_mdrk(tl, mesh, N, rec):
+    eq = tl.CompressibleEulerEquations2D(GAMMA)
+    vi = tl.VolumeIntegralFRShockCapturing(tl.IndicatorHennemannGassner(alpha_max=0.5, alpha_min=0.001),
+                                           tl.VolumeIntegralFR(tl.MDRK()),
+                                           reconstruction=tl.MUSCLReconstruction() if rec else
+                                           tl.FirstOrderReconstruction())
+    return tl.SemidiscretizationHyperbolic(mesh, tl.MDRK(), eq, tl.ConstantState(),
+                                           tl.DGSEM(N, tl.flux_lax_friedrichs, vi))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,rec", [(3, 1), (4, 0), (4, 1)])
+def test_gpu_curved_sc_mdrk_stages_match_oracle(oracle_mod, tl, N, rec):
+    """rhs_mdrk1 / rhs_mdrk2 with shock capturing on the rotated warped mesh against the oracle."""
+    _, cm, o = make(oracle_mod, tl, N, cells=(8, 8), rec=rec, rotate=True)
+    u = blast_state(cm)
+    o.steps(u, 4, 0.15, 0.0, 1e9, kind=1, nthreads=NTH)
+    semi = sc_semi_mdrk(tl, cm, N, rec)
+    dt = o.max_dt(u, 0.15)
+    semi.cache["dt"][0] = dt
+    d1_gpu = np.empty_like(u)
+    tl.rhs_mdrk1(d1_gpu, u, semi, 0.0)
+    d1_cpu = o.rhs(u, 0.0, dt, kind=1)
+    assert np.all(rel_l2(u + dt * d1_gpu, u + dt * d1_cpu) < 1e-12)
+    us = u + dt * d1_cpu
+    d2_gpu = np.empty_like(u)
+    tl.rhs_mdrk2(d2_gpu, u, semi, 0.0, us)
+    d2_cpu = o.rhs(u, 0.0, dt, kind=2, us=us)
+    assert np.all(rel_l2(u + dt * d2_gpu, u + dt * d2_cpu) < 1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rec", [0, 1])
+def test_gpu_curved_sc_mdrk_steps_match_oracle(oracle_mod, tl, rec):
+    _, cm, o = make(oracle_mod, tl, 4, cells=(8, 8), rec=rec, rotate=True)
+    semi = sc_semi_mdrk(tl, cm, 4, rec)
+    u0 = blast_state(cm)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, tl.MDRK(), (0.0, 1e9)))
+    integ.set_state(u0, 0.0)
+    integ.step(12, 0.15, use_graph=True)
+    integ.sync_time()
+    u_cpu = u0.copy()
+    s, t = o.steps(u_cpu, 12, 0.15, 0.0, 1e9, kind=1, nthreads=NTH)
+    assert s == integ.iter == 12 and integ.t == pytest.approx(t, rel=1e-12)
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-11)

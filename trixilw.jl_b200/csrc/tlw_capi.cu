@@ -123,11 +123,8 @@ struct Launch {
             cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
-        const int sc0 = (int)C::smem_bytes(8), sc1 = (int)C::smem_bytes(12);
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc0);
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc0);
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc1);
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc1);
+        curved_sc_attributes<0>();
+        curved_sc_attributes<1>();
         const int md = (int)C::smem_bytes(2);
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
@@ -148,6 +145,31 @@ struct Launch {
             else mdrk2_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, md, s>>>(a);
         }
     }
+    // curvilinear shock capturing: LW or an MDRK stage with first-order (REC 0) or MUSCL (REC 1) subcells
+    template <int REC>
+    static void curved_sc(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
+        const size_t sm = C::smem_bytes(REC ? 12 : 8);
+        if (stage == TLW_STAGE_MDRK1) {
+            if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS, true, true, REC><<<grid, C::THREADS, sm, s>>>(a);
+            else mdrk1_volume_kernel<N, MODE_STEP, true, true, REC><<<grid, C::THREADS, sm, s>>>(a);
+        } else if (stage == TLW_STAGE_MDRK2) {
+            if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS, true, true, REC><<<grid, C::THREADS, sm, s>>>(a);
+            else mdrk2_volume_kernel<N, MODE_STEP, true, true, REC><<<grid, C::THREADS, sm, s>>>(a);
+        } else {
+            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, REC><<<grid, C::THREADS, sm, s>>>(a);
+            else lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, REC><<<grid, C::THREADS, sm, s>>>(a);
+        }
+    }
+    template <int REC>
+    static void curved_sc_attributes() {
+        const int sm = (int)C::smem_bytes(REC ? 12 : 8);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, true, true, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, true, true, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, true, true, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, true, true, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    }
     static void volume(cudaStream_t s, int stage, int mode, bool sc, const VolArgs& a) {
         const int grid = (int)((a.E + C::EB - 1) / C::EB);
         if (grid == 0) return;
@@ -155,14 +177,9 @@ struct Launch {
             if constexpr (N >= 4) lw_volume_kernel<N, MODE_STEP, false, 0, false, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
             return;
         }
-        if (a.metrics && sc) {   // curvilinear mesh, LW with shock capturing (MUSCL when the geometry is given)
-            if (a.muscl_geom) {
-                if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, 1><<<grid, C::THREADS, C::smem_bytes(12), s>>>(a);
-                else lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, 1><<<grid, C::THREADS, C::smem_bytes(12), s>>>(a);
-            } else {
-                if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, 0><<<grid, C::THREADS, C::smem_bytes(8), s>>>(a);
-                else lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, 0><<<grid, C::THREADS, C::smem_bytes(8), s>>>(a);
-            }
+        if (a.metrics && sc) {   // curvilinear mesh with shock capturing (MUSCL when the geometry is given)
+            if (a.muscl_geom) curved_sc<1>(s, stage, mode, a, grid);
+            else curved_sc<0>(s, stage, mode, a, grid);
             return;
         }
         if (a.metrics) {   // curvilinear mesh (LW or MDRK, FR volume integral)
@@ -1020,8 +1037,8 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
                         const int32_t* secondary_faces, const int32_t* secondary_reversed) {
     if (!h) return TLW_E_ARG;
     if (h->N < 3) return fail(h, TLW_E_UNSUPPORTED, "curvilinear meshes: N >= 3");
-    if (h->sc && (h->opts.time_discretization != TLW_LW || h->opts.surface_flux != TLW_FLUX_RUSANOV))
-        return fail(h, TLW_E_UNSUPPORTED, "curvilinear shock capturing: LW with the Rusanov surface flux");
+    if (h->sc && h->opts.surface_flux != TLW_FLUX_RUSANOV)
+        return fail(h, TLW_E_UNSUPPORTED, "curvilinear shock capturing: the Rusanov surface flux");
     if (n_elements <= 0 || n_elements > (int64_t)0x7fffffff / 64 || !contravariant_vectors || !inverse_jacobian)
         return fail(h, TLW_E_ARG, "n_elements / metrics");
     if (n_interfaces < 0 || (n_interfaces > 0 && (!primary_elements || !primary_faces || !secondary_elements ||

@@ -866,9 +866,11 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
 // ------------------------------------------------------------------------------------------------
 // CURVED (mdrk_kernel_1!, src/solvers/dgsem_structured/multi_derivative_2d.jl:82-243): the contractions take the
 // contravariant fluxes, d carries the node's J^{-1}; F2, G2 stay physical, the traces are contravariant.
-template <int N, int MODE, bool SC, bool CURVED = false>
-static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk1_volume_kernel(VolArgs a) {
-    static_assert(!(SC && CURVED), "shock capturing is built for TreeMesh only");
+template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0>
+static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
+                                                                         : VolCfg<N>::MDRK_MIN_BLOCKS)
+    mdrk1_volume_kernel(VolArgs a) {
+    static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
@@ -880,6 +882,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
     double* VC = UU + C::PLANES;
     double* FVX = VC + C::PLANES;
     double* FVY = FVX + C::PLANES;
+    double* UF = FVY + C::PLANES;      // curvilinear MUSCL: face values, 4 regions (left, right, down, up)
     const int tid = threadIdx.x;
     const double gm1 = a.gamma - 1.0;
     const int el = tid / nn;
@@ -887,6 +890,13 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
     const int i = node % n, j = node / n;
     const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
+    double alpha_e = 0.0;
+    bool blended = false, muscl = false;
+    if (SC && CURVED && active) {
+        alpha_e = __ldg(a.alpha + e);
+        blended = !(fabs(alpha_e) <= 1e-12);
+        muscl = REC == 1 && blended && !__ldg(a.atb + e);
+    }
     // dt of this element's instance (batched form) or the single dt
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
     double uu[NV], f0[NV], g0[NV], ij = 0.0, Ja[4] = {0.0, 0.0, 0.0, 0.0};
@@ -917,6 +927,8 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
         }
     }
     __syncthreads();
+    // (the MUSCL face values are read by the neighbours after the next barrier)
+    if (SC && CURVED && REC == 1 && muscl) sc_muscl_faces<N, C>(UU, UF, a.muscl_geom, el, i, j, gm1);
     line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
     double U[NV], F[NV], G[NV];
@@ -961,7 +973,10 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
             for (int v = 0; v < NV; ++v) { F[v] = ft2[v]; G[v] = gt2[v]; }
         }
         node_put<N, C>(X, Y, el, i, j, F, G);
-        if (SC) sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
+        if (SC) {
+            if constexpr (CURVED) sc_faces_curved<N, C, REC>(a, UU, VC, F0X, F0Y, UF, FVX, FVY, el, e, i, j, blended, muscl);
+            else sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
+        }
     }
     __syncthreads();
     line_contract<N, C, true>(X, Y, tid);
@@ -969,7 +984,10 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
     if (active) {
         double acc[NV];
         node_sum<N, C>(X, Y, el, i, j, acc);
-        if (SC) sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
+        if (SC) {
+            if constexpr (CURVED) sc_blend_curved<N, C>(a, FVX, FVY, el, e, i, j, alpha_e, blended, acc);
+            else sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
+        }
         double o[NV];
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o);
     }
@@ -980,9 +998,11 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
 // F = F2 + f_t(u*)/3, U = U2 + u*_t/3.
 // ------------------------------------------------------------------------------------------------
 // CURVED (mdrk_kernel_2!, src/solvers/dgsem_structured/multi_derivative_2d.jl:245-445): as in stage 1.
-template <int N, int MODE, bool SC, bool CURVED = false>
-static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN_BLOCKS) mdrk2_volume_kernel(VolArgs a) {
-    static_assert(!(SC && CURVED), "shock capturing is built for TreeMesh only");
+template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0>
+static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
+                                                                         : VolCfg<N>::MDRK_MIN_BLOCKS)
+    mdrk2_volume_kernel(VolArgs a) {
+    static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
@@ -994,6 +1014,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
     double* VC = UU + C::PLANES;
     double* FVX = VC + C::PLANES;
     double* FVY = FVX + C::PLANES;
+    double* UF = FVY + C::PLANES;      // curvilinear MUSCL: face values, 4 regions (left, right, down, up)
     const int tid = threadIdx.x;
     const double gm1 = a.gamma - 1.0;
     const int el = tid / nn;
@@ -1001,6 +1022,13 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
     const int i = node % n, j = node / n;
     const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
+    double alpha_e = 0.0;
+    bool blended = false, muscl = false;
+    if (SC && CURVED && active) {
+        alpha_e = __ldg(a.alpha + e);
+        blended = !(fabs(alpha_e) <= 1e-12);
+        muscl = REC == 1 && blended && !__ldg(a.atb + e);
+    }
     // dt of this element's instance (batched form) or the single dt
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
     double us[NV], ij = 0.0, Ja[4] = {0.0, 0.0, 0.0, 0.0};
@@ -1031,6 +1059,8 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
         }
     }
     __syncthreads();
+    // (the MUSCL face values are read by the neighbours after the next barrier)
+    if (SC && CURVED && REC == 1 && muscl) sc_muscl_faces<N, C>(UU, UF, a.muscl_geom, el, i, j, gm1);
     line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
     double U[NV], F[NV], G[NV];
@@ -1072,7 +1102,10 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
             for (int v = 0; v < NV; ++v) { F[v] = ft2[v]; G[v] = gt2[v]; }
         }
         node_put<N, C>(X, Y, el, i, j, F, G);
-        if (SC) sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
+        if (SC) {
+            if constexpr (CURVED) sc_faces_curved<N, C, REC>(a, UU, VC, F0X, F0Y, UF, FVX, FVY, el, e, i, j, blended, muscl);
+            else sc_faces<N, C>(UU, VC, F0X, F0Y, FVX, FVY, el, i, j, a.speed_kind);
+        }
     }
     __syncthreads();
     line_contract<N, C, true>(X, Y, tid);
@@ -1080,7 +1113,10 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MDRK_MIN
     if (active) {
         double acc[NV];
         node_sum<N, C>(X, Y, el, i, j, acc);
-        if (SC) sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
+        if (SC) {
+            if constexpr (CURVED) sc_blend_curved<N, C>(a, FVX, FVY, el, e, i, j, alpha_e, blended, acc);
+            else sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
+        }
         double o[NV];
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o);
     }
