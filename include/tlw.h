@@ -192,8 +192,8 @@ int tlw_dd_finish(tlw_handle* h);
  * VolumeIntegralFRShockCapturing(...; reconstruction), src/solvers/dgsem_tree/dg_2d.jl:251-365):
  * TLW_RECONSTRUCTION_FIRST_ORDER (FirstOrderReconstruction, the default) or TLW_RECONSTRUCTION_MUSCL
  * (MUSCLReconstruction: calcflux_muscl!, src/solvers/dgsem_structured/dg_2d.jl:176-311, first order on elements
- * with a boundary face). Shock capturing on a curvilinear mesh follows the P4estMesh{2} path: LW, Rusanov surface
- * flux, the blended interface flux of get_blended_flux / zhang_shu_flux_fix (src/solvers/dgsem_p4est/
+ * with a boundary face). Shock capturing on a curvilinear mesh follows the P4estMesh{2} path: LW or MDRK (both
+ * stages blend with the indicator of u^n and take their subcells from u^n), Rusanov surface flux, the blended interface flux of get_blended_flux / zhang_shu_flux_fix (src/solvers/dgsem_p4est/
  * dg_2d.jl:199-250). TreeMesh shock capturing takes first-order subcells only. */
 #define TLW_RECONSTRUCTION_FIRST_ORDER 0
 #define TLW_RECONSTRUCTION_MUSCL 1
