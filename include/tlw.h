@@ -191,12 +191,14 @@ int tlw_dd_finish(tlw_handle* h);
 /* Subcell reconstruction of the blended elements under shock capturing on a curvilinear mesh (the reference's
  * VolumeIntegralFRShockCapturing(...; reconstruction), src/solvers/dgsem_tree/dg_2d.jl:251-365):
  * TLW_RECONSTRUCTION_FIRST_ORDER (FirstOrderReconstruction, the default) or TLW_RECONSTRUCTION_MUSCL
- * (MUSCLReconstruction: calcflux_muscl!, src/solvers/dgsem_structured/dg_2d.jl:176-311, first order on elements
- * with a boundary face). Shock capturing on a curvilinear mesh follows the P4estMesh{2} path: LW or MDRK (both
+ * (MUSCLReconstruction: calcflux_muscl!, src/solvers/dgsem_structured/dg_2d.jl:176-311) or
+ * TLW_RECONSTRUCTION_MUSCL_HANCOCK (MUSCLHancockReconstruction: calcflux_mh!, :313-538, the half step with the time
+ * step fv_kernel! is given: dt, dt / 2 in MDRK stage 1); both first order on elements with a boundary face. Shock capturing on a curvilinear mesh follows the P4estMesh{2} path: LW or MDRK (both
  * stages blend with the indicator of u^n and take their subcells from u^n), Rusanov surface flux, the blended interface flux of get_blended_flux / zhang_shu_flux_fix (src/solvers/dgsem_p4est/
  * dg_2d.jl:199-250). TreeMesh shock capturing takes first-order subcells only. */
 #define TLW_RECONSTRUCTION_FIRST_ORDER 0
 #define TLW_RECONSTRUCTION_MUSCL 1
+#define TLW_RECONSTRUCTION_MUSCL_HANCOCK 2
 int tlw_set_reconstruction(tlw_handle* h, int32_t reconstruction);
 
 /* Boundary faces of the curvilinear mesh (P4estMesh boundaries: element, face), after tlw_set_curved_mesh

@@ -33,7 +33,19 @@
 
 namespace tlwo {
 
-enum Reconstruction { REC_FIRST_ORDER = 0, REC_MUSCL = 1 };
+enum Reconstruction { REC_FIRST_ORDER = 0, REC_MUSCL = 1, REC_MUSCL_HANCOCK = 2 };
+
+// Trixi flux(u, normal_direction, equations) of CompressibleEulerEquations2D
+inline void flux_normal(const Euler& eq, const double* u, const double* nrm, double* f) {
+    double rho, v1, v2, p;
+    eq.cons2prim(u, rho, v1, v2, p);
+    const double vn = v1 * nrm[0] + v2 * nrm[1];
+    const double rvn = rho * vn;
+    f[0] = rvn;
+    f[1] = rvn * v1 + p * nrm[0];
+    f[2] = rvn * v2 + p * nrm[1];
+    f[3] = (u[3] + p) * vn;
+}
 
 // Trixi flux_lax_friedrichs(u_ll, u_rr, normal_direction, equations)
 inline void rusanov_normal(const Euler& eq, int speed_kind, const double* ul, const double* ur, const double* nrm,
@@ -201,11 +213,122 @@ inline void muscl_face_values(const Basis& b, const Euler& eq, const Subcells& s
         }
 }
 
+// minmod(a, b, c, beta, Mdx2) of dgsem_structured/dg_2d.jl:83-95 (with Mdx2 = 0)
+inline double minmod3(double a, double b, double c, double beta) {
+    const double slope = julia_min(julia_min(beta * std::fabs(a), std::fabs(b)), beta * std::fabs(c));
+    const double s1 = julia_sign(a), s2 = julia_sign(b), s3 = julia_sign(c);
+    if (s1 != s2 || s2 != s3) return 0.0;
+    return s1 * slope;
+}
+
+// The half-step face values of the MUSCL-Hancock reconstruction of one element (calcflux_mh!,
+// dgsem_structured/dg_2d.jl:313-483): slopes from minmod(backward, centred, forward; beta = 2 - alpha) of the
+// element-local extended state (finite_differences, :75-81), limited face values as in MUSCL, then every face
+// value of a subcell gets the same multi-D half-step increment, built as the reference builds it: along xi,
+// cell c receives +dt/2 J^{-1}(c) / w_{c+1} f(u_left(c)).n_c (1 <= c <= n-2) and -dt/2 J^{-1}(c) / w_{c+1}
+// f(u_right(c)).n_{c+1} (c <= n-2); along eta, +dt/2 J^{-1}(c+1) / w_{c+1} f(u_down(c)).n_c and -dt/2
+// J^{-1}(c+1) / w_{c+1} f(u_up(c)).n_{c+1} (the next cell's J^{-1}), with the subcell normals n.
+inline void muscl_hancock_face_values(const Basis& b, const Euler& eq, const Subcells& sc, const double* Jae,
+                                      const double* ije, const double* u, int e, double alpha, double dt,
+                                      std::vector<double>& uf) {
+    const int n = b.n;
+    uf.assign((size_t)4 * NV * n * n, 0.0);
+    auto ue = [&](int i, int j) {
+        i = std::min(std::max(i, 1), n);
+        j = std::min(std::max(j, 1), n);
+        return u + idx_u(n, 0, i - 1, j - 1, e);
+    };
+    const double beta = 2.0 - alpha;
+    for (int j = 1; j <= n; ++j)
+        for (int i = 1; i <= n; ++i) {
+            const double *u_ = ue(i, j), *ul = ue(i - 1, j), *ur = ue(i + 1, j), *ud = ue(i, j - 1),
+                         *uu = ue(i, j + 1);
+            const double h1x = sc.xi_ext[i] - sc.xi_ext[i - 1], h2x = sc.xi_ext[i + 1] - sc.xi_ext[i];
+            const double h1y = sc.xi_ext[j] - sc.xi_ext[j - 1], h2y = sc.xi_ext[j + 1] - sc.xi_ext[j];
+            const double ax = -(h2x / (h1x * (h1x + h2x))), bx = (h2x - h1x) / (h1x * h2x), cx = (h1x / (h2x * (h1x + h2x)));
+            const double ay = -(h2y / (h1y * (h1y + h2y))), by = (h2y - h1y) / (h1y * h2y), cy = (h1y / (h2y * (h1y + h2y)));
+            double sx[NV], sy[NV];
+            for (int v = 0; v < NV; ++v) {
+                const double bkx = (u_[v] - ul[v]) / h1x, fwx = (ur[v] - u_[v]) / h2x;
+                const double cnx = ax * ul[v] + bx * u_[v] + cx * ur[v];
+                const double bky = (u_[v] - ud[v]) / h1y, fwy = (uu[v] - u_[v]) / h2y;
+                const double cny = ay * ud[v] + by * u_[v] + cy * uu[v];
+                sx[v] = minmod3(bkx, cnx, fwx, beta);
+                sy[v] = minmod3(bky, cny, fwy, beta);
+            }
+            const double xl = sc.faces[i - 1] - sc.xi_ext[i], xr = sc.faces[i] - sc.xi_ext[i];
+            const double yl = sc.faces[j - 1] - sc.xi_ext[j], yr = sc.faces[j] - sc.xi_ext[j];
+            double usl[NV], usr[NV], usd[NV], usu[NV];
+            for (int v = 0; v < NV; ++v) {
+                usl[v] = u_[v] + 2.0 * sx[v] * xl;
+                usr[v] = u_[v] + 2.0 * sx[v] * xr;
+                usd[v] = u_[v] + 2.0 * sy[v] * yl;
+                usu[v] = u_[v] + 2.0 * sy[v] * yr;
+            }
+            double* o = uf.data() + (size_t)4 * NV * ((i - 1) + n * (j - 1));
+            limit_slope(eq, sx, usl, usr, u_, xl, xr, o + 0 * NV, o + 1 * NV);
+            limit_slope(eq, sy, usd, usu, u_, yl, yr, o + 2 * NV, o + 3 * NV);
+        }
+    // the half-step increments, from the limited face values of each cell (0-based cell c = (i, j))
+    auto normal = [&](int d, int line, int f, double* nrm) {   // subcell face f (1..n-1) of line `line`
+        const double* J0 = Jae + 4 * (d == 0 ? 0 + n * line : line + 0);
+        nrm[0] = J0[2 * d];
+        nrm[1] = J0[2 * d + 1];
+        for (int k = 0; k < f; ++k) {
+            double o[2];
+            metric_increment(b, Jae, d, line, k, o);
+            nrm[0] += o[0];
+            nrm[1] += o[1];
+        }
+    };
+    std::vector<double> unph = uf;
+    auto F = [&](int i, int j, int k) { return uf.data() + (size_t)4 * NV * (i + n * j) + NV * k; };
+    auto add = [&](int i, int j, const double* r) {
+        for (int k = 0; k < 4; ++k)
+            for (int v = 0; v < NV; ++v) unph[(size_t)4 * NV * (i + n * j) + NV * k + v] += r[v];
+    };
+    // xi lines: faces f = 1..n-1 in order; at face f the cell f-1 gets its "ll" part, the cell f (f < n-1) its
+    // "rr" part
+    for (int j = 0; j < n; ++j)
+        for (int f = 1; f < n; ++f) {
+            double nrm[2], fl[NV], r[NV];
+            normal(0, j, f, nrm);
+            flux_normal(eq, F(f - 1, j, 1), nrm, fl);
+            const double cl = -0.5 * dt * ije[(f - 1) + n * j] / b.weights[f];
+            for (int v = 0; v < NV; ++v) r[v] = cl * fl[v];
+            add(f - 1, j, r);
+            if (f < n - 1) {
+                flux_normal(eq, F(f, j, 0), nrm, fl);
+                const double cr = 0.5 * dt * ije[f + n * j] / b.weights[f + 1];
+                for (int v = 0; v < NV; ++v) r[v] = cr * fl[v];
+                add(f, j, r);
+            }
+        }
+    for (int i = 0; i < n; ++i)
+        for (int f = 1; f < n; ++f) {
+            double nrm[2], fl[NV], r[NV];
+            normal(1, i, f, nrm);
+            flux_normal(eq, F(i, f - 1, 3), nrm, fl);
+            const double cd = -0.5 * dt * ije[i + n * f] / b.weights[f];
+            for (int v = 0; v < NV; ++v) r[v] = cd * fl[v];
+            add(i, f - 1, r);
+            if (f < n - 1) {
+                flux_normal(eq, F(i, f, 2), nrm, fl);
+                const double cu = 0.5 * dt * ije[i + n * (f + 1)] / b.weights[f + 1];
+                for (int v = 0; v < NV; ++v) r[v] = cu * fl[v];
+                add(i, f, r);
+            }
+        }
+    uf.swap(unph);
+}
+
 // One element's subcell pass: blended elements add alpha_e times the FV divergence to du; every element fills
 // its fn_low slots (P4est order: bottom, right, top, left).
+// dt_fv: the time step fv_kernel! is given (MUSCL-Hancock's half step: dt for LW and MDRK stage 2, dt / 2 for
+// MDRK stage 1, src/solvers/dgsem_tree/multi_derivative_2d.jl:199, 256).
 inline void curved_subcells(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m,
                             const Subcells& sc, const std::vector<char>& at_boundary, int e, const double* u,
-                            double* du, double alpha, bool blended, Workspace& ws, bool& bad) {
+                            double* du, double alpha, bool blended, Workspace& ws, bool& bad, double dt_fv = 0.0) {
     const int n = b.n, nn = n * n;
     const double* Jae = &m.Ja[4 * (size_t)nn * e];
     SubcellFluxes S;
@@ -216,9 +339,10 @@ inline void curved_subcells(const Basis& b, const Euler& eq, const Options& opt,
     auto nodeR = [&](int d, int f, int line) { return d == 0 ? node(f, line) : node(line, f); };
     if (!blended) {
         subcell_fluxes_curved(b, eq, opt.speed_kind, Jae, true, nodeL, nodeR, S, bad);
-    } else if (opt.reconstruction == REC_MUSCL && !at_boundary[e]) {
+    } else if ((opt.reconstruction == REC_MUSCL || opt.reconstruction == REC_MUSCL_HANCOCK) && !at_boundary[e]) {
         std::vector<double> uf;
-        muscl_face_values(b, eq, sc, u, e, uf);
+        if (opt.reconstruction == REC_MUSCL) muscl_face_values(b, eq, sc, u, e, uf);
+        else muscl_hancock_face_values(b, eq, sc, Jae, &m.inv_jac[(size_t)nn * e], u, e, alpha, dt_fv, uf);
         auto F = [&](int i, int j, int k) { return uf.data() + (size_t)4 * NV * (i + n * j) + NV * k; };
         // u_ll: the right (up) face value of the node before the face, u_rr: the left (down) value after it
         auto fL = [&](int d, int f, int line) { return d == 0 ? F(f - 1, line, 1) : F(line, f - 1, 3); };
@@ -343,7 +467,7 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
         // pure_and_blended_element_ids!: DG only where isapprox(alpha, 0, atol = 1e-12)
         const bool blended = !(std::fabs(a) <= 1e-12);
         bool b_ = false;
-        curved_subcells(b, eq, opt, m, sc, at_boundary, e, u, du, a, blended, ws, b_);
+        curved_subcells(b, eq, opt, m, sc, at_boundary, e, u, du, a, blended, ws, b_, kind == 1 ? 0.5 * dt : dt);
         bad = bad || b_;
     }
 #pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad)

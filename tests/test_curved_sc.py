@@ -49,7 +49,7 @@ def test_oracle_curved_sc_without_blending_is_the_fr_rhs(oracle_mod, tl, N):
     assert np.all(o.get(6) == 0.0)
 
 
-@pytest.mark.parametrize("N,rec", [(3, 0), (4, 0), (4, 1), (5, 1)])
+@pytest.mark.parametrize("N,rec", [(3, 0), (4, 0), (4, 1), (5, 1), (3, 2), (4, 2)])
 def test_oracle_curved_sc_blast_conservation(oracle_mod, tl, N, rec):
     """The blast: blending is active near the discontinuity, the rhs conserves every variable on the
     periodic mesh, and a few steps stay admissible."""
@@ -84,15 +84,22 @@ def test_oracle_curved_muscl_differs_from_first_order(oracle_mod, tl):
     alpha = o1.get(6)
     diff = np.abs(d1 - d2).max(axis=1)
     assert diff[alpha > 0].max() > 1e-3
+    # MUSCL-Hancock (centred-difference slopes and the half-step update) differs from MUSCL as well
+    _, _, o3 = make(oracle_mod, tl, N, cells=(8, 8), rec=2)
+    d3 = o3.rhs(u, 0.0, dt).reshape(cm.n_elements, -1)
+    assert np.abs(d3 - d2).max(axis=1)[alpha > 0].max() > 1e-3
 
 
 # ---------------------------------------------------------------------------------------------- GPU
+RECONSTRUCTIONS = {0: lambda tl: tl.FirstOrderReconstruction(), 1: lambda tl: tl.MUSCLReconstruction(),
+                   2: lambda tl: tl.MUSCLHancockReconstruction()}
+
+
 def sc_semi(tl, mesh, N, rec, bc=None):
     eq = tl.CompressibleEulerEquations2D(GAMMA)
     vi = tl.VolumeIntegralFRShockCapturing(tl.IndicatorHennemannGassner(alpha_max=0.5, alpha_min=0.001),
                                            tl.VolumeIntegralFR(tl.LW()),
-                                           reconstruction=tl.MUSCLReconstruction() if rec else
-                                           tl.FirstOrderReconstruction())
+                                           reconstruction=RECONSTRUCTIONS[rec](tl))
     solver = tl.DGSEM(N, tl.flux_lax_friedrichs, vi)
     kw = {} if bc is None else {"boundary_conditions": bc}
     return tl.SemidiscretizationHyperbolic(mesh, tl.LW(), eq, tl.ConstantState(), solver, **kw)
@@ -107,7 +114,7 @@ def gpu_rhs(tl, semi, u, dt):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("N,rec,rotated", [(3, 0, False), (4, 0, True), (5, 0, False), (3, 1, True), (4, 1, False),
-                                           (5, 1, True)])
+                                           (5, 1, True), (3, 2, False), (4, 2, True), (5, 2, False)])
 def test_gpu_curved_sc_rhs_matches_oracle(oracle_mod, tl, N, rec, rotated):
     """One rhs of a blast that has run a few oracle steps (nonzero MUSCL slopes): blending factors, the
     face-adjacent subcell fluxes and du against the oracle."""
@@ -130,7 +137,7 @@ def test_gpu_curved_sc_rhs_matches_oracle(oracle_mod, tl, N, rec, rotated):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rec", [0, 1])
+@pytest.mark.parametrize("rec", [0, 1, 2])
 def test_gpu_curved_sc_steps_match_oracle(oracle_mod, tl, rec):
     """20 CFL steps of the blast (N = 4, rotated element frames) on the device against the oracle."""
     _, cm, o = make(oracle_mod, tl, 4, cells=(8, 8), rec=rec, rotate=True)
@@ -147,7 +154,7 @@ def test_gpu_curved_sc_steps_match_oracle(oracle_mod, tl, rec):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rec", [0, 1])
+@pytest.mark.parametrize("rec", [0, 1, 2])
 def test_gpu_curved_sc_walls_match_oracle(oracle_mod, tl, rec):
     """The blast in a warped box with slip walls: MUSCL falls back to first-order subcells on the elements
     next to the walls; 10 steps against the oracle."""
@@ -205,7 +212,7 @@ def test_gpu_curved_sc_with_positivity_limiter_matches_oracle(oracle_mod, tl):
 
 
 # ---------------------------------------------------------------------------------------------- MDRK
-@pytest.mark.parametrize("rec", [0, 1])
+@pytest.mark.parametrize("rec", [0, 1, 2])
 def test_oracle_curved_sc_mdrk_conservation(oracle_mod, tl, rec):
     """MDRK with shock capturing on the curvilinear mesh (the reference's double Mach elixirs): both stages
     conserve on the periodic mesh and a few two-stage steps stay admissible."""
@@ -228,14 +235,13 @@ def sc_semi_mdrk(tl, mesh, N, rec):
     eq = tl.CompressibleEulerEquations2D(GAMMA)
     vi = tl.VolumeIntegralFRShockCapturing(tl.IndicatorHennemannGassner(alpha_max=0.5, alpha_min=0.001),
                                            tl.VolumeIntegralFR(tl.MDRK()),
-                                           reconstruction=tl.MUSCLReconstruction() if rec else
-                                           tl.FirstOrderReconstruction())
+                                           reconstruction=RECONSTRUCTIONS[rec](tl))
     return tl.SemidiscretizationHyperbolic(mesh, tl.MDRK(), eq, tl.ConstantState(),
                                            tl.DGSEM(N, tl.flux_lax_friedrichs, vi))
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("N,rec", [(3, 1), (4, 0), (4, 1)])
+@pytest.mark.parametrize("N,rec", [(3, 1), (4, 0), (4, 1), (4, 2)])
 def test_gpu_curved_sc_mdrk_stages_match_oracle(oracle_mod, tl, N, rec):
     """rhs_mdrk1 / rhs_mdrk2 with shock capturing on the rotated warped mesh against the oracle."""
     _, cm, o = make(oracle_mod, tl, N, cells=(8, 8), rec=rec, rotate=True)
@@ -256,7 +262,7 @@ def test_gpu_curved_sc_mdrk_stages_match_oracle(oracle_mod, tl, N, rec):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rec", [0, 1])
+@pytest.mark.parametrize("rec", [0, 1, 2])
 def test_gpu_curved_sc_mdrk_steps_match_oracle(oracle_mod, tl, rec):
     _, cm, o = make(oracle_mod, tl, 4, cells=(8, 8), rec=rec, rotate=True)
     semi = sc_semi_mdrk(tl, cm, 4, rec)

@@ -125,6 +125,7 @@ struct Launch {
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
         curved_sc_attributes<0>();
         curved_sc_attributes<1>();
+        curved_sc_attributes<2>();
         const int md = (int)C::smem_bytes(2);
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
@@ -145,7 +146,8 @@ struct Launch {
             else mdrk2_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, md, s>>>(a);
         }
     }
-    // curvilinear shock capturing: LW or an MDRK stage with first-order (REC 0) or MUSCL (REC 1) subcells
+    // curvilinear shock capturing: LW or an MDRK stage with first-order (REC 0), MUSCL (REC 1) or MUSCL-Hancock
+    // (REC 2) subcells
     template <int REC>
     static void curved_sc(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
         const size_t sm = C::smem_bytes(REC ? 12 : 8);
@@ -178,7 +180,8 @@ struct Launch {
             return;
         }
         if (a.metrics && sc) {   // curvilinear mesh with shock capturing (MUSCL when the geometry is given)
-            if (a.muscl_geom) curved_sc<1>(s, stage, mode, a, grid);
+            if (a.reconstruction == TLW_RECONSTRUCTION_MUSCL_HANCOCK) curved_sc<2>(s, stage, mode, a, grid);
+            else if (a.reconstruction == TLW_RECONSTRUCTION_MUSCL) curved_sc<1>(s, stage, mode, a, grid);
             else curved_sc<0>(s, stage, mode, a, grid);
             return;
         }
@@ -642,7 +645,8 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
             va.subn = h->d_subn;
             va.subq = h->d_subq;
             va.atb = h->d_atb;
-            va.muscl_geom = h->reconstruction == 1 ? h->d_mgeom : nullptr;
+            va.muscl_geom = h->d_mgeom;
+            va.reconstruction = h->reconstruction;
         }
     }
     if (phases & 1) {
@@ -1022,10 +1026,11 @@ extern "C" {
 
 int tlw_set_reconstruction(tlw_handle* h, int32_t reconstruction) {
     if (!h) return TLW_E_ARG;
-    if (reconstruction != TLW_RECONSTRUCTION_FIRST_ORDER && reconstruction != TLW_RECONSTRUCTION_MUSCL)
+    if (reconstruction != TLW_RECONSTRUCTION_FIRST_ORDER && reconstruction != TLW_RECONSTRUCTION_MUSCL &&
+        reconstruction != TLW_RECONSTRUCTION_MUSCL_HANCOCK)
         return fail(h, TLW_E_ARG, "reconstruction");
-    if (reconstruction == TLW_RECONSTRUCTION_MUSCL && (!h->sc || (h->have_mesh && !h->curved)))
-        return fail(h, TLW_E_UNSUPPORTED, "MUSCL subcells: shock capturing on a curvilinear mesh");
+    if (reconstruction != TLW_RECONSTRUCTION_FIRST_ORDER && (!h->sc || (h->have_mesh && !h->curved)))
+        return fail(h, TLW_E_UNSUPPORTED, "MUSCL / MUSCL-Hancock subcells: shock capturing on a curvilinear mesh");
     drop_graphs(h);
     h->reconstruction = reconstruction;
     return TLW_OK;

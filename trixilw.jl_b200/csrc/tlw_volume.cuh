@@ -97,6 +97,7 @@ struct VolArgs {
     const double* subq;
     const unsigned char* atb;
     const double* muscl_geom;
+    int reconstruction;               // 0 first order, 1 MUSCL, 2 MUSCL-Hancock
 };
 
 // curvilinear: contravariant fluxes f~ = Ja^1_1 f + Ja^1_2 g, g~ = Ja^2_1 f + Ja^2_2 g of a node
@@ -315,52 +316,121 @@ __device__ __forceinline__ void limit_variable_slope(double gm1, int variable, d
     }
 }
 
-// MUSCL face values of node (i, j) (calcflux_muscl!, dgsem_structured/dg_2d.jl:196-253 with limit_slope,
-// src/equations/compressible_euler_2d.jl:9-21): minmod slopes of the element-local extended state, limited for
-// density then pressure; into the UF regions k = 0 left, 1 right, 2 down, 3 up
-template <int N, class C>
-__device__ __forceinline__ void sc_muscl_faces(const double* UU, double* UF, const double* geom, int el, int i, int j,
-                                               double gm1) {
-    constexpr int n = C::n;
+// Trixi flux(u, normal_direction, equations) of CompressibleEulerEquations2D
+__device__ __forceinline__ void euler_flux_normal(double gm1, const double* u, const double* nrm, double* f) {
+    const double rho = u[0], v1 = u[1] / rho, v2 = u[2] / rho;
+    const double p = gm1 * (u[3] - 0.5 * (u[1] * v1 + u[2] * v2));
+    const double vn = v1 * nrm[0] + v2 * nrm[1];
+    const double rvn = rho * vn;
+    f[0] = rvn;
+    f[1] = rvn * v1 + p * nrm[0];
+    f[2] = rvn * v2 + p * nrm[1];
+    f[3] = (u[3] + p) * vn;
+}
+
+// minmod(a, b, c, beta, 0) (src/solvers/dgsem_structured/dg_2d.jl:83-95)
+__device__ __forceinline__ double minmod3(double a, double b, double c, double beta) {
+    const double slope = julia_min(julia_min(beta * fabs(a), fabs(b)), beta * fabs(c));
+    const double s1 = julia_sign(a), s2 = julia_sign(b), s3 = julia_sign(c);
+    if (s1 != s2 || s2 != s3) return 0.0;
+    return s1 * slope;
+}
+
+// MUSCL (REC 1) and MUSCL-Hancock (REC 2) face values of node (i, j) into the UF regions k = 0 left, 1 right,
+// 2 down, 3 up: slopes of the element-local extended state (calcflux_muscl! / calcflux_mh!,
+// src/solvers/dgsem_structured/dg_2d.jl:196-253, 313-483: minmod of the one-sided differences, or with the centred
+// one and beta = 2 - alpha for MUSCL-Hancock), limited for density then pressure (limit_slope,
+// src/equations/compressible_euler_2d.jl:9-21). MUSCL-Hancock then adds to all four face values the multi-D
+// half-step increments of the subcell, as the reference builds them: along xi +dt/2 J^{-1}(i, j) / w_{i+1}
+// f(left).n_i (1 <= i <= n-2) and -dt/2 J^{-1}(i, j) / w_{i+1} f(right).n_{i+1} (i <= n-2); along eta the
+// same with J^{-1}(i, j+1) (dt_fv: the time step fv_kernel! is given).
+template <int N, class C, int REC>
+__device__ __forceinline__ void sc_muscl_faces(const VolArgs& a, const double* UU, double* UF, int el, int e, int i,
+                                               int j, double gm1, double alpha, double dt_fv, double ij) {
+    constexpr int n = C::n, nn = n * n;
     constexpr int PV = C::EB * C::P;
-    const double* sf = geom;           // subcell faces [0..n]
-    const double* xe = geom + n + 1;   // extended nodes [0..n+1]
+    const double* sf = a.muscl_geom;           // subcell faces [0..n]
+    const double* xe = a.muscl_geom + n + 1;   // extended nodes [0..n+1]
     auto at = [&](int ii, int jj, int v) {
         ii = ii < 0 ? 0 : (ii > n - 1 ? n - 1 : ii);
         jj = jj < 0 ? 0 : (jj > n - 1 ? n - 1 : jj);
         return UU[v * PV + el * C::P + ii + C::R * jj];
     };
     const int I = i + 1, J = j + 1;
-    const double dx1 = __ldg(xe + I) - __ldg(xe + I - 1), dx2 = __ldg(xe + I + 1) - __ldg(xe + I);
-    const double dy1 = __ldg(xe + J) - __ldg(xe + J - 1), dy2 = __ldg(xe + J + 1) - __ldg(xe + J);
+    const double h1x = __ldg(xe + I) - __ldg(xe + I - 1), h2x = __ldg(xe + I + 1) - __ldg(xe + I);
+    const double h1y = __ldg(xe + J) - __ldg(xe + J - 1), h2y = __ldg(xe + J + 1) - __ldg(xe + J);
     double u_[NV], sx[NV], sy[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         u_[v] = at(i, j, v);
-        sx[v] = minmod2((u_[v] - at(i - 1, j, v)) / dx1, (at(i + 1, j, v) - u_[v]) / dx2);
-        sy[v] = minmod2((u_[v] - at(i, j - 1, v)) / dy1, (at(i, j + 1, v) - u_[v]) / dy2);
+        const double ul = at(i - 1, j, v), ur = at(i + 1, j, v), ud = at(i, j - 1, v), uu = at(i, j + 1, v);
+        if (REC == 1) {
+            sx[v] = minmod2((u_[v] - ul) / h1x, (ur - u_[v]) / h2x);
+            sy[v] = minmod2((u_[v] - ud) / h1y, (uu - u_[v]) / h2y);
+        } else {
+            // finite_differences (dg_2d.jl:75-81)
+            const double beta = 2.0 - alpha;
+            const double ax = -(h2x / (h1x * (h1x + h2x))), bx = (h2x - h1x) / (h1x * h2x), cx = (h1x / (h2x * (h1x + h2x)));
+            const double ay = -(h2y / (h1y * (h1y + h2y))), by = (h2y - h1y) / (h1y * h2y), cy = (h1y / (h2y * (h1y + h2y)));
+            sx[v] = minmod3((u_[v] - ul) / h1x, ax * ul + bx * u_[v] + cx * ur, (ur - u_[v]) / h2x, beta);
+            sy[v] = minmod3((u_[v] - ud) / h1y, ay * ud + by * u_[v] + cy * uu, (uu - u_[v]) / h2y, beta);
+        }
     }
     const double xl = __ldg(sf + I - 1) - __ldg(xe + I), xr = __ldg(sf + I) - __ldg(xe + I);
     const double yl = __ldg(sf + J - 1) - __ldg(xe + J), yr = __ldg(sf + J) - __ldg(xe + J);
-    double a[NV], b[NV];
-    const int o = el * C::P + i + C::R * j;
+    double fv[4][NV];
 #pragma unroll
     for (int d = 0; d < 2; ++d) {
         double* s = d == 0 ? sx : sy;
         const double lo = d == 0 ? xl : yl, hi = d == 0 ? xr : yr;
+        double pa[NV], pb[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            a[v] = u_[v] + 2.0 * s[v] * lo;
-            b[v] = u_[v] + 2.0 * s[v] * hi;
+            pa[v] = u_[v] + 2.0 * s[v] * lo;
+            pb[v] = u_[v] + 2.0 * s[v] * hi;
         }
-        limit_variable_slope(gm1, 0, s, a, b, u_, lo, hi);
-        limit_variable_slope(gm1, 1, s, a, b, u_, lo, hi);
+        limit_variable_slope(gm1, 0, s, pa, pb, u_, lo, hi);
+        limit_variable_slope(gm1, 1, s, pa, pb, u_, lo, hi);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            UF[(2 * d) * C::PLANES + v * PV + o] = u_[v] + s[v] * lo;
-            UF[(2 * d + 1) * C::PLANES + v * PV + o] = u_[v] + s[v] * hi;
+            fv[2 * d][v] = u_[v] + s[v] * lo;
+            fv[2 * d + 1][v] = u_[v] + s[v] * hi;
         }
     }
+    if (REC == 2) {
+        // increments in the reference's order: xi "rr", xi "ll", eta "uu", eta "dd"
+        double inc[4][NV];
+        const double ijn = j + 1 < n ? __ldg(a.inv_jac_node + (size_t)e * nn + i + n * (j + 1)) : 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int d = q >> 1, c = d == 0 ? i : j, line = d == 0 ? j : i;
+            // q 0: the cell's own face c (its left / lower value, +), q 1: face c + 1 (right / upper value, -)
+            const int f = (q & 1) ? c + 1 : c;
+            const bool on = (q & 1) ? c <= n - 2 : (c >= 1 && c <= n - 2);
+            double r[NV] = {0.0, 0.0, 0.0, 0.0};
+            if (on) {
+                const double* np = a.subn + ((((size_t)e * 2 + d) * n + line) * (n - 1) + (f - 1)) * 2;
+                const double nrm[2] = {__ldg(np), __ldg(np + 1)};
+                double fl[NV];
+                euler_flux_normal(gm1, fv[2 * d + (q & 1)], nrm, fl);
+                const double jj = d == 0 ? ij : ijn;
+                const double cf = ((q & 1) ? -0.5 : 0.5) * dt_fv * jj / c_tlw_w[N][c + 1];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) r[v] = cf * fl[v];
+            }
+#pragma unroll
+            for (int v = 0; v < NV; ++v) inc[q][v] = r[v];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fv[k][v] = (((fv[k][v] + inc[0][v]) + inc[1][v]) + inc[2][v]) + inc[3][v];
+    }
+    const int o = el * C::P + i + C::R * j;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) UF[k * C::PLANES + v * PV + o] = fv[k][v];
 }
 
 // final stage on a curvilinear mesh: the subcell flux on the node's left (xi) and lower (eta) face along the
@@ -384,7 +454,7 @@ __device__ __forceinline__ void sc_faces_curved(const VolArgs& a, const double* 
         const int aL = el * C::P + (d == 0 ? i - 1 : i) + C::R * (d == 0 ? j : j - 1);
         const int aR = el * C::P + i + C::R * j;
         double uL[NV], uR[NV], fL[NV], gL[NV], fR[NV], gR[NV], vnL, vnR, cL, cR, out[NV];
-        if (REC == 1 && muscl) {
+        if (REC >= 1 && muscl) {
             // the right (up) face value of the node before the face, the left (down) one of the node after it
             const double* PL = UF + (d == 0 ? 1 : 3) * C::PLANES;
             const double* PR = UF + (d == 0 ? 0 : 2) * C::PLANES;
@@ -538,7 +608,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
     if (SC && CURVED && active) {
         alpha_e = __ldg(a.alpha + e);
         blended = !(fabs(alpha_e) <= 1e-12);
-        muscl = REC == 1 && blended && !__ldg(a.atb + e);
+        muscl = REC >= 1 && blended && !__ldg(a.atb + e);
     }
     // dt of this element's instance (batched form) or the single dt
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
@@ -587,7 +657,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
     __syncthreads();
     line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
-    if (SC && CURVED && REC == 1 && muscl) sc_muscl_faces<N, C>(UU, UF, a.muscl_geom, el, i, j, gm1);
+    if (SC && CURVED && REC >= 1 && muscl) sc_muscl_faces<N, C, REC>(a, UU, UF, el, e, i, j, gm1, alpha_e, dt, ij);
 
     // stage 1: ut; perturbed states; f_t (dg_2d.jl:972-1023 / :725-775 / :543-582 / :417-454)
     if (active) {
@@ -895,7 +965,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
     if (SC && CURVED && active) {
         alpha_e = __ldg(a.alpha + e);
         blended = !(fabs(alpha_e) <= 1e-12);
-        muscl = REC == 1 && blended && !__ldg(a.atb + e);
+        muscl = REC >= 1 && blended && !__ldg(a.atb + e);
     }
     // dt of this element's instance (batched form) or the single dt
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
@@ -928,7 +998,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
     }
     __syncthreads();
     // (the MUSCL face values are read by the neighbours after the next barrier)
-    if (SC && CURVED && REC == 1 && muscl) sc_muscl_faces<N, C>(UU, UF, a.muscl_geom, el, i, j, gm1);
+    if (SC && CURVED && REC >= 1 && muscl) sc_muscl_faces<N, C, REC>(a, UU, UF, el, e, i, j, gm1, alpha_e, 0.5 * dt, ij);
     line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
     double U[NV], F[NV], G[NV];
@@ -1027,7 +1097,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
     if (SC && CURVED && active) {
         alpha_e = __ldg(a.alpha + e);
         blended = !(fabs(alpha_e) <= 1e-12);
-        muscl = REC == 1 && blended && !__ldg(a.atb + e);
+        muscl = REC >= 1 && blended && !__ldg(a.atb + e);
     }
     // dt of this element's instance (batched form) or the single dt
     const double dt = a.inst ? a.dt[__ldg(a.inst + min(e, a.E - 1))] : *a.dt;
@@ -1060,7 +1130,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
     }
     __syncthreads();
     // (the MUSCL face values are read by the neighbours after the next barrier)
-    if (SC && CURVED && REC == 1 && muscl) sc_muscl_faces<N, C>(UU, UF, a.muscl_geom, el, i, j, gm1);
+    if (SC && CURVED && REC >= 1 && muscl) sc_muscl_faces<N, C, REC>(a, UU, UF, el, e, i, j, gm1, alpha_e, dt, ij);
     line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
     double U[NV], F[NV], G[NV];

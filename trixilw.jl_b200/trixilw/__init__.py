@@ -15,7 +15,7 @@ from .semidiscretization import (LW, MDRK, DGSEM, Adaptive, Adiabatic, BoundaryC
                                  boundary_condition_slip_wall_horizontal, boundary_condition_slip_wall_vertical,
                                  FluxLaxFriedrichs, IndicatorHennemannGassner, SemidiscretizationHyperbolic,
                                  SemidiscretizationHyperbolicParabolic,
-                                 VolumeIntegralFR, VolumeIntegralFRShockCapturing, FirstOrderReconstruction, MUSCLReconstruction,
+                                 VolumeIntegralFR, VolumeIntegralFRShockCapturing, FirstOrderReconstruction, MUSCLReconstruction, MUSCLHancockReconstruction,
                                  boundary_condition_periodic, flux_hll, flux_lax_friedrichs,
                                  get_time_discretization, lw_fourier_cfl, rhs, rhs_mdrk1, rhs_mdrk2,
                                  semidiscretize, trixi2lw)
@@ -25,7 +25,7 @@ __all__ = [
     "FourQuadrantRiemann", "IsentropicVortex", "LWIntegrator", "LWSolution", "l2_linf_errors", "solve_lwfr",
     "TreeMesh", "LW", "MDRK", "DGSEM", "Adaptive", "BoundaryConditionDirichlet", "CFLBased", "FluxHLL",
     "FluxLaxFriedrichs", "IndicatorHennemannGassner", "SemidiscretizationHyperbolic", "VolumeIntegralFR",
-    "VolumeIntegralFRShockCapturing", "FirstOrderReconstruction", "MUSCLReconstruction", "boundary_condition_periodic",
+    "VolumeIntegralFRShockCapturing", "FirstOrderReconstruction", "MUSCLReconstruction", "MUSCLHancockReconstruction", "boundary_condition_periodic",
     "flux_hll", "flux_lax_friedrichs", "get_time_discretization", "lw_fourier_cfl", "rhs", "rhs_mdrk1",
     "rhs_mdrk2", "semidiscretize", "trixi2lw", "LWBatch", "solve_lwfr_batch",
     "adjoint_solve", "adjoint_step", "adjoint_sweep", "forward_record", "lw_solve", "solve_dts",

@@ -29,7 +29,7 @@ TLW_VOLUME_FR, TLW_VOLUME_FR_SHOCK_CAPTURING = 0, 1
 TLW_LIMIT_DENSITY, TLW_LIMIT_PRESSURE, TLW_LIMIT_DENSITY_PRESSURE = 0, 1, 2
 TLW_BC_DIRICHLET, TLW_BC_SLIP_WALL_VERTICAL, TLW_BC_SLIP_WALL_HORIZONTAL = 0, 1, 2
 TLW_WALL_NOSLIP_ADIABATIC, TLW_WALL_NOSLIP_ISOTHERMAL = 1, 2
-TLW_RECONSTRUCTION_FIRST_ORDER, TLW_RECONSTRUCTION_MUSCL = 0, 1
+TLW_RECONSTRUCTION_FIRST_ORDER, TLW_RECONSTRUCTION_MUSCL, TLW_RECONSTRUCTION_MUSCL_HANCOCK = 0, 1, 2
 
 # every symbol include/tlw.h declares
 EXPORTED = (

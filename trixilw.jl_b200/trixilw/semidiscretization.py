@@ -103,12 +103,16 @@ class MUSCLReconstruction:
     """MUSCLReconstruction(): minmod-limited MUSCL subcells (curvilinear meshes)."""
 
 
+class MUSCLHancockReconstruction:
+    """MUSCLHancockReconstruction(): MUSCL subcells with the Hancock half step (curvilinear meshes)."""
+
+
 @dataclass
 class VolumeIntegralFRShockCapturing:
     """VolumeIntegralFRShockCapturing(indicator; volume_integralFR, volume_flux_fv, reconstruction)
     (src/solvers/fr.jl:59-86). Built: volume_flux_fv = flux_lax_friedrichs; reconstruction =
-    FirstOrderReconstruction() (every mesh) or MUSCLReconstruction() (curvilinear meshes), given as an instance
-    or by name."""
+    FirstOrderReconstruction() (every mesh), MUSCLReconstruction() or MUSCLHancockReconstruction() (curvilinear
+    meshes), given as an instance or by name."""
     indicator: IndicatorHennemannGassner = field(default_factory=IndicatorHennemannGassner)
     volume_integralFR: VolumeIntegralFR = field(default_factory=VolumeIntegralFR)
     volume_flux_fv: object = field(default_factory=FluxLaxFriedrichs)
@@ -117,7 +121,8 @@ class VolumeIntegralFRShockCapturing:
     def __post_init__(self):
         name = self.reconstruction if isinstance(self.reconstruction, str) else type(self.reconstruction).__name__
         codes = {"FirstOrderReconstruction": _lib.TLW_RECONSTRUCTION_FIRST_ORDER,
-                 "MUSCLReconstruction": _lib.TLW_RECONSTRUCTION_MUSCL}
+                 "MUSCLReconstruction": _lib.TLW_RECONSTRUCTION_MUSCL,
+                 "MUSCLHancockReconstruction": _lib.TLW_RECONSTRUCTION_MUSCL_HANCOCK}
         if name not in codes:
             raise NotImplementedError(f"{name} subcells are not built")
         self.reconstruction_code = codes[name]
