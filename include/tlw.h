@@ -188,6 +188,18 @@ int tlw_dd_begin(tlw_handle* h, double cfl, double fixed_dt, double t_end);
 int tlw_dd_volume(tlw_handle* h);
 int tlw_dd_finish(tlw_handle* h);
 
+/* L2 mortars of a curvilinear mesh after an AMR step (the reference's P4estMesh path: prolong2mortars! and
+ * calc_mortar_flux!, src/solvers/dgsem_p4est/dg_2d.jl:395-603, with Trixi's mortar_fluxes_to_elements!), after
+ * tlw_set_curved_mesh and before tlw_set_curved_boundaries. Mortar k: the small elements at positions 1 and 2
+ * (1-based; position 1 at the start of the large face's forward index) on small_faces[k], the large element on
+ * large_faces[k] (faces 0: -xi, 1: +xi, 2: -eta, 3: +eta), and whether the large face's index runs backwards
+ * along the mortar (P4est node_indices :i_backward); the small faces run forward. As the reference, the large
+ * side's normal flux is its instantaneous Trixi.flux(u, -n_large / 2), and the large face receives -2 times the
+ * L2 projection of the small faces' fluxes. LW or MDRK, FR volume integral, Euler, no positivity limiter. */
+int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* small1, const int64_t* small2,
+                           const int32_t* small_faces, const int64_t* large, const int32_t* large_faces,
+                           const int32_t* large_reversed);
+
 /* Subcell reconstruction of the blended elements under shock capturing on a curvilinear mesh (the reference's
  * VolumeIntegralFRShockCapturing(...; reconstruction), src/solvers/dgsem_tree/dg_2d.jl:251-365):
  * TLW_RECONSTRUCTION_FIRST_ORDER (FirstOrderReconstruction, the default) or TLW_RECONSTRUCTION_MUSCL

@@ -182,6 +182,22 @@ int oracle_set_curved_boundaries(oracle_handle* h, int B, const int32_t* elem, c
     return 0;
 }
 
+// L2 mortars of a curvilinear mesh (0-based elements): small elements at positions 1, 2, their face, the large
+// element, its face and whether its index runs backwards along the mortar
+int oracle_set_curved_mortars(oracle_handle* h, int M, const int32_t* small1, const int32_t* small2, const int32_t* sface,
+                              const int32_t* large, const int32_t* lface, const int32_t* lrev) {
+    if (!h->curved) return 1;
+    CurvedMesh& m = h->cmesh;
+    m.n_mortars = M;
+    m.m_small1.assign(small1, small1 + M);
+    m.m_small2.assign(small2, small2 + M);
+    m.m_sface.assign(sface, sface + M);
+    m.m_large.assign(large, large + M);
+    m.m_lface.assign(lface, lface + M);
+    m.m_lrev.assign(lrev, lrev + M);
+    return 0;
+}
+
 // per boundary: 0 time-averaged Dirichlet, 1 slip wall vertical, 2 slip wall horizontal
 int oracle_set_boundary_kinds(oracle_handle* h, const int32_t* kinds) {
     if (h->curved) return 1;

@@ -41,6 +41,7 @@ def lib():
         L.oracle_set_temporal_errors.argtypes = [P, i32, dbl, dbl]
         L.oracle_set_shock_capturing.argtypes = [P, i32, dbl, dbl, i32]
         L.oracle_set_reconstruction.argtypes = [P, i32]
+        L.oracle_set_curved_mortars.argtypes = [P, i32, P, P, P, P, P, P]
         L.oracle_set_boundary_data.argtypes = [P, P, P]
         L.oracle_rhs.argtypes = [P, i32, P, P, P, dbl, dbl, i32]
         L.oracle_get.argtypes = [P, i32, P]
@@ -138,6 +139,9 @@ class Oracle:
                                             _p(pe), _p(pf), _p(se), _p(sf), _p(rv))
         if not self.h:
             raise RuntimeError("oracle_create_curved failed")
+        if getattr(cm, "n_mortars", 0):
+            self.set_curved_mortars(cm.mortar_small1, cm.mortar_small2, cm.mortar_small_faces, cm.mortar_large,
+                                    cm.mortar_large_faces, cm.mortar_large_reversed)
 
     def __del__(self):
         try:
@@ -169,6 +173,13 @@ class Oracle:
         self._cbkeep = (np.ascontiguousarray(np.asarray(elements) - 1, dtype=np.int32),
                         np.ascontiguousarray(faces, dtype=np.int32), np.ascontiguousarray(kinds, dtype=np.int32))
         assert lib().oracle_set_curved_boundaries(self.h, len(self._cbkeep[0]), *[_p(a) for a in self._cbkeep]) == 0
+
+    def set_curved_mortars(self, small1, small2, small_faces, large, large_faces, large_reversed):
+        """L2 mortars of a curvilinear mesh: elements 1-based, faces 0..3."""
+        a = [np.ascontiguousarray(np.asarray(x) - (1 if k in (0, 1, 3) else 0), dtype=np.int32)
+             for k, x in enumerate((small1, small2, small_faces, large, large_faces, large_reversed))]
+        self._mkeep = a
+        assert lib().oracle_set_curved_mortars(self.h, len(a[0]), *[_p(x) for x in a]) == 0
 
     def set_walls(self, kinds, data):
         """Navier-Stokes walls per boundary (1 no-slip adiabatic, 2 no-slip isothermal), data [B, l, 3] =

@@ -34,6 +34,10 @@ struct CurvedMesh {
     // boundary faces (P4estMesh boundaries: element, face) with their condition (BC_SLIP_WALL_*)
     int n_boundaries = 0;
     std::vector<int32_t> b_elem, b_face, b_kind;
+    // L2 mortars (P4estMesh): two small elements (positions 1, 2 along the large face's forward index) on their
+    // face m_sface, the large element on m_lface, whose index runs backwards along the mortar when m_lrev
+    int n_mortars = 0;
+    std::vector<int32_t> m_small1, m_small2, m_sface, m_large, m_lface, m_lrev;
 };
 
 // node (i, j) of face f at face index l
@@ -243,6 +247,87 @@ inline void calc_boundary_flux_curved(const Basis& b, const Euler& eq, const Opt
     }
 }
 
+// Trixi flux(u, normal_direction, equations) of CompressibleEulerEquations2D
+inline void euler_flux_along(const Euler& eq, const double* u, const double* nrm, double* f) {
+    double rho, v1, v2, p;
+    eq.cons2prim(u, rho, v1, v2, p);
+    const double vn = v1 * nrm[0] + v2 * nrm[1];
+    const double rvn = rho * vn;
+    f[0] = rvn;
+    f[1] = rvn * v1 + p * nrm[0];
+    f[2] = rvn * v2 + p * nrm[1];
+    f[3] = (u[3] + p) * vn;
+}
+
+// L2 mortars of a curvilinear mesh as the reference's P4estMesh path computes them (prolong2mortars! and
+// calc_mortar_flux!, src/solvers/dgsem_p4est/dg_2d.jl:395-603, with Trixi's mortar_fluxes_to_elements!): the
+// small side keeps its time-averaged U and F.n along its own outward normal; the large side's u and U are
+// interpolated onto the small faces (forward operators), and its normal flux is the instantaneous
+// Trixi.flux(u, -n_large / 2) (the reference overwrites the time-averaged product, :455-458); the surface flux
+// takes the small side as _ll in the curvilinear order along the small element's normal. The small faces get
+// fstar, the large face -2 times its L2 projection (reverse operators), in its own index order.
+inline void calc_mortar_flux_curved(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m,
+                                    const double* u, Workspace& ws, bool& bad) {
+    const int n = b.n;
+    for (int k = 0; k < m.n_mortars; ++k) {
+        const int lg = m.m_large[k], lf = m.m_lface[k], sf = m.m_sface[k];
+        const bool rev = m.m_lrev[k] != 0;
+        std::vector<double> ub(n * NV), Ub(n * NV), Fb(n * NV), fstar(2 * n * NV);
+        for (int i = 0; i < n; ++i) {
+            const int li = rev ? n - 1 - i : i;
+            int il, jl;
+            face_node(n, lf, li, il, jl);
+            double nL[2];
+            outward_normal(m, n, lf, il, jl, lg, nL);
+            nL[0] *= -0.5;
+            nL[1] *= -0.5;
+            for (int v = 0; v < NV; ++v) {
+                ub[i * NV + v] = u[idx_u(n, v, il, jl, lg)];
+                Ub[i * NV + v] = ws.U[idx_u(n, v, il, jl, lg)];
+            }
+            euler_flux_along(eq, &ub[i * NV], nL, &Fb[i * NV]);
+        }
+        for (int h = 0; h < 2; ++h) {
+            const int se = h ? m.m_small2[k] : m.m_small1[k];
+            const std::vector<double>& fwd = h ? b.fwd_upper : b.fwd_lower;
+            for (int l = 0; l < n; ++l) {
+                int is, js;
+                face_node(n, sf, l, is, js);
+                double nS[2], f_ll[NV], u_ll[NV], U_ll[NV], u_rr[NV] = {0, 0, 0, 0}, U_rr[NV] = {0, 0, 0, 0},
+                                                            f_rr[NV] = {0, 0, 0, 0};
+                outward_normal(m, n, sf, is, js, se, nS);
+                for (int v = 0; v < NV; ++v) {
+                    f_ll[v] = ws.F[idx_F(n, v, 0, is, js, se)] * nS[0] + ws.F[idx_F(n, v, 1, is, js, se)] * nS[1];
+                    u_ll[v] = u[idx_u(n, v, is, js, se)];
+                    U_ll[v] = ws.U[idx_u(n, v, is, js, se)];
+                }
+                for (int i = 0; i < n; ++i) {
+                    const double c = fwd[l * n + i];
+                    for (int v = 0; v < NV; ++v) {
+                        u_rr[v] += c * ub[i * NV + v];
+                        U_rr[v] += c * Ub[i * NV + v];
+                        f_rr[v] += c * Fb[i * NV + v];
+                    }
+                }
+                double* out = &fstar[(h * n + l) * NV];
+                bool b_ = false;
+                lw_surface_flux_normal(eq, opt.flux_kind, opt.speed_kind, f_ll, f_rr, u_ll, u_rr, U_ll, U_rr, nS, out, b_);
+                bad = bad || b_;
+                for (int v = 0; v < NV; ++v) ws.surface_flux_values[v + NV * (l + n * (sf + 4 * (size_t)se))] = out[v];
+            }
+        }
+        for (int i = 0; i < n; ++i) {
+            const int li = rev ? n - 1 - i : i;
+            for (int v = 0; v < NV; ++v) {
+                double acc = 0.0;
+                for (int l = 0; l < n; ++l)
+                    acc += b.rev_upper[i * n + l] * fstar[(n + l) * NV + v] + b.rev_lower[i * n + l] * fstar[l * NV + v];
+                ws.surface_flux_values[v + NV * (li + n * (lf + 4 * (size_t)lg))] = -2.0 * acc;
+            }
+        }
+    }
+}
+
 // surface integral (outward fluxes) and apply_jacobian (per node) on a curvilinear mesh
 inline void surface_integral_and_jacobian_curved(const Basis& b, const CurvedMesh& m, double* du, const Workspace& ws,
                                                  int nthreads = 1) {
@@ -322,6 +407,9 @@ inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, cons
             }
         }
     }
+    ws.bad = ws.bad || bad;
+    bad = false;
+    calc_mortar_flux_curved(b, eq, opt, m, u, ws, bad);
     ws.bad = ws.bad || bad;
     // MDRK stage 1 scales the time averages by 1/2 (as the P4estMesh path does, multi_derivative_2d.jl:34)
     calc_boundary_flux_curved(b, eq, opt, m, u, ws, bd, kind == 1 ? 0.5 : 1.0);

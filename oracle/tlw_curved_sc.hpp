@@ -437,6 +437,7 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
                           double* du, double dt, Workspace& ws, int nthreads = 1, const BoundaryData* bd = nullptr,
                           int kind = 0, const double* u2 = nullptr) {
     if (opt.flux_kind != RUSANOV) throw std::invalid_argument("curvilinear shock capturing: Rusanov surface flux");
+    if (m.n_mortars > 0) throw std::invalid_argument("curvilinear shock capturing: conforming meshes");
     const int n = b.n, nn = n * n;
     const size_t ndof = (size_t)NV * nn * m.n_elements;
     const double nan = std::numeric_limits<double>::quiet_NaN();

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "trixilw", "libtlw.so")
 SOURCES = ["tlw_capi.cu", "tlw_noalloc.cu", "tlw_batch.cu", "tlw_adjoint.cu"]
-HEADERS = ["tlw_device.cuh", "tlw_volume.cuh", "tlw_surface.cuh", "tlw_basis.h", "tlw_handle.h", "tlw_curved.cuh", "tlw_mortar.cuh", "tlw_parabolic.cuh", "tlw_limiter.cuh", "tlw_halo.cuh"]
+HEADERS = ["tlw_device.cuh", "tlw_volume.cuh", "tlw_surface.cuh", "tlw_basis.h", "tlw_handle.h", "tlw_curved.cuh", "tlw_mortar.cuh", "tlw_parabolic.cuh", "tlw_limiter.cuh", "tlw_halo.cuh", "tlw_curved_mortar.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 

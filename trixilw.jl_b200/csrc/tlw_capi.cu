@@ -13,6 +13,7 @@
 #include "../../include/tlw.h"
 #include "tlw_basis.h"
 #include "tlw_curved.cuh"
+#include "tlw_curved_mortar.cuh"
 #include "tlw_handle.h"
 #include "tlw_mortar.cuh"
 #include "tlw_limiter.cuh"
@@ -86,6 +87,10 @@ void free_mesh(tlw_handle* h) {
     if (h->d_cbk) { cudaFree(h->d_cbk); h->d_cbk = nullptr; }
     if (h->d_cbi) { cudaFree(h->d_cbi); h->d_cbi = nullptr; }
     h->ncb = h->ncbx = 0;
+    for (int** d : {&h->d_cms1, &h->d_cms2, &h->d_cml, &h->d_cmc})
+        if (*d) { cudaFree(*d); *d = nullptr; }
+    h->ncm = 0;
+    h->mortar_off.clear();
     h->curved = false;
     h->have_mesh = false;
     h->have_bdata = false;
@@ -363,6 +368,13 @@ template <int N> struct Par {
 template <int N> struct ParSpd { static void run(cudaStream_t s, const tlw_handle* h, const double* u) { Launch<N>::par_speed(s, h, u); } };
 template <int N> struct ParAttr { static void run() { Launch<N>::par_attributes(); } };
 template <int N> struct Mrt { static void run(cudaStream_t s, const MortarArgs& a) { Launch<N>::mortars(s, a); } };
+template <int N> struct CMrt {
+    static void run(cudaStream_t s, const CurvedMortarArgs& a) {
+        if (a.count == 0) return;
+        using M = MortarCfg<N>;
+        curved_mortar_kernel<N><<<(a.count + M::PER_CTA - 1) / M::PER_CTA, M::THREADS, 0, s>>>(a);
+    }
+};
 template <int N> struct CIfc { static void run(cudaStream_t s, const CurvedSurfArgs& a) { Launch<N>::curved_interfaces(s, a); } };
 template <int N> struct Halo {
     static void run(cudaStream_t s, const HaloArgs& a, bool pack) {
@@ -509,6 +521,32 @@ void enqueue_curved_surfaces(tlw_handle* h, int mode, const double* u_jump, doub
         if (ev && c == 0) cudaEventRecord(ev->after_x, h->stream);
     }
     if (ev && h->color_off.size() <= 2) cudaEventRecord(ev->after_x, h->stream);
+    if (h->ncm > 0) {
+        CurvedMortarArgs ma{};
+        ma.u = u_jump;
+        ma.out = out;
+        ma.tU = h->d_tU;
+        ma.tF = h->d_tF;
+        ma.metrics = h->d_Ja;
+        ma.inv_jac = h->d_ijn;
+        ma.dt = dt_ptr;
+        ma.step_mode = mode == MODE_STEP;
+        ma.gamma = h->opts.gamma;
+        ma.flux_kind = h->opts.surface_flux;
+        ma.speed_kind = h->opts.max_speed;
+        ma.inv_w_first = h->h_basis.inv_w_first;
+        ma.inv_w_last = h->h_basis.inv_w_last;
+        ma.status = &h->d_step->status;
+        for (size_t c = 0; c + 1 < h->mortar_off.size(); ++c) {
+            const int b = h->mortar_off[c];
+            ma.small1 = h->d_cms1 + b;
+            ma.small2 = h->d_cms2 + b;
+            ma.large = h->d_cml + b;
+            ma.code = h->d_cmc + b;
+            ma.count = h->mortar_off[c + 1] - b;
+            dispatch<CMrt>(h->N, h->stream, ma);
+        }
+    }
     if (h->ncb > 0) {
         CurvedBndArgs cb{};
         cb.u = u_jump;
@@ -1274,6 +1312,76 @@ int tlw_dd_finish(tlw_handle* h) {
     return TLW_OK;
 }
 
+int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* small1, const int64_t* small2,
+                           const int32_t* small_faces, const int64_t* large, const int32_t* large_faces,
+                           const int32_t* large_reversed) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh || !h->curved) return fail(h, TLW_E_STATE, "curved mortars follow tlw_set_curved_mesh");
+    if (h->sc || h->parabolic || h->lim_count > 0 || h->ncb > 0)
+        return fail(h, TLW_E_UNSUPPORTED,
+                    "curvilinear mortars: before the boundaries, without shock capturing, Navier-Stokes or the limiter");
+    if (n_mortars < 0 || (n_mortars > 0 && (!small1 || !small2 || !small_faces || !large || !large_faces || !large_reversed)))
+        return fail(h, TLW_E_ARG, "mortars");
+    struct Mtr { int s1, s2, l, code, cs, cl; };
+    std::vector<Mtr> all;
+    std::vector<signed char> used = h->face_used;
+    for (int64_t k = 0; k < n_mortars; ++k) {
+        const int64_t a = small1[k] - 1, b = small2[k] - 1, g = large[k] - 1;
+        const int sf = small_faces[k], lf = large_faces[k], rv = large_reversed[k];
+        if (a < 0 || a >= h->E || b < 0 || b >= h->E || g < 0 || g >= h->E || sf < 0 || sf > 3 || lf < 0 || lf > 3 ||
+            (rv != 0 && rv != 1) || a == b || a == g || b == g)
+            return fail(h, TLW_E_ARG, "mortar " + std::to_string(k + 1) + " out of range");
+        for (size_t f : {(size_t)a * 4 + sf, (size_t)b * 4 + sf, (size_t)g * 4 + lf}) {
+            if (used[f]) return fail(h, TLW_E_ARG, "mortar " + std::to_string(k + 1) + ": element face used twice");
+            used[f] = 1;
+        }
+        all.push_back(Mtr{(int)a, (int)b, (int)g, sf | (lf << 2) | (rv << 4), sf >> 1, lf >> 1});
+    }
+    // colours as for the interfaces: within a colour no element has faces of both classes
+    std::vector<std::vector<signed char>> cls;
+    std::vector<std::vector<int>> bucket;
+    for (size_t k = 0; k < all.size(); ++k) {
+        const Mtr& m = all[k];
+        size_t c = 0;
+        for (; c < cls.size(); ++c) {
+            const signed char x = cls[c][m.s1], y = cls[c][m.s2], z = cls[c][m.l];
+            if ((x < 0 || x == m.cs) && (y < 0 || y == m.cs) && (z < 0 || z == m.cl)) break;
+        }
+        if (c == cls.size()) {
+            cls.emplace_back((size_t)h->E, (signed char)-1);
+            bucket.emplace_back();
+        }
+        cls[c][m.s1] = cls[c][m.s2] = (signed char)m.cs;
+        cls[c][m.l] = (signed char)m.cl;
+        bucket[c].push_back((int)k);
+    }
+    std::vector<int> v1, v2, vl, vc, off{0};
+    for (const auto& bk : bucket) {
+        for (int k : bk) {
+            v1.push_back(all[k].s1); v2.push_back(all[k].s2); vl.push_back(all[k].l); vc.push_back(all[k].code);
+        }
+        off.push_back((int)v1.size());
+    }
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    drop_graphs(h);
+    for (int** d : {&h->d_cms1, &h->d_cms2, &h->d_cml, &h->d_cmc})
+        if (*d) { cudaFree(*d); *d = nullptr; }
+    auto up = [&](int*& d, const std::vector<int>& v) -> int {
+        if (v.empty()) return TLW_OK;
+        TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
+        TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+        return TLW_OK;
+    };
+    int rc;
+    if ((rc = up(h->d_cms1, v1)) || (rc = up(h->d_cms2, v2)) || (rc = up(h->d_cml, vl)) || (rc = up(h->d_cmc, vc)))
+        return rc;
+    h->ncm = (int)n_mortars;
+    h->mortar_off = off;
+    h->face_used = used;
+    return TLW_OK;
+}
+
 int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t* elements, const int32_t* faces,
                               const int32_t* kinds) {
     if (!h) return TLW_E_ARG;
@@ -1378,6 +1486,8 @@ int tlw_set_positivity_limiter(tlw_handle* h, int32_t count, const double* thres
     if (!h) return TLW_E_ARG;
     if (count < 0 || count > TLW_LIMITER_MAX_PAIRS || (count > 0 && (!thresholds || !variables)))
         return fail(h, TLW_E_ARG, "limiter: 0..4 (threshold, variable) pairs");
+    if (count > 0 && h->ncm > 0)
+        return fail(h, TLW_E_UNSUPPORTED, "limiter: the P4estMesh mortar pass is not built (curvilinear mortars)");
     for (int p = 0; p < count; ++p)
         if (variables[p] < TLW_LIMIT_DENSITY || variables[p] > TLW_LIMIT_DENSITY_PRESSURE || !std::isfinite(thresholds[p]))
             return fail(h, TLW_E_ARG, "limiter: variable " + std::to_string(p + 1));
@@ -1403,8 +1513,8 @@ int tlw_apply_positivity_limiter(tlw_handle* h) {
 int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "the parabolic terms follow tlw_set_tree_mesh / tlw_set_curved_mesh");
-    if (h->opts.time_discretization != TLW_LW || h->sc || h->N < 3 || h->nmx + h->nmy > 0)
-        return fail(h, TLW_E_UNSUPPORTED, "Navier-Stokes: LW, FR volume integral, N >= 3, conforming TreeMesh");
+    if (h->opts.time_discretization != TLW_LW || h->sc || h->N < 3 || h->nmx + h->nmy > 0 || h->ncm > 0)
+        return fail(h, TLW_E_UNSUPPORTED, "Navier-Stokes: LW, FR volume integral, N >= 3, conforming mesh");
     if (!(mu >= 0.0) || !(prandtl > 0.0)) return fail(h, TLW_E_ARG, "mu / Prandtl");
     if (h->curved && h->ncb > 0 && h->bnd_dirichlet)
         return fail(h, TLW_E_UNSUPPORTED, "curvilinear Navier-Stokes: slip walls are built");

@@ -149,6 +149,11 @@ struct tlw_handle {
     // slip-wall kind and the boundary's index in the caller's order (wall data)
     int ncb = 0, ncbx = 0;
     int *d_cbe = nullptr, *d_cbf = nullptr, *d_cbk = nullptr, *d_cbi = nullptr;
+    // L2 mortars of the curvilinear mesh, sorted by colour: small elements (positions 1, 2), large element, and
+    // small face | large face << 2 | large reversed << 4
+    int ncm = 0;
+    int *d_cms1 = nullptr, *d_cms2 = nullptr, *d_cml = nullptr, *d_cmc = nullptr;
+    std::vector<int> mortar_off;            // mortar colour c covers [mortar_off[c], mortar_off[c + 1])
     // graphs: [start buffer] one step, two steps
     cudaGraphExec_t g_one[2] = {nullptr, nullptr};
     cudaGraphExec_t g_two[2] = {nullptr, nullptr};

@@ -4,7 +4,7 @@ the host-side mirror of the reference's Julia interface for that path."""
 from ._lib import DomainError, TlwError, lib
 from .adjoint import adjoint_solve, adjoint_step, adjoint_sweep, forward_record, lw_solve, solve_dts
 from .batch import LWBatch, solve_lwfr_batch
-from .curved_mesh import CurvedMesh, StructuredMesh, rotate_elements, rotate_state
+from .curved_mesh import CurvedMesh, RefinedStructuredMesh, StructuredMesh, rotate_elements, rotate_state
 from .equations import (CompressibleEulerEquations2D, CompressibleNavierStokesDiffusion2D, ConstantState,
                         DensityWave, FourQuadrantRiemann, GradientVariablesConservative, IsentropicVortex)
 from .limiters import PositivityPreservingLimiterZhangShu, density, density_pressure, pressure
@@ -29,7 +29,7 @@ __all__ = [
     "flux_hll", "flux_lax_friedrichs", "get_time_discretization", "lw_fourier_cfl", "rhs", "rhs_mdrk1",
     "rhs_mdrk2", "semidiscretize", "trixi2lw", "LWBatch", "solve_lwfr_batch",
     "adjoint_solve", "adjoint_step", "adjoint_sweep", "forward_record", "lw_solve", "solve_dts",
-    "CurvedMesh", "StructuredMesh", "rotate_elements", "rotate_state", "RefinedTreeMesh",
+    "CurvedMesh", "RefinedStructuredMesh", "StructuredMesh", "rotate_elements", "rotate_state", "RefinedTreeMesh",
     "CompressibleNavierStokesDiffusion2D", "GradientVariablesConservative", "SemidiscretizationHyperbolicParabolic",
     "PositivityPreservingLimiterZhangShu", "density", "pressure", "density_pressure",
     "boundary_condition_slip_wall_vertical", "boundary_condition_slip_wall_horizontal", "NoSlip", "Adiabatic",

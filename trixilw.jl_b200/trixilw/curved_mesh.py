@@ -41,9 +41,11 @@ def metric_terms(xy: np.ndarray, polydeg: int):
 class CurvedMesh:
     """A conforming curvilinear mesh in the form the library takes: per node metric terms and per
     interface (primary element, face; secondary element, face; secondary index reversed). Faces 0: -xi
-    (i = 1), 1: +xi (i = n), 2: -eta (j = 1), 3: +eta (j = n); elements 1-based as Trixi stores them."""
+    (i = 1), 1: +xi (i = n), 2: -eta (j = 1), 3: +eta (j = n); elements 1-based as Trixi stores them.
+    A non-conforming one (RefinedStructuredMesh) also lists L2 mortars (mortar_* arrays)."""
 
     n_boundaries = 0
+    n_mortars = 0
 
     def __init__(self, xy: np.ndarray, polydeg: int, primary_elements, primary_faces, secondary_elements,
                  secondary_faces, secondary_reversed, area: float, boundary_elements=(), boundary_faces=(),
@@ -166,6 +168,124 @@ class StructuredMesh:
 
     def boundary_node_coordinates(self, polydeg: int) -> np.ndarray:
         return self.curved(polydeg).boundary_node_coordinates(polydeg)
+
+
+class RefinedStructuredMesh:
+    """A StructuredMesh{2}-like mesh with some cells refined once into four children, as a P4estMesh{2} is after an
+    AMR step: elements are the unrefined cells and the children (each in the order of its parent cell, children
+    lower-left, lower-right, upper-left, upper-right), node coordinates mapping(xi_g, eta_g) of each element's box
+    in the reference square. Faces between equal elements are interfaces (the right / upper element primary, as
+    on the StructuredMesh); a refined cell next to an unrefined one gives an L2 mortar: the two children on
+    their faces (position 1 at the smaller coordinate along the face, the large face's index running forward)
+    against the unrefined cell's face. Non-periodic directions have boundary faces, by direction."""
+
+    def __init__(self, cells_per_dimension, mapping, refined_cells, periodicity=True):
+        if isinstance(periodicity, bool):
+            periodicity = (periodicity, periodicity)
+        self.periodicity = tuple(bool(p) for p in periodicity)
+        self.cells = tuple(int(c) for c in cells_per_dimension)
+        self.mapping = mapping
+        self.refined = {(int(a), int(b)) for a, b in refined_cells}
+        nx, ny = self.cells
+        self.boxes = []          # (level, ix, iy) with ix, iy in units of the level's cell size
+        self.index = {}
+        for cy in range(ny):
+            for cx in range(nx):
+                if (cx, cy) in self.refined:
+                    for dy in (0, 1):
+                        for dx in (0, 1):
+                            self.index[(1, 2 * cx + dx, 2 * cy + dy)] = len(self.boxes)
+                            self.boxes.append((1, 2 * cx + dx, 2 * cy + dy))
+                else:
+                    self.index[(0, cx, cy)] = len(self.boxes)
+                    self.boxes.append((0, cx, cy))
+        self.n_elements = len(self.boxes)
+        self._curved = {}
+
+    def node_coordinates(self, polydeg: int) -> np.ndarray:
+        nodes, _ = gauss_lobatto(polydeg)
+        nx, ny = self.cells
+        n = len(nodes)
+        XI = np.empty((n, n, self.n_elements))
+        ETA = np.empty((n, n, self.n_elements))
+        for e, (lev, ix, iy) in enumerate(self.boxes):
+            s = 1 << lev
+            xi = (ix + 0.5 * (nodes + 1.0)) * (2.0 / (nx * s)) - 1.0
+            eta = (iy + 0.5 * (nodes + 1.0)) * (2.0 / (ny * s)) - 1.0
+            XI[:, :, e] = xi[:, None]
+            ETA[:, :, e] = eta[None, :]
+        x, y = self.mapping(XI, ETA)
+        return np.stack([np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64)])
+
+    def _cell_refined(self, cx, cy):
+        return (cx % self.cells[0], cy % self.cells[1]) in self.refined
+
+    def curved(self, polydeg: int) -> CurvedMesh:
+        if polydeg in self._curved:
+            return self._curved[polydeg]
+        nx, ny = self.cells
+        px, py = self.periodicity
+        pe, pf, se, sf = [], [], [], []
+        ms1, ms2, msf, ml, mlf = [], [], [], [], []
+        bnd = {0: [], 1: [], 2: [], 3: []}
+        for e, (lev, ix, iy) in enumerate(self.boxes):
+            s = 1 << lev
+            for d in (0, 1):   # the element's + face in direction d: +xi (face 1) or +eta (face 3)
+                jx, jy = (ix + 1, iy) if d == 0 else (ix, iy + 1)
+                cells_d = (nx if d == 0 else ny) * s
+                at_edge = (jx if d == 0 else jy) == cells_d
+                periodic = px if d == 0 else py
+                if at_edge and not periodic:
+                    bnd[2 * d + 1].append((e, 2 * d + 1))
+                    continue
+                jx, jy = jx % (nx * s), jy % (ny * s)
+                # the neighbour cell at the base level and whether it is refined
+                bx, by = (jx // s, jy // s)
+                nref = (bx, by) in self.refined
+                if lev == 0 and nref:
+                    # mortar: this (large) element's + face against the two children on their - faces
+                    if d == 0:
+                        kids = [self.index[(1, 2 * bx, 2 * by)], self.index[(1, 2 * bx, 2 * by + 1)]]
+                    else:
+                        kids = [self.index[(1, 2 * bx, 2 * by)], self.index[(1, 2 * bx + 1, 2 * by)]]
+                    ms1.append(kids[0]); ms2.append(kids[1]); msf.append(2 * d); ml.append(e); mlf.append(2 * d + 1)
+                elif lev == 1 and not nref:
+                    # the neighbour is a large element: a mortar, once per pair of children (the lower / left one)
+                    if (iy if d == 0 else ix) % 2 == 0:
+                        large = self.index[(0, bx, by)]
+                        if d == 0:
+                            kids = [e, self.index[(1, ix, iy + 1)]]
+                        else:
+                            kids = [e, self.index[(1, ix + 1, iy)]]
+                        ms1.append(kids[0]); ms2.append(kids[1]); msf.append(2 * d + 1); ml.append(large); mlf.append(2 * d)
+                else:
+                    other = self.index[(lev, jx, jy)]
+                    pe.append(other); pf.append(2 * d); se.append(e); sf.append(2 * d + 1)
+            # the element's - faces on a non-periodic edge
+            for d in (0, 1):
+                if (ix if d == 0 else iy) == 0 and not (px if d == 0 else py):
+                    bnd[2 * d].append((e, 2 * d))
+        be = [b[0] for f in (0, 1, 2, 3) for b in bnd[f]]
+        bf = [b[1] for f in (0, 1, 2, 3) for b in bnd[f]]
+        per = np.array([len(bnd[f]) for f in (0, 1, 2, 3)], dtype=np.int64)
+        xy = self.node_coordinates(polydeg)
+        area = float(np.einsum("eji,j,i->", 1.0 / metric_terms(xy, polydeg)[1], *(2 * [gauss_lobatto(polydeg)[1]])))
+        cm = CurvedMesh(xy, polydeg, np.array(pe) + 1, pf, np.array(se) + 1, sf, np.zeros(len(pe), dtype=np.int32),
+                        area, np.array(be, dtype=np.int64) + 1, bf, per)
+        cm.n_mortars = len(ml)
+        cm.mortar_small1 = np.array(ms1, dtype=np.int64) + 1
+        cm.mortar_small2 = np.array(ms2, dtype=np.int64) + 1
+        cm.mortar_small_faces = np.array(msf, dtype=np.int32)
+        cm.mortar_large = np.array(ml, dtype=np.int64) + 1
+        cm.mortar_large_faces = np.array(mlf, dtype=np.int32)
+        cm.mortar_large_reversed = np.zeros(len(ml), dtype=np.int32)
+        self.n_boundaries_per_direction = per
+        self.n_boundaries = int(per.sum())
+        self._curved[polydeg] = cm
+        return cm
+
+    def ndofs(self, polydeg: int) -> int:
+        return self.n_elements * (polydeg + 1) ** 2
 
 
 # rotation of an element's local frame by a quarter turn: new node (a, b) holds old node (n-1-b, a);

@@ -293,15 +293,15 @@ class SemidiscretizationHyperbolic:
                  source_terms=None):
         if source_terms is not None:
             raise NotImplementedError("source terms are not built on the device path")
-        from .curved_mesh import CurvedMesh, StructuredMesh
-        if isinstance(mesh, StructuredMesh):
+        from .curved_mesh import CurvedMesh, RefinedStructuredMesh, StructuredMesh
+        if isinstance(mesh, (StructuredMesh, RefinedStructuredMesh)):
             self.curved = mesh.curved(solver.polydeg)
         elif isinstance(mesh, CurvedMesh):
             self.curved = mesh
         elif isinstance(mesh, (TreeMesh, RefinedTreeMesh)):
             self.curved = None
         else:
-            raise NotImplementedError("TreeMesh{2}, StructuredMesh{2} and conforming curvilinear meshes are built")
+            raise NotImplementedError("TreeMesh{2}, StructuredMesh{2} and curvilinear meshes (with L2 mortars) are built")
         self.mesh = mesh
         self.equations = equations
         self.initial_condition = initial_condition
@@ -365,6 +365,15 @@ class SemidiscretizationHyperbolic:
                                            _i64p(arrs[0]), i32p(arrs[1]), _i64p(arrs[2]), i32p(arrs[3]),
                                            i32p(arrs[4]))
             check(self.handle, rc)
+            if getattr(c, "n_mortars", 0):
+                mk = (np.ascontiguousarray(c.mortar_small1, dtype=np.int64),
+                      np.ascontiguousarray(c.mortar_small2, dtype=np.int64),
+                      np.ascontiguousarray(c.mortar_small_faces, dtype=np.int32),
+                      np.ascontiguousarray(c.mortar_large, dtype=np.int64),
+                      np.ascontiguousarray(c.mortar_large_faces, dtype=np.int32),
+                      np.ascontiguousarray(c.mortar_large_reversed, dtype=np.int32))
+                self._mkeep = mk
+                check(self.handle, lib().tlw_set_curved_mortars(self.handle, c.n_mortars, *[_ptr(a) for a in mk]))
             return
         m = self.mesh
         ij = np.ascontiguousarray(m.inverse_jacobian, dtype=np.float64)
