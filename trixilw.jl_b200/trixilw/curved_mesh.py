@@ -200,7 +200,17 @@ class RefinedStructuredMesh:
                     self.index[(0, cx, cy)] = len(self.boxes)
                     self.boxes.append((0, cx, cy))
         self.n_elements = len(self.boxes)
+        px, py = self.periodicity
+        side = lambda cells: sum(2 if c in self.refined else 1 for c in cells)
+        self.n_boundaries_per_direction = np.array(
+            [0 if px else side([(0, cy) for cy in range(ny)]), 0 if px else side([(nx - 1, cy) for cy in range(ny)]),
+             0 if py else side([(cx, 0) for cx in range(nx)]), 0 if py else side([(cx, ny - 1) for cx in range(nx)])],
+            dtype=np.int64)
+        self.n_boundaries = int(self.n_boundaries_per_direction.sum())
         self._curved = {}
+
+    def boundary_node_coordinates(self, polydeg: int) -> np.ndarray:
+        return self.curved(polydeg).boundary_node_coordinates(polydeg)
 
     def node_coordinates(self, polydeg: int) -> np.ndarray:
         nodes, _ = gauss_lobatto(polydeg)
@@ -279,8 +289,7 @@ class RefinedStructuredMesh:
         cm.mortar_large = np.array(ml, dtype=np.int64) + 1
         cm.mortar_large_faces = np.array(mlf, dtype=np.int32)
         cm.mortar_large_reversed = np.zeros(len(ml), dtype=np.int32)
-        self.n_boundaries_per_direction = per
-        self.n_boundaries = int(per.sum())
+        assert np.array_equal(per, self.n_boundaries_per_direction)
         self._curved[polydeg] = cm
         return cm
 
