@@ -195,7 +195,9 @@ int tlw_dd_finish(tlw_handle* h);
  * large_faces[k] (faces 0: -xi, 1: +xi, 2: -eta, 3: +eta), and whether the large face's index runs backwards
  * along the mortar (P4est node_indices :i_backward); the small faces run forward. As the reference, the large
  * side's normal flux is its instantaneous Trixi.flux(u, -n_large / 2), and the large face receives -2 times the
- * L2 projection of the small faces' fluxes. LW or MDRK, FR volume integral, Euler, no positivity limiter. */
+ * L2 projection of the small faces' fluxes. LW or MDRK, FR volume integral, Euler; the positivity limiter then runs
+ * the P4estMesh limit_mortars! (src/callbacks/callbacks_stage/positivity_zhang_shu_dg2d.jl:178-260) after its
+ * element pass. */
 int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* small1, const int64_t* small2,
                            const int32_t* small_faces, const int64_t* large, const int32_t* large_faces,
                            const int32_t* large_reversed);

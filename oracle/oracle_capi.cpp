@@ -56,6 +56,12 @@ void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, do
     rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, kind, u2, bd);
 }
 
+// one application of the positivity limiter on whichever mesh the handle holds
+void limit(oracle_handle* h, double* u) {
+    if (h->curved) apply_positivity_limiter_curved(h->basis, h->eq, h->cmesh, h->lim, u);
+    else apply_positivity_limiter(h->basis, h->eq, h->mesh, h->n_elements(), h->lim, u);
+}
+
 double any_max_dt(oracle_handle* h, const double* u, double cfl, bool& bad, int nthreads) {
     if (h->parabolic && h->curved) return max_dt_parabolic_curved(h->basis, h->eq, h->ns, h->cmesh, u, cfl, bad, nthreads);
     if (h->parabolic) return max_dt_parabolic(h->basis, h->eq, h->ns, h->mesh, u, cfl, bad, nthreads);
@@ -340,7 +346,7 @@ int oracle_steps(oracle_handle* h, int kind, double* u, int nsteps, double cfl, 
         // which the previous step's application has limited already)
         if (!h->lim.thresholds.empty())
             for (int a = 0; a < (kind == 0 ? 2 : 1); ++a)
-                apply_positivity_limiter(h->basis, h->eq, h->mesh, h->n_elements(), h->lim, u);
+                limit(h, u);
         t += dt;
     }
     *t_inout = t;
@@ -364,7 +370,7 @@ int oracle_set_limiter(oracle_handle* h, int count, const double* thresholds, co
 
 // one application of the limiter to u in place
 int oracle_apply_limiter(oracle_handle* h, double* u) {
-    apply_positivity_limiter(h->basis, h->eq, h->mesh, h->n_elements(), h->lim, u);
+    limit(h, u);
     return 0;
 }
 

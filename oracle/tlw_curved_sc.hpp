@@ -511,4 +511,47 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
     surface_integral_and_jacobian_curved(b, m, du, ws, nthreads);
 }
 
+// limit_mortars! for P4estMesh{2} (src/callbacks/callbacks_stage/positivity_zhang_shu_dg2d.jl:178-260): per
+// mortar in order, the large element's face in the mortar's forward order interpolated onto both halves; the
+// minimum of the variable over the first four nodes of each half (the loop `for i = 1:4`); theta = min(|(mean -
+// threshold) / (mean - min)|, 1) blends the large element unconditionally.
+inline void limit_mortars_p4est(const Basis& b, const Euler& eq, const CurvedMesh& m, double* u, double threshold,
+                                int variable) {
+    const int n = b.n;
+    std::vector<double> face(n * NV);
+    for (int k = 0; k < m.n_mortars; ++k) {
+        const int le = m.m_large[k], lf = m.m_lface[k];
+        const bool rev = m.m_lrev[k] != 0;
+        for (int i = 0; i < n; ++i) {
+            int il, jl;
+            face_node(n, lf, rev ? n - 1 - i : i, il, jl);
+            for (int v = 0; v < NV; ++v) face[i * NV + v] = u[idx_u(n, v, il, jl, le)];
+        }
+        double mean[NV];
+        element_mean(b, u, le, mean);
+        const double vmean = limiter_value(eq, variable, mean);
+        double vmin = std::numeric_limits<double>::infinity();
+        for (int jm = 0; jm < std::min(4, n); ++jm) {
+            double lo[NV] = {0, 0, 0, 0}, up[NV] = {0, 0, 0, 0};
+            for (int l = 0; l < n; ++l)
+                for (int v = 0; v < NV; ++v) {
+                    lo[v] += b.fwd_lower[jm * n + l] * face[l * NV + v];
+                    up[v] += b.fwd_upper[jm * n + l] * face[l * NV + v];
+                }
+            vmin = julia_min(julia_min(vmin, limiter_value(eq, variable, lo)), limiter_value(eq, variable, up));
+        }
+        const double theta = julia_min(std::fabs((vmean - threshold) / (vmean - vmin)), 1.0);
+        blend_element(b, u, le, theta, mean);
+    }
+}
+
+// one application of the limiter on a curvilinear mesh: every pair in order, elements then the mortars
+inline void apply_positivity_limiter_curved(const Basis& b, const Euler& eq, const CurvedMesh& m,
+                                            const PositivityLimiter& lim, double* u) {
+    for (size_t p = 0; p < lim.thresholds.size(); ++p) {
+        limit_elements(b, eq, m.n_elements, u, lim.thresholds[p], lim.variables[p]);
+        if (m.n_mortars > 0) limit_mortars_p4est(b, eq, m, u, lim.thresholds[p], lim.variables[p]);
+    }
+}
+
 }  // namespace tlwo

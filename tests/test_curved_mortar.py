@@ -123,3 +123,52 @@ def test_gpu_curved_mortar_with_walls_matches_oracle(oracle_mod, tl):
     s, _ = o.steps(u_cpu, 8, 0.3, 0.0, 1e9, nthreads=NTH)
     assert s == integ.iter == 8
     assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-12)
+
+
+def noisy_constant(cm, N, seed=4):
+    """rho = 1 (+-30 %), p = 1 (+-50 %) node noise at rest: nodes below the limiter's thresholds, element means
+    above them."""
+    rng = np.random.default_rng(seed)
+    k = cm.n_elements * (N + 1) ** 2
+    rho = 1.0 + 0.3 * rng.uniform(-1.0, 1.0, k)
+    p = 1.0 + 0.5 * rng.uniform(-1.0, 1.0, k)
+    return np.stack([rho, 0 * rho, 0 * rho, p / 0.4], axis=-1).reshape(-1)
+
+
+@pytest.mark.parametrize("N", [3, 4])
+def test_oracle_curved_mortar_limiter_acts_on_large_elements(oracle_mod, tl, N):
+    """The P4estMesh limit_mortars! blends large elements whose mortar trace dips below the threshold."""
+    cm = refined(tl).curved(N)
+    o = oracle_mod.Oracle(cm, N)
+    u = noisy_constant(cm, N)
+    o.set_positivity_limiter((0.8, 0.6), (0, 1))
+    lim = o.apply_positivity_limiter(u)
+    nn = 4 * (N + 1) ** 2
+    changed = np.any(lim.reshape(-1, nn) != u.reshape(-1, nn), axis=1)
+    assert changed[cm.mortar_large - 1].any()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N", [3, 4, 5])
+def test_gpu_curved_mortar_limiter_matches_oracle(oracle_mod, tl, N):
+    from trixilw import limiters
+    m = refined(tl)
+    cm = m.curved(N)
+    semi = make_semi(tl, m, N)
+    u = noisy_constant(cm, N)
+    thr = (0.8, 0.6)
+    o = oracle_mod.Oracle(cm, N)
+    o.set_positivity_limiter(thr, (0, 1))
+    expect = o.apply_positivity_limiter(u)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, semi.time_discretization, (0.0, 1.0)))
+    integ.set_state(u, 0.0)
+    limiters.install(semi, (tl.PositivityPreservingLimiterZhangShu(thr, (tl.density, tl.pressure)),))
+    tl._lib.check(semi.handle, tl._lib.lib().tlw_apply_positivity_limiter(semi.handle))
+    assert np.all(rel_l2(integ.get_state(), expect) < 1e-13)
+    # and limited steps
+    u_cpu = expect.copy()
+    integ.step(6, 0.3, use_graph=True)
+    integ.sync_time()
+    s, _ = o.steps(u_cpu, 6, 0.3, 0.0, 1e9, nthreads=NTH)
+    assert s == integ.iter == 6
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-12)

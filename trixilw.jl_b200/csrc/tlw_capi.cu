@@ -480,6 +480,7 @@ void enqueue_limiter(tlw_handle* h, double* u, int reps, unsigned long long* slo
     a.reps = reps;
     for (int p = 0; p < h->lim_count; ++p) { a.threshold[p] = h->lim_thr[p]; a.variable[p] = h->lim_var[p]; }
     a.mortar_faces = h->d_mface;
+    a.p4est = h->curved && h->ncm > 0 ? 1 : 0;
     a.cfl_slots = slots;
     a.status = &h->d_step->status;
     dispatch<Lim>(h->N, h->stream, a);
@@ -1317,9 +1318,9 @@ int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* smal
                            const int32_t* large_reversed) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh || !h->curved) return fail(h, TLW_E_STATE, "curved mortars follow tlw_set_curved_mesh");
-    if (h->sc || h->parabolic || h->lim_count > 0 || h->ncb > 0)
-        return fail(h, TLW_E_UNSUPPORTED,
-                    "curvilinear mortars: before the boundaries, without shock capturing, Navier-Stokes or the limiter");
+    if (h->sc || h->parabolic || h->ncb > 0)
+        return fail(h, TLW_E_UNSUPPORTED, "curvilinear mortars: before the boundaries, without shock capturing or "
+                                          "Navier-Stokes");
     if (n_mortars < 0 || (n_mortars > 0 && (!small1 || !small2 || !small_faces || !large || !large_faces || !large_reversed)))
         return fail(h, TLW_E_ARG, "mortars");
     struct Mtr { int s1, s2, l, code, cs, cl; };
@@ -1376,6 +1377,16 @@ int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* smal
     int rc;
     if ((rc = up(h->d_cms1, v1)) || (rc = up(h->d_cms2, v2)) || (rc = up(h->d_cml, vl)) || (rc = up(h->d_cmc, vc)))
         return rc;
+    // the positivity limiter's mortar pass: per large element its mortars in the caller's order (count in bits
+    // 0-2, then the large face and whether its index runs backwards, 3 bits each)
+    std::vector<int> desc((size_t)h->E, 0);
+    for (int64_t k = 0; k < n_mortars; ++k) {
+        const int g = (int)(large[k] - 1), c = desc[g] & 7;
+        if (c >= 4) return fail(h, TLW_E_ARG, "mortar " + std::to_string(k + 1) + ": a fifth mortar of one element");
+        desc[g] = (desc[g] & ~7) | (c + 1) | (((large_faces[k] & 3) | (large_reversed[k] << 2)) << (3 + 3 * c));
+    }
+    if (h->d_mface) { cudaFree(h->d_mface); h->d_mface = nullptr; }
+    if (n_mortars > 0 && (rc = up(h->d_mface, desc))) return rc;
     h->ncm = (int)n_mortars;
     h->mortar_off = off;
     h->face_used = used;
@@ -1486,8 +1497,6 @@ int tlw_set_positivity_limiter(tlw_handle* h, int32_t count, const double* thres
     if (!h) return TLW_E_ARG;
     if (count < 0 || count > TLW_LIMITER_MAX_PAIRS || (count > 0 && (!thresholds || !variables)))
         return fail(h, TLW_E_ARG, "limiter: 0..4 (threshold, variable) pairs");
-    if (count > 0 && h->ncm > 0)
-        return fail(h, TLW_E_UNSUPPORTED, "limiter: the P4estMesh mortar pass is not built (curvilinear mortars)");
     for (int p = 0; p < count; ++p)
         if (variables[p] < TLW_LIMIT_DENSITY || variables[p] > TLW_LIMIT_DENSITY_PRESSURE || !std::isfinite(thresholds[p]))
             return fail(h, TLW_E_ARG, "limiter: variable " + std::to_string(p + 1));

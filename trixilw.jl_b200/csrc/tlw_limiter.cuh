@@ -31,7 +31,9 @@ struct LimiterArgs {
     int reps;                           // applications of the whole pair sequence
     double threshold[LIMITER_MAX_PAIRS];
     int variable[LIMITER_MAX_PAIRS];    // 0 density, 1 pressure, 2 density_pressure
-    const int* mortar_faces;            // [e]: bits 0-2 count, then 2 bits per mortar (the large face, 0..3)
+    const int* mortar_faces;            // [e]: bits 0-2 count, then 2 bits per mortar (the large face, 0..3), or
+                                        // with p4est 3 bits (the large face, whether its index runs backwards)
+    int p4est;                          // curvilinear mortars: limit_mortars! of the P4estMesh
                                         // in mortar order; null without mortars
     unsigned long long* cfl_slots;      // or null
     unsigned* status;
@@ -115,22 +117,27 @@ static __global__ void __launch_bounds__(32 * LIMITER_WARPS) positivity_limiter_
                 const double vmean = limiter_value(a.gamma, var, m);
                 blend((vmean - thr) / (vmean - vmin), m);
             }
-            // mortar pass (limit_mortars!, :47-176), this element's mortars as the large element, in order
+            // mortar pass (limit_mortars!, :47-176 and, P4estMesh, :178-260), this element's mortars as the large
+            // element, in order; the P4estMesh pass takes the large face in the mortar's order and the first four
+            // nodes of each half only (its loop `for i = 1:4`)
             for (int q = 0; q < nmort; ++q) {
-                const int face = (desc >> (3 + 2 * q)) & 3;
+                const int face = (desc >> (3 + (a.p4est ? 3 : 2) * q)) & 3;
+                const bool rev = a.p4est && ((desc >> (3 + 3 * q + 2)) & 1);
                 double m[NV];
                 mean_of(m);
                 const double vmean = limiter_value(a.gamma, var, m);
                 // lanes 0..n-1: upper half node l; lanes n..2n-1: lower half node l - n
                 const int half = lane < n ? 0 : 1;
                 const int l = lane - half * n;
+                const bool take = lane < 2 * n && (!a.p4est || l < 4);
                 const double* fwd = c_tlw_mortar[N][half];   // 0 forward_upper, 1 forward_lower
                 double y[NV] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
                 for (int f = 0; f < n; ++f) {
-                    const int k = face == 0 ? n * f : face == 1 ? (n - 1) + n * f : face == 2 ? f : f + n * (n - 1);
+                    const int fi = rev ? n - 1 - f : f;
+                    const int k = face == 0 ? n * fi : face == 1 ? (n - 1) + n * fi : face == 2 ? fi : fi + n * (n - 1);
                     const int src = k & 31, slot = k >> 5;   // warp-uniform
-                    const double c = (lane < 2 * n) ? fwd[(l < n ? l : 0) * n + f] : 0.0;
+                    const double c = take ? fwd[(l < n ? l : 0) * n + f] : 0.0;
 #pragma unroll
                     for (int v = 0; v < NV; ++v) {
                         double t = x[0][v];
@@ -141,7 +148,7 @@ static __global__ void __launch_bounds__(32 * LIMITER_WARPS) positivity_limiter_
                     }
                 }
                 double mv = __longlong_as_double(0x7ff0000000000000ll);
-                if (lane < 2 * n) mv = limiter_value(a.gamma, var, y);
+                if (take) mv = limiter_value(a.gamma, var, y);
                 mv = warp_min(mv);
                 const double theta = julia_min(fabs((vmean - thr) / (vmean - mv)), 1.0);
                 blend(theta, m);
