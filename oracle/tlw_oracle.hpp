@@ -1122,6 +1122,14 @@ inline void indicator_hennemann_gassner(const Basis& b, const Euler& eq, const O
             alpha[l] = std::max(std::max(tmp[l], 0.5 * tmp[r]), alpha[l]);
             alpha[r] = std::max(std::max(tmp[r], 0.5 * tmp[l]), alpha[r]);
         }
+        // and over the L2 mortars: each small element with the large one
+        for (int k = 0; k < m.n_mortars; ++k) {
+            const int lo = m.mortar_lower[k], up = m.mortar_upper[k], lg = m.mortar_large[k];
+            alpha[lo] = std::max(std::max(tmp[lo], 0.5 * tmp[lg]), alpha[lo]);
+            alpha[up] = std::max(std::max(tmp[up], 0.5 * tmp[lg]), alpha[up]);
+            alpha[lg] = std::max(std::max(tmp[lg], 0.5 * tmp[lo]), alpha[lg]);
+            alpha[lg] = std::max(std::max(tmp[lg], 0.5 * tmp[up]), alpha[lg]);
+        }
     }
 }
 
@@ -1260,10 +1268,9 @@ inline void rhs(const Basis& b, const Euler& eq, const Options& opt, const TreeM
             throw std::invalid_argument("boundary data missing");
         calc_boundary_flux(b, eq, opt, m, u, bd ? *bd : BoundaryData{}, kind == 1 ? 0.5 : 1.0, ws);
     }
-    if (m.n_mortars > 0) {
-        if (opt.shock_capturing) throw std::invalid_argument("mortars with shock capturing are not restated");
-        calc_mortar_flux(b, eq, opt, m, u, ws, nthreads);
-    }
+    // (with shock capturing the mortars keep the plain LW flux: calc_mortar_flux!, dg_2d.jl:1596-1646, has no
+    // blending)
+    if (m.n_mortars > 0) calc_mortar_flux(b, eq, opt, m, u, ws, nthreads);
     surface_integral_and_jacobian(b, m, du, ws, nthreads);
 }
 

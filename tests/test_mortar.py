@@ -118,3 +118,74 @@ def test_gpu_mortar_steps_match_oracle(oracle_mod, tl, td, flux, speed):
     s, t = o.steps(u_cpu, 7, 0.3, 0.0, 1e9, kind=0 if td == "lw" else 1, nthreads=NTH)
     assert s == integ.iter == 7 and integ.t == pytest.approx(t, rel=1e-13)
     assert np.all(rel_l2(u_gpu, u_cpu) < 1e-12)
+
+
+# ------------------------------------------------------------------ shock capturing across mortars (TreeMesh)
+def blast(tl, mesh, N):
+    """A circular blast at rest around (-3, -3), across the refined patch's corner: (rho, p) = (1, 3) inside
+    radius 3, (0.5, 1) outside."""
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    x, y = mesh.node_coordinates(N)
+    inside = (x + 3.0) ** 2 + (y + 3.0) ** 2 < 9.0
+    z = np.zeros(x.shape)
+    v = eq.prim2cons(np.where(inside, 1.0, 0.5), z, z, np.where(inside, 3.0, 1.0))
+    return np.ascontiguousarray(np.transpose(v, (2, 1, 0, 3))).reshape(-1)
+
+
+def sc_semi(tl, mesh, N, td="lw"):
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    tdo = tl.LW() if td == "lw" else tl.MDRK()
+    vi = tl.VolumeIntegralFRShockCapturing(tl.IndicatorHennemannGassner(alpha_max=0.5), tl.VolumeIntegralFR(tdo))
+    return tl.SemidiscretizationHyperbolic(mesh, tdo, eq, tl.IsentropicVortex(5.0),
+                                           tl.DGSEM(N, tl.flux_lax_friedrichs, vi))
+
+
+@pytest.mark.parametrize("N", [3, 4])
+def test_oracle_sc_across_mortars_conserves(oracle_mod, tl, N):
+    """Shock capturing on the refined TreeMesh: the blending factors are smoothed across the mortars (a large
+    element next to a blended small one gets half its factor), the mortars keep the plain LW flux, the rhs
+    conserves."""
+    m = refined(tl)
+    o = oracle_mod.Oracle(m, N)
+    o.set_shock_capturing(True, 0.5, 0.001, True)
+    u = blast(tl, m, N)
+    du = o.rhs(u, 0.0, o.max_dt(u, 0.15))
+    alpha = o.get(6)
+    assert alpha.max() > 0.1
+    o2 = oracle_mod.Oracle(m, N)
+    o2.set_shock_capturing(True, 0.5, 0.001, False)
+    o2.rhs(u, 0.0, o.max_dt(u, 0.15))
+    raw = o2.get(6)
+    ids = np.asarray(m.mortar_neighbor_ids).reshape(-1, 3) - 1
+    for lo, up, lg in ids:
+        assert alpha[lg] >= 0.5 * max(raw[lo], raw[up]) and alpha[lo] >= 0.5 * raw[lg]
+    x, y = m.node_coordinates(N)
+    jac = (1.0 / m.inverse_jacobian) ** 2
+    from trixilw.basis import gauss_lobatto
+    _, w = gauss_lobatto(N)
+    tot = np.einsum("ejiv,e,j,i->v", du.reshape(-1, N + 1, N + 1, 4), jac, w, w)
+    assert np.all(np.abs(tot) < 1e-10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,td", [(3, "lw"), (4, "lw"), (4, "mdrk")])
+def test_gpu_sc_across_mortars_matches_oracle(oracle_mod, tl, N, td):
+    m = refined(tl)
+    semi = sc_semi(tl, m, N, td)
+    u0 = blast(tl, m, N)
+    o = oracle_mod.Oracle(m, N)
+    o.set_shock_capturing(True, 0.5, 0.001, True)
+    dt = o.max_dt(u0, 0.15)
+    if td == "lw":
+        semi.cache["dt"][0] = dt
+        du = np.empty_like(u0)
+        tl.rhs(du, u0, semi, 0.0)
+        assert np.all(rel_l2(u0 + dt * du, u0 + dt * o.rhs(u0, 0.0, dt)) < 1e-12)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, semi.time_discretization, (0.0, 1e9)))
+    integ.set_state(u0, 0.0)
+    integ.step(8, 0.15, use_graph=True)
+    integ.sync_time()
+    u_cpu = u0.copy()
+    s, t = o.steps(u_cpu, 8, 0.15, 0.0, 1e9, kind=0 if td == "lw" else 1, nthreads=NTH)
+    assert s == integ.iter == 8 and integ.t == pytest.approx(t, rel=1e-12)
+    assert np.all(rel_l2(integ.get_state(), u_cpu) < 1e-11)

@@ -974,7 +974,7 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
     h->jac_first = inverse_jacobian[0];
     if (h->sc) {
         if ((rc = up_i(h->d_il, al)) || (rc = up_i(h->d_ir, ar))) return rc;
-        h->ni = (int)al.size();
+        h->ni = h->ni_if = (int)al.size();
     }
     h->nb = n_boundaries; h->nbx = (int)bx.size(); h->nby = (int)by.size();
     TLW_CUDA(h, cudaMalloc(&h->d_slots, (size_t)n_elements * CFL_SLOTS * sizeof(unsigned long long)));
@@ -1178,7 +1178,6 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
                          const int64_t* mortar_large_sides, const int64_t* mortar_orientations) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh || h->curved) return fail(h, TLW_E_STATE, "mortars follow tlw_set_tree_mesh");
-    if (h->sc && n_mortars > 0) return fail(h, TLW_E_UNSUPPORTED, "mortars with shock capturing are not built");
     if (n_mortars < 0 || (n_mortars > 0 && (!mortar_neighbor_ids || !mortar_large_sides || !mortar_orientations)))
         return fail(h, TLW_E_ARG, "mortars");
     std::vector<int> ml[2], mu[2], mg[2], ms[2];
@@ -1217,6 +1216,28 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
             (rc = up_cat(h->d_mg, mg[0], mg[1])) || (rc = up_cat(h->d_ms, ms[0], ms[1])) ||
             (rc = up_cat(h->d_mface, mface, std::vector<int>())))
             return rc;
+    }
+    if (h->sc) {
+        // the blending factors are smoothed over the mortars too (each small element with the large one): the
+        // interface pairs, then (lower, large) and (upper, large) of every mortar
+        std::vector<int> l(h->ni_if), r(h->ni_if);
+        if (h->ni_if > 0) {
+            TLW_CUDA(h, cudaMemcpy(l.data(), h->d_il, h->ni_if * sizeof(int), cudaMemcpyDeviceToHost));
+            TLW_CUDA(h, cudaMemcpy(r.data(), h->d_ir, h->ni_if * sizeof(int), cudaMemcpyDeviceToHost));
+        }
+        for (int d = 0; d < 2; ++d)
+            for (size_t k = 0; k < ml[d].size(); ++k) {
+                l.push_back(ml[d][k]); r.push_back(mg[d][k]);
+                l.push_back(mu[d][k]); r.push_back(mg[d][k]);
+            }
+        dfree(h->d_il); dfree(h->d_ir);
+        if (!l.empty()) {
+            TLW_CUDA(h, cudaMalloc(&h->d_il, l.size() * sizeof(int)));
+            TLW_CUDA(h, cudaMalloc(&h->d_ir, r.size() * sizeof(int)));
+            TLW_CUDA(h, cudaMemcpy(h->d_il, l.data(), l.size() * sizeof(int), cudaMemcpyHostToDevice));
+            TLW_CUDA(h, cudaMemcpy(h->d_ir, r.data(), r.size() * sizeof(int), cudaMemcpyHostToDevice));
+        }
+        h->ni = (int)l.size();
     }
     return TLW_OK;
 }

@@ -96,8 +96,8 @@ struct tlw_handle {
     // shock capturing
     bool sc = false;
     double *d_alpha = nullptr, *d_alpha_raw = nullptr, *d_tFn = nullptr;
-    int *d_il = nullptr, *d_ir = nullptr;   // all interfaces (smoothing)
-    int ni = 0;
+    int *d_il = nullptr, *d_ir = nullptr;   // smoothing pairs: all interfaces, then the mortars' (small, large)
+    int ni = 0, ni_if = 0;                  // pairs, of which interfaces
     // curvilinear shock capturing: subcell normals, calc_fn_low! normals, boundary-element flags, MUSCL geometry
     double *d_subn = nullptr, *d_subq = nullptr, *d_mgeom = nullptr;
     unsigned char* d_atb = nullptr;
