@@ -767,78 +767,6 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     if (ev) cudaEventRecord(ev->after_y, h->stream);
 }
 
-// The plain LW step on a periodic conforming TreeMesh (use_slots) with the surface work overlapped: the volume
-// kernel runs over OVERLAP_CHUNKS element ranges in turn on the handle's stream, and as each range finishes, the
-// x interfaces whose elements both lie in the finished ranges run on the side stream (highest priority), where
-// the memory-bound interface sweep shares the SMs with the FP64-bound volume kernel; the y interfaces follow
-// once both streams have joined (they finalise the corner nodes' CFL speeds, after every x interface). Each node
-// of u_new receives the same contributions in the same order as in the serial step; only the launches differ.
-void enqueue_lw_step_overlapped(tlw_handle* h, const double* u, double* unew, const double* dtp) {
-    const int K = tlw_handle::OVERLAP_CHUNKS;
-    VolArgs va{};
-    va.u = u;
-    va.u_base = u;
-    va.out = unew;
-    va.tU = h->d_tU;
-    va.tF = h->d_tF;
-    va.inv_jac = h->d_inv_jac;
-    va.dt = dtp;
-    va.basis = h->d_basis;
-    va.gamma = h->opts.gamma;
-    va.status = &h->d_step->status;
-    va.speed_kind = h->opts.max_speed;
-    va.cfl_slots = h->d_slots;
-    SurfArgs sa{};
-    sa.u = u;
-    sa.out = unew;
-    sa.tU = h->d_tU;
-    sa.tF = h->d_tF;
-    sa.inv_jac = h->d_inv_jac;
-    sa.dt = dtp;
-    sa.step_mode = 1;
-    sa.gamma = h->opts.gamma;
-    sa.flux_kind = h->opts.surface_flux;
-    sa.speed_kind = h->opts.max_speed;
-    sa.inv_w_first = h->h_basis.inv_w_first;
-    sa.inv_w_last = h->h_basis.inv_w_last;
-    sa.status = &h->d_step->status;
-    sa.cfl_slots = h->d_slots;
-    cudaEventRecord(h->ev_fork, h->stream);
-    cudaStreamWaitEvent(h->s_side, h->ev_fork, 0);
-    const size_t nn = (size_t)h->nn, tn = (size_t)4 * h->n;
-    for (int c = 0; c < K; ++c) {
-        const int64_t e0 = h->chunk_bounds[c], ec = h->chunk_bounds[c + 1] - e0;
-        if (ec > 0) {
-            VolArgs vc = va;
-            vc.u = u + (size_t)e0 * nn * NV;
-            vc.u_base = vc.u;
-            vc.out = unew + (size_t)e0 * nn * NV;
-            vc.tU = h->d_tU + (size_t)e0 * tn * NV;
-            vc.tF = h->d_tF + (size_t)e0 * tn * NV;
-            vc.inv_jac = h->d_inv_jac + e0;
-            vc.cfl_slots = h->d_slots + (size_t)e0 * CFL_SLOTS;
-            vc.E = (int)ec;
-            dispatch<Vol>(h->N, h->stream, TLW_STAGE_LW, MODE_STEP, false, vc);
-        }
-        cudaEventRecord(h->ev_vol[c], h->stream);
-        cudaStreamWaitEvent(h->s_side, h->ev_vol[c], 0);
-        SurfArgs sx = sa;
-        sx.left = h->d_xl + h->xg_off[c];
-        sx.right = h->d_xr + h->xg_off[c];
-        sx.count = h->xg_off[c + 1] - h->xg_off[c];
-        sx.orientation = 1;
-        dispatch<Ifc>(h->N, h->s_side, sx);
-    }
-    cudaEventRecord(h->ev_join, h->s_side);
-    cudaStreamWaitEvent(h->stream, h->ev_join, 0);
-    SurfArgs sy = sa;
-    sy.left = h->d_yl;
-    sy.right = h->d_yr;
-    sy.count = h->ny;
-    sy.orientation = 2;
-    dispatch<Ifc>(h->N, h->stream, sy);
-}
-
 // one CFL step from state[from] into state[1 - from]; ev (optional): [after dt, stage 1 phases, stage 2 phases]
 void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const PhaseEvents* ev = nullptr) {
     const double* u = h->d_state[from];
@@ -862,8 +790,7 @@ void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const
     if (after_dt) cudaEventRecord(after_dt, h->stream);
     const double* dtp = &h->d_step->dt;
     if (h->opts.time_discretization == TLW_LW) {
-        if (use_slots(h) && !ev && !h->te_request) enqueue_lw_step_overlapped(h, u, unew, dtp);
-        else enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, dtp, ev, true);
+        enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, dtp, ev, true);
         // solve_lwfr limits twice per LW step: in perform_step! (src/solvers/lwfr.jl:226) and in its loop (:257)
         enqueue_limiter(h, unew, 2, use_slots(h) ? h->d_slots : nullptr);
     } else {
@@ -978,11 +905,6 @@ int tlw_destroy(tlw_handle* h) {
     free_mesh(h);
     dfree(h->d_basis);
     dfree(h->d_step);
-    for (cudaEvent_t ev : h->ev_vol)
-        if (ev) cudaEventDestroy(ev);
-    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-    if (h->ev_join) cudaEventDestroy(h->ev_join);
-    if (h->s_side) cudaStreamDestroy(h->s_side);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return TLW_OK;
@@ -1010,32 +932,6 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
         (o == 1 ? xr : yr).push_back((int)r);
         al.push_back((int)l);
         ar.push_back((int)r);
-    }
-    // the x interfaces sorted by the later of their elements' ranges (the order of a launch is free: no two x
-    // interfaces share a node)
-    std::vector<int64_t> bounds(tlw_handle::OVERLAP_CHUNKS + 1);
-    for (int c = 0; c <= tlw_handle::OVERLAP_CHUNKS; ++c) bounds[c] = n_elements * c / tlw_handle::OVERLAP_CHUNKS;
-    auto chunk_of = [&](int64_t e) {
-        return (int)(std::upper_bound(bounds.begin(), bounds.end(), e) - bounds.begin()) - 1;
-    };
-    std::vector<int> xg_off(tlw_handle::OVERLAP_CHUNKS + 1, 0);
-    {
-        std::vector<int> order(xl.size());
-        std::vector<int> grp(xl.size());
-        for (size_t k = 0; k < xl.size(); ++k) {
-            order[k] = (int)k;
-            grp[k] = std::max(chunk_of(xl[k]), chunk_of(xr[k]));
-        }
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return grp[a] < grp[b]; });
-        std::vector<int> sl(xl.size()), sr(xr.size());
-        for (size_t k = 0; k < order.size(); ++k) {
-            sl[k] = xl[order[k]];
-            sr[k] = xr[order[k]];
-            xg_off[grp[order[k]] + 1]++;
-        }
-        for (int c = 0; c < tlw_handle::OVERLAP_CHUNKS; ++c) xg_off[c + 1] += xg_off[c];
-        xl.swap(sl);
-        xr.swap(sr);
     }
     std::vector<int> belem, bdir, bx, by;
     if (n_boundaries > 0) {
@@ -1075,15 +971,6 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
         (rc = up_i(h->d_by, by)))
         return rc;
     h->nx = (int)xl.size(); h->ny = (int)yl.size();
-    h->chunk_bounds = bounds;
-    h->xg_off = xg_off;
-    if (!h->s_side) {
-        int least = 0, greatest = 0;
-        TLW_CUDA(h, cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        TLW_CUDA(h, cudaStreamCreateWithPriority(&h->s_side, cudaStreamNonBlocking, greatest));
-        for (cudaEvent_t* ev : {&h->ev_fork, &h->ev_join}) TLW_CUDA(h, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
-        for (cudaEvent_t& ev : h->ev_vol) TLW_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    }
     h->jac_first = inverse_jacobian[0];
     if (h->sc) {
         if ((rc = up_i(h->d_il, al)) || (rc = up_i(h->d_ir, ar))) return rc;

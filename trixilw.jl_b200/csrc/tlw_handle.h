@@ -154,14 +154,6 @@ struct tlw_handle {
     int ncm = 0;
     int *d_cms1 = nullptr, *d_cms2 = nullptr, *d_cml = nullptr, *d_cmc = nullptr;
     std::vector<int> mortar_off;            // mortar colour c covers [mortar_off[c], mortar_off[c + 1])
-    // the plain LW step on a periodic conforming TreeMesh: the volume kernel in OVERLAP_CHUNKS element ranges, the
-    // x interfaces of each finished range on a side stream (highest priority) meanwhile; the x interfaces are
-    // sorted by the later range of their two elements (xg_off)
-    static constexpr int OVERLAP_CHUNKS = 8;
-    std::vector<int64_t> chunk_bounds;      // [OVERLAP_CHUNKS + 1] element ranges
-    std::vector<int> xg_off;                // [OVERLAP_CHUNKS + 1] x-interface groups
-    cudaStream_t s_side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_vol[OVERLAP_CHUNKS] = {};
     // graphs: [start buffer] one step, two steps
     cudaGraphExec_t g_one[2] = {nullptr, nullptr};
     cudaGraphExec_t g_two[2] = {nullptr, nullptr};
