@@ -97,9 +97,11 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
                       const int64_t* boundary_orientations, const int64_t* boundary_neighbor_sides,
                       const int64_t* n_boundaries_per_direction);
 
-/* Adaptive (error-controlled) stepping, src/solvers/adaptive.jl:47-172 (LW on a TreeMesh, N >= 4): one trial
- * step u_trial = u + dt rhs(u) from the current state at the given dt, with lw_volume_kernel_4!'s temporal
- * error estimate (abstol, reltol; dg_2d.jl:1183-1265). *total_temporal_error = sqrt(sum_e errors / ndofs)
+/* Adaptive (error-controlled) stepping, src/solvers/adaptive.jl:47-172 (LW, hyperbolic; N >= 4 on a TreeMesh,
+ * N >= 3 on a curvilinear mesh; FR or shock-capturing volume integral): one trial step u_trial = u + dt rhs(u)
+ * from the current state at the given dt, with the LW volume kernels' temporal error estimate (abstol, reltol;
+ * dg_2d.jl:1183-1265, dgsem_structured/dg_2d.jl:1595-1682 and 1983-2075). MDRK and the TreeMesh kernel of
+ * depth 3 leave the reference's temporal_errors unset: TLW_E_UNSUPPORTED. *total_temporal_error = sqrt(sum_e errors / ndofs)
  * (load_temporal_errors!), *admissible = 0 when a square root of a negative number occurred (test_rhs!'s
  * DomainError) or a node of u_trial has rho <= 0 or p <= 0 (test_updated_solution). The state is not
  * changed until tlw_adaptive_accept(h, dt), which makes u_trial current and advances t by dt. Synchronous;

@@ -105,8 +105,14 @@ inline void lw_surface_flux_normal(const Euler& eq, int flux_kind, int speed_kin
 // One element of the curvilinear LW volume kernel. du receives Dhat F~ + Dhat G~ (before the surface
 // integral and the Jacobian); ws.U / ws.F receive the time-averaged U and the physical F, G.
 // alpha: the factor of the Dhat terms (1 - the element's blending factor under shock capturing).
+// te: with te->temporal_errors, the error estimate of the Adaptive step control as the curvilinear kernels
+// compute it inline (dgsem_structured/dg_2d.jl:1595-1619, 1669-1682 at depth 3; :1983-2007, 2061-2075 at
+// depth 4): u_np1 = u - dt J^{-1}(node) (D F~ + D G~) and u_np1_low with F~, G~ before the last stage's term,
+// ws.temporal_errors[e] = sum over nodes and variables of ((u_np1 - u_np1_low) / (abstol + reltol max))^2.
+// It does not depend on alpha: the shock-capturing path calls the same kernel for every element.
 inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, const CurvedMesh& m, int e,
-                                     const double* u, double* du, double dt, Workspace& ws, double alpha = 1.0) {
+                                     const double* u, double* du, double dt, Workspace& ws, double alpha = 1.0,
+                                     const Options* te = nullptr) {
     const int n = b.n, nn = n * n;
     const LWStencils S = lw_stencils(N);
     const int depth = S.depth;
@@ -115,7 +121,8 @@ inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, con
     const double* Jae = &m.Ja[4 * (size_t)nn * e];
     const double* ije = &m.inv_jac[(size_t)nn * e];
     std::vector<double> d(5 * NV * nn, 0.0), ft(NV * nn), gt(NV * nn), Fp(NV * nn), Gp(NV * nn), Ft(NV * nn),
-        Gt(NV * nn), Uc(NV * nn);
+        Gt(NV * nn), Uc(NV * nn), Flow, Glow;
+    const bool want_te = te && te->temporal_errors;
     auto Dm = [&](int k) { return d.data() + (size_t)k * NV * nn; };
     // physical and contravariant fluxes of a state at node (i, j) (contravariant_flux)
     auto cflux = [&](const double* s, int i, int j, double* f, double* g, double* cf, double* cg) {
@@ -175,6 +182,10 @@ inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, con
                         tf[v] += S.w[s][1 + q] * cf[v]; tg[v] += S.w[s][1 + q] * cg[v];
                     }
                 }
+                if (want_te && s == depth) {   // F~, G~ before the last stage's term (u_np1_low)
+                    if (Flow.empty()) { Flow.assign(NV * nn, 0.0); Glow.assign(NV * nn, 0.0); }
+                    for (int v = 0; v < NV; ++v) { Flow[o + v] = Ft[o + v]; Glow[o + v] = Gt[o + v]; }
+                }
                 for (int v = 0; v < NV; ++v) {
                     Fp[o + v] += S.tw[s] * pf[v]; Gp[o + v] += S.tw[s] * pg[v];
                     Ft[o + v] += S.tw[s] * tf[v]; Gt[o + v] += S.tw[s] * tg[v];
@@ -199,6 +210,18 @@ inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, con
                 ws.U[idx_u(n, v, i, j, e)] = Uc[o + v];
             }
         }
+    if (want_te) {
+        std::vector<double> hi(NV * nn), lo(NV * nn);
+        contract(Ft, Gt, hi.data());
+        contract(Flow, Glow, lo.data());
+        double err = 0.0;
+        for (int k = 0; k < NV * nn; ++k) {
+            const double a = ue[k] + hi[k], c = ue[k] + lo[k];
+            const double r = (a - c) / (te->abstol + te->reltol * std::max(std::fabs(a), std::fabs(c)));
+            err += r * r;
+        }
+        ws.temporal_errors[e] = err;
+    }
 }
 
 // Boundary faces with the LW slip walls in their normal-direction form (src/equations/equations.jl:137-169;
@@ -364,6 +387,7 @@ inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, cons
     ws.F.assign(2 * ndof, nan);
     ws.surface_flux_values.assign((size_t)NV * n * 4 * m.n_elements, nan);
     ws.bad = false;
+    if (opt.temporal_errors && kind == 0) ws.temporal_errors.assign(m.n_elements, nan);
     if (kind == 1) {
         ws.U2.assign(ndof, nan);
         ws.F2.assign(2 * ndof, nan);
@@ -374,7 +398,7 @@ inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, cons
     for (int e = 0; e < m.n_elements; ++e) {
         const double* Jae = &m.Ja[4 * (size_t)nn * e];
         const double* ije = &m.inv_jac[(size_t)nn * e];
-        if (kind == 0) lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws);
+        if (kind == 0) lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws, 1.0, &opt);
         else if (kind == 1) mdrk1_volume_element(b, eq, e, u, du, dt, 0.0, 1.0, ws, Jae, ije);
         else mdrk2_volume_element(b, eq, e, u2, du, dt, 0.0, 1.0, ws, Jae, ije);
     }

@@ -446,6 +446,7 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
     ws.surface_flux_values.assign((size_t)NV * n * 4 * m.n_elements, nan);
     ws.fn_low.assign((size_t)NV * n * 4 * m.n_elements, 0.0);
     ws.bad = false;
+    if (opt.temporal_errors && kind == 0) ws.temporal_errors.assign(m.n_elements, nan);
     if (kind == 1) {
         ws.U2.assign(ndof, nan);
         ws.F2.assign(2 * ndof, nan);
@@ -462,7 +463,7 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
         const double a = ws.alpha[e];
         const double* Jae = &m.Ja[4 * (size_t)nn * e];
         const double* ije = &m.inv_jac[(size_t)nn * e];
-        if (kind == 0) lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws, 1.0 - a);
+        if (kind == 0) lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws, 1.0 - a, &opt);
         else if (kind == 1) mdrk1_volume_element(b, eq, e, u, du, dt, 0.0, 1.0 - a, ws, Jae, ije);
         else mdrk2_volume_element(b, eq, e, u2, du, dt, 0.0, 1.0 - a, ws, Jae, ije);
         // pure_and_blended_element_ids!: DG only where isapprox(alpha, 0, atol = 1e-12)

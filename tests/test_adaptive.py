@@ -18,10 +18,10 @@ def vortex(tl, mesh, N):
     return np.ascontiguousarray(np.transpose(v, (2, 1, 0, 3))).reshape(-1)
 
 
-def oracle_adaptive(oracle_mod, mesh, N, u0, t_end, dt0, tol=TOL):
-    """The reference's adaptive loop with the oracle as the trial step."""
+def oracle_adaptive(oracle_mod, mesh, N, u0, t_end, dt0, tol=TOL, oracle_obj=None):
+    """The reference's adaptive loop with the oracle as the trial step (oracle_obj: a configured oracle)."""
     from trixilw.lwfr import AdaptiveController
-    o = oracle_mod.Oracle(mesh, N)
+    o = oracle_obj or oracle_mod.Oracle(mesh, N)
     o.set_temporal_errors(True, tol["abstol"], tol["reltol"])
     ctl = AdaptiveController(N + 1, 0.0, t_end, dt0)
     u = u0.copy()

@@ -124,9 +124,7 @@ struct Launch {
         set_attr_sc<true>();
         const int lw = (int)C::smem_bytes(4);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
-        if constexpr (N >= 4)
-            cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        te_volume(nullptr, VolArgs{}, 0, false, true);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
         curved_sc_attributes<0>();
         curved_sc_attributes<1>();
@@ -177,11 +175,38 @@ struct Launch {
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, true, true, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, true, true, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     }
+    // Adaptive trial step: the LW kernel with the temporal error estimate (a step into a.out), on a TreeMesh
+    // (N >= 4) or a curvilinear mesh (N >= 3), with or without shock capturing; attr_only sets the shared
+    // memory attributes of every variant instead
+    template <bool SC, bool CURVED, int REC>
+    static void te_launch(cudaStream_t s, const VolArgs& a, int grid, bool attr_only) {
+        const int sm = (int)C::smem_bytes(!SC ? 4 : REC ? 12 : 8);
+        if (attr_only)
+            cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, SC, 0, CURVED, true, false, REC>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        else
+            lw_volume_kernel<N, MODE_STEP, SC, 0, CURVED, true, false, REC><<<grid, C::THREADS, sm, s>>>(a);
+    }
+    static void te_volume(cudaStream_t s, const VolArgs& a, int grid, bool sc, bool attr_only) {
+        if constexpr (N >= 3) {
+            const bool curved = attr_only || a.metrics;
+            const int rec = a.reconstruction;
+            if (curved && (attr_only || !sc)) te_launch<false, true, 0>(s, a, grid, attr_only);
+            if (curved && (attr_only || (sc && rec == TLW_RECONSTRUCTION_FIRST_ORDER))) te_launch<true, true, 0>(s, a, grid, attr_only);
+            if (curved && (attr_only || (sc && rec == TLW_RECONSTRUCTION_MUSCL))) te_launch<true, true, 1>(s, a, grid, attr_only);
+            if (curved && (attr_only || (sc && rec == TLW_RECONSTRUCTION_MUSCL_HANCOCK))) te_launch<true, true, 2>(s, a, grid, attr_only);
+            if constexpr (N >= 4) {
+                const bool tree = attr_only || !a.metrics;
+                if (tree && (attr_only || !sc)) te_launch<false, false, 0>(s, a, grid, attr_only);
+                if (tree && (attr_only || sc)) te_launch<true, false, 0>(s, a, grid, attr_only);
+            }
+        }
+    }
     static void volume(cudaStream_t s, int stage, int mode, bool sc, const VolArgs& a) {
         const int grid = (int)((a.E + C::EB - 1) / C::EB);
         if (grid == 0) return;
-        if (a.temporal_errors) {   // Adaptive trial step: the depth-4 kernel with the error estimate
-            if constexpr (N >= 4) lw_volume_kernel<N, MODE_STEP, false, 0, false, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
+        if (a.temporal_errors) {
+            te_volume(s, a, grid, sc, false);
             return;
         }
         if (a.metrics && sc) {   // curvilinear mesh with shock capturing (MUSCL when the geometry is given)
@@ -1572,8 +1597,10 @@ int tlw_adaptive_trial(tlw_handle* h, double dt, double abstol, double reltol, d
     int rc = check_ready(h);
     if (rc) return rc;
     if (!total_temporal_error || !admissible || !(dt > 0.0)) return fail(h, TLW_E_ARG, "arguments");
-    if (h->opts.time_discretization != TLW_LW || h->sc || h->curved || h->parabolic || h->N < 4)
-        return fail(h, TLW_E_UNSUPPORTED, "Adaptive: LW on a TreeMesh with N >= 4 (the depth-4 kernel's estimate)");
+    // the reference's estimate comes from the LW volume kernels of depth 4 (TreeMesh) or 3 and 4 (curvilinear);
+    // its MDRK kernels and the TreeMesh kernel of depth 3 leave temporal_errors unset
+    if (h->opts.time_discretization != TLW_LW || h->parabolic || h->N < (h->curved ? 3 : 4))
+        return fail(h, TLW_E_UNSUPPORTED, "Adaptive: LW, hyperbolic, N >= 4 on a TreeMesh or N >= 3 on a curvilinear mesh");
     TLW_CUDA(h, cudaSetDevice(h->device));
     const int blocks = (int)std::min<int64_t>(((int64_t)h->nn * h->E + 255) / 256, 4 * 148);
     if (!h->d_te) {

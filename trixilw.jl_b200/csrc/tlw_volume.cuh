@@ -574,7 +574,9 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
                                                                                  : VolCfg<N, EBX>::MIN_BLOCKS)
     lw_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
-    static_assert(!TE || (N >= 4 && !SC && !CURVED), "temporal errors: depth-4 TreeMesh kernel");
+    // the temporal error estimate of the Adaptive step control: the TreeMesh computes it at depth 4 only
+    // (lw_volume_kernel_3! of dgsem_tree has none), the curvilinear kernels at depths 3 and 4
+    static_assert(!TE || (CURVED ? N >= 3 : N >= 4), "temporal errors: TreeMesh N >= 4, curvilinear N >= 3");
     static_assert(!DSTORE || (!SC && !CURVED && !TE), "stored stage derivatives: the plain TreeMesh kernel");
     using C = VolCfg<N, EBX>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
@@ -618,7 +620,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
     double U[NV], F[NV], G[NV], up[NV], um[NV], upp[NV], umm[NV];
     double s0 = 0.0, ij = 0.0;   // s0 = -dt J^{-1} (of the element, or of the node on curvilinear meshes)
     double Ja[4] = {0.0, 0.0, 0.0, 0.0};
-    double dF[NV], dG[NV], u0[NV];   // TE: the fourth-derivative term of F, G, and u
+    double dF[NV], dG[NV], u0[NV];   // TE: the last stage's term of F, G, and u
     // stage fluxes into the contraction planes (contravariant on curvilinear meshes)
     auto put = [&](const double* f, const double* g) {
         if (CURVED) {
@@ -788,6 +790,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
                 q[v] -= g[v];
                 F[v] = fma(C3 / 24.0, r[v], F[v]);
                 G[v] = fma(C3 / 24.0, q[v], G[v]);
+                if (TE && DEPTH == 3) { dF[v] = (C3 / 24.0) * r[v]; dG[v] = (C3 / 24.0) * q[v]; }
             }
             if (DEPTH >= 4) put(r, q);
         }
@@ -843,6 +846,11 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             contravariant(Ja, F, G, ft, gt);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { F[v] = ft[v]; G[v] = gt[v]; }
+            if (TE) {   // the last stage's term of F~, G~
+                contravariant(Ja, dF, dG, ft, gt);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) { dF[v] = ft[v]; dG[v] = gt[v]; }
+            }
         }
         node_put<N, C>(X, Y, el, i, j, F, G);
         if (SC) {
@@ -887,8 +895,9 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
         }
     }
     if (TE) {
-        // lw_volume_kernel_4!'s error estimate (dg_2d.jl:1183-1265): the strong-form volume updates
-        // u_np1 = u - dt J^{-1} (D F + D G) and u_np1_low with F, G before the fourth-derivative term;
+        // lw_volume_kernel_4!'s error estimate (dg_2d.jl:1183-1265; curvilinear, with F~, G~ and the node's
+        // J^{-1}: dgsem_structured/dg_2d.jl:1595-1682 at depth 3, :1983-2075 at depth 4): the strong-form volume
+        // updates u_np1 = u - dt J^{-1} (D F + D G) and u_np1_low with F, G before the last stage's term;
         // temporal_errors[e] = sum over nodes and variables of ((u_np1 - u_np1_low) / (abstol + reltol max))^2
         double un[NV], err = 0.0;
         __syncthreads();

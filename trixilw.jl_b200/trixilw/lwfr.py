@@ -195,8 +195,12 @@ def _solve_adaptive(lw_update: LWUpdate, callbacks, dt_initial: float, tolerance
     ctl = AdaptiveController(semi.nnodes, lw_update.tspan[0], lw_update.tspan[1], dt_initial)
     err = ctypes.c_double()
     ok = ctypes.c_int32()
+    # time-dependent exterior data is set for every trial's (t, dt)
+    time_dependent_bc = semi.mesh.n_boundaries > 0 and semi.time_dependent_boundaries()
     while not ctl.finished():
         dt = ctl.dt
+        if time_dependent_bc:
+            semi._prepare_boundaries(ctl.t, dt, 1.0)
         check(integ.handle, lib().tlw_adaptive_trial(integ.handle, float(dt), float(tol["abstol"]),
                                                      float(tol["reltol"]), ctypes.byref(err), ctypes.byref(ok)))
         if ctl.judge(err.value, bool(ok.value)):
