@@ -197,12 +197,22 @@ int tlw_dd_finish(tlw_handle* h);
  * large_faces[k] (faces 0: -xi, 1: +xi, 2: -eta, 3: +eta), and whether the large face's index runs backwards
  * along the mortar (P4est node_indices :i_backward); the small faces run forward. As the reference, the large
  * side's normal flux is its instantaneous Trixi.flux(u, -n_large / 2), and the large face receives -2 times the
- * L2 projection of the small faces' fluxes. LW or MDRK, FR volume integral, Euler; the positivity limiter then runs
- * the P4estMesh limit_mortars! (src/callbacks/callbacks_stage/positivity_zhang_shu_dg2d.jl:178-260) after its
- * element pass. */
+ * L2 projection of the small faces' fluxes. LW or MDRK, FR or shock-capturing volume integral, Euler; the
+ * positivity limiter then runs the P4estMesh limit_mortars! (src/callbacks/callbacks_stage/positivity_zhang_shu_dg2d.jl:
+ * 178-260) after its element pass. With shock capturing the blending factors are smoothed over the mortars too
+ * and each small node's flux goes through get_blended_flux (dg_2d.jl:227-250, 589-593) with the J^{-1} of
+ * tlw_set_curved_mortar_jacobian (zeros until it is called). */
 int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* small1, const int64_t* small2,
                            const int32_t* small_faces, const int64_t* large, const int32_t* large_faces,
                            const int32_t* large_reversed);
+
+/* lw_mortars.inverse_jacobian (dgsem_p4est/containers.jl:23-33), [n_mortars][n] in the order of
+ * tlw_set_curved_mortars, as the reference holds it: zeros from create_cache, then after each AMR step what
+ * load_inverse_jacobian!(lw_mortars.inverse_jacobian, mesh, eachmortar(dg, cache), dg, cache) loads
+ * (callbacks/amr.jl:203; that loader reads the interface arrays, so mortar k gets the J^{-1} of interface k's
+ * primary face nodes). Only the shock-capturing blend at the mortars reads it; null resets it to zeros. A
+ * shim passes cache.lw_mortars.inverse_jacobian unchanged. */
+int tlw_set_curved_mortar_jacobian(tlw_handle* h, const double* inverse_jacobian);
 
 /* Subcell reconstruction of the blended elements under shock capturing on a curvilinear mesh (the reference's
  * VolumeIntegralFRShockCapturing(...; reconstruction), src/solvers/dgsem_tree/dg_2d.jl:251-365):

@@ -201,6 +201,16 @@ int oracle_set_curved_mortars(oracle_handle* h, int M, const int32_t* small1, co
     m.m_large.assign(large, large + M);
     m.m_lface.assign(lface, lface + M);
     m.m_lrev.assign(lrev, lrev + M);
+    m.m_ij.clear();
+    return 0;
+}
+
+// lw_mortars.inverse_jacobian [mortar][l] for the shock-capturing blend at the mortars (null: zeros)
+int oracle_set_curved_mortar_jacobian(oracle_handle* h, const double* inv_jac) {
+    if (!h->curved) return 1;
+    CurvedMesh& m = h->cmesh;
+    if (!inv_jac) m.m_ij.clear();
+    else m.m_ij.assign(inv_jac, inv_jac + (size_t)m.n_mortars * h->basis.n);
     return 0;
 }
 

@@ -39,6 +39,7 @@ def lib():
         L.oracle_create.restype = P
         L.oracle_destroy.argtypes = [P]
         L.oracle_set_temporal_errors.argtypes = [P, i32, dbl, dbl]
+        L.oracle_set_curved_mortar_jacobian.argtypes = [P, P]
         L.oracle_set_shock_capturing.argtypes = [P, i32, dbl, dbl, i32]
         L.oracle_set_reconstruction.argtypes = [P, i32]
         L.oracle_set_curved_mortars.argtypes = [P, i32, P, P, P, P, P, P]
@@ -180,6 +181,14 @@ class Oracle:
              for k, x in enumerate((small1, small2, small_faces, large, large_faces, large_reversed))]
         self._mkeep = a
         assert lib().oracle_set_curved_mortars(self.h, len(a[0]), *[_p(x) for x in a]) == 0
+
+    def set_curved_mortar_jacobian(self, inverse_jacobian=None):
+        """lw_mortars.inverse_jacobian [mortar, l] of the shock-capturing blend at the mortars (None: zeros)."""
+        if inverse_jacobian is None:
+            assert lib().oracle_set_curved_mortar_jacobian(self.h, None) == 0
+            return
+        self._mjkeep = np.ascontiguousarray(inverse_jacobian, dtype=np.float64).reshape(-1)
+        assert lib().oracle_set_curved_mortar_jacobian(self.h, _p(self._mjkeep)) == 0
 
     def set_walls(self, kinds, data):
         """Navier-Stokes walls per boundary (1 no-slip adiabatic, 2 no-slip isothermal), data [B, l, 3] =

@@ -38,6 +38,9 @@ struct CurvedMesh {
     // face m_sface, the large element on m_lface, whose index runs backwards along the mortar when m_lrev
     int n_mortars = 0;
     std::vector<int32_t> m_small1, m_small2, m_sface, m_large, m_lface, m_lrev;
+    // lw_mortars.inverse_jacobian [mortar][l] (the J^{-1} of the shock-capturing blend at the mortars); empty:
+    // zeros, as the reference holds them until an AMR step loads them
+    std::vector<double> m_ij;
 };
 
 // node (i, j) of face f at face index l
@@ -289,8 +292,14 @@ inline void euler_flux_along(const Euler& eq, const double* u, const double* nrm
 // Trixi.flux(u, -n_large / 2) (the reference overwrites the time-averaged product, :455-458); the surface flux
 // takes the small side as _ll in the curvilinear order along the small element's normal. The small faces get
 // fstar, the large face -2 times its L2 projection (reverse operators), in its own index order.
+// blend: called per small node as blend(mortar, position, l, small element, u_ll, u_rr, normal, fstar) after the
+// LW flux is formed (the shock-capturing get_blended_flux; nothing without shock capturing).
+struct NoMortarBlend {
+    void operator()(int, int, int, int, const double*, const double*, const double*, double*) const {}
+};
+template <class Blend = NoMortarBlend>
 inline void calc_mortar_flux_curved(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m,
-                                    const double* u, Workspace& ws, bool& bad) {
+                                    const double* u, Workspace& ws, bool& bad, const Blend& blend = Blend()) {
     const int n = b.n;
     for (int k = 0; k < m.n_mortars; ++k) {
         const int lg = m.m_large[k], lf = m.m_lface[k], sf = m.m_sface[k];
@@ -335,6 +344,7 @@ inline void calc_mortar_flux_curved(const Basis& b, const Euler& eq, const Optio
                 double* out = &fstar[(h * n + l) * NV];
                 bool b_ = false;
                 lw_surface_flux_normal(eq, opt.flux_kind, opt.speed_kind, f_ll, f_rr, u_ll, u_rr, U_ll, U_rr, nS, out, b_);
+                blend(k, h, l, se, u_ll, u_rr, nS, out);
                 bad = bad || b_;
                 for (int v = 0; v < NV; ++v) ws.surface_flux_values[v + NV * (l + n * (sf + 4 * (size_t)se))] = out[v];
             }

@@ -378,10 +378,16 @@ inline void indicator_curved(const Basis& b, const Euler& eq, const Options& opt
     indicator_hennemann_gassner(b, eq, o, none, u, alpha);
     if (opt.alpha_smooth) {
         const std::vector<double> tmp = alpha;
-        for (int k = 0; k < m.n_interfaces; ++k) {
-            const int l = m.p_elem[k], r = m.s_elem[k];
+        auto pair = [&](int l, int r) {
             alpha[l] = std::max(std::max(tmp[l], 0.5 * tmp[r]), alpha[l]);
             alpha[r] = std::max(std::max(tmp[r], 0.5 * tmp[l]), alpha[r]);
+        };
+        for (int k = 0; k < m.n_interfaces; ++k) pair(m.p_elem[k], m.s_elem[k]);
+        // Trixi's apply_smoothing! for a P4estMesh continues over the mortars: each small element with the
+        // large one
+        for (int k = 0; k < m.n_mortars; ++k) {
+            pair(m.m_small1[k], m.m_large[k]);
+            pair(m.m_small2[k], m.m_large[k]);
         }
     }
 }
@@ -437,7 +443,6 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
                           double* du, double dt, Workspace& ws, int nthreads = 1, const BoundaryData* bd = nullptr,
                           int kind = 0, const double* u2 = nullptr) {
     if (opt.flux_kind != RUSANOV) throw std::invalid_argument("curvilinear shock capturing: Rusanov surface flux");
-    if (m.n_mortars > 0) throw std::invalid_argument("curvilinear shock capturing: conforming meshes");
     const int n = b.n, nn = n * n;
     const size_t ndof = (size_t)NV * nn * m.n_elements;
     const double nan = std::numeric_limits<double>::quiet_NaN();
@@ -507,6 +512,29 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
             }
         }
     }
+    ws.bad = ws.bad || bad;
+    // mortars (calc_mortar_flux!, src/solvers/dgsem_p4est/dg_2d.jl:506-603): get_blended_flux with the small
+    // element as the primary, u_rr the large element's u interpolated onto the small node, fn the first-order
+    // flux along the small element's normal, fn_inner_ll the small element's fn_low slot of its face at the
+    // node, fn_inner_rr the large element's fn_low slot of its face read in mortar order (index i, no
+    // reversal) and interpolated like u (prolong2mortars!, :429-500), and J^{-1} = lw_mortars.inverse_jacobian
+    bad = false;
+    auto mortar_blend = [&](int k, int h, int l, int se, const double* u_ll, const double* u_rr, const double* nS,
+                            double* fstar) {
+        const int lg = m.m_large[k], lf = m.m_lface[k], sf = m.m_sface[k];
+        const std::vector<double>& fwd = h ? b.fwd_upper : b.fwd_lower;
+        double fil[NV], fir[NV] = {0, 0, 0, 0}, fn[NV], Fn[NV];
+        for (int v = 0; v < NV; ++v) fil[v] = ws.fn_low[v + NV * (l + n * (sf + 4 * (size_t)se))];
+        for (int i = 0; i < n; ++i)
+            for (int v = 0; v < NV; ++v) fir[v] += fwd[l * n + i] * ws.fn_low[v + NV * (i + n * (lf + 4 * (size_t)lg))];
+        bool b_ = false;
+        rusanov_normal(eq, opt.speed_kind, u_ll, u_rr, nS, fn, b_);
+        bad = bad || b_;
+        const double J = m.m_ij.empty() ? 0.0 : m.m_ij[(size_t)k * n + l];
+        get_blended_flux(b, eq, u_ll, u_rr, ws.alpha[se], ws.alpha[lg], J, dt, fn, fstar, fil, fir, Fn);
+        for (int v = 0; v < NV; ++v) fstar[v] = Fn[v];
+    };
+    calc_mortar_flux_curved(b, eq, opt, m, u, ws, bad, mortar_blend);
     ws.bad = ws.bad || bad;
     calc_boundary_flux_curved(b, eq, opt, m, u, ws, bd, kind == 1 ? 0.5 : 1.0);
     surface_integral_and_jacobian_curved(b, m, du, ws, nthreads);

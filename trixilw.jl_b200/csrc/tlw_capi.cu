@@ -87,8 +87,9 @@ void free_mesh(tlw_handle* h) {
     if (h->d_cbk) { cudaFree(h->d_cbk); h->d_cbk = nullptr; }
     if (h->d_cbi) { cudaFree(h->d_cbi); h->d_cbi = nullptr; }
     h->ncb = h->ncbx = 0;
-    for (int** d : {&h->d_cms1, &h->d_cms2, &h->d_cml, &h->d_cmc})
+    for (int** d : {&h->d_cms1, &h->d_cms2, &h->d_cml, &h->d_cmc, &h->d_cmsl, &h->d_cmsr})
         if (*d) { cudaFree(*d); *d = nullptr; }
+    if (h->d_cmj) { cudaFree(h->d_cmj); h->d_cmj = nullptr; }
     h->ncm = 0;
     h->mortar_off.clear();
     h->curved = false;
@@ -458,6 +459,10 @@ void enqueue_indicator(tlw_handle* h, const double* u, bool speed) {
         alpha_smooth_kernel<<<(ni + 255) / 256, 256, 0, h->stream>>>(h->curved ? h->d_cp : h->d_il,
                                                                     h->curved ? h->d_cs : h->d_ir, ni,
                                                                     h->d_alpha_raw, h->d_alpha);
+    // and over the curvilinear mesh's mortars (each small element with the large one)
+    if (h->opts.alpha_smooth && h->curved && h->ncms > 0)
+        alpha_smooth_kernel<<<(h->ncms + 255) / 256, 256, 0, h->stream>>>(h->d_cmsl, h->d_cmsr, h->ncms,
+                                                                         h->d_alpha_raw, h->d_alpha);
 }
 
 // the step's final values all come from the volume and interface kernels: the plain LW step on a periodic
@@ -563,8 +568,15 @@ void enqueue_curved_surfaces(tlw_handle* h, int mode, const double* u_jump, doub
         ma.inv_w_first = h->h_basis.inv_w_first;
         ma.inv_w_last = h->h_basis.inv_w_last;
         ma.status = &h->d_step->status;
+        if (h->sc) {
+            ma.alpha = h->d_alpha;
+            ma.tFn = h->d_tFn;
+            ma.w_first = h->h_basis.weights[0];
+            ma.w_last = h->h_basis.weights[h->n - 1];
+        }
         for (size_t c = 0; c + 1 < h->mortar_off.size(); ++c) {
             const int b = h->mortar_off[c];
+            if (h->sc) ma.mortar_ij = h->d_cmj + (size_t)b * h->n;
             ma.small1 = h->d_cms1 + b;
             ma.small2 = h->d_cms2 + b;
             ma.large = h->d_cml + b;
@@ -1364,9 +1376,8 @@ int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* smal
                            const int32_t* large_reversed) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh || !h->curved) return fail(h, TLW_E_STATE, "curved mortars follow tlw_set_curved_mesh");
-    if (h->sc || h->parabolic || h->ncb > 0)
-        return fail(h, TLW_E_UNSUPPORTED, "curvilinear mortars: before the boundaries, without shock capturing or "
-                                          "Navier-Stokes");
+    if (h->parabolic || h->ncb > 0)
+        return fail(h, TLW_E_UNSUPPORTED, "curvilinear mortars: before the boundaries, without Navier-Stokes");
     if (n_mortars < 0 || (n_mortars > 0 && (!small1 || !small2 || !small_faces || !large || !large_faces || !large_reversed)))
         return fail(h, TLW_E_ARG, "mortars");
     struct Mtr { int s1, s2, l, code, cs, cl; };
@@ -1402,18 +1413,20 @@ int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* smal
         cls[c][m.l] = (signed char)m.cl;
         bucket[c].push_back((int)k);
     }
-    std::vector<int> v1, v2, vl, vc, off{0};
+    std::vector<int> v1, v2, vl, vc, off{0}, order;
     for (const auto& bk : bucket) {
         for (int k : bk) {
             v1.push_back(all[k].s1); v2.push_back(all[k].s2); vl.push_back(all[k].l); vc.push_back(all[k].code);
+            order.push_back(k);
         }
         off.push_back((int)v1.size());
     }
     TLW_CUDA(h, cudaSetDevice(h->device));
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));
     drop_graphs(h);
-    for (int** d : {&h->d_cms1, &h->d_cms2, &h->d_cml, &h->d_cmc})
+    for (int** d : {&h->d_cms1, &h->d_cms2, &h->d_cml, &h->d_cmc, &h->d_cmsl, &h->d_cmsr})
         if (*d) { cudaFree(*d); *d = nullptr; }
+    if (h->d_cmj) { cudaFree(h->d_cmj); h->d_cmj = nullptr; }
     auto up = [&](int*& d, const std::vector<int>& v) -> int {
         if (v.empty()) return TLW_OK;
         TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
@@ -1433,9 +1446,37 @@ int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* smal
     }
     if (h->d_mface) { cudaFree(h->d_mface); h->d_mface = nullptr; }
     if (n_mortars > 0 && (rc = up(h->d_mface, desc))) return rc;
+    // shock capturing: the blending factors are smoothed over the mortars too, (small 1, large) and
+    // (small 2, large); lw_mortars.inverse_jacobian starts as zeros (tlw_set_curved_mortar_jacobian)
+    std::vector<int> sl, sr;
+    for (const Mtr& m : all) {
+        sl.push_back(m.s1); sr.push_back(m.l);
+        sl.push_back(m.s2); sr.push_back(m.l);
+    }
+    if ((rc = up(h->d_cmsl, sl)) || (rc = up(h->d_cmsr, sr))) return rc;
+    h->ncms = (int)sl.size();
+    if (n_mortars > 0) {
+        TLW_CUDA(h, cudaMalloc(&h->d_cmj, (size_t)n_mortars * h->n * sizeof(double)));
+        TLW_CUDA(h, cudaMemset(h->d_cmj, 0, (size_t)n_mortars * h->n * sizeof(double)));
+    }
+    h->mortar_order = order;
     h->ncm = (int)n_mortars;
     h->mortar_off = off;
     h->face_used = used;
+    return TLW_OK;
+}
+
+int tlw_set_curved_mortar_jacobian(tlw_handle* h, const double* inverse_jacobian) {
+    if (!h) return TLW_E_ARG;
+    if (!h->have_mesh || !h->curved) return fail(h, TLW_E_STATE, "curved mortars follow tlw_set_curved_mesh");
+    if (h->ncm == 0) return TLW_OK;
+    std::vector<double> v((size_t)h->ncm * h->n, 0.0);
+    if (inverse_jacobian)
+        for (size_t c = 0; c < h->mortar_order.size(); ++c)
+            for (int l = 0; l < h->n; ++l) v[c * h->n + l] = inverse_jacobian[(size_t)h->mortar_order[c] * h->n + l];
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    TLW_CUDA(h, cudaMemcpy(h->d_cmj, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
     return TLW_OK;
 }
 

@@ -13,6 +13,12 @@
 // lifts it into the small element's face node and parks it in shared memory; then thread (1, i) lifts -2 times
 // the L2 projection of both positions' fluxes (reverse operators) into the large element's face node.
 // Launches take the mortars colour by colour (no element has faces of both classes in one colour).
+//
+// With shock capturing each small node's flux goes through get_blended_flux (dg_2d.jl:227-250, called at
+// :589-593) with the small element as the primary: the first-order flux fn along the small element's normal at
+// (u_small, interpolated u_large), fn_inner_ll the small element's fn_low slot of its face at the node,
+// fn_inner_rr the large element's fn_low slot of its face read in mortar order (index i, not reversed) and
+// interpolated like u (prolong2mortars!, :429-500), J^{-1} = lw_mortars.inverse_jacobian of the node.
 #pragma once
 #include "tlw_curved.cuh"
 #include "tlw_mortar.cuh"
@@ -38,6 +44,11 @@ struct CurvedMortarArgs {
     int flux_kind, speed_kind;
     double inv_w_first, inv_w_last;
     unsigned* status;
+    // shock capturing (null alpha: the plain LW flux)
+    const double* alpha;      // [e]
+    const double* tFn;        // fn_low slots [v, l, face, e]
+    const double* mortar_ij;  // lw_mortars.inverse_jacobian of this colour's mortars [k][l]
+    double w_first, w_last;
 };
 
 template <int N>
@@ -75,6 +86,7 @@ static __global__ void __launch_bounds__(128) curved_mortar_kernel(CurvedMortarA
         load4(a.metrics + ((size_t)se * nn + ns) * 4, J);
         const double nrm[2] = {sgS * (sf < 2 ? J[0] : J[2]), sgS * (sf < 2 ? J[1] : J[3])};
         const double* fwd = c_tlw_mortar[N][h ? 0 : 1];
+        double fir[NV] = {0, 0, 0, 0};
 #pragma unroll
         for (int i = 0; i < n; ++i) {
             const int li = rev ? n - 1 - i : i;
@@ -92,9 +104,44 @@ static __global__ void __launch_bounds__(128) curved_mortar_kernel(CurvedMortarA
                 Ul[v] = fma(c, y[v], Ul[v]);
                 Fl[v] = fma(c, z[v], Fl[v]);
             }
+            if (a.alpha) {
+                load4(a.tFn + (((size_t)lg * 4 + lf) * n + i) * NV, x);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) fir[v] = fma(c, x[v], fir[v]);
+            }
         }
         double fstar[NV];
         lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, Fs, Fl, us, ul, Us, Ul, nrm, fstar, a.status);
+        if (a.alpha) {   // get_blended_flux, small element as the primary
+            double fS[NV], gS[NV], fL[NV], gL[NV], fn[NV], fil[NV], test[NV], low[NV];
+            euler_fluxes(gm1, us[0], us[1], us[2], us[3], fS, gS);
+            euler_fluxes(gm1, ul[0], ul[1], ul[2], ul[3], fL, gL);
+            const double lam = max_abs_speed_normal(a.gamma, us, ul, nrm, a.speed_kind, a.status);
+#pragma unroll
+            for (int v = 0; v < NV; ++v)
+                fn[v] = 0.5 * ((fS[v] * nrm[0] + gS[v] * nrm[1]) + (fL[v] * nrm[0] + gL[v] * nrm[1])) +
+                        (-0.5 * lam * (ul[v] - us[v]));
+            load4(a.tFn + ts, fil);
+            const double alp = 0.5 * (__ldg(a.alpha + se) + __ldg(a.alpha + lg));
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fstar[v] = (1.0 - alp) * fstar[v] + alp * fn[v];
+            const double dt = *a.dt;
+            const double J = __ldg(a.mortar_ij + (size_t)k * n + l);
+            const double cl = dt * J / (a.w_last * 0.5);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                test[v] = us[v] - cl * (fstar[v] - fil[v]);
+                low[v] = us[v] - cl * (fn[v] - fil[v]);
+            }
+            if (!admissible(gm1, test)) zhang_shu_flux_fix(gm1, us, low, fstar, fil, fn, cl);
+            const double cr = -dt * J / (a.w_first * 0.5);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                test[v] = ul[v] - cr * (fstar[v] - fir[v]);
+                low[v] = ul[v] - cr * (fn[v] - fir[v]);
+            }
+            if (!admissible(gm1, test)) zhang_shu_flux_fix(gm1, ul, low, fstar, fir, fn, cr);
+        }
         dts = a.step_mode ? *a.dt : 1.0;
         const double cs = -dts * __ldg(a.inv_jac + (size_t)se * nn + ns) * ((sf & 1) ? a.inv_w_last : a.inv_w_first);
         double* os = a.out + ((size_t)se * nn + ns) * NV;

@@ -153,6 +153,12 @@ struct tlw_handle {
     // small face | large face << 2 | large reversed << 4
     int ncm = 0;
     int *d_cms1 = nullptr, *d_cms2 = nullptr, *d_cml = nullptr, *d_cmc = nullptr;
+    // shock capturing at the curvilinear mortars: smoothing pairs (small, large), lw_mortars.inverse_jacobian in
+    // colour order [k][l], and the caller's mortar index of each colour-ordered mortar
+    int *d_cmsl = nullptr, *d_cmsr = nullptr;
+    int ncms = 0;
+    double* d_cmj = nullptr;
+    std::vector<int> mortar_order;
     std::vector<int> mortar_off;            // mortar colour c covers [mortar_off[c], mortar_off[c + 1])
     // graphs: [start buffer] one step, two steps
     cudaGraphExec_t g_one[2] = {nullptr, nullptr};

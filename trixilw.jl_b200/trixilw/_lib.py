@@ -44,7 +44,7 @@ EXPORTED = (
     "tlw_solve_dts", "tlw_set_curved_mesh", "tlw_curved_colors", "tlw_set_tree_mortars",
     "tlw_set_parabolic", "tlw_adaptive_trial", "tlw_adaptive_accept",
     "tlw_set_positivity_limiter", "tlw_apply_positivity_limiter", "tlw_set_boundary_kinds", "tlw_set_parabolic_walls",
-    "tlw_set_curved_boundaries", "tlw_set_reconstruction", "tlw_set_curved_mortars",
+    "tlw_set_curved_boundaries", "tlw_set_reconstruction", "tlw_set_curved_mortars", "tlw_set_curved_mortar_jacobian",
     "tlw_set_halo", "tlw_dd_buffers", "tlw_dd_begin", "tlw_dd_volume", "tlw_dd_finish",
 )
 
@@ -124,6 +124,7 @@ def lib() -> ctypes.CDLL:
     L.tlw_set_curved_boundaries.argtypes = [P, i64, P, P, P]
     L.tlw_set_reconstruction.argtypes = [P, i32]
     L.tlw_set_curved_mortars.argtypes = [P, i64, P, P, P, P, P, P]
+    L.tlw_set_curved_mortar_jacobian.argtypes = [P, P]
     L.tlw_set_halo.argtypes = [P, i64, P, P]
     L.tlw_dd_buffers.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P)]
     L.tlw_dd_begin.argtypes = [P, dbl, dbl, dbl]

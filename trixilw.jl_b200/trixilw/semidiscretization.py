@@ -478,6 +478,17 @@ class SemidiscretizationHyperbolic:
         check(self.handle, L.tlw_get_cache(self.handle, item, _ptr(out), _lib.TLW_WHERE_HOST))
         return out
 
+    def set_mortar_inverse_jacobian(self, inverse_jacobian=None):
+        """lw_mortars.inverse_jacobian [n_mortars, n] of a curvilinear mesh with mortars, read by the
+        shock-capturing blend at the mortars (None: zeros, as the reference holds it before an AMR step)."""
+        if inverse_jacobian is None:
+            check(self.handle, lib().tlw_set_curved_mortar_jacobian(self.handle, None))
+            return
+        a = np.ascontiguousarray(inverse_jacobian, dtype=np.float64).reshape(-1)
+        if a.size != getattr(self.mesh, "n_mortars", 0) * self.nnodes:
+            raise ValueError("inverse_jacobian: n_mortars x nnodes values")
+        check(self.handle, lib().tlw_set_curved_mortar_jacobian(self.handle, _ptr(a)))
+
     def max_dt(self, u_ode: np.ndarray, cfl: float) -> float:
         dt = ctypes.c_double()
         check(self.handle, lib().tlw_max_dt(self.handle, _ptr(u_ode), _lib.TLW_WHERE_HOST, float(cfl), ctypes.byref(dt)))
