@@ -110,6 +110,18 @@ int tlw_adaptive_trial(tlw_handle* h, double dt, double abstol, double reltol, d
                        int32_t* admissible);
 int tlw_adaptive_accept(tlw_handle* h, double dt);
 
+/* The same Adaptive stepping with the controller on the device (perform_step!'s epsilon history, dt_factor,
+ * rejection and retry, set_dt! clamp; adaptive.jl:47-172), so that trials run back to back without a host
+ * round trip. tlw_adaptive_begin starts a run from the current state and time to t_end with dt_initial and the
+ * controller (beta1, beta2, beta3) (null: (0.6, -0.2, 0.0), lwfr.jl:162). tlw_adaptive_run enqueues n_trials
+ * trials (each: trial step with the estimate, limiter, admissibility, the controller's decision, the accepted
+ * state committed), then waits and reports the accepted steps so far (the handle's step count), the rejected
+ * trials of accepted steps (the reference's nreject) and whether t_end is reached; trials after that are
+ * no-ops. Synchronous; a mesh upload ends the run. */
+int tlw_adaptive_begin(tlw_handle* h, double t_end, double dt_initial, const double* controller);
+int tlw_adaptive_run(tlw_handle* h, int32_t n_trials, double abstol, double reltol, int64_t* steps,
+                     int64_t* rejected, int32_t* finished);
+
 /* Zhang-Shu positivity-preserving limiter, PositivityPreservingLimiterZhangShu(thresholds, variables) as a
  * stage limiter (src/callbacks/callbacks_stage/positivity_zhang_shu.jl:10-42, positivity_zhang_shu_dg2d.jl:8-176):
  * count (threshold, variable) pairs, applied in order; per pair the element pass and, on a TreeMesh with

@@ -180,3 +180,37 @@ def test_gpu_curved_adaptive_run_matches_oracle(oracle_mod, tl, rec):
     assert sol.t[0] == t_end and ctl.iter > 3
     assert sol.stats.nreject == ctl.nreject
     assert np.all(rel_l2(sol.u[0], u_cpu) < 1e-10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["tree", "curved_sc"])
+def test_gpu_device_controller_matches_host_controller(tl, kind):
+    """Adaptive(on_device=True): the controller on the device gives the host controller's run (the same
+    accepted steps and rejections, the same final state up to the last bits of pow / atan)."""
+    if kind == "tree":
+        N = 4
+        mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), 3)
+        eq = tl.CompressibleEulerEquations2D(1.4)
+        solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.LW()))
+        semi_of = lambda: tl.SemidiscretizationHyperbolic(mesh, tl.LW(), eq,
+                                                          tl.IsentropicVortex(5.0, center=(0.7, -0.4)), solver)
+        u0, t_end, dt0 = None, 1.0, 1e-3
+    else:
+        N = 4
+        m = tl.StructuredMesh((8, 8), warp)
+        mesh = tl.rotate_elements(m.curved(N), np.random.default_rng(11).integers(0, 4, 64))
+        semi_of = lambda: semi_for(tl, mesh, N, 2)
+        u0, t_end, dt0 = blast_state(mesh), 0.05, 1e-4
+    runs = []
+    for on_device in (False, True):
+        semi = semi_of()
+        upd = tl.semidiscretize(semi, tl.LW(), (0.0, t_end))
+        if u0 is not None:
+            upd.u0_ode[:] = u0
+        sol = tl.solve_lwfr(upd, (), dt0, TOL, tl.Adaptive(on_device=on_device, chunk=7))
+        runs.append(sol)
+    host, dev = runs
+    assert dev.t[0] == pytest.approx(t_end, rel=1e-14)
+    assert dev.stats.naccept == host.stats.naccept > 3
+    assert dev.stats.nreject == host.stats.nreject
+    assert np.all(rel_l2(dev.u[0], host.u[0]) < 1e-12)

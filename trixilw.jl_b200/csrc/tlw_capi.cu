@@ -76,6 +76,7 @@ void free_mesh(tlw_handle* h) {
     h->slots_valid = false;
     dfree(h->d_te); dfree(h->d_check);
     if (h->d_bad) { cudaFree(h->d_bad); h->d_bad = nullptr; }
+    if (h->d_adapt) { cudaFree(h->d_adapt); h->d_adapt = nullptr; }
     h->color_off.clear();
     h->face_used.clear();
     for (int** d : {&h->d_he, &h->d_hf, &h->d_hs})
@@ -1633,24 +1634,15 @@ int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl) {
     return TLW_OK;
 }
 
-int tlw_adaptive_trial(tlw_handle* h, double dt, double abstol, double reltol, double* total_temporal_error,
-                       int32_t* admissible) {
-    int rc = check_ready(h);
-    if (rc) return rc;
-    if (!total_temporal_error || !admissible || !(dt > 0.0)) return fail(h, TLW_E_ARG, "arguments");
-    // the reference's estimate comes from the LW volume kernels of depth 4 (TreeMesh) or 3 and 4 (curvilinear);
-    // its MDRK kernels and the TreeMesh kernel of depth 3 leave temporal_errors unset
-    if (h->opts.time_discretization != TLW_LW || h->parabolic || h->N < (h->curved ? 3 : 4))
-        return fail(h, TLW_E_UNSUPPORTED, "Adaptive: LW, hyperbolic, N >= 4 on a TreeMesh or N >= 3 on a curvilinear mesh");
-    TLW_CUDA(h, cudaSetDevice(h->device));
+static bool adaptive_finished_host(double t, double te) {
+    return t == te || std::fabs(t - te) <= 1.4901161193847656e-08 * std::max(std::fabs(t), std::fabs(te));
+}
+
+// the trial of one Adaptive iteration into the other state buffer, dt from d_step->dt_call: the LW step with
+// the temporal error estimate, the positivity limiter (perform_step!, adaptive.jl:131-132), the admissibility
+// check and the sum of the per-element errors (d_check[4 * 148])
+static int enqueue_adaptive_trial(tlw_handle* h, double abstol, double reltol) {
     const int blocks = (int)std::min<int64_t>(((int64_t)h->nn * h->E + 255) / 256, 4 * 148);
-    if (!h->d_te) {
-        TLW_CUDA(h, cudaMalloc(&h->d_te, (size_t)h->E * sizeof(double)));
-        TLW_CUDA(h, cudaMalloc(&h->d_check, (size_t)(4 * 148 + 1) * sizeof(double)));
-        TLW_CUDA(h, cudaMalloc(&h->d_bad, sizeof(unsigned)));
-    }
-    TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->dt_call, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    TLW_CUDA(h, cudaMemsetAsync(h->d_bad, 0, sizeof(unsigned), h->stream));
     const double* u = h->d_state[h->cur];
     double* trial = h->d_state[1 - h->cur];
     h->te_request = true;
@@ -1658,11 +1650,93 @@ int tlw_adaptive_trial(tlw_handle* h, double dt, double abstol, double reltol, d
     h->te_reltol = reltol;
     enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, trial, &h->d_step->dt_call);
     h->te_request = false;
-    enqueue_limiter(h, trial, 1, nullptr);   // perform_step!(..., ::Adaptive, ::LW) (adaptive.jl:131-132)
+    enqueue_limiter(h, trial, 1, nullptr);
     adaptive_check_kernel<<<blocks, 256, 0, h->stream>>>(h->d_te, (int)h->E, trial, (long long)h->nn * h->E,
                                                           h->opts.gamma, h->d_check, h->d_bad);
     adaptive_sum_kernel<<<1, 32, 0, h->stream>>>(h->d_check, blocks, h->d_check + 4 * 148);
     TLW_CUDA(h, cudaGetLastError());
+    return TLW_OK;
+}
+
+static int adaptive_supported(tlw_handle* h) {
+    // the reference's estimate comes from the LW volume kernels of depth 4 (TreeMesh) or 3 and 4 (curvilinear);
+    // its MDRK kernels and the TreeMesh kernel of depth 3 leave temporal_errors unset
+    if (h->opts.time_discretization != TLW_LW || h->parabolic || h->N < (h->curved ? 3 : 4))
+        return fail(h, TLW_E_UNSUPPORTED, "Adaptive: LW, hyperbolic, N >= 4 on a TreeMesh or N >= 3 on a curvilinear mesh");
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    if (!h->d_te) {
+        TLW_CUDA(h, cudaMalloc(&h->d_te, (size_t)h->E * sizeof(double)));
+        TLW_CUDA(h, cudaMalloc(&h->d_check, (size_t)(4 * 148 + 1) * sizeof(double)));
+        TLW_CUDA(h, cudaMalloc(&h->d_bad, sizeof(unsigned)));
+        TLW_CUDA(h, cudaMemset(h->d_bad, 0, sizeof(unsigned)));
+    }
+    return TLW_OK;
+}
+
+int tlw_adaptive_begin(tlw_handle* h, double t_end, double dt_initial, const double* controller) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!(dt_initial > 0.0) || !std::isfinite(t_end)) return fail(h, TLW_E_ARG, "t_end / dt_initial");
+    if ((rc = adaptive_supported(h))) return rc;
+    if (!h->d_adapt) TLW_CUDA(h, cudaMalloc(&h->d_adapt, sizeof(AdaptiveState)));
+    StepState st{};
+    TLW_CUDA(h, cudaMemcpyAsync(&st, h->d_step, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    AdaptiveState a{};
+    a.eps[0] = a.eps[1] = a.eps[2] = 1.0;
+    a.beta[0] = controller ? controller[0] : 0.6;
+    a.beta[1] = controller ? controller[1] : -0.2;
+    a.beta[2] = controller ? controller[2] : 0.0;
+    a.t_end = t_end;
+    a.dt = st.t + dt_initial > t_end ? t_end - st.t : dt_initial;   // set_dt!
+    a.k = (double)h->n;
+    a.ndofs = (double)h->nn * (double)h->E;
+    TLW_CUDA(h, cudaMemcpy(h->d_adapt, &a, sizeof(a), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, cudaMemset(h->d_bad, 0, sizeof(unsigned)));
+    return TLW_OK;
+}
+
+int tlw_adaptive_run(tlw_handle* h, int32_t n_trials, double abstol, double reltol, int64_t* steps,
+                     int64_t* rejected, int32_t* finished) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!h->d_adapt) return fail(h, TLW_E_STATE, "tlw_adaptive_run follows tlw_adaptive_begin");
+    if (n_trials < 0 || !steps || !rejected || !finished) return fail(h, TLW_E_ARG, "arguments");
+    if ((rc = adaptive_supported(h))) return rc;
+    const long long count = (long long)h->nn * h->E * NV;
+    const int cblocks = (int)std::min<long long>((count + 255) / 256, 8 * 148);
+    for (int q = 0; q < n_trials; ++q) {
+        adaptive_prepare_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->d_adapt);
+        if ((rc = enqueue_adaptive_trial(h, abstol, reltol))) return rc;
+        adaptive_judge_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->d_adapt, h->d_check + 4 * 148, h->d_bad);
+        // the accepted state is limited once more (solve_lwfr's loop, lwfr.jl:257); a rejected trial is
+        // overwritten by the next one
+        enqueue_limiter(h, h->d_state[1 - h->cur], 1, nullptr);
+        adaptive_commit_kernel<<<cblocks, 256, 0, h->stream>>>(h->d_adapt, h->d_state[1 - h->cur],
+                                                               h->d_state[h->cur], count);
+        TLW_CUDA(h, cudaGetLastError());
+    }
+    AdaptiveState a{};
+    StepState st{};
+    TLW_CUDA(h, cudaMemcpyAsync(&a, h->d_adapt, sizeof(a), cudaMemcpyDeviceToHost, h->stream));
+    TLW_CUDA(h, cudaMemcpyAsync(&st, h->d_step, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+    TLW_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->slots_valid = false;
+    *steps = st.steps;
+    *rejected = a.nreject;
+    *finished = adaptive_finished_host(st.t, a.t_end) ? 1 : 0;
+    return TLW_OK;
+}
+
+int tlw_adaptive_trial(tlw_handle* h, double dt, double abstol, double reltol, double* total_temporal_error,
+                       int32_t* admissible) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!total_temporal_error || !admissible || !(dt > 0.0)) return fail(h, TLW_E_ARG, "arguments");
+    if ((rc = adaptive_supported(h))) return rc;
+    TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->dt_call, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    TLW_CUDA(h, cudaMemsetAsync(h->d_bad, 0, sizeof(unsigned), h->stream));
+    if ((rc = enqueue_adaptive_trial(h, abstol, reltol))) return rc;
     double sum = 0.0;
     unsigned bad = 0, st = 0;
     TLW_CUDA(h, cudaMemcpyAsync(&sum, h->d_check + 4 * 148, sizeof(double), cudaMemcpyDeviceToHost, h->stream));

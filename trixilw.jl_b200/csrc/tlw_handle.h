@@ -107,6 +107,7 @@ struct tlw_handle {
     double* d_te = nullptr;
     double* d_check = nullptr;   // [blocks] partial sums, then the total
     unsigned* d_bad = nullptr;
+    tlw::AdaptiveState* d_adapt = nullptr;   // the device controller (tlw_adaptive_begin / tlw_adaptive_run)
     bool te_request = false;
     double te_abstol = 0.0, te_reltol = 0.0;
     // per-element CFL slots of the state in d_state[cur] (plain LW step on a periodic conforming TreeMesh)

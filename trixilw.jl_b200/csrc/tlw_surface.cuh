@@ -539,4 +539,74 @@ static __global__ void adaptive_accept_kernel(StepState* s, double dt) {
     s->steps += 1;
 }
 
+// The controller of perform_step!(..., ::Adaptive, ::LW) (src/solvers/adaptive.jl:101-172) on the device, so
+// that trials run back to back without a host round trip: the epsilon history of load_temporal_errors!
+// (:47-61; shifted only on the first try of a step, a non-finite error keeps the previous estimate),
+// dt_factor (:100-105) with the controller (beta1, beta2, beta3) of lwfr.jl:162, rejection when the trial is
+// not admissible or factor <= 0.81 (retry at min(factor, 0.95) dt), acceptance otherwise (next dt
+// min(factor, 1.5) dt), both clamped by set_dt! to end at t_end.
+struct AdaptiveState {
+    double eps[3];          // epsilon[-1], epsilon[0], epsilon[1]
+    double beta[3];
+    double dt;              // dt of the next trial
+    double t_end;
+    double k;               // nnodes
+    double ndofs;
+    double factor;
+    long long n_fail, nreject, trials;
+    int accept;             // the last trial was accepted
+    int finished;
+};
+
+__device__ __forceinline__ bool adaptive_finished(double t, double te) {
+    // isapprox(t, t_end) with the default rtol sqrt(eps(Float64))
+    return t == te || fabs(t - te) <= 1.4901161193847656e-08 * fmax(fabs(t), fabs(te));
+}
+
+static __global__ void adaptive_prepare_kernel(StepState* s, AdaptiveState* a) {
+    a->finished = adaptive_finished(s->t, a->t_end) ? 1 : 0;
+    s->dt_call = a->finished ? 0.0 : a->dt;
+}
+
+static __global__ void adaptive_judge_kernel(StepState* s, AdaptiveState* a, const double* sum, unsigned* bad) {
+    a->accept = 0;
+    const bool ok = *bad == 0 && s->status == 0;
+    *bad = 0;
+    s->status = 0;   // test_rhs! catches the DomainError: the trial is only inadmissible
+    if (a->finished) return;
+    const double err = sqrt(*sum / a->ndofs);
+    if (a->n_fail == 0) {
+        a->eps[0] = a->eps[1];
+        a->eps[1] = a->eps[2];
+    }
+    if (isfinite(err)) a->eps[2] = 1.0 / (err + 1e-12);
+    const double f = pow(a->eps[2], a->beta[0] / a->k) * pow(a->eps[1], a->beta[1] / a->k) *
+                     pow(a->eps[0], a->beta[2] / a->k);
+    const double factor = 1.0 + atan(f - 1.0);
+    a->factor = factor;
+    a->trials += 1;
+    double nd;
+    if (ok && !(factor <= 0.81)) {
+        a->nreject += a->n_fail;
+        a->n_fail = 0;
+        s->dt = a->dt;
+        s->t += a->dt;
+        s->steps += 1;
+        a->accept = 1;
+        nd = fmin(factor, 1.5) * a->dt;
+    } else {
+        a->n_fail += 1;
+        nd = fmin(factor, 0.95) * a->dt;
+    }
+    a->dt = s->t + nd > a->t_end ? a->t_end - s->t : nd;
+}
+
+// an accepted trial becomes the current state
+static __global__ void __launch_bounds__(256) adaptive_commit_kernel(const AdaptiveState* a, const double* __restrict__ trial,
+                                                                     double* __restrict__ u, long long count) {
+    if (!a->accept) return;
+    for (long long k = (long long)blockIdx.x * 256 + threadIdx.x; k < count; k += (long long)gridDim.x * 256)
+        u[k] = trial[k];
+}
+
 }  // namespace tlw

@@ -42,7 +42,7 @@ EXPORTED = (
     "tlw_batch_get_stream", "tlw_batch_autotune", "tlw_batch_num_groups", "tlw_batch_last_error",
     "tlw_adjoint_step", "tlw_forward_record", "tlw_adjoint_sweep", "tlw_adjoint_solve", "tlw_adjoint_dt_sequence",
     "tlw_solve_dts", "tlw_set_curved_mesh", "tlw_curved_colors", "tlw_set_tree_mortars",
-    "tlw_set_parabolic", "tlw_adaptive_trial", "tlw_adaptive_accept",
+    "tlw_set_parabolic", "tlw_adaptive_trial", "tlw_adaptive_accept", "tlw_adaptive_begin", "tlw_adaptive_run",
     "tlw_set_positivity_limiter", "tlw_apply_positivity_limiter", "tlw_set_boundary_kinds", "tlw_set_parabolic_walls",
     "tlw_set_curved_boundaries", "tlw_set_reconstruction", "tlw_set_curved_mortars", "tlw_set_curved_mortar_jacobian",
     "tlw_set_halo", "tlw_dd_buffers", "tlw_dd_begin", "tlw_dd_volume", "tlw_dd_finish",
@@ -132,6 +132,8 @@ def lib() -> ctypes.CDLL:
     L.tlw_dd_finish.argtypes = [P]
     L.tlw_adaptive_trial.argtypes = [P, dbl, dbl, dbl, dp, ctypes.POINTER(ctypes.c_int32)]
     L.tlw_adaptive_accept.argtypes = [P, dbl]
+    L.tlw_adaptive_begin.argtypes = [P, dbl, dbl, P]
+    L.tlw_adaptive_run.argtypes = [P, i32, dbl, dbl, P, P, P]
     L.tlw_curved_colors.argtypes = [P]
     L.tlw_curved_colors.restype = i32
     L.tlw_adjoint_step.argtypes = [P, P, P, P, dbl, i32]

@@ -96,6 +96,12 @@ def solve_lwfr(lw_update: LWUpdate, callbacks=(), dt_initial: float = 0.0, toler
     semi = lw_update.p
     n_pairs = install_limiters(semi, limiters)
     if isinstance(time_step_computation, Adaptive):
+        tsc = time_step_computation
+        semi_ = lw_update.p
+        on_host_only = (semi_.mesh.n_boundaries > 0 and semi_.time_dependent_boundaries()) or \
+            any(getattr(cb, "interval", 0) for cb in callbacks)
+        if getattr(tsc, "on_device", False) and not on_host_only:
+            return _solve_adaptive_device(lw_update, callbacks, dt_initial, tolerances, n_pairs > 0, tsc.chunk)
         return _solve_adaptive(lw_update, callbacks, dt_initial, tolerances, n_pairs > 0)
     assert isinstance(time_step_computation, CFLBased)
     cfl = time_step_computation.cfl_number
@@ -210,6 +216,33 @@ def _solve_adaptive(lw_update: LWUpdate, callbacks, dt_initial: float, tolerance
                     cb(integ, integ.get_state())
     integ.sync_time()
     integ.stats.nreject = ctl.nreject
+    u = integ.get_state()
+    for cb in callbacks:
+        cb(integ, u)
+    return LWSolution([u], lw_update, [integ.t], integ.stats)
+
+
+def _solve_adaptive_device(lw_update: LWUpdate, callbacks, dt_initial: float, tolerances, limit: bool,
+                           chunk: int) -> LWSolution:
+    """Adaptive stepping with the controller on the device: chunks of trials without host round trips."""
+    semi = lw_update.p
+    tol = tolerances or {"abstol": 1e-6, "reltol": 1e-6}
+    integ = LWIntegrator(lw_update, tol)
+    semi._prepare_boundaries(lw_update.tspan[0], 0.0, 1.0)
+    integ.set_state(lw_update.u0_ode, lw_update.tspan[0])
+    if limit:
+        check(integ.handle, lib().tlw_apply_positivity_limiter(integ.handle))
+    beta = (ctypes.c_double * 3)(*CONTROLLER)
+    check(integ.handle, lib().tlw_adaptive_begin(integ.handle, float(lw_update.tspan[1]), float(dt_initial), beta))
+    steps, rejected, finished = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+    while True:
+        check(integ.handle, lib().tlw_adaptive_run(integ.handle, int(chunk), float(tol["abstol"]),
+                                                   float(tol["reltol"]), ctypes.byref(steps),
+                                                   ctypes.byref(rejected), ctypes.byref(finished)))
+        if finished.value:
+            break
+    integ.sync_time()
+    integ.stats.nreject = int(rejected.value)
     u = integ.get_state()
     for cb in callbacks:
         cb(integ, u)

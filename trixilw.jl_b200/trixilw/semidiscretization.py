@@ -53,7 +53,15 @@ class CFLBased:
 class Adaptive:
     """Error-controlled stepping (src/solvers/adaptive.jl:47-172): the LW step's temporal error estimate,
     the PI controller with (beta1, beta2, beta3) = (0.6, -0.2, 0.0) (src/solvers/lwfr.jl:162) and rejection
-    below a factor of 0.81. LW on a TreeMesh with N >= 4."""
+    below a factor of 0.81. LW, hyperbolic; N >= 4 on a TreeMesh, N >= 3 on a curvilinear mesh.
+
+    on_device: the controller runs on the device too (tlw_adaptive_begin / tlw_adaptive_run), so trials follow
+    one another without a host round trip; chunk trials per call. Time-dependent boundary data and interval
+    callbacks keep the controller on the host (they act between steps)."""
+
+    def __init__(self, on_device: bool = False, chunk: int = 32):
+        self.on_device = on_device
+        self.chunk = chunk
 
 
 @dataclass
