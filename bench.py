@@ -31,6 +31,7 @@ sys.path.insert(0, os.path.join(ROOT, "trixilw.jl_b200"))
 METRIC = "LW-FR DOF-updates/s on 1 B200 (% HBM roofline); batched & adjoint vs plain"
 UNIT = "DOF-updates/s"
 
+DEFAULT_WORKLOAD = "vortex_tree512_N4_lw"
 # name -> (refinement level, N, time discretization, initial condition)
 WORKLOADS = {
     "vortex_tree512_N4_lw": (9, 4, "lw", "vortex"),
@@ -273,9 +274,10 @@ def cfl_for(N):
     return 0.98 * (N + 1) * table.get(N, 0.07)
 
 
-def cpu_oracle_rate(level, N, td, icname, steps_hint, budget_s=20.0):
+def cpu_oracle_rate(level, N, td, icname, steps_hint, budget_s=20.0, warmup=1):
     """Oracle port (C++/OpenMP, all host threads) on the same workload: DOF-updates/s over a bounded
-    number of steps (as many as fit in about budget_s seconds, at least one)."""
+    number of steps (steps_hint, or as many as fit in about budget_s seconds, at least one) after `warmup`
+    untimed steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import pyoracle
@@ -309,13 +311,21 @@ def cpu_oracle_rate(level, N, td, icname, steps_hint, budget_s=20.0):
     if icname == "blast":
         o.set_shock_capturing(True, 0.5, 0.001, True, reconstruction=1)
     t0 = time.perf_counter()
-    o.steps(u, 1, cfl, 0.0, 1e9, kind=kind, nthreads=threads)
-    one = time.perf_counter() - t0
+    o.steps(u, max(1, warmup), cfl, 0.0, 1e9, kind=kind, nthreads=threads)
+    one = (time.perf_counter() - t0) / max(1, warmup)
     nsteps = max(1, min(steps_hint, int(budget_s / max(one, 1e-3))))
     t0 = time.perf_counter()
     o.steps(u, nsteps, cfl, 0.0, 1e9, kind=kind, nthreads=threads)
     el = time.perf_counter() - t0
     return mesh.ndofs(N) * nsteps / el, threads, nsteps, el
+
+
+def workload_config(workload, N, E, ndofs, td, cfl, world):
+    """The `config` of a plain-workload line, the same for both arms."""
+    return {"workload": workload, "polydeg": N, "elements": E, "ndofs": ndofs, "time_discretization": td,
+            "cfl": cfl, "dt": "device CFL reduction every step",
+            "l2": "inputs larger than L2 (state %.0f MB per array)" % (8 * 4 * ndofs / 1e6),
+            "parallelism": f"replicas{world}" if world > 1 else "single"}
 
 
 def run_reference(args):
@@ -327,17 +337,20 @@ def run_reference(args):
     if args.workload in ADJOINT_WORKLOADS:
         return run_reference_adjoint(args, world)
     level, N, td, icname = WORKLOADS[args.workload]
-    # warm-up: one step; then K steps, each a bounded sample of the same workload (one full step)
-    rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=max(1, args.steps), budget_s=60.0)
-    ndofs = (1 << (2 * level)) * (N + 1) ** 2
+    # W warm-up steps, then K timed steps of the full workload (fewer when K steps would take over 2 minutes)
+    rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=max(1, args.steps), budget_s=120.0,
+                                                warmup=max(args.warmup, 3))
+    E = 1 << (2 * level)
+    ndofs = E * (N + 1) ** 2
+    cfl = RIEMANN_CFL if icname in ("riemann", "blast") else cfl_for(N)
     sample = f"{nsteps} full steps of the {args.workload} workload ({ndofs} DOF) in {el:.2f} s"
     out = {
         "metric": METRIC, "value": rate, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": nsteps,
-        "warmup": 1, "ms_per_step": 1e3 * el / nsteps, "higher_is_better": True, "scaling": "weak",
+        "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * el / nsteps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "ndofs": ndofs, "polydeg": N, "time_discretization": td,
-                   "elements": 1 << (2 * level), "implementation": "CPU oracle port (C++/OpenMP) of the TrixiLW "
-                   "LW rhs; the Julia reference cannot run here"},
+        "config": workload_config(args.workload, N, E, ndofs, td, cfl, 1),
+        "implementation": "CPU oracle port (C++/OpenMP, all host threads) of the TrixiLW LW / MDRK step; the Julia "
+                          "reference cannot run on these machines",
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -537,29 +550,36 @@ def run_ours(args):
                else f"lw_volume_kernel_N{N}_{'warped' if curved else 'tree'}{1 << level}")
         traffic = profile_traffic(tag)
         step_alg = alg_bytes_per_element_step(N, td, curved) * E
+        # the binding roof of the volume kernel: the slower of its byte floor (HBM) and its flop floor (FP64)
+        t_hbm = vol_bytes / (peak * 1e9)
+        t_fp64 = vol_flops / (fp64_peak * 1e12) if (vol_flops and fp64_peak) else 0.0
+        fp64_bound = t_fp64 > t_hbm
+        hbm_rec = {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                   "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                   "alg_bytes_per_launch": vol_bytes, "floor_ms": 1e3 * t_hbm}
+        fp64_rec = ({"achieved": vol_flops / (vol_ms * 1e-3) / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": (vol_flops / (vol_ms * 1e-3) / 1e12) / fp64_peak if fp64_peak else None,
+                     "peak_source": "measured live (register FMA loop)", "alg_flops_per_launch": vol_flops,
+                     "floor_ms": 1e3 * t_fp64} if vol_flops else
+                    {"achieved": None, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "note": "no algorithmic flop model for the Navier-Stokes or the shock-capturing kernels"})
+        binding = fp64_rec if fp64_bound else hbm_rec
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "polydeg": N, "elements": E, "ndofs": ndofs,
-                       "time_discretization": td, "cfl": cfl, "dt": "device CFL reduction every step",
-                       "l2": "inputs larger than L2 (state %.0f MB per array)" % (state_bytes / 1e6),
-                       "parallelism": f"replicas{world}" if world > 1 else "single"},
+            "config": workload_config(args.workload, N, E, ndofs, td, cfl, world),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                     "steps": n_e2e},
             "roofline": {"kernel": (f"grad_volume_kernel + curved_grad_*_kernel + par_volume_kernel<{N}, MODE_STEP, CURVED>"
                                     if ns else f"lw_volume_kernel<{N}, MODE_STEP, SC, CURVED, MUSCL>" if icname == "blast"
                                     else f"lw_volume_kernel<{N}, MODE_STEP{', SC' if sc else ''}{', CURVED' if curved else ''}>"),
-                         "bound": "hbm",
-                         "achieved": achieved,
-                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                         "alg_bytes_per_launch": vol_bytes, "ms_per_launch": vol_ms,
-                         "fp64": ({"achieved_tflops": vol_flops / (vol_ms * 1e-3) / 1e12, "peak_tflops": fp64_peak,
-                                   "frac": (vol_flops / (vol_ms * 1e-3) / 1e12) / fp64_peak if fp64_peak else None,
-                                   "peak_source": "measured live (register FMA loop)"} if vol_flops else
-                                  {"achieved_tflops": None, "peak_tflops": fp64_peak,
-                                   "note": "no algorithmic flop model for the Navier-Stokes or the shock-capturing kernels"}),
+                         "bound": "fp64" if fp64_bound else "hbm",
+                         "achieved": binding["achieved"], "peak": binding["peak"], "unit": binding["unit"],
+                         "frac": binding["frac"], "traffic": traffic,
+                         "peak_source": binding["peak_source"], "ms_per_launch": vol_ms,
+                         "binding_floor_ms": 1e3 * max(t_hbm, t_fp64),
+                         "hbm": hbm_rec, "fp64": fp64_rec,
                          "step": {"alg_bytes_per_step": step_alg,
                                   "achieved_gbs": step_alg * args.steps / (ms_max * 1e-3) / 1e9,
                                   "frac": step_alg * args.steps / (ms_max * 1e-3) / 1e9 / peak},
@@ -576,11 +596,38 @@ def run_ours(args):
             rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=args.steps)
             out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                                    "sample": f"{nsteps} full steps of the same workload ({ndofs} DOF), {el:.1f} s"}
+        if world == 1 and args.forms and args.workload == DEFAULT_WORKLOAD:
+            out.update(forms_records())
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def forms_records():
+    """The metric's other two forms, measured on their own workloads in the same run: the batched form against
+    looping the plain path (512 uneven instances, 50 steps) and the adjoint gradient against the forward solve
+    (128^2, N = 4, 200 steps, checkpoints every 20; 8 finite-difference directions)."""
+    b = run_batched(argparse.Namespace(workload="batched512_vortex_lw", steps=50, warmup=3, no_cpu_baseline=True),
+                    emit=False)
+    a = run_adjoint(argparse.Namespace(workload="adjoint128_vortex_lw", steps=5, warmup=3, fd_directions=8),
+                    emit=False)
+    return {
+        "batched": {"workload": "batched512_vortex_lw", "value": b["value"], "unit": UNIT, "steps": b["steps"],
+                    "ms_per_step": b["ms_per_step"], "looped_plain": b["looped_plain"]["value"],
+                    "speedup_vs_looped": b["speedup_vs_looped"],
+                    "speedup_vs_looped_async": b["speedup_vs_looped_async"],
+                    "per_instance_l2_error_max_rel_diff": b["per_instance_l2_error_max_rel_diff"],
+                    "bitwise_equal_to_looped": b["bitwise_equal_to_looped"], "e2e": b["e2e"],
+                    "instances": b["config"]["instances"], "ndofs_total": b["config"]["ndofs_total"]},
+        "adjoint": {"workload": "adjoint128_vortex_lw", "value": a["value"], "unit": a["unit"],
+                    "gradient_ms": a["gradient_ms"], "forward_solve_ms": a["forward_solve_ms"],
+                    "gradient_cost_vs_forward": a["gradient_cost_vs_forward"],
+                    "store_all_cost_vs_forward": a["store_all"]["gradient_cost_vs_forward"],
+                    "fd_check": a["fd_check"], "nsteps": a["config"]["nsteps"],
+                    "checkpoint_every": a["config"]["checkpoint_every"]},
+    }
 
 
 def run_decomposed(args):
@@ -695,8 +742,9 @@ def batch_instances(tl, count):
     return eq, out
 
 
-def run_batched(args):
-    """Batched form vs looping the plain (single-instance) path over the same instances."""
+def run_batched(args, emit=True):
+    """Batched form vs looping the plain (single-instance) path over the same instances. emit=False: return
+    the record instead of printing it (rank 0)."""
     import numpy as np
     import torch
 
@@ -888,6 +936,8 @@ def run_batched(args):
                     break
             out["cpu_baseline"] = {"value": done / el, "unit": UNIT, "cores": threads, "kind": "port",
                                    "sample": f"5 steps of each of the first {used} instances, {el:.1f} s"}
+        if not emit:
+            return out
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -895,7 +945,7 @@ def run_batched(args):
         dist.destroy_process_group()
 
 
-def run_adjoint(args):
+def run_adjoint(args, emit=True):
     """Gradient of J = 1/2 ||rho(T) - rho_target||^2 with respect to the discrete initial state by the
     checkpointed discrete adjoint, against the cost of the plain forward solve; central finite differences
     on 64 random unit directions check it."""
@@ -1029,6 +1079,8 @@ def run_adjoint(args):
             # adjoint 2 a step
             "gpu_launches": reps * (5 * nsteps + 2 + 3 * (nsteps - ck) - 2 * ((nsteps - 1) // ck) + 2 * nsteps),
         }
+        if not emit:
+            return out
         print(json.dumps(out), flush=True)
 
 
@@ -1038,8 +1090,10 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="vortex_tree512_N4_lw", choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + sorted(ADJOINT_WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + sorted(BATCH_WORKLOADS) + sorted(ADJOINT_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", dest="forms", action="store_false",
+                    help="default workload: leave out the batched and adjoint sub-records")
     ap.add_argument("--fd-directions", type=int, default=64,
                     help="adjoint workload: random directions of the finite-difference gradient check")
     ap.add_argument("--decompose", action="store_true",

@@ -117,7 +117,9 @@ int tlw_adaptive_accept(tlw_handle* h, double dt);
  * trials (each: trial step with the estimate, limiter, admissibility, the controller's decision, the accepted
  * state committed), then waits and reports the accepted steps so far (the handle's step count), the rejected
  * trials of accepted steps (the reference's nreject) and whether t_end is reached; trials after that are
- * no-ops. Synchronous; a mesh upload ends the run. */
+ * no-ops. Synchronous; a mesh upload ends the run. The reference retries a rejected trial without a limit;
+ * here, when repeated rejections bring the next dt to 1e-14 |t| or below, the run stops and tlw_adaptive_run
+ * returns TLW_E_NONADMISSIBLE. */
 int tlw_adaptive_begin(tlw_handle* h, double t_end, double dt_initial, const double* controller);
 int tlw_adaptive_run(tlw_handle* h, int32_t n_trials, double abstol, double reltol, int64_t* steps,
                      int64_t* rejected, int32_t* finished);
@@ -292,6 +294,9 @@ int tlw_step_timed(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, d
 /* Measures the device's dense FP64 FMA throughput (TFLOP/s) with a bounded register-resident loop.
  * Roofline calibration only (no counterpart in the reference). */
 int tlw_probe_fp64_tflops(int32_t device, double* tflops);
+/* y[k] = the kernels' reciprocal of x[k] (the 1/rho of every Euler flux) for n host values, on the given
+ * device; for accuracy tests of that routine against IEEE division (no counterpart in the reference). */
+int tlw_probe_reciprocal(int32_t device, const double* x, double* y, int64_t n);
 /* Synchronous: current time, last dt and number of accepted steps. */
 int tlw_get_time(tlw_handle* h, double* t, double* dt_last, int64_t* steps);
 
@@ -314,10 +319,11 @@ const char* tlw_last_error(tlw_handle* h);
  * All pointers are device pointers, 16-byte aligned: u, du [v, i, j, element]; inverse_jacobian
  * [element]; x_left/x_right, y_left/y_right the 0-based element ids of the x- and y-oriented interfaces.
  * The face-trace scratch is a static device array of TLW_NOALLOC_SCRATCH_BYTES: meshes with
- * n_elements * 2 * 4 * (N+1) * 4 * 8 bytes of traces beyond it are rejected with TLW_E_ARG. Calls share
- * that array, so calls that overlap on the GPU race. The first call on a device sets the device up
- * (make it before any stream capture). Runs on `stream` (a cudaStream_t, 0 = default) and returns
- * after the result is in du: TLW_OK, TLW_E_NONADMISSIBLE (DomainError), TLW_E_ARG or TLW_E_CUDA. */
+ * n_elements * 2 * 4 * (N+1) * 4 * 8 bytes of traces beyond it are rejected with TLW_E_ARG. Calls on a
+ * device share that array and the static dt and status words beside it, so calls that overlap on the GPU
+ * race. The first call on a device sets the device up (make it before any stream capture). Runs on `stream`
+ * (a cudaStream_t, 0 = default), waits for that stream and returns after the result is in du: TLW_OK,
+ * TLW_E_NONADMISSIBLE (DomainError), TLW_E_ARG or TLW_E_CUDA. */
 #define TLW_NOALLOC_SCRATCH_BYTES (32u << 20)
 int tlw_rhs_lw_noalloc(int32_t polydeg, double gamma, int32_t surface_flux, int32_t max_speed, int64_t n_elements,
                        const double* inverse_jacobian, int32_t n_x_interfaces, const int32_t* x_left,

@@ -74,3 +74,35 @@ def test_gpu_adaptive_matches_oracle_run(oracle_mod, tl):
     assert sol.stats.nreject == ctl.nreject
     d = (sol.u[0] - u_cpu).reshape(-1, 4)
     assert np.all(np.linalg.norm(d, axis=0) / np.linalg.norm(u_cpu.reshape(-1, 4), axis=0) < 1e-10)
+
+
+def test_host_controller_stops_when_dt_stalls(tl):
+    """Every trial rejected (a persistently non-admissible state): the reference would retry for ever; the
+    controller raises DomainError once dt no longer moves t."""
+    from trixilw.lwfr import ADAPTIVE_DT_FLOOR, AdaptiveController
+    ctl = AdaptiveController(5, 0.5, 1.0, 1e-3)
+    with pytest.raises(tl.DomainError):
+        for _ in range(10_000):
+            ctl.judge(float("nan"), False)
+    assert ctl.dt <= ADAPTIVE_DT_FLOOR * 1.0 and 400 < ctl.n_fail < 1000
+
+
+def _negative_pressure_semi(tl):
+    m = tl.TreeMesh((-1.0, -1.0), (1.0, 1.0), 2)
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    solver = tl.DGSEM(4, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.LW()))
+    semi = tl.SemidiscretizationHyperbolic(m, tl.LW(), eq, tl.IsentropicVortex(5.0), solver)
+    upd = tl.semidiscretize(semi, tl.LW(), (0.0, 1.0))
+    u = upd.u0_ode.reshape(-1, 4)
+    u[:, 1:3] = 0.0
+    u[:, 3] = -1.0          # rho e < 0 everywhere: every trial takes the square root of a negative pressure
+    return upd
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("on_device", [False, True])
+def test_gpu_adaptive_run_with_a_non_admissible_state_ends(tl, on_device):
+    """A run that can never accept a trial stops with DomainError (host controller and device controller)."""
+    upd = _negative_pressure_semi(tl)
+    with pytest.raises(tl.DomainError):
+        tl.solve_lwfr(upd, (), 1e-3, TOL, tl.Adaptive(on_device=on_device, chunk=64))

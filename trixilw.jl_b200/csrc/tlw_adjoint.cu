@@ -948,7 +948,7 @@ int adj_status(tlw_handle* h) {
     TLW_ACUDA(h, cudaStreamSynchronize(h->stream));
     if (st) {
         const unsigned zero = 0;
-        TLW_ACUDA(h, cudaMemcpy(&h->d_step->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+        TLW_ACUDA(h, upload_on(h->stream, &h->d_step->status, &zero, sizeof(zero)));
         return afail(h, TLW_E_NONADMISSIBLE, "non-admissible state: square root of a negative number (DomainError)");
     }
     return TLW_OK;

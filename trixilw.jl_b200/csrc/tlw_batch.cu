@@ -250,7 +250,7 @@ int read_batch_status(tlw_batch* b) {
     TLW_BCUDA(b, cudaStreamSynchronize(b->stream));
     if (st) {
         const unsigned zero = 0;
-        TLW_BCUDA(b, cudaMemcpy(&b->d_step->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+        TLW_BCUDA(b, upload_on(b->stream, &b->d_step->status, &zero, sizeof(zero)));
         return bfail(b, TLW_E_NONADMISSIBLE, "non-admissible state: square root of a negative number (DomainError)");
     }
     return TLW_OK;
@@ -280,7 +280,7 @@ int tlw_batch_create(const tlw_opts* opts, tlw_batch** out) {
     std::memset(&all[0], 0, sizeof(all[0]));
     for (int N = 1; N <= 7; ++N) host_build_basis(N, all[N]);
     if (upload_const_basis(all) != cudaSuccess || cudaMalloc(&b->d_step, sizeof(StepState)) != cudaSuccess ||
-        cudaMemset(b->d_step, 0, sizeof(StepState)) != cudaSuccess) {
+        zero_on(b->stream, b->d_step, sizeof(StepState)) != cudaSuccess) {
         tlw_batch_destroy(b);
         return TLW_E_CUDA;
     }
@@ -366,13 +366,13 @@ int tlw_batch_finalize(tlw_batch* b) {
         if (g.E > (int64_t)0x7fffffff / 64) return bfail(b, TLW_E_ARG, "batch group too large");
         auto up_d = [&](double*& d, const std::vector<double>& v) -> int {
             TLW_BCUDA(b, cudaMalloc(&d, v.size() * sizeof(double)));
-            TLW_BCUDA(b, cudaMemcpy(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+            TLW_BCUDA(b, upload_on(b->stream, d, v.data(), v.size() * sizeof(double)));
             return TLW_OK;
         };
         auto up_i = [&](int*& d, const std::vector<int>& v) -> int {
             if (v.empty()) return TLW_OK;
             TLW_BCUDA(b, cudaMalloc(&d, v.size() * sizeof(int)));
-            TLW_BCUDA(b, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+            TLW_BCUDA(b, upload_on(b->stream, d, v.data(), v.size() * sizeof(int)));
             return TLW_OK;
         };
         int rc;
@@ -389,22 +389,22 @@ int tlw_batch_finalize(tlw_batch* b) {
         b->groups.push_back(g);
     }
     TLW_BCUDA(b, cudaMalloc(&b->d_max, ninst * sizeof(unsigned long long)));
-    TLW_BCUDA(b, cudaMemset(b->d_max, 0, ninst * sizeof(unsigned long long)));
+    TLW_BCUDA(b, zero_on(b->stream, b->d_max, ninst * sizeof(unsigned long long)));
     TLW_BCUDA(b, cudaMalloc(&b->d_dt, ninst * sizeof(double)));
-    TLW_BCUDA(b, cudaMemset(b->d_dt, 0, ninst * sizeof(double)));
+    TLW_BCUDA(b, zero_on(b->stream, b->d_dt, ninst * sizeof(double)));
     TLW_BCUDA(b, cudaMalloc(&b->d_t, ninst * sizeof(double)));
-    TLW_BCUDA(b, cudaMemset(b->d_t, 0, ninst * sizeof(double)));
+    TLW_BCUDA(b, zero_on(b->stream, b->d_t, ninst * sizeof(double)));
     TLW_BCUDA(b, cudaMalloc(&b->d_t_end, ninst * sizeof(double)));
     TLW_BCUDA(b, cudaMalloc(&b->d_cfl, ninst * sizeof(double)));
     TLW_BCUDA(b, cudaMalloc(&b->d_steps, ninst * sizeof(long long)));
-    TLW_BCUDA(b, cudaMemset(b->d_steps, 0, ninst * sizeof(long long)));
+    TLW_BCUDA(b, zero_on(b->stream, b->d_steps, ninst * sizeof(long long)));
     std::vector<int> nn(ninst);
     std::vector<double> inf(ninst, INFINITY), one(ninst, 0.5);
     for (int i = 0; i < ninst; ++i) nn[i] = b->host[i].N + 1;
     TLW_BCUDA(b, cudaMalloc(&b->d_nnodes, ninst * sizeof(int)));
-    TLW_BCUDA(b, cudaMemcpy(b->d_nnodes, nn.data(), ninst * sizeof(int), cudaMemcpyHostToDevice));
-    TLW_BCUDA(b, cudaMemcpy(b->d_t_end, inf.data(), ninst * sizeof(double), cudaMemcpyHostToDevice));
-    TLW_BCUDA(b, cudaMemcpy(b->d_cfl, one.data(), ninst * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_BCUDA(b, upload_on(b->stream, b->d_nnodes, nn.data(), ninst * sizeof(int)));
+    TLW_BCUDA(b, upload_on(b->stream, b->d_t_end, inf.data(), ninst * sizeof(double)));
+    TLW_BCUDA(b, upload_on(b->stream, b->d_cfl, one.data(), ninst * sizeof(double)));
     b->finalized = true;
     b->cur = 0;
     return TLW_OK;

@@ -21,6 +21,7 @@
 #include "tlw_parabolic.cuh"
 #include "tlw_surface.cuh"
 #include "tlw_volume.cuh"
+#include "tlw_launch.cuh"
 
 using namespace tlw;
 
@@ -98,275 +99,6 @@ void free_mesh(tlw_handle* h) {
     h->have_bdata = false;
 }
 
-NSParams ns_params(const tlw_handle* h) {
-    NSParams p{};
-    p.gamma = h->opts.gamma;
-    p.mu = h->ns_mu;
-    p.Pr = h->ns_Pr;
-    p.kappa = h->opts.gamma / ((h->opts.gamma - 1.0) * h->ns_Pr);
-    return p;
-}
-
-// ---- kernel launch helpers (template dispatch over N) -------------------------------------------
-template <int N>
-struct Launch {
-    using C = VolCfg<N>;
-    template <bool SC>
-    static void set_attr_sc() {
-        const int lw = (int)C::smem_bytes(SC ? 8 : 4), md = (int)C::smem_bytes(SC ? 8 : 2);
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
-        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
-        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
-        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
-        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
-    }
-    static void set_attributes() {
-        set_attr_sc<false>();
-        set_attr_sc<true>();
-        const int lw = (int)C::smem_bytes(4);
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
-        te_volume(nullptr, VolArgs{}, 0, false, true);
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
-        curved_sc_attributes<0>();
-        curved_sc_attributes<1>();
-        curved_sc_attributes<2>();
-        const int md = (int)C::smem_bytes(2);
-        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
-        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
-        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
-        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
-    }
-    template <bool SC>
-    static void volume_sc(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
-        const size_t lw = C::smem_bytes(SC ? 8 : 4), md = C::smem_bytes(SC ? 8 : 2);
-        if (stage == TLW_STAGE_LW) {
-            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, SC><<<grid, C::THREADS, lw, s>>>(a);
-            else lw_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, lw, s>>>(a);
-        } else if (stage == TLW_STAGE_MDRK1) {
-            if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS, SC><<<grid, C::THREADS, md, s>>>(a);
-            else mdrk1_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, md, s>>>(a);
-        } else {
-            if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS, SC><<<grid, C::THREADS, md, s>>>(a);
-            else mdrk2_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, md, s>>>(a);
-        }
-    }
-    // curvilinear shock capturing: LW or an MDRK stage with first-order (REC 0), MUSCL (REC 1) or MUSCL-Hancock
-    // (REC 2) subcells
-    template <int REC>
-    static void curved_sc(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
-        const size_t sm = C::smem_bytes(REC ? 12 : 8);
-        if (stage == TLW_STAGE_MDRK1) {
-            if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS, true, true, REC><<<grid, C::THREADS, sm, s>>>(a);
-            else mdrk1_volume_kernel<N, MODE_STEP, true, true, REC><<<grid, C::THREADS, sm, s>>>(a);
-        } else if (stage == TLW_STAGE_MDRK2) {
-            if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS, true, true, REC><<<grid, C::THREADS, sm, s>>>(a);
-            else mdrk2_volume_kernel<N, MODE_STEP, true, true, REC><<<grid, C::THREADS, sm, s>>>(a);
-        } else {
-            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, REC><<<grid, C::THREADS, sm, s>>>(a);
-            else lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, REC><<<grid, C::THREADS, sm, s>>>(a);
-        }
-    }
-    template <int REC>
-    static void curved_sc_attributes() {
-        const int sm = (int)C::smem_bytes(REC ? 12 : 8);
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, true, 0, true, false, false, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, true, 0, true, false, false, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, true, true, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, true, true, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, true, true, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, true, true, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    }
-    // Adaptive trial step: the LW kernel with the temporal error estimate (a step into a.out), on a TreeMesh
-    // (N >= 4) or a curvilinear mesh (N >= 3), with or without shock capturing; attr_only sets the shared
-    // memory attributes of every variant instead
-    template <bool SC, bool CURVED, int REC>
-    static void te_launch(cudaStream_t s, const VolArgs& a, int grid, bool attr_only) {
-        const int sm = (int)C::smem_bytes(!SC ? 4 : REC ? 12 : 8);
-        if (attr_only)
-            cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, SC, 0, CURVED, true, false, REC>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        else
-            lw_volume_kernel<N, MODE_STEP, SC, 0, CURVED, true, false, REC><<<grid, C::THREADS, sm, s>>>(a);
-    }
-    static void te_volume(cudaStream_t s, const VolArgs& a, int grid, bool sc, bool attr_only) {
-        if constexpr (N >= 3) {
-            const bool curved = attr_only || a.metrics;
-            const int rec = a.reconstruction;
-            if (curved && (attr_only || !sc)) te_launch<false, true, 0>(s, a, grid, attr_only);
-            if (curved && (attr_only || (sc && rec == TLW_RECONSTRUCTION_FIRST_ORDER))) te_launch<true, true, 0>(s, a, grid, attr_only);
-            if (curved && (attr_only || (sc && rec == TLW_RECONSTRUCTION_MUSCL))) te_launch<true, true, 1>(s, a, grid, attr_only);
-            if (curved && (attr_only || (sc && rec == TLW_RECONSTRUCTION_MUSCL_HANCOCK))) te_launch<true, true, 2>(s, a, grid, attr_only);
-            if constexpr (N >= 4) {
-                const bool tree = attr_only || !a.metrics;
-                if (tree && (attr_only || !sc)) te_launch<false, false, 0>(s, a, grid, attr_only);
-                if (tree && (attr_only || sc)) te_launch<true, false, 0>(s, a, grid, attr_only);
-            }
-        }
-    }
-    static void volume(cudaStream_t s, int stage, int mode, bool sc, const VolArgs& a) {
-        const int grid = (int)((a.E + C::EB - 1) / C::EB);
-        if (grid == 0) return;
-        if (a.temporal_errors) {
-            te_volume(s, a, grid, sc, false);
-            return;
-        }
-        if (a.metrics && sc) {   // curvilinear mesh with shock capturing (MUSCL when the geometry is given)
-            if (a.reconstruction == TLW_RECONSTRUCTION_MUSCL_HANCOCK) curved_sc<2>(s, stage, mode, a, grid);
-            else if (a.reconstruction == TLW_RECONSTRUCTION_MUSCL) curved_sc<1>(s, stage, mode, a, grid);
-            else curved_sc<0>(s, stage, mode, a, grid);
-            return;
-        }
-        if (a.metrics) {   // curvilinear mesh (LW or MDRK, FR volume integral)
-            const size_t md = C::smem_bytes(2);
-            if (stage == TLW_STAGE_MDRK1) {
-                if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS, false, true><<<grid, C::THREADS, md, s>>>(a);
-                else mdrk1_volume_kernel<N, MODE_STEP, false, true><<<grid, C::THREADS, md, s>>>(a);
-            } else if (stage == TLW_STAGE_MDRK2) {
-                if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS, false, true><<<grid, C::THREADS, md, s>>>(a);
-                else mdrk2_volume_kernel<N, MODE_STEP, false, true><<<grid, C::THREADS, md, s>>>(a);
-            } else if (mode == MODE_RHS) {
-                lw_volume_kernel<N, MODE_RHS, false, 0, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
-            } else {
-                lw_volume_kernel<N, MODE_STEP, false, 0, true><<<grid, C::THREADS, C::smem_bytes(4), s>>>(a);
-            }
-            return;
-        }
-        if (sc) volume_sc<true>(s, stage, mode, a, grid);
-        else volume_sc<false>(s, stage, mode, a, grid);
-    }
-    static void interfaces(cudaStream_t s, const SurfArgs& a) {
-        const long long threads = (long long)a.count * (N + 1);
-        if (threads == 0) return;
-        interface_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
-    }
-    static void parabolic(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out,
-                          const double* dtp) {
-        if constexpr (N >= 3) {
-            const int E = (int)h->E;
-            using P = ParCfg<N>;
-            const int grid = (E + P::EB - 1) / P::EB;
-            const double iwf = h->h_basis.inv_w_first, iwl = h->h_basis.inv_w_last;
-            if (h->curved) {
-                grad_volume_kernel<N, true><<<grid, P::THREADS, 0, s>>>(u, h->d_ijn, E, h->d_gx, h->d_gy, h->d_Ja);
-                for (size_t c = 0; c + 1 < h->color_off.size(); ++c) {
-                    const int b = h->color_off[c], cnt = h->color_off[c + 1] - b;
-                    const long long th = (long long)cnt * (N + 1);
-                    if (th)
-                        curved_grad_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(
-                            u, h->d_cp + b, h->d_cs + b, h->d_cf + b, cnt, h->d_Ja, h->d_ijn, iwf, iwl, h->d_gx,
-                            h->d_gy);
-                }
-                // xi-face boundaries, then eta-face ones (they share corner nodes)
-                const int first[2] = {0, h->ncbx}, count[2] = {h->ncbx, h->ncb - h->ncbx};
-                for (int cls = 0; cls < 2; ++cls) {
-                    const long long tb = (long long)count[cls] * (N + 1);
-                    if (tb)
-                        curved_grad_boundary_kernel<N><<<(unsigned)((tb + 127) / 128), 128, 0, s>>>(
-                            u, h->d_cbe + first[cls], h->d_cbf + first[cls], h->d_cbi + first[cls], count[cls],
-                            h->d_wkind, h->d_wall, h->d_Ja, h->d_ijn, h->opts.gamma, iwf, iwl, h->d_gx, h->d_gy);
-                }
-            } else {
-                grad_volume_kernel<N><<<grid, P::THREADS, 0, s>>>(u, h->d_inv_jac, E, h->d_gx, h->d_gy);
-                const long long th = (long long)(h->nx + h->ny) * (N + 1);
-                if (th)
-                    grad_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(
-                        u, h->d_xl, h->d_xr, h->nx, h->d_yl, h->d_yr, h->ny, h->d_inv_jac, iwf, iwl, h->d_gx,
-                        h->d_gy);
-                const long long tb = (long long)h->nb * (N + 1);
-                if (tb)
-                    grad_boundary_kernel<N><<<(unsigned)((tb + 127) / 128), 128, 0, s>>>(
-                        u, h->d_b_elem, h->d_b_dir, h->d_wkind, h->d_wall, (int)h->nb, h->d_inv_jac, h->opts.gamma,
-                        iwf, iwl, h->d_gx, h->d_gy);
-            }
-            ParArgs pa{};
-            pa.u = u;
-            pa.gx = h->d_gx;
-            pa.gy = h->d_gy;
-            pa.out = out;
-            pa.tU = h->d_tU;
-            pa.tF = h->d_tF;
-            pa.tFv = h->d_tFv;
-            pa.inv_jac = h->d_inv_jac;
-            pa.dt = dtp;
-            pa.E = E;
-            pa.ns = ns_params(h);
-            if (h->curved) {
-                pa.inv_jac = h->d_ijn;
-                pa.metrics = h->d_Ja;
-                if (mode == MODE_RHS) par_volume_kernel<N, MODE_RHS, true><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
-                else par_volume_kernel<N, MODE_STEP, true><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
-            } else {
-                if (mode == MODE_RHS) par_volume_kernel<N, MODE_RHS><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
-                else par_volume_kernel<N, MODE_STEP><<<grid, P::THREADS, P::smem_bytes(), s>>>(pa);
-            }
-        }
-    }
-    static void par_speed(cudaStream_t s, const tlw_handle* h, const double* u) {
-        if constexpr (N >= 3) {
-            const int E = (int)h->E;
-            const int grid = (E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS;
-            if (h->curved) {
-                // the CFL maximum of the curvilinear max_dt, then the parabolic max_dt's own maxima
-                curved_max_speed_kernel<N><<<grid, MS_THREADS, 0, s>>>(u, h->d_Ja, h->d_ijn, E, h->opts.gamma,
-                                                                        h->d_step);
-                par_speed_kernel<N><<<grid, MS_THREADS, 0, s>>>(u, h->d_ijn, E, ns_params(h), h->d_step, h->d_visc,
-                                                                 h->d_visc + 1);
-            } else {
-                par_speed_kernel<N><<<grid, MS_THREADS, 0, s>>>(u, h->d_inv_jac, E, ns_params(h), h->d_step,
-                                                                 h->d_visc, &h->d_step->max_bits);
-            }
-        }
-    }
-    static void par_attributes() {
-        if constexpr (N >= 3) {
-            cudaFuncSetAttribute(par_volume_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ParCfg<N>::smem_bytes());
-            cudaFuncSetAttribute(par_volume_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ParCfg<N>::smem_bytes());
-            cudaFuncSetAttribute(par_volume_kernel<N, MODE_RHS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ParCfg<N>::smem_bytes());
-            cudaFuncSetAttribute(par_volume_kernel<N, MODE_STEP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)ParCfg<N>::smem_bytes());
-        }
-    }
-    static void mortars(cudaStream_t s, const MortarArgs& a) {
-        if (a.count == 0) return;
-        using M = MortarCfg<N>;
-        mortar_kernel<N><<<(a.count + M::PER_CTA - 1) / M::PER_CTA, M::THREADS, 0, s>>>(a);
-    }
-    static void curved_interfaces(cudaStream_t s, const CurvedSurfArgs& a) {
-        const long long threads = (long long)a.count * (N + 1);
-        if (threads == 0) return;
-        curved_interface_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
-    }
-    static void curved_speed(cudaStream_t s, const double* u, const double* Ja, const double* ij, int E, double g,
-                             StepState* st) {
-        if (E == 0) return;
-        curved_max_speed_kernel<N><<<(E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS, MS_THREADS, 0, s>>>(u, Ja, ij, E, g, st);
-    }
-    static void boundaries(cudaStream_t s, const BndArgs& a) {
-        const long long threads = (long long)a.count * (N + 1);
-        if (threads == 0) return;
-        boundary_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
-    }
-    // speed: CFL reduction; ind: Hennemann-Gassner indicator (both read u once)
-    static void max_speed(cudaStream_t s, const double* u, const double* ij, int E, double gamma, StepState* st,
-                          bool speed, bool ind, const IndicatorArgs& ia, BatchSpeedArgs bs = BatchSpeedArgs{}) {
-        if (E == 0) return;
-        const int grid = (E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS;
-        if (speed && ind) max_speed_kernel<N, true, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
-        else if (speed) max_speed_kernel<N, true, false><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
-        else if (ind) max_speed_kernel<N, false, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
-    }
-};
-
-template <int N> struct Lim {
-    static void run(cudaStream_t s, const LimiterArgs& a) {
-        if (a.E == 0) return;
-        positivity_limiter_kernel<N><<<(a.E + LIMITER_WARPS - 1) / LIMITER_WARPS, 32 * LIMITER_WARPS, 0, s>>>(a);
-    }
-};
 
 template <template <int> class F, class... A>
 void dispatch(int N, A&&... args) {
@@ -395,29 +127,12 @@ template <int N> struct Par {
 template <int N> struct ParSpd { static void run(cudaStream_t s, const tlw_handle* h, const double* u) { Launch<N>::par_speed(s, h, u); } };
 template <int N> struct ParAttr { static void run() { Launch<N>::par_attributes(); } };
 template <int N> struct Mrt { static void run(cudaStream_t s, const MortarArgs& a) { Launch<N>::mortars(s, a); } };
-template <int N> struct CMrt {
-    static void run(cudaStream_t s, const CurvedMortarArgs& a) {
-        if (a.count == 0) return;
-        using M = MortarCfg<N>;
-        curved_mortar_kernel<N><<<(a.count + M::PER_CTA - 1) / M::PER_CTA, M::THREADS, 0, s>>>(a);
-    }
-};
+template <int N> struct CMrt { static void run(cudaStream_t s, const CurvedMortarArgs& a) { Launch<N>::curved_mortars(s, a); } };
 template <int N> struct CIfc { static void run(cudaStream_t s, const CurvedSurfArgs& a) { Launch<N>::curved_interfaces(s, a); } };
-template <int N> struct Halo {
-    static void run(cudaStream_t s, const HaloArgs& a, bool pack) {
-        const long long threads = (long long)a.count * (N + 1);
-        if (threads == 0) return;
-        if (pack) halo_pack_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
-        else halo_face_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
-    }
-};
-template <int N> struct CBnd {
-    static void run(cudaStream_t s, const CurvedBndArgs& a) {
-        const long long threads = (long long)a.count * (N + 1);
-        if (threads == 0) return;
-        curved_boundary_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
-    }
-};
+template <int N> struct Halo { static void run(cudaStream_t s, const HaloArgs& a, bool pack) { Launch<N>::halo(s, a, pack); } };
+template <int N> struct CBnd { static void run(cudaStream_t s, const CurvedBndArgs& a) { Launch<N>::curved_boundaries(s, a); } };
+template <int N> struct Lim { static void run(cudaStream_t s, const LimiterArgs& a) { Launch<N>::limiter(s, a); } };
+template <int N> struct Const { static void run(const Basis* all, cudaError_t* e) { if (*e == cudaSuccess) *e = Launch<N>::upload_constants(all); } };
 template <int N> struct CSpd {
     static void run(cudaStream_t s, const double* u, const double* Ja, const double* ij, int E, double g, StepState* st) {
         Launch<N>::curved_speed(s, u, Ja, ij, E, g, st);
@@ -854,6 +569,11 @@ __global__ void fp64_probe_kernel(double* out, int iters, double a, double b) {
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+__global__ void reciprocal_probe_kernel(const double* __restrict__ x, double* __restrict__ y, long long n) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        y[k] = nr_reciprocal(x[k]);
+}
+
 int check_ready(tlw_handle* h) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
@@ -870,7 +590,7 @@ int read_status(tlw_handle* h) {
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));
     if (st) {
         const unsigned zero = 0;
-        TLW_CUDA(h, cudaMemcpy(&h->d_step->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+        TLW_CUDA(h, upload_on(h->stream, &h->d_step->status, &zero, sizeof(zero)));
         return fail(h, TLW_E_NONADMISSIBLE, "non-admissible state: square root of a negative number (DomainError)");
     }
     return TLW_OK;
@@ -913,16 +633,18 @@ int tlw_create(const tlw_opts* opts, tlw_handle** out) {
         if (cudaSetDevice(h->device) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "cudaSetDevice failed"); break; }
         if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "stream"); break; }
         if (cudaMalloc(&h->d_basis, sizeof(tlw::Basis)) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "alloc basis"); break; }
-        if (cudaMemcpy(h->d_basis, &h->h_basis, sizeof(tlw::Basis), cudaMemcpyHostToDevice) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "copy basis"); break; }
+        if (upload_on(h->stream, h->d_basis, &h->h_basis, sizeof(tlw::Basis)) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "copy basis"); break; }
         if (cudaMalloc(&h->d_step, sizeof(StepState)) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "alloc step"); break; }
         StepState st{};
         st.cfl = 1.0;
         st.t_end = INFINITY;
-        if (cudaMemcpy(h->d_step, &st, sizeof(st), cudaMemcpyHostToDevice) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "init step"); break; }
+        if (upload_on(h->stream, h->d_step, &st, sizeof(st)) != cudaSuccess) { rc = fail(h, TLW_E_CUDA, "init step"); break; }
         tlw::Basis all[8];
         std::memset(&all[0], 0, sizeof(all[0]));
         for (int N = 1; N <= 7; ++N) host_build_basis(N, all[N]);
-        if (upload_const_basis(all) != cudaSuccess || upload_const_mortar() != cudaSuccess) {
+        cudaError_t ce = cudaSuccess;
+        for (int k = 1; k <= 7; ++k) dispatch<Const>(k, (const Basis*)all, &ce);   // each degree's launch unit
+        if (ce != cudaSuccess || upload_const_basis(all) != cudaSuccess || upload_const_mortar() != cudaSuccess) {
             rc = fail(h, TLW_E_CUDA, "constant basis");
             break;
         }
@@ -998,12 +720,12 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
     auto up_i = [&](int*& d, const std::vector<int>& v) -> int {
         if (v.empty()) return TLW_OK;
         TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
-        TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+        TLW_CUDA(h, upload_on(h->stream, d, v.data(), v.size() * sizeof(int)));
         return TLW_OK;
     };
     int rc;
     TLW_CUDA(h, cudaMalloc(&h->d_inv_jac, n_elements * sizeof(double)));
-    TLW_CUDA(h, cudaMemcpy(h->d_inv_jac, inverse_jacobian, n_elements * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, upload_on(h->stream, h->d_inv_jac, inverse_jacobian, n_elements * sizeof(double)));
     if ((rc = up_i(h->d_xl, xl)) || (rc = up_i(h->d_xr, xr)) || (rc = up_i(h->d_yl, yl)) || (rc = up_i(h->d_yr, yr)) ||
         (rc = up_i(h->d_b_elem, belem)) || (rc = up_i(h->d_b_dir, bdir)) || (rc = up_i(h->d_bx, bx)) ||
         (rc = up_i(h->d_by, by)))
@@ -1089,11 +811,11 @@ int upload_curved_subcells(tlw_handle* h, const double* Ja) {
         (rc = ensure(h, h->d_mgeom, geom.size())) || (rc = ensure(h, h->d_alpha, (size_t)E)) ||
         (rc = ensure(h, h->d_alpha_raw, (size_t)E)) || (rc = ensure(h, h->d_tFn, trace_doubles(h))))
         return rc;
-    TLW_CUDA(h, cudaMemcpy(h->d_subn, subn.data(), subn.size() * sizeof(double), cudaMemcpyHostToDevice));
-    TLW_CUDA(h, cudaMemcpy(h->d_subq, subq.data(), subq.size() * sizeof(double), cudaMemcpyHostToDevice));
-    TLW_CUDA(h, cudaMemcpy(h->d_mgeom, geom.data(), geom.size() * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, upload_on(h->stream, h->d_subn, subn.data(), subn.size() * sizeof(double)));
+    TLW_CUDA(h, upload_on(h->stream, h->d_subq, subq.data(), subq.size() * sizeof(double)));
+    TLW_CUDA(h, upload_on(h->stream, h->d_mgeom, geom.data(), geom.size() * sizeof(double)));
     TLW_CUDA(h, cudaMalloc(&h->d_atb, (size_t)E));
-    TLW_CUDA(h, cudaMemset(h->d_atb, 0, (size_t)E));
+    TLW_CUDA(h, zero_on(h->stream, h->d_atb, (size_t)E));
     return TLW_OK;
 }
 
@@ -1181,14 +903,14 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
     auto up_i = [&](int*& d, const std::vector<int>& v) -> int {
         if (v.empty()) return TLW_OK;
         TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
-        TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+        TLW_CUDA(h, upload_on(h->stream, d, v.data(), v.size() * sizeof(int)));
         return TLW_OK;
     };
     int rc;
     TLW_CUDA(h, cudaMalloc(&h->d_Ja, nodes * 4 * sizeof(double)));
-    TLW_CUDA(h, cudaMemcpy(h->d_Ja, contravariant_vectors, nodes * 4 * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, upload_on(h->stream, h->d_Ja, contravariant_vectors, nodes * 4 * sizeof(double)));
     TLW_CUDA(h, cudaMalloc(&h->d_ijn, nodes * sizeof(double)));
-    TLW_CUDA(h, cudaMemcpy(h->d_ijn, inverse_jacobian, nodes * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, upload_on(h->stream, h->d_ijn, inverse_jacobian, nodes * sizeof(double)));
     if ((rc = up_i(h->d_cp, cp)) || (rc = up_i(h->d_cs, cs)) || (rc = up_i(h->d_cf, cf))) return rc;
     h->color_off = off;
     h->face_used.assign((size_t)n_elements * 4, 0);
@@ -1246,7 +968,7 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
             std::vector<int> v(a);
             v.insert(v.end(), b.begin(), b.end());
             TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
-            TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+            TLW_CUDA(h, upload_on(h->stream, d, v.data(), v.size() * sizeof(int)));
             return TLW_OK;
         };
         int rc;
@@ -1260,8 +982,8 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
         // interface pairs, then (lower, large) and (upper, large) of every mortar
         std::vector<int> l(h->ni_if), r(h->ni_if);
         if (h->ni_if > 0) {
-            TLW_CUDA(h, cudaMemcpy(l.data(), h->d_il, h->ni_if * sizeof(int), cudaMemcpyDeviceToHost));
-            TLW_CUDA(h, cudaMemcpy(r.data(), h->d_ir, h->ni_if * sizeof(int), cudaMemcpyDeviceToHost));
+            TLW_CUDA(h, download_on(h->stream, l.data(), h->d_il, h->ni_if * sizeof(int)));
+            TLW_CUDA(h, download_on(h->stream, r.data(), h->d_ir, h->ni_if * sizeof(int)));
         }
         for (int d = 0; d < 2; ++d)
             for (size_t k = 0; k < ml[d].size(); ++k) {
@@ -1272,8 +994,8 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
         if (!l.empty()) {
             TLW_CUDA(h, cudaMalloc(&h->d_il, l.size() * sizeof(int)));
             TLW_CUDA(h, cudaMalloc(&h->d_ir, r.size() * sizeof(int)));
-            TLW_CUDA(h, cudaMemcpy(h->d_il, l.data(), l.size() * sizeof(int), cudaMemcpyHostToDevice));
-            TLW_CUDA(h, cudaMemcpy(h->d_ir, r.data(), r.size() * sizeof(int), cudaMemcpyHostToDevice));
+            TLW_CUDA(h, upload_on(h->stream, h->d_il, l.data(), l.size() * sizeof(int)));
+            TLW_CUDA(h, upload_on(h->stream, h->d_ir, r.data(), r.size() * sizeof(int)));
         }
         h->ni = (int)l.size();
     }
@@ -1311,7 +1033,7 @@ int tlw_set_halo(tlw_handle* h, int64_t n_halo, const int64_t* elements, const i
             std::vector<int> v(a);
             v.insert(v.end(), b.begin(), b.end());
             TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
-            TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+            TLW_CUDA(h, upload_on(h->stream, d, v.data(), v.size() * sizeof(int)));
             return TLW_OK;
         };
         int rc;
@@ -1320,8 +1042,8 @@ int tlw_set_halo(tlw_handle* h, int64_t n_halo, const int64_t* elements, const i
         const size_t nd = (size_t)n_halo * h->n * HALO_VALUES;
         TLW_CUDA(h, cudaMalloc(&h->d_send, nd * sizeof(double)));
         TLW_CUDA(h, cudaMalloc(&h->d_recv, nd * sizeof(double)));
-        TLW_CUDA(h, cudaMemset(h->d_send, 0, nd * sizeof(double)));
-        TLW_CUDA(h, cudaMemset(h->d_recv, 0, nd * sizeof(double)));
+        TLW_CUDA(h, zero_on(h->stream, h->d_send, nd * sizeof(double)));
+        TLW_CUDA(h, zero_on(h->stream, h->d_recv, nd * sizeof(double)));
     }
     return TLW_OK;
 }
@@ -1431,7 +1153,7 @@ int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* smal
     auto up = [&](int*& d, const std::vector<int>& v) -> int {
         if (v.empty()) return TLW_OK;
         TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
-        TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+        TLW_CUDA(h, upload_on(h->stream, d, v.data(), v.size() * sizeof(int)));
         return TLW_OK;
     };
     int rc;
@@ -1458,7 +1180,7 @@ int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* smal
     h->ncms = (int)sl.size();
     if (n_mortars > 0) {
         TLW_CUDA(h, cudaMalloc(&h->d_cmj, (size_t)n_mortars * h->n * sizeof(double)));
-        TLW_CUDA(h, cudaMemset(h->d_cmj, 0, (size_t)n_mortars * h->n * sizeof(double)));
+        TLW_CUDA(h, zero_on(h->stream, h->d_cmj, (size_t)n_mortars * h->n * sizeof(double)));
     }
     h->mortar_order = order;
     h->ncm = (int)n_mortars;
@@ -1477,7 +1199,7 @@ int tlw_set_curved_mortar_jacobian(tlw_handle* h, const double* inverse_jacobian
             for (int l = 0; l < h->n; ++l) v[c * h->n + l] = inverse_jacobian[(size_t)h->mortar_order[c] * h->n + l];
     TLW_CUDA(h, cudaSetDevice(h->device));
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));
-    TLW_CUDA(h, cudaMemcpy(h->d_cmj, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, upload_on(h->stream, h->d_cmj, v.data(), v.size() * sizeof(double)));
     return TLW_OK;
 }
 
@@ -1522,7 +1244,7 @@ int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t
             std::vector<int> v(a);
             v.insert(v.end(), b.begin(), b.end());
             TLW_CUDA(h, cudaMalloc(&d, v.size() * sizeof(int)));
-            TLW_CUDA(h, cudaMemcpy(d, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice));
+            TLW_CUDA(h, upload_on(h->stream, d, v.data(), v.size() * sizeof(int)));
             return TLW_OK;
         };
         int rc;
@@ -1534,7 +1256,7 @@ int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t
         // shock capturing: calcflux_muscl! falls back to first-order subcells on elements with a boundary face
         std::vector<unsigned char> atb((size_t)h->E, 0);
         for (int64_t k = 0; k < n_boundaries; ++k) atb[(size_t)(elements[k] - 1)] = 1;
-        TLW_CUDA(h, cudaMemcpy(h->d_atb, atb.data(), atb.size(), cudaMemcpyHostToDevice));
+        TLW_CUDA(h, upload_on(h->stream, h->d_atb, atb.data(), atb.size()));
     }
     return TLW_OK;
 }
@@ -1554,7 +1276,7 @@ int tlw_set_boundary_kinds(tlw_handle* h, const int32_t* kinds) {
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));
     drop_graphs(h);
     if (!h->d_bkind) TLW_CUDA(h, cudaMalloc(&h->d_bkind, (size_t)h->nb * sizeof(int)));
-    TLW_CUDA(h, cudaMemcpy(h->d_bkind, kinds, (size_t)h->nb * sizeof(int), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, upload_on(h->stream, h->d_bkind, kinds, (size_t)h->nb * sizeof(int)));
     h->bnd_dirichlet = dirichlet;
     return TLW_OK;
 }
@@ -1576,8 +1298,8 @@ int tlw_set_parabolic_walls(tlw_handle* h, const int32_t* kinds, const double* w
     drop_graphs(h);
     if (!h->d_wkind) TLW_CUDA(h, cudaMalloc(&h->d_wkind, (size_t)nbnd * sizeof(int)));
     if (!h->d_wall) TLW_CUDA(h, cudaMalloc(&h->d_wall, nd * sizeof(double)));
-    TLW_CUDA(h, cudaMemcpy(h->d_wkind, kinds, (size_t)nbnd * sizeof(int), cudaMemcpyHostToDevice));
-    TLW_CUDA(h, cudaMemcpy(h->d_wall, wall_data, nd * sizeof(double), cudaMemcpyHostToDevice));
+    TLW_CUDA(h, upload_on(h->stream, h->d_wkind, kinds, (size_t)nbnd * sizeof(int)));
+    TLW_CUDA(h, upload_on(h->stream, h->d_wall, wall_data, nd * sizeof(double)));
     return TLW_OK;
 }
 
@@ -1624,7 +1346,7 @@ int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl) {
         return rc;
     if (!h->d_visc) {
         TLW_CUDA(h, cudaMalloc(&h->d_visc, 2 * sizeof(unsigned long long)));
-        TLW_CUDA(h, cudaMemset(h->d_visc, 0, 2 * sizeof(unsigned long long)));
+        TLW_CUDA(h, zero_on(h->stream, h->d_visc, 2 * sizeof(unsigned long long)));
     }
     dispatch<ParAttr>(h->N);
     TLW_CUDA(h, cudaGetLastError());
@@ -1668,7 +1390,7 @@ static int adaptive_supported(tlw_handle* h) {
         TLW_CUDA(h, cudaMalloc(&h->d_te, (size_t)h->E * sizeof(double)));
         TLW_CUDA(h, cudaMalloc(&h->d_check, (size_t)(4 * 148 + 1) * sizeof(double)));
         TLW_CUDA(h, cudaMalloc(&h->d_bad, sizeof(unsigned)));
-        TLW_CUDA(h, cudaMemset(h->d_bad, 0, sizeof(unsigned)));
+        TLW_CUDA(h, zero_on(h->stream, h->d_bad, sizeof(unsigned)));
     }
     return TLW_OK;
 }
@@ -1691,8 +1413,9 @@ int tlw_adaptive_begin(tlw_handle* h, double t_end, double dt_initial, const dou
     a.dt = st.t + dt_initial > t_end ? t_end - st.t : dt_initial;   // set_dt!
     a.k = (double)h->n;
     a.ndofs = (double)h->nn * (double)h->E;
-    TLW_CUDA(h, cudaMemcpy(h->d_adapt, &a, sizeof(a), cudaMemcpyHostToDevice));
-    TLW_CUDA(h, cudaMemset(h->d_bad, 0, sizeof(unsigned)));
+    TLW_CUDA(h, upload_on(h->stream, h->d_adapt, &a, sizeof(a)));
+    TLW_CUDA(h, zero_on(h->stream, h->d_bad, sizeof(unsigned)));
+    TLW_CUDA(h, zero_on(h->stream, &h->d_step->status, sizeof(unsigned)));   // no stale flag rejects trial 1
     return TLW_OK;
 }
 
@@ -1725,6 +1448,9 @@ int tlw_adaptive_run(tlw_handle* h, int32_t n_trials, double abstol, double relt
     *steps = st.steps;
     *rejected = a.nreject;
     *finished = adaptive_finished_host(st.t, a.t_end) ? 1 : 0;
+    if (a.stalled && !*finished)
+        return fail(h, TLW_E_NONADMISSIBLE, "Adaptive: dt fell below 1e-14 |t| after repeated rejections "
+                                            "(persistently non-admissible state)");
     return TLW_OK;
 }
 
@@ -1745,7 +1471,7 @@ int tlw_adaptive_trial(tlw_handle* h, double dt, double abstol, double reltol, d
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));
     if (st) {   // a square root of a negative number: the reference's test_rhs! catches the DomainError
         const unsigned zero = 0;
-        TLW_CUDA(h, cudaMemcpy(&h->d_step->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+        TLW_CUDA(h, upload_on(h->stream, &h->d_step->status, &zero, sizeof(zero)));
     }
     *admissible = (bad == 0 && st == 0) ? 1 : 0;
     *total_temporal_error = std::sqrt(sum / ((double)h->nn * (double)h->E));
@@ -2047,6 +1773,22 @@ int tlw_probe_fp64_tflops(int32_t device, double* tflops) {
     if (err != cudaSuccess) return TLW_E_CUDA;
     *tflops = 2.0 * 16.0 * iters * (double)threads * blocks / (best * 1e-3) / 1e12;
     return TLW_OK;
+}
+
+int tlw_probe_reciprocal(int32_t device, const double* x, double* y, int64_t n) {
+    if (!x || !y || n < 0) return TLW_E_ARG;
+    if (n == 0) return TLW_OK;
+    if (cudaSetDevice(device) != cudaSuccess) return TLW_E_CUDA;
+    double* d = nullptr;
+    if (cudaMalloc(&d, 2 * (size_t)n * sizeof(double)) != cudaSuccess) return TLW_E_CUDA;
+    cudaError_t e = cudaMemcpy(d, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        reciprocal_probe_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4 * 148), 256>>>(d, d + n, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(y, d + n, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? TLW_OK : TLW_E_CUDA;
 }
 
 int tlw_get_time(tlw_handle* h, double* t, double* dt_last, int64_t* steps) {

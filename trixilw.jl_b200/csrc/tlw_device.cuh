@@ -166,6 +166,22 @@ __device__ __forceinline__ void lw_surface_flux(double gamma, int flux_kind, int
     }
 }
 
+// Set-up copies ordered on a library stream and complete on return. A plain cudaMemcpy / cudaMemset runs on
+// the legacy default stream, which the library's non-blocking streams do not wait for, and a pageable
+// host-to-device cudaMemcpy may return before its DMA has landed.
+inline cudaError_t upload_on(cudaStream_t s, void* dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+    return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+inline cudaError_t download_on(cudaStream_t s, void* dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+    return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+inline cudaError_t zero_on(cudaStream_t s, void* dst, size_t bytes) {
+    cudaError_t e = cudaMemsetAsync(dst, 0, bytes, s);
+    return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+
 __device__ __forceinline__ void load4(const double* __restrict__ p, double* x) {
     const double2 a = __ldg(reinterpret_cast<const double2*>(p));
     const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);

@@ -16,8 +16,10 @@
 //  * size limit: n_elements * 2 * 4 * (N+1) * 4 * 8 bytes must fit the scratch array (32 MiB: 26214
 //    elements at N=4); larger meshes are rejected with TLW_E_ARG;
 //  * every GPU that loads the library holds the array until the process exits;
-//  * all calls on a device share the array, which keeps the last call's contents: calls that overlap on
-//    the GPU (different streams or host threads at once) race and must be serialised by the caller;
+//  * all calls on a device share the array and the dt and status words, which keep the last call's
+//    contents: calls that overlap on the GPU (different streams or host threads at once) race and must be
+//    serialised by the caller;
+//  * each call waits for its stream before it returns;
 //  * the first call on each device sets up that device (symbol addresses, basis, kernel attributes)
 //    with the device current; make that first call before any stream capture.
 #include <cuda_runtime.h>

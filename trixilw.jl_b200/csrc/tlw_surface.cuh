@@ -544,7 +544,10 @@ static __global__ void adaptive_accept_kernel(StepState* s, double dt) {
 // (:47-61; shifted only on the first try of a step, a non-finite error keeps the previous estimate),
 // dt_factor (:100-105) with the controller (beta1, beta2, beta3) of lwfr.jl:162, rejection when the trial is
 // not admissible or factor <= 0.81 (retry at min(factor, 0.95) dt), acceptance otherwise (next dt
-// min(factor, 1.5) dt), both clamped by set_dt! to end at t_end.
+// min(factor, 1.5) dt), both clamped by set_dt! to end at t_end. The reference retries without a limit; here a
+// run whose next dt falls to ADAPTIVE_DT_FLOOR |t| or below (t + dt no longer moves t) stops as stalled, and the
+// host reports it as a non-admissible state instead of enqueuing trials for ever.
+constexpr double ADAPTIVE_DT_FLOOR = 1e-14;
 struct AdaptiveState {
     double eps[3];          // epsilon[-1], epsilon[0], epsilon[1]
     double beta[3];
@@ -556,6 +559,7 @@ struct AdaptiveState {
     long long n_fail, nreject, trials;
     int accept;             // the last trial was accepted
     int finished;
+    int stalled;            // dt fell to the floor after repeated rejections: no further trials
 };
 
 __device__ __forceinline__ bool adaptive_finished(double t, double te) {
@@ -564,7 +568,7 @@ __device__ __forceinline__ bool adaptive_finished(double t, double te) {
 }
 
 static __global__ void adaptive_prepare_kernel(StepState* s, AdaptiveState* a) {
-    a->finished = adaptive_finished(s->t, a->t_end) ? 1 : 0;
+    a->finished = (a->stalled || adaptive_finished(s->t, a->t_end)) ? 1 : 0;
     s->dt_call = a->finished ? 0.0 : a->dt;
 }
 
@@ -599,6 +603,8 @@ static __global__ void adaptive_judge_kernel(StepState* s, AdaptiveState* a, con
         nd = fmin(factor, 0.95) * a->dt;
     }
     a->dt = s->t + nd > a->t_end ? a->t_end - s->t : nd;
+    if (!(a->dt > ADAPTIVE_DT_FLOOR * fmax(fabs(s->t), fabs(a->t_end))) && !adaptive_finished(s->t, a->t_end))
+        a->stalled = 1;
 }
 
 // an accepted trial becomes the current state

@@ -15,7 +15,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import check, lib
+from ._lib import DomainError, check, lib
 from .basis import gauss_lobatto
 from .limiters import install as install_limiters
 from .semidiscretization import Adaptive, CFLBased, LWUpdate, SemidiscretizationHyperbolic, _ptr
@@ -147,6 +147,10 @@ def dt_factor(epsilon: dict, k: int, controller=CONTROLLER) -> float:
     return 1.0 + math.atan(f - 1.0)
 
 
+# next dt relative to |t| at or below which a run of rejections stops (the device controller has the same)
+ADAPTIVE_DT_FLOOR = 1e-14
+
+
 class AdaptiveController:
     """The step-size logic of perform_step!(..., ::Adaptive, ::LW) (src/solvers/adaptive.jl:101-172), apart
     from the trial step itself: ``propose`` gives the dt to try, ``judge`` takes the trial's total temporal
@@ -183,6 +187,9 @@ class AdaptiveController:
             return True
         self.n_fail += 1
         self.dt = self._clamp(min(self.factor, 0.95) * self.dt)
+        if not self.dt > ADAPTIVE_DT_FLOOR * max(abs(self.t), abs(self.t_end)) and not self.finished():
+            # the reference retries for ever; stop once dt no longer moves t (the device controller's floor)
+            raise DomainError(f"Adaptive: dt fell to {self.dt:.3e} at t = {self.t} after {self.n_fail} rejections")
         return False
 
     def finished(self) -> bool:
