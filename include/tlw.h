@@ -286,6 +286,18 @@ int tlw_get_state(tlw_handle* h, double* u, int32_t where, double* t_out);
  * fixed_dt when > 0), clamped to t_end, u <- u + dt * rhs(u). dt never leaves the device. The steps are
  * replayed from a captured CUDA graph when use_graph != 0. Asynchronous. */
 int tlw_step(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double t_end, int32_t use_graph);
+/* Host-buffer stepping: uploads the state u_in (host, [v, i, j, element]) at time t, runs nsteps steps as
+ * tlw_step does (without graphs) and downloads the result into u_out (host). Asynchronous: it returns after
+ * enqueueing, and the caller keeps u_in and u_out untouched until tlw_synchronize (or until a later call that
+ * waits on them returns). Consecutive calls overlap: the upload of the next call and the download of the
+ * previous one run on copy streams of their own beside the steps, so a stream of independent states (an
+ * ensemble, or requests served one after another) moves through the GPU at the host link's bandwidth. With
+ * pinned (page-locked) host buffers the copies run asynchronously; pageable ones make the copies wait. A u_in
+ * equal to the previous call's u_out (the state round-tripping through the host) is read after that download. The
+ * handle's current state afterwards is the last call's result. (No counterpart in the reference, whose
+ * solution vectors stay in host memory; this is the host-side path of the drop-in at full link speed.) */
+int tlw_step_host(tlw_handle* h, const double* u_in, double* u_out, double t, int32_t nsteps, double cfl,
+                  double fixed_dt, double t_end);
 /* As tlw_step without graphs, with CUDA events between the phases of each step. Synchronous. On return
  * phase_ms[0..4] hold the summed device time of: CFL reduction (max speed + dt), volume kernel(s),
  * x interfaces + x boundaries, y interfaces + y boundaries, and the whole steps. (Measurement entry: no

@@ -1,0 +1,79 @@
+"""tlw_step_host: asynchronous host-buffer stepping with the copies of consecutive calls overlapped. Every
+call's result equals the plain path's (upload, the same steps, download), whether the calls carry
+independent states or feed each result back in, and the handle's state afterwards is the last result."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def make(tl, level=5, N=4, strength=5.0):
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), level)
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.LW()))
+    semi = tl.SemidiscretizationHyperbolic(mesh, tl.LW(), eq, tl.IsentropicVortex(strength), solver)
+    return semi, tl.LWIntegrator(tl.semidiscretize(semi, tl.LW(), (0.0, 1e9)))
+
+
+def plain(integ, u, t, nsteps, cfl):
+    integ.set_state(u, t)
+    integ.step(nsteps, cfl, use_graph=False)
+    return integ.get_state()
+
+
+def test_step_host_independent_states_match_the_plain_path(tl):
+    semi, integ = make(tl)
+    cfl = 0.5
+    states = []
+    for k, beta in enumerate((5.0, 3.0, 4.0, 2.0, 4.5)):
+        s, _ = make(tl, strength=beta)
+        states.append(s.compute_coefficients(0.0))
+    ins = [integ.pinned_state() for _ in states]
+    outs = [integ.pinned_state() for _ in states]
+    for a, u in zip(ins, states):
+        a[:] = u
+    for k in range(len(states)):      # no synchronisation between the calls
+        integ.step_host(ins[k], outs[k], 0.1 * k, 2 + k % 2, cfl)
+    integ.synchronize()
+    last = integ.get_state()
+    np.testing.assert_array_equal(last, outs[-1])
+    _, ref_integ = make(tl)
+    for k, u in enumerate(states):
+        ref = plain(ref_integ, u, 0.1 * k, 2 + k % 2, cfl)
+        np.testing.assert_array_equal(outs[k], ref)
+    integ.sync_time()
+    assert integ.iter == 2 + (len(states) - 1) % 2 and integ.t > 0.1 * (len(states) - 1)
+
+
+def test_step_host_round_trip_through_the_host(tl):
+    """Each call's input is the previous call's output buffer: the library orders the upload after the download."""
+    semi, integ = make(tl)
+    u0 = semi.compute_coefficients(0.0)
+    buf = integ.pinned_state()
+    buf[:] = u0
+    for _ in range(4):
+        integ.step_host(buf, buf, 0.0, 1, 0.5)
+    integ.synchronize()
+    _, ref_integ = make(tl)
+    u = u0.copy()
+    for _ in range(4):
+        u = plain(ref_integ, u, 0.0, 1, 0.5)
+    np.testing.assert_array_equal(buf, u)
+
+
+def test_other_entry_points_after_step_host(tl):
+    """tlw_set_state and tlw_step after asynchronous calls wait for their downloads and see the last result."""
+    semi, integ = make(tl)
+    u0 = semi.compute_coefficients(0.0)
+    a, b = integ.pinned_state(), integ.pinned_state()
+    a[:] = u0
+    integ.step_host(a, b, 0.0, 3, 0.5)
+    integ.step(2, 0.5)                  # continues from the downloaded result
+    u = integ.get_state()
+    _, ref_integ = make(tl)
+    ref3 = plain(ref_integ, u0, 0.0, 3, 0.5)
+    np.testing.assert_array_equal(b, ref3)
+    ref_integ.step(2, 0.5)
+    np.testing.assert_array_equal(u, ref_integ.get_state())
+    integ.set_state(u0, 0.0)            # overwrites the current state after the pending download
+    np.testing.assert_array_equal(integ.get_state(), u0)

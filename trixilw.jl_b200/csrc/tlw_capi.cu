@@ -60,7 +60,10 @@ void free_mesh(tlw_handle* h) {
     if (h->d_wkind) { cudaFree(h->d_wkind); h->d_wkind = nullptr; }
     dfree(h->d_wall);
     h->bnd_dirichlet = true;
-    dfree(h->d_state[0]); dfree(h->d_state[1]);
+    if (h->s_up) cudaStreamSynchronize(h->s_up);
+    if (h->s_down) cudaStreamSynchronize(h->s_down);
+    h->async_pending = false;
+    dfree(h->d_state[0]); dfree(h->d_state[1]); dfree(h->d_stage);
     dfree(h->d_us); dfree(h->d_in); dfree(h->d_in2); dfree(h->d_out);
     dfree(h->d_tU); dfree(h->d_tF); dfree(h->d_U2); dfree(h->d_F2);
     dfree(h->d_alpha); dfree(h->d_alpha_raw); dfree(h->d_tFn); dfree(h->d_il); dfree(h->d_ir);
@@ -574,8 +577,13 @@ __global__ void reciprocal_probe_kernel(const double* __restrict__ x, double* __
         y[k] = nr_reciprocal(x[k]);
 }
 
-int check_ready(tlw_handle* h) {
+int check_ready(tlw_handle* h, bool join_downloads = true) {
     if (!h) return TLW_E_ARG;
+    if (join_downloads && h->async_pending) {
+        // the entry point's work on the compute stream waits for tlw_step_host's last download
+        TLW_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_down[(h->host_calls - 1) & 1], 0));
+        h->async_pending = false;
+    }
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
     if ((h->nb > 0 || h->ncb > 0) && h->bnd_dirichlet && !h->have_bdata)
         return fail(h, TLW_E_STATE, "mesh has Dirichlet boundaries: call tlw_set_boundary_data first");
@@ -665,6 +673,10 @@ int tlw_destroy(tlw_handle* h) {
     free_mesh(h);
     dfree(h->d_basis);
     dfree(h->d_step);
+    for (cudaEvent_t ev : {h->ev_up, h->ev_computed, h->ev_down[0], h->ev_down[1], h->ev_prior})
+        if (ev) cudaEventDestroy(ev);
+    if (h->s_up) cudaStreamDestroy(h->s_up);
+    if (h->s_down) cudaStreamDestroy(h->s_down);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return TLW_OK;
@@ -1636,6 +1648,76 @@ int tlw_get_state(tlw_handle* h, double* u, int32_t where, double* t_out) {
     return TLW_OK;
 }
 
+namespace {
+// the copy streams, events and staging buffer of tlw_step_host (created on its first call)
+int ensure_host_stepping(tlw_handle* h) {
+    if (!h->d_stage) TLW_CUDA(h, cudaMalloc(&h->d_stage, state_doubles(h) * sizeof(double)));
+    if (!h->s_up) {
+        TLW_CUDA(h, cudaStreamCreateWithFlags(&h->s_up, cudaStreamNonBlocking));
+        TLW_CUDA(h, cudaStreamCreateWithFlags(&h->s_down, cudaStreamNonBlocking));
+        for (cudaEvent_t* ev : {&h->ev_up, &h->ev_computed, &h->ev_down[0], &h->ev_down[1], &h->ev_prior})
+            TLW_CUDA(h, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+        TLW_CUDA(h, cudaEventRecord(h->ev_down[0], h->s_down));   // nothing downloaded yet
+        TLW_CUDA(h, cudaEventRecord(h->ev_down[1], h->s_down));
+    }
+    return TLW_OK;
+}
+}  // namespace
+
+int tlw_step_host(tlw_handle* h, const double* u_in, double* u_out, double t, int32_t nsteps, double cfl,
+                  double fixed_dt, double t_end) {
+    int rc = check_ready(h, false);
+    if (rc) return rc;
+    if (!u_in || !u_out || nsteps < 1) return fail(h, TLW_E_ARG, "tlw_step_host: u_in, u_out, nsteps >= 1");
+    if (h->nh > 0) return fail(h, TLW_E_STATE, "a partitioned mesh steps with tlw_dd_begin / _volume / _finish");
+    TLW_CUDA(h, cudaSetDevice(h->device));
+    if ((rc = ensure_host_stepping(h))) return rc;
+    const size_t bytes = state_doubles(h) * sizeof(double);
+    // buffers: d_stage receives the upload (it holds the result of the call before the previous one);
+    // d_state[cur] holds the previous result (its download may still run); d_state[1 - cur] is free once the
+    // compute stream reaches this call
+    const int parity = (int)(h->host_calls & 1);
+    double* in = h->d_stage;
+    double* prev = h->d_state[h->cur];
+    double* scratch = h->d_state[1 - h->cur];
+    // 1. upload, once the download two calls back (from this buffer) has finished, and once every earlier use of
+    //    the buffer on the compute stream has (ev_prior of the previous call, waited below)
+    TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_down[parity], 0));
+    // a caller that feeds the previous result back in (the state round-trips through the host) reads it only
+    // after its download
+    if (u_in == h->last_out && h->host_calls > 0)
+        TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_down[parity ^ 1], 0));
+    TLW_CUDA(h, cudaMemcpyAsync(in, u_in, bytes, cudaMemcpyHostToDevice, h->s_up));
+    TLW_CUDA(h, cudaEventRecord(h->ev_up, h->s_up));
+    // 2. rotate: the upload becomes the current state; the previous result becomes the next upload's target,
+    //    free after its download (ev_down) and after the compute stream's work so far (ev_prior)
+    TLW_CUDA(h, cudaEventRecord(h->ev_prior, h->stream));
+    TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_prior, 0));   // orders the NEXT upload (same stream)
+    h->d_state[0] = in;
+    h->d_state[1] = scratch;
+    h->cur = 0;
+    h->d_stage = prev;
+    drop_graphs(h);   // they address the previous buffers
+    h->slots_valid = false;
+    // 3. the steps, after the upload
+    TLW_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_up, 0));
+    StepState* sp = h->d_step;
+    const long long zero = 0;
+    TLW_CUDA(h, cudaMemcpyAsync(&sp->t, &t, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    TLW_CUDA(h, cudaMemcpyAsync(&sp->steps, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
+    h->async_pending = false;
+    if ((rc = tlw_step(h, nsteps, cfl, fixed_dt, t_end, 0))) return rc;
+    TLW_CUDA(h, cudaEventRecord(h->ev_computed, h->stream));
+    // 4. download the result
+    TLW_CUDA(h, cudaStreamWaitEvent(h->s_down, h->ev_computed, 0));
+    TLW_CUDA(h, cudaMemcpyAsync(u_out, h->d_state[h->cur], bytes, cudaMemcpyDeviceToHost, h->s_down));
+    TLW_CUDA(h, cudaEventRecord(h->ev_down[parity], h->s_down));
+    h->host_calls += 1;
+    h->last_out = u_out;
+    h->async_pending = true;
+    return TLW_OK;
+}
+
 int tlw_step(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double t_end, int32_t use_graph) {
     int rc = check_ready(h);
     if (rc) return rc;
@@ -1833,6 +1915,8 @@ int tlw_get_cache(tlw_handle* h, int32_t item, double* out, int32_t where) {
 int tlw_synchronize(tlw_handle* h) {
     if (!h) return TLW_E_ARG;
     TLW_CUDA(h, cudaSetDevice(h->device));
+    if (h->s_up) TLW_CUDA(h, cudaStreamSynchronize(h->s_up));
+    if (h->s_down) TLW_CUDA(h, cudaStreamSynchronize(h->s_down));
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));
     TLW_CUDA(h, cudaGetLastError());
     return read_status(h);

@@ -161,6 +161,17 @@ struct tlw_handle {
     double* d_cmj = nullptr;
     std::vector<int> mortar_order;
     std::vector<int> mortar_off;            // mortar colour c covers [mortar_off[c], mortar_off[c + 1])
+    // host-buffer stepping (tlw_step_host): a third state buffer that uploads land in, the copy streams, and
+    // events: ev_down[call parity] after each call's download (the result of call k is the upload target of
+    // call k + 2), ev_prior on the compute stream before each call's steps; async_pending until another entry
+    // point has ordered itself after the last download
+    double* d_stage = nullptr;
+    cudaStream_t s_up = nullptr, s_down = nullptr;
+    cudaEvent_t ev_up = nullptr, ev_computed = nullptr, ev_prior = nullptr;
+    cudaEvent_t ev_down[2] = {nullptr, nullptr};
+    long long host_calls = 0;
+    const void* last_out = nullptr;          // u_out of the last call (a next u_in equal to it waits for it)
+    bool async_pending = false;
     // graphs: [start buffer] one step, two steps
     cudaGraphExec_t g_one[2] = {nullptr, nullptr};
     cudaGraphExec_t g_two[2] = {nullptr, nullptr};

@@ -74,6 +74,27 @@ class LWIntegrator:
         check(self.handle, lib().tlw_step(self.handle, int(nsteps), float(cfl), float(fixed_dt),
                                           float(self.tspan[1]), 1 if use_graph else 0))
 
+    def step_host(self, u_in: np.ndarray, u_out: np.ndarray, t: float, nsteps: int, cfl: float,
+                  fixed_dt: float = 0.0):
+        """Asynchronous host-buffer stepping (tlw_step_host): u_in at time t is uploaded, advanced nsteps steps and
+        downloaded into u_out; both arrays must stay alive and untouched until ``synchronize``. Consecutive calls
+        overlap their copies (pinned arrays, e.g. from ``pinned_state``, make the copies asynchronous)."""
+        n = 4 * self.p.ndofs()
+        if u_in.size != n or u_out.size != n or u_in.dtype != np.float64 or u_out.dtype != np.float64:
+            raise ValueError("u_in / u_out: float64 state vectors of the mesh's size")
+        if not (u_in.flags.c_contiguous and u_out.flags.c_contiguous):
+            raise ValueError("u_in / u_out must be contiguous")
+        check(self.handle, lib().tlw_step_host(self.handle, _ptr(u_in), _ptr(u_out), float(t), int(nsteps),
+                                               float(cfl), float(fixed_dt), float(self.tspan[1])))
+
+    def synchronize(self):
+        check(self.handle, lib().tlw_synchronize(self.handle))
+
+    def pinned_state(self) -> np.ndarray:
+        """A page-locked host state vector of the mesh's size (through torch's pinned allocator)."""
+        import torch
+        return torch.empty(4 * self.p.ndofs(), dtype=torch.float64, pin_memory=True).numpy()
+
     def isfinished(self) -> bool:
         # integrator.t ≈ last(tspan) (src/solvers/lwfr.jl:147-149): Julia isapprox, rtol = sqrt(eps)
         te = self.tspan[1]
