@@ -184,6 +184,23 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
                         const double* inverse_jacobian, int64_t n_interfaces, const int64_t* primary_elements,
                         const int32_t* primary_faces, const int64_t* secondary_elements,
                         const int32_t* secondary_faces, const int32_t* secondary_reversed);
+/* UnstructuredMesh2D in Trixi's conventions (src/solvers/dgsem_unstructured_2d/dg_2d.jl:14-280, containers.jl), in
+ * place of a TreeMesh: LW with the FR or the shock-capturing volume integral (first-order or MUSCL subcells, Rusanov),
+ * conforming and without boundaries, which is what the reference runs on it (its rhs! is LW only, and its
+ * calc_boundary_flux!, :421-450, calls the boundary condition with arguments no method accepts).
+ *   contravariant_vectors [2, 2, n, n, element], inverse_jacobian [n, n, element]: as for tlw_set_curved_mesh
+ *   normal_directions     [2, n, 4, element]  Trixi elements.normal_directions (outward, by side)
+ *   interface k: element_ids [2, k] (primary, secondary; 1-based), element_side_ids [2, k] (sides 1: bottom (j = 1),
+ *   2: right (i = n), 3: top (j = n), 4: left (i = 1)), start_index [k] and index_increment [k] (1 and 1, or n and
+ *   -1) of the secondary's node index along the primary's.
+ * The interface flux takes the primary's outward normal from normal_directions at its node, dots both sides'
+ * physical time-averaged fluxes with it, and with shock capturing blends by compute_alp (the admissibility of
+ * both sides' first-order subcell updates from the time-averaged U, J^{-1} of the primary face node). */
+int tlw_set_unstructured_mesh(tlw_handle* h, int64_t n_elements, const double* contravariant_vectors,
+                              const double* inverse_jacobian, const double* normal_directions, int64_t n_interfaces,
+                              const int64_t* element_ids, const int64_t* element_side_ids, const int64_t* start_index,
+                              const int64_t* index_increment);
+
 /* Domain decomposition (the reference's MPI path, src/solvers/dgsem_tree/dg_2d_parallel.jl:23-200, with the same
  * message per cut face node: the u face value, U trace and F.n trace, 3 nv doubles, dg_parallel.jl:12-13). A rank
  * uploads its part of the TreeMesh with tlw_set_tree_mesh (local elements, the interfaces between them, its

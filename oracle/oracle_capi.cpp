@@ -206,6 +206,16 @@ int oracle_set_curved_mortars(oracle_handle* h, int M, const int32_t* small1, co
 }
 
 // lw_mortars.inverse_jacobian [mortar][l] for the shock-capturing blend at the mortars (null: zeros)
+// UnstructuredMesh2D: the caller's outward normals by face [2, l, face, e] (faces as the curved interfaces);
+// null switches back to the StructuredMesh / P4estMesh interface conventions
+int oracle_set_unstructured_normals(oracle_handle* h, const double* normals) {
+    if (!h->curved) return 1;
+    CurvedMesh& m = h->cmesh;
+    if (!normals) m.unormals.clear();
+    else m.unormals.assign(normals, normals + (size_t)2 * h->basis.n * 4 * m.n_elements);
+    return 0;
+}
+
 int oracle_set_curved_mortar_jacobian(oracle_handle* h, const double* inv_jac) {
     if (!h->curved) return 1;
     CurvedMesh& m = h->cmesh;

@@ -40,6 +40,7 @@ def lib():
         L.oracle_destroy.argtypes = [P]
         L.oracle_set_temporal_errors.argtypes = [P, i32, dbl, dbl]
         L.oracle_set_curved_mortar_jacobian.argtypes = [P, P]
+        L.oracle_set_unstructured_normals.argtypes = [P, P]
         L.oracle_set_shock_capturing.argtypes = [P, i32, dbl, dbl, i32]
         L.oracle_set_reconstruction.argtypes = [P, i32]
         L.oracle_set_curved_mortars.argtypes = [P, i32, P, P, P, P, P, P]
@@ -143,6 +144,17 @@ class Oracle:
         if getattr(cm, "n_mortars", 0):
             self.set_curved_mortars(cm.mortar_small1, cm.mortar_small2, cm.mortar_small_faces, cm.mortar_large,
                                     cm.mortar_large_faces, cm.mortar_large_reversed)
+        if getattr(cm, "unstructured", False):
+            self.set_unstructured_normals(cm.unormals)
+
+    def set_unstructured_normals(self, normals):
+        """UnstructuredMesh2D interface conventions with the caller's outward normals by face, (E, 4, n, 2); None:
+        back to the StructuredMesh / P4estMesh ones."""
+        if normals is None:
+            assert lib().oracle_set_unstructured_normals(self.h, None) == 0
+            return
+        self._nkeep = np.ascontiguousarray(normals, dtype=np.float64)
+        assert lib().oracle_set_unstructured_normals(self.h, _p(self._nkeep)) == 0
 
     def __del__(self):
         try:

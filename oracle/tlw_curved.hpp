@@ -41,7 +41,17 @@ struct CurvedMesh {
     // lw_mortars.inverse_jacobian [mortar][l] (the J^{-1} of the shock-capturing blend at the mortars); empty:
     // zeros, as the reference holds them until an AMR step loads them
     std::vector<double> m_ij;
+    // UnstructuredMesh2D: the caller's outward normals (Trixi elements.normal_directions) by face, [2, l, face, e];
+    // empty for StructuredMesh / P4estMesh. The interfaces are then in the unstructured conventions below.
+    std::vector<double> unormals;
 };
+
+// UnstructuredMesh2D sides (1: bottom j = 1, 2: right i = n, 3: top j = n, 4: left i = 1) as faces, and the
+// fn_low slot of a face (load_fn_low! for UnstructuredMesh2D / P4estMesh{2}: bottom, right, top, left,
+// src/solvers/dgsem_tree/dg_2d.jl:236-249), which the unstructured path reads by side
+inline int face_of_side(int side) { return side == 1 ? 2 : side == 2 ? 1 : side == 3 ? 3 : 0; }
+inline int fn_low_slot(int face) { return face == 0 ? 3 : face == 1 ? 1 : face == 2 ? 0 : 2; }
+
 
 // node (i, j) of face f at face index l
 inline void face_node(int n, int f, int l, int& i, int& j) {
@@ -103,6 +113,35 @@ inline void lw_surface_flux_normal(const Euler& eq, int flux_kind, int speed_kin
             for (int v = 0; v < NV; ++v) out[v] = fll * f_ll[v] - frr * f_rr[v] + fd * (a4[v] - a3[v]);
         }
     }
+}
+
+// One interface node of an UnstructuredMesh2D (prolong2interfaces! and calc_interface_flux!,
+// src/solvers/dgsem_unstructured_2d/dg_2d.jl:60-280): the normal is the caller's outward normal of the primary at
+// its node l (normal_directions); both sides' normal fluxes are the physical time-averaged flux dotted with that
+// normal (the secondary node s(l) = start_index + (l - 1) index_increment is prolonged with the primary's normal at
+// its own secondary index, which is the primary's node l); the 8-argument surface flux takes the curvilinear order
+// (f_ll, f_rr, u_ll, u_rr, U_ll, U_rr, normal). Returns the primary's outward flux Fn_ (before any blending) and,
+// for shock capturing, the first-order flux fn = surface_flux(u_ll, u_rr, normal).
+inline void unstructured_interface_node(const Euler& eq, const Options& opt, const CurvedMesh& m, int n, const double* u,
+                                        const Workspace& ws, int pe, int pf, int se, int sf, int l, int ls,
+                                        double* nP, double* Fn_, double* u_ll, double* u_rr, double* U_ll,
+                                        double* U_rr, bool& bad) {
+    int ip, jp, is, js;
+    face_node(n, pf, l, ip, jp);
+    face_node(n, sf, ls, is, js);
+    nP[0] = m.unormals[2 * (l + (size_t)n * (pf + 4 * (size_t)pe))];
+    nP[1] = m.unormals[2 * (l + (size_t)n * (pf + 4 * (size_t)pe)) + 1];
+    double f_ll[NV], f_rr[NV];
+    for (int v = 0; v < NV; ++v) {
+        // normal_product(f, equations, n) = F[1] n[1] + F[2] n[2] (src/solvers/fr.jl:146-150)
+        f_ll[v] = ws.F[idx_F(n, v, 0, ip, jp, pe)] * nP[0] + ws.F[idx_F(n, v, 1, ip, jp, pe)] * nP[1];
+        f_rr[v] = ws.F[idx_F(n, v, 0, is, js, se)] * nP[0] + ws.F[idx_F(n, v, 1, is, js, se)] * nP[1];
+        u_ll[v] = u[idx_u(n, v, ip, jp, pe)];
+        u_rr[v] = u[idx_u(n, v, is, js, se)];
+        U_ll[v] = ws.U[idx_u(n, v, ip, jp, pe)];
+        U_rr[v] = ws.U[idx_u(n, v, is, js, se)];
+    }
+    lw_surface_flux_normal(eq, opt.flux_kind, opt.speed_kind, f_ll, f_rr, u_ll, u_rr, U_ll, U_rr, nP, Fn_, bad);
 }
 
 // One element of the curvilinear LW volume kernel. du receives Dhat F~ + Dhat G~ (before the surface
@@ -384,6 +423,18 @@ inline void surface_integral_and_jacobian_curved(const Basis& b, const CurvedMes
     }
 }
 
+// What the reference can run on an UnstructuredMesh2D: its rhs! (dgsem_unstructured_2d/dg_2d.jl:14-56) is LW only
+// (no mesh-level rhs_mdrk1! / rhs_mdrk2! takes an UnstructuredMesh2D), the mesh is conforming (no mortars), and its
+// calc_boundary_flux! (:421-450) calls the boundary condition with 11 arguments (U, F.n, normal, x, t, dt,
+// surface_flux, equations, dg, time discretization, scaling) that no method of src/equations/equations.jl
+// accepts, so only meshes without boundaries (periodic, like its Sedov elixir) run.
+inline void check_unstructured(const CurvedMesh& m, int kind) {
+    if (m.unormals.empty()) return;
+    if (kind != 0) throw std::invalid_argument("UnstructuredMesh2D: LW only");
+    if (m.n_boundaries > 0 || m.n_mortars > 0)
+        throw std::invalid_argument("UnstructuredMesh2D: conforming and without boundaries");
+}
+
 // du = rhs(u) on a conforming curvilinear mesh (LW, FR volume integral; boundaries: slip walls)
 // kind 0: LW rhs!; 1: rhs_mdrk1! (keeps U2, F2); 2: rhs_mdrk2! with the stage state u2 in the volume terms and
 // u (u^n) at the interfaces (src/solvers/dgsem_structured/multi_derivative_2d.jl:1-80)
@@ -403,6 +454,7 @@ inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, cons
         ws.F2.assign(2 * ndof, nan);
     }
     if (kind == 2 && (ws.U2.size() != ndof || !u2)) throw std::invalid_argument("rhs_mdrk2 before rhs_mdrk1");
+    check_unstructured(m, kind);
     for (size_t k = 0; k < ndof; ++k) du[k] = 0.0;
 #pragma omp parallel for num_threads(nthreads) schedule(static)
     for (int e = 0; e < m.n_elements; ++e) {
@@ -418,6 +470,17 @@ inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, cons
         const int pe = m.p_elem[k], pf = m.p_face[k], se = m.s_elem[k], sf = m.s_face[k];
         for (int l = 0; l < n; ++l) {
             const int ls = m.s_rev[k] ? n - 1 - l : l;
+            if (!m.unormals.empty()) {   // UnstructuredMesh2D
+                double nP[2], Fn[NV], u_ll[NV], u_rr[NV], U_ll[NV], U_rr[NV];
+                bool b_ = false;
+                unstructured_interface_node(eq, opt, m, n, u, ws, pe, pf, se, sf, l, ls, nP, Fn, u_ll, u_rr, U_ll, U_rr, b_);
+                bad = bad || b_;
+                for (int v = 0; v < NV; ++v) {
+                    ws.surface_flux_values[v + NV * (l + n * (pf + 4 * (size_t)pe))] = Fn[v];
+                    ws.surface_flux_values[v + NV * (ls + n * (sf + 4 * (size_t)se))] = -Fn[v];
+                }
+                continue;
+            }
             int ip, jp, is, js;
             face_node(n, pf, l, ip, jp);
             face_node(n, sf, ls, is, js);

@@ -439,6 +439,27 @@ inline void get_blended_flux(const Basis& b, const Euler& eq, const double* u_ll
 // the DG volume terms (calc_volume_integral_mdrk1! / _mdrk2!, src/solvers/dgsem_tree/multi_derivative_2d.jl:
 // 150-262: the indicator and the subcells take u in both stages; the interfaces blend with the full dt and the
 // instantaneous u, the boundaries of stage 1 halve their time averages).
+// compute_alp for Union{StructuredMesh, UnstructuredMesh2D} (src/solvers/dgsem_structured/dg_2d.jl:2169-2191), as
+// the UnstructuredMesh2D interface calls it (dgsem_unstructured_2d/dg_2d.jl:255-262): alp = (alpha_P + alpha_S) / 2,
+// or 1 when the first-order subcell update of either side with the blended flux is not admissible; the updates
+// start from the time-averaged U of each side (the call passes U as u_ll / u_rr) with J^{-1} of the primary's face
+// node (load_inverse_jacobian!, :452-472) for both. The interface flux is then alp fn + (1 - alp) Fn_. fn_low is
+// oriented along +xi / +eta, so the primary's test has the sign of its outward flux only when its side is the right
+// or the top one; restated as written (the result depends on which element an interface lists first).
+inline double compute_alp_unstructured(const Basis& b, const Euler& eq, const double* U_ll, const double* U_rr,
+                                       double alpha_p, double alpha_s, double J, double dt, const double* fn,
+                                       const double* Fn_, const double* fil, const double* fir) {
+    const double alp = 0.5 * (alpha_p + alpha_s);
+    double Fn[NV], low[NV];
+    for (int v = 0; v < NV; ++v) Fn[v] = (1.0 - alp) * Fn_[v] + alp * fn[v];
+    const double lam = 0.5;
+    for (int v = 0; v < NV; ++v) low[v] = U_ll[v] - dt * J / (b.weights[b.n - 1] * lam) * (Fn[v] - fil[v]);
+    if (!eq.is_admissible(low)) return 1.0;
+    for (int v = 0; v < NV; ++v) low[v] = U_rr[v] - dt * J / (b.weights[0] * lam) * (fir[v] - Fn[v]);
+    if (!eq.is_admissible(low)) return 1.0;
+    return alp;
+}
+
 inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m, const double* u,
                           double* du, double dt, Workspace& ws, int nthreads = 1, const BoundaryData* bd = nullptr,
                           int kind = 0, const double* u2 = nullptr) {
@@ -457,6 +478,7 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
         ws.F2.assign(2 * ndof, nan);
     }
     if (kind == 2 && (ws.U2.size() != ndof || !u2)) throw std::invalid_argument("rhs_mdrk2 before rhs_mdrk1");
+    check_unstructured(m, kind);
     for (size_t k = 0; k < ndof; ++k) du[k] = 0.0;
     indicator_curved(b, eq, opt, m, u, ws.alpha);
     const Subcells sc = compute_subcells(b);
@@ -482,6 +504,31 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
         const int pe = m.p_elem[k], pf = m.p_face[k], se = m.s_elem[k], sf = m.s_face[k];
         for (int l = 0; l < n; ++l) {
             const int ls = m.s_rev[k] ? n - 1 - l : l;
+            if (!m.unormals.empty()) {
+                // UnstructuredMesh2D (dgsem_unstructured_2d/dg_2d.jl:211-280): fn_low by side, each side at its
+                // own node index (the interface cache keeps them by local index, :72-75, read at :236-243)
+                double nP[2], Fn_[NV], fn[NV], u_ll[NV], u_rr[NV], U_ll[NV], U_rr[NV], fil[NV], fir[NV];
+                bool b_ = false;
+                unstructured_interface_node(eq, opt, m, n, u, ws, pe, pf, se, sf, l, ls, nP, Fn_, u_ll, u_rr, U_ll,
+                                            U_rr, b_);
+                rusanov_normal(eq, opt.speed_kind, u_ll, u_rr, nP, fn, b_);
+                bad = bad || b_;
+                for (int v = 0; v < NV; ++v) {
+                    fil[v] = ws.fn_low[v + NV * (l + n * (fn_low_slot(pf) + 4 * (size_t)pe))];
+                    fir[v] = ws.fn_low[v + NV * (ls + n * (fn_low_slot(sf) + 4 * (size_t)se))];
+                }
+                int ip, jp;
+                face_node(n, pf, l, ip, jp);
+                const double J = m.inv_jac[ip + n * (jp + (size_t)n * pe)];
+                const double alp = compute_alp_unstructured(b, eq, U_ll, U_rr, ws.alpha[pe], ws.alpha[se], J, dt, fn,
+                                                            Fn_, fil, fir);
+                for (int v = 0; v < NV; ++v) {
+                    const double F = alp * fn[v] + (1.0 - alp) * Fn_[v];
+                    ws.surface_flux_values[v + NV * (l + n * (pf + 4 * (size_t)pe))] = F;
+                    ws.surface_flux_values[v + NV * (ls + n * (sf + 4 * (size_t)se))] = -F;
+                }
+                continue;
+            }
             int ip, jp, is, js;
             face_node(n, pf, l, ip, jp);
             face_node(n, sf, ls, is, js);

@@ -97,6 +97,8 @@ void free_mesh(tlw_handle* h) {
     if (h->d_cmj) { cudaFree(h->d_cmj); h->d_cmj = nullptr; }
     h->ncm = 0;
     h->mortar_off.clear();
+    dfree(h->d_unorm); dfree(h->d_tG);
+    h->unstructured = false;
     h->curved = false;
     h->have_mesh = false;
     h->have_bdata = false;
@@ -260,6 +262,10 @@ void enqueue_curved_surfaces(tlw_handle* h, int mode, const double* u_jump, doub
         ca.tFn = h->d_tFn;
         ca.w_first = h->h_basis.weights[0];
         ca.w_last = h->h_basis.weights[h->n - 1];
+    }
+    if (h->unstructured) {
+        ca.tG = h->d_tG;
+        ca.unorm = h->d_unorm;
     }
     for (size_t c = 0; c + 1 < h->color_off.size(); ++c) {
         const int b = h->color_off[c];
@@ -436,6 +442,7 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     if (h->curved) {
         va.metrics = h->d_Ja;
         va.inv_jac_node = h->d_ijn;
+        if (h->unstructured) va.tG = h->d_tG;
         if (h->sc) {
             va.subn = h->d_subn;
             va.subq = h->d_subq;
@@ -946,6 +953,51 @@ int tlw_set_curved_mesh(tlw_handle* h, int64_t n_elements, const double* contrav
     return TLW_OK;
 }
 
+int tlw_set_unstructured_mesh(tlw_handle* h, int64_t n_elements, const double* contravariant_vectors,
+                              const double* inverse_jacobian, const double* normal_directions, int64_t n_interfaces,
+                              const int64_t* element_ids, const int64_t* element_side_ids, const int64_t* start_index,
+                              const int64_t* index_increment) {
+    if (!h) return TLW_E_ARG;
+    if (h->opts.time_discretization != TLW_LW)
+        return fail(h, TLW_E_UNSUPPORTED, "UnstructuredMesh2D: LW (the reference has no MDRK rhs for it)");
+    if (!normal_directions || n_elements <= 0 || n_elements > (int64_t)0x7fffffff / 64) return fail(h, TLW_E_ARG, "normals");
+    if (n_interfaces < 0 || (n_interfaces > 0 && (!element_ids || !element_side_ids || !start_index || !index_increment)))
+        return fail(h, TLW_E_ARG, "interfaces");
+    // Trixi sides 1: bottom (j = 1), 2: right (i = n), 3: top (j = n), 4: left (i = 1) as faces 0: -xi, 1: +xi,
+    // 2: -eta, 3: +eta; the secondary index runs forward (start 1, increment 1) or backward (start n, increment -1)
+    static const int face_of_side[5] = {-1, 2, 1, 3, 0};
+    std::vector<int64_t> pe((size_t)n_interfaces), se((size_t)n_interfaces);
+    std::vector<int32_t> pf((size_t)n_interfaces), sf((size_t)n_interfaces), rv((size_t)n_interfaces);
+    for (int64_t k = 0; k < n_interfaces; ++k) {
+        const int64_t s1 = element_side_ids[2 * k], s2 = element_side_ids[2 * k + 1];
+        const int64_t st = start_index[k], inc = index_increment[k];
+        if (s1 < 1 || s1 > 4 || s2 < 1 || s2 > 4 || !((st == 1 && inc == 1) || (st == h->n && inc == -1)))
+            return fail(h, TLW_E_ARG, "interface " + std::to_string(k + 1) + ": side or secondary index out of range");
+        pe[(size_t)k] = element_ids[2 * k];
+        se[(size_t)k] = element_ids[2 * k + 1];
+        pf[(size_t)k] = face_of_side[s1];
+        sf[(size_t)k] = face_of_side[s2];
+        rv[(size_t)k] = inc == -1 ? 1 : 0;
+    }
+    int rc = tlw_set_curved_mesh(h, n_elements, contravariant_vectors, inverse_jacobian, n_interfaces, pe.data(),
+                                 pf.data(), se.data(), sf.data(), rv.data());
+    if (rc) return rc;
+    // normal_directions [2, node, side, element] -> [2, l, face, e]
+    const int n = h->n;
+    std::vector<double> nd((size_t)2 * n * 4 * n_elements);
+    for (int64_t e = 0; e < n_elements; ++e)
+        for (int side = 1; side <= 4; ++side)
+            for (int l = 0; l < n; ++l)
+                for (int d = 0; d < 2; ++d)
+                    nd[(((size_t)e * 4 + face_of_side[side]) * n + l) * 2 + d] =
+                        normal_directions[d + 2 * (l + (size_t)n * ((side - 1) + 4 * (size_t)e))];
+    TLW_CUDA(h, cudaMalloc(&h->d_unorm, nd.size() * sizeof(double)));
+    TLW_CUDA(h, upload_on(h->stream, h->d_unorm, nd.data(), nd.size() * sizeof(double)));
+    if ((rc = ensure(h, h->d_tG, trace_doubles(h)))) return rc;
+    h->unstructured = true;
+    return TLW_OK;
+}
+
 int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar_neighbor_ids,
                          const int64_t* mortar_large_sides, const int64_t* mortar_orientations) {
     if (!h) return TLW_E_ARG;
@@ -1111,6 +1163,7 @@ int tlw_set_curved_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* smal
                            const int32_t* large_reversed) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh || !h->curved) return fail(h, TLW_E_STATE, "curved mortars follow tlw_set_curved_mesh");
+    if (h->unstructured && n_mortars > 0) return fail(h, TLW_E_UNSUPPORTED, "UnstructuredMesh2D is conforming");
     if (h->parabolic || h->ncb > 0)
         return fail(h, TLW_E_UNSUPPORTED, "curvilinear mortars: before the boundaries, without Navier-Stokes");
     if (n_mortars < 0 || (n_mortars > 0 && (!small1 || !small2 || !small_faces || !large || !large_faces || !large_reversed)))
@@ -1219,6 +1272,9 @@ int tlw_set_curved_boundaries(tlw_handle* h, int64_t n_boundaries, const int64_t
                               const int32_t* kinds) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh || !h->curved) return fail(h, TLW_E_STATE, "curved boundaries follow tlw_set_curved_mesh");
+    if (h->unstructured && n_boundaries > 0)
+        return fail(h, TLW_E_UNSUPPORTED, "UnstructuredMesh2D: meshes without boundaries (the reference's boundary "
+                                          "call matches no boundary-condition method)");
     if (n_boundaries < 0 || (n_boundaries > 0 && (!elements || !faces || !kinds))) return fail(h, TLW_E_ARG, "boundaries");
     std::vector<int> be[2], bf[2], bk[2], bi[2];
     std::vector<signed char> used = h->face_used;
@@ -1344,6 +1400,7 @@ int tlw_apply_positivity_limiter(tlw_handle* h) {
 int tlw_set_parabolic(tlw_handle* h, double mu, double prandtl) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "the parabolic terms follow tlw_set_tree_mesh / tlw_set_curved_mesh");
+    if (h->unstructured) return fail(h, TLW_E_UNSUPPORTED, "Navier-Stokes: TreeMesh or P4estMesh-style curvilinear meshes");
     if (h->opts.time_discretization != TLW_LW || h->sc || h->N < 3 || h->nmx + h->nmy > 0 || h->ncm > 0)
         return fail(h, TLW_E_UNSUPPORTED, "Navier-Stokes: LW, FR volume integral, N >= 3, conforming mesh");
     if (!(mu >= 0.0) || !(prandtl > 0.0)) return fail(h, TLW_E_ARG, "mu / Prandtl");

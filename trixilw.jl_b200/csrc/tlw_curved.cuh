@@ -107,7 +107,14 @@ struct CurvedSurfArgs {
     const double* alpha;
     const double* tFn;
     double w_first, w_last;
+    // UnstructuredMesh2D (or null): physical flux traces tF <- F, tG <- G, and the caller's outward normals
+    // [2, l, face, e]
+    const double* tG;
+    const double* unorm;
 };
+
+// fn_low slot of a face: load_fn_low! fills (bottom, right, top, left) (src/solvers/dgsem_tree/dg_2d.jl:236-249)
+__device__ __forceinline__ int fn_low_slot(int f) { return f == 0 ? 3 : f == 1 ? 1 : f == 2 ? 0 : 2; }
 
 // zhang_shu_flux_fix (src/solvers/dgsem_p4est/dg_2d.jl:199-225): Fn is pulled towards the first-order fn until
 // the density, then the pressure, of the subcell update uprev - c (Fn - fn_inner) is no further from the
@@ -174,6 +181,73 @@ __device__ __forceinline__ void blend_curved_flux(const CurvedSurfArgs& a, int p
     if (!admissible(gm1, test)) zhang_shu_flux_fix(gm1, uS, low, Fn, fir, fn, cr);
 }
 
+// compute_alp for Union{StructuredMesh, UnstructuredMesh2D} (src/solvers/dgsem_structured/dg_2d.jl:2169-2191) as the
+// UnstructuredMesh2D interface calls it (src/solvers/dgsem_unstructured_2d/dg_2d.jl:234-268): fn = Rusanov(u_P, u_S,
+// n); alp = (alpha_P + alpha_S) / 2, or 1 when the first-order subcell update of either side with the blended flux
+// is not admissible, the updates starting from the time-averaged U of each side with J^{-1} of the primary face
+// node; fn_low by side slot, each side at its own node index. Fn <- alp fn + (1 - alp) Fn.
+template <int N>
+__device__ __forceinline__ void blend_unstructured_flux(const CurvedSurfArgs& a, int pe, int se, int pf, int sf, int l,
+                                                        int ls, int np, const double* uP, const double* uS,
+                                                        const double* UP, const double* US, const double* nrm,
+                                                        double* Fn) {
+    constexpr int n = N + 1, nn = n * n;
+    const double gm1 = a.gamma - 1.0;
+    double fP[NV], gP[NV], fS[NV], gS[NV], fn[NV], fil[NV], fir[NV];
+    euler_fluxes(gm1, uP[0], uP[1], uP[2], uP[3], fP, gP);
+    euler_fluxes(gm1, uS[0], uS[1], uS[2], uS[3], fS, gS);
+    const double lam = max_abs_speed_normal(a.gamma, uP, uS, nrm, a.speed_kind, a.status);
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+        fn[v] = 0.5 * ((fP[v] * nrm[0] + gP[v] * nrm[1]) + (fS[v] * nrm[0] + gS[v] * nrm[1])) + (-0.5 * lam * (uS[v] - uP[v]));
+    load4(a.tFn + (((size_t)pe * 4 + fn_low_slot(pf)) * n + l) * NV, fil);
+    load4(a.tFn + (((size_t)se * 4 + fn_low_slot(sf)) * n + ls) * NV, fir);
+    double alp = 0.5 * (__ldg(a.alpha + pe) + __ldg(a.alpha + se));
+    const double dt = *a.dt;
+    const double J = __ldg(a.inv_jac + (size_t)pe * nn + np);
+    double Fb[NV], low[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Fb[v] = (1.0 - alp) * Fn[v] + alp * fn[v];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) low[v] = UP[v] - dt * J / (a.w_last * 0.5) * (Fb[v] - fil[v]);
+    if (!admissible(gm1, low)) {
+        alp = 1.0;
+    } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) low[v] = US[v] - dt * J / (a.w_first * 0.5) * (fir[v] - Fb[v]);
+        if (!admissible(gm1, low)) alp = 1.0;
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Fn[v] = alp * fn[v] + (1.0 - alp) * Fn[v];
+}
+
+// An UnstructuredMesh2D interface node (prolong2interfaces!, calc_interface_flux!, src/solvers/dgsem_unstructured_2d/
+// dg_2d.jl:60-280): the normal is the caller's outward normal of the primary at its node l; both sides' normal
+// fluxes are their physical time-averaged fluxes dotted with it (the secondary's node s(l) = start_index +
+// (l - 1) index_increment is prolonged with the primary normal at that index, i.e. at l); the curvilinear argument
+// order; Fn on the primary, -Fn on the secondary at s(l).
+template <int N>
+__device__ __forceinline__ void unstructured_interface_flux(const CurvedSurfArgs& a, int pe, int se, int pf, int sf,
+                                                            int l, int ls, int np, const double* uP, const double* uS,
+                                                            const double* UP, const double* US, double* Fn) {
+    constexpr int n = N + 1;
+    const size_t tp = (((size_t)pe * 4 + pf) * n + l) * NV, ts = (((size_t)se * 4 + sf) * n + ls) * NV;
+    double FP[NV], GP[NV], FS[NV], GS[NV], fl[NV], fr[NV];
+    load4(a.tF + tp, FP);
+    load4(a.tG + tp, GP);
+    load4(a.tF + ts, FS);
+    load4(a.tG + ts, GS);
+    const double2 nv = __ldg(reinterpret_cast<const double2*>(a.unorm) + ((size_t)pe * 4 + pf) * n + l);
+    const double nrm[2] = {nv.x, nv.y};
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        fl[v] = fma(FP[v], nrm[0], GP[v] * nrm[1]);   // normal_product (src/solvers/fr.jl:146-150)
+        fr[v] = fma(FS[v], nrm[0], GS[v] * nrm[1]);
+    }
+    lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, fl, fr, uP, uS, UP, US, nrm, Fn, a.status);
+    if (a.alpha) blend_unstructured_flux<N>(a, pe, se, pf, sf, l, ls, np, uP, uS, UP, US, nrm, Fn);
+}
+
 template <int N>
 static __global__ void __launch_bounds__(128) curved_interface_kernel(CurvedSurfArgs a) {
     constexpr int n = N + 1;
@@ -193,17 +267,21 @@ static __global__ void __launch_bounds__(128) curved_interface_kernel(CurvedSurf
     const size_t tp = (((size_t)pe * 4 + pf) * n + l) * NV, ts = (((size_t)se * 4 + sf) * n + ls) * NV;
     load4(a.tU + tp, UP);
     load4(a.tU + ts, US);
-    load4(a.tF + tp, FP);
-    load4(a.tF + ts, FS);
-    load4(a.metrics + ((size_t)pe * nn + np) * 4, J);
-    const double nrm[2] = {sgP * (pf < 2 ? J[0] : J[2]), sgP * (pf < 2 ? J[1] : J[3])};
+    if (a.tG) {
+        unstructured_interface_flux<N>(a, pe, se, pf, sf, l, ls, np, uP, uS, UP, US, Fn);
+    } else {
+        load4(a.tF + tp, FP);
+        load4(a.tF + ts, FS);
+        load4(a.metrics + ((size_t)pe * nn + np) * 4, J);
+        const double nrm[2] = {sgP * (pf < 2 ? J[0] : J[2]), sgP * (pf < 2 ? J[1] : J[3])};
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-        FP[v] *= sgP;     // F_P . n_P
-        FS[v] *= -sgS;    // F_S . (-n_S)
+        for (int v = 0; v < NV; ++v) {
+            FP[v] *= sgP;     // F_P . n_P
+            FS[v] *= -sgS;    // F_S . (-n_S)
+        }
+        lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, FP, FS, uP, uS, UP, US, nrm, Fn, a.status);
+        if (a.alpha) blend_curved_flux<N>(a, pe, se, pf, sf, l, np, uP, uS, nrm, Fn);
     }
-    lw_surface_flux_normal(a.gamma, a.flux_kind, a.speed_kind, FP, FS, uP, uS, UP, US, nrm, Fn, a.status);
-    if (a.alpha) blend_curved_flux<N>(a, pe, se, pf, sf, l, np, uP, uS, nrm, Fn);
     if (a.tFv) {
         // minus the mean of both sides' viscous normal fluxes (calc_interface_flux_hyperbolic_parabolic!,
         // src/solvers/dgsem_p4est/dg_2d_parabolic.jl:1878-1958)

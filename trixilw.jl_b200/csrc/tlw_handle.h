@@ -150,6 +150,11 @@ struct tlw_handle {
     // slip-wall kind and the boundary's index in the caller's order (wall data)
     int ncb = 0, ncbx = 0;
     int *d_cbe = nullptr, *d_cbf = nullptr, *d_cbk = nullptr, *d_cbi = nullptr;
+    // UnstructuredMesh2D (tlw_set_unstructured_mesh): the caller's outward normals [2, l, face, e] and the second
+    // physical flux trace (G; d_tF holds F)
+    bool unstructured = false;
+    double* d_unorm = nullptr;
+    double* d_tG = nullptr;
     // L2 mortars of the curvilinear mesh, sorted by colour: small elements (positions 1, 2), large element, and
     // small face | large face << 2 | large reversed << 4
     int ncm = 0;

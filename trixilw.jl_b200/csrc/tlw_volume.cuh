@@ -67,6 +67,7 @@ struct VolArgs {
     double* out;            // du (MODE_RHS) or the updated state (MODE_STEP)
     double* tU;             // face traces of U   [v, l, face, e]
     double* tF;             // face traces of F.n [v, l, face, e]
+    double* tG;             // UnstructuredMesh2D: physical flux traces, tF <- F and tG <- G (null otherwise)
     double* U2;             // MDRK: stage-1 U2 [v,i,j,e] (written by stage 1, read by stage 2)
     double* F2;             // MDRK: stage-1 F2 [v,d,i,j,e]
     const double* inv_jac;  // [e]
@@ -543,10 +544,23 @@ __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, 
     store4(a.out + off, o);
     // face traces [v, l, face, e]; face 0 = -x, 1 = +x, 2 = -y, 3 = +y
     const size_t tb = (size_t)e * 4 * n * NV;
-    if (i == 0) { store4(a.tU + tb + (0 * n + j) * NV, U); store4(a.tF + tb + (0 * n + j) * NV, F); }
-    if (i == n - 1) { store4(a.tU + tb + (1 * n + j) * NV, U); store4(a.tF + tb + (1 * n + j) * NV, F); }
-    if (j == 0) { store4(a.tU + tb + (2 * n + i) * NV, U); store4(a.tF + tb + (2 * n + i) * NV, G); }
-    if (j == n - 1) { store4(a.tU + tb + (3 * n + i) * NV, U); store4(a.tF + tb + (3 * n + i) * NV, G); }
+    const bool nf = a.tG == nullptr;   // UnstructuredMesh2D: the flux traces were written before (physical)
+    if (i == 0) { store4(a.tU + tb + (0 * n + j) * NV, U); if (nf) store4(a.tF + tb + (0 * n + j) * NV, F); }
+    if (i == n - 1) { store4(a.tU + tb + (1 * n + j) * NV, U); if (nf) store4(a.tF + tb + (1 * n + j) * NV, F); }
+    if (j == 0) { store4(a.tU + tb + (2 * n + i) * NV, U); if (nf) store4(a.tF + tb + (2 * n + i) * NV, G); }
+    if (j == n - 1) { store4(a.tU + tb + (3 * n + i) * NV, U); if (nf) store4(a.tF + tb + (3 * n + i) * NV, G); }
+}
+
+// UnstructuredMesh2D: the physical time-averaged fluxes F (x) and G (y) on every face the node lies on, which its
+// interfaces dot with the caller's normals (prolong2interfaces!, src/solvers/dgsem_unstructured_2d/dg_2d.jl:60-200)
+template <int n>
+__device__ __forceinline__ void physical_flux_traces(const VolArgs& a, int e, int i, int j, const double* F,
+                                                     const double* G) {
+    const size_t tb = (size_t)e * 4 * n * NV;
+    if (i == 0) { store4(a.tF + tb + (0 * n + j) * NV, F); store4(a.tG + tb + (0 * n + j) * NV, G); }
+    if (i == n - 1) { store4(a.tF + tb + (1 * n + j) * NV, F); store4(a.tG + tb + (1 * n + j) * NV, G); }
+    if (j == 0) { store4(a.tF + tb + (2 * n + i) * NV, F); store4(a.tG + tb + (2 * n + i) * NV, G); }
+    if (j == n - 1) { store4(a.tF + tb + (3 * n + i) * NV, F); store4(a.tG + tb + (3 * n + i) * NV, G); }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -840,6 +854,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
     // the last contraction before writing F, G over them: same address, same thread)
     if (active) {
         if (CURVED) {
+            if (a.tG) physical_flux_traces<n>(a, e, i, j, F, G);
             // the surface needs the normal fluxes: keep the contravariant time averages F~, G~ (their face
             // values are F . Ja^1 and F . Ja^2)
             double ft[NV], gt[NV];

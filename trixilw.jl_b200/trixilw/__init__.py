@@ -10,6 +10,7 @@ from .equations import (CompressibleEulerEquations2D, CompressibleNavierStokesDi
 from .limiters import PositivityPreservingLimiterZhangShu, density, density_pressure, pressure
 from .lwfr import LWIntegrator, LWSolution, l2_linf_errors, solve_lwfr
 from .mesh import RefinedTreeMesh, TreeMesh
+from .unstructured_mesh import UnstructuredMesh2D
 from .semidiscretization import (LW, MDRK, DGSEM, Adaptive, Adiabatic, BoundaryConditionDirichlet,
                                  BoundaryConditionNavierStokesWall, CFLBased, FluxHLL, Isothermal, NoSlip,
                                  boundary_condition_slip_wall_horizontal, boundary_condition_slip_wall_vertical,
@@ -33,5 +34,5 @@ __all__ = [
     "CompressibleNavierStokesDiffusion2D", "GradientVariablesConservative", "SemidiscretizationHyperbolicParabolic",
     "PositivityPreservingLimiterZhangShu", "density", "pressure", "density_pressure",
     "boundary_condition_slip_wall_vertical", "boundary_condition_slip_wall_horizontal", "NoSlip", "Adiabatic",
-    "Isothermal", "BoundaryConditionNavierStokesWall",
+    "Isothermal", "BoundaryConditionNavierStokesWall", "UnstructuredMesh2D",
 ]

@@ -301,15 +301,7 @@ class SemidiscretizationHyperbolic:
                  source_terms=None):
         if source_terms is not None:
             raise NotImplementedError("source terms are not built on the device path")
-        from .curved_mesh import CurvedMesh, RefinedStructuredMesh, StructuredMesh
-        if isinstance(mesh, (StructuredMesh, RefinedStructuredMesh)):
-            self.curved = mesh.curved(solver.polydeg)
-        elif isinstance(mesh, CurvedMesh):
-            self.curved = mesh
-        elif isinstance(mesh, (TreeMesh, RefinedTreeMesh)):
-            self.curved = None
-        else:
-            raise NotImplementedError("TreeMesh{2}, StructuredMesh{2} and curvilinear meshes (with L2 mortars) are built")
+        self.curved = self._curved_form(mesh, solver.polydeg)
         self.mesh = mesh
         self.equations = equations
         self.initial_condition = initial_condition
@@ -356,7 +348,57 @@ class SemidiscretizationHyperbolic:
     def handle(self):
         return self._handle.ptr
 
+    @staticmethod
+    def _curved_form(mesh, polydeg: int):
+        """The curvilinear form of a mesh (None for a TreeMesh)."""
+        from .curved_mesh import CurvedMesh, RefinedStructuredMesh, StructuredMesh
+        if isinstance(mesh, (StructuredMesh, RefinedStructuredMesh)):
+            return mesh.curved(polydeg)
+        if isinstance(mesh, CurvedMesh):
+            return mesh
+        if isinstance(mesh, (TreeMesh, RefinedTreeMesh)):
+            return None
+        raise NotImplementedError("TreeMesh{2}, StructuredMesh{2}, UnstructuredMesh2D and curvilinear meshes (with L2 "
+                                  "mortars) are built")
+
+    def remesh(self, mesh):
+        """The re-upload after an AMR step (what the drop-in does behind the reference's resize! of the integrator
+        and its caches, src/callbacks/amr.jl:2-208): the handle takes the new mesh's connectivity and element count,
+        sizes its buffers anew and drops its captured graphs; the state is set again by the caller (Trixi projects
+        it onto the new mesh on the host). Boundary conditions, the reconstruction and the positivity limiter carry
+        over; the mortar inverse Jacobian of the curvilinear shock-capturing blend goes back to zeros."""
+        curved = self._curved_form(mesh, self.polydeg)
+        if (curved is None) != (self.curved is None):
+            raise ValueError("remesh keeps the mesh family (TreeMesh or curvilinear)")
+        if mesh.n_boundaries:
+            bcs = digest_boundary_conditions(self.boundary_conditions)
+        self.curved = curved
+        self.mesh = mesh
+        self._upload_mesh()
+        vi = self.solver.volume_integral
+        if isinstance(vi, VolumeIntegralFRShockCapturing):
+            check(self.handle, lib().tlw_set_reconstruction(self.handle, vi.reconstruction_code))
+        self.node_coordinates = self.curved.xy if self.curved is not None else mesh.node_coordinates(self.polydeg)
+        self._bdata_key = None
+        self._bcs = bcs if mesh.n_boundaries else ()
+        if mesh.n_boundaries:
+            self._bnd_xy = mesh.boundary_node_coordinates(self.polydeg)
+            self._upload_boundary_kinds()
+
     def _upload_mesh(self):
+        if self.curved is not None and getattr(self.curved, "unstructured", False):
+            c = self.curved
+            Ja = np.ascontiguousarray(c.Ja, dtype=np.float64)
+            ij = np.ascontiguousarray(c.inverse_jacobian_nodes, dtype=np.float64)
+            nd = np.ascontiguousarray(c.normal_directions, dtype=np.float64)      # (E, 4, n, 2) = [2, n, 4, E]
+            arrs = (np.ascontiguousarray(c.element_ids.T, dtype=np.int64),         # [2, I] column-major
+                    np.ascontiguousarray(c.element_side_ids.T, dtype=np.int64),
+                    np.ascontiguousarray(c.start_index, dtype=np.int64),
+                    np.ascontiguousarray(c.index_increment, dtype=np.int64))
+            self._keep = (Ja, ij, nd) + arrs
+            check(self.handle, lib().tlw_set_unstructured_mesh(self.handle, c.n_elements, _ptr(Ja), _ptr(ij), _ptr(nd),
+                                                               c.n_interfaces, *[_ptr(a) for a in arrs]))
+            return
         if self.curved is not None:
             c = self.curved
             Ja = np.ascontiguousarray(c.Ja, dtype=np.float64)                     # [E, j, i, 4] = [4, i, j, E]
@@ -551,6 +593,13 @@ class SemidiscretizationHyperbolicParabolic(SemidiscretizationHyperbolic):
         super().__init__(mesh, get_time_discretization(solver), eq, initial_condition, solver, device=device,
                          boundary_conditions=bc_hyp, **kw)
         self.boundary_conditions_parabolic = bc_par
+        self._upload_parabolic()
+
+    def remesh(self, mesh):
+        """As SemidiscretizationHyperbolic.remesh, with the parabolic terms and walls uploaded again."""
+        if mesh.n_boundaries:
+            self._bcs_par = digest_boundary_conditions(self.boundary_conditions_parabolic)
+        super().remesh(mesh)
         self._upload_parabolic()
 
     def _upload_parabolic(self):
