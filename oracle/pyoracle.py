@@ -41,6 +41,7 @@ def lib():
         L.oracle_set_temporal_errors.argtypes = [P, i32, dbl, dbl]
         L.oracle_set_curved_mortar_jacobian.argtypes = [P, P]
         L.oracle_set_unstructured_normals.argtypes = [P, P]
+        L.oracle_dual_step.argtypes = [P, P, P, dbl, P, P]
         L.oracle_set_shock_capturing.argtypes = [P, i32, dbl, dbl, i32]
         L.oracle_set_reconstruction.argtypes = [P, i32]
         L.oracle_set_curved_mortars.argtypes = [P, i32, P, P, P, P, P, P]
@@ -253,6 +254,20 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(lib().oracle_last_error(self.h).decode())
         return out
+
+    def dual_step(self, u, dt, direction=None):
+        """One LW step of the scalar-templated restatement at a fixed dt (periodic TreeMesh, FR, Rusanov):
+        returns u + dt rhs(u), and with a direction also its directional derivative (forward-mode dual numbers)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        out = np.empty_like(u)
+        d = None if direction is None else np.ascontiguousarray(direction, dtype=np.float64)
+        dout = None if d is None else np.empty_like(u)
+        rc = lib().oracle_dual_step(self.h, _p(u), _p(d), float(dt), _p(out), _p(dout))
+        if rc == 4:
+            raise ValueError("dual step: periodic TreeMesh, FR volume integral, Rusanov flux and N >= 3 only")
+        if rc != 0:
+            raise RuntimeError(lib().oracle_last_error(self.h).decode())
+        return out if d is None else (out, dout)
 
     def step_fixed(self, u, dt, nthreads: int = 1):
         """One LW step u + dt rhs(u) at the given dt (returns a new array)."""

@@ -88,6 +88,55 @@ def test_oracle_multistep_gradient_matches_finite_differences(oracle_mod, tl):
         assert abs(g @ d - ref) <= 1e-5 * abs(ref)
 
 
+def forward_mode_directional(o, u0, dts, d, target):
+    """J'(u0) d for J = 1/2 ||rho(T) - target||^2 by dual numbers through the fixed-dt steps."""
+    u, t = u0, d
+    for dt in dts:
+        u, t = o.dual_step(u, dt, t)
+    return float(np.sum((u[0::4] - target) * t[0::4])), u
+
+
+@pytest.mark.parametrize("N,speed", [(3, 0), (4, 0), (4, 1), (5, 0)])
+def test_dual_step_restates_the_oracle_step(oracle_mod, tl, N, speed):
+    """The scalar-templated step in double is the oracle's step (to roundoff); its dual derivative is the step's
+    directional derivative (central differences)."""
+    eq, mesh, u = vortex(tl, 2, N, noise=1e-3)
+    o = oracle_mod.Oracle(mesh, N, speed_kind=speed)
+    dt = o.max_dt(u, 0.4)
+    ref = o.step_fixed(u, dt)
+    assert np.all(rel_l2(o.dual_step(u, dt), ref) < 1e-14)
+    d = np.random.default_rng(N).standard_normal(u.size)
+    val, der = o.dual_step(u, dt, d)
+    assert np.all(rel_l2(val, ref) < 1e-14)
+    h = 1e-6
+    fdd = (o.step_fixed(u + h * d, dt) - o.step_fixed(u - h * d, dt)) / (2 * h)
+    assert np.all(rel_l2(der, fdd) < 1e-7)
+
+
+def test_forward_mode_matches_the_oracle_adjoint_at_8x8(oracle_mod, tl):
+    """The differentiable form's second check (BASELINE: against forward-mode differentiation through the CPU
+    path on an 8 x 8 mesh): 20 fixed-dt steps, J = 1/2 ||rho(T) - rho_target||^2; dual-number directional
+    derivatives equal the oracle adjoint's dot products to 1e-10 relative on 16 random directions."""
+    eq, mesh, u0 = vortex(tl, 3, 4, noise=1e-3)
+    o = oracle_mod.Oracle(mesh, 4)
+    dts, u = [], u0.copy()
+    for _ in range(20):
+        dt = o.max_dt(u, 0.5)
+        dts.append(dt)
+        u = o.step_fixed(u, dt, nthreads=NTH)
+    target = np.random.default_rng(1).uniform(0.9, 1.1, u.size // 4)
+    lam_T = np.zeros_like(u)
+    lam_T[0::4] = u[0::4] - target
+    g = oracle_gradient(o, u0, dts, lam_T)
+    rng = np.random.default_rng(5)
+    for _ in range(16):
+        d = rng.standard_normal(u0.size)
+        d /= np.linalg.norm(d)
+        jd, uT = forward_mode_directional(o, u0, dts, d, target)
+        assert np.all(rel_l2(uT, u) < 1e-13)
+        assert abs(g @ d - jd) <= 1e-10 * abs(jd)
+
+
 def test_oracle_adjoint_rejects_unsupported(oracle_mod, tl):
     eq, mesh, u = vortex(tl, 2, 4)
     o = oracle_mod.Oracle(mesh, 4, flux_kind=1)
@@ -178,6 +227,28 @@ def test_gpu_objective_gradient_finite_differences(tl):
         d /= np.linalg.norm(d)
         ref = fd(Jf, u0, d, 1e-4)
         assert abs(g @ d - ref) <= 1e-6 * abs(ref) + 1e-14
+
+
+@pytest.mark.gpu
+def test_gpu_adjoint_matches_forward_mode_at_8x8(oracle_mod, tl):
+    """The device's checkpointed adjoint gradient on the 8 x 8, N = 4 vortex (200 steps of the workload's CFL,
+    checkpoints every 20; rho_target from a strength-4.5 run; u0 = strength 5 + N(0, 1e-3^2)) against dual-number
+    forward mode through the oracle's steps at the recorded dt sequence: 1e-10 relative on 8 random directions."""
+    eq, mesh, u0 = vortex(tl, 3, 4, beta=5.0, center=(0.0, 0.0), noise=1e-3)
+    semi = make_semi(tl, mesh, 4)
+    _, _, ut0 = vortex(tl, 3, 4, beta=4.5, center=(0.0, 0.0))
+    nsteps, cfl = 200, tl.trixi2lw(0.98, semi.solver)
+    target = tl.forward_record(semi, ut0, nsteps, cfl, 20)[0::4].copy()
+    J, g, uT = tl.adjoint_solve(semi, u0, nsteps, cfl, 20, target)
+    dts = tl.adjoint.dt_sequence(semi, nsteps)
+    o = oracle_mod.Oracle(mesh, 4)
+    rng = np.random.default_rng(11)
+    for _ in range(8):
+        d = rng.standard_normal(u0.size)
+        d /= np.linalg.norm(d)
+        jd, uT_cpu = forward_mode_directional(o, u0, dts, d, target)
+        assert np.all(rel_l2(uT, uT_cpu) < 1e-10)
+        assert abs(g @ d - jd) <= 1e-10 * abs(jd)
 
 
 @pytest.mark.gpu
