@@ -7,6 +7,10 @@ device every step. A step is one perform_step! (dt reduction + rhs + update) ove
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 
+Under torchrun with N > 1 ranks the default workload is one mesh split over the ranks (domain decomposition:
+space-filling-curve ranges, cut-face trace exchange and a MAX all-reduce of the CFL maximum over NCCL; strong
+scaling); --replicas runs N independent copies instead.
+
 One JSON line on rank 0. `value`: whole-job DOF-updates/s with the state resident in HBM (CUDA events on
 the library's stream around K graph-replayed steps, max over ranks). `e2e`: the same metric through
 the C ABI with host buffers (per step: pinned host -> device upload of u, one step, device -> host
@@ -32,6 +36,8 @@ METRIC = "LW-FR DOF-updates/s on 1 B200 (% HBM roofline); batched & adjoint vs p
 UNIT = "DOF-updates/s"
 
 DEFAULT_WORKLOAD = "vortex_tree512_N4_lw"
+# time discretizations of the domain-decomposed split step
+DECOMPOSED_TD = ("lw", "mdrk")
 # name -> (refinement level, N, time discretization, initial condition)
 WORKLOADS = {
     "vortex_tree512_N4_lw": (9, 4, "lw", "vortex"),
@@ -664,18 +670,21 @@ def run_decomposed(args):
 
     rank, local_rank, world = dist_env()
     torch.cuda.set_device(local_rank)
+    if "RANK" not in os.environ:   # one rank without torchrun
+        os.environ.update({"RANK": "0", "WORLD_SIZE": "1", "MASTER_ADDR": "127.0.0.1", "MASTER_PORT": "29511"})
     dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                             device_id=torch.device("cuda", local_rank))
     level, N, td, icname = WORKLOADS[args.workload]
-    if td != "lw" or icname not in ("vortex",):
-        raise SystemExit("--decompose: the periodic vortex LW workloads")
+    if td not in DECOMPOSED_TD or icname not in ("vortex",):
+        raise SystemExit("--decompose: the periodic vortex workloads")
     mesh = make_mesh(tl, level, icname)
     part = partition(mesh, world)[rank]
     eq = tl.CompressibleEulerEquations2D(1.4)
-    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.LW()))
-    semi = tl.SemidiscretizationHyperbolic(part.mesh, tl.LW(), eq, tl.IsentropicVortex(5.0), solver, device=local_rank)
+    tdo = tl.LW() if td == "lw" else tl.MDRK()
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tdo))
+    semi = tl.SemidiscretizationHyperbolic(part.mesh, tdo, eq, tl.IsentropicVortex(5.0), solver, device=local_rank)
     cfl = cfl_for(N)
-    integ = tl.LWIntegrator(tl.semidiscretize(semi, tl.LW(), (0.0, 1e9)))
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, tdo, (0.0, 1e9)))
     u0 = semi.compute_coefficients(0.0)
     integ.set_state(u0, 0.0)
     allreduce_max, exchange = torch_collectives()
@@ -724,7 +733,7 @@ def run_decomposed(args):
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "polydeg": N, "elements": mesh.n_elements, "ndofs": ndofs,
-                       "cfl": cfl, "parallelism": f"domain decomposition over {world} ranks (space-filling-curve "
+                       "time_discretization": td, "cfl": cfl, "parallelism": f"domain decomposition over {world} ranks (space-filling-curve "
                        "ranges; MAX all-reduce of the CFL maximum and cut-face trace exchange over NCCL)",
                        "halo_faces_rank0": int(len(part.halo_keys)),
                        "l2": "inputs larger than L2" if part_bytes > 126e6 else "state of a part may fit in L2"},
@@ -732,7 +741,8 @@ def run_decomposed(args):
                     "d2h_bytes_per_step": part_bytes, "steps": n_e2e, "note": "per rank: its part"},
             "clocks": clocks,
             # speed, dt, volume, x / y interfaces, and per class of cut faces one pack and one halo launch
-            "gpu_launches": args.steps * (5 + 2 * len({int(f) >> 1 for f in part.halo_faces})),
+            "gpu_launches": args.steps * (2 + (3 + 2 * len({int(f) >> 1 for f in part.halo_faces}))
+                                          * (2 if td == "mdrk" else 1)),
         }
         print(json.dumps(out), flush=True)
     dist.barrier()
@@ -1113,10 +1123,15 @@ def main():
     ap.add_argument("--fd-directions", type=int, default=64,
                     help="adjoint workload: random directions of the finite-difference gradient check")
     ap.add_argument("--decompose", action="store_true",
-                    help="under torchrun: split one mesh over the ranks (halo exchange over NCCL) instead of "
-                         "running independent replicas")
+                    help="split one mesh over the ranks (halo exchange over NCCL) also at one rank; under torchrun "
+                         "with more than one rank this is the default for the periodic vortex workloads")
+    ap.add_argument("--replicas", action="store_true",
+                    help="under torchrun: N independent replicas of the workload instead of one mesh split over the ranks")
     args = ap.parse_args()
-    if args.impl == "ours" and args.decompose:
+    world = dist_env()[2]
+    decomposable = args.workload in WORKLOADS and WORKLOADS[args.workload][3] == "vortex" and \
+        WORKLOADS[args.workload][2] in DECOMPOSED_TD
+    if args.impl == "ours" and decomposable and (args.decompose or (world > 1 and not args.replicas)):
         run_decomposed(args)
     elif args.impl == "reference":
         run_reference(args)

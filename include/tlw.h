@@ -220,6 +220,9 @@ int tlw_dd_buffers(tlw_handle* h, double** send, double** recv, unsigned long lo
 int tlw_dd_begin(tlw_handle* h, double cfl, double fixed_dt, double t_end);
 int tlw_dd_volume(tlw_handle* h);
 int tlw_dd_finish(tlw_handle* h);
+/* Rounds of tlw_dd_volume / exchange / tlw_dd_finish per step: 1 for LW, 2 for MDRK (stage 1 produces u*, stage 2
+ * the new state; each stage exchanges its own traces, the reference's two MPI exchanges of an MDRK step). */
+int32_t tlw_dd_stages(tlw_handle* h);
 
 /* L2 mortars of a curvilinear mesh after an AMR step (the reference's P4estMesh path: prolong2mortars! and
  * calc_mortar_flux!, src/solvers/dgsem_p4est/dg_2d.jl:395-603, with Trixi's mortar_fluxes_to_elements!), after

@@ -298,22 +298,26 @@ int oracle_adjoint_step(oracle_handle* h, const double* u, double dt, const doub
     }
 }
 
-// One LW step u_out = u + dt rhs(u) of the scalar-templated restatement (periodic TreeMesh, FR, Rusanov, N >= 3):
+// One step (kind 0 LW, 1 MDRK) u_out of the scalar-templated restatement (periodic TreeMesh, FR, Rusanov, N >= 3):
 // with dir == null in double; otherwise with dual numbers seeded by dir, and d_out = the step's directional
 // derivative along dir.
-int oracle_dual_step(oracle_handle* h, const double* u, const double* dir, double dt, double* u_out, double* d_out) {
+int oracle_dual_step(oracle_handle* h, int kind, const double* u, const double* dir, double dt, double* u_out,
+                     double* d_out) {
     try {
         if (h->curved || h->opt.flux_kind != RUSANOV || h->opt.shock_capturing || h->mesh.n_boundaries ||
             h->mesh.n_mortars || h->opt.N < 3)
             return 4;
         const size_t nd = (size_t)NV * h->basis.n * h->basis.n * h->mesh.n_elements;
+        const bool mdrk = kind == 1;
         if (!dir) {
-            lw_step_templated<double>(h->basis, h->eq.gamma, h->opt.speed_kind, h->mesh, h->opt.N, u, dt, u_out);
+            if (mdrk) mdrk_step_templated<double>(h->basis, h->eq.gamma, h->opt.speed_kind, h->mesh, u, dt, u_out);
+            else lw_step_templated<double>(h->basis, h->eq.gamma, h->opt.speed_kind, h->mesh, h->opt.N, u, dt, u_out);
             return 0;
         }
         std::vector<Dual> x(nd), y(nd);
         for (size_t k = 0; k < nd; ++k) x[k] = Dual(u[k], dir[k]);
-        lw_step_templated<Dual>(h->basis, h->eq.gamma, h->opt.speed_kind, h->mesh, h->opt.N, x.data(), dt, y.data());
+        if (mdrk) mdrk_step_templated<Dual>(h->basis, h->eq.gamma, h->opt.speed_kind, h->mesh, x.data(), dt, y.data());
+        else lw_step_templated<Dual>(h->basis, h->eq.gamma, h->opt.speed_kind, h->mesh, h->opt.N, x.data(), dt, y.data());
         for (size_t k = 0; k < nd; ++k) {
             u_out[k] = y[k].v;
             d_out[k] = y[k].d;

@@ -41,7 +41,7 @@ def lib():
         L.oracle_set_temporal_errors.argtypes = [P, i32, dbl, dbl]
         L.oracle_set_curved_mortar_jacobian.argtypes = [P, P]
         L.oracle_set_unstructured_normals.argtypes = [P, P]
-        L.oracle_dual_step.argtypes = [P, P, P, dbl, P, P]
+        L.oracle_dual_step.argtypes = [P, i32, P, P, dbl, P, P]
         L.oracle_set_shock_capturing.argtypes = [P, i32, dbl, dbl, i32]
         L.oracle_set_reconstruction.argtypes = [P, i32]
         L.oracle_set_curved_mortars.argtypes = [P, i32, P, P, P, P, P, P]
@@ -255,14 +255,15 @@ class Oracle:
             raise RuntimeError(lib().oracle_last_error(self.h).decode())
         return out
 
-    def dual_step(self, u, dt, direction=None):
-        """One LW step of the scalar-templated restatement at a fixed dt (periodic TreeMesh, FR, Rusanov):
-        returns u + dt rhs(u), and with a direction also its directional derivative (forward-mode dual numbers)."""
+    def dual_step(self, u, dt, direction=None, kind: int = 0):
+        """One step (kind 0 LW, 1 MDRK) of the scalar-templated restatement at a fixed dt (periodic TreeMesh, FR,
+        Rusanov): returns the new state, and with a direction also its directional derivative (forward-mode dual
+        numbers)."""
         u = np.ascontiguousarray(u, dtype=np.float64)
         out = np.empty_like(u)
         d = None if direction is None else np.ascontiguousarray(direction, dtype=np.float64)
         dout = None if d is None else np.empty_like(u)
-        rc = lib().oracle_dual_step(self.h, _p(u), _p(d), float(dt), _p(out), _p(dout))
+        rc = lib().oracle_dual_step(self.h, int(kind), _p(u), _p(d), float(dt), _p(out), _p(dout))
         if rc == 4:
             raise ValueError("dual step: periodic TreeMesh, FR volume integral, Rusanov flux and N >= 3 only")
         if rc != 0:

@@ -251,6 +251,79 @@ def test_gpu_adjoint_matches_forward_mode_at_8x8(oracle_mod, tl):
         assert abs(g @ d - jd) <= 1e-10 * abs(jd)
 
 
+def make_mdrk_semi(tl, mesh, N):
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.MDRK()))
+    return tl.SemidiscretizationHyperbolic(mesh, tl.MDRK(), eq, tl.IsentropicVortex(5.0), solver)
+
+
+def test_dual_mdrk_step_restates_the_oracle_step(oracle_mod, tl):
+    for N in (3, 4, 5):
+        eq, mesh, u = vortex(tl, 2, N, noise=1e-3)
+        o = oracle_mod.Oracle(mesh, N)
+        dt = o.max_dt(u, 0.4)
+        ref = u.copy()
+        o.steps(ref, 1, 0.4, 0.0, 1e9, kind=1, fixed_dt=dt)
+        assert np.all(rel_l2(o.dual_step(u, dt, kind=1), ref) < 1e-14)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N", [3, 4, 5])
+def test_gpu_mdrk_adjoint_step_matches_forward_mode(oracle_mod, tl, N):
+    """The discrete adjoint of one two-stage MDRK step (both stages, the jump in u^n at the interfaces of both,
+    the stage-2 time averages built on stage 1's F2 and U2) against dual-number directional derivatives."""
+    eq, mesh, u = vortex(tl, 3, N, noise=1e-3)
+    semi = make_mdrk_semi(tl, mesh, N)
+    o = oracle_mod.Oracle(mesh, N)
+    dt = o.max_dt(u, 0.4)
+    rng = np.random.default_rng(N)
+    lam = rng.standard_normal(u.size)
+    g = tl.adjoint_step(semi, lam, u, dt)
+    for _ in range(4):
+        d = rng.standard_normal(u.size)
+        _, der = o.dual_step(u, dt, d, kind=1)
+        assert abs(g @ d - lam @ der) <= 1e-11 * np.abs(lam).sum() * np.abs(der).max()
+        assert abs(g @ d - lam @ der) <= 1e-10 * abs(lam @ der)
+
+
+@pytest.mark.gpu
+def test_gpu_mdrk_fixed_dt_solve_matches_oracle(oracle_mod, tl):
+    eq, mesh, u0 = vortex(tl, 3, 4)
+    semi = make_mdrk_semi(tl, mesh, 4)
+    o = oracle_mod.Oracle(mesh, 4)
+    dts = [0.05, 0.04, 0.045]
+    u = u0.copy()
+    for dt in dts:
+        o.steps(u, 1, 0.4, 0.0, 1e9, kind=1, fixed_dt=dt)
+    assert np.all(rel_l2(tl.solve_dts(semi, u0, dts), u) < 1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ck", [1, 6, 40])
+def test_gpu_mdrk_gradient_matches_forward_mode(oracle_mod, tl, ck):
+    """The checkpointed MDRK gradient of J = 1/2 ||rho(T) - rho_target||^2 over 40 CFL steps on 8 x 8, N = 4,
+    against dual-number forward mode through the oracle's MDRK steps at the recorded dt sequence (1e-10), and the
+    same gradient for every checkpoint interval."""
+    eq, mesh, u0 = vortex(tl, 3, 4, beta=5.0, center=(0.0, 0.0), noise=1e-3)
+    semi = make_mdrk_semi(tl, mesh, 4)
+    _, _, ut0 = vortex(tl, 3, 4, beta=4.5, center=(0.0, 0.0))
+    nsteps, cfl = 40, 0.4
+    target = tl.forward_record(semi, ut0, nsteps, cfl, ck)[0::4].copy()
+    J, g, uT = tl.adjoint_solve(semi, u0, nsteps, cfl, ck, target)
+    dts = tl.adjoint.dt_sequence(semi, nsteps)
+    o = oracle_mod.Oracle(mesh, 4)
+    rng = np.random.default_rng(ck)
+    for _ in range(4):
+        d = rng.standard_normal(u0.size)
+        d /= np.linalg.norm(d)
+        u, t = u0, d
+        for dt in dts:
+            u, t = o.dual_step(u, dt, t, kind=1)
+        jd = float(np.sum((u[0::4] - target) * t[0::4]))
+        assert np.all(rel_l2(uT, u) < 1e-10)
+        assert abs(g @ d - jd) <= 1e-10 * abs(jd)
+
+
 @pytest.mark.gpu
 def test_torch_autograd_function(tl):
     import torch

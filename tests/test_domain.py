@@ -1,4 +1,4 @@
-"""Domain decomposition of the LW step over ranks (the reference's MPI path, src/solvers/dgsem_tree/
+"""Domain decomposition of the LW and MDRK steps over ranks (the reference's MPI path, src/solvers/dgsem_tree/
 dg_2d_parallel.jl): the partition's bookkeeping and the host collectives (world size 2 over gloo) on the CPU, and
 on one GPU the library's split step (tlw_dd_begin / _volume / _finish with the halo kernels) for 2 and 3 parts
 driven in lockstep in one process, equal to the single-domain run."""
@@ -98,14 +98,15 @@ def test_gloo_halo_exchange_world2():
 
 
 # ---------------------------------------------------------------------------------------------- GPU
-def _semi(tl, mesh, N, bc=None):
+def _semi(tl, mesh, N, bc=None, td="lw"):
     eq = tl.CompressibleEulerEquations2D(1.4)
-    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tl.LW()))
+    tdo = tl.LW() if td == "lw" else tl.MDRK()
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tdo))
     kw = {} if bc is None else {"boundary_conditions": bc}
     # with walls: a vortex at rest (no background flow into the walls)
     ic = (tl.IsentropicVortex(5.0, center=(0.3, -0.2)) if bc is None else
           tl.IsentropicVortex(3.0, center=(0.3, -0.2), domain=(-5.0, 5.0), velocity=(0.0, 0.0)))
-    return tl.SemidiscretizationHyperbolic(mesh, tl.LW(), eq, ic, solver, **kw)
+    return tl.SemidiscretizationHyperbolic(mesh, tdo, eq, ic, solver, **kw)
 
 
 def _lockstep(tl, parts, semis, steps, cfl):
@@ -127,43 +128,45 @@ def _lockstep(tl, parts, semis, steps, cfl):
         for d in dds:
             d.max_bits.fill_(m)
         torch.cuda.synchronize()
-        for d in dds:
-            _lib.check(d.semi.handle, L.tlw_dd_volume(d.semi.handle))
-        torch.cuda.synchronize()
-        for d in dds:
-            for q, (off, cnt) in d.part.segments.items():
-                oq, cq = dds[q].part.segments[d.part.rank]
-                d.recv[off:off + cnt].copy_(dds[q].send[oq:oq + cq])
-        torch.cuda.synchronize()
-        for d in dds:
-            _lib.check(d.semi.handle, L.tlw_dd_finish(d.semi.handle))
-        torch.cuda.synchronize()
+        for _stage in range(int(L.tlw_dd_stages(dds[0].semi.handle))):
+            for d in dds:
+                _lib.check(d.semi.handle, L.tlw_dd_volume(d.semi.handle))
+            torch.cuda.synchronize()
+            for d in dds:
+                for q, (off, cnt) in d.part.segments.items():
+                    oq, cq = dds[q].part.segments[d.part.rank]
+                    d.recv[off:off + cnt].copy_(dds[q].send[oq:oq + cq])
+            torch.cuda.synchronize()
+            for d in dds:
+                _lib.check(d.semi.handle, L.tlw_dd_finish(d.semi.handle))
+            torch.cuda.synchronize()
     return dds
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("nparts,N,walls", [(2, 4, False), (3, 3, False), (4, 4, True)])
-def test_gpu_split_step_equals_single_domain(tl, nparts, N, walls):
+@pytest.mark.parametrize("nparts,N,walls,td", [(2, 4, False, "lw"), (3, 3, False, "lw"), (4, 4, True, "lw"),
+                                               (2, 4, False, "mdrk"), (3, 5, False, "mdrk"), (4, 3, True, "mdrk")])
+def test_gpu_split_step_equals_single_domain(tl, nparts, N, walls, td):
     from trixilw.domain import partition
     mesh = tl.TreeMesh((-5.0, -5.0), (5.0, 5.0), 4, periodicity=not walls)
     bc = None
     if walls:
         bc = {"x_neg": tl.boundary_condition_slip_wall_vertical, "x_pos": tl.boundary_condition_slip_wall_vertical,
               "y_neg": tl.boundary_condition_slip_wall_horizontal, "y_pos": tl.boundary_condition_slip_wall_horizontal}
-    whole = _semi(tl, mesh, N, bc)
+    whole = _semi(tl, mesh, N, bc, td)
     u0 = whole.compute_coefficients(0.0)
-    integ = tl.LWIntegrator(tl.semidiscretize(whole, tl.LW(), (0.0, 1e9)))
+    integ = tl.LWIntegrator(tl.semidiscretize(whole, whole.time_discretization, (0.0, 1e9)))
     integ.set_state(u0, 0.0)
     steps, cfl = 6, 0.4
     integ.step(steps, cfl, use_graph=False)
     integ.sync_time()
     ref = integ.get_state()
     parts = partition(mesh, nparts)
-    semis = [_semi(tl, p.mesh, N, bc) for p in parts]
+    semis = [_semi(tl, p.mesh, N, bc, td) for p in parts]
     nn4 = 4 * (N + 1) ** 2
     integs = []
     for s, p in zip(semis, parts):
-        it = tl.LWIntegrator(tl.semidiscretize(s, tl.LW(), (0.0, 1e9)))
+        it = tl.LWIntegrator(tl.semidiscretize(s, s.time_discretization, (0.0, 1e9)))
         it.set_state(np.ascontiguousarray(u0.reshape(-1, nn4)[p.mesh.elements].reshape(-1)), 0.0)
         integs.append(it)
     _lockstep(tl, parts, semis, steps, cfl)

@@ -643,6 +643,226 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_re
     }
 }
 
+// ---- the two-stage MDRK step (mdrk.jl:1-29, rhs_mdrk1! / rhs_mdrk2!, src/solvers/dgsem_tree/multi_derivative_2d.jl)
+// Stage 1 at u: d = C(f(u)), P_q = u + a_q d (a = -1, +1, -2, +2), f_t = sum_q w_q f(P_q) (w = -8/12, 8/12, 1/12,
+// -1/12); Fh = f/2 + f_t/8, Uh = u/2 + d/8 feed the surface, F2 = f + f_t/6, U2 = u + d/6 go to stage 2;
+// u* = u + dt rhs_1. Stage 2 at u*: the same procedure, F = F2 + f*_t/3, U = U2 + d*/3, interfaces with the jump in
+// u^n; u_new = u + dt rhs_2. Both stages have the LW step's form x_out = u + dt rhs(.), so adj_interface_kernel
+// gives each stage's face adjoints (stage 2: U traces of stage 2, adjoint lam; stage 1: Uh traces, adjoint of u*).
+// adj_mdrk_volume_kernel<N, 2> turns lam into the adjoint of u* (out), of (F2, G2) and U2 (to stage 1), and
+// lam + the jump's direct term (lam_acc); adj_mdrk_volume_kernel<N, 1> takes the adjoint of u* as its lam and
+// writes lam_out = lam_acc + lam + (du*/du)^T-part of stage 1.
+struct AdjMdrkArgs {
+    const double* x;        // the stage's state: u^n (stage 1) or u* (stage 2)
+    const double* lam;      // adjoint of the stage's output: u_new (stage 2) or u* (stage 1)
+    const double* bF;       // face adjoints from adj_interface_kernel [v, l, face, e]
+    const double* bU;
+    const double* bu;
+    double* bF2;            // adjoint of (F2, G2) [v, d, node]: written by stage 2, read by stage 1
+    double* bU2;            // adjoint of U2 [v, node]
+    double* lam_acc;        // stage 2 writes lam + the jump's direct term; stage 1 adds it
+    double* out;            // stage 2: adjoint of u*; stage 1: the adjoint of u^n
+    const double* inv_jac;
+    const double* dt;
+    int E;
+    double gamma;
+};
+
+template <int N>
+struct AdjMdrkCfg {
+    static constexpr int n = N + 1, nn = n * n;
+    static constexpr int EB = VolCfg<N>::EB;
+    static constexpr int THREADS = VolCfg<N>::THREADS;
+    static constexpr int MIN_BLOCKS = THREADS <= 128 ? 3 : 1;
+    static constexpr int TILE = NV * EB * nn;
+    // D, Dhat and three tiles (X, Y, the adjoint of d)
+    static constexpr size_t smem_bytes() { return (size_t)(2 * nn + 3 * TILE) * sizeof(double); }
+};
+
+template <int N, int STAGE>
+static __global__ void __launch_bounds__(AdjMdrkCfg<N>::THREADS, AdjMdrkCfg<N>::MIN_BLOCKS)
+    adj_mdrk_volume_kernel(AdjMdrkArgs a) {
+    using C = AdjMdrkCfg<N>;
+    constexpr int n = C::n, nn = C::nn, EB = C::EB, TILE = C::TILE;
+    constexpr double A[4] = {-1.0, 1.0, -2.0, 2.0};
+    constexpr double W[4] = {-8.0 / 12.0, 8.0 / 12.0, 1.0 / 12.0, -1.0 / 12.0};
+    extern __shared__ double sm[];
+    double* sD = sm;
+    double* sDh = sm + nn;
+    double* X = sm + 2 * nn;
+    double* Y = X + TILE;
+    double* Bd = Y + TILE;
+    for (int k = threadIdx.x; k < nn; k += blockDim.x) {
+        sD[k] = c_tlw_D[N][k];
+        sDh[k] = c_tlw_Dhat[N][k];
+    }
+    const int el = threadIdx.x / nn;
+    const int node = threadIdx.x - el * nn;
+    const int i = node % n, j = node / n;
+    const long long e = (long long)blockIdx.x * EB + el;
+    const bool active = el < EB && e < a.E;
+    const bool in_tile = el < EB;
+    const int slot = in_tile ? el : 0;
+    const int me = slot * nn + node;
+    auto at = [&](double* T, int v) -> double* { return T + v * EB * nn + me; };
+    auto put = [&](double* T, int v, double x) {
+        if (in_tile) *at(T, v) = x;
+    };
+    auto cx = [&](const double* M, const double* F, int v) {
+        const double* p = F + v * EB * nn + slot * nn + n * j;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) s = fma(M[i * n + k], p[k], s);
+        return s;
+    };
+    auto cy = [&](const double* M, const double* F, int v) {
+        const double* p = F + v * EB * nn + slot * nn + i;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) s = fma(M[j * n + k], p[n * k], s);
+        return s;
+    };
+    auto cxt = [&](const double* M, const double* W_, int v) {
+        const double* p = W_ + v * EB * nn + slot * nn + n * j;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) s = fma(M[k * n + i], p[k], s);
+        return s;
+    };
+    auto cyt = [&](const double* M, const double* W_, int v) {
+        const double* p = W_ + v * EB * nn + slot * nn + i;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; ++k) s = fma(M[k * n + j], p[n * k], s);
+        return s;
+    };
+    double x[NV] = {1.0, 0.0, 0.0, 2.5};
+    double ij = 1.0;
+    const size_t off = (size_t)e * nn + node;
+    if (active) {
+        load4(a.x + off * NV, x);
+        ij = __ldg(a.inv_jac + e);
+    }
+    const double dt = *a.dt;
+    const double sc = -dt * ij;
+    const double gm1 = a.gamma - 1.0;
+    // forward: d = C(f(x), g(x))
+    {
+        double f[NV], g[NV];
+        euler_fluxes(gm1, x[0], x[1], x[2], x[3], f, g);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { put(X, v, f[v]); put(Y, v, g[v]); }
+    }
+    __syncthreads();
+    double d[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) d[v] = sc * (cx(sD, X, v) + cy(sD, Y, v));
+    __syncthreads();
+    // adjoint of the volume term sc (Dhat F + Dhat G), then the face traces
+    double lam[NV] = {0.0, 0.0, 0.0, 0.0};
+    if (active) load4(a.lam + off * NV, lam);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) put(X, v, sc * lam[v]);
+    __syncthreads();
+    double bF[NV], bG[NV], bU[NV] = {0.0, 0.0, 0.0, 0.0}, bud[NV] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { bF[v] = cxt(sDh, X, v); bG[v] = cyt(sDh, X, v); }
+    if (active) {
+        auto face = [&](int f, int l, double* tgt) {
+            const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
+            double y[NV];
+            load4(a.bF + t, y);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) tgt[v] += y[v];
+            load4(a.bU + t, y);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) bU[v] += y[v];
+            load4(a.bu + t, y);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) bud[v] += y[v];
+        };
+        if (i == 0) face(0, j, bF);
+        if (i == n - 1) face(1, j, bF);
+        if (j == 0) face(2, i, bG);
+        if (j == n - 1) face(3, i, bG);
+    }
+    // the stage's combination of f(x), f_t, x, d into its outputs
+    double bft[NV], bgt[NV], bf0[NV], bg0[NV], bx[NV], bd[NV];
+    if (STAGE == 2) {
+        // F = F2 + f_t / 3, U = U2 + d / 3
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            bft[v] = bF[v] * (1.0 / 3.0);
+            bgt[v] = bG[v] * (1.0 / 3.0);
+            bd[v] = bU[v] * (1.0 / 3.0);
+            bf0[v] = bg0[v] = bx[v] = 0.0;
+        }
+        if (active) {
+            store4(a.bF2 + off * 2 * NV, bF);
+            store4(a.bF2 + off * 2 * NV + NV, bG);
+            store4(a.bU2 + off * NV, bU);
+            double acc[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) acc[v] = lam[v] + bud[v];
+            store4(a.lam_acc + off * NV, acc);
+        }
+    } else {
+        // Fh = f/2 + f_t/8, Uh = x/2 + d/8; F2 = f + f_t/6, U2 = x + d/6
+        double b2f[NV] = {0.0, 0.0, 0.0, 0.0}, b2g[NV] = {0.0, 0.0, 0.0, 0.0}, b2u[NV] = {0.0, 0.0, 0.0, 0.0};
+        if (active) {
+            load4(a.bF2 + off * 2 * NV, b2f);
+            load4(a.bF2 + off * 2 * NV + NV, b2g);
+            load4(a.bU2 + off * NV, b2u);
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            bf0[v] = fma(0.5, bF[v], b2f[v]);
+            bg0[v] = fma(0.5, bG[v], b2g[v]);
+            bft[v] = fma(0.125, bF[v], b2f[v] * (1.0 / 6.0));
+            bgt[v] = fma(0.125, bG[v], b2g[v] * (1.0 / 6.0));
+            bx[v] = fma(0.5, bU[v], b2u[v]);
+            bd[v] = fma(0.125, bU[v], b2u[v] * (1.0 / 6.0));
+        }
+    }
+    // f_t = sum_q W_q f(x + A_q d)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        double P[NV], wf[NV], wg[NV], bP[NV] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            P[v] = fma(A[q], d[v], x[v]);
+            wf[v] = W[q] * bft[v];
+            wg[v] = W[q] * bgt[v];
+        }
+        euler_flux_vjp(a.gamma, P, wf, wg, bP);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            bx[v] += bP[v];
+            bd[v] = fma(A[q], bP[v], bd[v]);
+        }
+    }
+    // d = C(f(x), g(x))
+#pragma unroll
+    for (int v = 0; v < NV; ++v) put(Bd, v, bd[v]);
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { bf0[v] = fma(sc, cxt(sD, Bd, v), bf0[v]); bg0[v] = fma(sc, cyt(sD, Bd, v), bg0[v]); }
+    euler_flux_vjp(a.gamma, x, bf0, bg0, bx);
+    if (active) {
+        double o[NV];
+        if (STAGE == 2) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) o[v] = bx[v];
+        } else {
+            double acc[NV];
+            load4(a.lam_acc + off * NV, acc);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) o[v] = acc[v] + lam[v] + bx[v] + bud[v];
+        }
+        store4(a.out + off * NV, o);
+    }
+}
+
 // J = 1/2 sum_nodes (rho - rho_target)^2: per-block partial sums (fixed order) and the seed lam = (rho - rho_t, 0, 0, 0)
 constexpr int OBJ_THREADS = 256;
 static __global__ void __launch_bounds__(OBJ_THREADS) objective_kernel(const double* u, const double* target,
@@ -693,6 +913,29 @@ struct AL {
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VolCfg<N>::smem_bytes(4));
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, false, false, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VolCfg<N>::smem_bytes(4));
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)VolCfg<N>::smem_bytes(2));
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)VolCfg<N>::smem_bytes(2));
+        cudaFuncSetAttribute(adj_mdrk_volume_kernel<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)AdjMdrkCfg<N>::smem_bytes());
+        cudaFuncSetAttribute(adj_mdrk_volume_kernel<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)AdjMdrkCfg<N>::smem_bytes());
+    }
+    // the forward MDRK stages (stage 1: u -> u*, stage 2: u* -> u_new with u_base = u^n)
+    static void forward_mdrk_volume(cudaStream_t s, int stage, const VolArgs& va) {
+        using C = VolCfg<N>;
+        const int grid = (int)((va.E + C::EB - 1) / C::EB);
+        if (stage == 1) mdrk1_volume_kernel<N, MODE_STEP, false><<<grid, C::THREADS, C::smem_bytes(2), s>>>(va);
+        else mdrk2_volume_kernel<N, MODE_STEP, false><<<grid, C::THREADS, C::smem_bytes(2), s>>>(va);
+    }
+    static void adjoint_mdrk(cudaStream_t s, int stage, const AdjSurfArgs& sa, const AdjMdrkArgs& ma) {
+        const long long th = (long long)(sa.nx + sa.ny) * (N + 1);
+        if (th) adj_interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(sa);
+        using C = AdjMdrkCfg<N>;
+        const int grid = (ma.E + C::EB - 1) / C::EB;
+        if (stage == 2) adj_mdrk_volume_kernel<N, 2><<<grid, C::THREADS, C::smem_bytes(), s>>>(ma);
+        else adj_mdrk_volume_kernel<N, 1><<<grid, C::THREADS, C::smem_bytes(), s>>>(ma);
     }
     // with va.dstore: also store the stage derivatives for the adjoint
     static void forward_volume(cudaStream_t s, int mode, const VolArgs& va) {
@@ -758,17 +1001,25 @@ double* seg_trace(tlw_handle* h, int b, int j) {
     return h->adj.d_segU + ((size_t)b * h->adj.capacity_states + j) * ntrace(h);
 }
 double* seg_D(tlw_handle* h, int b, int j) {
-    return h->adj.d_segD + ((size_t)b * h->adj.capacity_states + j) * depth(h) * nstate(h);
+    return h->adj.d_segD ? h->adj.d_segD + ((size_t)b * h->adj.capacity_states + j) * depth(h) * nstate(h) : nullptr;
+}
+bool is_mdrk(const tlw_handle* h) { return h->opts.time_discretization == TLW_MDRK; }
+// MDRK: step j's stage state u* and stage-2 U traces (null for LW)
+double* seg_ustar(tlw_handle* h, int b, int j) {
+    return h->adj.d_segS ? h->adj.d_segS + ((size_t)b * h->adj.capacity_states + j) * nstate(h) : nullptr;
+}
+double* seg_trace2(tlw_handle* h, int b, int j) {
+    return h->adj.d_segU2 ? h->adj.d_segU2 + ((size_t)b * h->adj.capacity_states + j) * ntrace(h) : nullptr;
 }
 
 int adj_ready(tlw_handle* h) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh) return afail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
-    if (h->opts.time_discretization != TLW_LW || h->sc || h->opts.surface_flux != TLW_FLUX_RUSANOV || h->nb > 0 || h->curved ||
-        h->N < 3 || h->N > 5 || h->nmx + h->nmy > 0 || h->parabolic || h->lim_count > 0)
+    if (h->sc || h->opts.surface_flux != TLW_FLUX_RUSANOV || h->nb > 0 || h->curved || h->N < 3 || h->N > 5 ||
+        h->nmx + h->nmy > 0 || h->parabolic || h->lim_count > 0)
         return afail(h, TLW_E_UNSUPPORTED,
-                     "adjoint: LW, FR volume integral, Rusanov flux, periodic conforming TreeMesh, Euler, N = 3..5, "
-                     "no positivity limiter");
+                     "adjoint: LW or MDRK, FR volume integral, Rusanov flux, periodic conforming TreeMesh, Euler, "
+                     "N = 3..5, no positivity limiter");
     TLW_ACUDA(h, cudaSetDevice(h->device));
     AdjointBuffers& A = h->adj;
     if (!A.const_uploaded) {
@@ -793,6 +1044,14 @@ int adj_ready(tlw_handle* h) {
         TLW_ACUDA(h, cudaMalloc(&A.d_bu, ntrace(h) * sizeof(double)));
         const size_t blocks = ((size_t)h->nn * h->E + OBJ_THREADS - 1) / OBJ_THREADS;
         TLW_ACUDA(h, cudaMalloc(&A.d_work, (blocks + 8) * sizeof(double)));
+    }
+    if (is_mdrk(h) && !A.d_bus) {
+        TLW_ACUDA(h, cudaMalloc(&A.d_mus, nstate(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_mtU2, ntrace(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_bus, nstate(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_bF2, 2 * nstate(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_bU2, nstate(h) * sizeof(double)));
+        TLW_ACUDA(h, cudaMalloc(&A.d_lamacc, nstate(h) * sizeof(double)));
     }
     if (!A.s_rec) {
         // the reverse sweep's two streams: the adjoint chain (the critical path) above the recomputation in
@@ -836,11 +1095,19 @@ int ensure_steps(tlw_handle* h, int nsteps, int ck) {
         dfree(A.d_seg);
         dfree(A.d_segU);
         dfree(A.d_segD);
+        dfree(A.d_segS);
+        dfree(A.d_segU2);
         A.capacity_states = A.capacity_buffers = 0;
         A.last_resident = false;
         TLW_ACUDA(h, cudaMalloc(&A.d_seg, nbuf * (size_t)(ck + 1) * nstate(h) * sizeof(double)));
         TLW_ACUDA(h, cudaMalloc(&A.d_segU, nbuf * (size_t)ck * ntrace(h) * sizeof(double)));
-        TLW_ACUDA(h, cudaMalloc(&A.d_segD, nbuf * (size_t)ck * depth(h) * nstate(h) * sizeof(double)));
+        if (is_mdrk(h)) {
+            // the MDRK adjoint recomputes the stage derivatives; it keeps u* and the stage-2 U traces instead
+            TLW_ACUDA(h, cudaMalloc(&A.d_segS, nbuf * (size_t)ck * nstate(h) * sizeof(double)));
+            TLW_ACUDA(h, cudaMalloc(&A.d_segU2, nbuf * (size_t)ck * ntrace(h) * sizeof(double)));
+        } else {
+            TLW_ACUDA(h, cudaMalloc(&A.d_segD, nbuf * (size_t)ck * depth(h) * nstate(h) * sizeof(double)));
+        }
         A.capacity_states = ck;
         A.capacity_buffers = nbuf;
     }
@@ -893,9 +1160,29 @@ SurfArgs fwd_surf_args(tlw_handle* h, const double* u, double* out, const double
     return sa;
 }
 
-// one forward LW step on stream s at the dt stored at dtp; U traces into tU, stage derivatives into dstore
+// one forward step on stream s at the dt stored at dtp. LW: U traces into tU, stage derivatives into dstore. MDRK:
+// the stage state u* into us and the stage-1 / stage-2 U traces into tU / tU2 (scratch when null)
 void enqueue_fixed_step(tlw_handle* h, cudaStream_t s, const double* u, double* unew, double* tU, const double* dtp,
-                        double* dstore = nullptr) {
+                        double* dstore = nullptr, double* us = nullptr, double* tU2 = nullptr) {
+    if (is_mdrk(h)) {
+        if (!us) us = h->adj.d_mus;
+        if (!tU2) tU2 = h->adj.d_mtU2;
+        VolArgs v1 = fwd_vol_args(h, u, us, tU, dtp);
+        v1.U2 = h->d_U2;
+        v1.F2 = h->d_F2;
+        VolArgs v2 = fwd_vol_args(h, us, unew, tU2, dtp);
+        v2.u_base = u;
+        v2.U2 = h->d_U2;
+        v2.F2 = h->d_F2;
+        adj_degree(h->N, [&](auto Nc) {
+            constexpr int N = decltype(Nc)::value;
+            AL<N>::forward_mdrk_volume(s, 1, v1);
+            AL<N>::forward_interfaces(s, fwd_surf_args(h, u, us, tU, dtp, 1), h);
+            AL<N>::forward_mdrk_volume(s, 2, v2);
+            AL<N>::forward_interfaces(s, fwd_surf_args(h, u, unew, tU2, dtp, 1), h);
+        });
+        return;
+    }
     VolArgs va = fwd_vol_args(h, u, unew, tU, dtp);
     va.dstore = dstore;
     const SurfArgs sa = fwd_surf_args(h, u, unew, tU, dtp, 1);
@@ -906,10 +1193,62 @@ void enqueue_fixed_step(tlw_handle* h, cudaStream_t s, const double* u, double* 
     });
 }
 
-// lam_out = (du_new/du)^T lam_in for the step from u at dt (*dtp); tU = that step's forward U traces
+// lam_out = (du_new/du)^T lam_in for the step from u at dt (*dtp); tU = that step's forward U traces (MDRK: its
+// stage-1 traces, with us = u* and tU2 = the stage-2 traces)
 void enqueue_adjoint_step(tlw_handle* h, const double* u, const double* tU, const double* dtp, const double* lam_in,
-                          double* lam_out, const double* dstore = nullptr, cudaStream_t s = nullptr) {
+                          double* lam_out, const double* dstore = nullptr, cudaStream_t s = nullptr,
+                          const double* us = nullptr, const double* tU2 = nullptr) {
     AdjointBuffers& A = h->adj;
+    if (is_mdrk(h)) {
+        AdjSurfArgs sa{};
+        sa.u = u;   // both stages' jumps are in u^n
+        sa.bF = A.d_bF;
+        sa.bU = A.d_bU;
+        sa.bu = A.d_bu;
+        sa.xl = h->d_xl; sa.xr = h->d_xr; sa.yl = h->d_yl; sa.yr = h->d_yr;
+        sa.nx = h->nx; sa.ny = h->ny;
+        sa.inv_jac = h->d_inv_jac;
+        sa.dt = dtp;
+        sa.gamma = h->opts.gamma;
+        sa.speed_kind = h->opts.max_speed;
+        sa.inv_w_first = h->h_basis.inv_w_first;
+        sa.inv_w_last = h->h_basis.inv_w_last;
+        sa.status = &h->d_step->status;
+        AdjMdrkArgs ma{};
+        ma.bF = A.d_bF;
+        ma.bU = A.d_bU;
+        ma.bu = A.d_bu;
+        ma.bF2 = A.d_bF2;
+        ma.bU2 = A.d_bU2;
+        ma.lam_acc = A.d_lamacc;
+        ma.inv_jac = h->d_inv_jac;
+        ma.dt = dtp;
+        ma.E = (int)h->E;
+        ma.gamma = h->opts.gamma;
+        adj_degree(h->N, [&](auto Nc) {
+            constexpr int N = decltype(Nc)::value;
+            cudaStream_t st = s ? s : h->stream;
+            // stage 2: lam -> adjoint of u*, (F2, G2), U2, lam + jump term
+            AdjSurfArgs s2 = sa;
+            s2.tU = tU2;
+            s2.lam = lam_in;
+            AdjMdrkArgs m2 = ma;
+            m2.x = us;
+            m2.lam = lam_in;
+            m2.out = A.d_bus;
+            AL<N>::adjoint_mdrk(st, 2, s2, m2);
+            // stage 1: the adjoint of u* -> the adjoint of u^n
+            AdjSurfArgs s1 = sa;
+            s1.tU = tU;
+            s1.lam = A.d_bus;
+            AdjMdrkArgs m1 = ma;
+            m1.x = u;
+            m1.lam = A.d_bus;
+            m1.out = lam_out;
+            AL<N>::adjoint_mdrk(st, 1, s1, m1);
+        });
+        return;
+    }
     AdjSurfArgs sa{};
     sa.u = u;
     sa.tU = tU;
@@ -1010,10 +1349,18 @@ int tlw_adjoint_step(tlw_handle* h, double* lam_out, const double* lam_in, const
     if ((rc = ensure_given_dts(h, 1))) return rc;
     if ((rc = copy_in(h, A.d_seg, u, ns, where)) || (rc = copy_in(h, A.d_lam[0], lam_in, ns, where))) return rc;
     TLW_ACUDA(h, cudaMemcpyAsync(A.d_dts_given, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    // forward rhs for the U traces (du into lam[1] as scratch), then the adjoint
-    const VolArgs va = fwd_vol_args(h, A.d_seg, A.d_lam[1], A.d_segU, A.d_dts_given);
-    adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::forward_volume(h->stream, MODE_RHS, va); });
-    enqueue_adjoint_step(h, A.d_seg, A.d_segU, A.d_dts_given, A.d_lam[0], A.d_lam[1]);
+    // forward rhs for the U traces (du into lam[1] as scratch), then the adjoint; MDRK: the whole step (u*, both
+    // stages' U traces)
+    if (is_mdrk(h)) {
+        enqueue_fixed_step(h, h->stream, A.d_seg, A.d_lam[1], A.d_segU, A.d_dts_given, nullptr, seg_ustar(h, 0, 0),
+                           seg_trace2(h, 0, 0));
+        enqueue_adjoint_step(h, A.d_seg, A.d_segU, A.d_dts_given, A.d_lam[0], A.d_lam[1], nullptr, nullptr,
+                             seg_ustar(h, 0, 0), seg_trace2(h, 0, 0));
+    } else {
+        const VolArgs va = fwd_vol_args(h, A.d_seg, A.d_lam[1], A.d_segU, A.d_dts_given);
+        adj_degree(h->N, [&](auto Nc) { AL<decltype(Nc)::value>::forward_volume(h->stream, MODE_RHS, va); });
+        enqueue_adjoint_step(h, A.d_seg, A.d_segU, A.d_dts_given, A.d_lam[0], A.d_lam[1]);
+    }
     if ((rc = copy_out(h, lam_out, A.d_lam[1], ns, where))) return rc;
     return adj_status(h);
 }
@@ -1080,7 +1427,7 @@ int tlw_forward_record(tlw_handle* h, const double* u0, int32_t nsteps, double c
                                          h->stream));
             if (in_last) {
                 enqueue_fixed_step(h, h->stream, u, seg_state(h, bl, j + 1), seg_trace(h, bl, j), A.d_dts + k,
-                                   seg_D(h, bl, j));
+                                   seg_D(h, bl, j), seg_ustar(h, bl, j), seg_trace2(h, bl, j));
             } else {
                 enqueue_fixed_step(h, h->stream, s0, k + 1 == last ? seg_state(h, bl, 0) : s1, h->d_tU, A.d_dts + k);
                 std::swap(s0, s1);
@@ -1171,9 +1518,10 @@ int reverse_sweep_enqueue(tlw_handle* h, int& cur, double* phase_ms) {
             TLW_ACUDA(h, cudaMemcpyAsync(seg_state(h, b, 0), A.d_ckpt + (size_t)sgi * nstate(h),
                                          nstate(h) * sizeof(double), cudaMemcpyDeviceToDevice, sr));
             for (int j = 0; j < len; ++j) {
-                if (j + 1 < len) {
+                if (j + 1 < len || is_mdrk(h)) {
+                    // (MDRK: the last step too, for its u* and both stages' traces; its output goes to the spare slot)
                     enqueue_fixed_step(h, sr, seg_state(h, b, j), seg_state(h, b, j + 1), seg_trace(h, b, j),
-                                       A.d_dts + start + j, seg_D(h, b, j));
+                                       A.d_dts + start + j, seg_D(h, b, j), seg_ustar(h, b, j), seg_trace2(h, b, j));
                 } else {
                     // the segment's output state is not needed, only the U traces and stage derivatives of its
                     // last step (volume kernel alone, its du into the free state slot)
@@ -1193,7 +1541,7 @@ int reverse_sweep_enqueue(tlw_handle* h, int& cur, double* phase_ms) {
             if (overlap && !(resident && sgi == nseg - 1)) TLW_ACUDA(h, cudaStreamWaitEvent(sa, A.ev_ready[b], 0));
             for (int j = len - 1; j >= 0; --j) {
                 enqueue_adjoint_step(h, seg_state(h, b, j), seg_trace(h, b, j), A.d_dts + start + j, A.d_lam[cur],
-                                     A.d_lam[1 - cur], seg_D(h, b, j), sa);
+                                     A.d_lam[1 - cur], seg_D(h, b, j), sa, seg_ustar(h, b, j), seg_trace2(h, b, j));
                 cur ^= 1;
             }
             if (overlap) TLW_ACUDA(h, cudaEventRecord(A.ev_free[b], sa));

@@ -1069,8 +1069,8 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
 int tlw_set_halo(tlw_handle* h, int64_t n_halo, const int64_t* elements, const int32_t* faces) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh || h->curved) return fail(h, TLW_E_STATE, "halo faces follow tlw_set_tree_mesh");
-    if (n_halo > 0 && (h->opts.time_discretization != TLW_LW || h->sc || h->parabolic || h->nmx + h->nmy > 0))
-        return fail(h, TLW_E_UNSUPPORTED, "domain decomposition: LW, FR volume integral, conforming TreeMesh, Euler");
+    if (n_halo > 0 && (h->sc || h->parabolic || h->nmx + h->nmy > 0))
+        return fail(h, TLW_E_UNSUPPORTED, "domain decomposition: LW or MDRK, FR volume integral, conforming TreeMesh, Euler");
     if (n_halo < 0 || (n_halo > 0 && (!elements || !faces))) return fail(h, TLW_E_ARG, "halo faces");
     std::vector<int> he[2], hf[2], hs[2];
     std::vector<signed char> seen((size_t)h->E * 4, 0);
@@ -1126,6 +1126,7 @@ int tlw_dd_begin(tlw_handle* h, double cfl, double fixed_dt, double t_end) {
     TLW_CUDA(h, cudaSetDevice(h->device));
     double params[3] = {t_end, cfl, fixed_dt};
     TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->t_end, params, sizeof(params), cudaMemcpyHostToDevice, h->stream));
+    h->dd_stage = 0;   // a step starts with its first stage
     // this part's maximum; the caller reduces it over the ranks (MAX) before tlw_dd_volume
     const double* u = h->d_state[h->cur];
     dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, true, false,
@@ -1134,13 +1135,23 @@ int tlw_dd_begin(tlw_handle* h, double cfl, double fixed_dt, double t_end) {
     return TLW_OK;
 }
 
+int32_t tlw_dd_stages(tlw_handle* h) {
+    return (h && h->opts.time_discretization == TLW_MDRK) ? 2 : 1;
+}
+
 int tlw_dd_volume(tlw_handle* h) {
     int rc = check_ready(h);
     if (rc) return rc;
     TLW_CUDA(h, cudaSetDevice(h->device));
-    finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
     const double* u = h->d_state[h->cur];
-    enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, h->d_state[1 - h->cur], &h->d_step->dt, nullptr, true, 1);
+    double* unew = h->d_state[1 - h->cur];
+    if (h->dd_stage == 0) finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
+    if (h->opts.time_discretization == TLW_LW)
+        enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, &h->d_step->dt, nullptr, true, 1);
+    else if (h->dd_stage == 0)   // MDRK stage 1 into u*, stage 2 from u* (the jumps are in u^n in both)
+        enqueue_rhs(h, TLW_STAGE_MDRK1, MODE_STEP, u, u, u, h->d_us, &h->d_step->dt, nullptr, true, 1);
+    else
+        enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, &h->d_step->dt, nullptr, true, 1);
     TLW_CUDA(h, cudaGetLastError());
     return TLW_OK;
 }
@@ -1151,8 +1162,19 @@ int tlw_dd_finish(tlw_handle* h) {
     TLW_CUDA(h, cudaSetDevice(h->device));
     const double* u = h->d_state[h->cur];
     double* unew = h->d_state[1 - h->cur];
-    enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, &h->d_step->dt, nullptr, true, 2);
-    enqueue_limiter(h, unew, 2, nullptr);
+    if (h->opts.time_discretization == TLW_LW) {
+        enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, &h->d_step->dt, nullptr, true, 2);
+        enqueue_limiter(h, unew, 2, nullptr);
+    } else if (h->dd_stage == 0) {
+        enqueue_rhs(h, TLW_STAGE_MDRK1, MODE_STEP, u, u, u, h->d_us, &h->d_step->dt, nullptr, true, 2);
+        h->dd_stage = 1;
+        TLW_CUDA(h, cudaGetLastError());
+        return TLW_OK;
+    } else {
+        enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, &h->d_step->dt, nullptr, true, 2);
+        enqueue_limiter(h, unew, 1, nullptr);
+        h->dd_stage = 0;
+    }
     TLW_CUDA(h, cudaGetLastError());
     h->cur ^= 1;
     return TLW_OK;

@@ -43,6 +43,13 @@ struct AdjointBuffers {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
     cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
     double* d_work = nullptr;               // scratch (objective partial sums)
+    // MDRK: per step of a segment buffer the stage state u* and the stage-2 U traces (besides the step's state and
+    // stage-1 U traces); scratch for steps outside the segment buffers; the stage adjoints (u*, (F2, G2), U2, and
+    // the adjoint of u_new with the stage-2 jump term)
+    double* d_segS = nullptr;               // [buffers][capacity_states] states u*
+    double* d_segU2 = nullptr;              // [buffers][capacity_states] stage-2 U traces
+    double *d_mus = nullptr, *d_mtU2 = nullptr;
+    double *d_bus = nullptr, *d_bF2 = nullptr, *d_bU2 = nullptr, *d_lamacc = nullptr;
     double* d_final = nullptr;              // u(T) of the recorded run (one of the handle's state buffers)
     int rec_steps = 0, rec_ck = 0;          // recorded forward run: steps, checkpoint interval
     // the forward and reverse sweeps as CUDA graphs, keyed by (steps, interval); dropped whenever a buffer
@@ -57,6 +64,8 @@ inline void free_adjoint(AdjointBuffers& a) {
     if (a.g_rev) cudaGraphExecDestroy(a.g_rev);
     dfree(a.d_lam[0]); dfree(a.d_lam[1]); dfree(a.d_bF); dfree(a.d_bU); dfree(a.d_bu); dfree(a.d_dts);
     dfree(a.d_dts_given); dfree(a.d_ckpt); dfree(a.d_seg); dfree(a.d_segU); dfree(a.d_segD); dfree(a.d_work);
+    dfree(a.d_segS); dfree(a.d_segU2); dfree(a.d_mus); dfree(a.d_mtU2);
+    dfree(a.d_bus); dfree(a.d_bF2); dfree(a.d_bU2); dfree(a.d_lamacc);
     for (cudaEvent_t ev : {a.ev_fork, a.ev_join, a.ev_join2, a.ev_ready[0], a.ev_ready[1], a.ev_free[0], a.ev_free[1]})
         if (ev) cudaEventDestroy(ev);
     if (a.s_rec) cudaStreamDestroy(a.s_rec);
@@ -130,6 +139,7 @@ struct tlw_handle {
     // faces shared with other ranks' parts (domain decomposition): x-faces [0, nhx), y-faces [nhx, nh); local
     // element, face, position in the caller's order; send / receive buffers [halo][l][12]
     int nh = 0, nhx = 0;
+    int dd_stage = 0;                       // split step: the MDRK stage in progress (0: stage 1, 1: stage 2)
     int *d_he = nullptr, *d_hf = nullptr, *d_hs = nullptr;
     double *d_send = nullptr, *d_recv = nullptr;
     // per element: the faces (0..3) through which it is the large element of a mortar, in mortar order

@@ -6,8 +6,9 @@ ParallelTreeMesh partitions the leaves. Its part is a TreeMesh of the local elem
 them and its share of the boundaries; the faces it shares with another rank's part are its halo faces. A step
 (``DomainDecomposedLW.step``) is: this part's CFL maximum, a MAX all-reduce of it over the ranks, the volume
 kernel with the halo traces (u, U, F.n per node, 12 doubles, the reference's 3 nv message) packed into a send
-buffer, the halo exchange with the neighbouring ranks, then the interfaces, boundaries and halo faces. All of it
-runs on the library's stream; the collectives are ordered on that stream.
+buffer, the halo exchange with the neighbouring ranks, then the interfaces, boundaries and halo faces; an MDRK
+step does the volume / exchange / surface round once per stage. All of it runs on the library's stream; the
+collectives are ordered on that stream.
 """
 from __future__ import annotations
 
@@ -152,15 +153,17 @@ class DomainDecomposedLW:
 
         h = self.semi.handle
         L = lib()
+        stages = int(L.tlw_dd_stages(h))
         for _ in range(int(nsteps)):
             check(h, L.tlw_dd_begin(h, float(cfl), float(fixed_dt), float(t_end)))
             with torch.cuda.stream(self.stream):
                 self.allreduce_max(self.max_bits)
-            check(h, L.tlw_dd_volume(h))
-            if self.send is not None:
-                with torch.cuda.stream(self.stream):
-                    self.exchange(self.send, self.recv, self.part.segments)
-            check(h, L.tlw_dd_finish(h))
+            for _stage in range(stages):   # MDRK: stage 1 (into u*), then stage 2, each with its own exchange
+                check(h, L.tlw_dd_volume(h))
+                if self.send is not None:
+                    with torch.cuda.stream(self.stream):
+                        self.exchange(self.send, self.recv, self.part.segments)
+                check(h, L.tlw_dd_finish(h))
 
 
 def torch_collectives(group=None):
