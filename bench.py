@@ -102,6 +102,16 @@ def volume_kernel_bytes_per_element(N: int, td: str, curved: bool = False, sc: b
     return 8.0 * b
 
 
+def surface_pass_bytes_per_element(N: int) -> float:
+    """Algorithmic (unique) bytes of one element-centric surface launch per element: read the element's own U
+    and F.n face traces (2 x 4 faces x n x nv), read its 4(n - 1) face nodes of u for the jumps, read-modify-write
+    the same face nodes of the output, write two CFL slots. The neighbours' traces and face nodes are the
+    neighbours' own bytes, counted once there."""
+    n, nv = N + 1, 4
+    nb = 4 * (n - 1)
+    return 8.0 * (2 * 4 * n * nv + 3 * nb * nv + 2)
+
+
 def ns_volume_bytes_per_element(N: int) -> float:
     """Algorithmic bytes of the Navier-Stokes launches before the surfaces, per element on a curvilinear mesh:
     the BR1 gradient (read u, Ja, J^-1; write both gradients) and the parabolic LW volume kernel (read u, both
@@ -584,6 +594,22 @@ def run_ours(args):
                     {"achieved": None, "peak": fp64_peak, "unit": "TFLOP/s",
                      "note": "no algorithmic flop model for the Navier-Stokes or the shock-capturing kernels"})
         binding = fp64_rec if fp64_bound else hbm_rec
+        # a TreeMesh whose every face is an interface or a boundary runs one element-centric surface launch per
+        # stage (surface_kernel); other meshes run the x and y sweeps
+        surf_pass = not curved and not ns and getattr(semi.mesh, "n_mortars", 0) == 0
+        stages = 2 if td == "mdrk" else 1
+        surf_ms = (phase[2] + phase[3]) / args.steps
+        phases_rec = {"cfl_dt": phase[0] / args.steps, "volume": phase[1] / args.steps, "surfaces": surf_ms,
+                      "step": phase[4] / args.steps}
+        surf_rec = None
+        if surf_pass:
+            sb = surface_pass_bytes_per_element(N) * E
+            sgbs = sb / (surf_ms / stages * 1e-3) / 1e9
+            surf_rec = {"kernel": f"surface_kernel<{N}>", "ms_per_launch": surf_ms / stages,
+                        "alg_bytes_per_launch": sb, "achieved": sgbs, "unit": "GB/s", "frac": sgbs / peak,
+                        "traffic": profile_traffic(f"surface_kernel_N{N}_tree{1 << level}")}
+        else:
+            phases_rec.update({"x_faces": phase[2] / args.steps, "y_faces": phase[3] / args.steps})
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -605,14 +631,12 @@ def run_ours(args):
                          "step": {"alg_bytes_per_step": step_alg,
                                   "achieved_gbs": step_alg * args.steps / (ms_max * 1e-3) / 1e9,
                                   "frac": step_alg * args.steps / (ms_max * 1e-3) / 1e9 / peak},
-                         "phase_ms_per_step": {"cfl_dt": phase[0] / args.steps, "volume": phase[1] / args.steps,
-                                               "x_faces": phase[2] / args.steps, "y_faces": phase[3] / args.steps,
-                                               "step": phase[4] / args.steps}},
+                         "phase_ms_per_step": phases_rec,
+                         **({"surface": surf_rec} if surf_rec else {})},
             "clocks": clocks,
             "gpu_launches": args.steps * ((9 + 2 * int(L.tlw_curved_colors(semi.handle))) if ns else
                                           (5 + int(L.tlw_curved_colors(semi.handle))) if icname == "blast" else
-                                          (2 + (3 + (2 if semi.mesh.n_boundaries else 0)) * (2 if td == "mdrk" else 1)
-                                           + (1 if icname == "riemann" else 0))),
+                                          (2 + 2 * stages + (1 if icname == "riemann" else 0))),
         }
         if world == 1 and not args.no_cpu_baseline:
             rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=args.steps)
@@ -656,7 +680,7 @@ def run_decomposed(args):
     """Strong scaling of one TreeMesh over the ranks: each rank owns a contiguous range of the elements'
     space-filling-curve order and steps with the library's split step (tlw_dd_begin / _volume / _finish);
     the CFL maximum is all-reduced (MAX) and the cut-face traces exchanged with the neighbouring ranks over
-    NCCL, both ordered on the library's stream. value = the whole mesh's DOF-updates over the max-over-ranks
+    NCCL on the library's comm stream (the exchange overlaps the part's x interfaces). value = the whole mesh's DOF-updates over the max-over-ranks
     device time."""
     import datetime
 
@@ -699,9 +723,9 @@ def run_decomposed(args):
     dist.barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(dd.stream)
+    ev0.record(dd.lib_stream)
     dd.step(args.steps, cfl)
-    ev1.record(dd.stream)
+    ev1.record(dd.lib_stream)
     torch.cuda.synchronize()
     dist.barrier()
     clocks = sampler.stop()
@@ -715,12 +739,12 @@ def run_decomposed(args):
     dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(dd.stream)
+    e0.record(dd.lib_stream)
     for _ in range(n_e2e):
         integ.set_state(uh, 0.0)
         dd.step(1, cfl)
         uh[:] = integ.get_state()
-    e1.record(dd.stream)
+    e1.record(dd.lib_stream)
     torch.cuda.synchronize()
     t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -205,15 +205,24 @@ int tlw_set_unstructured_mesh(tlw_handle* h, int64_t n_elements, const double* c
  * message per cut face node: the u face value, U trace and F.n trace, 3 nv doubles, dg_parallel.jl:12-13). A rank
  * uploads its part of the TreeMesh with tlw_set_tree_mesh (local elements, the interfaces between them, its
  * boundaries) and lists its cut faces here: elements 1-based local, faces 0: -x, 1: +x, 2: -y, 3: +y, in the
- * order of its send / receive buffers ([halo][l][12] doubles, tlw_dd_buffers; a neighbour's send buffer
- * segment lands in this rank's receive buffer at the same positions). LW, FR volume integral, conforming
- * TreeMesh, Euler. A step is then
- *   tlw_dd_begin(h, cfl, fixed_dt, t_end)  this part's CFL maximum into *max_bits (a non-negative double's bits)
- *   caller: allreduce(MAX) of *max_bits over the ranks (uint64)
- *   tlw_dd_volume(h)                       dt, the volume kernel, this part's cut-face traces into send
+ * order of its send / receive buffers ([halo][l][tlw_dd_halo_values] doubles, tlw_dd_buffers; a neighbour's
+ * send buffer segment lands in this rank's receive buffer at the same positions). LW or MDRK, conforming
+ * TreeMesh, Euler, with the FR volume integral or shock capturing. A step is then
+ *   tlw_dd_begin(h, cfl, fixed_dt, t_end)  this part's CFL maximum into *max_bits (a non-negative double's bits);
+ *                                          with shock capturing also the raw alpha of each cut face's element
+ *                                          into the alpha send buffer (tlw_dd_alpha_buffers, [halo] doubles)
+ *   caller: allreduce(MAX) of *max_bits over the ranks (uint64); with shock capturing send / receive the
+ *           alpha buffers (same segments, one double per cut face)
+ *   tlw_dd_volume(h)                       (the alpha smoothing across the part's interfaces and cut faces) dt,
+ *                                          the volume kernel, this part's cut-face traces into send, then the x
+ *                                          faces inside the part (they overlap the exchange)
  *   caller: send / receive the halo buffers
- *   tlw_dd_finish(h)                       interfaces, boundaries, cut faces; the new state becomes current
- * all asynchronous on the handle's stream (tlw_get_stream): the caller orders its collectives on that stream.
+ *   tlw_dd_finish(h)                       the x cut faces, y interfaces, boundaries and cut faces; the new state
+ *                                          becomes current
+ * all asynchronous. The caller enqueues its collectives on the comm stream (tlw_dd_comm_stream): each tlw_dd_*
+ * call first waits for what the caller enqueued there, and the comm stream continues after tlw_dd_begin's work
+ * and after tlw_dd_volume's packing, so the exchange runs beside the part's x interfaces (the reference overlaps
+ * its MPI exchange with the local interface fluxes the same way, dg_2d_parallel.jl:209-320).
  * tlw_step / tlw_step_timed / tlw_rhs refuse a handle with cut faces. */
 int tlw_set_halo(tlw_handle* h, int64_t n_halo, const int64_t* elements, const int32_t* faces);
 int tlw_dd_buffers(tlw_handle* h, double** send, double** recv, unsigned long long** max_bits);
@@ -223,6 +232,17 @@ int tlw_dd_finish(tlw_handle* h);
 /* Rounds of tlw_dd_volume / exchange / tlw_dd_finish per step: 1 for LW, 2 for MDRK (stage 1 produces u*, stage 2
  * the new state; each stage exchanges its own traces, the reference's two MPI exchanges of an MDRK step). */
 int32_t tlw_dd_stages(tlw_handle* h);
+/* Doubles per cut face node in the halo buffers: 12 (u, U, F.n), or 20 with shock capturing (and the element's
+ * first-order subcell flux next to the face, fn_low, and its smoothed alpha, padded to 20), so that a cut face is blended as an
+ * interface inside one part is (compute_alp, src/solvers/dgsem_tree/dg_2d.jl:1879-1901) and the decomposed run
+ * equals the undecomposed one; the reference's calc_mpi_interface_flux! (dg_2d_parallel.jl:370-420) applies the
+ * plain LW flux there. */
+int32_t tlw_dd_halo_values(tlw_handle* h);
+/* The alpha send / receive buffers of the shock-capturing split step ([halo] doubles, null without shock
+ * capturing), exchanged between tlw_dd_begin and tlw_dd_volume. */
+int tlw_dd_alpha_buffers(tlw_handle* h, double** send, double** recv);
+/* The stream the caller's collectives of the split step go on (a cudaStream_t; created by tlw_set_halo). */
+int tlw_dd_comm_stream(tlw_handle* h, void** stream);
 
 /* L2 mortars of a curvilinear mesh after an AMR step (the reference's P4estMesh path: prolong2mortars! and
  * calc_mortar_flux!, src/solvers/dgsem_p4est/dg_2d.jl:395-603, with Trixi's mortar_fluxes_to_elements!), after
@@ -420,10 +440,11 @@ int tlw_batch_get_state(tlw_batch* b, int32_t instance, double* u, int32_t where
 int tlw_batch_step(tlw_batch* b, int32_t nsteps, int32_t use_graph);
 int tlw_batch_synchronize(tlw_batch* b);
 int tlw_batch_get_stream(tlw_batch* b, void** stream);
-/* Times the launch variants on this batch (elements per CTA of the volume kernel per degree group, CTA size of
- * the interface kernels, degree groups serial or concurrent) and keeps the fastest. choices_out (optional,
- * 2 * groups + 1 ints): per group (volume variant, interface CTA size), then the concurrency flag. The
- * current state is not changed. */
+/* Times the launch variants on this batch (elements per CTA of the volume kernel per degree group, the
+ * element-centric surface pass or the x / y interface sweeps and their CTA size, degree groups serial or
+ * concurrent) and keeps the fastest; every variant gives the same bits. choices_out (optional, 2 * groups + 1
+ * ints): per group (volume variant, interface CTA size or 0 for the surface pass), then the concurrency flag.
+ * The current state is not changed. */
 int tlw_batch_autotune(tlw_batch* b, int32_t trials, int32_t* choices_out);
 int32_t tlw_batch_num_groups(tlw_batch* b);
 const char* tlw_batch_last_error(tlw_batch* b);

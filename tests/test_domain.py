@@ -1,7 +1,8 @@
 """Domain decomposition of the LW and MDRK steps over ranks (the reference's MPI path, src/solvers/dgsem_tree/
 dg_2d_parallel.jl): the partition's bookkeeping and the host collectives (world size 2 over gloo) on the CPU, and
-on one GPU the library's split step (tlw_dd_begin / _volume / _finish with the halo kernels) for 2 and 3 parts
-driven in lockstep in one process, equal to the single-domain run."""
+on one GPU the library's split step (tlw_dd_begin / _volume / _finish with the halo kernels) for 2 to 4 parts
+driven in lockstep in one process, equal bit for bit to the single-domain run, with the FR volume integral and
+with shock capturing (alpha smoothed across the cut faces, cut faces blended)."""
 import os
 import socket
 
@@ -67,16 +68,25 @@ def _gloo_worker(rank, world, port, result):
         allreduce_max, exchange = torch_collectives()
         # what a rank sends for global face k, node l, value c: a code of (k, l, c, sender)
         H = len(part.halo_keys)
-        code = lambda k, r: (np.asarray(k)[:, None, None] * 1000.0 + np.arange(n)[None, :, None] * 10.0
-                             + np.arange(12)[None, None, :] * 0.01 + r * 0.0001)
-        send = torch.tensor(code(part.halo_keys, rank))
-        recv = torch.zeros(H, n, 12, dtype=torch.float64)
+        ok_x = len(part.segments) >= 1
+        # the trace buffers (12 values a node; 20 with shock capturing) and the [H] alpha buffer
+        for vals in (12, 20):
+            code = lambda k, r: (np.asarray(k)[:, None, None] * 1000.0 + np.arange(n)[None, :, None] * 10.0
+                                 + np.arange(vals)[None, None, :] * 0.01 + r * 0.0001)
+            send = torch.tensor(code(part.halo_keys, rank))
+            recv = torch.zeros(H, n, vals, dtype=torch.float64)
+            exchange(send, recv, part.segments)
+            expect = np.empty((H, n, vals))
+            for q, (off, cnt) in part.segments.items():
+                expect[off:off + cnt] = code(part.halo_keys[off:off + cnt], q)
+            ok_x = ok_x and bool(np.array_equal(recv.numpy(), expect))
+        send = torch.tensor(part.halo_keys * 10.0 + rank)
+        recv = torch.zeros(H, dtype=torch.float64)
         exchange(send, recv, part.segments)
-        others = [q for q in part.segments]
-        expect = np.empty((H, n, 12))
+        expect = np.empty(H)
         for q, (off, cnt) in part.segments.items():
-            expect[off:off + cnt] = code(part.halo_keys[off:off + cnt], q)
-        ok_x = bool(np.array_equal(recv.numpy(), expect)) and len(others) >= 1
+            expect[off:off + cnt] = part.halo_keys[off:off + cnt] * 10.0 + q
+        ok_x = ok_x and bool(np.array_equal(recv.numpy(), expect))
         # the CFL maximum: bits of non-negative doubles reduce like int64
         mine = np.array([1.5 + rank], dtype=np.float64).view(np.int64)
         t = torch.tensor(mine)
@@ -98,13 +108,22 @@ def test_gloo_halo_exchange_world2():
 
 
 # ---------------------------------------------------------------------------------------------- GPU
-def _semi(tl, mesh, N, bc=None, td="lw"):
+def _square(x, y, t, eq):
+    """A density square moving diagonally: discontinuous, so the indicator blends along its edges."""
+    rho = np.where((np.abs(x - 0.3) < 2.0) & (np.abs(y + 0.2) < 2.0), 2.0, 1.0)
+    return eq.prim2cons(rho, 0.5, 0.3, 1.0)
+
+
+def _semi(tl, mesh, N, bc=None, td="lw", sc=False):
     eq = tl.CompressibleEulerEquations2D(1.4)
     tdo = tl.LW() if td == "lw" else tl.MDRK()
-    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tdo))
+    vi = tl.VolumeIntegralFR(tdo)
+    if sc:
+        vi = tl.VolumeIntegralFRShockCapturing(tl.IndicatorHennemannGassner(alpha_max=0.5), vi)
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, vi)
     kw = {} if bc is None else {"boundary_conditions": bc}
     # with walls: a vortex at rest (no background flow into the walls)
-    ic = (tl.IsentropicVortex(5.0, center=(0.3, -0.2)) if bc is None else
+    ic = (_square if sc else tl.IsentropicVortex(5.0, center=(0.3, -0.2)) if bc is None else
           tl.IsentropicVortex(3.0, center=(0.3, -0.2), domain=(-5.0, 5.0), velocity=(0.0, 0.0)))
     return tl.SemidiscretizationHyperbolic(mesh, tdo, eq, ic, solver, **kw)
 
@@ -127,6 +146,10 @@ def _lockstep(tl, parts, semis, steps, cfl):
         m = torch.max(torch.cat([d.max_bits for d in dds]))
         for d in dds:
             d.max_bits.fill_(m)
+            if d.alpha_send is not None:   # shock capturing: the neighbours' raw alpha of the cut faces
+                for q, (off, cnt) in d.part.segments.items():
+                    oq, cq = dds[q].part.segments[d.part.rank]
+                    d.alpha_recv[off:off + cnt].copy_(dds[q].alpha_send[oq:oq + cq])
         torch.cuda.synchronize()
         for _stage in range(int(L.tlw_dd_stages(dds[0].semi.handle))):
             for d in dds:
@@ -144,16 +167,20 @@ def _lockstep(tl, parts, semis, steps, cfl):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("nparts,N,walls,td", [(2, 4, False, "lw"), (3, 3, False, "lw"), (4, 4, True, "lw"),
-                                               (2, 4, False, "mdrk"), (3, 5, False, "mdrk"), (4, 3, True, "mdrk")])
-def test_gpu_split_step_equals_single_domain(tl, nparts, N, walls, td):
+@pytest.mark.parametrize("nparts,N,walls,td,sc", [(2, 4, False, "lw", False), (3, 3, False, "lw", False),
+                                                  (4, 4, True, "lw", False), (2, 4, False, "mdrk", False),
+                                                  (3, 5, False, "mdrk", False), (4, 3, True, "mdrk", False),
+                                                  (2, 4, False, "lw", True), (3, 3, False, "lw", True),
+                                                  (4, 4, False, "mdrk", True)])
+def test_gpu_split_step_equals_single_domain(tl, nparts, N, walls, td, sc):
+    from trixilw import _lib
     from trixilw.domain import partition
     mesh = tl.TreeMesh((-5.0, -5.0), (5.0, 5.0), 4, periodicity=not walls)
     bc = None
     if walls:
         bc = {"x_neg": tl.boundary_condition_slip_wall_vertical, "x_pos": tl.boundary_condition_slip_wall_vertical,
               "y_neg": tl.boundary_condition_slip_wall_horizontal, "y_pos": tl.boundary_condition_slip_wall_horizontal}
-    whole = _semi(tl, mesh, N, bc, td)
+    whole = _semi(tl, mesh, N, bc, td, sc)
     u0 = whole.compute_coefficients(0.0)
     integ = tl.LWIntegrator(tl.semidiscretize(whole, whole.time_discretization, (0.0, 1e9)))
     integ.set_state(u0, 0.0)
@@ -161,8 +188,11 @@ def test_gpu_split_step_equals_single_domain(tl, nparts, N, walls, td):
     integ.step(steps, cfl, use_graph=False)
     integ.sync_time()
     ref = integ.get_state()
+    if sc:   # the blending reaches the cut faces
+        alpha = whole.get_cache(_lib.TLW_CACHE_ALPHA)
+        assert alpha.max() > 0.1 and (alpha == 0.0).sum() > 0
     parts = partition(mesh, nparts)
-    semis = [_semi(tl, p.mesh, N, bc, td) for p in parts]
+    semis = [_semi(tl, p.mesh, N, bc, td, sc) for p in parts]
     nn4 = 4 * (N + 1) ** 2
     integs = []
     for s, p in zip(semis, parts):

@@ -951,6 +951,14 @@ struct AL {
         }
     }
     static void forward_interfaces(cudaStream_t s, SurfArgs sa, const tlw_handle* h) {
+        if (h->d_nbr && h->nb == 0 && h->nmx + h->nmy == 0 && h->nh == 0) {
+            // the element-centric pass the plain step uses on a periodic mesh (same bits)
+            sa.nbr = h->d_nbr;
+            sa.E = (int)h->E;
+            using C = SurfCfg<N>;
+            surface_kernel<N, false, false><<<(unsigned)((sa.E + C::EB - 1) / C::EB), C::THREADS, 0, s>>>(sa, BndArgs{});
+            return;
+        }
         sa.left = h->d_xl; sa.right = h->d_xr; sa.count = h->nx; sa.orientation = 1;
         long long th = (long long)sa.count * (N + 1);
         if (th) interface_kernel<N><<<(unsigned)((th + 127) / 128), 128, 0, s>>>(sa);

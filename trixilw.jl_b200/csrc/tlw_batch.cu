@@ -8,9 +8,10 @@
 // into per-instance dt / t (each instance keeps its own CFL number and final time, exactly as if it ran
 // alone). A whole step of all groups - CFL pass, dt, volume, x and y interfaces - is captured once as a
 // CUDA graph and replayed, so a step of 512 instances costs a handful of launches instead of thousands.
-// The autotuner times, on the actual batch, the elements-per-CTA variant of the volume kernel per degree,
-// the interface CTA size, and whether the degree groups run one after another or concurrently on separate
-// streams (graph branches), and keeps the fastest.
+// The autotuner times, on the actual batch, the elements-per-CTA variant of the volume kernel per degree, the
+// element-centric surface pass against the x / y interface sweeps at two CTA sizes (all give the same bits),
+// and whether the degree groups run one after another or concurrently on separate streams (graph branches),
+// and keeps the fastest.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,7 +47,8 @@ struct Group {
     int *d_xl = nullptr, *d_xr = nullptr, *d_yl = nullptr, *d_yr = nullptr;
     int nx = 0, ny = 0;
     int eb_variant = 0;                     // 0: default elements per CTA, 1: the alternative
-    int ifc_block = 128;
+    int ifc_block = 0;                      // 0: the element-centric surface pass, else the sweeps' CTA size
+    int* d_nbr = nullptr;                   // the element across each face (every face an interface)
     Basis basis{};
 };
 
@@ -119,6 +121,10 @@ struct BLaunch {
                 <<<(unsigned)((a.E + C::EB - 1) / C::EB), C::THREADS, C::smem_bytes(4), s>>>(a);
         }
     }
+    static void surfaces(cudaStream_t s, const SurfArgs& a) {
+        using C = SurfCfg<N>;
+        surface_kernel<N, false, false><<<(unsigned)((a.E + C::EB - 1) / C::EB), C::THREADS, 0, s>>>(a, BndArgs{});
+    }
     static void interfaces(cudaStream_t s, int block, const SurfArgs& a) {
         const long long threads = (long long)a.count * (N + 1);
         if (threads == 0) return;
@@ -185,6 +191,12 @@ void enqueue_group_update(tlw_batch* b, Group& g, int from, cudaStream_t s) {
     with_degree(g.N, [&](auto Nc) {
         constexpr int N = decltype(Nc)::value;
         BLaunch<N>::volume(s, g.eb_variant, va);
+        if (g.ifc_block == 0 && g.d_nbr) {
+            sa.nbr = g.d_nbr;
+            sa.E = (int)g.E;
+            BLaunch<N>::surfaces(s, sa);
+            return;
+        }
         sa.left = g.d_xl; sa.right = g.d_xr; sa.count = g.nx; sa.orientation = 1;
         BLaunch<N>::interfaces(s, g.ifc_block, sa);
         sa.left = g.d_yl; sa.right = g.d_yr; sa.count = g.ny; sa.orientation = 2;
@@ -298,7 +310,7 @@ int tlw_batch_destroy(tlw_batch* b) {
     drop_batch_graphs(b);
     for (Group& g : b->groups) {
         dfree(g.d_state[0]); dfree(g.d_state[1]); dfree(g.d_tU); dfree(g.d_tF); dfree(g.d_inv_jac);
-        dfree(g.d_inst); dfree(g.d_xl); dfree(g.d_xr); dfree(g.d_yl); dfree(g.d_yr);
+        dfree(g.d_inst); dfree(g.d_xl); dfree(g.d_xr); dfree(g.d_yl); dfree(g.d_yr); dfree(g.d_nbr);
     }
     dfree(b->d_max); dfree(b->d_dt); dfree(b->d_t); dfree(b->d_t_end); dfree(b->d_cfl); dfree(b->d_steps);
     dfree(b->d_nnodes); dfree(b->d_step);
@@ -381,6 +393,20 @@ int tlw_batch_finalize(tlw_batch* b) {
             return rc;
         g.nx = (int)xl.size();
         g.ny = (int)yl.size();
+        if ((int64_t)(xl.size() + yl.size()) == 2 * g.E) {
+            // every face an interface: the element-centric surface pass (the element across each face)
+            std::vector<int> nbr((size_t)4 * g.E, -1);
+            bool ok = true;
+            auto put = [&](int e, int f, int other) {
+                int& slot = nbr[(size_t)4 * e + f];
+                if (slot != -1) ok = false;
+                slot = other;
+            };
+            for (size_t k = 0; k < xl.size(); ++k) { put(xl[k], 1, xr[k]); put(xr[k], 0, xl[k]); }
+            for (size_t k = 0; k < yl.size(); ++k) { put(yl[k], 3, yr[k]); put(yr[k], 2, yl[k]); }
+            if (ok && (rc = up_i(g.d_nbr, nbr))) return rc;
+        }
+        if (!g.d_nbr) g.ifc_block = 128;
         const size_t sd = (size_t)NV * g.nn * g.E, td = (size_t)NV * g.n * 4 * g.E;
         TLW_BCUDA(b, cudaMalloc(&g.d_state[0], sd * sizeof(double)));
         TLW_BCUDA(b, cudaMalloc(&g.d_state[1], sd * sizeof(double)));
@@ -511,9 +537,10 @@ int tlw_batch_autotune(tlw_batch* b, int32_t trials, int32_t* choices_out) {
     int gi = 0;
     for (Group& g : b->groups) {
         float best = 1e30f;
-        int bv = 0, bb = 128;
+        int bv = 0, bb = g.ifc_block;
         for (int v = 0; v < 2; ++v)
-            for (int blk : {128, 256}) {
+            for (int blk : {0, 128, 256}) {
+                if (blk == 0 && !g.d_nbr) continue;
                 g.eb_variant = v;
                 g.ifc_block = blk;
                 const float ms = time_group(g);

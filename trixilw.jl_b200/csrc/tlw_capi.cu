@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <new>
 #include <string>
 #include <vector>
@@ -53,7 +54,7 @@ void drop_graphs(tlw_handle* h) {
 void free_mesh(tlw_handle* h) {
     drop_graphs(h);
     dfree(h->d_inv_jac);
-    dfree(h->d_xl); dfree(h->d_xr); dfree(h->d_yl); dfree(h->d_yr);
+    dfree(h->d_xl); dfree(h->d_xr); dfree(h->d_yl); dfree(h->d_yr); dfree(h->d_nbr);
     dfree(h->d_b_elem); dfree(h->d_b_dir); dfree(h->d_bx); dfree(h->d_by);
     dfree(h->d_levels); dfree(h->d_now);
     if (h->d_bkind) { cudaFree(h->d_bkind); h->d_bkind = nullptr; }
@@ -85,7 +86,7 @@ void free_mesh(tlw_handle* h) {
     h->face_used.clear();
     for (int** d : {&h->d_he, &h->d_hf, &h->d_hs})
         if (*d) { cudaFree(*d); *d = nullptr; }
-    dfree(h->d_send); dfree(h->d_recv);
+    dfree(h->d_send); dfree(h->d_recv); dfree(h->d_asend); dfree(h->d_arecv);
     h->nh = h->nhx = 0;
     if (h->d_cbe) { cudaFree(h->d_cbe); h->d_cbe = nullptr; }
     if (h->d_cbf) { cudaFree(h->d_cbf); h->d_cbf = nullptr; }
@@ -123,6 +124,9 @@ template <int N> struct Vol {
     static void run(cudaStream_t s, int st, int m, bool sc, const VolArgs& a) { Launch<N>::volume(s, st, m, sc, a); }
 };
 template <int N> struct Ifc { static void run(cudaStream_t s, const SurfArgs& a) { Launch<N>::interfaces(s, a); } };
+template <int N> struct Srf {
+    static void run(cudaStream_t s, const SurfArgs& a, const BndArgs& b) { Launch<N>::surfaces(s, a, b); }
+};
 template <int N> struct Bnd { static void run(cudaStream_t s, const BndArgs& a) { Launch<N>::boundaries(s, a); } };
 template <int N> struct Par {
     static void run(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out, const double* dtp) {
@@ -193,6 +197,14 @@ bool use_slots(const tlw_handle* h) {
            h->nb == 0 && h->nmx + h->nmy == 0 && h->nh == 0;
 }
 
+// one element-centric pass for all faces instead of the x and y interface sweeps
+#ifndef TLW_SURFACE_PASS
+#define TLW_SURFACE_PASS 1
+#endif
+bool use_surface_pass(const tlw_handle* h) {
+    return TLW_SURFACE_PASS && h->d_nbr && !h->curved && h->nmx + h->nmy == 0 && h->nh == 0;
+}
+
 // the halo faces of one class (cls 0: x, 1: y) as kernel arguments
 HaloArgs halo_args(tlw_handle* h, int cls, int mode, const double* u_jump, double* out, const double* dt_ptr) {
     HaloArgs a{};
@@ -217,6 +229,14 @@ HaloArgs halo_args(tlw_handle* h, int cls, int mode, const double* u_jump, doubl
     a.inv_w_first = h->h_basis.inv_w_first;
     a.inv_w_last = h->h_basis.inv_w_last;
     a.status = &h->d_step->status;
+    a.values = h->halo_values;
+    if (h->sc) {
+        a.alpha = h->d_alpha;
+        a.tFn = h->d_tFn;
+        a.jac_first = h->jac_first;
+        a.w_first = h->h_basis.weights[0];
+        a.w_last = h->h_basis.weights[h->n - 1];
+    }
     return a;
 }
 
@@ -375,10 +395,12 @@ BndArgs boundary_args(tlw_handle* h, int stage, int mode, const double* u_jump, 
     return ba;
 }
 
-// phases: 1 the volume kernel (and the halo packing), 2 the surfaces (and the halo faces), 3 both
+// phases: 1 the volume kernel (and the halo packing); 2 the surfaces up to the x faces inside the part (x
+// interfaces, boundaries, mortars; everything on meshes without cut faces); 4 the x cut faces and the y faces.
+// 7: all of it. The split step runs 1 | 2 before the exchange and 4 after it.
 void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const double* u_jump, const double* u_base,
                  double* out, const double* dt_ptr, const PhaseEvents* ev = nullptr, bool alpha_ready = false,
-                 int phases = 3) {
+                 int phases = 7) {
     if (h->sc && !alpha_ready) enqueue_indicator(h, u_jump, false);   // indicator of the instantaneous u
     if (h->parabolic) {
         // BR1 gradients, parabolic LW volume kernel, then the interfaces with the viscous traces
@@ -404,6 +426,16 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
         sp.inv_w_last = h->h_basis.inv_w_last;
         sp.status = &h->d_step->status;
         BndArgs bp = boundary_args(h, stage, mode, u_jump, out, dt_ptr);
+        if (use_surface_pass(h)) {
+            sp.nbr = h->d_nbr;
+            sp.E = (int)h->E;
+            dispatch<Srf>(h->N, h->stream, sp, bp);
+            if (ev) {
+                cudaEventRecord(ev->after_x, h->stream);
+                cudaEventRecord(ev->after_y, h->stream);
+            }
+            return;
+        }
         sp.left = h->d_xl; sp.right = h->d_xr; sp.count = h->nx; sp.orientation = 1;
         dispatch<Ifc>(h->N, h->stream, sp);
         bp.bidx = h->d_bx; bp.count = h->nbx; bp.orientation = 1;
@@ -457,8 +489,9 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
         for (int cls = 0; cls < 2 && h->nh > 0; ++cls)
             dispatch<Halo>(h->N, h->stream, halo_args(h, cls, mode, u_jump, out, dt_ptr), true);
     }
-    if (!(phases & 2)) return;
+    if (!(phases & 6)) return;
     if (h->curved) {
+        if (!(phases & 2)) return;
         // MDRK stage 1 scales the Dirichlet time averages by 1/2, as the P4estMesh path does
         // (src/solvers/dgsem_tree/multi_derivative_2d.jl:34)
         enqueue_curved_surfaces(h, mode, u_jump, out, dt_ptr, ev, stage == TLW_STAGE_MDRK1 ? 0.5 : 1.0);
@@ -505,15 +538,29 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     ma.inv_w_first = h->h_basis.inv_w_first;
     ma.inv_w_last = h->h_basis.inv_w_last;
     ma.status = &h->d_step->status;
-    sa.left = h->d_xl; sa.right = h->d_xr; sa.count = h->nx; sa.orientation = 1;
-    dispatch<Ifc>(h->N, h->stream, sa);
-    ba.bidx = h->d_bx; ba.count = h->nbx; ba.orientation = 1;
-    dispatch<Bnd>(h->N, h->stream, ba);
-    if (h->nmx) {
-        ma.lower = h->d_ml; ma.upper = h->d_mu; ma.large = h->d_mg; ma.large_side = h->d_ms;
-        ma.count = h->nmx; ma.orientation = 1;
-        dispatch<Mrt>(h->N, h->stream, ma);
+    if (use_surface_pass(h)) {
+        if (!(phases & 2)) return;
+        sa.nbr = h->d_nbr;
+        sa.E = (int)h->E;
+        dispatch<Srf>(h->N, h->stream, sa, ba);
+        if (ev) {
+            cudaEventRecord(ev->after_x, h->stream);
+            cudaEventRecord(ev->after_y, h->stream);
+        }
+        return;
     }
+    if (phases & 2) {
+        sa.left = h->d_xl; sa.right = h->d_xr; sa.count = h->nx; sa.orientation = 1;
+        dispatch<Ifc>(h->N, h->stream, sa);
+        ba.bidx = h->d_bx; ba.count = h->nbx; ba.orientation = 1;
+        dispatch<Bnd>(h->N, h->stream, ba);
+        if (h->nmx) {
+            ma.lower = h->d_ml; ma.upper = h->d_mu; ma.large = h->d_mg; ma.large_side = h->d_ms;
+            ma.count = h->nmx; ma.orientation = 1;
+            dispatch<Mrt>(h->N, h->stream, ma);
+        }
+    }
+    if (!(phases & 4)) return;
     if (h->nh > 0) dispatch<Halo>(h->N, h->stream, halo_args(h, 0, mode, u_jump, out, dt_ptr), false);
     if (ev) cudaEventRecord(ev->after_x, h->stream);
     sa.left = h->d_yl; sa.right = h->d_yr; sa.count = h->ny; sa.orientation = 2;
@@ -680,8 +727,10 @@ int tlw_destroy(tlw_handle* h) {
     free_mesh(h);
     dfree(h->d_basis);
     dfree(h->d_step);
-    for (cudaEvent_t ev : {h->ev_up, h->ev_computed, h->ev_down[0], h->ev_down[1], h->ev_prior})
+    if (h->s_comm) cudaStreamSynchronize(h->s_comm);
+    for (cudaEvent_t ev : {h->ev_up, h->ev_computed, h->ev_down[0], h->ev_down[1], h->ev_prior, h->ev_lib, h->ev_comm})
         if (ev) cudaEventDestroy(ev);
+    if (h->s_comm) cudaStreamDestroy(h->s_comm);
     if (h->s_up) cudaStreamDestroy(h->s_up);
     if (h->s_down) cudaStreamDestroy(h->s_down);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -750,6 +799,22 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
         (rc = up_i(h->d_by, by)))
         return rc;
     h->nx = (int)xl.size(); h->ny = (int)yl.size();
+    if (2 * (int64_t)(xl.size() + yl.size()) + n_boundaries == 4 * n_elements) {
+        // every face a conforming interface or a boundary: the element-centric surface pass takes the element
+        // across each face, or -(k + 1) for boundary k
+        constexpr int unset = std::numeric_limits<int>::min();
+        std::vector<int> nbr((size_t)4 * n_elements, unset);
+        bool ok = true;
+        auto put = [&](int e, int f, int other) {
+            int& slot = nbr[(size_t)4 * e + f];
+            if (slot != unset) ok = false;
+            slot = other;
+        };
+        for (size_t k = 0; k < xl.size(); ++k) { put(xl[k], 1, xr[k]); put(xr[k], 0, xl[k]); }
+        for (size_t k = 0; k < yl.size(); ++k) { put(yl[k], 3, yr[k]); put(yr[k], 2, yl[k]); }
+        for (size_t k = 0; k < belem.size(); ++k) put(belem[k], bdir[k] - 1, -(int)k - 1);
+        if (ok && (rc = up_i(h->d_nbr, nbr))) return rc;
+    }
     h->jac_first = inverse_jacobian[0];
     if (h->sc) {
         if ((rc = up_i(h->d_il, al)) || (rc = up_i(h->d_ir, ar))) return rc;
@@ -1069,8 +1134,8 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
 int tlw_set_halo(tlw_handle* h, int64_t n_halo, const int64_t* elements, const int32_t* faces) {
     if (!h) return TLW_E_ARG;
     if (!h->have_mesh || h->curved) return fail(h, TLW_E_STATE, "halo faces follow tlw_set_tree_mesh");
-    if (n_halo > 0 && (h->sc || h->parabolic || h->nmx + h->nmy > 0))
-        return fail(h, TLW_E_UNSUPPORTED, "domain decomposition: LW or MDRK, FR volume integral, conforming TreeMesh, Euler");
+    if (n_halo > 0 && (h->parabolic || h->nmx + h->nmy > 0))
+        return fail(h, TLW_E_UNSUPPORTED, "domain decomposition: LW or MDRK, conforming TreeMesh, Euler");
     if (n_halo < 0 || (n_halo > 0 && (!elements || !faces))) return fail(h, TLW_E_ARG, "halo faces");
     std::vector<int> he[2], hf[2], hs[2];
     std::vector<signed char> seen((size_t)h->E * 4, 0);
@@ -1088,9 +1153,15 @@ int tlw_set_halo(tlw_handle* h, int64_t n_halo, const int64_t* elements, const i
     drop_graphs(h);
     for (int** d : {&h->d_he, &h->d_hf, &h->d_hs})
         if (*d) { cudaFree(*d); *d = nullptr; }
-    dfree(h->d_send); dfree(h->d_recv);
+    dfree(h->d_send); dfree(h->d_recv); dfree(h->d_asend); dfree(h->d_arecv);
     h->nh = (int)n_halo;
     h->nhx = (int)he[0].size();
+    h->halo_values = h->sc ? HALO_VALUES_SC : HALO_VALUES;
+    if (!h->s_comm) {
+        TLW_CUDA(h, cudaStreamCreateWithFlags(&h->s_comm, cudaStreamNonBlocking));
+        TLW_CUDA(h, cudaEventCreateWithFlags(&h->ev_lib, cudaEventDisableTiming));
+        TLW_CUDA(h, cudaEventCreateWithFlags(&h->ev_comm, cudaEventDisableTiming));
+    }
     h->slots_valid = false;
     if (n_halo > 0) {
         auto up = [&](int*& d, const std::vector<int>& a, const std::vector<int>& b) -> int {
@@ -1103,12 +1174,27 @@ int tlw_set_halo(tlw_handle* h, int64_t n_halo, const int64_t* elements, const i
         int rc;
         if ((rc = up(h->d_he, he[0], he[1])) || (rc = up(h->d_hf, hf[0], hf[1])) || (rc = up(h->d_hs, hs[0], hs[1])))
             return rc;
-        const size_t nd = (size_t)n_halo * h->n * HALO_VALUES;
+        const size_t nd = (size_t)n_halo * h->n * h->halo_values;
         TLW_CUDA(h, cudaMalloc(&h->d_send, nd * sizeof(double)));
         TLW_CUDA(h, cudaMalloc(&h->d_recv, nd * sizeof(double)));
         TLW_CUDA(h, zero_on(h->stream, h->d_send, nd * sizeof(double)));
         TLW_CUDA(h, zero_on(h->stream, h->d_recv, nd * sizeof(double)));
+        if (h->sc) {
+            TLW_CUDA(h, cudaMalloc(&h->d_asend, (size_t)n_halo * sizeof(double)));
+            TLW_CUDA(h, cudaMalloc(&h->d_arecv, (size_t)n_halo * sizeof(double)));
+            TLW_CUDA(h, zero_on(h->stream, h->d_asend, (size_t)n_halo * sizeof(double)));
+            TLW_CUDA(h, zero_on(h->stream, h->d_arecv, (size_t)n_halo * sizeof(double)));
+        }
     }
+    return TLW_OK;
+}
+
+int32_t tlw_dd_halo_values(tlw_handle* h) { return h ? h->halo_values : 0; }
+
+int tlw_dd_alpha_buffers(tlw_handle* h, double** send, double** recv) {
+    if (!h) return TLW_E_ARG;
+    if (send) *send = h->d_asend;
+    if (recv) *recv = h->d_arecv;
     return TLW_OK;
 }
 
@@ -1120,19 +1206,46 @@ int tlw_dd_buffers(tlw_handle* h, double** send, double** recv, unsigned long lo
     return TLW_OK;
 }
 
+// the comm stream continues after the work enqueued so far (the caller's collectives read what it wrote)
+int dd_to_comm(tlw_handle* h) {
+    if (!h->s_comm) return TLW_OK;
+    TLW_CUDA(h, cudaEventRecord(h->ev_lib, h->stream));
+    TLW_CUDA(h, cudaStreamWaitEvent(h->s_comm, h->ev_lib, 0));
+    return TLW_OK;
+}
+// the stream continues after the caller's collectives enqueued on the comm stream so far
+int dd_from_comm(tlw_handle* h) {
+    if (!h->s_comm) return TLW_OK;
+    TLW_CUDA(h, cudaEventRecord(h->ev_comm, h->s_comm));
+    TLW_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_comm, 0));
+    return TLW_OK;
+}
+
+int tlw_dd_comm_stream(tlw_handle* h, void** stream) {
+    if (!h || !stream) return TLW_E_ARG;
+    if (!h->s_comm) return fail(h, TLW_E_STATE, "the comm stream follows tlw_set_halo");
+    *stream = (void*)h->s_comm;
+    return TLW_OK;
+}
+
 int tlw_dd_begin(tlw_handle* h, double cfl, double fixed_dt, double t_end) {
     int rc = check_ready(h);
     if (rc) return rc;
     TLW_CUDA(h, cudaSetDevice(h->device));
+    if ((rc = dd_from_comm(h))) return rc;
     double params[3] = {t_end, cfl, fixed_dt};
     TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->t_end, params, sizeof(params), cudaMemcpyHostToDevice, h->stream));
     h->dd_stage = 0;   // a step starts with its first stage
     // this part's maximum; the caller reduces it over the ranks (MAX) before tlw_dd_volume
     const double* u = h->d_state[h->cur];
-    dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, true, false,
+    // with shock capturing the same pass gives the raw blending factors; the cut faces' go to the alpha buffer
+    dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, true, h->sc,
                   indicator_args(h));
+    if (h->sc && h->nh > 0)
+        halo_alpha_pack_kernel<<<(h->nh + 127) / 128, 128, 0, h->stream>>>(h->d_he, h->d_hs, h->nh, h->d_alpha_raw,
+                                                                          h->d_asend);
     TLW_CUDA(h, cudaGetLastError());
-    return TLW_OK;
+    return dd_to_comm(h);
 }
 
 int32_t tlw_dd_stages(tlw_handle* h) {
@@ -1143,15 +1256,32 @@ int tlw_dd_volume(tlw_handle* h) {
     int rc = check_ready(h);
     if (rc) return rc;
     TLW_CUDA(h, cudaSetDevice(h->device));
+    if ((rc = dd_from_comm(h))) return rc;   // the all-reduce (and the alpha exchange) first
     const double* u = h->d_state[h->cur];
     double* unew = h->d_state[1 - h->cur];
-    if (h->dd_stage == 0) finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
-    if (h->opts.time_discretization == TLW_LW)
-        enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, &h->d_step->dt, nullptr, true, 1);
-    else if (h->dd_stage == 0)   // MDRK stage 1 into u*, stage 2 from u* (the jumps are in u^n in both)
-        enqueue_rhs(h, TLW_STAGE_MDRK1, MODE_STEP, u, u, u, h->d_us, &h->d_step->dt, nullptr, true, 1);
-    else
-        enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, &h->d_step->dt, nullptr, true, 1);
+    if (h->dd_stage == 0) {
+        if (h->sc && h->opts.alpha_smooth) {
+            // the smoothing inside the part and, with the neighbours' raw alpha, across the cut faces
+            if (h->ni > 0)
+                alpha_smooth_kernel<<<(h->ni + 255) / 256, 256, 0, h->stream>>>(h->d_il, h->d_ir, h->ni,
+                                                                                h->d_alpha_raw, h->d_alpha);
+            if (h->nh > 0)
+                halo_alpha_smooth_kernel<<<(h->nh + 127) / 128, 128, 0, h->stream>>>(h->d_he, h->d_hs, h->nh,
+                                                                                    h->d_arecv, h->d_alpha);
+        }
+        finalize_dt_kernel<<<1, 1, 0, h->stream>>>(h->d_step, h->n);
+    }
+    // the volume kernel and the packing, the hand-over to the comm stream (the exchange can start), then the x
+    // faces inside the part while the traces travel
+    for (int phases : {1, 2}) {
+        if (h->opts.time_discretization == TLW_LW)
+            enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, &h->d_step->dt, nullptr, true, phases);
+        else if (h->dd_stage == 0)   // MDRK stage 1 into u*, stage 2 from u* (the jumps are in u^n in both)
+            enqueue_rhs(h, TLW_STAGE_MDRK1, MODE_STEP, u, u, u, h->d_us, &h->d_step->dt, nullptr, true, phases);
+        else
+            enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, &h->d_step->dt, nullptr, true, phases);
+        if (phases == 1 && (rc = dd_to_comm(h))) return rc;
+    }
     TLW_CUDA(h, cudaGetLastError());
     return TLW_OK;
 }
@@ -1160,18 +1290,19 @@ int tlw_dd_finish(tlw_handle* h) {
     int rc = check_ready(h);
     if (rc) return rc;
     TLW_CUDA(h, cudaSetDevice(h->device));
+    if ((rc = dd_from_comm(h))) return rc;   // the received traces
     const double* u = h->d_state[h->cur];
     double* unew = h->d_state[1 - h->cur];
     if (h->opts.time_discretization == TLW_LW) {
-        enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, &h->d_step->dt, nullptr, true, 2);
+        enqueue_rhs(h, TLW_STAGE_LW, MODE_STEP, u, u, u, unew, &h->d_step->dt, nullptr, true, 4);
         enqueue_limiter(h, unew, 2, nullptr);
     } else if (h->dd_stage == 0) {
-        enqueue_rhs(h, TLW_STAGE_MDRK1, MODE_STEP, u, u, u, h->d_us, &h->d_step->dt, nullptr, true, 2);
+        enqueue_rhs(h, TLW_STAGE_MDRK1, MODE_STEP, u, u, u, h->d_us, &h->d_step->dt, nullptr, true, 4);
         h->dd_stage = 1;
         TLW_CUDA(h, cudaGetLastError());
         return TLW_OK;
     } else {
-        enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, &h->d_step->dt, nullptr, true, 2);
+        enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, &h->d_step->dt, nullptr, true, 4);
         enqueue_limiter(h, unew, 1, nullptr);
         h->dd_stage = 0;
     }

@@ -102,9 +102,9 @@ __device__ __forceinline__ void node_speeds(double gamma, const double* x, unsig
 
 // Per-element CFL slots written by the kernels that produce the final values of a step (plain LW on a
 // periodic conforming TreeMesh): slot s of element e holds the bits of max(|v1| + c) and max(|v2| + c) over
-// the nodes finalised there: 0 interior (volume kernel), 1 / 2 the -x / +x face without corners
-// (x interfaces), 3 / 4 the -y / +y face with corners (y interfaces). The next step reduces them instead of
-// reading the whole state again.
+// the nodes finalised there: 0 interior (volume kernel); 1 all face nodes (the element-centric surface pass),
+// or with the interface sweeps 1 / 2 the -x / +x face without corners (x interfaces), 3 / 4 the -y / +y face
+// with corners (y interfaces). The next step reduces them instead of reading the whole state again.
 constexpr int CFL_SLOTS = 10;
 
 // Trixi max_abs_speed_naive (kind 0) / max_abs_speed (kind 1) for CompressibleEulerEquations2D

@@ -3,19 +3,31 @@
 // the u, U and F.n traces: 3 nv values, src/solvers/dgsem_tree/dg_parallel.jl:12-13).
 //
 // halo_pack_kernel: after the volume kernel, each cut face node's local u face value, U trace and normal flux
-// trace go to the send buffer [halo][l][12] in the caller's order; the caller moves it to the neighbour's
-// receive buffer (NCCL, or a device copy).
+// trace go to the send buffer [halo][l][values] in the caller's order; the caller moves it to the neighbour's
+// receive buffer (NCCL, or a device copy). With shock capturing a node also carries the element's first-order
+// subcell flux next to the face (fn_low, nv values) and its smoothed blending factor: 3 nv + nv + 1 values in a
+// 5 nv record (20 doubles, so that records stay 16-byte aligned).
 // halo_face_kernel: the LW surface flux of a cut face node in the TreeMesh argument order, with the local side
 // left on a +face and right on a -face, exactly as the interface kernel evaluates it for an interior
-// interface; only the local node is updated (the neighbour computes the same flux for its own node).
+// interface (blended with compute_alp from both sides' alpha and fn_low under shock capturing); only the local
+// node is updated (the neighbour computes the same flux for its own node).
 // x-faces and y-faces run as separate launches (corner nodes), after the interfaces of their orientation.
+// halo_alpha_pack_kernel / halo_alpha_smooth_kernel: the raw blending factor of each cut face's element goes to
+// the neighbour before the smoothing, which then takes max(alpha, alpha_raw_remote / 2) across the cut faces as
+// the interfaces do inside a part (Trixi apply_smoothing!), so the decomposed run blends as the whole mesh does.
+// (The reference's own MPI interface flux, calc_mpi_interface_flux!, dg_2d_parallel.jl:370-420, is the plain LW
+// flux; blending the cut faces keeps the decomposed solution equal to the undecomposed one.)
 #pragma once
 #include "tlw_device.cuh"
 #include "tlw_surface.cuh"
 
 namespace tlw {
 
-constexpr int HALO_VALUES = 3 * NV;   // u, U, F.n
+constexpr int HALO_VALUES = 3 * NV;            // u, U, F.n
+constexpr int HALO_VALUES_SC = 5 * NV;          // and fn_low, alpha (shock capturing; 3 doubles of padding)
+// node records are read and written as 16-byte vectors (load4 / store4): every record starts 16-byte aligned
+static_assert(HALO_VALUES * sizeof(double) % 16 == 0 && HALO_VALUES_SC * sizeof(double) % 16 == 0,
+              "halo node records must keep 16-byte alignment");
 
 struct HaloArgs {
     const double* u;          // state the jump is taken of
@@ -36,6 +48,12 @@ struct HaloArgs {
     int flux_kind, speed_kind;
     double inv_w_first, inv_w_last;
     unsigned* status;
+    int values;               // doubles per node in the buffers: HALO_VALUES or HALO_VALUES_SC
+    // shock capturing: smoothed alpha [e], fn_low traces [v, l, face, e], the admissibility test's J^{-1}
+    // (element 1's: on a conforming TreeMesh every element's) and the GLL end weights
+    const double* alpha;      // or null
+    const double* tFn;
+    double jac_first, w_first, w_last;
 };
 
 __device__ __forceinline__ int halo_face_node(int n, int f, int l) {
@@ -55,10 +73,15 @@ static __global__ void __launch_bounds__(128) halo_pack_kernel(HaloArgs a) {
     const size_t tb = (((size_t)e * 4 + f) * n + l) * NV;
     load4(a.tU + tb, y);
     load4(a.tF + tb, z);
-    double* s = a.send + ((size_t)__ldg(a.slot + k) * n + l) * HALO_VALUES;
+    double* s = a.send + ((size_t)__ldg(a.slot + k) * n + l) * a.values;
     store4(s, x);
     store4(s + NV, y);
     store4(s + 2 * NV, z);
+    if (a.alpha) {
+        load4(a.tFn + tb, x);
+        store4(s + 3 * NV, x);
+        s[4 * NV] = __ldg(a.alpha + e);
+    }
 }
 
 template <int N>
@@ -74,7 +97,7 @@ static __global__ void __launch_bounds__(128) halo_face_kernel(HaloArgs a) {
     const size_t tb = (((size_t)e * 4 + f) * n + l) * NV;
     load4(a.tU + tb, Ul);
     load4(a.tF + tb, Fl);
-    const double* r = a.recv + ((size_t)__ldg(a.slot + k) * n + l) * HALO_VALUES;
+    const double* r = a.recv + ((size_t)__ldg(a.slot + k) * n + l) * a.values;
     load4(r, ur);
     load4(r + NV, Ur);
     load4(r + 2 * NV, Fr);
@@ -83,6 +106,19 @@ static __global__ void __launch_bounds__(128) halo_face_kernel(HaloArgs a) {
         lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, Fl, Fr, Ul, Ur, ul, ur, a.orientation, Fn, a.status);
     else
         lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, Fr, Fl, Ur, Ul, ur, ul, a.orientation, Fn, a.status);
+    if (a.alpha) {
+        // the interface kernel's blend with the remote side's alpha and fn_low (compute_alp, dg_2d.jl:1879-1901)
+        double fl[NV], fr[NV];
+        load4(a.tFn + tb, fl);
+        load4(r + 3 * NV, fr);
+        const double al = __ldg(a.alpha + e), ar = r[4 * NV];
+        if (local_left)
+            blend_flux_values(a.gamma, a.speed_kind, a.status, a.jac_first, a.w_first, a.w_last, a.orientation, ul,
+                              ur, al, ar, fl, fr, *a.dt, Fn);
+        else
+            blend_flux_values(a.gamma, a.speed_kind, a.status, a.jac_first, a.w_first, a.w_last, a.orientation, ur,
+                              ul, ar, al, fr, fl, *a.dt, Fn);
+    }
     const double dts = a.step_mode ? *a.dt : 1.0;
     const double ij = __ldg(a.inv_jac + e);
     // the interface kernel's coefficients, in its order of operations
@@ -93,6 +129,22 @@ static __global__ void __launch_bounds__(128) halo_face_kernel(HaloArgs a) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) x[v] = fma(c, Fn[v], x[v]);
     store4(o, x);
+}
+
+// the raw blending factor of each cut face's element into the alpha send buffer [halo] (caller's order)
+static __global__ void halo_alpha_pack_kernel(const int* __restrict__ elem, const int* __restrict__ slot, int count,
+                                              const double* __restrict__ alpha_raw, double* __restrict__ send) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) send[__ldg(slot + k)] = __ldg(alpha_raw + __ldg(elem + k));
+}
+
+// alpha_e = max(alpha_e, alpha_raw_remote / 2) across the cut faces (the smoothing of alpha_smooth_kernel)
+static __global__ void halo_alpha_smooth_kernel(const int* __restrict__ elem, const int* __restrict__ slot, int count,
+                                                const double* __restrict__ recv, double* alpha) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    unsigned long long* ab = reinterpret_cast<unsigned long long*>(alpha);
+    atomicMax(ab + __ldg(elem + k), (unsigned long long)__double_as_longlong(0.5 * __ldg(recv + __ldg(slot + k))));
 }
 
 }  // namespace tlw

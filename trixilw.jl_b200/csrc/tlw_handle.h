@@ -90,6 +90,7 @@ struct tlw_handle {
     int64_t E = 0;
     double* d_inv_jac = nullptr;
     int *d_xl = nullptr, *d_xr = nullptr, *d_yl = nullptr, *d_yr = nullptr;
+    int* d_nbr = nullptr;   // [4, E] element across each face when every face is a conforming interface
     int nx = 0, ny = 0;
     int64_t nb = 0;
     int *d_b_elem = nullptr, *d_b_dir = nullptr, *d_bx = nullptr, *d_by = nullptr;
@@ -137,11 +138,18 @@ struct tlw_handle {
     int* d_wkind = nullptr;
     double* d_wall = nullptr;
     // faces shared with other ranks' parts (domain decomposition): x-faces [0, nhx), y-faces [nhx, nh); local
-    // element, face, position in the caller's order; send / receive buffers [halo][l][12]
+    // element, face, position in the caller's order; send / receive buffers [halo][l][halo_values]; with shock
+    // capturing also the raw alpha of each cut face's element [halo]
     int nh = 0, nhx = 0;
+    int halo_values = 12;
     int dd_stage = 0;                       // split step: the MDRK stage in progress (0: stage 1, 1: stage 2)
     int *d_he = nullptr, *d_hf = nullptr, *d_hs = nullptr;
     double *d_send = nullptr, *d_recv = nullptr;
+    double *d_asend = nullptr, *d_arecv = nullptr;
+    // the caller's collectives run on s_comm; ev_lib / ev_comm hand the order over between it and the stream, so
+    // that the exchange of the cut-face traces overlaps the part's x interfaces
+    cudaStream_t s_comm = nullptr;
+    cudaEvent_t ev_lib = nullptr, ev_comm = nullptr;
     // per element: the faces (0..3) through which it is the large element of a mortar, in mortar order
     // (bits 0-2 count, then 2 bits per mortar); for the positivity limiter's mortar pass
     int* d_mface = nullptr;

@@ -149,6 +149,18 @@ struct LaunchImpl {
         if (threads == 0) return;
         interface_kernel<N><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(a);
     }
+    static void surfaces(cudaStream_t s, const SurfArgs& a, const BndArgs& b) {
+        if (a.E <= 0) return;
+        using C = SurfCfg<N>;
+        const unsigned grid = (unsigned)((a.E + C::EB - 1) / C::EB);
+        if (a.shock_capturing) {
+            if (b.element) surface_kernel<N, true, true><<<grid, C::THREADS, 0, s>>>(a, b);
+            else surface_kernel<N, false, true><<<grid, C::THREADS, 0, s>>>(a, b);
+        } else {
+            if (b.element) surface_kernel<N, true, false><<<grid, C::THREADS, 0, s>>>(a, b);
+            else surface_kernel<N, false, false><<<grid, C::THREADS, 0, s>>>(a, b);
+        }
+    }
     static void parabolic(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out,
                           const double* dtp) {
         if constexpr (N >= 3) {
@@ -289,6 +301,9 @@ template <int N> void Launch<N>::volume(cudaStream_t s, int stage, int mode, boo
     LaunchImpl<N>::volume(s, stage, mode, sc, a);
 }
 template <int N> void Launch<N>::interfaces(cudaStream_t s, const SurfArgs& a) { LaunchImpl<N>::interfaces(s, a); }
+template <int N> void Launch<N>::surfaces(cudaStream_t s, const SurfArgs& a, const BndArgs& b) {
+    LaunchImpl<N>::surfaces(s, a, b);
+}
 template <int N> void Launch<N>::boundaries(cudaStream_t s, const BndArgs& a) { LaunchImpl<N>::boundaries(s, a); }
 template <int N>
 void Launch<N>::parabolic(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out,

@@ -23,6 +23,8 @@ struct Launch {
     static void par_attributes();
     static void volume(cudaStream_t s, int stage, int mode, bool sc, const VolArgs& a);
     static void interfaces(cudaStream_t s, const SurfArgs& a);
+    // all faces of a mesh whose every face is a conforming interface or a boundary, one pass over the elements
+    static void surfaces(cudaStream_t s, const SurfArgs& a, const BndArgs& b);
     static void boundaries(cudaStream_t s, const BndArgs& a);
     static void parabolic(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out,
                           const double* dtp);

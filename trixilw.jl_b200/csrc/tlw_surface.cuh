@@ -45,6 +45,8 @@ struct SurfArgs {
     const int* inst;         // batched form: instance of each element (dt indexed by it); null otherwise
     const double* tFv;      // compressible Navier-Stokes: viscous normal flux traces (null otherwise)
     unsigned long long* cfl_slots;   // plain LW step: per-element CFL slots of the nodes finalised here
+    const int* nbr;          // surface_kernel: the element across each face [4, e] (-x, +x, -y, +y)
+    int E;                   // surface_kernel: number of elements
 };
 
 __device__ __forceinline__ bool admissible(double gm1, const double* u) {
@@ -56,36 +58,76 @@ __device__ __forceinline__ bool admissible(double gm1, const double* u) {
 
 // Fn <- alp fn + (1 - alp) Fn with compute_alp (dg_2d.jl:1879-1901, 1929-1937): fn is the first-order
 // flux at the instantaneous u, alp = (alpha_L + alpha_R)/2, or 1 when the low-order update of either face
-// subcell (subcell flux next to the face from tFn, lambda = 1/2) is not admissible.
-template <int N>
-__device__ __forceinline__ void blend_interface_flux(const SurfArgs& a, int le, int re, int faceL, int faceR, int l,
-                                                     const double* uL, const double* uR, double dt, double* Fn) {
-    constexpr int n = N + 1;
-    const double gm1 = a.gamma - 1.0;
+// subcell (subcell flux next to the face, fil / fir, lambda = 1/2) is not admissible. jac is the J^{-1} the
+// reference takes for the test (element 1's on TreeMesh), wf / wl the GLL weights w_1 / w_n.
+__device__ __forceinline__ void blend_flux_values(double gamma, int speed_kind, unsigned* status, double jac,
+                                                  double wf, double wl, int orientation, const double* uL,
+                                                  const double* uR, double alphaL, double alphaR, const double* fil,
+                                                  const double* fir, double dt, double* Fn) {
+    const double gm1 = gamma - 1.0;
     double fl[NV], fr[NV], fn[NV];
-    euler_flux_dir(gm1, uL, a.orientation, fl);
-    euler_flux_dir(gm1, uR, a.orientation, fr);
-    const double lam = max_abs_speed(a.gamma, uL, uR, a.orientation, a.speed_kind, a.status);
+    euler_flux_dir(gm1, uL, orientation, fl);
+    euler_flux_dir(gm1, uR, orientation, fr);
+    const double lam = max_abs_speed(gamma, uL, uR, orientation, speed_kind, status);
 #pragma unroll
     for (int v = 0; v < NV; ++v) fn[v] = 0.5 * (fl[v] + fr[v]) + (-0.5 * lam * (uR[v] - uL[v]));
-    double alp = 0.5 * (__ldg(a.alpha + le) + __ldg(a.alpha + re));
-    double Fb[NV], fil[NV], fir[NV], low[NV];
+    double alp = 0.5 * (alphaL + alphaR);
+    double Fb[NV], low[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) Fb[v] = (1.0 - alp) * Fn[v] + alp * fn[v];
-    load4(a.tFn + (((size_t)le * 4 + faceL) * n + l) * NV, fil);
-    load4(a.tFn + (((size_t)re * 4 + faceR) * n + l) * NV, fir);
     const double lamx = 0.5;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) low[v] = uL[v] - dt * a.jac_first / (a.w_last * lamx) * (Fb[v] - fil[v]);
+    for (int v = 0; v < NV; ++v) low[v] = uL[v] - dt * jac / (wl * lamx) * (Fb[v] - fil[v]);
     if (!admissible(gm1, low)) {
         alp = 1.0;
     } else {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) low[v] = uR[v] - dt * a.jac_first / (a.w_first * lamx) * (fir[v] - Fb[v]);
+        for (int v = 0; v < NV; ++v) low[v] = uR[v] - dt * jac / (wf * lamx) * (fir[v] - Fb[v]);
         if (!admissible(gm1, low)) alp = 1.0;
     }
 #pragma unroll
     for (int v = 0; v < NV; ++v) Fn[v] = alp * fn[v] + (1.0 - alp) * Fn[v];
+}
+
+template <int N>
+__device__ __forceinline__ void blend_interface_flux(const SurfArgs& a, int orientation, int le, int re, int faceL,
+                                                     int faceR, int l, const double* uL, const double* uR, double dt,
+                                                     double* Fn) {
+    constexpr int n = N + 1;
+    double fil[NV], fir[NV];
+    load4(a.tFn + (((size_t)le * 4 + faceL) * n + l) * NV, fil);
+    load4(a.tFn + (((size_t)re * 4 + faceR) * n + l) * NV, fir);
+    blend_flux_values(a.gamma, a.speed_kind, a.status, a.jac_first, a.w_first, a.w_last, orientation, uL, uR,
+                      __ldg(a.alpha + le), __ldg(a.alpha + re), fil, fir, dt, Fn);
+}
+
+// The LW flux at node l of the interface (le, re) of one orientation, with the blending and the viscous
+// flux where they apply: calc_interface_flux! (dg_2d.jl:1903-1946) at one node.
+template <int N, bool SC = true>
+__device__ __forceinline__ void interface_node_flux(const SurfArgs& a, int orientation, int le, int re, int l,
+                                                    double dt, double* Fn) {
+    constexpr int n = N + 1;
+    int nodeL, nodeR, faceL, faceR;
+    if (orientation == 1) { nodeL = (n - 1) + n * l; nodeR = n * l; faceL = 1; faceR = 0; }
+    else { nodeL = l + n * (n - 1); nodeR = l; faceL = 3; faceR = 2; }
+    double uL[NV], uR[NV], UL[NV], UR[NV], FL[NV], FR[NV];
+    load4(a.u + ((size_t)le * n * n + nodeL) * NV, uL);
+    load4(a.u + ((size_t)re * n * n + nodeR) * NV, uR);
+    load4(a.tU + (((size_t)le * 4 + faceL) * n + l) * NV, UL);
+    load4(a.tU + (((size_t)re * 4 + faceR) * n + l) * NV, UR);
+    load4(a.tF + (((size_t)le * 4 + faceL) * n + l) * NV, FL);
+    load4(a.tF + (((size_t)re * 4 + faceR) * n + l) * NV, FR);
+    // TreeMesh argument order: surface_flux(f_ll, f_rr, U_ll, U_rr, u_ll, u_rr) (dg_2d.jl:1928)
+    lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, FL, FR, UL, UR, uL, uR, orientation, Fn, a.status);
+    if (SC && a.shock_capturing) blend_interface_flux<N>(a, orientation, le, re, faceL, faceR, l, uL, uR, dt, Fn);
+    if (a.tFv) {
+        // compressible Navier-Stokes: minus the central viscous flux (Fv_L + Fv_R) / 2
+        double vL[NV], vR[NV];
+        load4(a.tFv + (((size_t)le * 4 + faceL) * n + l) * NV, vL);
+        load4(a.tFv + (((size_t)re * 4 + faceR) * n + l) * NV, vR);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fn[v] -= 0.5 * (vL[v] + vR[v]);
+    }
 }
 
 template <int N>
@@ -96,28 +138,11 @@ static __global__ void __launch_bounds__(256) interface_kernel(SurfArgs a) {
     const int l = t - k * n;
     if (k >= a.count) return;
     const int le = __ldg(a.left + k), re = __ldg(a.right + k);
-    int nodeL, nodeR, faceL, faceR;
-    if (a.orientation == 1) { nodeL = (n - 1) + n * l; nodeR = n * l; faceL = 1; faceR = 0; }
-    else { nodeL = l + n * (n - 1); nodeR = l; faceL = 3; faceR = 2; }
-    double uL[NV], uR[NV], UL[NV], UR[NV], FL[NV], FR[NV], Fn[NV];
-    load4(a.u + ((size_t)le * n * n + nodeL) * NV, uL);
-    load4(a.u + ((size_t)re * n * n + nodeR) * NV, uR);
-    load4(a.tU + (((size_t)le * 4 + faceL) * n + l) * NV, UL);
-    load4(a.tU + (((size_t)re * 4 + faceR) * n + l) * NV, UR);
-    load4(a.tF + (((size_t)le * 4 + faceL) * n + l) * NV, FL);
-    load4(a.tF + (((size_t)re * 4 + faceR) * n + l) * NV, FR);
-    // TreeMesh argument order: surface_flux(f_ll, f_rr, U_ll, U_rr, u_ll, u_rr) (dg_2d.jl:1928)
-    lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, FL, FR, UL, UR, uL, uR, a.orientation, Fn, a.status);
+    const int nodeL = a.orientation == 1 ? (n - 1) + n * l : l + n * (n - 1);
+    const int nodeR = a.orientation == 1 ? n * l : l;
     const double dt = a.inst ? a.dt[__ldg(a.inst + le)] : *a.dt;
-    if (a.shock_capturing) blend_interface_flux<N>(a, le, re, faceL, faceR, l, uL, uR, dt, Fn);
-    if (a.tFv) {
-        // compressible Navier-Stokes: minus the central viscous flux (Fv_L + Fv_R) / 2
-        double vL[NV], vR[NV];
-        load4(a.tFv + (((size_t)le * 4 + faceL) * n + l) * NV, vL);
-        load4(a.tFv + (((size_t)re * 4 + faceR) * n + l) * NV, vR);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) Fn[v] -= 0.5 * (vL[v] + vR[v]);
-    }
+    double Fn[NV];
+    interface_node_flux<N>(a, a.orientation, le, re, l, dt, Fn);
     const double dts = a.step_mode ? dt : 1.0;
     const double sL = -__ldg(a.inv_jac + le) * a.inv_w_last * dts;
     const double sR = __ldg(a.inv_jac + re) * a.inv_w_first * dts;
@@ -146,7 +171,6 @@ static __global__ void __launch_bounds__(256) interface_kernel(SurfArgs a) {
         atomicMax(a.cfl_slots + (size_t)re * CFL_SLOTS + 2 * sR_slot + 1, (unsigned long long)__double_as_longlong(l2));
     }
 }
-
 
 struct BndArgs {
     const double* u;
@@ -190,16 +214,12 @@ __device__ __forceinline__ void slip_wall_exterior(int kind, const double* Fi, c
     uo[0] = ui[0]; uo[1] = vert ? -ui[1] : ui[1]; uo[2] = vert ? ui[2] : -ui[2]; uo[3] = ui[3];
 }
 
+// The LW flux at node l of boundary k (element e, Trixi direction dir): calc_boundary_flux! (dg_2d.jl:1385-1454)
+// with the time-averaged Dirichlet data or a slip wall, and the Navier-Stokes wall's viscous flux.
 template <int N>
-static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
+__device__ __forceinline__ void boundary_node_flux(const BndArgs& a, int k, int e, int dir, int l, double* Fn) {
     constexpr int n = N + 1;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int kk = t / n;
-    const int l = t - kk * n;
-    if (kk >= a.count) return;
-    const int k = __ldg(a.bidx + kk);
-    const int e = __ldg(a.element + k);
-    const int dir = __ldg(a.direction + k);
+    const int orientation = dir <= 2 ? 1 : 2;
     int node, face;
     switch (dir) {
         case 1: node = n * l; face = 0; break;
@@ -208,7 +228,7 @@ static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
         default: node = l + n * (n - 1); face = 3; break;
     }
     const double gm1 = a.gamma - 1.0;
-    double ui[NV], Ui[NV], Fi[NV], Uo[NV] = {0, 0, 0, 0}, Fo[NV] = {0, 0, 0, 0}, uo[NV], Fn[NV];
+    double ui[NV], Ui[NV], Fi[NV], Uo[NV] = {0, 0, 0, 0}, Fo[NV] = {0, 0, 0, 0}, uo[NV];
     load4(a.u + ((size_t)e * n * n + node) * NV, ui);
     load4(a.tU + (((size_t)e * 4 + face) * n + l) * NV, Ui);
     load4(a.tF + (((size_t)e * 4 + face) * n + l) * NV, Fi);
@@ -217,7 +237,7 @@ static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
         for (int q = 0; q < n; ++q) {
             double ub[NV], fb[NV];
             load4(a.levels + (((size_t)k * n + l) * n + q) * NV, ub);
-            euler_flux_dir(gm1, ub, a.orientation, fb);
+            euler_flux_dir(gm1, ub, orientation, fb);
             const double w = 0.5 * a.scaling_factor;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
@@ -230,9 +250,9 @@ static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
         slip_wall_exterior(kind, Fi, Ui, ui, Fo, Uo, uo);
     }
     if (dir % 2 == 0)
-        lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, Fi, Fo, Ui, Uo, ui, uo, a.orientation, Fn, a.status);
+        lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, Fi, Fo, Ui, Uo, ui, uo, orientation, Fn, a.status);
     else
-        lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, Fo, Fi, Uo, Ui, uo, ui, a.orientation, Fn, a.status);
+        lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, Fo, Fi, Uo, Ui, uo, ui, orientation, Fn, a.status);
     if (a.tFv) {
         // minus the wall's viscous flux (calc_boundary_flux_divergence_lw!, dg_2d_parabolic.jl:2005-2084;
         // BoundaryConditionNavierStokesWall, compressible_navier_stokes_2d.jl:81-108)
@@ -245,6 +265,21 @@ static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) Fn[v] -= fv[v];
     }
+}
+
+template <int N>
+static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
+    constexpr int n = N + 1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = t / n;
+    const int l = t - kk * n;
+    if (kk >= a.count) return;
+    const int k = __ldg(a.bidx + kk);
+    const int e = __ldg(a.element + k);
+    const int dir = __ldg(a.direction + k);
+    const int node = dir == 1 ? n * l : dir == 2 ? (n - 1) + n * l : dir == 3 ? l : l + n * (n - 1);
+    double Fn[NV];
+    boundary_node_flux<N>(a, k, e, dir, l, Fn);
     const double dts = a.step_mode ? *a.dt : 1.0;
     const double ij = __ldg(a.inv_jac + e);
     const double s = (dir % 2 == 0) ? -ij * a.inv_w_last * dts : ij * a.inv_w_first * dts;
@@ -255,6 +290,121 @@ static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
     for (int v = 0; v < NV; ++v) x[v] = fma(s, Fn[v], x[v]);
     store4(o, x);
 }
+
+// surface_kernel launch shape: about TLW_SURF_THREADS threads a CTA (4n flux threads per element); the plain
+// kernel (no boundaries, no blending) capped to TLW_SURF_MINB resident CTAs' registers (5 x 160 threads: 72
+// registers, no spills); TLW_SURF_PREFETCH 1 loads the output face node before the flux phase (more registers).
+// Measured on the 512 x 512, N = 4 vortex: 0.205 ms with (160, 5, 0), 0.232 ms with (160, 1, 1) at 90
+// registers, 0.236 ms with (320, 3, 0); the x / y sweeps take 0.236 ms.
+#ifndef TLW_SURF_THREADS
+#define TLW_SURF_THREADS 160
+#endif
+#ifndef TLW_SURF_MINB
+#define TLW_SURF_MINB 5
+#endif
+#ifndef TLW_SURF_PREFETCH
+#define TLW_SURF_PREFETCH 0
+#endif
+// Elements per CTA of surface_kernel: 4n flux threads per element, about TLW_SURF_THREADS threads a CTA.
+template <int N> struct SurfCfg {
+    static constexpr int n = N + 1;
+    static constexpr int EB = (TLW_SURF_THREADS + 4 * n - 1) / (4 * n);
+    static constexpr int THREADS = EB * 4 * n;
+    static constexpr int MIN_BLOCKS = TLW_SURF_MINB;
+};
+
+// All four faces of each element in one pass, for a mesh whose every face is a conforming interface or a
+// boundary: nbr[4e + f] (f = -x, +x, -y, +y) is the element across face f, or -(k + 1) for boundary k of the
+// boundary arguments. Phase 1: one thread per (element, face, node) evaluates that face's flux exactly as
+// interface_kernel / boundary_kernel do (an interface with its own (left, right) arguments, so both elements get
+// the same bits) into shared memory. Phase 2: one thread per face node of the element applies the x face's lift
+// and then the y face's (the order of the x and y launches), with the Jacobian and dt, and reduces the element's
+// face-node CFL speeds. Each interface is evaluated twice and each element's face nodes are read and written once:
+// no strided x sweep, no atomics.
+template <int N, bool BND, bool SC>
+static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? 1 : SurfCfg<N>::MIN_BLOCKS)
+    surface_kernel(SurfArgs a, BndArgs bnd) {
+    using C = SurfCfg<N>;
+    constexpr int n = N + 1, EB = C::EB, NB = 4 * (n - 1);
+    __shared__ double sF[EB * 4 * n * NV];
+    const int tid = threadIdx.x;
+    const int e0 = blockIdx.x * EB;
+    // phase-2 thread: element el2, boundary node b (bottom row, top row, left column, right column)
+    const int el2 = tid / NB, b = tid - el2 * NB, e2 = e0 + el2;
+    const bool has2 = el2 < EB && e2 < a.E;
+    int i2, j2;
+    if (b < n) { i2 = b; j2 = 0; }
+    else if (b < 2 * n) { i2 = b - n; j2 = n - 1; }
+    else if (b < 3 * n - 2) { i2 = 0; j2 = b - 2 * n + 1; }
+    else { i2 = n - 1; j2 = b - 3 * n + 3; }
+    double* o2 = a.out + ((size_t)e2 * n * n + i2 + n * j2) * NV;
+    double x[NV];
+    if (TLW_SURF_PREFETCH && has2) load4_rw(o2, x);
+    {
+        const int el = tid / (4 * n), r = tid - el * 4 * n, f = r / n, l = r - f * n, e = e0 + el;
+        if (e < a.E) {
+            const double dt = a.inst ? a.dt[__ldg(a.inst + e)] : *a.dt;   // (batched form: the instance's dt)
+            const int nb = __ldg(a.nbr + 4 * e + f);
+            const bool plus = f & 1;   // this element is the interface's left (lower) element
+            double Fn[NV];
+            if (!BND || nb >= 0) interface_node_flux<N, SC>(a, f < 2 ? 1 : 2, plus ? e : nb, plus ? nb : e, l, dt, Fn);
+            else boundary_node_flux<N>(bnd, -nb - 1, e, f + 1, l, Fn);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) sF[tid * NV + v] = Fn[v];
+        }
+    }
+    __syncthreads();
+    double l1 = 0.0, l2 = 0.0;
+    if (has2) {
+        if (!TLW_SURF_PREFETCH) load4_rw(o2, x);
+        const double dt = a.inst ? a.dt[__ldg(a.inst + e2)] : *a.dt;
+        const double dts = a.step_mode ? dt : 1.0;
+        const double ij = __ldg(a.inv_jac + e2);
+        const double sMinus = ij * a.inv_w_first * dts;   // the element is the right (upper) one of the interface
+        const double sPlus = -ij * a.inv_w_last * dts;    // the element is the left (lower) one
+        const double* F = sF + el2 * 4 * n * NV;
+        if (i2 == 0 || i2 == n - 1) {
+            const double s = i2 == 0 ? sMinus : sPlus;
+            const double* p = F + ((i2 == 0 ? 0 : 1) * n + j2) * NV;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) x[v] = fma(s, p[v], x[v]);
+        }
+        if (j2 == 0 || j2 == n - 1) {
+            const double s = j2 == 0 ? sMinus : sPlus;
+            const double* p = F + ((j2 == 0 ? 2 : 3) * n + i2) * NV;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) x[v] = fma(s, p[v], x[v]);
+        }
+        store4(o2, x);
+        if (a.cfl_slots) node_speeds(a.gamma, x, a.status, l1, l2);
+    }
+    if (a.cfl_slots && 32 % NB == 0) {
+        // the element's NB phase-2 threads are NB aligned consecutive lanes of one warp: reduce by shuffles
+#pragma unroll
+        for (int o = NB / 2; o > 0; o >>= 1) {
+            l1 = fmax(l1, __shfl_xor_sync(0xffffffffu, l1, o));
+            l2 = fmax(l2, __shfl_xor_sync(0xffffffffu, l2, o));
+        }
+        if (has2 && b < 2)
+            a.cfl_slots[(size_t)e2 * CFL_SLOTS + 2 + b] = (unsigned long long)__double_as_longlong(b ? l2 : l1);
+    } else if (a.cfl_slots) {
+        // the element's face-node maxima through shared memory (NB consecutive threads per element)
+        __syncthreads();
+        if (has2) {
+            sF[tid] = l1;
+            sF[EB * NB + tid] = l2;
+        }
+        __syncthreads();
+        if (has2 && b < 2) {
+            const double* p = sF + b * EB * NB + el2 * NB;
+            double m = 0.0;
+#pragma unroll
+            for (int k = 0; k < NB; ++k) m = fmax(m, p[k]);
+            a.cfl_slots[(size_t)e2 * CFL_SLOTS + 2 + b] = (unsigned long long)__double_as_longlong(m);
+        }
+    }
+}
+
 
 // ------------------------------------------------------------------------------------------------
 // CFL time step on the device.

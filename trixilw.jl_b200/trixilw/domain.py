@@ -7,8 +7,11 @@ them and its share of the boundaries; the faces it shares with another rank's pa
 (``DomainDecomposedLW.step``) is: this part's CFL maximum, a MAX all-reduce of it over the ranks, the volume
 kernel with the halo traces (u, U, F.n per node, 12 doubles, the reference's 3 nv message) packed into a send
 buffer, the halo exchange with the neighbouring ranks, then the interfaces, boundaries and halo faces; an MDRK
-step does the volume / exchange / surface round once per stage. All of it runs on the library's stream; the
-collectives are ordered on that stream.
+step does the volume / exchange / surface round once per stage. With shock capturing the raw blending factors
+of the cut faces' elements are exchanged after the all-reduce (for the smoothing across the cut faces), and a
+halo node also carries fn_low and the smoothed alpha (20 doubles with padding), so the cut faces are blended as interior
+interfaces are. The kernels run on the library's stream and the collectives on its comm stream; the library hands
+the order over between the two, so the trace exchange overlaps the part's x interfaces.
 """
 from __future__ import annotations
 
@@ -21,7 +24,7 @@ from . import _lib
 from ._lib import check, lib
 from .mesh import TreeMesh
 
-HALO_VALUES = 12
+HALO_VALUES = 12      # doubles per cut face node without shock capturing (20 with it: tlw_dd_halo_values)
 
 
 class LocalTreeMesh(TreeMesh):
@@ -122,8 +125,8 @@ class DomainDecomposedLW:
 
     ``allreduce_max(t)`` and ``exchange(send, recv, segments)`` are the rank's collectives on torch tensors that
     alias the library's device buffers: an int64 scalar holding the CFL maximum's bits (a non-negative double,
-    so int64 order is double order) and the [H, n, 12] halo buffers. ``torch_collectives`` gives them for
-    torch.distributed."""
+    so int64 order is double order), the [H, n, 12 or 20] halo buffers and, with shock capturing, the [H] alpha
+    buffers. ``torch_collectives`` gives them for torch.distributed."""
 
     def __init__(self, semi, part: Part, allreduce_max, exchange):
         import torch
@@ -141,12 +144,24 @@ class DomainDecomposedLW:
         check(h, lib().tlw_dd_buffers(h, ctypes.byref(send), ctypes.byref(recv), ctypes.byref(mx)))
         n = semi.nnodes
         dev = torch.device("cuda", semi.device)
-        self.send = torch.as_tensor(_DeviceArray(send.value or 0, (H, n, HALO_VALUES), "<f8"), device=dev) if H else None
-        self.recv = torch.as_tensor(_DeviceArray(recv.value or 0, (H, n, HALO_VALUES), "<f8"), device=dev) if H else None
+        nv = int(lib().tlw_dd_halo_values(h))
+        self.send = torch.as_tensor(_DeviceArray(send.value or 0, (H, n, nv), "<f8"), device=dev) if H else None
+        self.recv = torch.as_tensor(_DeviceArray(recv.value or 0, (H, n, nv), "<f8"), device=dev) if H else None
+        asend, arecv = ctypes.c_void_p(), ctypes.c_void_p()
+        check(h, lib().tlw_dd_alpha_buffers(h, ctypes.byref(asend), ctypes.byref(arecv)))
+        self.alpha_send = (torch.as_tensor(_DeviceArray(asend.value, (H,), "<f8"), device=dev)
+                           if H and asend.value else None)
+        self.alpha_recv = (torch.as_tensor(_DeviceArray(arecv.value, (H,), "<f8"), device=dev)
+                           if H and arecv.value else None)
         self.max_bits = torch.as_tensor(_DeviceArray(mx.value, (1,), "<i8"), device=dev)
+        # the collectives go on the library's comm stream: the split step hands the order over to it after the
+        # packing, so the exchange overlaps the part's x interfaces
         sp = ctypes.c_void_p()
-        check(h, lib().tlw_get_stream(h, ctypes.byref(sp)))
+        check(h, lib().tlw_dd_comm_stream(h, ctypes.byref(sp)))
         self.stream = torch.cuda.ExternalStream(sp.value, device=dev)
+        # the kernels' stream: a step's last work is on it (events that bracket whole steps go here)
+        check(h, lib().tlw_get_stream(h, ctypes.byref(sp)))
+        self.lib_stream = torch.cuda.ExternalStream(sp.value, device=dev)
 
     def step(self, nsteps: int, cfl: float, t_end: float = float("inf"), fixed_dt: float = 0.0):
         import torch
@@ -158,6 +173,8 @@ class DomainDecomposedLW:
             check(h, L.tlw_dd_begin(h, float(cfl), float(fixed_dt), float(t_end)))
             with torch.cuda.stream(self.stream):
                 self.allreduce_max(self.max_bits)
+                if self.alpha_send is not None:   # shock capturing: raw alpha across the cut faces
+                    self.exchange(self.alpha_send, self.alpha_recv, self.part.segments)
             for _stage in range(stages):   # MDRK: stage 1 (into u*), then stage 2, each with its own exchange
                 check(h, L.tlw_dd_volume(h))
                 if self.send is not None:
