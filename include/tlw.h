@@ -201,6 +201,16 @@ int tlw_set_unstructured_mesh(tlw_handle* h, int64_t n_elements, const double* c
                               const int64_t* element_ids, const int64_t* element_side_ids, const int64_t* start_index,
                               const int64_t* index_increment);
 
+/* Source terms (SemidiscretizationHyperbolic(...; source_terms), calc_source and its time-derivative stencils,
+ * src/solvers/dgsem_tree/dg_2d.jl:89-175, used by every LW kernel and by mdrk_kernel_1! / _2!,
+ * multi_derivative_2d.jl:321-400 and :484-550), after tlw_set_tree_mesh (and again after a new mesh): kind 0 none,
+ * 1 Trixi's source_terms_convergence_test for CompressibleEulerEquations2D (the source of
+ * initial_condition_convergence_test's manufactured solution); node_coordinates [2, i, j, e] as Trixi's
+ * cache.elements.node_coordinates. The source is evaluated at the step's t (tlw_step: the device time; tlw_rhs:
+ * its t argument; MDRK stage 2 at t + dt/2). TreeMesh, FR volume integral, Euler, LW or MDRK; not with
+ * Adaptive. */
+int tlw_set_source_terms(tlw_handle* h, int32_t kind, const double* node_coordinates);
+
 /* Domain decomposition (the reference's MPI path, src/solvers/dgsem_tree/dg_2d_parallel.jl:23-200, with the same
  * message per cut face node: the u face value, U trace and F.n trace, 3 nv doubles, dg_parallel.jl:12-13). A rank
  * uploads its part of the TreeMesh with tlw_set_tree_mesh (local elements, the interfaces between them, its

@@ -30,6 +30,7 @@ struct oracle_handle {
     bool parabolic = false;      // compressible Navier-Stokes (TreeMesh, periodic, LW)
     NavierStokes ns;
     PositivityLimiter lim;       // applied after every step of oracle_steps when not empty
+    std::vector<double> xnode;   // node coordinates [2, i, j, e] for source terms
     char err[256] = {0};
 
     int n_elements() const { return curved ? cmesh.n_elements : mesh.n_elements; }
@@ -209,6 +210,17 @@ int oracle_set_curved_mortars(oracle_handle* h, int M, const int32_t* small1, co
 // lw_mortars.inverse_jacobian [mortar][l] for the shock-capturing blend at the mortars (null: zeros)
 // UnstructuredMesh2D: the caller's outward normals by face [2, l, face, e] (faces as the curved interfaces);
 // null switches back to the StructuredMesh / P4estMesh interface conventions
+// source terms on the TreeMesh (LW and MDRK): kind 0 none, 1 source_terms_convergence_test; node coordinates
+// [2, i, j, e]
+int oracle_set_source(oracle_handle* h, int kind, const double* node_coordinates) {
+    if (h->curved || h->parabolic || kind < 0 || kind > 1 || (kind && !node_coordinates)) return 1;
+    if (kind) h->xnode.assign(node_coordinates, node_coordinates + (size_t)2 * h->basis.n * h->basis.n * h->mesh.n_elements);
+    else h->xnode.clear();
+    h->opt.source = kind;
+    h->opt.xnode = kind ? h->xnode.data() : nullptr;
+    return 0;
+}
+
 int oracle_set_unstructured_normals(oracle_handle* h, const double* normals) {
     if (!h->curved) return 1;
     CurvedMesh& m = h->cmesh;

@@ -41,6 +41,7 @@ def lib():
         L.oracle_set_temporal_errors.argtypes = [P, i32, dbl, dbl]
         L.oracle_set_curved_mortar_jacobian.argtypes = [P, P]
         L.oracle_set_unstructured_normals.argtypes = [P, P]
+        L.oracle_set_source.argtypes = [P, i32, P]
         L.oracle_dual_step.argtypes = [P, i32, P, P, dbl, P, P]
         L.oracle_set_shock_capturing.argtypes = [P, i32, dbl, dbl, i32]
         L.oracle_set_reconstruction.argtypes = [P, i32]
@@ -147,6 +148,15 @@ class Oracle:
                                     cm.mortar_large_faces, cm.mortar_large_reversed)
         if getattr(cm, "unstructured", False):
             self.set_unstructured_normals(cm.unormals)
+
+    def set_source(self, kind, node_coordinates=None):
+        """Source terms (TreeMesh, LW and MDRK): kind 0 none, 1 source_terms_convergence_test; node coordinates
+        [2, i, j, e] (the mesh's node_coordinates(N))."""
+        if kind:
+            self._xkeep = np.ascontiguousarray(node_coordinates, dtype=np.float64)
+            assert lib().oracle_set_source(self.h, int(kind), _p(self._xkeep)) == 0
+        else:
+            assert lib().oracle_set_source(self.h, 0, None) == 0
 
     def set_unstructured_normals(self, normals):
         """UnstructuredMesh2D interface conventions with the caller's outward normals by face, (E, 4, n, 2); None:

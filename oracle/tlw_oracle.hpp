@@ -358,12 +358,38 @@ struct Options {
     double alpha_max = 0.5, alpha_min = 0.001;
     bool alpha_smooth = true;
     int reconstruction = 0;        // curvilinear meshes: 0 FirstOrderReconstruction, 1 MUSCLReconstruction
+    // source terms (SemidiscretizationHyperbolic(...; source_terms)): 0 none, 1 Trixi's
+    // source_terms_convergence_test; node coordinates [2, i, j, e] (Trixi's cache.elements.node_coordinates)
+    int source = 0;
+    const double* xnode = nullptr;
 };
+
+// Trixi's source_terms_convergence_test for CompressibleEulerEquations2D: the source that makes the manufactured
+// solution rho = rho v1 = rho v2 = c + A sin(w (x + y - t)), rho e = rho^2 (c = 2, A = 0.1, L = 2, w = 2 pi / L,
+// initial_condition_convergence_test) exact. With rho' = w A cos(w (x + y - t)) (d/dt rho = -d/dx rho = -d/dy rho)
+// and p' = (gamma - 1)(2 rho - 1) rho': (rho', rho' (1 + tmp), rho' (1 + tmp), 2 rho' (rho + tmp)), tmp = (2 rho - 1)
+// (gamma - 1). It does not depend on u.
+inline void source_convergence_test(double gamma, double x1, double x2, double t, double* s) {
+    const double c = 2.0, A = 0.1, L = 2.0, f = 1.0 / L, w = 2.0 * 3.14159265358979323846 * f;
+    const double si = std::sin(w * (x1 + x2 - t)), co = std::cos(w * (x1 + x2 - t));
+    const double rho = c + A * si;
+    const double rho_x = w * A * co;
+    const double tmp = (2.0 * rho - 1.0) * (gamma - 1.0);
+    s[0] = rho_x;
+    s[1] = rho_x * (1.0 + tmp);
+    s[2] = s[1];
+    s[3] = 2.0 * rho_x * (rho + tmp);
+}
+inline void source_eval(int kind, double gamma, const double* /*u*/, double x1, double x2, double t, double* s) {
+    if (kind == 1) source_convergence_test(gamma, x1, x2, t, s);
+    else s[0] = s[1] = s[2] = s[3] = 0.0;
+}
 
 struct Workspace {
     // element cache
     std::vector<double> U, F;            // [v,i,j,e], [v,d,i,j,e]
     std::vector<double> U2, F2, us;      // MDRK cache (containers.jl:83-98)
+    std::vector<double> S2;              // MDRK stage 1's source S2 = s + st/6 [v,i,j,e] (source terms only)
     std::vector<double> temporal_errors; // [E]
     // interface cache [side, v, i, I]
     std::vector<double> iu, iU, iF;
@@ -390,14 +416,74 @@ inline size_t idx_F(int n, int v, int d, int i, int j, int e) {
 // du receives alpha * (Dhat F + Dhat G) (before surface integral and Jacobian); U/F are stored in ws.
 // ------------------------------------------------------------------------------------------------
 inline void lw_volume_element(const Basis& b, const Euler& eq, const Options& opt, int e, const double* u,
-                              double* du, double dt, double inv_jac, double alpha, Workspace& ws) {
+                              double* du, double dt, double inv_jac, double alpha, Workspace& ws, double t = 0.0) {
     const int n = b.n;
     const int nn = n * n;
     const int depth = std::min(opt.N, 4);
-    Tile f, g, Fc, Gc, Uc, up, um, upp, umm, ut, utt, uttt, utttt, unp1, unp1_low;
-    ut.zero(NV * nn); utt.zero(NV * nn); uttt.zero(NV * nn); utttt.zero(NV * nn);
+    Tile f, g, Fc, Gc, Uc, up, um, upp, umm, ut, utt, uttt, utttt, unp1, unp1_low, S;
+    ut.zero(NV * nn); utt.zero(NV * nn); uttt.zero(NV * nn); utttt.zero(NV * nn); S.zero(NV * nn);
     auto L = [&](int i, int j) { return NV * (i + n * j); };
     const double* ue = u + idx_u(n, 0, 0, 0, e);
+    // source terms: s(u_, dtau) = source_terms(u_, x, t + dtau) at node (i, j) (dg_2d.jl:89-175); the stencils
+    // calc_source_t_N12 / _t_N34 / _tt_N23 / _ttt_N34 / _tttt_N4 as the reference defines them
+    auto src = [&](const double* us, int i, int j, double dtau, double* o) {
+        const double* xn = opt.xnode + 2 * ((size_t)e * nn + i + (size_t)n * j);
+        source_eval(opt.source, eq.gamma, us, xn[0], xn[1], t + dtau, o);
+    };
+    auto st_N12 = [&](const double* up_, const double* um_, int i, int j, double* o) {
+        double a[NV], c[NV];
+        src(up_, i, j, dt, a);
+        src(um_, i, j, -dt, c);
+        for (int v = 0; v < NV; ++v) o[v] = 0.5 * (a[v] - c[v]);
+    };
+    auto st_N34 = [&](const double* up_, const double* upp_, const double* um_, const double* umm_, int i, int j,
+                      double* o) {
+        double a[NV], c[NV], d[NV], h[NV];
+        src(upp_, i, j, 2.0 * dt, a);
+        src(up_, i, j, dt, c);
+        src(um_, i, j, -dt, d);
+        src(umm_, i, j, -2.0 * dt, h);
+        for (int v = 0; v < NV; ++v) o[v] = (1.0 / 12.0) * (-a[v] + 8.0 * c[v] - 8.0 * d[v] + h[v]);
+    };
+    auto stt_N23 = [&](const double* u_, const double* up_, const double* um_, int i, int j, double* o) {
+        double a[NV], c[NV], d[NV];
+        src(up_, i, j, dt, a);
+        src(u_, i, j, 0.0, c);
+        src(um_, i, j, -dt, d);
+        for (int v = 0; v < NV; ++v) o[v] = a[v] - 2.0 * c[v] + d[v];
+    };
+    auto sttt_N34 = [&](const double* up_, const double* upp_, const double* um_, const double* umm_, int i, int j,
+                        double* o) {
+        double a[NV], c[NV], d[NV], h[NV];
+        src(upp_, i, j, 2.0 * dt, a);
+        src(up_, i, j, dt, c);
+        src(um_, i, j, -dt, d);
+        src(umm_, i, j, -2.0 * dt, h);
+        for (int v = 0; v < NV; ++v) o[v] = 0.5 * (a[v] - 2.0 * c[v] + 2.0 * d[v] - h[v]);
+    };
+    auto stttt_N4 = [&](const double* u_, const double* up_, const double* upp_, const double* um_,
+                        const double* umm_, int i, int j, double* o) {
+        double a[NV], c[NV], d[NV], h[NV], k[NV];
+        src(upp_, i, j, 2.0 * dt, a);
+        src(up_, i, j, dt, c);
+        src(u_, i, j, 0.0, d);
+        src(um_, i, j, -dt, h);
+        src(umm_, i, j, -2.0 * dt, k);
+        for (int v = 0; v < NV; ++v) o[v] = a[v] - 4.0 * c[v] + 6.0 * d[v] - 4.0 * h[v] + k[v];
+    };
+    // add (factor S, factor of the derivative) * stencil at every node; states read before this stage's update
+    auto add_source = [&](Tile& deriv, double cS, auto&& stencil) {
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const int o = L(i, j);
+                double st[NV];
+                stencil(o, i, j, st);
+                for (int v = 0; v < NV; ++v) {
+                    S[o + v] += cS * st[v];
+                    deriv[o + v] += dt * st[v];
+                }
+            }
+    };
 
     // contraction target += -dt * D (x: along i, y: along j), scatter form as in the reference loops
     auto contract = [&](const Tile& fx, const Tile& gy, Tile& tgt) {
@@ -444,6 +530,19 @@ inline void lw_volume_element(const Basis& b, const Euler& eq, const Options& op
     } else {
         contract(f, g, ut);
     }
+    if (opt.source) {
+        // S = s(u, x, t); ut += dt s (dg_2d.jl:979-987 and the same lines of kernels 1-3)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const int o = L(i, j);
+                double s0[NV];
+                src(ue + o, i, j, 0.0, s0);
+                for (int v = 0; v < NV; ++v) {
+                    S[o + v] = s0[v];
+                    ut[o + v] += dt * s0[v];
+                }
+            }
+    }
 
     double fp[NV], gp[NV], fm[NV], gm[NV], fpp[NV], gpp[NV], fmm[NV], gmm[NV];
     Tile ft, gt;
@@ -478,6 +577,13 @@ inline void lw_volume_element(const Basis& b, const Euler& eq, const Options& op
         }
     if (depth >= 2) {
         contract(ft, gt, utt);
+        if (opt.source) {
+            // st from the states after ut: N34 at depths 3, 4 (dg_2d.jl:1027-1040, :785-799), N12 at depth 2 (:605-615)
+            add_source(utt, 0.5, [&](int o, int i, int j, double* st) {
+                if (depth >= 3) st_N34(&up[o], &upp[o], &um[o], &umm[o], i, j, st);
+                else st_N12(&up[o], &um[o], i, j, st);
+            });
+        }
         // stage 2 (dg_2d.jl:1049-1083 depth 4; :801-831 depth 3; :617-634 depth 2)
         for (int j = 0; j < n; ++j)
             for (int i = 0; i < n; ++i) {
@@ -514,6 +620,10 @@ inline void lw_volume_element(const Basis& b, const Euler& eq, const Options& op
     }
     if (depth >= 3) {
         contract(ft, gt, uttt);
+        if (opt.source) {
+            // stt = calc_source_tt_N23 from the states after utt, at depth 4 as well (dg_2d.jl:1093-1104, :841-852)
+            add_source(uttt, 1.0 / 6.0, [&](int o, int i, int j, double* st) { stt_N23(ue + o, &up[o], &um[o], i, j, st); });
+        }
         // stage 3 (dg_2d.jl:1106-1138 depth 4; :854-875 depth 3)
         for (int j = 0; j < n; ++j)
             for (int i = 0; i < n; ++i) {
@@ -540,6 +650,12 @@ inline void lw_volume_element(const Basis& b, const Euler& eq, const Options& op
     }
     if (depth >= 4) {
         contract(ft, gt, utttt);
+        if (opt.source) {
+            // sttt from the states after uttt (dg_2d.jl:1148-1162)
+            add_source(utttt, 1.0 / 24.0, [&](int o, int i, int j, double* st) {
+                sttt_N34(&up[o], &upp[o], &um[o], &umm[o], i, j, st);
+            });
+        }
         // stage 4 (dg_2d.jl:1164-1226)
         for (int j = 0; j < n; ++j)
             for (int i = 0; i < n; ++i) {
@@ -585,6 +701,24 @@ inline void lw_volume_element(const Basis& b, const Euler& eq, const Options& op
                 }
             }
     }
+    if (opt.source) {
+        // the last stencil, from the states after the last derivative (the reference's argument lists as written):
+        //   depth 1: S += st_N12(up, um) / 2                         (dg_2d.jl:474-477)
+        //   depth 2: S += stt_N23(u, up, um) / 6                      (:651-654)
+        //   depth 3: S += sttt_N34(u, up, upp, upp, umm) / 24, i.e. upp in um's place (:891-897)
+        //   depth 4: S += stttt_N4(u, up, um, upp, umm) / 120 into (u, up, upp, um, umm): um and upp swap (:1227-1233)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const int o = L(i, j);
+                double st[NV];
+                double c;
+                if (depth == 1) { st_N12(&up[o], &um[o], i, j, st); c = 0.5; }
+                else if (depth == 2) { stt_N23(ue + o, &up[o], &um[o], i, j, st); c = 1.0 / 6.0; }
+                else if (depth == 3) { sttt_N34(&up[o], &upp[o], &upp[o], &umm[o], i, j, st); c = 1.0 / 24.0; }
+                else { stttt_N4(ue + o, &up[o], &um[o], &upp[o], &umm[o], i, j, st); c = 1.0 / 120.0; }
+                for (int v = 0; v < NV; ++v) S[o + v] += c * st[v];
+            }
+    }
     // final: du += alpha * Dhat (F, G); store U and F (dg_2d.jl:1208-1248, :876-912)
     double* due = du + idx_u(n, 0, 0, 0, e);
     for (int j = 0; j < n; ++j)
@@ -603,6 +737,9 @@ inline void lw_volume_element(const Basis& b, const Euler& eq, const Options& op
                 ws.F[idx_F(n, v, 1, i, j, e)] = Gc[o + v];
                 ws.U[idx_u(n, v, i, j, e)] = Uc[o + v];
             }
+            // du += -S / J^{-1} (apply_jacobian! multiplies by -J^{-1}: the source enters du unscaled)
+            if (opt.source)
+                for (int v = 0; v < NV; ++v) due[o + v] += (-1.0 / inv_jac) * S[o + v];
         }
     if (opt.temporal_errors && depth >= 4) {
         // dg_2d.jl:1251-1265
@@ -636,12 +773,37 @@ inline void mdrk_contra(const double* Jae, int n, int i, int j, const double* f,
     }
 }
 
+// source terms of the MDRK stages (TreeMesh): kind, node coordinates, gamma and the rhs call's t
+struct SourceArgs {
+    int kind = 0;
+    const double* xnode = nullptr;
+    double gamma = 1.4, t = 0.0;
+    // s(u_, x, t0 + dtau) at node (i, j) of element e
+    void at(int e, int n, int i, int j, const double* us, double t0, double dtau, double* o) const {
+        const double* xn = xnode + 2 * ((size_t)e * n * n + i + (size_t)n * j);
+        source_eval(kind, gamma, us, xn[0], xn[1], t0 + dtau, o);
+    }
+    // calc_source_t_N34 (dg_2d.jl:108-116) at time t0
+    void t_N34(int e, int n, int i, int j, const double* up, const double* upp, const double* um, const double* umm,
+               double t0, double dt, double* o) const {
+        double a[NV], c[NV], d[NV], h[NV];
+        at(e, n, i, j, upp, t0, 2.0 * dt, a);
+        at(e, n, i, j, up, t0, dt, c);
+        at(e, n, i, j, um, t0, -dt, d);
+        at(e, n, i, j, umm, t0, -2.0 * dt, h);
+        for (int v = 0; v < NV; ++v) o[v] = (1.0 / 12.0) * (-a[v] + 8.0 * c[v] - 8.0 * d[v] + h[v]);
+    }
+};
+
+// Stage 1 with source terms (multi_derivative_2d.jl:321-400): S = s/2 + st/8 enters du, S2 = s + st/6 is kept
+// for stage 2 (ws.S2); ut += dt s before the perturbed states.
 inline void mdrk1_volume_element(const Basis& b, const Euler& eq, int e, const double* u, double* du, double dt,
                                  double inv_jac, double alpha, Workspace& ws, const double* Jae = nullptr,
-                                 const double* ije = nullptr) {
+                                 const double* ije = nullptr, const SourceArgs* src = nullptr) {
     const int n = b.n, nn = n * n;
-    Tile Fh, Gh, F2, G2, Uh, U2, ut, f, g;
+    Tile Fh, Gh, F2, G2, Uh, U2, ut, f, g, Sh, S2;
     ut.zero(NV * nn);
+    const bool with_src = src && src->kind;
     auto L = [&](int i, int j) { return NV * (i + n * j); };
     const double* ue = u + idx_u(n, 0, 0, 0, e);
     for (int j = 0; j < n; ++j)
@@ -668,6 +830,18 @@ inline void mdrk1_volume_element(const Basis& b, const Euler& eq, int e, const d
             }
         }
     for (int k = 0; k < NV * nn; ++k) ut[k] *= Jae ? ije[k / NV] : inv_jac;
+    if (with_src)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const int o = L(i, j);
+                double s0[NV];
+                src->at(e, n, i, j, ue + o, src->t, 0.0, s0);
+                for (int v = 0; v < NV; ++v) {
+                    Sh[o + v] = 0.5 * s0[v];
+                    S2[o + v] = s0[v];
+                    ut[o + v] += dt * s0[v];
+                }
+            }
     double* due = du + idx_u(n, 0, 0, 0, e);
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
@@ -678,6 +852,16 @@ inline void mdrk1_volume_element(const Basis& b, const Euler& eq, int e, const d
                 up[v] = ue[o + v] + ut[o + v];
                 umm[v] = ue[o + v] - 2 * ut[o + v];
                 upp[v] = ue[o + v] + 2 * ut[o + v];
+            }
+            if (with_src) {
+                double st[NV];
+                src->t_N34(e, n, i, j, up, upp, um, umm, src->t, dt, st);
+                for (int v = 0; v < NV; ++v) {
+                    Sh[o + v] += 0.125 * st[v];
+                    S2[o + v] += 1.0 / 6.0 * st[v];
+                    due[o + v] += (-1.0 / inv_jac) * Sh[o + v];
+                    ws.S2[idx_u(n, v, i, j, e)] = S2[o + v];
+                }
             }
             double fm[NV], gm[NV], fp[NV], gp[NV], fmm[NV], gmm[NV], fpp[NV], gpp[NV];
             eq.fluxes(um, fm, gm);
@@ -716,12 +900,15 @@ inline void mdrk1_volume_element(const Basis& b, const Euler& eq, int e, const d
         }
 }
 
+// Stage 2 with source terms (multi_derivative_2d.jl:484-550): S = S2 + st(u*)/3 at t + dt/2, ust += dt s(u*, t + dt/2).
 inline void mdrk2_volume_element(const Basis& b, const Euler& eq, int e, const double* us, double* du, double dt,
                                  double inv_jac, double alpha, Workspace& ws, const double* Jae = nullptr,
-                                 const double* ije = nullptr) {
+                                 const double* ije = nullptr, const SourceArgs* src = nullptr) {
     const int n = b.n, nn = n * n;
     Tile Fc, Gc, Uc, ust;
     ust.zero(NV * nn);
+    const bool with_src = src && src->kind;
+    const double th = with_src ? src->t + 0.5 * dt : 0.0;
     auto L = [&](int i, int j) { return NV * (i + n * j); };
     const double* ue = us + idx_u(n, 0, 0, 0, e);
     for (int j = 0; j < n; ++j)
@@ -746,6 +933,14 @@ inline void mdrk2_volume_element(const Basis& b, const Euler& eq, int e, const d
             }
         }
     for (int k = 0; k < NV * nn; ++k) ust[k] *= Jae ? ije[k / NV] : inv_jac;
+    if (with_src)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const int o = L(i, j);
+                double s0[NV];
+                src->at(e, n, i, j, ue + o, th, 0.0, s0);
+                for (int v = 0; v < NV; ++v) ust[o + v] += dt * s0[v];
+            }
     double* due = du + idx_u(n, 0, 0, 0, e);
     for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
@@ -756,6 +951,12 @@ inline void mdrk2_volume_element(const Basis& b, const Euler& eq, int e, const d
                 up[v] = ue[o + v] + ust[o + v];
                 umm[v] = ue[o + v] - 2 * ust[o + v];
                 upp[v] = ue[o + v] + 2 * ust[o + v];
+            }
+            if (with_src) {
+                double st[NV];
+                src->t_N34(e, n, i, j, up, upp, um, umm, th, dt, st);
+                for (int v = 0; v < NV; ++v)
+                    due[o + v] += (-1.0 / inv_jac) * (ws.S2[idx_u(n, v, i, j, e)] + 1.0 / 3.0 * st[v]);
             }
             double fm[NV], gm[NV], fp[NV], gp[NV], fmm[NV], gmm[NV], fpp[NV], gpp[NV];
             eq.fluxes(um, fm, gm);
@@ -1023,6 +1224,7 @@ inline void ensure_workspace(const Basis& b, const TreeMesh& m, Workspace& ws, b
     if (mdrk) {
         if (ws.U2.size() != NV * nodes) ws.U2.assign(NV * nodes, nan);
         if (ws.F2.size() != 2 * NV * nodes) ws.F2.assign(2 * NV * nodes, nan);
+        if (ws.S2.size() != NV * nodes) ws.S2.assign(NV * nodes, nan);
     }
     ws.surface_flux_values.assign((size_t)NV * b.n * 4 * m.n_elements, nan);
     if (ws.temporal_errors.size() != (size_t)m.n_elements) ws.temporal_errors.assign(m.n_elements, nan);
@@ -1229,7 +1431,6 @@ inline void calc_interface_flux_blended(const Basis& b, const Euler& eq, const O
 inline void rhs(const Basis& b, const Euler& eq, const Options& opt, const TreeMesh& m, const double* u,
                 const double* u2, double* du, double t, double dt, const BoundaryData* bd, int kind, Workspace& ws,
                 int nthreads = 1) {
-    (void)t;
     ensure_workspace(b, m, ws, kind != 0);
     ws.bad = false;
     const size_t ndof = (size_t)NV * b.n * b.n * m.n_elements;
@@ -1245,12 +1446,13 @@ inline void rhs(const Basis& b, const Euler& eq, const Options& opt, const TreeM
 #pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad_fv)
     for (int e = 0; e < m.n_elements; ++e) {
         const double a = opt.shock_capturing ? 1.0 - ws.alpha[e] : 1.0;
+        const SourceArgs sa{opt.source, opt.xnode, eq.gamma, t};
         if (kind == 0)
-            lw_volume_element(b, eq, opt, e, u, du, dt, m.inverse_jacobian[e], a, ws);
+            lw_volume_element(b, eq, opt, e, u, du, dt, m.inverse_jacobian[e], a, ws, t);
         else if (kind == 1)
-            mdrk1_volume_element(b, eq, e, u, du, dt, m.inverse_jacobian[e], a, ws);
+            mdrk1_volume_element(b, eq, e, u, du, dt, m.inverse_jacobian[e], a, ws, nullptr, nullptr, &sa);
         else
-            mdrk2_volume_element(b, eq, e, u2, du, dt, m.inverse_jacobian[e], a, ws);
+            mdrk2_volume_element(b, eq, e, u2, du, dt, m.inverse_jacobian[e], a, ws, nullptr, nullptr, &sa);
         if (opt.shock_capturing) {
             // pure_and_blended_element_ids!: DG only where isapprox(alpha, 0, atol = 1e-12)
             const bool blended = !(std::fabs(ws.alpha[e]) <= 1e-12);

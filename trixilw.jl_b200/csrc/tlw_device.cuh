@@ -55,10 +55,9 @@ __device__ __forceinline__ double nr_reciprocal(double x) {
     return fma(y, e, y);
 }
 
-// Euler flux pair (Trixi flux(u, 1|2, eq) for CompressibleEulerEquations2D); 1 reciprocal, ~17 flops.
-__device__ __forceinline__ void euler_fluxes(double gm1, double r, double m1, double m2, double e, double* f,
-                                             double* g) {
-    const double ir = nr_reciprocal(r);
+// Euler flux pair (Trixi flux(u, 1|2, eq) for CompressibleEulerEquations2D) from 1/rho; ~17 flops.
+__device__ __forceinline__ void euler_fluxes_ir(double gm1, double ir, double m1, double m2, double e, double* f,
+                                                double* g) {
     const double v1 = m1 * ir, v2 = m2 * ir;
     const double p = gm1 * (e - 0.5 * (m1 * v1 + m2 * v2));
     const double ep = e + p;
@@ -70,6 +69,11 @@ __device__ __forceinline__ void euler_fluxes(double gm1, double r, double m1, do
     g[1] = f[2];
     g[2] = m2 * v2 + p;
     g[3] = ep * v2;
+}
+// the same from rho: 1 reciprocal
+__device__ __forceinline__ void euler_fluxes(double gm1, double r, double m1, double m2, double e, double* f,
+                                             double* g) {
+    euler_fluxes_ir(gm1, nr_reciprocal(r), m1, m2, e, f, g);
 }
 
 __device__ __forceinline__ void euler_flux_dir(double gm1, const double* u, int orientation, double* fo) {

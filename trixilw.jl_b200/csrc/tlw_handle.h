@@ -91,6 +91,10 @@ struct tlw_handle {
     double* d_inv_jac = nullptr;
     int *d_xl = nullptr, *d_xr = nullptr, *d_yl = nullptr, *d_yr = nullptr;
     int* d_nbr = nullptr;   // [4, E] element across each face when every face is a conforming interface
+    // source terms (TreeMesh, FR volume integral): kind, node coordinates [2, i, j, e], MDRK stage 1's S2
+    int source = 0;
+    double* d_xnode = nullptr;
+    double* d_S2 = nullptr;
     int nx = 0, ny = 0;
     int64_t nb = 0;
     int *d_b_elem = nullptr, *d_b_dir = nullptr, *d_bx = nullptr, *d_by = nullptr;

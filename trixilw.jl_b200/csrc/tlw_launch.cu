@@ -45,6 +45,29 @@ struct LaunchImpl {
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        // source terms (TreeMesh, FR)
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, false, false, false, 0, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, false, false, 0, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, false, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, false, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+    }
+    // source terms on the TreeMesh (FR volume integral): LW or an MDRK stage
+    static void volume_src(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
+        const size_t lw = C::smem_bytes(4), md = C::smem_bytes(2);
+        if (stage == TLW_STAGE_LW) {
+            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, false, 0, false, false, false, 0, true><<<grid, C::THREADS, lw, s>>>(a);
+            else lw_volume_kernel<N, MODE_STEP, false, 0, false, false, false, 0, true><<<grid, C::THREADS, lw, s>>>(a);
+        } else if (stage == TLW_STAGE_MDRK1) {
+            if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS, false, false, 0, true><<<grid, C::THREADS, md, s>>>(a);
+            else mdrk1_volume_kernel<N, MODE_STEP, false, false, 0, true><<<grid, C::THREADS, md, s>>>(a);
+        } else {
+            if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS, false, false, 0, true><<<grid, C::THREADS, md, s>>>(a);
+            else mdrk2_volume_kernel<N, MODE_STEP, false, false, 0, true><<<grid, C::THREADS, md, s>>>(a);
+        }
     }
     template <bool SC>
     static void volume_sc(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
@@ -118,6 +141,10 @@ struct LaunchImpl {
         if (grid == 0) return;
         if (a.temporal_errors) {
             te_volume(s, a, grid, sc, false);
+            return;
+        }
+        if (a.source && !a.metrics && !sc) {
+            volume_src(s, stage, mode, a, grid);
             return;
         }
         if (a.metrics && sc) {   // curvilinear mesh with shock capturing (MUSCL when the geometry is given)

@@ -420,6 +420,8 @@ struct StepState {
     unsigned status;               // STATUS_* bits
     int pad;
     double dt_call;                // dt for the rhs entry points (set from the host)
+    double t_step;                 // time at the start of the current step (source terms)
+    double t_call;                 // t of the rhs entry points (set from the host; source terms)
 };
 
 constexpr int MS_THREADS = 256;
@@ -614,6 +616,7 @@ static __global__ void finalize_dt_kernel(StepState* s, int n) {
     const bool finished = run_finished(t, te);
     if (finished) dt = 0.0;
     else if (t + dt > te) dt = te - t;
+    s->t_step = t;
     s->dt = dt;
     s->t = finished ? t : t + dt;
     if (!finished) s->steps += 1;

@@ -68,6 +68,12 @@ struct VolArgs {
     double* tU;             // face traces of U   [v, l, face, e]
     double* tF;             // face traces of F.n [v, l, face, e]
     double* tG;             // UnstructuredMesh2D: physical flux traces, tF <- F and tG <- G (null otherwise)
+    // source terms (TreeMesh, FR volume integral): kind (1: source_terms_convergence_test), node coordinates
+    // [2, i, j, e], the time of this rhs (device scalar), MDRK stage 1's S2 = s + s_t/6 [v, i, j, e]
+    int source;
+    const double* xnode;
+    const double* tnow;
+    double* S2;
     double* U2;             // MDRK: stage-1 U2 [v,i,j,e] (written by stage 1, read by stage 2)
     double* F2;             // MDRK: stage-1 F2 [v,d,i,j,e]
     const double* inv_jac;  // [e]
@@ -529,15 +535,23 @@ __device__ __forceinline__ void sc_blend_curved(const VolArgs& a, const double* 
 template <int n, int MODE>
 __device__ __forceinline__ void volume_epilogue(const VolArgs& a, int e, int i, int j, int node, double ij, double dt,
                                                 const double* acc, const double* U, const double* F,
-                                                const double* G, double* o) {
+                                                const double* G, double* o, const double* S = nullptr) {
     const size_t off = ((size_t)e * n * n + node) * NV;
     if (MODE == MODE_RHS) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) o[v] = -ij * acc[v];
+        if (S) {   // du += S (the source enters unscaled by J^{-1})
+#pragma unroll
+            for (int v = 0; v < NV; ++v) o[v] += S[v];
+        }
     } else {
         double ub[NV];
         load4(a.u_base + off, ub);
         const double s = -dt * ij;
+        if (S) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) ub[v] = fma(dt, S[v], ub[v]);
+        }
 #pragma unroll
         for (int v = 0; v < NV; ++v) o[v] = fma(s, acc[v], ub[v]);
     }
@@ -563,6 +577,77 @@ __device__ __forceinline__ void physical_flux_traces(const VolArgs& a, int e, in
     if (j == n - 1) { store4(a.tF + tb + (3 * n + i) * NV, F); store4(a.tG + tb + (3 * n + i) * NV, G); }
 }
 
+// ---- source terms (calc_source / calc_source_t_N12 ... _tttt_N4, src/solvers/dgsem_tree/dg_2d.jl:89-175) ----
+// Kind 1, Trixi's source_terms_convergence_test for CompressibleEulerEquations2D: the source of the manufactured
+// solution rho = rho v1 = rho v2 = c + A sin(w (x + y - t)), rho e = rho^2 (c = 2, A = 0.1, w = 2 pi / L, L = 2):
+// with rho' = w A cos(w (x + y - t)) and tmp = (2 rho - 1)(gamma - 1), s = (rho', rho' (1 + tmp), rho' (1 + tmp),
+// 2 rho' (rho + tmp)). It does not depend on u, so every stencil of the reference is a combination of
+// s(x, t + k dt), k = -2..2, and the reference's argument-order slips in two of its calls (dg_2d.jl:891-897,
+// :1227-1233: states in the wrong slots) leave the values unchanged.
+struct SrcNode {
+    double x1, x2, t, dt, gamma;
+};
+__device__ __forceinline__ void src_eval(const SrcNode& q, double k, double* s) {
+    const double w = 2.0 * 3.14159265358979323846 * (1.0 / 2.0);
+    const double arg = w * (q.x1 + q.x2 - (q.t + k * q.dt));
+    const double si = sin(arg), co = cos(arg);
+    const double rho = 2.0 + 0.1 * si;
+    const double rho_x = w * 0.1 * co;
+    const double tmp = (2.0 * rho - 1.0) * (q.gamma - 1.0);
+    s[0] = rho_x;
+    s[1] = rho_x * (1.0 + tmp);
+    s[2] = s[1];
+    s[3] = 2.0 * rho_x * (rho + tmp);
+}
+// o = c * sum_k w_k s(t + k dt), k = -2..2 (zero weights skipped)
+__device__ __forceinline__ void src_term(const SrcNode& q, double w, double k, double* acc) {
+    if (w == 0.0) return;
+    double s[NV];
+    src_eval(q, k, s);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = fma(w, s[v], acc[v]);
+}
+__device__ __forceinline__ void src_stencil(const SrcNode& q, double c, double wm2, double wm1, double w0, double wp1,
+                                            double wp2, double* o) {
+    double acc[NV] = {0.0, 0.0, 0.0, 0.0};
+    src_term(q, wm2, -2.0, acc);
+    src_term(q, wm1, -1.0, acc);
+    src_term(q, w0, 0.0, acc);
+    src_term(q, wp1, 1.0, acc);
+    src_term(q, wp2, 2.0, acc);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) o[v] = c * acc[v];
+}
+// the reference's stencils (each with its own time offsets)
+__device__ __forceinline__ void src_t_N12(const SrcNode& q, double* o) { src_stencil(q, 0.5, 0.0, -1.0, 0.0, 1.0, 0.0, o); }
+__device__ __forceinline__ void src_t_N34(const SrcNode& q, double* o) {
+    src_stencil(q, 1.0 / 12.0, 1.0, -8.0, 0.0, 8.0, -1.0, o);
+}
+__device__ __forceinline__ void src_tt_N23(const SrcNode& q, double* o) { src_stencil(q, 1.0, 0.0, 1.0, -2.0, 1.0, 0.0, o); }
+__device__ __forceinline__ void src_ttt_N34(const SrcNode& q, double* o) {
+    src_stencil(q, 0.5, -1.0, 2.0, 0.0, -2.0, 1.0, o);
+}
+__device__ __forceinline__ void src_tttt_N4(const SrcNode& q, double* o) {
+    src_stencil(q, 1.0, 1.0, -4.0, 6.0, -4.0, 1.0, o);
+}
+
+// The stage's four flux pairs at upp, up, um, umm. With TLW_VOL_ILP the four reciprocals 1/rho are refined
+// first, as four independent Newton chains, instead of one chain per flux pair; same operations, same bits.
+#ifndef TLW_VOL_ILP
+#define TLW_VOL_ILP 1
+#endif
+struct Recip4 {
+    double pp, p, m, mm;
+};
+__device__ __forceinline__ Recip4 recip4(const double* upp, const double* up, const double* um, const double* umm) {
+    Recip4 r;
+    r.pp = nr_reciprocal(upp[0]);
+    r.p = nr_reciprocal(up[0]);
+    r.m = nr_reciprocal(um[0]);
+    r.mm = nr_reciprocal(umm[0]);
+    return r;
+}
+
 // ------------------------------------------------------------------------------------------------
 // Plain LW volume kernel (depth = min(N, 4)).
 // The finite-difference stencils are accumulated unscaled ("raw"); their constant factors and -dt J^{-1}
@@ -583,11 +668,16 @@ __device__ __forceinline__ void store_stage_derivative(const VolArgs& a, int m, 
 }
 
 // REC (curvilinear shock capturing): 0 first-order subcells, 1 MUSCL subcells
-template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false, int REC = 0>
+// SRC: source terms (a.source, TreeMesh, FR volume integral): S = s + s_t/2 + s_tt/6 + ... with each stencil added
+// to its time derivative (dt s_k) before the perturbed states move, and S enters the update unscaled by J^{-1}.
+template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false, int REC = 0,
+          bool SRC = false>
 static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED) ? VolCfg<N, EBX>::SC_CURVED_MIN_BLOCKS
-                                                                                 : VolCfg<N, EBX>::MIN_BLOCKS)
+                                                                  : SRC ? VolCfg<N, EBX>::MDRK_MIN_BLOCKS - 1
+                                                                        : VolCfg<N, EBX>::MIN_BLOCKS)
     lw_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
+    static_assert(!SRC || (!SC && !CURVED && !TE && !DSTORE), "source terms: the plain TreeMesh kernel");
     // the temporal error estimate of the Adaptive step control: the TreeMesh computes it at depth 4 only
     // (lw_volume_kernel_3! of dgsem_tree has none), the curvilinear kernels at depths 3 and 4
     static_assert(!TE || (CURVED ? N >= 3 : N >= 4), "temporal errors: TreeMesh N >= 4, curvilinear N >= 3");
@@ -632,6 +722,8 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
     constexpr bool SLOTS = MODE == MODE_STEP && !SC && !CURVED;
 
     double U[NV], F[NV], G[NV], up[NV], um[NV], upp[NV], umm[NV];
+    double Ssrc[NV] = {0.0, 0.0, 0.0, 0.0};   // SRC: the source's time average S
+    SrcNode sq{};
     double s0 = 0.0, ij = 0.0;   // s0 = -dt J^{-1} (of the element, or of the node on curvilinear meshes)
     double Ja[4] = {0.0, 0.0, 0.0, 0.0};
     double dF[NV], dG[NV], u0[NV];   // TE: the last stage's term of F, G, and u
@@ -644,6 +736,11 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
         } else {
             node_put<N, C>(X, Y, el, i, j, f, g);
         }
+    };
+    // a flux pair at a perturbed state, from its precomputed 1/rho (TLW_VOL_ILP) or its own reciprocal
+    auto flux = [&](const double* st, double irr, double* f, double* g) {
+        if (TLW_VOL_ILP) euler_fluxes_ir(gm1, irr, st[1], st[2], st[3], f, g);
+        else euler_fluxes(gm1, st[0], st[1], st[2], st[3], f, g);
     };
     // stage 0: f, g at u (dg_2d.jl:941-971; dgsem_structured/dg_2d.jl:1709-1740)
     if (active) {
@@ -660,6 +757,12 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             ij = __ldg(a.inv_jac + e);
         }
         s0 = -dt * ij;
+        if (SRC) {
+            // S = s(u, x, t) (dg_2d.jl:979-987)
+            const double* xn = a.xnode + 2 * ((size_t)e * nn + node);
+            sq = SrcNode{__ldg(xn), __ldg(xn + 1), *a.tnow, dt, a.gamma};
+            src_eval(sq, 0.0, Ssrc);
+        }
         euler_fluxes(gm1, uu[0], uu[1], uu[2], uu[3], f, g);
         put(f, g);
         if (DEPTH >= 2 || SC) node_put<N, C>(F0X, F0Y, el, i, j, f, g);
@@ -682,6 +785,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             d[v] *= s0;
+            if (SRC) d[v] = fma(dt, Ssrc[v], d[v]);   // ut += dt s
             U[v] = fma(0.5, d[v], U[v]);
             up[v] += d[v];
             um[v] -= d[v];
@@ -690,16 +794,17 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
         if (DSTORE) store_stage_derivative<nn>(a, 1, e, node, d);
         if (DEPTH >= 3) {
             // raw1 = -f(u+2ut) + 8 f(u+ut) - 8 f(u-ut) + f(u-2ut)
-            euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
+            const Recip4 rc = TLW_VOL_ILP ? recip4(upp, up, um, umm) : Recip4{0.0, 0.0, 0.0, 0.0};
+            flux(upp, rc.pp, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { r[v] = -f[v]; q[v] = -g[v]; }
-            euler_fluxes(gm1, up[0], up[1], up[2], up[3], f, g);
+            flux(up, rc.p, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { r[v] = fma(8.0, f[v], r[v]); q[v] = fma(8.0, g[v], q[v]); }
-            euler_fluxes(gm1, um[0], um[1], um[2], um[3], f, g);
+            flux(um, rc.m, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { r[v] = fma(-8.0, f[v], r[v]); q[v] = fma(-8.0, g[v], q[v]); }
-            euler_fluxes(gm1, umm[0], umm[1], umm[2], umm[3], f, g);
+            flux(umm, rc.mm, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { r[v] += f[v]; q[v] += g[v]; }
         } else {
@@ -725,9 +830,18 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             node_sum<N, C>(X, Y, el, i, j, d);
             node_get<N, C>(F0X, F0Y, el, i, j, f0, g0);
             const double s = s0 * C1;
+            double sk[NV];
+            if (SRC) {   // s_t from the states after ut: N34 at depths 3, 4, N12 at depth 2 (dg_2d.jl:1027-1040)
+                if (DEPTH >= 3) src_t_N34(sq, sk);
+                else src_t_N12(sq, sk);
+            }
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 d[v] *= s;
+                if (SRC) {
+                    Ssrc[v] = fma(0.5, sk[v], Ssrc[v]);
+                    d[v] = fma(dt, sk[v], d[v]);
+                }
                 U[v] = fma(1.0 / 6.0, d[v], U[v]);
                 up[v] = fma(0.5, d[v], up[v]);
                 um[v] = fma(0.5, d[v], um[v]);
@@ -736,19 +850,20 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             if (DSTORE) store_stage_derivative<nn>(a, 2, e, node, d);
             if (DEPTH == 4) {
                 // raw2 = -f(upp) + 16 f(up) - 30 f0 + 16 f(um) - f(umm)
-                euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
+                const Recip4 rc = TLW_VOL_ILP ? recip4(upp, up, um, umm) : Recip4{0.0, 0.0, 0.0, 0.0};
+                flux(upp, rc.pp, f, g);
 #pragma unroll
                 for (int v = 0; v < NV; ++v) {
                     r[v] = fma(-30.0, f0[v], -f[v]);
                     q[v] = fma(-30.0, g0[v], -g[v]);
                 }
-                euler_fluxes(gm1, up[0], up[1], up[2], up[3], f, g);
+                flux(up, rc.p, f, g);
 #pragma unroll
                 for (int v = 0; v < NV; ++v) { r[v] = fma(16.0, f[v], r[v]); q[v] = fma(16.0, g[v], q[v]); }
-                euler_fluxes(gm1, um[0], um[1], um[2], um[3], f, g);
+                flux(um, rc.m, f, g);
 #pragma unroll
                 for (int v = 0; v < NV; ++v) { r[v] = fma(16.0, f[v], r[v]); q[v] = fma(16.0, g[v], q[v]); }
-                euler_fluxes(gm1, umm[0], umm[1], umm[2], umm[3], f, g);
+                flux(umm, rc.mm, f, g);
 #pragma unroll
                 for (int v = 0; v < NV; ++v) { r[v] -= f[v]; q[v] -= g[v]; }
             } else {
@@ -777,9 +892,15 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             double d[NV], r[NV], q[NV], f[NV], g[NV];
             node_sum<N, C>(X, Y, el, i, j, d);
             const double s = s0 * C2;
+            double sk[NV];
+            if (SRC) src_tt_N23(sq, sk);   // s_tt = calc_source_tt_N23 at depths 3 and 4 (dg_2d.jl:1093-1104)
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 d[v] *= s;
+                if (SRC) {
+                    Ssrc[v] = fma(1.0 / 6.0, sk[v], Ssrc[v]);
+                    d[v] = fma(dt, sk[v], d[v]);
+                }
                 U[v] = fma(1.0 / 24.0, d[v], U[v]);
                 um[v] = fma(-1.0 / 6.0, d[v], um[v]);
                 up[v] = fma(1.0 / 6.0, d[v], up[v]);
@@ -788,16 +909,17 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             }
             if (DSTORE) store_stage_derivative<nn>(a, 3, e, node, d);
             // raw3 = f(upp) - 2 f(up) + 2 f(um) - f(umm)
-            euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
+            const Recip4 rc = TLW_VOL_ILP ? recip4(upp, up, um, umm) : Recip4{0.0, 0.0, 0.0, 0.0};
+            flux(upp, rc.pp, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { r[v] = f[v]; q[v] = g[v]; }
-            euler_fluxes(gm1, up[0], up[1], up[2], up[3], f, g);
+            flux(up, rc.p, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { r[v] = fma(-2.0, f[v], r[v]); q[v] = fma(-2.0, g[v], q[v]); }
-            euler_fluxes(gm1, um[0], um[1], um[2], um[3], f, g);
+            flux(um, rc.m, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { r[v] = fma(2.0, f[v], r[v]); q[v] = fma(2.0, g[v], q[v]); }
-            euler_fluxes(gm1, umm[0], umm[1], umm[2], umm[3], f, g);
+            flux(umm, rc.mm, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 r[v] -= f[v];
@@ -819,9 +941,15 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             node_sum<N, C>(X, Y, el, i, j, d);
             node_get<N, C>(F0X, F0Y, el, i, j, f0, g0);
             const double s = s0 * C3;
+            double sk[NV];
+            if (SRC) src_ttt_N34(sq, sk);   // s_ttt (dg_2d.jl:1148-1162)
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 d[v] *= s;
+                if (SRC) {
+                    Ssrc[v] = fma(1.0 / 24.0, sk[v], Ssrc[v]);
+                    d[v] = fma(dt, sk[v], d[v]);
+                }
                 U[v] = fma(1.0 / 120.0, d[v], U[v]);
                 um[v] = fma(1.0 / 24.0, d[v], um[v]);
                 up[v] = fma(1.0 / 24.0, d[v], up[v]);
@@ -830,16 +958,17 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             }
             if (DSTORE) store_stage_derivative<nn>(a, 4, e, node, d);
             // raw4 = f(upp) - 4 f(up) + 6 f0 - 4 f(um) + f(umm)
-            euler_fluxes(gm1, upp[0], upp[1], upp[2], upp[3], f, g);
+            const Recip4 rc = TLW_VOL_ILP ? recip4(upp, up, um, umm) : Recip4{0.0, 0.0, 0.0, 0.0};
+            flux(upp, rc.pp, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { r[v] = fma(6.0, f0[v], f[v]); q[v] = fma(6.0, g0[v], g[v]); }
-            euler_fluxes(gm1, up[0], up[1], up[2], up[3], f, g);
+            flux(up, rc.p, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { r[v] = fma(-4.0, f[v], r[v]); q[v] = fma(-4.0, g[v], q[v]); }
-            euler_fluxes(gm1, um[0], um[1], um[2], um[3], f, g);
+            flux(um, rc.m, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) { r[v] = fma(-4.0, f[v], r[v]); q[v] = fma(-4.0, g[v], q[v]); }
-            euler_fluxes(gm1, umm[0], umm[1], umm[2], umm[3], f, g);
+            flux(umm, rc.mm, f, g);
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 r[v] += f[v];
@@ -852,6 +981,18 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
     }
     // final: Dhat contraction of the time-averaged fluxes (every owner has read its node's results of
     // the last contraction before writing F, G over them: same address, same thread)
+    if (SRC && active) {
+        // the last stencil: depth 1 s_t / 2 (N12), 2 s_tt / 6 (N23), 3 s_ttt / 24, 4 s_tttt / 120
+        // (dg_2d.jl:474-477, :651-654, :891-897, :1227-1233)
+        double sk[NV];
+        if (DEPTH == 1) src_t_N12(sq, sk);
+        else if (DEPTH == 2) src_tt_N23(sq, sk);
+        else if (DEPTH == 3) src_ttt_N34(sq, sk);
+        else src_tttt_N4(sq, sk);
+        const double c = DEPTH == 1 ? 0.5 : DEPTH == 2 ? 1.0 / 6.0 : DEPTH == 3 ? 1.0 / 24.0 : 1.0 / 120.0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Ssrc[v] = fma(c, sk[v], Ssrc[v]);
+    }
     if (active) {
         if (CURVED) {
             if (a.tG) physical_flux_traces<n>(a, e, i, j, F, G);
@@ -884,7 +1025,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             if constexpr (CURVED) sc_blend_curved<N, C>(a, FVX, FVY, el, e, i, j, alpha_e, blended, acc);
             else sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
         }
-        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o);
+        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o, SRC ? Ssrc : nullptr);
         if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) node_speeds(a.gamma, o, a.status, l1, l2);
     }
     if (SLOTS && a.cfl_slots) {
@@ -960,11 +1101,14 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
 // ------------------------------------------------------------------------------------------------
 // CURVED (mdrk_kernel_1!, src/solvers/dgsem_structured/multi_derivative_2d.jl:82-243): the contractions take the
 // contravariant fluxes, d carries the node's J^{-1}; F2, G2 stay physical, the traces are contravariant.
-template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0>
+// SRC (TreeMesh, FR): ut += dt s(u, t); S = s/2 + s_t/8 enters du, S2 = s + s_t/6 is stored for stage 2
+// (multi_derivative_2d.jl:321-400).
+template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false>
 static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
                                                                          : VolCfg<N>::MDRK_MIN_BLOCKS)
     mdrk1_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
+    static_assert(!SRC || (!SC && !CURVED), "source terms: the plain TreeMesh kernel");
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
@@ -1025,13 +1169,22 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
     if (SC && CURVED && REC >= 1 && muscl) sc_muscl_faces<N, C, REC>(a, UU, UF, el, e, i, j, gm1, alpha_e, 0.5 * dt, ij);
     line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
-    double U[NV], F[NV], G[NV];
+    double U[NV], F[NV], G[NV], Ssrc[NV] = {0.0, 0.0, 0.0, 0.0};
     if (active) {
         double d[NV], ft[NV], gt[NV], f[NV], g[NV], s[NV];
         node_sum<N, C>(X, Y, el, i, j, d);
         const double s0 = -dt * ij;
 #pragma unroll
         for (int v = 0; v < NV; ++v) d[v] *= s0;
+        SrcNode sq{};
+        double sn[NV];
+        if (SRC) {
+            const double* xn = a.xnode + 2 * ((size_t)e * nn + node);
+            sq = SrcNode{__ldg(xn), __ldg(xn + 1), *a.tnow, dt, a.gamma};
+            src_eval(sq, 0.0, sn);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) d[v] = fma(dt, sn[v], d[v]);
+        }
 #pragma unroll
         for (int v = 0; v < NV; ++v) s[v] = fma(2.0, d[v], uu[v]);
         euler_fluxes(gm1, s[0], s[1], s[2], s[3], f, g);
@@ -1060,6 +1213,16 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
         store4(a.U2 + off * NV, U2v);
         store4(a.F2 + off * 2 * NV, F2v);
         store4(a.F2 + off * 2 * NV + NV, G2v);
+        if (SRC) {
+            double st[NV], S2v[NV];
+            src_t_N34(sq, st);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                Ssrc[v] = fma(0.125, st[v], 0.5 * sn[v]);
+                S2v[v] = fma(1.0 / 6.0, st[v], sn[v]);
+            }
+            store4(a.S2 + off * NV, S2v);
+        }
         if (CURVED) {
             double ft2[NV], gt2[NV];
             contravariant(Ja, F, G, ft2, gt2);
@@ -1083,7 +1246,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
             else sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
         }
         double o[NV];
-        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o);
+        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o, SRC ? Ssrc : nullptr);
     }
 }
 
@@ -1092,11 +1255,13 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
 // F = F2 + f_t(u*)/3, U = U2 + u*_t/3.
 // ------------------------------------------------------------------------------------------------
 // CURVED (mdrk_kernel_2!, src/solvers/dgsem_structured/multi_derivative_2d.jl:245-445): as in stage 1.
-template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0>
+// SRC (TreeMesh, FR): at t + dt/2, u*_t += dt s(u*); S = S2 + s_t(u*)/3 (multi_derivative_2d.jl:484-550).
+template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false>
 static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
                                                                          : VolCfg<N>::MDRK_MIN_BLOCKS)
     mdrk2_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
+    static_assert(!SRC || (!SC && !CURVED), "source terms: the plain TreeMesh kernel");
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
@@ -1157,13 +1322,25 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
     if (SC && CURVED && REC >= 1 && muscl) sc_muscl_faces<N, C, REC>(a, UU, UF, el, e, i, j, gm1, alpha_e, dt, ij);
     line_contract<N, C, false>(X, Y, tid);
     __syncthreads();
-    double U[NV], F[NV], G[NV];
+    double U[NV], F[NV], G[NV], Ssrc[NV] = {0.0, 0.0, 0.0, 0.0};
     if (active) {
         double d[NV], ft[NV], gt[NV], f[NV], g[NV], s[NV];
         node_sum<N, C>(X, Y, el, i, j, d);
         const double s0 = -dt * ij;
 #pragma unroll
         for (int v = 0; v < NV; ++v) d[v] *= s0;
+        if (SRC) {
+            const double* xn = a.xnode + 2 * ((size_t)e * nn + node);
+            const SrcNode sq{__ldg(xn), __ldg(xn + 1), *a.tnow + 0.5 * dt, dt, a.gamma};
+            double sn[NV], st[NV];
+            src_eval(sq, 0.0, sn);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) d[v] = fma(dt, sn[v], d[v]);
+            src_t_N34(sq, st);
+            load4(a.S2 + ((size_t)e * nn + node) * NV, sn);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) Ssrc[v] = fma(1.0 / 3.0, st[v], sn[v]);
+        }
 #pragma unroll
         for (int v = 0; v < NV; ++v) s[v] = fma(2.0, d[v], us[v]);
         euler_fluxes(gm1, s[0], s[1], s[2], s[3], f, g);
@@ -1212,7 +1389,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
             else sc_blend<N, C>(a, FVX, FVY, el, e, i, j, __ldg(a.alpha + e), acc);
         }
         double o[NV];
-        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o);
+        volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o, SRC ? Ssrc : nullptr);
     }
 }
 

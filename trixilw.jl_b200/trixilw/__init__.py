@@ -6,7 +6,8 @@ from .adjoint import adjoint_solve, adjoint_step, adjoint_sweep, forward_record,
 from .batch import LWBatch, solve_lwfr_batch
 from .curved_mesh import CurvedMesh, RefinedStructuredMesh, StructuredMesh, rotate_elements, rotate_state
 from .equations import (CompressibleEulerEquations2D, CompressibleNavierStokesDiffusion2D, ConstantState,
-                        DensityWave, FourQuadrantRiemann, GradientVariablesConservative, IsentropicVortex)
+                        DensityWave, FourQuadrantRiemann, GradientVariablesConservative, IsentropicVortex,
+                        initial_condition_convergence_test, source_terms_convergence_test)
 from .limiters import PositivityPreservingLimiterZhangShu, density, density_pressure, pressure
 from .lwfr import LWIntegrator, LWSolution, l2_linf_errors, solve_lwfr
 from .mesh import RefinedTreeMesh, TreeMesh
@@ -23,7 +24,8 @@ from .semidiscretization import (LW, MDRK, DGSEM, Adaptive, Adiabatic, BoundaryC
 
 __all__ = [
     "DomainError", "TlwError", "lib", "CompressibleEulerEquations2D", "ConstantState", "DensityWave",
-    "FourQuadrantRiemann", "IsentropicVortex", "LWIntegrator", "LWSolution", "l2_linf_errors", "solve_lwfr",
+    "FourQuadrantRiemann", "IsentropicVortex", "initial_condition_convergence_test",
+    "source_terms_convergence_test", "LWIntegrator", "LWSolution", "l2_linf_errors", "solve_lwfr",
     "TreeMesh", "LW", "MDRK", "DGSEM", "Adaptive", "BoundaryConditionDirichlet", "CFLBased", "FluxHLL",
     "FluxLaxFriedrichs", "IndicatorHennemannGassner", "SemidiscretizationHyperbolic", "VolumeIntegralFR",
     "VolumeIntegralFRShockCapturing", "FirstOrderReconstruction", "MUSCLReconstruction", "MUSCLHancockReconstruction", "boundary_condition_periodic",

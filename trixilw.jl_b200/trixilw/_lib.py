@@ -36,7 +36,7 @@ EXPORTED = (
     "tlw_abi_version", "tlw_create", "tlw_destroy", "tlw_set_tree_mesh", "tlw_set_boundary_data", "tlw_rhs",
     "tlw_max_dt", "tlw_set_state", "tlw_get_state", "tlw_step", "tlw_get_time", "tlw_get_cache",
     "tlw_cache_size", "tlw_synchronize", "tlw_get_stream", "tlw_state_pointer", "tlw_last_error",
-    "tlw_step_timed", "tlw_step_host", "tlw_set_unstructured_mesh", "tlw_dd_stages", "tlw_dd_halo_values", "tlw_dd_alpha_buffers", "tlw_dd_comm_stream",
+    "tlw_step_timed", "tlw_step_host", "tlw_set_unstructured_mesh", "tlw_dd_stages", "tlw_dd_halo_values", "tlw_dd_alpha_buffers", "tlw_dd_comm_stream", "tlw_set_source_terms",
     "tlw_probe_fp64_tflops", "tlw_probe_reciprocal", "tlw_rhs_lw_noalloc",
     "tlw_batch_create", "tlw_batch_destroy", "tlw_batch_add_tree_mesh", "tlw_batch_finalize",
     "tlw_batch_set_state", "tlw_batch_get_state", "tlw_batch_step", "tlw_batch_synchronize",
@@ -112,6 +112,7 @@ def lib() -> ctypes.CDLL:
     L.tlw_dd_halo_values.restype = i32
     L.tlw_dd_alpha_buffers.argtypes = [P, P, P]
     L.tlw_dd_comm_stream.argtypes = [P, P]
+    L.tlw_set_source_terms.argtypes = [P, i32, P]
     L.tlw_probe_fp64_tflops.argtypes = [i32, dp]
     L.tlw_probe_reciprocal.argtypes = [i32, P, P, i64]
     L.tlw_rhs_lw_noalloc.argtypes = [i32, dbl, i32, i32, i64, P, i32, P, P, i32, P, P, P, P, dbl, P]

@@ -46,6 +46,36 @@ class CompressibleEulerEquations2D:
         return rho, v1, v2, p
 
 
+def initial_condition_convergence_test(x, y, t, eq: CompressibleEulerEquations2D):
+    """Trixi's initial_condition_convergence_test: rho = rho v1 = rho v2 = c + A sin(w (x + y - t)), rho e = rho^2
+    (c = 2, A = 0.1, L = 2, w = 2 pi / L), a smooth periodic solution on [0, 2]^2 when the source below is added."""
+    c, A, L = 2.0, 0.1, 2.0
+    w = 2.0 * np.pi / L
+    ini = c + A * np.sin(w * (np.asarray(x, dtype=np.float64) + y - t))
+    return np.stack(np.broadcast_arrays(ini, ini, ini, ini * ini), axis=-1)
+
+
+class _SourceTermsConvergenceTest:
+    """Trixi's source_terms_convergence_test(u, x, t, equations) for CompressibleEulerEquations2D: the source that
+    makes initial_condition_convergence_test an exact solution (independent of u). The device evaluates it in the
+    volume kernels (source kind 1); this host form is for checks."""
+
+    kind = 1
+
+    def __call__(self, u, x, y, t, eq: CompressibleEulerEquations2D):
+        c, A, L = 2.0, 0.1, 2.0
+        w = 2.0 * np.pi / L
+        arg = w * (np.asarray(x, dtype=np.float64) + y - t)
+        rho = c + A * np.sin(arg)
+        rho_x = w * A * np.cos(arg)
+        tmp = (2.0 * rho - 1.0) * (eq.gamma - 1.0)
+        s2 = rho_x * (1.0 + tmp)
+        return np.stack(np.broadcast_arrays(rho_x, s2, s2, 2.0 * rho_x * (rho + tmp)), axis=-1)
+
+
+source_terms_convergence_test = _SourceTermsConvergenceTest()
+
+
 class IsentropicVortex:
     """Isentropic vortex (Shu's form): background rho = 1, v = (1, 1), p = 1; strength beta, centre c;
     T = 1 - (gamma-1) beta^2 / (8 gamma pi^2) exp(1 - r^2), rho = T^(1/(gamma-1)), p = rho T,

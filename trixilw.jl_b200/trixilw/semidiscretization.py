@@ -294,13 +294,15 @@ def _i64p(a: np.ndarray):
 
 class SemidiscretizationHyperbolic:
     """SemidiscretizationHyperbolic(mesh, time_discretization, equations, initial_condition, solver;
-    boundary_conditions=boundary_condition_periodic). Builds the libtlw handle and uploads the mesh."""
+    boundary_conditions=boundary_condition_periodic, source_terms=nothing). Builds the libtlw handle and uploads the
+    mesh. source_terms: None or source_terms_convergence_test (TreeMesh, FR volume integral, LW or MDRK)."""
 
     def __init__(self, mesh: TreeMesh, time_discretization, equations: CompressibleEulerEquations2D,
                  initial_condition, solver: DGSEM, boundary_conditions=boundary_condition_periodic, device: int = 0,
                  source_terms=None):
-        if source_terms is not None:
-            raise NotImplementedError("source terms are not built on the device path")
+        if source_terms is not None and getattr(source_terms, "kind", None) != 1:
+            raise NotImplementedError("device source terms: source_terms_convergence_test")
+        self.source_terms = source_terms
         self.curved = self._curved_form(mesh, solver.polydeg)
         self.mesh = mesh
         self.equations = equations
@@ -343,6 +345,15 @@ class SemidiscretizationHyperbolic:
         if mesh.n_boundaries:
             self._bnd_xy = mesh.boundary_node_coordinates(self.polydeg)
             self._upload_boundary_kinds()
+        self._upload_source_terms()
+
+    def _upload_source_terms(self):
+        """The source kind and the node coordinates in Trixi's [2, i, j, e] order."""
+        if self.source_terms is None:
+            return
+        xy = self.node_coordinates
+        self._xnode = np.ascontiguousarray(np.transpose(xy, (3, 2, 1, 0)), dtype=np.float64)
+        check(self.handle, lib().tlw_set_source_terms(self.handle, int(self.source_terms.kind), _ptr(self._xnode)))
 
     @property
     def handle(self):
@@ -384,6 +395,7 @@ class SemidiscretizationHyperbolic:
         if mesh.n_boundaries:
             self._bnd_xy = mesh.boundary_node_coordinates(self.polydeg)
             self._upload_boundary_kinds()
+        self._upload_source_terms()
 
     def _upload_mesh(self):
         if self.curved is not None and getattr(self.curved, "unstructured", False):
