@@ -636,6 +636,7 @@ __device__ __forceinline__ void src_tttt_N4(const SrcNode& q, double* o) {
 #ifndef TLW_VOL_ILP
 #define TLW_VOL_ILP 1
 #endif
+
 struct Recip4 {
     double pp, p, m, mm;
 };
