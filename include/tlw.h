@@ -362,7 +362,9 @@ int tlw_probe_reciprocal(int32_t device, const double* x, double* y, int64_t n);
 /* Synchronous: current time, last dt and number of accepted steps. */
 int tlw_get_time(tlw_handle* h, double* t, double* dt_last, int64_t* steps);
 
-/* Element/interface caches of the last rhs (layouts in tlw_cache_item). Synchronous. */
+/* Element/interface caches of the last rhs (layouts in tlw_cache_item). Synchronous. U2 and F2 are those of the
+ * last tlw_rhs MDRK stage 1: the device step loop passes only u_t between its stages (a TreeMesh without shock
+ * capturing or source terms) and rebuilds U2 and F2 in stage 2. */
 int tlw_get_cache(tlw_handle* h, int32_t item, double* out, int32_t where);
 int64_t tlw_cache_size(tlw_handle* h, int32_t item);
 

@@ -195,13 +195,15 @@ void enqueue_indicator(tlw_handle* h, const double* u, bool speed) {
 // the step's final values all come from the volume and interface kernels: the plain LW step on a periodic
 // conforming TreeMesh (no boundaries, mortars, shock capturing, curvilinear or parabolic terms)
 bool use_slots(const tlw_handle* h) {
-    return h->d_slots && h->opts.time_discretization == TLW_LW && !h->sc && !h->curved && !h->parabolic &&
-           h->nb == 0 && h->nmx + h->nmy == 0 && h->nh == 0;
+    return h->d_slots && !h->sc && !h->curved && !h->parabolic && h->nb == 0 && h->nmx + h->nmy == 0 && h->nh == 0;
 }
 
 // one element-centric pass for all faces instead of the x and y interface sweeps
 #ifndef TLW_SURFACE_PASS
 #define TLW_SURFACE_PASS 1
+#endif
+#ifndef TLW_MDRK_COMPACT
+#define TLW_MDRK_COMPACT 1
 #endif
 // (not with shock capturing: the blended variant needs 142 registers and measured slower than the sweeps on the
 // 512^2 Riemann problem, 0.376 against about 0.34 ms)
@@ -469,7 +471,11 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
     va.tFn = h->d_tFn;
     va.status = &h->d_step->status;
     va.speed_kind = h->opts.max_speed;
-    if (mode == MODE_STEP && stage == TLW_STAGE_LW && use_slots(h) && !h->te_request) va.cfl_slots = h->d_slots;
+    // the stage that produces the step's final values (LW, or MDRK stage 2) fills the next step's CFL slots
+    if (mode == MODE_STEP && stage != TLW_STAGE_MDRK1 && use_slots(h) && !h->te_request) va.cfl_slots = h->d_slots;
+    // an MDRK step on a plain TreeMesh passes only u_t between its stages (stage 2 rebuilds U2 and F2)
+    va.compact = TLW_MDRK_COMPACT && mode == MODE_STEP && stage != TLW_STAGE_LW && !h->sc && !h->curved &&
+                 !h->source && !h->parabolic;
     if (h->source) {
         va.source = h->source;
         va.xnode = h->d_xnode;
@@ -618,7 +624,7 @@ void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const
         enqueue_rhs(h, TLW_STAGE_MDRK2, MODE_STEP, h->d_us, u, u, unew, dtp, ev ? ev + 1 : nullptr, true);
         // once per MDRK step (the loop); perform_step!'s mid-step call (src/solvers/mdrk.jl:19) acts on u^n,
         // which the previous step's application has limited already
-        enqueue_limiter(h, unew, 1, nullptr);
+        enqueue_limiter(h, unew, 1, use_slots(h) ? h->d_slots : nullptr);
     }
 }
 

@@ -45,6 +45,8 @@ struct LaunchImpl {
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false, false, 0, false, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(5));
         // source terms (TreeMesh, FR)
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, false, false, false, 0, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
@@ -77,9 +79,12 @@ struct LaunchImpl {
             else lw_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, lw, s>>>(a);
         } else if (stage == TLW_STAGE_MDRK1) {
             if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS, SC><<<grid, C::THREADS, md, s>>>(a);
+            else if (!SC && a.compact) mdrk1_volume_kernel<N, MODE_STEP, false, false, 0, false, true><<<grid, C::THREADS, md, s>>>(a);
             else mdrk1_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, md, s>>>(a);
         } else {
             if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS, SC><<<grid, C::THREADS, md, s>>>(a);
+            else if (!SC && a.compact)
+                mdrk2_volume_kernel<N, MODE_STEP, false, false, 0, false, true><<<grid, C::THREADS, C::smem_bytes(5), s>>>(a);
             else mdrk2_volume_kernel<N, MODE_STEP, SC><<<grid, C::THREADS, md, s>>>(a);
         }
     }

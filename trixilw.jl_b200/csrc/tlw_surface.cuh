@@ -295,7 +295,9 @@ static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
 // kernel (no boundaries, no blending) capped to TLW_SURF_MINB resident CTAs' registers (5 x 160 threads: 72
 // registers, no spills); TLW_SURF_PREFETCH 1 loads the output face node before the flux phase (more registers).
 // Measured on the 512 x 512, N = 4 vortex: 0.205 ms with (160, 5, 0), 0.232 ms with (160, 1, 1) at 90
-// registers, 0.236 ms with (320, 3, 0); the x / y sweeps take 0.236 ms.
+// registers, 0.236 ms with (320, 3, 0), 0.236 ms with (240, 3, 0), 0.216 ms with (120, 6, 0), 0.224 ms with
+// (160, 6, 0); an asynchronous copy of the output face nodes into shared memory during the flux phase: 0.222 ms.
+// The x / y sweeps take 0.236 ms.
 #ifndef TLW_SURF_THREADS
 #define TLW_SURF_THREADS 160
 #endif

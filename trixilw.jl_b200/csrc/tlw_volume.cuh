@@ -74,6 +74,7 @@ struct VolArgs {
     const double* xnode;
     const double* tnow;
     double* S2;
+    int compact;            // MDRK step on a plain TreeMesh: u_t between the stages instead of U2, F2
     double* U2;             // MDRK: stage-1 U2 [v,i,j,e] (written by stage 1, read by stage 2)
     double* F2;             // MDRK: stage-1 F2 [v,d,i,j,e]
     const double* inv_jac;  // [e]
@@ -631,6 +632,35 @@ __device__ __forceinline__ void src_tttt_N4(const SrcNode& q, double* o) {
     src_stencil(q, 1.0, 1.0, -4.0, 6.0, -4.0, 1.0, o);
 }
 
+// The per-element CFL slots of a step's final values (plain TreeMesh step): after the epilogue, every thread has
+// the speeds of its node in l1, l2 (interior nodes; zero otherwise); through the (now free) X plane, one thread per
+// (element, component) writes slot 0 (interior maxima) and clears the face slots, which the surfaces fill.
+// Every thread of the CTA calls it (barriers inside).
+template <int N, class C>
+__device__ __forceinline__ void write_interior_slots(const VolArgs& a, double* X, bool active, int el, int i, int j,
+                                                     int tid, double l1, double l2) {
+    constexpr int n = C::n, EB = C::EB;
+    __syncthreads();
+    if (active) {
+        X[el * C::P + i + C::R * j] = l1;
+        X[(EB + el) * C::P + i + C::R * j] = l2;
+    }
+    __syncthreads();
+    const int ee = blockIdx.x * EB + (tid >> 1);
+    if (tid < 2 * EB && ee < a.E) {
+        const double* p = X + ((tid & 1) * EB + (tid >> 1)) * C::P;
+        double m = 0.0;
+#pragma unroll
+        for (int jj = 1; jj < n - 1; ++jj)
+#pragma unroll
+            for (int ii = 1; ii < n - 1; ++ii) m = fmax(m, p[ii + C::R * jj]);
+        unsigned long long* sl = a.cfl_slots + (size_t)ee * CFL_SLOTS;
+        sl[tid & 1] = (unsigned long long)__double_as_longlong(m);
+#pragma unroll
+        for (int k = 1; k < CFL_SLOTS / 2; ++k) sl[2 * k + (tid & 1)] = 0ull;
+    }
+}
+
 // The stage's four flux pairs at upp, up, um, umm. With TLW_VOL_ILP the four reciprocals 1/rho are refined
 // first, as four independent Newton chains, instead of one chain per flux pair; same operations, same bits.
 #ifndef TLW_VOL_ILP
@@ -1029,28 +1059,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o, SRC ? Ssrc : nullptr);
         if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) node_speeds(a.gamma, o, a.status, l1, l2);
     }
-    if (SLOTS && a.cfl_slots) {
-        // the interior nodes' speeds through the (now free) X plane, one thread per (element, component)
-        __syncthreads();
-        if (active) {
-            X[el * C::P + i + C::R * j] = l1;
-            X[(EB + el) * C::P + i + C::R * j] = l2;
-        }
-        __syncthreads();
-        const int ee = blockIdx.x * EB + (tid >> 1);
-        if (tid < 2 * EB && ee < a.E) {
-            const double* p = X + ((tid & 1) * EB + (tid >> 1)) * C::P;
-            double m = 0.0;
-#pragma unroll
-            for (int jj = 1; jj < n - 1; ++jj)
-#pragma unroll
-                for (int ii = 1; ii < n - 1; ++ii) m = fmax(m, p[ii + C::R * jj]);
-            unsigned long long* sl = a.cfl_slots + (size_t)ee * CFL_SLOTS;
-            sl[tid & 1] = (unsigned long long)__double_as_longlong(m);
-#pragma unroll
-            for (int k = 1; k < CFL_SLOTS / 2; ++k) sl[2 * k + (tid & 1)] = 0ull;
-        }
-    }
+    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, l1, l2);
     if (TE) {
         // lw_volume_kernel_4!'s error estimate (dg_2d.jl:1183-1265; curvilinear, with F~, G~ and the node's
         // J^{-1}: dgsem_structured/dg_2d.jl:1595-1682 at depth 3, :1983-2075 at depth 4): the strong-form volume
@@ -1096,6 +1105,34 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
     }
 }
 
+// MDRK stage 1's stored sums from u^n and d = u_t: F2 = f + f_t/6, G2 = g + g_t/6, U2 = u + u_t/6 with f_t the
+// 4-point stencil at u +- d, u +- 2d (multi_derivative_2d.jl:337-371), the operations of mdrk1_volume_kernel
+__device__ __forceinline__ void mdrk_stage1_sums(double gm1, const double* uu, const double* d, double* F2v,
+                                                 double* G2v, double* U2v) {
+    double f0[NV], g0[NV], f[NV], g[NV], ft[NV], gt[NV], s[NV];
+    euler_fluxes(gm1, uu[0], uu[1], uu[2], uu[3], f0, g0);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] = fma(2.0, d[v], uu[v]);
+    euler_fluxes(gm1, s[0], s[1], s[2], s[3], f, g);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { ft[v] = -f[v]; gt[v] = -g[v]; s[v] = uu[v] + d[v]; }
+    euler_fluxes(gm1, s[0], s[1], s[2], s[3], f, g);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { ft[v] = fma(8.0, f[v], ft[v]); gt[v] = fma(8.0, g[v], gt[v]); s[v] = uu[v] - d[v]; }
+    euler_fluxes(gm1, s[0], s[1], s[2], s[3], f, g);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { ft[v] = fma(-8.0, f[v], ft[v]); gt[v] = fma(-8.0, g[v], gt[v]); s[v] = fma(-2.0, d[v], uu[v]); }
+    euler_fluxes(gm1, s[0], s[1], s[2], s[3], f, g);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        ft[v] = (ft[v] + f[v]) * (1.0 / 12.0);
+        gt[v] = (gt[v] + g[v]) * (1.0 / 12.0);
+        F2v[v] = fma(1.0 / 6.0, ft[v], f0[v]);
+        G2v[v] = fma(1.0 / 6.0, gt[v], g0[v]);
+        U2v[v] = fma(1.0 / 6.0, d[v], uu[v]);
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
 // MDRK stage 1 (mdrk_kernel_1!, multi_derivative_2d.jl:263-421): F = f/2 + f_t/8, U = u/2 + u_t/8,
 // F2 = f + f_t/6, U2 = u + u_t/6 (stored whole for stage 2).
@@ -1104,12 +1141,15 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
 // contravariant fluxes, d carries the node's J^{-1}; F2, G2 stay physical, the traces are contravariant.
 // SRC (TreeMesh, FR): ut += dt s(u, t); S = s/2 + s_t/8 enters du, S2 = s + s_t/6 is stored for stage 2
 // (multi_derivative_2d.jl:321-400).
-template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false>
+// COMPACT (the plain TreeMesh step): store only u_t (into a.U2) instead of U2 and F2; stage 2 recomputes them from
+// u^n and u_t with this kernel's operations (64 instead of 192 bytes a node between the stages).
+template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
 static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
                                                                          : VolCfg<N>::MDRK_MIN_BLOCKS)
     mdrk1_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     static_assert(!SRC || (!SC && !CURVED), "source terms: the plain TreeMesh kernel");
+    static_assert(!COMPACT || (!SC && !CURVED && !SRC && MODE == MODE_STEP), "compact stages: the plain TreeMesh step");
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
@@ -1211,9 +1251,13 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
             U2v[v] = fma(1.0 / 6.0, d[v], uu[v]);
         }
         const size_t off = ((size_t)e * nn + node);
-        store4(a.U2 + off * NV, U2v);
-        store4(a.F2 + off * 2 * NV, F2v);
-        store4(a.F2 + off * 2 * NV + NV, G2v);
+        if (COMPACT) {
+            store4(a.U2 + off * NV, d);
+        } else {
+            store4(a.U2 + off * NV, U2v);
+            store4(a.F2 + off * 2 * NV, F2v);
+            store4(a.F2 + off * 2 * NV + NV, G2v);
+        }
         if (SRC) {
             double st[NV], S2v[NV];
             src_t_N34(sq, st);
@@ -1257,12 +1301,15 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
 // ------------------------------------------------------------------------------------------------
 // CURVED (mdrk_kernel_2!, src/solvers/dgsem_structured/multi_derivative_2d.jl:245-445): as in stage 1.
 // SRC (TreeMesh, FR): at t + dt/2, u*_t += dt s(u*); S = S2 + s_t(u*)/3 (multi_derivative_2d.jl:484-550).
-template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false>
+// COMPACT: F2, G2, U2 recomputed from u^n (a.u_base) and stage 1's u_t (a.U2) at the start, parked in shared memory
+// (three more planes) until the stage's own sums are formed.
+template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
 static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
                                                                          : VolCfg<N>::MDRK_MIN_BLOCKS)
     mdrk2_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     static_assert(!SRC || (!SC && !CURVED), "source terms: the plain TreeMesh kernel");
+    static_assert(!COMPACT || (!SC && !CURVED && !SRC && MODE == MODE_STEP), "compact stages: the plain TreeMesh step");
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
     extern __shared__ double smem_d[];
@@ -1308,6 +1355,16 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
             node_put<N, C>(X, Y, el, i, j, ft, gt);
         } else {
             node_put<N, C>(X, Y, el, i, j, f, g);
+        }
+        if (COMPACT) {
+            // stage 1's F2, G2 (into the F0X, F0Y planes) and U2 (the UU plane) from u^n and u_t
+            double un[NV], dn[NV], F2v[NV], G2v[NV], U2v[NV];
+            const size_t off = ((size_t)e * nn + node);
+            load4(a.u_base + off * NV, un);
+            load4(a.U2 + off * NV, dn);
+            mdrk_stage1_sums(gm1, un, dn, F2v, G2v, U2v);
+            node_put<N, C>(F0X, F0Y, el, i, j, F2v, G2v);
+            node_put<N, C>(UU, UU, el, i, j, U2v, U2v);
         }
         if (SC) {
             // the subcell FV part uses the instantaneous u^n, not u* (multi_derivative_2d.jl:257)
@@ -1356,9 +1413,14 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
         euler_fluxes(gm1, s[0], s[1], s[2], s[3], f, g);
         const size_t off = ((size_t)e * nn + node);
         double U2v[NV], F2v[NV], G2v[NV];
-        load4(a.U2 + off * NV, U2v);
-        load4(a.F2 + off * 2 * NV, F2v);
-        load4(a.F2 + off * 2 * NV + NV, G2v);
+        if (COMPACT) {
+            node_get<N, C>(F0X, F0Y, el, i, j, F2v, G2v);
+            node_get<N, C>(UU, UU, el, i, j, U2v, U2v);
+        } else {
+            load4(a.U2 + off * NV, U2v);
+            load4(a.F2 + off * 2 * NV, F2v);
+            load4(a.F2 + off * 2 * NV + NV, G2v);
+        }
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             ft[v] = (ft[v] + f[v]) * (1.0 / 12.0);
@@ -1382,6 +1444,9 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
     __syncthreads();
     line_contract<N, C, true>(X, Y, tid);
     __syncthreads();
+    // the step's final values: per-element CFL slots as the LW kernel writes them (plain TreeMesh MDRK step)
+    constexpr bool SLOTS = MODE == MODE_STEP && !SC && !CURVED;
+    double l1 = 0.0, l2 = 0.0;
     if (active) {
         double acc[NV];
         node_sum<N, C>(X, Y, el, i, j, acc);
@@ -1391,7 +1456,9 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
         }
         double o[NV];
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o, SRC ? Ssrc : nullptr);
+        if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) node_speeds(a.gamma, o, a.status, l1, l2);
     }
+    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, l1, l2);
 }
 
 }  // namespace tlw
