@@ -166,6 +166,99 @@ def _lockstep(tl, parts, semis, steps, cfl):
     return dds
 
 
+def _streamed(tl, parts, semis, steps, cfl):
+    """The ranks' split steps in one process with the collectives enqueued on each part's comm stream and no
+    device synchronisation between the phases: a part's copies wait (by events) for the neighbours' comm streams,
+    which the library has handed the packed buffers to, and each tlw_dd_* call waits for its own comm stream.
+    This runs the hand-over between the kernels' stream and the comm stream as NCCL ranks would use it."""
+    import torch
+    from trixilw import _lib
+    from trixilw.domain import DomainDecomposedLW
+
+    L = _lib.lib()
+    dds = [DomainDecomposedLW(s, p, None, None) for s, p in zip(semis, parts)]
+
+    def comm_events():
+        evs = []
+        for d in dds:
+            ev = torch.cuda.Event()
+            ev.record(d.stream)
+            evs.append(ev)
+        return evs
+
+    def join():
+        # as a collective's completion: no part's comm stream goes on before every part's has arrived here
+        evs = comm_events()
+        for d in dds:
+            for ev in evs:
+                d.stream.wait_event(ev)
+
+    def exchange(get_send, get_recv):
+        evs = comm_events()
+        for d in dds:
+            with torch.cuda.stream(d.stream):
+                for q, (off, cnt) in d.part.segments.items():
+                    d.stream.wait_event(evs[q])
+                    oq, cq = dds[q].part.segments[d.part.rank]
+                    get_recv(d)[off:off + cnt].copy_(get_send(dds[q])[oq:oq + cq])
+        join()
+
+    for _ in range(steps):
+        for d in dds:
+            _lib.check(d.semi.handle, L.tlw_dd_begin(d.semi.handle, cfl, 0.0, float("inf")))
+        evs = comm_events()
+        maxes = []
+        for d in dds:   # the MAX all-reduce: every comm stream sees every part's CFL maximum
+            with torch.cuda.stream(d.stream):
+                for ev in evs:
+                    d.stream.wait_event(ev)
+                maxes.append(torch.max(torch.cat([x.max_bits for x in dds])))
+        join()
+        for d, m in zip(dds, maxes):
+            with torch.cuda.stream(d.stream):
+                d.max_bits.fill_(m)
+        if dds[0].alpha_send is not None:
+            exchange(lambda d: d.alpha_send, lambda d: d.alpha_recv)
+        for _stage in range(int(L.tlw_dd_stages(dds[0].semi.handle))):
+            for d in dds:
+                _lib.check(d.semi.handle, L.tlw_dd_volume(d.semi.handle))
+            exchange(lambda d: d.send, lambda d: d.recv)
+            for d in dds:
+                _lib.check(d.semi.handle, L.tlw_dd_finish(d.semi.handle))
+    torch.cuda.synchronize()
+    return dds
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nparts,td,sc", [(3, "lw", False), (2, "mdrk", False), (3, "lw", True)])
+def test_gpu_split_step_on_comm_streams_equals_single_domain(tl, nparts, td, sc):
+    from trixilw.domain import partition
+    N, steps, cfl = 4, 6, 0.4
+    mesh = tl.TreeMesh((-5.0, -5.0), (5.0, 5.0), 4)
+    whole = _semi(tl, mesh, N, None, td, sc)
+    u0 = whole.compute_coefficients(0.0)
+    integ = tl.LWIntegrator(tl.semidiscretize(whole, whole.time_discretization, (0.0, 1e9)))
+    integ.set_state(u0, 0.0)
+    integ.step(steps, cfl, use_graph=False)
+    integ.sync_time()
+    ref = integ.get_state()
+    parts = partition(mesh, nparts)
+    semis = [_semi(tl, p.mesh, N, None, td, sc) for p in parts]
+    nn4 = 4 * (N + 1) ** 2
+    integs = []
+    for s, p in zip(semis, parts):
+        it = tl.LWIntegrator(tl.semidiscretize(s, s.time_discretization, (0.0, 1e9)))
+        it.set_state(np.ascontiguousarray(u0.reshape(-1, nn4)[p.mesh.elements].reshape(-1)), 0.0)
+        integs.append(it)
+    _streamed(tl, parts, semis, steps, cfl)
+    got = np.empty_like(ref).reshape(-1, nn4)
+    for it, p in zip(integs, parts):
+        it.sync_time()
+        assert it.iter == steps and it.t == integ.t
+        got[p.mesh.elements] = it.get_state().reshape(-1, nn4)
+    np.testing.assert_array_equal(got.reshape(-1), ref)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("nparts,N,walls,td,sc", [(2, 4, False, "lw", False), (3, 3, False, "lw", False),
                                                   (4, 4, True, "lw", False), (2, 4, False, "mdrk", False),
