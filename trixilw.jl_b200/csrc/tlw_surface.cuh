@@ -311,7 +311,8 @@ static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
 template <int N> struct SurfCfg {
     static constexpr int n = N + 1;
     static constexpr int EB = (TLW_SURF_THREADS + 4 * n - 1) / (4 * n);
-    static constexpr int THREADS = EB * 4 * n;
+    // whole warps (the face-node maxima are reduced by warp shuffles over full masks)
+    static constexpr int THREADS = (EB * 4 * n + 31) / 32 * 32;
     static constexpr int MIN_BLOCKS = TLW_SURF_MINB;
 };
 
@@ -344,7 +345,7 @@ static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? 1 : 
     if (TLW_SURF_PREFETCH && has2) load4_rw(o2, x);
     {
         const int el = tid / (4 * n), r = tid - el * 4 * n, f = r / n, l = r - f * n, e = e0 + el;
-        if (e < a.E) {
+        if (el < EB && e < a.E) {
             const double dt = a.inst ? a.dt[__ldg(a.inst + e)] : *a.dt;   // (batched form: the instance's dt)
             const int nb = __ldg(a.nbr + 4 * e + f);
             const bool plus = f & 1;   // this element is the interface's left (lower) element
