@@ -55,7 +55,7 @@ void any_rhs(oracle_handle* h, const double* u, const double* u2, double* du, do
         rhs_curved_sc(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, bd, kind, u2);
         return;
     }
-    rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, kind, u2, bd);
+    rhs_curved(h->basis, h->eq, h->opt, h->cmesh, u, du, dt, h->ws, nthreads, kind, u2, bd, t);
 }
 
 // one application of the positivity limiter on whichever mesh the handle holds
@@ -213,8 +213,8 @@ int oracle_set_curved_mortars(oracle_handle* h, int M, const int32_t* small1, co
 // source terms on the TreeMesh (LW and MDRK): kind 0 none, 1 source_terms_convergence_test; node coordinates
 // [2, i, j, e]
 int oracle_set_source(oracle_handle* h, int kind, const double* node_coordinates) {
-    if (h->curved || h->parabolic || kind < 0 || kind > 1 || (kind && !node_coordinates)) return 1;
-    if (kind) h->xnode.assign(node_coordinates, node_coordinates + (size_t)2 * h->basis.n * h->basis.n * h->mesh.n_elements);
+    if (h->parabolic || kind < 0 || kind > 1 || (kind && !node_coordinates)) return 1;
+    if (kind) h->xnode.assign(node_coordinates, node_coordinates + (size_t)2 * h->basis.n * h->basis.n * h->n_elements());
     else h->xnode.clear();
     h->opt.source = kind;
     h->opt.xnode = kind ? h->xnode.data() : nullptr;

@@ -152,9 +152,13 @@ inline void unstructured_interface_node(const Euler& eq, const Options& opt, con
 // depth 4): u_np1 = u - dt J^{-1}(node) (D F~ + D G~) and u_np1_low with F~, G~ before the last stage's term,
 // ws.temporal_errors[e] = sum over nodes and variables of ((u_np1 - u_np1_low) / (abstol + reltol max))^2.
 // It does not depend on alpha: the shock-capturing path calls the same kernel for every element.
+// Source terms (opt->source, the FR volume integral; dgsem_structured/dg_2d.jl:578-964, 1379-2058): each derivative
+// gets dt times its stencil of the states before it (at depth 4 the second derivative's is the 5-point
+// calc_source_tt_N4, where the TreeMesh kernel takes N23), S = s + s_t/2 + s_tt/6 + s_ttt/24 (+ s_tttt/120) enters
+// du unscaled by the node's J^{-1}. The built source does not depend on u, so the stencils are taken by time offsets.
 inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, const CurvedMesh& m, int e,
                                      const double* u, double* du, double dt, Workspace& ws, double alpha = 1.0,
-                                     const Options* te = nullptr) {
+                                     const Options* te = nullptr, double t = 0.0) {
     const int n = b.n, nn = n * n;
     const LWStencils S = lw_stencils(N);
     const int depth = S.depth;
@@ -200,6 +204,25 @@ inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, con
             for (int v = 0; v < NV; ++v) { Ft[o + v] = ft[o + v]; Gt[o + v] = gt[o + v]; Uc[o + v] = ue[o + v]; }
         }
     contract(ft, gt, Dm(1));
+    const int src_kind = te ? te->source : 0;
+    std::vector<double> Ssrc(src_kind ? NV * nn : 0, 0.0);
+    // dt * stencil into derivative k, c * stencil into S, at every node
+    auto add_source = [&](double* Dk, double c, const double (&w)[5], double scale) {
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const double* xn = te->xnode + 2 * ((size_t)e * nn + i + (size_t)n * j);
+                double st[NV];
+                source_stencil_t(src_kind, eq.gamma, xn[0], xn[1], t, dt, scale, w, st);
+                for (int v = 0; v < NV; ++v) {
+                    Ssrc[L(i, j) + v] += c * st[v];
+                    if (Dk) Dk[L(i, j) + v] += dt * st[v];
+                }
+            }
+    };
+    static constexpr double W_S[5] = {0, 0, 1, 0, 0}, W_T12[5] = {0, -1, 0, 1, 0}, W_T34[5] = {1, -8, 0, 8, -1},
+                            W_TT23[5] = {0, 1, -2, 1, 0}, W_TT4[5] = {-1, 16, -30, 16, -1},
+                            W_TTT34[5] = {-1, 2, 0, -2, 1}, W_TTTT4[5] = {1, -4, 6, -4, 1};
+    if (src_kind) add_source(Dm(1), 1.0, W_S, 1.0);   // S = s, ut += dt s (:1750-1757)
     // stages 1 .. depth: stencils of physical and contravariant fluxes, time averages, next derivative
     for (int s = 1; s <= depth; ++s) {
         for (int j = 0; j < n; ++j)
@@ -235,7 +258,24 @@ inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, con
                     ft[o + v] = tf[v]; gt[o + v] = tg[v];
                 }
             }
-        if (s < depth) contract(ft, gt, Dm(s + 1));
+        if (s < depth) {
+            contract(ft, gt, Dm(s + 1));
+            if (src_kind) {
+                if (s + 1 == 2) {   // s_t: N34 at depths 3 and 4, N12 below (:1815, :1267)
+                    if (depth >= 3) add_source(Dm(2), 0.5, W_T34, 1.0 / 12.0);
+                    else add_source(Dm(2), 0.5, W_T12, 0.5);
+                } else if (s + 1 == 3) {   // s_tt: N4 at depth 4 (:1886), N23 at depth 3 (:1567)
+                    if (depth == 4) add_source(Dm(3), 1.0 / 6.0, W_TT4, 1.0 / 12.0);
+                    else add_source(Dm(3), 1.0 / 6.0, W_TT23, 1.0);
+                } else {   // s_ttt (:1949)
+                    add_source(Dm(4), 1.0 / 24.0, W_TTT34, 0.5);
+                }
+            }
+        }
+    }
+    if (src_kind) {   // the last stencil: s_ttt / 24 at depth 3 (:1649), s_tttt / 120 at depth 4 (:2042)
+        if (depth == 3) add_source(nullptr, 1.0 / 24.0, W_TTT34, 0.5);
+        else add_source(nullptr, 1.0 / 120.0, W_TTTT4, 1.0);
     }
     // du += Dhat F~ + Dhat G~; element cache
     double* due = du + idx_u(n, 0, 0, 0, e);
@@ -251,6 +291,8 @@ inline void lw_volume_element_curved(const Basis& b, const Euler& eq, int N, con
                 ws.F[idx_F(n, v, 1, i, j, e)] = Gp[o + v];
                 ws.U[idx_u(n, v, i, j, e)] = Uc[o + v];
             }
+            if (src_kind)
+                for (int v = 0; v < NV; ++v) due[o + v] += (-1.0 / ije[i + n * j]) * Ssrc[o + v];
         }
     if (want_te) {
         std::vector<double> hi(NV * nn), lo(NV * nn);
@@ -440,7 +482,7 @@ inline void check_unstructured(const CurvedMesh& m, int kind) {
 // u (u^n) at the interfaces (src/solvers/dgsem_structured/multi_derivative_2d.jl:1-80)
 inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, const CurvedMesh& m, const double* u,
                        double* du, double dt, Workspace& ws, int nthreads = 1, int kind = 0,
-                       const double* u2 = nullptr, const BoundaryData* bd = nullptr) {
+                       const double* u2 = nullptr, const BoundaryData* bd = nullptr, double t = 0.0) {
     const int n = b.n, nn = n * n;
     const size_t ndof = (size_t)NV * nn * m.n_elements;
     const double nan = std::numeric_limits<double>::quiet_NaN();
@@ -452,6 +494,7 @@ inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, cons
     if (kind == 1) {
         ws.U2.assign(ndof, nan);
         ws.F2.assign(2 * ndof, nan);
+        if (opt.source) ws.S2.assign(ndof, nan);
     }
     if (kind == 2 && (ws.U2.size() != ndof || !u2)) throw std::invalid_argument("rhs_mdrk2 before rhs_mdrk1");
     check_unstructured(m, kind);
@@ -460,9 +503,11 @@ inline void rhs_curved(const Basis& b, const Euler& eq, const Options& opt, cons
     for (int e = 0; e < m.n_elements; ++e) {
         const double* Jae = &m.Ja[4 * (size_t)nn * e];
         const double* ije = &m.inv_jac[(size_t)nn * e];
-        if (kind == 0) lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws, 1.0, &opt);
-        else if (kind == 1) mdrk1_volume_element(b, eq, e, u, du, dt, 0.0, 1.0, ws, Jae, ije);
-        else mdrk2_volume_element(b, eq, e, u2, du, dt, 0.0, 1.0, ws, Jae, ije);
+        SourceArgs sa{opt.source, opt.xnode, eq.gamma, t};
+        sa.stage2_at_t = true;
+        if (kind == 0) lw_volume_element_curved(b, eq, opt.N, m, e, u, du, dt, ws, 1.0, &opt, t);
+        else if (kind == 1) mdrk1_volume_element(b, eq, e, u, du, dt, 0.0, 1.0, ws, Jae, ije, &sa);
+        else mdrk2_volume_element(b, eq, e, u2, du, dt, 0.0, 1.0, ws, Jae, ije, &sa);
     }
     bool bad = false;
 #pragma omp parallel for num_threads(nthreads) schedule(static) reduction(|| : bad)

@@ -384,6 +384,18 @@ inline void source_eval(int kind, double gamma, const double* /*u*/, double x1, 
     if (kind == 1) source_convergence_test(gamma, x1, x2, t, s);
     else s[0] = s[1] = s[2] = s[3] = 0.0;
 }
+// c * sum_k w[k] s(x, t + (k - 2) dt), k = 0..4: a stencil of a source that does not depend on u (the only kind
+// built), for which the states of the reference's calls do not matter
+inline void source_stencil_t(int kind, double gamma, double x1, double x2, double t, double dt, double c,
+                             const double (&w)[5], double* o) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0}, sv[4];
+    for (int k = 0; k < 5; ++k) {
+        if (w[k] == 0.0) continue;
+        source_eval(kind, gamma, nullptr, x1, x2, t + (k - 2) * dt, sv);
+        for (int v = 0; v < 4; ++v) acc[v] += w[k] * sv[v];
+    }
+    for (int v = 0; v < 4; ++v) o[v] = c * acc[v];
+}
 
 struct Workspace {
     // element cache
@@ -778,6 +790,7 @@ struct SourceArgs {
     int kind = 0;
     const double* xnode = nullptr;
     double gamma = 1.4, t = 0.0;
+    bool stage2_at_t = false;   // curvilinear meshes: stage 2's source at t, not t + dt/2
     // s(u_, x, t0 + dtau) at node (i, j) of element e
     void at(int e, int n, int i, int j, const double* us, double t0, double dtau, double* o) const {
         const double* xn = xnode + 2 * ((size_t)e * n * n + i + (size_t)n * j);
@@ -856,10 +869,11 @@ inline void mdrk1_volume_element(const Basis& b, const Euler& eq, int e, const d
             if (with_src) {
                 double st[NV];
                 src->t_N34(e, n, i, j, up, upp, um, umm, src->t, dt, st);
+                const double ijn = Jae ? ije[i + n * j] : inv_jac;
                 for (int v = 0; v < NV; ++v) {
                     Sh[o + v] += 0.125 * st[v];
                     S2[o + v] += 1.0 / 6.0 * st[v];
-                    due[o + v] += (-1.0 / inv_jac) * Sh[o + v];
+                    due[o + v] += (-1.0 / ijn) * Sh[o + v];
                     ws.S2[idx_u(n, v, i, j, e)] = S2[o + v];
                 }
             }
@@ -908,7 +922,7 @@ inline void mdrk2_volume_element(const Basis& b, const Euler& eq, int e, const d
     Tile Fc, Gc, Uc, ust;
     ust.zero(NV * nn);
     const bool with_src = src && src->kind;
-    const double th = with_src ? src->t + 0.5 * dt : 0.0;
+    const double th = with_src ? (src->stage2_at_t ? src->t : src->t + 0.5 * dt) : 0.0;
     auto L = [&](int i, int j) { return NV * (i + n * j); };
     const double* ue = us + idx_u(n, 0, 0, 0, e);
     for (int j = 0; j < n; ++j)
@@ -955,8 +969,9 @@ inline void mdrk2_volume_element(const Basis& b, const Euler& eq, int e, const d
             if (with_src) {
                 double st[NV];
                 src->t_N34(e, n, i, j, up, upp, um, umm, th, dt, st);
+                const double ijn = Jae ? ije[i + n * j] : inv_jac;
                 for (int v = 0; v < NV; ++v)
-                    due[o + v] += (-1.0 / inv_jac) * (ws.S2[idx_u(n, v, i, j, e)] + 1.0 / 3.0 * st[v]);
+                    due[o + v] += (-1.0 / ijn) * (ws.S2[idx_u(n, v, i, j, e)] + 1.0 / 3.0 * st[v]);
             }
             double fm[NV], gm[NV], fp[NV], gp[NV], fmm[NV], gmm[NV], fpp[NV], gpp[NV];
             eq.fluxes(um, fm, gm);

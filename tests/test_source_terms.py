@@ -162,3 +162,105 @@ def test_gpu_elixir_euler_source_terms_converges(tl):
         errs.append(np.sqrt(np.mean((integ.get_state() - semi.compute_coefficients(integ.t)) ** 2)))
     orders = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
     assert np.all(orders > 3.5), (errs, orders)
+
+
+# ------------------------------------------------------------------------- curvilinear (StructuredMesh)
+def warp2(xi, eta):
+    """[-1, 1]^2 -> [0, 2]^2 with the interior warped by 5 % of the side (periodic-compatible)."""
+    X, Y = 1.0 + xi, 1.0 + eta
+    s = np.sin(np.pi * X) * np.sin(np.pi * Y)
+    return X + 0.05 * s, Y + 0.05 * s
+
+
+def curved_state(tl, mesh, N, t, eq):
+    xy = mesh.curved(N).xy
+    u = tl.initial_condition_convergence_test(xy[0], xy[1], t, eq)
+    return np.ascontiguousarray(np.transpose(u, (2, 1, 0, 3))).reshape(-1)
+
+
+def curved_xnode(mesh, N):
+    return np.ascontiguousarray(np.transpose(mesh.curved(N).xy, (3, 2, 1, 0)))
+
+
+def test_curved_oracle_with_source_terms_converges(tl, oracle_mod):
+    """The reference's structured kernels with the source (elixir_euler_source_terms_parallelogram.jl's kind of
+    setup on a warped periodic mesh): LW converges at order 4 (N = 4)."""
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    N = 4
+    errs = []
+    for cells in (4, 8, 16):
+        mesh = tl.StructuredMesh((cells, cells), warp2)
+        u = curved_state(tl, mesh, N, 0.0, eq)
+        o = oracle_mod.Oracle(mesh, N)
+        o.set_source(1, curved_xnode(mesh, N))
+        _, t = o.steps(u, 100000, 0.2, 0.0, 0.4, kind=0, nthreads=NTH)
+        errs.append(np.sqrt(np.mean((u - curved_state(tl, mesh, N, t, eq)) ** 2)))
+    orders = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
+    assert np.all(orders > 4.0), orders
+
+
+def make_curved_semi(tl, mesh, N, td="lw"):
+    eq = tl.CompressibleEulerEquations2D(1.4)
+    tdo = tl.LW() if td == "lw" else tl.MDRK()
+    solver = tl.DGSEM(N, tl.flux_lax_friedrichs, tl.VolumeIntegralFR(tdo))
+    return tl.SemidiscretizationHyperbolic(mesh, tdo, eq, tl.initial_condition_convergence_test, solver,
+                                           source_terms=tl.source_terms_convergence_test)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N", [3, 4, 5])
+def test_gpu_curved_rhs_with_source_terms_matches_oracle(tl, oracle_mod, N):
+    mesh = tl.StructuredMesh((6, 6), warp2)
+    semi = make_curved_semi(tl, mesh, N)
+    u = semi.compute_coefficients(0.0)
+    u = u * (1 + 1e-3 * np.random.default_rng(20 + N).standard_normal(u.shape))
+    o = oracle_mod.Oracle(mesh, N)
+    o.set_source(1, curved_xnode(mesh, N))
+    t, dt = 0.3, 0.5 * o.max_dt(u, 0.2)
+    semi.cache["dt"][0] = dt
+    du = np.empty_like(u)
+    tl.rhs(du, u, semi, t)
+    ref = o.rhs(u, t, dt, nthreads=NTH)
+    assert np.all(rel_l2(du, ref) < 1e-12), rel_l2(du, ref)
+
+
+@pytest.mark.gpu
+def test_gpu_curved_mdrk_with_source_terms_matches_oracle(tl, oracle_mod):
+    """MDRK on the curvilinear mesh: stage 2 takes the source at t, as the structured kernels do."""
+    N = 4
+    mesh = tl.StructuredMesh((6, 6), warp2)
+    semi = make_curved_semi(tl, mesh, N, "mdrk")
+    u = semi.compute_coefficients(0.0)
+    u = u * (1 + 1e-3 * np.random.default_rng(31).standard_normal(u.shape))
+    o = oracle_mod.Oracle(mesh, N)
+    o.set_source(1, curved_xnode(mesh, N))
+    t, dt = 0.2, 0.5 * o.max_dt(u, 0.2)
+    semi.cache["dt"][0] = dt
+    du1 = np.empty_like(u)
+    tl.rhs_mdrk1(du1, u, semi, t)
+    ref1 = o.rhs(u, t, dt, kind=1, nthreads=NTH)
+    assert np.all(rel_l2(du1, ref1) < 1e-12), rel_l2(du1, ref1)
+    us = u + dt * ref1
+    du2 = np.empty_like(u)
+    tl.rhs_mdrk2(du2, u, semi, t, us)
+    ref2 = o.rhs(u, t, dt, kind=2, us=us, nthreads=NTH)
+    assert np.all(rel_l2(du2, ref2) < 1e-12), rel_l2(du2, ref2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("td", ["lw", "mdrk"])
+def test_gpu_curved_steps_with_source_terms_match_oracle(tl, oracle_mod, td):
+    N = 4
+    mesh = tl.StructuredMesh((8, 8), warp2)
+    semi = make_curved_semi(tl, mesh, N, td)
+    u0 = semi.compute_coefficients(0.0)
+    integ = tl.LWIntegrator(tl.semidiscretize(semi, semi.time_discretization, (0.0, 1e9)))
+    integ.set_state(u0, 0.0)
+    integ.step(10, 0.2, use_graph=True)
+    integ.sync_time()
+    o = oracle_mod.Oracle(mesh, N)
+    o.set_source(1, curved_xnode(mesh, N))
+    u = u0.copy()
+    s, t = o.steps(u, 10, 0.2, 0.0, 1e9, kind=0 if td == "lw" else 1, nthreads=NTH)
+    assert s == integ.iter == 10 and integ.t == pytest.approx(t, rel=1e-13)
+    assert np.all(rel_l2(integ.get_state(), u) < 1e-12)

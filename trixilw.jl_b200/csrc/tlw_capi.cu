@@ -207,8 +207,12 @@ bool use_slots(const tlw_handle* h) {
 #endif
 // (not with shock capturing: the blended variant needs 142 registers and measured slower than the sweeps on the
 // 512^2 Riemann problem, 0.376 against about 0.34 ms)
+#ifndef TLW_SURFACE_PASS_SC
+#define TLW_SURFACE_PASS_SC 0
+#endif
 bool use_surface_pass(const tlw_handle* h) {
-    return TLW_SURFACE_PASS && h->d_nbr && !h->curved && !h->sc && h->nmx + h->nmy == 0 && h->nh == 0;
+    return TLW_SURFACE_PASS && h->d_nbr && !h->curved && (!h->sc || TLW_SURFACE_PASS_SC) && h->nmx + h->nmy == 0 &&
+           h->nh == 0;
 }
 
 // the halo faces of one class (cls 0: x, 1: y) as kernel arguments
@@ -1149,10 +1153,10 @@ int tlw_set_tree_mortars(tlw_handle* h, int64_t n_mortars, const int64_t* mortar
 
 int tlw_set_source_terms(tlw_handle* h, int32_t kind, const double* node_coordinates) {
     if (!h) return TLW_E_ARG;
-    if (!h->have_mesh) return fail(h, TLW_E_STATE, "source terms follow tlw_set_tree_mesh");
+    if (!h->have_mesh) return fail(h, TLW_E_STATE, "source terms follow the mesh upload");
     if (kind < 0 || kind > 1) return fail(h, TLW_E_ARG, "source kind: 0 none, 1 source_terms_convergence_test");
-    if (kind && (h->curved || h->parabolic || h->sc))
-        return fail(h, TLW_E_UNSUPPORTED, "source terms: TreeMesh, FR volume integral, Euler");
+    if (kind && (h->parabolic || h->sc))
+        return fail(h, TLW_E_UNSUPPORTED, "source terms: FR volume integral, Euler");
     if (kind && !node_coordinates) return fail(h, TLW_E_ARG, "node coordinates");
     TLW_CUDA(h, cudaSetDevice(h->device));
     TLW_CUDA(h, cudaStreamSynchronize(h->stream));

@@ -47,29 +47,42 @@ struct LaunchImpl {
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false, false, 0, false, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::smem_bytes(5));
-        // source terms (TreeMesh, FR)
+        // source terms (FR)
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, false, false, false, 0, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, false, false, false, 0, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, true, false, false, 0, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true, false, false, 0, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, false, true, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false, true, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, false, true, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
+        cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false, true, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_RHS, false, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk1_volume_kernel<N, MODE_STEP, false, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_RHS, false, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
         cudaFuncSetAttribute(mdrk2_volume_kernel<N, MODE_STEP, false, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, md);
     }
-    // source terms on the TreeMesh (FR volume integral): LW or an MDRK stage
-    static void volume_src(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
+    // source terms (FR volume integral, TreeMesh or curvilinear): LW or an MDRK stage
+    template <bool CURVED>
+    static void volume_src_on(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
         const size_t lw = C::smem_bytes(4), md = C::smem_bytes(2);
         if (stage == TLW_STAGE_LW) {
-            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, false, 0, false, false, false, 0, true><<<grid, C::THREADS, lw, s>>>(a);
-            else lw_volume_kernel<N, MODE_STEP, false, 0, false, false, false, 0, true><<<grid, C::THREADS, lw, s>>>(a);
+            if (mode == MODE_RHS) lw_volume_kernel<N, MODE_RHS, false, 0, CURVED, false, false, 0, true><<<grid, C::THREADS, lw, s>>>(a);
+            else lw_volume_kernel<N, MODE_STEP, false, 0, CURVED, false, false, 0, true><<<grid, C::THREADS, lw, s>>>(a);
         } else if (stage == TLW_STAGE_MDRK1) {
-            if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS, false, false, 0, true><<<grid, C::THREADS, md, s>>>(a);
-            else mdrk1_volume_kernel<N, MODE_STEP, false, false, 0, true><<<grid, C::THREADS, md, s>>>(a);
+            if (mode == MODE_RHS) mdrk1_volume_kernel<N, MODE_RHS, false, CURVED, 0, true><<<grid, C::THREADS, md, s>>>(a);
+            else mdrk1_volume_kernel<N, MODE_STEP, false, CURVED, 0, true><<<grid, C::THREADS, md, s>>>(a);
         } else {
-            if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS, false, false, 0, true><<<grid, C::THREADS, md, s>>>(a);
-            else mdrk2_volume_kernel<N, MODE_STEP, false, false, 0, true><<<grid, C::THREADS, md, s>>>(a);
+            if (mode == MODE_RHS) mdrk2_volume_kernel<N, MODE_RHS, false, CURVED, 0, true><<<grid, C::THREADS, md, s>>>(a);
+            else mdrk2_volume_kernel<N, MODE_STEP, false, CURVED, 0, true><<<grid, C::THREADS, md, s>>>(a);
         }
+    }
+    static void volume_src(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
+        if (a.metrics) volume_src_on<true>(s, stage, mode, a, grid);
+        else volume_src_on<false>(s, stage, mode, a, grid);
     }
     template <bool SC>
     static void volume_sc(cudaStream_t s, int stage, int mode, const VolArgs& a, int grid) {
@@ -148,7 +161,7 @@ struct LaunchImpl {
             te_volume(s, a, grid, sc, false);
             return;
         }
-        if (a.source && !a.metrics && !sc) {
+        if (a.source && !sc) {
             volume_src(s, stage, mode, a, grid);
             return;
         }

@@ -324,8 +324,11 @@ template <int N> struct SurfCfg {
 // and then the y face's (the order of the x and y launches), with the Jacobian and dt, and reduces the element's
 // face-node CFL speeds. Each interface is evaluated twice and each element's face nodes are read and written once:
 // no strided x sweep, no atomics.
+#ifndef TLW_SURF_MINB_SC
+#define TLW_SURF_MINB_SC 1
+#endif
 template <int N, bool BND, bool SC>
-static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? 1 : SurfCfg<N>::MIN_BLOCKS)
+static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? TLW_SURF_MINB_SC : SurfCfg<N>::MIN_BLOCKS)
     surface_kernel(SurfArgs a, BndArgs bnd) {
     using C = SurfCfg<N>;
     constexpr int n = N + 1, EB = C::EB, NB = 4 * (n - 1);

@@ -625,6 +625,9 @@ __device__ __forceinline__ void src_t_N34(const SrcNode& q, double* o) {
     src_stencil(q, 1.0 / 12.0, 1.0, -8.0, 0.0, 8.0, -1.0, o);
 }
 __device__ __forceinline__ void src_tt_N23(const SrcNode& q, double* o) { src_stencil(q, 1.0, 0.0, 1.0, -2.0, 1.0, 0.0, o); }
+__device__ __forceinline__ void src_tt_N4(const SrcNode& q, double* o) {
+    src_stencil(q, 1.0 / 12.0, -1.0, 16.0, -30.0, 16.0, -1.0, o);
+}
 __device__ __forceinline__ void src_ttt_N34(const SrcNode& q, double* o) {
     src_stencil(q, 0.5, -1.0, 2.0, 0.0, -2.0, 1.0, o);
 }
@@ -699,8 +702,10 @@ __device__ __forceinline__ void store_stage_derivative(const VolArgs& a, int m, 
 }
 
 // REC (curvilinear shock capturing): 0 first-order subcells, 1 MUSCL subcells
-// SRC: source terms (a.source, TreeMesh, FR volume integral): S = s + s_t/2 + s_tt/6 + ... with each stencil added
-// to its time derivative (dt s_k) before the perturbed states move, and S enters the update unscaled by J^{-1}.
+// SRC: source terms (a.source, FR volume integral): S = s + s_t/2 + s_tt/6 + ... with each stencil added to its time
+// derivative (dt s_k) before the perturbed states move, and S enters the update unscaled by J^{-1}. The curvilinear
+// kernel of depth 4 takes the 5-point s_tt (calc_source_tt_N4, dgsem_structured/dg_2d.jl:1886) where the TreeMesh
+// one takes the 3-point calc_source_tt_N23 (dgsem_tree/dg_2d.jl:1093-1104).
 template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false, int REC = 0,
           bool SRC = false>
 static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED) ? VolCfg<N, EBX>::SC_CURVED_MIN_BLOCKS
@@ -708,7 +713,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
                                                                         : VolCfg<N, EBX>::MIN_BLOCKS)
     lw_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
-    static_assert(!SRC || (!SC && !CURVED && !TE && !DSTORE), "source terms: the plain TreeMesh kernel");
+    static_assert(!SRC || (!SC && !TE && !DSTORE), "source terms: the FR volume integral, without the error estimate");
     // the temporal error estimate of the Adaptive step control: the TreeMesh computes it at depth 4 only
     // (lw_volume_kernel_3! of dgsem_tree has none), the curvilinear kernels at depths 3 and 4
     static_assert(!TE || (CURVED ? N >= 3 : N >= 4), "temporal errors: TreeMesh N >= 4, curvilinear N >= 3");
@@ -924,7 +929,10 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             node_sum<N, C>(X, Y, el, i, j, d);
             const double s = s0 * C2;
             double sk[NV];
-            if (SRC) src_tt_N23(sq, sk);   // s_tt = calc_source_tt_N23 at depths 3 and 4 (dg_2d.jl:1093-1104)
+            if (SRC) {   // s_tt: N23 at depths 3 and 4 on the TreeMesh (dg_2d.jl:1093-1104), N4 on curvilinear depth 4
+                if (CURVED && DEPTH == 4) src_tt_N4(sq, sk);
+                else src_tt_N23(sq, sk);
+            }
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 d[v] *= s;
@@ -1139,8 +1147,8 @@ __device__ __forceinline__ void mdrk_stage1_sums(double gm1, const double* uu, c
 // ------------------------------------------------------------------------------------------------
 // CURVED (mdrk_kernel_1!, src/solvers/dgsem_structured/multi_derivative_2d.jl:82-243): the contractions take the
 // contravariant fluxes, d carries the node's J^{-1}; F2, G2 stay physical, the traces are contravariant.
-// SRC (TreeMesh, FR): ut += dt s(u, t); S = s/2 + s_t/8 enters du, S2 = s + s_t/6 is stored for stage 2
-// (multi_derivative_2d.jl:321-400).
+// SRC (FR volume integral): ut += dt s(u, t); S = s/2 + s_t/8 enters du, S2 = s + s_t/6 is stored for stage 2
+// (multi_derivative_2d.jl:321-400; dgsem_structured/multi_derivative_2d.jl:151-239).
 // COMPACT (the plain TreeMesh step): store only u_t (into a.U2) instead of U2 and F2; stage 2 recomputes them from
 // u^n and u_t with this kernel's operations (64 instead of 192 bytes a node between the stages).
 template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
@@ -1148,7 +1156,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
                                                                          : VolCfg<N>::MDRK_MIN_BLOCKS)
     mdrk1_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
-    static_assert(!SRC || (!SC && !CURVED), "source terms: the plain TreeMesh kernel");
+    static_assert(!SRC || !SC, "source terms: the FR volume integral");
     static_assert(!COMPACT || (!SC && !CURVED && !SRC && MODE == MODE_STEP), "compact stages: the plain TreeMesh step");
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
@@ -1300,7 +1308,8 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
 // F = F2 + f_t(u*)/3, U = U2 + u*_t/3.
 // ------------------------------------------------------------------------------------------------
 // CURVED (mdrk_kernel_2!, src/solvers/dgsem_structured/multi_derivative_2d.jl:245-445): as in stage 1.
-// SRC (TreeMesh, FR): at t + dt/2, u*_t += dt s(u*); S = S2 + s_t(u*)/3 (multi_derivative_2d.jl:484-550).
+// SRC (FR volume integral): u*_t += dt s(u*); S = S2 + s_t(u*)/3 (multi_derivative_2d.jl:484-550), the source at
+// t + dt/2 on the TreeMesh and at t on curvilinear meshes (dgsem_structured/multi_derivative_2d.jl:325-361).
 // COMPACT: F2, G2, U2 recomputed from u^n (a.u_base) and stage 1's u_t (a.U2) at the start, parked in shared memory
 // (three more planes) until the stage's own sums are formed.
 template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
@@ -1308,7 +1317,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
                                                                          : VolCfg<N>::MDRK_MIN_BLOCKS)
     mdrk2_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
-    static_assert(!SRC || (!SC && !CURVED), "source terms: the plain TreeMesh kernel");
+    static_assert(!SRC || !SC, "source terms: the FR volume integral");
     static_assert(!COMPACT || (!SC && !CURVED && !SRC && MODE == MODE_STEP), "compact stages: the plain TreeMesh step");
     using C = VolCfg<N>;
     constexpr int n = C::n, nn = C::nn, EB = C::EB;
@@ -1389,7 +1398,9 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
         for (int v = 0; v < NV; ++v) d[v] *= s0;
         if (SRC) {
             const double* xn = a.xnode + 2 * ((size_t)e * nn + node);
-            const SrcNode sq{__ldg(xn), __ldg(xn + 1), *a.tnow + 0.5 * dt, dt, a.gamma};
+            // at t + dt/2 on the TreeMesh (multi_derivative_2d.jl:484-495), at t on curvilinear meshes
+            // (dgsem_structured/multi_derivative_2d.jl:336, 361)
+            const SrcNode sq{__ldg(xn), __ldg(xn + 1), CURVED ? *a.tnow : *a.tnow + 0.5 * dt, dt, a.gamma};
             double sn[NV], st[NV];
             src_eval(sq, 0.0, sn);
 #pragma unroll
