@@ -203,11 +203,13 @@ int tlw_set_unstructured_mesh(tlw_handle* h, int64_t n_elements, const double* c
 
 /* Source terms (SemidiscretizationHyperbolic(...; source_terms), calc_source and its time-derivative stencils,
  * src/solvers/dgsem_tree/dg_2d.jl:89-175, used by every LW kernel and by mdrk_kernel_1! / _2!,
- * multi_derivative_2d.jl:321-400 and :484-550), after tlw_set_tree_mesh (and again after a new mesh): kind 0 none,
+ * multi_derivative_2d.jl:321-400 and :484-550, and the structured kernels, dgsem_structured/dg_2d.jl:578-2058), after
+ * the mesh upload (and again after a new mesh): kind 0 none,
  * 1 Trixi's source_terms_convergence_test for CompressibleEulerEquations2D (the source of
  * initial_condition_convergence_test's manufactured solution); node_coordinates [2, i, j, e] as Trixi's
  * cache.elements.node_coordinates. The source is evaluated at the step's t (tlw_step: the device time; tlw_rhs:
- * its t argument; MDRK stage 2 at t + dt/2). TreeMesh, FR volume integral, Euler, LW or MDRK; not with
+ * its t argument; MDRK stage 2 at t + dt/2 on the TreeMesh, at t on curvilinear meshes, as the reference's
+ * structured kernels take it). TreeMesh or curvilinear mesh, FR volume integral, Euler, LW or MDRK; not with
  * Adaptive. */
 int tlw_set_source_terms(tlw_handle* h, int32_t kind, const double* node_coordinates);
 
