@@ -342,7 +342,7 @@ int oracle_dual_step(oracle_handle* h, int kind, const double* u, const double* 
 }
 
 // which: 0 U [v,i,j,e], 1 F [v,d,i,j,e], 2 U2, 3 F2, 4 temporal_errors [e], 5 surface_flux_values [v,l,face,e],
-//        6 alpha [e], 7 fn_low [v,l,face,e]
+//        6 alpha [e], 7 fn_low [v,l,face,e], 8 mortar_fixes [2] (curvilinear shock capturing)
 int oracle_get(oracle_handle* h, int which, double* out) {
     const std::vector<double>* src = nullptr;
     switch (which) {
@@ -354,6 +354,7 @@ int oracle_get(oracle_handle* h, int which, double* out) {
         case 5: src = &h->ws.surface_flux_values; break;
         case 6: src = &h->ws.alpha; break;
         case 7: src = &h->ws.fn_low; break;
+        case 8: src = &h->ws.mortar_fixes; break;
         default: return 1;
     }
     std::copy(src->begin(), src->end(), out);

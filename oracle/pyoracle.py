@@ -286,7 +286,7 @@ class Oracle:
 
     def get(self, which: int) -> np.ndarray:
         sizes = {0: self.size(), 1: 2 * self.size(), 2: self.size(), 3: 2 * self.size(), 4: self.E,
-                 5: 4 * self.n * 4 * self.E, 6: self.E, 7: 4 * self.n * 4 * self.E}
+                 5: 4 * self.n * 4 * self.E, 6: self.E, 7: 4 * self.n * 4 * self.E, 8: 2}
         out = np.empty(sizes[which])
         assert lib().oracle_get(self.h, which, _p(out)) == 0
         return out

@@ -411,8 +411,9 @@ inline void zhang_shu_flux_fix(const Euler& eq, const double* uprev, const doubl
         for (int v = 0; v < NV; ++v) Fn[v] = theta * Fn[v] + (1.0 - theta) * fn[v];
 }
 
-// get_blended_flux (src/solvers/dgsem_p4est/dg_2d.jl:227-250); J = the primary face node's J^{-1}
-inline void get_blended_flux(const Basis& b, const Euler& eq, const double* u_ll, const double* u_rr, double alpha_p,
+// get_blended_flux (src/solvers/dgsem_p4est/dg_2d.jl:227-250); J = the primary face node's J^{-1}. Returns which
+// sides took zhang_shu_flux_fix: bit 0 the primary (ll), bit 1 the secondary (rr).
+inline int get_blended_flux(const Basis& b, const Euler& eq, const double* u_ll, const double* u_rr, double alpha_p,
                              double alpha_s, double J, double dt, const double* fn, const double* Fn_,
                              const double* fil, const double* fir, double* Fn) {
     const int n = b.n;
@@ -425,13 +426,21 @@ inline void get_blended_flux(const Basis& b, const Euler& eq, const double* u_ll
         test[v] = u_ll[v] - c_ll * (Fn[v] - fil[v]);
         low[v] = u_ll[v] - c_ll * (fn[v] - fil[v]);
     }
-    if (!eq.is_admissible(test)) zhang_shu_flux_fix(eq, u_ll, low, Fn, fil, fn, c_ll);
+    int fixed = 0;
+    if (!eq.is_admissible(test)) {
+        zhang_shu_flux_fix(eq, u_ll, low, Fn, fil, fn, c_ll);
+        fixed |= 1;
+    }
     const double c_rr = -dt * J / (b.weights[0] * lam);
     for (int v = 0; v < NV; ++v) {
         test[v] = u_rr[v] - c_rr * (Fn[v] - fir[v]);
         low[v] = u_rr[v] - c_rr * (fn[v] - fir[v]);
     }
-    if (!eq.is_admissible(test)) zhang_shu_flux_fix(eq, u_rr, low, Fn, fir, fn, c_rr);
+    if (!eq.is_admissible(test)) {
+        zhang_shu_flux_fix(eq, u_rr, low, Fn, fir, fn, c_rr);
+        fixed |= 2;
+    }
+    return fixed;
 }
 
 // du = rhs(u) with VolumeIntegralFRShockCapturing on a conforming curvilinear mesh (Rusanov surface flux); the
@@ -566,6 +575,7 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
     // node, fn_inner_rr the large element's fn_low slot of its face read in mortar order (index i, no
     // reversal) and interpolated like u (prolong2mortars!, :429-500), and J^{-1} = lw_mortars.inverse_jacobian
     bad = false;
+    ws.mortar_fixes.assign(2, 0.0);
     auto mortar_blend = [&](int k, int h, int l, int se, const double* u_ll, const double* u_rr, const double* nS,
                             double* fstar) {
         const int lg = m.m_large[k], lf = m.m_lface[k], sf = m.m_sface[k];
@@ -578,7 +588,10 @@ inline void rhs_curved_sc(const Basis& b, const Euler& eq, const Options& opt, c
         rusanov_normal(eq, opt.speed_kind, u_ll, u_rr, nS, fn, b_);
         bad = bad || b_;
         const double J = m.m_ij.empty() ? 0.0 : m.m_ij[(size_t)k * n + l];
-        get_blended_flux(b, eq, u_ll, u_rr, ws.alpha[se], ws.alpha[lg], J, dt, fn, fstar, fil, fir, Fn);
+        const int fixed =
+            get_blended_flux(b, eq, u_ll, u_rr, ws.alpha[se], ws.alpha[lg], J, dt, fn, fstar, fil, fir, Fn);
+        if (fixed & 1) ws.mortar_fixes[0] += 1.0;
+        if (fixed & 2) ws.mortar_fixes[1] += 1.0;
         for (int v = 0; v < NV; ++v) fstar[v] = Fn[v];
     };
     calc_mortar_flux_curved(b, eq, opt, m, u, ws, bad, mortar_blend);

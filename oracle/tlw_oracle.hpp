@@ -410,6 +410,9 @@ struct Workspace {
     std::vector<double> bu, bU, bF;
     std::vector<double> alpha;           // blending factor per element (shock capturing)
     std::vector<double> fn_low;          // [v, l, face, e] first-order subcell flux next to each face
+    // small-mortar nodes of the last curvilinear shock-capturing rhs at which zhang_shu_flux_fix changed the
+    // blended flux: [0] the small element's side, [1] the large element's side
+    std::vector<double> mortar_fixes = std::vector<double>(2, 0.0);
     bool bad = false;                    // a sqrt of a negative number happened (Julia DomainError)
 };
 

@@ -74,6 +74,26 @@ def test_oracle_sc_mortar_conservation(oracle_mod, tl, rec, given_jacobian):
     assert np.all(np.abs(quad(cm, N, du)) < 1e-10)
 
 
+@pytest.mark.parametrize("rec", [0, 2])
+def test_oracle_sc_mortar_flux_fix_fires_on_both_sides(oracle_mod, tl, rec):
+    """With four times the small elements' J^{-1} as lw_mortars.inverse_jacobian the subcell test updates at the
+    mortars leave the admissible set, and zhang_shu_flux_fix (dgsem_p4est/dg_2d.jl:199-225) changes the blended
+    flux on the small side and on the large side; with a zero J^{-1} it never does. The rhs still conserves."""
+    N = 4
+    cm = refined(tl).curved(N)
+    u = evolved_blast(oracle_mod, cm, N, rec)
+    o = sc_oracle(oracle_mod, cm, N, rec)
+    dt = o.max_dt(u, 0.2)
+    o.rhs(u, 0.0, dt)
+    assert np.all(o.get(8) == 0)
+    o.set_curved_mortar_jacobian(4.0 * mortar_jacobian(cm, N))
+    du = o.rhs(u, 0.0, dt)
+    fixes = o.get(8)
+    assert fixes[0] > 0 and fixes[1] > 0
+    assert fixes.max() <= 2 * cm.n_mortars * (N + 1)
+    assert np.all(np.abs(quad(cm, N, du)) < 1e-10)
+
+
 def test_oracle_sc_mortar_smoothing_reaches_across(oracle_mod, tl):
     """Smoothing over the mortars: each small element's alpha is at least half its large neighbour's raw
     (unsmoothed) alpha, and the other way round."""
@@ -125,6 +145,29 @@ def test_gpu_sc_mortar_rhs_matches_oracle(oracle_mod, tl, N, rec, given_jacobian
     # the indicator's sigmoid is ill-conditioned near its threshold: small blending factors of the evolved
     # state agree to about 1e-13 absolute
     np.testing.assert_allclose(semi.get_cache(_lib.TLW_CACHE_ALPHA), o.get(6), rtol=1e-10, atol=1e-12)
+    assert np.all(rel_l2(u + dt * du_gpu, u + dt * du_cpu) < 1e-12)
+    assert np.all(rel_l2(du_gpu, du_cpu) < 1e-10)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,rec", [(3, 0), (4, 2), (5, 1)])
+def test_gpu_sc_mortar_flux_fix_matches_oracle(oracle_mod, tl, N, rec):
+    """The mortar nodes' zhang_shu_flux_fix branches on the GPU: four times the small elements' J^{-1} makes
+    the fix fire on both sides of many small-mortar nodes (counted by the oracle), and the rhs matches."""
+    cm = refined(tl).curved(N)
+    u = evolved_blast(oracle_mod, cm, N, rec)
+    mj = 4.0 * mortar_jacobian(cm, N)
+    o = sc_oracle(oracle_mod, cm, N, rec)
+    o.set_curved_mortar_jacobian(mj)
+    semi = sc_semi(tl, cm, N, rec)
+    semi.set_mortar_inverse_jacobian(mj)
+    dt = o.max_dt(u, 0.2)
+    du_cpu = o.rhs(u, 0.0, dt)
+    fixes = o.get(8)
+    assert fixes[0] > 0 and fixes[1] > 0
+    semi.cache["dt"][0] = dt
+    du_gpu = np.empty_like(u)
+    tl.rhs(du_gpu, u, semi, 0.0)
     assert np.all(rel_l2(u + dt * du_gpu, u + dt * du_cpu) < 1e-12)
     assert np.all(rel_l2(du_gpu, du_cpu) < 1e-10)
 
