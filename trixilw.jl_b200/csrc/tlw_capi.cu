@@ -55,6 +55,8 @@ void free_mesh(tlw_handle* h) {
     drop_graphs(h);
     dfree(h->d_inv_jac);
     dfree(h->d_xl); dfree(h->d_xr); dfree(h->d_yl); dfree(h->d_yr); dfree(h->d_nbr);
+    dfree(h->d_fuse_list); dfree(h->d_fuse_off); dfree(h->d_fuse_ticket); dfree(h->d_fuse_ready);
+    h->fuse_tiles = 0;
     dfree(h->d_xnode); dfree(h->d_S2);
     h->source = 0;
     dfree(h->d_b_elem); dfree(h->d_b_dir); dfree(h->d_bx); dfree(h->d_by);
@@ -122,6 +124,12 @@ void dispatch(int N, A&&... args) {
     }
 }
 template <int N> struct SetAttr { static void run() { Launch<N>::set_attributes(); } };
+template <int N> struct Tile { static void run(int& eb) { eb = Launch<N>::volume_tile(); } };
+template <int N> struct Fused {
+    static void run(cudaStream_t s, int mode, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa) {
+        Launch<N>::fused(s, mode, va, sa, fa);
+    }
+};
 template <int N> struct Vol {
     static void run(cudaStream_t s, int st, int m, bool sc, const VolArgs& a) { Launch<N>::volume(s, st, m, sc, a); }
 };
@@ -213,6 +221,34 @@ bool use_slots(const tlw_handle* h) {
 bool use_surface_pass(const tlw_handle* h) {
     return TLW_SURFACE_PASS && h->d_nbr && !h->curved && (!h->sc || TLW_SURFACE_PASS_SC) && h->nmx + h->nmy == 0 &&
            h->nh == 0;
+}
+
+// the volume and surface passes of an LW stage in one launch (lw_fused_kernel): a periodic conforming TreeMesh
+// with the FR volume integral and nothing else on its faces or in its volume
+#ifndef TLW_FUSED_STEP
+#define TLW_FUSED_STEP 1
+#endif
+bool use_fused(const tlw_handle* h, int stage, int phases) {
+    return TLW_FUSED_STEP && h->fuse_enabled && h->fuse_tiles > 0 && stage == TLW_STAGE_LW && phases == 7 &&
+           use_surface_pass(h) && !h->sc && !h->parabolic && !h->source && !h->te_request && h->nb == 0;
+}
+
+// the fused launch's surface lists: element s is surfaced by the ticket of the last tile among its own and its
+// four neighbours' (tile = element / eb); a counting sort by that ticket
+void fuse_lists(const std::vector<int>& nbr, int64_t E, int eb, std::vector<int>& list, std::vector<int>& off) {
+    const int tiles = (int)((E + eb - 1) / eb);
+    std::vector<int> r((size_t)E);
+    off.assign((size_t)tiles + 1, 0);
+    for (int64_t e = 0; e < E; ++e) {
+        int t = (int)(e / eb);
+        for (int f = 0; f < 4; ++f) t = std::max(t, nbr[(size_t)4 * e + f] / eb);
+        r[(size_t)e] = t;
+        ++off[(size_t)t + 1];
+    }
+    for (int t = 0; t < tiles; ++t) off[(size_t)t + 1] += off[(size_t)t];
+    list.assign((size_t)E, 0);
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int64_t e = 0; e < E; ++e) list[(size_t)fill[(size_t)r[(size_t)e]]++] = (int)e;
 }
 
 // the halo faces of one class (cls 0: x, 1: y) as kernel arguments
@@ -503,6 +539,33 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
             va.reconstruction = h->reconstruction;
         }
     }
+    if (use_fused(h, stage, phases)) {
+        SurfArgs sa{};
+        sa.u = u_jump;
+        sa.out = out;
+        sa.tU = h->d_tU;
+        sa.tF = h->d_tF;
+        sa.inv_jac = h->d_inv_jac;
+        sa.dt = dt_ptr;
+        sa.step_mode = mode == MODE_STEP;
+        sa.gamma = h->opts.gamma;
+        sa.flux_kind = h->opts.surface_flux;
+        sa.speed_kind = h->opts.max_speed;
+        sa.inv_w_first = h->h_basis.inv_w_first;
+        sa.inv_w_last = h->h_basis.inv_w_last;
+        sa.status = &h->d_step->status;
+        sa.cfl_slots = va.cfl_slots;
+        sa.nbr = h->d_nbr;
+        sa.E = (int)h->E;
+        FuseArgs fa{h->d_fuse_ticket, h->d_fuse_ready, h->d_fuse_list, h->d_fuse_off, h->d_nbr, h->fuse_tiles};
+        dispatch<Fused>(h->N, h->stream, mode, va, sa, fa);
+        if (ev) {
+            cudaEventRecord(ev->after_volume, h->stream);
+            cudaEventRecord(ev->after_x, h->stream);
+            cudaEventRecord(ev->after_y, h->stream);
+        }
+        return;
+    }
     if (phases & 1) {
         dispatch<Vol>(h->N, h->stream, stage, mode, h->sc, va);
         if (ev) cudaEventRecord(ev->after_volume, h->stream);
@@ -673,6 +736,8 @@ int read_status(tlw_handle* h) {
     if (st) {
         const unsigned zero = 0;
         TLW_CUDA(h, upload_on(h->stream, &h->d_step->status, &zero, sizeof(zero)));
+        if (st & STATUS_WAIT_LIMIT)
+            return fail(h, TLW_E_CUDA, "fused launch: a dependency wait gave up (results of the call are invalid)");
         return fail(h, TLW_E_NONADMISSIBLE, "non-admissible state: square root of a negative number (DomainError)");
     }
     return TLW_OK;
@@ -834,6 +899,18 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
         for (size_t k = 0; k < yl.size(); ++k) { put(yl[k], 3, yr[k]); put(yr[k], 2, yl[k]); }
         for (size_t k = 0; k < belem.size(); ++k) put(belem[k], bdir[k] - 1, -(int)k - 1);
         if (ok && (rc = up_i(h->d_nbr, nbr))) return rc;
+        if (ok && n_boundaries == 0) {
+            int eb = 0;
+            dispatch<Tile>(h->N, eb);
+            std::vector<int> list, off;
+            fuse_lists(nbr, n_elements, eb, list, off);
+            h->fuse_tiles = (int)off.size() - 1;
+            if ((rc = up_i(h->d_fuse_list, list)) || (rc = up_i(h->d_fuse_off, off))) return rc;
+            TLW_CUDA(h, cudaMalloc(&h->d_fuse_ticket, sizeof(unsigned long long)));
+            TLW_CUDA(h, cudaMalloc(&h->d_fuse_ready, (size_t)h->fuse_tiles * sizeof(unsigned)));
+            TLW_CUDA(h, zero_on(h->stream, h->d_fuse_ticket, sizeof(unsigned long long)));
+            TLW_CUDA(h, zero_on(h->stream, h->d_fuse_ready, (size_t)h->fuse_tiles * sizeof(unsigned)));
+        }
     }
     h->jac_first = inverse_jacobian[0];
     if (h->sc) {
@@ -2183,6 +2260,16 @@ int tlw_get_stream(tlw_handle* h, void** stream) {
     if (!h || !stream) return TLW_E_ARG;
     *stream = (void*)h->stream;
     return TLW_OK;
+}
+
+int32_t tlw_set_fused_step(tlw_handle* h, int32_t enable) {
+    if (!h) return -1;
+    const int32_t was = (h->fuse_enabled ? 1 : 0) | (h->fuse_tiles > 0 ? 2 : 0);
+    if ((enable == 0 || enable == 1) && (enable == 1) != h->fuse_enabled) {
+        h->fuse_enabled = enable == 1;
+        drop_graphs(h);   // captured steps hold the other path
+    }
+    return was;
 }
 
 int tlw_state_pointer(tlw_handle* h, double** dptr) {

@@ -34,6 +34,8 @@ struct LaunchImpl {
         set_attr_sc<false>();
         set_attr_sc<true>();
         const int lw = (int)C::smem_bytes(4);
+        cudaFuncSetAttribute(lw_fused_kernel<N, MODE_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
+        cudaFuncSetAttribute(lw_fused_kernel<N, MODE_STEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
         te_volume(nullptr, VolArgs{}, 0, false, true);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
@@ -206,6 +208,12 @@ struct LaunchImpl {
             else surface_kernel<N, false, false><<<grid, C::THREADS, 0, s>>>(a, b);
         }
     }
+    static void fused(cudaStream_t s, int mode, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa) {
+        if (fa.tiles <= 0) return;
+        const size_t sm = C::smem_bytes(4);
+        if (mode == MODE_RHS) lw_fused_kernel<N, MODE_RHS><<<fa.tiles, C::THREADS, sm, s>>>(va, sa, fa);
+        else lw_fused_kernel<N, MODE_STEP><<<fa.tiles, C::THREADS, sm, s>>>(va, sa, fa);
+    }
     static void parabolic(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out,
                           const double* dtp) {
         if constexpr (N >= 3) {
@@ -346,6 +354,11 @@ template <int N> void Launch<N>::volume(cudaStream_t s, int stage, int mode, boo
     LaunchImpl<N>::volume(s, stage, mode, sc, a);
 }
 template <int N> void Launch<N>::interfaces(cudaStream_t s, const SurfArgs& a) { LaunchImpl<N>::interfaces(s, a); }
+template <int N> int Launch<N>::volume_tile() { return VolCfg<N>::EB; }
+template <int N>
+void Launch<N>::fused(cudaStream_t s, int mode, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa) {
+    LaunchImpl<N>::fused(s, mode, va, sa, fa);
+}
 template <int N> void Launch<N>::surfaces(cudaStream_t s, const SurfArgs& a, const BndArgs& b) {
     LaunchImpl<N>::surfaces(s, a, b);
 }

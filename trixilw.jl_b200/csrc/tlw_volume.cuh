@@ -641,7 +641,7 @@ __device__ __forceinline__ void src_tttt_N4(const SrcNode& q, double* o) {
 // Every thread of the CTA calls it (barriers inside).
 template <int N, class C>
 __device__ __forceinline__ void write_interior_slots(const VolArgs& a, double* X, bool active, int el, int i, int j,
-                                                     int tid, double l1, double l2) {
+                                                     int tid, int e0, double l1, double l2) {
     constexpr int n = C::n, EB = C::EB;
     __syncthreads();
     if (active) {
@@ -649,7 +649,7 @@ __device__ __forceinline__ void write_interior_slots(const VolArgs& a, double* X
         X[(EB + el) * C::P + i + C::R * j] = l2;
     }
     __syncthreads();
-    const int ee = blockIdx.x * EB + (tid >> 1);
+    const int ee = e0 + (tid >> 1);
     if (tid < 2 * EB && ee < a.E) {
         const double* p = X + ((tid & 1) * EB + (tid >> 1)) * C::P;
         double m = 0.0;
@@ -706,12 +706,10 @@ __device__ __forceinline__ void store_stage_derivative(const VolArgs& a, int m, 
 // derivative (dt s_k) before the perturbed states move, and S enters the update unscaled by J^{-1}. The curvilinear
 // kernel of depth 4 takes the 5-point s_tt (calc_source_tt_N4, dgsem_structured/dg_2d.jl:1886) where the TreeMesh
 // one takes the 3-point calc_source_tt_N23 (dgsem_tree/dg_2d.jl:1093-1104).
+// lw_volume_tile: the elements [tile EB, tile EB + EB) of one CTA (lw_volume_kernel: tile = blockIdx.x).
 template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false, int REC = 0,
           bool SRC = false>
-static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED) ? VolCfg<N, EBX>::SC_CURVED_MIN_BLOCKS
-                                                                  : SRC ? VolCfg<N, EBX>::MDRK_MIN_BLOCKS - 1
-                                                                        : VolCfg<N, EBX>::MIN_BLOCKS)
-    lw_volume_kernel(VolArgs a) {
+__device__ __forceinline__ void lw_volume_tile(const VolArgs& a, const int tile) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     static_assert(!SRC || (!SC && !TE && !DSTORE), "source terms: the FR volume integral, without the error estimate");
     // the temporal error estimate of the Adaptive step control: the TreeMesh computes it at depth 4 only
@@ -741,7 +739,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
-    const int e = blockIdx.x * EB + el;
+    const int e = tile * EB + el;
     const bool active = el < EB && e < a.E;
     // curvilinear shock capturing: pure_and_blended_element_ids! (DG only where alpha is within 1e-12 of 0);
     // MUSCL subcells on blended elements without a boundary face
@@ -1067,7 +1065,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o, SRC ? Ssrc : nullptr);
         if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) node_speeds(a.gamma, o, a.status, l1, l2);
     }
-    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, l1, l2);
+    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, tile * EB, l1, l2);
     if (TE) {
         // lw_volume_kernel_4!'s error estimate (dg_2d.jl:1183-1265; curvilinear, with F~, G~ and the node's
         // J^{-1}: dgsem_structured/dg_2d.jl:1595-1682 at depth 3, :1983-2075 at depth 4): the strong-form volume
@@ -1103,7 +1101,7 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
         __syncthreads();
         if (active) X[el * C::P + i + C::R * j] = err;
         __syncthreads();
-        const int ee = blockIdx.x * EB + tid;
+        const int ee = tile * EB + tid;
         if (tid < EB && ee < a.E) {
             double sum = 0.0;
             for (int jj = 0; jj < n; ++jj)
@@ -1111,6 +1109,15 @@ static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED)
             a.temporal_errors[ee] = sum;
         }
     }
+}
+
+template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false, int REC = 0,
+          bool SRC = false>
+static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED) ? VolCfg<N, EBX>::SC_CURVED_MIN_BLOCKS
+                                                                  : SRC ? VolCfg<N, EBX>::MDRK_MIN_BLOCKS - 1
+                                                                        : VolCfg<N, EBX>::MIN_BLOCKS)
+    lw_volume_kernel(VolArgs a) {
+    lw_volume_tile<N, MODE, SC, EBX, CURVED, TE, DSTORE, REC, SRC>(a, blockIdx.x);
 }
 
 // MDRK stage 1's stored sums from u^n and d = u_t: F2 = f + f_t/6, G2 = g + g_t/6, U2 = u + u_t/6 with f_t the
@@ -1469,7 +1476,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o, SRC ? Ssrc : nullptr);
         if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) node_speeds(a.gamma, o, a.status, l1, l2);
     }
-    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, l1, l2);
+    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, blockIdx.x * EB, l1, l2);
 }
 
 }  // namespace tlw
