@@ -102,6 +102,22 @@ def volume_kernel_bytes_per_element(N: int, td: str, curved: bool = False, sc: b
     return 8.0 * b
 
 
+def mdrk_volume_bytes_per_element(N: int) -> float:
+    """Algorithmic bytes of the two compact MDRK stage kernels of a step per element: stage 1 reads u^n and writes
+    u*, u_t and the U, F.n face traces; stage 2 reads u*, u^n and u_t and writes u^{n+1} and the face traces."""
+    n, nv = N + 1, 4
+    return 8.0 * (7 * nv * n * n + 2 * 2 * 4 * n * nv)
+
+
+def mdrk_volume_flops_per_node(N: int) -> float:
+    """Algorithmic FP64 flops per node of the two compact MDRK stage kernels (FMA = 2, divides not counted), in
+    the terms of the LW model: four line contractions of F and G (16 n nv), 15 flux pairs at 17 (stage 1: u^n and
+    u^n +- u_t, +- 2 u_t; stage 2: the same five again for F2, G2 and five at u*) and about 250 for the stages'
+    sums and updates."""
+    n, nv = N + 1, 4
+    return 16 * n * nv + 15 * 17 + 250
+
+
 def surface_pass_bytes_per_element(N: int) -> float:
     """Algorithmic (unique) bytes of one element-centric surface launch per element: read the element's own U
     and F.n face traces (2 x 4 faces x n x nv), read its 4(n - 1) face nodes of u for the jumps, read-modify-write
@@ -510,10 +526,10 @@ def run_ours(args):
     # per-phase device time of K further steps (events between the kernels of each step)
     phase = (ctypes.c_double * 5)()
     _lib.check(semi.handle, L.tlw_step_timed(semi.handle, args.steps, cfl, 0.0, 1e9, phase))
-    # an LW step on a periodic conforming TreeMesh runs the volume and surface passes in one launch
+    # an LW step or MDRK stage on a periodic conforming TreeMesh runs the volume and surface passes in one launch
     # (lw_fused_kernel); the same K steps in the two-launch path, for comparison
-    fused = td == "lw" and (int(L.tlw_set_fused_step(semi.handle, 2)) & 3) == 3 and icname not in (
-        "riemann", "blast", "warped", "cavity")
+    fused = (int(L.tlw_set_fused_step(semi.handle, 2)) & 3) == 3 and icname not in ("riemann", "blast", "warped",
+                                                                                       "cavity")
     two_launch = None
     if fused:
         L.tlw_set_fused_step(semi.handle, 0)
@@ -590,13 +606,16 @@ def run_ours(args):
         sc = icname in ("riemann", "blast")
         peak, peak_kind = measured_peaks()
         vol_ms = phase[1] / args.steps
-        vol_bytes = (ns_volume_bytes_per_element(N) if ns else volume_kernel_bytes_per_element(N, td, curved, sc)) * E
-        if fused:   # the fused launch also moves the surface pass's bytes
-            vol_bytes += surface_pass_bytes_per_element(N) * E
+        plain_mdrk = td == "mdrk" and not (ns or sc or curved)
+        vol_bytes = (ns_volume_bytes_per_element(N) if ns else mdrk_volume_bytes_per_element(N) if plain_mdrk
+                     else volume_kernel_bytes_per_element(N, td, curved, sc)) * E
+        if fused:   # the fused launches also move the surface passes' bytes
+            vol_bytes += (2 if td == "mdrk" else 1) * surface_pass_bytes_per_element(N) * E
         achieved = vol_bytes / (vol_ms * 1e-3) / 1e9
         fp = ctypes.c_double()
         fp64_peak = fp.value if L.tlw_probe_fp64_tflops(local_rank, ctypes.byref(fp)) == 0 else None
-        vol_flops = None if (ns or sc) else volume_flops_per_node(N) * ndofs
+        vol_flops = (None if (ns or sc) else mdrk_volume_flops_per_node(N) * ndofs if plain_mdrk
+                     else volume_flops_per_node(N) * ndofs)
         tag = (f"par_volume_kernel_N{N}_cavity{1 << level}" if ns
                else f"lw_fused_kernel_N{N}_tree{1 << level}" if fused
                else f"lw_volume_kernel_N{N}_blast_muscl{1 << level}" if icname == "blast"
@@ -646,7 +665,8 @@ def run_ours(args):
                     "round_trip": {"value": e2e_rt, "unit": UNIT,
                                    "api": "tlw_set_state + tlw_step + tlw_get_state (synchronous, serial copies)"}},
             "roofline": {"kernel": (f"grad_volume_kernel + curved_grad_*_kernel + par_volume_kernel<{N}, MODE_STEP, CURVED>"
-                                    if ns else f"lw_fused_kernel<{N}, MODE_STEP> (volume and surface passes)" if fused
+                                    if ns else (f"lw_fused_kernel<{N}, MODE_STEP, {'MDRK stages 1 and 2' if td == 'mdrk' else 'LW'}>"
+                                                " (volume and surface passes)") if fused
                                     else f"lw_volume_kernel<{N}, MODE_STEP, SC, CURVED, MUSCL>" if icname == "blast"
                                     else f"lw_volume_kernel<{N}, MODE_STEP{', SC' if sc else ''}{', CURVED' if curved else ''}>"),
                          "bound": "fp64" if fp64_bound else "hbm",
@@ -664,7 +684,7 @@ def run_ours(args):
             "clocks": clocks,
             "gpu_launches": args.steps * ((9 + 2 * int(L.tlw_curved_colors(semi.handle))) if ns else
                                           (5 + int(L.tlw_curved_colors(semi.handle))) if icname == "blast" else
-                                          (3 if fused else 2 + 2 * stages + (1 if icname == "riemann" else 0))),
+                                          (2 + stages if fused else 2 + 2 * stages + (1 if icname == "riemann" else 0))),
         }
         if world == 1 and not args.no_cpu_baseline:
             rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=args.steps)

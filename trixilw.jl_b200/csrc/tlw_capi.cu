@@ -56,7 +56,7 @@ void free_mesh(tlw_handle* h) {
     dfree(h->d_inv_jac);
     dfree(h->d_xl); dfree(h->d_xr); dfree(h->d_yl); dfree(h->d_yr); dfree(h->d_nbr);
     dfree(h->d_fuse_list); dfree(h->d_fuse_off); dfree(h->d_fuse_ticket); dfree(h->d_fuse_ready);
-    h->fuse_tiles = 0;
+    h->fuse_tiles = h->fuse_grid = 0;
     dfree(h->d_xnode); dfree(h->d_S2);
     h->source = 0;
     dfree(h->d_b_elem); dfree(h->d_b_dir); dfree(h->d_bx); dfree(h->d_by);
@@ -125,9 +125,10 @@ void dispatch(int N, A&&... args) {
 }
 template <int N> struct SetAttr { static void run() { Launch<N>::set_attributes(); } };
 template <int N> struct Tile { static void run(int& eb) { eb = Launch<N>::volume_tile(); } };
+template <int N> struct Group { static void run(int& g) { g = FusedCfg<N>::GROUP; } };
 template <int N> struct Fused {
-    static void run(cudaStream_t s, int mode, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa) {
-        Launch<N>::fused(s, mode, va, sa, fa);
+    static void run(cudaStream_t s, int stage, int mode, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa) {
+        Launch<N>::fused(s, stage, mode, va, sa, fa);
     }
 };
 template <int N> struct Vol {
@@ -223,32 +224,46 @@ bool use_surface_pass(const tlw_handle* h) {
            h->nh == 0;
 }
 
-// the volume and surface passes of an LW stage in one launch (lw_fused_kernel): a periodic conforming TreeMesh
-// with the FR volume integral and nothing else on its faces or in its volume
+// the volume and surface passes of an LW step or an MDRK stage in one launch (lw_fused_kernel): a periodic
+// conforming TreeMesh with the FR volume integral and nothing else on its faces or in its volume
 #ifndef TLW_FUSED_STEP
 #define TLW_FUSED_STEP 1
 #endif
 bool use_fused(const tlw_handle* h, int stage, int phases) {
-    return TLW_FUSED_STEP && h->fuse_enabled && h->fuse_tiles > 0 && stage == TLW_STAGE_LW && phases == 7 &&
-           use_surface_pass(h) && !h->sc && !h->parabolic && !h->source && !h->te_request && h->nb == 0;
+    return TLW_FUSED_STEP && h->fuse_enabled && h->fuse_tiles > 0 && phases == 7 && use_surface_pass(h) && !h->sc &&
+           !h->parabolic && !h->source && !h->te_request && h->nb == 0;
 }
 
-// the fused launch's surface lists: element s is surfaced by the ticket of the last tile among its own and its
-// four neighbours' (tile = element / eb); a counting sort by that ticket
-void fuse_lists(const std::vector<int>& nbr, int64_t E, int eb, std::vector<int>& list, std::vector<int>& off) {
+// the fused launch's surface lists: element s depends on the volume phases of its own and its four neighbours'
+// tiles (tile = element / eb) and is ready after the last of them, r(s). Tickets take the ready elements in order
+// of r, at most cap a ticket, each no earlier than lag tickets after its r (tickets at or past the last tile take
+// any); the tickets past the last tile form the surface-only tail. Returns the tickets of a launch.
+#ifndef TLW_FUSE_LAG
+#define TLW_FUSE_LAG 0
+#endif
+int fuse_lists(const std::vector<int>& nbr, int64_t E, int eb, int lag, int cap, std::vector<int>& list,
+               std::vector<int>& off) {
     const int tiles = (int)((E + eb - 1) / eb);
-    std::vector<int> r((size_t)E);
-    off.assign((size_t)tiles + 1, 0);
+    std::vector<int> r((size_t)E), cnt((size_t)tiles + 1, 0);
     for (int64_t e = 0; e < E; ++e) {
         int t = (int)(e / eb);
         for (int f = 0; f < 4; ++f) t = std::max(t, nbr[(size_t)4 * e + f] / eb);
         r[(size_t)e] = t;
-        ++off[(size_t)t + 1];
+        ++cnt[(size_t)t + 1];
     }
-    for (int t = 0; t < tiles; ++t) off[(size_t)t + 1] += off[(size_t)t];
+    for (int t = 0; t < tiles; ++t) cnt[(size_t)t + 1] += cnt[(size_t)t];
     list.assign((size_t)E, 0);
-    std::vector<int> fill(off.begin(), off.end() - 1);
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
     for (int64_t e = 0; e < E; ++e) list[(size_t)fill[(size_t)r[(size_t)e]]++] = (int)e;
+    // list is sorted by r; ticket q takes up to cap of the next elements with r + lag <= q (any once q >= tiles)
+    off.assign(1, 0);
+    int64_t p = 0;
+    for (int q = 0; p < E || q < tiles; ++q) {
+        int k = 0;
+        while (p < E && k < cap && (q >= tiles || r[(size_t)list[(size_t)p]] + lag <= q)) { ++p; ++k; }
+        off.push_back((int)p);
+    }
+    return (int)off.size() - 1;
 }
 
 // the halo faces of one class (cls 0: x, 1: y) as kernel arguments
@@ -557,8 +572,9 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
         sa.cfl_slots = va.cfl_slots;
         sa.nbr = h->d_nbr;
         sa.E = (int)h->E;
-        FuseArgs fa{h->d_fuse_ticket, h->d_fuse_ready, h->d_fuse_list, h->d_fuse_off, h->d_nbr, h->fuse_tiles};
-        dispatch<Fused>(h->N, h->stream, mode, va, sa, fa);
+        FuseArgs fa{h->d_fuse_ticket, h->d_fuse_ready, h->d_fuse_list, h->d_fuse_off, h->d_nbr, h->fuse_tiles,
+                    h->fuse_grid};
+        dispatch<Fused>(h->N, h->stream, stage, mode, va, sa, fa);
         if (ev) {
             cudaEventRecord(ev->after_volume, h->stream);
             cudaEventRecord(ev->after_x, h->stream);
@@ -903,8 +919,10 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
             int eb = 0;
             dispatch<Tile>(h->N, eb);
             std::vector<int> list, off;
-            fuse_lists(nbr, n_elements, eb, list, off);
-            h->fuse_tiles = (int)off.size() - 1;
+            int cap = 0;
+            dispatch<Group>(h->N, cap);
+            h->fuse_tiles = (int)((n_elements + eb - 1) / eb);
+            h->fuse_grid = fuse_lists(nbr, n_elements, eb, TLW_FUSE_LAG, TLW_FUSE_LAG ? cap : (int)n_elements, list, off);
             if ((rc = up_i(h->d_fuse_list, list)) || (rc = up_i(h->d_fuse_off, off))) return rc;
             TLW_CUDA(h, cudaMalloc(&h->d_fuse_ticket, sizeof(unsigned long long)));
             TLW_CUDA(h, cudaMalloc(&h->d_fuse_ready, (size_t)h->fuse_tiles * sizeof(unsigned)));

@@ -1,4 +1,5 @@
-// tlw_fused.cuh -- the LW volume and surface passes of a conforming periodic TreeMesh in one launch.
+// tlw_fused.cuh -- the volume and surface passes of an LW step or MDRK stage on a conforming periodic TreeMesh
+// in one launch.
 //
 // The volume pass is FP64-bound and leaves HBM mostly idle; the element-centric surface pass is HBM-bound and
 // waits on the volume pass of the element and its four neighbours. lw_fused_kernel runs both in the same CTAs,
@@ -12,9 +13,11 @@
 //  - before a group it waits (acquire at GPU scope) on the flags of the group's tiles. Every tile waited on has
 //    a ticket below t, held by a CTA that is already running and publishes before any wait of its own, so the
 //    waits end; each is bounded all the same (STATUS_WAIT_LIMIT, results then invalid, no hang).
-// The counter runs on across launches: launch L's CTAs take tickets L tiles .. L tiles + tiles - 1, so the ticket
-// gives both the tile (ticket mod tiles) and the launch (ticket / tiles + 1, the value a finished tile's flag
-// holds), and no reset is needed between launches. The arithmetic of both phases is that of lw_volume_kernel and
+// Surfaces may also be scheduled a lag of tickets behind their last dependency (so that the tile has finished when
+// they start), with a tail of surface-only tickets after the tiles. The counter runs on across launches: launch L's
+// CTAs take tickets L grid .. L grid + grid - 1, so the ticket gives both the CTA's place q (ticket mod grid; a
+// volume tile when q < tiles) and the launch (ticket / grid + 1, the value a finished tile's flag holds), and no
+// reset is needed between launches. The arithmetic of both phases is that of lw_volume_kernel and
 // surface_kernel: the results equal the two-launch path's bit for bit.
 #pragma once
 #include "tlw_surface.cuh"
@@ -26,9 +29,10 @@ struct FuseArgs {
     unsigned long long* ticket;   // launch-order counter (zeroed with the flags when the mesh is set)
     unsigned* ready;              // [tiles] launch number (1-based) of the last finished volume phase of each tile
     const int* list;              // [E] elements in the order of their surface ticket
-    const int* off;               // [tiles + 1] list range of each ticket
+    const int* off;               // [grid + 1] list range of each ticket
     const int* nbr;               // [4, E] element across each face (-x, +x, -y, +y)
-    int tiles;                    // CTAs of every launch
+    int tiles;                    // volume tiles (tickets below tiles run a volume phase)
+    int grid;                     // CTAs (tickets) of every launch: the tiles and the tail of surface-only tickets
 };
 
 // iterations of a dependency wait before it gives up (about a second with the back-off below)
@@ -59,11 +63,16 @@ struct FusedCfg {
     // surface elements per group: one phase-1 thread per (element, face, node)
     static constexpr int GROUP = C::THREADS / (4 * n);
     static_assert(GROUP >= 1, "a CTA must hold one element's face nodes");
-    static_assert((size_t)GROUP * 4 * n * NV * sizeof(double) <= C::smem_bytes(4), "surface group fits the planes");
+    static constexpr size_t GROUP_BYTES = (size_t)GROUP * 4 * n * NV * sizeof(double);
+    // dynamic shared memory of a launch: the stage's planes, or the surface group if that is larger
+    static constexpr size_t smem(size_t stage_bytes) { return stage_bytes > GROUP_BYTES ? stage_bytes : GROUP_BYTES; }
 };
 
-template <int N, int MODE>
-static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOCKS)
+// STAGE: TLW_STAGE_LW (lw_volume_tile), TLW_STAGE_MDRK1 / _MDRK2 (mdrk1 / mdrk2_volume_tile; COMPACT: the plain
+// step's compact stages)
+template <int N, int MODE, int STAGE, bool COMPACT>
+static __global__ void __launch_bounds__(VolCfg<N>::THREADS,
+                                         STAGE == 0 ? VolCfg<N>::MIN_BLOCKS : VolCfg<N>::MDRK_MIN_BLOCKS)
     lw_fused_kernel(VolArgs a, SurfArgs sa, FuseArgs fa) {
     using C = VolCfg<N>;
     constexpr int EB = C::EB, GS = FusedCfg<N>::GROUP;
@@ -74,15 +83,19 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, VolCfg<N>::MIN_BLOC
     __syncthreads();
     const unsigned long long tk = *s_ticket;
     __syncthreads();
-    const int tile = (int)(tk % (unsigned long long)fa.tiles);
-    const unsigned launch = (unsigned)(tk / (unsigned long long)fa.tiles) + 1u;
-    lw_volume_tile<N, MODE, false>(a, tile);
-    __syncthreads();
-    if (tid == 0) {
-        __threadfence();
-        st_release_gpu(fa.ready + tile, launch);
+    const int q = (int)(tk % (unsigned long long)fa.grid);
+    const unsigned launch = (unsigned)(tk / (unsigned long long)fa.grid) + 1u;
+    if (q < fa.tiles) {
+        if constexpr (STAGE == 0) lw_volume_tile<N, MODE, false>(a, q);
+        else if constexpr (STAGE == 1) mdrk1_volume_tile<N, MODE, false, false, 0, false, COMPACT>(a, q);
+        else mdrk2_volume_tile<N, MODE, false, false, 0, false, COMPACT>(a, q);
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release_gpu(fa.ready + q, launch);
+        }
     }
-    const int beg = __ldg(fa.off + tile), end = __ldg(fa.off + tile + 1);
+    const int beg = __ldg(fa.off + q), end = __ldg(fa.off + q + 1);
     for (int g = beg; g < end; g += GS) {
         const int cnt = min(GS, end - g);
         if (tid < 5 * cnt) {

@@ -28,8 +28,9 @@ struct Launch {
     static void surfaces(cudaStream_t s, const SurfArgs& a, const BndArgs& b);
     // elements per CTA of the LW volume kernel (the tiles of the fused launch)
     static int volume_tile();
-    // the LW volume and surface passes of a conforming periodic TreeMesh in one launch (lw_fused_kernel)
-    static void fused(cudaStream_t s, int mode, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa);
+    // the volume and surface passes of an LW step or MDRK stage on a conforming periodic TreeMesh in one launch
+    // (lw_fused_kernel)
+    static void fused(cudaStream_t s, int stage, int mode, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa);
     static void boundaries(cudaStream_t s, const BndArgs& a);
     static void parabolic(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out,
                           const double* dtp);

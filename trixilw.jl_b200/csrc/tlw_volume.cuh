@@ -1159,9 +1159,7 @@ __device__ __forceinline__ void mdrk_stage1_sums(double gm1, const double* uu, c
 // COMPACT (the plain TreeMesh step): store only u_t (into a.U2) instead of U2 and F2; stage 2 recomputes them from
 // u^n and u_t with this kernel's operations (64 instead of 192 bytes a node between the stages).
 template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
-static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
-                                                                         : VolCfg<N>::MDRK_MIN_BLOCKS)
-    mdrk1_volume_kernel(VolArgs a) {
+__device__ __forceinline__ void mdrk1_volume_tile(const VolArgs& a, const int tile) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     static_assert(!SRC || !SC, "source terms: the FR volume integral");
     static_assert(!COMPACT || (!SC && !CURVED && !SRC && MODE == MODE_STEP), "compact stages: the plain TreeMesh step");
@@ -1182,7 +1180,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
-    const int e = blockIdx.x * EB + el;
+    const int e = tile * EB + el;
     const bool active = el < EB && e < a.E;
     double alpha_e = 0.0;
     bool blended = false, muscl = false;
@@ -1310,6 +1308,14 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
     }
 }
 
+template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
+static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
+                                                                         : VolCfg<N>::MDRK_MIN_BLOCKS)
+    mdrk1_volume_kernel(VolArgs a) {
+    mdrk1_volume_tile<N, MODE, SC, CURVED, REC, SRC, COMPACT>(a, blockIdx.x);
+
+}
+
 // ------------------------------------------------------------------------------------------------
 // MDRK stage 2 (mdrk_kernel_2!, multi_derivative_2d.jl:423-555): at u* = a.u,
 // F = F2 + f_t(u*)/3, U = U2 + u*_t/3.
@@ -1320,9 +1326,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
 // COMPACT: F2, G2, U2 recomputed from u^n (a.u_base) and stage 1's u_t (a.U2) at the start, parked in shared memory
 // (three more planes) until the stage's own sums are formed.
 template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
-static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
-                                                                         : VolCfg<N>::MDRK_MIN_BLOCKS)
-    mdrk2_volume_kernel(VolArgs a) {
+__device__ __forceinline__ void mdrk2_volume_tile(const VolArgs& a, const int tile) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     static_assert(!SRC || !SC, "source terms: the FR volume integral");
     static_assert(!COMPACT || (!SC && !CURVED && !SRC && MODE == MODE_STEP), "compact stages: the plain TreeMesh step");
@@ -1343,7 +1347,7 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
-    const int e = blockIdx.x * EB + el;
+    const int e = tile * EB + el;
     const bool active = el < EB && e < a.E;
     double alpha_e = 0.0;
     bool blended = false, muscl = false;
@@ -1476,7 +1480,15 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o, SRC ? Ssrc : nullptr);
         if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) node_speeds(a.gamma, o, a.status, l1, l2);
     }
-    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, blockIdx.x * EB, l1, l2);
+    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, tile * EB, l1, l2);
+}
+
+template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
+static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
+                                                                         : VolCfg<N>::MDRK_MIN_BLOCKS)
+    mdrk2_volume_kernel(VolArgs a) {
+    mdrk2_volume_tile<N, MODE, SC, CURVED, REC, SRC, COMPACT>(a, blockIdx.x);
+
 }
 
 }  // namespace tlw
