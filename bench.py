@@ -526,26 +526,6 @@ def run_ours(args):
     # per-phase device time of K further steps (events between the kernels of each step)
     phase = (ctypes.c_double * 5)()
     _lib.check(semi.handle, L.tlw_step_timed(semi.handle, args.steps, cfl, 0.0, 1e9, phase))
-    # an LW step or MDRK stage on a periodic conforming TreeMesh runs the volume and surface passes in one launch
-    # (lw_fused_kernel); the same K steps in the two-launch path, for comparison
-    fused = (int(L.tlw_set_fused_step(semi.handle, 2)) & 3) == 3 and icname not in ("riemann", "blast", "warped",
-                                                                                       "cavity")
-    two_launch = None
-    if fused:
-        L.tlw_set_fused_step(semi.handle, 0)
-        integ.step(2, cfl)
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        integ.step(args.steps, cfl)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        ph2 = (ctypes.c_double * 5)()
-        _lib.check(semi.handle, L.tlw_step_timed(semi.handle, args.steps, cfl, 0.0, 1e9, ph2))
-        L.tlw_set_fused_step(semi.handle, 1)
-        two_launch = {"ms_per_step": ev0.elapsed_time(ev1) / args.steps,
-                      "phase_ms_per_step": {"cfl_dt": ph2[0] / args.steps, "volume": ph2[1] / args.steps,
-                                            "surfaces": (ph2[2] + ph2[3]) / args.steps,
-                                            "step": ph2[4] / args.steps}}
     clocks = sampler.stop()
     ms_max = ms
     if world > 1:
@@ -609,15 +589,12 @@ def run_ours(args):
         plain_mdrk = td == "mdrk" and not (ns or sc or curved)
         vol_bytes = (ns_volume_bytes_per_element(N) if ns else mdrk_volume_bytes_per_element(N) if plain_mdrk
                      else volume_kernel_bytes_per_element(N, td, curved, sc)) * E
-        if fused:   # the fused launches also move the surface passes' bytes
-            vol_bytes += (2 if td == "mdrk" else 1) * surface_pass_bytes_per_element(N) * E
         achieved = vol_bytes / (vol_ms * 1e-3) / 1e9
         fp = ctypes.c_double()
         fp64_peak = fp.value if L.tlw_probe_fp64_tflops(local_rank, ctypes.byref(fp)) == 0 else None
         vol_flops = (None if (ns or sc) else mdrk_volume_flops_per_node(N) * ndofs if plain_mdrk
                      else volume_flops_per_node(N) * ndofs)
         tag = (f"par_volume_kernel_N{N}_cavity{1 << level}" if ns
-               else f"lw_fused_kernel_N{N}_tree{1 << level}" if fused
                else f"lw_volume_kernel_N{N}_blast_muscl{1 << level}" if icname == "blast"
                else f"lw_volume_kernel_N{N}_{'warped' if curved else 'tree'}{1 << level}")
         traffic = profile_traffic(tag)
@@ -644,10 +621,7 @@ def run_ours(args):
         phases_rec = {"cfl_dt": phase[0] / args.steps, "volume": phase[1] / args.steps, "surfaces": surf_ms,
                       "step": phase[4] / args.steps}
         surf_rec = None
-        if fused:
-            phases_rec = {"cfl_dt": phase[0] / args.steps, "volume_and_surfaces": phase[1] / args.steps,
-                          "step": phase[4] / args.steps}
-        elif surf_pass:
+        if surf_pass:
             sb = surface_pass_bytes_per_element(N) * E
             sgbs = sb / (surf_ms / stages * 1e-3) / 1e9
             surf_rec = {"kernel": f"surface_kernel<{N}>", "ms_per_launch": surf_ms / stages,
@@ -665,9 +639,7 @@ def run_ours(args):
                     "round_trip": {"value": e2e_rt, "unit": UNIT,
                                    "api": "tlw_set_state + tlw_step + tlw_get_state (synchronous, serial copies)"}},
             "roofline": {"kernel": (f"grad_volume_kernel + curved_grad_*_kernel + par_volume_kernel<{N}, MODE_STEP, CURVED>"
-                                    if ns else (f"lw_fused_kernel<{N}, MODE_STEP, {'MDRK stages 1 and 2' if td == 'mdrk' else 'LW'}>"
-                                                " (volume and surface passes)") if fused
-                                    else f"lw_volume_kernel<{N}, MODE_STEP, SC, CURVED, MUSCL>" if icname == "blast"
+                                    if ns else f"lw_volume_kernel<{N}, MODE_STEP, SC, CURVED, MUSCL>" if icname == "blast"
                                     else f"lw_volume_kernel<{N}, MODE_STEP{', SC' if sc else ''}{', CURVED' if curved else ''}>"),
                          "bound": "fp64" if fp64_bound else "hbm",
                          "achieved": binding["achieved"], "peak": binding["peak"], "unit": binding["unit"],
@@ -679,12 +651,11 @@ def run_ours(args):
                                   "achieved_gbs": step_alg * args.steps / (ms_max * 1e-3) / 1e9,
                                   "frac": step_alg * args.steps / (ms_max * 1e-3) / 1e9 / peak},
                          "phase_ms_per_step": phases_rec,
-                         **({"surface": surf_rec} if surf_rec else {}),
-                         **({"two_launch_path": two_launch} if two_launch else {})},
+                         **({"surface": surf_rec} if surf_rec else {})},
             "clocks": clocks,
             "gpu_launches": args.steps * ((9 + 2 * int(L.tlw_curved_colors(semi.handle))) if ns else
                                           (5 + int(L.tlw_curved_colors(semi.handle))) if icname == "blast" else
-                                          (2 + stages if fused else 2 + 2 * stages + (1 if icname == "riemann" else 0))),
+                                          (2 + 2 * stages + (1 if icname == "riemann" else 0))),
         }
         if world == 1 and not args.no_cpu_baseline:
             rate, threads, nsteps, el = cpu_oracle_rate(level, N, td, icname, steps_hint=args.steps)

@@ -374,13 +374,6 @@ int64_t tlw_cache_size(tlw_handle* h, int32_t item);
 int tlw_synchronize(tlw_handle* h);
 /* The handle's cudaStream_t (for event timing / interop). */
 int tlw_get_stream(tlw_handle* h, void** stream);
-/* LW stages on a periodic conforming TreeMesh (FR volume integral, no source terms) run the volume and surface
- * passes of rhs! (src/solvers/dgsem_tree/dg_2d.jl:28-83: calc_volume_integral!, prolong2interfaces!,
- * calc_interface_flux!, calc_surface_integral!, apply_jacobian!) in one launch by default; enable = 0 selects the
- * two-launch path (same results, bit for bit), enable = 1 the fused launch, any other value changes nothing.
- * Returns the setting in effect before the call (0 or 1), plus 2 when the handle's mesh is one the fused launch
- * applies to (a periodic conforming TreeMesh); -1 without a handle. */
-int32_t tlw_set_fused_step(tlw_handle* h, int32_t enable);
 /* Device address of the current state (valid until the next tlw_step / tlw_set_tree_mesh). */
 int tlw_state_pointer(tlw_handle* h, double** dptr);
 const char* tlw_last_error(tlw_handle* h);

@@ -20,7 +20,7 @@ SOURCES = ["tlw_capi.cu", "tlw_noalloc.cu", "tlw_batch.cu", "tlw_adjoint.cu"]
 DEGREES = range(1, 8)
 HEADERS = ["tlw_device.cuh", "tlw_volume.cuh", "tlw_surface.cuh", "tlw_basis.h", "tlw_handle.h", "tlw_curved.cuh",
            "tlw_mortar.cuh", "tlw_parabolic.cuh", "tlw_limiter.cuh", "tlw_halo.cuh", "tlw_curved_mortar.cuh",
-           "tlw_launch.cuh", "tlw_launch.cu", "tlw_fused.cuh"]
+           "tlw_launch.cuh", "tlw_launch.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC"]
 

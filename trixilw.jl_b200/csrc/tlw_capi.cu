@@ -55,8 +55,6 @@ void free_mesh(tlw_handle* h) {
     drop_graphs(h);
     dfree(h->d_inv_jac);
     dfree(h->d_xl); dfree(h->d_xr); dfree(h->d_yl); dfree(h->d_yr); dfree(h->d_nbr);
-    dfree(h->d_fuse_list); dfree(h->d_fuse_off); dfree(h->d_fuse_ticket); dfree(h->d_fuse_ready);
-    h->fuse_tiles = h->fuse_grid = 0;
     dfree(h->d_xnode); dfree(h->d_S2);
     h->source = 0;
     dfree(h->d_b_elem); dfree(h->d_b_dir); dfree(h->d_bx); dfree(h->d_by);
@@ -124,13 +122,6 @@ void dispatch(int N, A&&... args) {
     }
 }
 template <int N> struct SetAttr { static void run() { Launch<N>::set_attributes(); } };
-template <int N> struct Tile { static void run(int& eb) { eb = Launch<N>::volume_tile(); } };
-template <int N> struct Group { static void run(int& g) { g = FusedCfg<N>::GROUP; } };
-template <int N> struct Fused {
-    static void run(cudaStream_t s, int stage, int mode, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa) {
-        Launch<N>::fused(s, stage, mode, va, sa, fa);
-    }
-};
 template <int N> struct Vol {
     static void run(cudaStream_t s, int st, int m, bool sc, const VolArgs& a) { Launch<N>::volume(s, st, m, sc, a); }
 };
@@ -214,56 +205,14 @@ bool use_slots(const tlw_handle* h) {
 #ifndef TLW_MDRK_COMPACT
 #define TLW_MDRK_COMPACT 1
 #endif
-// (not with shock capturing: the blended variant needs 142 registers and measured slower than the sweeps on the
-// 512^2 Riemann problem, 0.376 against about 0.34 ms)
+// (not with shock capturing: on the 512^2 Riemann problem the blended variant's steps took 1.099 ms at 142
+// registers (one CTA per SM's worth) and 1.029 ms capped at 96 registers, against 0.993 ms with the sweeps)
 #ifndef TLW_SURFACE_PASS_SC
 #define TLW_SURFACE_PASS_SC 0
 #endif
 bool use_surface_pass(const tlw_handle* h) {
     return TLW_SURFACE_PASS && h->d_nbr && !h->curved && (!h->sc || TLW_SURFACE_PASS_SC) && h->nmx + h->nmy == 0 &&
            h->nh == 0;
-}
-
-// the volume and surface passes of an LW step or an MDRK stage in one launch (lw_fused_kernel): a periodic
-// conforming TreeMesh with the FR volume integral and nothing else on its faces or in its volume
-#ifndef TLW_FUSED_STEP
-#define TLW_FUSED_STEP 1
-#endif
-bool use_fused(const tlw_handle* h, int stage, int phases) {
-    return TLW_FUSED_STEP && h->fuse_enabled && h->fuse_tiles > 0 && phases == 7 && use_surface_pass(h) && !h->sc &&
-           !h->parabolic && !h->source && !h->te_request && h->nb == 0;
-}
-
-// the fused launch's surface lists: element s depends on the volume phases of its own and its four neighbours'
-// tiles (tile = element / eb) and is ready after the last of them, r(s). Tickets take the ready elements in order
-// of r, at most cap a ticket, each no earlier than lag tickets after its r (tickets at or past the last tile take
-// any); the tickets past the last tile form the surface-only tail. Returns the tickets of a launch.
-#ifndef TLW_FUSE_LAG
-#define TLW_FUSE_LAG 0
-#endif
-int fuse_lists(const std::vector<int>& nbr, int64_t E, int eb, int lag, int cap, std::vector<int>& list,
-               std::vector<int>& off) {
-    const int tiles = (int)((E + eb - 1) / eb);
-    std::vector<int> r((size_t)E), cnt((size_t)tiles + 1, 0);
-    for (int64_t e = 0; e < E; ++e) {
-        int t = (int)(e / eb);
-        for (int f = 0; f < 4; ++f) t = std::max(t, nbr[(size_t)4 * e + f] / eb);
-        r[(size_t)e] = t;
-        ++cnt[(size_t)t + 1];
-    }
-    for (int t = 0; t < tiles; ++t) cnt[(size_t)t + 1] += cnt[(size_t)t];
-    list.assign((size_t)E, 0);
-    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
-    for (int64_t e = 0; e < E; ++e) list[(size_t)fill[(size_t)r[(size_t)e]]++] = (int)e;
-    // list is sorted by r; ticket q takes up to cap of the next elements with r + lag <= q (any once q >= tiles)
-    off.assign(1, 0);
-    int64_t p = 0;
-    for (int q = 0; p < E || q < tiles; ++q) {
-        int k = 0;
-        while (p < E && k < cap && (q >= tiles || r[(size_t)list[(size_t)p]] + lag <= q)) { ++p; ++k; }
-        off.push_back((int)p);
-    }
-    return (int)off.size() - 1;
 }
 
 // the halo faces of one class (cls 0: x, 1: y) as kernel arguments
@@ -554,34 +503,6 @@ void enqueue_rhs(tlw_handle* h, int stage, int mode, const double* u_flux, const
             va.reconstruction = h->reconstruction;
         }
     }
-    if (use_fused(h, stage, phases)) {
-        SurfArgs sa{};
-        sa.u = u_jump;
-        sa.out = out;
-        sa.tU = h->d_tU;
-        sa.tF = h->d_tF;
-        sa.inv_jac = h->d_inv_jac;
-        sa.dt = dt_ptr;
-        sa.step_mode = mode == MODE_STEP;
-        sa.gamma = h->opts.gamma;
-        sa.flux_kind = h->opts.surface_flux;
-        sa.speed_kind = h->opts.max_speed;
-        sa.inv_w_first = h->h_basis.inv_w_first;
-        sa.inv_w_last = h->h_basis.inv_w_last;
-        sa.status = &h->d_step->status;
-        sa.cfl_slots = va.cfl_slots;
-        sa.nbr = h->d_nbr;
-        sa.E = (int)h->E;
-        FuseArgs fa{h->d_fuse_ticket, h->d_fuse_ready, h->d_fuse_list, h->d_fuse_off, h->d_nbr, h->fuse_tiles,
-                    h->fuse_grid};
-        dispatch<Fused>(h->N, h->stream, stage, mode, va, sa, fa);
-        if (ev) {
-            cudaEventRecord(ev->after_volume, h->stream);
-            cudaEventRecord(ev->after_x, h->stream);
-            cudaEventRecord(ev->after_y, h->stream);
-        }
-        return;
-    }
     if (phases & 1) {
         dispatch<Vol>(h->N, h->stream, stage, mode, h->sc, va);
         if (ev) cudaEventRecord(ev->after_volume, h->stream);
@@ -752,8 +673,6 @@ int read_status(tlw_handle* h) {
     if (st) {
         const unsigned zero = 0;
         TLW_CUDA(h, upload_on(h->stream, &h->d_step->status, &zero, sizeof(zero)));
-        if (st & STATUS_WAIT_LIMIT)
-            return fail(h, TLW_E_CUDA, "fused launch: a dependency wait gave up (results of the call are invalid)");
         return fail(h, TLW_E_NONADMISSIBLE, "non-admissible state: square root of a negative number (DomainError)");
     }
     return TLW_OK;
@@ -915,20 +834,6 @@ int tlw_set_tree_mesh(tlw_handle* h, int64_t n_elements, const double* inverse_j
         for (size_t k = 0; k < yl.size(); ++k) { put(yl[k], 3, yr[k]); put(yr[k], 2, yl[k]); }
         for (size_t k = 0; k < belem.size(); ++k) put(belem[k], bdir[k] - 1, -(int)k - 1);
         if (ok && (rc = up_i(h->d_nbr, nbr))) return rc;
-        if (ok && n_boundaries == 0) {
-            int eb = 0;
-            dispatch<Tile>(h->N, eb);
-            std::vector<int> list, off;
-            int cap = 0;
-            dispatch<Group>(h->N, cap);
-            h->fuse_tiles = (int)((n_elements + eb - 1) / eb);
-            h->fuse_grid = fuse_lists(nbr, n_elements, eb, TLW_FUSE_LAG, TLW_FUSE_LAG ? cap : (int)n_elements, list, off);
-            if ((rc = up_i(h->d_fuse_list, list)) || (rc = up_i(h->d_fuse_off, off))) return rc;
-            TLW_CUDA(h, cudaMalloc(&h->d_fuse_ticket, sizeof(unsigned long long)));
-            TLW_CUDA(h, cudaMalloc(&h->d_fuse_ready, (size_t)h->fuse_tiles * sizeof(unsigned)));
-            TLW_CUDA(h, zero_on(h->stream, h->d_fuse_ticket, sizeof(unsigned long long)));
-            TLW_CUDA(h, zero_on(h->stream, h->d_fuse_ready, (size_t)h->fuse_tiles * sizeof(unsigned)));
-        }
     }
     h->jac_first = inverse_jacobian[0];
     if (h->sc) {
@@ -2278,16 +2183,6 @@ int tlw_get_stream(tlw_handle* h, void** stream) {
     if (!h || !stream) return TLW_E_ARG;
     *stream = (void*)h->stream;
     return TLW_OK;
-}
-
-int32_t tlw_set_fused_step(tlw_handle* h, int32_t enable) {
-    if (!h) return -1;
-    const int32_t was = (h->fuse_enabled ? 1 : 0) | (h->fuse_tiles > 0 ? 2 : 0);
-    if ((enable == 0 || enable == 1) && (enable == 1) != h->fuse_enabled) {
-        h->fuse_enabled = enable == 1;
-        drop_graphs(h);   // captured steps hold the other path
-    }
-    return was;
 }
 
 int tlw_state_pointer(tlw_handle* h, double** dptr) {

@@ -9,7 +9,6 @@ constexpr int NV = 4;   // compressible Euler 2D: rho, rho v1, rho v2, rho e
 
 // status bits written by kernels (never a trap): the host maps them to TLW_E_* codes
 constexpr unsigned STATUS_NONADMISSIBLE = 1u;   // sqrt of a negative number (reference: DomainError)
-constexpr unsigned STATUS_WAIT_LIMIT = 2u;      // a bounded wait on another CTA's flag gave up (results invalid)
 
 struct Basis {
     double D[16 * 16];      // derivative matrix, D[a*n + b] = l_b'(x_a)
@@ -195,12 +194,6 @@ __device__ __forceinline__ void load4(const double* __restrict__ p, double* x) {
 __device__ __forceinline__ void load4_rw(const double* p, double* x) {
     const double2 a = *reinterpret_cast<const double2*>(p);
     const double2 b = *(reinterpret_cast<const double2*>(p) + 1);
-    x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
-}
-// through L2 only (ld.global.cg): data that other CTAs of the running launch wrote
-__device__ __forceinline__ void load4_cg(const double* p, double* x) {
-    const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
-    const double2 b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
     x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
 }
 __device__ __forceinline__ void store4(double* p, const double* x) {

@@ -91,14 +91,6 @@ struct tlw_handle {
     double* d_inv_jac = nullptr;
     int *d_xl = nullptr, *d_xr = nullptr, *d_yl = nullptr, *d_yr = nullptr;
     int* d_nbr = nullptr;   // [4, E] element across each face when every face is a conforming interface
-    // the fused LW launch (periodic conforming TreeMesh): its tiles, surface lists and dependency flags
-    int fuse_tiles = 0;                       // volume tiles
-    int fuse_grid = 0;                        // tickets (CTAs) of a launch: tiles plus the surface-only tail
-    bool fuse_enabled = true;
-    int* d_fuse_list = nullptr;               // [E] elements in the order of their surface ticket
-    int* d_fuse_off = nullptr;                // [tiles + 1]
-    unsigned long long* d_fuse_ticket = nullptr;
-    unsigned* d_fuse_ready = nullptr;         // [tiles]
     // source terms (TreeMesh, FR volume integral): kind, node coordinates [2, i, j, e], MDRK stage 1's S2
     int source = 0;
     double* d_xnode = nullptr;

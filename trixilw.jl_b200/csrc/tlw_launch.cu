@@ -34,7 +34,6 @@ struct LaunchImpl {
         set_attr_sc<false>();
         set_attr_sc<true>();
         const int lw = (int)C::smem_bytes(4);
-        fused_attributes();
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_RHS, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
         te_volume(nullptr, VolArgs{}, 0, false, true);
         cudaFuncSetAttribute(lw_volume_kernel<N, MODE_STEP, false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lw);
@@ -207,46 +206,6 @@ struct LaunchImpl {
             else surface_kernel<N, false, false><<<grid, C::THREADS, 0, s>>>(a, b);
         }
     }
-    // shared memory of each fused variant (the stage kernel's, or the surface group's if larger)
-    static size_t fused_smem(int stage, bool compact) {
-        using FC = FusedCfg<N>;
-        return FC::smem(stage == TLW_STAGE_LW ? C::smem_bytes(4) : stage == TLW_STAGE_MDRK2 && compact ? C::smem_bytes(5)
-                                                                                                    : C::smem_bytes(2));
-    }
-    template <int MODE, int STAGE, bool COMPACT>
-    static void fused_go(cudaStream_t s, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa, bool attr_only) {
-        const size_t sm = fused_smem(STAGE, COMPACT);
-        if (attr_only)
-            cudaFuncSetAttribute(lw_fused_kernel<N, MODE, STAGE, COMPACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sm);
-        else lw_fused_kernel<N, MODE, STAGE, COMPACT><<<fa.grid, C::THREADS, sm, s>>>(va, sa, fa);
-    }
-    static void fused_run(cudaStream_t s, int stage, int mode, const VolArgs& va, const SurfArgs& sa,
-                          const FuseArgs& fa, bool attr_only) {
-        if (!attr_only && fa.grid <= 0) return;
-        const bool compact = va.compact != 0;
-        if (stage == TLW_STAGE_LW) {
-            if (mode == MODE_RHS) fused_go<MODE_RHS, TLW_STAGE_LW, false>(s, va, sa, fa, attr_only);
-            else fused_go<MODE_STEP, TLW_STAGE_LW, false>(s, va, sa, fa, attr_only);
-        } else if (stage == TLW_STAGE_MDRK1) {
-            if (mode == MODE_RHS) fused_go<MODE_RHS, TLW_STAGE_MDRK1, false>(s, va, sa, fa, attr_only);
-            else if (compact) fused_go<MODE_STEP, TLW_STAGE_MDRK1, true>(s, va, sa, fa, attr_only);
-            else fused_go<MODE_STEP, TLW_STAGE_MDRK1, false>(s, va, sa, fa, attr_only);
-        } else {
-            if (mode == MODE_RHS) fused_go<MODE_RHS, TLW_STAGE_MDRK2, false>(s, va, sa, fa, attr_only);
-            else if (compact) fused_go<MODE_STEP, TLW_STAGE_MDRK2, true>(s, va, sa, fa, attr_only);
-            else fused_go<MODE_STEP, TLW_STAGE_MDRK2, false>(s, va, sa, fa, attr_only);
-        }
-    }
-    static void fused_attributes() {
-        VolArgs va{};
-        for (int stage : {TLW_STAGE_LW, TLW_STAGE_MDRK1, TLW_STAGE_MDRK2})
-            for (int mode : {MODE_RHS, MODE_STEP})
-                for (int compact = 0; compact < 2; ++compact) {
-                    va.compact = compact;
-                    fused_run(nullptr, stage, mode, va, SurfArgs{}, FuseArgs{}, true);
-                }
-    }
     static void parabolic(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out,
                           const double* dtp) {
         if constexpr (N >= 3) {
@@ -387,11 +346,6 @@ template <int N> void Launch<N>::volume(cudaStream_t s, int stage, int mode, boo
     LaunchImpl<N>::volume(s, stage, mode, sc, a);
 }
 template <int N> void Launch<N>::interfaces(cudaStream_t s, const SurfArgs& a) { LaunchImpl<N>::interfaces(s, a); }
-template <int N> int Launch<N>::volume_tile() { return VolCfg<N>::EB; }
-template <int N>
-void Launch<N>::fused(cudaStream_t s, int stage, int mode, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa) {
-    LaunchImpl<N>::fused_run(s, stage, mode, va, sa, fa, false);
-}
 template <int N> void Launch<N>::surfaces(cudaStream_t s, const SurfArgs& a, const BndArgs& b) {
     LaunchImpl<N>::surfaces(s, a, b);
 }

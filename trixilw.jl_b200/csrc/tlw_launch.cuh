@@ -5,7 +5,6 @@
 
 #include "tlw_curved.cuh"
 #include "tlw_curved_mortar.cuh"
-#include "tlw_fused.cuh"
 #include "tlw_halo.cuh"
 #include "tlw_handle.h"
 #include "tlw_limiter.cuh"
@@ -26,11 +25,6 @@ struct Launch {
     static void interfaces(cudaStream_t s, const SurfArgs& a);
     // all faces of a mesh whose every face is a conforming interface or a boundary, one pass over the elements
     static void surfaces(cudaStream_t s, const SurfArgs& a, const BndArgs& b);
-    // elements per CTA of the LW volume kernel (the tiles of the fused launch)
-    static int volume_tile();
-    // the volume and surface passes of an LW step or MDRK stage on a conforming periodic TreeMesh in one launch
-    // (lw_fused_kernel)
-    static void fused(cudaStream_t s, int stage, int mode, const VolArgs& va, const SurfArgs& sa, const FuseArgs& fa);
     static void boundaries(cudaStream_t s, const BndArgs& a);
     static void parabolic(cudaStream_t s, const tlw_handle* h, int mode, const double* u, double* out,
                           const double* dtp);

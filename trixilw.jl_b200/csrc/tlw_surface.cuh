@@ -103,7 +103,7 @@ __device__ __forceinline__ void blend_interface_flux(const SurfArgs& a, int orie
 
 // The LW flux at node l of the interface (le, re) of one orientation, with the blending and the viscous
 // flux where they apply: calc_interface_flux! (dg_2d.jl:1903-1946) at one node.
-template <int N, bool SC = true, bool COH = false>
+template <int N, bool SC = true>
 __device__ __forceinline__ void interface_node_flux(const SurfArgs& a, int orientation, int le, int re, int l,
                                                     double dt, double* Fn) {
     constexpr int n = N + 1;
@@ -113,15 +113,10 @@ __device__ __forceinline__ void interface_node_flux(const SurfArgs& a, int orien
     double uL[NV], uR[NV], UL[NV], UR[NV], FL[NV], FR[NV];
     load4(a.u + ((size_t)le * n * n + nodeL) * NV, uL);
     load4(a.u + ((size_t)re * n * n + nodeR) * NV, uR);
-    // (COH: traces written by other CTAs of the running launch, read through L2)
-    auto trace = [&](const double* p, double* x) {
-        if (COH) load4_cg(p, x);
-        else load4(p, x);
-    };
-    trace(a.tU + (((size_t)le * 4 + faceL) * n + l) * NV, UL);
-    trace(a.tU + (((size_t)re * 4 + faceR) * n + l) * NV, UR);
-    trace(a.tF + (((size_t)le * 4 + faceL) * n + l) * NV, FL);
-    trace(a.tF + (((size_t)re * 4 + faceR) * n + l) * NV, FR);
+    load4(a.tU + (((size_t)le * 4 + faceL) * n + l) * NV, UL);
+    load4(a.tU + (((size_t)re * 4 + faceR) * n + l) * NV, UR);
+    load4(a.tF + (((size_t)le * 4 + faceL) * n + l) * NV, FL);
+    load4(a.tF + (((size_t)re * 4 + faceR) * n + l) * NV, FR);
     // TreeMesh argument order: surface_flux(f_ll, f_rr, U_ll, U_rr, u_ll, u_rr) (dg_2d.jl:1928)
     lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, FL, FR, UL, UR, uL, uR, orientation, Fn, a.status);
     if (SC && a.shock_capturing) blend_interface_flux<N>(a, orientation, le, re, faceL, faceR, l, uL, uR, dt, Fn);
@@ -332,18 +327,17 @@ template <int N> struct SurfCfg {
 #ifndef TLW_SURF_MINB_SC
 #define TLW_SURF_MINB_SC 1
 #endif
-// One group of up to EBG elements; element el of the group is ids[el] (ids given) or first + el, for el < count.
-// The caller's threads: EBG 4n of them for phase 1, EBG NB for phase 2, whole warps (the face-node maxima are reduced
-// by warp shuffles over full masks); sF holds EBG 4n NV doubles. COH: the traces and the output are read through L2
-// (ld.global.cg), for a caller whose other CTAs wrote them during the same launch.
-template <int N, bool BND, bool SC, bool COH, int EBG>
-__device__ __forceinline__ void surface_group(const SurfArgs& a, const BndArgs& bnd, double* sF, const int tid,
-                                              const int first, const int* ids, const int count) {
-    constexpr int n = N + 1, NB = 4 * (n - 1);
+template <int N, bool BND, bool SC>
+static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? TLW_SURF_MINB_SC : SurfCfg<N>::MIN_BLOCKS)
+    surface_kernel(SurfArgs a, BndArgs bnd) {
+    using C = SurfCfg<N>;
+    constexpr int n = N + 1, EB = C::EB, NB = 4 * (n - 1);
+    __shared__ double sF[EB * 4 * n * NV];
+    const int tid = threadIdx.x;
+    const int e0 = blockIdx.x * EB;
     // phase-2 thread: element el2, boundary node b (bottom row, top row, left column, right column)
-    const int el2 = tid / NB, b = tid - el2 * NB;
-    const bool has2 = el2 < EBG && el2 < count;
-    const int e2 = ids ? (has2 ? __ldg(ids + el2) : 0) : first + el2;
+    const int el2 = tid / NB, b = tid - el2 * NB, e2 = e0 + el2;
+    const bool has2 = el2 < EB && e2 < a.E;
     int i2, j2;
     if (b < n) { i2 = b; j2 = 0; }
     else if (b < 2 * n) { i2 = b - n; j2 = n - 1; }
@@ -351,21 +345,15 @@ __device__ __forceinline__ void surface_group(const SurfArgs& a, const BndArgs& 
     else { i2 = n - 1; j2 = b - 3 * n + 3; }
     double* o2 = a.out + ((size_t)e2 * n * n + i2 + n * j2) * NV;
     double x[NV];
-    auto load_out = [&]() {
-        if (COH) load4_cg(o2, x);
-        else load4_rw(o2, x);
-    };
-    if (TLW_SURF_PREFETCH && has2) load_out();
+    if (TLW_SURF_PREFETCH && has2) load4_rw(o2, x);
     {
-        const int el = tid / (4 * n), r = tid - el * 4 * n, f = r / n, l = r - f * n;
-        if (el < EBG && el < count) {
-            const int e = ids ? __ldg(ids + el) : first + el;
+        const int el = tid / (4 * n), r = tid - el * 4 * n, f = r / n, l = r - f * n, e = e0 + el;
+        if (el < EB && e < a.E) {
             const double dt = a.inst ? a.dt[__ldg(a.inst + e)] : *a.dt;   // (batched form: the instance's dt)
             const int nb = __ldg(a.nbr + 4 * e + f);
             const bool plus = f & 1;   // this element is the interface's left (lower) element
             double Fn[NV];
-            if (!BND || nb >= 0)
-                interface_node_flux<N, SC, COH>(a, f < 2 ? 1 : 2, plus ? e : nb, plus ? nb : e, l, dt, Fn);
+            if (!BND || nb >= 0) interface_node_flux<N, SC>(a, f < 2 ? 1 : 2, plus ? e : nb, plus ? nb : e, l, dt, Fn);
             else boundary_node_flux<N>(bnd, -nb - 1, e, f + 1, l, Fn);
 #pragma unroll
             for (int v = 0; v < NV; ++v) sF[tid * NV + v] = Fn[v];
@@ -374,7 +362,7 @@ __device__ __forceinline__ void surface_group(const SurfArgs& a, const BndArgs& 
     __syncthreads();
     double l1 = 0.0, l2 = 0.0;
     if (has2) {
-        if (!TLW_SURF_PREFETCH) load_out();
+        if (!TLW_SURF_PREFETCH) load4_rw(o2, x);
         const double dt = a.inst ? a.dt[__ldg(a.inst + e2)] : *a.dt;
         const double dts = a.step_mode ? dt : 1.0;
         const double ij = __ldg(a.inv_jac + e2);
@@ -410,26 +398,17 @@ __device__ __forceinline__ void surface_group(const SurfArgs& a, const BndArgs& 
         __syncthreads();
         if (has2) {
             sF[tid] = l1;
-            sF[EBG * NB + tid] = l2;
+            sF[EB * NB + tid] = l2;
         }
         __syncthreads();
         if (has2 && b < 2) {
-            const double* p = sF + b * EBG * NB + el2 * NB;
+            const double* p = sF + b * EB * NB + el2 * NB;
             double m = 0.0;
 #pragma unroll
             for (int k = 0; k < NB; ++k) m = fmax(m, p[k]);
             a.cfl_slots[(size_t)e2 * CFL_SLOTS + 2 + b] = (unsigned long long)__double_as_longlong(m);
         }
     }
-}
-
-template <int N, bool BND, bool SC>
-static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? TLW_SURF_MINB_SC : SurfCfg<N>::MIN_BLOCKS)
-    surface_kernel(SurfArgs a, BndArgs bnd) {
-    using C = SurfCfg<N>;
-    __shared__ double sF[C::EB * 4 * (N + 1) * NV];
-    const int e0 = blockIdx.x * C::EB;
-    surface_group<N, BND, SC, false, C::EB>(a, bnd, sF, threadIdx.x, e0, nullptr, min(C::EB, a.E - e0));
 }
 
 

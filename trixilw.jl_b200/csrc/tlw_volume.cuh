@@ -641,7 +641,7 @@ __device__ __forceinline__ void src_tttt_N4(const SrcNode& q, double* o) {
 // Every thread of the CTA calls it (barriers inside).
 template <int N, class C>
 __device__ __forceinline__ void write_interior_slots(const VolArgs& a, double* X, bool active, int el, int i, int j,
-                                                     int tid, int e0, double l1, double l2) {
+                                                     int tid, double l1, double l2) {
     constexpr int n = C::n, EB = C::EB;
     __syncthreads();
     if (active) {
@@ -649,7 +649,7 @@ __device__ __forceinline__ void write_interior_slots(const VolArgs& a, double* X
         X[(EB + el) * C::P + i + C::R * j] = l2;
     }
     __syncthreads();
-    const int ee = e0 + (tid >> 1);
+    const int ee = blockIdx.x * EB + (tid >> 1);
     if (tid < 2 * EB && ee < a.E) {
         const double* p = X + ((tid & 1) * EB + (tid >> 1)) * C::P;
         double m = 0.0;
@@ -706,10 +706,12 @@ __device__ __forceinline__ void store_stage_derivative(const VolArgs& a, int m, 
 // derivative (dt s_k) before the perturbed states move, and S enters the update unscaled by J^{-1}. The curvilinear
 // kernel of depth 4 takes the 5-point s_tt (calc_source_tt_N4, dgsem_structured/dg_2d.jl:1886) where the TreeMesh
 // one takes the 3-point calc_source_tt_N23 (dgsem_tree/dg_2d.jl:1093-1104).
-// lw_volume_tile: the elements [tile EB, tile EB + EB) of one CTA (lw_volume_kernel: tile = blockIdx.x).
 template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false, int REC = 0,
           bool SRC = false>
-__device__ __forceinline__ void lw_volume_tile(const VolArgs& a, const int tile) {
+static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED) ? VolCfg<N, EBX>::SC_CURVED_MIN_BLOCKS
+                                                                  : SRC ? VolCfg<N, EBX>::MDRK_MIN_BLOCKS - 1
+                                                                        : VolCfg<N, EBX>::MIN_BLOCKS)
+    lw_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     static_assert(!SRC || (!SC && !TE && !DSTORE), "source terms: the FR volume integral, without the error estimate");
     // the temporal error estimate of the Adaptive step control: the TreeMesh computes it at depth 4 only
@@ -739,7 +741,7 @@ __device__ __forceinline__ void lw_volume_tile(const VolArgs& a, const int tile)
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
-    const int e = tile * EB + el;
+    const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
     // curvilinear shock capturing: pure_and_blended_element_ids! (DG only where alpha is within 1e-12 of 0);
     // MUSCL subcells on blended elements without a boundary face
@@ -1065,7 +1067,7 @@ __device__ __forceinline__ void lw_volume_tile(const VolArgs& a, const int tile)
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o, SRC ? Ssrc : nullptr);
         if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) node_speeds(a.gamma, o, a.status, l1, l2);
     }
-    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, tile * EB, l1, l2);
+    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, l1, l2);
     if (TE) {
         // lw_volume_kernel_4!'s error estimate (dg_2d.jl:1183-1265; curvilinear, with F~, G~ and the node's
         // J^{-1}: dgsem_structured/dg_2d.jl:1595-1682 at depth 3, :1983-2075 at depth 4): the strong-form volume
@@ -1101,7 +1103,7 @@ __device__ __forceinline__ void lw_volume_tile(const VolArgs& a, const int tile)
         __syncthreads();
         if (active) X[el * C::P + i + C::R * j] = err;
         __syncthreads();
-        const int ee = tile * EB + tid;
+        const int ee = blockIdx.x * EB + tid;
         if (tid < EB && ee < a.E) {
             double sum = 0.0;
             for (int jj = 0; jj < n; ++jj)
@@ -1109,15 +1111,6 @@ __device__ __forceinline__ void lw_volume_tile(const VolArgs& a, const int tile)
             a.temporal_errors[ee] = sum;
         }
     }
-}
-
-template <int N, int MODE, bool SC, int EBX = 0, bool CURVED = false, bool TE = false, bool DSTORE = false, int REC = 0,
-          bool SRC = false>
-static __global__ void __launch_bounds__(VolCfg<N, EBX>::THREADS, (SC && CURVED) ? VolCfg<N, EBX>::SC_CURVED_MIN_BLOCKS
-                                                                  : SRC ? VolCfg<N, EBX>::MDRK_MIN_BLOCKS - 1
-                                                                        : VolCfg<N, EBX>::MIN_BLOCKS)
-    lw_volume_kernel(VolArgs a) {
-    lw_volume_tile<N, MODE, SC, EBX, CURVED, TE, DSTORE, REC, SRC>(a, blockIdx.x);
 }
 
 // MDRK stage 1's stored sums from u^n and d = u_t: F2 = f + f_t/6, G2 = g + g_t/6, U2 = u + u_t/6 with f_t the
@@ -1159,7 +1152,9 @@ __device__ __forceinline__ void mdrk_stage1_sums(double gm1, const double* uu, c
 // COMPACT (the plain TreeMesh step): store only u_t (into a.U2) instead of U2 and F2; stage 2 recomputes them from
 // u^n and u_t with this kernel's operations (64 instead of 192 bytes a node between the stages).
 template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
-__device__ __forceinline__ void mdrk1_volume_tile(const VolArgs& a, const int tile) {
+static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
+                                                                         : VolCfg<N>::MDRK_MIN_BLOCKS)
+    mdrk1_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     static_assert(!SRC || !SC, "source terms: the FR volume integral");
     static_assert(!COMPACT || (!SC && !CURVED && !SRC && MODE == MODE_STEP), "compact stages: the plain TreeMesh step");
@@ -1180,7 +1175,7 @@ __device__ __forceinline__ void mdrk1_volume_tile(const VolArgs& a, const int ti
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
-    const int e = tile * EB + el;
+    const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
     double alpha_e = 0.0;
     bool blended = false, muscl = false;
@@ -1308,14 +1303,6 @@ __device__ __forceinline__ void mdrk1_volume_tile(const VolArgs& a, const int ti
     }
 }
 
-template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
-static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
-                                                                         : VolCfg<N>::MDRK_MIN_BLOCKS)
-    mdrk1_volume_kernel(VolArgs a) {
-    mdrk1_volume_tile<N, MODE, SC, CURVED, REC, SRC, COMPACT>(a, blockIdx.x);
-
-}
-
 // ------------------------------------------------------------------------------------------------
 // MDRK stage 2 (mdrk_kernel_2!, multi_derivative_2d.jl:423-555): at u* = a.u,
 // F = F2 + f_t(u*)/3, U = U2 + u*_t/3.
@@ -1326,7 +1313,9 @@ static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? Vo
 // COMPACT: F2, G2, U2 recomputed from u^n (a.u_base) and stage 1's u_t (a.U2) at the start, parked in shared memory
 // (three more planes) until the stage's own sums are formed.
 template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
-__device__ __forceinline__ void mdrk2_volume_tile(const VolArgs& a, const int tile) {
+static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
+                                                                         : VolCfg<N>::MDRK_MIN_BLOCKS)
+    mdrk2_volume_kernel(VolArgs a) {
     static_assert(REC == 0 || (SC && CURVED), "MUSCL subcells: curvilinear shock capturing");
     static_assert(!SRC || !SC, "source terms: the FR volume integral");
     static_assert(!COMPACT || (!SC && !CURVED && !SRC && MODE == MODE_STEP), "compact stages: the plain TreeMesh step");
@@ -1347,7 +1336,7 @@ __device__ __forceinline__ void mdrk2_volume_tile(const VolArgs& a, const int ti
     const int el = tid / nn;
     const int node = tid - el * nn;
     const int i = node % n, j = node / n;
-    const int e = tile * EB + el;
+    const int e = blockIdx.x * EB + el;
     const bool active = el < EB && e < a.E;
     double alpha_e = 0.0;
     bool blended = false, muscl = false;
@@ -1480,15 +1469,7 @@ __device__ __forceinline__ void mdrk2_volume_tile(const VolArgs& a, const int ti
         volume_epilogue<n, MODE>(a, e, i, j, node, ij, dt, acc, U, F, G, o, SRC ? Ssrc : nullptr);
         if (SLOTS && a.cfl_slots && i > 0 && i < n - 1 && j > 0 && j < n - 1) node_speeds(a.gamma, o, a.status, l1, l2);
     }
-    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, tile * EB, l1, l2);
-}
-
-template <int N, int MODE, bool SC, bool CURVED = false, int REC = 0, bool SRC = false, bool COMPACT = false>
-static __global__ void __launch_bounds__(VolCfg<N>::THREADS, (SC && CURVED) ? VolCfg<N>::SC_CURVED_MIN_BLOCKS
-                                                                         : VolCfg<N>::MDRK_MIN_BLOCKS)
-    mdrk2_volume_kernel(VolArgs a) {
-    mdrk2_volume_tile<N, MODE, SC, CURVED, REC, SRC, COMPACT>(a, blockIdx.x);
-
+    if (SLOTS && a.cfl_slots) write_interior_slots<N, C>(a, X, active, el, i, j, tid, l1, l2);
 }
 
 }  // namespace tlw

@@ -37,7 +37,7 @@ EXPORTED = (
     "tlw_max_dt", "tlw_set_state", "tlw_get_state", "tlw_step", "tlw_get_time", "tlw_get_cache",
     "tlw_cache_size", "tlw_synchronize", "tlw_get_stream", "tlw_state_pointer", "tlw_last_error",
     "tlw_step_timed", "tlw_step_host", "tlw_set_unstructured_mesh", "tlw_dd_stages", "tlw_dd_halo_values", "tlw_dd_alpha_buffers", "tlw_dd_comm_stream", "tlw_set_source_terms",
-    "tlw_probe_fp64_tflops", "tlw_probe_reciprocal", "tlw_rhs_lw_noalloc", "tlw_set_fused_step",
+    "tlw_probe_fp64_tflops", "tlw_probe_reciprocal", "tlw_rhs_lw_noalloc",
     "tlw_batch_create", "tlw_batch_destroy", "tlw_batch_add_tree_mesh", "tlw_batch_finalize",
     "tlw_batch_set_state", "tlw_batch_get_state", "tlw_batch_step", "tlw_batch_synchronize",
     "tlw_batch_get_stream", "tlw_batch_autotune", "tlw_batch_num_groups", "tlw_batch_last_error",
@@ -121,8 +121,6 @@ def lib() -> ctypes.CDLL:
     L.tlw_cache_size.restype = i64
     L.tlw_synchronize.argtypes = [P]
     L.tlw_get_stream.argtypes = [P, ctypes.POINTER(P)]
-    L.tlw_set_fused_step.argtypes = [P, i32]
-    L.tlw_set_fused_step.restype = i32
     L.tlw_state_pointer.argtypes = [P, ctypes.POINTER(P)]
     L.tlw_last_error.argtypes = [P]
     L.tlw_last_error.restype = ctypes.c_char_p
