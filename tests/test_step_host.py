@@ -22,10 +22,14 @@ def plain(integ, u, t, nsteps, cfl):
 
 
 def test_step_host_independent_states_match_the_plain_path(tl):
+    """Eleven calls without synchronisation (the five-buffer pool wraps around four times; 1, 2 and 3 steps a call
+    leave the result in either buffer of a call's pair)."""
     semi, integ = make(tl)
     cfl = 0.5
     states = []
-    for k, beta in enumerate((5.0, 3.0, 4.0, 2.0, 4.5)):
+    strengths = (5.0, 3.0, 4.0, 2.0, 4.5, 3.5, 2.5, 5.5, 1.5, 4.2, 3.3)
+    nsteps = [1 + k % 3 for k in range(len(strengths))]
+    for beta in strengths:
         s, _ = make(tl, strength=beta)
         states.append(s.compute_coefficients(0.0))
     ins = [integ.pinned_state() for _ in states]
@@ -33,16 +37,39 @@ def test_step_host_independent_states_match_the_plain_path(tl):
     for a, u in zip(ins, states):
         a[:] = u
     for k in range(len(states)):      # no synchronisation between the calls
-        integ.step_host(ins[k], outs[k], 0.1 * k, 2 + k % 2, cfl)
+        integ.step_host(ins[k], outs[k], 0.1 * k, nsteps[k], cfl)
     integ.synchronize()
     last = integ.get_state()
     np.testing.assert_array_equal(last, outs[-1])
     _, ref_integ = make(tl)
     for k, u in enumerate(states):
-        ref = plain(ref_integ, u, 0.1 * k, 2 + k % 2, cfl)
+        ref = plain(ref_integ, u, 0.1 * k, nsteps[k], cfl)
         np.testing.assert_array_equal(outs[k], ref)
     integ.sync_time()
-    assert integ.iter == 2 + (len(states) - 1) % 2 and integ.t > 0.1 * (len(states) - 1)
+    assert integ.iter == nsteps[-1] and integ.t > 0.1 * (len(states) - 1)
+
+
+def test_step_host_with_steps_between_the_calls(tl):
+    """Device-resident steps between asynchronous calls act on the last call's result; the later uploads into
+    the buffers those steps used wait for them."""
+    semi, integ = make(tl)
+    u0 = semi.compute_coefficients(0.0)
+    _, ref_integ = make(tl)
+    ins = [integ.pinned_state() for _ in range(6)]
+    outs = [integ.pinned_state() for _ in range(6)]
+    mids = []
+    for k in range(6):
+        ins[k][:] = u0 * (1.0 + 0.01 * k)
+    for k in range(6):
+        integ.step_host(ins[k], outs[k], 0.0, 1, 0.5)
+        integ.step(1 + k % 2, 0.5, use_graph=False)   # continues from the downloaded result
+        mids.append(integ.get_state())
+    integ.synchronize()
+    for k in range(6):
+        r1 = plain(ref_integ, ins[k], 0.0, 1, 0.5)
+        np.testing.assert_array_equal(outs[k], r1)
+        ref_integ.step(1 + k % 2, 0.5, use_graph=False)
+        np.testing.assert_array_equal(mids[k], ref_integ.get_state())
 
 
 def test_step_host_round_trip_through_the_host(tl):
@@ -51,14 +78,32 @@ def test_step_host_round_trip_through_the_host(tl):
     u0 = semi.compute_coefficients(0.0)
     buf = integ.pinned_state()
     buf[:] = u0
-    for _ in range(4):
+    for _ in range(7):
         integ.step_host(buf, buf, 0.0, 1, 0.5)
     integ.synchronize()
     _, ref_integ = make(tl)
     u = u0.copy()
-    for _ in range(4):
+    for _ in range(7):
         u = plain(ref_integ, u, 0.0, 1, 0.5)
     np.testing.assert_array_equal(buf, u)
+
+
+def test_step_host_input_downloaded_two_calls_back(tl):
+    """Three host buffers in rotation: call k reads the output of call k - 2, which may still be downloading."""
+    semi, integ = make(tl)
+    u0 = semi.compute_coefficients(0.0)
+    bufs = [integ.pinned_state() for _ in range(3)]
+    bufs[0][:] = u0
+    bufs[1][:] = u0 * 1.01
+    for k in range(6):
+        integ.step_host(bufs[k % 3], bufs[(k + 2) % 3], 0.0, 1, 0.5)
+    integ.synchronize()
+    _, ref_integ = make(tl)
+    ref = [u0.copy(), u0 * 1.01, None]
+    for k in range(6):
+        ref[(k + 2) % 3] = plain(ref_integ, ref[k % 3], 0.0, 1, 0.5)
+    for b, r in zip(bufs, ref):
+        np.testing.assert_array_equal(b, r)
 
 
 def test_other_entry_points_after_step_host(tl):

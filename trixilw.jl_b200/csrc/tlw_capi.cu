@@ -66,7 +66,12 @@ void free_mesh(tlw_handle* h) {
     if (h->s_up) cudaStreamSynchronize(h->s_up);
     if (h->s_down) cudaStreamSynchronize(h->s_down);
     h->async_pending = false;
-    dfree(h->d_state[0]); dfree(h->d_state[1]); dfree(h->d_stage);
+    if (h->host_pool[0]) {   // the state buffers are members of the host-stepping pool
+        for (double*& p : h->host_pool) dfree(p);
+        h->d_state[0] = h->d_state[1] = nullptr;
+    } else {
+        dfree(h->d_state[0]); dfree(h->d_state[1]);
+    }
     dfree(h->d_us); dfree(h->d_in); dfree(h->d_in2); dfree(h->d_out);
     dfree(h->d_tU); dfree(h->d_tF); dfree(h->d_U2); dfree(h->d_F2);
     dfree(h->d_alpha); dfree(h->d_alpha_raw); dfree(h->d_tFn); dfree(h->d_il); dfree(h->d_ir);
@@ -655,7 +660,7 @@ int check_ready(tlw_handle* h, bool join_downloads = true) {
     if (!h) return TLW_E_ARG;
     if (join_downloads && h->async_pending) {
         // the entry point's work on the compute stream waits for tlw_step_host's last download
-        TLW_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_down[(h->host_calls - 1) & 1], 0));
+        TLW_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_dl[(h->host_calls - 1) % tlw_handle::HOST_CALLS], 0));
         h->async_pending = false;
     }
     if (!h->have_mesh) return fail(h, TLW_E_STATE, "no mesh: call tlw_set_tree_mesh first");
@@ -748,7 +753,11 @@ int tlw_destroy(tlw_handle* h) {
     dfree(h->d_basis);
     dfree(h->d_step);
     if (h->s_comm) cudaStreamSynchronize(h->s_comm);
-    for (cudaEvent_t ev : {h->ev_up, h->ev_computed, h->ev_down[0], h->ev_down[1], h->ev_prior, h->ev_lib, h->ev_comm})
+    for (cudaEvent_t ev : {h->ev_up, h->ev_computed, h->ev_prior, h->ev_lib, h->ev_comm})
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : h->ev_free)
+        if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : h->ev_dl)
         if (ev) cudaEventDestroy(ev);
     if (h->s_comm) cudaStreamDestroy(h->s_comm);
     if (h->s_up) cudaStreamDestroy(h->s_up);
@@ -1906,16 +1915,24 @@ int tlw_get_state(tlw_handle* h, double* u, int32_t where, double* t_out) {
 }
 
 namespace {
-// the copy streams, events and staging buffer of tlw_step_host (created on its first call)
+// the buffer pool, copy streams and events of tlw_step_host (created on its first call)
 int ensure_host_stepping(tlw_handle* h) {
-    if (!h->d_stage) TLW_CUDA(h, cudaMalloc(&h->d_stage, state_doubles(h) * sizeof(double)));
+    if (!h->host_pool[0]) {
+        // the handle's two state buffers and three more (the current state stays in d_state[cur])
+        const size_t bytes = state_doubles(h) * sizeof(double);
+        h->host_pool[0] = h->d_state[0];
+        h->host_pool[1] = h->d_state[1];
+        for (int k = 0; k < tlw_handle::HOST_POOL; ++k)
+            if (!h->host_pool[k]) TLW_CUDA(h, cudaMalloc(&h->host_pool[k], bytes));
+    }
     if (!h->s_up) {
         TLW_CUDA(h, cudaStreamCreateWithFlags(&h->s_up, cudaStreamNonBlocking));
         TLW_CUDA(h, cudaStreamCreateWithFlags(&h->s_down, cudaStreamNonBlocking));
-        for (cudaEvent_t* ev : {&h->ev_up, &h->ev_computed, &h->ev_down[0], &h->ev_down[1], &h->ev_prior})
+        for (cudaEvent_t* ev : {&h->ev_up, &h->ev_computed, &h->ev_prior})
             TLW_CUDA(h, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
-        TLW_CUDA(h, cudaEventRecord(h->ev_down[0], h->s_down));   // nothing downloaded yet
-        TLW_CUDA(h, cudaEventRecord(h->ev_down[1], h->s_down));
+        // (a wait on an event never recorded returns at once: nothing is in flight yet)
+        for (cudaEvent_t& ev : h->ev_free) TLW_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        for (cudaEvent_t& ev : h->ev_dl) TLW_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     }
     return TLW_OK;
 }
@@ -1930,47 +1947,49 @@ int tlw_step_host(tlw_handle* h, const double* u_in, double* u_out, double t, in
     TLW_CUDA(h, cudaSetDevice(h->device));
     if ((rc = ensure_host_stepping(h))) return rc;
     const size_t bytes = state_doubles(h) * sizeof(double);
-    // buffers: d_stage receives the upload (it holds the result of the call before the previous one);
-    // d_state[cur] holds the previous result (its download may still run); d_state[1 - cur] is free once the
-    // compute stream reaches this call
-    const int parity = (int)(h->host_calls & 1);
-    double* in = h->d_stage;
-    double* prev = h->d_state[h->cur];
-    double* scratch = h->d_state[1 - h->cur];
-    // 1. upload, once the download two calls back (from this buffer) has finished, and once every earlier use of
-    //    the buffer on the compute stream has (ev_prior of the previous call, waited below)
-    TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_down[parity], 0));
-    // a caller that feeds the previous result back in (the state round-trips through the host) reads it only
-    // after its download
-    if (u_in == h->last_out && h->host_calls > 0)
-        TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_down[parity ^ 1], 0));
-    TLW_CUDA(h, cudaMemcpyAsync(in, u_in, bytes, cudaMemcpyHostToDevice, h->s_up));
+    constexpr int P = tlw_handle::HOST_POOL, K = tlw_handle::HOST_CALLS;
+    // call k takes pool buffers 2k and 2k + 1 (mod 5): A receives the upload, B is the steps' other buffer. A was
+    // last used three calls back and B two calls back, so the upload of call k waits at most for the download of
+    // call k - 3, and the uploads, steps and downloads of three consecutive calls overlap.
+    const long long k = h->host_calls;
+    const int ia = (int)((2 * k) % P), ib = (int)((2 * k + 1) % P);
+    double* A = h->host_pool[ia];
+    double* B = h->host_pool[ib];
+    // 1. upload into A after its last use; a u_in that one of the last calls downloads into is read after that
+    //    download (the state round-tripping through the host)
+    TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_free[ia], 0));
+    for (long long j = k - 1; j >= 0 && j >= k - (K - 1); --j)
+        if (h->dl_out[j % K] == u_in) TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_dl[j % K], 0));
+    TLW_CUDA(h, cudaMemcpyAsync(A, u_in, bytes, cudaMemcpyHostToDevice, h->s_up));
     TLW_CUDA(h, cudaEventRecord(h->ev_up, h->s_up));
-    // 2. rotate: the upload becomes the current state; the previous result becomes the next upload's target,
-    //    free after its download (ev_down) and after the compute stream's work so far (ev_prior)
+    // the next upload also waits for the compute stream's work enqueued so far (other entry points between the
+    // calls may have used any buffer of the pair that is current now)
     TLW_CUDA(h, cudaEventRecord(h->ev_prior, h->stream));
-    TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_prior, 0));   // orders the NEXT upload (same stream)
-    h->d_state[0] = in;
-    h->d_state[1] = scratch;
+    TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_prior, 0));
+    // 2. the steps from A, with B as the other buffer, after the upload and after B's last use
+    TLW_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_up, 0));
+    TLW_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_free[ib], 0));
+    h->d_state[0] = A;
+    h->d_state[1] = B;
     h->cur = 0;
-    h->d_stage = prev;
     drop_graphs(h);   // they address the previous buffers
     h->slots_valid = false;
-    // 3. the steps, after the upload
-    TLW_CUDA(h, cudaStreamWaitEvent(h->stream, h->ev_up, 0));
     StepState* sp = h->d_step;
     const long long zero = 0;
     TLW_CUDA(h, cudaMemcpyAsync(&sp->t, &t, sizeof(double), cudaMemcpyHostToDevice, h->stream));
     TLW_CUDA(h, cudaMemcpyAsync(&sp->steps, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->stream));
     h->async_pending = false;
     if ((rc = tlw_step(h, nsteps, cfl, fixed_dt, t_end, 0))) return rc;
+    const int ir = h->cur == 0 ? ia : ib, io = h->cur == 0 ? ib : ia;   // the result's buffer and the other
+    TLW_CUDA(h, cudaEventRecord(h->ev_free[io], h->stream));
     TLW_CUDA(h, cudaEventRecord(h->ev_computed, h->stream));
-    // 4. download the result
+    // 3. download the result
     TLW_CUDA(h, cudaStreamWaitEvent(h->s_down, h->ev_computed, 0));
     TLW_CUDA(h, cudaMemcpyAsync(u_out, h->d_state[h->cur], bytes, cudaMemcpyDeviceToHost, h->s_down));
-    TLW_CUDA(h, cudaEventRecord(h->ev_down[parity], h->s_down));
+    TLW_CUDA(h, cudaEventRecord(h->ev_free[ir], h->s_down));
+    TLW_CUDA(h, cudaEventRecord(h->ev_dl[k % K], h->s_down));
+    h->dl_out[k % K] = u_out;
     h->host_calls += 1;
-    h->last_out = u_out;
     h->async_pending = true;
     return TLW_OK;
 }

@@ -188,16 +188,19 @@ struct tlw_handle {
     double* d_cmj = nullptr;
     std::vector<int> mortar_order;
     std::vector<int> mortar_off;            // mortar colour c covers [mortar_off[c], mortar_off[c + 1])
-    // host-buffer stepping (tlw_step_host): a third state buffer that uploads land in, the copy streams, and
-    // events: ev_down[call parity] after each call's download (the result of call k is the upload target of
-    // call k + 2), ev_prior on the compute stream before each call's steps; async_pending until another entry
-    // point has ordered itself after the last download
-    double* d_stage = nullptr;
+    // host-buffer stepping (tlw_step_host): a pool of HOST_POOL state buffers taken round robin, two per call (the
+    // upload target and the steps' other buffer), each with an event after its last use; the copy streams; per
+    // call (ring of HOST_CALLS) the event after its download and its u_out; ev_prior on the compute stream at each
+    // call (the next upload waits for the work enqueued before it); async_pending until another entry point has
+    // ordered itself after the last download
+    static constexpr int HOST_POOL = 5, HOST_CALLS = 4;
+    double* host_pool[HOST_POOL] = {};
+    cudaEvent_t ev_free[HOST_POOL] = {};
+    cudaEvent_t ev_dl[HOST_CALLS] = {};
+    const void* dl_out[HOST_CALLS] = {};
     cudaStream_t s_up = nullptr, s_down = nullptr;
     cudaEvent_t ev_up = nullptr, ev_computed = nullptr, ev_prior = nullptr;
-    cudaEvent_t ev_down[2] = {nullptr, nullptr};
     long long host_calls = 0;
-    const void* last_out = nullptr;          // u_out of the last call (a next u_in equal to it waits for it)
     bool async_pending = false;
     // graphs: [start buffer] one step, two steps
     cudaGraphExec_t g_one[2] = {nullptr, nullptr};
