@@ -147,6 +147,45 @@ def volume_flops_per_node(N: int) -> float:
     return 16 * n * nv + 11 * 17 + 200
 
 
+def host_link(nbytes: int, stream) -> dict:
+    """The host link for one state: a pinned upload alone, a download alone, and both at once on two streams
+    (best of five, CUDA events)."""
+    import torch
+
+    n = nbytes // 8
+    h_in = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    h_out = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    d_a = torch.empty(n, dtype=torch.float64, device="cuda")
+    d_b = torch.empty(n, dtype=torch.float64, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(up, down):
+        best = float("inf")
+        for r in range(6):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s1.wait_stream(stream)
+            s2.wait_stream(stream)
+            if up:
+                with torch.cuda.stream(s1):
+                    d_a.copy_(h_in, non_blocking=True)
+            if down:
+                with torch.cuda.stream(s2):
+                    h_out.copy_(d_b, non_blocking=True)
+            stream.wait_stream(s1)
+            stream.wait_stream(s2)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if r:
+                best = min(best, e0.elapsed_time(e1))
+        return best
+
+    up, down, both = timed(True, False), timed(False, True), timed(True, True)
+    return {"h2d_ms": up, "d2h_ms": down, "both_ms": both, "h2d_gbs": nbytes / up / 1e6,
+            "d2h_gbs": nbytes / down / 1e6, "both_gbs": 2 * nbytes / both / 1e6}
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -578,6 +617,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_rt = ndofs * n_e2e / (e0.elapsed_time(e1) * 1e-3)
     state_bytes = 8 * 4 * ndofs
+    link = host_link(state_bytes, stream)
 
     if rank == 0:
         E = semi.mesh.n_elements
@@ -637,7 +677,10 @@ def run_ours(args):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                     "steps": n_e2e, "api": "tlw_step_host (pinned host in/out, one step per call, calls overlapped)",
                     "round_trip": {"value": e2e_rt, "unit": UNIT,
-                                   "api": "tlw_set_state + tlw_step + tlw_get_state (synchronous, serial copies)"}},
+                                   "api": "tlw_set_state + tlw_step + tlw_get_state (synchronous, serial copies)"},
+                    # the host link bounds it: a state up and a state down per step, at best concurrently
+                    "link": {**link, "bound_value": ndofs / (link["both_ms"] * 1e-3),
+                             "frac": e2e / (ndofs / (link["both_ms"] * 1e-3))}},
             "roofline": {"kernel": (f"grad_volume_kernel + curved_grad_*_kernel + par_volume_kernel<{N}, MODE_STEP, CURVED>"
                                     if ns else f"lw_volume_kernel<{N}, MODE_STEP, SC, CURVED, MUSCL>" if icname == "blast"
                                     else f"lw_volume_kernel<{N}, MODE_STEP{', SC' if sc else ''}{', CURVED' if curved else ''}>"),
