@@ -110,12 +110,12 @@ def mdrk_volume_bytes_per_element(N: int) -> float:
 
 
 def mdrk_volume_flops_per_node(N: int) -> float:
-    """Algorithmic FP64 flops per node of the two compact MDRK stage kernels (FMA = 2, divides not counted), in
-    the terms of the LW model: four line contractions of F and G (16 n nv), 15 flux pairs at 17 (stage 1: u^n and
-    u^n +- u_t, +- 2 u_t; stage 2: the same five again for F2, G2 and five at u*) and about 250 for the stages'
-    sums and updates."""
+    """Algorithmic FP64 flops per node of the two MDRK stage kernels of a step (FMA = 2, divides not counted):
+    2 (8 n nv + 5 F_pair + 120) with F_pair = 17, the survey's count for two stages of two line contractions and
+    five flux pairs each. (The compact stages recompute stage 1's five flux pairs in stage 2 instead of storing
+    U2 and F2; those flops are not algorithmic and not counted.)"""
     n, nv = N + 1, 4
-    return 16 * n * nv + 15 * 17 + 250
+    return 2 * (8 * n * nv + 5 * 17 + 120)
 
 
 def surface_pass_bytes_per_element(N: int) -> float:
