@@ -307,6 +307,9 @@ static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
 #ifndef TLW_SURF_PREFETCH
 #define TLW_SURF_PREFETCH 0
 #endif
+#ifndef TLW_SURF_REVERSE
+#define TLW_SURF_REVERSE 1
+#endif
 // Elements per CTA of surface_kernel: 4n flux threads per element, about TLW_SURF_THREADS threads a CTA.
 template <int N> struct SurfCfg {
     static constexpr int n = N + 1;
@@ -334,7 +337,11 @@ static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? TLW_
     constexpr int n = N + 1, EB = C::EB, NB = 4 * (n - 1);
     __shared__ double sF[EB * 4 * n * NV];
     const int tid = threadIdx.x;
-    const int e0 = blockIdx.x * EB;
+    // TLW_SURF_REVERSE: the CTAs take the elements from the last one down, so that the first ones read the traces
+    // and face nodes the volume kernel wrote last (still in L2), and the next volume kernel, which starts from the
+    // first element, finds the face nodes written last (512^2, N = 4: 0.2034 against 0.2051 ms a launch, LW step
+    // 0.7145 against 0.7173 ms, MDRK step 0.978 against 0.983 ms)
+    const int e0 = (TLW_SURF_REVERSE ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x) * EB;
     // phase-2 thread: element el2, boundary node b (bottom row, top row, left column, right column)
     const int el2 = tid / NB, b = tid - el2 * NB, e2 = e0 + el2;
     const bool has2 = el2 < EB && e2 < a.E;
