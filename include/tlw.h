@@ -387,7 +387,7 @@ const char* tlw_last_error(tlw_handle* h);
  * The face-trace scratch is a static device array of TLW_NOALLOC_SCRATCH_BYTES: meshes with
  * n_elements * 2 * 4 * (N+1) * 4 * 8 bytes of traces beyond it are rejected with TLW_E_ARG. Calls on a
  * device share that array and the static dt and status words beside it, so calls that overlap on the GPU
- * race. The first call on a device sets the device up (make it before any stream capture). Runs on `stream`
+ * race. The first call on a device sets the device up. Runs on `stream`
  * (a cudaStream_t, 0 = default), waits for that stream and returns after the result is in du: TLW_OK,
  * TLW_E_NONADMISSIBLE (DomainError), TLW_E_ARG or TLW_E_CUDA. */
 #define TLW_NOALLOC_SCRATCH_BYTES (32u << 20)

@@ -21,7 +21,7 @@
 //    serialised by the caller;
 //  * each call waits for its stream before it returns;
 //  * the first call on each device sets up that device (symbol addresses, basis, kernel attributes)
-//    with the device current; make that first call before any stream capture.
+//    with the device current.
 #include <cuda_runtime.h>
 
 #include <cmath>
