@@ -1,8 +1,8 @@
 """GPU parity at the sizes the throughput numbers are quoted on: libtlw (through the C ABI) against the
 multithreaded oracle on the full meshes, not on reduced ones.
 
-* isentropic vortex, periodic TreeMesh 512 x 512, N = 4, LW: one rhs, then 3 device CFL steps;
-* the same vortex on 256 x 256 with the two-stage MDRK step, N = 3, 4, 5: 3 device steps;
+* isentropic vortex, periodic TreeMesh 512 x 512, N = 3, 4, 5, LW: one rhs, then 3 device CFL steps;
+* the same vortex with the two-stage MDRK step on 256 x 256 (N = 3, 4, 5) and 512 x 512 (N = 4): 3 device steps;
 * four-quadrant Riemann problem on [0, 1]^2, TreeMesh 512 x 512, N = 4, Hennemann-Gassner blending
   (alpha_max = 0.5) with first-order subcells and Dirichlet(initial condition) boundaries: one rhs with the
   blending factors and the subcell fluxes next to the faces (fn_low), then 3 device steps;
@@ -52,11 +52,12 @@ def device_steps(tl, semi, u0, nsteps, cfl, **kw):
     return integ.get_state(), integ
 
 
-def test_vortex_512_N4_rhs_and_steps(tl, oracle_mod):
-    semi = vortex_semi(tl, 9, 4, "lw")
+@pytest.mark.parametrize("N", [3, 4, 5])
+def test_vortex_512_rhs_and_steps(tl, oracle_mod, N):
+    semi = vortex_semi(tl, 9, N, "lw")
     u0 = semi.compute_coefficients(0.0)
-    o = oracle_mod.Oracle(semi.mesh, 4)
-    cfl = cfl_lw(4)
+    o = oracle_mod.Oracle(semi.mesh, N)
+    cfl = cfl_lw(N)
     dt = o.max_dt(u0, cfl)
     assert semi.max_dt(u0, cfl) == pytest.approx(dt, rel=1e-14)
     semi.cache["dt"][0] = dt
@@ -73,9 +74,9 @@ def test_vortex_512_N4_rhs_and_steps(tl, oracle_mod):
     assert np.all(rel_l2(u_gpu, u_cpu) < RTOL), rel_l2(u_gpu, u_cpu)
 
 
-@pytest.mark.parametrize("N", [3, 4, 5])
-def test_vortex_256_mdrk_steps(tl, oracle_mod, N):
-    semi = vortex_semi(tl, 8, N, "mdrk")
+@pytest.mark.parametrize("level,N", [(8, 3), (8, 4), (8, 5), (9, 4)])
+def test_vortex_mdrk_steps(tl, oracle_mod, level, N):
+    semi = vortex_semi(tl, level, N, "mdrk")
     u0 = semi.compute_coefficients(0.0)
     cfl = cfl_lw(N)
     u_gpu, integ = device_steps(tl, semi, u0, 3, cfl)
