@@ -345,8 +345,8 @@ int tlw_step(tlw_handle* h, int32_t nsteps, double cfl, double fixed_dt, double 
  * previous one run on copy streams of their own beside the steps, so a stream of independent states (an
  * ensemble, or requests served one after another) moves through the GPU at the host link's bandwidth. With
  * pinned (page-locked) host buffers the copies run asynchronously; pageable ones make the copies wait. A u_in
- * equal to the u_out of one of the last three calls (the state round-tripping through the host) is read after that
- * download; older outputs have been downloaded by then. The
+ * equal to the u_out of an earlier call (the state round-tripping through the host) is read after that download:
+ * each upload waits for the downloads up to three calls back, and for the last two calls' where u_in is their u_out. The
  * handle's current state afterwards is the last call's result. (No counterpart in the reference, whose
  * solution vectors stay in host memory; this is the host-side path of the drop-in at full link speed.) */
 int tlw_step_host(tlw_handle* h, const double* u_in, double* u_out, double t, int32_t nsteps, double cfl,

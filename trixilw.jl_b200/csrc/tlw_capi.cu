@@ -1955,10 +1955,12 @@ int tlw_step_host(tlw_handle* h, const double* u_in, double* u_out, double t, in
     const int ia = (int)((2 * k) % P), ib = (int)((2 * k + 1) % P);
     double* A = h->host_pool[ia];
     double* B = h->host_pool[ib];
-    // 1. upload into A after its last use; a u_in that one of the last calls downloads into is read after that
+    // 1. upload into A after its last use and after the downloads up to call k - 3 (in order on their stream; they
+    //    have finished by then in a full pipeline); a u_in that call k - 1 or k - 2 downloads into is read after that
     //    download (the state round-tripping through the host)
     TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_free[ia], 0));
-    for (long long j = k - 1; j >= 0 && j >= k - (K - 1); --j)
+    if (k >= 3) TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_dl[(k - 3) % K], 0));
+    for (long long j = k - 1; j >= 0 && j >= k - 2; --j)
         if (h->dl_out[j % K] == u_in) TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_dl[j % K], 0));
     TLW_CUDA(h, cudaMemcpyAsync(A, u_in, bytes, cudaMemcpyHostToDevice, h->s_up));
     TLW_CUDA(h, cudaEventRecord(h->ev_up, h->s_up));
