@@ -122,3 +122,22 @@ def test_other_entry_points_after_step_host(tl):
     np.testing.assert_array_equal(u, ref_integ.get_state())
     integ.set_state(u0, 0.0)            # overwrites the current state after the pending download
     np.testing.assert_array_equal(integ.get_state(), u0)
+
+
+def test_step_host_input_downloaded_four_calls_back(tl):
+    """Five host buffers in rotation, two steps a call (the result in the upload's own device buffer): call k reads
+    the output of call k - 4."""
+    semi, integ = make(tl)
+    u0 = semi.compute_coefficients(0.0)
+    bufs = [integ.pinned_state() for _ in range(5)]
+    for q in range(4):
+        bufs[q][:] = u0 * (1.0 + 0.01 * q)
+    for k in range(10):
+        integ.step_host(bufs[k % 5], bufs[(k + 4) % 5], 0.0, 2, 0.5)
+    integ.synchronize()
+    _, ref_integ = make(tl)
+    ref = [u0 * (1.0 + 0.01 * q) for q in range(4)] + [None]
+    for k in range(10):
+        ref[(k + 4) % 5] = plain(ref_integ, ref[k % 5], 0.0, 2, 0.5)
+    for b, r in zip(bufs, ref):
+        np.testing.assert_array_equal(b, r)
