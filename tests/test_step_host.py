@@ -141,3 +141,18 @@ def test_step_host_input_downloaded_four_calls_back(tl):
         ref[(k + 4) % 5] = plain(ref_integ, ref[k % 5], 0.0, 2, 0.5)
     for b, r in zip(bufs, ref):
         np.testing.assert_array_equal(b, r)
+
+
+def test_step_host_after_device_steps(tl):
+    """The first asynchronous call uploads into the handle's state buffers: it waits for the device steps that
+    other entry points enqueued on them."""
+    semi, integ = make(tl, level=6)
+    u0 = semi.compute_coefficients(0.0)
+    integ.set_state(u0, 0.0)
+    integ.step(30, 0.5, use_graph=False)        # enqueued, still running when the call below uploads
+    a, b = integ.pinned_state(), integ.pinned_state()
+    a[:] = u0 * 1.02
+    integ.step_host(a, b, 0.0, 1, 0.5)
+    integ.synchronize()
+    _, ref_integ = make(tl, level=6)
+    np.testing.assert_array_equal(b, plain(ref_integ, u0 * 1.02, 0.0, 1, 0.5))

@@ -1917,14 +1917,6 @@ int tlw_get_state(tlw_handle* h, double* u, int32_t where, double* t_out) {
 namespace {
 // the buffer pool, copy streams and events of tlw_step_host (created on its first call)
 int ensure_host_stepping(tlw_handle* h) {
-    if (!h->host_pool[0]) {
-        // the handle's two state buffers and three more (the current state stays in d_state[cur])
-        const size_t bytes = state_doubles(h) * sizeof(double);
-        h->host_pool[0] = h->d_state[0];
-        h->host_pool[1] = h->d_state[1];
-        for (int k = 0; k < tlw_handle::HOST_POOL; ++k)
-            if (!h->host_pool[k]) TLW_CUDA(h, cudaMalloc(&h->host_pool[k], bytes));
-    }
     if (!h->s_up) {
         TLW_CUDA(h, cudaStreamCreateWithFlags(&h->s_up, cudaStreamNonBlocking));
         TLW_CUDA(h, cudaStreamCreateWithFlags(&h->s_down, cudaStreamNonBlocking));
@@ -1933,6 +1925,17 @@ int ensure_host_stepping(tlw_handle* h) {
         // (a wait on an event never recorded returns at once: nothing is in flight yet)
         for (cudaEvent_t& ev : h->ev_free) TLW_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         for (cudaEvent_t& ev : h->ev_dl) TLW_CUDA(h, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    if (!h->host_pool[0]) {
+        // the handle's two state buffers and three more; the first upload into the state buffers waits for the
+        // work other entry points have enqueued on them
+        const size_t bytes = state_doubles(h) * sizeof(double);
+        h->host_pool[0] = h->d_state[0];
+        h->host_pool[1] = h->d_state[1];
+        for (int k = 0; k < tlw_handle::HOST_POOL; ++k)
+            if (!h->host_pool[k]) TLW_CUDA(h, cudaMalloc(&h->host_pool[k], bytes));
+        TLW_CUDA(h, cudaEventRecord(h->ev_prior, h->stream));
+        TLW_CUDA(h, cudaStreamWaitEvent(h->s_up, h->ev_prior, 0));
     }
     return TLW_OK;
 }
