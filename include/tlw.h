@@ -324,7 +324,8 @@ int tlw_set_boundary_data(tlw_handle* h, const double* levels, const double* now
 /* One right-hand side evaluation: du = rhs(u) exactly as the reference's rhs!/rhs_mdrk1!/rhs_mdrk2!
  * (du already multiplied by -J^{-1}, ready for u_new = u + dt*du). For TLW_STAGE_MDRK2, `us` is the
  * stage state u* = u + dt*du1 (cache.element_cache.mdrk_cache.us); U2/F2 come from the preceding
- * TLW_STAGE_MDRK1 call on the same handle. */
+ * TLW_STAGE_MDRK1 call on the same handle. Device arrays (where = TLW_WHERE_DEVICE) are used in place when they
+ * are 32-byte aligned (one node's four doubles per access) and copied through the handle's buffers otherwise. */
 int tlw_rhs(tlw_handle* h, int32_t stage, double* du, const double* u, const double* us, double t, double dt,
             int32_t where);
 

@@ -305,3 +305,40 @@ def test_full_size_properties(tl):
     scale = np.einsum("ejiv,j,i->v", np.abs(d), w, w)
     # the sum runs over 6.5 M nodes: its own rounding is ~1e-13 of the absolute sum
     assert np.all(np.abs(total) <= 1e-10 * scale)
+
+
+@pytest.mark.parametrize("offset", [0, 1, 2, 3])
+def test_rhs_with_device_arrays_at_any_alignment(tl, offset):
+    """tlw_rhs and tlw_max_dt on device arrays that start 8 offset bytes into an allocation: used in place when
+    32-byte aligned, copied through the handle's buffers otherwise; the results equal the host-array call."""
+    import ctypes
+
+    import torch
+    from trixilw import _lib
+    L = _lib.lib()
+    mesh = tl.TreeMesh((-10.0, -10.0), (10.0, 10.0), 4)
+    semi = make_semi(tl, mesh, 4, tl.IsentropicVortex(5.0, center=(0.2, 0.1)), "mdrk")
+    u = semi.compute_coefficients(0.0)
+    dt = semi.max_dt(u, 0.4)
+    semi.cache["dt"][0] = dt
+    du_h = np.empty_like(u)
+    tl.rhs_mdrk1(du_h, u, semi, 0.0)
+    us = u + 0.5 * dt * du_h
+    du2_h = np.empty_like(u)
+    tl.rhs_mdrk2(du2_h, u, semi, 0.0, us)
+    n = u.size
+    bufs = [torch.zeros(n + 4, dtype=torch.float64, device="cuda") for _ in range(4)]
+    d_u, d_us, d_du, d_du2 = (b[offset:offset + n] for b in bufs)
+    d_u.copy_(torch.from_numpy(u))
+    d_us.copy_(torch.from_numpy(us))
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    _lib.check(semi.handle, L.tlw_rhs(semi.handle, _lib.TLW_STAGE_MDRK1, p(d_du), p(d_u), None, 0.0, dt,
+                                      _lib.TLW_WHERE_DEVICE))
+    _lib.check(semi.handle, L.tlw_rhs(semi.handle, _lib.TLW_STAGE_MDRK2, p(d_du2), p(d_u), p(d_us), 0.0, dt,
+                                      _lib.TLW_WHERE_DEVICE))
+    dt_d = ctypes.c_double()
+    _lib.check(semi.handle, L.tlw_max_dt(semi.handle, p(d_u), _lib.TLW_WHERE_DEVICE, 0.4, ctypes.byref(dt_d)))
+    _lib.check(semi.handle, L.tlw_synchronize(semi.handle))
+    np.testing.assert_array_equal(d_du.cpu().numpy(), du_h)
+    np.testing.assert_array_equal(d_du2.cpu().numpy(), du2_h)
+    assert dt_d.value == dt

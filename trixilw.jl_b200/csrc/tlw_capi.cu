@@ -1804,13 +1804,18 @@ int tlw_rhs(tlw_handle* h, int32_t stage, double* du, const double* u, const dou
     TLW_CUDA(h, cudaMemcpyAsync(&h->d_step->t_call, &tdt[1], sizeof(double), cudaMemcpyHostToDevice, h->stream));
     const double *du_in = u, *dus = us;
     double* dout = du;
-    if (where == TLW_WHERE_HOST) {
+    // host arrays, and device arrays whose node records are not 32-byte aligned (the surface pass reads and writes
+    // a node's four doubles at once), go through the handle's own buffers
+    const uintptr_t bits = (uintptr_t)u | (uintptr_t)du | (stage == TLW_STAGE_MDRK2 ? (uintptr_t)us : 0);
+    const bool staged = where == TLW_WHERE_HOST || bits % 32 != 0;
+    if (staged) {
+        const cudaMemcpyKind in = where == TLW_WHERE_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
         if ((rc = ensure(h, h->d_in, state_doubles(h))) || (rc = ensure(h, h->d_out, state_doubles(h)))) return rc;
-        TLW_CUDA(h, cudaMemcpyAsync(h->d_in, u, bytes, cudaMemcpyHostToDevice, h->stream));
+        TLW_CUDA(h, cudaMemcpyAsync(h->d_in, u, bytes, in, h->stream));
         du_in = h->d_in;
         if (stage == TLW_STAGE_MDRK2) {
             if ((rc = ensure(h, h->d_in2, state_doubles(h)))) return rc;
-            TLW_CUDA(h, cudaMemcpyAsync(h->d_in2, us, bytes, cudaMemcpyHostToDevice, h->stream));
+            TLW_CUDA(h, cudaMemcpyAsync(h->d_in2, us, bytes, in, h->stream));
             dus = h->d_in2;
         }
         dout = h->d_out;
@@ -1818,9 +1823,10 @@ int tlw_rhs(tlw_handle* h, int32_t stage, double* du, const double* u, const dou
     const double* u_flux = stage == TLW_STAGE_MDRK2 ? dus : du_in;
     enqueue_rhs(h, stage, MODE_RHS, u_flux, du_in, du_in, dout, &h->d_step->dt_call);
     TLW_CUDA(h, cudaGetLastError());
-    if (where == TLW_WHERE_HOST) {
-        TLW_CUDA(h, cudaMemcpyAsync(du, h->d_out, bytes, cudaMemcpyDeviceToHost, h->stream));
-        return read_status(h);
+    if (staged) {
+        const cudaMemcpyKind out = where == TLW_WHERE_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+        TLW_CUDA(h, cudaMemcpyAsync(du, h->d_out, bytes, out, h->stream));
+        if (where == TLW_WHERE_HOST) return read_status(h);
     }
     return TLW_OK;
 }
@@ -1831,9 +1837,11 @@ int tlw_max_dt(tlw_handle* h, const double* u, int32_t where, double cfl, double
     if (!u || !dt_out) return fail(h, TLW_E_ARG, "null pointer");
     TLW_CUDA(h, cudaSetDevice(h->device));
     const double* du_in = u;
-    if (where == TLW_WHERE_HOST) {
+    // host arrays, and device arrays whose node records are not 32-byte aligned, through the handle's buffer
+    if (where == TLW_WHERE_HOST || (uintptr_t)u % 32 != 0) {
+        const cudaMemcpyKind in = where == TLW_WHERE_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
         if ((rc = ensure(h, h->d_in, state_doubles(h)))) return rc;
-        TLW_CUDA(h, cudaMemcpyAsync(h->d_in, u, state_doubles(h) * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        TLW_CUDA(h, cudaMemcpyAsync(h->d_in, u, state_doubles(h) * sizeof(double), in, h->stream));
         du_in = h->d_in;
     }
     const unsigned long long zero = 0;

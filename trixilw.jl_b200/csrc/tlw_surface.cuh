@@ -103,7 +103,8 @@ __device__ __forceinline__ void blend_interface_flux(const SurfArgs& a, int orie
 
 // The LW flux at node l of the interface (le, re) of one orientation, with the blending and the viscous
 // flux where they apply: calc_interface_flux! (dg_2d.jl:1903-1946) at one node.
-template <int N, bool SC = true>
+// WIDE: 256-bit loads of the node records (the element-centric surface pass; 32-byte aligned arrays)
+template <int N, bool SC = true, bool WIDE = false>
 __device__ __forceinline__ void interface_node_flux(const SurfArgs& a, int orientation, int le, int re, int l,
                                                     double dt, double* Fn) {
     constexpr int n = N + 1;
@@ -111,12 +112,16 @@ __device__ __forceinline__ void interface_node_flux(const SurfArgs& a, int orien
     if (orientation == 1) { nodeL = (n - 1) + n * l; nodeR = n * l; faceL = 1; faceR = 0; }
     else { nodeL = l + n * (n - 1); nodeR = l; faceL = 3; faceR = 2; }
     double uL[NV], uR[NV], UL[NV], UR[NV], FL[NV], FR[NV];
-    load4(a.u + ((size_t)le * n * n + nodeL) * NV, uL);
-    load4(a.u + ((size_t)re * n * n + nodeR) * NV, uR);
-    load4(a.tU + (((size_t)le * 4 + faceL) * n + l) * NV, UL);
-    load4(a.tU + (((size_t)re * 4 + faceR) * n + l) * NV, UR);
-    load4(a.tF + (((size_t)le * 4 + faceL) * n + l) * NV, FL);
-    load4(a.tF + (((size_t)re * 4 + faceR) * n + l) * NV, FR);
+    auto ld = [](const double* p, double* x) {
+        if (WIDE) load4w(p, x);
+        else load4(p, x);
+    };
+    ld(a.u + ((size_t)le * n * n + nodeL) * NV, uL);
+    ld(a.u + ((size_t)re * n * n + nodeR) * NV, uR);
+    ld(a.tU + (((size_t)le * 4 + faceL) * n + l) * NV, UL);
+    ld(a.tU + (((size_t)re * 4 + faceR) * n + l) * NV, UR);
+    ld(a.tF + (((size_t)le * 4 + faceL) * n + l) * NV, FL);
+    ld(a.tF + (((size_t)re * 4 + faceR) * n + l) * NV, FR);
     // TreeMesh argument order: surface_flux(f_ll, f_rr, U_ll, U_rr, u_ll, u_rr) (dg_2d.jl:1928)
     lw_surface_flux(a.gamma, a.flux_kind, a.speed_kind, FL, FR, UL, UR, uL, uR, orientation, Fn, a.status);
     if (SC && a.shock_capturing) blend_interface_flux<N>(a, orientation, le, re, faceL, faceR, l, uL, uR, dt, Fn);
@@ -352,7 +357,7 @@ static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? TLW_
     else { i2 = n - 1; j2 = b - 3 * n + 3; }
     double* o2 = a.out + ((size_t)e2 * n * n + i2 + n * j2) * NV;
     double x[NV];
-    if (TLW_SURF_PREFETCH && has2) load4_rw(o2, x);
+    if (TLW_SURF_PREFETCH && has2) load4w_rw(o2, x);
     {
         const int el = tid / (4 * n), r = tid - el * 4 * n, f = r / n, l = r - f * n, e = e0 + el;
         if (el < EB && e < a.E) {
@@ -360,7 +365,8 @@ static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? TLW_
             const int nb = __ldg(a.nbr + 4 * e + f);
             const bool plus = f & 1;   // this element is the interface's left (lower) element
             double Fn[NV];
-            if (!BND || nb >= 0) interface_node_flux<N, SC>(a, f < 2 ? 1 : 2, plus ? e : nb, plus ? nb : e, l, dt, Fn);
+            if (!BND || nb >= 0)
+                interface_node_flux<N, SC, true>(a, f < 2 ? 1 : 2, plus ? e : nb, plus ? nb : e, l, dt, Fn);
             else boundary_node_flux<N>(bnd, -nb - 1, e, f + 1, l, Fn);
 #pragma unroll
             for (int v = 0; v < NV; ++v) sF[tid * NV + v] = Fn[v];
@@ -369,7 +375,7 @@ static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? TLW_
     __syncthreads();
     double l1 = 0.0, l2 = 0.0;
     if (has2) {
-        if (!TLW_SURF_PREFETCH) load4_rw(o2, x);
+        if (!TLW_SURF_PREFETCH) load4w_rw(o2, x);
         const double dt = a.inst ? a.dt[__ldg(a.inst + e2)] : *a.dt;
         const double dts = a.step_mode ? dt : 1.0;
         const double ij = __ldg(a.inv_jac + e2);
@@ -388,7 +394,7 @@ static __global__ void __launch_bounds__(SurfCfg<N>::THREADS, (BND || SC) ? TLW_
 #pragma unroll
             for (int v = 0; v < NV; ++v) x[v] = fma(s, p[v], x[v]);
         }
-        store4(o2, x);
+        store4w(o2, x);
         if (a.cfl_slots) node_speeds(a.gamma, x, a.status, l1, l2);
     }
     if (a.cfl_slots && 32 % NB == 0) {
