@@ -384,7 +384,7 @@ const char* tlw_last_error(tlw_handle* h);
  * reference's Julia rhs! allocates nothing per call because its caches are built once; this entry point
  * gives a caller whose device memory is owned by another pool, or who cannot accept cudaMalloc's implicit
  * synchronisation, the same rhs without a handle). Periodic TreeMesh{2} only (no boundaries, no mortars).
- * All pointers are device pointers, 16-byte aligned: u, du [v, i, j, element]; inverse_jacobian
+ * All pointers are device pointers; u and du 32-byte aligned (TLW_E_ARG otherwise): u, du [v, i, j, element]; inverse_jacobian
  * [element]; x_left/x_right, y_left/y_right the 0-based element ids of the x- and y-oriented interfaces.
  * The face-trace scratch is a static device array of TLW_NOALLOC_SCRATCH_BYTES: meshes with
  * n_elements * 2 * 4 * (N+1) * 4 * 8 bytes of traces beyond it are rejected with TLW_E_ARG. Calls on a

@@ -113,7 +113,7 @@ extern "C" int tlw_rhs_lw_noalloc(int32_t polydeg, double gamma, int32_t surface
     const int n = polydeg + 1;
     const size_t trace_doubles = (size_t)NV * n * 4 * (size_t)n_elements;
     if (2 * trace_doubles * sizeof(double) > kScratchBytes) return TLW_E_ARG;   // mesh too large for the scratch
-    if (((uintptr_t)u | (uintptr_t)du) % 16 != 0) return TLW_E_ARG;             // 16-byte vector loads/stores
+    if (((uintptr_t)u | (uintptr_t)du) % 32 != 0) return TLW_E_ARG;             // 32-byte node records
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return TLW_E_CUDA;
     int rc = setup_device(dev);

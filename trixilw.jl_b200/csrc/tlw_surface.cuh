@@ -147,7 +147,7 @@ static __global__ void __launch_bounds__(256) interface_kernel(SurfArgs a) {
     const int nodeR = a.orientation == 1 ? n * l : l;
     const double dt = a.inst ? a.dt[__ldg(a.inst + le)] : *a.dt;
     double Fn[NV];
-    interface_node_flux<N>(a, a.orientation, le, re, l, dt, Fn);
+    interface_node_flux<N, true, true>(a, a.orientation, le, re, l, dt, Fn);
     const double dts = a.step_mode ? dt : 1.0;
     const double sL = -__ldg(a.inv_jac + le) * a.inv_w_last * dts;
     const double sR = __ldg(a.inv_jac + re) * a.inv_w_first * dts;
@@ -157,19 +157,19 @@ static __global__ void __launch_bounds__(256) interface_kernel(SurfArgs a) {
     const bool slots = a.cfl_slots && (a.orientation == 2 || (l > 0 && l < n - 1));
     const int sL_slot = a.orientation == 1 ? 2 : 4, sR_slot = a.orientation == 1 ? 1 : 3;
     double x[NV], l1, l2;
-    load4_rw(oL, x);
+    load4w_rw(oL, x);
 #pragma unroll
     for (int v = 0; v < NV; ++v) x[v] = fma(sL, Fn[v], x[v]);
-    store4(oL, x);
+    store4w(oL, x);
     if (slots) {
         node_speeds(a.gamma, x, a.status, l1, l2);
         atomicMax(a.cfl_slots + (size_t)le * CFL_SLOTS + 2 * sL_slot, (unsigned long long)__double_as_longlong(l1));
         atomicMax(a.cfl_slots + (size_t)le * CFL_SLOTS + 2 * sL_slot + 1, (unsigned long long)__double_as_longlong(l2));
     }
-    load4_rw(oR, x);
+    load4w_rw(oR, x);
 #pragma unroll
     for (int v = 0; v < NV; ++v) x[v] = fma(sR, Fn[v], x[v]);
-    store4(oR, x);
+    store4w(oR, x);
     if (slots) {
         node_speeds(a.gamma, x, a.status, l1, l2);
         atomicMax(a.cfl_slots + (size_t)re * CFL_SLOTS + 2 * sR_slot, (unsigned long long)__double_as_longlong(l1));
