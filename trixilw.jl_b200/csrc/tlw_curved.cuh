@@ -262,17 +262,18 @@ static __global__ void __launch_bounds__(128) curved_interface_kernel(CurvedSurf
     const int np = face_node_index(n, pf, l), ns = face_node_index(n, sf, ls);
     const double sgP = (pf & 1) ? 1.0 : -1.0, sgS = (sf & 1) ? 1.0 : -1.0;
     double uP[NV], uS[NV], UP[NV], US[NV], FP[NV], FS[NV], Fn[NV], J[4];
-    load4(a.u + ((size_t)pe * nn + np) * NV, uP);
-    load4(a.u + ((size_t)se * nn + ns) * NV, uS);
+    // (node records, traces and metrics move as one 256-bit access each)
+    load4w(a.u + ((size_t)pe * nn + np) * NV, uP);
+    load4w(a.u + ((size_t)se * nn + ns) * NV, uS);
     const size_t tp = (((size_t)pe * 4 + pf) * n + l) * NV, ts = (((size_t)se * 4 + sf) * n + ls) * NV;
-    load4(a.tU + tp, UP);
-    load4(a.tU + ts, US);
+    load4w(a.tU + tp, UP);
+    load4w(a.tU + ts, US);
     if (a.tG) {
         unstructured_interface_flux<N>(a, pe, se, pf, sf, l, ls, np, uP, uS, UP, US, Fn);
     } else {
-        load4(a.tF + tp, FP);
-        load4(a.tF + ts, FS);
-        load4(a.metrics + ((size_t)pe * nn + np) * 4, J);
+        load4w(a.tF + tp, FP);
+        load4w(a.tF + ts, FS);
+        load4w(a.metrics + ((size_t)pe * nn + np) * 4, J);
         const double nrm[2] = {sgP * (pf < 2 ? J[0] : J[2]), sgP * (pf < 2 ? J[1] : J[3])};
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
@@ -297,14 +298,14 @@ static __global__ void __launch_bounds__(128) curved_interface_kernel(CurvedSurf
     double* oP = a.out + ((size_t)pe * nn + np) * NV;
     double* oS = a.out + ((size_t)se * nn + ns) * NV;
     double x[NV];
-    load4_rw(oP, x);
+    load4w_rw(oP, x);
 #pragma unroll
     for (int v = 0; v < NV; ++v) x[v] = fma(cP, Fn[v], x[v]);
-    store4(oP, x);
-    load4_rw(oS, x);
+    store4w(oP, x);
+    load4w_rw(oS, x);
 #pragma unroll
     for (int v = 0; v < NV; ++v) x[v] = fma(cS, Fn[v], x[v]);
-    store4(oS, x);
+    store4w(oS, x);
 }
 
 // Boundary faces of a curvilinear mesh: the LW slip walls in their normal-direction form
