@@ -636,6 +636,8 @@ def run_ours(args):
                      else volume_flops_per_node(N) * ndofs)
         tag = (f"par_volume_kernel_N{N}_cavity{1 << level}" if ns
                else f"lw_volume_kernel_N{N}_blast_muscl{1 << level}" if icname == "blast"
+               else f"mdrk_volume_kernels_N{N}_{'warped' if curved else 'tree'}{1 << level}" if td == "mdrk"
+               else f"lw_volume_kernel_sc_N{N}_tree{1 << level}" if sc
                else f"lw_volume_kernel_N{N}_{'warped' if curved else 'tree'}{1 << level}")
         traffic = profile_traffic(tag)
         step_alg = alg_bytes_per_element_step(N, td, curved) * E
@@ -683,6 +685,9 @@ def run_ours(args):
                              "frac": e2e / (ndofs / (link["both_ms"] * 1e-3))}},
             "roofline": {"kernel": (f"grad_volume_kernel + curved_grad_*_kernel + par_volume_kernel<{N}, MODE_STEP, CURVED>"
                                     if ns else f"lw_volume_kernel<{N}, MODE_STEP, SC, CURVED, MUSCL>" if icname == "blast"
+                                    else (f"mdrk1_volume_kernel<{N}, MODE_STEP{', CURVED' if curved else ', compact'}> + "
+                                          f"mdrk2_volume_kernel<{N}, MODE_STEP{', CURVED' if curved else ', compact'}>")
+                                    if td == "mdrk"
                                     else f"lw_volume_kernel<{N}, MODE_STEP{', SC' if sc else ''}{', CURVED' if curved else ''}>"),
                          "bound": "fp64" if fp64_bound else "hbm",
                          "achieved": binding["achieved"], "peak": binding["peak"], "unit": binding["unit"],
