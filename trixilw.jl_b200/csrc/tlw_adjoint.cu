@@ -38,6 +38,20 @@ using namespace tlw;
 
 namespace {
 
+// The adjoint kernels read and write the library's own arrays (segment states and traces, the adjoint states, the
+// face-trace adjoints), whose node records are 32-byte aligned: one 256-bit access per record.
+#ifndef TLW_ADJ_WIDE
+#define TLW_ADJ_WIDE 1
+#endif
+__device__ __forceinline__ void aload4(const double* p, double* x) {
+    if (TLW_ADJ_WIDE) load4w(p, x);
+    else load4(p, x);
+}
+__device__ __forceinline__ void astore4(double* p, const double* x) {
+    if (TLW_ADJ_WIDE) store4w(p, x);
+    else store4(p, x);
+}
+
 int afail(tlw_handle* h, int code, const std::string& msg) {
     if (h) h->err = msg;
     return code;
@@ -156,12 +170,12 @@ static __global__ void __launch_bounds__(128) adj_interface_kernel(AdjSurfArgs a
     if (orientation == 1) { nodeL = (n - 1) + n * l; nodeR = n * l; faceL = 1; faceR = 0; }
     else { nodeL = l + n * (n - 1); nodeR = l; faceL = 3; faceR = 2; }
     double uL[NV], uR[NV], UL[NV], UR[NV], lL[NV], lR[NV];
-    load4(a.u + ((size_t)le * n * n + nodeL) * NV, uL);
-    load4(a.u + ((size_t)re * n * n + nodeR) * NV, uR);
-    load4(a.tU + (((size_t)le * 4 + faceL) * n + l) * NV, UL);
-    load4(a.tU + (((size_t)re * 4 + faceR) * n + l) * NV, UR);
-    load4(a.lam + ((size_t)le * n * n + nodeL) * NV, lL);
-    load4(a.lam + ((size_t)re * n * n + nodeR) * NV, lR);
+    aload4(a.u + ((size_t)le * n * n + nodeL) * NV, uL);
+    aload4(a.u + ((size_t)re * n * n + nodeR) * NV, uR);
+    aload4(a.tU + (((size_t)le * 4 + faceL) * n + l) * NV, UL);
+    aload4(a.tU + (((size_t)re * 4 + faceR) * n + l) * NV, UR);
+    aload4(a.lam + ((size_t)le * n * n + nodeL) * NV, lL);
+    aload4(a.lam + ((size_t)re * n * n + nodeR) * NV, lR);
     const double dt = *a.dt;
     const double sL = -dt * __ldg(a.inv_jac + le) * a.inv_w_last;
     const double sR = dt * __ldg(a.inv_jac + re) * a.inv_w_first;
@@ -180,14 +194,14 @@ static __global__ void __launch_bounds__(128) adj_interface_kernel(AdjSurfArgs a
         blam -= 0.5 * bFn[v] * (uR[v] - uL[v]);
         o[v] = 0.5 * bFn[v];
     }
-    store4(a.bF + tl, o);
-    store4(a.bF + tr, o);
+    astore4(a.bF + tl, o);
+    astore4(a.bF + tr, o);
 #pragma unroll
     for (int v = 0; v < NV; ++v) o[v] = 0.5 * lambda * bFn[v];
-    store4(a.bu + tl, o);
+    astore4(a.bu + tl, o);
 #pragma unroll
     for (int v = 0; v < NV; ++v) o[v] = -o[v];
-    store4(a.bu + tr, o);
+    astore4(a.bu + tr, o);
     // speed adjoint goes to the side whose |v| (and c) the max selected; the left argument wins ties
     double gL[NV], gR[NV];
     if (a.speed_kind == 0) {
@@ -208,8 +222,8 @@ static __global__ void __launch_bounds__(128) adj_interface_kernel(AdjSurfArgs a
             gR[v] = wR * (dvR[v] + dcR[v]);
         }
     }
-    store4(a.bU + tl, gL);
-    store4(a.bU + tr, gR);
+    astore4(a.bU + tl, gL);
+    astore4(a.bU + tr, gR);
 }
 
 template <int N>
@@ -276,7 +290,7 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
     double u[NV] = {1.0, 0.0, 0.0, 2.5};
     double ij = 1.0;
     if (active) {
-        load4(a.u + ((size_t)e * nn + node) * NV, u);
+        aload4(a.u + ((size_t)e * nn + node) * NV, u);
         ij = __ldg(a.inv_jac + e);
     }
     const double dt = *a.dt;
@@ -372,7 +386,7 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
     double bF[NV], bG[NV], bU[NV] = {0.0, 0.0, 0.0, 0.0}, bud[NV] = {0.0, 0.0, 0.0, 0.0};
     {
         double lam[NV] = {0.0, 0.0, 0.0, 0.0};
-        if (active) load4(a.lam + ((size_t)e * nn + node) * NV, lam);
+        if (active) aload4(a.lam + ((size_t)e * nn + node) * NV, lam);
 #pragma unroll
         for (int v = 0; v < NV; ++v) put(X, v, sc * lam[v]);
     }
@@ -383,13 +397,13 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
         auto face = [&](int f, int l, double* tgt) {
             const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
             double x[NV];
-            load4(a.bF + t, x);
+            aload4(a.bF + t, x);
 #pragma unroll
             for (int v = 0; v < NV; ++v) tgt[v] += x[v];
-            load4(a.bU + t, x);
+            aload4(a.bU + t, x);
 #pragma unroll
             for (int v = 0; v < NV; ++v) bU[v] += x[v];
-            load4(a.bu + t, x);
+            aload4(a.bu + t, x);
 #pragma unroll
             for (int v = 0; v < NV; ++v) bud[v] += x[v];
         };
@@ -455,10 +469,10 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, AdjCfg<N>::MIN_BLOC
     euler_flux_vjp(a.gamma, u, bf0, bg0, bu);
     if (active) {
         double lam[NV], o[NV];
-        load4(a.lam + ((size_t)e * nn + node) * NV, lam);
+        aload4(a.lam + ((size_t)e * nn + node) * NV, lam);
 #pragma unroll
         for (int v = 0; v < NV; ++v) o[v] = lam[v] + bu[v] + bud[v];
-        store4(a.lam_out + ((size_t)e * nn + node) * NV, o);
+        astore4(a.lam_out + ((size_t)e * nn + node) * NV, o);
     }
 }
 
@@ -502,14 +516,14 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_re
         for (int v = 0; v < NV; ++v) dm[m][v] = 0.0;
     double lam[NV] = {0.0, 0.0, 0.0, 0.0};
     if (active) {
-        load4(a.u + ((size_t)e * nn + node) * NV, u);
+        aload4(a.u + ((size_t)e * nn + node) * NV, u);
         ij = __ldg(a.inv_jac + e);
         if (DREG) {
 #pragma unroll
             for (int m = 0; m < DEPTH; ++m)
                 for (int v = 0; v < NV; ++v) dm[DREG ? m : 0][v] = a.dstore[((size_t)m * a.E + e) * NV * nn + v * nn + node];
         }
-        load4(a.lam + ((size_t)e * nn + node) * NV, lam);
+        aload4(a.lam + ((size_t)e * nn + node) * NV, lam);
     }
     if (!DREG) {
 #pragma unroll
@@ -556,13 +570,13 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_re
         auto face = [&](int f, int l, double* tgt) {
             const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
             double x[NV];
-            load4(a.bF + t, x);
+            aload4(a.bF + t, x);
 #pragma unroll
             for (int v = 0; v < NV; ++v) tgt[v] += x[v];
-            load4(a.bU + t, x);
+            aload4(a.bU + t, x);
 #pragma unroll
             for (int v = 0; v < NV; ++v) bU[v] += x[v];
-            load4(a.bu + t, x);
+            aload4(a.bu + t, x);
 #pragma unroll
             for (int v = 0; v < NV; ++v) bud[v] += x[v];
         };
@@ -639,7 +653,7 @@ static __global__ void __launch_bounds__(AdjCfg<N>::THREADS, MINB) adj_volume_re
         double o[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) o[v] = lam[v] + bu[v] + bud[v];
-        store4(a.lam_out + ((size_t)e * nn + node) * NV, o);
+        astore4(a.lam_out + ((size_t)e * nn + node) * NV, o);
     }
 }
 
@@ -740,7 +754,7 @@ static __global__ void __launch_bounds__(AdjMdrkCfg<N>::THREADS, AdjMdrkCfg<N>::
     double ij = 1.0;
     const size_t off = (size_t)e * nn + node;
     if (active) {
-        load4(a.x + off * NV, x);
+        aload4(a.x + off * NV, x);
         ij = __ldg(a.inv_jac + e);
     }
     const double dt = *a.dt;
@@ -760,7 +774,7 @@ static __global__ void __launch_bounds__(AdjMdrkCfg<N>::THREADS, AdjMdrkCfg<N>::
     __syncthreads();
     // adjoint of the volume term sc (Dhat F + Dhat G), then the face traces
     double lam[NV] = {0.0, 0.0, 0.0, 0.0};
-    if (active) load4(a.lam + off * NV, lam);
+    if (active) aload4(a.lam + off * NV, lam);
 #pragma unroll
     for (int v = 0; v < NV; ++v) put(X, v, sc * lam[v]);
     __syncthreads();
@@ -771,13 +785,13 @@ static __global__ void __launch_bounds__(AdjMdrkCfg<N>::THREADS, AdjMdrkCfg<N>::
         auto face = [&](int f, int l, double* tgt) {
             const size_t t = (((size_t)e * 4 + f) * n + l) * NV;
             double y[NV];
-            load4(a.bF + t, y);
+            aload4(a.bF + t, y);
 #pragma unroll
             for (int v = 0; v < NV; ++v) tgt[v] += y[v];
-            load4(a.bU + t, y);
+            aload4(a.bU + t, y);
 #pragma unroll
             for (int v = 0; v < NV; ++v) bU[v] += y[v];
-            load4(a.bu + t, y);
+            aload4(a.bu + t, y);
 #pragma unroll
             for (int v = 0; v < NV; ++v) bud[v] += y[v];
         };
@@ -798,21 +812,21 @@ static __global__ void __launch_bounds__(AdjMdrkCfg<N>::THREADS, AdjMdrkCfg<N>::
             bf0[v] = bg0[v] = bx[v] = 0.0;
         }
         if (active) {
-            store4(a.bF2 + off * 2 * NV, bF);
-            store4(a.bF2 + off * 2 * NV + NV, bG);
-            store4(a.bU2 + off * NV, bU);
+            astore4(a.bF2 + off * 2 * NV, bF);
+            astore4(a.bF2 + off * 2 * NV + NV, bG);
+            astore4(a.bU2 + off * NV, bU);
             double acc[NV];
 #pragma unroll
             for (int v = 0; v < NV; ++v) acc[v] = lam[v] + bud[v];
-            store4(a.lam_acc + off * NV, acc);
+            astore4(a.lam_acc + off * NV, acc);
         }
     } else {
         // Fh = f/2 + f_t/8, Uh = x/2 + d/8; F2 = f + f_t/6, U2 = x + d/6
         double b2f[NV] = {0.0, 0.0, 0.0, 0.0}, b2g[NV] = {0.0, 0.0, 0.0, 0.0}, b2u[NV] = {0.0, 0.0, 0.0, 0.0};
         if (active) {
-            load4(a.bF2 + off * 2 * NV, b2f);
-            load4(a.bF2 + off * 2 * NV + NV, b2g);
-            load4(a.bU2 + off * NV, b2u);
+            aload4(a.bF2 + off * 2 * NV, b2f);
+            aload4(a.bF2 + off * 2 * NV + NV, b2g);
+            aload4(a.bU2 + off * NV, b2u);
         }
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
@@ -855,11 +869,11 @@ static __global__ void __launch_bounds__(AdjMdrkCfg<N>::THREADS, AdjMdrkCfg<N>::
             for (int v = 0; v < NV; ++v) o[v] = bx[v];
         } else {
             double acc[NV];
-            load4(a.lam_acc + off * NV, acc);
+            aload4(a.lam_acc + off * NV, acc);
 #pragma unroll
             for (int v = 0; v < NV; ++v) o[v] = acc[v] + lam[v] + bx[v] + bud[v];
         }
-        store4(a.out + off * NV, o);
+        astore4(a.out + off * NV, o);
     }
 }
 
@@ -873,7 +887,7 @@ static __global__ void __launch_bounds__(OBJ_THREADS) objective_kernel(const dou
     if (k < nodes) {
         r = u[k * NV] - target[k];
         double o[NV] = {r, 0.0, 0.0, 0.0};
-        store4(lam + k * NV, o);
+        astore4(lam + k * NV, o);
     }
     red[threadIdx.x] = 0.5 * r * r;
     __syncthreads();
