@@ -427,8 +427,8 @@ static __global__ void __launch_bounds__(MS_THREADS) curved_max_speed_kernel(con
     for (int k = threadIdx.x; k < ne * nn; k += MS_THREADS) {
         const size_t node = (size_t)e0 * nn + k;
         double x[NV], J[4];
-        load4(u + node * NV, x);
-        load4(metrics + node * 4, J);
+        load4w(u + node * NV, x);
+        load4w(metrics + node * 4, J);
         const double ir = 1.0 / x[0];
         const double v1 = x[1] * ir, v2 = x[2] * ir;
         const double p = gm1 * (x[3] - 0.5 * (x[1] * v1 + x[2] * v2));

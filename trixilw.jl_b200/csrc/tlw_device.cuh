@@ -201,8 +201,8 @@ __device__ __forceinline__ void store4(double* p, const double* x) {
     reinterpret_cast<double2*>(p)[1] = make_double2(x[2], x[3]);
 }
 // One 256-bit access per 4-double node record (global memory only; the record 32-byte aligned): the surface
-// pass, the interface sweeps and the curvilinear interfaces, whose arrays are the library's own or were checked
-// by the entry point.
+// pass, the interface sweeps, the curvilinear interfaces, the CFL / indicator passes and the adjoint kernels,
+// whose arrays are the library's own or were checked (or copied) by the entry point.
 __device__ __forceinline__ void load4w(const double* __restrict__ p, double* x) {
     asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(x[0]), "=d"(x[1]), "=d"(x[2]), "=d"(x[3]) : "l"(p));
 }

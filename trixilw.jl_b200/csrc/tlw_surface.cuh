@@ -484,7 +484,7 @@ static __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const doub
     const double gm1 = gamma - 1.0;
     for (int k = threadIdx.x; k < ne * nn; k += MS_THREADS) {
         double x[NV];
-        load4(u + ((size_t)e0 * nn + k) * NV, x);
+        load4w(u + ((size_t)e0 * nn + k) * NV, x);
         if (SPEED) node_speeds(gamma, x, &s->status, l1s[k], l2s[k]);
         // indicator variable density_pressure = (gamma - 1)(rho rho_e - |rho v|^2 / 2)
         if (IND) inds[k] = gm1 * (x[0] * x[3] - 0.5 * (x[1] * x[1] + x[2] * x[2]));
