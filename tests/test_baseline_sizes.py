@@ -6,6 +6,8 @@ multithreaded oracle on the full meshes, not on reduced ones.
 * four-quadrant Riemann problem on [0, 1]^2, TreeMesh 512 x 512, N = 4, Hennemann-Gassner blending
   (alpha_max = 0.5) with first-order subcells and Dirichlet(initial condition) boundaries: one rhs with the
   blending factors and the subcell fluxes next to the faces (fn_low), then 3 device steps;
+* the curvilinear bench workloads on the warped 512 x 512 StructuredMesh, N = 4: the LW vortex and the
+  shock-capturing blast with MUSCL subcells, 2 device steps;
 * the warped 64 x 64 Navier-Stokes lid-driven cavity (Re = 1000, Ma = 0.1, Pr = 0.72, N = 4, slip walls for
   the advective part, no-slip adiabatic walls with the lid at v1 = 1): 20 steps at the workload's fixed dt.
 
@@ -137,3 +139,31 @@ def test_warped_cavity_64_N4_steps(tl, oracle_mod):
     assert s == 20
     assert np.all(rel_l2(u_gpu, u_cpu) < RTOL), rel_l2(u_gpu, u_cpu)
     assert np.all(rel_l2(u_gpu, u0) > 1e-9)
+
+
+def _bench():
+    """bench.py's workload builders (the same meshes, initial conditions and CFL numbers as the timed runs)."""
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    import bench
+    return bench
+
+
+@pytest.mark.parametrize("icname", ["warped", "blast"])
+def test_curvilinear_512_bench_workloads_steps(tl, oracle_mod, icname):
+    """The curvilinear throughput workloads at their own size (warped 512 x 512 StructuredMesh, N = 4): the LW
+    vortex and the shock-capturing blast with MUSCL subcells, 2 device CFL steps against the oracle."""
+    bench = _bench()
+    semi = bench.build_semi(tl, 9, 4, "lw", icname, 0)
+    u0 = semi.compute_coefficients(0.0)
+    cfl = bench.RIEMANN_CFL if icname == "blast" else bench.cfl_for(4)
+    u_gpu, integ = device_steps(tl, semi, u0, 2, cfl)
+    o = oracle_mod.Oracle(bench.make_mesh(tl, 9, icname), 4)
+    if icname == "blast":
+        o.set_shock_capturing(True, 0.5, 0.001, True, reconstruction=1)
+    u_cpu = u0.copy()
+    s, t = o.steps(u_cpu, 2, cfl, 0.0, 1e9, nthreads=NTH)
+    assert s == integ.iter == 2 and integ.t == pytest.approx(t, rel=1e-13)
+    assert np.all(rel_l2(u_gpu, u_cpu) < RTOL), rel_l2(u_gpu, u_cpu)
