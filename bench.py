@@ -701,7 +701,7 @@ def run_ours(args):
                          "phase_ms_per_step": phases_rec,
                          **({"surface": surf_rec} if surf_rec else {})},
             "clocks": clocks,
-            "gpu_launches": args.steps * ((9 + 2 * int(L.tlw_curved_colors(semi.handle))) if ns else
+            "gpu_launches": args.steps * ((8 + 2 * int(L.tlw_curved_colors(semi.handle))) if ns else
                                           (5 + int(L.tlw_curved_colors(semi.handle))) if icname == "blast" else
                                           (2 + 2 * stages + (1 if icname == "riemann" else 0))),
         }

@@ -273,11 +273,9 @@ struct LaunchImpl {
             const int E = (int)h->E;
             const int grid = (E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS;
             if (h->curved) {
-                // the CFL maximum of the curvilinear max_dt, then the parabolic max_dt's own maxima
-                curved_max_speed_kernel<N><<<grid, MS_THREADS, 0, s>>>(u, h->d_Ja, h->d_ijn, E, h->opts.gamma,
-                                                                        h->d_step);
-                par_speed_kernel<N><<<grid, MS_THREADS, 0, s>>>(u, h->d_ijn, E, ns_params(h), h->d_step, h->d_visc,
-                                                                 h->d_visc + 1);
+                // the CFL maximum of the curvilinear max_dt and the parabolic max_dt's own maxima, one pass
+                curved_par_speed_kernel<N><<<grid, MS_THREADS, 0, s>>>(u, h->d_Ja, h->d_ijn, E, ns_params(h),
+                                                                        h->d_step, h->d_visc, h->d_visc + 1);
             } else {
                 par_speed_kernel<N><<<grid, MS_THREADS, 0, s>>>(u, h->d_inv_jac, E, ns_params(h), h->d_step,
                                                                  h->d_visc, &h->d_step->max_bits);

@@ -569,6 +569,80 @@ static __global__ void __launch_bounds__(MS_THREADS) par_speed_kernel(const doub
     }
 }
 
+// Curvilinear Navier-Stokes: curved_max_speed_kernel's CFL maximum (into s->max_bits) and par_speed_kernel's
+// parabolic maxima (adv_bits, visc_bits; inv_jac_lin read by the element-linear index, as that kernel reads it)
+// in one pass over u, with the same operations for each.
+template <int N>
+static __global__ void __launch_bounds__(MS_THREADS) curved_par_speed_kernel(const double* __restrict__ u,
+                                                                             const double* __restrict__ metrics,
+                                                                             const double* __restrict__ inv_jac,
+                                                                             int E, NSParams ns, StepState* s,
+                                                                             unsigned long long* visc_bits,
+                                                                             unsigned long long* adv_bits) {
+    constexpr int n = N + 1, nn = n * n;
+    constexpr int ELEMS = MsCfg<N>::ELEMS;
+    __shared__ double c1s[ELEMS * nn], c2s[ELEMS * nn], l1s[ELEMS * nn], l2s[ELEMS * nn];
+    __shared__ double wmax[MS_THREADS / 32], wadv[MS_THREADS / 32], wvis[MS_THREADS / 32];
+    const int e0 = blockIdx.x * ELEMS;
+    const int ne = min(ELEMS, E - e0);
+    const double gm1 = ns.gamma - 1.0;
+    double vis = 0.0;
+    for (int k = threadIdx.x; k < ne * nn; k += MS_THREADS) {
+        const size_t node = (size_t)e0 * nn + k;
+        double x[NV], J[4];
+        load4w(u + node * NV, x);
+        load4w(metrics + node * 4, J);
+        const double ir = 1.0 / x[0];
+        const double v1 = x[1] * ir, v2 = x[2] * ir;
+        const double p = gm1 * (x[3] - 0.5 * (x[1] * v1 + x[2] * v2));
+        const double c = checked_sqrt(ns.gamma * p * ir, &s->status);
+        const double l1 = fabs(v1) + c, l2 = fabs(v2) + c;
+        const double ijn = fabs(__ldg(inv_jac + node));
+        c1s[k] = fabs(J[0] * l1 + J[1] * l2) * ijn;
+        c2s[k] = fabs(J[2] * l1 + J[3] * l2) * ijn;
+        l1s[k] = l1;
+        l2s[k] = l2;
+        const double ij = __ldg(inv_jac + e0 + k / nn);
+        vis = fmax(vis, ij * ij * fmax(4.0 * ns.mu / (3.0 * x[0]), ns.mu * ns.kappa / (x[0] * ns.Pr)));
+    }
+    __syncthreads();
+    double m = 0.0, ma = 0.0;
+    if (threadIdx.x < ne) {
+        double m1 = 0.0, m2 = 0.0, ml1 = 0.0, ml2 = 0.0;
+        for (int k = 0; k < nn; ++k) {
+            m1 = fmax(m1, c1s[threadIdx.x * nn + k]);
+            m2 = fmax(m2, c2s[threadIdx.x * nn + k]);
+            ml1 = fmax(ml1, l1s[threadIdx.x * nn + k]);
+            ml2 = fmax(ml2, l2s[threadIdx.x * nn + k]);
+        }
+        m = m1 + m2;
+        ma = __ldg(inv_jac + e0 + threadIdx.x) * (ml1 + ml2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+        vis = fmax(vis, __shfl_xor_sync(0xffffffffu, vis, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        wmax[threadIdx.x >> 5] = m;
+        wadv[threadIdx.x >> 5] = ma;
+        wvis[threadIdx.x >> 5] = vis;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = wmax[0], ba = wadv[0], bv = wvis[0];
+        for (int w = 1; w < MS_THREADS / 32; ++w) {
+            b = fmax(b, wmax[w]);
+            ba = fmax(ba, wadv[w]);
+            bv = fmax(bv, wvis[w]);
+        }
+        if (b > 0.0) atomicMax(&s->max_bits, (unsigned long long)__double_as_longlong(b));
+        if (ba > 0.0) atomicMax(adv_bits, (unsigned long long)__double_as_longlong(ba));
+        if (bv > 0.0) atomicMax(visc_bits, (unsigned long long)__double_as_longlong(bv));
+    }
+}
+
 // dt = min(cfl 2 / (n lam_a), cfl / ((lam_a' + 2 (2N + 1) lam_v) 2 (2N + 1))), then the set_dt! clamp;
 // lam_a' = lam_a on a TreeMesh, visc_bits[1] (the parabolic max_dt's own advective maximum) when curved
 static __global__ void par_finalize_dt_kernel(StepState* s, unsigned long long* visc_bits, int N, int curved = 0) {
