@@ -183,8 +183,13 @@ IndicatorArgs indicator_args(tlw_handle* h) {
 
 // alpha of u (indicator + smoothing); with `speed` the same pass also feeds the CFL reduction
 void enqueue_indicator(tlw_handle* h, const double* u, bool speed) {
+    IndicatorArgs ia = indicator_args(h);
+    if (speed && h->curved) {   // the curvilinear CFL speeds in the same pass
+        ia.metrics = h->d_Ja;
+        ia.inv_jac_node = h->d_ijn;
+    }
     dispatch<Spd>(h->N, h->stream, u, (const double*)h->d_inv_jac, (int)h->E, h->opts.gamma, h->d_step, speed, true,
-                  indicator_args(h));
+                  ia);
     // interfaces for the smoothing: the TreeMesh list, or the curvilinear mesh's (primary, secondary) pairs
     const int ni = h->curved ? (h->color_off.empty() ? 0 : h->color_off.back()) : h->ni;
     if (h->opts.alpha_smooth && ni > 0)
@@ -610,10 +615,6 @@ void enqueue_step(tlw_handle* h, int from, cudaEvent_t after_dt = nullptr, const
         // the previous step left the per-element maxima of this state
         const int grid = std::min<int>((int)((h->E + 255) / 256), 4 * 148);
         cfl_slots_reduce_kernel<<<grid, 256, 0, h->stream>>>(h->d_slots, h->d_inv_jac, (int)h->E, h->d_step);
-    } else if (h->sc && h->curved) {
-        dispatch<CSpd>(h->N, h->stream, u, (const double*)h->d_Ja, (const double*)h->d_ijn, (int)h->E, h->opts.gamma,
-                       h->d_step);
-        enqueue_indicator(h, u, false);
     } else if (h->sc) enqueue_indicator(h, u, true);   // CFL reduction and indicator in one pass over u
     else if (h->parabolic) dispatch<ParSpd>(h->N, h->stream, (const tlw_handle*)h, u);   // (curvilinear too)
     else if (h->curved) dispatch<CSpd>(h->N, h->stream, u, (const double*)h->d_Ja, (const double*)h->d_ijn, (int)h->E,

@@ -319,7 +319,8 @@ struct LaunchImpl {
                           bool speed, bool ind, const IndicatorArgs& ia, BatchSpeedArgs bs = BatchSpeedArgs{}) {
         if (E == 0) return;
         const int grid = (E + MsCfg<N>::ELEMS - 1) / MsCfg<N>::ELEMS;
-        if (speed && ind) max_speed_kernel<N, true, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
+        if (speed && ind && ia.metrics) max_speed_kernel<N, true, true, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
+        else if (speed && ind) max_speed_kernel<N, true, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
         else if (speed) max_speed_kernel<N, true, false><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
         else if (ind) max_speed_kernel<N, false, true><<<grid, MS_THREADS, 0, s>>>(u, ij, E, gamma, st, ia, bs);
     }

@@ -454,6 +454,9 @@ struct IndicatorArgs {
     double* alpha_raw;       // [e] indicator before smoothing
     double* alpha;           // [e] blending factor (smoothed afterwards)
     double alpha_max, alpha_min, threshold, parameter_s;
+    // curvilinear meshes: the CFL speeds of the same pass take the node's metrics and J^{-1} (null on a TreeMesh)
+    const double* metrics;
+    const double* inv_jac_node;
 };
 
 // One pass over u for the CFL reduction (SPEED) and/or the Hennemann-Gassner indicator (IND).
@@ -468,7 +471,9 @@ struct BatchSpeedArgs {
     unsigned long long* inst_max;   // [instance] bits of the max scaled speed
 };
 
-template <int N, bool SPEED, bool IND>
+// CSPEED (curvilinear meshes): the speeds of curved_max_speed_kernel, |Ja^d . (l1, l2)| |J^{-1}| per node, and the
+// element's value max l1 + max l2 without the element J^{-1}
+template <int N, bool SPEED, bool IND, bool CSPEED = false>
 static __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const double* __restrict__ u,
                                                                const double* __restrict__ inv_jac, int E,
                                                                double gamma, StepState* s, IndicatorArgs ia,
@@ -485,7 +490,17 @@ static __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const doub
     for (int k = threadIdx.x; k < ne * nn; k += MS_THREADS) {
         double x[NV];
         load4w(u + ((size_t)e0 * nn + k) * NV, x);
-        if (SPEED) node_speeds(gamma, x, &s->status, l1s[k], l2s[k]);
+        if (SPEED && CSPEED) {
+            const size_t node = (size_t)e0 * nn + k;
+            double J[4], l1, l2;
+            load4w(ia.metrics + node * 4, J);
+            node_speeds(gamma, x, &s->status, l1, l2);
+            const double ij = fabs(__ldg(ia.inv_jac_node + node));
+            l1s[k] = fabs(J[0] * l1 + J[1] * l2) * ij;
+            l2s[k] = fabs(J[2] * l1 + J[3] * l2) * ij;
+        } else if (SPEED) {
+            node_speeds(gamma, x, &s->status, l1s[k], l2s[k]);
+        }
         // indicator variable density_pressure = (gamma - 1)(rho rho_e - |rho v|^2 / 2)
         if (IND) inds[k] = gm1 * (x[0] * x[3] - 0.5 * (x[1] * x[1] + x[2] * x[2]));
     }
@@ -497,7 +512,7 @@ static __global__ void __launch_bounds__(MS_THREADS) max_speed_kernel(const doub
             ml1 = fmax(ml1, l1s[threadIdx.x * nn + k]);
             ml2 = fmax(ml2, l2s[threadIdx.x * nn + k]);
         }
-        m = __ldg(inv_jac + e0 + threadIdx.x) * (ml1 + ml2);
+        m = CSPEED ? ml1 + ml2 : __ldg(inv_jac + e0 + threadIdx.x) * (ml1 + ml2);
     }
     if (IND) {
         const int el = threadIdx.x >> 3, q = threadIdx.x & 7;
