@@ -297,17 +297,18 @@ static __global__ void __launch_bounds__(128) boundary_kernel(BndArgs a) {
 }
 
 // surface_kernel launch shape: about TLW_SURF_THREADS threads a CTA (4n flux threads per element); the plain
-// kernel (no boundaries, no blending) capped to TLW_SURF_MINB resident CTAs' registers (5 x 160 threads: 72
-// registers, no spills); TLW_SURF_PREFETCH 1 loads the output face node before the flux phase (more registers).
-// Measured on the 512 x 512, N = 4 vortex: 0.205 ms with (160, 5, 0), 0.232 ms with (160, 1, 1) at 90
-// registers, 0.236 ms with (320, 3, 0), 0.236 ms with (240, 3, 0), 0.216 ms with (120, 6, 0), 0.224 ms with
-// (160, 6, 0); an asynchronous copy of the output face nodes into shared memory during the flux phase: 0.222 ms.
-// The x / y sweeps take 0.236 ms.
+// kernel (no boundaries, no blending) capped to TLW_SURF_MINB resident CTAs' registers when the CTA has at most
+// 128 threads (7 x 128 threads: 72 registers, no spills), 5 otherwise; TLW_SURF_PREFETCH 1 loads the output face
+// node before the flux phase (more registers). Measured on the 512 x 512, N = 4 vortex with one 256-bit access
+// per node record: 0.1836 ms with (120, 7, 0), 0.187 ms with (160, 5, 0), 0.1996 ms with (120, 6, 0); before
+// the wide accesses: 0.205 ms with (160, 5, 0), 0.232 ms with (160, 1, 1) at 90 registers, 0.236 ms with
+// (320, 3, 0) and (240, 3, 0), 0.216 ms with (120, 6, 0), 0.224 ms with (160, 6, 0); an asynchronous copy of the
+// output face nodes into shared memory during the flux phase: 0.222 ms. The x / y sweeps took 0.236 ms.
 #ifndef TLW_SURF_THREADS
-#define TLW_SURF_THREADS 160
+#define TLW_SURF_THREADS 120
 #endif
 #ifndef TLW_SURF_MINB
-#define TLW_SURF_MINB 5
+#define TLW_SURF_MINB 7
 #endif
 #ifndef TLW_SURF_PREFETCH
 #define TLW_SURF_PREFETCH 0
@@ -321,7 +322,7 @@ template <int N> struct SurfCfg {
     static constexpr int EB = (TLW_SURF_THREADS + 4 * n - 1) / (4 * n);
     // whole warps (the face-node maxima are reduced by warp shuffles over full masks)
     static constexpr int THREADS = (EB * 4 * n + 31) / 32 * 32;
-    static constexpr int MIN_BLOCKS = TLW_SURF_MINB;
+    static constexpr int MIN_BLOCKS = THREADS <= 128 ? TLW_SURF_MINB : 5;
 };
 
 // All four faces of each element in one pass, for a mesh whose every face is a conforming interface or a
