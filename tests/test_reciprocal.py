@@ -1,5 +1,5 @@
 """The reciprocal every Euler flux evaluation takes of the density (the hardware approximation refined by
-Newton-Raphson steps, in place of a correctly rounded divide): at most one unit in the last place from IEEE
+one third-order step, in place of a correctly rounded divide): at most one unit in the last place from IEEE
 1/x, over the density range of the workloads (the Riemann states' 0.13 .. 1.5, the vortex core's ~0.1 .. 1)
 and far beyond it, and exact on powers of two."""
 import ctypes

@@ -24,9 +24,33 @@ static __constant__ double c_tlw_D[8][64];
 static __constant__ double c_tlw_Dhat[8][64];
 static __constant__ double c_tlw_Vinv[8][64];
 static __constant__ double c_tlw_w[8][8];       // GLL weights
+// D and Dhat in even-odd form (both are centro-antisymmetric on the symmetric GLL nodes: M[n-1-o][n-1-k] =
+// -M[o][k]), for the line contractions of n >= 5 nodes; with h = n / 2, per matrix:
+//   [0, h*h)        A[o][k] = (M[o][k] + M[o][n-1-k]) / 2      (o, k < h)
+//   [h*h, 2h*h)     B[o][k] = (M[o][k] - M[o][n-1-k]) / 2
+//   [2h*h, 2h*h+h)  M[o][h]                                    (odd n: the middle column)
+//   [2h*h+h, ...)   M[h][k]                                    (odd n: the middle row)
+// so that, with s_k = a_k + a_{n-1-k} and d_k = a_k - a_{n-1-k}, (M a)_o = A s + B d (+ M[o][h] a_h) and
+// (M a)_{n-1-o} = B d - A s (- M[o][h] a_h): 2 h^2 + 2h multiply-adds per line instead of n^2 (Kopriva,
+// Implementing Spectral Methods for PDEs, 2009, even-odd decomposition of the derivative matrix).
+static __constant__ double c_tlw_D_eo[8][64];
+static __constant__ double c_tlw_Dhat_eo[8][64];
+
+static inline void even_odd_form(const double* M, int n, double* out) {
+    const int h = n / 2;
+    for (int o = 0; o < h; ++o)
+        for (int k = 0; k < h; ++k) {
+            out[o * h + k] = 0.5 * (M[o * n + k] + M[o * n + n - 1 - k]);
+            out[h * h + o * h + k] = 0.5 * (M[o * n + k] - M[o * n + n - 1 - k]);
+        }
+    if (n % 2) {
+        for (int o = 0; o < h; ++o) out[2 * h * h + o] = M[o * n + h];
+        for (int k = 0; k < h; ++k) out[2 * h * h + h + k] = M[h * n + k];
+    }
+}
 
 static inline cudaError_t upload_const_basis(const Basis* bases /* [8], index = N */) {
-    static double d[8][64], dh[8][64], vi[8][64], w[8][8];
+    static double d[8][64], dh[8][64], vi[8][64], w[8][8], deo[8][64], dheo[8][64];
     for (int N = 0; N < 8; ++N) {
         for (int k = 0; k < 64; ++k) {
             d[N][k] = bases[N].D[k];
@@ -34,25 +58,43 @@ static inline cudaError_t upload_const_basis(const Basis* bases /* [8], index = 
             vi[N][k] = bases[N].Vinv[k];
         }
         for (int k = 0; k < 8; ++k) w[N][k] = bases[N].weights[k];
+        const int n = N + 1;
+        for (int k = 0; k < 64; ++k) deo[N][k] = dheo[N][k] = 0.0;
+        if (n * n <= 64) {
+            even_odd_form(d[N], n, deo[N]);
+            even_odd_form(dh[N], n, dheo[N]);
+        }
     }
     cudaError_t e = cudaMemcpyToSymbol(c_tlw_D, d, sizeof(d));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_Dhat, dh, sizeof(dh));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_Vinv, vi, sizeof(vi));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_w, w, sizeof(w));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_D_eo, deo, sizeof(deo));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_tlw_Dhat_eo, dheo, sizeof(dheo));
     return e;
 }
 
-// Reciprocal by Newton-Raphson refinement of the hardware approximation (rcp.approx.ftz.f64, about 20
-// correct bits): two steps y <- y + y (1 - x y) square the relative error twice, so the result is within
-// one ulp of 1/x for normal x (Newton's method for f(y) = 1/y - x; e.g. P. Markstein, IBM J. Res. Dev. 34
-// (1990) 111-119). No branch, 1 MUFU + 4 DFMA instead of a correctly rounded divide.
+// Reciprocal by refinement of the hardware approximation (rcp.approx.ftz.f64, about 20 correct bits).
+// With e = 1 - x y the exact reciprocal is y / (1 - e) = y (1 + e + e^2 + ...). TLW_RCP_CUBIC = 1 takes the
+// series to e^2 in one step, y <- y + y (e + e^2), which cubes the relative error (third-order iteration; J.-M.
+// Muller et al., Handbook of Floating-Point Arithmetic, 2010, ch. 5); 0 takes two Newton-Raphson steps
+// y <- y + y e, which square it twice (P. Markstein, IBM J. Res. Dev. 34 (1990) 111-119). Either way the
+// result is within one ulp of 1/x for normal x; no branch, 1 MUFU + 3 (or 4) DFMA instead of a correctly
+// rounded divide.
+#ifndef TLW_RCP_CUBIC
+#define TLW_RCP_CUBIC 1
+#endif
 __device__ __forceinline__ double nr_reciprocal(double x) {
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
     double e = fma(-x, y, 1.0);
+#if TLW_RCP_CUBIC
+    return fma(y, fma(e, e, e), y);
+#else
     y = fma(y, e, y);
     e = fma(-x, y, 1.0);
     return fma(y, e, y);
+#endif
 }
 
 // Euler flux pair (Trixi flux(u, 1|2, eq) for CompressibleEulerEquations2D) from 1/rho; ~17 flops.
